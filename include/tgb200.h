@@ -1,0 +1,155 @@
+/* tgb200 - a B200 (sm_100a) CUDA backend for TerrainGen's per-cell terrain evaluation path.
+ *
+ * The C ABI of libtgb200.so: plain pointers, sizes and status codes, no C++ or torch types. It is
+ * the boundary the reference's GPU backend interface crosses today (src/gpu/kernel.h:46
+ * `RunKernel`, src/gpu/device.h:49-68 `ComputeDevice`, `GpuDevice`), plus the hooks for the three
+ * stages the reference runs only on the CPU (boulder baking, diamond-square refinement, the seam
+ * solve). Each entry point names the reference interface it replaces.
+ *
+ * Parameter blocks are passed as the reference's own std430 bytes (`NoiseLayerKernel` 420 B,
+ * `CraterShapeKernel` 188 B, `CraterRecord` 144 B each), exactly what its host code already
+ * builds for RunKernel; sizes are checked.
+ *
+ * Memory: every compute entry point takes `memory`. With TG_MEMORY_HOST its buffers are host
+ * memory, copied to the device and back inside the call, which returns when the result is in
+ * place (RunKernel's contract). With TG_MEMORY_DEVICE they are device pointers and the work is
+ * ordered on `stream` (a cudaStream_t; NULL for the device's own stream); the call may return
+ * before the work finishes.
+ *
+ * Errors: a nonzero tg_status; tg_last_error() gives the message of the calling thread's last
+ * failure. A device is thread-safe: calls on one device are serialized, as the reference's runs
+ * are (src/gpu/cuda.cpp:303).
+ */
+#ifndef TGB200_H
+#define TGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TGB200_ABI_VERSION 1
+
+typedef struct tg_device tg_device;
+
+typedef enum tg_status {
+    TG_OK = 0,
+    TG_ERROR_ARGUMENT = 1,    /* a size, pointer or value is out of range */
+    TG_ERROR_CUDA = 2,        /* the CUDA runtime failed; the message says how */
+    TG_ERROR_UNSUPPORTED = 3, /* valid input this backend does not run (the caller's CPU path
+                                 should take it, as RunKernel returning false asks) */
+    TG_ERROR_MEMORY = 4,      /* a device allocation failed or a budget was exceeded */
+    TG_ERROR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    TG_ERROR_STATE = 6        /* the call does not fit the object's state */
+} tg_status;
+
+enum { TG_MEMORY_HOST = 0, TG_MEMORY_DEVICE = 1 };
+
+/* A north-up grid: the reference's GeoTransform coefficients in GDAL order
+ * (include/terraingen/raster/geo_transform.h:17-35). Cell (col, row) is centered at
+ * origin_x + (col + 0.5) * pixel_width, origin_y + (row + 0.5) * pixel_height. Rotated grids
+ * (nonzero rotation terms) are TG_ERROR_UNSUPPORTED, as RunKernel refuses them
+ * (src/gpu/kernel.cpp:44-48). Heights are row-major, row 0 first. */
+typedef struct tg_grid {
+    uint32_t width;
+    uint32_t height;
+    double origin_x;
+    double pixel_width;
+    double row_rotation;
+    double origin_y;
+    double col_rotation;
+    double pixel_height;
+} tg_grid;
+
+/* No-data marking of a grid (src/gpu/kernel.cpp:28-31, Raster::NoData): mode 0 none, 1 NaN,
+ * 2 `value`. Cells holding no-data are left as they are. */
+typedef struct tg_nodata {
+    uint32_t mode;
+    float value;
+} tg_nodata;
+
+/* --- device ------------------------------------------------------------------------------- */
+
+/* Opens CUDA device `ordinal` (replaces CudaCompute::Open / GpuDevice(Backend::Cuda),
+ * src/gpu/cuda.cpp:188-240, src/gpu/device.h:68). Fails with TG_ERROR_UNSUPPORTED on a device
+ * that is not sm_100. */
+int tg_open(int ordinal, tg_device** device);
+/* Releases the device's memory and stream. */
+void tg_close(tg_device* device);
+/* The message of the calling thread's last failure; "" when none. */
+const char* tg_last_error(void);
+/* ComputeDevice::DeviceName (src/gpu/device.h:41). */
+int tg_device_name(tg_device* device, char* name, size_t capacity);
+/* Waits for the device's stream. */
+int tg_synchronize(tg_device* device);
+
+/* --- noise (fBm sources and layers) --------------------------------------------------------- */
+
+/* NoiseLayer on a grid: heights += the stacked fractals of the 420-byte `NoiseLayerKernel` at each
+ * cell center measured from (origin_x, origin_y), cells holding no-data skipped. Replaces
+ * RunKernel(backend, CompiledKernel<NoiseLayerKernel>(), kernel, grid, origin)
+ * (src/layers/noise_layer.cpp:113-117; kernel src/layers/kernels/noise_layer.slang). Bit-exact
+ * with the reference CPU path (AddNoiseRows, noise_layer.cpp:28). */
+int tg_noise_layer(tg_device* device, const void* kernel, size_t kernel_bytes,
+                   const tg_grid* grid, double origin_x, double origin_y, float* heights,
+                   tg_nodata nodata, int memory, void* stream);
+
+/* The same over RunKernel's strip buffers (src/gpu/kernel.cpp:98-111): per-column `xs` and
+ * per-row `ys` positions, `rows` rows of `width` heights. */
+int tg_noise_layer_rows(tg_device* device, const void* kernel, size_t kernel_bytes,
+                        const float* xs, const float* ys, uint32_t width, uint32_t rows,
+                        float* heights, tg_nodata nodata, int memory, void* stream);
+
+/* SyntheticSource without posts on a grid: heights = elevation + the stacked `fractals` (`count`
+ * 52-byte `Fractal`s, at most 8, disabled ones skipped) at each cell center. Replaces
+ * SyntheticSource::FillSamples (src/sources/synthetic_source.cpp:87-95), which the reference runs
+ * only on the CPU. Bit-exact with it. */
+int tg_noise_source(tg_device* device, const void* fractals, uint32_t count, float elevation,
+                    const tg_grid* grid, float* heights, int memory, void* stream);
+
+/* Conformance probe, the analogue of the reference's GPU test kernel
+ * (tests/unit/gpu/kernels/noise_conformance.slang): for each of `n` points (x, y) in `xy`,
+ * hashes[4i..4i+3] = PcgHash(i), Pcg3dHash(bits(x), bits(y), seed), and values[12i..12i+11] =
+ * Perlin, simplex, value, Worley F1, F2, cell value, Perlin fBm / ridged / billow / hybrid
+ * (wavelength 1000, amplitude 100, 8 octaves), 3D Perlin at (x, y, (x - y) / 2) and
+ * Fractal3Float at (x, y, x / 4) with 3 octaves. */
+int tg_noise_probe(tg_device* device, const float* xy, uint32_t n, uint32_t seed,
+                   uint32_t* hashes, float* values, int memory);
+
+/* --- craters ------------------------------------------------------------------------------ */
+
+/* ApplyCraters' shaping on a plane grid: each cell holding data gets each crater of `records`
+ * (`n` 144-byte `CraterRecord`s, with `data` their `n_data` variable-length floats) shaped by the
+ * 188-byte `CraterShapeKernel`, at every cell of each 16x16 tile the crater's footprint touches,
+ * as ShapeTilesOnCpu / ShapeTilesOnGpu do (src/layers/craters/shaping/apply.cpp:174-222). The
+ * binning the reference does on the host (TileLists, apply.cpp:119) runs on the device.
+ * `footprints` (optional; 3 doubles per crater: center x, y and reach in meters, as
+ * CraterReach gives it) makes the footprint windows exactly the reference's; without it they
+ * follow from the records. Craters with a datum are TG_ERROR_UNSUPPORTED here (their blend reads
+ * the running height in apply order; tg_craters_apply_lists takes them). */
+int tg_craters_apply(tg_device* device, const void* kernel, size_t kernel_bytes,
+                     const void* records, uint32_t n, const float* data, uint32_t n_data,
+                     const double* footprints, const tg_grid* grid, float* heights,
+                     tg_nodata nodata, int memory, void* stream);
+
+/* The drop-in strip form of the reference's crater kernel (src/layers/kernels/craters.slang,
+ * bound by ShapeTilesOnGpu, apply.cpp:174-196): the host's tile lists `heads` (tiles across,
+ * tile side, 0 for a plane, then first entry and count per tile) and `entries`, column
+ * positions `xs` / `x_lows` [width] and row positions `ys` [rows] / `y_lows` [first_row + rows]
+ * as MakeCellPositions builds them (apply.cpp:149-170). Craters apply in list order, datums
+ * included. */
+int tg_craters_apply_lists(tg_device* device, const void* kernel, size_t kernel_bytes,
+                           const void* records, uint32_t n, const float* data, uint32_t n_data,
+                           const uint32_t* heads, uint32_t n_heads, const uint32_t* entries,
+                           uint32_t n_entries, const float* xs, const float* x_lows,
+                           const float* ys, const float* y_lows, uint32_t width, uint32_t rows,
+                           uint32_t first_row, float* heights, tg_nodata nodata, int memory,
+                           void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TGB200_H */

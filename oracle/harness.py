@@ -1,0 +1,204 @@
+"""ctypes access to the oracle: test infrastructure only.
+
+The product never imports this module. Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline / reference legs use it, as the checker and the CPU baseline.
+
+  - `restate()`  - oracle/_ref/libtgrestate.so, the FP32/FP64 restatement (oracle/restate.cpp);
+  - `reference()` - oracle/_ref/libtgref.so, the reference CPU path built from its own sources;
+  - `capture()`  - oracle/_ref/libtgref_capture.so, the reference pipeline recording what it hands
+                   its GPU backend through the product's drop-in device;
+  - `dropin()`   - oracle/_ref/libtgref_cuda.so, the reference pipeline on libtgb200 (GPU).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE / "_ref"
+
+_U32, _I32, _F, _D = C.c_uint32, C.c_int32, C.c_float, C.c_double
+
+
+class Scene(C.Structure):
+    """`tgref_scene` (oracle/ref_harness.cpp)."""
+
+    _fields_ = [
+        ("width", _U32), ("height", _U32), ("transform", _D * 6),
+        ("source", _I32), ("elevation", _F), ("sourceFractals", _U32),
+        ("sourceStack", C.c_ubyte * (52 * 8)),
+        ("layerFractals", _U32), ("layerStack", C.c_ubyte * (52 * 8)),
+        ("craters", _I32), ("seed", _U32),
+        ("sfdCoefficient", _D), ("sfdExponent", _D), ("minDiameter", _D), ("maxDiameter", _D),
+        ("lifetimeGyr", _D), ("depthRatio", _D), ("rimRatio", _D),
+        ("profile", _I32), ("transitionDiameter", _D), ("applyPreset", _I32),
+        ("noiseAmplitude", _D), ("rimNoiseAmplitude", _D), ("wallStreaks", _D), ("ejecta", _D),
+        ("rimSigma", _D), ("terraceOnset", _D), ("terraceFull", _D),
+    ]
+
+
+def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, craters=None):
+    """A Scene on `grid` (terraingen_b200.GridSpec). `craters` is a dict of crater-layer fields
+    (seed, sfdCoefficient, sfdExponent, minDiameter, maxDiameter, lifetimeGyr, depthRatio,
+    rimRatio, profile, transitionDiameter, applyPreset, noiseAmplitude, ...)."""
+    s = Scene()
+    s.width, s.height = grid.width, grid.height
+    for i, v in enumerate(grid.transform()):
+        s.transform[i] = v
+    s.elevation = elevation
+    if source_fractals is not None:
+        fr = np.atleast_1d(source_fractals)
+        s.source = 1
+        s.sourceFractals = len(fr)
+        C.memmove(s.sourceStack, fr.tobytes(), fr.nbytes)
+    if layer_fractals is not None:
+        fr = np.atleast_1d(layer_fractals)
+        s.layerFractals = len(fr)
+        C.memmove(s.layerStack, fr.tobytes(), fr.nbytes)
+    if craters is not None:
+        s.craters = 1
+        defaults = dict(seed=1, sfdCoefficient=1e-3, sfdExponent=2.0, minDiameter=2.0,
+                        maxDiameter=60.0, lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04,
+                        profile=0, transitionDiameter=15000.0, applyPreset=0,
+                        noiseAmplitude=0.0, rimNoiseAmplitude=0.0, wallStreaks=0.0, ejecta=0.0,
+                        rimSigma=0.0, terraceOnset=0.0, terraceFull=0.0)
+        defaults.update(craters)
+        for k, v in defaults.items():
+            setattr(s, k, v)
+    return s
+
+
+def config1_craters() -> dict:
+    """The 257 x 257, 1 m crater scene (2000 craters expected over the extent, N(>D) ~ D^-2 on
+    [2, 60] m, depth/diameter 0.2, rim 0.04 D, uniform ages over 1 Gyr, seed 1)."""
+    area = 257.0 * 257.0
+    c = 2000.0 / (area * (2.0 ** -2.0 - 60.0 ** -2.0))
+    return dict(seed=1, sfdCoefficient=c, sfdExponent=2.0, minDiameter=2.0, maxDiameter=60.0,
+                lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04, profile=0, applyPreset=0)
+
+
+def build(target: str = "all") -> None:
+    """Builds oracle/_ref (needs the reference sources; the restatement needs none)."""
+    subprocess.run(["make", "-C", str(HERE), "-j8", target], check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+_libs: dict = {}
+
+
+def _load(name: str) -> C.CDLL:
+    if name not in _libs:
+        path = REF / name
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is not built (make -C oracle)")
+        _libs[name] = C.CDLL(str(path))
+    return _libs[name]
+
+
+def available(name: str) -> bool:
+    return (REF / name).exists()
+
+
+def restate() -> C.CDLL:
+    lib = _load("libtgrestate.so")
+    lib.rs_pcg.restype = _U32
+    lib.rs_pcg.argtypes = [_U32]
+    lib.rs_pcg3d.argtypes = [_U32, _U32, _U32, C.c_void_p]
+    lib.rs_perlin2_f32.restype = _F
+    lib.rs_perlin2_f32.argtypes = [_F, _F, _U32]
+    lib.rs_perlin2_f64.restype = _D
+    lib.rs_perlin2_f64.argtypes = [_D, _D, _U32]
+    lib.rs_fbm2_f32.restype = _F
+    lib.rs_fbm2_f32.argtypes = [_F, _F, _U32, _F, _F, C.c_int, _F, _F]
+    lib.rs_fbm2_f64.restype = _D
+    lib.rs_fbm2_f64.argtypes = [_D, _D, _U32, _D, _D, C.c_int, _D, _D]
+    lib.rs_fbm_grid_f32.argtypes = [_U32, _U32, _D, _D, _D, _U32, _F, _F, C.c_int, _F, _F, _F,
+                                    C.c_void_p]
+    lib.rs_fbm_grid_f64.argtypes = [_U32, _U32, _D, _D, _D, _U32, _D, _D, C.c_int, _D, _D, _D,
+                                    C.c_void_p]
+    lib.rs_crater_profile_f64.restype = _D
+    lib.rs_crater_profile_f64.argtypes = [C.c_int, _U32, _D, _D, _D, _D, _D, _D]
+    return lib
+
+
+def _harness(name: str) -> C.CDLL:
+    lib = _load(name)
+    lib.tgref_evaluate.argtypes = [C.POINTER(Scene), C.c_int, C.c_uint, C.c_void_p,
+                                   C.POINTER(_D)]
+    lib.tgref_evaluate.restype = C.c_int
+    lib.tgref_error.restype = C.c_char_p
+    lib.tgref_craters.argtypes = [C.POINTER(Scene), C.c_void_p, _D, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
+    lib.tgref_craters.restype = C.c_long
+    return lib
+
+
+def reference() -> C.CDLL:
+    return _harness("libtgref.so")
+
+
+def dropin() -> C.CDLL:
+    return _harness("libtgref_cuda.so")
+
+
+def capture() -> C.CDLL:
+    lib = _harness("libtgref_capture.so")
+    lib.tgref_capture_count.restype = C.c_int
+    lib.tgref_capture_info.argtypes = [C.c_int, C.c_void_p]
+    lib.tgref_capture_field.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_size_t)]
+    return lib
+
+
+def evaluate(lib: C.CDLL, scene: Scene, backend: int = 0, threads: int = 0):
+    """(heights [height, width] float32, milliseconds) from the harness `lib`."""
+    out = np.zeros((scene.height, scene.width), np.float32)
+    ms = _D()
+    if lib.tgref_evaluate(C.byref(scene), backend, threads, out.ctypes.data, C.byref(ms)) != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return out, ms.value
+
+
+def craters(lib: C.CDLL, scene: Scene, region, spacing: float = 0.0) -> dict:
+    """The crater population the scene's layer generates over region (x0, y0, x1, y1)."""
+    reg = np.asarray(region, np.float64)
+    n = lib.tgref_craters(C.byref(scene), reg.ctypes.data, spacing, None, None, None, None, None,
+                          0)
+    if n < 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    out = {k: np.zeros(n, np.float64) for k in ("x", "y", "diameter", "age")}
+    out["id"] = np.zeros(n, np.uint64)
+    lib.tgref_craters(C.byref(scene), reg.ctypes.data, spacing, out["x"].ctypes.data,
+                      out["y"].ctypes.data, out["diameter"].ctypes.data, out["age"].ctypes.data,
+                      out["id"].ctypes.data, n)
+    return out
+
+
+CRATER_FIELDS = ["kernel", "records", "data", "heads", "entries", "xs", "x_lows", "ys", "y_lows",
+                 "heights"]
+NOISE_FIELDS = ["kernel", "xs", "ys", "heights"]
+
+
+def captured(lib: C.CDLL) -> list:
+    """Every captured backend call as a dict of numpy arrays."""
+    calls = []
+    for call in range(lib.tgref_capture_count()):
+        info = np.zeros(8, np.uint32)
+        lib.tgref_capture_info(call, info.ctypes.data)
+        kind = int(info[0])
+        names = CRATER_FIELDS if kind == 2 else NOISE_FIELDS
+        rec = {"kind": kind, "width": int(info[1]), "rows": int(info[2]),
+               "first_row": int(info[3]), "nodata_mode": int(info[4]),
+               "nodata_value": float(info[5:6].view(np.float32)[0])}
+        for f, name in enumerate(names):
+            ptr, size = C.c_void_p(), C.c_size_t()
+            lib.tgref_capture_field(call, f, C.byref(ptr), C.byref(size))
+            buf = (C.c_ubyte * size.value).from_address(ptr.value) if size.value else b""
+            rec[name] = np.frombuffer(bytes(buf), np.uint8).copy()
+        calls.append(rec)
+    lib.tgref_capture_clear()
+    return calls

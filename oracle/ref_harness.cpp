@@ -1,0 +1,324 @@
+// Oracle harness: the reference TerrainGen pipeline behind a small C ABI, for tests only.
+//
+// Built three ways by oracle/Makefile, all from the reference's own sources:
+//   libtgref.so         - the reference CPU path (`tgref_evaluate` with backend 0);
+//   libtgref_capture.so - the reference pipeline with Backend::Cuda routed through the product's
+//                         drop-in CudaCompute (terraingen_b200/adapter/cuda_compute.cpp), whose
+//                         tg_* calls land in the capture stubs below: they record exactly what
+//                         the reference hands its GPU backend (kernel bytes, crater records,
+//                         tile lists, positions) and leave the heights as they were. Runs
+//                         without a GPU; tests/golden/make_fixtures.py stores the captures;
+//   libtgref_cuda.so    - the same pipeline with the adapter linked to libtgb200.so, so
+//                         Backend::Cuda runs the product's kernels inside the reference's
+//                         Terrain::Evaluate (GPU parity tests).
+#include "terraingen/terraingen.h"
+
+#include "terraingen/distribution/power_law.h"
+#include "terraingen/layers/craters/degradation/diffusion.h"
+#include "terraingen/layers/craters/degradation/diffusivities.h"
+#include "terraingen/layers/craters/degradation/freshness_degradation.h"
+#include "terraingen/layers/craters/profiles/complex.h"
+#include "terraingen/layers/craters/profiles/fassett_thomson.h"
+#include "terraingen/layers/craters/profiles/martin_parkes_dunstan.h"
+#include "terraingen/layers/craters/shaping/morphometry.h"
+#include "terraingen/util/log.h"
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace terraingen;
+
+namespace {
+
+thread_local std::string g_error;
+
+}  // namespace
+
+extern "C" {
+
+/// One scene: a grid, a source and up to one noise layer and one crater layer.
+struct tgref_scene {
+    uint32_t width, height;
+    double transform[6];  // GDAL order: origin x, pixel width, 0, origin y, 0, pixel height
+    // source: 0 flat, 1 synthetic fractal stack
+    int32_t source;
+    float elevation;
+    uint32_t sourceFractals;
+    Fractal sourceStack[8];
+    // noise layer (none when 0 fractals)
+    uint32_t layerFractals;
+    Fractal layerStack[8];
+    // crater layer (none when craters == 0)
+    int32_t craters;
+    uint32_t seed;
+    double sfdCoefficient, sfdExponent, minDiameter, maxDiameter;
+    double lifetimeGyr, depthRatio, rimRatio;
+    // 0 Fassett-Thomson, 1 Martin-Parkes-Dunstan, 2 complex over FT (lunar shape with
+    // transitionDiameter), 3 diffused MPD with matched diffusion (the reference's default models)
+    int32_t profile;
+    double transitionDiameter;
+    // 0 DefaultCraterApply (irregular outlines, terraces, peaks), 1 plain CraterApplyOptions
+    int32_t applyPreset;
+    double noiseAmplitude, rimNoiseAmplitude, wallStreaks, ejecta, rimSigma;
+    double terraceOnset, terraceFull;
+};
+
+const char* tgref_error() {
+    return g_error.c_str();
+}
+
+}  // extern "C"
+
+namespace {
+
+std::vector<Fractal> Stack(const Fractal* fractals, uint32_t count) {
+    return std::vector<Fractal>(fractals, fractals + count);
+}
+
+std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s) {
+    auto density = std::make_shared<PowerLawSfd>(s.sfdCoefficient, s.sfdExponent, SfdKind::Density,
+                                                  DiameterRange{s.minDiameter, s.maxDiameter});
+    CraterModels models;
+    models.density = density;
+    const double depth = s.depthRatio, rim = s.rimRatio;
+    FreshMorphometry fresh = [depth, rim](double) { return CraterMorphometry{depth, rim}; };
+    if (s.profile == 3) {
+        // The reference's default models (steady-state ages, matched diffusion of diffused MPD
+        // profiles) on the scene's density.
+        CraterModels defaults = DefaultCraterModels();
+        defaults.density = density;
+        models = defaults;
+    } else {
+        auto ages = std::make_shared<UniformAges>(s.lifetimeGyr);
+        models.ages = ages;
+        models.degradation = std::make_shared<FreshnessDegradation>(ages, fresh);
+        std::shared_ptr<const CraterProfile> simple;
+        if (s.profile == 1) {
+            simple = std::make_shared<MartinParkesDunstanProfile>();
+        } else {
+            simple = std::make_shared<FassettThomsonProfile>();
+        }
+        if (s.profile == 2) {
+            ComplexCraterShape shape = LunarComplexCraterShape();
+            shape.transitionDiameter = s.transitionDiameter;
+            models.profile = std::make_shared<ComplexCraterProfile>(simple, shape);
+        } else {
+            models.profile = simple;
+        }
+    }
+    CraterLayerOptions options;
+    options.seed = s.seed;
+    options.generation.minDiameter = s.minDiameter;
+    options.generation.maxDiameter = s.maxDiameter;
+    if (s.applyPreset == 1) {
+        options.apply = CraterApplyOptions{};
+    }
+    options.apply.noise.amplitude = s.noiseAmplitude;
+    options.apply.noise.rimAmplitude = s.rimNoiseAmplitude;
+    options.apply.texture.wallStreaks = s.wallStreaks;
+    options.apply.texture.ejecta = s.ejecta;
+    options.apply.rimSmoothing.sigmaRadii = s.rimSigma;
+    if (s.terraceOnset > 0.0) {
+        options.apply.terraces.onsetDiameter = s.terraceOnset;
+        options.apply.terraces.fullDiameter = s.terraceFull;
+    }
+    return std::make_shared<CraterLayer>(std::move(models), std::move(options));
+}
+
+Terrain MakeTerrain(const tgref_scene& s) {
+    std::shared_ptr<const Source> source;
+    if (s.source == 1) {
+        source = std::make_shared<SyntheticSource>(Stack(s.sourceStack, s.sourceFractals),
+                                                   s.elevation);
+    } else {
+        source = std::make_shared<FlatSource>(s.width, s.height,
+                                              std::fabs(s.transform[1]), s.elevation);
+    }
+    std::vector<LayerPtr> layers;
+    if (s.layerFractals > 0) {
+        NoiseLayerOptions options;
+        options.fractals = Stack(s.layerStack, s.layerFractals);
+        options.sourceResolvesPixels = std::nullopt;
+        layers.push_back(std::make_shared<NoiseLayer>(options));
+    }
+    if (s.craters != 0) {
+        layers.push_back(MakeCraterLayer(s));
+    }
+    return Terrain(Surface{}, source, layers);
+}
+
+}  // namespace
+
+extern "C" {
+
+/// Evaluates the scene's grid on the CPU (backend 0) or on Backend::Cuda (backend 1) with
+/// `threads` threads (0: every core); heights into `out` (width x height floats). `ms` gets the
+/// wall time of the evaluation alone. Returns 0, or -1 with tgref_error() set.
+int tgref_evaluate(const tgref_scene* s, int backend, unsigned threads, float* out, double* ms) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const Terrain terrain = MakeTerrain(*s);
+        const GeoTransform transform = GeoTransform::FromGdal(
+            {s->transform[0], s->transform[1], s->transform[2], s->transform[3], s->transform[4],
+             s->transform[5]});
+        const RasterGrid grid{s->width, s->height, transform};
+        EvaluationOptions options;
+        options.threads = threads;
+        options.backend = backend == 1 ? Backend::Cuda : Backend::Cpu;
+        const auto t0 = std::chrono::steady_clock::now();
+        const Raster<float> heights = terrain.Evaluate(grid, options);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (ms != nullptr) {
+            *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        }
+        std::memcpy(out, heights.Values().data(), heights.Values().size() * sizeof(float));
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// The number of craters the scene's crater layer generates over `region`
+/// (x0, y0, x1, y1 in meters), and their centers, diameters and ids into the arrays when given
+/// (capacity `n`).
+long tgref_craters(const tgref_scene* s, const double* region, double spacing, double* x,
+                   double* y, double* diameter, double* age, uint64_t* id, long n) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const auto layer = MakeCraterLayer(*s);
+        const CraterList list =
+            layer->Craters({region[0], region[1], region[2], region[3]}, spacing);
+        const long count = static_cast<long>(list.Size());
+        for (long i = 0; i < count && i < n; ++i) {
+            const Crater c = list.At(static_cast<std::size_t>(i));
+            if (x) x[i] = c.x;
+            if (y) y[i] = c.y;
+            if (diameter) diameter[i] = c.diameter;
+            if (age) age[i] = c.ageGyr;
+            if (id) id[i] = c.id;
+        }
+        return count;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+}  // extern "C"
+
+#ifdef TGREF_CAPTURE
+// --- capture stubs for the tg_* C ABI the adapter calls ------------------------------------
+#include "tgb200.h"
+
+namespace {
+
+struct Capture {
+    int kind = 0;  // 1 noise layer rows, 2 crater lists
+    std::vector<std::vector<unsigned char>> fields;
+    uint32_t width = 0, rows = 0, firstRow = 0;
+    tg_nodata nodata{};
+};
+
+std::vector<Capture> g_captures;
+
+template <typename T> std::vector<unsigned char> Bytes(const T* p, size_t count) {
+    const auto* b = reinterpret_cast<const unsigned char*>(p);
+    return std::vector<unsigned char>(b, b + count * sizeof(T));
+}
+
+}  // namespace
+
+struct tg_device {
+    int unused;
+};
+
+extern "C" {
+
+int tg_open(int, tg_device** device) {
+    static tg_device one{};
+    *device = &one;
+    return TG_OK;
+}
+void tg_close(tg_device*) {}
+const char* tg_last_error(void) {
+    return "";
+}
+int tg_device_name(tg_device*, char* name, size_t capacity) {
+    std::snprintf(name, capacity, "capture");
+    return TG_OK;
+}
+
+int tg_noise_layer_rows(tg_device*, const void* kernel, size_t kernelBytes, const float* xs,
+                        const float* ys, uint32_t width, uint32_t rows, float* heights,
+                        tg_nodata nodata, int, void*) {
+    Capture c;
+    c.kind = 1;
+    c.fields = {Bytes(static_cast<const unsigned char*>(kernel), kernelBytes), Bytes(xs, width),
+                Bytes(ys, rows), Bytes(heights, size_t(width) * rows)};
+    c.width = width;
+    c.rows = rows;
+    c.nodata = nodata;
+    g_captures.push_back(std::move(c));
+    return TG_OK;
+}
+
+int tg_craters_apply_lists(tg_device*, const void* kernel, size_t kernelBytes, const void* records,
+                           uint32_t n, const float* data, uint32_t nData, const uint32_t* heads,
+                           uint32_t nHeads, const uint32_t* entries, uint32_t nEntries,
+                           const float* xs, const float* xLows, const float* ys,
+                           const float* yLows, uint32_t width, uint32_t rows, uint32_t firstRow,
+                           float* heights, tg_nodata nodata, int, void*) {
+    Capture c;
+    c.kind = 2;
+    c.fields = {Bytes(static_cast<const unsigned char*>(kernel), kernelBytes),
+                Bytes(static_cast<const unsigned char*>(records), size_t(n) * 144),
+                Bytes(data, nData),
+                Bytes(heads, nHeads),
+                Bytes(entries, nEntries),
+                Bytes(xs, width),
+                Bytes(xLows, width),
+                Bytes(ys, rows),
+                Bytes(yLows, size_t(firstRow) + rows),
+                Bytes(heights, size_t(width) * rows)};
+    c.width = width;
+    c.rows = rows;
+    c.firstRow = firstRow;
+    c.nodata = nodata;
+    g_captures.push_back(std::move(c));
+    return TG_OK;
+}
+
+/// Captured calls so far.
+int tgref_capture_count() {
+    return static_cast<int>(g_captures.size());
+}
+void tgref_capture_clear() {
+    g_captures.clear();
+}
+/// Call `call`'s kind, strip geometry and nodata marking.
+int tgref_capture_info(int call, uint32_t* info) {
+    const Capture& c = g_captures.at(static_cast<size_t>(call));
+    info[0] = static_cast<uint32_t>(c.kind);
+    info[1] = c.width;
+    info[2] = c.rows;
+    info[3] = c.firstRow;
+    info[4] = c.nodata.mode;
+    std::memcpy(info + 5, &c.nodata.value, sizeof(float));
+    info[6] = static_cast<uint32_t>(c.fields.size());
+    return 0;
+}
+/// Field `field` of call `call`: its bytes and size.
+int tgref_capture_field(int call, int field, const void** data, size_t* bytes) {
+    const Capture& c = g_captures.at(static_cast<size_t>(call));
+    const auto& f = c.fields.at(static_cast<size_t>(field));
+    *data = f.data();
+    *bytes = f.size();
+    return 0;
+}
+
+}  // extern "C"
+#endif

@@ -1,0 +1,92 @@
+"""ctypes bindings of libtgb200.so (include/tgb200.h).
+
+Loading fails loudly: there is no CPU fallback, so a missing or unloadable library is an error
+the caller sees, never a silent change of code path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIBRARY = Path(__file__).resolve().parent / "lib" / "libtgb200.so"
+
+TG_MEMORY_HOST = 0
+TG_MEMORY_DEVICE = 1
+
+STATUS = {0: "ok", 1: "argument", 2: "cuda", 3: "unsupported", 4: "memory", 5: "timeout",
+          6: "state"}
+
+
+class TgError(RuntimeError):
+    """A tg_* call failed; `status` is its tg_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class Grid(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("origin_x", C.c_double),
+                ("pixel_width", C.c_double), ("row_rotation", C.c_double),
+                ("origin_y", C.c_double), ("col_rotation", C.c_double),
+                ("pixel_height", C.c_double)]
+
+
+class NoData(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("value", C.c_float)]
+
+
+_P = C.c_void_p
+_U32 = C.c_uint32
+_SZ = C.c_size_t
+_I = C.c_int
+_D = C.c_double
+_F = C.c_float
+
+# name -> argument types; every function returns int except where noted.
+SIGNATURES = {
+    "tg_open": [_I, C.POINTER(_P)],
+    "tg_close": [_P],
+    "tg_last_error": [],
+    "tg_device_name": [_P, C.c_char_p, _SZ],
+    "tg_synchronize": [_P],
+    "tg_noise_layer": [_P, _P, _SZ, C.POINTER(Grid), _D, _D, _P, NoData, _I, _P],
+    "tg_noise_layer_rows": [_P, _P, _SZ, _P, _P, _U32, _U32, _P, NoData, _I, _P],
+    "tg_noise_source": [_P, _P, _U32, _F, C.POINTER(Grid), _P, _I, _P],
+    "tg_noise_probe": [_P, _P, _U32, _U32, _P, _P, _I],
+    "tg_craters_apply": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, C.POINTER(Grid), _P, NoData, _I,
+                         _P],
+    "tg_craters_apply_lists": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _P, _P,
+                               _P, _U32, _U32, _U32, _P, NoData, _I, _P],
+}
+RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p}
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """The loaded libtgb200.so, with argument types set; raises if it cannot be loaded."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise RuntimeError(
+                f"{LIBRARY} is missing: build it with `python -m terraingen_b200.build` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(str(LIBRARY))
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = RESTYPES.get(name, C.c_int)
+        _lib = lib
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    """The C ABI names the header declares (every one must be exported)."""
+    return list(SIGNATURES)
+
+
+def check(status: int) -> None:
+    if status != 0:
+        raise TgError(status, library().tg_last_error().decode())

@@ -1,0 +1,140 @@
+// TerrainGen's CUDA device on libtgb200: a drop-in replacement for the reference's
+// src/gpu/cuda.cpp, implementing the same `CudaCompute` (src/gpu/cuda.h) over the C ABI in
+// include/tgb200.h.
+//
+// Built inside a TerrainGen tree in place of src/gpu/cuda.cpp, it makes
+// Backend::Cuda run the noise-layer and crater kernels on the B200 kernels of libtgb200 instead of
+// JIT-compiled Slang PTX: RunKernel (src/gpu/kernel.cpp) binds the same buffers and push
+// constants, and this device maps them onto tg_noise_layer_rows and tg_craters_apply_lists.
+// Programs are told apart by their compiled form's address, so the generated CompiledKernel<>
+// definitions (cmake/Kernel.cpp.in) are used as they are; PTX is not read.
+#include "gpu/cuda.h"
+
+#include "terraingen/layers/kernels/craters.h"
+#include "terraingen/layers/kernels/noise_layer.h"
+#include "tgb200.h"
+
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+namespace terraingen {
+
+namespace {
+
+/// The push constants RunKernel passes (src/gpu/kernel.cpp:34-40).
+struct Params {
+    std::uint32_t width;
+    std::uint32_t rows;
+    std::uint32_t noData;
+    float noDataValue;
+    std::uint32_t firstRow;
+};
+
+enum class Program { None, NoiseLayer, Craters };
+
+/// Whether `program` is the compiled form of kernel `Kernel`.
+template <typename Kernel> bool Is(const KernelProgram& program) {
+    const KernelProgram compiled = CompiledKernel<Kernel>();
+    return program.ptx.data() == compiled.ptx.data() &&
+           program.spirv.data() == compiled.spirv.data();
+}
+
+Program Identify(const KernelProgram& program) {
+    if (Is<NoiseLayerKernel>(program)) {
+        return Program::NoiseLayer;
+    }
+    if (Is<CraterShapeKernel>(program)) {
+        return Program::Craters;
+    }
+    return Program::None;
+}
+
+[[noreturn]] void Throw(const char* what) {
+    throw std::runtime_error(std::string("tgb200 ") + what + ": " + tg_last_error());
+}
+
+template <typename T> const T* As(const DeviceBuffer& buffer) {
+    return reinterpret_cast<const T*>(buffer.bytes.data());
+}
+
+template <typename T> std::uint32_t Count(const DeviceBuffer& buffer) {
+    return static_cast<std::uint32_t>(buffer.bytes.size() / sizeof(T));
+}
+
+}  // namespace
+
+struct CudaCompute::State {
+    tg_device* device = nullptr;
+    std::string name;
+};
+
+CudaCompute::CudaCompute(std::unique_ptr<State> state) : m_state(std::move(state)) {}
+
+CudaCompute::~CudaCompute() {
+    if (m_state && m_state->device != nullptr) {
+        tg_close(m_state->device);
+    }
+}
+
+std::unique_ptr<CudaCompute> CudaCompute::Open() {
+    auto state = std::make_unique<State>();
+    if (tg_open(0, &state->device) != TG_OK) {
+        throw std::runtime_error(std::string("tgb200: ") + tg_last_error());
+    }
+    char name[256] = {};
+    tg_device_name(state->device, name, sizeof(name));
+    state->name = std::string(name) + " (tgb200)";
+    return std::unique_ptr<CudaCompute>(new CudaCompute(std::move(state)));
+}
+
+const std::string& CudaCompute::DeviceName() const {
+    return m_state->name;
+}
+
+bool CudaCompute::CanRun(const KernelProgram& program) const {
+    return Identify(program) != Program::None;
+}
+
+void CudaCompute::Run(const KernelProgram& program, Span<const DeviceBuffer> buffers,
+                      Span<const std::byte> pushConstants, const Dispatch& /*dispatch*/) {
+    if (pushConstants.size() < sizeof(Params)) {
+        throw std::runtime_error("tgb200: push constants are not RunKernel's");
+    }
+    Params params;
+    std::memcpy(&params, pushConstants.data(), sizeof(params));
+    const tg_nodata nodata{params.noData, params.noDataValue};
+    const Program kind = Identify(program);
+    if (kind == Program::NoiseLayer && buffers.size() >= 4) {
+        // heights, xs, ys, NoiseLayerKernel (src/layers/kernels/noise_layer.slang)
+        float* heights = reinterpret_cast<float*>(buffers[0].output);
+        if (tg_noise_layer_rows(m_state->device, buffers[3].bytes.data(), buffers[3].bytes.size(),
+                                As<float>(buffers[1]), As<float>(buffers[2]), params.width,
+                                params.rows, heights, nodata, TG_MEMORY_HOST,
+                                nullptr) != TG_OK) {
+            Throw("noise layer");
+        }
+        return;
+    }
+    if (kind == Program::Craters && buffers.size() >= 11) {
+        // heights, xs, ys, CraterShapeKernel, records, data, tiles, entries, frames, points,
+        // lows (src/layers/kernels/craters.slang, bound by ShapeTilesOnGpu, apply.cpp:174-196)
+        float* heights = reinterpret_cast<float*>(buffers[0].output);
+        const float* lows = As<float>(buffers[10]);
+        if (tg_craters_apply_lists(
+                m_state->device, buffers[3].bytes.data(), buffers[3].bytes.size(),
+                buffers[4].bytes.data(), Count<CraterRecord>(buffers[4]), As<float>(buffers[5]),
+                Count<float>(buffers[5]), As<std::uint32_t>(buffers[6]),
+                Count<std::uint32_t>(buffers[6]), As<std::uint32_t>(buffers[7]),
+                Count<std::uint32_t>(buffers[7]), As<float>(buffers[1]), lows,
+                As<float>(buffers[2]), lows + params.width, params.width, params.rows,
+                params.firstRow, heights, nodata, TG_MEMORY_HOST, nullptr) != TG_OK) {
+            Throw("craters");
+        }
+        return;
+    }
+    throw std::runtime_error("tgb200: no form of this kernel");
+}
+
+}  // namespace terraingen

@@ -1,0 +1,679 @@
+// The C ABI of libtgb200.so (include/tgb200.h): argument checks, device memory, host<->device
+// staging and kernel launches. Kernels live in noise.cu and craters.cu.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/tgb200.h"
+#include "kernels.h"
+
+using namespace tgb;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int status, const char* format, ...) {
+    char buffer[512];
+    va_list args;
+    va_start(args, format);
+    std::vsnprintf(buffer, sizeof(buffer), format, args);
+    va_end(args);
+    g_error = buffer;
+    return status;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    return fail(TG_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+}
+
+#define TG_CUDA(call, what)                    \
+    do {                                       \
+        const cudaError_t e_ = (call);         \
+        if (e_ != cudaSuccess) {               \
+            return cuda_fail(e_, what);        \
+        }                                      \
+    } while (0)
+
+// One growable device allocation.
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    cudaError_t reserve(size_t need) {
+        if (need <= bytes) {
+            return cudaSuccess;
+        }
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+            ptr = nullptr;
+            bytes = 0;
+        }
+        // Grow by half again to amortise repeated growth.
+        const size_t size = need + need / 2;
+        const cudaError_t err = cudaMalloc(&ptr, size);
+        if (err == cudaSuccess) {
+            bytes = size;
+        }
+        return err;
+    }
+    void release() {
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+        }
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+enum Slot {
+    kHeights,
+    kXs,
+    kYs,
+    kXLows,
+    kYLows,
+    kRecords,
+    kData,
+    kFootprints,
+    kHeads,
+    kEntries,
+    kCounts,
+    kCursor,
+    kBoxes,
+    kCulls,
+    kBinEntries,
+    kScan,
+    kStatus,
+    kProbeIn,
+    kProbeHashes,
+    kProbeValues,
+    kSlotCount
+};
+
+}  // namespace
+
+struct tg_device {
+    int ordinal = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mutex;
+    std::string name;
+    Buffer slots[kSlotCount];
+    uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
+};
+
+namespace {
+
+int check_device(tg_device* d) {
+    if (d == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "device is null");
+    }
+    const cudaError_t err = cudaSetDevice(d->ordinal);
+    if (err != cudaSuccess) {
+        return cuda_fail(err, "cudaSetDevice");
+    }
+    return TG_OK;
+}
+
+int check_memory(int memory) {
+    if (memory != TG_MEMORY_HOST && memory != TG_MEMORY_DEVICE) {
+        return fail(TG_ERROR_ARGUMENT, "memory must be TG_MEMORY_HOST or TG_MEMORY_DEVICE");
+    }
+    return TG_OK;
+}
+
+int to_grid(const tg_grid* g, Grid& out) {
+    if (g == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "grid is null");
+    }
+    if (g->row_rotation != 0.0 || g->col_rotation != 0.0) {
+        return fail(TG_ERROR_UNSUPPORTED, "rotated grids are not supported");
+    }
+    if (!(g->pixel_width != 0.0) || !(g->pixel_height != 0.0) || !std::isfinite(g->origin_x) ||
+        !std::isfinite(g->origin_y) || !std::isfinite(g->pixel_width) ||
+        !std::isfinite(g->pixel_height)) {
+        return fail(TG_ERROR_ARGUMENT, "grid transform must be finite and invertible");
+    }
+    // Tile indices are kept in 16 bits (BinEntry); 65535 tiles of 16 cells bound a side, as
+    // RunKernel's 65535 workgroups of 16 do (src/gpu/kernel.cpp:25).
+    if (g->width > 65535u * 16u || g->height > 65535u * 16u) {
+        return fail(TG_ERROR_UNSUPPORTED, "grid side above %u cells", 65535u * 16u);
+    }
+    out = Grid{g->width,       g->height,       g->origin_x,    g->pixel_width,
+               g->row_rotation, g->origin_y,    g->col_rotation, g->pixel_height};
+    return TG_OK;
+}
+
+NoData to_nodata(tg_nodata n) {
+    return NoData{n.mode, n.value};
+}
+
+int check_nodata(tg_nodata n) {
+    if (n.mode > 2u) {
+        return fail(TG_ERROR_ARGUMENT, "nodata mode must be 0, 1 or 2");
+    }
+    return TG_OK;
+}
+
+// A buffer the kernels read: the caller's pointer in device mode, else a copy in `slot`.
+int stage_in(tg_device* d, int memory, Slot slot, const void* src, size_t bytes,
+             const void** out) {
+    if (bytes == 0) {
+        *out = nullptr;
+        return TG_OK;
+    }
+    if (src == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "a required buffer is null");
+    }
+    if (memory == TG_MEMORY_DEVICE) {
+        *out = src;
+        return TG_OK;
+    }
+    TG_CUDA(d->slots[slot].reserve(bytes), "device allocation");
+    TG_CUDA(cudaMemcpyAsync(d->slots[slot].ptr, src, bytes, cudaMemcpyHostToDevice, d->stream),
+            "copy to device");
+    *out = d->slots[slot].ptr;
+    return TG_OK;
+}
+
+cudaStream_t stream_of(tg_device* d, int memory, void* stream) {
+    if (memory == TG_MEMORY_DEVICE && stream != nullptr) {
+        return static_cast<cudaStream_t>(stream);
+    }
+    return d->stream;
+}
+
+template <typename T>
+T* slot_ptr(tg_device* d, Slot s) {
+    return static_cast<T*>(d->slots[s].ptr);
+}
+
+int copy_heights_back(tg_device* d, int memory, float* heights, const float* device,
+                      size_t count) {
+    if (memory != TG_MEMORY_HOST || count == 0) {
+        return TG_OK;
+    }
+    TG_CUDA(cudaMemcpyAsync(heights, device, count * sizeof(float), cudaMemcpyDeviceToHost,
+                            d->stream),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(d->stream), "synchronize");
+    return TG_OK;
+}
+
+int noise_run(tg_device* d, const FractalStack& stack, const Grid& grid, const Positions& at,
+              bool fill, float elevation, tg_nodata nodata, float* heights, int memory,
+              void* stream) {
+    const size_t cells = size_t(grid.width) * grid.height;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    const cudaStream_t s = stream_of(d, memory, stream);
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+        if (!fill) {
+            TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
+                    "copy to device");
+        }
+    }
+    TG_CUDA(launch_noise(stack, grid, at, fill, elevation, to_nodata(nodata), dh, s),
+            "noise kernel launch");
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int check_stack(const FractalStack& stack) {
+    if (stack.count > kMaxFractals) {
+        return fail(TG_ERROR_ARGUMENT, "a fractal stack holds at most %u fractals", kMaxFractals);
+    }
+    for (uint32_t i = 0; i < stack.count; ++i) {
+        const Fractal& f = stack.fractals[i];
+        if (!f.enabled) {
+            continue;
+        }
+        // ValidateFractalParams (src/noise/validate.cpp) bounds; kernels assume them.
+        if (f.octaves < 1 || f.octaves > 32 || !(f.wavelength > 0.0f) ||
+            !(f.lacunarity > 1.0f) || !(f.gain > 0.0f) || f.basis > 6u || f.type > 3u ||
+            f.blend > 3u) {
+            return fail(TG_ERROR_ARGUMENT, "fractal %u is invalid", i);
+        }
+    }
+    return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tg_last_error(void) {
+    return g_error.c_str();
+}
+
+int tg_open(int ordinal, tg_device** device) {
+    if (device == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "device is null");
+    }
+    *device = nullptr;
+    int count = 0;
+    TG_CUDA(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (ordinal < 0 || ordinal >= count) {
+        return fail(TG_ERROR_ARGUMENT, "device %d of %d", ordinal, count);
+    }
+    cudaDeviceProp prop;
+    TG_CUDA(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
+    if (prop.major != 10) {
+        return fail(TG_ERROR_UNSUPPORTED, "%s is sm_%d%d; this build runs on sm_100 (B200)",
+                    prop.name, prop.major, prop.minor);
+    }
+    TG_CUDA(cudaSetDevice(ordinal), "cudaSetDevice");
+    tg_device* d = new tg_device();
+    d->ordinal = ordinal;
+    d->name = prop.name;
+    cudaError_t err = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess) {
+        err = cudaMallocHost(&d->pinnedStatus, 4 * sizeof(uint32_t));
+    }
+    if (err != cudaSuccess) {
+        delete d;
+        return cuda_fail(err, "device set-up");
+    }
+    *device = d;
+    return TG_OK;
+}
+
+void tg_close(tg_device* d) {
+    if (d == nullptr) {
+        return;
+    }
+    cudaSetDevice(d->ordinal);
+    cudaStreamSynchronize(d->stream);
+    for (Buffer& b : d->slots) {
+        b.release();
+    }
+    if (d->pinnedStatus != nullptr) {
+        cudaFreeHost(d->pinnedStatus);
+    }
+    cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+int tg_device_name(tg_device* d, char* name, size_t capacity) {
+    if (d == nullptr || name == nullptr || capacity == 0) {
+        return fail(TG_ERROR_ARGUMENT, "device, name and capacity are required");
+    }
+    std::snprintf(name, capacity, "%s", d->name.c_str());
+    return TG_OK;
+}
+
+int tg_synchronize(tg_device* d) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    TG_CUDA(cudaStreamSynchronize(d->stream), "synchronize");
+    return TG_OK;
+}
+
+int tg_noise_layer(tg_device* d, const void* kernel, size_t kernel_bytes, const tg_grid* grid,
+                   double origin_x, double origin_y, float* heights, tg_nodata nodata,
+                   int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (kernel == nullptr || kernel_bytes != sizeof(FractalStack)) {
+        return fail(TG_ERROR_ARGUMENT, "NoiseLayerKernel is %zu bytes", sizeof(FractalStack));
+    }
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    FractalStack stack;
+    std::memcpy(&stack, kernel, sizeof(stack));
+    if (int s = check_stack(stack)) {
+        return s;
+    }
+    if (heights == nullptr && size_t(g.width) * g.height > 0) {
+        return fail(TG_ERROR_ARGUMENT, "heights is null");
+    }
+    const Positions at{origin_x, origin_y, nullptr, nullptr};
+    return noise_run(d, stack, g, at, false, 0.0f, nodata, heights, memory, stream);
+}
+
+int tg_noise_layer_rows(tg_device* d, const void* kernel, size_t kernel_bytes, const float* xs,
+                        const float* ys, uint32_t width, uint32_t rows, float* heights,
+                        tg_nodata nodata, int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (kernel == nullptr || kernel_bytes != sizeof(FractalStack)) {
+        return fail(TG_ERROR_ARGUMENT, "NoiseLayerKernel is %zu bytes", sizeof(FractalStack));
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    FractalStack stack;
+    std::memcpy(&stack, kernel, sizeof(stack));
+    if (int s = check_stack(stack)) {
+        return s;
+    }
+    if (size_t(width) * rows == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "heights is null");
+    }
+    const void* dxs = nullptr;
+    const void* dys = nullptr;
+    if (int s = stage_in(d, memory, kXs, xs, width * sizeof(float), &dxs)) {
+        return s;
+    }
+    if (int s = stage_in(d, memory, kYs, ys, rows * sizeof(float), &dys)) {
+        return s;
+    }
+    // Unit transform: the positions come from xs / ys.
+    const Grid g{width, rows, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+    const Positions at{0.0, 0.0, static_cast<const float*>(dxs), static_cast<const float*>(dys)};
+    return noise_run(d, stack, g, at, false, 0.0f, nodata, heights, memory, stream);
+}
+
+int tg_noise_source(tg_device* d, const void* fractals, uint32_t count, float elevation,
+                    const tg_grid* grid, float* heights, int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (count > kMaxFractals || (count > 0 && fractals == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "at most %u fractals, and a pointer to them",
+                    kMaxFractals);
+    }
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    FractalStack stack;
+    std::memset(&stack, 0, sizeof(stack));
+    std::memcpy(stack.fractals, fractals, count * sizeof(Fractal));
+    stack.count = count;
+    if (int s = check_stack(stack)) {
+        return s;
+    }
+    if (heights == nullptr && size_t(g.width) * g.height > 0) {
+        return fail(TG_ERROR_ARGUMENT, "heights is null");
+    }
+    // SyntheticSource evaluates at float(world x), its origin being zero
+    // (synthetic_source.cpp:76-80, surface_noise.cpp:31-33).
+    const Positions at{0.0, 0.0, nullptr, nullptr};
+    return noise_run(d, stack, g, at, true, elevation, tg_nodata{0u, 0.0f}, heights, memory,
+                     stream);
+}
+
+int tg_noise_probe(tg_device* d, const float* xy, uint32_t n, uint32_t seed, uint32_t* hashes,
+                   float* values, int memory) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (n == 0) {
+        return TG_OK;
+    }
+    if (xy == nullptr || hashes == nullptr || values == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "probe buffers are required");
+    }
+    const void* dxy = nullptr;
+    if (int s = stage_in(d, memory, kProbeIn, xy, size_t(n) * 2 * sizeof(float), &dxy)) {
+        return s;
+    }
+    uint32_t* dh = hashes;
+    float* dv = values;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kProbeHashes].reserve(size_t(n) * 4 * sizeof(uint32_t)), "allocation");
+        TG_CUDA(d->slots[kProbeValues].reserve(size_t(n) * 12 * sizeof(float)), "allocation");
+        dh = slot_ptr<uint32_t>(d, kProbeHashes);
+        dv = slot_ptr<float>(d, kProbeValues);
+    }
+    TG_CUDA(launch_noise_probe(static_cast<const float*>(dxy), n, seed, dh, dv, d->stream),
+            "probe launch");
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(cudaMemcpyAsync(hashes, dh, size_t(n) * 4 * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, d->stream),
+                "copy to host");
+        TG_CUDA(cudaMemcpyAsync(values, dv, size_t(n) * 12 * sizeof(float), cudaMemcpyDeviceToHost,
+                                d->stream),
+                "copy to host");
+    }
+    TG_CUDA(cudaStreamSynchronize(d->stream), "synchronize");
+    return TG_OK;
+}
+
+int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, const void* records,
+                     uint32_t n, const float* data, uint32_t n_data, const double* footprints,
+                     const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
+                     void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (kernel == nullptr || kernel_bytes != sizeof(CraterShapeKernel)) {
+        return fail(TG_ERROR_ARGUMENT, "CraterShapeKernel is %zu bytes", sizeof(CraterShapeKernel));
+    }
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    if (cells == 0 || n == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr || records == nullptr || (n_data > 0 && data == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "heights, records and data are required");
+    }
+    CraterShapeKernel k;
+    std::memcpy(&k, kernel, sizeof(k));
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void* drec = nullptr;
+    const void* ddata = nullptr;
+    const void* dfoot = nullptr;
+    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kData, data, size_t(n_data) * sizeof(float), &ddata)) {
+        return st;
+    }
+    if (footprints != nullptr) {
+        if (int st = stage_in(d, memory, kFootprints, footprints, size_t(n) * 3 * sizeof(double),
+                              &dfoot)) {
+            return st;
+        }
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+        TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
+                "copy to device");
+    }
+    CraterBins bins{};
+    bins.binsX = (g.width + kBinCells - 1) / kBinCells;
+    bins.binsY = (g.height + kBinCells - 1) / kBinCells;
+    const uint32_t nbins = bins.binsX * bins.binsY;
+    TG_CUDA(d->slots[kCounts].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kBoxes].reserve(size_t(n) * sizeof(int4)), "allocation");
+    TG_CUDA(d->slots[kCulls].reserve(size_t(n) * sizeof(float)), "allocation");
+    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
+    bins.counts = slot_ptr<uint32_t>(d, kCounts);
+    bins.cursor = slot_ptr<uint32_t>(d, kCursor);
+    bins.boxes = slot_ptr<int4>(d, kBoxes);
+    bins.culls = slot_ptr<float>(d, kCulls);
+    bins.total = slot_ptr<uint32_t>(d, kStatus);
+    TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.total, 0, 4 * sizeof(uint32_t), s), "memset");
+    const CraterRecord* rec = static_cast<const CraterRecord*>(drec);
+    const float* dd = static_cast<const float*>(ddata);
+    TG_CUDA(launch_crater_count(k, rec, n, dd, static_cast<const double*>(dfoot), g, bins, s),
+            "crater count launch");
+    TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
+            "scan launch");
+    // The entries needed and the datum flag, to size the bins.
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    const uint32_t total = d->pinnedStatus[0];
+    if (d->pinnedStatus[1] & 1u) {
+        return fail(TG_ERROR_UNSUPPORTED,
+                    "craters with a datum need the ordered form (tg_craters_apply_lists)");
+    }
+    if (total == 0) {
+        return copy_heights_back(d, memory, heights, dh, cells);
+    }
+    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
+    bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
+    bins.capacity = total;
+    TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
+    const Positions at{0.0, 0.0, nullptr, nullptr};
+    TG_CUDA(launch_crater_shape(k, dd, g, at, to_nodata(nodata), bins, dh, s),
+            "crater shape launch");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(cudaMemcpyAsync(heights, dh, cells * sizeof(float), cudaMemcpyDeviceToHost, s),
+                "copy to host");
+    }
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    if (d->pinnedStatus[1] & 2u) {
+        return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
+    }
+    return TG_OK;
+}
+
+int tg_craters_apply_lists(tg_device* d, const void* kernel, size_t kernel_bytes,
+                           const void* records, uint32_t n, const float* data, uint32_t n_data,
+                           const uint32_t* heads, uint32_t n_heads, const uint32_t* entries,
+                           uint32_t n_entries, const float* xs, const float* x_lows,
+                           const float* ys, const float* y_lows, uint32_t width, uint32_t rows,
+                           uint32_t first_row, float* heights, tg_nodata nodata, int memory,
+                           void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (kernel == nullptr || kernel_bytes != sizeof(CraterShapeKernel)) {
+        return fail(TG_ERROR_ARGUMENT, "CraterShapeKernel is %zu bytes", sizeof(CraterShapeKernel));
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    const size_t cells = size_t(width) * rows;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (heads == nullptr || n_heads < 3 || entries == nullptr || n_entries == 0 ||
+        heights == nullptr || xs == nullptr || x_lows == nullptr || ys == nullptr ||
+        y_lows == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "tile lists, positions and heights are required");
+    }
+    // The lists' geometry is read on the device; check it here where the host can.
+    if (memory == TG_MEMORY_HOST) {
+        if (heads[2] != 0u) {
+            return fail(TG_ERROR_UNSUPPORTED, "crater tiles on a body are not supported");
+        }
+        const uint32_t tilesX = heads[0], side = heads[1];
+        if (side == 0 || tilesX == 0 || tilesX < (width + side - 1) / side ||
+            n_heads < 3 + 2 * tilesX * ((first_row + rows + side - 1) / side)) {
+            return fail(TG_ERROR_ARGUMENT, "tile heads do not cover the strip");
+        }
+        for (uint32_t t = 3; t + 1 < n_heads; t += 2) {
+            if (uint64_t(heads[t]) + heads[t + 1] > n_entries) {
+                return fail(TG_ERROR_ARGUMENT, "tile list past the entries");
+            }
+        }
+        for (uint32_t e = 0; e < n_entries; ++e) {
+            if (entries[e] >= n && !(n == 0 && e == 0)) {
+                return fail(TG_ERROR_ARGUMENT, "entry %u names crater %u of %u", e, entries[e], n);
+            }
+        }
+    }
+    CraterShapeKernel k;
+    std::memcpy(&k, kernel, sizeof(k));
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void *drec, *ddata, *dheads, *dentries, *dxs, *dxl, *dys, *dyl;
+    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kData, data, size_t(n_data) * sizeof(float), &ddata)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kHeads, heads, size_t(n_heads) * sizeof(uint32_t), &dheads)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kEntries, entries, size_t(n_entries) * sizeof(uint32_t),
+                          &dentries)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kXs, xs, size_t(width) * sizeof(float), &dxs)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kXLows, x_lows, size_t(width) * sizeof(float), &dxl)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kYs, ys, size_t(rows) * sizeof(float), &dys)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kYLows, y_lows, size_t(first_row + rows) * sizeof(float),
+                          &dyl)) {
+        return st;
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+        TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
+                "copy to device");
+    }
+    TG_CUDA(launch_crater_shape_lists(
+                k, static_cast<const CraterRecord*>(drec), static_cast<const float*>(ddata),
+                static_cast<const uint32_t*>(dheads), static_cast<const uint32_t*>(dentries), width,
+                rows, first_row, static_cast<const float*>(dxs), static_cast<const float*>(dxl),
+                static_cast<const float*>(dys), static_cast<const float*>(dyl), to_nodata(nodata),
+                dh, s),
+            "crater lists launch");
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+}  // extern "C"

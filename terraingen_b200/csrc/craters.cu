@@ -1,0 +1,576 @@
+// Crater shaping over a grid (ApplyCraters, src/layers/craters/shaping/apply.cpp:339-376).
+//
+// Plain path, in four stream-ordered launches:
+//   1. count   - one warp per crater: its footprint window on the grid, exactly as
+//                CratersOnRaster / PixelWindowIn compute it (apply.cpp:225-237,
+//                src/raster/cell_loops.cpp:21-28), turned into the range of the reference's
+//                16-cell tiles it touches, and one count per kBinCells-square bin it covers;
+//   2. scan    - exclusive prefix sum of the bin counts;
+//   3. scatter - one warp per crater: a 160-byte BinEntry (record + tile range) into each bin;
+//   4. shape   - one CTA per bin: the bin's entries are staged in shared memory by TMA bulk
+//                copies (cp.async.bulk + mbarrier, double-buffered), each warp ballots whether
+//                any of its cells needs a crater, and each thread adds the crater to its 4 cells
+//                (one 16-byte store per thread at the end).
+//
+// Coverage matches the reference's: a crater is evaluated at every cell of each 16x16 tile its
+// window touches (apply.cpp:119-143, 199-222), whatever the bin size here.
+//
+// Accumulation: without a datum a crater adds resolution * shaped relief independently of the
+// height beneath it (apply_test.cpp:276-286), so the contributions are summed in an FP64
+// accumulator. Each contribution is an FP32 value and the sum stays far inside 53 bits, so the
+// accumulation is error-free: the result is the FP32 rounding of the exact sum, independent of
+// the order atomics put the entries in, so every run gives the same bits.
+#include "crater_math.cuh"
+#include "kernels.h"
+
+namespace tgb {
+namespace {
+
+constexpr int kShapeThreads = 256;     // 8 warps; warp w covers rows 4w..4w+3 of a 32x32 bin
+constexpr int kCellsPerThread = 4;     // 4 adjacent columns, one row
+constexpr uint32_t kChunk = 48;        // entries per staged chunk (7680 bytes)
+constexpr uint32_t kSpinLimit = 1u << 26;  // bounded mbarrier waits
+
+__device__ __forceinline__ bool is_nodata(NoData nd, float h) {
+    if (nd.mode == 1u) {
+        return isnan(h);
+    }
+    return nd.mode != 0u && h == nd.value;
+}
+
+// `CraterOutline::MaxScale` (src/layers/craters/shaping/irregularity.cpp:229) from the record:
+// sqrt(ellipticity) * (the largest 1 + table deviation, or 1 plus the harmonic amplitudes).
+__device__ double max_outline_scale(const CraterRecord& r, const float* data) {
+    double sum = 1.0;
+    if (r.tableCount > 0u) {
+        for (uint32_t n = 0; n < r.tableCount; ++n) {
+            sum = fmax(sum, 1.0 + double(__ldg(data + r.tableOffset + n)));
+        }
+    } else {
+        for (uint32_t n = 0; n < r.harmonicCount; ++n) {
+            sum += fabs(double(__ldg(data + r.harmonicOffset + 2u * n)));
+        }
+    }
+    return sqrt(double(r.ellipticity)) * sum;
+}
+
+__device__ __forceinline__ void world_to_pixel(const Grid& g, double x, double y, double& px,
+                                               double& py) {
+    // GeoTransform::WorldToPixel (include/terraingen/raster/geo_transform.h:70)
+    const double det = g.pixelWidth * g.pixelHeight - g.rowRotation * g.colRotation;
+    const double dx = x - g.originX;
+    const double dy = y - g.originY;
+    px = (dx * g.pixelHeight - dy * g.rowRotation) / det;
+    py = (dy * g.pixelWidth - dx * g.colRotation) / det;
+}
+
+__device__ __forceinline__ int64_t clamp_index(double v, uint32_t limit) {
+    // ClampIndex(v, limit + 1) (include/terraingen/util/bits.h:42)
+    const double c = v < 0.0 ? 0.0 : (double(limit) < v ? double(limit) : v);
+    return int64_t(c);
+}
+
+// The reference tile range a crater's footprint window touches; x0 > x1 when the window is
+// empty. Also the radius beyond which a cell cannot be within the crater's reach, or +inf when
+// marks, terraces or a floor shift stretch the profile distance past the outline's bound.
+struct Footprint {
+    int4 tiles;
+    float cull;
+};
+
+__device__ Footprint crater_footprint(const CraterShapeKernel& k, const CraterRecord& r,
+                                      const float* data, const double* footprints, uint32_t i,
+                                      const Grid& g) {
+    double x, y, reach;
+    const double scale = max_outline_scale(r, data);
+    if (footprints != nullptr) {
+        x = footprints[3 * i];
+        y = footprints[3 * i + 1];
+        reach = footprints[3 * i + 2];
+    } else {
+        x = double(r.x) + double(r.xLow);
+        y = double(r.y) + double(r.yLow);
+        reach = scale * double(k.reachRadii) * (0.5 * double(r.diameter));
+    }
+    // Surface::Expand on a plane, then MappedBounds of WorldToPixel (mapped_bounds.h).
+    const double xs[2] = {x - reach, x + reach};
+    const double ys[2] = {y - reach, y + reach};
+    double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
+    for (int a = 0; a < 2; ++a) {
+        for (int b = 0; b < 2; ++b) {
+            double px, py;
+            world_to_pixel(g, xs[a], ys[b], px, py);
+            minX = fmin(minX, px);
+            minY = fmin(minY, py);
+            maxX = fmax(maxX, px);
+            maxY = fmax(maxY, py);
+        }
+    }
+    const int64_t c0 = clamp_index(floor(minX), g.width);
+    const int64_t c1 = clamp_index(ceil(maxX), g.width);
+    const int64_t r0 = clamp_index(floor(minY), g.height);
+    const int64_t r1 = clamp_index(ceil(maxY), g.height);
+    Footprint f;
+    if (c0 >= c1 || r0 >= r1) {
+        f.tiles = make_int4(1, 0, 1, 0);
+    } else {
+        f.tiles = make_int4(int(c0 / kRefTileCells), int((c1 - 1) / kRefTileCells),
+                            int(r0 / kRefTileCells), int((r1 - 1) / kRefTileCells));
+    }
+    const bool stretched = r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
+                           r.shiftY != 0.0f;
+    // A little slack over the bound: the profile distance is rounded in float.
+    f.cull = stretched ? INFINITY
+                       : float(scale * double(k.reachRadii) * (0.5 * double(r.diameter)) *
+                               (1.0 + 1e-5)) + 1e-6f;
+    return f;
+}
+
+__global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
+                                    uint32_t n, const float* __restrict__ data,
+                                    const double* __restrict__ footprints, const Grid grid,
+                                    CraterBins bins, uint32_t* __restrict__ flags) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp >= n) {
+        return;
+    }
+    int4 tiles = make_int4(1, 0, 1, 0);
+    if (lane == 0) {
+        const CraterRecord r = records[warp];
+        const Footprint f = crater_footprint(k, r, data, footprints, warp, grid);
+        tiles = f.tiles;
+        bins.boxes[warp] = tiles;
+        bins.culls[warp] = f.cull;
+        if (r.hasDatum == 1u && tiles.x <= tiles.y) {
+            atomicOr(flags, 1u);
+        }
+    }
+    tiles.x = __shfl_sync(0xffffffffu, tiles.x, 0);
+    tiles.y = __shfl_sync(0xffffffffu, tiles.y, 0);
+    tiles.z = __shfl_sync(0xffffffffu, tiles.z, 0);
+    tiles.w = __shfl_sync(0xffffffffu, tiles.w, 0);
+    if (tiles.x > tiles.y) {
+        return;
+    }
+    constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
+    const uint32_t bx0 = uint32_t(tiles.x) / kTilesPerBin, bx1 = uint32_t(tiles.y) / kTilesPerBin;
+    const uint32_t by0 = uint32_t(tiles.z) / kTilesPerBin, by1 = uint32_t(tiles.w) / kTilesPerBin;
+    const uint32_t wide = bx1 - bx0 + 1u;
+    const uint32_t total = wide * (by1 - by0 + 1u);
+    for (uint32_t t = lane; t < total; t += 32u) {
+        const uint32_t b = (by0 + t / wide) * bins.binsX + bx0 + t % wide;
+        atomicAdd(bins.counts + b, 1u);
+    }
+}
+
+__global__ void crater_scatter_kernel(const CraterRecord* __restrict__ records, uint32_t n,
+                                      CraterBins bins) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (warp >= n) {
+        return;
+    }
+    const int4 tiles = bins.boxes[warp];
+    if (tiles.x > tiles.y) {
+        return;
+    }
+    constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
+    const uint32_t bx0 = uint32_t(tiles.x) / kTilesPerBin, bx1 = uint32_t(tiles.y) / kTilesPerBin;
+    const uint32_t by0 = uint32_t(tiles.z) / kTilesPerBin, by1 = uint32_t(tiles.w) / kTilesPerBin;
+    const uint32_t wide = bx1 - bx0 + 1u;
+    const uint32_t total = wide * (by1 - by0 + 1u);
+    const int4* src = reinterpret_cast<const int4*>(records + warp);
+    const float cull = bins.culls[warp];
+    int4 tail;
+    tail.x = int(uint32_t(tiles.x) | (uint32_t(tiles.y) << 16));
+    tail.y = int(uint32_t(tiles.z) | (uint32_t(tiles.w) << 16));
+    tail.z = __float_as_int(cull);
+    tail.w = int(warp);
+    for (uint32_t t = lane; t < total; t += 32u) {
+        const uint32_t b = (by0 + t / wide) * bins.binsX + bx0 + t % wide;
+        const uint32_t slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
+        if (slot >= bins.capacity) {
+            continue;  // the host sized the entries from the counts; never taken
+        }
+        int4* dst = reinterpret_cast<int4*>(bins.entries + slot);
+#pragma unroll
+        for (int w = 0; w < 9; ++w) {
+            dst[w] = __ldg(src + w);
+        }
+        dst[9] = tail;
+    }
+}
+
+// --- TMA bulk copy helpers (PTX ISA: cp.async.bulk, mbarrier) -------------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, "
+        "1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return done != 0u;
+}
+
+// Waits for the barrier's phase, giving up after kSpinLimit polls (returns false then).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+    for (uint32_t spin = 0; spin < kSpinLimit; ++spin) {
+        if (mbar_try_wait(bar, phase)) {
+            return true;
+        }
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kShapeThreads)
+    crater_shape_kernel(const CraterShapeKernel k, const float* __restrict__ data,
+                        const Grid grid, const NoData nodata, const CraterBins bins,
+                        float* __restrict__ heights, uint32_t* __restrict__ flags) {
+    __shared__ __align__(128) BinEntry stage[2][kChunk];
+    __shared__ __align__(8) uint64_t bars[2];
+
+    const uint32_t bin = blockIdx.x;
+    const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
+    const uint32_t first = bins.counts[bin];
+    const uint32_t count = bins.counts[bin + 1] - first;
+    if (count == 0u) {
+        return;
+    }
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t row = binY * kBinCells + warp * 4u + lane / 8u;
+    const uint32_t col0 = binX * kBinCells + (lane % 8u) * kCellsPerThread;
+
+    // This thread's cells: split positions (MakeSplitPoint, crater_kernel.cpp:303) of the
+    // column centers at row 0 and the row center at column 0, as the reference's strips carry.
+    float pxh[kCellsPerThread], pxl[kCellsPerThread];
+    double acc[kCellsPerThread];
+    bool live[kCellsPerThread];
+    const double yd = grid.originY + 0.5 * grid.colRotation + (double(row) + 0.5) * grid.pixelHeight;
+    const float pyh = float(yd);
+    const float pyl = float(yd - double(pyh));
+    const bool rowIn = row < grid.height;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        const uint32_t col = col0 + j;
+        const double xd =
+            grid.originX + (double(col) + 0.5) * grid.pixelWidth + 0.5 * grid.rowRotation;
+        pxh[j] = float(xd);
+        pxl[j] = float(xd - double(pxh[j]));
+        live[j] = rowIn && col < grid.width;
+        acc[j] = 0.0;
+        if (live[j]) {
+            const float h = heights[size_t(row) * grid.width + col];
+            live[j] = !is_nodata(nodata, h);
+            acc[j] = double(h);
+        }
+    }
+    const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
+    const bool anyLive = live[0] || live[1] || live[2] || live[3];
+
+    const uint32_t chunks = (count + kChunk - 1) / kChunk;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](uint32_t c) {
+        const uint32_t s = c & 1u;
+        const uint32_t n = min(kChunk, count - c * kChunk);
+        const uint32_t bytes = n * uint32_t(sizeof(BinEntry));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bars[s], bytes);
+        bulk_copy_g2s(&stage[s][0], bins.entries + first + c * kChunk, bytes, &bars[s]);
+    };
+    if (tid == 0) {
+        issue(0);
+        if (chunks > 1) {
+            issue(1);
+        }
+    }
+    uint32_t phase[2] = {0u, 0u};
+    bool failed = false;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t s = c & 1u;
+        if (!mbar_wait(&bars[s], phase[s])) {
+            failed = true;
+        }
+        phase[s] ^= 1u;
+        if (__syncthreads_or(failed)) {
+            // A copy did not land: record it and wait (bounded) for the other buffer's copy
+            // before leaving, so no bulk copy is left writing into a finished CTA.
+            if (tid == 0) {
+                atomicOr(flags, 2u);
+                if (c + 1 < chunks) {
+                    mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                }
+            }
+            return;
+        }
+        const uint32_t n = min(kChunk, count - c * kChunk);
+        for (uint32_t e = 0; e < n; ++e) {
+            const BinEntry& entry = stage[s][e];
+            const CraterRecord& r = entry.record;
+            const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
+                                tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
+                                tileY <= int(entry.tileY1);
+            const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
+            const float cull2 = entry.cull * entry.cull;
+            bool need[kCellsPerThread];
+            float dxs[kCellsPerThread];
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                dxs[j] = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
+                need[j] = inTile && live[j] && dxs[j] * dxs[j] + dy * dy < cull2;
+                any |= need[j];
+            }
+            if (!__any_sync(0xffffffffu, any)) {
+                continue;
+            }
+#pragma unroll
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                if (need[j]) {
+                    const float dx = dxs[j];
+                    const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
+                    if (q.reached) {
+                        acc[j] += double(q.shaped);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + 2 < chunks) {
+            issue(c + 2);
+        }
+    }
+    if (!rowIn) {
+        return;
+    }
+    float out[kCellsPerThread];
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        out[j] = float(acc[j]);
+    }
+    float* dst = heights + size_t(row) * grid.width + col0;
+    const bool vec = (grid.width % 4u == 0u) && col0 + 3 < grid.width &&
+                     ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0u) && live[0] && live[1] &&
+                     live[2] && live[3];
+    if (vec) {
+        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kCellsPerThread; ++j) {
+            if (live[j]) {
+                dst[j] = out[j];
+            }
+        }
+    }
+}
+
+// The drop-in form: cell by cell over its tile's ordered crater list, in float, as
+// ShapeTilesOnCpu / craters.slang do (apply.cpp:199-222, src/layers/kernels/craters.slang).
+__global__ void crater_shape_lists_kernel(const CraterShapeKernel k,
+                                          const CraterRecord* __restrict__ records,
+                                          const float* __restrict__ data,
+                                          const uint32_t* __restrict__ heads,
+                                          const uint32_t* __restrict__ entries, uint32_t width,
+                                          uint32_t rows, uint32_t firstRow,
+                                          const float* __restrict__ xs,
+                                          const float* __restrict__ xLows,
+                                          const float* __restrict__ ys,
+                                          const float* __restrict__ yLows, const NoData nodata,
+                                          float* __restrict__ heights) {
+    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= width || r >= rows) {
+        return;
+    }
+    const size_t i = size_t(r) * width + col;
+    float height = heights[i];
+    if (is_nodata(nodata, height)) {
+        return;
+    }
+    const uint32_t row = firstRow + r;
+    const uint32_t side = heads[1];
+    const uint32_t head = 3u + 2u * ((row / side) * heads[0] + col / side);
+    const uint32_t first = heads[head], n = heads[head + 1];
+    const float px = xs[col], pxl = xLows[col], py = ys[r], pyl = yLows[row];
+    for (uint32_t e = first; e < first + n; ++e) {
+        const CraterRecord& c = records[entries[e]];
+        const float dx = crater::split_difference(px, pxl, c.x, c.xLow);
+        const float dy = crater::split_difference(py, pyl, c.y, c.yLow);
+        const crater::Contribution q = crater::crater_contribution(k, data, c, dx, dy);
+        if (!q.reached) {
+            continue;
+        }
+        height = c.hasDatum == 1u ? crater::apply_with_datum(c, q, height, dx, dy)
+                                  : height + q.shaped;
+    }
+    heights[i] = height;
+}
+
+// --- exclusive scan ------------------------------------------------------------------------
+
+constexpr uint32_t kScanBlock = 1024;
+
+__global__ void scan_block_kernel(uint32_t* data, uint32_t n, uint32_t* blockSums) {
+    __shared__ uint32_t warpSums[32];
+    const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+    const uint32_t v = i < n ? data[i] : 0u;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) {
+            x += y;
+        }
+    }
+    if (lane == 31u) {
+        warpSums[warp] = x;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warpSums[lane];
+#pragma unroll
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= d) {
+                w += y;
+            }
+        }
+        warpSums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? warpSums[warp - 1] : 0u) + x - v;
+    if (i < n) {
+        data[i] = before;
+    }
+    if (threadIdx.x == kScanBlock - 1) {
+        blockSums[blockIdx.x] = warpSums[31];
+    }
+}
+
+__global__ void scan_add_kernel(uint32_t* data, uint32_t n, const uint32_t* blockOffsets) {
+    const uint32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+    if (i < n) {
+        data[i] += blockOffsets[blockIdx.x];
+    }
+}
+
+}  // namespace
+
+size_t scan_scratch_words(uint32_t n) {
+    // Mirrors launch_exclusive_scan: n + 1 values in blocks of kScanBlock, one block sum each plus
+    // the slot the next level's total lands in, recursively.
+    const uint32_t blocks = (n + 1 + kScanBlock - 1) / kScanBlock;
+    return size_t(blocks) + 1 + (blocks > 1 ? scan_scratch_words(blocks) : 0);
+}
+
+// In place over counts[0..n); counts[n] receives the total.
+cudaError_t launch_exclusive_scan(uint32_t* counts, uint32_t n, uint32_t* scratch,
+                                  cudaStream_t stream) {
+    // Scanning n + 1 values leaves the total of the first n at index n.
+    const uint32_t m = n + 1;
+    const uint32_t blocks = (m + kScanBlock - 1) / kScanBlock;
+    scan_block_kernel<<<blocks, kScanBlock, 0, stream>>>(counts, m, scratch);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess || blocks == 1) {
+        return err;
+    }
+    // Block sums -> block offsets, recursively (blocks + 1 entries with the total last).
+    err = cudaMemsetAsync(scratch + blocks, 0, sizeof(uint32_t), stream);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    err = launch_exclusive_scan(scratch, blocks, scratch + blocks + 1, stream);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    scan_add_kernel<<<blocks, kScanBlock, 0, stream>>>(counts, m, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
+                                uint32_t n, const float* data, const double* footprints,
+                                const Grid& grid, const CraterBins& bins, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    const uint32_t threads = 256;
+    const uint32_t blocks = uint32_t((uint64_t(n) * 32u + threads - 1) / threads);
+    crater_count_kernel<<<blocks, threads, 0, stream>>>(k, records, n, data, footprints, grid,
+                                                        bins, bins.total + 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const Grid& grid,
+                                  const CraterBins& bins, cudaStream_t stream) {
+    (void)grid;
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    const uint32_t threads = 256;
+    const uint32_t blocks = uint32_t((uint64_t(n) * 32u + threads - 1) / threads);
+    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(records, n, bins);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data, const Grid& grid,
+                                const Positions& at, NoData nodata, const CraterBins& bins,
+                                float* heights, cudaStream_t stream) {
+    (void)at;
+    const uint32_t nbins = bins.binsX * bins.binsY;
+    if (nbins == 0) {
+        return cudaSuccess;
+    }
+    crater_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, data, grid, nodata, bins, heights,
+                                                             bins.total + 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_shape_lists(const CraterShapeKernel& k, const CraterRecord* records,
+                                      const float* data, const uint32_t* heads,
+                                      const uint32_t* entries, uint32_t width, uint32_t rows,
+                                      uint32_t firstRow, const float* xs, const float* xLows,
+                                      const float* ys, const float* yLows, NoData nodata,
+                                      float* heights, cudaStream_t stream) {
+    if (width == 0 || rows == 0) {
+        return cudaSuccess;
+    }
+    const dim3 block(16, 16);
+    const dim3 blocks((width + 15) / 16, (rows + 15) / 16);
+    crater_shape_lists_kernel<<<blocks, block, 0, stream>>>(k, records, data, heads, entries,
+                                                            width, rows, firstRow, xs, xLows, ys,
+                                                            yLows, nodata, heights);
+    return cudaGetLastError();
+}
+
+}  // namespace tgb

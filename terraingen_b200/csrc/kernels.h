@@ -1,0 +1,106 @@
+// Launchers of the device kernels, called by the C ABI (api.cu). Every launcher is
+// stream-ordered, takes device pointers only and returns the launch's cudaError_t.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "layouts.h"
+
+namespace tgb {
+
+// A non-rotated grid's GeoTransform (include/terraingen/raster/geo_transform.h:17-35): cell
+// (col, row) has its center at originX + (col + 0.5) * pixelWidth + (row + 0.5) * rowRotation,
+// originY + (col + 0.5) * colRotation + (row + 0.5) * pixelHeight.
+struct Grid {
+    uint32_t width, height;
+    double originX, pixelWidth, rowRotation, originY, colRotation, pixelHeight;
+};
+
+// How no-data cells are marked (src/gpu/kernel.cpp:28-31): none, NaN, or a value.
+struct NoData {
+    uint32_t mode;
+    float value;
+};
+
+// Where a kernel reads cell positions: computed from the grid in double and narrowed after
+// subtracting `originX/Y` (what RunKernel's xs/ys hold, src/gpu/kernel.cpp:56-71), or read from
+// per-column and per-row arrays when given.
+struct Positions {
+    double originX, originY;
+    const float* xs;  // optional, [width]
+    const float* ys;  // optional, [height]
+};
+
+// --- noise ---------------------------------------------------------------------------------
+// heights[row * width + col] = base + stack(x, y), where base is `elevation` when `fill` is set
+// and the cell's current height otherwise (cells holding no-data are skipped then).
+cudaError_t launch_noise(const FractalStack& stack, const Grid& grid, const Positions& at,
+                         bool fill, float elevation, NoData nodata, float* heights,
+                         cudaStream_t stream);
+
+// Conformance probe (the reference's tests/unit/gpu/kernels/noise_conformance.slang analogue):
+// for each input point, the PCG hashes and basis/fractal values, for testing against the oracle.
+cudaError_t launch_noise_probe(const float* xy, uint32_t n, uint32_t seed, uint32_t* hashes,
+                               float* values, cudaStream_t stream);
+
+// --- craters -------------------------------------------------------------------------------
+// Side of the square bins craters are sorted into for shaping, in cells.
+constexpr uint32_t kBinCells = 32;
+// Side of the reference's crater tiles (src/layers/craters/shaping/apply.cpp:109); a crater is
+// evaluated at every cell of each such tile its footprint window touches.
+constexpr uint32_t kRefTileCells = 16;
+
+// One crater binned for shaping: its record, the inclusive range of reference tiles its
+// footprint touches, and the distance (m) beyond which no cell can be within its reach (+inf
+// when marks, terraces or a floor shift leave no such bound). 160 bytes, so a bin's entries copy
+// to shared memory in 16-byte units.
+struct BinEntry {
+    CraterRecord record;
+    uint16_t tileX0, tileX1, tileY0, tileY1;
+    float cull;
+    uint32_t index;
+};
+static_assert(sizeof(BinEntry) == 160, "BinEntry must be a multiple of 16 bytes");
+
+struct CraterBins {
+    uint32_t binsX, binsY;
+    uint32_t* counts;    // [bins + 1]: entries per bin, then exclusive offsets after the scan
+    uint32_t* cursor;    // [bins]
+    BinEntry* entries;   // [capacity]
+    uint32_t capacity;
+    uint32_t* total;     // [1] entries needed
+    int4* boxes;         // [craters] reference-tile box per crater (x0, x1, y0, y1); empty: x0 > x1
+    float* culls;        // [craters] cull distance per crater
+};
+
+// Per crater: its footprint's reference-tile box on `grid` and the number of bins it covers,
+// added to bins.counts. `footprints` (x, y, reach in meters, as doubles) is optional; without it
+// the footprint follows from the record (center hi + lo, reach = outline stretch x reachRadii x
+// radius).
+cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
+                                uint32_t n, const float* data, const double* footprints,
+                                const Grid& grid, const CraterBins& bins, cudaStream_t stream);
+cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const Grid& grid,
+                                  const CraterBins& bins, cudaStream_t stream);
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data, const Grid& grid,
+                                const Positions& at, NoData nodata, const CraterBins& bins,
+                                float* heights, cudaStream_t stream);
+
+// The drop-in form: the reference's own tile lists (`CraterTiles`, apply.cpp:111-143), craters
+// applied in list order exactly as ShapeTilesOnCpu does (apply.cpp:199-222).
+cudaError_t launch_crater_shape_lists(const CraterShapeKernel& k, const CraterRecord* records,
+                                      const float* data, const uint32_t* heads,
+                                      const uint32_t* entries, uint32_t width, uint32_t rows,
+                                      uint32_t firstRow, const float* xs, const float* xLows,
+                                      const float* ys, const float* yLows, NoData nodata,
+                                      float* heights, cudaStream_t stream);
+
+// Exclusive prefix sum of n counts in place, writing the total to counts[n]. `scratch` holds
+// scan_scratch_words(n) words.
+size_t scan_scratch_words(uint32_t n);
+cudaError_t launch_exclusive_scan(uint32_t* counts, uint32_t n, uint32_t* scratch,
+                                  cudaStream_t stream);
+
+}  // namespace tgb

@@ -1,0 +1,216 @@
+"""Python face of the C ABI: a `Device` whose methods mirror the reference's backend entry points
+(RunKernel for noise layers and craters, SyntheticSource::FillSamples, and the CPU-only stages).
+
+Buffers are numpy arrays (host memory: copied in and out inside the call, as RunKernel does) or
+torch CUDA tensors (device memory: stream-ordered on torch's current stream, no copies).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .layouts import CRATER_RECORD, CRATER_SHAPE_KERNEL, FRACTAL, NOISE_LAYER_KERNEL
+
+
+@dataclass(frozen=True)
+class GridSpec:
+    """A north-up grid: `width` x `height` cells of `pixel` meters, its top-left corner at
+    (`x0`, `y0`); row 0 is north (GeoTransform::NorthUp, geo_transform.h:33)."""
+
+    width: int
+    height: int
+    x0: float
+    y0: float
+    pixel: float
+
+    def native(self) -> N.Grid:
+        return N.Grid(self.width, self.height, self.x0, self.pixel, 0.0, self.y0, 0.0, -self.pixel)
+
+    def transform(self) -> tuple:
+        """GDAL-order coefficients."""
+        return (self.x0, self.pixel, 0.0, self.y0, 0.0, -self.pixel)
+
+    @property
+    def cells(self) -> int:
+        return self.width * self.height
+
+
+def centered(width: int, height: int, pixel: float, cx: float = 0.0, cy: float = 0.0) -> GridSpec:
+    """A grid of `width` x `height` cells of `pixel` meters centered on (cx, cy)."""
+    return GridSpec(width, height, cx - 0.5 * pixel * width, cy + 0.5 * pixel * height, pixel)
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+class _Buffers:
+    """Resolves each argument to a pointer and records whether the call is host or device."""
+
+    def __init__(self):
+        self.memory = None
+        self.keep = []
+
+    def ptr(self, x, dtype=None):
+        if x is None:
+            return None
+        if _is_torch(x):
+            if not x.is_cuda:
+                raise ValueError("torch tensors must be on the GPU")
+            if not x.is_contiguous():
+                raise ValueError("tensors must be contiguous")
+            self._kind(N.TG_MEMORY_DEVICE)
+            return C.c_void_p(x.data_ptr())
+        arr = np.asarray(x)
+        if dtype is not None and arr.dtype != dtype:
+            raise TypeError(f"expected {dtype}, got {arr.dtype}")
+        if not arr.flags.c_contiguous:
+            raise ValueError("arrays must be C-contiguous")
+        self._kind(N.TG_MEMORY_HOST)
+        self.keep.append(arr)
+        return C.c_void_p(arr.ctypes.data)
+
+    def _kind(self, memory):
+        if self.memory is None:
+            self.memory = memory
+        elif self.memory != memory:
+            raise ValueError("mix of host arrays and device tensors in one call")
+
+
+def _stream(memory):
+    if memory == N.TG_MEMORY_DEVICE:
+        import torch
+
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return None
+
+
+def _bytes(block: np.ndarray, dtype: np.dtype) -> np.ndarray:
+    block = np.ascontiguousarray(block)
+    if block.dtype != dtype:
+        raise TypeError(f"expected a {dtype.itemsize}-byte block")
+    return block
+
+
+class Device:
+    """One B200 (tg_open). Methods raise TgError with the library's message on failure."""
+
+    def __init__(self, ordinal: int = 0):
+        self._lib = N.library()
+        handle = C.c_void_p()
+        N.check(self._lib.tg_open(ordinal, C.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if self._handle:
+            self._lib.tg_close(self._handle)
+            self._handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def name(self) -> str:
+        buf = C.create_string_buffer(256)
+        N.check(self._lib.tg_device_name(self._handle, buf, 256))
+        return buf.value.decode()
+
+    def synchronize(self) -> None:
+        N.check(self._lib.tg_synchronize(self._handle))
+
+    # --- noise ----------------------------------------------------------------------------
+    def noise_source(self, fractals: np.ndarray, grid: GridSpec, heights, elevation: float = 0.0):
+        """SyntheticSource::FillSamples on `grid` (synthetic_source.cpp:87): heights = elevation +
+        the fractal stack. `fractals` is an array of FRACTAL (at most 8)."""
+        fr = _bytes(np.atleast_1d(fractals), FRACTAL)
+        b = _Buffers()
+        h = b.ptr(heights, np.float32)
+        g = grid.native()
+        N.check(self._lib.tg_noise_source(self._handle, fr.ctypes.data, len(fr), elevation,
+                                          C.byref(g), h, b.memory, _stream(b.memory)))
+        return heights
+
+    def noise_layer(self, kernel: np.ndarray, grid: GridSpec, heights, origin=(0.0, 0.0),
+                    nodata=(0, 0.0)):
+        """NoiseLayer's RunKernel (noise_layer.cpp:113): heights += the NoiseLayerKernel stack."""
+        k = _bytes(kernel, NOISE_LAYER_KERNEL)
+        b = _Buffers()
+        h = b.ptr(heights, np.float32)
+        g = grid.native()
+        N.check(self._lib.tg_noise_layer(self._handle, k.ctypes.data, k.nbytes, C.byref(g),
+                                         origin[0], origin[1], h, N.NoData(*nodata), b.memory,
+                                         _stream(b.memory)))
+        return heights
+
+    def noise_layer_rows(self, kernel: np.ndarray, xs, ys, heights, nodata=(0, 0.0)):
+        """The strip form RunKernel binds (kernel.cpp:98-111)."""
+        k = _bytes(kernel, NOISE_LAYER_KERNEL)
+        b = _Buffers()
+        px, py, h = b.ptr(xs, np.float32), b.ptr(ys, np.float32), b.ptr(heights, np.float32)
+        N.check(self._lib.tg_noise_layer_rows(self._handle, k.ctypes.data, k.nbytes, px, py,
+                                              len(xs), len(ys), h, N.NoData(*nodata), b.memory,
+                                              _stream(b.memory)))
+        return heights
+
+    def noise_probe(self, xy: np.ndarray, seed: int):
+        """The conformance probe: (hashes [n, 4] u32, values [n, 12] f32)."""
+        xy = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+        n = len(xy)
+        hashes = np.zeros((n, 4), np.uint32)
+        values = np.zeros((n, 12), np.float32)
+        N.check(self._lib.tg_noise_probe(self._handle, xy.ctypes.data, n, seed,
+                                         hashes.ctypes.data, values.ctypes.data,
+                                         N.TG_MEMORY_HOST))
+        return hashes, values
+
+    # --- craters --------------------------------------------------------------------------
+    def craters_apply(self, kernel: np.ndarray, records, data, grid: GridSpec, heights,
+                      footprints=None, nodata=(0, 0.0)):
+        """ApplyCraters' shaping with device binning (apply.cpp:339-376). `records` is an array
+        of CRATER_RECORD (or a uint8 device tensor of its bytes), `data` float32."""
+        k = _bytes(kernel, CRATER_SHAPE_KERNEL)
+        b = _Buffers()
+        if isinstance(records, np.ndarray) and records.dtype == CRATER_RECORD:
+            n = len(records)
+            rec = b.ptr(records)
+        else:
+            n = records.numel() // CRATER_RECORD.itemsize if _is_torch(records) else \
+                len(records) // CRATER_RECORD.itemsize
+            rec = b.ptr(records)
+        nd = data.numel() if _is_torch(data) else len(data)
+        dp = b.ptr(data, np.float32)
+        fp = b.ptr(footprints, np.float64) if footprints is not None else None
+        h = b.ptr(heights, np.float32)
+        g = grid.native()
+        N.check(self._lib.tg_craters_apply(self._handle, k.ctypes.data, k.nbytes, rec, n, dp, nd,
+                                           fp, C.byref(g), h, N.NoData(*nodata), b.memory,
+                                           _stream(b.memory)))
+        return heights
+
+    def craters_apply_lists(self, kernel, records, data, heads, entries, xs, x_lows, ys, y_lows,
+                            heights, first_row=0, nodata=(0, 0.0)):
+        """The drop-in strip form (craters.slang via ShapeTilesOnGpu, apply.cpp:174-196)."""
+        k = _bytes(kernel, CRATER_SHAPE_KERNEL)
+        b = _Buffers()
+        args = [b.ptr(records), b.ptr(data, np.float32), b.ptr(heads, np.uint32),
+                b.ptr(entries, np.uint32), b.ptr(xs, np.float32), b.ptr(x_lows, np.float32),
+                b.ptr(ys, np.float32), b.ptr(y_lows, np.float32), b.ptr(heights, np.float32)]
+        n = len(records) if records.dtype == CRATER_RECORD else len(records) // 144
+        N.check(self._lib.tg_craters_apply_lists(
+            self._handle, k.ctypes.data, k.nbytes, args[0], n, args[1], len(data), args[2],
+            len(heads), args[3], len(entries), args[4], args[5], args[6], args[7], len(xs),
+            len(ys), first_row, args[8], N.NoData(*nodata), b.memory, _stream(b.memory)))
+        return heights

@@ -1,0 +1,141 @@
+"""Generates the golden fixtures under tests/golden/ from the reference itself.
+
+Run here, where the reference sources are, after `make -C oracle`:
+
+    python tests/golden/make_fixtures.py
+
+Each fixture holds the inputs the reference hands its GPU backend (captured through the drop-in
+device, oracle/ref_harness.cpp) and the reference CPU path's heights for the same scene, so the
+GPU tests need nothing from the reference at run time.
+"""
+
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import harness as H  # noqa: E402
+from terraingen_b200 import centered, layouts as L  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def noise_fixtures() -> None:
+    ref = H.reference()
+    cases = {}
+    # The synthetic source of the 4097^2 terrain (8-octave Perlin fBm, 512 m, 5 m), a window.
+    g = centered(96, 80, 0.5, 123.25, -37.5)
+    f = L.fractal(seed=7, wavelength=512.0, amplitude=5.0, octaves=8)
+    cases["fbm"] = (g, np.array([f]), 0.0)
+    # The DEM source (12 octaves, 20 km, 2000 m) at 5 m.
+    g = centered(64, 64, 5.0, -2500.0, 4000.0)
+    f = L.fractal(seed=3, wavelength=20000.0, amplitude=2000.0, octaves=12)
+    cases["dem"] = (g, np.array([f]), 100.0)
+    # A stack with every basis, type and blend, a warp and a disabled fractal.
+    g = centered(48, 40, 2.0, 900.0, 700.0)
+    stack = np.array([
+        L.fractal(seed=1, wavelength=300.0, amplitude=20.0, octaves=5),
+        L.fractal(seed=2, wavelength=120.0, amplitude=6.0, octaves=3, basis=1, type=1, blend=0),
+        L.fractal(seed=3, wavelength=90.0, amplitude=4.0, octaves=4, basis=2, type=2, blend=1),
+        L.fractal(seed=4, wavelength=70.0, amplitude=5.0, octaves=3, basis=3, type=3, blend=2,
+                  offset=0.7),
+        L.fractal(seed=5, wavelength=60.0, amplitude=3.0, octaves=2, basis=5, blend=0,
+                  warp_amplitude=25.0, warp_wavelength=200.0),
+        L.fractal(seed=6, wavelength=50.0, amplitude=2.0, octaves=2, basis=6, blend=3),
+        L.fractal(seed=8, wavelength=40.0, amplitude=9.0, octaves=2, basis=4, enabled=False),
+        L.fractal(seed=9, wavelength=33.0, amplitude=1.5, octaves=6, type=1, offset=1.2),
+    ])
+    cases["stack"] = (g, stack, -5.0)
+    # Far from the origin (1.2e5 m): float positions as the reference narrows them.
+    g = centered(40, 40, 1.0, 120000.0, -80000.0)
+    cases["far"] = (g, np.array([L.fractal(seed=11, wavelength=800.0, amplitude=40.0)]), 0.0)
+    arrays = {}
+    for name, (grid, fractals, elevation) in cases.items():
+        scene = H.make_scene(grid, source_fractals=fractals, elevation=elevation)
+        heights, _ = H.evaluate(ref, scene, 0, 1)
+        arrays[f"{name}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])
+        arrays[f"{name}_fractals"] = fractals.view(np.uint8)
+        arrays[f"{name}_elevation"] = np.float32(elevation)
+        arrays[f"{name}_heights"] = heights
+    # A noise layer over a synthetic source: the layer runs through RunKernel (captured).
+    g = centered(70, 50, 1.0, 10.0, 20.0)
+    src = np.array([L.fractal(seed=21, wavelength=400.0, amplitude=30.0, octaves=6)])
+    lay = np.array([L.fractal(seed=22, wavelength=60.0, amplitude=2.0, octaves=4),
+                    L.fractal(seed=23, wavelength=25.0, amplitude=0.5, octaves=3, basis=1)])
+    scene = H.make_scene(g, source_fractals=src, layer_fractals=lay)
+    heights, _ = H.evaluate(ref, scene, 0, 1)
+    cap = H.capture()
+    H.evaluate(cap, scene, 1, 1)
+    (call,) = H.captured(cap)
+    assert call["kind"] == 1
+    for k in ("kernel", "xs", "ys", "heights"):
+        arrays[f"layer_{k}"] = call[k]
+    arrays["layer_expected"] = heights
+    np.savez_compressed(OUT / "noise.npz", **arrays)
+
+
+CRATER_SCENES = {
+    # The 257^2, 1 m crater terrain: Fassett-Thomson, irregular outlines (the default apply).
+    "config1": (centered(257, 257, 1.0), H.config1_craters()),
+    # Martin-Parkes-Dunstan, plain options, off-center grid.
+    "mpd": (centered(160, 144, 0.5, 40.0, -25.0),
+            dict(seed=5, sfdCoefficient=4e-2, minDiameter=1.0, maxDiameter=40.0, profile=1,
+                 applyPreset=1)),
+    # Complex craters (lowered transition) with peaks and terraces, rim smoothing.
+    "complex": (centered(192, 192, 2.0),
+                dict(seed=9, sfdCoefficient=0.6, minDiameter=8.0, maxDiameter=300.0, profile=2,
+                     transitionDiameter=60.0, terraceOnset=80.0, terraceFull=200.0,
+                     rimSigma=0.08)),
+    # The reference's default crater models (diffused MPD profiles, matched diffusion).
+    "diffused": (centered(160, 160, 2.0, 300.0, 300.0),
+                 dict(seed=3, sfdCoefficient=0.2, minDiameter=10.0, maxDiameter=120.0, profile=3)),
+    # Crater noise and texture (wall streaks, ejecta).
+    "textured": (centered(128, 128, 1.0),
+                 dict(seed=4, sfdCoefficient=3e-2, minDiameter=4.0, maxDiameter=60.0, profile=1,
+                      noiseAmplitude=0.02, rimNoiseAmplitude=0.01, wallStreaks=0.01,
+                      ejecta=0.5)),
+}
+
+
+def crater_fixtures() -> None:
+    ref = H.reference()
+    cap = H.capture()
+    arrays = {}
+    for name, (grid, fields) in CRATER_SCENES.items():
+        scene = H.make_scene(grid, craters=fields)
+        heights, _ = H.evaluate(ref, scene, 0, 1)
+        H.evaluate(cap, scene, 1, 1)
+        calls = [c for c in H.captured(cap) if c["kind"] == 2]
+        assert len(calls) == 1, (name, len(calls))
+        call = calls[0]
+        arrays[f"{name}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0,
+                                           grid.pixel])
+        for k in H.CRATER_FIELDS:
+            arrays[f"{name}_{k}"] = call[k]
+        arrays[f"{name}_expected"] = heights
+        print(name, len(call["records"]) // 144, "craters",
+              len(call["data"]) // 4, "data floats", float(np.abs(heights).max()))
+    np.savez_compressed(OUT / "craters.npz", **arrays)
+
+
+def population_fixture() -> None:
+    """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
+    ref = H.reference()
+    scene = H.make_scene(centered(257, 257, 1.0), craters=H.config1_craters())
+    pop = H.craters(ref, scene, (-128.5, -128.5, 128.5, 128.5), 1.0)
+    np.savez_compressed(OUT / "population.npz", **pop)
+
+
+if __name__ == "__main__":
+    H.build("ref")
+    H.build("capture")
+    noise_fixtures()
+    crater_fixtures()
+    population_fixture()
+    for p in sorted(OUT.glob("*.npz")):
+        print(p.name, p.stat().st_size)

@@ -1,0 +1,43 @@
+"""The drop-in device inside the reference's own pipeline: Terrain::Evaluate with Backend::Cuda,
+whose CudaCompute is the product's adapter (terraingen_b200/adapter/cuda_compute.cpp) on
+libtgb200, against Backend::Cpu of the same build and the committed fixture."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import harness as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dropin(device):
+    if not H.available("libtgref_cuda.so"):
+        pytest.skip("oracle/_ref/libtgref_cuda.so was not built with the reference")
+    return H.dropin()
+
+
+def test_config1_through_reference_pipeline(dropin, crater_fixture):
+    from terraingen_b200 import centered
+
+    scene = H.make_scene(centered(257, 257, 1.0), craters=H.config1_craters())
+    cpu, _ = H.evaluate(dropin, scene, 0, 1)
+    gpu, _ = H.evaluate(dropin, scene, 1, 1)
+    assert np.array_equal(cpu.view(np.uint32), crater_fixture["config1_expected"].view(np.uint32))
+    err = np.abs(gpu.astype(np.float64) - cpu)
+    assert err.max() <= 1e-3, err.max()
+
+
+def test_noise_layer_through_reference_pipeline(dropin, noise_fixture):
+    from terraingen_b200 import centered
+    from terraingen_b200.layouts import fractal
+
+    g = centered(70, 50, 1.0, 10.0, 20.0)
+    src = np.array([fractal(seed=21, wavelength=400.0, amplitude=30.0, octaves=6)])
+    lay = np.array([fractal(seed=22, wavelength=60.0, amplitude=2.0, octaves=4),
+                    fractal(seed=23, wavelength=25.0, amplitude=0.5, octaves=3, basis=1)])
+    scene = H.make_scene(g, source_fractals=src, layer_fractals=lay)
+    gpu, _ = H.evaluate(dropin, scene, 1, 1)
+    assert np.array_equal(gpu.view(np.uint32), noise_fixture["layer_expected"].view(np.uint32))
