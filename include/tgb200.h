@@ -148,6 +148,114 @@ int tg_craters_apply_lists(tg_device* device, const void* kernel, size_t kernel_
                            uint32_t first_row, float* heights, tg_nodata nodata, int memory,
                            void* stream);
 
+
+/* --- boulders ----------------------------------------------------------------------------- */
+
+/* One boulder drawn as a dome: center (m), diameter (m), exposed height (m; Boulder::ExposedHeight,
+ * include/terraingen/layers/boulders/boulder.h:84) and resolution weight (ResolutionWeight at the
+ * spacing, src/layers/fade.cpp:50). 40 bytes. */
+typedef struct tg_boulder {
+    double x;
+    double y;
+    double diameter;
+    double exposed_height;
+    double weight;
+} tg_boulder;
+
+/* BoulderLayer's dome relief on a plane grid: every cell holding data within each boulder's box
+ * (half-width 0.5 (diameter + width)) becomes max(height, base + weight * dome), base being the
+ * cell's height before the call and the dome averaged over a band `width` meters wide (the
+ * spacing; 0 samples it at the point). Replaces BoulderLayer::ApplySamples' DrawFeatures /
+ * AddRelief / DomeHeight (src/layers/boulders/boulder_relief.cpp:44-57,244-275,426-439), which the
+ * reference runs only on the CPU, for boulders without facets or fillets (the defaults). The
+ * result does not depend on the boulders' order. */
+int tg_boulders_bake(tg_device* device, const void* boulders, uint32_t n, double width,
+                     const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
+                     void* stream);
+
+/* --- whole evaluations --------------------------------------------------------------------- */
+
+/* A terrain as Terrain::Evaluate runs it on one grid (src/pipeline/terrain.cpp:289-331): a
+ * synthetic source (`n_fractals` 52-byte Fractals plus `elevation`; none for a flat source at
+ * `elevation`), then optionally a noise layer (a 420-byte NoiseLayerKernel, measured from the
+ * origin), a crater layer (as tg_craters_apply takes it) and a boulder layer (as
+ * tg_boulders_bake takes it), in that order. Every pointer is host memory for TG_MEMORY_HOST and
+ * device memory for TG_MEMORY_DEVICE, like the heights. */
+typedef struct tg_terrain {
+    const void* fractals;
+    uint32_t n_fractals;
+    float elevation;
+    const void* noise_layer;
+    const void* crater_kernel;
+    const void* crater_records;
+    uint32_t n_craters;
+    const float* crater_data;
+    uint32_t n_crater_data;
+    const double* crater_footprints;
+    const void* boulders;
+    uint32_t n_boulders;
+    double boulder_width;
+} tg_terrain;
+
+/* Evaluates `terrain` on `grid` into `heights` (row-major, width x height floats): the source
+ * fills, each layer applies in turn, all on the device; with host memory the layer inputs are
+ * copied in once and the heights copied out once. Replaces Terrain::Evaluate / Fill for this
+ * stack (src/pipeline/terrain.cpp:289-331). */
+int tg_evaluate(tg_device* device, const tg_terrain* terrain, const tg_grid* grid,
+                float* heights, int memory, void* stream);
+
+/* The device's measured lane-operation rate for a mix of 32-bit integer multiply-adds and FP32
+ * fused multiply-adds (the noise and shaping kernels' roofline denominator), in operations per
+ * second. */
+int tg_measure_alu(tg_device* device, double* lane_ops_per_second);
+
+/* --- crater populations and kernel batches (host) ------------------------------------------ */
+
+/* A crater layer's population on a plane: a power-law density N(>D) = c D^-exponent per m^2 on
+ * [min_diameter, max_diameter] (PowerLawSfd, include/terraingen/distribution/power_law.h:54),
+ * uniform ages over lifetime_gyr (UniformAges, ages/age_model.h:46), constant fresh depth and rim
+ * ratios worn by FreshnessDegradation (degradation/freshness_degradation.h:22), seeded by `seed`
+ * (CraterLayerOptions::seed). */
+typedef struct tg_crater_population {
+    uint32_t seed;
+    double sfd_coefficient;
+    double sfd_exponent;
+    double min_diameter;
+    double max_diameter;
+    double lifetime_gyr;
+    double depth_ratio;
+    double rim_ratio;
+    double cutoff_depth_ratio;    /* kVisibilityDepthRatio, 0.04 */
+    double cell_size_factor;      /* CraterGenerationOptions::cellSizeFactor, 16 */
+    double margin_radii;          /* candidate margin in radii (tg_crater_population only) */
+    double min_resolved_diameter; /* bands wholly below are skipped (tg_crater_population only) */
+} tg_crater_population;
+
+/* How the layer shapes its craters: `profile` 0 Fassett-Thomson, 1 Martin-Parkes-Dunstan;
+ * `irregular` 1 for the default irregular outlines (DefaultCraterApply, apply_options.cpp:49). */
+typedef struct tg_crater_shaping {
+    uint32_t profile;
+    uint32_t irregular;
+} tg_crater_shaping;
+
+/* The craters the layer draws over `region` (x0, y0, x1, y1 in meters), in the reference's order
+ * (GenerateCraters, src/layers/craters/generation/population.cpp:414): centers, diameters, ages
+ * and 64-bit ids, bit-exact. `count` receives the number; arrays (any may be null) hold at most
+ * `capacity`. Host only. */
+int tg_crater_generate(const tg_crater_population* population, const double* region,
+                       double* x, double* y, double* diameter, double* age, uint64_t* id,
+                       size_t capacity, size_t* count);
+
+/* What CraterLayer::ApplySamples hands the crater kernel for `grid`
+ * (src/layers/craters/crater_layer.cpp:337-359, shaping/apply.cpp:339-370): the 188-byte
+ * CraterShapeKernel, the 144-byte CraterRecords of the craters on the grid in apply order, their
+ * float data, and 3 doubles per record (center x, y and footprint reach) for tg_craters_apply.
+ * Call with null outputs to learn `n_records` and `n_data`. Host only. */
+int tg_crater_batch(const tg_crater_population* population, const tg_crater_shaping* shaping,
+                    const tg_grid* grid, void* kernel, void* records, size_t record_capacity,
+                    float* data, size_t data_capacity, double* footprints, size_t* n_records,
+                    size_t* n_data);
+
 #ifdef __cplusplus
 }
 #endif

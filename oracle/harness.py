@@ -38,10 +38,13 @@ class Scene(C.Structure):
         ("profile", _I32), ("transitionDiameter", _D), ("applyPreset", _I32),
         ("noiseAmplitude", _D), ("rimNoiseAmplitude", _D), ("wallStreaks", _D), ("ejecta", _D),
         ("rimSigma", _D), ("terraceOnset", _D), ("terraceFull", _D),
+        ("boulders", _I32), ("boulderSeed", _U32), ("boulderCoefficient", _D),
+        ("boulderExponent", _D), ("boulderMin", _D), ("boulderMax", _D), ("heightRatio", _D),
     ]
 
 
-def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, craters=None):
+def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, craters=None,
+               boulders=None):
     """A Scene on `grid` (terraingen_b200.GridSpec). `craters` is a dict of crater-layer fields
     (seed, sfdCoefficient, sfdExponent, minDiameter, maxDiameter, lifetimeGyr, depthRatio,
     rimRatio, profile, transitionDiameter, applyPreset, noiseAmplitude, ...)."""
@@ -69,7 +72,31 @@ def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, c
         defaults.update(craters)
         for k, v in defaults.items():
             setattr(s, k, v)
+    if boulders is not None:
+        s.boulders = 1
+        defaults = dict(boulderSeed=1, boulderCoefficient=0.05, boulderExponent=2.5,
+                        boulderMin=0.2, boulderMax=3.0, heightRatio=0.5)
+        defaults.update(boulders)
+        for k, v in defaults.items():
+            setattr(s, k, v)
     return s
+
+
+def boulders(lib: C.CDLL, scene: Scene) -> np.ndarray:
+    """The boulders the scene's boulder layer draws: [n, 5] (x, y, diameter, exposed, weight)."""
+    n = lib.tgref_boulders(C.byref(scene), None, 0)
+    if n < 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    out = np.zeros((n, 5), np.float64)
+    lib.tgref_boulders(C.byref(scene), out.ctypes.data, n)
+    return out
+
+
+def below_boulders(lib: C.CDLL, scene: Scene, threads: int = 0) -> np.ndarray:
+    out = np.zeros((scene.height, scene.width), np.float32)
+    if lib.tgref_evaluate_below_boulders(C.byref(scene), threads, out.ctypes.data) != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return out
 
 
 def config1_craters() -> dict:
@@ -134,6 +161,10 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_craters.argtypes = [C.POINTER(Scene), C.c_void_p, _D, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
     lib.tgref_craters.restype = C.c_long
+    lib.tgref_boulders.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_long]
+    lib.tgref_boulders.restype = C.c_long
+    lib.tgref_evaluate_below_boulders.argtypes = [C.POINTER(Scene), C.c_uint, C.c_void_p]
+    lib.tgref_evaluate_below_boulders.restype = C.c_int
     return lib
 
 

@@ -21,6 +21,8 @@
 #include "terraingen/layers/craters/profiles/fassett_thomson.h"
 #include "terraingen/layers/craters/profiles/martin_parkes_dunstan.h"
 #include "terraingen/layers/craters/shaping/morphometry.h"
+#include "terraingen/layers/boulders/boulder_layer.h"
+#include "terraingen/layers/fade.h"
 #include "terraingen/util/log.h"
 
 #include <chrono>
@@ -64,6 +66,11 @@ struct tgref_scene {
     int32_t applyPreset;
     double noiseAmplitude, rimNoiseAmplitude, wallStreaks, ejecta, rimSigma;
     double terraceOnset, terraceFull;
+    // boulder layer (none when boulders == 0): sizes N(>D) = c D^-exponent per m^2 on
+    // [min, max], height ratio fixed, no burial
+    int32_t boulders;
+    uint32_t boulderSeed;
+    double boulderCoefficient, boulderExponent, boulderMin, boulderMax, heightRatio;
 };
 
 const char* tgref_error() {
@@ -128,7 +135,22 @@ std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s) {
     return std::make_shared<CraterLayer>(std::move(models), std::move(options));
 }
 
-Terrain MakeTerrain(const tgref_scene& s) {
+std::shared_ptr<BoulderLayer> MakeBoulderLayer(const tgref_scene& s) {
+    BoulderLayerOptions options;
+    options.seed = s.boulderSeed;
+    options.sizes.distribution = std::make_shared<PowerLawSfd>(
+        s.boulderCoefficient, s.boulderExponent, SfdKind::Density,
+        DiameterRange{s.boulderMin, s.boulderMax});
+    options.sizes.minDiameter = s.boulderMin;
+    options.sizes.maxDiameter = s.boulderMax;
+    options.pose.minHeightRatio = s.heightRatio;
+    options.pose.maxHeightRatio = s.heightRatio;
+    options.pose.minBurial = 0.0;
+    options.pose.maxBurial = 0.0;
+    return std::make_shared<BoulderLayer>(options);
+}
+
+Terrain MakeTerrain(const tgref_scene& s, bool withBoulders = true) {
     std::shared_ptr<const Source> source;
     if (s.source == 1) {
         source = std::make_shared<SyntheticSource>(Stack(s.sourceStack, s.sourceFractals),
@@ -146,6 +168,9 @@ Terrain MakeTerrain(const tgref_scene& s) {
     }
     if (s.craters != 0) {
         layers.push_back(MakeCraterLayer(s));
+    }
+    if (s.boulders != 0 && withBoulders) {
+        layers.push_back(MakeBoulderLayer(s));
     }
     return Terrain(Surface{}, source, layers);
 }
@@ -202,6 +227,69 @@ long tgref_craters(const tgref_scene* s, const double* region, double spacing, d
             if (id) id[i] = c.id;
         }
         return count;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// The boulders the scene's boulder layer draws into its grid as domes, as its ApplySamples picks
+/// them (boulder_relief.cpp:298-302, 372-425): placed over the grid's bounds grown by half a
+/// sample, on the ground of the layers below, drawn when their relief range holds them and their
+/// resolution weight is positive. Per boulder: x, y, diameter, exposed height, weight (5 doubles)
+/// into `out` (capacity `n` boulders); returns the count, or -1.
+long tgref_boulders(const tgref_scene* s, double* out, long n) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const auto layer = MakeBoulderLayer(*s);
+        const Terrain below = MakeTerrain(*s, false);
+        const GeoTransform transform = GeoTransform::FromGdal(
+            {s->transform[0], s->transform[1], s->transform[2], s->transform[3], s->transform[4],
+             s->transform[5]});
+        const RasterGrid grid{s->width, s->height, transform};
+        const double spacing = std::fabs(s->transform[1]);
+        const Bounds2d bounds = grid.Bounds().Expanded(0.5 * spacing);
+        const BoulderList list = layer->Boulders(bounds, spacing, &below);
+        const BoulderLayerOptions& options = layer->Options();
+        long count = 0;
+        for (std::size_t i = 0; i < list.Size(); ++i) {
+            const Boulder b = list.At(i);
+            const double weight = ResolutionWeight(b.diameter, spacing, options.fade);
+            if (!options.rendering.reliefRange.Holds(b.diameter, b.model) || weight <= 0.0) {
+                continue;
+            }
+            if (count < n && out != nullptr) {
+                double* o = out + 5 * count;
+                o[0] = b.x;
+                o[1] = b.y;
+                o[2] = b.diameter;
+                o[3] = b.ExposedHeight();
+                o[4] = weight;
+            }
+            ++count;
+        }
+        return count;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// The scene's heights without its boulder layer (the base the boulders are drawn on).
+int tgref_evaluate_below_boulders(const tgref_scene* s, unsigned threads, float* out) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const Terrain terrain = MakeTerrain(*s, false);
+        const GeoTransform transform = GeoTransform::FromGdal(
+            {s->transform[0], s->transform[1], s->transform[2], s->transform[3], s->transform[4],
+             s->transform[5]});
+        EvaluationOptions options;
+        options.threads = threads;
+        options.backend = Backend::Cpu;
+        const Raster<float> heights =
+            terrain.Evaluate(RasterGrid{s->width, s->height, transform}, options);
+        std::memcpy(out, heights.Values().data(), heights.Values().size() * sizeof(float));
+        return 0;
     } catch (const std::exception& error) {
         g_error = error.what();
         return -1;

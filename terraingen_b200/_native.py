@@ -60,6 +60,37 @@ SIGNATURES = {
     "tg_craters_apply_lists": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _P, _P,
                                _P, _U32, _U32, _U32, _P, NoData, _I, _P],
 }
+
+class Population(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("sfd_coefficient", C.c_double),
+                ("sfd_exponent", C.c_double), ("min_diameter", C.c_double),
+                ("max_diameter", C.c_double), ("lifetime_gyr", C.c_double),
+                ("depth_ratio", C.c_double), ("rim_ratio", C.c_double),
+                ("cutoff_depth_ratio", C.c_double), ("cell_size_factor", C.c_double),
+                ("margin_radii", C.c_double), ("min_resolved_diameter", C.c_double)]
+
+
+class Shaping(C.Structure):
+    _fields_ = [("profile", C.c_uint32), ("irregular", C.c_uint32)]
+
+
+class Terrain(C.Structure):
+    _fields_ = [("fractals", _P), ("n_fractals", _U32), ("elevation", _F), ("noise_layer", _P),
+                ("crater_kernel", _P), ("crater_records", _P), ("n_craters", _U32),
+                ("crater_data", _P), ("n_crater_data", _U32), ("crater_footprints", _P),
+                ("boulders", _P), ("n_boulders", _U32), ("boulder_width", _D)]
+
+
+SIGNATURES.update({
+    "tg_evaluate": [_P, C.POINTER(Terrain), C.POINTER(Grid), _P, _I, _P],
+    "tg_measure_alu": [_P, C.POINTER(_D)],
+    "tg_boulders_bake": [_P, _P, _U32, _D, C.POINTER(Grid), _P, NoData, _I, _P],
+    "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,
+                             C.POINTER(_SZ)],
+    "tg_crater_batch": [C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid), _P, _P, _SZ,
+                        _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ)],
+})
+
 RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p}
 
 _lib = None

@@ -34,8 +34,15 @@ UNITS = {
     "diamond_square.cu": ["-fmad=false"],
     "seams.cu": [],
     "batch.cu": [],
+    "probe.cu": [],
     "api.cu": [],
+    "population.cpp": [],
 }
+
+# Host units are compiled by the host compiler with the reference's floating-point flags, so
+# their draws and records round as the reference's do.
+HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", str(CSRC), "-I",
+              str(INCLUDE)]
 
 
 def nvcc() -> str:
@@ -70,6 +77,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objects = []
     for src in sources():
         obj = objdir / (src.stem + ".o")
+        if src.suffix == ".cpp":
+            cxx = shutil.which("g++") or "g++"
+            subprocess.run([cxx, *HOST_FLAGS, *UNITS[src.name], "-c", str(src), "-o", str(obj)],
+                           check=True)
+            objects.append(str(obj))
+            continue
         cmd = [compiler, *ARCH, *COMMON, *UNITS[src.name], "-c", str(src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

@@ -2,6 +2,7 @@
 // staging and kernel launches. Kernels live in noise.cu and craters.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -89,6 +90,9 @@ enum Slot {
     kBinEntries,
     kScan,
     kStatus,
+    kBoulders,
+    kBoulderWindows,
+    kBoulderEntries,
     kProbeIn,
     kProbeHashes,
     kProbeValues,
@@ -465,6 +469,136 @@ int tg_noise_probe(tg_device* d, const float* xy, uint32_t n, uint32_t seed, uin
     return TG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The crater pipeline on device buffers (count, scan, scatter, shape), on stream `s`. It reads
+// the number of binned entries back once to size the bins, and the status word at the end.
+int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
+                   const float* data, const double* foot, const Grid& g, float* dh,
+                   tg_nodata nodata, cudaStream_t s) {
+    if (size_t(g.width) * g.height == 0 || n == 0) {
+        return TG_OK;
+    }
+    CraterBins bins{};
+    bins.binsX = (g.width + kBinCells - 1) / kBinCells;
+    bins.binsY = (g.height + kBinCells - 1) / kBinCells;
+    const uint32_t nbins = bins.binsX * bins.binsY;
+    TG_CUDA(d->slots[kCounts].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kBoxes].reserve(size_t(n) * sizeof(int4)), "allocation");
+    TG_CUDA(d->slots[kCulls].reserve(size_t(n) * sizeof(float)), "allocation");
+    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
+    bins.counts = slot_ptr<uint32_t>(d, kCounts);
+    bins.cursor = slot_ptr<uint32_t>(d, kCursor);
+    bins.boxes = slot_ptr<int4>(d, kBoxes);
+    bins.culls = slot_ptr<float>(d, kCulls);
+    bins.total = slot_ptr<uint32_t>(d, kStatus);
+    TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.total, 0, 4 * sizeof(uint32_t), s), "memset");
+    TG_CUDA(launch_crater_count(k, rec, n, data, foot, g, bins, s), "crater count launch");
+    TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
+            "scan launch");
+    // The entries needed and the datum flag, to size the bins.
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    const uint32_t total = d->pinnedStatus[0];
+    if (d->pinnedStatus[1] & 1u) {
+        return fail(TG_ERROR_UNSUPPORTED,
+                    "craters with a datum need the ordered form (tg_craters_apply_lists)");
+    }
+    if (total == 0) {
+        return TG_OK;
+    }
+    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
+    bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
+    bins.capacity = total;
+    TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
+    const Positions at{0.0, 0.0, nullptr, nullptr};
+    TG_CUDA(launch_crater_shape(k, data, g, at, to_nodata(nodata), bins, dh, s),
+            "crater shape launch");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    if (d->pinnedStatus[1] & 2u) {
+        return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
+    }
+    return TG_OK;
+}
+
+// The boulder pipeline on device buffers (count, scan, scatter, bake), on stream `s`.
+int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double width,
+                    const Grid& g, float* dh, tg_nodata nodata, cudaStream_t s) {
+    if (size_t(g.width) * g.height == 0 || n == 0) {
+        return TG_OK;
+    }
+    BoulderBins bins{};
+    bins.binsX = (g.width + kBinCells - 1) / kBinCells;
+    bins.binsY = (g.height + kBinCells - 1) / kBinCells;
+    const uint32_t nbins = bins.binsX * bins.binsY;
+    TG_CUDA(d->slots[kCounts].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kBoulderWindows].reserve(size_t(n) * sizeof(int4)), "allocation");
+    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
+    bins.counts = slot_ptr<uint32_t>(d, kCounts);
+    bins.cursor = slot_ptr<uint32_t>(d, kCursor);
+    bins.windows = slot_ptr<int4>(d, kBoulderWindows);
+    uint32_t* status = slot_ptr<uint32_t>(d, kStatus);
+    TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), s), "memset");
+    TG_CUDA(launch_boulder_count(rec, n, g, width, bins, s), "boulder count launch");
+    TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
+            "scan launch");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    const uint32_t total = d->pinnedStatus[0];
+    if (total == 0) {
+        return TG_OK;
+    }
+    TG_CUDA(d->slots[kBoulderEntries].reserve(size_t(total) * sizeof(BoulderEntry)), "allocation");
+    bins.entries = slot_ptr<BoulderEntry>(d, kBoulderEntries);
+    bins.capacity = total;
+    TG_CUDA(launch_boulder_scatter(rec, n, bins, s), "boulder scatter launch");
+    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), bins, dh, status, s),
+            "boulder bake launch");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    if (d->pinnedStatus[1] & 2u) {
+        return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
+    }
+    return TG_OK;
+}
+
+int check_boulders(const void* boulders, uint32_t n) {
+    const BoulderRecord* b = static_cast<const BoulderRecord*>(boulders);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!(b[i].diameter > 0.0) || !std::isfinite(b[i].x) || !std::isfinite(b[i].y) ||
+            !(b[i].exposedHeight >= 0.0) || !(b[i].weight >= 0.0 && b[i].weight <= 1.0)) {
+            return fail(TG_ERROR_ARGUMENT, "boulder %u is invalid", i);
+        }
+    }
+    return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, const void* records,
                      uint32_t n, const float* data, uint32_t n_data, const double* footprints,
                      const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
@@ -518,65 +652,12 @@ int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, cons
         TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
                 "copy to device");
     }
-    CraterBins bins{};
-    bins.binsX = (g.width + kBinCells - 1) / kBinCells;
-    bins.binsY = (g.height + kBinCells - 1) / kBinCells;
-    const uint32_t nbins = bins.binsX * bins.binsY;
-    TG_CUDA(d->slots[kCounts].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(d->slots[kBoxes].reserve(size_t(n) * sizeof(int4)), "allocation");
-    TG_CUDA(d->slots[kCulls].reserve(size_t(n) * sizeof(float)), "allocation");
-    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
-    bins.counts = slot_ptr<uint32_t>(d, kCounts);
-    bins.cursor = slot_ptr<uint32_t>(d, kCursor);
-    bins.boxes = slot_ptr<int4>(d, kBoxes);
-    bins.culls = slot_ptr<float>(d, kCulls);
-    bins.total = slot_ptr<uint32_t>(d, kStatus);
-    TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
-    TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
-    TG_CUDA(cudaMemsetAsync(bins.total, 0, 4 * sizeof(uint32_t), s), "memset");
-    const CraterRecord* rec = static_cast<const CraterRecord*>(drec);
-    const float* dd = static_cast<const float*>(ddata);
-    TG_CUDA(launch_crater_count(k, rec, n, dd, static_cast<const double*>(dfoot), g, bins, s),
-            "crater count launch");
-    TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
-            "scan launch");
-    // The entries needed and the datum flag, to size the bins.
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    const uint32_t total = d->pinnedStatus[0];
-    if (d->pinnedStatus[1] & 1u) {
-        return fail(TG_ERROR_UNSUPPORTED,
-                    "craters with a datum need the ordered form (tg_craters_apply_lists)");
+    if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), n,
+                                static_cast<const float*>(ddata), static_cast<const double*>(dfoot),
+                                g, dh, nodata, s)) {
+        return st;
     }
-    if (total == 0) {
-        return copy_heights_back(d, memory, heights, dh, cells);
-    }
-    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
-    bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
-    bins.capacity = total;
-    TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
-    const Positions at{0.0, 0.0, nullptr, nullptr};
-    TG_CUDA(launch_crater_shape(k, dd, g, at, to_nodata(nodata), bins, dh, s),
-            "crater shape launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    if (memory == TG_MEMORY_HOST) {
-        TG_CUDA(cudaMemcpyAsync(heights, dh, cells * sizeof(float), cudaMemcpyDeviceToHost, s),
-                "copy to host");
-    }
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    if (d->pinnedStatus[1] & 2u) {
-        return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
-    }
-    return TG_OK;
+    return copy_heights_back(d, memory, heights, dh, cells);
 }
 
 int tg_craters_apply_lists(tg_device* d, const void* kernel, size_t kernel_bytes,
@@ -674,6 +755,202 @@ int tg_craters_apply_lists(tg_device* d, const void* kernel, size_t kernel_bytes
                 dh, s),
             "crater lists launch");
     return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int tg_boulders_bake(tg_device* d, const void* boulders, uint32_t n, double width,
+                     const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
+                     void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    if (!(width >= 0.0) || !std::isfinite(width)) {
+        return fail(TG_ERROR_ARGUMENT, "the dome width must be finite and not negative");
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    if (cells == 0 || n == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr || boulders == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "heights and boulders are required");
+    }
+    if (memory == TG_MEMORY_HOST) {
+        if (int st = check_boulders(boulders, n)) {
+            return st;
+        }
+    }
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void* db = nullptr;
+    if (int st = stage_in(d, memory, kBoulders, boulders, size_t(n) * sizeof(BoulderRecord), &db)) {
+        return st;
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+        TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
+                "copy to device");
+    }
+    if (int st = boulders_device(d, static_cast<const BoulderRecord*>(db), n, width, g, dh,
+                                 nodata, s)) {
+        return st;
+    }
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* heights,
+                int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (t == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "terrain is null");
+    }
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "heights is null");
+    }
+    if (t->n_fractals > kMaxFractals || (t->n_fractals > 0 && t->fractals == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "at most %u source fractals", kMaxFractals);
+    }
+    FractalStack source;
+    std::memset(&source, 0, sizeof(source));
+    if (t->n_fractals > 0) {
+        std::memcpy(source.fractals, t->fractals, t->n_fractals * sizeof(Fractal));
+    }
+    source.count = t->n_fractals;
+    if (int s = check_stack(source)) {
+        return s;
+    }
+    FractalStack layer;
+    if (t->noise_layer != nullptr) {
+        std::memcpy(&layer, t->noise_layer, sizeof(layer));
+        if (int s = check_stack(layer)) {
+            return s;
+        }
+    }
+    CraterShapeKernel k;
+    if (t->n_craters > 0) {
+        if (t->crater_kernel == nullptr || t->crater_records == nullptr ||
+            (t->n_crater_data > 0 && t->crater_data == nullptr)) {
+            return fail(TG_ERROR_ARGUMENT, "craters need a kernel, records and data");
+        }
+        std::memcpy(&k, t->crater_kernel, sizeof(k));
+    }
+    if (t->n_boulders > 0) {
+        if (t->boulders == nullptr || !(t->boulder_width >= 0.0)) {
+            return fail(TG_ERROR_ARGUMENT, "boulders need records and a width");
+        }
+        if (memory == TG_MEMORY_HOST) {
+            if (int st = check_boulders(t->boulders, t->n_boulders)) {
+                return st;
+            }
+        }
+    }
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void *drec = nullptr, *ddata = nullptr, *dfoot = nullptr, *db = nullptr;
+    if (t->n_craters > 0) {
+        if (int st = stage_in(d, memory, kRecords, t->crater_records,
+                              size_t(t->n_craters) * sizeof(CraterRecord), &drec)) {
+            return st;
+        }
+        if (int st = stage_in(d, memory, kData, t->crater_data,
+                              size_t(t->n_crater_data) * sizeof(float), &ddata)) {
+            return st;
+        }
+        if (t->crater_footprints != nullptr) {
+            if (int st = stage_in(d, memory, kFootprints, t->crater_footprints,
+                                  size_t(t->n_craters) * 3 * sizeof(double), &dfoot)) {
+                return st;
+            }
+        }
+    }
+    if (t->n_boulders > 0) {
+        if (int st = stage_in(d, memory, kBoulders, t->boulders,
+                              size_t(t->n_boulders) * sizeof(BoulderRecord), &db)) {
+            return st;
+        }
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+    }
+    // Terrain::Fill: the source, then each layer in order (src/pipeline/terrain.cpp:299-331).
+    const Positions origin{0.0, 0.0, nullptr, nullptr};
+    TG_CUDA(launch_noise(source, g, origin, true, t->elevation, NoData{0u, 0.0f}, dh, s),
+            "noise source launch");
+    if (t->noise_layer != nullptr) {
+        TG_CUDA(launch_noise(layer, g, origin, false, 0.0f, NoData{0u, 0.0f}, dh, s),
+                "noise layer launch");
+    }
+    if (t->n_craters > 0) {
+        if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,
+                                    static_cast<const float*>(ddata),
+                                    static_cast<const double*>(dfoot), g, dh, tg_nodata{0u, 0.0f},
+                                    s)) {
+            return st;
+        }
+    }
+    if (t->n_boulders > 0) {
+        if (int st = boulders_device(d, static_cast<const BoulderRecord*>(db), t->n_boulders,
+                                     t->boulder_width, g, dh, tg_nodata{0u, 0.0f}, s)) {
+            return st;
+        }
+    }
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int tg_measure_alu(tg_device* d, double* lane_ops_per_second) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (lane_ops_per_second == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "output is null");
+    }
+    TG_CUDA(d->slots[kStatus].reserve(4096 * sizeof(uint32_t)), "allocation");
+    double best = 0.0;
+    cudaEvent_t start, stop;
+    TG_CUDA(cudaEventCreate(&start), "event");
+    TG_CUDA(cudaEventCreate(&stop), "event");
+    for (int rep = 0; rep < 5; ++rep) {
+        uint64_t ops = 0;
+        TG_CUDA(cudaEventRecord(start, d->stream), "event");
+        TG_CUDA(launch_alu_probe(slot_ptr<uint32_t>(d, kStatus), &ops, d->stream), "alu launch");
+        TG_CUDA(cudaEventRecord(stop, d->stream), "event");
+        TG_CUDA(cudaEventSynchronize(stop), "event");
+        float ms = 0.0f;
+        TG_CUDA(cudaEventElapsedTime(&ms, start, stop), "event");
+        if (rep > 0 && ms > 0.0f) {
+            best = std::max(best, double(ops) / (double(ms) * 1e-3));
+        }
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    *lane_ops_per_second = best;
+    return TG_OK;
 }
 
 }  // extern "C"

@@ -1,0 +1,293 @@
+// Boulder relief baking (BoulderLayer::ApplySamples with dome relief,
+// src/layers/boulders/boulder_relief.cpp:426-439): each cell of each boulder's box gets
+// max(height, base + weight * dome), base being the cell's height before the layer
+// (DrawFeatures, include/terraingen/sources/sample_block.h:107-116) and the dome averaged over a
+// sample width (DomeHeight, boulder_relief.cpp:44-57), in double as the reference computes it.
+//
+// Max-compositing is order-free: rounding to float is monotonic, so the result is
+// float(max(height, max over boulders of base + weight * dome)) whatever order boulders come in,
+// which lets them be binned by atomics. Launch structure as crater shaping (craters.cu): count,
+// scan, scatter into kBinCells-square bins, then one CTA per bin stages its entries in shared
+// memory by TMA bulk copies and each thread bakes 4 cells. A boulder touches the cells of its
+// box's pixel window (ForEachFeatureCell, include/terraingen/raster/cell_loops.h:129-152).
+#include "kernels.h"
+
+namespace tgb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCellsPerThread = 4;
+constexpr uint32_t kChunk = 96;  // 64-byte entries per staged chunk (6 KB)
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+__device__ __forceinline__ bool is_nodata(NoData nd, float h) {
+    if (nd.mode == 1u) {
+        return isnan(h);
+    }
+    return nd.mode != 0u && h == nd.value;
+}
+
+// The pixel window of a box on the grid (PixelWindowIn, src/raster/cell_loops.cpp:21-28).
+__device__ void window_of(const Grid& g, double minX, double minY, double maxX, double maxY,
+                          int& c0, int& c1, int& r0, int& r1) {
+    const double det = g.pixelWidth * g.pixelHeight - g.rowRotation * g.colRotation;
+    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+    const double xs[2] = {minX, maxX}, ys[2] = {minY, maxY};
+    for (int a = 0; a < 2; ++a) {
+        for (int b = 0; b < 2; ++b) {
+            const double dx = xs[a] - g.originX, dy = ys[b] - g.originY;
+            const double px = (dx * g.pixelHeight - dy * g.rowRotation) / det;
+            const double py = (dy * g.pixelWidth - dx * g.colRotation) / det;
+            lo[0] = fmin(lo[0], px);
+            lo[1] = fmin(lo[1], py);
+            hi[0] = fmax(hi[0], px);
+            hi[1] = fmax(hi[1], py);
+        }
+    }
+    auto clampi = [](double v, uint32_t limit) {
+        return int(v < 0.0 ? 0.0 : (double(limit) < v ? double(limit) : v));
+    };
+    c0 = clampi(floor(lo[0]), g.width);
+    c1 = clampi(ceil(hi[0]), g.width);
+    r0 = clampi(floor(lo[1]), g.height);
+    r1 = clampi(ceil(hi[1]), g.height);
+}
+
+__global__ void boulder_count_kernel(const BoulderRecord* __restrict__ boulders, uint32_t n,
+                                     const Grid grid, double width, BoulderBins bins) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const BoulderRecord b = boulders[i];
+    // ReliefBox on a plane (boulder_relief.cpp:24): reach 0.5 (diameter + width).
+    const double reach = 0.5 * (b.diameter + width);
+    int c0, c1, r0, r1;
+    window_of(grid, b.x - reach, b.y - reach, b.x + reach, b.y + reach, c0, c1, r0, r1);
+    const bool drawn = c0 < c1 && r0 < r1 && b.weight > 0.0;
+    bins.windows[i] = drawn ? make_int4(c0, c1, r0, r1) : make_int4(1, 0, 1, 0);
+    if (!drawn) {
+        return;
+    }
+    const uint32_t bx0 = uint32_t(c0) / kBinCells, bx1 = uint32_t(c1 - 1) / kBinCells;
+    const uint32_t by0 = uint32_t(r0) / kBinCells, by1 = uint32_t(r1 - 1) / kBinCells;
+    for (uint32_t by = by0; by <= by1; ++by) {
+        for (uint32_t bx = bx0; bx <= bx1; ++bx) {
+            atomicAdd(bins.counts + by * bins.binsX + bx, 1u);
+        }
+    }
+}
+
+__global__ void boulder_scatter_kernel(const BoulderRecord* __restrict__ boulders, uint32_t n,
+                                       BoulderBins bins) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const int4 w = bins.windows[i];
+    if (w.x >= w.y) {
+        return;
+    }
+    const BoulderRecord b = boulders[i];
+    BoulderEntry e;
+    e.x = b.x;
+    e.y = b.y;
+    e.radius = 0.5 * b.diameter;
+    e.exposed = b.exposedHeight;
+    e.weight = b.weight;
+    e.c0 = w.x;
+    e.c1 = w.y;
+    e.r0 = w.z;
+    e.r1 = w.w;
+    const uint32_t bx0 = uint32_t(w.x) / kBinCells, bx1 = uint32_t(w.y - 1) / kBinCells;
+    const uint32_t by0 = uint32_t(w.z) / kBinCells, by1 = uint32_t(w.w - 1) / kBinCells;
+    for (uint32_t by = by0; by <= by1; ++by) {
+        for (uint32_t bx = bx0; bx <= bx1; ++bx) {
+            const uint32_t bin = by * bins.binsX + bx;
+            const uint32_t slot = bins.counts[bin] + atomicAdd(bins.cursor + bin, 1u);
+            if (slot < bins.capacity) {
+                bins.entries[slot] = e;
+            }
+        }
+    }
+}
+
+// DomeHeight (boulder_relief.cpp:44): the dome's height at `distance` averaged over a band
+// `width` wide, or at the point for a zero width.
+__device__ __forceinline__ double dome(const BoulderEntry& b, double distance, double width) {
+    const double radius = b.radius;
+    if (!(width > 0.0)) {
+        const double r2 = (distance * distance) / (radius * radius);
+        return r2 < 1.0 ? b.exposed * sqrt(1.0 - r2) : 0.0;
+    }
+    auto area = [](double u) { return 0.5 * (u * sqrt(1.0 - u * u) + asin(u)); };
+    const double low = fmin(fmax((distance - 0.5 * width) / radius, -1.0), 1.0);
+    const double high = fmin(fmax((distance + 0.5 * width) / radius, -1.0), 1.0);
+    if (!(high > low)) {
+        return 0.0;
+    }
+    return b.exposed * (area(high) - area(low)) * radius / width;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+
+__global__ void __launch_bounds__(kThreads)
+    boulder_bake_kernel(const Grid grid, const double width, const NoData nodata,
+                        const BoulderBins bins, float* __restrict__ heights,
+                        uint32_t* __restrict__ flags) {
+    __shared__ __align__(128) BoulderEntry stage[2][kChunk];
+    __shared__ __align__(8) uint64_t bars[2];
+    const uint32_t bin = blockIdx.x;
+    const uint32_t first = bins.counts[bin];
+    const uint32_t count = bins.counts[bin + 1] - first;
+    if (count == 0u) {
+        return;
+    }
+    const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const int row = int(binY * kBinCells + warp * 4u + lane / 8u);
+    const int col0 = int(binX * kBinCells + (lane % 8u) * kCellsPerThread);
+    const bool rowIn = row < int(grid.height);
+    // Cell centers in double (Raster::CellCenter), the base heights and the running maxima.
+    const double cy = grid.originY + (double(col0) + 0.5) * grid.colRotation +
+                      (double(row) + 0.5) * grid.pixelHeight;
+    double cx[kCellsPerThread], best[kCellsPerThread];
+    float base[kCellsPerThread];
+    bool live[kCellsPerThread];
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        const int col = col0 + j;
+        cx[j] = grid.originX + (double(col) + 0.5) * grid.pixelWidth +
+                (double(row) + 0.5) * grid.rowRotation;
+        live[j] = rowIn && col < int(grid.width);
+        base[j] = 0.0f;
+        if (live[j]) {
+            base[j] = heights[size_t(row) * grid.width + col];
+            live[j] = !is_nodata(nodata, base[j]);
+        }
+        best[j] = double(base[j]);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const uint32_t chunks = (count + kChunk - 1) / kChunk;
+    auto issue = [&](uint32_t c) {
+        const uint32_t s = c & 1u;
+        const uint32_t bytes = min(kChunk, count - c * kChunk) * uint32_t(sizeof(BoulderEntry));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_addr(&bars[s])),
+                     "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(smem_addr(&stage[s][0])),
+            "l"(bins.entries + first + c * kChunk), "r"(bytes), "r"(smem_addr(&bars[s]))
+            : "memory");
+    };
+    if (tid == 0) {
+        issue(0);
+        if (chunks > 1) {
+            issue(1);
+        }
+    }
+    uint32_t phase[2] = {0u, 0u};
+    for (uint32_t c = 0; c < chunks; ++c) {
+        const uint32_t s = c & 1u;
+        bool arrived = false;
+        for (uint32_t spin = 0; spin < kSpinLimit && !arrived; ++spin) {
+            uint32_t done;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n "
+                "selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(smem_addr(&bars[s])), "r"(phase[s])
+                : "memory");
+            arrived = done != 0u;
+        }
+        phase[s] ^= 1u;
+        if (__syncthreads_or(!arrived)) {
+            if (tid == 0) {
+                atomicOr(flags, 2u);
+            }
+            return;
+        }
+        const uint32_t n = min(kChunk, count - c * kChunk);
+        for (uint32_t e = 0; e < n; ++e) {
+            const BoulderEntry& b = stage[s][e];
+            const bool inRows = row >= b.r0 && row < b.r1;
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                any |= live[j] && inRows && col0 + j >= b.c0 && col0 + j < b.c1;
+            }
+            if (!__any_sync(0xffffffffu, any)) {
+                continue;
+            }
+            const double dy = cy - b.y;
+#pragma unroll
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                if (live[j] && inRows && col0 + j >= b.c0 && col0 + j < b.c1) {
+                    const double dx = cx[j] - b.x;
+                    // RockRelief without facets: the dome, not below 0 (boulder.h:90-95).
+                    const double relief = fmax(dome(b, hypot(dx, dy), width), 0.0);
+                    if (relief > 0.0) {
+                        best[j] = fmax(best[j], double(base[j]) + b.weight * relief);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && c + 2 < chunks) {
+            issue(c + 2);
+        }
+    }
+    if (!rowIn) {
+        return;
+    }
+    float* dst = heights + size_t(row) * grid.width + col0;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        if (live[j]) {
+            dst[j] = float(best[j]);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_boulder_count(const BoulderRecord* boulders, uint32_t n, const Grid& grid,
+                                 double width, const BoulderBins& bins, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    boulder_count_kernel<<<(n + 255) / 256, 256, 0, stream>>>(boulders, n, grid, width, bins);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
+                                   const BoulderBins& bins, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    boulder_scatter_kernel<<<(n + 255) / 256, 256, 0, stream>>>(boulders, n, bins);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
+                                const BoulderBins& bins, float* heights, uint32_t* flags,
+                                cudaStream_t stream) {
+    const uint32_t nbins = bins.binsX * bins.binsY;
+    if (nbins == 0) {
+        return cudaSuccess;
+    }
+    boulder_bake_kernel<<<nbins, kThreads, 0, stream>>>(grid, width, nodata, bins, heights, flags);
+    return cudaGetLastError();
+}
+
+}  // namespace tgb

@@ -97,6 +97,43 @@ cudaError_t launch_crater_shape_lists(const CraterShapeKernel& k, const CraterRe
                                       const float* ys, const float* yLows, NoData nodata,
                                       float* heights, cudaStream_t stream);
 
+// --- boulders ------------------------------------------------------------------------------
+// One boulder drawn as a dome (tg_boulder in include/tgb200.h).
+struct BoulderRecord {
+    double x, y, diameter, exposedHeight, weight;
+};
+static_assert(sizeof(BoulderRecord) == 40, "BoulderRecord is 5 doubles");
+
+// A boulder in a bin: its center, radius, exposed height, weight and pixel window
+// [c0, c1) x [r0, r1). 64 bytes, so bins copy to shared memory in 16-byte units.
+struct BoulderEntry {
+    double x, y, radius, exposed, weight;
+    int32_t c0, c1, r0, r1;
+    double pad_;
+};
+static_assert(sizeof(BoulderEntry) == 64, "BoulderEntry must be a multiple of 16 bytes");
+
+struct BoulderBins {
+    uint32_t binsX, binsY;
+    uint32_t* counts;  // [bins + 1]
+    uint32_t* cursor;  // [bins]
+    BoulderEntry* entries;
+    uint32_t capacity;
+    int4* windows;     // [boulders]
+};
+
+cudaError_t launch_boulder_count(const BoulderRecord* boulders, uint32_t n, const Grid& grid,
+                                 double width, const BoulderBins& bins, cudaStream_t stream);
+cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
+                                   const BoulderBins& bins, cudaStream_t stream);
+cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
+                                const BoulderBins& bins, float* heights, uint32_t* flags,
+                                cudaStream_t stream);
+
+// The ALU issue-rate probe (probe.cu): one launch of a fixed IMAD/FFMA mix; `laneOps` receives
+// the lane operations it performs.
+cudaError_t launch_alu_probe(uint32_t* sink, uint64_t* laneOps, cudaStream_t stream);
+
 // Exclusive prefix sum of n counts in place, writing the total to counts[n]. `scratch` holds
 // scan_scratch_words(n) words.
 size_t scan_scratch_words(uint32_t n);

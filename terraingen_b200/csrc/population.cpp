@@ -1,0 +1,548 @@
+// Host-side crater populations and kernel records on a plane: what a CraterLayer's ApplySamples
+// hands the crater kernel, restated so the batched and served forms (and the benchmarks) can
+// build their own batches without the reference library.
+//
+// The random draws must be the reference's bit for bit (the determinism contract,
+// include/terraingen/pipeline/terrain.h:65-67), so the steps are kept in the reference's order:
+//   Philox4x32-10 and RandomStream        (include/terraingen/random/philox.h:82, stream.cpp:7-27)
+//   SamplePoisson (multiplication / PTRS) (src/random/samplers.cpp:14-55)
+//   CraterBands, GenerateCellCraters,
+//   the band plan and DrawKept filters    (src/layers/craters/generation/population.cpp)
+//   CraterApplyOrder, ResolutionWeight    (apply_options.cpp:96, src/layers/fade.cpp:50)
+//   FreshnessDegradation::State           (degradation/freshness_degradation.cpp)
+//   IrregularOutline, power-law harmonics (shaping/irregularity.cpp:165-260)
+//   BaseRecord / AppendKernelOutline      (shaping/crater_kernel.cpp:187, irregularity.cpp:295)
+// This file is compiled with -ffp-contract=off and uses the host libm, as the reference does.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tgb200.h"
+#include "layouts.h"
+
+namespace tgb {
+namespace host {
+
+// --- Philox4x32-10 and the keyed streams ----------------------------------------------------
+
+struct Words4 {
+    uint32_t x, y, z, w;
+};
+
+inline Words4 philox(Words4 c, uint32_t k0, uint32_t k1) {
+    for (int round = 0; round < 10; ++round) {
+        if (round > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = uint64_t(0xD2511F53u) * c.x;
+        const uint64_t p1 = uint64_t(0xCD9E8D57u) * c.z;
+        c = Words4{uint32_t(p1 >> 32) ^ c.y ^ k0, uint32_t(p1), uint32_t(p0 >> 32) ^ c.w ^ k1,
+                   uint32_t(p0)};
+    }
+    return c;
+}
+
+// Stream tags (include/terraingen/random/streams.h:15-26).
+constexpr uint32_t kCraterStream = 0x43524154u;
+constexpr uint32_t kCraterAgeStream = 0x43524147u;
+constexpr uint32_t kCraterIdStream = 0x43524944u;
+constexpr uint32_t kCraterSlopeStream = 0x534C4F50u;
+constexpr uint32_t kCraterTerraceStream = 0x54455252u;
+constexpr uint32_t kCraterPeakStream = 0x5045414Bu;
+constexpr uint32_t kCraterIrregularityStream = 0x49525247u;
+constexpr uint32_t kCraterTextureStream = 0x54455854u;
+constexpr uint32_t kCraterNoiseStream = 0x434E4F53u;
+
+class Stream {
+  public:
+    Stream(uint32_t seed, uint32_t stream, uint32_t a = 0, uint32_t b = 0, uint32_t c = 0)
+        : k0_(seed), k1_(stream), counter_{a, b, c, 0u} {}
+
+    uint32_t next_u32() {
+        if (used_ == 4) {
+            block_ = philox(counter_, k0_, k1_);
+            ++counter_.w;
+            used_ = 0;
+        }
+        const uint32_t words[4] = {block_.x, block_.y, block_.z, block_.w};
+        return words[used_++];
+    }
+
+    double next_double() {
+        const uint64_t high = next_u32() >> 5u;
+        const uint64_t low = next_u32() >> 6u;
+        return double((high << 26u) | low) * 0x1p-53;
+    }
+
+  private:
+    uint32_t k0_, k1_;
+    Words4 counter_;
+    Words4 block_{};
+    int used_ = 4;
+};
+
+uint32_t substream_seed(uint32_t seed, uint32_t stream, uint32_t a = 0) {
+    return philox(Words4{a, 0u, 0u, 0xFFFFFFFFu}, seed, stream).x;
+}
+
+uint32_t pcg(uint32_t v) {  // include/terraingen/noise/hash.h:33
+    const uint32_t state = v * 747796405u + 2891336453u;
+    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+uint32_t crater_key(uint64_t id, uint32_t seed) {  // crater.h:99, hash.h:68 HashWord64
+    return pcg(uint32_t(id) ^ pcg(uint32_t(id >> 32u) ^ seed));
+}
+
+uint64_t poisson(Stream& random, double mean) {
+    if (mean == 0.0) {
+        return 0;
+    }
+    if (mean < 10.0) {
+        const double limit = std::exp(-mean);
+        uint64_t count = 0;
+        double product = random.next_double();
+        while (product > limit) {
+            ++count;
+            product *= random.next_double();
+        }
+        return count;
+    }
+    // Hoermann's transformed rejection with squeeze (PTRS).
+    const double sqrtMean = std::sqrt(mean);
+    const double logMean = std::log(mean);
+    const double b = 0.931 + 2.53 * sqrtMean;
+    const double a = -0.059 + 0.02483 * b;
+    const double inverseAlpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    while (true) {
+        const double u = random.next_double() - 0.5;
+        const double v = random.next_double();
+        const double us = 0.5 - std::fabs(u);
+        const double k = std::floor((2.0 * a / us + b) * u + mean + 0.43);
+        if (us >= 0.07 && v <= vr) {
+            return uint64_t(k);
+        }
+        if (k < 0.0 || (us < 0.013 && v > us)) {
+            continue;
+        }
+        if (std::log(v) + std::log(inverseAlpha) - std::log(a / (us * us) + b) <=
+            -mean + k * logMean - std::lgamma(k + 1.0)) {
+            return uint64_t(k);
+        }
+    }
+}
+
+// --- the population ---------------------------------------------------------------------------
+
+struct Box {
+    double minX, minY, maxX, maxY;
+    Box expanded(double m) const { return Box{minX - m, minY - m, maxX + m, maxY + m}; }
+    bool contains(double x, double y) const {
+        return x >= minX && x < maxX && y >= minY && y < maxY;
+    }
+};
+
+struct Crater {
+    double x, y, diameter, age;
+    uint64_t id;
+};
+
+struct Band {
+    int exponent;
+    double low, high, cellSize;
+};
+
+std::vector<Band> crater_bands(double minD, double maxD, double factor) {
+    std::vector<Band> bands;
+    for (int k = std::ilogb(minD); std::ldexp(1.0, k) < maxD; ++k) {
+        const double low = std::fmax(minD, std::ldexp(1.0, k));
+        const double high = std::fmin(maxD, std::ldexp(1.0, k + 1));
+        bands.push_back({k, low, high, factor * std::ldexp(1.0, k + 1)});
+    }
+    return bands;
+}
+
+struct PowerLaw {
+    double c, e;
+    double cumulative(double d) const { return c * std::pow(d, -e); }
+    double expected(double lo, double hi) const { return 1.0 * (cumulative(lo) - cumulative(hi)); }
+    double sample(Stream& random, double lo, double hi) const {
+        const double count = expected(lo, hi);
+        const double top = cumulative(lo);
+        const double target = top - random.next_double() * count;
+        return std::clamp(std::pow(target / c, -1.0 / e), lo, hi);
+    }
+};
+
+int32_t cell_coordinate(double v) {
+    return int32_t(v);
+}
+
+// GenerateCellCraters on a plane (population.cpp:381).
+std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const PowerLaw& law,
+                                 double lifetime, uint32_t seed) {
+    const uint32_t k = uint32_t(band.exponent);
+    Stream geometry(seed, kCraterStream, uint32_t(i), uint32_t(j), k);
+    Stream ages(seed, kCraterAgeStream, uint32_t(i), uint32_t(j), k);
+    const double perArea = law.expected(band.low, band.high);
+    const double area = band.cellSize * band.cellSize;
+    const uint64_t count = poisson(geometry, perArea * area);
+    std::vector<Crater> out;
+    out.reserve(size_t(count));
+    for (uint64_t index = 0; index < count; ++index) {
+        const double diameter = law.sample(geometry, band.low, band.high);
+        const double u = geometry.next_double();
+        const double v = geometry.next_double();
+        const double x = (i + u) * band.cellSize;
+        const double y = (j + v) * band.cellSize;
+        const double age = std::clamp(ages.next_double() * lifetime, 0.0, lifetime);
+        const Words4 id = philox(Words4{uint32_t(i), uint32_t(j), k, uint32_t(index)}, seed,
+                                 kCraterIdStream);
+        out.push_back({x, y, diameter, age, (uint64_t(id.x) << 32) | id.y});
+    }
+    return out;
+}
+
+// Craters over `region` with their candidate margin (GenerateCraters, planar, no spacing,
+// density map or manual craters).
+std::vector<Crater> generate(const tg_crater_population& spec, const Box& region) {
+    const PowerLaw law{spec.sfd_coefficient, spec.sfd_exponent};
+    const double marginRadii = spec.margin_radii;
+    auto margin = [&](double d) { return 0.5 * marginRadii * d; };
+    std::vector<Crater> out;
+    for (const Band& band : crater_bands(spec.min_diameter, spec.max_diameter,
+                                         spec.cell_size_factor)) {
+        if (band.high <= spec.min_resolved_diameter) {
+            continue;
+        }
+        const Box cover = region.expanded(margin(band.high));
+        const int32_t iMin = cell_coordinate(std::floor(cover.minX / band.cellSize));
+        const int32_t jMin = cell_coordinate(std::floor(cover.minY / band.cellSize));
+        const int32_t iMax = cell_coordinate(std::ceil(cover.maxX / band.cellSize) - 1.0);
+        const int32_t jMax = cell_coordinate(std::ceil(cover.maxY / band.cellSize) - 1.0);
+        const Box inner = region.expanded(margin(band.low));
+        const Box outer = region.expanded(margin(band.high));
+        for (int32_t j = jMin; j <= jMax; ++j) {
+            for (int32_t i = iMin; i <= iMax; ++i) {
+                std::vector<Crater> list = cell_craters(band, i, j, law, spec.lifetime_gyr,
+                                                        spec.seed);
+                // CellCraters::Rows(outer y range): the draw order, filtered by y.
+                for (const Crater& c : list) {
+                    if (!(c.y >= outer.minY && c.y <= outer.maxY)) {
+                        continue;
+                    }
+                    const bool inBand = c.diameter >= band.low && c.diameter <= band.high;
+                    if (inBand && !outer.contains(c.x, c.y)) {
+                        continue;
+                    }
+                    bool keep;
+                    if (!inBand) {
+                        keep = region.expanded(margin(c.diameter)).contains(c.x, c.y);
+                    } else {
+                        keep = inner.contains(c.x, c.y) ||
+                               region.expanded(margin(c.diameter)).contains(c.x, c.y);
+                    }
+                    if (keep) {
+                        out.push_back(c);
+                    }
+                }
+            }
+        }
+    }
+    return out;
+}
+
+// --- preparation and records ----------------------------------------------------------------
+
+double smoothstep(double t) {
+    t = std::clamp(t, 0.0, 1.0);
+    return t * t * (3.0 - 2.0 * t);
+}
+
+double resolution_weight(double diameter, double spacing) {
+    // 1 - Falloff(D / spacing, 2, 4, Smoothstep) (src/layers/fade.cpp:18-52)
+    const double x = diameter / spacing;
+    double f;
+    if (x <= 2.0) {
+        f = 1.0;
+    } else if (x >= 4.0) {
+        f = 0.0;
+    } else {
+        f = 1.0 - smoothstep((x - 2.0) / 2.0);
+    }
+    return 1.0 - f;
+}
+
+struct Outline {
+    double ellipticity = 1.0, heading = 0.0;
+    std::vector<double> amplitudes, phases;
+    int firstHarmonic = 2;
+};
+
+// IrregularOutline with the default irregularity (power-law harmonics 2-12, roughness uniform
+// in [0.01, 0.03], slope 1.5, 5.4% elliptical with ellipticity uniform in [1.1, 1.5]).
+Outline irregular_outline(const Crater& c, uint32_t seed) {
+    Outline o;
+    Stream random(seed, kCraterIrregularityStream, uint32_t(c.id), uint32_t(c.id >> 32));
+    double d[9];
+    for (double& v : d) {
+        v = random.next_double();
+    }
+    const double rough = d[0], elongated = d[1], r1 = d[2], s1 = d[4], e1 = d[6], h = d[8];
+    (void)s1;
+    if (elongated < 0.054) {
+        o.ellipticity = 1.1 + (1.5 - 1.1) * e1;  // clamped to (-inf, inf)
+        o.heading = 3.14159265358979323846 * h;
+    }
+    if (rough < 1.0) {
+        const double roughness = 0.01 + (0.03 - 0.01) * r1;  // clamped to (-inf, inf)
+        const double slope = 1.5;
+        double sum = 0.0;
+        for (int k = 2; k <= 12; ++k) {
+            sum += std::pow(double(k), -2.0 * slope);
+        }
+        const double norm = roughness * std::sqrt(2.0 / sum);
+        o.firstHarmonic = 2;
+        if (roughness > 0.0) {
+            for (int k = 2; k <= 12; ++k) {
+                o.amplitudes.push_back(norm * std::pow(double(k), -slope));
+                o.phases.push_back(2.0 * 3.14159265358979323846 * random.next_double());
+            }
+        }
+    }
+    return o;
+}
+
+double max_outline_scale(bool irregular) {  // MaxOutlineScale (irregularity.cpp:279)
+    if (!irregular) {
+        return 1.0;
+    }
+    const double rough = 1.0 + 0.03 * std::sqrt(2.0 * 11);
+    return rough * std::sqrt(1.5);
+}
+
+}  // namespace host
+}  // namespace tgb
+
+using namespace tgb;
+using namespace tgb::host;
+
+namespace {
+thread_local std::string g_population_error;
+}
+
+extern "C" {
+
+int tg_crater_generate(const tg_crater_population* spec, const double* region, double* x,
+                         double* y, double* diameter, double* age, uint64_t* id, size_t capacity,
+                         size_t* count) {
+    if (spec == nullptr || region == nullptr || count == nullptr) {
+        return TG_ERROR_ARGUMENT;
+    }
+    if (!(spec->min_diameter > 0.0) || !(spec->max_diameter > spec->min_diameter) ||
+        !std::isfinite(spec->max_diameter) || !(spec->sfd_coefficient > 0.0) ||
+        !(spec->sfd_exponent > 0.0) || !(spec->lifetime_gyr > 0.0) ||
+        !(spec->cell_size_factor > 0.0) || !(region[2] >= region[0]) ||
+        !(region[3] >= region[1])) {
+        return TG_ERROR_ARGUMENT;
+    }
+    const std::vector<Crater> craters =
+        generate(*spec, Box{region[0], region[1], region[2], region[3]});
+    *count = craters.size();
+    for (size_t n = 0; n < craters.size() && n < capacity; ++n) {
+        if (x) x[n] = craters[n].x;
+        if (y) y[n] = craters[n].y;
+        if (diameter) diameter[n] = craters[n].diameter;
+        if (age) age[n] = craters[n].age;
+        if (id) id[n] = craters[n].id;
+    }
+    return TG_OK;
+}
+
+int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* shaping,
+                    const tg_grid* grid, void* kernel, void* records, size_t record_capacity,
+                    float* data, size_t data_capacity, double* footprints, size_t* n_records,
+                    size_t* n_data) {
+    if (spec == nullptr || shaping == nullptr || grid == nullptr || n_records == nullptr ||
+        n_data == nullptr) {
+        return TG_ERROR_ARGUMENT;
+    }
+    if (grid->row_rotation != 0.0 || grid->col_rotation != 0.0 || !(grid->pixel_width > 0.0) ||
+        !(grid->pixel_height < 0.0)) {
+        return TG_ERROR_UNSUPPORTED;
+    }
+    const double spacing = std::max(grid->pixel_width, -grid->pixel_height);
+    // The grid's bounds (its cell edges), the region CraterLayer::ApplySamples draws over.
+    const Box bounds{grid->origin_x, grid->origin_y + grid->height * grid->pixel_height,
+                     grid->origin_x + grid->width * grid->pixel_width, grid->origin_y};
+    tg_crater_population p = *spec;
+    const bool irregular = shaping->irregular != 0;
+    const double reachRadii = shaping->profile == 1 ? 2.0 : 1.5;  // MPD reaches 2 R, FT 1.5 R
+    p.margin_radii = reachRadii * max_outline_scale(irregular);
+    p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
+    std::vector<Crater> craters = generate(p, bounds);
+
+    // CraterApplyOrder, oldest first (apply_options.cpp:96).
+    std::vector<size_t> order(craters.size());
+    for (size_t n = 0; n < order.size(); ++n) {
+        order[n] = n;
+    }
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        const Crater& ca = craters[a];
+        const Crater& cb = craters[b];
+        if (ca.age != cb.age) {
+            return ca.age > cb.age;
+        }
+        if (ca.diameter != cb.diameter) {
+            return ca.diameter > cb.diameter;
+        }
+        return ca.id != cb.id ? ca.id < cb.id : a < b;
+    });
+
+    // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
+    const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
+    const uint32_t noiseSeed = substream_seed(spec->seed, kCraterNoiseStream);
+    const uint32_t textureSeed = substream_seed(spec->seed, kCraterTextureStream);
+    const uint32_t textureKeySeed = substream_seed(textureSeed, kCraterTextureStream);
+
+    std::vector<CraterRecord> out;
+    std::vector<float> values;
+    std::vector<double> foot;
+    for (const size_t n : order) {
+        const Crater& c = craters[n];
+        const double resolution = resolution_weight(c.diameter, spacing);
+        if (resolution == 0.0) {
+            continue;
+        }
+        const Outline outline = irregular ? irregular_outline(c, irregularitySeed) : Outline{};
+        // CratersOnRaster: the footprint window must hold a cell of the grid.
+        double scale = 1.0;
+        for (const double a : outline.amplitudes) {
+            scale += std::fabs(a);
+        }
+        scale *= std::sqrt(outline.ellipticity);
+        const double reach = scale * reachRadii * (0.5 * c.diameter);
+        // Surface::Expand, then MappedBounds of GeoTransform::WorldToPixel over the box's corners
+        // (src/raster/cell_loops.cpp:21-28, geo_transform.h:70), then ClampIndex.
+        const double det =
+            grid->pixel_width * grid->pixel_height - grid->row_rotation * grid->col_rotation;
+        double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
+        for (const double wx : {c.x - reach, c.x + reach}) {
+            for (const double wy : {c.y - reach, c.y + reach}) {
+                const double dx = wx - grid->origin_x;
+                const double dy = wy - grid->origin_y;
+                const double px = (dx * grid->pixel_height - dy * grid->row_rotation) / det;
+                const double py = (dy * grid->pixel_width - dx * grid->col_rotation) / det;
+                minX = std::fmin(minX, px);
+                minY = std::fmin(minY, py);
+                maxX = std::fmax(maxX, px);
+                maxY = std::fmax(maxY, py);
+            }
+        }
+        const double w = grid->width, h = grid->height;
+        const double c0 = std::clamp(std::floor(minX), 0.0, w);
+        const double c1 = std::clamp(std::ceil(maxX), 0.0, w);
+        const double r0 = std::clamp(std::floor(minY), 0.0, h);
+        const double r1 = std::clamp(std::ceil(maxY), 0.0, h);
+        if (!(size_t(c0) < size_t(c1) && size_t(r0) < size_t(r1))) {
+            continue;
+        }
+        // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
+        const double freshDepth = spec->depth_ratio, freshRim = spec->rim_ratio;
+        const double floorShare = std::fmin(spec->cutoff_depth_ratio / freshDepth, 1.0);
+        const double remaining = std::clamp(1.0 - c.age / spec->lifetime_gyr, 0.0, 1.0);
+        const double erosion = floorShare + (1.0 - floorShare) * remaining;
+        CraterRecord r{};
+        r.diameter = float(c.diameter);
+        r.freshDepth = float(freshDepth);
+        r.freshRim = float(freshRim);
+        r.currentDepth = float(erosion * freshDepth);
+        r.currentRim = float(erosion * freshRim);
+        r.diffusion = 0.0f;
+        r.resolution = float(resolution);
+        r.noiseKey = crater_key(c.id, noiseSeed);
+        r.textureKey = crater_key(c.id, textureKeySeed);
+        r.x = float(c.x);
+        r.xLow = float(c.x - double(r.x));
+        r.y = float(c.y);
+        r.yLow = float(c.y - double(r.y));
+        r.ellipticity = float(outline.ellipticity);
+        r.heading = float(outline.heading);
+        r.harmonicOffset = uint32_t(values.size());
+        r.firstHarmonic = uint32_t(outline.firstHarmonic);
+        r.harmonicCount = uint32_t(outline.amplitudes.size());
+        for (size_t k = 0; k < outline.amplitudes.size(); ++k) {
+            values.push_back(float(outline.amplitudes[k]));
+            values.push_back(float(outline.phases[k]));
+        }
+        r.tableCount = 0;
+        r.tableOffset = uint32_t(values.size());
+        r.markCount = 0;
+        r.markOffset = uint32_t(values.size());
+        out.push_back(r);
+        foot.push_back(c.x);
+        foot.push_back(c.y);
+        foot.push_back(reach);
+    }
+    if (values.empty()) {
+        values.push_back(0.0f);
+    }
+    *n_records = out.size();
+    *n_data = values.size();
+    if (kernel != nullptr) {
+        // MakeCraterShapeKernel (crater_kernel.cpp:277) for a simple FT or MPD profile and the
+        // default shaping options.
+        CraterShapeKernel k{};
+        k.profile.simple = shaping->profile == 1 ? kProfileMartinParkesDunstan
+                                                 : kProfileFassettThomson;
+        k.profile.ejectaExponent = 3.0f;
+        k.profile.complexReachRadii = 3.0f;
+        k.profile.tableExtent = 1.5f;
+        k.reachRadii = float(reachRadii);
+        k.profileReachRadii = float(reachRadii);
+        k.blendStart = 0.8f;
+        k.blendEnd = 1.2f;
+        k.blendShape = 2u;
+        k.replaceStart = 1.0f;
+        k.replaceEnd = float(reachRadii);
+        k.ejectaReachRadii = 3.0f;
+        k.rimInner = 0.8f;
+        k.rimOuter = 1.2f;
+        k.rimStrength = 1.0f;
+        k.rimShape = 2u;
+        k.noiseWavelength = 0.5f;
+        k.noiseOctaves = 4;
+        k.noiseGain = 0.5f;
+        k.noiseRimWavelength = 0.1f;
+        k.noiseRimInner = 0.8f;
+        k.noiseRimOuter = 1.2f;
+        k.wallStreakWidth = 0.15f;
+        k.ejectaLineation = 0.15f;
+        k.minFreshness = 0.5f;
+        std::memcpy(kernel, &k, sizeof(k));
+    }
+    if (records != nullptr) {
+        if (record_capacity < out.size()) {
+            return TG_ERROR_ARGUMENT;
+        }
+        std::memcpy(records, out.data(), out.size() * sizeof(CraterRecord));
+    }
+    if (data != nullptr) {
+        if (data_capacity < values.size()) {
+            return TG_ERROR_ARGUMENT;
+        }
+        std::memcpy(data, values.data(), values.size() * sizeof(float));
+    }
+    if (footprints != nullptr && record_capacity >= out.size()) {
+        std::memcpy(footprints, foot.data(), foot.size() * sizeof(double));
+    }
+    return TG_OK;
+}
+
+}  // extern "C"

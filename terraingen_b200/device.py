@@ -176,6 +176,69 @@ class Device:
                                          N.TG_MEMORY_HOST))
         return hashes, values
 
+    # --- whole evaluations ----------------------------------------------------------------
+    def evaluate(self, grid: GridSpec, heights, fractals=None, elevation: float = 0.0,
+                 noise_layer=None, craters=None, boulders=None, boulder_width: float = 0.0):
+        """Terrain::Evaluate of a source + noise / crater / boulder stack (tg_evaluate).
+        `craters` is (kernel, records, data[, footprints]); host arrays or device tensors alike,
+        as the heights are."""
+        b = _Buffers()
+        h = b.ptr(heights, np.float32)
+        t = N.Terrain()
+        keep = []
+        if fractals is not None:
+            fr = _bytes(np.atleast_1d(fractals), FRACTAL)
+            keep.append(fr)
+            t.fractals, t.n_fractals = fr.ctypes.data, len(fr)
+        t.elevation = elevation
+        if noise_layer is not None:
+            nl = _bytes(noise_layer, NOISE_LAYER_KERNEL)
+            keep.append(nl)
+            t.noise_layer = nl.ctypes.data
+        if craters is not None:
+            k = _bytes(craters[0], CRATER_SHAPE_KERNEL)
+            keep.append(k)
+            t.crater_kernel = k.ctypes.data
+            rec, data = craters[1], craters[2]
+            t.crater_records = b.ptr(rec)
+            t.n_craters = (rec.numel() if _is_torch(rec) else rec.nbytes) // CRATER_RECORD.itemsize
+            t.crater_data = b.ptr(data, np.float32)
+            t.n_crater_data = data.numel() if _is_torch(data) else len(data)
+            if len(craters) > 3 and craters[3] is not None:
+                t.crater_footprints = b.ptr(craters[3], np.float64)
+        if boulders is not None:
+            t.boulders = b.ptr(boulders)
+            t.n_boulders = (boulders.numel() if _is_torch(boulders) else boulders.size) // 5
+            t.boulder_width = boulder_width
+        g = grid.native()
+        N.check(self._lib.tg_evaluate(self._handle, C.byref(t), C.byref(g), h, b.memory,
+                                      _stream(b.memory)))
+        return heights
+
+    def measure_alu(self) -> float:
+        """Measured IMAD/FFMA lane operations per second (tg_measure_alu)."""
+        out = C.c_double()
+        N.check(self._lib.tg_measure_alu(self._handle, C.byref(out)))
+        return out.value
+
+    # --- boulders -------------------------------------------------------------------------
+    def boulders_bake(self, boulders, grid: GridSpec, heights, width: float, nodata=(0, 0.0)):
+        """BoulderLayer's dome relief (boulder_relief.cpp:426-439): `boulders` is [n, 5] float64
+        (x, y, diameter, exposed height, weight) or a device tensor of the same bytes; `width` the
+        band the domes are averaged over (the spacing)."""
+        b = _Buffers()
+        if _is_torch(boulders):
+            n = boulders.numel() // 5
+        else:
+            boulders = np.ascontiguousarray(boulders, np.float64).reshape(-1, 5)
+            n = len(boulders)
+        bp = b.ptr(boulders)
+        h = b.ptr(heights, np.float32)
+        g = grid.native()
+        N.check(self._lib.tg_boulders_bake(self._handle, bp, n, width, C.byref(g), h,
+                                           N.NoData(*nodata), b.memory, _stream(b.memory)))
+        return heights
+
     # --- craters --------------------------------------------------------------------------
     def craters_apply(self, kernel: np.ndarray, records, data, grid: GridSpec, heights,
                       footprints=None, nodata=(0, 0.0)):

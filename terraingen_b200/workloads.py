@@ -1,0 +1,134 @@
+"""The evaluation workloads of the benchmark configurations, built with the product's own host
+code (no reference library): crater batches through tg_crater_batch (the reference's population
+and records, bit for bit) and boulder lists as a seeded stand-in with the configured size law.
+
+Synthetic terrain, 4097 x 4097 at 0.5 m ("terrain4097"): an 8-octave Perlin fBm source
+(wavelength 512 m, lacunarity 2, gain 0.5, amplitude 5 m, seed 7); 200,000 craters expected over
+the tile, N(>D) ~ D^-2 on [1, 500] m, uniform ages over 1 Gyr, fresh depth 0.2 D and rim 0.04 D
+worn by freshness, Fassett-Thomson profiles with the default irregular outlines; 1,000,000
+boulders expected, N(>D) ~ D^-2.5 on [0.2, 3] m, heights 0.5 D, of which those 2 samples or more
+across (D > 1 m at 0.5 m, about 1.7 %) are drawn.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .device import GridSpec, centered
+from .layouts import CRATER_RECORD, CRATER_SHAPE_KERNEL, fractal
+
+
+@dataclass
+class Workload:
+    name: str
+    grid: GridSpec
+    fractals: np.ndarray
+    elevation: float
+    crater_kernel: np.ndarray
+    crater_records: np.ndarray
+    crater_data: np.ndarray
+    crater_footprints: np.ndarray
+    boulders: np.ndarray
+    boulder_width: float
+
+    @property
+    def cells(self) -> int:
+        return self.grid.cells
+
+    def input_bytes(self) -> int:
+        """Bytes of layer inputs a host-memory evaluation copies to the device."""
+        return (self.crater_records.nbytes + self.crater_data.nbytes +
+                self.crater_footprints.nbytes + self.boulders.nbytes)
+
+
+def crater_population(seed: int, coefficient: float, dmin: float, dmax: float,
+                      exponent: float = 2.0) -> N.Population:
+    return N.Population(seed=seed, sfd_coefficient=coefficient, sfd_exponent=exponent,
+                        min_diameter=dmin, max_diameter=dmax, lifetime_gyr=1.0, depth_ratio=0.2,
+                        rim_ratio=0.04, cutoff_depth_ratio=0.04, cell_size_factor=16.0,
+                        margin_radii=0.0, min_resolved_diameter=0.0)
+
+
+def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
+                 irregular: int = 1):
+    """(kernel, records, data, footprints) a crater layer hands the kernel for `grid`."""
+    lib = N.library()
+    shaping = N.Shaping(profile=profile, irregular=irregular)
+    g = grid.native()
+    nr, nd = C.c_size_t(), C.c_size_t()
+    N.check(lib.tg_crater_batch(C.byref(population), C.byref(shaping), C.byref(g), None, None, 0,
+                                None, 0, None, C.byref(nr), C.byref(nd)))
+    kernel = np.zeros((), CRATER_SHAPE_KERNEL)
+    records = np.zeros(nr.value, CRATER_RECORD)
+    data = np.zeros(nd.value, np.float32)
+    footprints = np.zeros(3 * nr.value, np.float64)
+    N.check(lib.tg_crater_batch(C.byref(population), C.byref(shaping), C.byref(g),
+                                kernel.ctypes.data, records.ctypes.data, nr.value,
+                                data.ctypes.data, nd.value, footprints.ctypes.data,
+                                C.byref(nr), C.byref(nd)))
+    return kernel, records, data, footprints
+
+
+def resolution_weight(diameter: np.ndarray, spacing: float) -> np.ndarray:
+    """1 - Falloff(D / spacing, 2, 4, smoothstep) (src/layers/fade.cpp:50)."""
+    x = diameter / spacing
+    t = np.clip((x - 2.0) / 2.0, 0.0, 1.0)
+    falloff = np.where(x <= 2.0, 1.0, np.where(x >= 4.0, 0.0, 1.0 - t * t * (3.0 - 2.0 * t)))
+    return 1.0 - falloff
+
+
+def stand_in_boulders(grid: GridSpec, expected: float, exponent: float, dmin: float, dmax: float,
+                      height_ratio: float, seed: int) -> np.ndarray:
+    """[n, 5] boulders (x, y, diameter, exposed height, weight): a Poisson count of boulders with
+    N(>D) ~ D^-exponent, uniform centers over the grid and half the largest boulder around it,
+    keeping those resolved at the grid's spacing."""
+    rng = np.random.default_rng(seed)
+    spacing = grid.pixel
+    area = grid.width * grid.height * spacing * spacing
+    c = expected / (area * (dmin ** -exponent - dmax ** -exponent))
+    lo = max(dmin, 2.0 * spacing)
+    margin = 0.5 * dmax
+    w, h = grid.width * spacing + 2 * margin, grid.height * spacing + 2 * margin
+    n = rng.poisson(c * w * h * (lo ** -exponent - dmax ** -exponent))
+    u = rng.random(n)
+    top = lo ** -exponent
+    diameter = (top - u * (top - dmax ** -exponent)) ** (-1.0 / exponent)
+    x = grid.x0 - margin + rng.random(n) * w
+    y = grid.y0 + margin - rng.random(n) * h
+    out = np.stack([x, y, diameter, height_ratio * diameter, resolution_weight(diameter, spacing)],
+                   axis=1)
+    return np.ascontiguousarray(out[out[:, 4] > 0.0])
+
+
+def terrain4097(side: int = 4097, pixel: float = 0.5, cx: float = 0.0, cy: float = 0.0,
+                seed: int = 7) -> Workload:
+    """The synthetic 4097^2 terrain (or a `side`^2 window of it centered at (cx, cy))."""
+    full_area = (4097 * pixel) ** 2
+    grid = centered(side, side, pixel, cx, cy)
+    crater_c = 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
+    kernel, records, data, footprints = crater_batch(
+        crater_population(seed, crater_c, 1.0, 500.0), grid)
+    boulders = stand_in_boulders(grid, 1e6 * grid.cells / (4097 * 4097), 2.5, 0.2, 3.0, 0.5,
+                                 seed + 1000 + int(cx) * 7 + int(cy) * 13)
+    return Workload("terrain4097", grid,
+                    np.array([fractal(seed=seed, wavelength=512.0, amplitude=5.0, octaves=8)]),
+                    0.0, kernel, records, data, footprints, boulders, pixel)
+
+
+def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
+    """The same terrain as the reference CPU path builds it (oracle harness scene fields)."""
+    full_area = (4097 * pixel) ** 2
+    crater_c = 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
+    boulder_c = 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5))
+    craters = dict(seed=seed, sfdCoefficient=crater_c, sfdExponent=2.0, minDiameter=1.0,
+                   maxDiameter=500.0, lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04, profile=0,
+                   applyPreset=0)
+    boulders = dict(boulderSeed=seed, boulderCoefficient=boulder_c, boulderExponent=2.5,
+                    boulderMin=0.2, boulderMax=3.0, heightRatio=0.5)
+    grid = centered(side, side, pixel)
+    fr = np.array([fractal(seed=seed, wavelength=512.0, amplitude=5.0, octaves=8)])
+    return grid, fr, craters, boulders

@@ -123,6 +123,29 @@ def crater_fixtures() -> None:
     np.savez_compressed(OUT / "craters.npz", **arrays)
 
 
+def boulder_fixtures() -> None:
+    """Boulders drawn as domes over an fBm source: the boulders the reference's layer draws, the
+    heights beneath them and the reference heights with them."""
+    ref = H.reference()
+    arrays = {}
+    cases = {
+        # 0.5 m cells, sizes D^-2.5 on [0.2, 3] m, heights 0.5 D (the 4097^2 terrain's boulders).
+        "dense": (centered(200, 160, 0.5, 10.0, 5.0), dict(boulderCoefficient=0.5)),
+        # 0.25 m cells: more boulders resolved, off-center.
+        "fine": (centered(128, 128, 0.25, -300.0, 120.0),
+                 dict(boulderSeed=4, boulderCoefficient=0.3, heightRatio=0.4)),
+    }
+    for name, (grid, fields) in cases.items():
+        src = np.array([L.fractal(seed=7, wavelength=64.0, amplitude=1.5, octaves=5)])
+        scene = H.make_scene(grid, source_fractals=src, boulders=fields)
+        arrays[f"{name}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])
+        arrays[f"{name}_boulders"] = H.boulders(ref, scene)
+        arrays[f"{name}_base"] = H.below_boulders(ref, scene, 1)
+        arrays[f"{name}_expected"], _ = H.evaluate(ref, scene, 0, 1)
+        print(name, len(arrays[f"{name}_boulders"]), "boulders")
+    np.savez_compressed(OUT / "boulders.npz", **arrays)
+
+
 def population_fixture() -> None:
     """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
     ref = H.reference()
@@ -136,6 +159,7 @@ if __name__ == "__main__":
     H.build("capture")
     noise_fixtures()
     crater_fixtures()
+    boulder_fixtures()
     population_fixture()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)

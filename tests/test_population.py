@@ -1,0 +1,125 @@
+"""Crater populations and kernel batches built by the product's host code, bit-exact against the
+reference (CPU only): the population fixture and the batches the reference hands its GPU
+backend (tests/golden/make_fixtures.py)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import harness as H
+from terraingen_b200 import _native as N, centered
+from terraingen_b200.layouts import CRATER_RECORD, CRATER_SHAPE_KERNEL
+
+
+def population(fields: dict, margin_radii=0.0, min_resolved=0.0) -> N.Population:
+    return N.Population(seed=fields["seed"], sfd_coefficient=fields["sfdCoefficient"],
+                        sfd_exponent=fields.get("sfdExponent", 2.0),
+                        min_diameter=fields["minDiameter"], max_diameter=fields["maxDiameter"],
+                        lifetime_gyr=fields.get("lifetimeGyr", 1.0),
+                        depth_ratio=fields.get("depthRatio", 0.2),
+                        rim_ratio=fields.get("rimRatio", 0.04), cutoff_depth_ratio=0.04,
+                        cell_size_factor=16.0, margin_radii=margin_radii,
+                        min_resolved_diameter=min_resolved)
+
+
+def generate(pop: N.Population, region) -> dict:
+    lib = N.library()
+    region = np.asarray(region, np.float64)
+    n = C.c_size_t()
+    N.check(lib.tg_crater_generate(C.byref(pop), region.ctypes.data, None, None, None, None, None,
+                                   0, C.byref(n)))
+    out = {k: np.zeros(n.value) for k in ("x", "y", "diameter", "age")}
+    out["id"] = np.zeros(n.value, np.uint64)
+    N.check(lib.tg_crater_generate(C.byref(pop), region.ctypes.data, out["x"].ctypes.data,
+                                   out["y"].ctypes.data, out["diameter"].ctypes.data,
+                                   out["age"].ctypes.data, out["id"].ctypes.data, n.value,
+                                   C.byref(n)))
+    return out
+
+
+def batch(pop: N.Population, profile: int, irregular: int, grid):
+    lib = N.library()
+    shp = N.Shaping(profile=profile, irregular=irregular)
+    g = grid.native()
+    nr, nd = C.c_size_t(), C.c_size_t()
+    N.check(lib.tg_crater_batch(C.byref(pop), C.byref(shp), C.byref(g), None, None, 0, None, 0,
+                                None, C.byref(nr), C.byref(nd)))
+    k = np.zeros((), CRATER_SHAPE_KERNEL)
+    rec = np.zeros(nr.value, CRATER_RECORD)
+    data = np.zeros(nd.value, np.float32)
+    foot = np.zeros(3 * nr.value)
+    N.check(lib.tg_crater_batch(C.byref(pop), C.byref(shp), C.byref(g), k.ctypes.data,
+                                rec.ctypes.data, nr.value, data.ctypes.data, nd.value,
+                                foot.ctypes.data, C.byref(nr), C.byref(nd)))
+    return k, rec, data, foot
+
+
+def test_population_matches_reference_fixture():
+    # The 257^2 scene's layer over its grid: CraterLayer::Craters with the layer's margin
+    # (reach 1.5 x the default irregular outline's largest stretch) and 2-sample resolution.
+    want = np.load(GOLDEN / "population.npz")
+    margin = 1.5 * (1 + 0.03 * math.sqrt(22)) * math.sqrt(1.5)
+    got = generate(population(H.config1_craters(), margin, 2.0), (-128.5, -128.5, 128.5, 128.5))
+    for key in ("x", "y", "diameter", "age", "id"):
+        assert np.array_equal(got[key], want[key]), key
+
+
+def test_batch_matches_captured_config1(crater_fixture):
+    k, rec, data, _ = batch(population(H.config1_craters()), 0, 1, centered(257, 257, 1.0))
+    assert k.tobytes() == crater_fixture["config1_kernel"].tobytes()
+    assert rec.tobytes() == crater_fixture["config1_records"].tobytes()
+    assert data.tobytes() == crater_fixture["config1_data"].tobytes()
+
+
+def test_batch_matches_captured_mpd(crater_fixture):
+    # Martin-Parkes-Dunstan with plain (round) outlines on an off-center 0.5 m grid.
+    # The "mpd" scene of tests/golden/make_fixtures.py.
+    grid = centered(160, 144, 0.5, 40.0, -25.0)
+    fields = dict(seed=5, sfdCoefficient=4e-2, minDiameter=1.0, maxDiameter=40.0)
+    k, rec, data, _ = batch(population(fields), 1, 0, grid)
+    assert k.tobytes() == crater_fixture["mpd_kernel"].tobytes()
+    assert rec.tobytes() == crater_fixture["mpd_records"].tobytes()
+    assert data.tobytes() == crater_fixture["mpd_data"].tobytes()
+
+
+def test_population_deterministic_and_tiled():
+    # Regions that tile a larger one draw the same craters (population_test.cpp:86-130): every
+    # crater of the whole region centered in a tile appears in that tile's draw.
+    fields = dict(seed=9, sfdCoefficient=0.05, minDiameter=1.0, maxDiameter=80.0)
+    whole = generate(population(fields), (0.0, 0.0, 400.0, 400.0))
+    again = generate(population(fields), (0.0, 0.0, 400.0, 400.0))
+    assert np.array_equal(whole["id"], again["id"])
+    ids = set()
+    for x0 in (0.0, 200.0):
+        for y0 in (0.0, 200.0):
+            part = generate(population(fields), (x0, y0, x0 + 200.0, y0 + 200.0))
+            ids |= set(part["id"].tolist())
+    assert ids == set(whole["id"].tolist())
+
+
+def test_population_rejects_bad_ranges():
+    lib = N.library()
+    pop = population(dict(seed=1, sfdCoefficient=0.1, minDiameter=5.0, maxDiameter=2.0))
+    region = np.zeros(4)
+    n = C.c_size_t()
+    assert lib.tg_crater_generate(C.byref(pop), region.ctypes.data, None, None, None, None, None,
+                                  0, C.byref(n)) == 1
+
+
+@pytest.mark.skipif(not H.available("libtgref.so"), reason="reference build not present")
+@pytest.mark.parametrize("seed,coefficient,lo,hi", [(2, 0.3, 1.0, 30.0), (77, 2.0, 0.5, 8.0)])
+def test_population_matches_reference_live(seed, coefficient, lo, hi):
+    # Denser draws (Poisson means above 10 take the PTRS branch) against the reference itself.
+    fields = dict(seed=seed, sfdCoefficient=coefficient, minDiameter=lo, maxDiameter=hi,
+                  profile=1, applyPreset=1)
+    scene = H.make_scene(centered(100, 100, 0.5), craters=fields)
+    region = (-30.0, -20.0, 45.0, 35.0)
+    want = H.craters(H.reference(), scene, region, 0.0)
+    got = generate(population(fields, margin_radii=2.0, min_resolved=0.0), region)
+    for key in ("x", "y", "diameter", "age", "id"):
+        assert np.array_equal(got[key], want[key]), key
