@@ -28,7 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 # Per-unit extra flags.
 UNITS = {
-    "noise.cu": ["-fmad=false"],
+    "noise.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
     "craters.cu": [],
     "boulders.cu": [],
     "diamond_square.cu": ["-fmad=false"],

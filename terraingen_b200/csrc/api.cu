@@ -88,6 +88,7 @@ enum Slot {
     kBoxes,
     kCulls,
     kBinEntries,
+    kHarmonics,
     kScan,
     kStatus,
     kBoulders,
@@ -476,8 +477,8 @@ namespace {
 // The crater pipeline on device buffers (count, scan, scatter, shape), on stream `s`. It reads
 // the number of binned entries back once to size the bins, and the status word at the end.
 int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
-                   const float* data, const double* foot, const Grid& g, float* dh,
-                   tg_nodata nodata, cudaStream_t s) {
+                   const float* data, uint32_t nData, const double* foot, const Grid& g,
+                   float* dh, tg_nodata nodata, cudaStream_t s) {
     if (size_t(g.width) * g.height == 0 || n == 0) {
         return TG_OK;
     }
@@ -521,9 +522,15 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
     bins.capacity = total;
+    const bool fast = crater_fast_path(k, d->pinnedStatus[1]);
+    float* harmonics = nullptr;
+    if (fast && nData > 0) {
+        TG_CUDA(d->slots[kHarmonics].reserve(size_t(nData) * sizeof(float)), "allocation");
+        harmonics = slot_ptr<float>(d, kHarmonics);
+        TG_CUDA(launch_crater_harmonics(rec, n, data, harmonics, s), "harmonics launch");
+    }
     TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
-    const Positions at{0.0, 0.0, nullptr, nullptr};
-    TG_CUDA(launch_crater_shape(k, data, g, at, to_nodata(nodata), bins, dh, s),
+    TG_CUDA(launch_crater_shape(k, data, harmonics, fast, g, to_nodata(nodata), bins, dh, s),
             "crater shape launch");
     TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
                             cudaMemcpyDeviceToHost, s),
@@ -653,8 +660,8 @@ int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, cons
                 "copy to device");
     }
     if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), n,
-                                static_cast<const float*>(ddata), static_cast<const double*>(dfoot),
-                                g, dh, nodata, s)) {
+                                static_cast<const float*>(ddata), n_data,
+                                static_cast<const double*>(dfoot), g, dh, nodata, s)) {
         return st;
     }
     return copy_heights_back(d, memory, heights, dh, cells);
@@ -907,7 +914,7 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     }
     if (t->n_craters > 0) {
         if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,
-                                    static_cast<const float*>(ddata),
+                                    static_cast<const float*>(ddata), t->n_crater_data,
                                     static_cast<const double*>(dfoot), g, dh, tg_nodata{0u, 0.0f},
                                     s)) {
             return st;

@@ -915,5 +915,100 @@ __device__ __forceinline__ float apply_with_datum(const CraterRecord& c, const C
     return height + q.shaped + c.resolution * replaced;
 }
 
+// --- the common case, evaluated lean ----------------------------------------------------------
+//
+// Batches whose kernel has a closed-form simple profile (Fassett-Thomson or Martin-Parkes-Dunstan,
+// neither complex, diffused nor tabulated), no rim smoothing, noise or texture, and whose records
+// carry at most an ellipse and power-law outline harmonics (no rim table, marks, terraces, peaks,
+// floor shift, upslope or datum) shape each crater by `fast_contribution`. It gives the
+// reference's heights (craters.h:1028-1212 on that path) with fewer operations:
+//   - the direction enters only through cos and sin of multiples of the angle, so they are
+//     rotated by complex multiplication from (dx, dy) / r instead of atan2 then one cos per
+//     harmonic: cos(k theta + phase) = A_k cos(k theta) - B_k sin(k theta), with
+//     (A_k, B_k) = amplitude (cos phase, sin phase) prepared once per batch (`harmonics`);
+//   - each harmonic's kept share, share^(k / 2), is a running product of sqrt(share).
+// Both differ from the reference's float cosf / powf by a few ulp of terms of order 0.01.
+struct FastKernel {
+    uint32_t simple;  // kProfileFassettThomson or kProfileMartinParkesDunstan
+    uint32_t rim;     // Fassett-Thomson rim mode
+    float reachRadii;
+};
+
+__device__ __forceinline__ float fast_outline_scale(const float* __restrict__ harmonics,
+                                                    const CraterRecord& c, float dx, float dy,
+                                                    float distance, float share) {
+    float c1 = 1.0f, s1 = 0.0f;  // the direction; angle 0 at the center, as KernelAngle
+    if (distance > 0.0f) {
+        c1 = dx / distance;
+        s1 = dy / distance;
+    }
+    float scale = 1.0f;
+    if (c.ellipticity != 1.0f) {
+        // KernelEllipseScale (craters.h:737) with cos and sin of theta - heading by rotation.
+        float sh, ch;
+        sincosf(c.heading, &sh, &ch);
+        const float cd = c1 * ch + s1 * sh;
+        const float sd = s1 * ch - c1 * sh;
+        const float along = sqrtf(c.ellipticity);
+        const float across = 1.0f / along;
+        const float u = cd / along;
+        const float v = sd / across;
+        scale = 1.0f / sqrtf(u * u + v * v);
+    }
+    float wobble = 1.0f;
+    if (share > 0.0f && c.harmonicCount > 0u) {
+        // (cm, sm) = (c1 + i s1)^m for the first harmonic's order m.
+        float cm = 1.0f, sm = 0.0f;
+        for (uint32_t i = 0; i < c.firstHarmonic; ++i) {
+            const float t = cm * c1 - sm * s1;
+            sm = cm * s1 + sm * c1;
+            cm = t;
+        }
+        const bool partial = share < 1.0f;
+        const float q = sqrtf(share);
+        float kept = 1.0f;
+        if (partial) {
+            for (uint32_t i = 0; i < c.firstHarmonic; ++i) {
+                kept *= q;
+            }
+        }
+        const float2* h = reinterpret_cast<const float2*>(harmonics + c.harmonicOffset);
+        for (uint32_t n = 0; n < c.harmonicCount; ++n) {
+            const float2 ab = __ldg(h + n);
+            wobble += kept * (ab.x * cm - ab.y * sm);
+            const float t = cm * c1 - sm * s1;
+            sm = cm * s1 + sm * c1;
+            cm = t;
+            if (partial) {
+                kept *= q;
+            }
+        }
+    }
+    return scale * wobble;
+}
+
+__device__ __forceinline__ float fast_contribution(const FastKernel& k,
+                                                   const float* __restrict__ harmonics,
+                                                   const CraterRecord& c, float dx, float dy,
+                                                   bool& reached) {
+    const float radius = 0.5f * c.diameter;
+    float distance = sqrtf(dx * dx + dy * dy);
+    if (c.ellipticity != 1.0f || c.harmonicCount > 0u) {
+        const float share = outline_share(distance / radius) * worn_outline_share(c);
+        distance /= fast_outline_scale(harmonics, c, dx, dy, distance, share);
+    }
+    reached = distance < k.reachRadii * radius;
+    if (!reached) {
+        return 0.0f;
+    }
+    float height;
+    if (k.simple == kProfileMartinParkesDunstan) {
+        height = mpd_height(distance, c.diameter, c.freshRim, c.currentDepth, c.currentRim);
+    } else {
+        height = ft_shape(distance / radius, k.rim, c.freshRim, c.currentDepth) * c.diameter;
+    }
+    return c.resolution * height;
+}
+
 }  // namespace crater
 }  // namespace tgb

@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kShapeThreads = 256;     // 8 warps; warp w covers rows 4w..4w+3 of a 32x32 bin
 constexpr int kCellsPerThread = 4;     // 4 adjacent columns, one row
-constexpr uint32_t kChunk = 48;        // entries per staged chunk (7680 bytes)
+constexpr uint32_t kChunk = 96;        // entries per staged chunk (15 KB)
 constexpr uint32_t kSpinLimit = 1u << 26;  // bounded mbarrier waits
 
 __device__ __forceinline__ bool is_nodata(NoData nd, float h) {
@@ -142,8 +142,16 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
         tiles = f.tiles;
         bins.boxes[warp] = tiles;
         bins.culls[warp] = f.cull;
-        if (r.hasDatum == 1u && tiles.x <= tiles.y) {
-            atomicOr(flags, 1u);
+        if (tiles.x <= tiles.y) {
+            if (r.hasDatum == 1u) {
+                atomicOr(flags, 1u);
+            }
+            // Anything beyond an ellipse and power-law harmonics needs the general path.
+            if (r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u ||
+                r.peakCount > 0u || r.shiftX != 0.0f || r.shiftY != 0.0f || r.upslopeX != 0.0f ||
+                r.upslopeY != 0.0f || r.hasDatum == 1u) {
+                atomicOr(flags, 4u);
+            }
         }
     }
     tiles.x = __shfl_sync(0xffffffffu, tiles.x, 0);
@@ -202,6 +210,26 @@ __global__ void crater_scatter_kernel(const CraterRecord* __restrict__ records, 
     }
 }
 
+// (amplitude, phase) of each record's outline harmonics as (amplitude cos phase,
+// amplitude sin phase), at the same offsets, for the lean path (crater_math.cuh).
+__global__ void crater_harmonics_kernel(const CraterRecord* __restrict__ records, uint32_t n,
+                                        const float* __restrict__ data, float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const uint32_t offset = records[i].harmonicOffset;
+    const uint32_t count = records[i].harmonicCount;
+    for (uint32_t h = 0; h < count; ++h) {
+        const float amplitude = __ldg(data + offset + 2u * h);
+        const float phase = __ldg(data + offset + 2u * h + 1u);
+        float s, c;
+        sincosf(phase, &s, &c);
+        out[offset + 2u * h] = amplitude * c;
+        out[offset + 2u * h + 1u] = amplitude * s;
+    }
+}
+
 // --- TMA bulk copy helpers (PTX ISA: cp.async.bulk, mbarrier) -------------------------------
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -248,10 +276,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     return false;
 }
 
+template <bool kFast>
 __global__ void __launch_bounds__(kShapeThreads)
     crater_shape_kernel(const CraterShapeKernel k, const float* __restrict__ data,
-                        const Grid grid, const NoData nodata, const CraterBins bins,
-                        float* __restrict__ heights, uint32_t* __restrict__ flags) {
+                        const float* __restrict__ harmonics, const Grid grid, const NoData nodata,
+                        const CraterBins bins, float* __restrict__ heights,
+                        uint32_t* __restrict__ flags) {
+    const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
     __shared__ __align__(128) BinEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
 
@@ -358,16 +389,29 @@ __global__ void __launch_bounds__(kShapeThreads)
             for (int j = 0; j < kCellsPerThread; ++j) {
                 if (need[j]) {
                     const float dx = dxs[j];
-                    const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
-                    if (q.reached) {
-                        acc[j] += double(q.shaped);
+                    if (kFast) {
+                        bool reached;
+                        const float shaped =
+                            crater::fast_contribution(fk, harmonics, r, dx, dy, reached);
+                        if (reached) {
+                            acc[j] += double(shaped);
+                        }
+                    } else {
+                        const crater::Contribution q =
+                            crater::crater_contribution(k, data, r, dx, dy);
+                        if (q.reached) {
+                            acc[j] += double(q.shaped);
+                        }
                     }
                 }
             }
         }
-        __syncthreads();
-        if (tid == 0 && c + 2 < chunks) {
-            issue(c + 2);
+        if (c + 2 < chunks) {
+            // The buffer is read by every warp before it is refilled.
+            __syncthreads();
+            if (tid == 0) {
+                issue(c + 2);
+            }
         }
     }
     if (!rowIn) {
@@ -543,16 +587,39 @@ cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const
     return cudaGetLastError();
 }
 
-cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data, const Grid& grid,
-                                const Positions& at, NoData nodata, const CraterBins& bins,
-                                float* heights, cudaStream_t stream) {
-    (void)at;
+cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, const float* data,
+                                    float* harmonics, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    crater_harmonics_kernel<<<(n + 255) / 256, 256, 0, stream>>>(records, n, data, harmonics);
+    return cudaGetLastError();
+}
+
+bool crater_fast_path(const CraterShapeKernel& k, uint32_t batchFlags) {
+    const CraterProfileKernel& p = k.profile;
+    return (batchFlags & 4u) == 0u &&
+           (p.simple == kProfileFassettThomson || p.simple == kProfileMartinParkesDunstan) &&
+           p.complex == 0u && p.diffused == 0u && k.rimSigma == 0.0f &&
+           k.noiseAmplitude == 0.0f && k.noiseRimAmplitude == 0.0f && k.wallStreaks == 0.0f &&
+           k.ejecta == 0.0f;
+}
+
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
+                                const float* harmonics, bool fast, const Grid& grid,
+                                NoData nodata, const CraterBins& bins, float* heights,
+                                cudaStream_t stream) {
     const uint32_t nbins = bins.binsX * bins.binsY;
     if (nbins == 0) {
         return cudaSuccess;
     }
-    crater_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, data, grid, nodata, bins, heights,
-                                                             bins.total + 1);
+    if (fast) {
+        crater_shape_kernel<true><<<nbins, kShapeThreads, 0, stream>>>(
+            k, data, harmonics, grid, nodata, bins, heights, bins.total + 1);
+    } else {
+        crater_shape_kernel<false><<<nbins, kShapeThreads, 0, stream>>>(
+            k, data, harmonics, grid, nodata, bins, heights, bins.total + 1);
+    }
     return cudaGetLastError();
 }
 

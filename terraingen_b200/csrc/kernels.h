@@ -84,9 +84,17 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
                                 const Grid& grid, const CraterBins& bins, cudaStream_t stream);
 cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const Grid& grid,
                                   const CraterBins& bins, cudaStream_t stream);
-cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data, const Grid& grid,
-                                const Positions& at, NoData nodata, const CraterBins& bins,
-                                float* heights, cudaStream_t stream);
+// Whether a batch takes the lean shaping path (crater_math.cuh `fast_contribution`): the
+// kernel's options allow it and the count pass saw no record feature beyond outlines
+// (`batchFlags` bit 2).
+bool crater_fast_path(const CraterShapeKernel& k, uint32_t batchFlags);
+// The lean path's harmonics: (amplitude cos phase, amplitude sin phase) at the data's offsets.
+cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, const float* data,
+                                    float* harmonics, cudaStream_t stream);
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
+                                const float* harmonics, bool fast, const Grid& grid,
+                                NoData nodata, const CraterBins& bins, float* heights,
+                                cudaStream_t stream);
 
 // The drop-in form: the reference's own tile lists (`CraterTiles`, apply.cpp:111-143), craters
 // applied in list order exactly as ShapeTilesOnCpu does (apply.cpp:199-222).

@@ -4,9 +4,9 @@
 // Compiled with -fmad=false: positions (double) and the lattice math (float) round exactly as the
 // reference's -ffp-contract=off build does, so heights carry the reference CPU path's bits.
 //
-// The kernel is ALU-bound (about 1.6k integer and float operations per cell for 8 Perlin
-// octaves, 4 bytes written). Each thread evaluates kRowsPerThread cells of one column, so a warp
-// covers 32 consecutive columns and every store is a full 128-byte line.
+// The kernels are ALU-bound (about 1.5k integer and float operations per cell for 8 Perlin
+// octaves, 4 bytes written). Each thread evaluates several cells of one column, so a warp covers
+// 32 consecutive columns and every store is a full 128-byte line.
 #include "kernels.h"
 #include "noise_math.cuh"
 
@@ -46,24 +46,114 @@ __device__ __forceinline__ float row_y(const Grid& g, const Positions& at, uint3
     return float(y - at.originY);
 }
 
-// One enabled Perlin fBm fractal without a warp: the configurations' source, the hot case.
-struct SingleFbm {
-    uint32_t seed;
-    float wavelength, amplitude, lacunarity, gain;
-    int octaves;
+// One enabled Perlin fBm fractal without a warp, the configurations' source: its per-octave
+// constants are computed once on the host, with the same float recurrences Fractal2 runs per
+// cell (fractal.h:219-240), so each cell performs exactly the reference's operations on them.
+constexpr int kMaxOctaves = 32;
+struct Octaves {
+    int count;
+    float amplitude;
+    float total;                       // sum of the weights
+    uint32_t seedTerm[kMaxOctaves];    // octave seed, through pcg3d's first LCG step
+    float ox[kMaxOctaves], oy[kMaxOctaves];
+    float frequency[kMaxOctaves], weight[kMaxOctaves];
+    float tc[kMaxOctaves], ts[kMaxOctaves];
 };
 
-template <bool kSingle>
+constexpr uint32_t kLcgA = 1664525u, kLcgC = 1013904223u;
+
+// pcg3d's x word for a corner whose first-step terms are already applied (hash.h:40-57).
+__device__ __forceinline__ uint32_t corner_from_terms(uint32_t x, uint32_t y, uint32_t z) {
+    x += y * z;
+    y += z * x;
+    z += x * y;
+    x ^= x >> 16u;
+    y ^= y >> 16u;
+    z ^= z >> 16u;
+    return x + y * z;
+}
+
+constexpr int kFbmRows = 8;  // rows per thread in the fBm kernel
+
+// The fBm source: octave-outer over kFbmRows cells of a column, reusing a lattice cell's four
+// corner hashes from the row above when the cell is the same (most rows, at broad octaves).
 __global__ void __launch_bounds__(kBlockX* kBlockY)
-    noise_kernel(const FractalStack stack, const SingleFbm fbm, const Grid grid,
-                 const Positions at, const bool fill, const float elevation, const NoData nodata,
-                 float* __restrict__ heights) {
+    fbm_kernel(const Octaves oct, const Grid grid, const Positions at, const bool fill,
+               const float elevation, const NoData nodata, float* __restrict__ heights) {
+    const uint32_t col = blockIdx.x * kBlockX + threadIdx.x;
+    const uint32_t row0 = (blockIdx.y * kBlockY + threadIdx.y) * kFbmRows;
+    if (col >= grid.width || row0 >= grid.height) {
+        return;
+    }
+    const int rows = min(kFbmRows, int(grid.height - row0));
+    float xs[kFbmRows], ys[kFbmRows], sum[kFbmRows];
+#pragma unroll
+    for (int r = 0; r < kFbmRows; ++r) {
+        const uint32_t row = row0 + min(r, rows - 1);
+        xs[r] = column_x(grid, at, col, row);
+        ys[r] = row_y(grid, at, col, row);
+        sum[r] = 0.0f;
+    }
+    for (int o = 0; o < oct.count; ++o) {
+        const float tc = oct.tc[o], ts = oct.ts[o], f = oct.frequency[o];
+        const float ox = oct.ox[o], oy = oct.oy[o], w = oct.weight[o];
+        const uint32_t sz = oct.seedTerm[o];
+        int32_t cx = INT32_MIN, cy = INT32_MIN;
+        uint32_t h00 = 0, h10 = 0, h01 = 0, h11 = 0;
+#pragma unroll
+        for (int r = 0; r < kFbmRows; ++r) {
+            // Fractal2's rotation and lattice position, then PerlinNoise2 (perlin.h:72-98).
+            const float rx = xs[r] * tc - ys[r] * ts;
+            const float ry = xs[r] * ts + ys[r] * tc;
+            const noise::Cell2 c = noise::split2(rx * f + ox, ry * f + oy);
+            if (c.ix != cx || c.iy != cy) {
+                cx = c.ix;
+                cy = c.iy;
+                const uint32_t ax0 = uint32_t(c.ix) * kLcgA + kLcgC, ax1 = ax0 + kLcgA;
+                const uint32_t ay0 = uint32_t(c.iy) * kLcgA + kLcgC, ay1 = ay0 + kLcgA;
+                h00 = corner_from_terms(ax0, ay0, sz);
+                h10 = corner_from_terms(ax1, ay0, sz);
+                h01 = corner_from_terms(ax0, ay1, sz);
+                h11 = corner_from_terms(ax1, ay1, sz);
+            }
+            const float n00 = noise::gradient2(h00, c.fx, c.fy);
+            const float n10 = noise::gradient2(h10, c.fx - 1.0f, c.fy);
+            const float n01 = noise::gradient2(h01, c.fx, c.fy - 1.0f);
+            const float n11 = noise::gradient2(h11, c.fx - 1.0f, c.fy - 1.0f);
+            const float u = noise::fade(c.fx);
+            const float v = noise::fade(c.fy);
+            const float n = 1.41421356237309505f *
+                            noise::lerp(v, noise::lerp(u, n00, n10), noise::lerp(u, n01, n11));
+            sum[r] += w * n;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kFbmRows; ++r) {
+        if (r >= rows) {
+            break;
+        }
+        const size_t i = size_t(row0 + r) * grid.width + col;
+        float base = elevation;
+        if (!fill) {
+            base = heights[i];
+            if (is_nodata(nodata, base)) {
+                continue;
+            }
+        }
+        // EvaluateFractals of one enabled fractal: amplitude * (1 * sum / total).
+        heights[i] = base + oct.amplitude * (1.0f * sum[r] / oct.total);
+    }
+}
+
+// Any stack of fractals (bases, types, blends, warps), cell by cell.
+__global__ void __launch_bounds__(kBlockX* kBlockY)
+    noise_kernel(const FractalStack stack, const Grid grid, const Positions at, const bool fill,
+                 const float elevation, const NoData nodata, float* __restrict__ heights) {
     const uint32_t col = blockIdx.x * kBlockX + threadIdx.x;
     const uint32_t row0 = (blockIdx.y * kBlockY + threadIdx.y) * kRowsPerThread;
     if (col >= grid.width) {
         return;
     }
-#pragma unroll
     for (int r = 0; r < kRowsPerThread; ++r) {
         const uint32_t row = row0 + r;
         if (row >= grid.height) {
@@ -79,15 +169,7 @@ __global__ void __launch_bounds__(kBlockX* kBlockY)
         }
         const float x = column_x(grid, at, col, row);
         const float y = row_y(grid, at, col, row);
-        float n;
-        if (kSingle) {
-            // EvaluateFractals of one enabled fractal: amplitude * (unit-amplitude fBm).
-            n = fbm.amplitude * noise::perlin_fbm2(x, y, fbm.seed, fbm.wavelength, 1.0f,
-                                                   fbm.octaves, fbm.lacunarity, fbm.gain);
-        } else {
-            n = noise::evaluate_stack(x, y, stack.fractals, stack.count);
-        }
-        heights[i] = base + n;
+        heights[i] = base + noise::evaluate_stack(x, y, stack.fractals, stack.count);
     }
 }
 
@@ -134,7 +216,6 @@ cudaError_t launch_noise(const FractalStack& stack, const Grid& grid, const Posi
         return cudaSuccess;
     }
     // The fast path: exactly one enabled fractal, Perlin fBm, no warp.
-    SingleFbm fbm{};
     int enabled = 0;
     const Fractal* only = nullptr;
     for (uint32_t i = 0; i < stack.count && i < kMaxFractals; ++i) {
@@ -144,22 +225,55 @@ cudaError_t launch_noise(const FractalStack& stack, const Grid& grid, const Posi
         }
     }
     const bool single = enabled == 1 && only->basis == kBasisPerlin && only->type == kTypeFbm &&
-                        !(only->warpAmplitude > 0.0f);
-    if (single) {
-        fbm = SingleFbm{only->seed, only->wavelength, only->amplitude, only->lacunarity,
-                        only->gain, only->octaves};
-    }
+                        !(only->warpAmplitude > 0.0f) && only->octaves <= kMaxOctaves;
     const dim3 block(kBlockX, kBlockY);
+    if (single) {
+        // Fractal2's per-octave values, in its order of float operations (fractal.h:219-240);
+        // this unit is built without contraction, so they round as on the reference's CPU.
+        Octaves oct{};
+        oct.count = only->octaves;
+        oct.amplitude = only->amplitude;
+        float frequency = 1.0f / only->wavelength;
+        float tc = 1.0f, ts = 0.0f, weight = 1.0f, total = 0.0f;
+        for (int o = 0; o < only->octaves; ++o) {
+            uint32_t v[3] = {only->seed, uint32_t(o), 0u};
+            v[0] = v[0] * kLcgA + kLcgC;
+            v[1] = v[1] * kLcgA + kLcgC;
+            v[2] = v[2] * kLcgA + kLcgC;
+            v[0] += v[1] * v[2];
+            v[1] += v[2] * v[0];
+            v[2] += v[0] * v[1];
+            v[0] ^= v[0] >> 16u;
+            v[1] ^= v[1] >> 16u;
+            v[2] ^= v[2] >> 16u;
+            v[0] += v[1] * v[2];
+            v[1] += v[2] * v[0];
+            v[2] += v[0] * v[1];
+            oct.seedTerm[o] = v[0] * kLcgA + kLcgC;  // the octave seed's first LCG step
+            oct.ox[o] = float(v[1] >> 8u) * 0x1p-24f;
+            oct.oy[o] = float(v[2] >> 8u) * 0x1p-24f;
+            oct.frequency[o] = frequency;
+            oct.tc[o] = tc;
+            oct.ts[o] = ts;
+            oct.weight[o] = weight;
+            total += weight;
+            weight *= only->gain;
+            frequency *= only->lacunarity;
+            const float nc = tc * TGB_TURN_COS - ts * TGB_TURN_SIN;
+            ts = ts * TGB_TURN_COS + tc * TGB_TURN_SIN;
+            tc = nc;
+        }
+        oct.total = total;
+        const uint32_t rowsPerBlock = kBlockY * kFbmRows;
+        const dim3 blocks((grid.width + kBlockX - 1) / kBlockX,
+                          (grid.height + rowsPerBlock - 1) / rowsPerBlock);
+        fbm_kernel<<<blocks, block, 0, stream>>>(oct, grid, at, fill, elevation, nodata, heights);
+        return cudaGetLastError();
+    }
     const uint32_t rowsPerBlock = kBlockY * kRowsPerThread;
     const dim3 blocks((grid.width + kBlockX - 1) / kBlockX,
                       (grid.height + rowsPerBlock - 1) / rowsPerBlock);
-    if (single) {
-        noise_kernel<true><<<blocks, block, 0, stream>>>(stack, fbm, grid, at, fill, elevation,
-                                                         nodata, heights);
-    } else {
-        noise_kernel<false><<<blocks, block, 0, stream>>>(stack, fbm, grid, at, fill, elevation,
-                                                          nodata, heights);
-    }
+    noise_kernel<<<blocks, block, 0, stream>>>(stack, grid, at, fill, elevation, nodata, heights);
     return cudaGetLastError();
 }
 

@@ -81,11 +81,17 @@ class _Buffers:
             raise ValueError("mix of host arrays and device tensors in one call")
 
 
+# cudaStreamLegacy: torch's default stream has handle 0, which the C ABI reads as "the device's
+# own stream", so it is passed as the legacy default stream's handle instead.
+_CUDA_STREAM_LEGACY = 0x1
+
+
 def _stream(memory):
     if memory == N.TG_MEMORY_DEVICE:
         import torch
 
-        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        handle = torch.cuda.current_stream().cuda_stream
+        return C.c_void_p(handle if handle != 0 else _CUDA_STREAM_LEGACY)
     return None
 
 
