@@ -173,6 +173,22 @@ int tg_boulders_bake(tg_device* device, const void* boulders, uint32_t n, double
                      const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
                      void* stream);
 
+/* tg_boulders_bake without any allocation, for callers that must not allocate GPU memory while
+ * they evaluate: a streaming renderer's frame thread, where cudaMalloc or cudaFree would
+ * synchronize the whole device and stall the frame, or a host that fixes its GPU memory at
+ * start-up. No counterpart in the reference, which allocates per strip (src/gpu/cuda.cpp:244-313).
+ * `boulders` (n tg_boulder) and `heights` are device memory; the work runs on `stream` (a
+ * cudaStream_t; NULL for the legacy default stream) and the call returns when it is done. Its
+ * scratch is one static 16 MiB device array inside the library, which every GPU that loads the
+ * library holds until exit; at most 65536 boulders, 32768 bins of 32x32 cells (a 5792 x 5792 grid)
+ * and 196608 binned boulders (TG_ERROR_MEMORY past that). The first call on a device finds the
+ * array's device address (cudaGetSymbolAddress) and should come before any stream capture. Calls
+ * share the array: calls whose work overlaps on the GPU race and must not overlap. Errors go to
+ * `error` (capacity bytes, may be null), not to tg_last_error. */
+int tg_boulders_bake_static(const void* boulders, uint32_t n, double width, const tg_grid* grid,
+                            float* heights, tg_nodata nodata, void* stream, char* error,
+                            size_t error_capacity);
+
 /* --- whole evaluations --------------------------------------------------------------------- */
 
 /* A terrain as Terrain::Evaluate runs it on one grid (src/pipeline/terrain.cpp:289-331): a

@@ -85,6 +85,7 @@ SIGNATURES.update({
     "tg_evaluate": [_P, C.POINTER(Terrain), C.POINTER(Grid), _P, _I, _P],
     "tg_measure_alu": [_P, C.POINTER(_D)],
     "tg_boulders_bake": [_P, _P, _U32, _D, C.POINTER(Grid), _P, NoData, _I, _P],
+    "tg_boulders_bake_static": [_P, _U32, _D, C.POINTER(Grid), _P, NoData, _P, C.c_char_p, _SZ],
     "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,
                              C.POINTER(_SZ)],
     "tg_crater_batch": [C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid), _P, _P, _SZ,

@@ -35,6 +35,7 @@ UNITS = {
     "seams.cu": [],
     "batch.cu": [],
     "probe.cu": [],
+    "static_scratch.cu": [],
     "api.cu": [],
     "population.cpp": [],
 }

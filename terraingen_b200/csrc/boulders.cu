@@ -140,8 +140,17 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ __align__(128) BoulderEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
     const uint32_t bin = blockIdx.x;
-    const uint32_t first = bins.counts[bin];
-    const uint32_t count = bins.counts[bin + 1] - first;
+    uint32_t first = bins.counts[bin];
+    uint32_t end = bins.counts[bin + 1];
+    if (end > bins.capacity) {
+        // Entries past the capacity were never scattered: bake what is there and flag it.
+        if (threadIdx.x == 0) {
+            atomicOr(flags, 4u);
+        }
+        end = bins.capacity;
+        first = min(first, end);
+    }
+    const uint32_t count = end - first;
     if (count == 0u) {
         return;
     }
