@@ -34,6 +34,16 @@ PIXEL = 0.5
 # key hash and offsets 21, turn 6, lattice 4, split 6, 4 corner hashes 45, 4 gradients 56 plus 2
 # offsets, 2 fades 14, lerps and scale 10, sums 5, turn update 6, loop 3.
 NOISE_OPS_PER_CELL_OCTAVE = 180
+# Counted from terraingen_b200/csrc/crater_math.cuh (fast_contribution) per (cell, crater) pair of
+# a Fassett-Thomson crater with 11 outline harmonics: distance and radii 12, outline share 14,
+# direction 18, first-harmonic rotation and kept share 14, 11 harmonics x 10, scale and division
+# 10, profile 18, resolution and FP64 sum 4.
+CRATER_OPS_PER_PAIR = 200
+# Counted from terraingen_b200/csrc/boulders.cu per (cell, boulder) pair: window test 6, offset
+# and hypot 12, dome band average (2 sqrt, 2 asin, clamps) 60, max-composite 4; FP64.
+BOULDER_OPS_PER_PAIR = 82
+# DRAM bytes per launch from the ncu capture of this workload (profiles/terrain4097_kernels.md).
+TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 136.5e6 + 27.0e6, "boulders": 61.9e6 + 7.9e6}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -238,6 +248,7 @@ def main():
             step(timers)
         torch.cuda.synchronize()
     barrier(world)
+    counters = dev.counters()
     phases = np.array([[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in timers])
     step_ms = float(phases.sum(axis=1).mean())
     total_s = max_over_ranks(float(phases.sum()) * 1e-3, world)
@@ -276,8 +287,19 @@ def main():
     crater_ms = float(phases[:, 1].mean())
     boulder_ms = float(phases[:, 2].mean())
     octaves = int(w.fractals[0]["octaves"])
-    noise_ops = w.cells * octaves * NOISE_OPS_PER_CELL_OCTAVE
-    achieved = noise_ops / (noise_ms * 1e-3) / 1e12
+    work = {"noise": (w.cells * octaves * NOISE_OPS_PER_CELL_OCTAVE, noise_ms,
+                      "fbm_kernel (fBm source)", f"{NOISE_OPS_PER_CELL_OCTAVE} per cell-octave"),
+            "craters": (counters["crater_pairs"] * CRATER_OPS_PER_PAIR, crater_ms,
+                        "crater pipeline (count, scan, scatter, crater_shape_kernel)",
+                        f"{CRATER_OPS_PER_PAIR} per (cell, crater) pair, "
+                        f"{counters['crater_pairs']} pairs"),
+            "boulders": (counters["boulder_pairs"] * BOULDER_OPS_PER_PAIR, boulder_ms,
+                         "boulder pipeline (count, scan, scatter, boulder_bake_kernel)",
+                         f"{BOULDER_OPS_PER_PAIR} per (cell, boulder) pair, "
+                         f"{counters['boulder_pairs']} pairs")}
+    dominant = max(work, key=lambda k: work[k][1])
+    ops, ms, kernel_name, unit_note = work[dominant]
+    achieved = ops / (ms * 1e-3) / 1e12
     peak = alu_peak / 1e12
     nbins = ((w.grid.width + 31) // 32) * ((w.grid.height + 31) // 32)
     launches = 1 + (3 + scan_launches(nbins)) * 2  # noise; count, scan, scatter, shape/bake x 2
@@ -294,11 +316,16 @@ def main():
                    "parallelism": f"replicas x{world} (one tile per GPU)"},
         "phases_ms": {"noise": round(noise_ms, 4), "craters": round(crater_ms, 4),
                       "boulders": round(boulder_ms, 4)},
-        "roofline": {"kernel": "noise_kernel (fBm source)", "bound": "alu",
+        "roofline": {"kernel": kernel_name, "bound": "alu",
                      "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "Tops/s",
                      "frac": round(achieved / peak, 3) if peak else None,
                      "peak_source": "measured IMAD+FFMA lane-op rate (tg_measure_alu) on this GPU",
-                     "ops_per_cell_octave": NOISE_OPS_PER_CELL_OCTAVE, "traffic": None},
+                     "algorithmic_ops": unit_note, "traffic": TRAFFIC[dominant],
+                     "traffic_source": "ncu dram__bytes_read+write of the shaping/bake/fill "
+                                       "kernel, profiles/terrain4097_kernels.md",
+                     "others": {k: {"ms": round(v[1], 4),
+                                    "achieved": round(v[0] / (v[1] * 1e-3) / 1e12, 3)}
+                                for k, v in work.items() if k != dominant}},
         "cpu_baseline": {"value": round(cpu_value, 3), "unit": UNIT, "cores": os.cpu_count(),
                          "kind": "reference",
                          "sample": f"{cpu_grid.width}x{cpu_grid.height} window of the same terrain "

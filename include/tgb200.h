@@ -220,6 +220,11 @@ typedef struct tg_terrain {
 int tg_evaluate(tg_device* device, const tg_terrain* terrain, const tg_grid* grid,
                 float* heights, int memory, void* stream);
 
+/* Work counters of the device's last runs: counters[0] the (cell, crater) pairs the last crater
+ * shaping evaluated, counters[1] the (cell, boulder) pairs the last boulder bake evaluated; at
+ * most `n` are written. */
+int tg_device_counters(tg_device* device, uint64_t* counters, size_t n);
+
 /* The device's measured lane-operation rate for a mix of 32-bit integer multiply-adds and FP32
  * fused multiply-adds (the noise and shaping kernels' roofline denominator), in operations per
  * second. */

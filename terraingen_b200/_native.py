@@ -84,6 +84,7 @@ class Terrain(C.Structure):
 SIGNATURES.update({
     "tg_evaluate": [_P, C.POINTER(Terrain), C.POINTER(Grid), _P, _I, _P],
     "tg_measure_alu": [_P, C.POINTER(_D)],
+    "tg_device_counters": [_P, _P, _SZ],
     "tg_boulders_bake": [_P, _P, _U32, _D, C.POINTER(Grid), _P, NoData, _I, _P],
     "tg_boulders_bake_static": [_P, _U32, _D, C.POINTER(Grid), _P, NoData, _P, C.c_char_p, _SZ],
     "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,

@@ -109,6 +109,8 @@ struct tg_device {
     std::string name;
     Buffer slots[kSlotCount];
     uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
+    // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
+    unsigned long long craterPairs = 0, boulderPairs = 0;
 };
 
 namespace {
@@ -532,10 +534,12 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
     TG_CUDA(launch_crater_shape(k, data, harmonics, fast, g, to_nodata(nodata), bins, dh, s),
             "crater shape launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, 3 * sizeof(uint32_t),
                             cudaMemcpyDeviceToHost, s),
             "copy to host");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    d->craterPairs = (static_cast<unsigned long long>(d->pinnedStatus[3]) << 32) |
+                     d->pinnedStatus[2];
     if (d->pinnedStatus[1] & 2u) {
         return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
     }
@@ -581,11 +585,13 @@ int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
     TG_CUDA(launch_boulder_scatter(rec, n, bins, s), "boulder scatter launch");
     TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), bins, dh, status, s),
             "boulder bake launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                            s),
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, status, 4 * sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost, s),
             "copy to host");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    if (d->pinnedStatus[1] & 2u) {
+    d->boulderPairs = (static_cast<unsigned long long>(d->pinnedStatus[3]) << 32) |
+                      d->pinnedStatus[2];
+    if (d->pinnedStatus[0] & 2u) {
         return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
     }
     return TG_OK;
@@ -927,6 +933,18 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         }
     }
     return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int tg_device_counters(tg_device* d, uint64_t* counters, size_t n) {
+    if (d == nullptr || (n > 0 && counters == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "device and counters are required");
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    const uint64_t values[2] = {d->craterPairs, d->boulderPairs};
+    for (size_t i = 0; i < n && i < 2; ++i) {
+        counters[i] = values[i];
+    }
+    return TG_OK;
 }
 
 int tg_measure_alu(tg_device* d, double* lane_ops_per_second) {

@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kThreads)
         }
     }
     uint32_t phase[2] = {0u, 0u};
+    uint32_t evaluated = 0;
     for (uint32_t c = 0; c < chunks; ++c) {
         const uint32_t s = c & 1u;
         bool arrived = false;
@@ -242,6 +243,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
             for (int j = 0; j < kCellsPerThread; ++j) {
                 if (live[j] && inRows && col0 + j >= b.c0 && col0 + j < b.c1) {
+                    ++evaluated;
                     const double dx = cx[j] - b.x;
                     // RockRelief without facets: the dome, not below 0 (boulder.h:90-95).
                     const double relief = fmax(dome(b, hypot(dx, dy), width), 0.0);
@@ -255,6 +257,10 @@ __global__ void __launch_bounds__(kThreads)
         if (tid == 0 && c + 2 < chunks) {
             issue(c + 2);
         }
+    }
+    const uint32_t warpPairs = __reduce_add_sync(0xffffffffu, evaluated);
+    if (lane == 0 && warpPairs > 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(flags + 2), (unsigned long long)warpPairs);
     }
     if (!rowIn) {
         return;

@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(kShapeThreads)
     }
     uint32_t phase[2] = {0u, 0u};
     bool failed = false;
+    uint32_t evaluated = 0;  // (cell, crater) pairs this thread evaluates, for the pair counter
     for (uint32_t c = 0; c < chunks; ++c) {
         const uint32_t s = c & 1u;
         if (!mbar_wait(&bars[s], phase[s])) {
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(kShapeThreads)
 #pragma unroll
             for (int j = 0; j < kCellsPerThread; ++j) {
                 if (need[j]) {
+                    ++evaluated;
                     const float dx = dxs[j];
                     if (kFast) {
                         bool reached;
@@ -413,6 +415,11 @@ __global__ void __launch_bounds__(kShapeThreads)
                 issue(c + 2);
             }
         }
+    }
+    // One atomic per warp: the pairs this CTA evaluated, into the 64-bit counter after the flags.
+    const uint32_t warpPairs = __reduce_add_sync(0xffffffffu, evaluated);
+    if (lane == 0 && warpPairs > 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(flags + 1), (unsigned long long)warpPairs);
     }
     if (!rowIn) {
         return;

@@ -221,6 +221,12 @@ class Device:
                                       _stream(b.memory)))
         return heights
 
+    def counters(self) -> dict:
+        """Pairs evaluated by the last crater shaping and boulder bake (tg_device_counters)."""
+        out = np.zeros(2, np.uint64)
+        N.check(self._lib.tg_device_counters(self._handle, out.ctypes.data, 2))
+        return {"crater_pairs": int(out[0]), "boulder_pairs": int(out[1])}
+
     def measure_alu(self) -> float:
         """Measured IMAD/FFMA lane operations per second (tg_measure_alu)."""
         out = C.c_double()
