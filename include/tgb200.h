@@ -189,6 +189,37 @@ int tg_boulders_bake_static(const void* boulders, uint32_t n, double width, cons
                             float* heights, tg_nodata nodata, void* stream, char* error,
                             size_t error_capacity);
 
+/* --- diamond-square refinement ------------------------------------------------------------ */
+
+/* DiamondSquareOptions (include/terraingen/sources/diamond_square.h:26-33) with a given scale:
+ * fractal dimension D in [2, 3] (the displacement shrinks by 2^-((3 - D) / 2) per step), scale Se
+ * (m), interp 0 bilinear (1 Catmull-Rom is TG_ERROR_UNSUPPORTED for now), seed, and
+ * min_pixel_size (m; 0 for none) capping the levels. */
+typedef struct tg_ds_options {
+    double fractal_dimension;
+    double scale;
+    uint32_t interp;
+    uint32_t seed;
+    double min_pixel_size;
+} tg_ds_options;
+
+/* DiamondSquareUpsampler::FillSamples on a grid (src/sources/diamond_square.cpp:488-516), which
+ * the reference runs only on the CPU: the `pw` x `ph` float posts on `post_grid` (row 0 north,
+ * reads past the edge repeating it) refined Levels(post spacing, grid spacing) times and read
+ * bilinearly at every cell of `grid` into `heights`. Nodes are doubles in device memory; the finest
+ * two levels are resident at once (8 bytes per node). */
+int tg_ds_refine(tg_device* device, const float* posts, uint32_t pw, uint32_t ph,
+                 const tg_grid* post_grid, const tg_ds_options* options, const tg_grid* grid,
+                 float* heights, int memory, void* stream);
+
+/* Philox4x32-10 conformance (the analogue of the reference's Philox tests,
+ * tests/unit/random/philox_test.cpp): for each of `n` sextets (counter x, y, z, w, key x, y) in
+ * `in`, the four output words into `out`, and into `normals` the diamond-square displacement normal
+ * of node (in[0], in[1]) as signed 32-bit indices at level in[2] & 31 with seed in[4]. Host
+ * buffers. */
+int tg_philox_probe(tg_device* device, const uint32_t* in, uint32_t n, uint32_t* out,
+                    double* normals);
+
 /* --- whole evaluations --------------------------------------------------------------------- */
 
 /* A terrain as Terrain::Evaluate runs it on one grid (src/pipeline/terrain.cpp:289-331): a

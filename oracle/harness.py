@@ -99,6 +99,22 @@ def below_boulders(lib: C.CDLL, scene: Scene, threads: int = 0) -> np.ndarray:
     return out
 
 
+def diamond_square(lib: C.CDLL, posts: np.ndarray, post_grid, grid, fractal_dimension: float,
+                   scale: float, seed: int = 1, interp: int = 0, threads: int = 0):
+    """(heights [h, w] float32, ms): the reference's DiamondSquareUpsampler through a RasterSource."""
+    posts = np.ascontiguousarray(posts, np.float32)
+    ph, pw = posts.shape
+    pt = np.array(post_grid.transform(), np.float64)
+    ot = np.array(grid.transform(), np.float64)
+    out = np.zeros((grid.height, grid.width), np.float32)
+    ms = _D()
+    if lib.tgref_ds(posts.ctypes.data, pw, ph, pt.ctypes.data, fractal_dimension, scale, interp,
+                    seed, grid.width, grid.height, ot.ctypes.data, threads, out.ctypes.data,
+                    C.byref(ms)) != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return out, ms.value
+
+
 def config1_craters() -> dict:
     """The 257 x 257, 1 m crater scene (2000 craters expected over the extent, N(>D) ~ D^-2 on
     [2, 60] m, depth/diameter 0.2, rim 0.04 D, uniform ages over 1 Gyr, seed 1)."""
@@ -147,6 +163,9 @@ def restate() -> C.CDLL:
                                     C.c_void_p]
     lib.rs_fbm_grid_f64.argtypes = [_U32, _U32, _D, _D, _D, _U32, _D, _D, C.c_int, _D, _D, _D,
                                     C.c_void_p]
+    lib.rs_philox.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_ds_normal.restype = _D
+    lib.rs_ds_normal.argtypes = [C.c_int64, C.c_int64, C.c_int, _U32]
     lib.rs_crater_profile_f64.restype = _D
     lib.rs_crater_profile_f64.argtypes = [C.c_int, _U32, _D, _D, _D, _D, _D, _D]
     return lib
@@ -165,6 +184,9 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_boulders.restype = C.c_long
     lib.tgref_evaluate_below_boulders.argtypes = [C.POINTER(Scene), C.c_uint, C.c_void_p]
     lib.tgref_evaluate_below_boulders.restype = C.c_int
+    lib.tgref_ds.argtypes = [C.c_void_p, _U32, _U32, C.c_void_p, _D, _D, C.c_int, _U32, _U32, _U32,
+                             C.c_void_p, C.c_uint, C.c_void_p, C.POINTER(_D)]
+    lib.tgref_ds.restype = C.c_int
     return lib
 
 

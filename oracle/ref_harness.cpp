@@ -23,6 +23,8 @@
 #include "terraingen/layers/craters/shaping/morphometry.h"
 #include "terraingen/layers/boulders/boulder_layer.h"
 #include "terraingen/layers/fade.h"
+#include "terraingen/sources/diamond_square.h"
+#include "terraingen/sources/raster_source.h"
 #include "terraingen/util/log.h"
 
 #include <chrono>
@@ -269,6 +271,50 @@ long tgref_boulders(const tgref_scene* s, double* out, long n) {
             ++count;
         }
         return count;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// The reference's DiamondSquareUpsampler over `posts` (pw x ph floats on `postTransform`), read at
+/// the cells of an `ow` x `oh` grid on `outTransform`, through a RasterSource in a Terrain: the
+/// heights into `out`, the evaluation's wall time into `ms`.
+int tgref_ds(const float* posts, uint32_t pw, uint32_t ph, const double* postTransform,
+             double fractalDimension, double scale, int interp, uint32_t seed, uint32_t ow,
+             uint32_t oh, const double* outTransform, unsigned threads, float* out, double* ms) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const RasterGrid postGrid{pw, ph,
+                                  GeoTransform::FromGdal({postTransform[0], postTransform[1],
+                                                          postTransform[2], postTransform[3],
+                                                          postTransform[4], postTransform[5]})};
+        Raster<float> raster(postGrid);
+        std::memcpy(raster.Values().data(), posts, size_t(pw) * ph * sizeof(float));
+        DiamondSquareOptions options;
+        options.fractalDimension = fractalDimension;
+        options.scale = scale;
+        options.interp = interp == 1 ? DiamondSquareInterp::CatmullRom : DiamondSquareInterp::Bilinear;
+        options.seed = seed;
+        RasterSourceOptions sourceOptions;
+        sourceOptions.upsampler = std::make_shared<DiamondSquareUpsampler>(options);
+        auto source = std::make_shared<RasterSource>(std::move(raster), sourceOptions);
+        const Terrain terrain(Surface{}, source, {});
+        EvaluationOptions evaluation;
+        evaluation.threads = threads;
+        evaluation.backend = Backend::Cpu;
+        const RasterGrid grid{ow, oh,
+                              GeoTransform::FromGdal({outTransform[0], outTransform[1],
+                                                      outTransform[2], outTransform[3],
+                                                      outTransform[4], outTransform[5]})};
+        const auto t0 = std::chrono::steady_clock::now();
+        const Raster<float> heights = terrain.Evaluate(grid, evaluation);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (ms != nullptr) {
+            *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        }
+        std::memcpy(out, heights.Values().data(), heights.Values().size() * sizeof(float));
+        return 0;
     } catch (const std::exception& error) {
         g_error = error.what();
         return -1;

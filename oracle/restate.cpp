@@ -232,4 +232,36 @@ double rs_crater_profile_f64(int profile, uint32_t rim, double distance, double 
     return std::max(h, freshRim - currentDepth) * diameter;
 }
 
+void rs_philox(const uint32_t* counter, const uint32_t* key, uint32_t* out) {
+    uint32_t c[4] = {counter[0], counter[1], counter[2], counter[3]};
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int round = 0; round < 10; ++round) {
+        if (round > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = uint64_t(0xD2511F53u) * c[0];
+        const uint64_t p1 = uint64_t(0xCD9E8D57u) * c[2];
+        const uint32_t n[4] = {uint32_t(p1 >> 32) ^ c[1] ^ k0, uint32_t(p1),
+                               uint32_t(p0 >> 32) ^ c[3] ^ k1, uint32_t(p0)};
+        for (int i = 0; i < 4; ++i) {
+            c[i] = n[i];
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        out[i] = c[i];
+    }
+}
+
+double rs_ds_normal(int64_t col, int64_t row, int level, uint32_t seed) {
+    const uint32_t counter[4] = {uint32_t(col), uint32_t(row),
+                                 uint32_t(level) | (uint32_t((col >> 32) ^ (row >> 32)) << 5), 0u};
+    const uint32_t key[2] = {seed, 0x524D4450u};
+    uint32_t w[4];
+    rs_philox(counter, key, w);
+    const double u1 = double((uint64_t(w[0] >> 5u) << 26u) | uint64_t(w[1] >> 6u)) * 0x1p-53;
+    const double u2 = double((uint64_t(w[2] >> 5u) << 26u) | uint64_t(w[3] >> 6u)) * 0x1p-53;
+    return std::sqrt(-2.0 * std::log1p(-u1)) * std::cos(2.0 * 3.14159265358979323846 * u2);
+}
+
 }  // extern "C"

@@ -46,6 +46,13 @@ double rs_crater_profile_f64(int profile, uint32_t rim, double distance, double 
                              double freshDepth, double freshRim, double currentDepth,
                              double currentRim);
 
+/* Philox4x32-10 (include/terraingen/random/philox.h:82) of `counter` and `key` into `out`. */
+void rs_philox(const uint32_t* counter, const uint32_t* key, uint32_t* out);
+/* The standard normal diamond-square draws for node (col, row) of `level` with `seed`:
+ * RandomStream(seed, kMidpointDisplacementStream, col, row, level | high << 5) then
+ * StandardNormal (src/sources/diamond_square.cpp:382, src/random/samplers.cpp:65). */
+double rs_ds_normal(int64_t col, int64_t row, int level, uint32_t seed);
+
 #ifdef __cplusplus
 }
 #endif

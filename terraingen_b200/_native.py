@@ -74,6 +74,11 @@ class Shaping(C.Structure):
     _fields_ = [("profile", C.c_uint32), ("irregular", C.c_uint32)]
 
 
+class DsOptions(C.Structure):
+    _fields_ = [("fractal_dimension", _D), ("scale", _D), ("interp", _U32), ("seed", _U32),
+                ("min_pixel_size", _D)]
+
+
 class Terrain(C.Structure):
     _fields_ = [("fractals", _P), ("n_fractals", _U32), ("elevation", _F), ("noise_layer", _P),
                 ("crater_kernel", _P), ("crater_records", _P), ("n_craters", _U32),
@@ -85,6 +90,9 @@ SIGNATURES.update({
     "tg_evaluate": [_P, C.POINTER(Terrain), C.POINTER(Grid), _P, _I, _P],
     "tg_measure_alu": [_P, C.POINTER(_D)],
     "tg_device_counters": [_P, _P, _SZ],
+    "tg_ds_refine": [_P, _P, _U32, _U32, C.POINTER(Grid), C.POINTER(DsOptions), C.POINTER(Grid),
+                     _P, _I, _P],
+    "tg_philox_probe": [_P, _P, _U32, _P, _P],
     "tg_boulders_bake": [_P, _P, _U32, _D, C.POINTER(Grid), _P, NoData, _I, _P],
     "tg_boulders_bake_static": [_P, _U32, _D, C.POINTER(Grid), _P, NoData, _P, C.c_char_p, _SZ],
     "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,

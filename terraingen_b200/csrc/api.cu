@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/tgb200.h"
 #include "kernels.h"
@@ -94,6 +95,9 @@ enum Slot {
     kBoulders,
     kBoulderWindows,
     kBoulderEntries,
+    kDsPosts,
+    kDsLevelA,
+    kDsLevelB,
     kProbeIn,
     kProbeHashes,
     kProbeValues,
@@ -933,6 +937,176 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         }
     }
     return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+namespace {
+
+int64_t host_floor_half(int64_t v) {
+    return v >= 0 ? v / 2 : -((1 - v) / 2);
+}
+
+struct Box {
+    int64_t c0, c1, r0, r1;  // inclusive
+    uint32_t w() const { return uint32_t(c1 - c0 + 1); }
+    uint32_t h() const { return uint32_t(r1 - r0 + 1); }
+    size_t size() const { return size_t(w()) * h(); }
+};
+
+}  // namespace
+
+int tg_ds_refine(tg_device* d, const float* posts, uint32_t pw, uint32_t ph,
+                 const tg_grid* post_grid, const tg_ds_options* o, const tg_grid* grid,
+                 float* heights, int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (o == nullptr || post_grid == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "options and the post grid are required");
+    }
+    Grid g, pg;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = to_grid(post_grid, pg)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (!(o->fractal_dimension >= 2.0 && o->fractal_dimension <= 3.0) || !(o->scale >= 0.0) ||
+        !std::isfinite(o->scale) || !(o->min_pixel_size >= 0.0)) {
+        return fail(TG_ERROR_ARGUMENT, "fractal dimension in [2, 3], scale and min pixel size >= 0");
+    }
+    if (o->interp != 0u) {
+        return fail(TG_ERROR_UNSUPPORTED, "Catmull-Rom diamond-square is not supported yet");
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (pw == 0 || ph == 0 || posts == nullptr || heights == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "posts and heights are required");
+    }
+    // Levels(post spacing, spacing) (diamond_square.cpp:289-300).
+    const double postSpacing = std::max(std::fabs(pg.pixelWidth), std::fabs(pg.pixelHeight));
+    const double spacing = std::max(std::fabs(g.pixelWidth), std::fabs(g.pixelHeight));
+    const double ratio = postSpacing / spacing;
+    int levels = 0;
+    if (ratio > 1.0) {
+        double most = 30.0;
+        if (o->min_pixel_size > 0.0) {
+            most = std::min(std::max(std::floor(std::log2(postSpacing / o->min_pixel_size) + 1e-9),
+                                     0.0),
+                            30.0);
+        }
+        levels = int(std::min(std::ceil(std::log2(ratio) - 1e-9), most));
+    }
+    // Frame (diamond_square.cpp:299-306): post (0, 0)'s center and the node steps.
+    DsFrame frame;
+    frame.originX = pg.originX + 0.5 * pg.pixelWidth + 0.5 * pg.rowRotation;
+    frame.originY = pg.originY + 0.5 * pg.colRotation + 0.5 * pg.pixelHeight;
+    frame.stepX = std::ldexp(pg.pixelWidth, -levels);
+    frame.stepY = std::ldexp(-pg.pixelHeight, -levels);
+    // The finest nodes the read-out touches, with a node to spare on every side.
+    auto node_range = [](double a, double b, int64_t& lo, int64_t& hi) {
+        lo = int64_t(std::floor(std::min(a, b))) - 1;
+        hi = int64_t(std::ceil(std::max(a, b))) + 1;
+    };
+    const double x0 = g.originX + 0.5 * g.pixelWidth, x1 = g.originX + (g.width - 0.5) * g.pixelWidth;
+    const double y0 = g.originY + 0.5 * g.pixelHeight,
+                 y1 = g.originY + (g.height - 0.5) * g.pixelHeight;
+    std::vector<Box> inner(levels + 1);
+    node_range((x0 - frame.originX) / frame.stepX, (x1 - frame.originX) / frame.stepX,
+               inner[levels].c0, inner[levels].c1);
+    node_range((y0 - frame.originY) / frame.stepY, (y1 - frame.originY) / frame.stepY,
+               inner[levels].r0, inner[levels].r1);
+    const int64_t reach = 1;
+    for (int l = levels; l >= 1; --l) {
+        const Box outer{inner[l].c0 - reach, inner[l].c1 + reach, inner[l].r0 - reach,
+                        inner[l].r1 + reach};
+        inner[l - 1] = Box{host_floor_half(outer.c0) - 2, host_floor_half(outer.c1) + 3,
+                           host_floor_half(outer.r0) - 2, host_floor_half(outer.r1) + 3};
+    }
+    auto array_box = [&](int l) {
+        return l == 0 ? inner[0]
+                      : Box{inner[l].c0 - reach, inner[l].c1 + reach, inner[l].r0 - reach,
+                            inner[l].r1 + reach};
+    };
+    size_t most = 0;
+    for (int l = 0; l <= levels; ++l) {
+        const Box b = array_box(l);
+        if (b.w() > (1u << 30) || b.h() > (1u << 30)) {
+            return fail(TG_ERROR_ARGUMENT, "the refined node grid is too large");
+        }
+        most = std::max(most, b.size());
+    }
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void* dposts = nullptr;
+    if (int st = stage_in(d, memory, kDsPosts, posts, size_t(pw) * ph * sizeof(float), &dposts)) {
+        return st;
+    }
+    if (d->slots[kDsLevelA].reserve(most * sizeof(double)) != cudaSuccess ||
+        d->slots[kDsLevelB].reserve(most * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TG_ERROR_MEMORY, "no room for two levels of %zu nodes", most);
+    }
+    double* buffers[2] = {slot_ptr<double>(d, kDsLevelA), slot_ptr<double>(d, kDsLevelB)};
+    const Box b0 = array_box(0);
+    DsLevel current{b0.c0, b0.r0, b0.w(), b0.h(), buffers[0]};
+    TG_CUDA(launch_ds_base(static_cast<const float*>(dposts), pw, ph, current, s), "ds base");
+    // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
+    const double stepFactor = std::pow(2.0, -(3.0 - o->fractal_dimension) / 2.0);
+    for (int l = 1; l <= levels; ++l) {
+        const Box b = array_box(l);
+        DsLevel next{b.c0, b.r0, b.w(), b.h(), buffers[l & 1]};
+        const double squareStep = o->scale * std::pow(stepFactor, 2 * l - 1);
+        const double diamondStep = o->scale * std::pow(stepFactor, 2 * l);
+        TG_CUDA(launch_ds_level(current, next, inner[l].c0, inner[l].r0, inner[l].w(), inner[l].h(),
+                                l, squareStep, diamondStep, o->seed, false, s),
+                "ds level");
+        current = next;
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+    }
+    TG_CUDA(launch_ds_read(current, frame, g, dh, s), "ds read");
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
+int tg_philox_probe(tg_device* d, const uint32_t* in, uint32_t n, uint32_t* out,
+                    double* normals) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (n == 0) {
+        return TG_OK;
+    }
+    if (in == nullptr || out == nullptr || normals == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "probe buffers are required");
+    }
+    const void* din = nullptr;
+    if (int st = stage_in(d, TG_MEMORY_HOST, kProbeIn, in, size_t(n) * 6 * sizeof(uint32_t),
+                          &din)) {
+        return st;
+    }
+    TG_CUDA(d->slots[kProbeHashes].reserve(size_t(n) * 4 * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kProbeValues].reserve(size_t(n) * sizeof(double)), "allocation");
+    TG_CUDA(launch_philox_probe(static_cast<const uint32_t*>(din), n,
+                                slot_ptr<uint32_t>(d, kProbeHashes),
+                                slot_ptr<double>(d, kProbeValues), d->stream),
+            "philox probe");
+    TG_CUDA(cudaMemcpyAsync(out, slot_ptr<uint32_t>(d, kProbeHashes), size_t(n) * 16,
+                            cudaMemcpyDeviceToHost, d->stream),
+            "copy to host");
+    TG_CUDA(cudaMemcpyAsync(normals, slot_ptr<double>(d, kProbeValues), size_t(n) * 8,
+                            cudaMemcpyDeviceToHost, d->stream),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(d->stream), "synchronize");
+    return TG_OK;
 }
 
 int tg_device_counters(tg_device* d, uint64_t* counters, size_t n) {

@@ -138,6 +138,32 @@ cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 const BoulderBins& bins, float* heights, uint32_t* flags,
                                 cudaStream_t stream);
 
+// --- diamond-square ----------------------------------------------------------------------
+// Nodes of one level over columns [c0, c0 + w) and rows [r0, r0 + h), row-major doubles.
+struct DsLevel {
+    int64_t c0, r0;
+    uint32_t w, h;
+    double* nodes;
+};
+// Where the finest nodes lie: node (0, 0) and the node steps along x and y (north up).
+struct DsFrame {
+    double originX, originY, stepX, stepY;
+};
+
+cudaError_t launch_ds_base(const float* posts, uint32_t pw, uint32_t ph, const DsLevel& out,
+                           cudaStream_t stream);
+// The square step over `out`'s whole box, then the diamond step over the inner box
+// [c0, c0 + w) x [r0, r0 + h), displacements scaled by `squareStep` and `diamondStep`.
+cudaError_t launch_ds_level(const DsLevel& parents, const DsLevel& out, int64_t c0, int64_t r0,
+                            uint32_t w, uint32_t h, int level, double squareStep,
+                            double diamondStep, uint32_t seed, bool spline, cudaStream_t stream);
+cudaError_t launch_ds_read(const DsLevel& nodes, const DsFrame& frame, const Grid& grid,
+                           float* heights, cudaStream_t stream);
+// Philox4x32-10 of n (counter, key) sextets, and the displacement normal the first two counter
+// words, the third's low 5 bits and the key's first word key as (col, row, level, seed).
+cudaError_t launch_philox_probe(const uint32_t* in, uint32_t n, uint32_t* out, double* normals,
+                                cudaStream_t stream);
+
 // The ALU issue-rate probe (probe.cu): one launch of a fixed IMAD/FFMA mix; `laneOps` receives
 // the lane operations it performs.
 cudaError_t launch_alu_probe(uint32_t* sink, uint64_t* laneOps, cudaStream_t stream);

@@ -221,6 +221,36 @@ class Device:
                                       _stream(b.memory)))
         return heights
 
+    # --- diamond-square -------------------------------------------------------------------
+    def ds_refine(self, posts, post_grid: GridSpec, grid: GridSpec, heights,
+                  fractal_dimension: float, scale: float, seed: int = 1, interp: int = 0,
+                  min_pixel_size: float = 0.0):
+        """DiamondSquareUpsampler::FillSamples (diamond_square.cpp:488): `posts` [ph, pw] float32
+        on `post_grid`, refined and read at every cell of `grid` into `heights`."""
+        b = _Buffers()
+        if _is_torch(posts):
+            ph, pw = posts.shape
+        else:
+            posts = np.ascontiguousarray(posts, np.float32)
+            ph, pw = posts.shape
+        pp = b.ptr(posts, np.float32)
+        h = b.ptr(heights, np.float32)
+        o = N.DsOptions(fractal_dimension, scale, interp, seed, min_pixel_size)
+        pg, g = post_grid.native(), grid.native()
+        N.check(self._lib.tg_ds_refine(self._handle, pp, pw, ph, C.byref(pg), C.byref(o),
+                                       C.byref(g), h, b.memory, _stream(b.memory)))
+        return heights
+
+    def philox_probe(self, sextets: np.ndarray):
+        """(words [n, 4] u32, normals [n] f64) of n (counter x4, key x2) sextets."""
+        sextets = np.ascontiguousarray(sextets, np.uint32).reshape(-1, 6)
+        n = len(sextets)
+        out = np.zeros((n, 4), np.uint32)
+        normals = np.zeros(n, np.float64)
+        N.check(self._lib.tg_philox_probe(self._handle, sextets.ctypes.data, n, out.ctypes.data,
+                                          normals.ctypes.data))
+        return out, normals
+
     def counters(self) -> dict:
         """Pairs evaluated by the last crater shaping and boulder bake (tg_device_counters)."""
         out = np.zeros(2, np.uint64)

@@ -146,6 +146,35 @@ def boulder_fixtures() -> None:
     np.savez_compressed(OUT / "boulders.npz", **arrays)
 
 
+def ds_fixtures() -> None:
+    """Diamond-square refinement of seeded DEMs by the reference's DiamondSquareUpsampler."""
+    ref = H.reference()
+    rs = H.restate()
+    arrays = {}
+    cases = {
+        # 65 x 65 posts at 5 m (a 12-octave fBm DEM, 20 km / 2000 m), read at 1 m: 3 levels.
+        "dem5m": (centered(65, 65, 5.0), centered(301, 301, 1.0, 3.25, -1.75), 2.2, 1.5, 7),
+        # Posts at 4 m read at 0.5 m off-center: exactly 3 levels, nodes on cell centers.
+        "exact": (centered(48, 40, 4.0, 100.0, 60.0), centered(240, 200, 0.5, 90.0, 70.0), 2.5,
+                  0.8, 3),
+        # Ten-fold, as the 20481^2 refinement (4 levels), on a small window.
+        "tenfold": (centered(41, 41, 5.0), centered(351, 351, 0.5, -10.0, 5.0), 2.2, 2.0, 11),
+    }
+    for name, (pg, grid, fd, scale, seed) in cases.items():
+        posts = np.zeros((pg.height, pg.width), np.float32)
+        rs.rs_fbm_grid_f32(pg.width, pg.height, pg.x0, pg.y0, pg.pixel, 3, 20000.0, 2000.0, 12,
+                           2.0, 0.5, 0.0, posts.ctypes.data)
+        heights, _ = H.diamond_square(ref, posts, pg, grid, fd, scale, seed, 0, 1)
+        assert not np.isnan(heights).any(), name
+        arrays[f"{name}_posts"] = posts
+        arrays[f"{name}_post_grid"] = np.array([pg.width, pg.height, pg.x0, pg.y0, pg.pixel])
+        arrays[f"{name}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])
+        arrays[f"{name}_options"] = np.array([fd, scale, seed], np.float64)
+        arrays[f"{name}_expected"] = heights
+        print(name, heights.shape, float(heights.std()))
+    np.savez_compressed(OUT / "ds.npz", **arrays)
+
+
 def population_fixture() -> None:
     """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
     ref = H.reference()
@@ -160,6 +189,7 @@ if __name__ == "__main__":
     noise_fixtures()
     crater_fixtures()
     boulder_fixtures()
+    ds_fixtures()
     population_fixture()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)

@@ -1,0 +1,94 @@
+"""GPU parity of diamond-square refinement against the reference's DiamondSquareUpsampler, and
+the Philox4x32-10 draws against the Random123 known answers the reference's tests use
+(tests/unit/random/philox_test.cpp:14-23) and the restated oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, grid_of
+
+pytestmark = pytest.mark.gpu
+
+# Heights are FP64 nodes read to float; only CUDA's double log1p / cos may differ from the host's
+# by an ulp, so the bar is far below the 1e-3 m of the configurations.
+TOLERANCE_M = 1e-3
+
+
+@pytest.fixture(scope="module")
+def fx():
+    return dict(np.load(GOLDEN / "ds.npz"))
+
+
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+def test_ds_matches_reference(device, fx, name):
+    pg = grid_of(fx[f"{name}_post_grid"])
+    grid = grid_of(fx[f"{name}_grid"])
+    fd, scale, seed = fx[f"{name}_options"]
+    heights = np.zeros((grid.height, grid.width), np.float32)
+    device.ds_refine(fx[f"{name}_posts"], pg, grid, heights, fd, scale, int(seed))
+    err = np.abs(heights.astype(np.float64) - fx[f"{name}_expected"])
+    assert err.max() <= TOLERANCE_M, (name, err.max())
+
+
+def test_philox_known_answers(device):
+    sextets = np.array([[0, 0, 0, 0, 0, 0],
+                        [0xffffffff] * 6,
+                        [0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344, 0xa4093822, 0x299f31d0]],
+                       np.uint32)
+    words, _ = device.philox_probe(sextets)
+    assert [list(map(int, w)) for w in words] == [
+        [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8],
+        [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd],
+        [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]]
+
+
+def test_displacement_draws_match_oracle(device):
+    from oracle import harness as H
+
+    rs = H.restate()
+    rng = np.random.default_rng(4)
+    cols = rng.integers(-50000, 50000, 500)
+    rows = rng.integers(-50000, 50000, 500)
+    levels = rng.integers(1, 6, 500)
+    sext = np.zeros((500, 6), np.uint32)
+    sext[:, 0] = cols.astype(np.int64).astype(np.uint32)
+    sext[:, 1] = rows.astype(np.int64).astype(np.uint32)
+    sext[:, 2] = levels
+    sext[:, 4] = 7
+    sext[:, 5] = 0x524D4450
+    words, normals = device.philox_probe(sext)
+    for i in range(500):
+        want = rs.rs_ds_normal(int(cols[i]), int(rows[i]), int(levels[i]), 7)
+        assert abs(normals[i] - want) <= 1e-13 * max(1.0, abs(want))
+
+
+def test_ds_deterministic_and_windowed(device, fx):
+    # A window of the output is the same as the window cut from the whole: node values do not
+    # depend on the box they are computed in.
+    from terraingen_b200 import GridSpec
+
+    pg = grid_of(fx["exact_post_grid"])
+    grid = grid_of(fx["exact_grid"])
+    fd, scale, seed = fx["exact_options"]
+    whole = np.zeros((grid.height, grid.width), np.float32)
+    device.ds_refine(fx["exact_posts"], pg, grid, whole, fd, scale, int(seed))
+    again = np.zeros_like(whole)
+    device.ds_refine(fx["exact_posts"], pg, grid, again, fd, scale, int(seed))
+    assert np.array_equal(whole.view(np.uint32), again.view(np.uint32))
+    c0, r0, w, h = 37, 51, 90, 70
+    sub = GridSpec(w, h, grid.x0 + c0 * grid.pixel, grid.y0 - r0 * grid.pixel, grid.pixel)
+    part = np.zeros((h, w), np.float32)
+    device.ds_refine(fx["exact_posts"], pg, sub, part, fd, scale, int(seed))
+    assert np.array_equal(part.view(np.uint32), whole[r0:r0 + h, c0:c0 + w].view(np.uint32))
+
+
+def test_ds_zero_scale_is_interpolation(device, fx):
+    # With no displacement, refinement averages: the result stays within the posts' range.
+    pg = grid_of(fx["dem5m_post_grid"])
+    grid = grid_of(fx["dem5m_grid"])
+    posts = fx["dem5m_posts"]
+    heights = np.zeros((grid.height, grid.width), np.float32)
+    device.ds_refine(posts, pg, grid, heights, 2.2, 0.0, 1)
+    assert heights.min() >= posts.min() - 1e-3 and heights.max() <= posts.max() + 1e-3
