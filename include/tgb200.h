@@ -308,6 +308,99 @@ int tg_crater_batch(const tg_crater_population* population, const tg_crater_shap
                     float* data, size_t data_capacity, double* footprints, size_t* n_records,
                     size_t* n_data);
 
+/* --- batched tiles ---------------------------------------------------------------------------
+ * Many tiles of one layer stack (a Perlin fBm source, a crater layer and a boulder layer)
+ * evaluated together: one count / scan / scatter of every tile's craters and boulders into bins,
+ * then ONE persistent launch in which each CTA takes bins from a device work queue and writes
+ * each cell once (source, craters, boulders). The launches are captured in a CUDA graph on the
+ * first evaluation and replayed while the batch fits the plan's capacities. World-to-lattice
+ * offsets are split in double per tile and octave, so tiles far from the origin keep float
+ * lattice fractions (heights within 1e-3 m of an FP64 evaluation at 1.7e6 m). The reference
+ * evaluates tiles one at a time (Terrain::EvaluateTiles, src/pipeline/terrain.cpp:158); this is
+ * its batched form. */
+typedef struct tg_batch tg_batch;
+
+/* One tile of a batch. Cell (col, row) of the tile is heights[height_offset + row * pitch + col].
+ * Its craters are records [crater_begin, crater_begin + crater_count) of the batch, their data
+ * offsets relative to crater_data + data_begin (what tg_crater_batch returns for the tile's grid);
+ * its boulders are [boulder_begin, boulder_begin + boulder_count), baked with dome band width
+ * `boulder_width` (the tile's sample spacing). A record or boulder belongs to one tile. */
+typedef struct tg_tile {
+    tg_grid grid;
+    uint64_t height_offset;
+    uint32_t pitch;
+    uint32_t crater_begin;
+    uint32_t crater_count;
+    uint32_t data_begin;
+    uint32_t boulder_begin;
+    uint32_t boulder_count;
+    double boulder_width;
+} tg_tile;
+
+/* A batch's inputs (host memory). `fractals` holds `n_fractals` 52-byte Fractals of which at most
+ * one is enabled, a Perlin fBm without warp; `crater_kernel` is one CraterShapeKernel for every
+ * tile; crater_footprints (optional) holds 3 doubles per record as tg_crater_batch writes them. */
+typedef struct tg_batch_input {
+    const tg_tile* tiles;
+    uint32_t n_tiles;
+    const void* fractals;
+    uint32_t n_fractals;
+    float elevation;
+    const void* crater_kernel;
+    const void* crater_records;
+    uint32_t n_craters;
+    const float* crater_data;
+    uint32_t n_crater_data;
+    const double* crater_footprints;
+    const tg_boulder* boulders;
+    uint32_t n_boulders;
+} tg_batch_input;
+
+/* What the batch last did. */
+typedef struct tg_batch_stats {
+    uint32_t variant;            /* kernel shape in use (tg_batch_variant) */
+    uint32_t bin_width, bin_height, cells_per_thread;
+    uint32_t fast;               /* 1: the lean crater path */
+    uint32_t bins;               /* bins (work items) of the loaded batch */
+    uint64_t cells;              /* cells of the loaded batch */
+    uint64_t crater_pairs;       /* (cell, crater) pairs the last evaluation shaped */
+    uint64_t boulder_pairs;      /* (cell, boulder) pairs it baked */
+    uint64_t crater_entries;     /* binned entries */
+    uint64_t boulder_entries;
+    uint32_t captures;           /* CUDA graphs captured so far */
+    uint32_t replays;            /* graph launches so far */
+    float bin_ms;                /* device time of the last binning (count, scan, scatter) */
+    float evaluate_ms;           /* device time of the last persistent evaluation */
+    float graph_ms;              /* device time of the last graph launch, end to end */
+    uint32_t ctas;               /* persistent CTAs of the last evaluation */
+} tg_batch_stats;
+
+int tg_batch_create(tg_device* device, tg_batch** batch);
+void tg_batch_destroy(tg_batch* batch);
+/* Copies `input` to the device and plans capacities (the next evaluation re-captures its graph
+ * when they grow). Fails with TG_ERROR_UNSUPPORTED for a source other than one unwarped Perlin
+ * fBm, for rotated tile grids and for crater datums. */
+int tg_batch_load(tg_batch* batch, const tg_batch_input* input);
+/* Evaluates the loaded batch into `heights` (n_heights floats; device pointer for
+ * TG_MEMORY_DEVICE, else host memory the result is copied to). Stream-ordered on `stream` in
+ * device mode; returns after the evaluation has finished. */
+int tg_batch_evaluate(tg_batch* batch, float* heights, size_t n_heights, int memory,
+                      void* stream);
+/* tg_batch_load then tg_batch_evaluate. */
+int tg_batch_run(tg_batch* batch, const tg_batch_input* input, float* heights, size_t n_heights,
+                 int memory, void* stream);
+/* The autotuner: evaluates the loaded batch with every kernel shape (bin size, cells per thread),
+ * `trials` timed replays each after a warm-up, and keeps the fastest. `ms` (optional) receives
+ * each variant's median time, tg_batch_variant_count() values. */
+int tg_batch_tune(tg_batch* batch, int trials, float* ms);
+int tg_batch_variant_count(void);
+/* Selects a kernel shape by index (0 .. tg_batch_variant_count() - 1); bin_width, bin_height and
+ * cells_per_thread (optional) describe it. */
+int tg_batch_set_variant(tg_batch* batch, int index);
+int tg_batch_variant(int index, uint32_t* bin_width, uint32_t* bin_height,
+                     uint32_t* cells_per_thread);
+int tg_batch_stats_get(tg_batch* batch, tg_batch_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

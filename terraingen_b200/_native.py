@@ -101,7 +101,42 @@ SIGNATURES.update({
                         _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ)],
 })
 
-RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p}
+class Tile(C.Structure):
+    _fields_ = [("grid", Grid), ("height_offset", C.c_uint64), ("pitch", _U32),
+                ("crater_begin", _U32), ("crater_count", _U32), ("data_begin", _U32),
+                ("boulder_begin", _U32), ("boulder_count", _U32), ("boulder_width", _D)]
+
+
+class BatchInput(C.Structure):
+    _fields_ = [("tiles", _P), ("n_tiles", _U32), ("fractals", _P), ("n_fractals", _U32),
+                ("elevation", _F), ("crater_kernel", _P), ("crater_records", _P),
+                ("n_craters", _U32), ("crater_data", _P), ("n_crater_data", _U32),
+                ("crater_footprints", _P), ("boulders", _P), ("n_boulders", _U32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("variant", _U32), ("bin_width", _U32), ("bin_height", _U32),
+                ("cells_per_thread", _U32), ("fast", _U32), ("bins", _U32),
+                ("cells", C.c_uint64), ("crater_pairs", C.c_uint64),
+                ("boulder_pairs", C.c_uint64), ("crater_entries", C.c_uint64),
+                ("boulder_entries", C.c_uint64), ("captures", _U32), ("replays", _U32),
+                ("bin_ms", _F), ("evaluate_ms", _F), ("graph_ms", _F), ("ctas", _U32)]
+
+
+SIGNATURES.update({
+    "tg_batch_create": [_P, C.POINTER(_P)],
+    "tg_batch_destroy": [_P],
+    "tg_batch_load": [_P, C.POINTER(BatchInput)],
+    "tg_batch_evaluate": [_P, _P, _SZ, _I, _P],
+    "tg_batch_run": [_P, C.POINTER(BatchInput), _P, _SZ, _I, _P],
+    "tg_batch_tune": [_P, _I, _P],
+    "tg_batch_variant_count": [],
+    "tg_batch_set_variant": [_P, _I],
+    "tg_batch_variant": [_I, C.POINTER(_U32), C.POINTER(_U32), C.POINTER(_U32)],
+    "tg_batch_stats_get": [_P, C.POINTER(BatchStats)],
+})
+
+RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p, "tg_batch_destroy": None}
 
 _lib = None
 

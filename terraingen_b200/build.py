@@ -33,7 +33,8 @@ UNITS = {
     "boulders.cu": [],
     "diamond_square.cu": ["-fmad=false"],
     "seams.cu": [],
-    "batch.cu": [],
+    "batch.cu": ["-fmad=false"],
+    "batch_api.cu": [],
     "probe.cu": [],
     "static_scratch.cu": [],
     "api.cu": [],

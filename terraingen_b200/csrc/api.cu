@@ -12,11 +12,13 @@
 #include <vector>
 
 #include "../../include/tgb200.h"
+#include "api_internal.h"
 #include "kernels.h"
 
 using namespace tgb;
 
-namespace {
+namespace tgb {
+namespace api {
 
 thread_local std::string g_error;
 
@@ -33,91 +35,6 @@ int fail(int status, const char* format, ...) {
 int cuda_fail(cudaError_t err, const char* what) {
     return fail(TG_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(err));
 }
-
-#define TG_CUDA(call, what)                    \
-    do {                                       \
-        const cudaError_t e_ = (call);         \
-        if (e_ != cudaSuccess) {               \
-            return cuda_fail(e_, what);        \
-        }                                      \
-    } while (0)
-
-// One growable device allocation.
-struct Buffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-
-    cudaError_t reserve(size_t need) {
-        if (need <= bytes) {
-            return cudaSuccess;
-        }
-        if (ptr != nullptr) {
-            cudaFree(ptr);
-            ptr = nullptr;
-            bytes = 0;
-        }
-        // Grow by half again to amortise repeated growth.
-        const size_t size = need + need / 2;
-        const cudaError_t err = cudaMalloc(&ptr, size);
-        if (err == cudaSuccess) {
-            bytes = size;
-        }
-        return err;
-    }
-    void release() {
-        if (ptr != nullptr) {
-            cudaFree(ptr);
-        }
-        ptr = nullptr;
-        bytes = 0;
-    }
-};
-
-enum Slot {
-    kHeights,
-    kXs,
-    kYs,
-    kXLows,
-    kYLows,
-    kRecords,
-    kData,
-    kFootprints,
-    kHeads,
-    kEntries,
-    kCounts,
-    kCursor,
-    kBoxes,
-    kCulls,
-    kBinEntries,
-    kHarmonics,
-    kScan,
-    kStatus,
-    kBoulders,
-    kBoulderWindows,
-    kBoulderEntries,
-    kDsPosts,
-    kDsLevelA,
-    kDsLevelB,
-    kProbeIn,
-    kProbeHashes,
-    kProbeValues,
-    kSlotCount
-};
-
-}  // namespace
-
-struct tg_device {
-    int ordinal = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mutex;
-    std::string name;
-    Buffer slots[kSlotCount];
-    uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
-    // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
-    unsigned long long craterPairs = 0, boulderPairs = 0;
-};
-
-namespace {
 
 int check_device(tg_device* d) {
     if (d == nullptr) {
@@ -159,6 +76,13 @@ int to_grid(const tg_grid* g, Grid& out) {
     return TG_OK;
 }
 
+}  // namespace api
+}  // namespace tgb
+
+using namespace tgb::api;
+
+namespace {
+
 NoData to_nodata(tg_nodata n) {
     return NoData{n.mode, n.value};
 }
@@ -171,8 +95,10 @@ int check_nodata(tg_nodata n) {
 }
 
 // A buffer the kernels read: the caller's pointer in device mode, else a copy in `slot`.
+// A device buffer must be aligned to `align` bytes (16 for CraterRecords, read as 16-byte words;
+// 8 for doubles); a host buffer is copied into an aligned slot.
 int stage_in(tg_device* d, int memory, Slot slot, const void* src, size_t bytes,
-             const void** out) {
+             const void** out, size_t align = sizeof(float)) {
     if (bytes == 0) {
         *out = nullptr;
         return TG_OK;
@@ -181,6 +107,9 @@ int stage_in(tg_device* d, int memory, Slot slot, const void* src, size_t bytes,
         return fail(TG_ERROR_ARGUMENT, "a required buffer is null");
     }
     if (memory == TG_MEMORY_DEVICE) {
+        if (reinterpret_cast<uintptr_t>(src) % align != 0) {
+            return fail(TG_ERROR_ARGUMENT, "a device buffer is not %zu-byte aligned", align);
+        }
         *out = src;
         return TG_OK;
     }
@@ -650,7 +579,7 @@ int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, cons
     const void* drec = nullptr;
     const void* ddata = nullptr;
     const void* dfoot = nullptr;
-    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec)) {
+    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec, 16)) {
         return st;
     }
     if (int st = stage_in(d, memory, kData, data, size_t(n_data) * sizeof(float), &ddata)) {
@@ -658,7 +587,7 @@ int tg_craters_apply(tg_device* d, const void* kernel, size_t kernel_bytes, cons
     }
     if (footprints != nullptr) {
         if (int st = stage_in(d, memory, kFootprints, footprints, size_t(n) * 3 * sizeof(double),
-                              &dfoot)) {
+                              &dfoot, 8)) {
             return st;
         }
     }
@@ -731,7 +660,7 @@ int tg_craters_apply_lists(tg_device* d, const void* kernel, size_t kernel_bytes
     std::memcpy(&k, kernel, sizeof(k));
     const cudaStream_t s = stream_of(d, memory, stream);
     const void *drec, *ddata, *dheads, *dentries, *dxs, *dxl, *dys, *dyl;
-    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec)) {
+    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec, 16)) {
         return st;
     }
     if (int st = stage_in(d, memory, kData, data, size_t(n_data) * sizeof(float), &ddata)) {
@@ -808,7 +737,7 @@ int tg_boulders_bake(tg_device* d, const void* boulders, uint32_t n, double widt
     }
     const cudaStream_t s = stream_of(d, memory, stream);
     const void* db = nullptr;
-    if (int st = stage_in(d, memory, kBoulders, boulders, size_t(n) * sizeof(BoulderRecord), &db)) {
+    if (int st = stage_in(d, memory, kBoulders, boulders, size_t(n) * sizeof(BoulderRecord), &db, 8)) {
         return st;
     }
     float* dh = heights;
@@ -889,7 +818,7 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     const void *drec = nullptr, *ddata = nullptr, *dfoot = nullptr, *db = nullptr;
     if (t->n_craters > 0) {
         if (int st = stage_in(d, memory, kRecords, t->crater_records,
-                              size_t(t->n_craters) * sizeof(CraterRecord), &drec)) {
+                              size_t(t->n_craters) * sizeof(CraterRecord), &drec, 16)) {
             return st;
         }
         if (int st = stage_in(d, memory, kData, t->crater_data,
@@ -898,14 +827,14 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         }
         if (t->crater_footprints != nullptr) {
             if (int st = stage_in(d, memory, kFootprints, t->crater_footprints,
-                                  size_t(t->n_craters) * 3 * sizeof(double), &dfoot)) {
+                                  size_t(t->n_craters) * 3 * sizeof(double), &dfoot, 8)) {
                 return st;
             }
         }
     }
     if (t->n_boulders > 0) {
         if (int st = stage_in(d, memory, kBoulders, t->boulders,
-                              size_t(t->n_boulders) * sizeof(BoulderRecord), &db)) {
+                              size_t(t->n_boulders) * sizeof(BoulderRecord), &db, 8)) {
             return st;
         }
     }

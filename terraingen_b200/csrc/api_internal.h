@@ -1,0 +1,107 @@
+// Internals of the C ABI shared by its units (api.cu, batch_api.cu): error reporting, growable
+// device buffers, the device handle and argument checks.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/tgb200.h"
+#include "kernels.h"
+
+namespace tgb {
+namespace api {
+
+// Records the message for tg_last_error (thread-local) and returns `status`.
+int fail(int status, const char* format, ...);
+int cuda_fail(cudaError_t err, const char* what);
+
+#define TG_CUDA(call, what)                    \
+    do {                                       \
+        const cudaError_t e_ = (call);         \
+        if (e_ != cudaSuccess) {               \
+            return ::tgb::api::cuda_fail(e_, what); \
+        }                                      \
+    } while (0)
+
+// One growable device allocation.
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    cudaError_t reserve(size_t need) {
+        if (need <= bytes) {
+            return cudaSuccess;
+        }
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+            ptr = nullptr;
+            bytes = 0;
+        }
+        // Grow by half again to amortise repeated growth, except for buffers of a GiB or more,
+        // which are sized exactly (a grid of billions of cells).
+        const size_t size = need < (size_t(1) << 30) ? need + need / 2 : need;
+        const cudaError_t err = cudaMalloc(&ptr, size);
+        if (err == cudaSuccess) {
+            bytes = size;
+        }
+        return err;
+    }
+    void release() {
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+        }
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+enum Slot {
+    kHeights,
+    kXs,
+    kYs,
+    kXLows,
+    kYLows,
+    kRecords,
+    kData,
+    kFootprints,
+    kHeads,
+    kEntries,
+    kCounts,
+    kCursor,
+    kBoxes,
+    kCulls,
+    kBinEntries,
+    kHarmonics,
+    kScan,
+    kStatus,
+    kBoulders,
+    kBoulderWindows,
+    kBoulderEntries,
+    kDsPosts,
+    kDsLevelA,
+    kDsLevelB,
+    kProbeIn,
+    kProbeHashes,
+    kProbeValues,
+    kSlotCount
+};
+
+int check_device(tg_device* d);
+int check_memory(int memory);
+int to_grid(const tg_grid* g, Grid& out);
+
+}  // namespace api
+}  // namespace tgb
+
+struct tg_device {
+    int ordinal = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mutex;
+    std::string name;
+    tgb::api::Buffer slots[tgb::api::kSlotCount];
+    uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
+    // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
+    unsigned long long craterPairs = 0, boulderPairs = 0;
+};

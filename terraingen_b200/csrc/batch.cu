@@ -1,0 +1,728 @@
+// The batched form: many tiles of different sizes, spacings and places evaluated together.
+//
+// Binning (launch_batch_bin), once per batch over all its tiles:
+//   count   - one warp per crater record (thread per boulder): its footprint window on its own
+//             tile's grid (the reference's CratersOnRaster / ReliefBox windows, as the plain
+//             path computes them) and one count per bin of that tile it covers;
+//   scan    - one exclusive prefix sum over the bins of every tile;
+//   scatter - the 160-byte BinEntry (64-byte BoulderEntry) into each covered bin.
+// Evaluation (launch_batch_evaluate) is ONE persistent launch: each CTA takes the next bin from
+// a device work-queue cursor, finds its tile, and for the bin's cells
+//   1. evaluates the source fBm with world-to-lattice offsets split in double per tile and octave
+//      (OctaveAnchor), so cells millions of meters from the origin keep their lattice fraction
+//      to float precision;
+//   2. adds the bin's craters (entries staged in shared memory by TMA bulk copies, warp-ballot
+//      culling, FP64 accumulation of FP32 contributions, as the plain path);
+//   3. max-composites the bin's boulders (FP64 dome relief, as the plain path);
+//   4. writes each cell once.
+// The launches read their sizes from the BatchHeader in device memory, so one captured CUDA
+// graph serves every batch that fits the plan's capacities.
+//
+// Built with -fmad=false: every fused multiply-add is written out, so heights are the same bits
+// whichever kernel shape (bin size, cells per thread) the autotuner picks.
+#include "binning.cuh"
+#include "crater_math.cuh"
+#include "kernels.h"
+#include "noise_math.cuh"
+
+namespace tgb {
+namespace {
+
+using namespace binning;
+
+constexpr uint32_t kStageBytes = 15360;  // one staging buffer: 96 crater or 240 boulder entries
+constexpr uint32_t kCraterChunk = kStageBytes / sizeof(BinEntry);
+constexpr uint32_t kBoulderChunk = kStageBytes / sizeof(BoulderEntry);
+static_assert(kCraterChunk * sizeof(BinEntry) == kStageBytes, "whole crater entries per stage");
+static_assert(kBoulderChunk * sizeof(BoulderEntry) == kStageBytes, "whole boulder entries");
+
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kLcgA = 1664525u, kLcgC = 1013904223u;
+
+// Perlin's quintic fade and the lerp (include/terraingen/noise/lattice.h:76-86) with explicit
+// fused multiply-adds. This unit is built with -fmad=false, so these are the only contractions:
+// a cell's height does not depend on how a kernel shape happens to be compiled.
+__device__ __forceinline__ float fade_fma(float t) {
+    return t * t * t * fmaf(t, fmaf(t, 6.0f, -15.0f), 10.0f);
+}
+
+__device__ __forceinline__ float lerp_fma(float t, float a, float b) {
+    return fmaf(t, b - a, a);
+}
+
+// pcg3d's x word for a corner whose first LCG step is already applied (hash.h:40-57).
+__device__ __forceinline__ uint32_t corner_hash(uint32_t x, uint32_t y, uint32_t z) {
+    x += y * z;
+    y += z * x;
+    z += x * y;
+    x ^= x >> 16u;
+    y ^= y >> 16u;
+    z ^= z >> 16u;
+    return x + y * z;
+}
+
+// --- binning -------------------------------------------------------------------------------
+
+__global__ void batch_crater_count_kernel(const CraterShapeKernel k, const BatchView v,
+                                          uint32_t tpbX, uint32_t tpbY) {
+    const uint32_t n = v.header->records;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        int4 box = make_int4(1, 0, 1, 0);
+        uint32_t tile = kNone;
+        if (lane == 0) {
+            tile = v.recordTile[i];
+            if (tile != kNone) {
+                const BatchTile& t = v.tiles[tile];
+                const CraterRecord r = v.records[i];
+                const Footprint f =
+                    crater_footprint(k, r, v.data + t.dataBase, v.footprints, i, t.grid);
+                box = f.tiles;
+                v.craterCulls[i] = f.cull;
+                if (box.x <= box.y) {
+                    if (r.hasDatum == 1u) {
+                        atomicOr(&v.header->flags, 1u);
+                    }
+                    if (crater_heavy(r)) {
+                        atomicOr(&v.header->flags, 8u);
+                    }
+                }
+            }
+            v.craterBoxes[i] = box;
+        }
+        box.x = __shfl_sync(0xffffffffu, box.x, 0);
+        box.y = __shfl_sync(0xffffffffu, box.y, 0);
+        box.z = __shfl_sync(0xffffffffu, box.z, 0);
+        box.w = __shfl_sync(0xffffffffu, box.w, 0);
+        tile = __shfl_sync(0xffffffffu, tile, 0);
+        if (box.x > box.y) {
+            continue;
+        }
+        const uint32_t binsX = v.tiles[tile].binsX, base = v.tiles[tile].binBase;
+        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
+        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
+        const uint32_t wide = bx1 - bx0 + 1u;
+        const uint32_t total = wide * (by1 - by0 + 1u);
+        for (uint32_t t = lane; t < total; t += 32u) {
+            atomicAdd(v.craterCounts + base + (by0 + t / wide) * binsX + bx0 + t % wide, 1u);
+        }
+    }
+}
+
+__global__ void batch_crater_scatter_kernel(const BatchView v, uint32_t tpbX, uint32_t tpbY) {
+    const uint32_t n = v.header->records;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const int4 box = v.craterBoxes[i];
+        if (box.x > box.y) {
+            continue;
+        }
+        const uint32_t tile = v.recordTile[i];
+        const uint32_t binsX = v.tiles[tile].binsX, base = v.tiles[tile].binBase;
+        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
+        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
+        const uint32_t wide = bx1 - bx0 + 1u;
+        const uint32_t total = wide * (by1 - by0 + 1u);
+        const int4* src = reinterpret_cast<const int4*>(v.records + i);
+        int4 tail;
+        tail.x = int(uint32_t(box.x) | (uint32_t(box.y) << 16));
+        tail.y = int(uint32_t(box.z) | (uint32_t(box.w) << 16));
+        tail.z = __float_as_int(v.craterCulls[i]);
+        tail.w = int(i);
+        for (uint32_t t = lane; t < total; t += 32u) {
+            const uint32_t b = base + (by0 + t / wide) * binsX + bx0 + t % wide;
+            const uint32_t slot = v.craterCounts[b] + atomicAdd(v.craterCursor + b, 1u);
+            if (slot >= v.craterCapacity) {
+                continue;  // counted in the header's entry total; the host re-plans
+            }
+            int4* dst = reinterpret_cast<int4*>(v.craterEntries + slot);
+#pragma unroll
+            for (int w = 0; w < 9; ++w) {
+                dst[w] = __ldg(src + w);
+            }
+            dst[9] = tail;
+        }
+    }
+}
+
+// The lean path's (amplitude cos phase, amplitude sin phase), at each tile's data offsets.
+__global__ void batch_harmonics_kernel(const BatchView v) {
+    const uint32_t n = v.header->records;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t tile = v.recordTile[i];
+        if (tile == kNone) {
+            continue;
+        }
+        const uint32_t base = v.tiles[tile].dataBase;
+        const uint32_t offset = base + v.records[i].harmonicOffset;
+        const uint32_t count = v.records[i].harmonicCount;
+        for (uint32_t h = 0; h < count; ++h) {
+            const float amplitude = __ldg(v.data + offset + 2u * h);
+            const float phase = __ldg(v.data + offset + 2u * h + 1u);
+            float s, c;
+            sincosf(phase, &s, &c);
+            v.harmonics[offset + 2u * h] = amplitude * c;
+            v.harmonics[offset + 2u * h + 1u] = amplitude * s;
+        }
+    }
+}
+
+__global__ void batch_boulder_count_kernel(const BatchView v, uint32_t binW, uint32_t binH) {
+    const uint32_t n = v.header->boulders;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t tile = v.boulderTile[i];
+        int4 w = make_int4(1, 0, 1, 0);
+        if (tile != kNone) {
+            const BatchTile& t = v.tiles[tile];
+            const BoulderRecord b = v.boulders[i];
+            // ReliefBox on a plane (boulder_relief.cpp:24): reach 0.5 (diameter + width).
+            const double reach = 0.5 * (b.diameter + t.boulderWidth);
+            int c0, c1, r0, r1;
+            window_of(t.grid, b.x - reach, b.y - reach, b.x + reach, b.y + reach, c0, c1, r0,
+                      r1);
+            if (c0 < c1 && r0 < r1 && b.weight > 0.0) {
+                w = make_int4(c0, c1, r0, r1);
+                const uint32_t bx0 = uint32_t(c0) / binW, bx1 = uint32_t(c1 - 1) / binW;
+                const uint32_t by0 = uint32_t(r0) / binH, by1 = uint32_t(r1 - 1) / binH;
+                for (uint32_t by = by0; by <= by1; ++by) {
+                    for (uint32_t bx = bx0; bx <= bx1; ++bx) {
+                        atomicAdd(v.boulderCounts + t.binBase + by * t.binsX + bx, 1u);
+                    }
+                }
+            }
+        }
+        v.boulderWindows[i] = w;
+    }
+}
+
+__global__ void batch_boulder_scatter_kernel(const BatchView v, uint32_t binW, uint32_t binH) {
+    const uint32_t n = v.header->boulders;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 w = v.boulderWindows[i];
+        if (w.x >= w.y) {
+            continue;
+        }
+        const BatchTile& t = v.tiles[v.boulderTile[i]];
+        const BoulderRecord b = v.boulders[i];
+        BoulderEntry e;
+        e.x = b.x;
+        e.y = b.y;
+        e.radius = 0.5 * b.diameter;
+        e.exposed = b.exposedHeight;
+        e.weight = b.weight;
+        e.c0 = w.x;
+        e.c1 = w.y;
+        e.r0 = w.z;
+        e.r1 = w.w;
+        e.pad_ = 0.0;
+        const uint32_t bx0 = uint32_t(w.x) / binW, bx1 = uint32_t(w.y - 1) / binW;
+        const uint32_t by0 = uint32_t(w.z) / binH, by1 = uint32_t(w.w - 1) / binH;
+        for (uint32_t by = by0; by <= by1; ++by) {
+            for (uint32_t bx = bx0; bx <= bx1; ++bx) {
+                const uint32_t bin = t.binBase + by * t.binsX + bx;
+                const uint32_t slot = v.boulderCounts[bin] + atomicAdd(v.boulderCursor + bin, 1u);
+                if (slot < v.boulderCapacity) {
+                    v.boulderEntries[slot] = e;
+                }
+            }
+        }
+    }
+}
+
+// The entry totals the scans left after the last bin, for the host's capacity check.
+__global__ void batch_totals_kernel(const BatchView v) {
+    v.header->craterEntries = v.craterCounts[v.capacityBins];
+    v.header->boulderEntries = v.boulderCounts[v.capacityBins];
+}
+
+// --- the persistent evaluation -------------------------------------------------------------
+
+// Issues the bulk copy of chunk `c` of `count` entries (of `entryBytes`) from `src` into stage
+// buffer c & 1. Thread 0 only.
+__device__ __forceinline__ void issue_chunk(unsigned char (*stage)[kStageBytes], uint64_t* bars,
+                                            const unsigned char* src, uint32_t entryBytes,
+                                            uint32_t chunk, uint32_t count, uint32_t c) {
+    const uint32_t s = c & 1u;
+    const uint32_t n = min(chunk, count - c * chunk);
+    const uint32_t bytes = n * entryBytes;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&bars[s], bytes);
+    bulk_copy_g2s(&stage[s][0], src + size_t(c) * chunk * entryBytes, bytes, &bars[s]);
+}
+
+template <int kBinW, int kBinH, int kCells, bool kFast>
+__global__ void __launch_bounds__(kBinW* kBinH / kCells)
+    batch_evaluate_kernel(const CraterShapeKernel k, const BatchNoise noise, const BatchView v) {
+    constexpr uint32_t kRowThreads = kBinW / kCells;  // threads along one row of a bin
+    static_assert(kBinW % kCells == 0 && kRefTileCells % kCells == 0, "cells per thread");
+    static_assert(kBinW % kRefTileCells == 0 && kBinH % kRefTileCells == 0, "bins of 16-tiles");
+
+    __shared__ __align__(128) unsigned char stage[2][kStageBytes];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t sItem, sTile;
+
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
+    BatchHeader* header = v.header;
+    const uint32_t nbins = header->bins, ntiles = header->tiles;
+    float* const heights = header->heights;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    uint32_t phase[2] = {0u, 0u};
+    uint32_t craterPairs = 0, boulderPairs = 0;
+
+    for (;;) {
+        __syncthreads();  // the previous bin's stage and item are no longer read
+        if (tid == 0) {
+            const uint32_t item = atomicAdd(&header->next, 1u);
+            uint32_t lo = 0;
+            if (item < nbins) {
+                // The last tile whose first bin is at or before the item.
+                uint32_t hi = ntiles;
+                while (hi - lo > 1u) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (v.tiles[mid].binBase <= item) {
+                        lo = mid;
+                    } else {
+                        hi = mid;
+                    }
+                }
+            }
+            sItem = item;
+            sTile = lo;
+        }
+        __syncthreads();
+        const uint32_t item = sItem;
+        if (item >= nbins) {
+            break;
+        }
+        const BatchTile& t = v.tiles[sTile];
+        const Grid grid = t.grid;
+        const uint32_t local = item - t.binBase;
+        const uint32_t binX = local % t.binsX, binY = local / t.binsX;
+        const uint32_t row = binY * kBinH + tid / kRowThreads;
+        const uint32_t col0 = binX * kBinW + (tid % kRowThreads) * kCells;
+        const bool rowIn = row < grid.height;
+        bool live[kCells];
+#pragma unroll
+        for (int j = 0; j < kCells; ++j) {
+            live[j] = rowIn && col0 + j < grid.width;
+        }
+
+        // 1. The source: Fractal2's octaves (fractal.h:219-240) at lattice positions split per
+        //    tile in double; corner hashes reused while the lattice cell does not change.
+        float sum[kCells];
+#pragma unroll
+        for (int j = 0; j < kCells; ++j) {
+            sum[j] = 0.0f;
+        }
+        const float fr = float(row);
+        for (int o = 0; o < noise.octaves; ++o) {
+            const OctaveAnchor a = v.anchors[t.anchorBase + o];
+            // Each cell from its own column, so heights do not depend on the kernel shape.
+            const float px = fmaf(fr, a.ay, a.fx);
+            const float py = fmaf(fr, a.by, a.fy);
+            const uint32_t sz = noise.seedTerm[o];
+            const float w = noise.weight[o];
+            int32_t cx = INT32_MIN, cy = INT32_MIN;
+            uint32_t h00 = 0, h10 = 0, h01 = 0, h11 = 0;
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                const float qx = fmaf(float(col0 + j), a.ax, px);
+                const float qy = fmaf(float(col0 + j), a.bx, py);
+                const float lx = floorf(qx), ly = floorf(qy);
+                const int32_t ix = int32_t(uint32_t(a.ix) + uint32_t(int32_t(lx)));
+                const int32_t iy = int32_t(uint32_t(a.iy) + uint32_t(int32_t(ly)));
+                const float fx = qx - lx, fy = qy - ly;
+                if (ix != cx || iy != cy) {
+                    cx = ix;
+                    cy = iy;
+                    const uint32_t ax0 = uint32_t(ix) * kLcgA + kLcgC, ax1 = ax0 + kLcgA;
+                    const uint32_t ay0 = uint32_t(iy) * kLcgA + kLcgC, ay1 = ay0 + kLcgA;
+                    h00 = corner_hash(ax0, ay0, sz);
+                    h10 = corner_hash(ax1, ay0, sz);
+                    h01 = corner_hash(ax0, ay1, sz);
+                    h11 = corner_hash(ax1, ay1, sz);
+                }
+                const float n00 = noise::gradient2(h00, fx, fy);
+                const float n10 = noise::gradient2(h10, fx - 1.0f, fy);
+                const float n01 = noise::gradient2(h01, fx, fy - 1.0f);
+                const float n11 = noise::gradient2(h11, fx - 1.0f, fy - 1.0f);
+                const float u = fade_fma(fx), vv = fade_fma(fy);
+                const float n = 1.41421356237309505f *
+                                lerp_fma(vv, lerp_fma(u, n00, n10), lerp_fma(u, n01, n11));
+                sum[j] = fmaf(w, n, sum[j]);
+            }
+        }
+        float h[kCells];
+#pragma unroll
+        for (int j = 0; j < kCells; ++j) {
+            h[j] = fmaf(noise.amplitude, sum[j] / noise.total, noise.elevation);
+        }
+
+        // 2. Craters.
+        const uint32_t cFirst = v.craterCounts[item];
+        const uint32_t cEndRaw = v.craterCounts[item + 1];
+        const uint32_t cEnd = min(cEndRaw, v.craterCapacity);
+        const uint32_t cCount = cEnd > cFirst ? cEnd - cFirst : 0u;
+        if (cCount > 0u) {
+            const float* data = v.data + t.dataBase;
+            const float* harmonics = v.harmonics + t.dataBase;
+            // Split positions of the cell centers (MakeSplitPoint, crater_kernel.cpp:303).
+            float pxh[kCells], pxl[kCells];
+            double acc[kCells];
+            const double yd =
+                grid.originY + 0.5 * grid.colRotation + (double(row) + 0.5) * grid.pixelHeight;
+            const float pyh = float(yd);
+            const float pyl = float(yd - double(pyh));
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                const double xd = grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
+                                  0.5 * grid.rowRotation;
+                pxh[j] = float(xd);
+                pxl[j] = float(xd - double(pxh[j]));
+                acc[j] = double(h[j]);
+            }
+            const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
+            bool anyLive = false;
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                anyLive |= live[j];
+            }
+            const unsigned char* src =
+                reinterpret_cast<const unsigned char*>(v.craterEntries + cFirst);
+            const uint32_t chunks = (cCount + kCraterChunk - 1) / kCraterChunk;
+            if (tid == 0) {
+                issue_chunk(stage, bars, src, sizeof(BinEntry), kCraterChunk, cCount, 0);
+                if (chunks > 1) {
+                    issue_chunk(stage, bars, src, sizeof(BinEntry), kCraterChunk, cCount, 1);
+                }
+            }
+            bool failed = false;
+            for (uint32_t c = 0; c < chunks; ++c) {
+                const uint32_t s = c & 1u;
+                if (!mbar_wait(&bars[s], phase[s])) {
+                    failed = true;
+                }
+                phase[s] ^= 1u;
+                if (__syncthreads_or(failed)) {
+                    if (tid == 0) {
+                        atomicOr(&header->flags, 2u);
+                        if (c + 1 < chunks) {
+                            mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                        }
+                    }
+                    return;
+                }
+                const BinEntry* entries = reinterpret_cast<const BinEntry*>(&stage[s][0]);
+                const uint32_t n = min(kCraterChunk, cCount - c * kCraterChunk);
+                for (uint32_t e = 0; e < n; ++e) {
+                    const BinEntry& entry = entries[e];
+                    const CraterRecord& r = entry.record;
+                    const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
+                                        tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
+                                        tileY <= int(entry.tileY1);
+                    const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
+                    const float cull2 = entry.cull * entry.cull;
+                    bool need[kCells];
+                    float dxs[kCells];
+                    bool any = false;
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        dxs[j] = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
+                        need[j] = inTile && live[j] && dxs[j] * dxs[j] + dy * dy < cull2;
+                        any |= need[j];
+                    }
+                    if (!__any_sync(0xffffffffu, any)) {
+                        continue;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        if (need[j]) {
+                            ++craterPairs;
+                            if (kFast) {
+                                bool reached;
+                                const float shaped =
+                                    crater::fast_contribution(fk, harmonics, r, dxs[j], dy, reached);
+                                if (reached) {
+                                    acc[j] += double(shaped);
+                                }
+                            } else {
+                                const crater::Contribution q =
+                                    crater::crater_contribution(k, data, r, dxs[j], dy);
+                                if (q.reached) {
+                                    acc[j] += double(q.shaped);
+                                }
+                            }
+                        }
+                    }
+                }
+                if (c + 2 < chunks) {
+                    __syncthreads();  // every warp has read the buffer before it is refilled
+                    if (tid == 0) {
+                        issue_chunk(stage, bars, src, sizeof(BinEntry), kCraterChunk, cCount,
+                                    c + 2);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                h[j] = float(acc[j]);
+            }
+        }
+
+        // 3. Boulders: max(height, base + weight * dome), base being the height after craters.
+        const uint32_t bFirst = v.boulderCounts[item];
+        const uint32_t bEndRaw = v.boulderCounts[item + 1];
+        const uint32_t bEnd = min(bEndRaw, v.boulderCapacity);
+        const uint32_t bCount = bEnd > bFirst ? bEnd - bFirst : 0u;
+        if (bCount > 0u) {
+            __syncthreads();  // the crater stage is no longer read
+            const double width = t.boulderWidth;
+            const double cy = grid.originY + (double(col0) + 0.5) * grid.colRotation +
+                              (double(row) + 0.5) * grid.pixelHeight;
+            double cxs[kCells], best[kCells];
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                cxs[j] = grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
+                         (double(row) + 0.5) * grid.rowRotation;
+                best[j] = double(h[j]);
+            }
+            const unsigned char* src =
+                reinterpret_cast<const unsigned char*>(v.boulderEntries + bFirst);
+            const uint32_t chunks = (bCount + kBoulderChunk - 1) / kBoulderChunk;
+            if (tid == 0) {
+                issue_chunk(stage, bars, src, sizeof(BoulderEntry), kBoulderChunk, bCount, 0);
+                if (chunks > 1) {
+                    issue_chunk(stage, bars, src, sizeof(BoulderEntry), kBoulderChunk, bCount, 1);
+                }
+            }
+            bool failed = false;
+            for (uint32_t c = 0; c < chunks; ++c) {
+                const uint32_t s = c & 1u;
+                if (!mbar_wait(&bars[s], phase[s])) {
+                    failed = true;
+                }
+                phase[s] ^= 1u;
+                if (__syncthreads_or(failed)) {
+                    if (tid == 0) {
+                        atomicOr(&header->flags, 2u);
+                        if (c + 1 < chunks) {
+                            mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                        }
+                    }
+                    return;
+                }
+                const BoulderEntry* entries = reinterpret_cast<const BoulderEntry*>(&stage[s][0]);
+                const uint32_t n = min(kBoulderChunk, bCount - c * kBoulderChunk);
+                for (uint32_t e = 0; e < n; ++e) {
+                    const BoulderEntry& b = entries[e];
+                    const bool inRows = int(row) >= b.r0 && int(row) < b.r1;
+                    bool any = false;
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        any |= live[j] && inRows && int(col0) + j >= b.c0 && int(col0) + j < b.c1;
+                    }
+                    if (!__any_sync(0xffffffffu, any)) {
+                        continue;
+                    }
+                    const double dy = cy - b.y;
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        if (live[j] && inRows && int(col0) + j >= b.c0 && int(col0) + j < b.c1) {
+                            ++boulderPairs;
+                            const double relief = fmax(dome(b, hypot(cxs[j] - b.x, dy), width), 0.0);
+                            if (relief > 0.0) {
+                                best[j] = fmax(best[j], double(h[j]) + b.weight * relief);
+                            }
+                        }
+                    }
+                }
+                if (c + 2 < chunks) {
+                    __syncthreads();
+                    if (tid == 0) {
+                        issue_chunk(stage, bars, src, sizeof(BoulderEntry), kBoulderChunk, bCount,
+                                    c + 2);
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                h[j] = float(best[j]);
+            }
+        }
+
+        // 4. One write per cell.
+        if (rowIn) {
+            float* dst = heights + t.heightOffset + size_t(row) * t.pitch + col0;
+            bool all = true;
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                all &= live[j];
+            }
+            const uintptr_t address = reinterpret_cast<uintptr_t>(dst);
+            if (kCells % 4 == 0 && all && (address & 15u) == 0u) {
+#pragma unroll
+                for (int j = 0; j < kCells; j += 4) {
+                    *reinterpret_cast<float4*>(dst + j) =
+                        make_float4(h[j], h[j + 1], h[j + 2], h[j + 3]);
+                }
+            } else if (kCells == 2 && all && (address & 7u) == 0u) {
+                *reinterpret_cast<float2*>(dst) = make_float2(h[0], h[kCells - 1]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < kCells; ++j) {
+                    if (live[j]) {
+                        dst[j] = h[j];
+                    }
+                }
+            }
+        }
+    }
+    const uint32_t warpCraters = __reduce_add_sync(0xffffffffu, craterPairs);
+    const uint32_t warpBoulders = __reduce_add_sync(0xffffffffu, boulderPairs);
+    if (lane == 0) {
+        if (warpCraters > 0) {
+            atomicAdd(&header->craterPairs, (unsigned long long)warpCraters);
+        }
+        if (warpBoulders > 0) {
+            atomicAdd(&header->boulderPairs, (unsigned long long)warpBoulders);
+        }
+    }
+}
+
+// The compiled variants: (bin width, bin height, cells per thread).
+constexpr BatchVariant kVariants[] = {
+    {32, 32, 4}, {32, 32, 8}, {64, 32, 8}, {32, 16, 2}, {64, 64, 8},
+};
+constexpr int kVariantCount = int(sizeof(kVariants) / sizeof(kVariants[0]));
+
+template <int kBinW, int kBinH, int kCells, bool kFast>
+cudaError_t launch_variant(const CraterShapeKernel& k, const BatchNoise& noise,
+                           const BatchView& v, uint32_t ctas, cudaStream_t stream) {
+    batch_evaluate_kernel<kBinW, kBinH, kCells, kFast>
+        <<<ctas, kBinW * kBinH / kCells, 0, stream>>>(k, noise, v);
+    return cudaGetLastError();
+}
+
+template <int kBinW, int kBinH, int kCells, bool kFast>
+int occupancy() {
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &blocks, batch_evaluate_kernel<kBinW, kBinH, kCells, kFast>, kBinW * kBinH / kCells,
+            0) != cudaSuccess) {
+        return 1;
+    }
+    return blocks > 0 ? blocks : 1;
+}
+
+uint32_t grid_for(uint32_t items, uint32_t perBlock) {
+    const uint64_t blocks = (uint64_t(items) + perBlock - 1) / perBlock;
+    return uint32_t(blocks < 1 ? 1 : (blocks > 148u * 32u ? 148u * 32u : blocks));
+}
+
+}  // namespace
+
+int batch_variant_count() {
+    return kVariantCount;
+}
+
+BatchVariant batch_variant(int index) {
+    return kVariants[index < 0 || index >= kVariantCount ? 0 : index];
+}
+
+int batch_blocks_per_sm(int index, bool fast) {
+    if (!fast) {
+        return occupancy<32, 32, 4, false>();
+    }
+    switch (index) {
+        case 1: return occupancy<32, 32, 8, true>();
+        case 2: return occupancy<64, 32, 8, true>();
+        case 3: return occupancy<32, 16, 2, true>();
+        case 4: return occupancy<64, 64, 8, true>();
+        default: return occupancy<32, 32, 4, true>();
+    }
+}
+
+cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
+                             const BatchVariant& variant, uint32_t maxRecords,
+                             uint32_t maxBoulders, uint32_t* scanScratch, cudaStream_t stream) {
+    const size_t words = size_t(v.capacityBins) + 1;
+    cudaError_t err = cudaMemsetAsync(v.craterCounts, 0, words * sizeof(uint32_t), stream);
+    if (err == cudaSuccess) {
+        err = cudaMemsetAsync(v.craterCursor, 0, size_t(v.capacityBins) * sizeof(uint32_t), stream);
+    }
+    if (err == cudaSuccess) {
+        err = cudaMemsetAsync(v.boulderCounts, 0, words * sizeof(uint32_t), stream);
+    }
+    if (err == cudaSuccess) {
+        err = cudaMemsetAsync(v.boulderCursor, 0, size_t(v.capacityBins) * sizeof(uint32_t),
+                              stream);
+    }
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const uint32_t tpbX = variant.binW / kRefTileCells, tpbY = variant.binH / kRefTileCells;
+    if (maxRecords > 0) {
+        batch_crater_count_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(k, v, tpbX, tpbY);
+        if ((err = cudaGetLastError()) != cudaSuccess) {
+            return err;
+        }
+    }
+    if (maxBoulders > 0) {
+        batch_boulder_count_kernel<<<grid_for(maxBoulders, 256), 256, 0, stream>>>(
+            v, variant.binW, variant.binH);
+        if ((err = cudaGetLastError()) != cudaSuccess) {
+            return err;
+        }
+    }
+    if ((err = launch_exclusive_scan(v.craterCounts, v.capacityBins, scanScratch, stream)) !=
+        cudaSuccess) {
+        return err;
+    }
+    if ((err = launch_exclusive_scan(v.boulderCounts, v.capacityBins, scanScratch, stream)) !=
+        cudaSuccess) {
+        return err;
+    }
+    if (maxRecords > 0) {
+        batch_crater_scatter_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(v, tpbX, tpbY);
+        if ((err = cudaGetLastError()) != cudaSuccess) {
+            return err;
+        }
+        batch_harmonics_kernel<<<grid_for(maxRecords, 256), 256, 0, stream>>>(v);
+        if ((err = cudaGetLastError()) != cudaSuccess) {
+            return err;
+        }
+    }
+    if (maxBoulders > 0) {
+        batch_boulder_scatter_kernel<<<grid_for(maxBoulders, 256), 256, 0, stream>>>(
+            v, variant.binW, variant.binH);
+        if ((err = cudaGetLastError()) != cudaSuccess) {
+            return err;
+        }
+    }
+    batch_totals_kernel<<<1, 1, 0, stream>>>(v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_evaluate(const CraterShapeKernel& k, const BatchNoise& noise,
+                                  const BatchView& v, int variant, bool fast, uint32_t ctas,
+                                  cudaStream_t stream) {
+    if (!fast) {
+        return launch_variant<32, 32, 4, false>(k, noise, v, ctas, stream);
+    }
+    switch (variant) {
+        case 1: return launch_variant<32, 32, 8, true>(k, noise, v, ctas, stream);
+        case 2: return launch_variant<64, 32, 8, true>(k, noise, v, ctas, stream);
+        case 3: return launch_variant<32, 16, 2, true>(k, noise, v, ctas, stream);
+        case 4: return launch_variant<64, 64, 8, true>(k, noise, v, ctas, stream);
+        default: return launch_variant<32, 32, 4, true>(k, noise, v, ctas, stream);
+    }
+}
+
+}  // namespace tgb

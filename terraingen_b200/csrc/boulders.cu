@@ -10,6 +10,7 @@
 // scan, scatter into kBinCells-square bins, then one CTA per bin stages its entries in shared
 // memory by TMA bulk copies and each thread bakes 4 cells. A boulder touches the cells of its
 // box's pixel window (ForEachFeatureCell, include/terraingen/raster/cell_loops.h:129-152).
+#include "binning.cuh"
 #include "kernels.h"
 
 namespace tgb {
@@ -18,40 +19,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCellsPerThread = 4;
 constexpr uint32_t kChunk = 96;  // 64-byte entries per staged chunk (6 KB)
-constexpr uint32_t kSpinLimit = 1u << 26;
 
-__device__ __forceinline__ bool is_nodata(NoData nd, float h) {
-    if (nd.mode == 1u) {
-        return isnan(h);
-    }
-    return nd.mode != 0u && h == nd.value;
-}
-
-// The pixel window of a box on the grid (PixelWindowIn, src/raster/cell_loops.cpp:21-28).
-__device__ void window_of(const Grid& g, double minX, double minY, double maxX, double maxY,
-                          int& c0, int& c1, int& r0, int& r1) {
-    const double det = g.pixelWidth * g.pixelHeight - g.rowRotation * g.colRotation;
-    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
-    const double xs[2] = {minX, maxX}, ys[2] = {minY, maxY};
-    for (int a = 0; a < 2; ++a) {
-        for (int b = 0; b < 2; ++b) {
-            const double dx = xs[a] - g.originX, dy = ys[b] - g.originY;
-            const double px = (dx * g.pixelHeight - dy * g.rowRotation) / det;
-            const double py = (dy * g.pixelWidth - dx * g.colRotation) / det;
-            lo[0] = fmin(lo[0], px);
-            lo[1] = fmin(lo[1], py);
-            hi[0] = fmax(hi[0], px);
-            hi[1] = fmax(hi[1], py);
-        }
-    }
-    auto clampi = [](double v, uint32_t limit) {
-        return int(v < 0.0 ? 0.0 : (double(limit) < v ? double(limit) : v));
-    };
-    c0 = clampi(floor(lo[0]), g.width);
-    c1 = clampi(ceil(hi[0]), g.width);
-    r0 = clampi(floor(lo[1]), g.height);
-    r1 = clampi(ceil(hi[1]), g.height);
-}
+using namespace binning;
 
 __global__ void boulder_count_kernel(const BoulderRecord* __restrict__ boulders, uint32_t n,
                                      const Grid grid, double width, BoulderBins bins) {
@@ -110,27 +79,6 @@ __global__ void boulder_scatter_kernel(const BoulderRecord* __restrict__ boulder
             }
         }
     }
-}
-
-// DomeHeight (boulder_relief.cpp:44): the dome's height at `distance` averaged over a band
-// `width` wide, or at the point for a zero width.
-__device__ __forceinline__ double dome(const BoulderEntry& b, double distance, double width) {
-    const double radius = b.radius;
-    if (!(width > 0.0)) {
-        const double r2 = (distance * distance) / (radius * radius);
-        return r2 < 1.0 ? b.exposed * sqrt(1.0 - r2) : 0.0;
-    }
-    auto area = [](double u) { return 0.5 * (u * sqrt(1.0 - u * u) + asin(u)); };
-    const double low = fmin(fmax((distance - 0.5 * width) / radius, -1.0), 1.0);
-    const double high = fmin(fmax((distance + 0.5 * width) / radius, -1.0), 1.0);
-    if (!(high > low)) {
-        return 0.0;
-    }
-    return b.exposed * (area(high) - area(low)) * radius / width;
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return uint32_t(__cvta_generic_to_shared(p));
 }
 
 __global__ void __launch_bounds__(kThreads)

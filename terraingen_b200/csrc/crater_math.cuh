@@ -404,7 +404,7 @@ __device__ __forceinline__ float profile_height(const CraterShapeKernel& k, cons
 }
 
 // `KernelRoundedHeight` (craters.h:628): the profile with its rim rounded by a Gaussian.
-__device__ __noinline__ float rounded_height(const CraterShapeKernel& k, const float* data,
+static __device__ __noinline__ float rounded_height(const CraterShapeKernel& k, const float* data,
                                              float distance, float diameter, const CraterRecord& c,
                                              const State& s) {
     const float height = profile_height(k, data, distance, diameter, c, s);
@@ -441,7 +441,7 @@ __device__ __forceinline__ FractalParams kernel_fractal(uint32_t seed, float wav
 }
 
 // `KernelNoiseHeight` (craters.h:673).
-__device__ __noinline__ float noise_height(const CraterShapeKernel& k, const CraterRecord& c,
+static __device__ __noinline__ float noise_height(const CraterShapeKernel& k, const CraterRecord& c,
                                            float dx, float dy, float radii) {
     if (k.noiseAmplitude == 0.0f && k.noiseRimAmplitude == 0.0f) {
         return 0.0f;
@@ -473,7 +473,7 @@ __device__ __forceinline__ float radial_streaks(float radii, float theta, float 
 }
 
 // `KernelTextureHeight` (craters.h:706).
-__device__ __noinline__ float texture_height(const CraterShapeKernel& k, const CraterRecord& c,
+static __device__ __noinline__ float texture_height(const CraterShapeKernel& k, const CraterRecord& c,
                                              float dx, float dy, float radii) {
     if (k.wallStreaks == 0.0f && k.ejecta == 0.0f) {
         return 0.0f;
@@ -685,7 +685,7 @@ __device__ __forceinline__ float terrace_ease(float v, float rounding) {  // cra
 }
 
 // `KernelTerracedRadii` (craters.h:990).
-__device__ __noinline__ float terraced_radii(const float* data, const CraterRecord& c, float radii,
+static __device__ __noinline__ float terraced_radii(const float* data, const CraterRecord& c, float radii,
                                              float theta) {
     const uint32_t o = c.terraceOffset;
     const float inner = value(data, o);
@@ -813,7 +813,7 @@ __device__ __forceinline__ float peak_massif(const float* data, uint32_t m, floa
     return value(data, m + 6u) * powf(flank, value(data, m + 10u));
 }
 
-__device__ __noinline__ float peak_massifs(const float* data, const CraterRecord& c, PeakSize size,
+static __device__ __noinline__ float peak_massifs(const float* data, const CraterRecord& c, PeakSize size,
                                            float dx, float dy) {  // craters.h:1128
     const uint32_t o = c.peakOffset;
     float px = dx / size.base;
@@ -972,10 +972,11 @@ __device__ __forceinline__ float fast_outline_scale(const float* __restrict__ ha
                 kept *= q;
             }
         }
-        const float2* h = reinterpret_cast<const float2*>(harmonics + c.harmonicOffset);
+        // Two 4-byte loads per harmonic: a record's offset into the data may be odd.
+        const float* h = harmonics + c.harmonicOffset;
         for (uint32_t n = 0; n < c.harmonicCount; ++n) {
-            const float2 ab = __ldg(h + n);
-            wobble += kept * (ab.x * cm - ab.y * sm);
+            const float a = __ldg(h + 2u * n), b = __ldg(h + 2u * n + 1u);
+            wobble += kept * (a * cm - b * sm);
             const float t = cm * c1 - sm * s1;
             sm = cm * s1 + sm * c1;
             cm = t;

@@ -20,6 +20,7 @@
 // accumulator. Each contribution is an FP32 value and the sum stays far inside 53 bits, so the
 // accumulation is error-free: the result is the FP32 rounding of the exact sum, independent of
 // the order atomics put the entries in, so every run gives the same bits.
+#include "binning.cuh"
 #include "crater_math.cuh"
 #include "kernels.h"
 
@@ -29,102 +30,8 @@ namespace {
 constexpr int kShapeThreads = 256;     // 8 warps; warp w covers rows 4w..4w+3 of a 32x32 bin
 constexpr int kCellsPerThread = 4;     // 4 adjacent columns, one row
 constexpr uint32_t kChunk = 96;        // entries per staged chunk (15 KB)
-constexpr uint32_t kSpinLimit = 1u << 26;  // bounded mbarrier waits
 
-__device__ __forceinline__ bool is_nodata(NoData nd, float h) {
-    if (nd.mode == 1u) {
-        return isnan(h);
-    }
-    return nd.mode != 0u && h == nd.value;
-}
-
-// `CraterOutline::MaxScale` (src/layers/craters/shaping/irregularity.cpp:229) from the record:
-// sqrt(ellipticity) * (the largest 1 + table deviation, or 1 plus the harmonic amplitudes).
-__device__ double max_outline_scale(const CraterRecord& r, const float* data) {
-    double sum = 1.0;
-    if (r.tableCount > 0u) {
-        for (uint32_t n = 0; n < r.tableCount; ++n) {
-            sum = fmax(sum, 1.0 + double(__ldg(data + r.tableOffset + n)));
-        }
-    } else {
-        for (uint32_t n = 0; n < r.harmonicCount; ++n) {
-            sum += fabs(double(__ldg(data + r.harmonicOffset + 2u * n)));
-        }
-    }
-    return sqrt(double(r.ellipticity)) * sum;
-}
-
-__device__ __forceinline__ void world_to_pixel(const Grid& g, double x, double y, double& px,
-                                               double& py) {
-    // GeoTransform::WorldToPixel (include/terraingen/raster/geo_transform.h:70)
-    const double det = g.pixelWidth * g.pixelHeight - g.rowRotation * g.colRotation;
-    const double dx = x - g.originX;
-    const double dy = y - g.originY;
-    px = (dx * g.pixelHeight - dy * g.rowRotation) / det;
-    py = (dy * g.pixelWidth - dx * g.colRotation) / det;
-}
-
-__device__ __forceinline__ int64_t clamp_index(double v, uint32_t limit) {
-    // ClampIndex(v, limit + 1) (include/terraingen/util/bits.h:42)
-    const double c = v < 0.0 ? 0.0 : (double(limit) < v ? double(limit) : v);
-    return int64_t(c);
-}
-
-// The reference tile range a crater's footprint window touches; x0 > x1 when the window is
-// empty. Also the radius beyond which a cell cannot be within the crater's reach, or +inf when
-// marks, terraces or a floor shift stretch the profile distance past the outline's bound.
-struct Footprint {
-    int4 tiles;
-    float cull;
-};
-
-__device__ Footprint crater_footprint(const CraterShapeKernel& k, const CraterRecord& r,
-                                      const float* data, const double* footprints, uint32_t i,
-                                      const Grid& g) {
-    double x, y, reach;
-    const double scale = max_outline_scale(r, data);
-    if (footprints != nullptr) {
-        x = footprints[3 * i];
-        y = footprints[3 * i + 1];
-        reach = footprints[3 * i + 2];
-    } else {
-        x = double(r.x) + double(r.xLow);
-        y = double(r.y) + double(r.yLow);
-        reach = scale * double(k.reachRadii) * (0.5 * double(r.diameter));
-    }
-    // Surface::Expand on a plane, then MappedBounds of WorldToPixel (mapped_bounds.h).
-    const double xs[2] = {x - reach, x + reach};
-    const double ys[2] = {y - reach, y + reach};
-    double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
-    for (int a = 0; a < 2; ++a) {
-        for (int b = 0; b < 2; ++b) {
-            double px, py;
-            world_to_pixel(g, xs[a], ys[b], px, py);
-            minX = fmin(minX, px);
-            minY = fmin(minY, py);
-            maxX = fmax(maxX, px);
-            maxY = fmax(maxY, py);
-        }
-    }
-    const int64_t c0 = clamp_index(floor(minX), g.width);
-    const int64_t c1 = clamp_index(ceil(maxX), g.width);
-    const int64_t r0 = clamp_index(floor(minY), g.height);
-    const int64_t r1 = clamp_index(ceil(maxY), g.height);
-    Footprint f;
-    if (c0 >= c1 || r0 >= r1) {
-        f.tiles = make_int4(1, 0, 1, 0);
-    } else {
-        f.tiles = make_int4(int(c0 / kRefTileCells), int((c1 - 1) / kRefTileCells),
-                            int(r0 / kRefTileCells), int((r1 - 1) / kRefTileCells));
-    }
-    const bool stretched = r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
-                           r.shiftY != 0.0f;
-    // A little slack over the bound: the profile distance is rounded in float.
-    f.cull = stretched ? INFINITY
-                       : float(scale * double(k.reachRadii) * (0.5 * double(r.diameter)) *
-                               (1.0 + 1e-5)) + 1e-6f;
-    return f;
-}
+using namespace binning;
 
 __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
                                     uint32_t n, const float* __restrict__ data,
@@ -147,9 +54,7 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
                 atomicOr(flags, 1u);
             }
             // Anything beyond an ellipse and power-law harmonics needs the general path.
-            if (r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u ||
-                r.peakCount > 0u || r.shiftX != 0.0f || r.shiftY != 0.0f || r.upslopeX != 0.0f ||
-                r.upslopeY != 0.0f || r.hasDatum == 1u) {
+            if (crater_heavy(r)) {
                 atomicOr(flags, 4u);
             }
         }
@@ -228,52 +133,6 @@ __global__ void crater_harmonics_kernel(const CraterRecord* __restrict__ records
         out[offset + 2u * h] = amplitude * c;
         out[offset + 2u * h + 1u] = amplitude * s;
     }
-}
-
-// --- TMA bulk copy helpers (PTX ISA: cp.async.bulk, mbarrier) -------------------------------
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return uint32_t(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
-                                              uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, "
-        "1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(smem_addr(bar)), "r"(phase)
-        : "memory");
-    return done != 0u;
-}
-
-// Waits for the barrier's phase, giving up after kSpinLimit polls (returns false then).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    for (uint32_t spin = 0; spin < kSpinLimit; ++spin) {
-        if (mbar_try_wait(bar, phase)) {
-            return true;
-        }
-    }
-    return false;
 }
 
 template <bool kFast>

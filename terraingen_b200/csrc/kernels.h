@@ -164,6 +164,102 @@ cudaError_t launch_ds_read(const DsLevel& nodes, const DsFrame& frame, const Gri
 cudaError_t launch_philox_probe(const uint32_t* in, uint32_t n, uint32_t* out, double* normals,
                                 cudaStream_t stream);
 
+// --- batched tiles (batch.cu) ------------------------------------------------------------
+// Many tiles evaluated together: source fBm, craters and boulders of every tile in one
+// persistent launch over all the tiles' bins, after one count / scan / scatter per feature kind.
+
+constexpr int kBatchMaxOctaves = 32;
+
+// One tile of a batch. Its bins are numbered binBase .. binBase + binsX * binsY - 1 in the
+// batch's bin order, which is the work queue's order.
+struct BatchTile {
+    Grid grid;
+    uint64_t heightOffset;  // output index of cell (0, 0)
+    uint32_t pitch;         // output floats from one row to the next
+    uint32_t binsX, binsY;
+    uint32_t binBase;
+    uint32_t dataBase;      // added to the tile's record data offsets
+    uint32_t anchorBase;    // the tile's first OctaveAnchor
+    double boulderWidth;    // dome band width (the tile's sample spacing)
+};
+static_assert(sizeof(BatchTile) == 96, "BatchTile layout");
+
+// The lattice position of a tile's cell (0, 0) for one octave, split in double into an integer
+// cell (ix, iy) and a float fraction (fx, fy), and the lattice steps of one column (ax, bx) and
+// one row (ay, by): cell (c, r) lies at (ix + fx + c ax + r ay, iy + fy + c bx + r by).
+struct OctaveAnchor {
+    int32_t ix, iy;
+    float fx, fy;
+    float ax, ay, bx, by;
+};
+static_assert(sizeof(OctaveAnchor) == 32, "OctaveAnchor layout");
+
+// The batch's source: elevation + amplitude * (sum of weight * Perlin octave) / total.
+struct BatchNoise {
+    int32_t octaves;
+    float amplitude, total, elevation;
+    uint32_t seedTerm[kBatchMaxOctaves];  // octave seed through pcg3d's first LCG step
+    float weight[kBatchMaxOctaves];
+};
+
+// Per-run values the launches read from device memory, so one captured graph serves any batch
+// within the plan's capacities.
+struct BatchHeader {
+    uint32_t tiles, records, boulders, bins;
+    float* heights;
+    uint32_t next;     // work-queue cursor
+    uint32_t flags;    // 1 datum seen, 2 staged copy timed out, 4 entries over capacity,
+                       // 8 a record needs the general shaping path
+    unsigned long long craterPairs, boulderPairs;
+    uint32_t craterEntries, boulderEntries;  // entries the bins needed
+};
+
+struct BatchView {
+    BatchHeader* header;
+    const BatchTile* tiles;
+    const OctaveAnchor* anchors;
+    const CraterRecord* records;
+    const uint32_t* recordTile;    // tile of each record, ~0u for none
+    const double* footprints;      // optional (x, y, reach) per record
+    const float* data;
+    float* harmonics;
+    const BoulderRecord* boulders;
+    const uint32_t* boulderTile;
+    uint32_t* craterCounts;        // [capacityBins + 1]
+    uint32_t* craterCursor;        // [capacityBins]
+    BinEntry* craterEntries;
+    uint32_t craterCapacity;
+    int4* craterBoxes;             // [records]
+    float* craterCulls;            // [records]
+    uint32_t* boulderCounts;
+    uint32_t* boulderCursor;
+    BoulderEntry* boulderEntries;
+    uint32_t boulderCapacity;
+    int4* boulderWindows;          // [boulders]
+    uint32_t capacityBins;
+};
+
+// A kernel shape of the persistent evaluation: bins of binW x binH cells, cellsPerThread
+// adjacent cells of one row per thread.
+struct BatchVariant {
+    uint32_t binW, binH, cellsPerThread;
+};
+// The variants compiled in; variant 0 also serves batches that need the general shaping path.
+int batch_variant_count();
+BatchVariant batch_variant(int index);
+// Persistent CTAs of `index` that fit on one SM (occupancy), for sizing the launch.
+int batch_blocks_per_sm(int index, bool fast);
+
+// Counting and scattering of the batch's craters and boulders into its bins, for `variant`'s
+// bin size (launches sized for `maxRecords` / `maxBoulders`, counts read from the header).
+cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
+                             const BatchVariant& variant, uint32_t maxRecords,
+                             uint32_t maxBoulders, uint32_t* scanScratch, cudaStream_t stream);
+// The persistent evaluation over every bin of the batch, `ctas` CTAs.
+cudaError_t launch_batch_evaluate(const CraterShapeKernel& k, const BatchNoise& noise,
+                                  const BatchView& v, int variant, bool fast, uint32_t ctas,
+                                  cudaStream_t stream);
+
 // The ALU issue-rate probe (probe.cu): one launch of a fixed IMAD/FFMA mix; `laneOps` receives
 // the lane operations it performs.
 cudaError_t launch_alu_probe(uint32_t* sink, uint64_t* laneOps, cudaStream_t stream);

@@ -114,6 +114,10 @@ extern "C" int tg_boulders_bake_static(const void* boulders, uint32_t n, double 
     if (boulders == nullptr || heights == nullptr) {
         return fail(TG_ERROR_ARGUMENT, "boulders and heights are required");
     }
+    if (reinterpret_cast<uintptr_t>(boulders) % 8u != 0u ||
+        reinterpret_cast<uintptr_t>(heights) % 4u != 0u) {
+        return fail(TG_ERROR_ARGUMENT, "boulders must be 8-byte and heights 4-byte aligned");
+    }
     const Grid g{grid->width,        grid->height,   grid->origin_x,    grid->pixel_width,
                  grid->row_rotation, grid->origin_y, grid->col_rotation, grid->pixel_height};
     BoulderBins bins{};

@@ -91,6 +91,8 @@ def stand_in_boulders(grid: GridSpec, expected: float, exponent: float, dmin: fl
     area = grid.width * grid.height * spacing * spacing
     c = expected / (area * (dmin ** -exponent - dmax ** -exponent))
     lo = max(dmin, 2.0 * spacing)
+    if lo >= dmax:
+        return np.zeros((0, 5), np.float64)  # none resolved at this spacing
     margin = 0.5 * dmax
     w, h = grid.width * spacing + 2 * margin, grid.height * spacing + 2 * margin
     n = rng.poisson(c * w * h * (lo ** -exponent - dmax ** -exponent))
@@ -132,3 +134,64 @@ def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
     grid = centered(side, side, pixel)
     fr = np.array([fractal(seed=seed, wavelength=512.0, amplitude=5.0, octaves=8)])
     return grid, fr, craters, boulders
+
+
+def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: float = 1.7e6,
+                 density: float = 0.1, seed: int = 11, boulders: bool = True):
+    """Uneven tiles of the synthetic terrain's stack ("tiles4096"): `n` square tiles with sides
+    log-uniform on `side` cells, spacings log-uniform on `spacing` m, centers uniform over a disk
+    of `radius` m around the origin (the polar frame of a 1737.4 km sphere), the 4097^2 terrain's
+    source, and its craters and boulders at `density` times their density. Each tile carries the
+    craters tg_crater_batch builds for its grid and its own seeded boulders."""
+    from .batch import TILE, TileSet, layout
+
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(side[0]), np.log(side[1] + 1), n)).astype(np.int64)
+    sides = np.clip(sides, side[0], side[1])
+    pixels = np.exp(rng.uniform(np.log(spacing[0]), np.log(spacing[1]), n))
+    r = radius * np.sqrt(rng.random(n))
+    theta = rng.uniform(0.0, 2.0 * np.pi, n)
+    cxs, cys = r * np.cos(theta), r * np.sin(theta)
+    full_area = (4097 * 0.5) ** 2
+    crater_c = density * 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
+    population = crater_population(7, crater_c, 1.0, 500.0)
+    grids = [centered(int(s), int(s), float(p), float(x), float(y))
+             for s, p, x, y in zip(sides, pixels, cxs, cys)]
+    offsets, pitch = layout(grids)
+    tiles = np.zeros(n, TILE)
+    kernel = None
+    records, data, footprints, stones = [], [], [], []
+    nrec = ndata = nstone = 0
+    for i, g in enumerate(grids):
+        k, rec, dat, foot = crater_batch(population, g)
+        kernel = k if kernel is None else kernel
+        if boulders:
+            b = stand_in_boulders(g, density * 1e6 * g.cells * g.pixel ** 2 / full_area, 2.5, 0.2,
+                                  3.0, 0.5, seed * 100003 + i)
+        else:
+            b = np.zeros((0, 5), np.float64)
+        t = tiles[i]
+        t["width"], t["height"] = g.width, g.height
+        t["origin_x"], t["pixel_width"], t["origin_y"], t["pixel_height"] = (
+            g.x0, g.pixel, g.y0, -g.pixel)
+        t["height_offset"], t["pitch"] = offsets[i], pitch[i]
+        t["crater_begin"], t["crater_count"], t["data_begin"] = nrec, len(rec), ndata
+        t["boulder_begin"], t["boulder_count"] = nstone, len(b)
+        t["boulder_width"] = g.pixel
+        records.append(rec)
+        data.append(dat)
+        footprints.append(foot)
+        stones.append(b)
+        nrec += len(rec)
+        ndata += len(dat)
+        nstone += len(b)
+    return TileSet(
+        tiles=tiles,
+        fractals=np.array([fractal(seed=7, wavelength=512.0, amplitude=5.0, octaves=8)]),
+        elevation=0.0,
+        crater_kernel=kernel if kernel is not None else np.zeros((), CRATER_SHAPE_KERNEL),
+        crater_records=np.concatenate(records) if records else np.zeros(0, CRATER_RECORD),
+        crater_data=np.concatenate(data).astype(np.float32) if data else np.zeros(0, np.float32),
+        crater_footprints=np.concatenate(footprints) if footprints else np.zeros(0),
+        boulders=np.ascontiguousarray(np.concatenate(stones)) if stones else np.zeros((0, 5)),
+        grids=grids)

@@ -144,3 +144,29 @@ def test_datum_records_rejected_by_binned_form(device, crater_fixture):
     with pytest.raises(TgError) as info:
         device.craters_apply(kernel, rec, data, grid, h)
     assert info.value.status == 3
+
+
+def test_binned_odd_data_offsets_and_alignment(device, crater_fixture):
+    # Record data may start at an odd float offset (the lean path reads harmonics as scalars);
+    # device records that are not 16-byte aligned are refused, not read.
+    import torch
+
+    from terraingen_b200 import TgError
+
+    fx = crater_fixture
+    kernel, records, data = inputs(fx, "config1")
+    grid = grid_of(fx["config1_grid"])
+    base = np.zeros((grid.height, grid.width), np.float32)
+    device.craters_apply(kernel, records, data, grid, base)
+    shifted = records.copy()
+    shifted["harmonicOffset"] += 1
+    odd = np.zeros_like(base)
+    device.craters_apply(kernel, shifted, np.concatenate([np.zeros(1, np.float32), data]), grid,
+                         odd)
+    assert np.array_equal(odd.view(np.uint32), base.view(np.uint32))
+    raw = torch.zeros(records.nbytes + 16, dtype=torch.uint8, device="cuda")
+    raw[8:8 + records.nbytes] = torch.from_numpy(records.view(np.uint8).copy()).cuda()
+    h = torch.zeros((grid.height, grid.width), dtype=torch.float32, device="cuda")
+    with pytest.raises(TgError):
+        device.craters_apply(kernel, raw[8:8 + records.nbytes], torch.from_numpy(data).cuda(), grid,
+                             h)
