@@ -1,5 +1,6 @@
 """Benchmark: Mcells/s of the plain GPU path on the synthetic 4097 x 4097 terrain at 0.5 m
-(8-octave fBm source, 200,000 craters, 1,000,000 boulders of which those resolved are drawn).
+(8-octave fBm source, 200,000 craters, 1,000,000 boulders of which those resolved are drawn), and
+under "forms" the batched form on 4096 uneven tiles against the plain per-tile path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tgb200|reference]
 
@@ -16,7 +17,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import time
 from pathlib import Path
@@ -50,11 +50,17 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="tgb200", choices=["tgb200", "reference"])
     p.add_argument("--cpu-window", type=int, default=1025,
                    help="side of the window the CPU baseline evaluates")
+    p.add_argument("--tiles", type=int, default=4096,
+                   help="tiles of the batched form's uneven-tile workload (0 skips it)")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="batched kernel shape (tg_batch_variant index); -1 runs the autotuner")
+    p.add_argument("--batched-only", action="store_true",
+                   help="run the batched form alone and print its line (profiling)")
     return p.parse_args()
 
 
@@ -93,54 +99,74 @@ def max_over_ranks(value, world):
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled every few milliseconds during the timed region, by
+    NVML queries (read-only) from a background thread; nvidia-smi when NVML is unavailable."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(self.index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            handle = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(handle, nv.NVML_CLOCK_SM))
+        except Exception:
+            return self
+        self._stop = threading.Event()
+
+        def poll():
+            while not self._stop.is_set():
+                try:
+                    mhz = nv.nvmlDeviceGetClockInfo(handle, nv.NVML_CLOCK_SM)
+                    reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    self.samples.append((float(mhz), int(reasons)))
+                except Exception:
+                    break
+                self._stop.wait(0.002)
+
+        self._thread = threading.Thread(target=poll, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                out, _ = self.proc.communicate(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
+        import pynvml as nv
+
+        reasons = set()
+        for _, bits in self.samples:
+            for name, const in self.REASONS.items():
+                if bits & getattr(nv, const, 0):
                     reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [m for m, _ in self.samples]
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, 2 ms"}
 
 
 def cpu_sample(steps, warmup, window, quiet=False):
@@ -191,6 +217,130 @@ def scan_launches(n):
     return 1 if blocks == 1 else 2 + scan_launches(blocks)
 
 
+def batched_form(dev, args, rank, world, alu_peak):
+    """The batched form on uneven tiles (tiles4096): every rank its own 4096 tiles, evaluated in
+    one persistent launch replayed from CUDA graphs, against the plain per-tile path on the same
+    tiles (tg_noise_source, tg_craters_apply, tg_boulders_bake per tile, device-resident)."""
+    import torch
+
+    from terraingen_b200.batch import Batch
+    from terraingen_b200.workloads import uneven_tiles
+
+    ts = uneven_tiles(args.tiles, seed=11 + 7919 * rank)
+    batch = Batch(dev)
+    batch.load(ts)
+    out = torch.empty(ts.output_floats, dtype=torch.float32, device="cuda")
+    if args.variant >= 0:
+        batch.set_variant(args.variant)
+        tune_ms = []
+    else:
+        tune_ms = batch.tune(trials=2)
+    for _ in range(args.warmup):
+        batch.evaluate(out)
+    barrier(world)
+    bins, evals, graphs = [], [], []
+    with Clocks(torch.cuda.current_device()) as clocks:
+        for _ in range(args.steps):
+            batch.evaluate(out)  # writes 4 B x cells (far above L2) each step
+            st = batch.stats()
+            bins.append(st["bin_ms"])
+            evals.append(st["evaluate_ms"])
+            graphs.append(st["graph_ms"])
+    total_s = max_over_ranks(float(np.sum(graphs)) * 1e-3, world)
+    value = world * ts.cells * args.steps / total_s / 1e6
+
+    # The plain per-tile path over the same tiles, inputs resident on the device.
+    stream = torch.cuda.current_stream()
+    per_tile = []
+    t = ts.tiles
+    for i, g in enumerate(ts.grids):
+        r0, rn = int(t["crater_begin"][i]), int(t["crater_count"][i])
+        d0 = int(t["data_begin"][i])
+        d1 = int(t["data_begin"][i + 1]) if i + 1 < len(ts.grids) else len(ts.crater_data)
+        b0, bn = int(t["boulder_begin"][i]), int(t["boulder_count"][i])
+        per_tile.append((
+            g, rn,
+            torch.from_numpy(ts.crater_records[r0:r0 + rn].view(np.uint8).copy()).cuda(),
+            torch.from_numpy(ts.crater_data[d0:max(d1, d0 + 1)].copy()).cuda(),
+            torch.from_numpy(ts.crater_footprints[3 * r0:3 * (r0 + rn)].copy()).cuda(),
+            bn, torch.from_numpy(np.ascontiguousarray(ts.boulders[b0:b0 + bn])).cuda(),
+            torch.empty((g.height, g.width), dtype=torch.float32, device="cuda"),
+            float(t["boulder_width"][i])))
+
+    def plain():
+        for g, rn, rec, dat, foot, bn, bou, h, width in per_tile:
+            dev.noise_source(ts.fractals, g, h, ts.elevation)
+            if rn:
+                dev.craters_apply(ts.crater_kernel, rec, dat, g, h, footprints=foot)
+            if bn:
+                dev.boulders_bake(bou, g, h, width=width)
+
+    plain()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_s = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world)
+    plain_value = world * ts.cells / plain_s / 1e6
+
+    # End to end: tg_batch_run from host arrays into pinned host memory (inputs copied in and
+    # heights copied out inside each call).
+    host_out = torch.empty(ts.output_floats, dtype=torch.float32).pin_memory().numpy()
+    batch.run(ts, host_out)
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        batch.run(ts, host_out)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * ts.cells * e2e_steps / e2e_s / 1e6
+    same = bool(np.array_equal(host_out, out.cpu().numpy()))
+    st = batch.stats()
+    octaves = int(ts.fractals[0]["octaves"])
+    eval_ms = float(np.mean(evals))
+    ops = (ts.cells * octaves * NOISE_OPS_PER_CELL_OCTAVE + st["crater_pairs"] * CRATER_OPS_PER_PAIR
+           + st["boulder_pairs"] * BOULDER_OPS_PER_PAIR)
+    achieved = ops / (eval_ms * 1e-3) / 1e12
+    peak = alu_peak / 1e12
+    batch.close()
+    return {
+        "workload": f"tiles{args.tiles}: sides log-uniform 65-1025, 0.25-2 m/px, centers within "
+                    "1.7e6 m (polar frame of a 1737.4 km sphere); terrain4097 stack at 1/10 "
+                    "crater and boulder density",
+        "tiles": int(len(ts.tiles)), "cells_per_gpu": ts.cells,
+        "craters": int(len(ts.crater_records)), "boulders": int(len(ts.boulders)),
+        "value": round(value, 3), "unit": UNIT,
+        "ms_per_step": round(float(np.mean(graphs)), 4),
+        "bin_ms": round(float(np.mean(bins)), 4), "evaluate_ms": round(eval_ms, 4),
+        "plain_per_tile": {"value": round(plain_value, 3), "unit": UNIT,
+                           "ms": round(plain_s * 1e3, 3),
+                           "path": "tg_noise_source + tg_craters_apply + tg_boulders_bake per tile"},
+        "speedup_vs_plain": round(value / plain_value, 2),
+        "kernel_shape": {"bin": [st["bin_width"], st["bin_height"]],
+                         "cells_per_thread": st["cells_per_thread"], "ctas": st["ctas"]},
+        "autotuner_ms": [None if not np.isfinite(m) else round(m, 3) for m in tune_ms],
+        "graph": {"captures": st["captures"], "replays": st["replays"]},
+        "roofline": {"kernel": "batch_evaluate_kernel (persistent: fBm + craters + boulders)",
+                     "bound": "alu", "achieved": round(achieved, 3), "peak": round(peak, 3),
+                     "unit": "Tops/s", "frac": round(achieved / peak, 3) if peak else None,
+                     "algorithmic_ops": f"{NOISE_OPS_PER_CELL_OCTAVE} per cell-octave + "
+                                        f"{CRATER_OPS_PER_PAIR} per crater pair "
+                                        f"({st['crater_pairs']}) + {BOULDER_OPS_PER_PAIR} per "
+                                        f"boulder pair ({st['boulder_pairs']})"},
+        "accuracy": "source within 1e-4 m of the FP64 oracle at 1.7e6 m "
+                    "(tests/test_batch_gpu.py); craters and boulders evaluate the plain path's "
+                    "pairs, within 1e-4 m of it",
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(ts.input_bytes()),
+                "d2h_bytes_per_step": int(ts.output_floats * 4), "matches_device_path": same},
+        "gpu_launches_per_step": int(6 + 2 * scan_launches(st["bins"]) + 1),
+        "clocks": clocks.summary(),
+        "l2": "output (4 B per cell) far above L2, written every step",
+    }
+
+
 def main():
     args = parse()
     rank, world, local = dist_setup(args.gpus)
@@ -208,6 +358,11 @@ def main():
     barrier(world)
     torch.cuda.set_device(local)
     dev = Device(local)
+    if args.batched_only:
+        form = batched_form(dev, args, rank, world, dev.measure_alu())
+        if rank == 0:
+            print(json.dumps({"form": "batched", **form}), flush=True)
+        return
     # Each rank's own tile, side by side along x (independent tiles, no exchange).
     w = terrain4097(SIDE, PIXEL, cx=rank * SIDE * PIXEL)
     stream = torch.cuda.current_stream()
@@ -280,6 +435,9 @@ def main():
 
     # Parity of the device-resident and end-to-end results (same inputs, same bits).
     same = bool(torch.equal(heights.cpu(), h_heights))
+    forms = {}
+    if args.tiles > 0:
+        forms["batched"] = batched_form(dev, args, rank, world, alu_peak)
 
     if rank != 0:
         return
@@ -334,6 +492,7 @@ def main():
                 "d2h_bytes_per_step": int(d2h), "matches_device_path": same},
         "gpu_launches": int(launches * args.steps),
         "clocks": clocks.summary(),
+        "forms": forms,
     }
     print(json.dumps(line), flush=True)
 

@@ -312,8 +312,9 @@ int tg_crater_batch(const tg_crater_population* population, const tg_crater_shap
  * Many tiles of one layer stack (a Perlin fBm source, a crater layer and a boulder layer)
  * evaluated together: one count / scan / scatter of every tile's craters and boulders into bins,
  * then ONE persistent launch in which each CTA takes bins from a device work queue and writes
- * each cell once (source, craters, boulders). The launches are captured in a CUDA graph on the
- * first evaluation and replayed while the batch fits the plan's capacities. World-to-lattice
+ * each cell once (source, craters, boulders). The launches are captured in two CUDA graphs
+ * (binning, evaluation) on the first evaluation and replayed while the batch fits the plan's
+ * capacities. World-to-lattice
  * offsets are split in double per tile and octave, so tiles far from the origin keep float
  * lattice fractions (heights within 1e-3 m of an FP64 evaluation at 1.7e6 m). The reference
  * evaluates tiles one at a time (Terrain::EvaluateTiles, src/pipeline/terrain.cpp:158); this is
@@ -371,7 +372,7 @@ typedef struct tg_batch_stats {
     uint32_t replays;            /* graph launches so far */
     float bin_ms;                /* device time of the last binning (count, scan, scatter) */
     float evaluate_ms;           /* device time of the last persistent evaluation */
-    float graph_ms;              /* device time of the last graph launch, end to end */
+    float graph_ms;              /* device time of the last binning + evaluation, end to end */
     uint32_t ctas;               /* persistent CTAs of the last evaluation */
 } tg_batch_stats;
 

@@ -85,9 +85,8 @@ struct Signature {
 struct tg_batch {
     tg_device* dev = nullptr;
     cudaStream_t stream = nullptr;
-    // [0..2] inside the graph (before binning, between binning and evaluation, after it),
-    // [3..4] around each graph launch.
-    cudaEvent_t events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // Recorded before the binning graph, between it and the evaluation graph, and after.
+    cudaEvent_t events[3] = {nullptr, nullptr, nullptr};
     BatchHeader* pinned = nullptr;  // [0] written before each replay, [1] read back after
     Buffer slots[kSlotBatchSlots];
     int variant = 0;
@@ -106,8 +105,8 @@ struct tg_batch {
     uint32_t bins = 0;
 
     // Graph state.
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph[2] = {nullptr, nullptr};  // binning, evaluation
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
     Signature captured{};
     uint32_t captures = 0, replays = 0;
     tg_batch_stats last{};
@@ -220,44 +219,20 @@ Signature signature(tg_batch* b) {
 }
 
 void drop_graph(tg_batch* b) {
-    if (b->exec != nullptr) {
-        cudaGraphExecDestroy(b->exec);
-        b->exec = nullptr;
-    }
-    if (b->graph != nullptr) {
-        cudaGraphDestroy(b->graph);
-        b->graph = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (b->exec[i] != nullptr) {
+            cudaGraphExecDestroy(b->exec[i]);
+            b->exec[i] = nullptr;
+        }
+        if (b->graph[i] != nullptr) {
+            cudaGraphDestroy(b->graph[i]);
+            b->graph[i] = nullptr;
+        }
     }
 }
 
-// Captures header upload, binning, evaluation and status read-back as one graph.
-int capture(tg_batch* b, const Signature& s) {
-    drop_graph(b);
-    (void)cudaGetLastError();  // a stale launch error must not be read as one of this capture's
-    TG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    cudaError_t err = cudaMemcpyAsync(s.view.header, &b->pinned[0], sizeof(BatchHeader),
-                                      cudaMemcpyHostToDevice, b->stream);
-    if (err == cudaSuccess) {
-        err = cudaEventRecord(b->events[0], b->stream);
-    }
-    if (err == cudaSuccess) {
-        err = launch_batch_bin(s.kernel, s.view, batch_variant(s.variant), s.maxRecords,
-                               s.maxBoulders, ptr<uint32_t>(b, kSlotScanScratch), b->stream);
-    }
-    if (err == cudaSuccess) {
-        err = cudaEventRecord(b->events[1], b->stream);
-    }
-    if (err == cudaSuccess) {
-        err = launch_batch_evaluate(s.kernel, s.noise, s.view, s.variant, s.fast, s.ctas,
-                                    b->stream);
-    }
-    if (err == cudaSuccess) {
-        err = cudaEventRecord(b->events[2], b->stream);
-    }
-    if (err == cudaSuccess) {
-        err = cudaMemcpyAsync(&b->pinned[1], s.view.header, sizeof(BatchHeader),
-                              cudaMemcpyDeviceToHost, b->stream);
-    }
+// Ends a capture begun on the batch's stream and instantiates it as graph `i`.
+int finish_capture(tg_batch* b, int i, cudaError_t err) {
     cudaGraph_t graph = nullptr;
     const cudaError_t end = cudaStreamEndCapture(b->stream, &graph);
     if (err != cudaSuccess) {
@@ -267,8 +242,36 @@ int capture(tg_batch* b, const Signature& s) {
         return cuda_fail(err, "batch capture");
     }
     TG_CUDA(end, "end capture");
-    b->graph = graph;
-    TG_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+    b->graph[i] = graph;
+    TG_CUDA(cudaGraphInstantiate(&b->exec[i], graph, 0), "graph instantiate");
+    return TG_OK;
+}
+
+// Captures two graphs: the header upload and the binning (count, scan, scatter), then the
+// persistent evaluation and the status read-back. Launched back to back; events between them
+// time each part.
+int capture(tg_batch* b, const Signature& s) {
+    drop_graph(b);
+    (void)cudaGetLastError();  // a stale launch error must not be read as one of this capture's
+    TG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaMemcpyAsync(s.view.header, &b->pinned[0], sizeof(BatchHeader),
+                                      cudaMemcpyHostToDevice, b->stream);
+    if (err == cudaSuccess) {
+        err = launch_batch_bin(s.kernel, s.view, batch_variant(s.variant), s.maxRecords,
+                               s.maxBoulders, ptr<uint32_t>(b, kSlotScanScratch), b->stream);
+    }
+    if (int st = finish_capture(b, 0, err)) {
+        return st;
+    }
+    TG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    err = launch_batch_evaluate(s.kernel, s.noise, s.view, s.variant, s.fast, s.ctas, b->stream);
+    if (err == cudaSuccess) {
+        err = cudaMemcpyAsync(&b->pinned[1], s.view.header, sizeof(BatchHeader),
+                              cudaMemcpyDeviceToHost, b->stream);
+    }
+    if (int st = finish_capture(b, 1, err)) {
+        return st;
+    }
     b->captured = s;
     ++b->captures;
     return TG_OK;
@@ -286,14 +289,16 @@ int replay(tg_batch* b, float* out, cudaStream_t stream) {
         h.heights = out;
         b->pinned[0] = h;
         const Signature s = signature(b);
-        if (b->exec == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
+        if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
             if (int st = capture(b, s)) {
                 return st;
             }
         }
-        TG_CUDA(cudaEventRecord(b->events[3], stream), "event record");
-        TG_CUDA(cudaGraphLaunch(b->exec, stream), "graph launch");
-        TG_CUDA(cudaEventRecord(b->events[4], stream), "event record");
+        TG_CUDA(cudaEventRecord(b->events[0], stream), "event record");
+        TG_CUDA(cudaGraphLaunch(b->exec[0], stream), "graph launch");
+        TG_CUDA(cudaEventRecord(b->events[1], stream), "event record");
+        TG_CUDA(cudaGraphLaunch(b->exec[1], stream), "graph launch");
+        TG_CUDA(cudaEventRecord(b->events[2], stream), "event record");
         ++b->replays;
         TG_CUDA(cudaStreamSynchronize(stream), "synchronize");
         const BatchHeader r = b->pinned[1];
@@ -313,16 +318,9 @@ int replay(tg_batch* b, float* out, cudaStream_t stream) {
         b->last.crater_entries = r.craterEntries;
         b->last.boulder_entries = r.boulderEntries;
         b->last.ctas = s.ctas;
-        TG_CUDA(cudaEventElapsedTime(&b->last.graph_ms, b->events[3], b->events[4]),
-                "elapsed time");
-        // The split between binning and evaluation comes from the events inside the graph.
-        if (cudaEventElapsedTime(&b->last.bin_ms, b->events[0], b->events[1]) != cudaSuccess ||
-            cudaEventElapsedTime(&b->last.evaluate_ms, b->events[1], b->events[2]) !=
-                cudaSuccess) {
-            (void)cudaGetLastError();
-            b->last.bin_ms = NAN;
-            b->last.evaluate_ms = NAN;
-        }
+        TG_CUDA(cudaEventElapsedTime(&b->last.bin_ms, b->events[0], b->events[1]), "elapsed");
+        TG_CUDA(cudaEventElapsedTime(&b->last.evaluate_ms, b->events[1], b->events[2]), "elapsed");
+        TG_CUDA(cudaEventElapsedTime(&b->last.graph_ms, b->events[0], b->events[2]), "elapsed");
         if (!craterShort && !boulderShort) {
             return TG_OK;
         }
@@ -373,7 +371,7 @@ int tg_batch_create(tg_device* device, tg_batch** batch) {
     tg_batch* b = new tg_batch();
     b->dev = device;
     cudaError_t err = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-    for (int i = 0; i < 5 && err == cudaSuccess; ++i) {
+    for (int i = 0; i < 3 && err == cudaSuccess; ++i) {
         err = cudaEventCreate(&b->events[i]);
     }
     if (err == cudaSuccess) {
