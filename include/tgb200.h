@@ -325,7 +325,7 @@ typedef struct tg_batch tg_batch;
  * Its craters are records [crater_begin, crater_begin + crater_count) of the batch, their data
  * offsets relative to crater_data + data_begin (what tg_crater_batch returns for the tile's grid);
  * its boulders are [boulder_begin, boulder_begin + boulder_count), baked with dome band width
- * `boulder_width` (the tile's sample spacing). A record or boulder belongs to one tile. */
+ * `boulder_width` (the tile's sample spacing). */
 typedef struct tg_tile {
     tg_grid grid;
     uint64_t height_offset;
@@ -338,9 +338,27 @@ typedef struct tg_tile {
     double boulder_width;
 } tg_tile;
 
+/* One set of scattered point queries of a batch (Terrain::EvaluatePoints,
+ * src/pipeline/terrain.cpp:133): points [point_begin, point_begin + point_count) of the batch's
+ * `points` (x, y doubles), point i's height going to heights[height_offset + i]. Craters and
+ * boulders as a tile's; a crater or boulder changes a point within its reach. */
+typedef struct tg_point_set {
+    uint32_t point_begin;
+    uint32_t point_count;
+    uint64_t height_offset;
+    uint32_t crater_begin;
+    uint32_t crater_count;
+    uint32_t data_begin;
+    uint32_t boulder_begin;
+    uint32_t boulder_count;
+    uint32_t reserved;
+    double boulder_width;
+} tg_point_set;
+
 /* A batch's inputs (host memory). `fractals` holds `n_fractals` 52-byte Fractals of which at most
  * one is enabled, a Perlin fBm without warp; `crater_kernel` is one CraterShapeKernel for every
- * tile; crater_footprints (optional) holds 3 doubles per record as tg_crater_batch writes them. */
+ * tile; crater_footprints (optional) holds 3 doubles per record as tg_crater_batch writes them.
+ * Tiles and point sets may name the same records and boulders. */
 typedef struct tg_batch_input {
     const tg_tile* tiles;
     uint32_t n_tiles;
@@ -355,6 +373,10 @@ typedef struct tg_batch_input {
     const double* crater_footprints;
     const tg_boulder* boulders;
     uint32_t n_boulders;
+    const tg_point_set* point_sets;
+    uint32_t n_point_sets;
+    const double* points;
+    uint32_t n_points;
 } tg_batch_input;
 
 /* What the batch last did. */

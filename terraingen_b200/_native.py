@@ -107,11 +107,19 @@ class Tile(C.Structure):
                 ("boulder_begin", _U32), ("boulder_count", _U32), ("boulder_width", _D)]
 
 
+class PointSet(C.Structure):
+    _fields_ = [("point_begin", _U32), ("point_count", _U32), ("height_offset", C.c_uint64),
+                ("crater_begin", _U32), ("crater_count", _U32), ("data_begin", _U32),
+                ("boulder_begin", _U32), ("boulder_count", _U32), ("reserved", _U32),
+                ("boulder_width", _D)]
+
+
 class BatchInput(C.Structure):
     _fields_ = [("tiles", _P), ("n_tiles", _U32), ("fractals", _P), ("n_fractals", _U32),
                 ("elevation", _F), ("crater_kernel", _P), ("crater_records", _P),
                 ("n_craters", _U32), ("crater_data", _P), ("n_crater_data", _U32),
-                ("crater_footprints", _P), ("boulders", _P), ("n_boulders", _U32)]
+                ("crater_footprints", _P), ("boulders", _P), ("n_boulders", _U32),
+                ("point_sets", _P), ("n_point_sets", _U32), ("points", _P), ("n_points", _U32)]
 
 
 class BatchStats(C.Structure):

@@ -23,6 +23,11 @@ TILE = np.dtype([("width", "<u4"), ("height", "<u4"), ("origin_x", "<f8"), ("pix
                  ("crater_begin", "<u4"), ("crater_count", "<u4"), ("data_begin", "<u4"),
                  ("boulder_begin", "<u4"), ("boulder_count", "<u4"), ("boulder_width", "<f8")])
 assert TILE.itemsize == C.sizeof(N.Tile)
+POINT_SET = np.dtype([("point_begin", "<u4"), ("point_count", "<u4"), ("height_offset", "<u8"),
+                      ("crater_begin", "<u4"), ("crater_count", "<u4"), ("data_begin", "<u4"),
+                      ("boulder_begin", "<u4"), ("boulder_count", "<u4"), ("reserved", "<u4"),
+                      ("boulder_width", "<f8")])
+assert POINT_SET.itemsize == C.sizeof(N.PointSet)
 
 
 @dataclass
@@ -38,22 +43,34 @@ class TileSet:
     crater_footprints: np.ndarray      # float64 [3 * records]
     boulders: np.ndarray               # float64 [n, 5]
     grids: list = field(default_factory=list)  # GridSpec per tile
+    point_sets: np.ndarray = field(default_factory=lambda: np.zeros(0, POINT_SET))
+    points: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))  # float64 (x, y)
 
     @property
     def output_floats(self) -> int:
-        t = self.tiles
-        if len(t) == 0:
-            return 0
-        end = t["height_offset"] + (t["height"].astype(np.int64) - 1) * t["pitch"] + t["width"]
-        return int(end.max())
+        t, p = self.tiles, self.point_sets
+        ends = [0]
+        if len(t):
+            ends.append(int((t["height_offset"] + (t["height"].astype(np.int64) - 1) * t["pitch"]
+                             + t["width"]).max()))
+        if len(p):
+            ends.append(int((p["height_offset"] + p["point_count"]).max()))
+        return max(ends)
 
     @property
     def cells(self) -> int:
-        return int((self.tiles["width"].astype(np.int64) * self.tiles["height"]).sum())
+        return int((self.tiles["width"].astype(np.int64) * self.tiles["height"]).sum() +
+                   self.point_sets["point_count"].astype(np.int64).sum())
 
     def input_bytes(self) -> int:
         return (self.tiles.nbytes + self.crater_records.nbytes + self.crater_data.nbytes +
-                self.crater_footprints.nbytes + self.boulders.nbytes)
+                self.crater_footprints.nbytes + self.boulders.nbytes + self.point_sets.nbytes +
+                self.points.nbytes)
+
+    def point_view(self, out: np.ndarray, i: int) -> np.ndarray:
+        """Point set i's heights."""
+        p = self.point_sets[i]
+        return out[int(p["height_offset"]):int(p["height_offset"]) + int(p["point_count"])]
 
     def tile_view(self, out: np.ndarray, i: int) -> np.ndarray:
         """Tile i's heights as a (height, width) view of the output array."""
@@ -66,8 +83,11 @@ class TileSet:
     def native(self) -> N.BatchInput:
         self._keep = [np.ascontiguousarray(a) for a in (
             self.tiles, self.fractals, self.crater_kernel, self.crater_records, self.crater_data,
-            self.crater_footprints, self.boulders)]
-        tiles, fractals, kernel, records, data, footprints, boulders = self._keep
+            self.crater_footprints, self.boulders, self.point_sets,
+            np.asarray(self.points, np.float64).reshape(-1, 2))]
+        tiles, fractals, kernel, records, data, footprints, boulders, sets, points = self._keep
+        if sets.dtype != POINT_SET:
+            raise TypeError("point sets must use the POINT_SET layout")
         if records.dtype != CRATER_RECORD or kernel.dtype != CRATER_SHAPE_KERNEL:
             raise TypeError("crater records and kernel must use the std430 layouts")
         if boulders.size and (boulders.dtype != np.float64 or boulders.shape[-1] != 5):
@@ -76,7 +96,9 @@ class TileSet:
             tiles.ctypes.data, len(tiles), fractals.ctypes.data, len(fractals),
             float(self.elevation), kernel.ctypes.data, records.ctypes.data, len(records),
             data.ctypes.data, len(data), footprints.ctypes.data if footprints.size else None,
-            boulders.ctypes.data if boulders.size else None, len(boulders))
+            boulders.ctypes.data if boulders.size else None, len(boulders),
+            sets.ctypes.data if len(sets) else None, len(sets),
+            points.ctypes.data if len(points) else None, len(points))
 
 
 def layout(grids: list[GridSpec], align: int = 4) -> tuple[np.ndarray, np.ndarray]:

@@ -63,79 +63,113 @@ __device__ __forceinline__ uint32_t corner_hash(uint32_t x, uint32_t y, uint32_t
 
 // --- binning -------------------------------------------------------------------------------
 
+// The ref holding pair `p` of a prefix numbering: the last ref whose first pair is at or before
+// p (refs with no pairs share their successor's first pair and are passed over).
+template <typename First>
+__device__ __forceinline__ uint32_t ref_of_pair(const BatchRef* refs, uint32_t n, uint32_t p,
+                                                First first) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (first(refs[mid]) <= p) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool is_points(const BatchTile& t) {
+    return t.pointBase != kNone;
+}
+
+// One warp per (ref, record) pair: grid tiles count the bins of the reference tiles the
+// footprint window touches (as the plain path), point sets the blocks whose bounding box the
+// footprint disk meets.
 __global__ void batch_crater_count_kernel(const CraterShapeKernel k, const BatchView v,
                                           uint32_t tpbX, uint32_t tpbY) {
-    const uint32_t n = v.header->records;
+    const uint32_t n = v.header->refRecords, nrefs = v.header->refs;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n; p += warps) {
+        const BatchRef ref =
+            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
+        const uint32_t i = ref.recordBegin + (p - ref.recordPairs);
+        const BatchTile& t = v.tiles[ref.tile];
+        const float* data = v.data + ref.dataBase;
         int4 box = make_int4(1, 0, 1, 0);
-        uint32_t tile = kNone;
         if (lane == 0) {
-            tile = v.recordTile[i];
-            if (tile != kNone) {
-                const BatchTile& t = v.tiles[tile];
-                const CraterRecord r = v.records[i];
-                const Footprint f =
-                    crater_footprint(k, r, v.data + t.dataBase, v.footprints, i, t.grid);
+            const CraterRecord r = v.records[i];
+            if (is_points(t)) {
+                const CraterReach c = crater_reach(k, r, data, v.footprints, i);
+                v.craterCulls[p] = c.cull;
+                box = make_int4(0, 0, 0, 0);  // non-empty: the blocks are tested below
+            } else {
+                const Footprint f = crater_footprint(k, r, data, v.footprints, i, t.grid);
                 box = f.tiles;
-                v.craterCulls[i] = f.cull;
-                if (box.x <= box.y) {
-                    if (r.hasDatum == 1u) {
-                        atomicOr(&v.header->flags, 1u);
-                    }
-                    if (crater_heavy(r)) {
-                        atomicOr(&v.header->flags, 8u);
-                    }
+                v.craterCulls[p] = f.cull;
+            }
+            if (box.x <= box.y) {
+                if (r.hasDatum == 1u) {
+                    atomicOr(&v.header->flags, 1u);
+                }
+                if (crater_heavy(r)) {
+                    atomicOr(&v.header->flags, 8u);
                 }
             }
-            v.craterBoxes[i] = box;
+            v.craterBoxes[p] = box;
         }
         box.x = __shfl_sync(0xffffffffu, box.x, 0);
         box.y = __shfl_sync(0xffffffffu, box.y, 0);
         box.z = __shfl_sync(0xffffffffu, box.z, 0);
         box.w = __shfl_sync(0xffffffffu, box.w, 0);
-        tile = __shfl_sync(0xffffffffu, tile, 0);
         if (box.x > box.y) {
             continue;
         }
-        const uint32_t binsX = v.tiles[tile].binsX, base = v.tiles[tile].binBase;
+        if (is_points(t)) {
+            const CraterReach c = crater_reach(k, v.records[i], data, v.footprints, i);
+            for (uint32_t b = lane; b < t.binsX; b += 32u) {
+                if (disk_meets_box(c.x, c.y, c.reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
+                    atomicAdd(v.craterCounts + t.binBase + b, 1u);
+                }
+            }
+            continue;
+        }
         const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
         const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
         const uint32_t wide = bx1 - bx0 + 1u;
         const uint32_t total = wide * (by1 - by0 + 1u);
-        for (uint32_t t = lane; t < total; t += 32u) {
-            atomicAdd(v.craterCounts + base + (by0 + t / wide) * binsX + bx0 + t % wide, 1u);
+        for (uint32_t q = lane; q < total; q += 32u) {
+            atomicAdd(v.craterCounts + t.binBase + (by0 + q / wide) * t.binsX + bx0 + q % wide, 1u);
         }
     }
 }
 
-__global__ void batch_crater_scatter_kernel(const BatchView v, uint32_t tpbX, uint32_t tpbY) {
-    const uint32_t n = v.header->records;
+__global__ void batch_crater_scatter_kernel(const CraterShapeKernel k, const BatchView v,
+                                            uint32_t tpbX, uint32_t tpbY) {
+    const uint32_t n = v.header->refRecords, nrefs = v.header->refs;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-        const int4 box = v.craterBoxes[i];
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n; p += warps) {
+        const int4 box = v.craterBoxes[p];
         if (box.x > box.y) {
             continue;
         }
-        const uint32_t tile = v.recordTile[i];
-        const uint32_t binsX = v.tiles[tile].binsX, base = v.tiles[tile].binBase;
-        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
-        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
-        const uint32_t wide = bx1 - bx0 + 1u;
-        const uint32_t total = wide * (by1 - by0 + 1u);
+        const BatchRef ref =
+            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
+        const uint32_t i = ref.recordBegin + (p - ref.recordPairs);
+        const BatchTile& t = v.tiles[ref.tile];
         const int4* src = reinterpret_cast<const int4*>(v.records + i);
         int4 tail;
         tail.x = int(uint32_t(box.x) | (uint32_t(box.y) << 16));
         tail.y = int(uint32_t(box.z) | (uint32_t(box.w) << 16));
-        tail.z = __float_as_int(v.craterCulls[i]);
-        tail.w = int(i);
-        for (uint32_t t = lane; t < total; t += 32u) {
-            const uint32_t b = base + (by0 + t / wide) * binsX + bx0 + t % wide;
+        tail.z = __float_as_int(v.craterCulls[p]);
+        tail.w = int(ref.dataBase);  // the shaping reads the record's data from here
+        auto put = [&](uint32_t b) {
             const uint32_t slot = v.craterCounts[b] + atomicAdd(v.craterCursor + b, 1u);
             if (slot >= v.craterCapacity) {
-                continue;  // counted in the header's entry total; the host re-plans
+                return;  // counted in the header's entry total; the host re-plans
             }
             int4* dst = reinterpret_cast<int4*>(v.craterEntries + slot);
 #pragma unroll
@@ -143,20 +177,36 @@ __global__ void batch_crater_scatter_kernel(const BatchView v, uint32_t tpbX, ui
                 dst[w] = __ldg(src + w);
             }
             dst[9] = tail;
+        };
+        if (is_points(t)) {
+            const CraterReach c =
+                crater_reach(k, v.records[i], v.data + ref.dataBase, v.footprints, i);
+            for (uint32_t b = lane; b < t.binsX; b += 32u) {
+                if (disk_meets_box(c.x, c.y, c.reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
+                    put(t.binBase + b);
+                }
+            }
+            continue;
+        }
+        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
+        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
+        const uint32_t wide = bx1 - bx0 + 1u;
+        const uint32_t total = wide * (by1 - by0 + 1u);
+        for (uint32_t q = lane; q < total; q += 32u) {
+            put(t.binBase + (by0 + q / wide) * t.binsX + bx0 + q % wide);
         }
     }
 }
 
-// The lean path's (amplitude cos phase, amplitude sin phase), at each tile's data offsets.
+// The lean path's (amplitude cos phase, amplitude sin phase) at each record's data offsets. A
+// record named by several refs is written with the same values by each.
 __global__ void batch_harmonics_kernel(const BatchView v) {
-    const uint32_t n = v.header->records;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t tile = v.recordTile[i];
-        if (tile == kNone) {
-            continue;
-        }
-        const uint32_t base = v.tiles[tile].dataBase;
-        const uint32_t offset = base + v.records[i].harmonicOffset;
+    const uint32_t n = v.header->refRecords, nrefs = v.header->refs;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const BatchRef ref =
+            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
+        const uint32_t i = ref.recordBegin + (p - ref.recordPairs);
+        const uint32_t offset = ref.dataBase + v.records[i].harmonicOffset;
         const uint32_t count = v.records[i].harmonicCount;
         for (uint32_t h = 0; h < count; ++h) {
             const float amplitude = __ldg(v.data + offset + 2u * h);
@@ -169,42 +219,60 @@ __global__ void batch_harmonics_kernel(const BatchView v) {
     }
 }
 
+// One thread per (ref, boulder) pair: the bins its box's pixel window covers (point sets: the
+// blocks its box meets).
 __global__ void batch_boulder_count_kernel(const BatchView v, uint32_t binW, uint32_t binH) {
-    const uint32_t n = v.header->boulders;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t tile = v.boulderTile[i];
+    const uint32_t n = v.header->refBoulders, nrefs = v.header->refs;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const BatchRef ref =
+            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.boulderPairs; })];
+        const uint32_t i = ref.boulderBegin + (p - ref.boulderPairs);
+        const BatchTile& t = v.tiles[ref.tile];
+        const BoulderRecord b = v.boulders[i];
+        // ReliefBox on a plane (boulder_relief.cpp:24): reach 0.5 (diameter + width).
+        const double reach = 0.5 * (b.diameter + t.boulderWidth);
         int4 w = make_int4(1, 0, 1, 0);
-        if (tile != kNone) {
-            const BatchTile& t = v.tiles[tile];
-            const BoulderRecord b = v.boulders[i];
-            // ReliefBox on a plane (boulder_relief.cpp:24): reach 0.5 (diameter + width).
-            const double reach = 0.5 * (b.diameter + t.boulderWidth);
-            int c0, c1, r0, r1;
-            window_of(t.grid, b.x - reach, b.y - reach, b.x + reach, b.y + reach, c0, c1, r0,
-                      r1);
-            if (c0 < c1 && r0 < r1 && b.weight > 0.0) {
-                w = make_int4(c0, c1, r0, r1);
-                const uint32_t bx0 = uint32_t(c0) / binW, bx1 = uint32_t(c1 - 1) / binW;
-                const uint32_t by0 = uint32_t(r0) / binH, by1 = uint32_t(r1 - 1) / binH;
-                for (uint32_t by = by0; by <= by1; ++by) {
-                    for (uint32_t bx = bx0; bx <= bx1; ++bx) {
-                        atomicAdd(v.boulderCounts + t.binBase + by * t.binsX + bx, 1u);
+        if (b.weight > 0.0) {
+            if (is_points(t)) {
+                w = make_int4(INT32_MIN, INT32_MAX, INT32_MIN, INT32_MAX);
+                for (uint32_t q = 0; q < t.binsX; ++q) {
+                    const double* box = v.pointBoxes + 4 * size_t(t.binBase + q);
+                    if (b.x + reach >= box[0] && b.x - reach <= box[2] && b.y + reach >= box[1] &&
+                        b.y - reach <= box[3]) {
+                        atomicAdd(v.boulderCounts + t.binBase + q, 1u);
+                    }
+                }
+            } else {
+                int c0, c1, r0, r1;
+                window_of(t.grid, b.x - reach, b.y - reach, b.x + reach, b.y + reach, c0, c1, r0,
+                          r1);
+                if (c0 < c1 && r0 < r1) {
+                    w = make_int4(c0, c1, r0, r1);
+                    const uint32_t bx0 = uint32_t(c0) / binW, bx1 = uint32_t(c1 - 1) / binW;
+                    const uint32_t by0 = uint32_t(r0) / binH, by1 = uint32_t(r1 - 1) / binH;
+                    for (uint32_t by = by0; by <= by1; ++by) {
+                        for (uint32_t bx = bx0; bx <= bx1; ++bx) {
+                            atomicAdd(v.boulderCounts + t.binBase + by * t.binsX + bx, 1u);
+                        }
                     }
                 }
             }
         }
-        v.boulderWindows[i] = w;
+        v.boulderWindows[p] = w;
     }
 }
 
 __global__ void batch_boulder_scatter_kernel(const BatchView v, uint32_t binW, uint32_t binH) {
-    const uint32_t n = v.header->boulders;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int4 w = v.boulderWindows[i];
+    const uint32_t n = v.header->refBoulders, nrefs = v.header->refs;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const int4 w = v.boulderWindows[p];
         if (w.x >= w.y) {
             continue;
         }
-        const BatchTile& t = v.tiles[v.boulderTile[i]];
+        const BatchRef ref =
+            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.boulderPairs; })];
+        const uint32_t i = ref.boulderBegin + (p - ref.boulderPairs);
+        const BatchTile& t = v.tiles[ref.tile];
         const BoulderRecord b = v.boulders[i];
         BoulderEntry e;
         e.x = b.x;
@@ -217,15 +285,28 @@ __global__ void batch_boulder_scatter_kernel(const BatchView v, uint32_t binW, u
         e.r0 = w.z;
         e.r1 = w.w;
         e.pad_ = 0.0;
+        auto put = [&](uint32_t bin) {
+            const uint32_t slot = v.boulderCounts[bin] + atomicAdd(v.boulderCursor + bin, 1u);
+            if (slot < v.boulderCapacity) {
+                v.boulderEntries[slot] = e;
+            }
+        };
+        if (is_points(t)) {
+            const double reach = 0.5 * (b.diameter + t.boulderWidth);
+            for (uint32_t q = 0; q < t.binsX; ++q) {
+                const double* box = v.pointBoxes + 4 * size_t(t.binBase + q);
+                if (b.x + reach >= box[0] && b.x - reach <= box[2] && b.y + reach >= box[1] &&
+                    b.y - reach <= box[3]) {
+                    put(t.binBase + q);
+                }
+            }
+            continue;
+        }
         const uint32_t bx0 = uint32_t(w.x) / binW, bx1 = uint32_t(w.y - 1) / binW;
         const uint32_t by0 = uint32_t(w.z) / binH, by1 = uint32_t(w.w - 1) / binH;
         for (uint32_t by = by0; by <= by1; ++by) {
             for (uint32_t bx = bx0; bx <= bx1; ++bx) {
-                const uint32_t bin = t.binBase + by * t.binsX + bx;
-                const uint32_t slot = v.boulderCounts[bin] + atomicAdd(v.boulderCursor + bin, 1u);
-                if (slot < v.boulderCapacity) {
-                    v.boulderEntries[slot] = e;
-                }
+                put(t.binBase + by * t.binsX + bx);
             }
         }
     }
@@ -252,10 +333,33 @@ __device__ __forceinline__ void issue_chunk(unsigned char (*stage)[kStageBytes],
     bulk_copy_g2s(&stage[s][0], src + size_t(c) * chunk * entryBytes, bytes, &bars[s]);
 }
 
+// Perlin noise at one lattice point split into cell (ix, iy) and fraction (fx, fy), its four
+// corner hashes given (PerlinNoise2, include/terraingen/noise/perlin.h:72-98).
+__device__ __forceinline__ float perlin_at(uint32_t h00, uint32_t h10, uint32_t h01, uint32_t h11,
+                                          float fx, float fy) {
+    const float n00 = noise::gradient2(h00, fx, fy);
+    const float n10 = noise::gradient2(h10, fx - 1.0f, fy);
+    const float n01 = noise::gradient2(h01, fx, fy - 1.0f);
+    const float n11 = noise::gradient2(h11, fx - 1.0f, fy - 1.0f);
+    const float u = fade_fma(fx), vv = fade_fma(fy);
+    return 1.41421356237309505f * lerp_fma(vv, lerp_fma(u, n00, n10), lerp_fma(u, n01, n11));
+}
+
+__device__ __forceinline__ void corners(int32_t ix, int32_t iy, uint32_t sz, uint32_t& h00,
+                                        uint32_t& h10, uint32_t& h01, uint32_t& h11) {
+    const uint32_t ax0 = uint32_t(ix) * kLcgA + kLcgC, ax1 = ax0 + kLcgA;
+    const uint32_t ay0 = uint32_t(iy) * kLcgA + kLcgC, ay1 = ay0 + kLcgA;
+    h00 = corner_hash(ax0, ay0, sz);
+    h10 = corner_hash(ax1, ay0, sz);
+    h01 = corner_hash(ax0, ay1, sz);
+    h11 = corner_hash(ax1, ay1, sz);
+}
+
 template <int kBinW, int kBinH, int kCells, bool kFast>
 __global__ void __launch_bounds__(kBinW* kBinH / kCells)
     batch_evaluate_kernel(const CraterShapeKernel k, const BatchNoise noise, const BatchView v) {
     constexpr uint32_t kRowThreads = kBinW / kCells;  // threads along one row of a bin
+    constexpr uint32_t kBinCellCount = kBinW * kBinH;  // cells of a bin, points of a point block
     static_assert(kBinW % kCells == 0 && kRefTileCells % kCells == 0, "cells per thread");
     static_assert(kBinW % kRefTileCells == 0 && kBinH % kRefTileCells == 0, "bins of 16-tiles");
 
@@ -303,60 +407,93 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
         }
         const BatchTile& t = v.tiles[sTile];
         const Grid grid = t.grid;
+        const bool points = t.pointBase != kNone;
         const uint32_t local = item - t.binBase;
-        const uint32_t binX = local % t.binsX, binY = local / t.binsX;
-        const uint32_t row = binY * kBinH + tid / kRowThreads;
-        const uint32_t col0 = binX * kBinW + (tid % kRowThreads) * kCells;
-        const bool rowIn = row < grid.height;
+        // Grid: this thread's kCells cells of one row. Point set: kCells consecutive points.
+        uint32_t row = 0, col0 = 0, first = 0;
         bool live[kCells];
+        if (points) {
+            first = local * kBinCellCount + tid * kCells;
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                live[j] = first + j < grid.width;
+            }
+        } else {
+            const uint32_t binX = local % t.binsX, binY = local / t.binsX;
+            row = binY * kBinH + tid / kRowThreads;
+            col0 = binX * kBinW + (tid % kRowThreads) * kCells;
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                live[j] = row < grid.height && col0 + j < grid.width;
+            }
+        }
+        // Cell centers (Raster::CellCenter) or points, in double.
+        double xd[kCells], yd[kCells];
 #pragma unroll
         for (int j = 0; j < kCells; ++j) {
-            live[j] = rowIn && col0 + j < grid.width;
+            if (points) {
+                const uint32_t i = live[j] ? first + j : 0u;
+                xd[j] = v.points[2 * (size_t(t.pointBase) + i)];
+                yd[j] = v.points[2 * (size_t(t.pointBase) + i) + 1];
+            } else {
+                xd[j] = grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
+                        (double(row) + 0.5) * grid.rowRotation;
+                yd[j] = grid.originY + (double(col0 + j) + 0.5) * grid.colRotation +
+                        (double(row) + 0.5) * grid.pixelHeight;
+            }
         }
 
-        // 1. The source: Fractal2's octaves (fractal.h:219-240) at lattice positions split per
-        //    tile in double; corner hashes reused while the lattice cell does not change.
+        // 1. The source: Fractal2's octaves (fractal.h:219-240). Grid cells take their lattice
+        //    position from the tile's per-octave anchor (split in double) plus float steps;
+        //    points split their own position in double. Corner hashes are reused while the
+        //    lattice cell does not change.
         float sum[kCells];
 #pragma unroll
         for (int j = 0; j < kCells; ++j) {
             sum[j] = 0.0f;
         }
-        const float fr = float(row);
         for (int o = 0; o < noise.octaves; ++o) {
-            const OctaveAnchor a = v.anchors[t.anchorBase + o];
-            // Each cell from its own column, so heights do not depend on the kernel shape.
-            const float px = fmaf(fr, a.ay, a.fx);
-            const float py = fmaf(fr, a.by, a.fy);
             const uint32_t sz = noise.seedTerm[o];
             const float w = noise.weight[o];
             int32_t cx = INT32_MIN, cy = INT32_MIN;
             uint32_t h00 = 0, h10 = 0, h01 = 0, h11 = 0;
+            if (points) {
+                const double tc = noise.tc[o], ts = noise.ts[o], f = noise.frequency[o];
 #pragma unroll
-            for (int j = 0; j < kCells; ++j) {
-                const float qx = fmaf(float(col0 + j), a.ax, px);
-                const float qy = fmaf(float(col0 + j), a.bx, py);
-                const float lx = floorf(qx), ly = floorf(qy);
-                const int32_t ix = int32_t(uint32_t(a.ix) + uint32_t(int32_t(lx)));
-                const int32_t iy = int32_t(uint32_t(a.iy) + uint32_t(int32_t(ly)));
-                const float fx = qx - lx, fy = qy - ly;
-                if (ix != cx || iy != cy) {
-                    cx = ix;
-                    cy = iy;
-                    const uint32_t ax0 = uint32_t(ix) * kLcgA + kLcgC, ax1 = ax0 + kLcgA;
-                    const uint32_t ay0 = uint32_t(iy) * kLcgA + kLcgC, ay1 = ay0 + kLcgA;
-                    h00 = corner_hash(ax0, ay0, sz);
-                    h10 = corner_hash(ax1, ay0, sz);
-                    h01 = corner_hash(ax0, ay1, sz);
-                    h11 = corner_hash(ax1, ay1, sz);
+                for (int j = 0; j < kCells; ++j) {
+                    const double px = fma(fma(xd[j], tc, -yd[j] * ts), f, noise.ox[o]);
+                    const double py = fma(fma(xd[j], ts, yd[j] * tc), f, noise.oy[o]);
+                    const double lx = floor(px), ly = floor(py);
+                    const int32_t ix = int32_t(uint32_t(uint64_t(int64_t(lx))));
+                    const int32_t iy = int32_t(uint32_t(uint64_t(int64_t(ly))));
+                    if (ix != cx || iy != cy) {
+                        cx = ix;
+                        cy = iy;
+                        corners(ix, iy, sz, h00, h10, h01, h11);
+                    }
+                    sum[j] = fmaf(w, perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)),
+                                  sum[j]);
                 }
-                const float n00 = noise::gradient2(h00, fx, fy);
-                const float n10 = noise::gradient2(h10, fx - 1.0f, fy);
-                const float n01 = noise::gradient2(h01, fx, fy - 1.0f);
-                const float n11 = noise::gradient2(h11, fx - 1.0f, fy - 1.0f);
-                const float u = fade_fma(fx), vv = fade_fma(fy);
-                const float n = 1.41421356237309505f *
-                                lerp_fma(vv, lerp_fma(u, n00, n10), lerp_fma(u, n01, n11));
-                sum[j] = fmaf(w, n, sum[j]);
+            } else {
+                const OctaveAnchor a = v.anchors[t.anchorBase + o];
+                // Each cell from its own column, so heights do not depend on the kernel shape.
+                const float fr = float(row);
+                const float px = fmaf(fr, a.ay, a.fx);
+                const float py = fmaf(fr, a.by, a.fy);
+#pragma unroll
+                for (int j = 0; j < kCells; ++j) {
+                    const float qx = fmaf(float(col0 + j), a.ax, px);
+                    const float qy = fmaf(float(col0 + j), a.bx, py);
+                    const float lx = floorf(qx), ly = floorf(qy);
+                    const int32_t ix = int32_t(uint32_t(a.ix) + uint32_t(int32_t(lx)));
+                    const int32_t iy = int32_t(uint32_t(a.iy) + uint32_t(int32_t(ly)));
+                    if (ix != cx || iy != cy) {
+                        cx = ix;
+                        cy = iy;
+                        corners(ix, iy, sz, h00, h10, h01, h11);
+                    }
+                    sum[j] = fmaf(w, perlin_at(h00, h10, h01, h11, qx - lx, qy - ly), sum[j]);
+                }
             }
         }
         float h[kCells];
@@ -365,35 +502,33 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
             h[j] = fmaf(noise.amplitude, sum[j] / noise.total, noise.elevation);
         }
 
-        // 2. Craters.
+        // 2. Craters: each entry's data at its ref's base (the BinEntry's index field).
         const uint32_t cFirst = v.craterCounts[item];
-        const uint32_t cEndRaw = v.craterCounts[item + 1];
-        const uint32_t cEnd = min(cEndRaw, v.craterCapacity);
+        const uint32_t cEnd = min(v.craterCounts[item + 1], v.craterCapacity);
         const uint32_t cCount = cEnd > cFirst ? cEnd - cFirst : 0u;
         if (cCount > 0u) {
-            const float* data = v.data + t.dataBase;
-            const float* harmonics = v.harmonics + t.dataBase;
             // Split positions of the cell centers (MakeSplitPoint, crater_kernel.cpp:303).
-            float pxh[kCells], pxl[kCells];
+            float pxh[kCells], pxl[kCells], pyh[kCells], pyl[kCells];
             double acc[kCells];
-            const double yd =
-                grid.originY + 0.5 * grid.colRotation + (double(row) + 0.5) * grid.pixelHeight;
-            const float pyh = float(yd);
-            const float pyl = float(yd - double(pyh));
-#pragma unroll
-            for (int j = 0; j < kCells; ++j) {
-                const double xd = grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
-                                  0.5 * grid.rowRotation;
-                pxh[j] = float(xd);
-                pxl[j] = float(xd - double(pxh[j]));
-                acc[j] = double(h[j]);
-            }
-            const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
             bool anyLive = false;
 #pragma unroll
             for (int j = 0; j < kCells; ++j) {
+                // Grid rows take the row center at column 0 (the reference's strips carry one
+                // y per row); points their own y.
+                const double y = points ? yd[j]
+                                        : grid.originY + 0.5 * grid.colRotation +
+                                              (double(row) + 0.5) * grid.pixelHeight;
+                const double x = points ? xd[j]
+                                        : grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
+                                              0.5 * grid.rowRotation;
+                pxh[j] = float(x);
+                pxl[j] = float(x - double(pxh[j]));
+                pyh[j] = float(y);
+                pyl[j] = float(y - double(pyh[j]));
+                acc[j] = double(h[j]);
                 anyLive |= live[j];
             }
+            const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
             const unsigned char* src =
                 reinterpret_cast<const unsigned char*>(v.craterEntries + cFirst);
             const uint32_t chunks = (cCount + kCraterChunk - 1) / kCraterChunk;
@@ -424,37 +559,44 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                 for (uint32_t e = 0; e < n; ++e) {
                     const BinEntry& entry = entries[e];
                     const CraterRecord& r = entry.record;
-                    const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
-                                        tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
-                                        tileY <= int(entry.tileY1);
-                    const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
+                    // Grid cells: every cell of each reference tile the footprint touches.
+                    const bool inTile = anyLive &&
+                                        (points || (tileX >= int(entry.tileX0) &&
+                                                    tileX <= int(entry.tileX1) &&
+                                                    tileY >= int(entry.tileY0) &&
+                                                    tileY <= int(entry.tileY1)));
                     const float cull2 = entry.cull * entry.cull;
                     bool need[kCells];
-                    float dxs[kCells];
+                    float dxs[kCells], dys[kCells];
                     bool any = false;
 #pragma unroll
                     for (int j = 0; j < kCells; ++j) {
                         dxs[j] = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
-                        need[j] = inTile && live[j] && dxs[j] * dxs[j] + dy * dy < cull2;
+                        dys[j] = crater::split_difference(pyh[j], pyl[j], r.y, r.yLow);
+                        need[j] = inTile && live[j] &&
+                                  __fadd_rn(__fmul_rn(dxs[j], dxs[j]), __fmul_rn(dys[j], dys[j])) <
+                                      cull2;
                         any |= need[j];
                     }
                     if (!__any_sync(0xffffffffu, any)) {
                         continue;
                     }
+                    const float* data = v.data + entry.index;
+                    const float* harmonics = v.harmonics + entry.index;
 #pragma unroll
                     for (int j = 0; j < kCells; ++j) {
                         if (need[j]) {
                             ++craterPairs;
                             if (kFast) {
                                 bool reached;
-                                const float shaped =
-                                    crater::fast_contribution(fk, harmonics, r, dxs[j], dy, reached);
+                                const float shaped = crater::fast_contribution(
+                                    fk, harmonics, r, dxs[j], dys[j], reached);
                                 if (reached) {
                                     acc[j] += double(shaped);
                                 }
                             } else {
                                 const crater::Contribution q =
-                                    crater::crater_contribution(k, data, r, dxs[j], dy);
+                                    crater::crater_contribution(k, data, r, dxs[j], dys[j]);
                                 if (q.reached) {
                                     acc[j] += double(q.shaped);
                                 }
@@ -478,19 +620,14 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
 
         // 3. Boulders: max(height, base + weight * dome), base being the height after craters.
         const uint32_t bFirst = v.boulderCounts[item];
-        const uint32_t bEndRaw = v.boulderCounts[item + 1];
-        const uint32_t bEnd = min(bEndRaw, v.boulderCapacity);
+        const uint32_t bEnd = min(v.boulderCounts[item + 1], v.boulderCapacity);
         const uint32_t bCount = bEnd > bFirst ? bEnd - bFirst : 0u;
         if (bCount > 0u) {
             __syncthreads();  // the crater stage is no longer read
             const double width = t.boulderWidth;
-            const double cy = grid.originY + (double(col0) + 0.5) * grid.colRotation +
-                              (double(row) + 0.5) * grid.pixelHeight;
-            double cxs[kCells], best[kCells];
+            double best[kCells];
 #pragma unroll
             for (int j = 0; j < kCells; ++j) {
-                cxs[j] = grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
-                         (double(row) + 0.5) * grid.rowRotation;
                 best[j] = double(h[j]);
             }
             const unsigned char* src =
@@ -522,23 +659,28 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                 const uint32_t n = min(kBoulderChunk, bCount - c * kBoulderChunk);
                 for (uint32_t e = 0; e < n; ++e) {
                     const BoulderEntry& b = entries[e];
-                    const bool inRows = int(row) >= b.r0 && int(row) < b.r1;
+                    // Grid cells: the pixel window of the boulder's box (ForEachFeatureCell);
+                    // points: wherever the dome reaches.
+                    bool in[kCells];
                     bool any = false;
 #pragma unroll
                     for (int j = 0; j < kCells; ++j) {
-                        any |= live[j] && inRows && int(col0) + j >= b.c0 && int(col0) + j < b.c1;
+                        in[j] = live[j] &&
+                                (points || (int(row) >= b.r0 && int(row) < b.r1 &&
+                                            int(col0) + j >= b.c0 && int(col0) + j < b.c1));
+                        any |= in[j];
                     }
                     if (!__any_sync(0xffffffffu, any)) {
                         continue;
                     }
-                    const double dy = cy - b.y;
 #pragma unroll
                     for (int j = 0; j < kCells; ++j) {
-                        if (live[j] && inRows && int(col0) + j >= b.c0 && int(col0) + j < b.c1) {
+                        if (in[j]) {
                             ++boulderPairs;
-                            const double relief = fmax(dome(b, hypot(cxs[j] - b.x, dy), width), 0.0);
+                            const double relief =
+                                fmax(dome(b, hypot(xd[j] - b.x, yd[j] - b.y), width), 0.0);
                             if (relief > 0.0) {
-                                best[j] = fmax(best[j], double(h[j]) + b.weight * relief);
+                                best[j] = fmax(best[j], fma(b.weight, relief, double(h[j])));
                             }
                         }
                     }
@@ -557,14 +699,24 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
             }
         }
 
-        // 4. One write per cell.
-        if (rowIn) {
-            float* dst = heights + t.heightOffset + size_t(row) * t.pitch + col0;
-            bool all = true;
+        // 4. One write per cell; a point to its caller's index.
+        if (points) {
 #pragma unroll
             for (int j = 0; j < kCells; ++j) {
-                all &= live[j];
+                if (live[j]) {
+                    heights[t.heightOffset + v.pointIndex[t.pointBase + first + j]] = h[j];
+                }
             }
+            continue;
+        }
+        float* dst = heights + t.heightOffset + size_t(row) * t.pitch + col0;
+        bool all = true, none = true;
+#pragma unroll
+        for (int j = 0; j < kCells; ++j) {
+            all &= live[j];
+            none &= !live[j];
+        }
+        if (!none) {
             const uintptr_t address = reinterpret_cast<uintptr_t>(dst);
             if (kCells % 4 == 0 && all && (address & 15u) == 0u) {
 #pragma unroll
@@ -652,6 +804,7 @@ int batch_blocks_per_sm(int index, bool fast) {
 cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
                              const BatchVariant& variant, uint32_t maxRecords,
                              uint32_t maxBoulders, uint32_t* scanScratch, cudaStream_t stream) {
+    // maxRecords / maxBoulders: the (ref, record) and (ref, boulder) pairs the plan holds.
     const size_t words = size_t(v.capacityBins) + 1;
     cudaError_t err = cudaMemsetAsync(v.craterCounts, 0, words * sizeof(uint32_t), stream);
     if (err == cudaSuccess) {
@@ -690,7 +843,8 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
         return err;
     }
     if (maxRecords > 0) {
-        batch_crater_scatter_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(v, tpbX, tpbY);
+        batch_crater_scatter_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(k, v, tpbX,
+                                                                                  tpbY);
         if ((err = cudaGetLastError()) != cudaSuccess) {
             return err;
         }

@@ -1,6 +1,7 @@
-// The batched form's C ABI (tg_batch_* in include/tgb200.h): input checks, the per-tile lattice
-// anchors (double), the tiles' bin numbering and queue order, device buffers sized by capacity,
-// CUDA graph capture and replay, and the autotuner over kernel shapes.
+// The batched form's C ABI (tg_batch_* in include/tgb200.h) and engine (batch_internal.h):
+// input checks, the source's octave constants and per-tile lattice anchors (double), point sets
+// in Morton order, the bin numbering and queue order, device buffers sized by capacity, CUDA
+// graph capture and replay, and the autotuner over kernel shapes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -11,10 +12,12 @@
 
 #include "../../include/tgb200.h"
 #include "api_internal.h"
+#include "batch_internal.h"
 #include "kernels.h"
 
 using namespace tgb;
 using namespace tgb::api;
+using namespace tgb::batch;
 
 namespace {
 
@@ -39,22 +42,18 @@ void pcg3d(uint32_t v[3]) {  // include/terraingen/noise/hash.h:40
     v[2] += v[0] * v[1];
 }
 
-// The octaves of a Perlin fBm: what every cell shares (float, as Fractal2 accumulates them) and
-// what the per-tile anchors need in double.
-struct Octave {
-    double frequency, tc, ts, ox, oy;
-};
-
 enum BatchSlot {
     kSlotTiles,
+    kSlotRefs,
     kSlotAnchors,
+    kSlotPoints,
+    kSlotPointIndex,
+    kSlotPointBoxes,
     kSlotRecords,
-    kSlotRecordTile,
     kSlotFootprints,
     kSlotData,
     kSlotHarmonics,
     kSlotBoulders,
-    kSlotBoulderTile,
     kSlotCraterCounts,
     kSlotCraterCursor,
     kSlotCraterEntries,
@@ -67,7 +66,7 @@ enum BatchSlot {
     kSlotScanScratch,
     kSlotHeader,
     kSlotOutput,
-    kSlotBatchSlots
+    kBatchSlotCount
 };
 
 // What a captured graph depends on; a change means a new capture.
@@ -75,7 +74,7 @@ struct Signature {
     BatchView view;
     int variant;
     bool fast;
-    uint32_t ctas, maxRecords, maxBoulders;
+    uint32_t ctas, maxRecordPairs, maxBoulderPairs;
     CraterShapeKernel kernel;
     BatchNoise noise;
 };
@@ -87,24 +86,24 @@ struct tg_batch {
     cudaStream_t stream = nullptr;
     // Recorded before the binning graph, between it and the evaluation graph, and after.
     cudaEvent_t events[3] = {nullptr, nullptr, nullptr};
-    BatchHeader* pinned = nullptr;  // [0] written before each replay, [1] read back after
-    Buffer slots[kSlotBatchSlots];
+    BatchHeader* pinned = nullptr;  // [0] written before each launch, [1] read back after
+    Buffer slots[kBatchSlotCount];
     int variant = 0;
 
-    // The loaded batch.
     bool loaded = false;
-    std::vector<tg_tile> tiles;  // queue order
-    std::vector<OctaveAnchor> anchors;
-    BatchNoise noise{};
-    CraterShapeKernel kernel{};
-    bool fast = true;
-    uint32_t records = 0, boulders = 0, nData = 0;
-    bool footprints = false;
+    Spec spec;
+    std::vector<BatchTile> tiles;   // spec.items numbered for the current variant
+    uint32_t bins = 0;
+    uint32_t recordPairs = 0, boulderPairs = 0;
     size_t outputFloats = 0;
     uint64_t cells = 0;
-    uint32_t bins = 0;
 
-    // Graph state.
+    // The launch in flight.
+    bool pending = false;
+    float* out = nullptr;
+    cudaStream_t launchStream = nullptr;
+    Signature launched{};
+
     cudaGraph_t graph[2] = {nullptr, nullptr};  // binning, evaluation
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     Signature captured{};
@@ -126,65 +125,113 @@ uint32_t capacity(tg_batch* b, BatchSlot s) {
 }
 
 int effective_variant(const tg_batch* b) {
-    return b->fast ? b->variant : 0;
+    return b->spec.fast ? b->variant : 0;
 }
 
-// Numbers the loaded tiles' bins for the current kernel shape and uploads the tile table.
+template <typename T>
+int upload(tg_batch* b, BatchSlot slot, const T* src, size_t count) {
+    if (count == 0) {
+        return TG_OK;
+    }
+    TG_CUDA(b->slots[slot].reserve(count * sizeof(T)), "allocation");
+    TG_CUDA(cudaMemcpyAsync(b->slots[slot].ptr, src, count * sizeof(T), cudaMemcpyHostToDevice,
+                            b->stream),
+            "copy to device");
+    return TG_OK;
+}
+
+uint32_t capacity_bins(tg_batch* b) {
+    return std::min({capacity<uint32_t>(b, kSlotCraterCounts),
+                     capacity<uint32_t>(b, kSlotCraterCursor),
+                     capacity<uint32_t>(b, kSlotBoulderCounts),
+                     capacity<uint32_t>(b, kSlotBoulderCursor)}) - 1;
+}
+
+// Numbers the loaded items' bins for the current kernel shape, bounds each point block, and
+// uploads the tile table and the blocks' boxes.
 int plan_bins(tg_batch* b) {
     const BatchVariant v = batch_variant(effective_variant(b));
-    std::vector<BatchTile> out(b->tiles.size());
+    const uint32_t block = v.binW * v.binH;  // points per point-set block
+    const Spec& spec = b->spec;
+    std::vector<BatchTile> out(spec.items.size());
+    std::vector<double> boxes;
     uint64_t base = 0;
-    for (size_t i = 0; i < b->tiles.size(); ++i) {
-        const tg_tile& t = b->tiles[i];
+    const int stride = std::max(spec.noise.octaves, 1);
+    for (size_t i = 0; i < spec.items.size(); ++i) {
+        const Item& it = spec.items[i];
         BatchTile& d = out[i];
-        d.grid = Grid{t.grid.width,        t.grid.height,       t.grid.origin_x,
-                      t.grid.pixel_width,  t.grid.row_rotation, t.grid.origin_y,
-                      t.grid.col_rotation, t.grid.pixel_height};
-        d.heightOffset = t.height_offset;
-        d.pitch = t.pitch;
-        d.binsX = (t.grid.width + v.binW - 1) / v.binW;
-        d.binsY = (t.grid.height + v.binH - 1) / v.binH;
+        d.grid = it.grid;
+        d.heightOffset = it.heightOffset;
+        d.pitch = it.pitch;
         d.binBase = uint32_t(base);
-        d.dataBase = t.data_begin;
-        d.anchorBase = uint32_t(i) * uint32_t(std::max(b->noise.octaves, 1));
-        d.boulderWidth = t.boulder_width;
+        d.anchorBase = uint32_t(i) * uint32_t(stride);
+        d.boulderWidth = it.boulderWidth;
+        if (it.points) {
+            d.pointBase = it.pointBegin;
+            d.binsX = (it.grid.width + block - 1) / block;
+            d.binsY = 1;
+            // Boxes are indexed by bin: pad up to this item's first bin.
+            boxes.resize(size_t(base) * 4, 0.0);
+            for (uint32_t q = 0; q < d.binsX; ++q) {
+                double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+                const uint32_t end = std::min(it.grid.width, (q + 1) * block);
+                for (uint32_t p = q * block; p < end; ++p) {
+                    const double* xy = &spec.points[2 * (size_t(it.pointBegin) + p)];
+                    lo[0] = std::min(lo[0], xy[0]);
+                    lo[1] = std::min(lo[1], xy[1]);
+                    hi[0] = std::max(hi[0], xy[0]);
+                    hi[1] = std::max(hi[1], xy[1]);
+                }
+                boxes.insert(boxes.end(), {lo[0], lo[1], hi[0], hi[1]});
+            }
+        } else {
+            d.pointBase = kNone;
+            d.binsX = (it.grid.width + v.binW - 1) / v.binW;
+            d.binsY = (it.grid.height + v.binH - 1) / v.binH;
+        }
         base += uint64_t(d.binsX) * d.binsY;
     }
     if (base >= 0xffffffffull) {
         return fail(TG_ERROR_UNSUPPORTED, "a batch holds fewer than 2^32 bins");
     }
     b->bins = uint32_t(base);
+    b->tiles = out;
     const size_t words = size_t(b->bins) + 1;
     TG_CUDA(b->slots[kSlotCraterCounts].reserve(words * sizeof(uint32_t)), "allocation");
     TG_CUDA(b->slots[kSlotCraterCursor].reserve(words * sizeof(uint32_t)), "allocation");
     TG_CUDA(b->slots[kSlotBoulderCounts].reserve(words * sizeof(uint32_t)), "allocation");
     TG_CUDA(b->slots[kSlotBoulderCursor].reserve(words * sizeof(uint32_t)), "allocation");
-    const uint32_t capBins =
-        std::min(capacity<uint32_t>(b, kSlotCraterCounts), capacity<uint32_t>(b, kSlotBoulderCounts)) - 1;
-    TG_CUDA(b->slots[kSlotScanScratch].reserve(scan_scratch_words(capBins) * sizeof(uint32_t)),
+    TG_CUDA(b->slots[kSlotScanScratch].reserve(scan_scratch_words(capacity_bins(b)) *
+                                               sizeof(uint32_t)),
             "allocation");
-    if (!out.empty()) {
-        TG_CUDA(b->slots[kSlotTiles].reserve(out.size() * sizeof(BatchTile)), "allocation");
-        TG_CUDA(cudaMemcpyAsync(b->slots[kSlotTiles].ptr, out.data(), out.size() * sizeof(BatchTile),
-                                cudaMemcpyHostToDevice, b->stream),
-                "copy to device");
+    if (int s = upload(b, kSlotTiles, out.data(), out.size())) {
+        return s;
+    }
+    if (!boxes.empty()) {
+        boxes.resize(size_t(b->bins) * 4, 0.0);
+        if (int s = upload(b, kSlotPointBoxes, boxes.data(), boxes.size())) {
+            return s;
+        }
     }
     TG_CUDA(cudaStreamSynchronize(b->stream), "synchronize");
     return TG_OK;
 }
 
 BatchView make_view(tg_batch* b) {
+    const Features& f = b->spec.features;
     BatchView v{};
     v.header = ptr<BatchHeader>(b, kSlotHeader);
     v.tiles = ptr<BatchTile>(b, kSlotTiles);
+    v.refs = ptr<BatchRef>(b, kSlotRefs);
     v.anchors = ptr<OctaveAnchor>(b, kSlotAnchors);
-    v.records = ptr<CraterRecord>(b, kSlotRecords);
-    v.recordTile = ptr<uint32_t>(b, kSlotRecordTile);
-    v.footprints = b->footprints ? ptr<double>(b, kSlotFootprints) : nullptr;
-    v.data = ptr<float>(b, kSlotData);
-    v.harmonics = ptr<float>(b, kSlotHarmonics);
-    v.boulders = ptr<BoulderRecord>(b, kSlotBoulders);
-    v.boulderTile = ptr<uint32_t>(b, kSlotBoulderTile);
+    v.points = ptr<double>(b, kSlotPoints);
+    v.pointIndex = ptr<uint32_t>(b, kSlotPointIndex);
+    v.pointBoxes = ptr<double>(b, kSlotPointBoxes);
+    v.records = f.records;
+    v.footprints = f.footprints;
+    v.data = f.data;
+    v.harmonics = f.harmonics;
+    v.boulders = f.boulders;
     v.craterCounts = ptr<uint32_t>(b, kSlotCraterCounts);
     v.craterCursor = ptr<uint32_t>(b, kSlotCraterCursor);
     v.craterEntries = ptr<BinEntry>(b, kSlotCraterEntries);
@@ -196,25 +243,25 @@ BatchView make_view(tg_batch* b) {
     v.boulderEntries = ptr<BoulderEntry>(b, kSlotBoulderEntries);
     v.boulderCapacity = capacity<BoulderEntry>(b, kSlotBoulderEntries);
     v.boulderWindows = ptr<int4>(b, kSlotBoulderWindows);
-    v.capacityBins =
-        std::min(capacity<uint32_t>(b, kSlotCraterCounts), capacity<uint32_t>(b, kSlotBoulderCounts)) - 1;
+    v.capacityBins = capacity_bins(b);
     return v;
 }
 
 Signature signature(tg_batch* b) {
     Signature s;
     std::memset(&s, 0, sizeof(s));
-    s.view = make_view(b);
+    const BatchView view = make_view(b);
+    std::memcpy(&s.view, &view, sizeof(view));
     s.variant = effective_variant(b);
-    s.fast = b->fast;
+    s.fast = b->spec.fast;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev->ordinal);
-    s.ctas = uint32_t(sms * batch_blocks_per_sm(s.variant, b->fast));
-    s.maxRecords = std::min(capacity<CraterRecord>(b, kSlotRecords), capacity<uint32_t>(b, kSlotRecordTile));
-    s.maxBoulders =
-        std::min(capacity<BoulderRecord>(b, kSlotBoulders), capacity<uint32_t>(b, kSlotBoulderTile));
-    s.kernel = b->kernel;
-    s.noise = b->noise;
+    s.ctas = uint32_t(sms * batch_blocks_per_sm(s.variant, s.fast));
+    s.maxRecordPairs =
+        std::min(capacity<int4>(b, kSlotCraterBoxes), capacity<float>(b, kSlotCraterCulls));
+    s.maxBoulderPairs = capacity<int4>(b, kSlotBoulderWindows);
+    std::memcpy(&s.kernel, &b->spec.kernel, sizeof(s.kernel));
+    std::memcpy(&s.noise, &b->spec.noise, sizeof(s.noise));
     return s;
 }
 
@@ -257,8 +304,8 @@ int capture(tg_batch* b, const Signature& s) {
     cudaError_t err = cudaMemcpyAsync(s.view.header, &b->pinned[0], sizeof(BatchHeader),
                                       cudaMemcpyHostToDevice, b->stream);
     if (err == cudaSuccess) {
-        err = launch_batch_bin(s.kernel, s.view, batch_variant(s.variant), s.maxRecords,
-                               s.maxBoulders, ptr<uint32_t>(b, kSlotScanScratch), b->stream);
+        err = launch_batch_bin(s.kernel, s.view, batch_variant(s.variant), s.maxRecordPairs,
+                               s.maxBoulderPairs, ptr<uint32_t>(b, kSlotScanScratch), b->stream);
     }
     if (int st = finish_capture(b, 0, err)) {
         return st;
@@ -277,30 +324,252 @@ int capture(tg_batch* b, const Signature& s) {
     return TG_OK;
 }
 
-// One replay of the loaded batch into `out` on `stream`, growing the entry capacities (and
-// re-capturing) when the bins needed more than they held.
-int replay(tg_batch* b, float* out, cudaStream_t stream) {
-    for (int attempt = 0; attempt < 3; ++attempt) {
-        BatchHeader h{};
-        h.tiles = uint32_t(b->tiles.size());
-        h.records = b->records;
-        h.boulders = b->boulders;
-        h.bins = b->bins;
-        h.heights = out;
-        b->pinned[0] = h;
-        const Signature s = signature(b);
-        if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
-            if (int st = capture(b, s)) {
-                return st;
-            }
+int check_batch(tg_batch* b) {
+    if (b == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "batch is null");
+    }
+    return check_device(b->dev);
+}
+
+// The (x, y) of a point set scaled to 16-bit cells of its bounding box, bits interleaved.
+uint32_t morton(double x, double y, const double* lo, const double* scale) {
+    auto spread = [](uint32_t v) {
+        v &= 0xffffu;
+        v = (v | (v << 8)) & 0x00ff00ffu;
+        v = (v | (v << 4)) & 0x0f0f0f0fu;
+        v = (v | (v << 2)) & 0x33333333u;
+        v = (v | (v << 1)) & 0x55555555u;
+        return v;
+    };
+    const uint32_t qx = uint32_t(std::min(65535.0, std::max(0.0, (x - lo[0]) * scale[0])));
+    const uint32_t qy = uint32_t(std::min(65535.0, std::max(0.0, (y - lo[1]) * scale[1])));
+    return spread(qx) | (spread(qy) << 1);
+}
+
+}  // namespace
+
+namespace tgb {
+namespace batch {
+
+int make_noise(const void* fractals, uint32_t n, float elevation, BatchNoise& noise,
+               std::vector<Octave>& octaves) {
+    noise = BatchNoise{};
+    octaves.clear();
+    noise.elevation = elevation;
+    noise.total = 1.0f;
+    const Fractal* only = nullptr;
+    for (uint32_t i = 0; i < n; ++i) {
+        const Fractal* f = static_cast<const Fractal*>(fractals) + i;
+        if (!f->enabled) {
+            continue;
         }
-        TG_CUDA(cudaEventRecord(b->events[0], stream), "event record");
-        TG_CUDA(cudaGraphLaunch(b->exec[0], stream), "graph launch");
-        TG_CUDA(cudaEventRecord(b->events[1], stream), "event record");
-        TG_CUDA(cudaGraphLaunch(b->exec[1], stream), "graph launch");
-        TG_CUDA(cudaEventRecord(b->events[2], stream), "event record");
-        ++b->replays;
-        TG_CUDA(cudaStreamSynchronize(stream), "synchronize");
+        if (only != nullptr) {
+            return fail(TG_ERROR_UNSUPPORTED, "a batch's source is one fractal");
+        }
+        only = f;
+    }
+    if (only == nullptr) {
+        return TG_OK;
+    }
+    if (only->basis != kBasisPerlin || only->type != kTypeFbm || only->warpAmplitude > 0.0f) {
+        return fail(TG_ERROR_UNSUPPORTED, "a batch's source is a Perlin fBm without warp");
+    }
+    if (only->octaves < 1 || only->octaves > kBatchMaxOctaves || !(only->wavelength > 0.0f) ||
+        !(only->lacunarity > 1.0f) || !(only->gain > 0.0f)) {
+        return fail(TG_ERROR_ARGUMENT, "the fractal is invalid");
+    }
+    // Fractal2's octaves (fractal.h:219-240): weights in float as the reference accumulates
+    // them; frequency, turn and offsets in double for the lattice positions.
+    noise.octaves = only->octaves;
+    noise.amplitude = only->amplitude;
+    float weight = 1.0f, total = 0.0f;
+    double frequency = 1.0 / double(only->wavelength);
+    double tc = 1.0, ts = 0.0;
+    for (int o = 0; o < only->octaves; ++o) {
+        uint32_t h[3] = {only->seed, uint32_t(o), 0u};
+        pcg3d(h);
+        noise.seedTerm[o] = h[0] * kLcgA + kLcgC;
+        noise.weight[o] = weight;
+        total += weight;
+        weight *= only->gain;
+        Octave oc;
+        oc.frequency = frequency;
+        oc.tc = tc;
+        oc.ts = ts;
+        oc.ox = double(float(h[1] >> 8u) * 0x1p-24f);
+        oc.oy = double(float(h[2] >> 8u) * 0x1p-24f);
+        octaves.push_back(oc);
+        noise.tc[o] = tc;
+        noise.ts[o] = ts;
+        noise.frequency[o] = frequency;
+        noise.ox[o] = oc.ox;
+        noise.oy[o] = oc.oy;
+        frequency *= double(only->lacunarity);
+        const double c = double(kTurnCos), s = double(kTurnSin);
+        const double nc = tc * c - ts * s;
+        ts = ts * c + tc * s;
+        tc = nc;
+    }
+    noise.total = total;
+    return TG_OK;
+}
+
+void append_points(Spec& spec, const double* xy, uint32_t count) {
+    double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+    for (uint32_t i = 0; i < count; ++i) {
+        lo[0] = std::min(lo[0], xy[2 * i]);
+        lo[1] = std::min(lo[1], xy[2 * i + 1]);
+        hi[0] = std::max(hi[0], xy[2 * i]);
+        hi[1] = std::max(hi[1], xy[2 * i + 1]);
+    }
+    const double scale[2] = {hi[0] > lo[0] ? 65535.0 / (hi[0] - lo[0]) : 0.0,
+                             hi[1] > lo[1] ? 65535.0 / (hi[1] - lo[1]) : 0.0};
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    std::vector<uint32_t> key(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        key[i] = morton(xy[2 * i], xy[2 * i + 1], lo, scale);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t c) { return key[a] < key[c]; });
+    for (uint32_t i : order) {
+        spec.points.push_back(xy[2 * i]);
+        spec.points.push_back(xy[2 * i + 1]);
+        spec.pointIndex.push_back(i);
+    }
+}
+
+int load(tg_batch* b, Spec&& spec) {
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
+    b->loaded = false;
+    b->spec = std::move(spec);
+    Spec& s = b->spec;
+    // Refs numbered by pairs; the per-octave anchors of grid items (the lattice position of cell
+    // (0, 0) split in double, and the lattice steps of a column and a row: Fractal2's rotation and
+    // frequency applied to the grid's axes).
+    uint64_t rp = 0, bp = 0;
+    for (BatchRef& r : s.refs) {
+        r.recordPairs = uint32_t(rp);
+        r.boulderPairs = uint32_t(bp);
+        rp += r.recordCount;
+        bp += r.boulderCount;
+    }
+    if (rp >= 0xffffffffull || bp >= 0xffffffffull) {
+        return fail(TG_ERROR_UNSUPPORTED, "a batch holds fewer than 2^32 feature pairs");
+    }
+    b->recordPairs = uint32_t(rp);
+    b->boulderPairs = uint32_t(bp);
+    const int stride = std::max(s.noise.octaves, 1);
+    std::vector<OctaveAnchor> anchors(s.items.size() * size_t(stride));
+    size_t outputFloats = 0;
+    uint64_t cells = 0;
+    for (size_t q = 0; q < s.items.size(); ++q) {
+        const Item& it = s.items[q];
+        if (it.points) {
+            outputFloats = std::max<size_t>(outputFloats, size_t(it.heightOffset) + it.grid.width);
+            cells += it.grid.width;
+            continue;
+        }
+        const Grid& g = it.grid;
+        outputFloats = std::max(outputFloats, size_t(it.heightOffset) +
+                                                  size_t(g.height - 1) * it.pitch + g.width);
+        cells += uint64_t(g.width) * g.height;
+        const double x0 = g.originX + 0.5 * g.pixelWidth + 0.5 * g.rowRotation;
+        const double y0 = g.originY + 0.5 * g.colRotation + 0.5 * g.pixelHeight;
+        for (int o = 0; o < s.noise.octaves; ++o) {
+            const Octave& oc = s.octaves[size_t(o)];
+            const double px = (x0 * oc.tc - y0 * oc.ts) * oc.frequency + oc.ox;
+            const double py = (x0 * oc.ts + y0 * oc.tc) * oc.frequency + oc.oy;
+            const double fx = std::floor(px), fy = std::floor(py);
+            OctaveAnchor& a = anchors[q * size_t(stride) + size_t(o)];
+            a.ix = int32_t(uint32_t(uint64_t(int64_t(fx))));
+            a.iy = int32_t(uint32_t(uint64_t(int64_t(fy))));
+            a.fx = float(px - fx);
+            a.fy = float(py - fy);
+            a.ax = float(oc.frequency * (g.pixelWidth * oc.tc - g.colRotation * oc.ts));
+            a.ay = float(oc.frequency * (g.rowRotation * oc.tc - g.pixelHeight * oc.ts));
+            a.bx = float(oc.frequency * (g.pixelWidth * oc.ts + g.colRotation * oc.tc));
+            a.by = float(oc.frequency * (g.rowRotation * oc.ts + g.pixelHeight * oc.tc));
+        }
+    }
+    b->outputFloats = outputFloats;
+    b->cells = cells;
+    if (int st = upload(b, kSlotAnchors, anchors.data(), anchors.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotRefs, s.refs.data(), s.refs.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotPoints, s.points.data(), s.points.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotPointIndex, s.pointIndex.data(), s.pointIndex.size())) {
+        return st;
+    }
+    TG_CUDA(b->slots[kSlotCraterBoxes].reserve(std::max<size_t>(rp, 1) * sizeof(int4)),
+            "allocation");
+    TG_CUDA(b->slots[kSlotCraterCulls].reserve(std::max<size_t>(rp, 1) * sizeof(float)),
+            "allocation");
+    TG_CUDA(b->slots[kSlotBoulderWindows].reserve(std::max<size_t>(bp, 1) * sizeof(int4)),
+            "allocation");
+    // A first guess at the entries (a few bins per pair); a launch that needs more grows them.
+    TG_CUDA(b->slots[kSlotCraterEntries].reserve((size_t(rp) * 4 + 64) * sizeof(BinEntry)),
+            "allocation");
+    TG_CUDA(b->slots[kSlotBoulderEntries].reserve((size_t(bp) * 2 + 64) * sizeof(BoulderEntry)),
+            "allocation");
+    TG_CUDA(b->slots[kSlotHeader].reserve(sizeof(BatchHeader)), "allocation");
+    if (int st = plan_bins(b)) {
+        return st;
+    }
+    b->loaded = true;
+    b->last.cells = cells;
+    return TG_OK;
+}
+
+int launch(tg_batch* b, float* out, cudaStream_t stream) {
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
+    BatchHeader h{};
+    h.tiles = uint32_t(b->tiles.size());
+    h.refs = uint32_t(b->spec.refs.size());
+    h.bins = b->bins;
+    h.refRecords = b->recordPairs;
+    h.refBoulders = b->boulderPairs;
+    h.heights = out;
+    b->pinned[0] = h;
+    const Signature s = signature(b);
+    if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
+        if (int st = capture(b, s)) {
+            return st;
+        }
+    }
+    TG_CUDA(cudaEventRecord(b->events[0], stream), "event record");
+    TG_CUDA(cudaGraphLaunch(b->exec[0], stream), "graph launch");
+    TG_CUDA(cudaEventRecord(b->events[1], stream), "event record");
+    TG_CUDA(cudaGraphLaunch(b->exec[1], stream), "graph launch");
+    TG_CUDA(cudaEventRecord(b->events[2], stream), "event record");
+    ++b->replays;
+    b->pending = true;
+    b->out = out;
+    b->launchStream = stream;
+    b->launched = s;
+    return TG_OK;
+}
+
+bool done(tg_batch* b) {
+    return !b->pending || cudaEventQuery(b->events[2]) == cudaSuccess;
+}
+
+int finish(tg_batch* b) {
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        if (!b->pending) {
+            return TG_OK;
+        }
+        TG_CUDA(cudaEventSynchronize(b->events[2]), "synchronize");
+        b->pending = false;
         const BatchHeader r = b->pinned[1];
         if (r.flags & 2u) {
             return fail(TG_ERROR_TIMEOUT, "a bin's staged copy did not arrive");
@@ -308,52 +577,110 @@ int replay(tg_batch* b, float* out, cudaStream_t stream) {
         if (r.flags & 1u) {
             return fail(TG_ERROR_UNSUPPORTED, "crater datums are not supported in batches");
         }
-        if ((r.flags & 8u) && b->fast) {
+        if ((r.flags & 8u) && b->spec.fast) {
             return fail(TG_ERROR_STATE, "a record needs the general shaping path");
         }
-        const bool craterShort = r.craterEntries > s.view.craterCapacity;
-        const bool boulderShort = r.boulderEntries > s.view.boulderCapacity;
         b->last.crater_pairs = r.craterPairs;
         b->last.boulder_pairs = r.boulderPairs;
         b->last.crater_entries = r.craterEntries;
         b->last.boulder_entries = r.boulderEntries;
-        b->last.ctas = s.ctas;
+        b->last.ctas = b->launched.ctas;
         TG_CUDA(cudaEventElapsedTime(&b->last.bin_ms, b->events[0], b->events[1]), "elapsed");
         TG_CUDA(cudaEventElapsedTime(&b->last.evaluate_ms, b->events[1], b->events[2]), "elapsed");
         TG_CUDA(cudaEventElapsedTime(&b->last.graph_ms, b->events[0], b->events[2]), "elapsed");
+        const bool craterShort = r.craterEntries > b->launched.view.craterCapacity;
+        const bool boulderShort = r.boulderEntries > b->launched.view.boulderCapacity;
         if (!craterShort && !boulderShort) {
             return TG_OK;
         }
         if (craterShort) {
-            TG_CUDA(b->slots[kSlotCraterEntries].reserve(size_t(r.craterEntries) * sizeof(BinEntry)),
+            TG_CUDA(b->slots[kSlotCraterEntries].reserve(size_t(r.craterEntries) *
+                                                         sizeof(BinEntry)),
                     "allocation");
         }
         if (boulderShort) {
             TG_CUDA(b->slots[kSlotBoulderEntries].reserve(size_t(r.boulderEntries) *
-                                                      sizeof(BoulderEntry)),
+                                                          sizeof(BoulderEntry)),
                     "allocation");
+        }
+        if (int st = launch(b, b->out, b->launchStream)) {
+            return st;
         }
     }
     return fail(TG_ERROR_STATE, "batch entry capacities did not settle");
 }
 
-template <typename T>
-int upload(tg_batch* b, BatchSlot slot, const T* src, size_t count) {
-    if (count == 0) {
-        return TG_OK;
+size_t output_floats(const tg_batch* b) {
+    return b->outputFloats;
+}
+
+uint64_t cells(const tg_batch* b) {
+    return b->cells;
+}
+
+}  // namespace batch
+}  // namespace tgb
+
+namespace {
+
+int replay(tg_batch* b, float* out, cudaStream_t stream) {
+    if (int st = batch::launch(b, out, stream)) {
+        return st;
     }
-    TG_CUDA(b->slots[slot].reserve(count * sizeof(T)), "allocation");
-    TG_CUDA(cudaMemcpyAsync(b->slots[slot].ptr, src, count * sizeof(T), cudaMemcpyHostToDevice,
-                            b->stream),
-            "copy to device");
+    return batch::finish(b);
+}
+
+// A host input's features copied into the batch's own slots.
+int upload_features(tg_batch* b, const tg_batch_input* in, Features& f) {
+    if (int s = upload(b, kSlotRecords, static_cast<const CraterRecord*>(in->crater_records),
+                       in->n_craters)) {
+        return s;
+    }
+    if (in->crater_footprints != nullptr) {
+        if (int s = upload(b, kSlotFootprints, in->crater_footprints, size_t(in->n_craters) * 3)) {
+            return s;
+        }
+    }
+    if (int s = upload(b, kSlotData, in->crater_data, in->n_crater_data)) {
+        return s;
+    }
+    static_assert(sizeof(tg_boulder) == sizeof(BoulderRecord), "tg_boulder is a BoulderRecord");
+    if (int s = upload(b, kSlotBoulders, reinterpret_cast<const BoulderRecord*>(in->boulders),
+                       in->n_boulders)) {
+        return s;
+    }
+    TG_CUDA(b->slots[kSlotHarmonics].reserve(std::max<size_t>(in->n_crater_data, 1) *
+                                             sizeof(float)),
+            "allocation");
+    f.records = ptr<CraterRecord>(b, kSlotRecords);
+    f.footprints = in->crater_footprints != nullptr ? ptr<double>(b, kSlotFootprints) : nullptr;
+    f.data = ptr<float>(b, kSlotData);
+    f.harmonics = ptr<float>(b, kSlotHarmonics);
+    f.boulders = ptr<BoulderRecord>(b, kSlotBoulders);
     return TG_OK;
 }
 
-int check_batch(tg_batch* b) {
-    if (b == nullptr) {
-        return fail(TG_ERROR_ARGUMENT, "batch is null");
+// Checks a tile's or point set's feature ranges and the data its records read.
+int check_ranges(const tg_batch_input* in, uint32_t crater_begin, uint32_t crater_count,
+                 uint32_t data_begin, uint32_t boulder_begin, uint32_t boulder_count,
+                 double boulder_width, const char* what, uint32_t i) {
+    if (uint64_t(crater_begin) + crater_count > in->n_craters ||
+        uint64_t(boulder_begin) + boulder_count > in->n_boulders ||
+        data_begin > in->n_crater_data) {
+        return fail(TG_ERROR_ARGUMENT, "%s %u: ranges outside the batch's arrays", what, i);
     }
-    return check_device(b->dev);
+    if (!(boulder_width >= 0.0) || !std::isfinite(boulder_width)) {
+        return fail(TG_ERROR_ARGUMENT, "%s %u: boulder width must be finite, >= 0", what, i);
+    }
+    const CraterRecord* records = static_cast<const CraterRecord*>(in->crater_records);
+    const uint64_t room = in->n_crater_data - data_begin;
+    for (uint32_t r = crater_begin; r < crater_begin + crater_count; ++r) {
+        if (uint64_t(records[r].harmonicOffset) + 2ull * records[r].harmonicCount > room ||
+            uint64_t(records[r].tableOffset) + records[r].tableCount > room) {
+            return fail(TG_ERROR_ARGUMENT, "crater record %u: data outside the batch's", r);
+        }
+    }
+    return TG_OK;
 }
 
 }  // namespace
@@ -396,6 +723,9 @@ void tg_batch_destroy(tg_batch* b) {
     if (b->dev != nullptr) {
         cudaSetDevice(b->dev->ordinal);
     }
+    if (b->pending) {
+        cudaEventSynchronize(b->events[2]);
+    }
     if (b->stream != nullptr) {
         cudaStreamSynchronize(b->stream);
     }
@@ -424,73 +754,28 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
     if (in == nullptr) {
         return fail(TG_ERROR_ARGUMENT, "input is null");
     }
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
     b->loaded = false;
     if ((in->n_tiles > 0 && in->tiles == nullptr) ||
         (in->n_fractals > 0 && in->fractals == nullptr) ||
         (in->n_craters > 0 && (in->crater_records == nullptr || in->crater_kernel == nullptr)) ||
         (in->n_crater_data > 0 && in->crater_data == nullptr) ||
-        (in->n_boulders > 0 && in->boulders == nullptr)) {
+        (in->n_boulders > 0 && in->boulders == nullptr) ||
+        (in->n_point_sets > 0 && in->point_sets == nullptr) ||
+        (in->n_points > 0 && in->points == nullptr)) {
         return fail(TG_ERROR_ARGUMENT, "a batch input array is null");
     }
-
-    // The source: at most one enabled fractal, a Perlin fBm without warp (fractal.h:219-240).
-    BatchNoise noise{};
-    noise.elevation = in->elevation;
-    noise.total = 1.0f;
-    std::vector<Octave> octaves;
-    const Fractal* only = nullptr;
-    for (uint32_t i = 0; i < in->n_fractals; ++i) {
-        const Fractal* f = static_cast<const Fractal*>(in->fractals) + i;
-        if (!f->enabled) {
-            continue;
-        }
-        if (only != nullptr) {
-            return fail(TG_ERROR_UNSUPPORTED, "a batch's source is one fractal");
-        }
-        only = f;
+    Spec spec;
+    if (int s = make_noise(in->fractals, in->n_fractals, in->elevation, spec.noise,
+                           spec.octaves)) {
+        return s;
     }
-    if (only != nullptr) {
-        if (only->basis != kBasisPerlin || only->type != kTypeFbm ||
-            only->warpAmplitude > 0.0f) {
-            return fail(TG_ERROR_UNSUPPORTED, "a batch's source is a Perlin fBm without warp");
-        }
-        if (only->octaves < 1 || only->octaves > kBatchMaxOctaves || !(only->wavelength > 0.0f) ||
-            !(only->lacunarity > 1.0f) || !(only->gain > 0.0f)) {
-            return fail(TG_ERROR_ARGUMENT, "the fractal is invalid");
-        }
-        noise.octaves = only->octaves;
-        noise.amplitude = only->amplitude;
-        float weight = 1.0f, total = 0.0f;
-        double frequency = 1.0 / double(only->wavelength);
-        double tc = 1.0, ts = 0.0;
-        for (int o = 0; o < only->octaves; ++o) {
-            uint32_t h[3] = {only->seed, uint32_t(o), 0u};
-            pcg3d(h);
-            noise.seedTerm[o] = h[0] * kLcgA + kLcgC;
-            noise.weight[o] = weight;
-            total += weight;
-            weight *= only->gain;
-            Octave oc;
-            oc.frequency = frequency;
-            oc.tc = tc;
-            oc.ts = ts;
-            oc.ox = double(float(h[1] >> 8u) * 0x1p-24f);
-            oc.oy = double(float(h[2] >> 8u) * 0x1p-24f);
-            octaves.push_back(oc);
-            frequency *= double(only->lacunarity);
-            const double c = double(kTurnCos), s = double(kTurnSin);
-            const double nc = tc * c - ts * s;
-            ts = ts * c + tc * s;
-            tc = nc;
-        }
-        noise.total = total;
-    }
-
-    // Craters: one kernel for every tile; datums are refused, features beyond outlines take the
+    // Craters: one kernel for every item; datums are refused, features beyond outlines take the
     // general shaping path.
-    CraterShapeKernel kernel{};
     if (in->crater_kernel != nullptr) {
-        std::memcpy(&kernel, in->crater_kernel, sizeof(kernel));
+        std::memcpy(&spec.kernel, in->crater_kernel, sizeof(spec.kernel));
     }
     const CraterRecord* records = static_cast<const CraterRecord*>(in->crater_records);
     uint32_t heavy = 0;
@@ -504,13 +789,11 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
             heavy = 4u;
         }
     }
+    spec.fast = crater_fast_path(spec.kernel, heavy);
 
     // Tiles: checked, empty ones dropped, queued coarsest spacing first (their bins hold the
-    // most entries), then largest first.
+    // most entries), then largest first; point sets after them.
     std::vector<uint32_t> order;
-    size_t outputFloats = 0;
-    uint64_t cells = 0;
-    std::vector<uint32_t> recordTile(in->n_craters, kNone), boulderTile(in->n_boulders, kNone);
     for (uint32_t i = 0; i < in->n_tiles; ++i) {
         const tg_tile& t = in->tiles[i];
         Grid g;
@@ -520,23 +803,13 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
         if (t.pitch < t.grid.width) {
             return fail(TG_ERROR_ARGUMENT, "tile %u: pitch below its width", i);
         }
-        if (uint64_t(t.crater_begin) + t.crater_count > in->n_craters ||
-            uint64_t(t.boulder_begin) + t.boulder_count > in->n_boulders ||
-            t.data_begin > in->n_crater_data) {
-            return fail(TG_ERROR_ARGUMENT, "tile %u: ranges outside the batch's arrays", i);
+        if (int s = check_ranges(in, t.crater_begin, t.crater_count, t.data_begin,
+                                 t.boulder_begin, t.boulder_count, t.boulder_width, "tile", i)) {
+            return s;
         }
-        if (!(t.boulder_width >= 0.0) || !std::isfinite(t.boulder_width)) {
-            return fail(TG_ERROR_ARGUMENT, "tile %u: boulder width must be finite, >= 0", i);
+        if (uint64_t(t.grid.width) * t.grid.height > 0) {
+            order.push_back(i);
         }
-        const uint64_t n = uint64_t(t.grid.width) * t.grid.height;
-        if (n == 0) {
-            continue;
-        }
-        const size_t end = size_t(t.height_offset) + size_t(t.grid.height - 1) * t.pitch +
-                           t.grid.width;
-        outputFloats = std::max(outputFloats, end);
-        cells += n;
-        order.push_back(i);
     }
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) {
         const tg_grid& ga = in->tiles[a].grid;
@@ -548,115 +821,54 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
         }
         return uint64_t(ga.width) * ga.height > uint64_t(gc.width) * gc.height;
     });
-    const uint32_t available = in->n_crater_data;
-    for (uint32_t q = 0; q < order.size(); ++q) {
-        const tg_tile& t = in->tiles[order[q]];
-        for (uint32_t i = t.crater_begin; i < t.crater_begin + t.crater_count; ++i) {
-            if (recordTile[i] != kNone) {
-                return fail(TG_ERROR_ARGUMENT, "crater record %u belongs to two tiles", i);
-            }
-            const CraterRecord& r = records[i];
-            const uint64_t room = available - t.data_begin;
-            if (uint64_t(r.harmonicOffset) + 2ull * r.harmonicCount > room ||
-                uint64_t(r.tableOffset) + r.tableCount > room) {
-                return fail(TG_ERROR_ARGUMENT, "crater record %u: data outside the batch's", i);
-            }
-            recordTile[i] = q;
-        }
-        for (uint32_t i = t.boulder_begin; i < t.boulder_begin + t.boulder_count; ++i) {
-            if (boulderTile[i] != kNone) {
-                return fail(TG_ERROR_ARGUMENT, "boulder %u belongs to two tiles", i);
-            }
-            boulderTile[i] = q;
-        }
-    }
-
-    // Per tile and octave, the lattice position of cell (0, 0) split in double, and the lattice
-    // steps of a column and a row (the rotation and frequency of Fractal2 applied to the grid's
-    // axes).
-    const int stride = std::max(noise.octaves, 1);
-    std::vector<OctaveAnchor> anchors(order.size() * size_t(stride));
-    for (size_t q = 0; q < order.size(); ++q) {
-        const tg_grid& g = in->tiles[order[q]].grid;
-        const double x0 = g.origin_x + 0.5 * g.pixel_width + 0.5 * g.row_rotation;
-        const double y0 = g.origin_y + 0.5 * g.col_rotation + 0.5 * g.pixel_height;
-        for (int o = 0; o < noise.octaves; ++o) {
-            const Octave& oc = octaves[size_t(o)];
-            const double px = (x0 * oc.tc - y0 * oc.ts) * oc.frequency + oc.ox;
-            const double py = (x0 * oc.ts + y0 * oc.tc) * oc.frequency + oc.oy;
-            const double fx = std::floor(px), fy = std::floor(py);
-            OctaveAnchor& a = anchors[q * size_t(stride) + size_t(o)];
-            a.ix = int32_t(uint32_t(uint64_t(int64_t(fx))));
-            a.iy = int32_t(uint32_t(uint64_t(int64_t(fy))));
-            a.fx = float(px - fx);
-            a.fy = float(py - fy);
-            a.ax = float(oc.frequency * (g.pixel_width * oc.tc - g.col_rotation * oc.ts));
-            a.ay = float(oc.frequency * (g.row_rotation * oc.tc - g.pixel_height * oc.ts));
-            a.bx = float(oc.frequency * (g.pixel_width * oc.ts + g.col_rotation * oc.tc));
-            a.by = float(oc.frequency * (g.row_rotation * oc.ts + g.pixel_height * oc.tc));
-        }
-    }
-
-    // Device copies.
-    b->tiles.clear();
     for (uint32_t i : order) {
-        b->tiles.push_back(in->tiles[i]);
+        const tg_tile& t = in->tiles[i];
+        Item it{};
+        to_grid(&t.grid, it.grid);
+        it.heightOffset = t.height_offset;
+        it.pitch = t.pitch;
+        it.points = false;
+        it.pointBegin = kNone;
+        it.boulderWidth = t.boulder_width;
+        spec.refs.push_back(BatchRef{uint32_t(spec.items.size()), t.crater_begin, t.crater_count,
+                                     t.data_begin, t.boulder_begin, t.boulder_count, 0, 0});
+        spec.items.push_back(it);
     }
-    b->anchors = anchors;
-    b->noise = noise;
-    b->kernel = kernel;
-    b->fast = crater_fast_path(kernel, heavy);
-    b->records = in->n_craters;
-    b->boulders = in->n_boulders;
-    b->nData = in->n_crater_data;
-    b->footprints = in->crater_footprints != nullptr;
-    b->outputFloats = outputFloats;
-    b->cells = cells;
-    if (int s = upload(b, kSlotAnchors, anchors.data(), anchors.size())) {
-        return s;
-    }
-    if (int s = upload(b, kSlotRecords, records, in->n_craters)) {
-        return s;
-    }
-    if (int s = upload(b, kSlotRecordTile, recordTile.data(), recordTile.size())) {
-        return s;
-    }
-    if (b->footprints) {
-        if (int s = upload(b, kSlotFootprints, in->crater_footprints, size_t(in->n_craters) * 3)) {
+    for (uint32_t i = 0; i < in->n_point_sets; ++i) {
+        const tg_point_set& p = in->point_sets[i];
+        if (uint64_t(p.point_begin) + p.point_count > in->n_points) {
+            return fail(TG_ERROR_ARGUMENT, "point set %u: points outside the batch's", i);
+        }
+        if (int s = check_ranges(in, p.crater_begin, p.crater_count, p.data_begin,
+                                 p.boulder_begin, p.boulder_count, p.boulder_width, "point set",
+                                 i)) {
             return s;
         }
+        for (uint32_t q = p.point_begin; q < p.point_begin + p.point_count; ++q) {
+            if (!std::isfinite(in->points[2 * size_t(q)]) ||
+                !std::isfinite(in->points[2 * size_t(q) + 1])) {
+                return fail(TG_ERROR_ARGUMENT, "point set %u: a point is not finite", i);
+            }
+        }
+        if (p.point_count == 0) {
+            continue;
+        }
+        Item it{};
+        it.grid = Grid{p.point_count, 1, 0.0, 1.0, 0.0, 0.0, 0.0, -1.0};
+        it.heightOffset = p.height_offset;
+        it.pitch = p.point_count;
+        it.points = true;
+        it.pointBegin = uint32_t(spec.pointIndex.size());
+        it.boulderWidth = p.boulder_width;
+        append_points(spec, in->points + 2 * size_t(p.point_begin), p.point_count);
+        spec.refs.push_back(BatchRef{uint32_t(spec.items.size()), p.crater_begin, p.crater_count,
+                                     p.data_begin, p.boulder_begin, p.boulder_count, 0, 0});
+        spec.items.push_back(it);
     }
-    if (int s = upload(b, kSlotData, in->crater_data, in->n_crater_data)) {
+    if (int s = upload_features(b, in, spec.features)) {
         return s;
     }
-    static_assert(sizeof(tg_boulder) == sizeof(BoulderRecord), "tg_boulder is a BoulderRecord");
-    if (int s = upload(b, kSlotBoulders, reinterpret_cast<const BoulderRecord*>(in->boulders),
-                       in->n_boulders)) {
-        return s;
-    }
-    if (int s = upload(b, kSlotBoulderTile, boulderTile.data(), boulderTile.size())) {
-        return s;
-    }
-    TG_CUDA(b->slots[kSlotHarmonics].reserve(std::max<size_t>(in->n_crater_data, 1) * sizeof(float)),
-            "allocation");
-    TG_CUDA(b->slots[kSlotCraterBoxes].reserve(std::max<size_t>(in->n_craters, 1) * sizeof(int4)),
-            "allocation");
-    TG_CUDA(b->slots[kSlotCraterCulls].reserve(std::max<size_t>(in->n_craters, 1) * sizeof(float)),
-            "allocation");
-    TG_CUDA(b->slots[kSlotBoulderWindows].reserve(std::max<size_t>(in->n_boulders, 1) * sizeof(int4)),
-            "allocation");
-    // A first guess at the entries (a few bins per record); a replay that needs more grows them.
-    TG_CUDA(b->slots[kSlotCraterEntries].reserve((size_t(in->n_craters) * 4 + 64) * sizeof(BinEntry)),
-            "allocation");
-    TG_CUDA(b->slots[kSlotBoulderEntries].reserve((size_t(in->n_boulders) * 2 + 64) *
-                                              sizeof(BoulderEntry)),
-            "allocation");
-    if (int s = plan_bins(b)) {
-        return s;
-    }
-    b->loaded = true;
-    b->last.cells = cells;
-    return TG_OK;
+    return load(b, std::move(spec));
 }
 
 int tg_batch_evaluate(tg_batch* b, float* heights, size_t n_heights, int memory, void* stream) {
@@ -678,6 +890,9 @@ int tg_batch_evaluate(tg_batch* b, float* heights, size_t n_heights, int memory,
     float* out = heights;
     cudaStream_t s = b->stream;
     if (memory == TG_MEMORY_DEVICE) {
+        if (reinterpret_cast<uintptr_t>(heights) % sizeof(float) != 0) {
+            return fail(TG_ERROR_ARGUMENT, "heights must be 4-byte aligned");
+        }
         if (stream != nullptr) {
             s = static_cast<cudaStream_t>(stream);
         }
@@ -734,6 +949,9 @@ int tg_batch_set_variant(tg_batch* b, int index) {
     if (index < 0 || index >= batch_variant_count()) {
         return fail(TG_ERROR_ARGUMENT, "variant %d of %d", index, batch_variant_count());
     }
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
     b->variant = index;
     return b->loaded ? plan_bins(b) : TG_OK;
 }
@@ -758,7 +976,7 @@ int tg_batch_tune(tg_batch* b, int trials, float* ms) {
     float bestMs = INFINITY;
     for (int v = 0; v < count; ++v) {
         float median = NAN;
-        if (b->fast || v == 0) {
+        if (b->spec.fast || v == 0) {
             b->variant = v;
             if (int s = plan_bins(b)) {
                 return s;
@@ -799,7 +1017,7 @@ int tg_batch_stats_get(tg_batch* b, tg_batch_stats* stats) {
     s.bin_width = shape.binW;
     s.bin_height = shape.binH;
     s.cells_per_thread = shape.cellsPerThread;
-    s.fast = b->fast ? 1u : 0u;
+    s.fast = b->spec.fast ? 1u : 0u;
     s.bins = b->bins;
     s.cells = b->cells;
     s.captures = b->captures;

@@ -59,6 +59,45 @@ struct Footprint {
     float cull;
 };
 
+// A crater's center and footprint reach in meters: from `footprints` (x, y, reach per record)
+// when given, else from the record (center hi + lo, reach = outline stretch x reachRadii x
+// radius); and its cull distance (see Footprint).
+struct CraterReach {
+    double x, y, reach;
+    float cull;
+};
+
+__device__ inline CraterReach crater_reach(const CraterShapeKernel& k, const CraterRecord& r,
+                                           const float* data, const double* footprints,
+                                           uint32_t i) {
+    CraterReach c;
+    const double scale = max_outline_scale(r, data);
+    if (footprints != nullptr) {
+        c.x = footprints[3 * size_t(i)];
+        c.y = footprints[3 * size_t(i) + 1];
+        c.reach = footprints[3 * size_t(i) + 2];
+    } else {
+        c.x = double(r.x) + double(r.xLow);
+        c.y = double(r.y) + double(r.yLow);
+        c.reach = scale * double(k.reachRadii) * (0.5 * double(r.diameter));
+    }
+    const bool stretched = r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
+                           r.shiftY != 0.0f;
+    // A little slack over the bound: the profile distance is rounded in float.
+    c.cull = stretched ? INFINITY
+                       : float(scale * double(k.reachRadii) * (0.5 * double(r.diameter)) *
+                               (1.0 + 1e-5)) + 1e-6f;
+    return c;
+}
+
+// Whether a disk of `radius` around (x, y) meets the box (x0, y0, x1, y1).
+__device__ __forceinline__ bool disk_meets_box(double x, double y, double radius,
+                                               const double* box) {
+    const double dx = fmax(fmax(box[0] - x, x - box[2]), 0.0);
+    const double dy = fmax(fmax(box[1] - y, y - box[3]), 0.0);
+    return dx * dx + dy * dy <= radius * radius;
+}
+
 __device__ inline Footprint crater_footprint(const CraterShapeKernel& k, const CraterRecord& r,
                                              const float* data, const double* footprints,
                                              uint32_t i, const Grid& g) {

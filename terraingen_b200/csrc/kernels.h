@@ -164,25 +164,41 @@ cudaError_t launch_ds_read(const DsLevel& nodes, const DsFrame& frame, const Gri
 cudaError_t launch_philox_probe(const uint32_t* in, uint32_t n, uint32_t* out, double* normals,
                                 cudaStream_t stream);
 
-// --- batched tiles (batch.cu) ------------------------------------------------------------
-// Many tiles evaluated together: source fBm, craters and boulders of every tile in one
-// persistent launch over all the tiles' bins, after one count / scan / scatter per feature kind.
+// --- batched tiles and point sets (batch.cu) ----------------------------------------------
+// Many tiles and point sets evaluated together: source fBm, craters and boulders of every item in
+// one persistent launch over all the items' bins, after one count / scan / scatter per feature
+// kind.
 
 constexpr int kBatchMaxOctaves = 32;
 
-// One tile of a batch. Its bins are numbered binBase .. binBase + binsX * binsY - 1 in the
-// batch's bin order, which is the work queue's order.
+// One tile (a grid) or one point set of a batch. Its bins are numbered binBase .. binBase +
+// binsX * binsY - 1 in the batch's bin order, which is the work queue's order. A point set's
+// "bins" are blocks of consecutive points (binsY = 1), its points at points[pointBase ..] and its
+// heights at heightOffset + i; grid.width holds its point count.
 struct BatchTile {
     Grid grid;
-    uint64_t heightOffset;  // output index of cell (0, 0)
+    uint64_t heightOffset;  // output index of cell (0, 0) or of point 0
     uint32_t pitch;         // output floats from one row to the next
     uint32_t binsX, binsY;
     uint32_t binBase;
-    uint32_t dataBase;      // added to the tile's record data offsets
     uint32_t anchorBase;    // the tile's first OctaveAnchor
+    uint32_t pointBase;     // point sets: first point; ~0u for a grid
     double boulderWidth;    // dome band width (the tile's sample spacing)
 };
 static_assert(sizeof(BatchTile) == 96, "BatchTile layout");
+
+// A run of crater records and boulders one tile (or point set) takes: records [recordBegin,
+// recordBegin + recordCount) with data offsets relative to data + dataBase, boulders [boulderBegin,
+// boulderBegin + boulderCount). Several refs may name the same records (regions shared by tiles).
+// recordPairs / boulderPairs are the refs' exclusive prefix sums of the counts: the batch's
+// (ref, record) pairs are numbered by them.
+struct BatchRef {
+    uint32_t tile;
+    uint32_t recordBegin, recordCount, dataBase;
+    uint32_t boulderBegin, boulderCount;
+    uint32_t recordPairs, boulderPairs;
+};
+static_assert(sizeof(BatchRef) == 32, "BatchRef layout");
 
 // The lattice position of a tile's cell (0, 0) for one octave, split in double into an integer
 // cell (ix, iy) and a float fraction (fx, fy), and the lattice steps of one column (ax, bx) and
@@ -194,53 +210,58 @@ struct OctaveAnchor {
 };
 static_assert(sizeof(OctaveAnchor) == 32, "OctaveAnchor layout");
 
-// The batch's source: elevation + amplitude * (sum of weight * Perlin octave) / total.
+// The batch's source: elevation + amplitude * (sum of weight * Perlin octave) / total. Points take
+// each octave's lattice position in double from the rotation (tc, ts), frequency and offsets.
 struct BatchNoise {
     int32_t octaves;
     float amplitude, total, elevation;
     uint32_t seedTerm[kBatchMaxOctaves];  // octave seed through pcg3d's first LCG step
     float weight[kBatchMaxOctaves];
+    double tc[kBatchMaxOctaves], ts[kBatchMaxOctaves], frequency[kBatchMaxOctaves];
+    double ox[kBatchMaxOctaves], oy[kBatchMaxOctaves];
 };
 
 // Per-run values the launches read from device memory, so one captured graph serves any batch
 // within the plan's capacities.
 struct BatchHeader {
-    uint32_t tiles, records, boulders, bins;
+    uint32_t tiles, refs, bins, pad_;
+    uint32_t refRecords, refBoulders;    // (ref, record) and (ref, boulder) pairs in all
     float* heights;
     uint32_t next;     // work-queue cursor
-    uint32_t flags;    // 1 datum seen, 2 staged copy timed out, 4 entries over capacity,
-                       // 8 a record needs the general shaping path
-    unsigned long long craterPairs, boulderPairs;
-    uint32_t craterEntries, boulderEntries;  // entries the bins needed
+    uint32_t flags;    // 1 datum seen, 2 staged copy timed out, 8 a record needs the general path
+    unsigned long long craterPairs, boulderPairs;  // (cell, feature) pairs evaluated
+    uint32_t craterEntries, boulderEntries;         // entries the bins needed
 };
 
 struct BatchView {
     BatchHeader* header;
     const BatchTile* tiles;
+    const BatchRef* refs;
     const OctaveAnchor* anchors;
+    const double* points;          // (x, y) per point of every point set, blocks spatially sorted
+    const uint32_t* pointIndex;    // the caller's index of each point within its set
+    const double* pointBoxes;      // (min x, min y, max x, max y) per point-set bin
     const CraterRecord* records;
-    const uint32_t* recordTile;    // tile of each record, ~0u for none
     const double* footprints;      // optional (x, y, reach) per record
     const float* data;
-    float* harmonics;
+    float* harmonics;              // mirrors data
     const BoulderRecord* boulders;
-    const uint32_t* boulderTile;
     uint32_t* craterCounts;        // [capacityBins + 1]
     uint32_t* craterCursor;        // [capacityBins]
     BinEntry* craterEntries;
     uint32_t craterCapacity;
-    int4* craterBoxes;             // [records]
-    float* craterCulls;            // [records]
+    int4* craterBoxes;             // [record pairs]
+    float* craterCulls;            // [record pairs]
     uint32_t* boulderCounts;
     uint32_t* boulderCursor;
     BoulderEntry* boulderEntries;
     uint32_t boulderCapacity;
-    int4* boulderWindows;          // [boulders]
+    int4* boulderWindows;          // [boulder pairs]
     uint32_t capacityBins;
 };
 
-// A kernel shape of the persistent evaluation: bins of binW x binH cells, cellsPerThread
-// adjacent cells of one row per thread.
+// A kernel shape of the persistent evaluation: bins of binW x binH cells (point sets: blocks of
+// binW x binH points), cellsPerThread adjacent cells of one row per thread.
 struct BatchVariant {
     uint32_t binW, binH, cellsPerThread;
 };
@@ -250,11 +271,12 @@ BatchVariant batch_variant(int index);
 // Persistent CTAs of `index` that fit on one SM (occupancy), for sizing the launch.
 int batch_blocks_per_sm(int index, bool fast);
 
-// Counting and scattering of the batch's craters and boulders into its bins, for `variant`'s
-// bin size (launches sized for `maxRecords` / `maxBoulders`, counts read from the header).
+// Counting and scattering of the batch's (ref, record) and (ref, boulder) pairs into its bins,
+// for `variant`'s bin size (launches sized for `maxRecordPairs` / `maxBoulderPairs`, counts read
+// from the header).
 cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
-                             const BatchVariant& variant, uint32_t maxRecords,
-                             uint32_t maxBoulders, uint32_t* scanScratch, cudaStream_t stream);
+                             const BatchVariant& variant, uint32_t maxRecordPairs,
+                             uint32_t maxBoulderPairs, uint32_t* scanScratch, cudaStream_t stream);
 // The persistent evaluation over every bin of the batch, `ctas` CTAs.
 cudaError_t launch_batch_evaluate(const CraterShapeKernel& k, const BatchNoise& noise,
                                   const BatchView& v, int variant, bool fast, uint32_t ctas,

@@ -156,11 +156,9 @@ def test_batch_refuses_what_it_cannot_do(device, batch, tiles):
     rec["hasDatum"][0] = 1
     with pytest.raises(TgError):
         batch.load(replace(tiles, crater_records=rec))
-    # A record claimed by two tiles.
+    # Features outside the batch's arrays.
     t = tiles.tiles.copy()
-    t["crater_begin"][1] = t["crater_begin"][0]
-    t["crater_count"][1] = max(1, int(t["crater_count"][0]))
-    t["crater_count"][0] = max(1, int(t["crater_count"][0]))
+    t["crater_count"][1] = len(tiles.crater_records) + 1
     with pytest.raises(TgError):
         batch.load(replace(tiles, tiles=t))
     # An output too small.
@@ -195,3 +193,81 @@ def test_batch_odd_data_offsets(batch, tiles):
     odd = np.zeros(tiles.output_floats, np.float32)
     batch.run(shifted, odd)
     assert np.array_equal(odd.view(np.uint32), even.view(np.uint32))
+
+
+def _with_points(ts, picks, per_tile, seed=0):
+    """`ts` plus one point set per picked tile: `per_tile` of the tile's cell centers, naming the
+    tile's own craters and boulders (the same records as the tile)."""
+    from dataclasses import replace
+
+    from terraingen_b200.batch import POINT_SET
+
+    rng = np.random.default_rng(seed)
+    sets = np.zeros(len(picks), POINT_SET)
+    points, cells = [], []
+    base = ts.output_floats
+    for k, i in enumerate(picks):
+        g, t = ts.grids[i], ts.tiles[i]
+        n = min(per_tile, g.cells)
+        flat = rng.choice(g.cells, n, replace=False)
+        r, c = flat // g.width, flat % g.width
+        points.append(np.stack([g.x0 + (c + 0.5) * g.pixel, g.y0 - (r + 0.5) * g.pixel], axis=1))
+        cells.append((i, r, c))
+        sets[k]["point_begin"] = sum(len(p) for p in points[:-1])
+        sets[k]["point_count"] = n
+        sets[k]["height_offset"] = base
+        for name in ("crater_begin", "crater_count", "data_begin", "boulder_begin",
+                     "boulder_count", "boulder_width"):
+            sets[k][name] = t[name]
+        base += n
+    return replace(ts, point_sets=sets, points=np.concatenate(points)), cells
+
+
+def test_batch_point_sets_match_tiles(batch, tiles):
+    # Points at cell centers of three tiles (one far out), sharing the tiles' records: heights
+    # within 1e-4 m of the tiles' cells.
+    far = max(range(len(tiles.grids)), key=lambda i: abs(tiles.grids[i].x0) + abs(tiles.grids[i].y0))
+    ts, cells = _with_points(tiles, [0, 3, far], 2000)
+    out = np.zeros(ts.output_floats, np.float32)
+    batch.run(ts, out)
+    assert batch.stats()["crater_pairs"] > 0
+    for k, (i, r, c) in enumerate(cells):
+        got = ts.point_view(out, k).astype(np.float64)
+        want = ts.tile_view(out, i)[r, c].astype(np.float64)
+        assert np.abs(got - want).max() <= 1e-4, (k, np.abs(got - want).max())
+
+
+def test_batch_points_source_matches_fp64_oracle(batch, tiles):
+    ts, _ = _with_points(_noise_only(tiles), [1, 2], 500, seed=4)
+    pts = ts.points.copy()
+    pts[:500] += 1.6e6  # far out, where float positions lose the lattice fraction
+    from dataclasses import replace
+
+    ts = replace(ts, points=pts)
+    out = np.zeros(ts.output_floats, np.float32)
+    batch.run(ts, out)
+    rs = H.restate()
+    f = ts.fractals[0]
+    for k in range(2):
+        p = ts.point_sets[k]
+        xy = ts.points[int(p["point_begin"]):int(p["point_begin"]) + int(p["point_count"])]
+        want = np.array([ts.elevation + rs.rs_fbm2_f64(x, y, int(f["seed"]), float(f["wavelength"]),
+                                                       float(f["amplitude"]), int(f["octaves"]),
+                                                       float(f["lacunarity"]), float(f["gain"]))
+                         for x, y in xy])
+        got = ts.point_view(out, k).astype(np.float64)
+        assert np.abs(got - want).max() <= 1e-4, (k, np.abs(got - want).max())
+
+
+def test_batch_shared_records(batch, tiles):
+    # Two tiles over the same grid naming the same records and boulders: the same heights.
+    from dataclasses import replace
+
+    t = np.concatenate([tiles.tiles, tiles.tiles[:1]])
+    t["height_offset"][-1] = tiles.output_floats
+    ts = replace(tiles, tiles=t, grids=tiles.grids + tiles.grids[:1])
+    out = np.zeros(ts.output_floats, np.float32)
+    batch.run(ts, out)
+    a = ts.tile_view(out, 0)
+    b = ts.tile_view(out, len(t) - 1)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

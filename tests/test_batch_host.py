@@ -19,7 +19,10 @@ def test_tile_layout_matches_the_header():
         if name == "grid":
             continue
         assert TILE.fields[name][1] == getattr(N.Tile, name).offset, name
-    assert C.sizeof(N.BatchInput) == 96
+    assert C.sizeof(N.BatchInput) == 128
+    from terraingen_b200.batch import POINT_SET
+
+    assert POINT_SET.itemsize == C.sizeof(N.PointSet) == 48
     assert C.sizeof(N.BatchStats) == 88
 
 
