@@ -424,6 +424,69 @@ int tg_batch_variant(int index, uint32_t* bin_width, uint32_t* bin_height,
                      uint32_t* cells_per_thread);
 int tg_batch_stats_get(tg_batch* batch, tg_batch_stats* stats);
 
+/* --- serving -----------------------------------------------------------------------------------
+ * A request server for the streaming-renderer use case: tile and point-query requests are
+ * submitted as they arrive and evaluated by continuous batching. Whenever one of the server's
+ * batch slots is free, the requests waiting then (up to max_batch_cells, and within the device
+ * memory budget) become one batch, launched on the slot's own stream while earlier batches may
+ * still run; tg_server_poll hands back the finished requests. Crater records are built per
+ * feature region (a square of region_cells cells of a level of detail, owning the craters whose
+ * centers lie in it) and kept resident in device memory, least recently used regions evicted
+ * first. Each request's heights are the same whichever requests share its batch. The reference
+ * evaluates such requests one at a time (Terrain::EvaluateTiles / EvaluatePoints,
+ * src/pipeline/terrain.cpp:133-158); this form has no counterpart there. */
+typedef struct tg_server tg_server;
+
+typedef struct tg_server_options {
+    const void* fractals;           /* the source: at most one enabled Perlin fBm Fractal */
+    uint32_t n_fractals;
+    float elevation;
+    tg_crater_population craters;   /* the crater layer */
+    tg_crater_shaping shaping;
+    double base_spacing;            /* finest level of detail, meters; levels are base * 2^k */
+    double point_spacing;           /* the level whose craters point queries take */
+    uint64_t hbm_budget;            /* device bytes the server may hold */
+    uint64_t max_batch_cells;       /* cells admitted into one batch (at least one request) */
+    uint32_t slots;                 /* batches in flight, 1 to 8 */
+    uint32_t region_cells;          /* side of a feature region in cells of its level */
+    int32_t variant;                /* batch kernel shape; -1 lets the autotuner pick */
+    uint32_t reserved;
+} tg_server_options;
+
+typedef struct tg_request {
+    uint64_t id;
+    uint32_t kind;                  /* 0 a tile, 1 a set of points */
+    uint32_t memory;                /* where `heights` lies: TG_MEMORY_HOST or TG_MEMORY_DEVICE */
+    tg_grid grid;                   /* tile: north up, spacing base_spacing * 2^k */
+    const double* points;           /* points: n_points (x, y) pairs (host), copied at submit */
+    uint32_t n_points;
+    float* heights;                 /* where the heights go (row-major tile, or one per point),
+                                       valid until the request is handed back; device heights are
+                                       written by a device-to-device copy on the server's stream */
+} tg_request;
+
+typedef struct tg_server_stats {
+    uint64_t submitted, completed, batches, cells;
+    uint64_t regions_built, regions_evicted, regions_resident;
+    uint64_t feature_bytes;         /* device bytes reserved for resident regions */
+    uint64_t device_bytes;          /* device bytes the server holds now */
+    uint64_t peak_bytes;            /* most it has held */
+    uint64_t deferred;              /* admissions put off by the memory budget */
+    double gpu_ms;                  /* device time of the batches (binning + evaluation) */
+    double region_ms;               /* host time spent building regions */
+} tg_server_stats;
+
+int tg_server_create(tg_device* device, const tg_server_options* options, tg_server** server);
+void tg_server_destroy(tg_server* server);
+/* Queues a request (TG_ERROR_ARGUMENT for a malformed one). */
+int tg_server_submit(tg_server* server, const tg_request* request);
+/* Advances the server: hands back finished batches' requests (their heights written) and launches
+ * waiting requests into free slots. `ids` receives up to `capacity` finished request ids and
+ * `count` how many; with `wait` set it blocks until at least one request finishes while any is
+ * queued or running. */
+int tg_server_poll(tg_server* server, int wait, uint64_t* ids, size_t capacity, size_t* count);
+int tg_server_stats_get(tg_server* server, tg_server_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,7 +144,38 @@ SIGNATURES.update({
     "tg_batch_stats_get": [_P, C.POINTER(BatchStats)],
 })
 
-RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p, "tg_batch_destroy": None}
+class ServerOptions(C.Structure):
+    _fields_ = [("fractals", _P), ("n_fractals", _U32), ("elevation", _F),
+                ("craters", Population), ("shaping", Shaping), ("base_spacing", _D),
+                ("point_spacing", _D), ("hbm_budget", C.c_uint64),
+                ("max_batch_cells", C.c_uint64), ("slots", _U32), ("region_cells", _U32),
+                ("variant", C.c_int32), ("reserved", _U32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("kind", _U32), ("memory", _U32), ("grid", Grid),
+                ("points", _P), ("n_points", _U32), ("heights", _P)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("cells", C.c_uint64), ("regions_built", C.c_uint64),
+                ("regions_evicted", C.c_uint64), ("regions_resident", C.c_uint64),
+                ("feature_bytes", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("peak_bytes", C.c_uint64), ("deferred", C.c_uint64), ("gpu_ms", _D),
+                ("region_ms", _D)]
+
+
+SIGNATURES.update({
+    "tg_server_create": [_P, C.POINTER(ServerOptions), C.POINTER(_P)],
+    "tg_server_destroy": [_P],
+    "tg_server_submit": [_P, C.POINTER(Request)],
+    "tg_server_poll": [_P, _I, _P, _SZ, C.POINTER(_SZ)],
+    "tg_server_stats_get": [_P, C.POINTER(ServerStats)],
+})
+
+RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p, "tg_batch_destroy": None,
+            "tg_server_destroy": None}
 
 _lib = None
 

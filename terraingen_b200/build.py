@@ -35,6 +35,7 @@ UNITS = {
     "seams.cu": [],
     "batch.cu": ["-fmad=false"],
     "batch_api.cu": [],
+    "serve.cu": [],
     "probe.cu": [],
     "static_scratch.cu": [],
     "api.cu": [],

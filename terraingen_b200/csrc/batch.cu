@@ -84,33 +84,56 @@ __device__ __forceinline__ bool is_points(const BatchTile& t) {
     return t.pointBase != kNone;
 }
 
-// One warp per (ref, record) pair: grid tiles count the bins of the reference tiles the
-// footprint window touches (as the plain path), point sets the blocks whose bounding box the
-// footprint disk meets.
+// A (ref, record) pair's place: its record, data base, item, and footprint (grid tiles: the
+// reference-tile box; point sets: the disk).
+struct PairSpot {
+    uint32_t record, dataBase, tile;
+    int4 box;         // empty: x > y
+    double x, y, reach;
+};
+
+__device__ __forceinline__ PairSpot pair_spot(const BatchView& v, uint32_t p, uint32_t nrefs) {
+    const BatchRef ref =
+        v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
+    PairSpot s;
+    s.record = ref.recordBegin + (p - ref.recordPairs);
+    s.dataBase = ref.dataBase;
+    s.tile = ref.tile;
+    return s;
+}
+
+// Counts of the bins each (ref, record) pair covers. The lanes of a warp take 32 pairs (each lane
+// one footprint: CratersOnRaster's window on a grid tile, as the plain path, or the disk a point
+// set's blocks are tested against); then the warp spreads each pair's bins over its lanes.
 __global__ void batch_crater_count_kernel(const CraterShapeKernel k, const BatchView v,
                                           uint32_t tpbX, uint32_t tpbY) {
     const uint32_t n = v.header->refRecords, nrefs = v.header->refs;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n; p += warps) {
-        const BatchRef ref =
-            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
-        const uint32_t i = ref.recordBegin + (p - ref.recordPairs);
-        const BatchTile& t = v.tiles[ref.tile];
-        const float* data = v.data + ref.dataBase;
-        int4 box = make_int4(1, 0, 1, 0);
-        if (lane == 0) {
-            const CraterRecord r = v.records[i];
+    for (uint32_t first = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; first < n;
+         first += warps * 32u) {
+        const uint32_t p = first + lane;
+        PairSpot me{0, 0, 0, make_int4(1, 0, 1, 0), 0.0, 0.0, 0.0};
+        if (p < n) {
+            me = pair_spot(v, p, nrefs);
+            me.box = make_int4(1, 0, 1, 0);
+            const BatchTile& t = v.tiles[me.tile];
+            const CraterRecord r = v.records[me.record];
+            const float* data = v.data + me.dataBase;
+            float cull;
             if (is_points(t)) {
-                const CraterReach c = crater_reach(k, r, data, v.footprints, i);
-                v.craterCulls[p] = c.cull;
-                box = make_int4(0, 0, 0, 0);  // non-empty: the blocks are tested below
+                const CraterReach c = crater_reach(k, r, data, v.footprints, me.record);
+                me.x = c.x;
+                me.y = c.y;
+                me.reach = c.reach;
+                cull = c.cull;
+                me.box = make_int4(0, 0, 0, 0);  // non-empty: the blocks are tested below
             } else {
-                const Footprint f = crater_footprint(k, r, data, v.footprints, i, t.grid);
-                box = f.tiles;
-                v.craterCulls[p] = f.cull;
+                const Footprint f = crater_footprint(k, r, data, v.footprints, me.record, t.grid);
+                me.box = f.tiles;
+                cull = f.cull;
             }
-            if (box.x <= box.y) {
+            if (me.box.x <= me.box.y) {
                 if (r.hasDatum == 1u) {
                     atomicOr(&v.header->flags, 1u);
                 }
@@ -118,82 +141,117 @@ __global__ void batch_crater_count_kernel(const CraterShapeKernel k, const Batch
                     atomicOr(&v.header->flags, 8u);
                 }
             }
-            v.craterBoxes[p] = box;
+            v.craterBoxes[p] = me.box;
+            v.craterCulls[p] = cull;
         }
-        box.x = __shfl_sync(0xffffffffu, box.x, 0);
-        box.y = __shfl_sync(0xffffffffu, box.y, 0);
-        box.z = __shfl_sync(0xffffffffu, box.z, 0);
-        box.w = __shfl_sync(0xffffffffu, box.w, 0);
-        if (box.x > box.y) {
-            continue;
-        }
-        if (is_points(t)) {
-            const CraterReach c = crater_reach(k, v.records[i], data, v.footprints, i);
-            for (uint32_t b = lane; b < t.binsX; b += 32u) {
-                if (disk_meets_box(c.x, c.y, c.reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
-                    atomicAdd(v.craterCounts + t.binBase + b, 1u);
+        const uint32_t live = __ballot_sync(0xffffffffu, me.box.x <= me.box.y);
+        for (uint32_t rest = live; rest != 0u; rest &= rest - 1u) {
+            const int q = __ffs(rest) - 1;
+            const int4 box = make_int4(__shfl_sync(0xffffffffu, me.box.x, q),
+                                       __shfl_sync(0xffffffffu, me.box.y, q),
+                                       __shfl_sync(0xffffffffu, me.box.z, q),
+                                       __shfl_sync(0xffffffffu, me.box.w, q));
+            const uint32_t tile = __shfl_sync(0xffffffffu, me.tile, q);
+            const BatchTile& t = v.tiles[tile];
+            if (is_points(t)) {
+                const double x = __shfl_sync(0xffffffffu, me.x, q);
+                const double y = __shfl_sync(0xffffffffu, me.y, q);
+                const double reach = __shfl_sync(0xffffffffu, me.reach, q);
+                for (uint32_t b = lane; b < t.binsX; b += 32u) {
+                    if (disk_meets_box(x, y, reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
+                        atomicAdd(v.craterCounts + t.binBase + b, 1u);
+                    }
                 }
+                continue;
             }
-            continue;
-        }
-        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
-        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
-        const uint32_t wide = bx1 - bx0 + 1u;
-        const uint32_t total = wide * (by1 - by0 + 1u);
-        for (uint32_t q = lane; q < total; q += 32u) {
-            atomicAdd(v.craterCounts + t.binBase + (by0 + q / wide) * t.binsX + bx0 + q % wide, 1u);
+            const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
+            const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
+            const uint32_t wide = bx1 - bx0 + 1u;
+            const uint32_t total = wide * (by1 - by0 + 1u);
+            for (uint32_t c = lane; c < total; c += 32u) {
+                atomicAdd(v.craterCounts + t.binBase + (by0 + c / wide) * t.binsX + bx0 + c % wide,
+                          1u);
+            }
         }
     }
 }
 
+// The 160-byte BinEntry of each pair into every bin it covers: the lanes of a warp read 32 pairs'
+// boxes, then the warp spreads each pair's bins over its lanes. The entry's index field holds the
+// pair's data base, where the shaping reads the record's data.
 __global__ void batch_crater_scatter_kernel(const CraterShapeKernel k, const BatchView v,
                                             uint32_t tpbX, uint32_t tpbY) {
     const uint32_t n = v.header->refRecords, nrefs = v.header->refs;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n; p += warps) {
-        const int4 box = v.craterBoxes[p];
-        if (box.x > box.y) {
-            continue;
-        }
-        const BatchRef ref =
-            v.refs[ref_of_pair(v.refs, nrefs, p, [](const BatchRef& r) { return r.recordPairs; })];
-        const uint32_t i = ref.recordBegin + (p - ref.recordPairs);
-        const BatchTile& t = v.tiles[ref.tile];
-        const int4* src = reinterpret_cast<const int4*>(v.records + i);
-        int4 tail;
-        tail.x = int(uint32_t(box.x) | (uint32_t(box.y) << 16));
-        tail.y = int(uint32_t(box.z) | (uint32_t(box.w) << 16));
-        tail.z = __float_as_int(v.craterCulls[p]);
-        tail.w = int(ref.dataBase);  // the shaping reads the record's data from here
-        auto put = [&](uint32_t b) {
-            const uint32_t slot = v.craterCounts[b] + atomicAdd(v.craterCursor + b, 1u);
-            if (slot >= v.craterCapacity) {
-                return;  // counted in the header's entry total; the host re-plans
-            }
-            int4* dst = reinterpret_cast<int4*>(v.craterEntries + slot);
-#pragma unroll
-            for (int w = 0; w < 9; ++w) {
-                dst[w] = __ldg(src + w);
-            }
-            dst[9] = tail;
-        };
-        if (is_points(t)) {
-            const CraterReach c =
-                crater_reach(k, v.records[i], v.data + ref.dataBase, v.footprints, i);
-            for (uint32_t b = lane; b < t.binsX; b += 32u) {
-                if (disk_meets_box(c.x, c.y, c.reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
-                    put(t.binBase + b);
+    for (uint32_t first = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; first < n;
+         first += warps * 32u) {
+        const uint32_t p = first + lane;
+        PairSpot me{0, 0, 0, make_int4(1, 0, 1, 0), 0.0, 0.0, 0.0};
+        float cull = 0.0f;
+        if (p < n) {
+            me.box = v.craterBoxes[p];
+            if (me.box.x <= me.box.y) {
+                const int4 box = me.box;
+                me = pair_spot(v, p, nrefs);
+                me.box = box;
+                cull = v.craterCulls[p];
+                if (is_points(v.tiles[me.tile])) {
+                    const CraterReach c = crater_reach(k, v.records[me.record],
+                                                       v.data + me.dataBase, v.footprints,
+                                                       me.record);
+                    me.x = c.x;
+                    me.y = c.y;
+                    me.reach = c.reach;
                 }
             }
-            continue;
         }
-        const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
-        const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
-        const uint32_t wide = bx1 - bx0 + 1u;
-        const uint32_t total = wide * (by1 - by0 + 1u);
-        for (uint32_t q = lane; q < total; q += 32u) {
-            put(t.binBase + (by0 + q / wide) * t.binsX + bx0 + q % wide);
+        const uint32_t live = __ballot_sync(0xffffffffu, me.box.x <= me.box.y);
+        for (uint32_t rest = live; rest != 0u; rest &= rest - 1u) {
+            const int q = __ffs(rest) - 1;
+            const int4 box = make_int4(__shfl_sync(0xffffffffu, me.box.x, q),
+                                       __shfl_sync(0xffffffffu, me.box.y, q),
+                                       __shfl_sync(0xffffffffu, me.box.z, q),
+                                       __shfl_sync(0xffffffffu, me.box.w, q));
+            const uint32_t tile = __shfl_sync(0xffffffffu, me.tile, q);
+            const uint32_t record = __shfl_sync(0xffffffffu, me.record, q);
+            int4 tail;
+            tail.x = int(uint32_t(box.x) | (uint32_t(box.y) << 16));
+            tail.y = int(uint32_t(box.z) | (uint32_t(box.w) << 16));
+            tail.z = __float_as_int(__shfl_sync(0xffffffffu, cull, q));
+            tail.w = int(__shfl_sync(0xffffffffu, me.dataBase, q));
+            const int4* src = reinterpret_cast<const int4*>(v.records + record);
+            auto put = [&](uint32_t b) {
+                const uint32_t slot = v.craterCounts[b] + atomicAdd(v.craterCursor + b, 1u);
+                if (slot >= v.craterCapacity) {
+                    return;  // counted in the header's entry total; the host re-plans
+                }
+                int4* dst = reinterpret_cast<int4*>(v.craterEntries + slot);
+#pragma unroll
+                for (int w = 0; w < 9; ++w) {
+                    dst[w] = __ldg(src + w);
+                }
+                dst[9] = tail;
+            };
+            const BatchTile& t = v.tiles[tile];
+            if (is_points(t)) {
+                const double x = __shfl_sync(0xffffffffu, me.x, q);
+                const double y = __shfl_sync(0xffffffffu, me.y, q);
+                const double reach = __shfl_sync(0xffffffffu, me.reach, q);
+                for (uint32_t b = lane; b < t.binsX; b += 32u) {
+                    if (disk_meets_box(x, y, reach, v.pointBoxes + 4 * size_t(t.binBase + b))) {
+                        put(t.binBase + b);
+                    }
+                }
+                continue;
+            }
+            const uint32_t bx0 = uint32_t(box.x) / tpbX, bx1 = uint32_t(box.y) / tpbX;
+            const uint32_t by0 = uint32_t(box.z) / tpbY, by1 = uint32_t(box.w) / tpbY;
+            const uint32_t wide = bx1 - bx0 + 1u;
+            const uint32_t total = wide * (by1 - by0 + 1u);
+            for (uint32_t c = lane; c < total; c += 32u) {
+                put(t.binBase + (by0 + c / wide) * t.binsX + bx0 + c % wide);
+            }
         }
     }
 }
@@ -345,6 +403,17 @@ __device__ __forceinline__ float perlin_at(uint32_t h00, uint32_t h10, uint32_t 
     return 1.41421356237309505f * lerp_fma(vv, lerp_fma(u, n00, n10), lerp_fma(u, n01, n11));
 }
 
+// sum + err += w * n, keeping the product's and the sum's rounding errors in err.
+__device__ __forceinline__ void accumulate(float& sum, float& err, float w, float n) {
+    const float t = w * n;
+    const float te = fmaf(w, n, -t);  // w * n - t, exactly
+    const float s = sum + t;
+    const float bp = s - sum;
+    const float se = (sum - (s - bp)) + (t - bp);  // TwoSum: sum + t - s, exactly
+    sum = s;
+    err += se + te;
+}
+
 __device__ __forceinline__ void corners(int32_t ix, int32_t iy, uint32_t sz, uint32_t& h00,
                                         uint32_t& h10, uint32_t& h01, uint32_t& h11) {
     const uint32_t ax0 = uint32_t(ix) * kLcgA + kLcgC, ax1 = ax0 + kLcgA;
@@ -447,10 +516,14 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
         //    position from the tile's per-octave anchor (split in double) plus float steps;
         //    points split their own position in double. Corner hashes are reused while the
         //    lattice cell does not change.
-        float sum[kCells];
+        // Compensated octave sums: sum + err carries the weighted octaves to about twice float
+        // precision (each product's rounding from an FMA residual, each sum's by TwoSum), so a
+        // source of kilometers keeps its millimeters.
+        float sum[kCells], err[kCells];
 #pragma unroll
         for (int j = 0; j < kCells; ++j) {
             sum[j] = 0.0f;
+            err[j] = 0.0f;
         }
         for (int o = 0; o < noise.octaves; ++o) {
             const uint32_t sz = noise.seedTerm[o];
@@ -471,8 +544,8 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                         cy = iy;
                         corners(ix, iy, sz, h00, h10, h01, h11);
                     }
-                    sum[j] = fmaf(w, perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)),
-                                  sum[j]);
+                    accumulate(sum[j], err[j], w,
+                               perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)));
                 }
             } else {
                 const OctaveAnchor a = v.anchors[t.anchorBase + o];
@@ -492,14 +565,15 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                         cy = iy;
                         corners(ix, iy, sz, h00, h10, h01, h11);
                     }
-                    sum[j] = fmaf(w, perlin_at(h00, h10, h01, h11, qx - lx, qy - ly), sum[j]);
+                    accumulate(sum[j], err[j], w, perlin_at(h00, h10, h01, h11, qx - lx, qy - ly));
                 }
             }
         }
         float h[kCells];
 #pragma unroll
         for (int j = 0; j < kCells; ++j) {
-            h[j] = fmaf(noise.amplitude, sum[j] / noise.total, noise.elevation);
+            // elevation + amplitude * sum / total, formed once per cell in double.
+            h[j] = float(fma(noise.scale, double(sum[j]) + double(err[j]), double(noise.elevation)));
         }
 
         // 2. Craters: each entry's data at its ref's base (the BinEntry's index field).
@@ -822,7 +896,8 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
     }
     const uint32_t tpbX = variant.binW / kRefTileCells, tpbY = variant.binH / kRefTileCells;
     if (maxRecords > 0) {
-        batch_crater_count_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(k, v, tpbX, tpbY);
+        batch_crater_count_kernel<<<grid_for(maxRecords, 256), 256, 0, stream>>>(k, v, tpbX,
+                                                                                   tpbY);
         if ((err = cudaGetLastError()) != cudaSuccess) {
             return err;
         }
@@ -843,8 +918,8 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
         return err;
     }
     if (maxRecords > 0) {
-        batch_crater_scatter_kernel<<<grid_for(maxRecords, 8), 256, 0, stream>>>(k, v, tpbX,
-                                                                                  tpbY);
+        batch_crater_scatter_kernel<<<grid_for(maxRecords, 256), 256, 0, stream>>>(k, v, tpbX,
+                                                                                     tpbY);
         if ((err = cudaGetLastError()) != cudaSuccess) {
             return err;
         }

@@ -357,6 +357,7 @@ int make_noise(const void* fractals, uint32_t n, float elevation, BatchNoise& no
     octaves.clear();
     noise.elevation = elevation;
     noise.total = 1.0f;
+    noise.scale = 0.0;
     const Fractal* only = nullptr;
     for (uint32_t i = 0; i < n; ++i) {
         const Fractal* f = static_cast<const Fractal*>(fractals) + i;
@@ -411,6 +412,7 @@ int make_noise(const void* fractals, uint32_t n, float elevation, BatchNoise& no
         tc = nc;
     }
     noise.total = total;
+    noise.scale = double(noise.amplitude) / double(total);
     return TG_OK;
 }
 
@@ -514,15 +516,19 @@ int load(tg_batch* b, Spec&& spec) {
             "allocation");
     TG_CUDA(b->slots[kSlotBoulderWindows].reserve(std::max<size_t>(bp, 1) * sizeof(int4)),
             "allocation");
-    // A first guess at the entries (a few bins per pair); a launch that needs more grows them.
-    TG_CUDA(b->slots[kSlotCraterEntries].reserve((size_t(rp) * 4 + 64) * sizeof(BinEntry)),
-            "allocation");
-    TG_CUDA(b->slots[kSlotBoulderEntries].reserve((size_t(bp) * 2 + 64) * sizeof(BoulderEntry)),
-            "allocation");
     TG_CUDA(b->slots[kSlotHeader].reserve(sizeof(BatchHeader)), "allocation");
     if (int st = plan_bins(b)) {
         return st;
     }
+    // A first guess at the entries (a few per bin, not above a few per pair); a launch that
+    // needs more grows them.
+    TG_CUDA(b->slots[kSlotCraterEntries].reserve(
+                (std::min<size_t>(size_t(rp) * 4, size_t(b->bins) * 8) + 1024) * sizeof(BinEntry)),
+            "allocation");
+    TG_CUDA(b->slots[kSlotBoulderEntries].reserve(
+                (std::min<size_t>(size_t(bp) * 2, size_t(b->bins) * 4) + 1024) *
+                sizeof(BoulderEntry)),
+            "allocation");
     b->loaded = true;
     b->last.cells = cells;
     return TG_OK;
@@ -616,6 +622,18 @@ size_t output_floats(const tg_batch* b) {
 
 uint64_t cells(const tg_batch* b) {
     return b->cells;
+}
+
+uint32_t replays(const tg_batch* b) {
+    return b->replays;
+}
+
+size_t device_bytes(const tg_batch* b) {
+    size_t total = 0;
+    for (const Buffer& s : b->slots) {
+        total += s.bytes;
+    }
+    return total;
 }
 
 }  // namespace batch

@@ -76,6 +76,10 @@ bool done(tg_batch* b);
 
 size_t output_floats(const tg_batch* b);
 uint64_t cells(const tg_batch* b);
+// Graph launches so far (a finish that re-launched for more entries adds one).
+uint32_t replays(const tg_batch* b);
+// Device bytes the batch's buffers hold.
+size_t device_bytes(const tg_batch* b);
 
 }  // namespace batch
 }  // namespace tgb

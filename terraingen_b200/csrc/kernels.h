@@ -215,6 +215,7 @@ static_assert(sizeof(OctaveAnchor) == 32, "OctaveAnchor layout");
 struct BatchNoise {
     int32_t octaves;
     float amplitude, total, elevation;
+    double scale;  // amplitude / total
     uint32_t seedTerm[kBatchMaxOctaves];  // octave seed through pcg3d's first LCG step
     float weight[kBatchMaxOctaves];
     double tc[kBatchMaxOctaves], ts[kBatchMaxOctaves], frequency[kBatchMaxOctaves];
