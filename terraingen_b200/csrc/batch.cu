@@ -36,7 +36,6 @@ constexpr uint32_t kBoulderChunk = kStageBytes / sizeof(BoulderEntry);
 static_assert(kCraterChunk * sizeof(BinEntry) == kStageBytes, "whole crater entries per stage");
 static_assert(kBoulderChunk * sizeof(BoulderEntry) == kStageBytes, "whole boulder entries");
 
-constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kLcgA = 1664525u, kLcgC = 1013904223u;
 
 // Perlin's quintic fade and the lerp (include/terraingen/noise/lattice.h:76-86) with explicit
@@ -81,7 +80,7 @@ __device__ __forceinline__ uint32_t ref_of_pair(const BatchRef* refs, uint32_t n
 }
 
 __device__ __forceinline__ bool is_points(const BatchTile& t) {
-    return t.pointBase != kNone;
+    return t.kind == kTilePoints;
 }
 
 // A (ref, record) pair's place: its record, data base, item, and footprint (grid tiles: the
@@ -120,8 +119,10 @@ __global__ void batch_crater_count_kernel(const CraterShapeKernel k, const Batch
             const BatchTile& t = v.tiles[me.tile];
             const CraterRecord r = v.records[me.record];
             const float* data = v.data + me.dataBase;
-            float cull;
-            if (is_points(t)) {
+            float cull = 0.0f;
+            if (t.kind == kTileIndexedPoints) {
+                // Read from the resident cell lists, not binned.
+            } else if (is_points(t)) {
                 const CraterReach c = crater_reach(k, r, data, v.footprints, me.record);
                 me.x = c.x;
                 me.y = c.y;
@@ -424,6 +425,86 @@ __device__ __forceinline__ void corners(int32_t ix, int32_t iy, uint32_t sz, uin
     h11 = corner_hash(ax1, ay1, sz);
 }
 
+// The source at a point: Fractal2's octaves with each lattice position split in double, summed
+// with compensation (see the grid path), as elevation + amplitude * sum / total.
+__device__ __forceinline__ float point_source(const BatchNoise& noise, double x, double y) {
+    float sum = 0.0f, err = 0.0f;
+    for (int o = 0; o < noise.octaves; ++o) {
+        const double px = fma(fma(x, noise.tc[o], -y * noise.ts[o]), noise.frequency[o],
+                              noise.ox[o]);
+        const double py = fma(fma(x, noise.ts[o], y * noise.tc[o]), noise.frequency[o],
+                              noise.oy[o]);
+        const double lx = floor(px), ly = floor(py);
+        uint32_t h00, h10, h01, h11;
+        corners(int32_t(uint32_t(uint64_t(int64_t(lx)))), int32_t(uint32_t(uint64_t(int64_t(ly)))),
+                noise.seedTerm[o], h00, h10, h01, h11);
+        accumulate(sum, err, noise.weight[o],
+                   perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)));
+    }
+    return float(fma(noise.scale, double(sum) + double(err), double(noise.elevation)));
+}
+
+// One point of an indexed point set per thread: the source, then the craters of its resident
+// region's cell list (each within its cull distance), one write. Threads run independently.
+template <bool kFast>
+__device__ __forceinline__ void indexed_points(const CraterShapeKernel& k,
+                                               const crater::FastKernel& fk,
+                                               const BatchNoise& noise, const BatchView& v,
+                                               const BatchTile& t, uint32_t i, float* heights,
+                                               uint32_t& pairs) {
+    if (i >= t.grid.width) {
+        return;
+    }
+    const size_t at = size_t(t.pointBase) + i;
+    const double x = v.points[2 * at], y = v.points[2 * at + 1];
+    const float base = point_source(noise, x, y);
+    double acc = double(base);
+    // The point's region from the set's region table.
+    const double side = t.grid.pixelWidth;
+    const uint32_t tw = t.grid.height, th = t.pitch;
+    const int rx = min(max(int(floor((x - t.grid.originX) / side)), 0), int(tw) - 1);
+    const int ry = min(max(int(floor((y - t.grid.originY) / side)), 0), int(th) - 1);
+    const uint32_t region = v.pointTable[t.tableBase + uint32_t(ry) * tw + uint32_t(rx)];
+    if (region == 0xffffffffu) {
+        heights[t.heightOffset + i] = base;  // no region: the source alone (not reached)
+        return;
+    }
+    const PointRegion pr = v.pointRegions[region];
+    const int gx = min(max(int(floor((x - pr.x0) / pr.cell)), 0), int(pr.g) - 1);
+    const int gy = min(max(int(floor((y - pr.y0) / pr.cell)), 0), int(pr.g) - 1);
+    const uint32_t* lists = v.pointLists + pr.listBase;
+    const uint32_t cell = uint32_t(gy) * pr.g + uint32_t(gx);
+    const uint32_t* entries = lists + pr.g * pr.g + 1;
+    const float pxh = float(x), pxl = float(x - double(pxh));
+    const float pyh = float(y), pyl = float(y - double(pyh));
+    const float* data = v.data + pr.dataBase;
+    const float* harmonics = v.harmonics + pr.dataBase;
+    for (uint32_t e = lists[cell]; e < lists[cell + 1]; ++e) {
+        const uint32_t rec = pr.recBase + entries[e];
+        const CraterRecord r = v.records[rec];
+        const float cull = v.culls[rec];
+        const float dx = crater::split_difference(pxh, pxl, r.x, r.xLow);
+        const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
+        if (!(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) < cull * cull)) {
+            continue;
+        }
+        ++pairs;
+        if (kFast) {
+            bool reached;
+            const float shaped = crater::fast_contribution(fk, harmonics, r, dx, dy, reached);
+            if (reached) {
+                acc += double(shaped);
+            }
+        } else {
+            const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
+            if (q.reached) {
+                acc += double(q.shaped);
+            }
+        }
+    }
+    heights[t.heightOffset + i] = float(acc);
+}
+
 template <int kBinW, int kBinH, int kCells, bool kFast>
 __global__ void __launch_bounds__(kBinW* kBinH / kCells)
     batch_evaluate_kernel(const CraterShapeKernel k, const BatchNoise noise, const BatchView v) {
@@ -476,8 +557,13 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
         }
         const BatchTile& t = v.tiles[sTile];
         const Grid grid = t.grid;
-        const bool points = t.pointBase != kNone;
         const uint32_t local = item - t.binBase;
+        if (t.kind == kTileIndexedPoints) {
+            indexed_points<kFast>(k, fk, noise, v, t, local * (kBinW * kBinH / kCells) + tid,
+                                  heights, craterPairs);
+            continue;
+        }
+        const bool points = t.kind == kTilePoints;
         // Grid: this thread's kCells cells of one row. Point set: kCells consecutive points.
         uint32_t row = 0, col0 = 0, first = 0;
         bool live[kCells];
@@ -923,9 +1009,11 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
         if ((err = cudaGetLastError()) != cudaSuccess) {
             return err;
         }
-        batch_harmonics_kernel<<<grid_for(maxRecords, 256), 256, 0, stream>>>(v);
-        if ((err = cudaGetLastError()) != cudaSuccess) {
-            return err;
+        if (!v.harmonicsReady) {
+            batch_harmonics_kernel<<<grid_for(maxRecords, 256), 256, 0, stream>>>(v);
+            if ((err = cudaGetLastError()) != cudaSuccess) {
+                return err;
+            }
         }
     }
     if (maxBoulders > 0) {

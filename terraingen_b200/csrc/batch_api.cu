@@ -49,6 +49,8 @@ enum BatchSlot {
     kSlotPoints,
     kSlotPointIndex,
     kSlotPointBoxes,
+    kSlotPointTable,
+    kSlotPointRegions,
     kSlotRecords,
     kSlotFootprints,
     kSlotData,
@@ -166,7 +168,15 @@ int plan_bins(tg_batch* b) {
         d.binBase = uint32_t(base);
         d.anchorBase = uint32_t(i) * uint32_t(stride);
         d.boulderWidth = it.boulderWidth;
-        if (it.points) {
+        d.kind = it.kind;
+        d.tableBase = it.tableBase;
+        if (it.kind == kTileIndexedPoints) {
+            // One point per thread of the kernel shape.
+            const uint32_t threads = v.binW * v.binH / v.cellsPerThread;
+            d.pointBase = it.pointBegin;
+            d.binsX = (it.grid.width + threads - 1) / threads;
+            d.binsY = 1;
+        } else if (it.points) {
             d.pointBase = it.pointBegin;
             d.binsX = (it.grid.width + block - 1) / block;
             d.binsY = 1;
@@ -244,6 +254,11 @@ BatchView make_view(tg_batch* b) {
     v.boulderCapacity = capacity<BoulderEntry>(b, kSlotBoulderEntries);
     v.boulderWindows = ptr<int4>(b, kSlotBoulderWindows);
     v.capacityBins = capacity_bins(b);
+    v.harmonicsReady = f.harmonicsReady ? 1u : 0u;
+    v.pointTable = ptr<uint32_t>(b, kSlotPointTable);
+    v.pointRegions = ptr<PointRegion>(b, kSlotPointRegions);
+    v.pointLists = f.pointLists;
+    v.culls = f.culls;
     return v;
 }
 
@@ -426,18 +441,20 @@ void append_points(Spec& spec, const double* xy, uint32_t count) {
     }
     const double scale[2] = {hi[0] > lo[0] ? 65535.0 / (hi[0] - lo[0]) : 0.0,
                              hi[1] > lo[1] ? 65535.0 / (hi[1] - lo[1]) : 0.0};
-    std::vector<uint32_t> order(count);
-    std::iota(order.begin(), order.end(), 0u);
-    std::vector<uint32_t> key(count);
+    // (Morton code, index) in one word: sorting the words orders by code, ties by index.
+    std::vector<uint64_t> key(count);
     for (uint32_t i = 0; i < count; ++i) {
-        key[i] = morton(xy[2 * i], xy[2 * i + 1], lo, scale);
+        key[i] = (uint64_t(morton(xy[2 * i], xy[2 * i + 1], lo, scale)) << 32) | i;
     }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t c) { return key[a] < key[c]; });
-    for (uint32_t i : order) {
-        spec.points.push_back(xy[2 * i]);
-        spec.points.push_back(xy[2 * i + 1]);
-        spec.pointIndex.push_back(i);
+    std::sort(key.begin(), key.end());
+    const size_t at = spec.pointIndex.size();
+    spec.points.resize(2 * (at + count));
+    spec.pointIndex.resize(at + count);
+    for (uint32_t n = 0; n < count; ++n) {
+        const uint32_t i = uint32_t(key[n]);
+        spec.points[2 * (at + n)] = xy[2 * i];
+        spec.points[2 * (at + n) + 1] = xy[2 * i + 1];
+        spec.pointIndex[at + n] = i;
     }
 }
 
@@ -508,6 +525,12 @@ int load(tg_batch* b, Spec&& spec) {
         return st;
     }
     if (int st = upload(b, kSlotPointIndex, s.pointIndex.data(), s.pointIndex.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotPointTable, s.pointTable.data(), s.pointTable.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotPointRegions, s.pointRegions.data(), s.pointRegions.size())) {
         return st;
     }
     TG_CUDA(b->slots[kSlotCraterBoxes].reserve(std::max<size_t>(rp, 1) * sizeof(int4)),
@@ -846,6 +869,7 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
         it.heightOffset = t.height_offset;
         it.pitch = t.pitch;
         it.points = false;
+        it.kind = kTileGrid;
         it.pointBegin = kNone;
         it.boulderWidth = t.boulder_width;
         spec.refs.push_back(BatchRef{uint32_t(spec.items.size()), t.crater_begin, t.crater_count,
@@ -876,6 +900,7 @@ int tg_batch_load(tg_batch* b, const tg_batch_input* in) {
         it.heightOffset = p.height_offset;
         it.pitch = p.point_count;
         it.points = true;
+        it.kind = kTilePoints;
         it.pointBegin = uint32_t(spec.pointIndex.size());
         it.boulderWidth = p.boulder_width;
         append_points(spec, in->points + 2 * size_t(p.point_begin), p.point_count);

@@ -33,6 +33,8 @@ struct Item {
     bool points;
     uint32_t pointBegin;
     double boulderWidth;
+    uint32_t kind = kTileGrid;  // kTileGrid, kTilePoints or kTileIndexedPoints
+    uint32_t tableBase = 0;     // indexed points: their region table in Spec::pointTable
 };
 
 // Device arrays the refs index; the batch reads them and owns none.
@@ -42,6 +44,9 @@ struct Features {
     const float* data = nullptr;
     float* harmonics = nullptr;  // as long as data
     const BoulderRecord* boulders = nullptr;
+    bool harmonicsReady = false;  // harmonics already computed (no per-batch pass)
+    const uint32_t* pointLists = nullptr;  // indexed points: resident cell lists
+    const float* culls = nullptr;          // indexed points: cull distance per record
 };
 
 // A whole batch, host side. `points` holds (x, y) per point in device order (each set's points
@@ -51,6 +56,8 @@ struct Spec {
     std::vector<BatchRef> refs;  // recordPairs / boulderPairs filled by the engine
     std::vector<double> points;
     std::vector<uint32_t> pointIndex;
+    std::vector<PointRegion> pointRegions;  // indexed points: the regions they read
+    std::vector<uint32_t> pointTable;       // indexed points: region tables (kernels.h)
     BatchNoise noise{};
     std::vector<Octave> octaves;
     CraterShapeKernel kernel{};

@@ -184,8 +184,27 @@ struct BatchTile {
     uint32_t anchorBase;    // the tile's first OctaveAnchor
     uint32_t pointBase;     // point sets: first point; ~0u for a grid
     double boulderWidth;    // dome band width (the tile's sample spacing)
+    uint32_t kind;          // kTileGrid, kTilePoints or kTileIndexedPoints
+    uint32_t tableBase;     // indexed points: their region table (see below)
 };
-static_assert(sizeof(BatchTile) == 96, "BatchTile layout");
+static_assert(sizeof(BatchTile) == 104, "BatchTile layout");
+
+// Item kinds: a grid; a point set whose blocks are binned like a grid's bins; a point set whose
+// craters come from resident per-region cell lists (PointRegion), one point per thread. An
+// indexed point set's regions cover its bounding box: region (ix, iy) is pointTable[tableBase +
+// (iy - iy0) * tableWidth + (ix - ix0)] (a PointRegion index, ~0u for none), with ix0 * side and
+// iy0 * side in grid.originX / grid.originY, the region side in grid.pixelWidth, tableWidth in
+// grid.height and the table's rows in pitch; its points keep the caller's order.
+constexpr uint32_t kTileGrid = 0, kTilePoints = 1, kTileIndexedPoints = 2;
+
+// A resident feature region as indexed points read it: its square of g x g cells of side `cell`
+// from (x0, y0), each cell listing the records (relative to recBase) whose footprint disk meets
+// it: lists[listBase + c] .. lists[listBase + c + 1] index lists[listBase + g * g + 1 + k].
+struct PointRegion {
+    double x0, y0, cell;
+    uint32_t recBase, dataBase, listBase, g;
+};
+static_assert(sizeof(PointRegion) == 40, "PointRegion layout");
 
 // A run of crater records and boulders one tile (or point set) takes: records [recordBegin,
 // recordBegin + recordCount) with data offsets relative to data + dataBase, boulders [boulderBegin,
@@ -259,6 +278,11 @@ struct BatchView {
     uint32_t boulderCapacity;
     int4* boulderWindows;          // [boulder pairs]
     uint32_t capacityBins;
+    uint32_t harmonicsReady;       // the harmonics are already in place (resident regions)
+    const uint32_t* pointTable;    // indexed points: region tables
+    const PointRegion* pointRegions;
+    const uint32_t* pointLists;    // the regions' cell lists
+    const float* culls;            // indexed points: each record's cull distance
 };
 
 // A kernel shape of the persistent evaluation: bins of binW x binH cells (point sets: blocks of

@@ -46,8 +46,11 @@ struct RegionHash {
 
 // A feature region resident on the device: its records (with footprints) and data in the arenas.
 struct Region {
-    uint32_t recBegin = 0, recCount = 0;
+    uint32_t recBegin = 0, recCount = 0;  // owned records (tiles read these)
+    uint32_t recTotal = 0;                // owned, then the others reaching in (indexed points)
     uint32_t dataBegin = 0, dataCount = 0;
+    uint32_t listBegin = 0, listCount = 0;  // the cell lists (0 when not indexed)
+    PointRegion index{};
     uint64_t lastUse = 0;
     uint32_t inFlight = 0;  // batches in flight that read it
 };
@@ -108,25 +111,56 @@ struct Pending {
     int lod = 0;
     uint64_t cells = 0;
     std::vector<RegionKey> keys;  // the regions whose craters can reach it
+    int64_t ix0 = 0, iy0 = 0;     // points: the regions covering their bounding box
+    uint32_t tw = 0, th = 0;
+    std::vector<uint8_t> occupied;  // points: regions holding a point, tw x th
 };
 
 // A region's records built on the host, waiting to be copied into the arenas.
 struct Built {
     RegionKey key;
     int status = TG_OK;
-    std::vector<CraterRecord> records;
+    std::vector<CraterRecord> records;  // owned first
     std::vector<double> footprints;
+    std::vector<float> culls;
     std::vector<float> data;
+    uint32_t owned = 0;
+    std::vector<uint32_t> lists;        // the cell lists (indexed regions)
+    PointRegion index{};
     bool heavy = false;
     double ms = 0.0;
 };
+
+constexpr uint32_t kIndexCells = 16;  // cells across an indexed region
+
+// The cull distance of a record (as the device's crater_reach computes it): beyond it no cell
+// is within the crater's reach.
+float cull_of(const CraterRecord& r, const float* data, float reachRadii) {
+    double sum = 1.0;
+    if (r.tableCount > 0u) {
+        for (uint32_t n = 0; n < r.tableCount; ++n) {
+            sum = std::fmax(sum, 1.0 + double(data[r.tableOffset + n]));
+        }
+    } else {
+        for (uint32_t n = 0; n < r.harmonicCount; ++n) {
+            sum += std::fabs(double(data[r.harmonicOffset + 2u * n]));
+        }
+    }
+    const double scale = std::sqrt(double(r.ellipticity)) * sum;
+    const bool stretched = r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
+                           r.shiftY != 0.0f;
+    return stretched ? INFINITY
+                     : float(scale * double(reachRadii) * (0.5 * double(r.diameter)) *
+                             (1.0 + 1e-5)) + 1e-6f;
+}
 
 // Builds regions' crater records on host worker threads: tg_crater_batch over the region's
 // grid, then the craters whose centers lie in the region.
 class Builders {
 public:
-    void start(unsigned n, const tg_server_options& opt) {
+    void start(unsigned n, const tg_server_options& opt, int pointLevel) {
         opt_ = opt;
+        pointLevel_ = pointLevel;
         for (unsigned i = 0; i < n; ++i) {
             threads_.emplace_back([this] { work(); });
         }
@@ -220,9 +254,16 @@ private:
             foot.resize(3 * nr);
         }
         if (b.status == TG_OK) {
-            for (size_t i = 0; i < nr; ++i) {
-                const double x = foot[3 * i], y = foot[3 * i + 1];
-                if (x >= x0 && x < x0 + side && y >= y0 && y < y0 + side) {
+            // Owned records (centers in the region) first; an indexed region (the level point
+            // queries read) keeps the others reaching in after them.
+            const bool indexed = k.lod == pointLevel_;
+            for (int pass = 0; pass < (indexed ? 2 : 1); ++pass) {
+                for (size_t i = 0; i < nr; ++i) {
+                    const double x = foot[3 * i], y = foot[3 * i + 1];
+                    const bool owned = x >= x0 && x < x0 + side && y >= y0 && y < y0 + side;
+                    if (owned != (pass == 0)) {
+                        continue;
+                    }
                     const CraterRecord& r = recs[i];
                     b.heavy |= r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u ||
                                r.peakCount > 0u || r.shiftX != 0.0f || r.shiftY != 0.0f ||
@@ -233,16 +274,68 @@ private:
                     b.records.push_back(r);
                     b.footprints.insert(b.footprints.end(),
                                         {foot[3 * i], foot[3 * i + 1], foot[3 * i + 2]});
+                    b.culls.push_back(cull_of(r, values.data(), kernel.reachRadii));
+                }
+                if (pass == 0) {
+                    b.owned = uint32_t(b.records.size());
                 }
             }
             b.data.assign(values.begin(), values.begin() + std::ptrdiff_t(nd));
+            if (indexed) {
+                index(b, x0, y0, side);
+            }
         }
         b.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
                    .count();
         return b;
     }
 
+    // Cell lists of an indexed region: each of kIndexCells^2 cells lists the records whose
+    // footprint disk (the larger of reach and cull distance) meets it.
+    static void index(Built& b, double x0, double y0, double side) {
+        const uint32_t g = kIndexCells;
+        const double cell = side / g;
+        std::vector<std::vector<uint32_t>> cells(size_t(g) * g);
+        for (uint32_t i = 0; i < b.records.size(); ++i) {
+            const double x = b.footprints[3 * size_t(i)], y = b.footprints[3 * size_t(i) + 1];
+            const double reach = std::fmax(b.footprints[3 * size_t(i) + 2], double(b.culls[i])) +
+                                 1e-3;
+            if (!std::isfinite(reach)) {
+                for (auto& c : cells) {
+                    c.push_back(i);
+                }
+                continue;
+            }
+            const int cx0 = std::max(0, int(std::floor((x - reach - x0) / cell)));
+            const int cx1 = std::min(int(g) - 1, int(std::floor((x + reach - x0) / cell)));
+            const int cy0 = std::max(0, int(std::floor((y - reach - y0) / cell)));
+            const int cy1 = std::min(int(g) - 1, int(std::floor((y + reach - y0) / cell)));
+            for (int cy = cy0; cy <= cy1; ++cy) {
+                for (int cx = cx0; cx <= cx1; ++cx) {
+                    const double bx0 = x0 + cx * cell, by0 = y0 + cy * cell;
+                    const double dx = std::fmax(std::fmax(bx0 - x, x - (bx0 + cell)), 0.0);
+                    const double dy = std::fmax(std::fmax(by0 - y, y - (by0 + cell)), 0.0);
+                    if (dx * dx + dy * dy <= reach * reach) {
+                        cells[size_t(cy) * g + size_t(cx)].push_back(i);
+                    }
+                }
+            }
+        }
+        b.lists.assign(size_t(g) * g + 1, 0u);
+        for (size_t c = 0; c < cells.size(); ++c) {
+            b.lists[c + 1] = b.lists[c] + uint32_t(cells[c].size());
+        }
+        for (const auto& c : cells) {
+            b.lists.insert(b.lists.end(), c.begin(), c.end());
+        }
+        b.index.x0 = x0;
+        b.index.y0 = y0;
+        b.index.cell = cell;
+        b.index.g = g;
+    }
+
     tg_server_options opt_{};
+    int pointLevel_ = -1;
     std::vector<std::thread> threads_;
     std::mutex mutex_;
     std::condition_variable wake_, finished_;
@@ -281,9 +374,10 @@ struct tg_server {
     bool tuned = false;
     double margin = 0.0;  // meters a crater can reach beyond its region
 
-    Buffer records, footprints, data, harmonics;
-    uint32_t recCap = 0, dataCap = 0;
-    Ranges recRanges, dataRanges;
+    Buffer records, footprints, culls, data, harmonics, lists;
+    uint32_t recCap = 0, dataCap = 0, listCap = 0;
+    Ranges recRanges, dataRanges, listRanges;
+    cudaStream_t installStream = nullptr;
     std::unordered_map<RegionKey, Region, RegionHash> regions;
     std::list<Pending> waiting;
     Builders builders;
@@ -311,7 +405,8 @@ int level_of(const tg_server* s, double spacing) {
 }
 
 size_t server_bytes(const tg_server* s) {
-    size_t total = s->records.bytes + s->footprints.bytes + s->data.bytes + s->harmonics.bytes;
+    size_t total = s->records.bytes + s->footprints.bytes + s->culls.bytes + s->data.bytes +
+                   s->harmonics.bytes + s->lists.bytes;
     for (const ServeSlot& slot : s->slots) {
         total += slot.out.bytes + (slot.batch ? batch::device_bytes(slot.batch) : 0);
     }
@@ -324,22 +419,28 @@ void note_bytes(tg_server* s) {
 }
 
 void evict(tg_server* s, std::unordered_map<RegionKey, Region, RegionHash>::iterator it) {
-    s->recRanges.give(it->second.recBegin, it->second.recCount);
+    s->recRanges.give(it->second.recBegin, it->second.recTotal);
     s->dataRanges.give(it->second.dataBegin, it->second.dataCount);
+    s->listRanges.give(it->second.listBegin, it->second.listCount);
     s->regions.erase(it);
     ++s->stats.regions_evicted;
 }
 
-// Arena room for `records` records and `values` data floats, evicting least recently used
-// regions that no batch in flight reads.
-bool make_room(tg_server* s, size_t records, size_t values, size_t& recAt, size_t& dataAt) {
+// Arena room for `records` records, `values` data floats and `entries` list words, evicting least
+// recently used regions that no batch in flight reads.
+bool make_room(tg_server* s, size_t records, size_t values, size_t entries, size_t& recAt,
+               size_t& dataAt, size_t& listAt) {
     for (;;) {
-        size_t r = 0, d = 0;
+        size_t r = 0, d = 0, l = 0;
         if (s->recRanges.take(records, r)) {
             if (s->dataRanges.take(values, d)) {
-                recAt = r;
-                dataAt = d;
-                return true;
+                if (s->listRanges.take(entries, l)) {
+                    recAt = r;
+                    dataAt = d;
+                    listAt = l;
+                    return true;
+                }
+                s->dataRanges.give(d, values);
             }
             s->recRanges.give(r, records);
         }
@@ -372,34 +473,59 @@ int install_regions(tg_server* s) {
         if (s->regions.count(b.key)) {
             continue;
         }
-        size_t recAt = 0, dataAt = 0;
-        if (!make_room(s, b.records.size(), b.data.size(), recAt, dataAt)) {
+        size_t recAt = 0, dataAt = 0, listAt = 0;
+        if (!make_room(s, b.records.size(), b.data.size(), b.lists.size(), recAt, dataAt,
+                       listAt)) {
             s->stash.push_back(std::move(b));
             continue;
         }
+        const cudaStream_t st = s->installStream;
         if (!b.records.empty()) {
-            TG_CUDA(cudaMemcpy(static_cast<CraterRecord*>(s->records.ptr) + recAt,
-                               b.records.data(), b.records.size() * sizeof(CraterRecord),
-                               cudaMemcpyHostToDevice),
+            TG_CUDA(cudaMemcpyAsync(static_cast<CraterRecord*>(s->records.ptr) + recAt,
+                                    b.records.data(), b.records.size() * sizeof(CraterRecord),
+                                    cudaMemcpyHostToDevice, st),
                     "copy to device");
-            TG_CUDA(cudaMemcpy(static_cast<double*>(s->footprints.ptr) + 3 * recAt,
-                               b.footprints.data(), b.footprints.size() * sizeof(double),
-                               cudaMemcpyHostToDevice),
+            TG_CUDA(cudaMemcpyAsync(static_cast<double*>(s->footprints.ptr) + 3 * recAt,
+                                    b.footprints.data(), b.footprints.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, st),
+                    "copy to device");
+            TG_CUDA(cudaMemcpyAsync(static_cast<float*>(s->culls.ptr) + recAt, b.culls.data(),
+                                    b.culls.size() * sizeof(float), cudaMemcpyHostToDevice, st),
                     "copy to device");
         }
         if (!b.data.empty()) {
-            TG_CUDA(cudaMemcpy(static_cast<float*>(s->data.ptr) + dataAt, b.data.data(),
-                               b.data.size() * sizeof(float), cudaMemcpyHostToDevice),
+            TG_CUDA(cudaMemcpyAsync(static_cast<float*>(s->data.ptr) + dataAt, b.data.data(),
+                                    b.data.size() * sizeof(float), cudaMemcpyHostToDevice, st),
                     "copy to device");
         }
+        if (!b.lists.empty()) {
+            TG_CUDA(cudaMemcpyAsync(static_cast<uint32_t*>(s->lists.ptr) + listAt, b.lists.data(),
+                                    b.lists.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                    st),
+                    "copy to device");
+        }
+        // The lean path's harmonics of the region, once, where every batch reads them.
+        TG_CUDA(launch_crater_harmonics(static_cast<const CraterRecord*>(s->records.ptr) + recAt,
+                                        uint32_t(b.records.size()),
+                                        static_cast<const float*>(s->data.ptr) + dataAt,
+                                        static_cast<float*>(s->harmonics.ptr) + dataAt, st),
+                "harmonics launch");
+        TG_CUDA(cudaStreamSynchronize(st), "synchronize");
         if (b.heavy) {
             s->fast = false;
         }
         Region r;
         r.recBegin = uint32_t(recAt);
-        r.recCount = uint32_t(b.records.size());
+        r.recCount = b.owned;
+        r.recTotal = uint32_t(b.records.size());
         r.dataBegin = uint32_t(dataAt);
         r.dataCount = uint32_t(b.data.size());
+        r.listBegin = uint32_t(listAt);
+        r.listCount = uint32_t(b.lists.size());
+        r.index = b.index;
+        r.index.recBase = uint32_t(recAt);
+        r.index.dataBase = uint32_t(dataAt);
+        r.index.listBase = uint32_t(listAt);
         r.lastUse = ++s->tick;
         s->regions.emplace(b.key, r);
         ++s->stats.regions_built;
@@ -472,14 +598,17 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
     spec.features.footprints = static_cast<const double*>(s->footprints.ptr);
     spec.features.data = static_cast<const float*>(s->data.ptr);
     spec.features.harmonics = static_cast<float*>(s->harmonics.ptr);
+    spec.features.harmonicsReady = true;  // computed when each region was installed
+    spec.features.pointLists = static_cast<const uint32_t*>(s->lists.ptr);
+    spec.features.culls = static_cast<const float*>(s->culls.ptr);
+    std::unordered_map<RegionKey, uint32_t, RegionHash> table;  // region -> pointRegions index
     slot.reqs.clear();
     slot.offsets.clear();
     slot.pitches.clear();
     slot.used.clear();
     uint64_t cells = 0, outFloats = 0, bytes = 0;
     // Each slot's share of the budget left after the feature arenas bounds its batch.
-    const uint64_t arenas = s->records.bytes + s->footprints.bytes + s->data.bytes +
-                            s->harmonics.bytes;
+    const uint64_t arenas = s->stats.feature_bytes;
     const uint64_t allowance =
         s->opt.hbm_budget > arenas ? (s->opt.hbm_budget - arenas) / s->slots.size() : 0;
     // Requests in arrival order whose regions are resident; the others wait for their builds.
@@ -497,7 +626,7 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
         // always takes its first request.
         uint64_t pairs = 0;
         for (const RegionKey& k : p.keys) {
-            pairs += s->regions[k].recCount;
+            pairs += p.req.kind == 0 ? s->regions[k].recCount : 0u;
         }
         const uint64_t need = p.cells * 6 + pairs * 24;
         if (!slot.reqs.empty() && bytes + need > allowance) {
@@ -518,21 +647,44 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
             it.heightOffset = outFloats;
             outFloats += uint64_t(it.pitch) * g.height;
         } else {
-            it.grid = Grid{p.req.n_points, 1, 0.0, 1.0, 0.0, 0.0, 0.0, -1.0};
-            it.pitch = p.req.n_points;
+            // Points read their regions' resident cell lists: no refs, no binning.
+            const double side = level_spacing(s, p.lod) * s->opt.region_cells;
+            it.grid = Grid{p.req.n_points, p.tw, double(p.ix0) * side, side, 0.0,
+                           double(p.iy0) * side, 0.0, -side};
+            it.pitch = p.th;
             it.points = true;
-            it.pointBegin = uint32_t(spec.pointIndex.size());
+            it.kind = kTileIndexedPoints;
+            it.pointBegin = uint32_t(spec.points.size() / 2);
+            it.tableBase = uint32_t(spec.pointTable.size());
             it.boulderWidth = 0.0;
             it.heightOffset = outFloats;
             outFloats += p.req.n_points;
-            batch::append_points(spec, p.xy.data(), p.req.n_points);
+            spec.points.insert(spec.points.end(), p.xy.begin(), p.xy.end());
+            for (uint32_t ry = 0; ry < p.th; ++ry) {
+                for (uint32_t rx = 0; rx < p.tw; ++rx) {
+                    uint32_t index = 0xffffffffu;
+                    if (p.occupied[size_t(ry) * p.tw + rx]) {
+                        const RegionKey k{p.lod, p.ix0 + rx, p.iy0 + ry};
+                        auto found = table.find(k);
+                        if (found == table.end()) {
+                            found = table.emplace(k, uint32_t(spec.pointRegions.size())).first;
+                            spec.pointRegions.push_back(s->regions[k].index);
+                        }
+                        index = found->second;
+                    }
+                    spec.pointTable.push_back(index);
+                }
+            }
         }
         for (const RegionKey& k : p.keys) {
             Region& r = s->regions[k];
             r.lastUse = ++s->tick;
             ++r.inFlight;  // held until the batch completes
             slot.used.push_back(k);
-            spec.refs.push_back(BatchRef{item, r.recBegin, r.recCount, r.dataBegin, 0, 0, 0, 0});
+            if (p.req.kind == 0) {
+                spec.refs.push_back(
+                    BatchRef{item, r.recBegin, r.recCount, r.dataBegin, 0, 0, 0, 0});
+            }
         }
         slot.offsets.push_back(it.heightOffset);
         slot.pitches.push_back(it.pitch);
@@ -690,15 +842,22 @@ int tg_server_create(tg_device* device, const tg_server_options* options, tg_ser
     s->margin = double(s->kernel.reachRadii) * 2.5 * 0.5 * o.craters.max_diameter;
     // Feature arenas: a quarter of the budget, records and their footprints (168 B) and 24 data
     // floats per record.
+    // Feature arenas: a quarter of the budget; per record its record, footprint and cull
+    // (172 B), 24 data floats and their harmonics, and 4 list words.
     const size_t arenaBytes = size_t(o.hbm_budget / 4);
-    const size_t perRecord = sizeof(CraterRecord) + 3 * sizeof(double) + 2 * 24 * sizeof(float);
+    const size_t perRecord = sizeof(CraterRecord) + 3 * sizeof(double) + sizeof(float) +
+                             2 * 24 * sizeof(float) + 4 * sizeof(uint32_t);
     const size_t nRecords = std::max<size_t>(1024, std::min<size_t>(arenaBytes / perRecord,
                                                                     0x7fffffffu / 24));
     s->recCap = uint32_t(nRecords);
     s->dataCap = uint32_t(nRecords * 24);
+    s->listCap = uint32_t(nRecords * 4);
     cudaError_t err = s->records.reserve(size_t(s->recCap) * sizeof(CraterRecord));
     if (err == cudaSuccess) {
         err = s->footprints.reserve(size_t(s->recCap) * 3 * sizeof(double));
+    }
+    if (err == cudaSuccess) {
+        err = s->culls.reserve(size_t(s->recCap) * sizeof(float));
     }
     if (err == cudaSuccess) {
         err = s->data.reserve(size_t(s->dataCap) * sizeof(float));
@@ -706,15 +865,22 @@ int tg_server_create(tg_device* device, const tg_server_options* options, tg_ser
     if (err == cudaSuccess) {
         err = s->harmonics.reserve(size_t(s->dataCap) * sizeof(float));
     }
+    if (err == cudaSuccess) {
+        err = s->lists.reserve(size_t(s->listCap) * sizeof(uint32_t));
+    }
+    if (err == cudaSuccess) {
+        err = cudaStreamCreateWithFlags(&s->installStream, cudaStreamNonBlocking);
+    }
     if (err != cudaSuccess) {
         return undo(cuda_fail(err, "feature arena allocation"));
     }
     s->recRanges.reset(s->recCap);
     s->dataRanges.reset(s->dataCap);
+    s->listRanges.reset(s->listCap);
     const unsigned cores = std::max(2u, std::thread::hardware_concurrency());
-    s->builders.start(std::min(16u, cores - 1u), o);
-    s->stats.feature_bytes = s->records.bytes + s->footprints.bytes + s->data.bytes +
-                             s->harmonics.bytes;
+    s->builders.start(std::min(16u, cores - 1u), o, level_of(s, o.point_spacing));
+    s->stats.feature_bytes = s->records.bytes + s->footprints.bytes + s->culls.bytes +
+                             s->data.bytes + s->harmonics.bytes + s->lists.bytes;
     s->slots.resize(o.slots);
     for (ServeSlot& slot : s->slots) {
         if (int st = tg_batch_create(device, &slot.batch)) {
@@ -762,8 +928,13 @@ void tg_server_destroy(tg_server* s) {
     }
     s->records.release();
     s->footprints.release();
+    s->culls.release();
     s->data.release();
     s->harmonics.release();
+    s->lists.release();
+    if (s->installStream != nullptr) {
+        cudaStreamDestroy(s->installStream);
+    }
     delete s;
 }
 
@@ -817,6 +988,9 @@ int tg_server_submit(tg_server* s, const tg_request* request) {
         p.lod = level_of(s, s->opt.point_spacing);
         p.cells = r.n_points;
         p.req.points = nullptr;
+        // The regions holding the points (each lists every crater reaching into it), found in
+        // a table over the regions of the points' bounding box.
+        const double side = level_spacing(s, p.lod) * s->opt.region_cells;
         double lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
         for (uint32_t i = 0; i < r.n_points; ++i) {
             lo[0] = std::min(lo[0], p.xy[2 * i]);
@@ -824,7 +998,35 @@ int tg_server_submit(tg_server* s, const tg_request* request) {
             hi[0] = std::max(hi[0], p.xy[2 * i]);
             hi[1] = std::max(hi[1], p.xy[2 * i + 1]);
         }
-        keys_for(s, p.lod, lo[0], lo[1], hi[0], hi[1], p.keys);
+        // Region (rx, ry) of the table as the device finds it: floor((x - x0) / side).
+        p.ix0 = int64_t(std::floor(lo[0] / side));
+        p.iy0 = int64_t(std::floor(lo[1] / side));
+        const double ox = double(p.ix0) * side, oy = double(p.iy0) * side;
+        const int64_t w = int64_t(std::floor((hi[0] - ox) / side)) + 1;
+        const int64_t h = int64_t(std::floor((hi[1] - oy) / side)) + 1;
+        if (w * h > (int64_t(1) << 22)) {
+            return fail(TG_ERROR_UNSUPPORTED, "request %llu: points span too many regions",
+                        (unsigned long long)r.id);
+        }
+        p.tw = uint32_t(w);
+        p.th = uint32_t(h);
+        p.occupied.assign(size_t(w * h), 0);
+        for (uint32_t i = 0; i < r.n_points; ++i) {
+            const int64_t rx = std::min(std::max<int64_t>(
+                                            int64_t(std::floor((p.xy[2 * i] - ox) / side)), 0),
+                                        w - 1);
+            const int64_t ry = std::min(std::max<int64_t>(
+                                            int64_t(std::floor((p.xy[2 * i + 1] - oy) / side)), 0),
+                                        h - 1);
+            p.occupied[size_t(ry * w + rx)] = 1;
+        }
+        for (int64_t ry = 0; ry < h; ++ry) {
+            for (int64_t rx = 0; rx < w; ++rx) {
+                if (p.occupied[size_t(ry * w + rx)]) {
+                    p.keys.push_back(RegionKey{p.lod, p.ix0 + rx, p.iy0 + ry});
+                }
+            }
+        }
     } else {
         return fail(TG_ERROR_ARGUMENT, "request kind is 0 (tile) or 1 (points)");
     }

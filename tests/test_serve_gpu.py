@@ -127,3 +127,38 @@ def test_served_device_outputs_equal_host_outputs(device):
         a = host.outputs[r.rid]
         b = dev.outputs[r.rid].cpu().numpy()
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), r.kind
+
+
+def test_served_points_equal_batched_points(device):
+    # Points read their regions' resident cell lists; the batch engine bins the same points
+    # against tg_crater_batch's records over their bounding box: the same heights.
+    from terraingen_b200.batch import POINT_SET, Batch, TileSet
+    from terraingen_b200.device import GridSpec
+    from terraingen_b200.serve import Server, dem_stack_options
+    from terraingen_b200.workloads import crater_batch
+
+    opts = dem_stack_options(slots=1)
+    rng = np.random.default_rng(4)
+    xy = np.stack([1.0e6 + 300.0 + 1500.0 * rng.random(3000),
+                   -2.0e3 + 1200.0 * rng.random(3000)], axis=1)
+    out = np.empty(len(xy), np.float32)
+    with Server(device, opts) as s:
+        s.submit_points(3, xy, out)
+        assert s.drain() == [3]
+    pixel = opts.point_spacing
+    x0, y1 = np.floor(xy[:, 0].min()) - 1, np.ceil(xy[:, 1].max()) + 1
+    w = int(np.ceil((xy[:, 0].max() + 1 - x0) / pixel))
+    h = int(np.ceil((y1 - xy[:, 1].min() + 1) / pixel))
+    kernel, records, data, foot = crater_batch(opts.craters, GridSpec(w, h, x0, y1, pixel))
+    sets = np.zeros(1, POINT_SET)
+    sets["point_count"], sets["crater_count"] = len(xy), len(records)
+    ts = TileSet(tiles=np.zeros(0, __import__("terraingen_b200.batch", fromlist=["TILE"]).TILE),
+                 fractals=opts._fractals, elevation=0.0, crater_kernel=kernel,
+                 crater_records=records, crater_data=data, crater_footprints=foot,
+                 boulders=np.zeros((0, 5)), point_sets=sets, points=xy)
+    want = np.zeros(ts.output_floats, np.float32)
+    with Batch(device) as b:
+        b.run(ts, want)
+        assert b.stats()["crater_pairs"] > 0
+    err = np.abs(out.astype(np.float64) - want).max()
+    assert err <= 1e-5, err
