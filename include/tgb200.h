@@ -261,6 +261,51 @@ int tg_device_counters(tg_device* device, uint64_t* counters, size_t n);
  * second. */
 int tg_measure_alu(tg_device* device, double* lane_ops_per_second);
 
+/* --- seams between chained sources ---------------------------------------------------------
+ * A SourceChain fills an earlier source's gaps from a later source and joins the two
+ * (ChainSeams, include/terraingen/sources/source_chain.h:24-62): the seam field is solved once on
+ * the lattice of the earlier source's grid widened by the seam's reach (SeamLattice,
+ * src/sources/source_chain.cpp:94) and read between its posts by Catmull-Rom interpolation. The
+ * reference solves it on the CPU only (detail::BuildSeamField, src/sources/seam_field.cpp:663);
+ * these replace it and FillGridGaps (source_chain.cpp:167). */
+
+/* mode: 0 none, 1 feather, 2 height, 3 slope (ChainSeamMode). levels, sweeps and
+ * coarsest_sweeps shape the multigrid preconditioner (4, 2 and 100 by default in the Python
+ * layer); tolerance is the conjugate gradients' stop, relative to the first residual (1e-10 as
+ * the reference when 0). */
+typedef struct tg_seam_options {
+    uint32_t mode;
+    uint32_t levels;
+    uint32_t sweeps;
+    uint32_t coarsest_sweeps;
+    double width;        /* Feather's band, in the lattice's units */
+    double decay_length; /* L of Height and Slope; they reach 3 L beyond a gap's edge */
+    double tolerance;
+} tg_seam_options;
+
+typedef struct tg_seam_stats {
+    uint32_t unknowns;   /* posts solved for */
+    uint32_t levels;     /* multigrid levels used */
+    uint32_t iterations; /* conjugate gradient iterations */
+    uint32_t reserved;
+} tg_seam_stats;
+
+/* The seam field on a width x height lattice of posts dx by dy apart (row 0 first), from the
+ * samples BuildSeamField starts from: `data` 1 where the earlier source has data, `difference` the
+ * earlier source's height minus the later one's where both have data (NaN elsewhere). `field`
+ * receives the correction at every post (0 where none). */
+int tg_seam_solve(tg_device* device, const uint8_t* data, const float* difference,
+                  uint32_t width, uint32_t height, double dx, double dy,
+                  const tg_seam_options* options, float* field, int memory, void* stream);
+/* What the calling thread's last tg_seam_solve did. */
+int tg_seam_stats_get(tg_seam_stats* stats);
+/* FillGridGaps: each cell of `heights` (on `grid`) holding no data takes `later` (the later
+ * source's height on the same grid) plus the field (posts on `lattice`) read at the cell's
+ * center by Catmull-Rom interpolation; cells where `later` has no data are left alone. */
+int tg_seam_fill(tg_device* device, const float* field, const tg_grid* lattice,
+                 const float* later, const tg_grid* grid, float* heights, tg_nodata nodata,
+                 int memory, void* stream);
+
 /* --- crater populations and kernel batches (host) ------------------------------------------ */
 
 /* A crater layer's population on a plane: a power-law density N(>D) = c D^-exponent per m^2 on

@@ -115,6 +115,50 @@ def diamond_square(lib: C.CDLL, posts: np.ndarray, post_grid, grid, fractal_dime
     return out, ms.value
 
 
+def seam(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: int,
+         width: float = 50.0, decay: float = 50.0) -> dict:
+    """The reference's seam between two rasters on one grid (tgref_seam): the lattice's size and
+    transform, the samples the solve starts from (data, difference) and the field's posts."""
+    earlier = np.ascontiguousarray(earlier, np.float32)
+    later = np.ascontiguousarray(later, np.float32)
+    h, w = earlier.shape
+    t = np.array(transform, np.float64)
+    pad = 64 + int(np.ceil(max(width, 3.0 * decay) / min(abs(t[1]), abs(t[5])))) + 3
+    capacity = (w + 2 * pad) * (h + 2 * pad)
+    data = np.zeros(capacity, np.uint8)
+    diff = np.zeros(capacity, np.float32)
+    field = np.zeros(capacity, np.float32)
+    lw, lh, lt, ms = C.c_uint32(), C.c_uint32(), np.zeros(6), C.c_double()
+    st = lib.tgref_seam(earlier.ctypes.data, later.ctypes.data, w, h, t.ctypes.data, mode,
+                        width, decay, C.addressof(lw), C.addressof(lh), lt.ctypes.data,
+                        data.ctypes.data, diff.ctypes.data, field.ctypes.data, capacity,
+                        C.addressof(ms))
+    if st != 0:
+        raise RuntimeError(f"tgref_seam failed ({st}): {lib.tgref_error().decode()}")
+    n = lw.value * lh.value
+    shape = (lh.value, lw.value)
+    return {"width": lw.value, "height": lh.value, "transform": lt,
+            "data": data[:n].reshape(shape), "difference": diff[:n].reshape(shape),
+            "field": field[:n].reshape(shape), "ms": ms.value}
+
+
+def chain(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: int,
+          width: float, decay: float, out_grid) -> np.ndarray:
+    """A SourceChain of the two rasters joined by `mode`, evaluated on `out_grid`."""
+    earlier = np.ascontiguousarray(earlier, np.float32)
+    later = np.ascontiguousarray(later, np.float32)
+    h, w = earlier.shape
+    t = np.array(transform, np.float64)
+    ot = np.array(out_grid.transform(), np.float64)
+    out = np.zeros((out_grid.height, out_grid.width), np.float32)
+    st = lib.tgref_chain(earlier.ctypes.data, later.ctypes.data, w, h, t.ctypes.data, mode,
+                         width, decay, out_grid.width, out_grid.height, ot.ctypes.data,
+                         out.ctypes.data)
+    if st != 0:
+        raise RuntimeError(f"tgref_chain failed: {lib.tgref_error().decode()}")
+    return out
+
+
 def config1_craters() -> dict:
     """The 257 x 257, 1 m crater scene (2000 craters expected over the extent, N(>D) ~ D^-2 on
     [2, 60] m, depth/diameter 0.2, rim 0.04 D, uniform ages over 1 Gyr, seed 1)."""
@@ -187,6 +231,13 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_ds.argtypes = [C.c_void_p, _U32, _U32, C.c_void_p, _D, _D, C.c_int, _U32, _U32, _U32,
                              C.c_void_p, C.c_uint, C.c_void_p, C.POINTER(_D)]
     lib.tgref_ds.restype = C.c_int
+    if hasattr(lib, "tgref_seam"):
+        P = C.c_void_p
+        lib.tgref_seam.argtypes = [P, P, _U32, _U32, P, C.c_int, _D, _D, P, P, P, P, P, P,
+                                   C.c_size_t, P]
+        lib.tgref_seam.restype = C.c_int
+        lib.tgref_chain.argtypes = [P, P, _U32, _U32, P, C.c_int, _D, _D, _U32, _U32, P, P]
+        lib.tgref_chain.restype = C.c_int
     return lib
 
 

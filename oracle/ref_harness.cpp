@@ -25,10 +25,16 @@
 #include "terraingen/layers/fade.h"
 #include "terraingen/sources/diamond_square.h"
 #include "terraingen/sources/raster_source.h"
+#include "terraingen/sources/source_chain.h"
+
+#include "sources/seam_field.h"
 #include "terraingen/util/log.h"
 
+#include <array>
 #include <chrono>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <string>
 #include <vector>
@@ -313,6 +319,134 @@ int tgref_ds(const float* posts, uint32_t pw, uint32_t ph, const double* postTra
         if (ms != nullptr) {
             *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
         }
+        std::memcpy(out, heights.Values().data(), heights.Values().size() * sizeof(float));
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// Two raster sources on `grid` (GDAL `transform`): `earlier` (NaN where it has no data) and
+/// `later`, cubic-upsampled RasterSources as a SourceChain joins them.
+struct SeamPair {
+    std::shared_ptr<const Source> earlier, later;
+    RasterGrid grid;
+};
+
+SeamPair MakeSeamPair(const float* earlier, const float* later, uint32_t w, uint32_t h,
+                      const double* transform) {
+    const RasterGrid grid{w, h, GeoTransform::FromGdal({transform[0], transform[1], transform[2],
+                                                        transform[3], transform[4], transform[5]})};
+    Raster<float> a(grid), b(grid);
+    std::memcpy(a.Values().data(), earlier, size_t(w) * h * sizeof(float));
+    std::memcpy(b.Values().data(), later, size_t(w) * h * sizeof(float));
+    a.SetNoData(std::numeric_limits<float>::quiet_NaN());
+    b.SetNoData(std::numeric_limits<float>::quiet_NaN());
+    return SeamPair{std::make_shared<RasterSource>(std::move(a)),
+                    std::make_shared<RasterSource>(std::move(b)), grid};
+}
+
+ChainSeams MakeSeams(int mode, double width, double decay) {
+    ChainSeams seams;
+    seams.mode = mode == 1   ? ChainSeamMode::Feather
+                 : mode == 2 ? ChainSeamMode::Height
+                 : mode == 3 ? ChainSeamMode::Slope
+                             : ChainSeamMode::None;
+    seams.width = width;
+    seams.decayLength = decay;
+    return seams;
+}
+
+/// The reference's seam between the two sources (detail::BuildSeamField, seam_field.cpp:663):
+/// the lattice (SeamLattice) size and GDAL transform, and at each of its posts (at most
+/// `capacity`) the samples the solve starts from - 1 where `earlier` has data, `earlier` minus
+/// `later` where both do (NaN elsewhere), filled 64 rows at a time as SampleSources does - and
+/// the field's value.
+int tgref_seam(const float* earlier, const float* later, uint32_t w, uint32_t h,
+               const double* transform, int mode, double width, double decay, uint32_t* lw,
+               uint32_t* lh, double* latticeTransform, uint8_t* data, float* difference,
+               float* field, size_t capacity, double* ms) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const SeamPair pair = MakeSeamPair(earlier, later, w, h, transform);
+        const ChainSeams seams = MakeSeams(mode, width, decay);
+        const RasterGrid lattice = SeamLattice(pair.grid, seams);
+        *lw = uint32_t(lattice.width);
+        *lh = uint32_t(lattice.height);
+        const std::array<double, 6> gdal = lattice.transform.ToGdal();
+        for (int i = 0; i < 6; ++i) {
+            latticeTransform[i] = gdal[size_t(i)];
+        }
+        const size_t posts = lattice.width * lattice.height;
+        if (posts > capacity) {
+            return 1;
+        }
+        const double spacing = pair.grid.PixelSize();
+        for (size_t top = 0; top < lattice.height; top += 64) {
+            const size_t rows = std::min<size_t>(64, lattice.height - top);
+            GeoTransform t = lattice.transform;
+            const Vec2d origin = lattice.transform.PixelToWorld(0.0, double(top));
+            t.originX = origin.x;
+            t.originY = origin.y;
+            Raster<float> above(RasterGrid{lattice.width, rows, t});
+            Raster<float> below(RasterGrid{lattice.width, rows, t});
+            pair.earlier->Fill(above, spacing);
+            pair.later->Fill(below, spacing);
+            for (size_t row = 0; row < rows; ++row) {
+                for (size_t col = 0; col < lattice.width; ++col) {
+                    const float a = above(col, row), b = below(col, row);
+                    const size_t k = (top + row) * lattice.width + col;
+                    data[k] = above.IsMissing(a) ? 0 : 1;
+                    difference[k] =
+                        !above.IsMissing(a) && !below.IsMissing(b) && std::isfinite(a) &&
+                                std::isfinite(b)
+                            ? float(double(a) - double(b))
+                            : std::numeric_limits<float>::quiet_NaN();
+                }
+            }
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        const detail::SeamField seam =
+            detail::BuildSeamField(*pair.earlier, *pair.later, pair.grid, seams);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (ms != nullptr) {
+            *ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        }
+        for (size_t row = 0; row < lattice.height; ++row) {
+            for (size_t col = 0; col < lattice.width; ++col) {
+                field[row * lattice.width + col] =
+                    seam.Post(std::ptrdiff_t(col), std::ptrdiff_t(row));
+            }
+        }
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// A SourceChain of the two sources joined by `mode` evaluated on an `ow` x `oh` grid
+/// (`outTransform`): the later source plus the seam where the earlier has no data
+/// (SourceChain::FillGridGaps, source_chain.cpp:167).
+int tgref_chain(const float* earlier, const float* later, uint32_t w, uint32_t h,
+                const double* transform, int mode, double width, double decay, uint32_t ow,
+                uint32_t oh, const double* outTransform, float* out) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const SeamPair pair = MakeSeamPair(earlier, later, w, h, transform);
+        auto chain = std::make_shared<SourceChain>(
+            std::vector<std::shared_ptr<const Source>>{pair.earlier, pair.later},
+            MakeSeams(mode, width, decay));
+        const Terrain terrain(Surface{}, chain, {});
+        EvaluationOptions evaluation;
+        evaluation.threads = 1;
+        evaluation.backend = Backend::Cpu;
+        const RasterGrid grid{ow, oh,
+                              GeoTransform::FromGdal({outTransform[0], outTransform[1],
+                                                      outTransform[2], outTransform[3],
+                                                      outTransform[4], outTransform[5]})};
+        const Raster<float> heights = terrain.Evaluate(grid, evaluation);
         std::memcpy(out, heights.Values().data(), heights.Values().size() * sizeof(float));
         return 0;
     } catch (const std::exception& error) {

@@ -144,6 +144,22 @@ SIGNATURES.update({
     "tg_batch_stats_get": [_P, C.POINTER(BatchStats)],
 })
 
+class SeamOptions(C.Structure):
+    _fields_ = [("mode", _U32), ("levels", _U32), ("sweeps", _U32), ("coarsest_sweeps", _U32),
+                ("width", _D), ("decay_length", _D), ("tolerance", _D)]
+
+
+class SeamStats(C.Structure):
+    _fields_ = [("unknowns", _U32), ("levels", _U32), ("iterations", _U32), ("reserved", _U32)]
+
+
+SIGNATURES.update({
+    "tg_seam_solve": [_P, _P, _P, _U32, _U32, _D, _D, C.POINTER(SeamOptions), _P, _I, _P],
+    "tg_seam_stats_get": [C.POINTER(SeamStats)],
+    "tg_seam_fill": [_P, _P, C.POINTER(Grid), _P, C.POINTER(Grid), _P, NoData, _I, _P],
+})
+
+
 class ServerOptions(C.Structure):
     _fields_ = [("fractals", _P), ("n_fractals", _U32), ("elevation", _F),
                 ("craters", Population), ("shaping", Shaping), ("base_spacing", _D),

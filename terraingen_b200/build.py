@@ -32,7 +32,7 @@ UNITS = {
     "craters.cu": [],
     "boulders.cu": [],
     "diamond_square.cu": ["-fmad=false"],
-    "seams.cu": [],
+    "seams.cu": ["-fmad=false"],
     "batch.cu": ["-fmad=false"],
     "batch_api.cu": [],
     "serve.cu": [],

@@ -1,0 +1,1203 @@
+// The seam a source chain adds to a later source in an earlier one's gaps
+// (detail::BuildSeamField, src/sources/seam_field.cpp:663-710; SourceChain::FillGridGaps,
+// src/sources/source_chain.cpp:167-192), on the device.
+//
+// From the samples on the seam lattice (1 where the earlier source has data, earlier minus later
+// where both do):
+//   1. the band: posts with data within 3 posts of a gap keep their difference (NearGaps);
+//   2. the chamfer distance from each post to the nearest post with data (DataDistances), in the
+//      reference's own relaxation order: rows top down then bottom up, each row as a recurrence
+//      along it, so every distance (and carried value) has the reference's float bits; values
+//      beyond the reach are never read back, so they are dropped and each thread runs a short
+//      window of the recurrence;
+//   3a. Feather: gap posts within `width` take the carried difference faded by a smoothstep;
+//   3b. Height / Slope: gap posts within the reach (3 decay lengths, away from the lattice's 3
+//      border posts) are solved for (-Laplacian + 1/L^2) d = 0, or its square, with the band's
+//      values fixed: conjugate gradients in FP64 preconditioned by a symmetric multigrid V-cycle
+//      (damped Jacobi smoothing in FP32, the coarsest level's residual and sweeps in FP64) over
+//      the unknowns compacted on each level. The reference solves the same system per connected
+//      region with Gauss-Seidel smoothing; the converged field is the same.
+// The field is read between posts by Catmull-Rom interpolation (SeamField::At) when a grid's
+// gaps are filled from the later source.
+//
+// Built with -fmad=false: the distances and the interpolation round as the reference's
+// -ffp-contract=off build does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/tgb200.h"
+#include "api_internal.h"
+#include "kernels.h"
+
+using namespace tgb;
+using namespace tgb::api;
+
+namespace {
+
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kBandPosts = 3;     // seam_field.cpp:29
+constexpr int kBorderPosts = 3;   // seam_field.cpp:32
+constexpr int kSegment = 32;      // cells of a row a thread of the distance passes writes
+constexpr int kMaxLevels = 8;
+
+// --- band and fixed values ---------------------------------------------------------------
+
+__global__ void count_data_kernel(const uint8_t* __restrict__ data, size_t n,
+                                  unsigned long long* __restrict__ count) {
+    unsigned long long mine = 0;
+    for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += size_t(gridDim.x) * blockDim.x) {
+        mine += data[k] != 0 ? 1u : 0u;
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        mine += __shfl_down_sync(0xffffffffu, mine, d);
+    }
+    if ((threadIdx.x & 31u) == 0 && mine > 0) {
+        atomicAdd(count, mine);
+    }
+}
+
+// NearGaps (seam_field.cpp:117): 1 where a post without data lies within `radius` columns...
+__global__ void gaps_across_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
+                                   int radius, uint8_t* __restrict__ across) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= size_t(w) * h) {
+        return;
+    }
+    const int col = int(k % w);
+    const size_t row0 = k - size_t(col);
+    uint8_t any = 0;
+    for (int c = max(0, col - radius); c <= min(int(w) - 1, col + radius); ++c) {
+        any |= data[row0 + size_t(c)] == 0 ? 1 : 0;
+    }
+    across[k] = any;
+}
+
+// ... then of those within `radius` rows; the posts with data there hold their difference.
+__global__ void band_kernel(const uint8_t* __restrict__ data, const float* __restrict__ difference,
+                            const uint8_t* __restrict__ across, uint32_t w, uint32_t h,
+                            int radius, float* __restrict__ field) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= size_t(w) * h) {
+        return;
+    }
+    const int row = int(k / w);
+    const size_t col = k % w;
+    uint8_t near = 0;
+    for (int r = max(0, row - radius); r <= min(int(h) - 1, row + radius); ++r) {
+        near |= across[size_t(r) * w + col];
+    }
+    const float d = difference[k];
+    field[k] = data[k] != 0 && near != 0 && !isnan(d) ? d : 0.0f;
+}
+
+// --- distances (DataDistances, seam_field.cpp:151) -----------------------------------------
+
+struct DistanceRow {
+    const uint8_t* data;
+    const float* field;    // the carried value of a post with data (Feather)
+    float* distance;       // forward pass output, backward pass input
+    float* carried;        // optional, as distance
+    float* distanceOut;    // backward pass output
+    float* carriedOut;
+    uint32_t w, h;
+    float dx, dy, diagonal;
+    float cap;       // distances above it are dropped (+inf): they are never read back
+    int window;      // cells of recurrence before a thread's segment
+};
+
+// The forward pass over row `row`: each post without data relaxes from its left neighbor, then
+// the posts above, up-left and up-right (strictly smaller wins, in that order), the row above
+// already final. Each thread writes kSegment posts, running the recurrence along the row from
+// `window` posts before them.
+__global__ void distance_forward_kernel(const DistanceRow p, uint32_t row) {
+    const int c0 = int(blockIdx.x * blockDim.x + threadIdx.x) * kSegment;
+    if (c0 >= int(p.w)) {
+        return;
+    }
+    const int w = int(p.w);
+    const size_t base = size_t(row) * p.w;
+    const float inf = INFINITY;
+    float left = inf, leftCarried = 0.0f;
+    const int end = min(w, c0 + kSegment);
+    for (int c = max(0, c0 - p.window); c < end; ++c) {
+        const size_t k = base + size_t(c);
+        float d, carried = p.data[k] != 0 && p.carried != nullptr ? p.field[k] : 0.0f;
+        if (p.data[k] != 0) {
+            d = 0.0f;
+        } else {
+            d = inf;
+            if (c > 0) {
+                const float t = left + p.dx;
+                if (t < d) {
+                    d = t;
+                    carried = leftCarried;
+                }
+            }
+            if (row > 0) {
+                const size_t up = k - p.w;
+                float t = p.distance[up] + p.dy;
+                if (t < d) {
+                    d = t;
+                    if (p.carried) carried = p.carried[up];
+                }
+                if (c > 0) {
+                    t = p.distance[up - 1] + p.diagonal;
+                    if (t < d) {
+                        d = t;
+                        if (p.carried) carried = p.carried[up - 1];
+                    }
+                }
+                if (c + 1 < w) {
+                    t = p.distance[up + 1] + p.diagonal;
+                    if (t < d) {
+                        d = t;
+                        if (p.carried) carried = p.carried[up + 1];
+                    }
+                }
+            }
+            if (d > p.cap) {
+                d = inf;
+            }
+        }
+        if (c >= c0) {
+            p.distance[k] = d;
+            if (p.carried) {
+                p.carried[k] = carried;
+            }
+        }
+        left = d;
+        leftCarried = carried;
+    }
+}
+
+// The backward pass over row `row`, right to left: a post without data keeps its forward value
+// unless its right neighbor, then the posts below, down-right and down-left give a strictly
+// smaller one. Forward values are read from `distance`, the rows below from `distanceOut`.
+__global__ void distance_backward_kernel(const DistanceRow p, uint32_t row) {
+    const int w = int(p.w);
+    const int segment = int(blockIdx.x * blockDim.x + threadIdx.x);
+    const int hi = w - 1 - segment * kSegment;  // this thread writes [lo, hi]
+    if (hi < 0) {
+        return;
+    }
+    const int lo = max(0, hi - kSegment + 1);
+    const size_t base = size_t(row) * p.w;
+    const float inf = INFINITY;
+    float right = inf, rightCarried = 0.0f;
+    for (int c = min(w - 1, hi + p.window); c >= lo; --c) {
+        const size_t k = base + size_t(c);
+        float d = p.distance[k];
+        float carried = p.carried != nullptr ? p.carried[k] : 0.0f;
+        if (p.data[k] == 0) {
+            if (c + 1 < w) {
+                const float t = right + p.dx;
+                if (t < d) {
+                    d = t;
+                    carried = rightCarried;
+                }
+            }
+            if (row + 1 < p.h) {
+                const size_t down = k + p.w;
+                float t = p.distanceOut[down] + p.dy;
+                if (t < d) {
+                    d = t;
+                    if (p.carried) carried = p.carriedOut[down];
+                }
+                if (c + 1 < w) {
+                    t = p.distanceOut[down + 1] + p.diagonal;
+                    if (t < d) {
+                        d = t;
+                        if (p.carried) carried = p.carriedOut[down + 1];
+                    }
+                }
+                if (c > 0) {
+                    t = p.distanceOut[down - 1] + p.diagonal;
+                    if (t < d) {
+                        d = t;
+                        if (p.carried) carried = p.carriedOut[down - 1];
+                    }
+                }
+            }
+            if (d > p.cap) {
+                d = inf;
+            }
+        }
+        if (c <= hi) {
+            p.distanceOut[k] = d;
+            if (p.carried) {
+                p.carriedOut[k] = carried;
+            }
+        }
+        right = d;
+        rightCarried = carried;
+    }
+}
+
+// Feather (seam_field.cpp:218): gap posts within `width` take the carried difference, faded by a
+// smoothstep from 1 at the edge to 0 at `width`.
+__global__ void feather_kernel(const uint8_t* __restrict__ data,
+                               const float* __restrict__ distance,
+                               const float* __restrict__ carried, size_t n, double width,
+                               float* __restrict__ field) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n || data[k] != 0 || !(distance[k] < width)) {
+        return;
+    }
+    const double t = double(distance[k]) / width;
+    const double weight = 1.0 - t * t * (3.0 - 2.0 * t);
+    field[k] = float(weight * double(carried[k]));
+}
+
+// --- unknowns and the level hierarchy ------------------------------------------------------
+
+// 1 at the posts solved for: no data, off the border, within the reach.
+__global__ void unknown_kernel(const uint8_t* __restrict__ data,
+                               const float* __restrict__ distance, uint32_t w, uint32_t h,
+                               double reach, uint32_t* __restrict__ flags) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= size_t(w) * h) {
+        return;
+    }
+    const uint32_t col = uint32_t(k % w), row = uint32_t(k / w);
+    const bool inside = col >= uint32_t(kBorderPosts) && col + kBorderPosts < w &&
+                        row >= uint32_t(kBorderPosts) && row + kBorderPosts < h;
+    flags[k] = data[k] == 0 && inside && double(distance[k]) <= reach ? 1u : 0u;
+}
+
+// A coarser level's posts: the parents (col / 2, row / 2) of the finer level's unknowns.
+__global__ void coarsen_kernel(const uint32_t* __restrict__ finePos, uint32_t n, uint32_t fineW,
+                               uint32_t coarseW, uint32_t* __restrict__ coarseFlags) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) {
+        return;
+    }
+    const uint32_t p = finePos[k];
+    coarseFlags[size_t(p / fineW / 2) * coarseW + (p % fineW) / 2] = 1u;
+}
+
+// Flags (0 / 1) scanned in place into offsets: the compact index of each flagged post, its
+// position, and ~0u at the others. `scanned` holds the exclusive scan, `flags` the marks.
+__global__ void compact_kernel(const uint32_t* __restrict__ scanned,
+                               const uint8_t* __restrict__ marks, size_t n,
+                               uint32_t* __restrict__ index, uint32_t* __restrict__ position) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) {
+        return;
+    }
+    if (marks[k] != 0) {
+        position[scanned[k]] = uint32_t(k);
+        index[k] = scanned[k];
+    } else {
+        index[k] = kNone;
+    }
+}
+
+__global__ void flags_to_marks_kernel(const uint32_t* __restrict__ flags, size_t n,
+                                      uint8_t* __restrict__ marks) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k < n) {
+        marks[k] = flags[k] != 0 ? 1 : 0;
+    }
+}
+
+// One level: its lattice, its unknowns and the operator's weights.
+struct LevelView {
+    uint32_t w, h, n;
+    const uint32_t* index;     // [w * h] compact index or ~0u
+    const uint32_t* position;  // [n] post of each unknown
+    double cx, cy, center;     // 1/dx^2, 1/dy^2, 2 cx + 2 cy + 1/L^2
+    double diagonal;           // the operator's center weight
+};
+
+// u at post (col + dc, row + dr), 0 off the unknowns.
+template <typename T>
+__device__ __forceinline__ T at(const LevelView& L, const T* u, int col, int row, int dc, int dr) {
+    const int c = col + dc, r = row + dr;
+    if (c < 0 || r < 0 || c >= int(L.w) || r >= int(L.h)) {
+        return T(0);
+    }
+    const uint32_t j = L.index[size_t(r) * L.w + uint32_t(c)];
+    return j == kNone ? T(0) : u[j];
+}
+
+// The operator at unknown k of u (0 off the unknowns): B = -Laplacian + 1/L^2 on 5 points
+// (order 1), or B applied twice on 13 points (order 2), as ApplyScreened / Apply
+// (seam_field.cpp:389-407).
+template <int kOrder, typename T>
+__device__ __forceinline__ double apply_at(const LevelView& L, const T* u, uint32_t k) {
+    const uint32_t p = L.position[k];
+    const int col = int(p % L.w), row = int(p / L.w);
+    const double cx = L.cx, cy = L.cy, c0 = L.center;
+    const double sx = double(at(L, u, col, row, -1, 0)) + double(at(L, u, col, row, 1, 0));
+    const double sy = double(at(L, u, col, row, 0, -1)) + double(at(L, u, col, row, 0, 1));
+    if (kOrder == 1) {
+        return c0 * double(u[k]) - cx * sx - cy * sy;
+    }
+    const double s2x = double(at(L, u, col, row, -2, 0)) + double(at(L, u, col, row, 2, 0));
+    const double s2y = double(at(L, u, col, row, 0, -2)) + double(at(L, u, col, row, 0, 2));
+    const double sd = double(at(L, u, col, row, -1, -1)) + double(at(L, u, col, row, 1, -1)) +
+                      double(at(L, u, col, row, -1, 1)) + double(at(L, u, col, row, 1, 1));
+    return L.diagonal * double(u[k]) - 2.0 * c0 * (cx * sx + cy * sy) + cx * cx * s2x +
+           cy * cy * s2y + 2.0 * cx * cy * sd;
+}
+
+// The right-hand side: minus the operator of the fixed values (the field at every post that is
+// not an unknown, 0 at the unknowns).
+template <int kOrder>
+__global__ void rhs_kernel(const LevelView L, const float* __restrict__ field,
+                           double* __restrict__ rhs) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= L.n) {
+        return;
+    }
+    const uint32_t p = L.position[k];
+    const int col = int(p % L.w), row = int(p / L.w);
+    auto f = [&](int dc, int dr) -> double {
+        const size_t q = size_t(row + dr) * L.w + uint32_t(col + dc);
+        return L.index[q] == kNone ? double(field[q]) : 0.0;
+    };
+    const double cx = L.cx, cy = L.cy, c0 = L.center;
+    const double sx = f(-1, 0) + f(1, 0), sy = f(0, -1) + f(0, 1);
+    double a;
+    if (kOrder == 1) {
+        a = -cx * sx - cy * sy;
+    } else {
+        const double s2x = f(-2, 0) + f(2, 0), s2y = f(0, -2) + f(0, 2);
+        const double sd = f(-1, -1) + f(1, -1) + f(-1, 1) + f(1, 1);
+        a = -2.0 * c0 * (cx * sx + cy * sy) + cx * cx * s2x + cy * cy * s2y + 2.0 * cx * cy * sd;
+    }
+    rhs[k] = -a;
+}
+
+// Damped Jacobi: xn = x + omega (b - A x) / diagonal; from x = 0 when `x` is null.
+template <int kOrder, typename T>
+__global__ void jacobi_kernel(const LevelView L, const T* __restrict__ b, const T* __restrict__ x,
+                              T* __restrict__ xn, double omega) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= L.n) {
+        return;
+    }
+    if (x == nullptr) {
+        xn[k] = T(omega * double(b[k]) / L.diagonal);
+        return;
+    }
+    const double r = double(b[k]) - apply_at<kOrder>(L, x, k);
+    xn[k] = T(double(x[k]) + omega * r / L.diagonal);
+}
+
+template <int kOrder, typename T>
+__global__ void residual_kernel(const LevelView L, const T* __restrict__ b,
+                                const T* __restrict__ x, T* __restrict__ r) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < L.n) {
+        r[k] = T(double(b[k]) - apply_at<kOrder>(L, x, k));
+    }
+}
+
+// The operator applied to a direction (FP64, for the conjugate gradients).
+template <int kOrder>
+__global__ void apply_kernel(const LevelView L, const double* __restrict__ u,
+                             double* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < L.n) {
+        out[k] = apply_at<kOrder>(L, u, k);
+    }
+}
+
+// Restriction, gathered: coarse unknown (C, R) takes 1/4 of each fine residual whose parent or
+// parent's neighbor it is, weighted 3/4 or 1/4 per axis (the transfer weights 9/16, 3/16, 3/16,
+// 1/16, seam_field.cpp:56).
+template <typename Tf, typename Tc>
+__global__ void restrict_kernel(const LevelView F, const LevelView Cl, const Tf* __restrict__ r,
+                                Tc* __restrict__ b) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Cl.n) {
+        return;
+    }
+    const uint32_t p = Cl.position[k];
+    const int C = int(p % Cl.w), R = int(p / Cl.w);
+    const double axis[4] = {0.25, 0.75, 0.75, 0.25};  // fine 2C-1, 2C, 2C+1, 2C+2
+    double sum = 0.0;
+    for (int j = 0; j < 4; ++j) {
+        const int fy = 2 * R - 1 + j;
+        if (fy < 0 || fy >= int(F.h)) {
+            continue;
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int fx = 2 * C - 1 + i;
+            if (fx < 0 || fx >= int(F.w)) {
+                continue;
+            }
+            const uint32_t q = F.index[size_t(fy) * F.w + uint32_t(fx)];
+            if (q != kNone) {
+                sum += 0.25 * axis[i] * axis[j] * double(r[q]);
+            }
+        }
+    }
+    b[k] = Tc(sum);
+}
+
+// Prolongation: each fine unknown adds its parent's correction and its parent's neighbors' across
+// its column, its row and diagonally (Link, seam_field.cpp:367).
+template <typename Tc, typename Tf>
+__global__ void prolong_kernel(const LevelView F, const LevelView Cl, const Tc* __restrict__ xc,
+                               Tf* __restrict__ x) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= F.n) {
+        return;
+    }
+    const uint32_t p = F.position[k];
+    const int col = int(p % F.w), row = int(p / F.w);
+    const int pc = col / 2, pr = row / 2;
+    const int ac = pc + (col % 2 == 1 ? 1 : -1), ar = pr + (row % 2 == 1 ? 1 : -1);
+    const double correction = 0.5625 * double(at(Cl, xc, pc, pr, 0, 0)) +
+                              0.1875 * double(at(Cl, xc, ac, pr, 0, 0)) +
+                              0.1875 * double(at(Cl, xc, pc, ar, 0, 0)) +
+                              0.0625 * double(at(Cl, xc, ac, ar, 0, 0));
+    x[k] = Tf(double(x[k]) + correction);
+}
+
+// --- vectors -------------------------------------------------------------------------------
+
+constexpr int kDotBlocks = 512;
+
+// Partial sums of a . b (and of c . d when given) per block; summed by dot_finish_kernel in a
+// fixed order, so every run gives the same bits.
+__global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                           const double* __restrict__ c, const double* __restrict__ d, uint32_t n,
+                           double* __restrict__ partial) {
+    __shared__ double s0[256], s1[256];
+    double x = 0.0, y = 0.0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        x += a[k] * b[k];
+        if (c != nullptr) {
+            y += c[k] * d[k];
+        }
+    }
+    s0[threadIdx.x] = x;
+    s1[threadIdx.x] = y;
+    __syncthreads();
+    for (int half = 128; half > 0; half >>= 1) {
+        if (int(threadIdx.x) < half) {
+            s0[threadIdx.x] += s0[threadIdx.x + half];
+            s1[threadIdx.x] += s1[threadIdx.x + half];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = s0[0];
+        partial[kDotBlocks + blockIdx.x] = s1[0];
+    }
+}
+
+__global__ void dot_finish_kernel(const double* __restrict__ partial, double* __restrict__ out) {
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int i = 0; i < kDotBlocks; ++i) {
+            x += partial[i];
+            y += partial[kDotBlocks + i];
+        }
+        out[0] = x;
+        out[1] = y;
+    }
+}
+
+// x += step p, r -= step ap.
+__global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
+                                 const double* __restrict__ p, const double* __restrict__ ap,
+                                 uint32_t n, double step) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        x[k] += step * p[k];
+        r[k] -= step * ap[k];
+    }
+}
+
+// p = z + ratio p.
+__global__ void cg_direction_kernel(double* __restrict__ p, const double* __restrict__ z,
+                                    uint32_t n, double ratio) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        p[k] = z[k] + ratio * p[k];
+    }
+}
+
+template <typename A, typename B>
+__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        out[k] = B(in[k]);
+    }
+}
+
+__global__ void scatter_solution_kernel(const uint32_t* __restrict__ position,
+                                        const double* __restrict__ x, uint32_t n,
+                                        float* __restrict__ field) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        field[position[k]] = float(x[k]);
+    }
+}
+
+// --- reading the field (SeamField::At, seam_field.cpp:644) ---------------------------------
+
+// The cubic convolution kernel (a = -0.5) of the reference's resampling (CubicWeight,
+// src/raster/resample.cpp:20).
+__device__ __forceinline__ double cubic_weight(double x) {
+    const double a = -0.5;
+    x = fabs(x);
+    if (x <= 1.0) {
+        return ((a + 2.0) * x - (a + 3.0)) * x * x + 1.0;
+    }
+    if (x < 2.0) {
+        return ((a * x - 5.0 * a) * x + 8.0 * a) * x - 4.0 * a;
+    }
+    return 0.0;
+}
+
+struct SeamRead {
+    const float* field;
+    uint32_t w, h;          // the lattice
+    double originX, pixelWidth, rowRotation, originY, colRotation, pixelHeight;
+    bool set;               // any post set
+};
+
+__device__ __forceinline__ double post(const SeamRead& s, double col, double row) {
+    const long long c = (long long)col, r = (long long)row;
+    if (c < 0 || r < 0 || c >= (long long)s.w || r >= (long long)s.h) {
+        return 0.0;
+    }
+    return double(s.field[size_t(r) * s.w + size_t(c)]);
+}
+
+// The correction at (x, y): Catmull-Rom over the 4 x 4 posts around it, taps of zero weight
+// skipped, as InterpolateLattice (src/raster/kernels.h:62) with ResampleMethod::Cubic.
+__device__ double seam_at(const SeamRead& s, double x, double y) {
+    if (!s.set) {
+        return 0.0;
+    }
+    // GeoTransform::WorldToPixel (include/terraingen/raster/geo_transform.h:70)
+    const double det = s.pixelWidth * s.pixelHeight - s.rowRotation * s.colRotation;
+    const double dx = x - s.originX, dy = y - s.originY;
+    const double px = (dx * s.pixelHeight - dy * s.rowRotation) / det;
+    const double py = (dy * s.pixelWidth - dx * s.colRotation) / det;
+    const double fx = px - 0.5, fy = py - 0.5;
+    const double left = floor(fx), top = floor(fy);
+    if (!(left >= -2.0 && top >= -2.0 && left <= double(s.w) && top <= double(s.h))) {
+        return 0.0;
+    }
+    double wx[4], wy[4];
+    for (int i = -1; i <= 2; ++i) {
+        wx[i + 1] = cubic_weight((fx - left) - i);
+        wy[i + 1] = cubic_weight((fy - top) - i);
+    }
+    double sum = 0.0;
+    for (int j = -1; j <= 2; ++j) {
+        for (int i = -1; i <= 2; ++i) {
+            if (wx[i + 1] * wy[j + 1] == 0.0) {
+                continue;
+            }
+            sum += wx[i + 1] * wy[j + 1] * post(s, left + i, top + j);
+        }
+    }
+    return double(float(sum));
+}
+
+// FillGridGaps: each cell holding no data takes the later source's height plus the correction
+// at its center (unchanged where the correction is 0; still no data where the later source has
+// none).
+// A cell is missing when it is not finite or, with a no-data value, equal to it
+// (Raster::IsMissing, include/terraingen/raster/raster.h:167).
+__global__ void seam_fill_kernel(const SeamRead s, const Grid g, const float* __restrict__ later,
+                                 const NoData nodata, float* __restrict__ heights) {
+    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= g.width) {
+        return;
+    }
+    for (uint32_t row = blockIdx.y; row < g.height; row += gridDim.y) {
+        const size_t k = size_t(row) * g.width + col;
+        const float cell = heights[k];
+        const float value = later[k];
+        const bool missing = !isfinite(cell) || (nodata.mode == 2u && cell == nodata.value);
+        const bool laterMissing = !isfinite(value) || (nodata.mode == 2u && value == nodata.value);
+        if (!missing || laterMissing) {
+            continue;
+        }
+        const double x = g.originX + (double(col) + 0.5) * g.pixelWidth +
+                         (double(row) + 0.5) * g.rowRotation;
+        const double y = g.originY + (double(col) + 0.5) * g.colRotation +
+                         (double(row) + 0.5) * g.pixelHeight;
+        const double correction = seam_at(s, x, y);
+        heights[k] = correction == 0.0 ? value : float(double(value) + correction);
+    }
+}
+
+uint32_t blocks_for(size_t n, uint32_t threads = 256) {
+    return uint32_t((n + threads - 1) / threads);
+}
+
+// A level's device arrays.
+struct Level {
+    LevelView view{};
+    Buffer index, position, x, b, t;  // x, b, t: float (double on the coarsest level)
+};
+
+struct Work {
+    Buffer marks, flags, scan, distance, carried, distance2, carried2, count, partial, dots;
+    Buffer cgX, cgR, cgP, cgAp, cgZ, rhs;
+    Level levels[kMaxLevels];
+    ~Work() {
+        for (Buffer* b : {&marks, &flags, &scan, &distance, &carried, &distance2, &carried2,
+                          &count, &partial, &dots,
+                          &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs}) {
+            b->release();
+        }
+        for (Level& l : levels) {
+            l.index.release();
+            l.position.release();
+            l.x.release();
+            l.b.release();
+            l.t.release();
+        }
+    }
+};
+
+// Compacts `flags` (0 / 1 per post of a w x h lattice) into the level's index and positions.
+int compact(Work& wk, Level& level, uint32_t w, uint32_t h, cudaStream_t s) {
+    const size_t n = size_t(w) * h;
+    if (n >= 0xffffffffull) {
+        return fail(TG_ERROR_UNSUPPORTED, "a seam lattice holds fewer than 2^32 posts");
+    }
+    uint32_t* flags = static_cast<uint32_t*>(wk.flags.ptr);
+    TG_CUDA(wk.marks.reserve(n), "allocation");
+    flags_to_marks_kernel<<<blocks_for(n), 256, 0, s>>>(flags, n,
+                                                       static_cast<uint8_t*>(wk.marks.ptr));
+    TG_CUDA(wk.scan.reserve(scan_scratch_words(uint32_t(n)) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(launch_exclusive_scan(flags, uint32_t(n), static_cast<uint32_t*>(wk.scan.ptr), s),
+            "scan");
+    uint32_t total = 0;
+    TG_CUDA(cudaMemcpyAsync(&total, flags + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    TG_CUDA(level.index.reserve(n * sizeof(uint32_t)), "allocation");
+    TG_CUDA(level.position.reserve(std::max<size_t>(total, 1) * sizeof(uint32_t)), "allocation");
+    compact_kernel<<<blocks_for(n), 256, 0, s>>>(flags, static_cast<const uint8_t*>(wk.marks.ptr),
+                                                n, static_cast<uint32_t*>(level.index.ptr),
+                                                static_cast<uint32_t*>(level.position.ptr));
+    TG_CUDA(cudaGetLastError(), "compact launch");
+    level.view.w = w;
+    level.view.h = h;
+    level.view.n = total;
+    level.view.index = static_cast<const uint32_t*>(level.index.ptr);
+    level.view.position = static_cast<const uint32_t*>(level.position.ptr);
+    return TG_OK;
+}
+
+struct Solver {
+    Work* wk;
+    int levels;
+    int order;
+    cudaStream_t s;
+    double omega;
+    int sweeps, coarsest;
+};
+
+template <int kOrder>
+cudaError_t jacobi(const LevelView& L, const void* b, const void* x, void* xn, double omega,
+                   bool coarsest, cudaStream_t s) {
+    if (coarsest) {
+        jacobi_kernel<kOrder, double><<<blocks_for(L.n), 256, 0, s>>>(
+            L, static_cast<const double*>(b), static_cast<const double*>(x),
+            static_cast<double*>(xn), omega);
+    } else {
+        jacobi_kernel<kOrder, float><<<blocks_for(L.n), 256, 0, s>>>(
+            L, static_cast<const float*>(b), static_cast<const float*>(x),
+            static_cast<float*>(xn), omega);
+    }
+    return cudaGetLastError();
+}
+
+// The V-cycle from level `d` (VCycle, seam_field.cpp:423): an approximate solution of the level's
+// operator for its b, from 0, into its x.
+template <int kOrder>
+int vcycle(Solver& sv, int d) {
+    Level& L = sv.wk->levels[d];
+    const bool last = d + 1 == sv.levels;
+    if (L.view.n == 0) {
+        return TG_OK;
+    }
+    const int sweeps = last ? sv.coarsest : sv.sweeps;
+    // Sweeps alternate between x and t; the first starts from 0.
+    void* cur = nullptr;
+    for (int i = 0; i < sweeps; ++i) {
+        void* next = (i % 2 == 0) ? L.x.ptr : L.t.ptr;
+        TG_CUDA(jacobi<kOrder>(L.view, L.b.ptr, cur, next, sv.omega, last, sv.s), "jacobi");
+        cur = next;
+    }
+    if (cur != L.x.ptr) {
+        TG_CUDA(cudaMemcpyAsync(L.x.ptr, cur, size_t(L.view.n) * (last ? 8 : 4),
+                                cudaMemcpyDeviceToDevice, sv.s),
+                "copy");
+    }
+    if (last) {
+        return TG_OK;
+    }
+    Level& C = sv.wk->levels[d + 1];
+    const bool coarseLast = d + 2 == sv.levels;
+    // residual into t, restricted into the coarse b
+    residual_kernel<kOrder, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+        L.view, static_cast<const float*>(L.b.ptr), static_cast<const float*>(L.x.ptr),
+        static_cast<float*>(L.t.ptr));
+    if (coarseLast) {
+        restrict_kernel<float, double><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
+            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<double*>(C.b.ptr));
+    } else {
+        restrict_kernel<float, float><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
+            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<float*>(C.b.ptr));
+    }
+    TG_CUDA(cudaGetLastError(), "restrict launch");
+    if (int st = vcycle<kOrder>(sv, d + 1)) {
+        return st;
+    }
+    if (coarseLast) {
+        prolong_kernel<double, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+            L.view, C.view, static_cast<const double*>(C.x.ptr), static_cast<float*>(L.x.ptr));
+    } else {
+        prolong_kernel<float, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+            L.view, C.view, static_cast<const float*>(C.x.ptr), static_cast<float*>(L.x.ptr));
+    }
+    TG_CUDA(cudaGetLastError(), "prolong launch");
+    for (int i = 0; i < sv.sweeps; ++i) {
+        TG_CUDA(jacobi<kOrder>(L.view, L.b.ptr, i % 2 == 0 ? L.x.ptr : L.t.ptr,
+                               i % 2 == 0 ? L.t.ptr : L.x.ptr, sv.omega, false, sv.s),
+                "jacobi");
+    }
+    if (sv.sweeps % 2 == 1) {
+        TG_CUDA(cudaMemcpyAsync(L.x.ptr, L.t.ptr, size_t(L.view.n) * 4, cudaMemcpyDeviceToDevice,
+                                sv.s),
+                "copy");
+    }
+    return TG_OK;
+}
+
+// z = M r: the V-cycle on r (FP64 in, through FP32 levels, FP64 out).
+template <int kOrder>
+int precondition(Solver& sv, const double* r, double* z) {
+    Level& L0 = sv.wk->levels[0];
+    const uint32_t n = L0.view.n;
+    if (sv.levels == 1) {
+        TG_CUDA(cudaMemcpyAsync(L0.b.ptr, r, size_t(n) * 8, cudaMemcpyDeviceToDevice, sv.s),
+                "copy");
+        if (int st = vcycle<kOrder>(sv, 0)) {
+            return st;
+        }
+        TG_CUDA(cudaMemcpyAsync(z, L0.x.ptr, size_t(n) * 8, cudaMemcpyDeviceToDevice, sv.s),
+                "copy");
+        return TG_OK;
+    }
+    convert_kernel<double, float><<<blocks_for(n), 256, 0, sv.s>>>(
+        r, static_cast<float*>(L0.b.ptr), n);
+    if (int st = vcycle<kOrder>(sv, 0)) {
+        return st;
+    }
+    convert_kernel<float, double><<<blocks_for(n), 256, 0, sv.s>>>(
+        static_cast<const float*>(L0.x.ptr), z, n);
+    TG_CUDA(cudaGetLastError(), "convert launch");
+    return TG_OK;
+}
+
+// a . b and c . d (c may be null), read back.
+int dots(Solver& sv, const double* a, const double* b, const double* c, const double* d,
+         uint32_t n, double out[2]) {
+    dot_kernel<<<kDotBlocks, 256, 0, sv.s>>>(a, b, c, d, n,
+                                             static_cast<double*>(sv.wk->partial.ptr));
+    dot_finish_kernel<<<1, 32, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
+                                          static_cast<double*>(sv.wk->dots.ptr));
+    TG_CUDA(cudaGetLastError(), "dot launch");
+    TG_CUDA(cudaMemcpyAsync(out, sv.wk->dots.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                            sv.s),
+            "copy to host");
+    TG_CUDA(cudaStreamSynchronize(sv.s), "synchronize");
+    return TG_OK;
+}
+
+// PreconditionedCg (seam_field.cpp:497) on the finest level: the correction at the unknowns.
+template <int kOrder>
+int solve(Solver& sv, double tolerance, int maxIterations, int* iterations) {
+    Work& wk = *sv.wk;
+    const LevelView& L0 = wk.levels[0].view;
+    const uint32_t n = L0.n;
+    double* x = static_cast<double*>(wk.cgX.ptr);
+    double* r = static_cast<double*>(wk.cgR.ptr);
+    double* p = static_cast<double*>(wk.cgP.ptr);
+    double* ap = static_cast<double*>(wk.cgAp.ptr);
+    double* z = static_cast<double*>(wk.cgZ.ptr);
+    TG_CUDA(cudaMemsetAsync(x, 0, size_t(n) * 8, sv.s), "memset");
+    double d[2];
+    if (int st = dots(sv, r, r, nullptr, nullptr, n, d)) {
+        return st;
+    }
+    const double target = tolerance * std::sqrt(d[0]);
+    if (int st = precondition<kOrder>(sv, r, p)) {
+        return st;
+    }
+    if (int st = dots(sv, r, p, nullptr, nullptr, n, d)) {
+        return st;
+    }
+    double fit = d[0];
+    int it = 0;
+    for (; it < maxIterations && fit > 0.0; ++it) {
+        apply_kernel<kOrder><<<blocks_for(n), 256, 0, sv.s>>>(L0, p, ap);
+        TG_CUDA(cudaGetLastError(), "apply launch");
+        if (int st = dots(sv, p, ap, nullptr, nullptr, n, d)) {
+            return st;
+        }
+        const double curvature = d[0];
+        if (!(curvature > 0.0)) {
+            break;
+        }
+        const double step = fit / curvature;
+        cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, step);
+        if (int st = precondition<kOrder>(sv, r, z)) {
+            return st;
+        }
+        if (int st = dots(sv, r, r, r, z, n, d)) {
+            return st;
+        }
+        if (std::sqrt(d[0]) <= target) {
+            ++it;
+            break;
+        }
+        const double ratio = d[1] / fit;
+        fit = d[1];
+        cg_direction_kernel<<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, ratio);
+    }
+    *iterations = it;
+    return TG_OK;
+}
+
+thread_local tg_seam_stats g_last{};
+
+}  // namespace
+
+extern "C" {
+
+int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, uint32_t width,
+                  uint32_t height, double dx, double dy, const tg_seam_options* options,
+                  float* field, int memory, void* stream) {
+    if (int st = check_device(d)) {
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (int st = check_memory(memory)) {
+        return st;
+    }
+    if (options == nullptr || data == nullptr || difference == nullptr || field == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "data, difference, options and field are required");
+    }
+    const tg_seam_options& o = *options;
+    if (o.mode > 3u || !(dx > 0.0) || !(dy > 0.0) || !std::isfinite(dx) || !std::isfinite(dy) ||
+        ((o.mode == 1u) && !(o.width > 0.0 && std::isfinite(o.width))) ||
+        ((o.mode >= 2u) && !(o.decay_length > 0.0 && std::isfinite(o.decay_length))) ||
+        o.levels < 1 || o.levels > kMaxLevels || o.sweeps < 1 || o.coarsest_sweeps < 1) {
+        return fail(TG_ERROR_ARGUMENT, "seam options out of range");
+    }
+    const size_t n = size_t(width) * height;
+    g_last = tg_seam_stats{};
+    if (n == 0) {
+        return TG_OK;
+    }
+    if (n >= 0xffffffffull) {
+        return fail(TG_ERROR_UNSUPPORTED, "a seam lattice holds fewer than 2^32 posts");
+    }
+    const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
+                               ? static_cast<cudaStream_t>(stream)
+                               : d->stream;
+    Work wk;
+    Buffer hostData, hostDiff, hostField;  // device copies in host mode
+    const uint8_t* dData = data;
+    const float* dDiff = difference;
+    float* dField = field;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(hostData.reserve(n), "allocation");
+        TG_CUDA(hostDiff.reserve(n * 4), "allocation");
+        TG_CUDA(hostField.reserve(n * 4), "allocation");
+        TG_CUDA(cudaMemcpyAsync(hostData.ptr, data, n, cudaMemcpyHostToDevice, s), "copy");
+        TG_CUDA(cudaMemcpyAsync(hostDiff.ptr, difference, n * 4, cudaMemcpyHostToDevice, s),
+                "copy");
+        dData = static_cast<const uint8_t*>(hostData.ptr);
+        dDiff = static_cast<const float*>(hostDiff.ptr);
+        dField = static_cast<float*>(hostField.ptr);
+    }
+    auto finish = [&](int st) {
+        if (st == TG_OK && memory == TG_MEMORY_HOST) {
+            if (cudaMemcpyAsync(field, dField, n * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                st = fail(TG_ERROR_CUDA, "copy to host");
+            }
+        }
+        hostData.release();
+        hostDiff.release();
+        hostField.release();
+        return st;
+    };
+    TG_CUDA(cudaMemsetAsync(dField, 0, n * 4, s), "memset");
+    if (o.mode == 0u) {
+        return finish(TG_OK);
+    }
+    // The field is 0 when the earlier source has data at every post or at none.
+    TG_CUDA(wk.count.reserve(8), "allocation");
+    TG_CUDA(cudaMemsetAsync(wk.count.ptr, 0, 8, s), "memset");
+    count_data_kernel<<<1184, 256, 0, s>>>(dData, n,
+                                           static_cast<unsigned long long*>(wk.count.ptr));
+    unsigned long long withData = 0;
+    TG_CUDA(cudaMemcpyAsync(&withData, wk.count.ptr, 8, cudaMemcpyDeviceToHost, s), "copy");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    if (withData == 0 || withData == n) {
+        return finish(TG_OK);
+    }
+    // The band's differences.
+    TG_CUDA(wk.marks.reserve(n), "allocation");
+    gaps_across_kernel<<<blocks_for(n), 256, 0, s>>>(dData, width, height, kBandPosts,
+                                                    static_cast<uint8_t*>(wk.marks.ptr));
+    band_kernel<<<blocks_for(n), 256, 0, s>>>(dData, dDiff, static_cast<uint8_t*>(wk.marks.ptr),
+                                             width, height, kBandPosts, dField);
+    TG_CUDA(cudaGetLastError(), "band launch");
+    // Distances to the nearest post with data, up to the reach (Height, Slope) or the width
+    // (Feather).
+    const bool feather = o.mode == 1u;
+    const double reach = feather ? o.width : 3.0 * o.decay_length;  // kSeamReachDecays
+    TG_CUDA(wk.distance.reserve(n * 4), "allocation");
+    TG_CUDA(wk.distance2.reserve(n * 4), "allocation");
+    if (feather) {
+        TG_CUDA(wk.carried.reserve(n * 4), "allocation");
+        TG_CUDA(wk.carried2.reserve(n * 4), "allocation");
+    }
+    DistanceRow row{};
+    row.data = dData;
+    row.field = dField;
+    row.distance = static_cast<float*>(wk.distance.ptr);
+    row.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
+    row.distanceOut = static_cast<float*>(wk.distance2.ptr);
+    row.carriedOut = feather ? static_cast<float*>(wk.carried2.ptr) : nullptr;
+    row.w = width;
+    row.h = height;
+    row.dx = float(dx);
+    row.dy = float(dy);
+    row.diagonal = float(std::hypot(dx, dy));
+    row.cap = float(reach) < reach ? std::nextafter(float(reach), INFINITY) : float(reach);
+    // A recurrence along a row stays within the cap for at most cap / dx steps.
+    const double steps = std::ceil(double(row.cap) / double(row.dx)) + 2.0;
+    row.window = int(std::min(steps, double(width)));
+    const uint32_t segments = (width + kSegment - 1) / kSegment;
+    for (uint32_t r = 0; r < height; ++r) {
+        distance_forward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+    }
+    for (uint32_t r = height; r-- > 0;) {
+        distance_backward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+    }
+    TG_CUDA(cudaGetLastError(), "distance launch");
+    const float* distance = row.distanceOut;
+    if (feather) {
+        feather_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, row.carriedOut, n, o.width,
+                                                    dField);
+        TG_CUDA(cudaGetLastError(), "feather launch");
+        return finish(TG_OK);
+    }
+    // The unknowns of each level.
+    TG_CUDA(wk.flags.reserve((n + 1) * sizeof(uint32_t)), "allocation");
+    unknown_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, width, height, reach,
+                                                static_cast<uint32_t*>(wk.flags.ptr));
+    TG_CUDA(cudaGetLastError(), "unknown launch");
+    const int order = o.mode == 3u ? 2 : 1;
+    const double screening = 1.0 / (o.decay_length * o.decay_length);
+    int levels = 0;
+    uint32_t lw = width, lh = height;
+    double ldx = dx, ldy = dy;
+    for (; levels < int(o.levels); ++levels) {
+        Level& L = wk.levels[levels];
+        if (levels > 0) {
+            const Level& F = wk.levels[levels - 1];
+            lw = (lw + 1) / 2;
+            lh = (lh + 1) / 2;
+            ldx *= 2.0;
+            ldy *= 2.0;
+            TG_CUDA(cudaMemsetAsync(wk.flags.ptr, 0, (size_t(lw) * lh + 1) * sizeof(uint32_t), s),
+                    "memset");
+            coarsen_kernel<<<blocks_for(F.view.n), 256, 0, s>>>(
+                F.view.position, F.view.n, F.view.w, lw, static_cast<uint32_t*>(wk.flags.ptr));
+            TG_CUDA(cudaGetLastError(), "coarsen launch");
+        }
+        if (int st = compact(wk, L, lw, lh, s)) {
+            return finish(st);
+        }
+        L.view.cx = 1.0 / (ldx * ldx);
+        L.view.cy = 1.0 / (ldy * ldy);
+        L.view.center = 2.0 * L.view.cx + 2.0 * L.view.cy + screening;
+        L.view.diagonal = order == 1 ? L.view.center
+                                     : L.view.center * L.view.center +
+                                           2.0 * L.view.cx * L.view.cx +
+                                           2.0 * L.view.cy * L.view.cy;
+        if (levels == 0 && L.view.n == 0) {
+            return finish(TG_OK);
+        }
+        if (L.view.n <= 32u || lw < 4 || lh < 4) {  // the coarsest, as kCoarsestPosts
+            ++levels;
+            break;
+        }
+    }
+    for (int l = 0; l < levels; ++l) {
+        Level& L = wk.levels[l];
+        const size_t bytes = (l + 1 == levels ? 8 : 4) * std::max<size_t>(L.view.n, 1);
+        TG_CUDA(L.x.reserve(bytes), "allocation");
+        TG_CUDA(L.b.reserve(bytes), "allocation");
+        TG_CUDA(L.t.reserve(bytes), "allocation");
+    }
+    const uint32_t nu = wk.levels[0].view.n;
+    for (Buffer* b : {&wk.cgX, &wk.cgR, &wk.cgP, &wk.cgAp, &wk.cgZ}) {
+        TG_CUDA(b->reserve(size_t(nu) * 8), "allocation");
+    }
+    TG_CUDA(wk.partial.reserve(2 * kDotBlocks * 8), "allocation");
+    TG_CUDA(wk.dots.reserve(16), "allocation");
+    // The right-hand side from the fixed values, then the conjugate gradients.
+    if (order == 1) {
+        rhs_kernel<1><<<blocks_for(nu), 256, 0, s>>>(wk.levels[0].view, dField,
+                                                    static_cast<double*>(wk.cgR.ptr));
+    } else {
+        rhs_kernel<2><<<blocks_for(nu), 256, 0, s>>>(wk.levels[0].view, dField,
+                                                    static_cast<double*>(wk.cgR.ptr));
+    }
+    TG_CUDA(cudaGetLastError(), "rhs launch");
+    Solver sv{&wk, levels, order, s, order == 1 ? 0.8 : 0.5, int(o.sweeps),
+              int(o.coarsest_sweeps)};
+    int iterations = 0;
+    const double tolerance = o.tolerance > 0.0 ? o.tolerance : 1e-10;
+    const int st = order == 1 ? solve<1>(sv, tolerance, 200, &iterations)
+                              : solve<2>(sv, tolerance, 200, &iterations);
+    if (st != TG_OK) {
+        return finish(st);
+    }
+    scatter_solution_kernel<<<blocks_for(nu), 256, 0, s>>>(
+        wk.levels[0].view.position, static_cast<const double*>(wk.cgX.ptr), nu, dField);
+    TG_CUDA(cudaGetLastError(), "scatter launch");
+    g_last.unknowns = nu;
+    g_last.levels = uint32_t(levels);
+    g_last.iterations = uint32_t(iterations);
+    return finish(TG_OK);
+}
+
+int tg_seam_stats_get(tg_seam_stats* stats) {
+    if (stats == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "stats is null");
+    }
+    *stats = g_last;
+    return TG_OK;
+}
+
+int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const float* later,
+                 const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
+                 void* stream) {
+    if (int st = check_device(d)) {
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (int st = check_memory(memory)) {
+        return st;
+    }
+    Grid g, lg;
+    if (int st = to_grid(grid, g)) {
+        return st;
+    }
+    if (lattice == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "lattice is null");
+    }
+    lg = Grid{lattice->width,       lattice->height,       lattice->origin_x,
+              lattice->pixel_width, lattice->row_rotation, lattice->origin_y,
+              lattice->col_rotation, lattice->pixel_height};
+    const double det = lg.pixelWidth * lg.pixelHeight - lg.rowRotation * lg.colRotation;
+    if (!(det != 0.0) || !std::isfinite(det)) {
+        return fail(TG_ERROR_ARGUMENT, "lattice transform must be invertible");
+    }
+    if (nodata.mode > 2u) {
+        return fail(TG_ERROR_ARGUMENT, "nodata mode must be 0, 1 or 2");
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    const size_t posts = size_t(lg.width) * lg.height;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (field == nullptr || later == nullptr || heights == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "field, later and heights are required");
+    }
+    const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
+                               ? static_cast<cudaStream_t>(stream)
+                               : d->stream;
+    Buffer bf, bl, bh;
+    const float* df = field;
+    const float* dl = later;
+    float* dh = heights;
+    auto done = [&](int st) {
+        bf.release();
+        bl.release();
+        bh.release();
+        return st;
+    };
+    if (memory == TG_MEMORY_HOST) {
+        if (bf.reserve(std::max<size_t>(posts, 1) * 4) != cudaSuccess ||
+            bl.reserve(cells * 4) != cudaSuccess || bh.reserve(cells * 4) != cudaSuccess) {
+            return done(fail(TG_ERROR_MEMORY, "device allocation"));
+        }
+        if (cudaMemcpyAsync(bf.ptr, field, posts * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(bl.ptr, later, cells * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(bh.ptr, heights, cells * 4, cudaMemcpyHostToDevice, s) !=
+                cudaSuccess) {
+            return done(fail(TG_ERROR_CUDA, "copy to device"));
+        }
+        df = static_cast<const float*>(bf.ptr);
+        dl = static_cast<const float*>(bl.ptr);
+        dh = static_cast<float*>(bh.ptr);
+    }
+    // Whether any post is set (SeamField::At is 0 everywhere otherwise).
+    std::vector<float> probe;
+    bool set = false;
+    {
+        Buffer count;
+        if (count.reserve(8) != cudaSuccess) {
+            return done(fail(TG_ERROR_MEMORY, "device allocation"));
+        }
+        cudaMemsetAsync(count.ptr, 0, 8, s);
+        // Posts holding a nonzero value, counted as "data" of their bits.
+        count_data_kernel<<<1184, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(df), posts * 4,
+                                               static_cast<unsigned long long*>(count.ptr));
+        unsigned long long nonzero = 0;
+        cudaMemcpyAsync(&nonzero, count.ptr, 8, cudaMemcpyDeviceToHost, s);
+        const cudaError_t e = cudaStreamSynchronize(s);
+        count.release();
+        if (e != cudaSuccess) {
+            return done(fail(TG_ERROR_CUDA, "synchronize: %s", cudaGetErrorString(e)));
+        }
+        set = nonzero > 0;
+    }
+    SeamRead sr{df, lg.width, lg.height, lg.originX, lg.pixelWidth, lg.rowRotation,
+                lg.originY, lg.colRotation, lg.pixelHeight, set};
+    const NoData nd{nodata.mode, nodata.value};
+    seam_fill_kernel<<<dim3(blocks_for(g.width), std::min<uint32_t>(g.height, 65535u)), 256, 0, s>>>(
+        sr, g, dl, nd, dh);
+    if (cudaGetLastError() != cudaSuccess) {
+        return done(fail(TG_ERROR_CUDA, "seam fill launch"));
+    }
+    if (memory == TG_MEMORY_HOST) {
+        if (cudaMemcpyAsync(heights, dh, cells * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            return done(fail(TG_ERROR_CUDA, "copy to host"));
+        }
+    }
+    return done(TG_OK);
+}
+
+}  // extern "C"

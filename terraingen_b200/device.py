@@ -241,6 +241,55 @@ class Device:
                                        C.byref(g), h, b.memory, _stream(b.memory)))
         return heights
 
+    # --- seams ---------------------------------------------------------------------------
+    SEAM_MODES = {"none": 0, "feather": 1, "height": 2, "slope": 3}
+
+    def seam_solve(self, data, difference, dx: float, dy: float, mode: str, width: float = 50.0,
+                   decay_length: float = 50.0, field=None, levels: int = 4, sweeps: int = 2,
+                   coarsest_sweeps: int = 100, tolerance: float = 0.0):
+        """BuildSeamField (src/sources/seam_field.cpp:663) on the device from the lattice's
+        samples: `data` (uint8, 1 where the earlier source has data) and `difference` (float32,
+        earlier minus later, NaN elsewhere), both (height, width). Returns the field's posts
+        (float32) and the solve's statistics."""
+        b = _Buffers()
+        if _is_torch(data):
+            height, width_ = data.shape
+        else:
+            data = np.ascontiguousarray(data, np.uint8)
+            difference = np.ascontiguousarray(difference, np.float32)
+            height, width_ = data.shape
+        if field is None:
+            if _is_torch(data):
+                import torch
+
+                field = torch.empty((height, width_), dtype=torch.float32, device=data.device)
+            else:
+                field = np.zeros((height, width_), np.float32)
+        dp = b.ptr(data)
+        fp = b.ptr(difference)
+        out = b.ptr(field)
+        opts = N.SeamOptions(self.SEAM_MODES[mode], levels, sweeps, coarsest_sweeps, width,
+                             decay_length, tolerance)
+        N.check(self._lib.tg_seam_solve(self._handle, dp, fp, width_, height, dx, dy,
+                                        C.byref(opts), out, b.memory, _stream(b.memory)))
+        st = N.SeamStats()
+        N.check(self._lib.tg_seam_stats_get(C.byref(st)))
+        return field, {"unknowns": st.unknowns, "levels": st.levels,
+                       "iterations": st.iterations}
+
+    def seam_fill(self, field, lattice: GridSpec, later, grid: GridSpec, heights,
+                  nodata=(1, 0.0)):
+        """FillGridGaps (src/sources/source_chain.cpp:167): cells of `heights` holding no data
+        take `later` plus the field read at their centers."""
+        b = _Buffers()
+        fp = b.ptr(field, np.float32)
+        lp = b.ptr(later, np.float32)
+        hp = b.ptr(heights, np.float32)
+        lg, g = lattice.native(), grid.native()
+        N.check(self._lib.tg_seam_fill(self._handle, fp, C.byref(lg), lp, C.byref(g), hp,
+                                       N.NoData(*nodata), b.memory, _stream(b.memory)))
+        return heights
+
     def philox_probe(self, sextets: np.ndarray):
         """(words [n, 4] u32, normals [n] f64) of n (counter x4, key x2) sextets."""
         sextets = np.ascontiguousarray(sextets, np.uint32).reshape(-1, 6)

@@ -175,6 +175,82 @@ def ds_fixtures() -> None:
     np.savez_compressed(OUT / "ds.npz", **arrays)
 
 
+def _seam_rasters(grid, seed: int, hole) -> tuple[np.ndarray, np.ndarray]:
+    """An fBm `earlier` raster with NaN where `hole(x, y)` holds, and a `later` one offset from it
+    by a smooth bias of a few meters (a coarser DEM that disagrees with the patch)."""
+    rs = H.restate()
+    earlier = np.zeros((grid.height, grid.width), np.float32)
+    rs.rs_fbm_grid_f32(grid.width, grid.height, grid.x0, grid.y0, grid.pixel, seed, 300.0, 25.0,
+                       6, 2.0, 0.5, 0.0, earlier.ctypes.data)
+    cols = np.arange(grid.width) + 0.5
+    rows = np.arange(grid.height) + 0.5
+    x = grid.x0 + cols[None, :] * grid.pixel
+    y = grid.y0 - rows[:, None] * grid.pixel
+    u = (x - grid.x0) / (grid.width * grid.pixel)
+    v = (grid.y0 - y) / (grid.height * grid.pixel)
+    bias = 2.5 + 1.5 * u - 2.0 * v + 0.8 * np.sin(6.0 * u + 1.0) * np.cos(4.0 * v)
+    later = (earlier - bias).astype(np.float32)
+    earlier = np.where(hole(x, y), np.float32(np.nan), earlier).astype(np.float32)
+    return earlier, later
+
+
+SEAM_SCENES = {
+    # A hole inside a 200 x 150 m patch at 1 m (an ellipse with a notch): the three modes.
+    "hole": (centered(200, 150, 1.0, 500.0, -300.0),
+             lambda x, y: (((x - 490.0) / 45.0) ** 2 + ((y + 310.0) / 30.0) ** 2 < 1.0)
+             | ((np.abs(x - 540.0) < 6.0) & (np.abs(y + 300.0) < 20.0)), 3),
+    # One of 2 x 2 patches at 2 m: the earlier source covers the top-left quadrant only, so the
+    # gap is an L reaching the raster's edges (the seam between patches).
+    "patch": (centered(160, 140, 2.0, -1200.0, 800.0),
+              lambda x, y: (x > -1200.0 + 4.0) | (y < 800.0 - 10.0), 5),
+}
+SEAM_MODES = {
+    "hole": [("feather", 1, 10.0, 0.0), ("height", 2, 0.0, 6.0), ("slope", 3, 0.0, 6.0)],
+    "patch": [("feather", 1, 16.0, 0.0), ("height", 2, 0.0, 8.0), ("slope", 3, 0.0, 8.0)],
+}
+
+
+def seam_fixtures() -> None:
+    """The reference's seam fields (BuildSeamField) from its own lattice samples, and the chain's
+    heights (SourceChain::FillGridGaps) on the rasters' grid and on a finer window."""
+    ref = H.reference()
+    arrays = {}
+    nan = np.float32(np.nan)
+    for scene, (grid, hole, seed) in SEAM_SCENES.items():
+        earlier, later = _seam_rasters(grid, seed, hole)
+        t = grid.transform()
+        arrays[f"{scene}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0,
+                                            grid.pixel])
+        arrays[f"{scene}_earlier"] = earlier
+        arrays[f"{scene}_later"] = later
+        # A finer window across the gap's edge, read from each source alone: the earlier source
+        # (NaN where it has no data) and the later one.
+        fine = centered(150, 110, 0.5 * grid.pixel, grid.x0 + 0.55 * grid.width * grid.pixel,
+                        grid.y0 - 0.5 * grid.height * grid.pixel)
+        arrays[f"{scene}_fine_grid"] = np.array([fine.width, fine.height, fine.x0, fine.y0,
+                                                 fine.pixel])
+        none_later = np.full_like(later, nan)
+        none_earlier = np.full_like(earlier, nan)
+        arrays[f"{scene}_fine_earlier"] = H.chain(ref, earlier, none_later, t, 0, 1.0, 1.0, fine)
+        arrays[f"{scene}_fine_later"] = H.chain(ref, none_earlier, later, t, 0, 1.0, 1.0, fine)
+        for name, mode, width, decay in SEAM_MODES[scene]:
+            s = H.seam(ref, earlier, later, t, mode, width or 50.0, decay or 50.0)
+            key = f"{scene}_{name}"
+            arrays[f"{key}_options"] = np.array([mode, width or 50.0, decay or 50.0])
+            arrays[f"{key}_lattice"] = np.array([s["width"], s["height"], *s["transform"]])
+            arrays[f"{key}_data"] = s["data"]
+            arrays[f"{key}_difference"] = s["difference"]
+            arrays[f"{key}_field"] = s["field"]
+            arrays[f"{key}_ms"] = np.float64(s["ms"])
+            arrays[f"{key}_chain"] = H.chain(ref, earlier, later, t, mode, width or 50.0,
+                                             decay or 50.0, grid)
+            arrays[f"{key}_fine_chain"] = H.chain(ref, earlier, later, t, mode, width or 50.0,
+                                                  decay or 50.0, fine)
+            print(key, s["width"], "x", s["height"], "posts,",
+                  int(np.count_nonzero(s["field"])), "set,", f"{s['ms']:.1f} ms")
+    np.savez_compressed(OUT / "seams.npz", **arrays)
+
+
 def population_fixture() -> None:
     """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
     ref = H.reference()
@@ -191,5 +267,6 @@ if __name__ == "__main__":
     boulder_fixtures()
     ds_fixtures()
     population_fixture()
+    seam_fixtures()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)
