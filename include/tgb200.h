@@ -305,6 +305,15 @@ int tg_seam_stats_get(tg_seam_stats* stats);
 int tg_seam_fill(tg_device* device, const float* field, const tg_grid* lattice,
                  const float* later, const tg_grid* grid, float* heights, tg_nodata nodata,
                  int memory, void* stream);
+/* SampleSources (seam_field.cpp:76-113) for two sources held as rasters on one grid: the lattice
+ * is the `lw` x `lh` posts whose first post is cell (`col0`, `row0`) of `grid` (negative, or past
+ * the grid's edge, where the lattice pads it; its posts there have no data). `data` gets 1 where
+ * `earlier` has data (finite, and not the no-data value), `difference` earlier minus later (in
+ * double, rounded to float) where both have, NaN elsewhere. */
+int tg_seam_samples(tg_device* device, const float* earlier, const float* later,
+                    const tg_grid* grid, int64_t col0, int64_t row0, uint32_t lw, uint32_t lh,
+                    tg_nodata nodata, uint8_t* data, float* difference, int memory,
+                    void* stream);
 
 /* --- crater populations and kernel batches (host) ------------------------------------------ */
 

@@ -43,6 +43,7 @@ constexpr int kBandPosts = 3;     // seam_field.cpp:29
 constexpr int kBorderPosts = 3;   // seam_field.cpp:32
 constexpr int kSegment = 32;      // cells of a row a thread of the distance passes writes
 constexpr int kMaxLevels = 8;
+constexpr size_t kTileSharedBytes = 200 * 1024;  // a distance window's shared memory at most
 
 // --- band and fixed values ---------------------------------------------------------------
 
@@ -235,6 +236,257 @@ __global__ void distance_backward_kernel(const DistanceRow p, uint32_t row) {
         }
         right = d;
         rightCarried = carried;
+    }
+}
+
+// --- distances by tiles ---------------------------------------------------------------------
+//
+// A distance at most `cap` comes from a path of steps that each add at least dx (a step across
+// columns) or dy (across rows), so it reaches no further than cap / dx columns and cap / dy rows:
+// both passes, run over a window that holds a tile plus a halo of mx = cap / dx + 2 columns and
+// my = cap / dy + 2 rows (clipped to the lattice, whose edges the reference's passes start from
+// too) and started from no distance outside it, give every post of the tile the reference's
+// distance and carried value wherever the distance is at most `cap`. Larger values are never
+// read back, so they are written as +inf. Inside a window the passes run as wavefronts: the
+// forward pass reads the left, upper-left, upper and upper-right posts, all on earlier fronts
+// 2 row + col, and the backward pass mirrors it, so every post sees the same operands, in the
+// same order, as in the row-by-row relaxation.
+//
+// Only tiles that hold a post without data and see a post with data within their halo are
+// computed; distance_init_kernel gives every other post its value (0 with data, +inf without).
+
+struct DistanceTiles {
+    const uint8_t* data;
+    const float* field;  // the carried value of a post with data, or null (no carried values)
+    float* distance;
+    float* carried;
+    uint32_t w, h;
+    float dx, dy, diagonal, cap;
+    int ts;              // tile side
+    int mx, my;          // halo columns and rows
+    int maxPosts;        // posts of the largest window
+    uint32_t tilesX, tilesY;
+    const uint32_t* list;
+    const uint32_t* count;
+};
+
+__global__ void distance_init_kernel(const uint8_t* __restrict__ data,
+                                     const float* __restrict__ field, size_t n,
+                                     float* __restrict__ distance, float* __restrict__ carried) {
+    for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
+         k += size_t(gridDim.x) * blockDim.x) {
+        const bool has = data[k] != 0;
+        distance[k] = has ? 0.0f : INFINITY;
+        if (carried != nullptr) {
+            carried[k] = has ? field[k] : 0.0f;
+        }
+    }
+}
+
+// Posts with data per tile (one block per tile).
+__global__ void tile_counts_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
+                                   int ts, uint32_t tilesX, uint32_t* __restrict__ counts) {
+    const uint32_t tile = blockIdx.x;
+    const uint32_t r0 = (tile / tilesX) * uint32_t(ts), c0 = (tile % tilesX) * uint32_t(ts);
+    const uint32_t rows = min(uint32_t(ts), h - r0), cols = min(uint32_t(ts), w - c0);
+    uint32_t mine = 0;
+    for (uint32_t i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+        mine += data[size_t(r0 + i / cols) * w + c0 + i % cols] != 0 ? 1u : 0u;
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        mine += __shfl_down_sync(0xffffffffu, mine, d);
+    }
+    __shared__ uint32_t warps[32];
+    if ((threadIdx.x & 31u) == 0) {
+        warps[threadIdx.x >> 5] = mine;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t total = 0;
+        for (uint32_t i = 0; i < (blockDim.x + 31) / 32; ++i) {
+            total += warps[i];
+        }
+        counts[tile] = total;
+    }
+}
+
+// The tiles to compute: a post without data, and a post with data within `rx` tiles across and
+// `ry` down or up (a superset of the halo).
+__global__ void active_tiles_kernel(const uint32_t* __restrict__ counts, uint32_t w, uint32_t h,
+                                    int ts, uint32_t tilesX, uint32_t tilesY, int rx, int ry,
+                                    uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+    const uint32_t tile = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= tilesX * tilesY) {
+        return;
+    }
+    const int tx = int(tile % tilesX), ty = int(tile / tilesX);
+    const uint32_t rows = min(uint32_t(ts), h - uint32_t(ty) * ts);
+    const uint32_t cols = min(uint32_t(ts), w - uint32_t(tx) * ts);
+    if (counts[tile] == rows * cols) {
+        return;  // all posts have data
+    }
+    bool near = false;
+    for (int y = max(0, ty - ry); y <= min(int(tilesY) - 1, ty + ry) && !near; ++y) {
+        for (int x = max(0, tx - rx); x <= min(int(tilesX) - 1, tx + rx); ++x) {
+            if (counts[size_t(y) * tilesX + x] != 0) {
+                near = true;
+                break;
+            }
+        }
+    }
+    if (near) {
+        list[atomicAdd(count, 1u)] = tile;
+    }
+}
+
+// Posts of the largest window of a tile of side `ts` on a w x h lattice, and the shared memory
+// it takes.
+size_t tile_window_posts(int ts, int mx, int my, uint32_t w, uint32_t h) {
+    return std::min<size_t>(size_t(ts) + 2 * size_t(my), h) *
+           std::min<size_t>(size_t(ts) + 2 * size_t(mx), w);
+}
+
+size_t tile_window_bytes(size_t posts, bool carried) {
+    return posts * (carried ? 8 : 4) + ((posts + 31) / 32) * 4;
+}
+
+// One block per listed tile, blocks looping over the list.
+__global__ void __launch_bounds__(128) distance_tile_kernel(const DistanceTiles p) {
+    extern __shared__ float smem[];
+    const uint32_t total = *p.count;
+    const int maxPosts = p.maxPosts;
+    float* F = smem;
+    float* Cc = p.carried != nullptr ? smem + maxPosts : nullptr;
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + (p.carried != nullptr ? 2 : 1) * maxPosts);
+    const int tid = int(threadIdx.x), lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
+    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const uint32_t tile = p.list[item];
+        const int r0 = int(tile / p.tilesX) * p.ts, c0 = int(tile % p.tilesX) * p.ts;
+        const int rw0 = max(0, r0 - p.my), rw1 = min(int(p.h), r0 + p.ts + p.my);
+        const int cw0 = max(0, c0 - p.mx), cw1 = min(int(p.w), c0 + p.ts + p.mx);
+        const int hw = rw1 - rw0, ww = cw1 - cw0, posts = hw * ww;
+        // Which window posts have data, one bit each.
+        for (int base = warp * 32; base < posts; base += warps * 32) {
+            const int i = base + lane;
+            const bool has = i < posts &&
+                             p.data[size_t(rw0 + i / ww) * p.w + size_t(cw0 + i % ww)] != 0;
+            const uint32_t word = __ballot_sync(0xffffffffu, has);
+            if (lane == 0) {
+                bits[base >> 5] = word;
+            }
+        }
+        __syncthreads();
+        const int fronts = 2 * (hw - 1) + ww;
+        // Forward: front t holds the posts with 2 row + col = t.
+        for (int t = 0; t < fronts; ++t) {
+            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hw - 1, t / 2);
+            for (int r = rlo + tid; r <= rhi; r += int(blockDim.x)) {
+                const int c = t - 2 * r, k = r * ww + c;
+                if ((bits[k >> 5] >> (k & 31)) & 1u) {
+                    F[k] = 0.0f;
+                    if (Cc) {
+                        Cc[k] = p.field[size_t(rw0 + r) * p.w + size_t(cw0 + c)];
+                    }
+                    continue;
+                }
+                float d = INFINITY, carried = 0.0f;
+                if (c > 0) {
+                    const float s = F[k - 1] + p.dx;
+                    if (s < d) {
+                        d = s;
+                        if (Cc) carried = Cc[k - 1];
+                    }
+                }
+                if (r > 0) {
+                    const int up = k - ww;
+                    float s = F[up] + p.dy;
+                    if (s < d) {
+                        d = s;
+                        if (Cc) carried = Cc[up];
+                    }
+                    if (c > 0) {
+                        s = F[up - 1] + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            if (Cc) carried = Cc[up - 1];
+                        }
+                    }
+                    if (c + 1 < ww) {
+                        s = F[up + 1] + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            if (Cc) carried = Cc[up + 1];
+                        }
+                    }
+                }
+                F[k] = d;
+                if (Cc) {
+                    Cc[k] = carried;
+                }
+            }
+            __syncthreads();
+        }
+        // Backward, in place: front t holds the posts with 2 (hw-1-row) + (ww-1-col) = t.
+        for (int t = 0; t < fronts; ++t) {
+            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hw - 1, t / 2);
+            for (int q = rlo + tid; q <= rhi; q += int(blockDim.x)) {
+                const int r = hw - 1 - q, c = ww - 1 - (t - 2 * q), k = r * ww + c;
+                if ((bits[k >> 5] >> (k & 31)) & 1u) {
+                    continue;
+                }
+                float d = F[k];
+                float carried = Cc ? Cc[k] : 0.0f;
+                if (c + 1 < ww) {
+                    const float s = F[k + 1] + p.dx;
+                    if (s < d) {
+                        d = s;
+                        if (Cc) carried = Cc[k + 1];
+                    }
+                }
+                if (r + 1 < hw) {
+                    const int down = k + ww;
+                    float s = F[down] + p.dy;
+                    if (s < d) {
+                        d = s;
+                        if (Cc) carried = Cc[down];
+                    }
+                    if (c + 1 < ww) {
+                        s = F[down + 1] + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            if (Cc) carried = Cc[down + 1];
+                        }
+                    }
+                    if (c > 0) {
+                        s = F[down - 1] + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            if (Cc) carried = Cc[down - 1];
+                        }
+                    }
+                }
+                F[k] = d;
+                if (Cc) {
+                    Cc[k] = carried;
+                }
+            }
+            __syncthreads();
+        }
+        // The tile's posts without data.
+        const int rows = min(p.ts, int(p.h) - r0), cols = min(p.ts, int(p.w) - c0);
+        for (int i = tid; i < rows * cols; i += int(blockDim.x)) {
+            const int r = r0 + i / cols - rw0, c = c0 + i % cols - cw0, k = r * ww + c;
+            if ((bits[k >> 5] >> (k & 31)) & 1u) {
+                continue;
+            }
+            const size_t g = size_t(rw0 + r) * p.w + size_t(cw0 + c);
+            const float d = F[k];
+            p.distance[g] = d <= p.cap ? d : INFINITY;
+            if (Cc) {
+                p.carried[g] = Cc[k];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -637,6 +889,38 @@ __global__ void seam_fill_kernel(const SeamRead s, const Grid g, const float* __
     }
 }
 
+// SampleSources on a window of a grid both sources are rasters on: post (i, j) is cell
+// (col0 + i, row0 + j); off the grid neither source has data.
+__global__ void seam_samples_kernel(const float* __restrict__ earlier,
+                                    const float* __restrict__ later, uint32_t gw, uint32_t gh,
+                                    int64_t col0, int64_t row0, uint32_t lw, uint32_t lh,
+                                    const NoData nodata, uint8_t* __restrict__ data,
+                                    float* __restrict__ difference) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= lw) {
+        return;
+    }
+    for (uint32_t j = blockIdx.y; j < lh; j += gridDim.y) {
+        const int64_t col = col0 + int64_t(i), row = row0 + int64_t(j);
+        const size_t k = size_t(j) * lw + i;
+        uint8_t has = 0;
+        float diff = NAN;
+        if (col >= 0 && row >= 0 && col < int64_t(gw) && row < int64_t(gh)) {
+            const size_t c = size_t(row) * gw + size_t(col);
+            const float a = earlier[c];
+            has = isfinite(a) && !(nodata.mode == 2u && a == nodata.value) ? 1 : 0;
+            if (has) {
+                const float b = later[c];
+                if (isfinite(b) && !(nodata.mode == 2u && b == nodata.value)) {
+                    diff = float(double(a) - double(b));
+                }
+            }
+        }
+        data[k] = has;
+        difference[k] = diff;
+    }
+}
+
 uint32_t blocks_for(size_t n, uint32_t threads = 256) {
     return uint32_t((n + threads - 1) / threads);
 }
@@ -649,11 +933,12 @@ struct Level {
 
 struct Work {
     Buffer marks, flags, scan, distance, carried, distance2, carried2, count, partial, dots;
+    Buffer tileCounts, tileList;
     Buffer cgX, cgR, cgP, cgAp, cgZ, rhs;
     Level levels[kMaxLevels];
     ~Work() {
         for (Buffer* b : {&marks, &flags, &scan, &distance, &carried, &distance2, &carried2,
-                          &count, &partial, &dots,
+                          &count, &partial, &dots, &tileCounts, &tileList,
                           &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs}) {
             b->release();
         }
@@ -973,38 +1258,105 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     const bool feather = o.mode == 1u;
     const double reach = feather ? o.width : 3.0 * o.decay_length;  // kSeamReachDecays
     TG_CUDA(wk.distance.reserve(n * 4), "allocation");
-    TG_CUDA(wk.distance2.reserve(n * 4), "allocation");
     if (feather) {
         TG_CUDA(wk.carried.reserve(n * 4), "allocation");
-        TG_CUDA(wk.carried2.reserve(n * 4), "allocation");
     }
-    DistanceRow row{};
-    row.data = dData;
-    row.field = dField;
-    row.distance = static_cast<float*>(wk.distance.ptr);
-    row.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
-    row.distanceOut = static_cast<float*>(wk.distance2.ptr);
-    row.carriedOut = feather ? static_cast<float*>(wk.carried2.ptr) : nullptr;
-    row.w = width;
-    row.h = height;
-    row.dx = float(dx);
-    row.dy = float(dy);
-    row.diagonal = float(std::hypot(dx, dy));
-    row.cap = float(reach) < reach ? std::nextafter(float(reach), INFINITY) : float(reach);
-    // A recurrence along a row stays within the cap for at most cap / dx steps.
-    const double steps = std::ceil(double(row.cap) / double(row.dx)) + 2.0;
-    row.window = int(std::min(steps, double(width)));
-    const uint32_t segments = (width + kSegment - 1) / kSegment;
-    for (uint32_t r = 0; r < height; ++r) {
-        distance_forward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+    const float cap =
+        float(reach) < reach ? std::nextafter(float(reach), INFINITY) : float(reach);
+    const float* distance = nullptr;
+    const float* carried = nullptr;
+    // Halo of the tiled passes: a distance at most `cap` reaches cap / dx columns, cap / dy rows.
+    const int mx = int(std::min(std::ceil(double(cap) / dx) + 2.0, double(width)));
+    const int my = int(std::min(std::ceil(double(cap) / dy) + 2.0, double(height)));
+    int ts = 0;
+    for (int side : {128, 96, 64, 32}) {
+        if (tile_window_bytes(tile_window_posts(side, mx, my, width, height), feather) <=
+            kTileSharedBytes) {
+            ts = side;
+            break;
+        }
     }
-    for (uint32_t r = height; r-- > 0;) {
-        distance_backward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+    if (ts > 0) {
+        DistanceTiles t{};
+        t.data = dData;
+        t.field = feather ? dField : nullptr;
+        t.distance = static_cast<float*>(wk.distance.ptr);
+        t.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
+        t.w = width;
+        t.h = height;
+        t.dx = float(dx);
+        t.dy = float(dy);
+        t.diagonal = float(std::hypot(dx, dy));
+        t.cap = cap;
+        t.ts = ts;
+        t.mx = mx;
+        t.my = my;
+        t.maxPosts = int(tile_window_posts(ts, mx, my, width, height));
+        t.tilesX = (width + ts - 1) / ts;
+        t.tilesY = (height + ts - 1) / ts;
+        const size_t tiles = size_t(t.tilesX) * t.tilesY;
+        TG_CUDA(wk.tileCounts.reserve(tiles * 4), "allocation");
+        TG_CUDA(wk.tileList.reserve(tiles * 4 + 4), "allocation");
+        uint32_t* counts = static_cast<uint32_t*>(wk.tileCounts.ptr);
+        uint32_t* list = static_cast<uint32_t*>(wk.tileList.ptr);
+        t.list = list + 1;
+        t.count = list;
+        distance_init_kernel<<<2368, 256, 0, s>>>(dData, dField, n, t.distance, t.carried);
+        tile_counts_kernel<<<uint32_t(tiles), 256, 0, s>>>(dData, width, height, ts, t.tilesX,
+                                                          counts);
+        TG_CUDA(cudaMemsetAsync(list, 0, 4, s), "memset");
+        active_tiles_kernel<<<blocks_for(tiles), 256, 0, s>>>(
+            counts, width, height, ts, t.tilesX, t.tilesY, (mx + ts - 1) / ts,
+            (my + ts - 1) / ts, list + 1, list);
+        const size_t bytes = tile_window_bytes(size_t(t.maxPosts), feather);
+        TG_CUDA(cudaFuncSetAttribute(distance_tile_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+                "shared memory attribute");
+        int perSm = 0, sms = 0;
+        TG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, distance_tile_kernel, 128,
+                                                              bytes),
+                "occupancy");
+        TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->ordinal),
+                "attribute");
+        const uint32_t blocks = uint32_t(std::max(1, perSm) * sms);
+        distance_tile_kernel<<<std::min<uint32_t>(blocks, uint32_t(tiles)), 128, bytes, s>>>(t);
+        TG_CUDA(cudaGetLastError(), "distance launch");
+        distance = t.distance;
+        carried = t.carried;
+    } else {
+        // Halos too wide for a window in shared memory: the passes row by row.
+        TG_CUDA(wk.distance2.reserve(n * 4), "allocation");
+        if (feather) {
+            TG_CUDA(wk.carried2.reserve(n * 4), "allocation");
+        }
+        DistanceRow row{};
+        row.data = dData;
+        row.field = dField;
+        row.distance = static_cast<float*>(wk.distance.ptr);
+        row.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
+        row.distanceOut = static_cast<float*>(wk.distance2.ptr);
+        row.carriedOut = feather ? static_cast<float*>(wk.carried2.ptr) : nullptr;
+        row.w = width;
+        row.h = height;
+        row.dx = float(dx);
+        row.dy = float(dy);
+        row.diagonal = float(std::hypot(dx, dy));
+        row.cap = cap;
+        // A recurrence along a row stays within the cap for at most cap / dx steps.
+        row.window = mx;
+        const uint32_t segments = (width + kSegment - 1) / kSegment;
+        for (uint32_t r = 0; r < height; ++r) {
+            distance_forward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+        }
+        for (uint32_t r = height; r-- > 0;) {
+            distance_backward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
+        }
+        TG_CUDA(cudaGetLastError(), "distance launch");
+        distance = row.distanceOut;
+        carried = row.carriedOut;
     }
-    TG_CUDA(cudaGetLastError(), "distance launch");
-    const float* distance = row.distanceOut;
     if (feather) {
-        feather_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, row.carriedOut, n, o.width,
+        feather_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, carried, n, o.width,
                                                     dField);
         TG_CUDA(cudaGetLastError(), "feather launch");
         return finish(TG_OK);
@@ -1193,6 +1545,80 @@ int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const
     }
     if (memory == TG_MEMORY_HOST) {
         if (cudaMemcpyAsync(heights, dh, cells * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
+            return done(fail(TG_ERROR_CUDA, "copy to host"));
+        }
+    }
+    return done(TG_OK);
+}
+
+int tg_seam_samples(tg_device* d, const float* earlier, const float* later, const tg_grid* grid,
+                    int64_t col0, int64_t row0, uint32_t lw, uint32_t lh, tg_nodata nodata,
+                    uint8_t* data, float* difference, int memory, void* stream) {
+    if (int st = check_device(d)) {
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (int st = check_memory(memory)) {
+        return st;
+    }
+    Grid g;
+    if (int st = to_grid(grid, g)) {
+        return st;
+    }
+    if (nodata.mode > 2u) {
+        return fail(TG_ERROR_ARGUMENT, "nodata mode must be 0, 1 or 2");
+    }
+    const size_t posts = size_t(lw) * lh;
+    const size_t cells = size_t(g.width) * g.height;
+    if (posts == 0) {
+        return TG_OK;
+    }
+    if (earlier == nullptr || later == nullptr || data == nullptr || difference == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "earlier, later, data and difference are required");
+    }
+    const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
+                               ? static_cast<cudaStream_t>(stream)
+                               : d->stream;
+    Buffer be, bl, bd, bf;
+    auto done = [&](int st) {
+        be.release();
+        bl.release();
+        bd.release();
+        bf.release();
+        return st;
+    };
+    const float* de = earlier;
+    const float* dl = later;
+    uint8_t* dd = data;
+    float* df = difference;
+    if (memory == TG_MEMORY_HOST) {
+        if (be.reserve(std::max<size_t>(cells, 1) * 4) != cudaSuccess ||
+            bl.reserve(std::max<size_t>(cells, 1) * 4) != cudaSuccess ||
+            bd.reserve(posts) != cudaSuccess || bf.reserve(posts * 4) != cudaSuccess) {
+            return done(fail(TG_ERROR_MEMORY, "device allocation"));
+        }
+        if (cells > 0 &&
+            (cudaMemcpyAsync(be.ptr, earlier, cells * 4, cudaMemcpyHostToDevice, s) !=
+                 cudaSuccess ||
+             cudaMemcpyAsync(bl.ptr, later, cells * 4, cudaMemcpyHostToDevice, s) !=
+                 cudaSuccess)) {
+            return done(fail(TG_ERROR_CUDA, "copy to device"));
+        }
+        de = static_cast<const float*>(be.ptr);
+        dl = static_cast<const float*>(bl.ptr);
+        dd = static_cast<uint8_t*>(bd.ptr);
+        df = static_cast<float*>(bf.ptr);
+    }
+    seam_samples_kernel<<<dim3(blocks_for(lw), std::min<uint32_t>(lh, 65535u)), 256, 0, s>>>(
+        de, dl, g.width, g.height, col0, row0, lw, lh, NoData{nodata.mode, nodata.value}, dd, df);
+    if (cudaGetLastError() != cudaSuccess) {
+        return done(fail(TG_ERROR_CUDA, "seam samples launch"));
+    }
+    if (memory == TG_MEMORY_HOST) {
+        if (cudaMemcpyAsync(data, dd, posts, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaMemcpyAsync(difference, df, posts * 4, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) {
             return done(fail(TG_ERROR_CUDA, "copy to host"));
         }

@@ -290,6 +290,32 @@ class Device:
                                        N.NoData(*nodata), b.memory, _stream(b.memory)))
         return heights
 
+    def seam_samples(self, earlier, later, grid: GridSpec, col0: int, row0: int, lw: int,
+                     lh: int, data=None, difference=None, nodata=(1, 0.0)):
+        """SampleSources (src/sources/seam_field.cpp:76) for two rasters on `grid`: the lattice
+        of `lw` x `lh` posts from cell (`col0`, `row0`). Returns (data uint8, difference f32),
+        both (lh, lw), on the host or the device as the inputs are."""
+        if _is_torch(earlier):
+            import torch
+
+            if data is None:
+                data = torch.empty((lh, lw), dtype=torch.uint8, device=earlier.device)
+            if difference is None:
+                difference = torch.empty((lh, lw), dtype=torch.float32, device=earlier.device)
+        else:
+            data = np.zeros((lh, lw), np.uint8) if data is None else data
+            difference = np.zeros((lh, lw), np.float32) if difference is None else difference
+        b = _Buffers()
+        ep = b.ptr(earlier, np.float32)
+        lp = b.ptr(later, np.float32)
+        dp = b.ptr(data)
+        fp = b.ptr(difference)
+        g = grid.native()
+        N.check(self._lib.tg_seam_samples(self._handle, ep, lp, C.byref(g), col0, row0, lw, lh,
+                                          N.NoData(*nodata), dp, fp, b.memory,
+                                          _stream(b.memory)))
+        return data, difference
+
     def philox_probe(self, sextets: np.ndarray):
         """(words [n, 4] u32, normals [n] f64) of n (counter x4, key x2) sextets."""
         sextets = np.ascontiguousarray(sextets, np.uint32).reshape(-1, 6)

@@ -195,3 +195,53 @@ def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: fl
         crater_footprints=np.concatenate(footprints) if footprints else np.zeros(0),
         boulders=np.ascontiguousarray(np.concatenate(stones)) if stones else np.zeros((0, 5)),
         grids=grids)
+
+
+@dataclass
+class DemRefinement:
+    """The DEM refinement ("dem20481"): a 2049^2 float32 DEM at 5 m (12-octave fBm, wavelength
+    20 km, amplitude 2000 m) refined 10-fold by diamond-square (F = 2.2, i.e. Hurst 0.8, 4 levels,
+    bilinear read) to 20481^2 at 0.5 m as 2 x 2 patches, each its own refinement (its own seed)
+    of a quadrant with a 64-cell overlap, chained with Height seams reaching 64 cells (3 L = 32 m);
+    then 2,000,000 craters expected over the grid, N(>D) ~ D^-2 on [1, 100] m."""
+
+    post_grid: GridSpec
+    fractals: np.ndarray
+    grid: GridSpec
+    windows: list
+    seeds: list
+    fractal_dimension: float
+    scale: float
+    decay_length: float
+    crater_kernel: np.ndarray
+    crater_records: np.ndarray
+    crater_data: np.ndarray
+    crater_footprints: np.ndarray
+
+    @property
+    def cells(self) -> int:
+        return self.grid.cells
+
+
+def dem20481(side: int = 20481, posts: int = 2049, overlap: int = 64, seed: int = 7,
+             craters: float = 2e6, crater_seed: int = 11) -> DemRefinement:
+    """The DEM refinement workload (or a smaller one of the same make: `side` output cells a
+    side at 0.5 m over `posts` posts at 5 m; craters scale with the area)."""
+    from .chain import Window
+
+    post_grid = centered(posts, posts, 5.0)
+    grid = centered(side, side, 0.5)
+    half = side // 2
+    lo, hi = half + overlap // 2, half - overlap // 2
+    windows = [Window(0, 0, lo, lo), Window(hi, 0, side - hi, lo),
+               Window(0, hi, lo, side - hi), Window(hi, hi, side - hi, side - hi)]
+    area = grid.width * grid.height * grid.pixel ** 2
+    expected = craters * area / (20481 * 0.5) ** 2
+    c = expected / (area * (1.0 ** -2.0 - 100.0 ** -2.0))
+    kernel, records, data, footprints = crater_batch(
+        crater_population(crater_seed, c, 1.0, 100.0), grid)
+    return DemRefinement(post_grid,
+                         np.array([fractal(seed=3, wavelength=20000.0, amplitude=2000.0,
+                                           octaves=12)]),
+                         grid, windows, [seed + k for k in range(4)], 2.2, 1.5,
+                         overlap * grid.pixel / 3.0, kernel, records, data, footprints)

@@ -163,3 +163,39 @@ def test_refuses_bad_options(device):
         device.seam_solve(data, diff, 1.0, 1.0, "feather", width=-1.0)
     with pytest.raises(TgError):
         device.seam_solve(data, diff, 1.0, 1.0, "slope", levels=0)
+
+
+@pytest.mark.parametrize("scene,mode", CASES)
+def test_samples_are_the_reference_lattice(device, z, scene, mode):
+    # The lattice pads the rasters' grid by ceil(reach / spacing) + 3 posts on every side.
+    import math
+
+    key = f"{scene}_{mode}"
+    g = grid_of(z[f"{scene}_grid"])
+    lat = z[f"{key}_lattice"]
+    pad = (int(lat[0]) - g.width) // 2
+    _, width, decay = z[f"{key}_options"]
+    assert pad == math.ceil((width if mode == "feather" else 3.0 * decay) / g.pixel) + 3
+    data, diff = device.seam_samples(z[f"{scene}_earlier"], z[f"{scene}_later"], g, -pad, -pad,
+                                     int(lat[0]), int(lat[1]))
+    assert np.array_equal(data, z[f"{key}_data"])
+    assert np.array_equal(diff.view(np.uint32), z[f"{key}_difference"].view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", ["feather", "height"])
+def test_wide_reach(device, mode):
+    # A reach wider than a distance window in shared memory holds: the row-by-row passes.
+    rng = np.random.default_rng(12)
+    h, w = 240, 260
+    data = np.ones((h, w), np.uint8)
+    yy, xx = np.mgrid[0:h, 0:w]
+    data[((yy - 120) / 70.0) ** 2 + ((xx - 140) / 90.0) ** 2 < 1.0] = 0
+    diff = np.where(data != 0, 2.0 + 0.01 * xx - 0.02 * yy + 0.1 * rng.standard_normal((h, w)),
+                    np.nan).astype(np.float32)
+    field, _ = device.seam_solve(data, diff, 0.5, 0.5, mode, width=120.0, decay_length=40.0)
+    if mode == "feather":
+        want = S.feather(data, diff, 0.5, 0.5, 120.0)
+        assert np.array_equal(field.view(np.uint32), want.view(np.uint32))
+    else:
+        want = S.solve(data, diff, 0.5, 0.5, mode, 40.0)
+        assert np.abs(field.astype(np.float64) - want).max() <= 1e-4
