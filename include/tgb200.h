@@ -270,7 +270,7 @@ int tg_measure_alu(tg_device* device, double* lane_ops_per_second);
  * these replace it and FillGridGaps (source_chain.cpp:167). */
 
 /* mode: 0 none, 1 feather, 2 height, 3 slope (ChainSeamMode). levels, sweeps and
- * coarsest_sweeps shape the multigrid preconditioner (4, 2 and 100 by default in the Python
+ * coarsest_sweeps shape the multigrid preconditioner (4, 2 and 20 by default in the Python
  * layer); tolerance is the conjugate gradients' stop, relative to the first residual (1e-10 as
  * the reference when 0). */
 typedef struct tg_seam_options {
@@ -288,6 +288,8 @@ typedef struct tg_seam_stats {
     uint32_t levels;     /* multigrid levels used */
     uint32_t iterations; /* conjugate gradient iterations */
     uint32_t reserved;
+    double prepare_ms;   /* band, distances, unknowns and levels (device time) */
+    double solve_ms;     /* the conjugate gradients (device time) */
 } tg_seam_stats;
 
 /* The seam field on a width x height lattice of posts dx by dy apart (row 0 first), from the

@@ -159,6 +159,25 @@ def chain(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: 
     return out
 
 
+def patch_chain(lib: C.CDLL, rasters: list, grids: list, mode: int, width: float, decay: float,
+                out_grid) -> np.ndarray:
+    """A SourceChain of raster patches, each on its own grid (tgref_patch_chain), on `out_grid`."""
+    rasters = [np.ascontiguousarray(r, np.float32) for r in rasters]
+    n = len(rasters)
+    ptrs = (C.c_void_p * n)(*[r.ctypes.data for r in rasters])
+    widths = np.array([g.width for g in grids], np.uint32)
+    heights = np.array([g.height for g in grids], np.uint32)
+    transforms = np.array([g.transform() for g in grids], np.float64).ravel()
+    ot = np.array(out_grid.transform(), np.float64)
+    out = np.zeros((out_grid.height, out_grid.width), np.float32)
+    st = lib.tgref_patch_chain(n, C.cast(ptrs, C.c_void_p), widths.ctypes.data,
+                               heights.ctypes.data, transforms.ctypes.data, mode, width, decay,
+                               out_grid.width, out_grid.height, ot.ctypes.data, out.ctypes.data)
+    if st != 0:
+        raise RuntimeError(f"tgref_patch_chain failed: {lib.tgref_error().decode()}")
+    return out
+
+
 def config1_craters() -> dict:
     """The 257 x 257, 1 m crater scene (2000 craters expected over the extent, N(>D) ~ D^-2 on
     [2, 60] m, depth/diameter 0.2, rim 0.04 D, uniform ages over 1 Gyr, seed 1)."""
@@ -238,6 +257,8 @@ def _harness(name: str) -> C.CDLL:
         lib.tgref_seam.restype = C.c_int
         lib.tgref_chain.argtypes = [P, P, _U32, _U32, P, C.c_int, _D, _D, _U32, _U32, P, P]
         lib.tgref_chain.restype = C.c_int
+        lib.tgref_patch_chain.argtypes = [_U32, P, P, P, P, C.c_int, _D, _D, _U32, _U32, P, P]
+        lib.tgref_patch_chain.restype = C.c_int
     return lib
 
 

@@ -455,6 +455,45 @@ int tgref_chain(const float* earlier, const float* later, uint32_t w, uint32_t h
     }
 }
 
+/// A SourceChain of `n` raster sources, source k (`widths[k]` x `heights[k]` floats at `rasters[k]`,
+/// NaN where it has no data) on its own grid (GDAL transform `transforms[6k..6k+5]`), joined by
+/// `mode`, evaluated on an `ow` x `oh` grid: the chain's nested seams as the reference builds
+/// them (SourceChain::Seam over BoundedGrid of the source before the last, source_chain.cpp:144).
+int tgref_patch_chain(uint32_t n, const float* const* rasters, const uint32_t* widths,
+                      const uint32_t* heights, const double* transforms, int mode, double width,
+                      double decay, uint32_t ow, uint32_t oh, const double* outTransform,
+                      float* out) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        std::vector<std::shared_ptr<const Source>> sources;
+        for (uint32_t k = 0; k < n; ++k) {
+            const double* t = transforms + 6 * k;
+            const RasterGrid grid{widths[k], heights[k],
+                                  GeoTransform::FromGdal({t[0], t[1], t[2], t[3], t[4], t[5]})};
+            Raster<float> r(grid);
+            std::memcpy(r.Values().data(), rasters[k], size_t(widths[k]) * heights[k] * 4);
+            r.SetNoData(std::numeric_limits<float>::quiet_NaN());
+            sources.push_back(std::make_shared<RasterSource>(std::move(r)));
+        }
+        auto chain = std::make_shared<SourceChain>(std::move(sources),
+                                                   MakeSeams(mode, width, decay));
+        const Terrain terrain(Surface{}, chain, {});
+        EvaluationOptions evaluation;
+        evaluation.threads = 0;
+        evaluation.backend = Backend::Cpu;
+        const RasterGrid grid{ow, oh,
+                              GeoTransform::FromGdal({outTransform[0], outTransform[1],
+                                                      outTransform[2], outTransform[3],
+                                                      outTransform[4], outTransform[5]})};
+        const Raster<float> result = terrain.Evaluate(grid, evaluation);
+        std::memcpy(out, result.Values().data(), result.Values().size() * sizeof(float));
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
 /// The scene's heights without its boulder layer (the base the boulders are drawn on).
 int tgref_evaluate_below_boulders(const tgref_scene* s, unsigned threads, float* out) {
     try {

@@ -224,3 +224,51 @@ def fill(field: np.ndarray, lattice: tuple, later: np.ndarray, grid, heights: np
     out[rows, cols] = np.where(correction == 0.0, value,
                                (value.astype(np.float64) + correction).astype(np.float32))
     return out
+
+
+def chain(patches: list, windows: list, grid, mode: str, width: float = 50.0,
+          decay_length: float = 50.0) -> np.ndarray:
+    """SourceChain::FillSamples (src/sources/source_chain.cpp:154-192) of raster patches on
+    windows (col0, row0, width, height) of `grid`: each later patch fills the cells the chain
+    before it leaves without data, plus the seam of its link, whose lattice is the window of the
+    patch before it padded by ceil(reach / spacing) + 3 posts (SourceChain::Seam, SeamLattice,
+    source_chain.cpp:94-152)."""
+    reach = width if mode == "feather" else REACH_DECAYS * decay_length
+    pad = math.ceil(reach / grid.pixel) + 3
+    h, w = grid.height, grid.width
+    heights = np.full((h, w), np.nan, np.float32)
+
+    def place(k):
+        out = np.full((h, w), np.nan, np.float32)
+        c0, r0, pw, ph = windows[k]
+        out[r0:r0 + ph, c0:c0 + pw] = patches[k]
+        return out
+
+    heights[:] = place(0)
+    for k in range(1, len(patches)):
+        later = place(k)
+        c0, r0, pw, ph = windows[k - 1]
+        lc0, lr0, lw, lh = c0 - pad, r0 - pad, pw + 2 * pad, ph + 2 * pad
+        data = np.zeros((lh, lw), np.uint8)
+        diff = np.full((lh, lw), np.nan, np.float32)
+        rows = np.arange(lr0, lr0 + lh)
+        cols = np.arange(lc0, lc0 + lw)
+        ri = (rows >= 0) & (rows < h)
+        ci = (cols >= 0) & (cols < w)
+        a = heights[np.ix_(rows[ri], cols[ci])]
+        b = later[np.ix_(rows[ri], cols[ci])]
+        has = np.isfinite(a)
+        sub = data[np.ix_(ri, ci)]
+        sub[:] = has
+        data[np.ix_(ri, ci)] = sub
+        both = has & np.isfinite(b)
+        d = np.where(both, (a.astype(np.float64) - b).astype(np.float32), np.float32(np.nan))
+        diff[np.ix_(ri, ci)] = d
+        if mode == "feather":
+            field = feather(data, diff, grid.pixel, grid.pixel, width)
+        else:
+            field = solve(data, diff, grid.pixel, grid.pixel, mode, decay_length)
+        lattice = (grid.x0 + lc0 * grid.pixel, grid.pixel, 0.0, grid.y0 - lr0 * grid.pixel, 0.0,
+                   -grid.pixel)
+        heights = fill(field, lattice, later, grid, heights)
+    return heights

@@ -150,7 +150,8 @@ class SeamOptions(C.Structure):
 
 
 class SeamStats(C.Structure):
-    _fields_ = [("unknowns", _U32), ("levels", _U32), ("iterations", _U32), ("reserved", _U32)]
+    _fields_ = [("unknowns", _U32), ("levels", _U32), ("iterations", _U32), ("reserved", _U32),
+                ("prepare_ms", _D), ("solve_ms", _D)]
 
 
 SIGNATURES.update({

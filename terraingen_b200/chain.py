@@ -48,7 +48,7 @@ class Seams:
     decay_length: float = 50.0
     levels: int = 4
     sweeps: int = 2
-    coarsest_sweeps: int = 100
+    coarsest_sweeps: int = 20
 
     @property
     def reach(self) -> float:

@@ -234,6 +234,9 @@ void tg_close(tg_device* d) {
     for (Buffer& b : d->slots) {
         b.release();
     }
+    if (d->releaseSeams != nullptr) {
+        d->releaseSeams(d->seams);
+    }
     if (d->pinnedStatus != nullptr) {
         cudaFreeHost(d->pinnedStatus);
     }

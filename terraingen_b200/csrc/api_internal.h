@@ -104,4 +104,7 @@ struct tg_device {
     uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
     // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
     unsigned long long craterPairs = 0, boulderPairs = 0;
+    // The seam solve's scratch, kept across calls and released by tg_close.
+    void* seams = nullptr;
+    void (*releaseSeams)(void*) = nullptr;
 };

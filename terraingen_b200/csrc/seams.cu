@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -564,38 +565,107 @@ struct LevelView {
     const uint32_t* position;  // [n] post of each unknown
     double cx, cy, center;     // 1/dx^2, 1/dy^2, 2 cx + 2 cy + 1/L^2
     double diagonal;           // the operator's center weight
+    // Per unknown, the compact indices (or ~0u) of the posts the operator reads around it, in
+    // kStencil order: 4 of them for order 1, 12 for order 2.
+    const uint32_t* nbr;
+    // Per unknown, the next coarser level's parent, across its column, across its row and
+    // diagonally (Link, seam_field.cpp:367); null on the coarsest level.
+    const uint32_t* parents;
+    // Per unknown of a coarser level, the 4 x 4 finer posts (2C-1 .. 2C+2 by 2R-1 .. 2R+2) its
+    // restriction gathers, row by row; null on the finest level.
+    const uint32_t* children;
 };
 
-// u at post (col + dc, row + dr), 0 off the unknowns.
-template <typename T>
-__device__ __forceinline__ T at(const LevelView& L, const T* u, int col, int row, int dc, int dr) {
-    const int c = col + dc, r = row + dr;
-    if (c < 0 || r < 0 || c >= int(L.w) || r >= int(L.h)) {
-        return T(0);
-    }
-    const uint32_t j = L.index[size_t(r) * L.w + uint32_t(c)];
-    return j == kNone ? T(0) : u[j];
-}
+// The offsets of the 13-point stencil after its center (kNear13, seam_field.cpp:267); the first
+// four are the 5-point stencil's.
+__constant__ int2 kStencil[12] = {{-1, 0}, {1, 0},  {0, -1}, {0, 1},  {-2, 0}, {2, 0},
+                                  {0, -2}, {0, 2},  {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
 
 // The operator at unknown k of u (0 off the unknowns): B = -Laplacian + 1/L^2 on 5 points
 // (order 1), or B applied twice on 13 points (order 2), as ApplyScreened / Apply
-// (seam_field.cpp:389-407).
-template <int kOrder, typename T>
-__device__ __forceinline__ double apply_at(const LevelView& L, const T* u, uint32_t k) {
+// (seam_field.cpp:389-407), in the arithmetic of `A` (float on the FP32 levels).
+template <typename T, typename A>
+__device__ __forceinline__ A tap(const T* u, uint32_t j) {
+    return j == kNone ? A(0) : A(u[j]);
+}
+
+template <int kOrder, typename T, typename A = double>
+__device__ __forceinline__ A apply_at(const LevelView& L, const T* u, uint32_t k) {
+    const uint4 n0 = reinterpret_cast<const uint4*>(L.nbr)[size_t(k) * (kOrder == 1 ? 1 : 3)];
+    const A cx = A(L.cx), cy = A(L.cy), c0 = A(L.center);
+    const A sx = tap<T, A>(u, n0.x) + tap<T, A>(u, n0.y);
+    const A sy = tap<T, A>(u, n0.z) + tap<T, A>(u, n0.w);
+    if (kOrder == 1) {
+        return c0 * A(u[k]) - cx * sx - cy * sy;
+    }
+    const uint4 n1 = reinterpret_cast<const uint4*>(L.nbr)[size_t(k) * 3 + 1];
+    const uint4 n2 = reinterpret_cast<const uint4*>(L.nbr)[size_t(k) * 3 + 2];
+    const A s2x = tap<T, A>(u, n1.x) + tap<T, A>(u, n1.y);
+    const A s2y = tap<T, A>(u, n1.z) + tap<T, A>(u, n1.w);
+    const A sd = tap<T, A>(u, n2.x) + tap<T, A>(u, n2.y) + tap<T, A>(u, n2.z) +
+                 tap<T, A>(u, n2.w);
+    return A(L.diagonal) * A(u[k]) - A(2) * c0 * (cx * sx + cy * sy) + cx * cx * s2x +
+           cy * cy * s2y + A(2) * cx * cy * sd;
+}
+
+// The stencil's neighbors of each unknown (compact indices, ~0u off the unknowns).
+template <int kOrder>
+__global__ void neighbors_kernel(const LevelView L, uint32_t* __restrict__ nbr) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= L.n) {
+        return;
+    }
+    constexpr int kTaps = kOrder == 1 ? 4 : 12;
     const uint32_t p = L.position[k];
     const int col = int(p % L.w), row = int(p / L.w);
-    const double cx = L.cx, cy = L.cy, c0 = L.center;
-    const double sx = double(at(L, u, col, row, -1, 0)) + double(at(L, u, col, row, 1, 0));
-    const double sy = double(at(L, u, col, row, 0, -1)) + double(at(L, u, col, row, 0, 1));
-    if (kOrder == 1) {
-        return c0 * double(u[k]) - cx * sx - cy * sy;
+    for (int j = 0; j < kTaps; ++j) {
+        const int c = col + kStencil[j].x, r = row + kStencil[j].y;
+        nbr[size_t(k) * kTaps + j] =
+            c < 0 || r < 0 || c >= int(L.w) || r >= int(L.h)
+                ? kNone
+                : L.index[size_t(r) * L.w + uint32_t(c)];
     }
-    const double s2x = double(at(L, u, col, row, -2, 0)) + double(at(L, u, col, row, 2, 0));
-    const double s2y = double(at(L, u, col, row, 0, -2)) + double(at(L, u, col, row, 0, 2));
-    const double sd = double(at(L, u, col, row, -1, -1)) + double(at(L, u, col, row, 1, -1)) +
-                      double(at(L, u, col, row, -1, 1)) + double(at(L, u, col, row, 1, 1));
-    return L.diagonal * double(u[k]) - 2.0 * c0 * (cx * sx + cy * sy) + cx * cx * s2x +
-           cy * cy * s2y + 2.0 * cx * cy * sd;
+}
+
+// Each unknown's coarse parent and its neighbors across the unknown's column, row and diagonal.
+__global__ void parents_kernel(const LevelView F, const LevelView Cl,
+                               uint32_t* __restrict__ parents) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= F.n) {
+        return;
+    }
+    const uint32_t p = F.position[k];
+    const int col = int(p % F.w), row = int(p / F.w);
+    const int pc = col / 2, pr = row / 2;
+    const int ac = pc + (col % 2 == 1 ? 1 : -1), ar = pr + (row % 2 == 1 ? 1 : -1);
+    const int cs[4] = {pc, ac, pc, ac}, rs[4] = {pr, pr, ar, ar};
+    for (int j = 0; j < 4; ++j) {
+        parents[size_t(k) * 4 + j] =
+            cs[j] < 0 || rs[j] < 0 || cs[j] >= int(Cl.w) || rs[j] >= int(Cl.h)
+                ? kNone
+                : Cl.index[size_t(rs[j]) * Cl.w + uint32_t(cs[j])];
+    }
+}
+
+// Each coarse unknown's 4 x 4 finer posts, as restriction gathers them.
+__global__ void children_kernel(const LevelView F, const LevelView Cl,
+                                uint32_t* __restrict__ children) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Cl.n) {
+        return;
+    }
+    const uint32_t p = Cl.position[k];
+    const int C = int(p % Cl.w), R = int(p / Cl.w);
+    for (int j = 0; j < 4; ++j) {
+        const int fy = 2 * R - 1 + j;
+        for (int i = 0; i < 4; ++i) {
+            const int fx = 2 * C - 1 + i;
+            children[size_t(k) * 16 + j * 4 + i] =
+                fx < 0 || fy < 0 || fx >= int(F.w) || fy >= int(F.h)
+                    ? kNone
+                    : F.index[size_t(fy) * F.w + uint32_t(fx)];
+        }
+    }
 }
 
 // The right-hand side: minus the operator of the fixed values (the field at every post that is
@@ -626,38 +696,58 @@ __global__ void rhs_kernel(const LevelView L, const float* __restrict__ field,
     rhs[k] = -a;
 }
 
+// The conjugate gradients' scalars, on the device so an iteration needs no host round trip.
+// Once `done` is set every kernel of an iteration returns at once, so iterations launched after
+// the stop leave the solution as it was.
+struct CgState {
+    double fit;        // r . z of the current direction
+    double target;     // the residual norm to stop at
+    double step;
+    double ratio;
+    double dots[2];
+    uint32_t done;
+    uint32_t iterations;
+    uint32_t maxIterations;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ bool stopped(const CgState* cg) {
+    return cg != nullptr && cg->done != 0u;
+}
+
 // Damped Jacobi: xn = x + omega (b - A x) / diagonal; from x = 0 when `x` is null.
 template <int kOrder, typename T>
 __global__ void jacobi_kernel(const LevelView L, const T* __restrict__ b, const T* __restrict__ x,
-                              T* __restrict__ xn, double omega) {
+                              T* __restrict__ xn, double omega, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= L.n) {
+    if (k >= L.n || stopped(cg)) {
         return;
     }
+    const T scale = T(omega / L.diagonal);
     if (x == nullptr) {
-        xn[k] = T(omega * double(b[k]) / L.diagonal);
+        xn[k] = scale * b[k];
         return;
     }
-    const double r = double(b[k]) - apply_at<kOrder>(L, x, k);
-    xn[k] = T(double(x[k]) + omega * r / L.diagonal);
+    const T r = b[k] - apply_at<kOrder, T, T>(L, x, k);
+    xn[k] = x[k] + scale * r;
 }
 
 template <int kOrder, typename T>
 __global__ void residual_kernel(const LevelView L, const T* __restrict__ b,
-                                const T* __restrict__ x, T* __restrict__ r) {
+                                const T* __restrict__ x, T* __restrict__ r, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < L.n) {
-        r[k] = T(double(b[k]) - apply_at<kOrder>(L, x, k));
+    if (k < L.n && !stopped(cg)) {
+        r[k] = b[k] - apply_at<kOrder, T, T>(L, x, k);
     }
 }
 
 // The operator applied to a direction (FP64, for the conjugate gradients).
 template <int kOrder>
 __global__ void apply_kernel(const LevelView L, const double* __restrict__ u,
-                             double* __restrict__ out) {
+                             double* __restrict__ out, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < L.n) {
-        out[k] = apply_at<kOrder>(L, u, k);
+    if (k < L.n && !stopped(cg)) {
+        out[k] = apply_at<kOrder, double, double>(L, u, k);
     }
 }
 
@@ -666,28 +756,20 @@ __global__ void apply_kernel(const LevelView L, const double* __restrict__ u,
 // 1/16, seam_field.cpp:56).
 template <typename Tf, typename Tc>
 __global__ void restrict_kernel(const LevelView F, const LevelView Cl, const Tf* __restrict__ r,
-                                Tc* __restrict__ b) {
+                                Tc* __restrict__ b, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= Cl.n) {
+    if (k >= Cl.n || stopped(cg)) {
         return;
     }
-    const uint32_t p = Cl.position[k];
-    const int C = int(p % Cl.w), R = int(p / Cl.w);
     const double axis[4] = {0.25, 0.75, 0.75, 0.25};  // fine 2C-1, 2C, 2C+1, 2C+2
+    const uint4* kids = reinterpret_cast<const uint4*>(Cl.children) + size_t(k) * 4;
     double sum = 0.0;
     for (int j = 0; j < 4; ++j) {
-        const int fy = 2 * R - 1 + j;
-        if (fy < 0 || fy >= int(F.h)) {
-            continue;
-        }
+        const uint4 row = kids[j];
+        const uint32_t q[4] = {row.x, row.y, row.z, row.w};
         for (int i = 0; i < 4; ++i) {
-            const int fx = 2 * C - 1 + i;
-            if (fx < 0 || fx >= int(F.w)) {
-                continue;
-            }
-            const uint32_t q = F.index[size_t(fy) * F.w + uint32_t(fx)];
-            if (q != kNone) {
-                sum += 0.25 * axis[i] * axis[j] * double(r[q]);
+            if (q[i] != kNone) {
+                sum += 0.25 * axis[i] * axis[j] * double(r[q[i]]);
             }
         }
     }
@@ -698,19 +780,16 @@ __global__ void restrict_kernel(const LevelView F, const LevelView Cl, const Tf*
 // its column, its row and diagonally (Link, seam_field.cpp:367).
 template <typename Tc, typename Tf>
 __global__ void prolong_kernel(const LevelView F, const LevelView Cl, const Tc* __restrict__ xc,
-                               Tf* __restrict__ x) {
+                               Tf* __restrict__ x, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= F.n) {
+    if (k >= F.n || stopped(cg)) {
         return;
     }
-    const uint32_t p = F.position[k];
-    const int col = int(p % F.w), row = int(p / F.w);
-    const int pc = col / 2, pr = row / 2;
-    const int ac = pc + (col % 2 == 1 ? 1 : -1), ar = pr + (row % 2 == 1 ? 1 : -1);
-    const double correction = 0.5625 * double(at(Cl, xc, pc, pr, 0, 0)) +
-                              0.1875 * double(at(Cl, xc, ac, pr, 0, 0)) +
-                              0.1875 * double(at(Cl, xc, pc, ar, 0, 0)) +
-                              0.0625 * double(at(Cl, xc, ac, ar, 0, 0));
+    const uint4 q = reinterpret_cast<const uint4*>(F.parents)[k];
+    const double correction = 0.5625 * tap<Tc, double>(xc, q.x) +
+                              0.1875 * tap<Tc, double>(xc, q.y) +
+                              0.1875 * tap<Tc, double>(xc, q.z) +
+                              0.0625 * tap<Tc, double>(xc, q.w);
     x[k] = Tf(double(x[k]) + correction);
 }
 
@@ -722,7 +801,10 @@ constexpr int kDotBlocks = 512;
 // fixed order, so every run gives the same bits.
 __global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
                            const double* __restrict__ c, const double* __restrict__ d, uint32_t n,
-                           double* __restrict__ partial) {
+                           double* __restrict__ partial, const CgState* cg) {
+    if (stopped(cg)) {
+        return;
+    }
     __shared__ double s0[256], s1[256];
     double x = 0.0, y = 0.0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -747,8 +829,9 @@ __global__ void dot_kernel(const double* __restrict__ a, const double* __restric
     }
 }
 
-__global__ void dot_finish_kernel(const double* __restrict__ partial, double* __restrict__ out) {
-    if (threadIdx.x == 0) {
+__global__ void dot_finish_kernel(const double* __restrict__ partial, double* __restrict__ out,
+                                  const CgState* cg) {
+    if (threadIdx.x == 0 && !stopped(cg)) {
         double x = 0.0, y = 0.0;
         for (int i = 0; i < kDotBlocks; ++i) {
             x += partial[i];
@@ -759,12 +842,43 @@ __global__ void dot_finish_kernel(const double* __restrict__ partial, double* __
     }
 }
 
+// After p . Ap: the step, or the stop when the curvature is not positive or the iterations are
+// spent (PreconditionedCg, seam_field.cpp:519-527).
+__global__ void cg_step_kernel(CgState* cg) {
+    if (cg->done != 0u) {
+        return;
+    }
+    const double curvature = cg->dots[0];
+    if (cg->iterations >= cg->maxIterations || !(cg->fit > 0.0) || !(curvature > 0.0)) {
+        cg->done = 1u;
+        return;
+    }
+    cg->step = cg->fit / curvature;
+    cg->iterations += 1u;
+}
+
+// After r . r and r . z: the stop at the target residual, else the direction's ratio
+// (seam_field.cpp:532-542).
+__global__ void cg_next_kernel(CgState* cg) {
+    if (cg->done != 0u) {
+        return;
+    }
+    if (sqrt(cg->dots[0]) <= cg->target) {
+        cg->done = 1u;
+        return;
+    }
+    const double next = cg->dots[1];
+    cg->ratio = next / cg->fit;
+    cg->fit = next;
+}
+
 // x += step p, r -= step ap.
 __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
                                  const double* __restrict__ p, const double* __restrict__ ap,
-                                 uint32_t n, double step) {
+                                 uint32_t n, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) {
+    if (k < n && !stopped(cg)) {
+        const double step = cg->step;
         x[k] += step * p[k];
         r[k] -= step * ap[k];
     }
@@ -772,18 +886,28 @@ __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
 
 // p = z + ratio p.
 __global__ void cg_direction_kernel(double* __restrict__ p, const double* __restrict__ z,
-                                    uint32_t n, double ratio) {
+                                    uint32_t n, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) {
-        p[k] = z[k] + ratio * p[k];
+    if (k < n && !stopped(cg)) {
+        p[k] = z[k] + cg->ratio * p[k];
     }
 }
 
 template <typename A, typename B>
-__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, uint32_t n) {
+__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, uint32_t n,
+                               const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) {
+    if (k < n && !stopped(cg)) {
         out[k] = B(in[k]);
+    }
+}
+
+template <typename T>
+__global__ void copy_kernel(const T* __restrict__ in, T* __restrict__ out, uint32_t n,
+                            const CgState* cg) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n && !stopped(cg)) {
+        out[k] = in[k];
     }
 }
 
@@ -921,6 +1045,26 @@ __global__ void seam_samples_kernel(const float* __restrict__ earlier,
     }
 }
 
+// Three timing events, released with the scope.
+struct Events {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    cudaError_t create() {
+        for (cudaEvent_t& x : e) {
+            if (cudaError_t err = cudaEventCreate(&x)) {
+                return err;
+            }
+        }
+        return cudaSuccess;
+    }
+    ~Events() {
+        for (cudaEvent_t x : e) {
+            if (x != nullptr) {
+                cudaEventDestroy(x);
+            }
+        }
+    }
+};
+
 uint32_t blocks_for(size_t n, uint32_t threads = 256) {
     return uint32_t((n + threads - 1) / threads);
 }
@@ -929,28 +1073,40 @@ uint32_t blocks_for(size_t n, uint32_t threads = 256) {
 struct Level {
     LevelView view{};
     Buffer index, position, x, b, t;  // x, b, t: float (double on the coarsest level)
+    Buffer nbr, parents, children;
 };
 
+// The seam calls' device scratch, one per device, grown as needed and kept across calls (no
+// allocation, and so no device-wide synchronization of a free, on a call that fits).
 struct Work {
     Buffer marks, flags, scan, distance, carried, distance2, carried2, count, partial, dots;
-    Buffer tileCounts, tileList;
+    Buffer tileCounts, tileList, cg;
     Buffer cgX, cgR, cgP, cgAp, cgZ, rhs;
+    Buffer hostIn, hostIn2, hostOut, hostOut2;  // device copies of host-memory arguments
     Level levels[kMaxLevels];
     ~Work() {
         for (Buffer* b : {&marks, &flags, &scan, &distance, &carried, &distance2, &carried2,
-                          &count, &partial, &dots, &tileCounts, &tileList,
-                          &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs}) {
+                          &count, &partial, &dots, &tileCounts, &tileList, &cg,
+                          &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs,
+                          &hostIn, &hostIn2, &hostOut, &hostOut2}) {
             b->release();
         }
         for (Level& l : levels) {
-            l.index.release();
-            l.position.release();
-            l.x.release();
-            l.b.release();
-            l.t.release();
+            for (Buffer* b : {&l.index, &l.position, &l.x, &l.b, &l.t, &l.nbr, &l.parents,
+                              &l.children}) {
+                b->release();
+            }
         }
     }
 };
+
+Work& device_work(tg_device* d) {
+    if (d->seams == nullptr) {
+        d->seams = new Work();
+        d->releaseSeams = [](void* w) { delete static_cast<Work*>(w); };
+    }
+    return *static_cast<Work*>(d->seams);
+}
 
 // Compacts `flags` (0 / 1 per post of a w x h lattice) into the level's index and positions.
 int compact(Work& wk, Level& level, uint32_t w, uint32_t h, cudaStream_t s) {
@@ -990,19 +1146,36 @@ struct Solver {
     cudaStream_t s;
     double omega;
     int sweeps, coarsest;
+    const CgState* cg;     // the device state iterations stop on (null: always run)
+    cudaStream_t capture;  // a stream of the library's own, the iterations are captured on
 };
 
+double* cg_dots(CgState* cg) {
+    return reinterpret_cast<double*>(reinterpret_cast<char*>(cg) + offsetof(CgState, dots));
+}
+
 template <int kOrder>
-cudaError_t jacobi(const LevelView& L, const void* b, const void* x, void* xn, double omega,
-                   bool coarsest, cudaStream_t s) {
+cudaError_t jacobi(const Solver& sv, const LevelView& L, const void* b, const void* x, void* xn,
+                   bool coarsest) {
     if (coarsest) {
-        jacobi_kernel<kOrder, double><<<blocks_for(L.n), 256, 0, s>>>(
+        jacobi_kernel<kOrder, double><<<blocks_for(L.n), 256, 0, sv.s>>>(
             L, static_cast<const double*>(b), static_cast<const double*>(x),
-            static_cast<double*>(xn), omega);
+            static_cast<double*>(xn), sv.omega, sv.cg);
     } else {
-        jacobi_kernel<kOrder, float><<<blocks_for(L.n), 256, 0, s>>>(
+        jacobi_kernel<kOrder, float><<<blocks_for(L.n), 256, 0, sv.s>>>(
             L, static_cast<const float*>(b), static_cast<const float*>(x),
-            static_cast<float*>(xn), omega);
+            static_cast<float*>(xn), sv.omega, sv.cg);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t copy_level(const Solver& sv, const void* from, void* to, uint32_t n, bool wide) {
+    if (wide) {
+        copy_kernel<double><<<blocks_for(n), 256, 0, sv.s>>>(static_cast<const double*>(from),
+                                                            static_cast<double*>(to), n, sv.cg);
+    } else {
+        copy_kernel<float><<<blocks_for(n), 256, 0, sv.s>>>(static_cast<const float*>(from),
+                                                           static_cast<float*>(to), n, sv.cg);
     }
     return cudaGetLastError();
 }
@@ -1021,13 +1194,11 @@ int vcycle(Solver& sv, int d) {
     void* cur = nullptr;
     for (int i = 0; i < sweeps; ++i) {
         void* next = (i % 2 == 0) ? L.x.ptr : L.t.ptr;
-        TG_CUDA(jacobi<kOrder>(L.view, L.b.ptr, cur, next, sv.omega, last, sv.s), "jacobi");
+        TG_CUDA(jacobi<kOrder>(sv, L.view, L.b.ptr, cur, next, last), "jacobi");
         cur = next;
     }
     if (cur != L.x.ptr) {
-        TG_CUDA(cudaMemcpyAsync(L.x.ptr, cur, size_t(L.view.n) * (last ? 8 : 4),
-                                cudaMemcpyDeviceToDevice, sv.s),
-                "copy");
+        TG_CUDA(copy_level(sv, cur, L.x.ptr, L.view.n, last), "copy");
     }
     if (last) {
         return TG_OK;
@@ -1037,13 +1208,15 @@ int vcycle(Solver& sv, int d) {
     // residual into t, restricted into the coarse b
     residual_kernel<kOrder, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
         L.view, static_cast<const float*>(L.b.ptr), static_cast<const float*>(L.x.ptr),
-        static_cast<float*>(L.t.ptr));
+        static_cast<float*>(L.t.ptr), sv.cg);
     if (coarseLast) {
         restrict_kernel<float, double><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
-            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<double*>(C.b.ptr));
+            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<double*>(C.b.ptr),
+            sv.cg);
     } else {
         restrict_kernel<float, float><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
-            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<float*>(C.b.ptr));
+            L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<float*>(C.b.ptr),
+            sv.cg);
     }
     TG_CUDA(cudaGetLastError(), "restrict launch");
     if (int st = vcycle<kOrder>(sv, d + 1)) {
@@ -1051,21 +1224,21 @@ int vcycle(Solver& sv, int d) {
     }
     if (coarseLast) {
         prolong_kernel<double, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
-            L.view, C.view, static_cast<const double*>(C.x.ptr), static_cast<float*>(L.x.ptr));
+            L.view, C.view, static_cast<const double*>(C.x.ptr), static_cast<float*>(L.x.ptr),
+            sv.cg);
     } else {
         prolong_kernel<float, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
-            L.view, C.view, static_cast<const float*>(C.x.ptr), static_cast<float*>(L.x.ptr));
+            L.view, C.view, static_cast<const float*>(C.x.ptr), static_cast<float*>(L.x.ptr),
+            sv.cg);
     }
     TG_CUDA(cudaGetLastError(), "prolong launch");
     for (int i = 0; i < sv.sweeps; ++i) {
-        TG_CUDA(jacobi<kOrder>(L.view, L.b.ptr, i % 2 == 0 ? L.x.ptr : L.t.ptr,
-                               i % 2 == 0 ? L.t.ptr : L.x.ptr, sv.omega, false, sv.s),
+        TG_CUDA(jacobi<kOrder>(sv, L.view, L.b.ptr, i % 2 == 0 ? L.x.ptr : L.t.ptr,
+                               i % 2 == 0 ? L.t.ptr : L.x.ptr, false),
                 "jacobi");
     }
     if (sv.sweeps % 2 == 1) {
-        TG_CUDA(cudaMemcpyAsync(L.x.ptr, L.t.ptr, size_t(L.view.n) * 4, cudaMemcpyDeviceToDevice,
-                                sv.s),
-                "copy");
+        TG_CUDA(copy_level(sv, L.t.ptr, L.x.ptr, L.view.n, false), "copy");
     }
     return TG_OK;
 }
@@ -1076,44 +1249,40 @@ int precondition(Solver& sv, const double* r, double* z) {
     Level& L0 = sv.wk->levels[0];
     const uint32_t n = L0.view.n;
     if (sv.levels == 1) {
-        TG_CUDA(cudaMemcpyAsync(L0.b.ptr, r, size_t(n) * 8, cudaMemcpyDeviceToDevice, sv.s),
-                "copy");
+        TG_CUDA(copy_level(sv, r, L0.b.ptr, n, true), "copy");
         if (int st = vcycle<kOrder>(sv, 0)) {
             return st;
         }
-        TG_CUDA(cudaMemcpyAsync(z, L0.x.ptr, size_t(n) * 8, cudaMemcpyDeviceToDevice, sv.s),
-                "copy");
+        TG_CUDA(copy_level(sv, L0.x.ptr, z, n, true), "copy");
         return TG_OK;
     }
     convert_kernel<double, float><<<blocks_for(n), 256, 0, sv.s>>>(
-        r, static_cast<float*>(L0.b.ptr), n);
+        r, static_cast<float*>(L0.b.ptr), n, sv.cg);
     if (int st = vcycle<kOrder>(sv, 0)) {
         return st;
     }
     convert_kernel<float, double><<<blocks_for(n), 256, 0, sv.s>>>(
-        static_cast<const float*>(L0.x.ptr), z, n);
+        static_cast<const float*>(L0.x.ptr), z, n, sv.cg);
     TG_CUDA(cudaGetLastError(), "convert launch");
     return TG_OK;
 }
 
-// a . b and c . d (c may be null), read back.
-int dots(Solver& sv, const double* a, const double* b, const double* c, const double* d,
-         uint32_t n, double out[2]) {
+// a . b and c . d (c may be null) into `out` on the device.
+cudaError_t dots(const Solver& sv, const double* a, const double* b, const double* c,
+                 const double* d, uint32_t n, double* out) {
     dot_kernel<<<kDotBlocks, 256, 0, sv.s>>>(a, b, c, d, n,
-                                             static_cast<double*>(sv.wk->partial.ptr));
-    dot_finish_kernel<<<1, 32, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
-                                          static_cast<double*>(sv.wk->dots.ptr));
-    TG_CUDA(cudaGetLastError(), "dot launch");
-    TG_CUDA(cudaMemcpyAsync(out, sv.wk->dots.ptr, 2 * sizeof(double), cudaMemcpyDeviceToHost,
-                            sv.s),
-            "copy to host");
-    TG_CUDA(cudaStreamSynchronize(sv.s), "synchronize");
-    return TG_OK;
+                                             static_cast<double*>(sv.wk->partial.ptr), sv.cg);
+    dot_finish_kernel<<<1, 32, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr), out,
+                                          sv.cg);
+    return cudaGetLastError();
 }
 
-// PreconditionedCg (seam_field.cpp:497) on the finest level: the correction at the unknowns.
+// Iterations launched between looks at whether the conjugate gradients stopped.
+constexpr int kIterationsPerGraph = 4;
+
+// One iteration of PreconditionedCg (seam_field.cpp:517-542), every scalar on the device.
 template <int kOrder>
-int solve(Solver& sv, double tolerance, int maxIterations, int* iterations) {
+int iteration(Solver& sv, CgState* cg) {
     Work& wk = *sv.wk;
     const LevelView& L0 = wk.levels[0].view;
     const uint32_t n = L0.n;
@@ -1122,47 +1291,96 @@ int solve(Solver& sv, double tolerance, int maxIterations, int* iterations) {
     double* p = static_cast<double*>(wk.cgP.ptr);
     double* ap = static_cast<double*>(wk.cgAp.ptr);
     double* z = static_cast<double*>(wk.cgZ.ptr);
-    TG_CUDA(cudaMemsetAsync(x, 0, size_t(n) * 8, sv.s), "memset");
-    double d[2];
-    if (int st = dots(sv, r, r, nullptr, nullptr, n, d)) {
+    apply_kernel<kOrder><<<blocks_for(n), 256, 0, sv.s>>>(L0, p, ap, cg);
+    TG_CUDA(dots(sv, p, ap, nullptr, nullptr, n, cg_dots(cg)), "dot launch");
+    cg_step_kernel<<<1, 1, 0, sv.s>>>(cg);
+    cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, cg);
+    if (int st = precondition<kOrder>(sv, r, z)) {
         return st;
     }
-    const double target = tolerance * std::sqrt(d[0]);
+    TG_CUDA(dots(sv, r, r, r, z, n, cg_dots(cg)), "dot launch");
+    cg_next_kernel<<<1, 1, 0, sv.s>>>(cg);
+    cg_direction_kernel<<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, cg);
+    TG_CUDA(cudaGetLastError(), "iteration launch");
+    return TG_OK;
+}
+
+// PreconditionedCg (seam_field.cpp:497) on the finest level: the correction at the unknowns in
+// cgX. The iterations run as a CUDA graph of kIterationsPerGraph of them, replayed until the
+// device state says they stopped.
+template <int kOrder>
+int solve(Solver& sv, double tolerance, int maxIterations, int* iterations) {
+    Work& wk = *sv.wk;
+    const uint32_t n = wk.levels[0].view.n;
+    double* x = static_cast<double*>(wk.cgX.ptr);
+    double* r = static_cast<double*>(wk.cgR.ptr);
+    double* p = static_cast<double*>(wk.cgP.ptr);
+    CgState* cg = static_cast<CgState*>(wk.cg.ptr);
+    TG_CUDA(cudaMemsetAsync(x, 0, size_t(n) * 8, sv.s), "memset");
+    double* scratch = static_cast<double*>(wk.dots.ptr);
+    sv.cg = nullptr;
+    TG_CUDA(dots(sv, r, r, nullptr, nullptr, n, scratch), "dot launch");
     if (int st = precondition<kOrder>(sv, r, p)) {
         return st;
     }
-    if (int st = dots(sv, r, p, nullptr, nullptr, n, d)) {
-        return st;
+    TG_CUDA(dots(sv, r, p, nullptr, nullptr, n, scratch + 2), "dot launch");
+    double d[4];
+    TG_CUDA(cudaMemcpyAsync(d, scratch, sizeof(d), cudaMemcpyDeviceToHost, sv.s), "copy");
+    TG_CUDA(cudaStreamSynchronize(sv.s), "synchronize");
+    CgState host{};
+    host.fit = d[2];
+    host.target = tolerance * std::sqrt(d[0]);
+    host.maxIterations = uint32_t(maxIterations);
+    host.done = host.fit > 0.0 ? 0u : 1u;
+    *iterations = 0;
+    if (host.done) {
+        return TG_OK;
     }
-    double fit = d[0];
-    int it = 0;
-    for (; it < maxIterations && fit > 0.0; ++it) {
-        apply_kernel<kOrder><<<blocks_for(n), 256, 0, sv.s>>>(L0, p, ap);
-        TG_CUDA(cudaGetLastError(), "apply launch");
-        if (int st = dots(sv, p, ap, nullptr, nullptr, n, d)) {
-            return st;
+    TG_CUDA(cudaMemcpyAsync(cg, &host, sizeof(host), cudaMemcpyHostToDevice, sv.s), "copy");
+    TG_CUDA(cudaStreamSynchronize(sv.s), "synchronize");
+    // Everything before is complete: the iterations run on the library's stream, which can be
+    // captured whatever stream the caller gave.
+    sv.cg = cg;
+    sv.s = sv.capture;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    TG_CUDA(cudaStreamBeginCapture(sv.s, cudaStreamCaptureModeThreadLocal), "capture");
+    int st = TG_OK;
+    for (int i = 0; i < kIterationsPerGraph && st == TG_OK; ++i) {
+        st = iteration<kOrder>(sv, cg);
+    }
+    const cudaError_t ended = cudaStreamEndCapture(sv.s, &graph);
+    if (st != TG_OK || ended != cudaSuccess) {
+        if (graph != nullptr) {
+            cudaGraphDestroy(graph);
         }
-        const double curvature = d[0];
-        if (!(curvature > 0.0)) {
+        return st != TG_OK ? st : fail(TG_ERROR_CUDA, "capture: %s", cudaGetErrorString(ended));
+    }
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        return fail(TG_ERROR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    uint32_t state[2] = {0, 0};  // done, iterations
+    for (int launched = 0; launched < maxIterations + kIterationsPerGraph;
+         launched += kIterationsPerGraph) {
+        e = cudaGraphLaunch(exec, sv.s);
+        if (e == cudaSuccess) {
+            e = cudaMemcpyAsync(state, reinterpret_cast<char*>(cg) + offsetof(CgState, done),
+                                sizeof(state), cudaMemcpyDeviceToHost, sv.s);
+        }
+        if (e == cudaSuccess) {
+            e = cudaStreamSynchronize(sv.s);
+        }
+        if (e != cudaSuccess || state[0] != 0u) {
             break;
         }
-        const double step = fit / curvature;
-        cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, step);
-        if (int st = precondition<kOrder>(sv, r, z)) {
-            return st;
-        }
-        if (int st = dots(sv, r, r, r, z, n, d)) {
-            return st;
-        }
-        if (std::sqrt(d[0]) <= target) {
-            ++it;
-            break;
-        }
-        const double ratio = d[1] / fit;
-        fit = d[1];
-        cg_direction_kernel<<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, ratio);
     }
-    *iterations = it;
+    cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) {
+        return fail(TG_ERROR_CUDA, "solve: %s", cudaGetErrorString(e));
+    }
+    *iterations = int(state[1]);
     return TG_OK;
 }
 
@@ -1203,35 +1421,40 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
                                ? static_cast<cudaStream_t>(stream)
                                : d->stream;
-    Work wk;
-    Buffer hostData, hostDiff, hostField;  // device copies in host mode
+    Work& wk = device_work(d);
     const uint8_t* dData = data;
     const float* dDiff = difference;
     float* dField = field;
     if (memory == TG_MEMORY_HOST) {
-        TG_CUDA(hostData.reserve(n), "allocation");
-        TG_CUDA(hostDiff.reserve(n * 4), "allocation");
-        TG_CUDA(hostField.reserve(n * 4), "allocation");
-        TG_CUDA(cudaMemcpyAsync(hostData.ptr, data, n, cudaMemcpyHostToDevice, s), "copy");
-        TG_CUDA(cudaMemcpyAsync(hostDiff.ptr, difference, n * 4, cudaMemcpyHostToDevice, s),
+        TG_CUDA(wk.hostIn.reserve(n), "allocation");
+        TG_CUDA(wk.hostIn2.reserve(n * 4), "allocation");
+        TG_CUDA(wk.hostOut.reserve(n * 4), "allocation");
+        TG_CUDA(cudaMemcpyAsync(wk.hostIn.ptr, data, n, cudaMemcpyHostToDevice, s), "copy");
+        TG_CUDA(cudaMemcpyAsync(wk.hostIn2.ptr, difference, n * 4, cudaMemcpyHostToDevice, s),
                 "copy");
-        dData = static_cast<const uint8_t*>(hostData.ptr);
-        dDiff = static_cast<const float*>(hostDiff.ptr);
-        dField = static_cast<float*>(hostField.ptr);
+        dData = static_cast<const uint8_t*>(wk.hostIn.ptr);
+        dDiff = static_cast<const float*>(wk.hostIn2.ptr);
+        dField = static_cast<float*>(wk.hostOut.ptr);
     }
+    // The call ends with its work done: the scratch it used is free for the next call, on
+    // whatever stream that comes.
     auto finish = [&](int st) {
-        if (st == TG_OK && memory == TG_MEMORY_HOST) {
-            if (cudaMemcpyAsync(field, dField, n * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                cudaStreamSynchronize(s) != cudaSuccess) {
-                st = fail(TG_ERROR_CUDA, "copy to host");
-            }
+        if (st == TG_OK && memory == TG_MEMORY_HOST &&
+            cudaMemcpyAsync(field, dField, n * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            st = fail(TG_ERROR_CUDA, "copy to host");
         }
-        hostData.release();
-        hostDiff.release();
-        hostField.release();
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (st == TG_OK && e != cudaSuccess) {
+            st = fail(TG_ERROR_CUDA, "synchronize: %s", cudaGetErrorString(e));
+        }
         return st;
     };
     TG_CUDA(cudaMemsetAsync(dField, 0, n * 4, s), "memset");
+    Events ev;
+    if (ev.create() != cudaSuccess) {
+        return finish(fail(TG_ERROR_CUDA, "event"));
+    }
+    TG_CUDA(cudaEventRecord(ev.e[0], s), "event");
     if (o.mode == 0u) {
         return finish(TG_OK);
     }
@@ -1405,17 +1628,54 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     }
     for (int l = 0; l < levels; ++l) {
         Level& L = wk.levels[l];
-        const size_t bytes = (l + 1 == levels ? 8 : 4) * std::max<size_t>(L.view.n, 1);
+        const size_t n1 = std::max<size_t>(L.view.n, 1);
+        const size_t bytes = (l + 1 == levels ? 8 : 4) * n1;
         TG_CUDA(L.x.reserve(bytes), "allocation");
         TG_CUDA(L.b.reserve(bytes), "allocation");
         TG_CUDA(L.t.reserve(bytes), "allocation");
+        // The operator's neighbors, and the links to the next coarser level both ways.
+        const int taps = order == 1 ? 4 : 12;
+        TG_CUDA(L.nbr.reserve(n1 * taps * 4), "allocation");
+        L.view.nbr = static_cast<const uint32_t*>(L.nbr.ptr);
+        if (L.view.n > 0) {
+            if (order == 1) {
+                neighbors_kernel<1><<<blocks_for(L.view.n), 256, 0, s>>>(
+                    L.view, static_cast<uint32_t*>(L.nbr.ptr));
+            } else {
+                neighbors_kernel<2><<<blocks_for(L.view.n), 256, 0, s>>>(
+                    L.view, static_cast<uint32_t*>(L.nbr.ptr));
+            }
+        }
+        L.view.parents = nullptr;
+        L.view.children = nullptr;
+        if (l + 1 < levels) {
+            Level& C = wk.levels[l + 1];
+            TG_CUDA(L.parents.reserve(n1 * 16), "allocation");
+            L.view.parents = static_cast<const uint32_t*>(L.parents.ptr);
+            if (L.view.n > 0) {
+                parents_kernel<<<blocks_for(L.view.n), 256, 0, s>>>(
+                    L.view, C.view, static_cast<uint32_t*>(L.parents.ptr));
+            }
+        }
+        if (l > 0) {
+            const Level& F = wk.levels[l - 1];
+            TG_CUDA(L.children.reserve(n1 * 64), "allocation");
+            L.view.children = static_cast<const uint32_t*>(L.children.ptr);
+            if (L.view.n > 0) {
+                children_kernel<<<blocks_for(L.view.n), 256, 0, s>>>(
+                    F.view, L.view, static_cast<uint32_t*>(L.children.ptr));
+            }
+        }
+        TG_CUDA(cudaGetLastError(), "level links launch");
     }
     const uint32_t nu = wk.levels[0].view.n;
     for (Buffer* b : {&wk.cgX, &wk.cgR, &wk.cgP, &wk.cgAp, &wk.cgZ}) {
         TG_CUDA(b->reserve(size_t(nu) * 8), "allocation");
     }
     TG_CUDA(wk.partial.reserve(2 * kDotBlocks * 8), "allocation");
-    TG_CUDA(wk.dots.reserve(16), "allocation");
+    TG_CUDA(wk.dots.reserve(32), "allocation");
+    TG_CUDA(wk.cg.reserve(sizeof(CgState)), "allocation");
+    TG_CUDA(cudaEventRecord(ev.e[1], s), "event");
     // The right-hand side from the fixed values, then the conjugate gradients.
     if (order == 1) {
         rhs_kernel<1><<<blocks_for(nu), 256, 0, s>>>(wk.levels[0].view, dField,
@@ -1426,7 +1686,7 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     }
     TG_CUDA(cudaGetLastError(), "rhs launch");
     Solver sv{&wk, levels, order, s, order == 1 ? 0.8 : 0.5, int(o.sweeps),
-              int(o.coarsest_sweeps)};
+              int(o.coarsest_sweeps), nullptr, d->stream};
     int iterations = 0;
     const double tolerance = o.tolerance > 0.0 ? o.tolerance : 1e-10;
     const int st = order == 1 ? solve<1>(sv, tolerance, 200, &iterations)
@@ -1437,9 +1697,16 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     scatter_solution_kernel<<<blocks_for(nu), 256, 0, s>>>(
         wk.levels[0].view.position, static_cast<const double*>(wk.cgX.ptr), nu, dField);
     TG_CUDA(cudaGetLastError(), "scatter launch");
+    TG_CUDA(cudaEventRecord(ev.e[2], s), "event");
+    TG_CUDA(cudaEventSynchronize(ev.e[2]), "synchronize");
+    float prepare = 0.0f, solved = 0.0f;
+    cudaEventElapsedTime(&prepare, ev.e[0], ev.e[1]);
+    cudaEventElapsedTime(&solved, ev.e[1], ev.e[2]);
     g_last.unknowns = nu;
     g_last.levels = uint32_t(levels);
     g_last.iterations = uint32_t(iterations);
+    g_last.prepare_ms = prepare;
+    g_last.solve_ms = solved;
     return finish(TG_OK);
 }
 
@@ -1489,17 +1756,15 @@ int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const
     const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
                                ? static_cast<cudaStream_t>(stream)
                                : d->stream;
-    Buffer bf, bl, bh;
     const float* df = field;
     const float* dl = later;
     float* dh = heights;
-    auto done = [&](int st) {
-        bf.release();
-        bl.release();
-        bh.release();
-        return st;
-    };
+    auto done = [](int st) { return st; };
     if (memory == TG_MEMORY_HOST) {
+        Work& wk = device_work(d);
+        Buffer& bf = wk.hostIn2;
+        Buffer& bl = wk.hostOut;
+        Buffer& bh = wk.hostOut2;
         if (bf.reserve(std::max<size_t>(posts, 1) * 4) != cudaSuccess ||
             bl.reserve(cells * 4) != cudaSuccess || bh.reserve(cells * 4) != cudaSuccess) {
             return done(fail(TG_ERROR_MEMORY, "device allocation"));
@@ -1514,27 +1779,9 @@ int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const
         dl = static_cast<const float*>(bl.ptr);
         dh = static_cast<float*>(bh.ptr);
     }
-    // Whether any post is set (SeamField::At is 0 everywhere otherwise).
-    std::vector<float> probe;
-    bool set = false;
-    {
-        Buffer count;
-        if (count.reserve(8) != cudaSuccess) {
-            return done(fail(TG_ERROR_MEMORY, "device allocation"));
-        }
-        cudaMemsetAsync(count.ptr, 0, 8, s);
-        // Posts holding a nonzero value, counted as "data" of their bits.
-        count_data_kernel<<<1184, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(df), posts * 4,
-                                               static_cast<unsigned long long*>(count.ptr));
-        unsigned long long nonzero = 0;
-        cudaMemcpyAsync(&nonzero, count.ptr, 8, cudaMemcpyDeviceToHost, s);
-        const cudaError_t e = cudaStreamSynchronize(s);
-        count.release();
-        if (e != cudaSuccess) {
-            return done(fail(TG_ERROR_CUDA, "synchronize: %s", cudaGetErrorString(e)));
-        }
-        set = nonzero > 0;
-    }
+    // SeamField::At is 0 everywhere when no post was set; reading an all-zero field gives the
+    // same 0, so the field is always read.
+    const bool set = true;
     SeamRead sr{df, lg.width, lg.height, lg.originX, lg.pixelWidth, lg.rowRotation,
                 lg.originY, lg.colRotation, lg.pixelHeight, set};
     const NoData nd{nodata.mode, nodata.value};
@@ -1580,19 +1827,17 @@ int tg_seam_samples(tg_device* d, const float* earlier, const float* later, cons
     const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
                                ? static_cast<cudaStream_t>(stream)
                                : d->stream;
-    Buffer be, bl, bd, bf;
-    auto done = [&](int st) {
-        be.release();
-        bl.release();
-        bd.release();
-        bf.release();
-        return st;
-    };
+    auto done = [](int st) { return st; };
     const float* de = earlier;
     const float* dl = later;
     uint8_t* dd = data;
     float* df = difference;
     if (memory == TG_MEMORY_HOST) {
+        Work& wk = device_work(d);
+        Buffer& be = wk.hostIn2;
+        Buffer& bl = wk.hostOut;
+        Buffer& bd = wk.hostIn;
+        Buffer& bf = wk.hostOut2;
         if (be.reserve(std::max<size_t>(cells, 1) * 4) != cudaSuccess ||
             bl.reserve(std::max<size_t>(cells, 1) * 4) != cudaSuccess ||
             bd.reserve(posts) != cudaSuccess || bf.reserve(posts * 4) != cudaSuccess) {

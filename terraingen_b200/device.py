@@ -246,7 +246,7 @@ class Device:
 
     def seam_solve(self, data, difference, dx: float, dy: float, mode: str, width: float = 50.0,
                    decay_length: float = 50.0, field=None, levels: int = 4, sweeps: int = 2,
-                   coarsest_sweeps: int = 100, tolerance: float = 0.0):
+                   coarsest_sweeps: int = 20, tolerance: float = 0.0):
         """BuildSeamField (src/sources/seam_field.cpp:663) on the device from the lattice's
         samples: `data` (uint8, 1 where the earlier source has data) and `difference` (float32,
         earlier minus later, NaN elsewhere), both (height, width). Returns the field's posts
@@ -275,7 +275,8 @@ class Device:
         st = N.SeamStats()
         N.check(self._lib.tg_seam_stats_get(C.byref(st)))
         return field, {"unknowns": st.unknowns, "levels": st.levels,
-                       "iterations": st.iterations}
+                       "iterations": st.iterations, "prepare_ms": st.prepare_ms,
+                       "solve_ms": st.solve_ms}
 
     def seam_fill(self, field, lattice: GridSpec, later, grid: GridSpec, heights,
                   nodata=(1, 0.0)):

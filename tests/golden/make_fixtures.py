@@ -20,7 +20,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle import harness as H  # noqa: E402
-from terraingen_b200 import centered, layouts as L  # noqa: E402
+from terraingen_b200 import GridSpec, centered, layouts as L  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -251,6 +251,37 @@ def seam_fixtures() -> None:
     np.savez_compressed(OUT / "seams.npz", **arrays)
 
 
+def chain_fixture() -> None:
+    """Four raster patches (2 x 2 windows of a grid with a 16-cell overlap, each its own fBm and a
+    datum offset) chained by the reference's SourceChain with each seam mode."""
+    ref = H.reference()
+    rs = H.restate()
+    grid = centered(300, 260, 1.0, 2000.0, -500.0)
+    arrays = {"grid": np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])}
+    windows = []
+    for r0, r1 in ((0, 138), (122, 260)):
+        for c0, c1 in ((0, 158), (142, 300)):
+            windows.append((c0, r0, c1 - c0, r1 - r0))
+    patches, grids = [], []
+    for k, (c0, r0, w, h) in enumerate(windows):
+        g = GridSpec(w, h, grid.x0 + c0 * grid.pixel, grid.y0 - r0 * grid.pixel, grid.pixel)
+        p = np.zeros((h, w), np.float32)
+        rs.rs_fbm_grid_f32(w, h, g.x0, g.y0, g.pixel, 40 + k, 200.0, 12.0, 5, 2.0, 0.5,
+                           0.6 * k, p.ctypes.data)
+        patches.append(p)
+        grids.append(g)
+        arrays[f"patch{k}"] = p
+    arrays["windows"] = np.array(windows)
+    for name, mode, width, decay in (("feather", 1, 10.0, 50.0), ("height", 2, 50.0, 4.0),
+                                     ("slope", 3, 50.0, 4.0)):
+        out = H.patch_chain(ref, patches, grids, mode, width, decay, grid)
+        assert not np.isnan(out).any(), name
+        arrays[f"{name}_options"] = np.array([mode, width, decay])
+        arrays[f"{name}_heights"] = out
+        print("chain", name, float(out.min()), float(out.max()))
+    np.savez_compressed(OUT / "chain.npz", **arrays)
+
+
 def population_fixture() -> None:
     """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
     ref = H.reference()
@@ -268,5 +299,6 @@ if __name__ == "__main__":
     ds_fixtures()
     population_fixture()
     seam_fixtures()
+    chain_fixture()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)

@@ -103,3 +103,23 @@ def test_distances_carry_the_nearest_difference():
     diag = np.float32(math.hypot(1.0, 2.0))
     assert d[4, 5] == 0.0 and d[4, 8] == 3.0 and d[2, 5] == 4.0 and d[3, 6] == diag
     assert (carried == 2.5).all()
+
+
+def test_chain_restatement_is_the_reference_chain():
+    # Four patches on 2 x 2 windows chained by the reference's SourceChain (nested seams, each
+    # link's lattice over the patch before it).
+    from terraingen_b200 import GridSpec
+
+    z = dict(np.load(GOLDEN / "chain.npz"))
+    g = grid_of(z["grid"])
+    assert isinstance(g, GridSpec)
+    wins = [tuple(int(x) for x in w) for w in z["windows"]]
+    patches = [z[f"patch{k}"] for k in range(4)]
+    for name in ("feather", "height", "slope"):
+        _, width, decay = z[f"{name}_options"]
+        got = S.chain(patches, wins, g, name, float(width), float(decay))
+        want = z[f"{name}_heights"]
+        if name == "feather":
+            assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        else:
+            assert np.abs(got.astype(np.float64) - want).max() <= 1e-6, name

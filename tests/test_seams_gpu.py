@@ -199,3 +199,27 @@ def test_wide_reach(device, mode):
     else:
         want = S.solve(data, diff, 0.5, 0.5, mode, 40.0)
         assert np.abs(field.astype(np.float64) - want).max() <= 1e-4
+
+
+@pytest.mark.parametrize("mode", ["feather", "height", "slope"])
+def test_patch_chain_is_the_reference_chain(device, mode):
+    # PatchChain (samples, solve and fill per link, on the device) against the reference's
+    # SourceChain of the same four patches.
+    import torch
+
+    from terraingen_b200.chain import PatchChain, Seams, Window
+
+    z = dict(np.load(GOLDEN / "chain.npz"))
+    g = grid_of(z["grid"])
+    wins = [Window(*(int(x) for x in w)) for w in z["windows"]]
+    _, width, decay = z[f"{mode}_options"]
+    chain = PatchChain(device, g, wins, Seams(mode, width=float(width),
+                                              decay_length=float(decay)))
+    patches = [torch.from_numpy(z[f"patch{k}"]).cuda() for k in range(4)]
+    got = chain.compose(patches).cpu().numpy()
+    want = z[f"{mode}_heights"]
+    assert len(chain.solves) == 3
+    if mode == "feather":
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    else:
+        assert np.abs(got.astype(np.float64) - want).max() <= 1e-4
