@@ -66,6 +66,8 @@ def parse():
                    help="length of the real-time request stream of the served form (0 skips it)")
     p.add_argument("--dem-steps", type=int, default=5,
                    help="timed steps of the DEM refinement form (0 skips it)")
+    p.add_argument("--dem-only", action="store_true",
+                   help="run the DEM refinement form alone and print its line (profiling)")
     return p.parse_args()
 
 
@@ -543,6 +545,11 @@ def main():
         form = batched_form(dev, args, rank, world, dev.measure_alu())
         if rank == 0:
             print(json.dumps({"form": "batched", **form}), flush=True)
+        return
+    if args.dem_only:
+        form = dem_form(dev, args, rank, world)
+        if rank == 0:
+            print(json.dumps({"form": "dem_refinement", **form}), flush=True)
         return
     # Each rank's own tile, side by side along x (independent tiles, no exchange).
     w = terrain4097(SIDE, PIXEL, cx=rank * SIDE * PIXEL)

@@ -54,14 +54,6 @@ __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int leve
     return sqrt(-2.0 * log1p(-u1)) * cos(2.0 * kPi * u2);
 }
 
-__device__ __forceinline__ int64_t floor_half(int64_t v) {  // diamond_square.cpp:41
-    return v >= 0 ? v / 2 : -((1 - v) / 2);
-}
-
-__device__ __forceinline__ bool odd(int64_t v) {
-    return (v & 1) != 0;
-}
-
 __device__ __forceinline__ double at(const DsLevel& l, int64_t col, int64_t row) {
     return l.nodes[size_t(row - l.r0) * l.w + size_t(col - l.c0)];
 }
@@ -84,57 +76,58 @@ __global__ void ds_base_kernel(const float* __restrict__ posts, uint32_t pw, uin
     out.nodes[size_t(j) * out.w + i] = double(posts[size_t(pr) * pw + size_t(pc)]);
 }
 
-// The square step of `level` over `out`'s box: kept parents and displaced odd/odd nodes
-// (SquareStep, diamond_square.cpp:392-407). Mixed nodes are left for the diamond step.
+// Nodes are handled in 2 x 2 blocks anchored at even (col, row): every thread of a step draws
+// the same number of normals (one in the square step, two in the diamond step), so no lane of
+// a warp idles while the others run Philox and Box-Muller.
+
+// The square step of `level` over `out`'s box: kept parents (even/even) and displaced odd/odd
+// nodes (SquareStep, diamond_square.cpp:392-407), block (bc0 + i, br0 + j) per thread. Mixed
+// nodes are left for the diamond step.
 template <bool kSpline>
-__global__ void ds_square_kernel(const DsLevel parents, DsLevel out, int level, double step,
+__global__ void ds_square_kernel(const DsLevel parents, DsLevel out, int64_t bc0, int64_t br0,
+                                 uint32_t bw, uint32_t bh, int level, double step,
                                  uint32_t seed) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= out.w || j >= out.h) {
+    if (i >= bw || j >= bh) {
         return;
     }
-    const int64_t col = out.c0 + i, row = out.r0 + j;
-    double value;
-    if (!odd(col) && !odd(row)) {
-        value = at(parents, col / 2, row / 2);
-    } else if (odd(col) && odd(row)) {
-        const int64_t left = floor_half(col), bottom = floor_half(row);
-        double mean;
-        if (!kSpline) {
-            mean = 0.25 * (at(parents, left, bottom) + at(parents, left + 1, bottom) +
-                           at(parents, left, bottom + 1) + at(parents, left + 1, bottom + 1));
-        } else {
-            mean = 0.0;
-            for (int64_t b = 0; b < 4; ++b) {
-                double line = 0.0;
-                for (int64_t a = 0; a < 4; ++a) {
-                    line += kMid[a] * at(parents, left - 1 + a, bottom - 1 + b);
-                }
-                mean += kMid[b] * line;
-            }
-        }
-        value = mean + step * node_normal(col, row, level, seed);
+    const int64_t bc = bc0 + i, br = br0 + j;
+    const int64_t c1 = out.c0 + int64_t(out.w), r1 = out.r0 + int64_t(out.h);
+    // The kept parent at (2 bc, 2 br).
+    const int64_t ec = 2 * bc, er = 2 * br;
+    if (ec >= out.c0 && ec < c1 && er >= out.r0 && er < r1) {
+        out.nodes[size_t(er - out.r0) * out.w + size_t(ec - out.c0)] = at(parents, bc, br);
+    }
+    // The displaced node at (2 bc + 1, 2 br + 1): the mean of the four parents around it.
+    const int64_t col = ec + 1, row = er + 1;
+    if (col < out.c0 || col >= c1 || row < out.r0 || row >= r1) {
+        return;
+    }
+    const int64_t left = bc, bottom = br;
+    double mean;
+    if (!kSpline) {
+        mean = 0.25 * (at(parents, left, bottom) + at(parents, left + 1, bottom) +
+                       at(parents, left, bottom + 1) + at(parents, left + 1, bottom + 1));
     } else {
-        return;
+        mean = 0.0;
+        for (int64_t b = 0; b < 4; ++b) {
+            double line = 0.0;
+            for (int64_t a = 0; a < 4; ++a) {
+                line += kMid[a] * at(parents, left - 1 + a, bottom - 1 + b);
+            }
+            mean += kMid[b] * line;
+        }
     }
-    out.nodes[size_t(j) * out.w + i] = value;
+    out.nodes[size_t(row - out.r0) * out.w + size_t(col - out.c0)] =
+        mean + step * node_normal(col, row, level, seed);
 }
 
-// The diamond step of `level`: mixed nodes of `box` (inner box of `nodes`), from the square
-// step's nodes around them (DiamondStep, diamond_square.cpp:410-424).
+// A mixed node (col, row) of the diamond step: the mean of the four square-step nodes around it
+// plus its displacement.
 template <bool kSpline>
-__global__ void ds_diamond_kernel(DsLevel nodes, int64_t c0, int64_t r0, uint32_t w, uint32_t h,
-                                  int level, double step, uint32_t seed) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= w || j >= h) {
-        return;
-    }
-    const int64_t col = c0 + i, row = r0 + j;
-    if (odd(col) == odd(row)) {
-        return;
-    }
+__device__ __forceinline__ void diamond_node(DsLevel& nodes, int64_t col, int64_t row, int level,
+                                             double step, uint32_t seed) {
     double mean;
     if (!kSpline) {
         mean = 0.25 * (at(nodes, col - 1, row) + at(nodes, col + 1, row) + at(nodes, col, row - 1) +
@@ -149,6 +142,28 @@ __global__ void ds_diamond_kernel(DsLevel nodes, int64_t c0, int64_t r0, uint32_
     }
     nodes.nodes[size_t(row - nodes.r0) * nodes.w + size_t(col - nodes.c0)] =
         mean + step * node_normal(col, row, level, seed);
+}
+
+// The diamond step of `level`: the mixed nodes (2 bc + 1, 2 br) and (2 bc, 2 br + 1) of block
+// (bc0 + i, br0 + j) that lie in `box` (inner box of `nodes`), from the square step's nodes
+// around them (DiamondStep, diamond_square.cpp:410-424).
+template <bool kSpline>
+__global__ void ds_diamond_kernel(DsLevel nodes, int64_t c0, int64_t r0, uint32_t w, uint32_t h,
+                                  int64_t bc0, int64_t br0, uint32_t bw, uint32_t bh, int level,
+                                  double step, uint32_t seed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= bw || j >= bh) {
+        return;
+    }
+    const int64_t bc = bc0 + i, br = br0 + j;
+    const int64_t c1 = c0 + int64_t(w), r1 = r0 + int64_t(h);
+    const int64_t cols[2] = {2 * bc + 1, 2 * bc}, rows[2] = {2 * br, 2 * br + 1};
+    for (int n = 0; n < 2; ++n) {
+        if (cols[n] >= c0 && cols[n] < c1 && rows[n] >= r0 && rows[n] < r1) {
+            diamond_node<kSpline>(nodes, cols[n], rows[n], level, step, seed);
+        }
+    }
 }
 
 // `value` as an integer when within 1e-6 of one (NearestWhole, src/sources/lattice.h:33), else
@@ -226,21 +241,34 @@ cudaError_t launch_ds_base(const float* posts, uint32_t pw, uint32_t ph, const D
     return cudaGetLastError();
 }
 
+// The 2 x 2 blocks anchored at even coordinates that hold the nodes [lo, lo + n).
+void block_range(int64_t lo, uint32_t n, int64_t& b0, uint32_t& count) {
+    const auto half = [](int64_t v) { return v >= 0 ? v / 2 : -((1 - v) / 2); };
+    b0 = half(lo);
+    count = n == 0 ? 0u : uint32_t(half(lo + int64_t(n) - 1) - b0 + 1);
+}
+
 cudaError_t launch_ds_level(const DsLevel& parents, const DsLevel& out, int64_t c0, int64_t r0,
                             uint32_t w, uint32_t h, int level, double squareStep,
                             double diamondStep, uint32_t seed, bool spline,
                             cudaStream_t stream) {
     const dim3 block(32, 8);
+    int64_t sc0, sr0, dc0, dr0;
+    uint32_t sw, sh, dw, dh;
+    block_range(out.c0, out.w, sc0, sw);
+    block_range(out.r0, out.h, sr0, sh);
+    block_range(c0, w, dc0, dw);
+    block_range(r0, h, dr0, dh);
     if (spline) {
-        ds_square_kernel<true><<<blocks_for(out.w, out.h, block), block, 0, stream>>>(
-            parents, out, level, squareStep, seed);
-        ds_diamond_kernel<true><<<blocks_for(w, h, block), block, 0, stream>>>(
-            out, c0, r0, w, h, level, diamondStep, seed);
+        ds_square_kernel<true><<<blocks_for(sw, sh, block), block, 0, stream>>>(
+            parents, out, sc0, sr0, sw, sh, level, squareStep, seed);
+        ds_diamond_kernel<true><<<blocks_for(dw, dh, block), block, 0, stream>>>(
+            out, c0, r0, w, h, dc0, dr0, dw, dh, level, diamondStep, seed);
     } else {
-        ds_square_kernel<false><<<blocks_for(out.w, out.h, block), block, 0, stream>>>(
-            parents, out, level, squareStep, seed);
-        ds_diamond_kernel<false><<<blocks_for(w, h, block), block, 0, stream>>>(
-            out, c0, r0, w, h, level, diamondStep, seed);
+        ds_square_kernel<false><<<blocks_for(sw, sh, block), block, 0, stream>>>(
+            parents, out, sc0, sr0, sw, sh, level, squareStep, seed);
+        ds_diamond_kernel<false><<<blocks_for(dw, dh, block), block, 0, stream>>>(
+            out, c0, r0, w, h, dc0, dr0, dw, dh, level, diamondStep, seed);
     }
     return cudaGetLastError();
 }
