@@ -658,7 +658,8 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded): fBm source, reference-exact crater batch, stand-in boulders",
+        "data": "synthetic (seeded): fBm source, the reference's crater batch and boulders "
+                "(restated on the host, bit-exact)",
         "config": {"workload": "terrain4097: 4097x4097 at 0.5 m, 8-octave fBm + 200k craters + "
                                "1M boulders (resolved ones drawn)",
                    "cells_per_gpu": w.cells, "craters_on_tile": int(len(w.crater_records)),

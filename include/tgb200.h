@@ -354,6 +354,37 @@ int tg_crater_generate(const tg_crater_population* population, const double* reg
                        double* x, double* y, double* diameter, double* age, uint64_t* id,
                        size_t capacity, size_t* count);
 
+/* A boulder layer's sizes and pose (BoulderLayerOptions, include/terraingen/layers/boulders/
+ * boulder_options.h): power-law sizes N(>D) = c D^-exponent per m^2 on [min_diameter,
+ * max_diameter] (BoulderSizes with a PowerLawSfd), height ratio and buried share uniform between
+ * their bounds (BoulderPose), the resolution fade in samples (ResolutionFade, 2 and 4), and the
+ * candidate cells' size factor (16). */
+typedef struct tg_boulder_population {
+    uint32_t seed;
+    double sfd_coefficient;
+    double sfd_exponent;
+    double min_diameter;
+    double max_diameter;
+    double min_height_ratio;
+    double max_height_ratio;
+    double min_burial;
+    double max_burial;
+    double fade_start_samples;
+    double fade_end_samples;
+    double cell_size_factor;
+} tg_boulder_population;
+
+/* The boulders a BoulderLayer with these sizes and pose, and otherwise its defaults (no patches,
+ * clusters, density or slope maps, crater ejecta, bedrock, fragmentation, settling or facets, on
+ * a plane), draws into a grid of `spacing` over `region` (x0, y0, x1, y1 in meters; the reference
+ * bakes over the grid's bounds grown by half a sample): PlaceBoulders (src/layers/boulders/
+ * boulder_layer.cpp:263-405) restated, bit-exact, in the reference's order, as the 40-byte
+ * tg_boulder tg_boulders_bake takes (x, y, diameter, exposed height, resolution weight), those
+ * of positive weight only. `count` receives the number; `out` (may be null) holds at most
+ * `capacity`. Host only. */
+int tg_boulder_generate(const tg_boulder_population* population, const double* region,
+                        double spacing, tg_boulder* out, size_t capacity, size_t* count);
+
 /* What CraterLayer::ApplySamples hands the crater kernel for `grid`
  * (src/layers/craters/crater_layer.cpp:337-359, shaping/apply.cpp:339-370): the 188-byte
  * CraterShapeKernel, the 144-byte CraterRecords of the craters on the grid in apply order, their

@@ -92,6 +92,18 @@ def boulders(lib: C.CDLL, scene: Scene) -> np.ndarray:
     return out
 
 
+def boulders_posed(lib: C.CDLL, scene: Scene, pose) -> np.ndarray:
+    """tgref_boulders_posed: the layer's boulders with height ratio and burial drawn between
+    bounds (min ratio, max ratio, min burial, max burial)."""
+    pose = np.array(pose, np.float64)
+    n = lib.tgref_boulders_posed(C.byref(scene), pose.ctypes.data, None, 0)
+    if n < 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    out = np.zeros((n, 5), np.float64)
+    lib.tgref_boulders_posed(C.byref(scene), pose.ctypes.data, out.ctypes.data, n)
+    return out
+
+
 def below_boulders(lib: C.CDLL, scene: Scene, threads: int = 0) -> np.ndarray:
     out = np.zeros((scene.height, scene.width), np.float32)
     if lib.tgref_evaluate_below_boulders(C.byref(scene), threads, out.ctypes.data) != 0:
@@ -245,6 +257,9 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_craters.restype = C.c_long
     lib.tgref_boulders.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_long]
     lib.tgref_boulders.restype = C.c_long
+    if hasattr(lib, "tgref_boulders_posed"):
+        lib.tgref_boulders_posed.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_void_p, C.c_long]
+        lib.tgref_boulders_posed.restype = C.c_long
     lib.tgref_evaluate_below_boulders.argtypes = [C.POINTER(Scene), C.c_uint, C.c_void_p]
     lib.tgref_evaluate_below_boulders.restype = C.c_int
     lib.tgref_ds.argtypes = [C.c_void_p, _U32, _U32, C.c_void_p, _D, _D, C.c_int, _U32, _U32, _U32,

@@ -283,6 +283,48 @@ long tgref_boulders(const tgref_scene* s, double* out, long n) {
     }
 }
 
+/// tgref_boulders with the pose drawn between bounds: height ratio in [pose[0], pose[1]] and
+/// buried share in [pose[2], pose[3]] (BoulderPose).
+long tgref_boulders_posed(const tgref_scene* s, const double* pose, double* out, long n) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        BoulderLayerOptions options = MakeBoulderLayer(*s)->Options();
+        options.pose.minHeightRatio = pose[0];
+        options.pose.maxHeightRatio = pose[1];
+        options.pose.minBurial = pose[2];
+        options.pose.maxBurial = pose[3];
+        const auto layer = std::make_shared<BoulderLayer>(options);
+        const GeoTransform transform = GeoTransform::FromGdal(
+            {s->transform[0], s->transform[1], s->transform[2], s->transform[3], s->transform[4],
+             s->transform[5]});
+        const RasterGrid grid{s->width, s->height, transform};
+        const double spacing = std::fabs(s->transform[1]);
+        const BoulderList list = layer->Boulders(grid.Bounds().Expanded(0.5 * spacing), spacing,
+                                                 nullptr);
+        long count = 0;
+        for (std::size_t i = 0; i < list.Size(); ++i) {
+            const Boulder b = list.At(i);
+            const double weight = ResolutionWeight(b.diameter, spacing, options.fade);
+            if (!options.rendering.reliefRange.Holds(b.diameter, b.model) || weight <= 0.0) {
+                continue;
+            }
+            if (count < n && out != nullptr) {
+                double* o = out + 5 * count;
+                o[0] = b.x;
+                o[1] = b.y;
+                o[2] = b.diameter;
+                o[3] = b.ExposedHeight();
+                o[4] = weight;
+            }
+            ++count;
+        }
+        return count;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
 /// The reference's DiamondSquareUpsampler over `posts` (pw x ph floats on `postTransform`), read at
 /// the cells of an `ow` x `oh` grid on `outTransform`, through a RasterSource in a Terrain: the
 /// heights into `out`, the evaluation's wall time into `ms`.

@@ -74,6 +74,15 @@ class Shaping(C.Structure):
     _fields_ = [("profile", C.c_uint32), ("irregular", C.c_uint32)]
 
 
+class BoulderPopulation(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("sfd_coefficient", C.c_double),
+                ("sfd_exponent", C.c_double), ("min_diameter", C.c_double),
+                ("max_diameter", C.c_double), ("min_height_ratio", C.c_double),
+                ("max_height_ratio", C.c_double), ("min_burial", C.c_double),
+                ("max_burial", C.c_double), ("fade_start_samples", C.c_double),
+                ("fade_end_samples", C.c_double), ("cell_size_factor", C.c_double)]
+
+
 class DsOptions(C.Structure):
     _fields_ = [("fractal_dimension", _D), ("scale", _D), ("interp", _U32), ("seed", _U32),
                 ("min_pixel_size", _D)]
@@ -97,6 +106,7 @@ SIGNATURES.update({
     "tg_boulders_bake_static": [_P, _U32, _D, C.POINTER(Grid), _P, NoData, _P, C.c_char_p, _SZ],
     "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,
                              C.POINTER(_SZ)],
+    "tg_boulder_generate": [C.POINTER(BoulderPopulation), _P, _D, _P, _SZ, C.POINTER(_SZ)],
     "tg_crater_batch": [C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid), _P, _P, _SZ,
                         _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ)],
 })

@@ -56,6 +56,8 @@ constexpr uint32_t kCraterPeakStream = 0x5045414Bu;
 constexpr uint32_t kCraterIrregularityStream = 0x49525247u;
 constexpr uint32_t kCraterTextureStream = 0x54455854u;
 constexpr uint32_t kCraterNoiseStream = 0x434E4F53u;
+constexpr uint32_t kBoulderCandidateStream = 0x524F434Bu;  // streams.h:31
+constexpr uint32_t kBoulderAttributeStream = 0x41545452u;  // streams.h:32
 
 class Stream {
   public:
@@ -168,15 +170,85 @@ std::vector<Band> crater_bands(double minD, double maxD, double factor) {
     return bands;
 }
 
+// N(>=D) = c D^-e (PowerLawSfd, include/terraingen/distribution/power_law.h:20-33). With
+// `weight` > 0 it is instead the one-term SummedSfd `weight` x that law (summed.cpp:33-47), which
+// a boulder layer draws its candidates from: the sum has no closed-form inverse, so a diameter is
+// found as SizeFrequencyDistribution::InvertCumulative does (size_frequency.cpp:34-113), by
+// Illinois steps on log N over log D, then bisection if they stall.
 struct PowerLaw {
     double c, e;
-    double cumulative(double d) const { return c * std::pow(d, -e); }
+    double weight = 0.0;
+
+    double law(double d) const { return c * std::pow(d, -e); }
+    double cumulative(double d) const { return weight > 0.0 ? 0.0 + weight * law(d) : law(d); }
+    double incremental(double d) const {
+        const double one = c * e * std::pow(d, -e - 1.0);
+        return weight > 0.0 ? 0.0 + weight * one : one;
+    }
     double expected(double lo, double hi) const { return 1.0 * (cumulative(lo) - cumulative(hi)); }
     double sample(Stream& random, double lo, double hi) const {
         const double count = expected(lo, hi);
         const double top = cumulative(lo);
         const double target = top - random.next_double() * count;
-        return std::clamp(std::pow(target / c, -1.0 / e), lo, hi);
+        const double d = weight > 0.0 ? invert(target, lo, hi) : std::pow(target / c, -1.0 / e);
+        return std::clamp(d, lo, hi);
+    }
+
+    // The diameter in [lo, hi] where N = target.
+    double invert(double target, double lo, double hi) const {
+        double low = std::log(lo), high = std::log(hi);
+        if (target > 0.0) {
+            const double logTarget = std::log(target);
+            const auto excess = [&](double u) {
+                return std::log(cumulative(std::exp(u))) - logTarget;
+            };
+            // Illinois regula falsi on the bracket [a, b] (util/numerics.h:33-61).
+            double a = low, b = high, fa = excess(low), fb = excess(high);
+            int side = 0;
+            if (!(fa > 0.0)) {
+                return std::exp(low);
+            }
+            if (!(fb < 0.0)) {
+                return std::exp(high);
+            }
+            double u = low;
+            bool stalled = true;
+            for (int i = 0; i < 100; ++i) {
+                const double previous = u;
+                const double secant = b - fb * (b - a) / (fb - fa);
+                u = secant > a && secant < b ? secant : 0.5 * (a + b);
+                const double g = excess(u);
+                if (std::isnan(g)) {
+                    break;
+                }
+                if (g == 0.0 || std::fabs(u - previous) <= 1e-14 * std::fmax(1.0, std::fabs(u))) {
+                    stalled = false;
+                    break;
+                }
+                if ((g < 0.0) == (fa < 0.0)) {
+                    a = u;
+                    fa = g;
+                    fb *= side == -1 ? 0.5 : 1.0;
+                    side = -1;
+                } else {
+                    b = u;
+                    fb = g;
+                    fa *= side == 1 ? 0.5 : 1.0;
+                    side = 1;
+                }
+            }
+            if (!stalled) {
+                return std::exp(u);
+            }
+            low = a;
+            high = b;
+        }
+        const double tolerance = 1e-15 * std::fmax(1.0, std::fabs(high));
+        for (int i = 0; i < 200 && high - low > tolerance; ++i) {
+            const double middle = 0.5 * (low + high);
+            (!(cumulative(std::exp(middle)) > target) ? high : low) = middle;
+        }
+        return std::exp(0.5 * (low + high));
     }
 };
 
@@ -211,8 +283,8 @@ std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const P
 
 // Craters over `region` with their candidate margin (GenerateCraters, planar, no spacing,
 // density map or manual craters).
-std::vector<Crater> generate(const tg_crater_population& spec, const Box& region) {
-    const PowerLaw law{spec.sfd_coefficient, spec.sfd_exponent};
+std::vector<Crater> generate(const tg_crater_population& spec, const Box& region,
+                             const PowerLaw& law) {
     const double marginRadii = spec.margin_radii;
     auto margin = [&](double d) { return 0.5 * marginRadii * d; };
     std::vector<Crater> out;
@@ -265,16 +337,17 @@ double smoothstep(double t) {
     return t * t * (3.0 - 2.0 * t);
 }
 
-double resolution_weight(double diameter, double spacing) {
-    // 1 - Falloff(D / spacing, 2, 4, Smoothstep) (src/layers/fade.cpp:18-52)
+double resolution_weight(double diameter, double spacing, double start = 2.0,
+                         double end = 4.0) {
+    // 1 - Falloff(D / spacing, start, end, Smoothstep) (src/layers/fade.cpp:18-52)
     const double x = diameter / spacing;
     double f;
-    if (x <= 2.0) {
+    if (x <= start) {
         f = 1.0;
-    } else if (x >= 4.0) {
+    } else if (x >= end) {
         f = 0.0;
     } else {
-        f = 1.0 - smoothstep((x - 2.0) / 2.0);
+        f = 1.0 - smoothstep((x - start) / (end - start));
     }
     return 1.0 - f;
 }
@@ -353,7 +426,8 @@ int tg_crater_generate(const tg_crater_population* spec, const double* region, d
         return TG_ERROR_ARGUMENT;
     }
     const std::vector<Crater> craters =
-        generate(*spec, Box{region[0], region[1], region[2], region[3]});
+        generate(*spec, Box{region[0], region[1], region[2], region[3]},
+                 PowerLaw{spec->sfd_coefficient, spec->sfd_exponent});
     *count = craters.size();
     for (size_t n = 0; n < craters.size() && n < capacity; ++n) {
         if (x) x[n] = craters[n].x;
@@ -362,6 +436,73 @@ int tg_crater_generate(const tg_crater_population* spec, const double* region, d
         if (age) age[n] = craters[n].age;
         if (id) id[n] = craters[n].id;
     }
+    return TG_OK;
+}
+
+int tg_boulder_generate(const tg_boulder_population* spec, const double* region, double spacing,
+                        tg_boulder* out, size_t capacity, size_t* count) {
+    if (spec == nullptr || region == nullptr || count == nullptr) {
+        return TG_ERROR_ARGUMENT;
+    }
+    const tg_boulder_population& b = *spec;
+    if (!(b.min_diameter > 0.0) || !(b.max_diameter > b.min_diameter) ||
+        !std::isfinite(b.max_diameter) || !(b.sfd_coefficient > 0.0) ||
+        !(b.sfd_exponent > 0.0) || !(b.cell_size_factor > 0.0) || !(spacing > 0.0) ||
+        !(b.fade_start_samples >= 0.0) || !(b.fade_end_samples > b.fade_start_samples) ||
+        !(region[2] >= region[0]) || !(region[3] >= region[1])) {
+        return TG_ERROR_ARGUMENT;
+    }
+    // ScatterBoulderCandidates (boulder_layer.cpp:263-295): craters of the candidate sizes
+    // (BoulderCandidates: the sizes weighted by the richest background abundance, 1 without
+    // patches, clusters, maps or bedrock) in the candidate substream, reaching the region by a
+    // dome's own margin of 1 radius, bands below the fade's start skipped (BoulderRecords,
+    // boulder_layer.cpp:370-374).
+    tg_crater_population p{};
+    p.seed = substream_seed(b.seed, kBoulderCandidateStream);
+    p.min_diameter = b.min_diameter;
+    p.max_diameter = b.max_diameter;
+    p.lifetime_gyr = 1.0;
+    p.cell_size_factor = b.cell_size_factor;
+    p.margin_radii = 1.0;
+    p.min_resolved_diameter = b.fade_start_samples * spacing;
+    const PowerLaw sizes{b.sfd_coefficient, b.sfd_exponent};
+    const PowerLaw candidates{b.sfd_coefficient, b.sfd_exponent, 1.0};
+    const std::vector<Crater> drawn =
+        generate(p, Box{region[0], region[1], region[2], region[3]}, candidates);
+    size_t n = 0;
+    for (const Crater& c : drawn) {
+        const uint32_t low = uint32_t(c.id), high = uint32_t(c.id >> 32);
+        // Thin (boulder_layer.cpp:345-358): kept when a draw falls below the background density
+        // over the candidates' (1 here: the background abundance is 1 everywhere).
+        Stream keep(b.seed, kBoulderAttributeStream, low, high, 0u /* Keep */);
+        const double density = 1.0 * sizes.incremental(c.diameter);
+        if (keep.next_double() >= density / candidates.incremental(c.diameter)) {
+            continue;
+        }
+        // DrawPose and Wear (boulder_pose.cpp:28-77): height ratio, then wear (its own stream),
+        // then the buried share, each uniform between its bounds.
+        Stream pose(b.seed, kBoulderAttributeStream, low, high, 1u /* Pose */);
+        const double ratio =
+            b.min_height_ratio + (b.max_height_ratio - b.min_height_ratio) * pose.next_double();
+        Stream wear(b.seed, kBoulderAttributeStream, low, high, 2u /* Wear */);
+        wear.next_double();
+        wear.next_double();
+        const double share = pose.next_double();
+        const double burial = b.min_burial + (b.max_burial - b.min_burial) * share;
+        const double height = ratio * c.diameter;
+        // Drawn into the heights when its resolution weight is positive (boulder_relief.cpp:
+        // 298-302, the default relief range holding every boulder that is not a model).
+        const double weight = resolution_weight(c.diameter, spacing, b.fade_start_samples,
+                                                b.fade_end_samples);
+        if (!(weight > 0.0)) {
+            continue;
+        }
+        if (out != nullptr && n < capacity) {
+            out[n] = tg_boulder{c.x, c.y, c.diameter, height * (1.0 - burial), weight};
+        }
+        ++n;
+    }
+    *count = n;
     return TG_OK;
 }
 
@@ -386,7 +527,7 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     const double reachRadii = shaping->profile == 1 ? 2.0 : 1.5;  // MPD reaches 2 R, FT 1.5 R
     p.margin_radii = reachRadii * max_outline_scale(irregular);
     p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
-    std::vector<Crater> craters = generate(p, bounds);
+    std::vector<Crater> craters = generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent});
 
     // CraterApplyOrder, oldest first (apply_options.cpp:96).
     std::vector<size_t> order(craters.size());

@@ -1,6 +1,6 @@
 """The evaluation workloads of the benchmark configurations, built with the product's own host
-code (no reference library): crater batches through tg_crater_batch (the reference's population
-and records, bit for bit) and boulder lists as a seeded stand-in with the configured size law.
+code (no reference library): crater batches through tg_crater_batch and boulders through
+tg_boulder_generate (the reference's populations, records and boulders, bit for bit).
 
 Synthetic terrain, 4097 x 4097 at 0.5 m ("terrain4097"): an 8-octave Perlin fBm source
 (wavelength 512 m, lacunarity 2, gain 0.5, amplitude 5 m, seed 7); 200,000 craters expected over
@@ -73,37 +73,38 @@ def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
     return kernel, records, data, footprints
 
 
+def boulder_population(seed: int, coefficient: float, exponent: float = 2.5, dmin: float = 0.2,
+                       dmax: float = 3.0, height_ratio=(0.5, 0.5),
+                       burial=(0.0, 0.0)) -> N.BoulderPopulation:
+    return N.BoulderPopulation(seed=seed, sfd_coefficient=coefficient, sfd_exponent=exponent,
+                               min_diameter=dmin, max_diameter=dmax,
+                               min_height_ratio=height_ratio[0], max_height_ratio=height_ratio[1],
+                               min_burial=burial[0], max_burial=burial[1], fade_start_samples=2.0,
+                               fade_end_samples=4.0, cell_size_factor=16.0)
+
+
+def generate_boulders(population: N.BoulderPopulation, grid: GridSpec) -> np.ndarray:
+    """[n, 5] boulders (x, y, diameter, exposed height, weight) the boulder layer draws into
+    `grid` (tg_boulder_generate over the grid's bounds grown by half a sample)."""
+    lib = N.library()
+    half = 0.5 * grid.pixel
+    region = np.array([grid.x0 - half, grid.y0 - grid.height * grid.pixel - half,
+                       grid.x0 + grid.width * grid.pixel + half, grid.y0 + half], np.float64)
+    n = C.c_size_t()
+    N.check(lib.tg_boulder_generate(C.byref(population), region.ctypes.data, grid.pixel, None, 0,
+                                    C.byref(n)))
+    out = np.zeros((n.value, 5), np.float64)
+    N.check(lib.tg_boulder_generate(C.byref(population), region.ctypes.data, grid.pixel,
+                                    out.ctypes.data, n.value, C.byref(n)))
+    return out
+
+
 def resolution_weight(diameter: np.ndarray, spacing: float) -> np.ndarray:
     """1 - Falloff(D / spacing, 2, 4, smoothstep) (src/layers/fade.cpp:50)."""
     x = diameter / spacing
     t = np.clip((x - 2.0) / 2.0, 0.0, 1.0)
     falloff = np.where(x <= 2.0, 1.0, np.where(x >= 4.0, 0.0, 1.0 - t * t * (3.0 - 2.0 * t)))
     return 1.0 - falloff
-
-
-def stand_in_boulders(grid: GridSpec, expected: float, exponent: float, dmin: float, dmax: float,
-                      height_ratio: float, seed: int) -> np.ndarray:
-    """[n, 5] boulders (x, y, diameter, exposed height, weight): a Poisson count of boulders with
-    N(>D) ~ D^-exponent, uniform centers over the grid and half the largest boulder around it,
-    keeping those resolved at the grid's spacing."""
-    rng = np.random.default_rng(seed)
-    spacing = grid.pixel
-    area = grid.width * grid.height * spacing * spacing
-    c = expected / (area * (dmin ** -exponent - dmax ** -exponent))
-    lo = max(dmin, 2.0 * spacing)
-    if lo >= dmax:
-        return np.zeros((0, 5), np.float64)  # none resolved at this spacing
-    margin = 0.5 * dmax
-    w, h = grid.width * spacing + 2 * margin, grid.height * spacing + 2 * margin
-    n = rng.poisson(c * w * h * (lo ** -exponent - dmax ** -exponent))
-    u = rng.random(n)
-    top = lo ** -exponent
-    diameter = (top - u * (top - dmax ** -exponent)) ** (-1.0 / exponent)
-    x = grid.x0 - margin + rng.random(n) * w
-    y = grid.y0 + margin - rng.random(n) * h
-    out = np.stack([x, y, diameter, height_ratio * diameter, resolution_weight(diameter, spacing)],
-                   axis=1)
-    return np.ascontiguousarray(out[out[:, 4] > 0.0])
 
 
 def terrain4097(side: int = 4097, pixel: float = 0.5, cx: float = 0.0, cy: float = 0.0,
@@ -114,8 +115,8 @@ def terrain4097(side: int = 4097, pixel: float = 0.5, cx: float = 0.0, cy: float
     crater_c = 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
     kernel, records, data, footprints = crater_batch(
         crater_population(seed, crater_c, 1.0, 500.0), grid)
-    boulders = stand_in_boulders(grid, 1e6 * grid.cells / (4097 * 4097), 2.5, 0.2, 3.0, 0.5,
-                                 seed + 1000 + int(cx) * 7 + int(cy) * 13)
+    boulder_c = 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5))
+    boulders = generate_boulders(boulder_population(seed, boulder_c), grid)
     return Workload("terrain4097", grid,
                     np.array([fractal(seed=seed, wavelength=512.0, amplitude=5.0, octaves=8)]),
                     0.0, kernel, records, data, footprints, boulders, pixel)
@@ -142,7 +143,8 @@ def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: fl
     log-uniform on `side` cells, spacings log-uniform on `spacing` m, centers uniform over a disk
     of `radius` m around the origin (the polar frame of a 1737.4 km sphere), the 4097^2 terrain's
     source, and its craters and boulders at `density` times their density. Each tile carries the
-    craters tg_crater_batch builds for its grid and its own seeded boulders."""
+    craters tg_crater_batch builds for its grid and the boulders tg_boulder_generate draws into
+    it."""
     from .batch import TILE, TileSet, layout
 
     rng = np.random.default_rng(seed)
@@ -155,6 +157,7 @@ def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: fl
     full_area = (4097 * 0.5) ** 2
     crater_c = density * 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
     population = crater_population(7, crater_c, 1.0, 500.0)
+    stones_of = boulder_population(7, density * 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5)))
     grids = [centered(int(s), int(s), float(p), float(x), float(y))
              for s, p, x, y in zip(sides, pixels, cxs, cys)]
     offsets, pitch = layout(grids)
@@ -166,8 +169,7 @@ def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: fl
         k, rec, dat, foot = crater_batch(population, g)
         kernel = k if kernel is None else kernel
         if boulders:
-            b = stand_in_boulders(g, density * 1e6 * g.cells * g.pixel ** 2 / full_area, 2.5, 0.2,
-                                  3.0, 0.5, seed * 100003 + i)
+            b = generate_boulders(stones_of, g)
         else:
             b = np.zeros((0, 5), np.float64)
         t = tiles[i]

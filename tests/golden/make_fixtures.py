@@ -143,6 +143,14 @@ def boulder_fixtures() -> None:
         arrays[f"{name}_base"] = H.below_boulders(ref, scene, 1)
         arrays[f"{name}_expected"], _ = H.evaluate(ref, scene, 0, 1)
         print(name, len(arrays[f"{name}_boulders"]), "boulders")
+    # Heights and burial drawn between bounds (the pose streams), without ground.
+    grid = centered(180, 150, 0.5, -40.0, 75.0)
+    scene = H.make_scene(grid, boulders=dict(boulderSeed=9, boulderCoefficient=0.4))
+    pose = (0.3, 0.7, 0.1, 0.4)
+    arrays["posed_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])
+    arrays["posed_pose"] = np.array(pose)
+    arrays["posed_boulders"] = H.boulders_posed(ref, scene, pose)
+    print("posed", len(arrays["posed_boulders"]), "boulders")
     np.savez_compressed(OUT / "boulders.npz", **arrays)
 
 

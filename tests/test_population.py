@@ -123,3 +123,48 @@ def test_population_matches_reference_live(seed, coefficient, lo, hi):
     got = generate(population(fields, margin_radii=2.0, min_resolved=0.0), region)
     for key in ("x", "y", "diameter", "age", "id"):
         assert np.array_equal(got[key], want[key]), key
+
+
+# --- boulders (tg_boulder_generate) -------------------------------------------------------------
+
+BOULDER_SCENES = {
+    # (seed, coefficient, height ratio bounds, burial bounds), as tests/golden/make_fixtures.py
+    # builds the reference's layers: exponent 2.5 on [0.2, 3] m.
+    "dense": (1, 0.5, (0.5, 0.5), (0.0, 0.0)),
+    "fine": (4, 0.3, (0.4, 0.4), (0.0, 0.0)),
+    "posed": (9, 0.4, (0.3, 0.7), (0.1, 0.4)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(BOULDER_SCENES))
+def test_boulders_are_the_references(name):
+    # The boulders the reference's BoulderLayer draws into the fixture grid (candidates from the
+    # summed candidate SFD inverted numerically, thinning, pose and burial draws, resolution
+    # weights): bit for bit, in its order.
+    from terraingen_b200 import GridSpec
+    from terraingen_b200.workloads import boulder_population, generate_boulders
+
+    z = np.load(GOLDEN / "boulders.npz")
+    g = z[f"{name}_grid"]
+    grid = GridSpec(int(g[0]), int(g[1]), float(g[2]), float(g[3]), float(g[4]))
+    seed, coefficient, ratio, burial = BOULDER_SCENES[name]
+    got = generate_boulders(boulder_population(seed, coefficient, height_ratio=ratio,
+                                               burial=burial), grid)
+    want = z[f"{name}_boulders"]
+    assert len(want) > 1000
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+def test_boulder_generate_refuses_bad_input():
+    from terraingen_b200.workloads import boulder_population
+
+    lib = N.library()
+    region = np.array([0.0, 0.0, 10.0, 10.0])
+    n = C.c_size_t()
+    pop = boulder_population(1, 0.5, dmin=3.0, dmax=0.2)
+    assert lib.tg_boulder_generate(C.byref(pop), region.ctypes.data, 0.5, None, 0,
+                                   C.byref(n)) == 1  # TG_ERROR_ARGUMENT
+    pop = boulder_population(1, 0.5)
+    assert lib.tg_boulder_generate(C.byref(pop), region.ctypes.data, 0.0, None, 0,
+                                   C.byref(n)) == 1  # TG_ERROR_ARGUMENT
