@@ -135,6 +135,15 @@ __global__ void crater_harmonics_kernel(const CraterRecord* __restrict__ records
     }
 }
 
+// Shaping a bin. Each warp owns 4 rows x 32 columns of the bin (each thread 4 adjacent cells of
+// one row). For every staged crater the warp first finds which of its 128 cells need it (inside
+// a reference tile the crater's window touches, and within its cull radius), then queues those
+// (crater, cell) pairs in shared memory and evaluates them 32 at a time, one pair per lane, so a
+// small crater that needs a handful of cells no longer leaves most lanes of the warp idle. The
+// contributions are FP32 values added into FP64 accumulators in shared memory: that sum is exact
+// for these magnitudes, so the atomic adds give the same bits in any order.
+constexpr int kQueue = 160;  // 31 pairs left over plus one crater's 128
+
 template <bool kFast>
 __global__ void __launch_bounds__(kShapeThreads)
     crater_shape_kernel(const CraterShapeKernel k, const float* __restrict__ data,
@@ -144,6 +153,10 @@ __global__ void __launch_bounds__(kShapeThreads)
     const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
     __shared__ __align__(128) BinEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
+    __shared__ double accs[kShapeThreads / 32][128];
+    __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
+    __shared__ float2 columns[kShapeThreads / 32][32];  // split x of the warp's 32 columns
+    __shared__ float2 rows[kShapeThreads / 32][4];      // split y of its 4 rows
 
     const uint32_t bin = blockIdx.x;
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
@@ -155,11 +168,13 @@ __global__ void __launch_bounds__(kShapeThreads)
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t row = binY * kBinCells + warp * 4u + lane / 8u;
     const uint32_t col0 = binX * kBinCells + (lane % 8u) * kCellsPerThread;
+    double* acc = accs[warp];
+    uint16_t* queue = queues[warp];
+    const uint32_t cell0 = (lane / 8u) * 32u + (lane % 8u) * kCellsPerThread;
 
     // This thread's cells: split positions (MakeSplitPoint, crater_kernel.cpp:303) of the
     // column centers at row 0 and the row center at column 0, as the reference's strips carry.
     float pxh[kCellsPerThread], pxl[kCellsPerThread];
-    double acc[kCellsPerThread];
     bool live[kCellsPerThread];
     const double yd = grid.originY + 0.5 * grid.colRotation + (double(row) + 0.5) * grid.pixelHeight;
     const float pyh = float(yd);
@@ -173,15 +188,48 @@ __global__ void __launch_bounds__(kShapeThreads)
         pxh[j] = float(xd);
         pxl[j] = float(xd - double(pxh[j]));
         live[j] = rowIn && col < grid.width;
-        acc[j] = 0.0;
+        double h = 0.0;
         if (live[j]) {
-            const float h = heights[size_t(row) * grid.width + col];
-            live[j] = !is_nodata(nodata, h);
-            acc[j] = double(h);
+            const float v = heights[size_t(row) * grid.width + col];
+            live[j] = !is_nodata(nodata, v);
+            h = double(v);
         }
+        acc[cell0 + j] = h;
+        if (lane < 8u) {
+            columns[warp][(lane % 8u) * kCellsPerThread + j] = make_float2(pxh[j], pxl[j]);
+        }
+    }
+    if (lane % 8u == 0u) {
+        rows[warp][lane / 8u] = make_float2(pyh, pyl);
     }
     const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
     const bool anyLive = live[0] || live[1] || live[2] || live[3];
+
+    // Evaluates the 32 (or, at a flush, `n`) queued pairs from `from`, one per lane.
+    auto drain = [&](const BinEntry* chunk, uint32_t from, uint32_t n) {
+        if (lane < n) {
+            const uint32_t code = queue[from + lane];
+            const BinEntry& entry = chunk[code >> 7];
+            const CraterRecord& r = entry.record;
+            const uint32_t cell = code & 127u;
+            const float2 cx = columns[warp][cell & 31u];
+            const float2 cy = rows[warp][cell >> 5];
+            const float dy = crater::split_difference(cy.x, cy.y, r.y, r.yLow);
+            const float dx = crater::split_difference(cx.x, cx.y, r.x, r.xLow);
+            if (kFast) {
+                bool reached;
+                const float shaped = crater::fast_contribution(fk, harmonics, r, dx, dy, reached);
+                if (reached) {
+                    atomicAdd(acc + cell, double(shaped));
+                }
+            } else {
+                const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
+                if (q.reached) {
+                    atomicAdd(acc + cell, double(q.shaped));
+                }
+            }
+        }
+    };
 
     const uint32_t chunks = (count + kChunk - 1) / kChunk;
     if (tid == 0) {
@@ -206,7 +254,7 @@ __global__ void __launch_bounds__(kShapeThreads)
     }
     uint32_t phase[2] = {0u, 0u};
     bool failed = false;
-    uint32_t evaluated = 0;  // (cell, crater) pairs this thread evaluates, for the pair counter
+    uint32_t evaluated = 0;  // (cell, crater) pairs this warp queued, for the pair counter
     for (uint32_t c = 0; c < chunks; ++c) {
         const uint32_t s = c & 1u;
         if (!mbar_wait(&bars[s], phase[s])) {
@@ -225,6 +273,7 @@ __global__ void __launch_bounds__(kShapeThreads)
             return;
         }
         const uint32_t n = min(kChunk, count - c * kChunk);
+        uint32_t queued = 0;  // warp-uniform
         for (uint32_t e = 0; e < n; ++e) {
             const BinEntry& entry = stage[s][e];
             const CraterRecord& r = entry.record;
@@ -233,39 +282,47 @@ __global__ void __launch_bounds__(kShapeThreads)
                                 tileY <= int(entry.tileY1);
             const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
             const float cull2 = entry.cull * entry.cull;
-            bool need[kCellsPerThread];
-            float dxs[kCellsPerThread];
-            bool any = false;
+            uint32_t need = 0;
 #pragma unroll
             for (int j = 0; j < kCellsPerThread; ++j) {
-                dxs[j] = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
-                need[j] = inTile && live[j] && dxs[j] * dxs[j] + dy * dy < cull2;
-                any |= need[j];
-            }
-            if (!__any_sync(0xffffffffu, any)) {
-                continue;
-            }
-#pragma unroll
-            for (int j = 0; j < kCellsPerThread; ++j) {
-                if (need[j]) {
-                    ++evaluated;
-                    const float dx = dxs[j];
-                    if (kFast) {
-                        bool reached;
-                        const float shaped =
-                            crater::fast_contribution(fk, harmonics, r, dx, dy, reached);
-                        if (reached) {
-                            acc[j] += double(shaped);
-                        }
-                    } else {
-                        const crater::Contribution q =
-                            crater::crater_contribution(k, data, r, dx, dy);
-                        if (q.reached) {
-                            acc[j] += double(q.shaped);
-                        }
-                    }
+                const float dx = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
+                if (inTile && live[j] && dx * dx + dy * dy < cull2) {
+                    need |= 1u << j;
                 }
             }
+            const uint32_t mine = __popc(need);
+            // Exclusive prefix of the lanes' counts.
+            uint32_t before = mine;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, before, d);
+                if (lane >= uint32_t(d)) {
+                    before += v;
+                }
+            }
+            const uint32_t total = __shfl_sync(0xffffffffu, before, 31);
+            if (total == 0u) {
+                continue;
+            }
+            before -= mine;
+            uint32_t slot = queued + before;
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                if (need & (1u << j)) {
+                    queue[slot++] = uint16_t((e << 7) | (cell0 + j));
+                }
+            }
+            evaluated += mine;
+            queued += total;
+            __syncwarp();
+            while (queued >= 32u) {
+                queued -= 32u;
+                drain(stage[s], queued, 32u);
+                __syncwarp();
+            }
+        }
+        if (queued > 0u) {
+            drain(stage[s], 0u, queued);
+            __syncwarp();
         }
         if (c + 2 < chunks) {
             // The buffer is read by every warp before it is refilled.
@@ -280,13 +337,14 @@ __global__ void __launch_bounds__(kShapeThreads)
     if (lane == 0 && warpPairs > 0) {
         atomicAdd(reinterpret_cast<unsigned long long*>(flags + 1), (unsigned long long)warpPairs);
     }
+    __syncwarp();
     if (!rowIn) {
         return;
     }
     float out[kCellsPerThread];
 #pragma unroll
     for (int j = 0; j < kCellsPerThread; ++j) {
-        out[j] = float(acc[j]);
+        out[j] = float(acc[cell0 + j]);
     }
     float* dst = heights + size_t(row) * grid.width + col0;
     const bool vec = (grid.width % 4u == 0u) && col0 + 3 < grid.width &&
