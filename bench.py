@@ -44,7 +44,7 @@ CRATER_OPS_PER_PAIR = 200
 # and hypot 12, dome band average (2 sqrt, 2 asin, clamps) 60, max-composite 4; FP64.
 BOULDER_OPS_PER_PAIR = 82
 # DRAM bytes per launch from the ncu capture of this workload (profiles/terrain4097_kernels.md).
-TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 136.5e6 + 27.0e6, "boulders": 61.9e6 + 7.9e6}
+TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 136.2e6 + 26.4e6, "boulders": 61.9e6 + 7.9e6}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -66,6 +66,10 @@ def parse():
                    help="length of the real-time request stream of the served form (0 skips it)")
     p.add_argument("--dem-steps", type=int, default=5,
                    help="timed steps of the DEM refinement form (0 skips it)")
+    p.add_argument("--dem-side", type=int, default=20481,
+                   help="output side of the DEM refinement form (20481; smaller for profiling)")
+    p.add_argument("--served-only", action="store_true",
+                   help="run the served form alone and print its line (profiling)")
     p.add_argument("--dem-only", action="store_true",
                    help="run the DEM refinement form alone and print its line (profiling)")
     return p.parse_args()
@@ -358,7 +362,7 @@ def dem_form(dev, args, rank, world):
     from terraingen_b200.chain import PatchChain, Seams
     from terraingen_b200.workloads import dem20481
 
-    w = dem20481(seed=7 + 10 * rank)
+    w = dem20481(args.dem_side, (args.dem_side - 1) // 10 + 1, seed=7 + 10 * rank)
     pg = w.post_grid
     posts = torch.empty((pg.height, pg.width), dtype=torch.float32, device="cuda")
     dev.noise_source(w.fractals, pg, posts, 0.0)
@@ -421,7 +425,8 @@ def dem_form(dev, args, rank, world):
     solves = chain.solves
     per_link = link_ms.reshape(-1, len(w.windows) - 1, 3).mean(axis=0)
     return {
-        "workload": "dem20481: 2049^2 DEM at 5 m (12-octave fBm, 20 km, +-2000 m) refined 10x by "
+        "workload": f"dem{w.grid.width}: {w.post_grid.width}^2 DEM at 5 m (12-octave fBm, 20 km, "
+                    "+-2000 m) refined 10x by "
                     "diamond-square (F 2.2, scale 1.5 m, 4 levels, bilinear) to 20481^2 at 0.5 m "
                     "as 2x2 patches (own seeds, 64-cell overlap) chained with Height seams "
                     "(3 L = 64 cells, 4-level V-cycle, Jacobi smoother, FP64 PCG to 1e-10), then "
@@ -545,6 +550,11 @@ def main():
         form = batched_form(dev, args, rank, world, dev.measure_alu())
         if rank == 0:
             print(json.dumps({"form": "batched", **form}), flush=True)
+        return
+    if args.served_only:
+        form = served_form(dev, args, rank, world)
+        if rank == 0:
+            print(json.dumps({"form": "served", **form}), flush=True)
         return
     if args.dem_only:
         form = dem_form(dev, args, rank, world)

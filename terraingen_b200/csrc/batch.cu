@@ -516,6 +516,12 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
     __shared__ __align__(128) unsigned char stage[2][kStageBytes];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t sItem, sTile;
+    // Dynamic: per warp, FP64 accumulators of its cells and the queue of (crater, cell) pairs.
+    constexpr uint32_t kWarpCells = 32u * kCells;
+    constexpr uint32_t kQueueCap = 31u + kWarpCells;
+    extern __shared__ double craterAcc[];
+    uint16_t* const craterQueue =
+        reinterpret_cast<uint16_t*>(craterAcc + (kBinW * kBinH / kCells / 32) * kWarpCells);
 
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
@@ -667,25 +673,41 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
         const uint32_t cEnd = min(v.craterCounts[item + 1], v.craterCapacity);
         const uint32_t cCount = cEnd > cFirst ? cEnd - cFirst : 0u;
         if (cCount > 0u) {
-            // Split positions of the cell centers (MakeSplitPoint, crater_kernel.cpp:303).
+            // Split positions of the cell centers (MakeSplitPoint, crater_kernel.cpp:303): grid
+            // rows take the row center at column 0 (the reference's strips carry one y per row),
+            // points their own y. `split_of` gives any cell of this warp's, so a lane can shape
+            // another lane's cell.
+            const uint32_t warpBase = tid & ~31u;
+            auto split_of = [&](uint32_t owner, int j, float& xh, float& xl, float& yh,
+                                float& yl) {
+                double x, y;
+                if (points) {
+                    const uint32_t f = local * kBinCellCount + (warpBase + owner) * kCells;
+                    const uint32_t i = f + j < grid.width ? f + j : 0u;
+                    x = v.points[2 * (size_t(t.pointBase) + i)];
+                    y = v.points[2 * (size_t(t.pointBase) + i) + 1];
+                } else {
+                    const uint32_t o = warpBase + owner;
+                    const uint32_t binX = local % t.binsX, binY = local / t.binsX;
+                    const uint32_t r = binY * kBinH + o / kRowThreads;
+                    const uint32_t c = binX * kBinW + (o % kRowThreads) * kCells + j;
+                    y = grid.originY + 0.5 * grid.colRotation + (double(r) + 0.5) * grid.pixelHeight;
+                    x = grid.originX + (double(c) + 0.5) * grid.pixelWidth +
+                        0.5 * grid.rowRotation;
+                }
+                xh = float(x);
+                xl = float(x - double(xh));
+                yh = float(y);
+                yl = float(y - double(yh));
+            };
             float pxh[kCells], pxl[kCells], pyh[kCells], pyl[kCells];
-            double acc[kCells];
+            double* acc = craterAcc + (tid >> 5) * kWarpCells;
+            uint16_t* queue = craterQueue + (tid >> 5) * kQueueCap;
             bool anyLive = false;
 #pragma unroll
             for (int j = 0; j < kCells; ++j) {
-                // Grid rows take the row center at column 0 (the reference's strips carry one
-                // y per row); points their own y.
-                const double y = points ? yd[j]
-                                        : grid.originY + 0.5 * grid.colRotation +
-                                              (double(row) + 0.5) * grid.pixelHeight;
-                const double x = points ? xd[j]
-                                        : grid.originX + (double(col0 + j) + 0.5) * grid.pixelWidth +
-                                              0.5 * grid.rowRotation;
-                pxh[j] = float(x);
-                pxl[j] = float(x - double(pxh[j]));
-                pyh[j] = float(y);
-                pyl[j] = float(y - double(pyh[j]));
-                acc[j] = double(h[j]);
+                split_of(lane, j, pxh[j], pxl[j], pyh[j], pyl[j]);
+                acc[lane * kCells + j] = double(h[j]);
                 anyLive |= live[j];
             }
             const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
@@ -716,6 +738,35 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                 }
                 const BinEntry* entries = reinterpret_cast<const BinEntry*>(&stage[s][0]);
                 const uint32_t n = min(kCraterChunk, cCount - c * kCraterChunk);
+                // Shapes the queued pairs [from, from + count), one per lane: each entry's data
+                // at its ref's base (the BinEntry's index field).
+                auto drain = [&](uint32_t from, uint32_t count) {
+                    if (lane < count) {
+                        const uint32_t code = queue[from + lane];
+                        const BinEntry& entry = entries[code >> 8];
+                        const CraterRecord& r = entry.record;
+                        const uint32_t cell = code & 255u;
+                        float xh, xl, yh, yl;
+                        split_of(cell / kCells, int(cell % kCells), xh, xl, yh, yl);
+                        const float dx = crater::split_difference(xh, xl, r.x, r.xLow);
+                        const float dy = crater::split_difference(yh, yl, r.y, r.yLow);
+                        if (kFast) {
+                            bool reached;
+                            const float shaped = crater::fast_contribution(
+                                fk, v.harmonics + entry.index, r, dx, dy, reached);
+                            if (reached) {
+                                atomicAdd(acc + cell, double(shaped));
+                            }
+                        } else {
+                            const crater::Contribution q =
+                                crater::crater_contribution(k, v.data + entry.index, r, dx, dy);
+                            if (q.reached) {
+                                atomicAdd(acc + cell, double(q.shaped));
+                            }
+                        }
+                    }
+                };
+                uint32_t queued = 0;  // warp-uniform
                 for (uint32_t e = 0; e < n; ++e) {
                     const BinEntry& entry = entries[e];
                     const CraterRecord& r = entry.record;
@@ -726,43 +777,47 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                                                     tileY >= int(entry.tileY0) &&
                                                     tileY <= int(entry.tileY1)));
                     const float cull2 = entry.cull * entry.cull;
-                    bool need[kCells];
-                    float dxs[kCells], dys[kCells];
-                    bool any = false;
+                    uint32_t need = 0;
 #pragma unroll
                     for (int j = 0; j < kCells; ++j) {
-                        dxs[j] = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
-                        dys[j] = crater::split_difference(pyh[j], pyl[j], r.y, r.yLow);
-                        need[j] = inTile && live[j] &&
-                                  __fadd_rn(__fmul_rn(dxs[j], dxs[j]), __fmul_rn(dys[j], dys[j])) <
-                                      cull2;
-                        any |= need[j];
-                    }
-                    if (!__any_sync(0xffffffffu, any)) {
-                        continue;
-                    }
-                    const float* data = v.data + entry.index;
-                    const float* harmonics = v.harmonics + entry.index;
-#pragma unroll
-                    for (int j = 0; j < kCells; ++j) {
-                        if (need[j]) {
-                            ++craterPairs;
-                            if (kFast) {
-                                bool reached;
-                                const float shaped = crater::fast_contribution(
-                                    fk, harmonics, r, dxs[j], dys[j], reached);
-                                if (reached) {
-                                    acc[j] += double(shaped);
-                                }
-                            } else {
-                                const crater::Contribution q =
-                                    crater::crater_contribution(k, data, r, dxs[j], dys[j]);
-                                if (q.reached) {
-                                    acc[j] += double(q.shaped);
-                                }
-                            }
+                        const float dx = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
+                        const float dy = crater::split_difference(pyh[j], pyl[j], r.y, r.yLow);
+                        if (inTile && live[j] &&
+                            __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) < cull2) {
+                            need |= 1u << j;
                         }
                     }
+                    const uint32_t mine = __popc(need);
+                    uint32_t before = mine;
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const uint32_t other = __shfl_up_sync(0xffffffffu, before, d);
+                        if (lane >= uint32_t(d)) {
+                            before += other;
+                        }
+                    }
+                    const uint32_t total = __shfl_sync(0xffffffffu, before, 31);
+                    if (total == 0u) {
+                        continue;
+                    }
+                    uint32_t slot = queued + before - mine;
+                    for (int j = 0; j < kCells; ++j) {
+                        if (need & (1u << j)) {
+                            queue[slot++] = uint16_t((e << 8) | (lane * kCells + j));
+                        }
+                    }
+                    craterPairs += mine;
+                    queued += total;
+                    __syncwarp();
+                    while (queued >= 32u) {
+                        queued -= 32u;
+                        drain(queued, 32u);
+                        __syncwarp();
+                    }
+                }
+                if (queued > 0u) {
+                    drain(0u, queued);
+                    __syncwarp();
                 }
                 if (c + 2 < chunks) {
                     __syncthreads();  // every warp has read the buffer before it is refilled
@@ -774,7 +829,7 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
             }
 #pragma unroll
             for (int j = 0; j < kCells; ++j) {
-                h[j] = float(acc[j]);
+                h[j] = float(acc[lane * kCells + j]);
             }
         }
 
@@ -914,20 +969,42 @@ constexpr BatchVariant kVariants[] = {
 };
 constexpr int kVariantCount = int(sizeof(kVariants) / sizeof(kVariants[0]));
 
+// The dynamic shared memory of a variant: per warp, 8 bytes per cell and its pair queue.
+template <int kBinW, int kBinH, int kCells>
+constexpr size_t dynamic_bytes() {
+    constexpr size_t warps = size_t(kBinW) * kBinH / kCells / 32;
+    return warps * 32 * kCells * sizeof(double) + warps * (31 + 32 * kCells) * sizeof(uint16_t);
+}
+
+// Lets the variant take its dynamic shared memory (set once, before any capture: occupancy()
+// runs when a batch is planned).
+template <int kBinW, int kBinH, int kCells, bool kFast>
+cudaError_t allow_shared() {
+    static const cudaError_t done = cudaFuncSetAttribute(
+        batch_evaluate_kernel<kBinW, kBinH, kCells, kFast>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, int(dynamic_bytes<kBinW, kBinH, kCells>()));
+    return done;
+}
+
 template <int kBinW, int kBinH, int kCells, bool kFast>
 cudaError_t launch_variant(const CraterShapeKernel& k, const BatchNoise& noise,
                            const BatchView& v, uint32_t ctas, cudaStream_t stream) {
+    if (cudaError_t err = allow_shared<kBinW, kBinH, kCells, kFast>()) {
+        return err;
+    }
     batch_evaluate_kernel<kBinW, kBinH, kCells, kFast>
-        <<<ctas, kBinW * kBinH / kCells, 0, stream>>>(k, noise, v);
+        <<<ctas, kBinW * kBinH / kCells, dynamic_bytes<kBinW, kBinH, kCells>(), stream>>>(
+            k, noise, v);
     return cudaGetLastError();
 }
 
 template <int kBinW, int kBinH, int kCells, bool kFast>
 int occupancy() {
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+    if (allow_shared<kBinW, kBinH, kCells, kFast>() != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &blocks, batch_evaluate_kernel<kBinW, kBinH, kCells, kFast>, kBinW * kBinH / kCells,
-            0) != cudaSuccess) {
+            dynamic_bytes<kBinW, kBinH, kCells>()) != cudaSuccess) {
         return 1;
     }
     return blocks > 0 ? blocks : 1;

@@ -11,14 +11,13 @@
 // is what lets the GPU compute every node once instead of recomputing parents per tile.
 //
 // Compiled with -fmad=false, so the means and the read-out round as the reference's; the normal
-// draws use CUDA's double log1p and cos, within an ulp of the host's.
+// draws are float Box-Muller on exact double uniforms (node_normal).
 #include "kernels.h"
 
 namespace tgb {
 namespace {
 
 constexpr uint32_t kMidpointDisplacementStream = 0x524D4450u;  // streams.h:73
-constexpr double kPi = 3.14159265358979323846;
 
 struct Words {
     uint32_t x, y, z, w;
@@ -40,8 +39,12 @@ __device__ __forceinline__ Words philox(Words c, uint32_t k0, uint32_t k1) {
 }
 
 // The standard normal of node (col, row) of `level` (Refinement::Displacement,
-// diamond_square.cpp:382-389): one Philox block is RandomStream's first two NextDouble draws,
-// turned into a normal by Box-Muller (StandardNormal, src/random/samplers.cpp:65-69).
+// diamond_square.cpp:382-389): one Philox block is RandomStream's first two NextDouble draws
+// (u1, u2, 53 bits each, exact), turned into a normal by Box-Muller (StandardNormal,
+// src/random/samplers.cpp:65-69), sqrt(-2 log(1 - u1)) cos(2 pi u2). The reference evaluates it
+// in double; here the logarithm, the square root and the cosine run in float on arguments formed
+// exactly in double, within 2e-6 of the double normal (a few 1e-7 of the radius; under 1e-5 m in
+// the refined heights) for a fraction of the instructions: the steps are bound by issuing them.
 __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int level,
                                               uint32_t seed) {
     const uint32_t high = uint32_t((col >> 32) ^ (row >> 32));
@@ -51,7 +54,18 @@ __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int leve
         double((uint64_t(b.x >> 5u) << 26u) | uint64_t(b.y >> 6u)) * 0x1p-53;
     const double u2 =
         double((uint64_t(b.z >> 5u) << 26u) | uint64_t(b.w >> 6u)) * 0x1p-53;
-    return sqrt(-2.0 * log1p(-u1)) * cos(2.0 * kPi * u2);
+    // log(1 - u1): log1p of the float u1 while it is small, else log of the float 1 - u1 (exact
+    // in double), each a few 1e-8 relative.
+    const float logRest = u1 < 0.5 ? log1pf(-float(u1)) : logf(float(1.0 - u1));
+    const float radius = sqrtf(-2.0f * logRest);
+    // cos(pi a) for a = 2 u2 split into float parts a = high + low: cos(pi high) - pi low
+    // sin(pi high), so the float rounding of a costs no accuracy.
+    const double a = 2.0 * u2;
+    const float aHigh = float(a), aLow = float(a - double(aHigh));
+    float sine, cosine;
+    sincospif(aHigh, &sine, &cosine);
+    const float c = fmaf(-3.14159265f * aLow, sine, cosine);
+    return double(radius) * double(c);
 }
 
 __device__ __forceinline__ double at(const DsLevel& l, int64_t col, int64_t row) {

@@ -427,9 +427,12 @@ __global__ void __launch_bounds__(128) distance_tile_kernel(const DistanceTiles 
             }
             __syncthreads();
         }
-        // Backward, in place: front t holds the posts with 2 (hw-1-row) + (ww-1-col) = t.
-        for (int t = 0; t < fronts; ++t) {
-            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hw - 1, t / 2);
+        // Backward, in place: front t holds the posts with 2 (hw-1-row) + (ww-1-col) = t. A row
+        // reads only the rows below it, so the pass stops at the tile's first row.
+        const int hb = hw - (r0 - rw0);
+        const int backFronts = 2 * (hb - 1) + ww;
+        for (int t = 0; t < backFronts; ++t) {
+            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hb - 1, t / 2);
             for (int q = rlo + tid; q <= rhi; q += int(blockDim.x)) {
                 const int r = hw - 1 - q, c = ww - 1 - (t - 2 * q), k = r * ww + c;
                 if ((bits[k >> 5] >> (k & 31)) & 1u) {
@@ -829,16 +832,27 @@ __global__ void dot_kernel(const double* __restrict__ a, const double* __restric
     }
 }
 
+// The block partials summed by one block of kDotBlocks threads as a fixed tree, so every run
+// adds them in the same order.
 __global__ void dot_finish_kernel(const double* __restrict__ partial, double* __restrict__ out,
                                   const CgState* cg) {
-    if (threadIdx.x == 0 && !stopped(cg)) {
-        double x = 0.0, y = 0.0;
-        for (int i = 0; i < kDotBlocks; ++i) {
-            x += partial[i];
-            y += partial[kDotBlocks + i];
+    if (stopped(cg)) {
+        return;
+    }
+    __shared__ double s0[kDotBlocks], s1[kDotBlocks];
+    s0[threadIdx.x] = partial[threadIdx.x];
+    s1[threadIdx.x] = partial[kDotBlocks + threadIdx.x];
+    __syncthreads();
+    for (int half = kDotBlocks / 2; half > 0; half >>= 1) {
+        if (int(threadIdx.x) < half) {
+            s0[threadIdx.x] += s0[threadIdx.x + half];
+            s1[threadIdx.x] += s1[threadIdx.x + half];
         }
-        out[0] = x;
-        out[1] = y;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s0[0];
+        out[1] = s1[0];
     }
 }
 
@@ -941,6 +955,9 @@ struct SeamRead {
     uint32_t w, h;          // the lattice
     double originX, pixelWidth, rowRotation, originY, colRotation, pixelHeight;
     bool set;               // any post set
+    // Cells of the grid outside [c0, c1] x [r0, r1] read no post (a conservative box; the exact
+    // test is seam_at's).
+    int64_t c0, c1, r0, r1;
 };
 
 __device__ __forceinline__ double post(const SeamRead& s, double col, double row) {
@@ -998,17 +1015,24 @@ __global__ void seam_fill_kernel(const SeamRead s, const Grid g, const float* __
     for (uint32_t row = blockIdx.y; row < g.height; row += gridDim.y) {
         const size_t k = size_t(row) * g.width + col;
         const float cell = heights[k];
-        const float value = later[k];
         const bool missing = !isfinite(cell) || (nodata.mode == 2u && cell == nodata.value);
-        const bool laterMissing = !isfinite(value) || (nodata.mode == 2u && value == nodata.value);
-        if (!missing || laterMissing) {
+        if (!missing) {
             continue;
         }
-        const double x = g.originX + (double(col) + 0.5) * g.pixelWidth +
-                         (double(row) + 0.5) * g.rowRotation;
-        const double y = g.originY + (double(col) + 0.5) * g.colRotation +
-                         (double(row) + 0.5) * g.pixelHeight;
-        const double correction = seam_at(s, x, y);
+        const float value = later[k];
+        const bool laterMissing = !isfinite(value) || (nodata.mode == 2u && value == nodata.value);
+        if (laterMissing) {
+            continue;
+        }
+        double correction = 0.0;
+        if (int64_t(col) >= s.c0 && int64_t(col) <= s.c1 && int64_t(row) >= s.r0 &&
+            int64_t(row) <= s.r1) {
+            const double x = g.originX + (double(col) + 0.5) * g.pixelWidth +
+                             (double(row) + 0.5) * g.rowRotation;
+            const double y = g.originY + (double(col) + 0.5) * g.colRotation +
+                             (double(row) + 0.5) * g.pixelHeight;
+            correction = seam_at(s, x, y);
+        }
         heights[k] = correction == 0.0 ? value : float(double(value) + correction);
     }
 }
@@ -1272,8 +1296,8 @@ cudaError_t dots(const Solver& sv, const double* a, const double* b, const doubl
                  const double* d, uint32_t n, double* out) {
     dot_kernel<<<kDotBlocks, 256, 0, sv.s>>>(a, b, c, d, n,
                                              static_cast<double*>(sv.wk->partial.ptr), sv.cg);
-    dot_finish_kernel<<<1, 32, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr), out,
-                                          sv.cg);
+    dot_finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
+                                                  out, sv.cg);
     return cudaGetLastError();
 }
 
@@ -1782,8 +1806,39 @@ int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const
     // SeamField::At is 0 everywhere when no post was set; reading an all-zero field gives the
     // same 0, so the field is always read.
     const bool set = true;
-    SeamRead sr{df, lg.width, lg.height, lg.originX, lg.pixelWidth, lg.rowRotation,
-                lg.originY, lg.colRotation, lg.pixelHeight, set};
+    SeamRead sr{df,         lg.width,       lg.height,       lg.originX,
+                lg.pixelWidth, lg.rowRotation, lg.originY,      lg.colRotation,
+                lg.pixelHeight, set,           0,               int64_t(g.width) - 1,
+                0,           int64_t(g.height) - 1};
+    // Without rotations, the cells whose centers fall within 3 posts of the lattice: the field
+    // reads no post anywhere else (SeamField::At's taps are the 4 x 4 posts around the point).
+    if (lg.rowRotation == 0.0 && lg.colRotation == 0.0 && g.rowRotation == 0.0 &&
+        g.colRotation == 0.0) {
+        // Points whose lattice position is within [-3, n + 3] posts on both axes.
+        const double xa = lg.originX - 3.0 * lg.pixelWidth;
+        const double xb = lg.originX + (double(lg.width) + 3.0) * lg.pixelWidth;
+        const double ya = lg.originY - 3.0 * lg.pixelHeight;
+        const double yb = lg.originY + (double(lg.height) + 3.0) * lg.pixelHeight;
+        const double xlo = std::min(xa, xb), xhi = std::max(xa, xb);
+        const double ylo = std::min(ya, yb), yhi = std::max(ya, yb);
+        // Cell (col, row) has its center at origin + (index + 0.5) * pixel.
+        auto range = [](double lo, double hi, double origin, double pixel, int64_t n,
+                        int64_t& a, int64_t& b) {
+            double u = (lo - origin) / pixel - 0.5, v = (hi - origin) / pixel - 0.5;
+            if (u > v) {
+                std::swap(u, v);
+            }
+            if (!(std::isfinite(u) && std::isfinite(v))) {
+                return;
+            }
+            u = std::clamp(u, -1e15, 1e15);
+            v = std::clamp(v, -1e15, 1e15);
+            a = std::max<int64_t>(0, int64_t(std::floor(u)) - 1);
+            b = std::min<int64_t>(n - 1, int64_t(std::ceil(v)) + 1);
+        };
+        range(xlo, xhi, g.originX, g.pixelWidth, g.width, sr.c0, sr.c1);
+        range(ylo, yhi, g.originY, g.pixelHeight, g.height, sr.r0, sr.r1);
+    }
     const NoData nd{nodata.mode, nodata.value};
     seam_fill_kernel<<<dim3(blocks_for(g.width), std::min<uint32_t>(g.height, 65535u)), 256, 0, s>>>(
         sr, g, dl, nd, dh);

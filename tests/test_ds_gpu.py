@@ -61,7 +61,8 @@ def test_displacement_draws_match_oracle(device):
     words, normals = device.philox_probe(sext)
     for i in range(500):
         want = rs.rs_ds_normal(int(cols[i]), int(rows[i]), int(levels[i]), 7)
-        assert abs(normals[i] - want) <= 1e-13 * max(1.0, abs(want))
+        # Box-Muller in float on the exact uniforms: a few 1e-7 of the radius (at most 8.6).
+        assert abs(normals[i] - want) <= 2e-6, (i, normals[i], want)
 
 
 def test_ds_deterministic_and_windowed(device, fx):
