@@ -317,6 +317,23 @@ int tg_seam_samples(tg_device* device, const float* earlier, const float* later,
                     tg_nodata nodata, uint8_t* data, float* difference, int memory,
                     void* stream);
 
+/* Crater datums: the relief of the older craters under each fitted crater's datum footprint
+ * (KernelDatumRelief, include/terraingen/layers/kernels/craters.h:1214-1316), which RunKernel runs
+ * for FitDatumsWithKernel (src/layers/craters/shaping/datum_fit.cpp:303-328) with the program
+ * src/layers/kernels/crater_datums.slang. `kernel` is the 200-byte CraterDatumKernel, read on
+ * the host in either memory mode (a parameter block, as tg_craters_apply's); records
+ * (144 bytes each), data, the band floats and cells, cells, entries and targets are the index the
+ * reference builds (IndexDatumRelief, datum_fit.cpp:268-296). `heights` is the lattice strip:
+ * `rows` rows of `width` points (one row per fitted crater, from target `first_row`), each point
+ * receiving its relief added. */
+int tg_crater_datums(tg_device* device, const void* kernel, size_t kernel_bytes,
+                     const void* records, uint32_t n_records, const float* data, uint32_t n_data,
+                     const float* band_floats, uint32_t n_band_floats, const uint32_t* band_cells,
+                     uint32_t n_band_cells, const uint32_t* cells, uint32_t n_cells,
+                     const uint32_t* entries, uint32_t n_entries, const uint32_t* targets,
+                     uint32_t n_targets, uint32_t width, uint32_t rows, uint32_t first_row,
+                     float* heights, int memory, void* stream);
+
 /* --- crater populations and kernel batches (host) ------------------------------------------ */
 
 /* A crater layer's population on a plane: a power-law density N(>D) = c D^-exponent per m^2 on

@@ -40,6 +40,7 @@ class Scene(C.Structure):
         ("rimSigma", _D), ("terraceOnset", _D), ("terraceFull", _D),
         ("boulders", _I32), ("boulderSeed", _U32), ("boulderCoefficient", _D),
         ("boulderExponent", _D), ("boulderMin", _D), ("boulderMax", _D), ("heightRatio", _D),
+        ("datum", _I32), ("interiorReplacement", _D),
     ]
 
 
@@ -68,7 +69,8 @@ def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, c
                         maxDiameter=60.0, lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04,
                         profile=0, transitionDiameter=15000.0, applyPreset=0,
                         noiseAmplitude=0.0, rimNoiseAmplitude=0.0, wallStreaks=0.0, ejecta=0.0,
-                        rimSigma=0.0, terraceOnset=0.0, terraceFull=0.0)
+                        rimSigma=0.0, terraceOnset=0.0, terraceFull=0.0, datum=0,
+                        interiorReplacement=0.0)
         defaults.update(craters)
         for k, v in defaults.items():
             setattr(s, k, v)
@@ -257,6 +259,9 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_craters.restype = C.c_long
     lib.tgref_boulders.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_long]
     lib.tgref_boulders.restype = C.c_long
+    if hasattr(lib, "tgref_datum_relief"):
+        lib.tgref_datum_relief.argtypes = [C.c_void_p] * 8 + [_U32, _U32, _U32, C.c_void_p]
+        lib.tgref_datum_relief.restype = C.c_int
     if hasattr(lib, "tgref_boulders_posed"):
         lib.tgref_boulders_posed.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_void_p, C.c_long]
         lib.tgref_boulders_posed.restype = C.c_long
@@ -323,6 +328,25 @@ CRATER_FIELDS = ["kernel", "records", "data", "heads", "entries", "xs", "x_lows"
 NOISE_FIELDS = ["kernel", "xs", "ys", "heights"]
 
 
+DATUM_FIELDS = ["kernel", "records", "data", "band_floats", "band_cells", "cells", "entries",
+                "targets", "heights"]
+
+
+def datum_relief(lib: C.CDLL, call: dict) -> np.ndarray:
+    """The reference's KernelDatumRelief over a captured tg_crater_datums call (tgref_datum_relief):
+    the lattice strip's heights after the relief is added."""
+    heights = call["heights"].view(np.float32).copy()
+    f = {k: np.ascontiguousarray(call[k]) for k in DATUM_FIELDS[:8]}
+    st = lib.tgref_datum_relief(f["kernel"].ctypes.data, f["records"].ctypes.data,
+                                f["data"].ctypes.data, f["band_floats"].ctypes.data,
+                                f["band_cells"].ctypes.data, f["cells"].ctypes.data,
+                                f["entries"].ctypes.data, f["targets"].ctypes.data, call["width"],
+                                call["rows"], call["first_row"], heights.ctypes.data)
+    if st != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return heights
+
+
 def captured(lib: C.CDLL) -> list:
     """Every captured backend call as a dict of numpy arrays."""
     calls = []
@@ -330,7 +354,7 @@ def captured(lib: C.CDLL) -> list:
         info = np.zeros(8, np.uint32)
         lib.tgref_capture_info(call, info.ctypes.data)
         kind = int(info[0])
-        names = CRATER_FIELDS if kind == 2 else NOISE_FIELDS
+        names = {2: CRATER_FIELDS, 3: DATUM_FIELDS}.get(kind, NOISE_FIELDS)
         rec = {"kind": kind, "width": int(info[1]), "rows": int(info[2]),
                "first_row": int(info[3]), "nodata_mode": int(info[4]),
                "nodata_value": float(info[5:6].view(np.float32)[0])}

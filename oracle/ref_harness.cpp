@@ -23,6 +23,7 @@
 #include "terraingen/layers/craters/shaping/morphometry.h"
 #include "terraingen/layers/boulders/boulder_layer.h"
 #include "terraingen/layers/fade.h"
+#include "terraingen/layers/kernels/craters.h"
 #include "terraingen/sources/diamond_square.h"
 #include "terraingen/sources/raster_source.h"
 #include "terraingen/sources/source_chain.h"
@@ -79,6 +80,10 @@ struct tgref_scene {
     int32_t boulders;
     uint32_t boulderSeed;
     double boulderCoefficient, boulderExponent, boulderMin, boulderMax, heightRatio;
+    // crater datums: 0 none, 1 plane, 2 mean height, 3 center height (CraterDatum), and the
+    // share of the interior they replace
+    int32_t datum;
+    double interiorReplacement;
 };
 
 const char* tgref_error() {
@@ -136,6 +141,10 @@ std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s) {
     options.apply.texture.wallStreaks = s.wallStreaks;
     options.apply.texture.ejecta = s.ejecta;
     options.apply.rimSmoothing.sigmaRadii = s.rimSigma;
+    if (s.datum > 0) {
+        options.apply.datum = static_cast<CraterDatum>(s.datum);
+        options.apply.interiorReplacement = s.interiorReplacement;
+    }
     if (s.terraceOnset > 0.0) {
         options.apply.terraces.onsetDiameter = s.terraceOnset;
         options.apply.terraces.fullDiameter = s.terraceFull;
@@ -559,6 +568,37 @@ int tgref_evaluate_below_boulders(const tgref_scene* s, unsigned threads, float*
 
 }  // extern "C"
 
+extern "C" {
+
+/// KernelDatumRelief (the reference's header function, on the CPU) at every point of a lattice
+/// strip as crater_datums.slang adds it: `heights` (rows x width) += the relief of target
+/// first_row + row at point column, over the index a captured tg_crater_datums call holds.
+int tgref_datum_relief(const void* kernel, const void* records, const float* data,
+                       const float* bandFloats, const uint32_t* bandCells, const uint32_t* cells,
+                       const uint32_t* entries, const uint32_t* targets, uint32_t width,
+                       uint32_t rows, uint32_t firstRow, float* heights) {
+    try {
+        CraterDatumKernel k;
+        std::memcpy(&k, kernel, sizeof(k));
+        const auto* recs = static_cast<const CraterRecord*>(records);
+        CraterData values;
+        values.values = data;
+        for (uint32_t r = 0; r < rows; ++r) {
+            for (uint32_t p = 0; p < width; ++p) {
+                float& h = heights[size_t(r) * width + p];
+                h = h + KernelDatumRelief(k, values, recs, bandFloats, bandCells, cells, entries,
+                                          targets[firstRow + r], p);
+            }
+        }
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+}  // extern "C"
+
 #ifdef TGREF_CAPTURE
 // --- capture stubs for the tg_* C ABI the adapter calls ------------------------------------
 #include "tgb200.h"
@@ -637,6 +677,31 @@ int tg_craters_apply_lists(tg_device*, const void* kernel, size_t kernelBytes, c
     c.rows = rows;
     c.firstRow = firstRow;
     c.nodata = nodata;
+    g_captures.push_back(std::move(c));
+    return TG_OK;
+}
+
+int tg_crater_datums(tg_device*, const void* kernel, size_t kernelBytes, const void* records,
+                     uint32_t nRecords, const float* data, uint32_t nData,
+                     const float* bandFloats, uint32_t nBandFloats, const uint32_t* bandCells,
+                     uint32_t nBandCells, const uint32_t* cells, uint32_t nCells,
+                     const uint32_t* entries, uint32_t nEntries, const uint32_t* targets,
+                     uint32_t nTargets, uint32_t width, uint32_t rows, uint32_t firstRow,
+                     float* heights, int, void*) {
+    Capture c;
+    c.kind = 3;
+    c.fields = {Bytes(static_cast<const unsigned char*>(kernel), kernelBytes),
+                Bytes(static_cast<const unsigned char*>(records), size_t(nRecords) * 144),
+                Bytes(data, nData),
+                Bytes(bandFloats, nBandFloats),
+                Bytes(bandCells, nBandCells),
+                Bytes(cells, nCells),
+                Bytes(entries, nEntries),
+                Bytes(targets, nTargets),
+                Bytes(heights, size_t(width) * rows)};
+    c.width = width;
+    c.rows = rows;
+    c.firstRow = firstRow;
     g_captures.push_back(std::move(c));
     return TG_OK;
 }

@@ -167,6 +167,8 @@ class SeamStats(C.Structure):
 SIGNATURES.update({
     "tg_seam_solve": [_P, _P, _P, _U32, _U32, _D, _D, C.POINTER(SeamOptions), _P, _I, _P],
     "tg_seam_stats_get": [C.POINTER(SeamStats)],
+    "tg_crater_datums": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32,
+                         _P, _U32, _U32, _U32, _U32, _P, _I, _P],
     "tg_seam_fill": [_P, _P, C.POINTER(Grid), _P, C.POINTER(Grid), _P, NoData, _I, _P],
     "tg_seam_samples": [_P, _P, _P, C.POINTER(Grid), C.c_int64, C.c_int64, _U32, _U32, NoData,
                         _P, _P, _I, _P],

@@ -5,7 +5,8 @@
 // Built inside a TerrainGen tree in place of src/gpu/cuda.cpp, it makes
 // Backend::Cuda run the noise-layer and crater kernels on the B200 kernels of libtgb200 instead of
 // JIT-compiled Slang PTX: RunKernel (src/gpu/kernel.cpp) binds the same buffers and push
-// constants, and this device maps them onto tg_noise_layer_rows and tg_craters_apply_lists.
+// constants, and this device maps them onto tg_noise_layer_rows, tg_craters_apply_lists and
+// tg_crater_datums.
 // Programs are told apart by their compiled form's address, so the generated CompiledKernel<>
 // definitions (cmake/Kernel.cpp.in) are used as they are; PTX is not read.
 #include "gpu/cuda.h"
@@ -32,7 +33,7 @@ struct Params {
     std::uint32_t firstRow;
 };
 
-enum class Program { None, NoiseLayer, Craters };
+enum class Program { None, NoiseLayer, Craters, Datums };
 
 /// Whether `program` is the compiled form of kernel `Kernel`.
 template <typename Kernel> bool Is(const KernelProgram& program) {
@@ -47,6 +48,9 @@ Program Identify(const KernelProgram& program) {
     }
     if (Is<CraterShapeKernel>(program)) {
         return Program::Craters;
+    }
+    if (Is<CraterDatumKernel>(program)) {
+        return Program::Datums;
     }
     return Program::None;
 }
@@ -131,6 +135,25 @@ void CudaCompute::Run(const KernelProgram& program, Span<const DeviceBuffer> buf
                 As<float>(buffers[2]), lows + params.width, params.width, params.rows,
                 params.firstRow, heights, nodata, TG_MEMORY_HOST, nullptr) != TG_OK) {
             Throw("craters");
+        }
+        return;
+    }
+    if (kind == Program::Datums && buffers.size() >= 11) {
+        // heights, xs, ys, CraterDatumKernel, records, data, band floats, band cells, cells,
+        // entries, targets (src/layers/kernels/crater_datums.slang, bound by AddDatumRelief,
+        // datum_fit.cpp:303-328)
+        float* heights = reinterpret_cast<float*>(buffers[0].output);
+        if (tg_crater_datums(m_state->device, buffers[3].bytes.data(), buffers[3].bytes.size(),
+                             buffers[4].bytes.data(), Count<CraterRecord>(buffers[4]),
+                             As<float>(buffers[5]), Count<float>(buffers[5]),
+                             As<float>(buffers[6]), Count<float>(buffers[6]),
+                             As<std::uint32_t>(buffers[7]), Count<std::uint32_t>(buffers[7]),
+                             As<std::uint32_t>(buffers[8]), Count<std::uint32_t>(buffers[8]),
+                             As<std::uint32_t>(buffers[9]), Count<std::uint32_t>(buffers[9]),
+                             As<std::uint32_t>(buffers[10]), Count<std::uint32_t>(buffers[10]),
+                             params.width, params.rows, params.firstRow, heights, TG_MEMORY_HOST,
+                             nullptr) != TG_OK) {
+            Throw("crater datums");
         }
         return;
     }

@@ -33,6 +33,7 @@ UNITS = {
     "boulders.cu": [],
     "diamond_square.cu": ["-fmad=false"],
     "seams.cu": ["-fmad=false"],
+    "datums.cu": ["-fmad=false"],
     "batch.cu": ["-fmad=false"],
     "batch_api.cu": [],
     "serve.cu": [],

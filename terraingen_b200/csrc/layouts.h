@@ -126,6 +126,16 @@ struct CraterShapeKernel {  // craters.h:49
 };
 static_assert(sizeof(CraterShapeKernel) == 188, "CraterShapeKernel must match std430");
 
+// What fitting crater datums takes (craters.h:1214): the craters' shapes, the fit footprint in
+// radii, the lattice points per side across it, and the size bands of the crater index.
+struct CraterDatumKernel {
+    CraterShapeKernel shape;
+    float fitRadii;
+    uint32_t latticeSide;
+    uint32_t bandCount;
+};
+static_assert(sizeof(CraterDatumKernel) == 200, "CraterDatumKernel must match std430");
+
 struct CraterRecord {  // craters.h:81
     float x;
     float y;

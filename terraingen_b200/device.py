@@ -317,6 +317,30 @@ class Device:
                                           _stream(b.memory)))
         return data, difference
 
+    def crater_datums(self, kernel, records, data, band_floats, band_cells, cells, entries,
+                      targets, heights, width: int, rows: int, first_row: int = 0):
+        """FitDatumsWithKernel's relief (KernelDatumRelief, craters.h:1214-1316): `heights`
+        (rows x width lattice points, float32) += the relief of the older craters at each point
+        of each target crater's fit footprint. `kernel` is the CraterDatumKernel's bytes (host);
+        the rest host arrays (raw bytes for `records`) or device tensors."""
+        b = _Buffers()
+        # The parameter block is read on the host whatever the memory of the rest.
+        k = np.ascontiguousarray(np.asarray(kernel), np.uint8)
+        kp = C.c_void_p(k.ctypes.data)
+        rp = b.ptr(records)
+        n_records = (records.numel() if _is_torch(records) else np.asarray(records).nbytes) // 144
+        args = []
+        for arr, dtype in ((data, np.float32), (band_floats, np.float32),
+                           (band_cells, np.uint32), (cells, np.uint32), (entries, np.uint32),
+                           (targets, np.uint32)):
+            args.append(b.ptr(arr, None if _is_torch(arr) else dtype))
+            args.append(arr.numel() if _is_torch(arr) else len(arr))
+        hp = b.ptr(heights, None if _is_torch(heights) else np.float32)
+        kbytes = k.nbytes
+        N.check(self._lib.tg_crater_datums(self._handle, kp, kbytes, rp, n_records, *args, width,
+                                           rows, first_row, hp, b.memory, _stream(b.memory)))
+        return heights
+
     def philox_probe(self, sextets: np.ndarray):
         """(words [n, 4] u32, normals [n] f64) of n (counter x4, key x2) sextets."""
         sextets = np.ascontiguousarray(sextets, np.uint32).reshape(-1, 6)

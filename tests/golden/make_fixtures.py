@@ -290,6 +290,34 @@ def chain_fixture() -> None:
     np.savez_compressed(OUT / "chain.npz", **arrays)
 
 
+DATUM_SCENE = (centered(200, 200, 1.0, 40.0, -30.0),
+               dict(seed=3, sfdCoefficient=0.08, minDiameter=3.0, maxDiameter=60.0, profile=0,
+                    applyPreset=1, datum=1, interiorReplacement=0.5))
+
+
+def datum_fixture() -> None:
+    """Crater datums fitted as planes: the tg_crater_datums call the reference makes (captured)
+    with the lattice after the reference's own KernelDatumRelief, and the scene's CPU heights."""
+    ref = H.reference()
+    cap = H.capture()
+    grid, fields = DATUM_SCENE
+    src = np.array([L.fractal(seed=5, wavelength=150.0, amplitude=8.0, octaves=5)])
+    scene = H.make_scene(grid, source_fractals=src, craters=fields)
+    arrays = {"grid": np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel]),
+              "source": src.view(np.uint8)}
+    arrays["expected"], _ = H.evaluate(ref, scene, 0, 1)
+    H.evaluate(cap, scene, 1, 1)
+    calls = [c for c in H.captured(cap) if c["kind"] == 3]
+    assert len(calls) == 1, len(calls)
+    call = calls[0]
+    for k in H.DATUM_FIELDS:
+        arrays[f"call_{k}"] = call[k]
+    arrays["call_shape"] = np.array([call["width"], call["rows"], call["first_row"]])
+    arrays["relief"] = H.datum_relief(ref, call)
+    print("datums", call["rows"], "fitted,", len(call["records"]) // 144, "records")
+    np.savez_compressed(OUT / "datums.npz", **arrays)
+
+
 def population_fixture() -> None:
     """The config-1 crater population (centers, diameters, ages, ids): bit-exact targets."""
     ref = H.reference()
@@ -308,5 +336,6 @@ if __name__ == "__main__":
     population_fixture()
     seam_fixtures()
     chain_fixture()
+    datum_fixture()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size)
