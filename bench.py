@@ -27,6 +27,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from terraingen_b200 import ranks  # noqa: E402
+
 METRIC = "Mcells/s at <=1e-3 m err: served/batched vs plain GPU; p50/p99 tile ms"
 UNIT = "Mcells/s"
 SIDE = 4097
@@ -76,37 +78,21 @@ def parse():
 
 
 def dist_setup(n):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    r = ranks.setup("nccl")
+    return r.rank, r.world, r.local
 
-        import torch
-        import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return rank, world, local
+def _ranks(world):
+    return ranks.Ranks(int(os.environ.get("RANK", "0")), world,
+                       int(os.environ.get("LOCAL_RANK", "0")), "cuda")
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
+    ranks.barrier(_ranks(world))
 
 
 def max_over_ranks(value, world):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return ranks.max_over_ranks(value, _ranks(world))
 
 
 class Clocks:
@@ -237,7 +223,7 @@ def batched_form(dev, args, rank, world, alu_peak):
     from terraingen_b200.batch import Batch
     from terraingen_b200.workloads import uneven_tiles
 
-    ts = uneven_tiles(args.tiles, seed=11 + 7919 * rank)
+    ts = uneven_tiles(args.tiles, seed=ranks.tiles_seed(rank))
     batch = Batch(dev)
     batch.load(ts)
     out = torch.empty(ts.output_floats, dtype=torch.float32, device="cuda")
@@ -362,7 +348,7 @@ def dem_form(dev, args, rank, world):
     from terraingen_b200.chain import PatchChain, Seams
     from terraingen_b200.workloads import dem20481
 
-    w = dem20481(args.dem_side, (args.dem_side - 1) // 10 + 1, seed=7 + 10 * rank)
+    w = dem20481(args.dem_side, (args.dem_side - 1) // 10 + 1, seed=ranks.dem_seed(rank))
     pg = w.post_grid
     posts = torch.empty((pg.height, pg.width), dtype=torch.float32, device="cuda")
     dev.noise_source(w.fractals, pg, posts, 0.0)
@@ -469,10 +455,11 @@ def served_form(dev, args, rank, world):
     opts = dem_stack_options(slots=3, max_batch_cells=8 << 20)
     seconds = max(1.0, min(3.0, args.serve_seconds))
     with Server(dev, opts) as server:
-        run_stream(server, camera_stream(0.5, seed=1 + rank), realtime=False, device=True)
-        nominal = run_stream(server, camera_stream(seconds, seed=2 + rank), realtime=True,
+        warm, real, sat = ranks.stream_seeds(rank)
+        run_stream(server, camera_stream(0.5, seed=warm), realtime=False, device=True)
+        nominal = run_stream(server, camera_stream(seconds, seed=real), realtime=True,
                              device=True)
-        sat_reqs = camera_stream(1.0, seed=3 + rank)
+        sat_reqs = camera_stream(1.0, seed=sat)
         run_stream(server, sat_reqs, realtime=False, device=True)  # regions and buffers warm
         saturated = run_stream(server, sat_reqs, realtime=False, device=True)
         tiles = [r for r in sat_reqs if r.grid is not None]
@@ -562,7 +549,7 @@ def main():
             print(json.dumps({"form": "dem_refinement", **form}), flush=True)
         return
     # Each rank's own tile, side by side along x (independent tiles, no exchange).
-    w = terrain4097(SIDE, PIXEL, cx=rank * SIDE * PIXEL)
+    w = terrain4097(SIDE, PIXEL, cx=ranks.terrain_center(rank, SIDE, PIXEL)[0])
     stream = torch.cuda.current_stream()
     rec = torch.from_numpy(w.crater_records.view(np.uint8)).cuda()
     data = torch.from_numpy(w.crater_data).cuda()
