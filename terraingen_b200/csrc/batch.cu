@@ -506,7 +506,7 @@ __device__ __forceinline__ void indexed_points(const CraterShapeKernel& k,
 }
 
 template <int kBinW, int kBinH, int kCells, bool kFast>
-__global__ void __launch_bounds__(kBinW* kBinH / kCells)
+__global__ void __launch_bounds__(kBinW* kBinH / kCells, 768 / (kBinW * kBinH / kCells))
     batch_evaluate_kernel(const CraterShapeKernel k, const BatchNoise noise, const BatchView v) {
     constexpr uint32_t kRowThreads = kBinW / kCells;  // threads along one row of a bin
     constexpr uint32_t kBinCellCount = kBinW * kBinH;  // cells of a bin, points of a point block
@@ -776,6 +776,9 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                                                     tileX <= int(entry.tileX1) &&
                                                     tileY >= int(entry.tileY0) &&
                                                     tileY <= int(entry.tileY1)));
+                    if (!__any_sync(0xffffffffu, inTile)) {
+                        continue;  // none of the warp's cells is in the crater's window
+                    }
                     const float cull2 = entry.cull * entry.cull;
                     uint32_t need = 0;
 #pragma unroll
@@ -786,6 +789,9 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells)
                             __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) < cull2) {
                             need |= 1u << j;
                         }
+                    }
+                    if (!__any_sync(0xffffffffu, need != 0u)) {
+                        continue;
                     }
                     const uint32_t mine = __popc(need);
                     uint32_t before = mine;

@@ -280,6 +280,9 @@ __global__ void __launch_bounds__(kShapeThreads)
             const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
                                 tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
                                 tileY <= int(entry.tileY1);
+            if (!__any_sync(0xffffffffu, inTile)) {
+                continue;  // none of the warp's reference tiles is in the crater's window
+            }
             const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
             const float cull2 = entry.cull * entry.cull;
             uint32_t need = 0;
@@ -289,6 +292,9 @@ __global__ void __launch_bounds__(kShapeThreads)
                 if (inTile && live[j] && dx * dx + dy * dy < cull2) {
                     need |= 1u << j;
                 }
+            }
+            if (!__any_sync(0xffffffffu, need != 0u)) {
+                continue;
             }
             const uint32_t mine = __popc(need);
             // Exclusive prefix of the lanes' counts.
