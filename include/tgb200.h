@@ -303,10 +303,12 @@ int tg_seam_solve(tg_device* device, const uint8_t* data, const float* differenc
 int tg_seam_stats_get(tg_seam_stats* stats);
 /* FillGridGaps: each cell of `heights` (on `grid`) holding no data takes `later` (the later
  * source's height on the same grid) plus the field (posts on `lattice`) read at the cell's
- * center by Catmull-Rom interpolation; cells where `later` has no data are left alone. */
+ * center by Catmull-Rom interpolation; cells where `later` has no data are left alone.
+ * `window` (host memory, may be null for the whole grid) limits the cells visited to
+ * col0, row0, width, height: the later source's window, outside which it has no data. */
 int tg_seam_fill(tg_device* device, const float* field, const tg_grid* lattice,
                  const float* later, const tg_grid* grid, float* heights, tg_nodata nodata,
-                 int memory, void* stream);
+                 const uint32_t* window, int memory, void* stream);
 /* SampleSources (seam_field.cpp:76-113) for two sources held as rasters on one grid: the lattice
  * is the `lw` x `lh` posts whose first post is cell (`col0`, `row0`) of `grid` (negative, or past
  * the grid's edge, where the lattice pads it; its posts there have no data). `data` gets 1 where

@@ -124,7 +124,9 @@ class PatchChain:
                                       coarsest_sweeps=s.coarsest_sweeps)
             if ev:
                 ev[2].record(stream)
-            dev.seam_fill(field, lgrid, later, self.grid, self.heights)
+            wk = self.windows[k]
+            dev.seam_fill(field, lgrid, later, self.grid, self.heights,
+                          window=(wk.col0, wk.row0, wk.width, wk.height))
             if ev:
                 ev[3].record(stream)
                 events.append(ev)

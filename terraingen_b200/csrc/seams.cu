@@ -1006,34 +1006,45 @@ __device__ double seam_at(const SeamRead& s, double x, double y) {
 // none).
 // A cell is missing when it is not finite or, with a no-data value, equal to it
 // (Raster::IsMissing, include/terraingen/raster/raster.h:167).
-__global__ void seam_fill_kernel(const SeamRead s, const Grid g, const float* __restrict__ later,
-                                 const NoData nodata, float* __restrict__ heights) {
-    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= g.width) {
+// Cells [c0, c0 + w) x [r0, r0 + h) of the grid, 4 adjacent cells of a row per thread.
+struct FillWindow {
+    uint32_t c0, r0, w, h;
+};
+
+__global__ void seam_fill_kernel(const SeamRead s, const Grid g, const FillWindow win,
+                                 const float* __restrict__ later, const NoData nodata,
+                                 float* __restrict__ heights) {
+    const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+    if (first >= win.w) {
         return;
     }
-    for (uint32_t row = blockIdx.y; row < g.height; row += gridDim.y) {
-        const size_t k = size_t(row) * g.width + col;
-        const float cell = heights[k];
-        const bool missing = !isfinite(cell) || (nodata.mode == 2u && cell == nodata.value);
-        if (!missing) {
-            continue;
+    for (uint32_t rr = blockIdx.y; rr < win.h; rr += gridDim.y) {
+        const uint32_t row = win.r0 + rr;
+        for (uint32_t j = first; j < min(first + 4u, win.w); ++j) {
+            const uint32_t col = win.c0 + j;
+            const size_t k = size_t(row) * g.width + col;
+            const float cell = heights[k];
+            const bool missing = !isfinite(cell) || (nodata.mode == 2u && cell == nodata.value);
+            if (!missing) {
+                continue;
+            }
+            const float value = later[k];
+            const bool laterMissing =
+                !isfinite(value) || (nodata.mode == 2u && value == nodata.value);
+            if (laterMissing) {
+                continue;
+            }
+            double correction = 0.0;
+            if (int64_t(col) >= s.c0 && int64_t(col) <= s.c1 && int64_t(row) >= s.r0 &&
+                int64_t(row) <= s.r1) {
+                const double x = g.originX + (double(col) + 0.5) * g.pixelWidth +
+                                 (double(row) + 0.5) * g.rowRotation;
+                const double y = g.originY + (double(col) + 0.5) * g.colRotation +
+                                 (double(row) + 0.5) * g.pixelHeight;
+                correction = seam_at(s, x, y);
+            }
+            heights[k] = correction == 0.0 ? value : float(double(value) + correction);
         }
-        const float value = later[k];
-        const bool laterMissing = !isfinite(value) || (nodata.mode == 2u && value == nodata.value);
-        if (laterMissing) {
-            continue;
-        }
-        double correction = 0.0;
-        if (int64_t(col) >= s.c0 && int64_t(col) <= s.c1 && int64_t(row) >= s.r0 &&
-            int64_t(row) <= s.r1) {
-            const double x = g.originX + (double(col) + 0.5) * g.pixelWidth +
-                             (double(row) + 0.5) * g.rowRotation;
-            const double y = g.originY + (double(col) + 0.5) * g.colRotation +
-                             (double(row) + 0.5) * g.pixelHeight;
-            correction = seam_at(s, x, y);
-        }
-        heights[k] = correction == 0.0 ? value : float(double(value) + correction);
     }
 }
 
@@ -1743,8 +1754,8 @@ int tg_seam_stats_get(tg_seam_stats* stats) {
 }
 
 int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const float* later,
-                 const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
-                 void* stream) {
+                 const tg_grid* grid, float* heights, tg_nodata nodata, const uint32_t* window,
+                 int memory, void* stream) {
     if (int st = check_device(d)) {
         return st;
     }
@@ -1840,8 +1851,17 @@ int tg_seam_fill(tg_device* d, const float* field, const tg_grid* lattice, const
         range(ylo, yhi, g.originY, g.pixelHeight, g.height, sr.r0, sr.r1);
     }
     const NoData nd{nodata.mode, nodata.value};
-    seam_fill_kernel<<<dim3(blocks_for(g.width), std::min<uint32_t>(g.height, 65535u)), 256, 0, s>>>(
-        sr, g, dl, nd, dh);
+    FillWindow win{0, 0, g.width, g.height};
+    if (window != nullptr) {
+        win = FillWindow{window[0], window[1], window[2], window[3]};
+        if (uint64_t(win.c0) + win.w > g.width || uint64_t(win.r0) + win.h > g.height) {
+            return done(fail(TG_ERROR_ARGUMENT, "the fill window leaves the grid"));
+        }
+    }
+    if (win.w > 0 && win.h > 0) {
+        seam_fill_kernel<<<dim3(blocks_for((win.w + 3) / 4), std::min<uint32_t>(win.h, 65535u)),
+                           256, 0, s>>>(sr, g, win, dl, nd, dh);
+    }
     if (cudaGetLastError() != cudaSuccess) {
         return done(fail(TG_ERROR_CUDA, "seam fill launch"));
     }

@@ -279,16 +279,20 @@ class Device:
                        "solve_ms": st.solve_ms}
 
     def seam_fill(self, field, lattice: GridSpec, later, grid: GridSpec, heights,
-                  nodata=(1, 0.0)):
+                  nodata=(1, 0.0), window=None):
         """FillGridGaps (src/sources/source_chain.cpp:167): cells of `heights` holding no data
-        take `later` plus the field read at their centers."""
+        take `later` plus the field read at their centers. `window` (col0, row0, width, height)
+        limits the cells visited to where `later` can have data."""
         b = _Buffers()
         fp = b.ptr(field, np.float32)
         lp = b.ptr(later, np.float32)
         hp = b.ptr(heights, np.float32)
         lg, g = lattice.native(), grid.native()
+        win = None if window is None else np.ascontiguousarray(window, np.uint32)
         N.check(self._lib.tg_seam_fill(self._handle, fp, C.byref(lg), lp, C.byref(g), hp,
-                                       N.NoData(*nodata), b.memory, _stream(b.memory)))
+                                       N.NoData(*nodata),
+                                       None if win is None else C.c_void_p(win.ctypes.data),
+                                       b.memory, _stream(b.memory)))
         return heights
 
     def seam_samples(self, earlier, later, grid: GridSpec, col0: int, row0: int, lw: int,

@@ -223,3 +223,22 @@ def test_patch_chain_is_the_reference_chain(device, mode):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
     else:
         assert np.abs(got.astype(np.float64) - want).max() <= 1e-4
+
+
+def test_fill_window_is_the_fill_within_it(device, z):
+    # A window of the grid: the same cells as the whole fill inside it, nothing outside.
+    key = "hole_height"
+    lattice = _lattice_grid(z, key)
+    g = grid_of(z["hole_fine_grid"])
+    whole = z["hole_fine_earlier"].copy()
+    device.seam_fill(z[f"{key}_field"], lattice, z["hole_fine_later"], g, whole)
+    part = z["hole_fine_earlier"].copy()
+    c0, r0, w, h = 17, 9, 101, 77
+    device.seam_fill(z[f"{key}_field"], lattice, z["hole_fine_later"], g, part,
+                     window=(c0, r0, w, h))
+    inside = np.zeros(part.shape, bool)
+    inside[r0:r0 + h, c0:c0 + w] = True
+    assert np.array_equal(part[inside].view(np.uint32), whole[inside].view(np.uint32))
+    before = z["hole_fine_earlier"]
+    assert np.array_equal(part[~inside].view(np.uint32), before[~inside].view(np.uint32))
+    assert np.count_nonzero(part[inside] != before[inside]) > 100
