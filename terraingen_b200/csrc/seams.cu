@@ -5,11 +5,11 @@
 // From the samples on the seam lattice (1 where the earlier source has data, earlier minus later
 // where both do):
 //   1. the band: posts with data within 3 posts of a gap keep their difference (NearGaps);
-//   2. the chamfer distance from each post to the nearest post with data (DataDistances), in the
-//      reference's own relaxation order: rows top down then bottom up, each row as a recurrence
-//      along it, so every distance (and carried value) has the reference's float bits; values
-//      beyond the reach are never read back, so they are dropped and each thread runs a short
-//      window of the recurrence;
+//   2. the chamfer distance from each post to the nearest post with data (DataDistances), with
+//      every post relaxed from the same neighbors in the same order as the reference's rows top
+//      down then bottom up, so every distance (and carried value) has its float bits; values
+//      beyond the reach are never read back, so each tile of the lattice is run in a window of
+//      its own, one warp per tile;
 //   3a. Feather: gap posts within `width` take the carried difference faded by a smoothstep;
 //   3b. Height / Slope: gap posts within the reach (3 decay lengths, away from the lattice's 3
 //      border posts) are solved for (-Laplacian + 1/L^2) d = 0, or its square, with the band's
@@ -42,272 +42,436 @@ namespace {
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kBandPosts = 3;     // seam_field.cpp:29
 constexpr int kBorderPosts = 3;   // seam_field.cpp:32
-constexpr int kSegment = 32;      // cells of a row a thread of the distance passes writes
 constexpr int kMaxLevels = 8;
-constexpr size_t kTileSharedBytes = 200 * 1024;  // a distance window's shared memory at most
+constexpr size_t kRowSharedBytes = 200 * 1024;   // a distance block's rows in shared memory
+constexpr size_t kScratchBytes = size_t(1) << 30;  // the distance warps' stored steps at most
 
-// --- band and fixed values ---------------------------------------------------------------
+// --- the band, in bits ------------------------------------------------------------------------
+//
+// The prepare passes keep the lattice's masks one bit per post: word j of row r holds columns
+// 32 j .. 32 j + 31 (bit = column % 32), `pitch` = ceil(w / 32) words a row, the bits past the
+// last column 0.
 
-__global__ void count_data_kernel(const uint8_t* __restrict__ data, size_t n,
-                                  unsigned long long* __restrict__ count) {
-    unsigned long long mine = 0;
-    for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
-         k += size_t(gridDim.x) * blockDim.x) {
-        mine += data[k] != 0 ? 1u : 0u;
+constexpr int kBandRows = 64;  // rows of a band warp's span
+
+__device__ __forceinline__ uint32_t row_tail_mask(uint32_t j, uint32_t pitch, uint32_t w) {
+    return j + 1 == pitch && (w & 31u) != 0 ? (1u << (w & 31u)) - 1u : 0xffffffffu;
+}
+
+// Which posts have data, one bit each, and how many have.
+__global__ void pack_data_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
+                                 uint32_t pitch, uint32_t* __restrict__ bits,
+                                 unsigned long long* __restrict__ count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const size_t words = size_t(pitch) * h;
+    const size_t warps = size_t(gridDim.x) * (blockDim.x >> 5);
+    uint32_t mine = 0;
+    for (size_t q = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; q < words; q += warps) {
+        const uint32_t row = uint32_t(q / pitch), col = uint32_t(q % pitch) * 32u + lane;
+        const bool has = col < w && data[size_t(row) * w + col] != 0;
+        const uint32_t word = __ballot_sync(0xffffffffu, has);
+        if (lane == 0) {
+            bits[q] = word;
+            mine += __popc(word);
+        }
     }
-    for (int d = 16; d > 0; d >>= 1) {
-        mine += __shfl_down_sync(0xffffffffu, mine, d);
-    }
-    if ((threadIdx.x & 31u) == 0 && mine > 0) {
-        atomicAdd(count, mine);
+    if (lane == 0 && mine != 0) {
+        atomicAdd(count, static_cast<unsigned long long>(mine));
     }
 }
 
-// NearGaps (seam_field.cpp:117): 1 where a post without data lies within `radius` columns...
-__global__ void gaps_across_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
-                                   int radius, uint8_t* __restrict__ across) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= size_t(w) * h) {
-        return;
-    }
-    const int col = int(k % w);
-    const size_t row0 = k - size_t(col);
-    uint8_t any = 0;
-    for (int c = max(0, col - radius); c <= min(int(w) - 1, col + radius); ++c) {
-        any |= data[row0 + size_t(c)] == 0 ? 1 : 0;
-    }
-    across[k] = any;
-}
+struct BandBits {
+    const uint32_t* bits;
+    const float* difference;
+    float* field;
+    uint32_t* tileCounts;  // posts with data per distance tile
+    uint32_t w, h, pitch;
+    int ts;
+    uint32_t tilesX;
+};
 
-// ... then of those within `radius` rows; the posts with data there hold their difference.
-__global__ void band_kernel(const uint8_t* __restrict__ data, const float* __restrict__ difference,
-                            const uint8_t* __restrict__ across, uint32_t w, uint32_t h,
-                            int radius, float* __restrict__ field) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= size_t(w) * h) {
+// NearGaps (seam_field.cpp:117) and the band's values: a post with data keeps its difference
+// where a post without data lies within 3 columns and 3 rows of it; every other post is 0. A
+// warp takes 32 words across (lane = word) and kBandRows rows down, dilating each row's gap bits
+// by 3 columns with funnel shifts and OR-ing the last 7 rows as it goes; the field is written a
+// row of 32 posts at a time. The posts with data are counted per distance tile on the way.
+__global__ void band_bits_kernel(const BandBits p) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t spans = (p.pitch + 31u) / 32u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t j0 = (warp % spans) * 32u, j = j0 + lane;
+    const int q0 = int(warp / spans) * kBandRows;
+    if (q0 >= int(p.h)) {
         return;
     }
-    const int row = int(k / w);
-    const size_t col = k % w;
-    uint8_t near = 0;
-    for (int r = max(0, row - radius); r <= min(int(h) - 1, row + radius); ++r) {
-        near |= across[size_t(r) * w + col];
+    const int q1 = min(int(p.h), q0 + kBandRows);
+    const bool inWord = j < p.pitch;
+    const uint32_t valid = inWord ? row_tail_mask(j, p.pitch, p.w) : 0u;
+    auto word_at = [&](int q, uint32_t jj) -> uint32_t {
+        return p.bits[size_t(q) * p.pitch + jj];
+    };
+    uint32_t near[7] = {0, 0, 0, 0, 0, 0, 0};  // dilated gaps of rows q-6 .. q
+    uint32_t has[4] = {0, 0, 0, 0};             // data bits of rows q-3 .. q
+    uint32_t counted = 0;
+    int countRow = q0;
+    for (int q = q0 - kBandPosts; q < q1 + kBandPosts; ++q) {
+        const bool rowIn = q >= 0 && q < int(p.h);
+        const uint32_t d = rowIn && inWord ? word_at(q, j) : 0u;
+        const uint32_t g = rowIn ? ~d & valid : 0u;
+        uint32_t gl = __shfl_up_sync(0xffffffffu, g, 1);
+        uint32_t gr = __shfl_down_sync(0xffffffffu, g, 1);
+        if (lane == 0) {
+            gl = rowIn && j0 > 0 ? ~word_at(q, j0 - 1) : 0u;
+        }
+        if (lane == 31) {
+            gr = rowIn && j + 1 < p.pitch ? ~word_at(q, j + 1) & row_tail_mask(j + 1, p.pitch, p.w)
+                                          : 0u;
+        }
+        uint32_t dil = g;
+#pragma unroll
+        for (int s = 1; s <= kBandPosts; ++s) {
+            dil |= __funnelshift_l(gl, g, s) | __funnelshift_r(g, gr, s);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            near[k] = near[k + 1];
+        }
+        near[6] = dil;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            has[k] = has[k + 1];
+        }
+        has[3] = d;
+        const int c = q - kBandPosts;  // the row whose 7 rows of gaps are in
+        if (c < q0) {
+            continue;
+        }
+        const uint32_t band =
+            has[0] & (near[0] | near[1] | near[2] | near[3] | near[4] | near[5] | near[6]);
+        if (p.tileCounts != nullptr) {
+            if (c / p.ts != countRow / p.ts) {
+                if (counted != 0) {
+                    atomicAdd(&p.tileCounts[uint32_t(countRow / p.ts) * p.tilesX + j * 32u / p.ts],
+                              counted);
+                }
+                counted = 0;
+                countRow = c;
+            }
+            counted += __popc(has[0]);
+        }
+        const size_t base = size_t(c) * p.w;
+        for (int k = 0; k < 32; ++k) {
+            const uint32_t b = __shfl_sync(0xffffffffu, band, k);
+            const uint32_t col = (j0 + uint32_t(k)) * 32u + lane;
+            if (col < p.w) {
+                float v = 0.0f;
+                if ((b >> lane) & 1u) {
+                    v = p.difference[base + col];
+                    v = isnan(v) ? 0.0f : v;
+                }
+                p.field[base + col] = v;
+            }
+        }
     }
-    const float d = difference[k];
-    field[k] = data[k] != 0 && near != 0 && !isnan(d) ? d : 0.0f;
+    if (p.tileCounts != nullptr && counted != 0) {
+        atomicAdd(&p.tileCounts[uint32_t(countRow / p.ts) * p.tilesX + j * 32u / p.ts], counted);
+    }
 }
 
 // --- distances (DataDistances, seam_field.cpp:151) -----------------------------------------
-
-struct DistanceRow {
-    const uint8_t* data;
-    const float* field;    // the carried value of a post with data (Feather)
-    float* distance;       // forward pass output, backward pass input
-    float* carried;        // optional, as distance
-    float* distanceOut;    // backward pass output
-    float* carriedOut;
-    uint32_t w, h;
-    float dx, dy, diagonal;
-    float cap;       // distances above it are dropped (+inf): they are never read back
-    int window;      // cells of recurrence before a thread's segment
-};
-
-// The forward pass over row `row`: each post without data relaxes from its left neighbor, then
-// the posts above, up-left and up-right (strictly smaller wins, in that order), the row above
-// already final. Each thread writes kSegment posts, running the recurrence along the row from
-// `window` posts before them.
-__global__ void distance_forward_kernel(const DistanceRow p, uint32_t row) {
-    const int c0 = int(blockIdx.x * blockDim.x + threadIdx.x) * kSegment;
-    if (c0 >= int(p.w)) {
-        return;
-    }
-    const int w = int(p.w);
-    const size_t base = size_t(row) * p.w;
-    const float inf = INFINITY;
-    float left = inf, leftCarried = 0.0f;
-    const int end = min(w, c0 + kSegment);
-    for (int c = max(0, c0 - p.window); c < end; ++c) {
-        const size_t k = base + size_t(c);
-        float d, carried = p.data[k] != 0 && p.carried != nullptr ? p.field[k] : 0.0f;
-        if (p.data[k] != 0) {
-            d = 0.0f;
-        } else {
-            d = inf;
-            if (c > 0) {
-                const float t = left + p.dx;
-                if (t < d) {
-                    d = t;
-                    carried = leftCarried;
-                }
-            }
-            if (row > 0) {
-                const size_t up = k - p.w;
-                float t = p.distance[up] + p.dy;
-                if (t < d) {
-                    d = t;
-                    if (p.carried) carried = p.carried[up];
-                }
-                if (c > 0) {
-                    t = p.distance[up - 1] + p.diagonal;
-                    if (t < d) {
-                        d = t;
-                        if (p.carried) carried = p.carried[up - 1];
-                    }
-                }
-                if (c + 1 < w) {
-                    t = p.distance[up + 1] + p.diagonal;
-                    if (t < d) {
-                        d = t;
-                        if (p.carried) carried = p.carried[up + 1];
-                    }
-                }
-            }
-            if (d > p.cap) {
-                d = inf;
-            }
-        }
-        if (c >= c0) {
-            p.distance[k] = d;
-            if (p.carried) {
-                p.carried[k] = carried;
-            }
-        }
-        left = d;
-        leftCarried = carried;
-    }
-}
-
-// The backward pass over row `row`, right to left: a post without data keeps its forward value
-// unless its right neighbor, then the posts below, down-right and down-left give a strictly
-// smaller one. Forward values are read from `distance`, the rows below from `distanceOut`.
-__global__ void distance_backward_kernel(const DistanceRow p, uint32_t row) {
-    const int w = int(p.w);
-    const int segment = int(blockIdx.x * blockDim.x + threadIdx.x);
-    const int hi = w - 1 - segment * kSegment;  // this thread writes [lo, hi]
-    if (hi < 0) {
-        return;
-    }
-    const int lo = max(0, hi - kSegment + 1);
-    const size_t base = size_t(row) * p.w;
-    const float inf = INFINITY;
-    float right = inf, rightCarried = 0.0f;
-    for (int c = min(w - 1, hi + p.window); c >= lo; --c) {
-        const size_t k = base + size_t(c);
-        float d = p.distance[k];
-        float carried = p.carried != nullptr ? p.carried[k] : 0.0f;
-        if (p.data[k] == 0) {
-            if (c + 1 < w) {
-                const float t = right + p.dx;
-                if (t < d) {
-                    d = t;
-                    carried = rightCarried;
-                }
-            }
-            if (row + 1 < p.h) {
-                const size_t down = k + p.w;
-                float t = p.distanceOut[down] + p.dy;
-                if (t < d) {
-                    d = t;
-                    if (p.carried) carried = p.carriedOut[down];
-                }
-                if (c + 1 < w) {
-                    t = p.distanceOut[down + 1] + p.diagonal;
-                    if (t < d) {
-                        d = t;
-                        if (p.carried) carried = p.carriedOut[down + 1];
-                    }
-                }
-                if (c > 0) {
-                    t = p.distanceOut[down - 1] + p.diagonal;
-                    if (t < d) {
-                        d = t;
-                        if (p.carried) carried = p.carriedOut[down - 1];
-                    }
-                }
-            }
-            if (d > p.cap) {
-                d = inf;
-            }
-        }
-        if (c <= hi) {
-            p.distanceOut[k] = d;
-            if (p.carried) {
-                p.carriedOut[k] = carried;
-            }
-        }
-        right = d;
-        rightCarried = carried;
-    }
-}
-
-// --- distances by tiles ---------------------------------------------------------------------
 //
 // A distance at most `cap` comes from a path of steps that each add at least dx (a step across
 // columns) or dy (across rows), so it reaches no further than cap / dx columns and cap / dy rows:
 // both passes, run over a window that holds a tile plus a halo of mx = cap / dx + 2 columns and
 // my = cap / dy + 2 rows (clipped to the lattice, whose edges the reference's passes start from
 // too) and started from no distance outside it, give every post of the tile the reference's
-// distance and carried value wherever the distance is at most `cap`. Larger values are never
-// read back, so they are written as +inf. Inside a window the passes run as wavefronts: the
-// forward pass reads the left, upper-left, upper and upper-right posts, all on earlier fronts
-// 2 row + col, and the backward pass mirrors it, so every post sees the same operands, in the
-// same order, as in the row-by-row relaxation.
+// distance and carried value wherever the distance is at most `cap`; larger values are never
+// read back. Only tiles that hold a post without data and see a post with data within their halo
+// are computed.
 //
-// Only tiles that hold a post without data and see a post with data within their halo are
-// computed; distance_init_kernel gives every other post its value (0 with data, +inf without).
+// One warp runs a tile's window. The forward pass reads the left, upper-left, upper and
+// upper-right posts: the warp takes the window's rows 32 at a time (lane = row), lane l at column
+// t - 2 l on step t, so the row above has just passed the three columns a post reads, and they
+// come across by shuffles (lane 0 reads the band above from a row in shared memory, which lane 31
+// writes as it goes). The backward pass mirrors it from the bottom right, starting from the
+// forward values, which the forward pass stores per step as 32 lanes (coalesced both ways: the
+// backward step reads one stored step of the forward pass, lanes reversed). Every post sees the
+// same operands in the same order as in the reference's row-by-row relaxation, so distances and
+// carried values have its float bits. The backward pass stops at the tile's first row (a row
+// reads only the rows below it). Each tile post's result goes straight out: its unknown bit
+// (Height, Slope) or its Feather value.
 
-struct DistanceTiles {
-    const uint8_t* data;
-    const float* field;  // the carried value of a post with data, or null (no carried values)
-    float* distance;
-    float* carried;
-    uint32_t w, h;
-    float dx, dy, diagonal, cap;
-    int ts;              // tile side
-    int mx, my;          // halo columns and rows
-    int maxPosts;        // posts of the largest window
-    uint32_t tilesX, tilesY;
+struct DistanceWarps {
+    const uint32_t* bits;  // data bits
+    const float* field;    // the carried value of a post with data (Feather), or null
+    uint32_t w, h, pitch;
+    float dx, dy, diagonal;
+    int ts;                // tile side, a multiple of 32
+    int mx, my;            // halo columns and rows
+    int rowFloats;         // floats of a warp's row in shared memory (or in `rows`)
+    uint32_t tilesX;
     const uint32_t* list;
     const uint32_t* count;
+    float* scratch;        // per warp slot: the forward pass's stored steps (then carried)
+    size_t scratchFloats;  // per warp slot
+    float* rows;           // per warp slot, when the rows are not in shared memory
+    uint32_t slots;        // warps of the launch
+    // Height / Slope: the unknowns (no data, 3 posts off the border, distance within `reach`).
+    uint32_t* unknown;
+    double reach;
+    // Feather: gap posts within `width` take the carried difference faded by a smoothstep.
+    float* feather;
+    double width;
 };
 
-__global__ void distance_init_kernel(const uint8_t* __restrict__ data,
-                                     const float* __restrict__ field, size_t n,
-                                     float* __restrict__ distance, float* __restrict__ carried) {
-    for (size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n;
-         k += size_t(gridDim.x) * blockDim.x) {
-        const bool has = data[k] != 0;
-        distance[k] = has ? 0.0f : INFINITY;
-        if (carried != nullptr) {
-            carried[k] = has ? field[k] : 0.0f;
-        }
-    }
-}
+constexpr int kDistanceWarps = 4;  // warps of a distance block
 
-// Posts with data per tile (one block per tile).
-__global__ void tile_counts_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
-                                   int ts, uint32_t tilesX, uint32_t* __restrict__ counts) {
-    const uint32_t tile = blockIdx.x;
-    const uint32_t r0 = (tile / tilesX) * uint32_t(ts), c0 = (tile % tilesX) * uint32_t(ts);
-    const uint32_t rows = min(uint32_t(ts), h - r0), cols = min(uint32_t(ts), w - c0);
-    uint32_t mine = 0;
-    for (uint32_t i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-        mine += data[size_t(r0 + i / cols) * w + c0 + i % cols] != 0 ? 1u : 0u;
+template <bool kCarried, bool kSharedRows>
+__global__ void __launch_bounds__(32 * kDistanceWarps)
+    distance_warp_kernel(const DistanceWarps p) {
+    extern __shared__ float smem[];
+    const int lane = int(threadIdx.x & 31u), warp = int(threadIdx.x >> 5);
+    const uint32_t slot = blockIdx.x * kDistanceWarps + uint32_t(warp);
+    if (slot >= p.slots) {
+        return;
     }
-    for (int d = 16; d > 0; d >>= 1) {
-        mine += __shfl_down_sync(0xffffffffu, mine, d);
-    }
-    __shared__ uint32_t warps[32];
-    if ((threadIdx.x & 31u) == 0) {
-        warps[threadIdx.x >> 5] = mine;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t total = 0;
-        for (uint32_t i = 0; i < (blockDim.x + 31) / 32; ++i) {
-            total += warps[i];
+    float* rowF = kSharedRows ? smem + size_t(warp) * p.rowFloats * (kCarried ? 2 : 1)
+                              : p.rows + size_t(slot) * p.rowFloats * (kCarried ? 2 : 1);
+    float* rowC = rowF + p.rowFloats;
+    float* store = p.scratch + size_t(slot) * p.scratchFloats;
+    const float inf = INFINITY;
+    const uint32_t total = *p.count;
+    for (uint32_t item = slot; item < total; item += p.slots) {
+        const uint32_t tile = p.list[item];
+        const int r0 = int(tile / p.tilesX) * p.ts, c0 = int(tile % p.tilesX) * p.ts;
+        const int rw0 = max(0, r0 - p.my), rw1 = min(int(p.h), r0 + p.ts + p.my);
+        const int cw0 = max(0, c0 - p.mx), cw1 = min(int(p.w), c0 + p.ts + p.mx);
+        const int ww = cw1 - cw0, steps = ww + 62;
+        const int bandsAbove = (r0 - rw0 + 31) / 32, bandsBelow = (rw1 - r0 + 31) / 32;
+        const int tr1 = min(int(p.h), r0 + p.ts), tc1 = min(int(p.w), c0 + p.ts);
+        float* storeC = store + size_t(bandsBelow) * steps * 32;
+        for (int c = lane; c < ww; c += 32) {
+            rowF[c] = inf;
+            if (kCarried) rowC[c] = 0.0f;
         }
-        counts[tile] = total;
+        __syncwarp();
+        // Forward, bands top down.
+        for (int band = -bandsAbove; band < bandsBelow; ++band) {
+            const int row = r0 + 32 * band + lane;
+            const bool active = row >= rw0 && row < rw1;
+            const size_t rowBits = size_t(active ? row : rw0) * p.pitch;
+            float h1 = inf, h2 = inf, h3 = inf;
+            float g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
+            uint32_t word = 0, next = 0;
+            if (active) {
+                word = p.bits[rowBits + uint32_t(cw0 >> 5)];
+                next = (cw0 >> 5) + 1 < int(p.pitch) ? p.bits[rowBits + uint32_t(cw0 >> 5) + 1]
+                                                     : 0u;
+            }
+            // Lane 0's row above: columns c - 1, c, c + 1 and the next one.
+            float aL = inf, aU = inf, aR = lane == 0 && ww > 0 ? rowF[0] : inf;
+            float bL = 0.0f, bU = 0.0f, bR = kCarried && lane == 0 && ww > 0 ? rowC[0] : 0.0f;
+            float* out = store + size_t(max(band, 0)) * steps * 32;
+            float* outC = storeC + size_t(max(band, 0)) * steps * 32;
+            for (int t = 0; t < steps; ++t) {
+                const int c = t - 2 * lane;
+                float uR = __shfl_up_sync(0xffffffffu, h1, 1);
+                float uU = __shfl_up_sync(0xffffffffu, h2, 1);
+                float uL = __shfl_up_sync(0xffffffffu, h3, 1);
+                float vR = 0.0f, vU = 0.0f, vL = 0.0f;
+                if (kCarried) {
+                    vR = __shfl_up_sync(0xffffffffu, g1, 1);
+                    vU = __shfl_up_sync(0xffffffffu, g2, 1);
+                    vL = __shfl_up_sync(0xffffffffu, g3, 1);
+                }
+                if (lane == 0) {
+                    aL = aU;
+                    aU = aR;
+                    aR = c + 1 < ww ? rowF[c + 1] : inf;
+                    uL = aL;
+                    uU = aU;
+                    uR = aR;
+                    if (kCarried) {
+                        bL = bU;
+                        bU = bR;
+                        bR = c + 1 < ww ? rowC[c + 1] : 0.0f;
+                        vL = bL;
+                        vU = bU;
+                        vR = bR;
+                    }
+                }
+                float d = inf, car = 0.0f;
+                if (active && c >= 0 && c < ww) {
+                    const int x = cw0 + c;
+                    if ((x & 31) == 0 && c > 0) {
+                        word = next;
+                        next = (x >> 5) + 1 < int(p.pitch) ? p.bits[rowBits + uint32_t(x >> 5) + 1]
+                                                           : 0u;
+                    }
+                    if ((word >> (x & 31)) & 1u) {
+                        d = 0.0f;
+                        if (kCarried) car = p.field[size_t(row) * p.w + uint32_t(x)];
+                    } else {
+                        float s = h1 + p.dx;
+                        if (s < d) {
+                            d = s;
+                            car = g1;
+                        }
+                        s = uU + p.dy;
+                        if (s < d) {
+                            d = s;
+                            car = vU;
+                        }
+                        s = uL + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            car = vL;
+                        }
+                        s = uR + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            car = vR;
+                        }
+                    }
+                    if (lane == 31) {
+                        rowF[c] = d;
+                        if (kCarried) rowC[c] = car;
+                    }
+                }
+                h3 = h2;
+                h2 = h1;
+                h1 = d;
+                if (kCarried) {
+                    g3 = g2;
+                    g2 = g1;
+                    g1 = car;
+                }
+                if (band >= 0) {
+                    out[size_t(t) * 32 + lane] = d;
+                    if (kCarried) outC[size_t(t) * 32 + lane] = car;
+                }
+            }
+            __syncwarp();
+        }
+        // Backward, bands bottom up over the tile's rows and the halo below; lane 0 is a band's
+        // lowest row.
+        for (int c = lane; c < ww; c += 32) {
+            rowF[c] = inf;
+            if (kCarried) rowC[c] = 0.0f;
+        }
+        __syncwarp();
+        for (int band = bandsBelow - 1; band >= 0; --band) {
+            const int row = r0 + 32 * band + 31 - lane;
+            const bool active = row < rw1;
+            const size_t rowBits = size_t(active ? row : r0) * p.pitch;
+            float h1 = inf, h2 = inf, h3 = inf;
+            float g1 = 0.0f, g2 = 0.0f, g3 = 0.0f;
+            uint32_t word = 0, next = 0, unknownBits = 0;
+            const int last = cw1 - 1;
+            if (active) {
+                word = p.bits[rowBits + uint32_t(last >> 5)];
+                next = (last >> 5) > 0 ? p.bits[rowBits + uint32_t(last >> 5) - 1] : 0u;
+            }
+            float aL = lane == 0 && ww > 0 ? rowF[ww - 1] : inf, aU = inf, aR = inf;
+            float bL = kCarried && lane == 0 && ww > 0 ? rowC[ww - 1] : 0.0f, bU = 0.0f, bR = 0.0f;
+            const float* in = store + size_t(band) * steps * 32;
+            const float* inC = storeC + size_t(band) * steps * 32;
+            const bool tileRow = active && row < tr1;
+            for (int t = 0; t < steps; ++t) {
+                const int c = ww - 1 - t + 2 * lane;
+                float dL = __shfl_up_sync(0xffffffffu, h1, 1);
+                float dD = __shfl_up_sync(0xffffffffu, h2, 1);
+                float dR = __shfl_up_sync(0xffffffffu, h3, 1);
+                float eL = 0.0f, eD = 0.0f, eR = 0.0f;
+                if (kCarried) {
+                    eL = __shfl_up_sync(0xffffffffu, g1, 1);
+                    eD = __shfl_up_sync(0xffffffffu, g2, 1);
+                    eR = __shfl_up_sync(0xffffffffu, g3, 1);
+                }
+                if (lane == 0) {
+                    aR = aU;
+                    aU = aL;
+                    aL = c - 1 >= 0 ? rowF[c - 1] : inf;
+                    dL = aL;
+                    dD = aU;
+                    dR = aR;
+                    if (kCarried) {
+                        bR = bU;
+                        bU = bL;
+                        bL = c - 1 >= 0 ? rowC[c - 1] : 0.0f;
+                        eL = bL;
+                        eD = bU;
+                        eR = bR;
+                    }
+                }
+                const size_t stored = size_t(ww + 61 - t) * 32 + uint32_t(31 - lane);
+                float d = inf, car = 0.0f;
+                if (active && c >= 0 && c < ww) {
+                    const int x = cw0 + c;
+                    if ((x & 31) == 31 && c < ww - 1) {
+                        word = next;
+                        next = (x >> 5) > 0 ? p.bits[rowBits + uint32_t(x >> 5) - 1] : 0u;
+                    }
+                    d = in[stored];
+                    if (kCarried) car = inC[stored];
+                    const bool has = (word >> (x & 31)) & 1u;
+                    if (!has) {
+                        float s = h1 + p.dx;
+                        if (s < d) {
+                            d = s;
+                            car = g1;
+                        }
+                        s = dD + p.dy;
+                        if (s < d) {
+                            d = s;
+                            car = eD;
+                        }
+                        s = dR + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            car = eR;
+                        }
+                        s = dL + p.diagonal;
+                        if (s < d) {
+                            d = s;
+                            car = eL;
+                        }
+                    }
+                    if (lane == 31) {
+                        rowF[c] = d;
+                        if (kCarried) rowC[c] = car;
+                    }
+                    if (tileRow && x >= c0 && x < tc1) {
+                        if (p.unknown != nullptr) {
+                            const bool inside = x >= kBorderPosts && x + kBorderPosts < int(p.w) &&
+                                                row >= kBorderPosts &&
+                                                row + kBorderPosts < int(p.h);
+                            if (!has && inside && double(d) <= p.reach) {
+                                unknownBits |= 1u << (x & 31);
+                            }
+                            if ((x & 31) == 0) {
+                                p.unknown[rowBits + uint32_t(x >> 5)] = unknownBits;
+                                unknownBits = 0;
+                            }
+                        } else if (!has && double(d) < p.width) {
+                            const double u = double(d) / p.width;
+                            const double weight = 1.0 - u * u * (3.0 - 2.0 * u);
+                            p.feather[size_t(row) * p.w + uint32_t(x)] =
+                                float(weight * double(car));
+                        }
+                    }
+                }
+                h3 = h2;
+                h2 = h1;
+                h1 = d;
+                if (kCarried) {
+                    g3 = g2;
+                    g2 = g1;
+                    g1 = car;
+                }
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -340,231 +504,54 @@ __global__ void active_tiles_kernel(const uint32_t* __restrict__ counts, uint32_
     }
 }
 
-// Posts of the largest window of a tile of side `ts` on a w x h lattice, and the shared memory
-// it takes.
-size_t tile_window_posts(int ts, int mx, int my, uint32_t w, uint32_t h) {
-    return std::min<size_t>(size_t(ts) + 2 * size_t(my), h) *
-           std::min<size_t>(size_t(ts) + 2 * size_t(mx), w);
-}
-
-size_t tile_window_bytes(size_t posts, bool carried) {
-    return posts * (carried ? 8 : 4) + ((posts + 31) / 32) * 4;
-}
-
-// One block per listed tile, blocks looping over the list.
-__global__ void __launch_bounds__(128) distance_tile_kernel(const DistanceTiles p) {
-    extern __shared__ float smem[];
-    const uint32_t total = *p.count;
-    const int maxPosts = p.maxPosts;
-    float* F = smem;
-    float* Cc = p.carried != nullptr ? smem + maxPosts : nullptr;
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + (p.carried != nullptr ? 2 : 1) * maxPosts);
-    const int tid = int(threadIdx.x), lane = tid & 31, warp = tid >> 5, warps = blockDim.x >> 5;
-    for (uint32_t item = blockIdx.x; item < total; item += gridDim.x) {
-        const uint32_t tile = p.list[item];
-        const int r0 = int(tile / p.tilesX) * p.ts, c0 = int(tile % p.tilesX) * p.ts;
-        const int rw0 = max(0, r0 - p.my), rw1 = min(int(p.h), r0 + p.ts + p.my);
-        const int cw0 = max(0, c0 - p.mx), cw1 = min(int(p.w), c0 + p.ts + p.mx);
-        const int hw = rw1 - rw0, ww = cw1 - cw0, posts = hw * ww;
-        // Which window posts have data, one bit each.
-        for (int base = warp * 32; base < posts; base += warps * 32) {
-            const int i = base + lane;
-            const bool has = i < posts &&
-                             p.data[size_t(rw0 + i / ww) * p.w + size_t(cw0 + i % ww)] != 0;
-            const uint32_t word = __ballot_sync(0xffffffffu, has);
-            if (lane == 0) {
-                bits[base >> 5] = word;
-            }
-        }
-        __syncthreads();
-        const int fronts = 2 * (hw - 1) + ww;
-        // Forward: front t holds the posts with 2 row + col = t.
-        for (int t = 0; t < fronts; ++t) {
-            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hw - 1, t / 2);
-            for (int r = rlo + tid; r <= rhi; r += int(blockDim.x)) {
-                const int c = t - 2 * r, k = r * ww + c;
-                if ((bits[k >> 5] >> (k & 31)) & 1u) {
-                    F[k] = 0.0f;
-                    if (Cc) {
-                        Cc[k] = p.field[size_t(rw0 + r) * p.w + size_t(cw0 + c)];
-                    }
-                    continue;
-                }
-                float d = INFINITY, carried = 0.0f;
-                if (c > 0) {
-                    const float s = F[k - 1] + p.dx;
-                    if (s < d) {
-                        d = s;
-                        if (Cc) carried = Cc[k - 1];
-                    }
-                }
-                if (r > 0) {
-                    const int up = k - ww;
-                    float s = F[up] + p.dy;
-                    if (s < d) {
-                        d = s;
-                        if (Cc) carried = Cc[up];
-                    }
-                    if (c > 0) {
-                        s = F[up - 1] + p.diagonal;
-                        if (s < d) {
-                            d = s;
-                            if (Cc) carried = Cc[up - 1];
-                        }
-                    }
-                    if (c + 1 < ww) {
-                        s = F[up + 1] + p.diagonal;
-                        if (s < d) {
-                            d = s;
-                            if (Cc) carried = Cc[up + 1];
-                        }
-                    }
-                }
-                F[k] = d;
-                if (Cc) {
-                    Cc[k] = carried;
-                }
-            }
-            __syncthreads();
-        }
-        // Backward, in place: front t holds the posts with 2 (hw-1-row) + (ww-1-col) = t. A row
-        // reads only the rows below it, so the pass stops at the tile's first row.
-        const int hb = hw - (r0 - rw0);
-        const int backFronts = 2 * (hb - 1) + ww;
-        for (int t = 0; t < backFronts; ++t) {
-            const int rlo = t >= ww ? (t - ww + 2) / 2 : 0, rhi = min(hb - 1, t / 2);
-            for (int q = rlo + tid; q <= rhi; q += int(blockDim.x)) {
-                const int r = hw - 1 - q, c = ww - 1 - (t - 2 * q), k = r * ww + c;
-                if ((bits[k >> 5] >> (k & 31)) & 1u) {
-                    continue;
-                }
-                float d = F[k];
-                float carried = Cc ? Cc[k] : 0.0f;
-                if (c + 1 < ww) {
-                    const float s = F[k + 1] + p.dx;
-                    if (s < d) {
-                        d = s;
-                        if (Cc) carried = Cc[k + 1];
-                    }
-                }
-                if (r + 1 < hw) {
-                    const int down = k + ww;
-                    float s = F[down] + p.dy;
-                    if (s < d) {
-                        d = s;
-                        if (Cc) carried = Cc[down];
-                    }
-                    if (c + 1 < ww) {
-                        s = F[down + 1] + p.diagonal;
-                        if (s < d) {
-                            d = s;
-                            if (Cc) carried = Cc[down + 1];
-                        }
-                    }
-                    if (c > 0) {
-                        s = F[down - 1] + p.diagonal;
-                        if (s < d) {
-                            d = s;
-                            if (Cc) carried = Cc[down - 1];
-                        }
-                    }
-                }
-                F[k] = d;
-                if (Cc) {
-                    Cc[k] = carried;
-                }
-            }
-            __syncthreads();
-        }
-        // The tile's posts without data.
-        const int rows = min(p.ts, int(p.h) - r0), cols = min(p.ts, int(p.w) - c0);
-        for (int i = tid; i < rows * cols; i += int(blockDim.x)) {
-            const int r = r0 + i / cols - rw0, c = c0 + i % cols - cw0, k = r * ww + c;
-            if ((bits[k >> 5] >> (k & 31)) & 1u) {
-                continue;
-            }
-            const size_t g = size_t(rw0 + r) * p.w + size_t(cw0 + c);
-            const float d = F[k];
-            p.distance[g] = d <= p.cap ? d : INFINITY;
-            if (Cc) {
-                p.carried[g] = Cc[k];
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// Feather (seam_field.cpp:218): gap posts within `width` take the carried difference, faded by a
-// smoothstep from 1 at the edge to 0 at `width`.
-__global__ void feather_kernel(const uint8_t* __restrict__ data,
-                               const float* __restrict__ distance,
-                               const float* __restrict__ carried, size_t n, double width,
-                               float* __restrict__ field) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= n || data[k] != 0 || !(distance[k] < width)) {
-        return;
-    }
-    const double t = double(distance[k]) / width;
-    const double weight = 1.0 - t * t * (3.0 - 2.0 * t);
-    field[k] = float(weight * double(carried[k]));
-}
-
 // --- unknowns and the level hierarchy ------------------------------------------------------
-
-// 1 at the posts solved for: no data, off the border, within the reach.
-__global__ void unknown_kernel(const uint8_t* __restrict__ data,
-                               const float* __restrict__ distance, uint32_t w, uint32_t h,
-                               double reach, uint32_t* __restrict__ flags) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= size_t(w) * h) {
-        return;
-    }
-    const uint32_t col = uint32_t(k % w), row = uint32_t(k / w);
-    const bool inside = col >= uint32_t(kBorderPosts) && col + kBorderPosts < w &&
-                        row >= uint32_t(kBorderPosts) && row + kBorderPosts < h;
-    flags[k] = data[k] == 0 && inside && double(distance[k]) <= reach ? 1u : 0u;
-}
+//
+// A level's unknowns are a bit mask over its lattice; the compact index of an unknown is the
+// count of unknowns before its word (an exclusive scan of the words' counts) plus those before
+// it in the word.
 
 // A coarser level's posts: the parents (col / 2, row / 2) of the finer level's unknowns.
 __global__ void coarsen_kernel(const uint32_t* __restrict__ finePos, uint32_t n, uint32_t fineW,
-                               uint32_t coarseW, uint32_t* __restrict__ coarseFlags) {
+                               uint32_t coarsePitch, uint32_t* __restrict__ coarseMask) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) {
         return;
     }
     const uint32_t p = finePos[k];
-    coarseFlags[size_t(p / fineW / 2) * coarseW + (p % fineW) / 2] = 1u;
+    const uint32_t col = (p % fineW) / 2, row = p / fineW / 2;
+    atomicOr(&coarseMask[size_t(row) * coarsePitch + (col >> 5)], 1u << (col & 31u));
 }
 
-// Flags (0 / 1) scanned in place into offsets: the compact index of each flagged post, its
-// position, and ~0u at the others. `scanned` holds the exclusive scan, `flags` the marks.
-__global__ void compact_kernel(const uint32_t* __restrict__ scanned,
-                               const uint8_t* __restrict__ marks, size_t n,
-                               uint32_t* __restrict__ index, uint32_t* __restrict__ position) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= n) {
+__global__ void word_counts_kernel(const uint32_t* __restrict__ mask, size_t words,
+                                   uint32_t* __restrict__ counts) {
+    const size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q < words) {
+        counts[q] = __popc(mask[q]);
+    }
+}
+
+// Each unknown's post, from its word's offset.
+__global__ void positions_kernel(const uint32_t* __restrict__ mask,
+                                 const uint32_t* __restrict__ offsets, size_t words,
+                                 uint32_t pitch, uint32_t w, uint32_t* __restrict__ position) {
+    const size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= words) {
         return;
     }
-    if (marks[k] != 0) {
-        position[scanned[k]] = uint32_t(k);
-        index[k] = scanned[k];
-    } else {
-        index[k] = kNone;
-    }
-}
-
-__global__ void flags_to_marks_kernel(const uint32_t* __restrict__ flags, size_t n,
-                                      uint8_t* __restrict__ marks) {
-    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k < n) {
-        marks[k] = flags[k] != 0 ? 1 : 0;
+    uint32_t m = mask[q];
+    uint32_t at = offsets[q];
+    const uint32_t base = uint32_t(q / pitch) * w + uint32_t(q % pitch) * 32u;
+    while (m != 0) {
+        position[at++] = base + uint32_t(__ffs(int(m)) - 1);
+        m &= m - 1u;
     }
 }
 
 // One level: its lattice, its unknowns and the operator's weights.
 struct LevelView {
-    uint32_t w, h, n;
-    const uint32_t* index;     // [w * h] compact index or ~0u
+    uint32_t w, h, n, pitch;
+    const uint32_t* mask;      // [pitch * h] 1 at the unknowns
+    const uint32_t* offsets;   // [pitch * h] unknowns before each word
     const uint32_t* position;  // [n] post of each unknown
     double cx, cy, center;     // 1/dx^2, 1/dy^2, 2 cx + 2 cy + 1/L^2
     double diagonal;           // the operator's center weight
@@ -583,6 +570,17 @@ struct LevelView {
 // four are the 5-point stencil's.
 __constant__ int2 kStencil[12] = {{-1, 0}, {1, 0},  {0, -1}, {0, 1},  {-2, 0}, {2, 0},
                                   {0, -2}, {0, 2},  {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+
+// The compact index of the post (c, r), or ~0u where it is not an unknown.
+__device__ __forceinline__ uint32_t index_at(const LevelView& L, int c, int r) {
+    const size_t q = size_t(r) * L.pitch + uint32_t(c >> 5);
+    const uint32_t m = L.mask[q], b = uint32_t(c & 31);
+    return (m >> b) & 1u ? L.offsets[q] + __popc(m & ((1u << b) - 1u)) : kNone;
+}
+
+__device__ __forceinline__ bool unknown_at(const LevelView& L, int c, int r) {
+    return (L.mask[size_t(r) * L.pitch + uint32_t(c >> 5)] >> (c & 31)) & 1u;
+}
 
 // The operator at unknown k of u (0 off the unknowns): B = -Laplacian + 1/L^2 on 5 points
 // (order 1), or B applied twice on 13 points (order 2), as ApplyScreened / Apply
@@ -626,7 +624,7 @@ __global__ void neighbors_kernel(const LevelView L, uint32_t* __restrict__ nbr) 
         nbr[size_t(k) * kTaps + j] =
             c < 0 || r < 0 || c >= int(L.w) || r >= int(L.h)
                 ? kNone
-                : L.index[size_t(r) * L.w + uint32_t(c)];
+                : index_at(L, c, r);
     }
 }
 
@@ -646,7 +644,7 @@ __global__ void parents_kernel(const LevelView F, const LevelView Cl,
         parents[size_t(k) * 4 + j] =
             cs[j] < 0 || rs[j] < 0 || cs[j] >= int(Cl.w) || rs[j] >= int(Cl.h)
                 ? kNone
-                : Cl.index[size_t(rs[j]) * Cl.w + uint32_t(cs[j])];
+                : index_at(Cl, cs[j], rs[j]);
     }
 }
 
@@ -666,7 +664,7 @@ __global__ void children_kernel(const LevelView F, const LevelView Cl,
             children[size_t(k) * 16 + j * 4 + i] =
                 fx < 0 || fy < 0 || fx >= int(F.w) || fy >= int(F.h)
                     ? kNone
-                    : F.index[size_t(fy) * F.w + uint32_t(fx)];
+                    : index_at(F, fx, fy);
         }
     }
 }
@@ -683,8 +681,9 @@ __global__ void rhs_kernel(const LevelView L, const float* __restrict__ field,
     const uint32_t p = L.position[k];
     const int col = int(p % L.w), row = int(p / L.w);
     auto f = [&](int dc, int dr) -> double {
-        const size_t q = size_t(row + dr) * L.w + uint32_t(col + dc);
-        return L.index[q] == kNone ? double(field[q]) : 0.0;
+        return unknown_at(L, col + dc, row + dr)
+                   ? 0.0
+                   : double(field[size_t(row + dr) * L.w + uint32_t(col + dc)]);
     };
     const double cx = L.cx, cy = L.cy, c0 = L.center;
     const double sx = f(-1, 0) + f(1, 0), sy = f(0, -1) + f(0, 1);
@@ -1107,28 +1106,27 @@ uint32_t blocks_for(size_t n, uint32_t threads = 256) {
 // A level's device arrays.
 struct Level {
     LevelView view{};
-    Buffer index, position, x, b, t;  // x, b, t: float (double on the coarsest level)
+    Buffer mask, offsets, position, x, b, t;  // x, b, t: float (double on the coarsest level)
     Buffer nbr, parents, children;
 };
 
 // The seam calls' device scratch, one per device, grown as needed and kept across calls (no
 // allocation, and so no device-wide synchronization of a free, on a call that fits).
 struct Work {
-    Buffer marks, flags, scan, distance, carried, distance2, carried2, count, partial, dots;
+    Buffer bits, count, scan, steps, rows, partial, dots;
     Buffer tileCounts, tileList, cg;
     Buffer cgX, cgR, cgP, cgAp, cgZ, rhs;
     Buffer hostIn, hostIn2, hostOut, hostOut2;  // device copies of host-memory arguments
     Level levels[kMaxLevels];
     ~Work() {
-        for (Buffer* b : {&marks, &flags, &scan, &distance, &carried, &distance2, &carried2,
-                          &count, &partial, &dots, &tileCounts, &tileList, &cg,
-                          &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs,
-                          &hostIn, &hostIn2, &hostOut, &hostOut2}) {
+        for (Buffer* b : {&bits, &count, &scan, &steps, &rows, &partial, &dots, &tileCounts,
+                          &tileList, &cg, &cgX, &cgR, &cgP, &cgAp, &cgZ, &rhs, &hostIn, &hostIn2,
+                          &hostOut, &hostOut2}) {
             b->release();
         }
         for (Level& l : levels) {
-            for (Buffer* b : {&l.index, &l.position, &l.x, &l.b, &l.t, &l.nbr, &l.parents,
-                              &l.children}) {
+            for (Buffer* b : {&l.mask, &l.offsets, &l.position, &l.x, &l.b, &l.t, &l.nbr,
+                              &l.parents, &l.children}) {
                 b->release();
             }
         }
@@ -1143,33 +1141,34 @@ Work& device_work(tg_device* d) {
     return *static_cast<Work*>(d->seams);
 }
 
-// Compacts `flags` (0 / 1 per post of a w x h lattice) into the level's index and positions.
-int compact(Work& wk, Level& level, uint32_t w, uint32_t h, cudaStream_t s) {
-    const size_t n = size_t(w) * h;
-    if (n >= 0xffffffffull) {
-        return fail(TG_ERROR_UNSUPPORTED, "a seam lattice holds fewer than 2^32 posts");
-    }
-    uint32_t* flags = static_cast<uint32_t*>(wk.flags.ptr);
-    TG_CUDA(wk.marks.reserve(n), "allocation");
-    flags_to_marks_kernel<<<blocks_for(n), 256, 0, s>>>(flags, n,
-                                                       static_cast<uint8_t*>(wk.marks.ptr));
-    TG_CUDA(wk.scan.reserve(scan_scratch_words(uint32_t(n)) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(launch_exclusive_scan(flags, uint32_t(n), static_cast<uint32_t*>(wk.scan.ptr), s),
+// The level's compact index and positions from its unknown mask (`level.mask`, `pitch` words a
+// row of a w x h lattice).
+int compact(Work& wk, Level& level, uint32_t w, uint32_t h, uint32_t pitch, cudaStream_t s) {
+    const size_t words = size_t(pitch) * h;
+    uint32_t* offsets = nullptr;
+    TG_CUDA(level.offsets.reserve((words + 1) * sizeof(uint32_t)), "allocation");
+    offsets = static_cast<uint32_t*>(level.offsets.ptr);
+    const uint32_t* mask = static_cast<const uint32_t*>(level.mask.ptr);
+    word_counts_kernel<<<blocks_for(words), 256, 0, s>>>(mask, words, offsets);
+    TG_CUDA(wk.scan.reserve(scan_scratch_words(uint32_t(words)) * sizeof(uint32_t)),
+            "allocation");
+    TG_CUDA(launch_exclusive_scan(offsets, uint32_t(words), static_cast<uint32_t*>(wk.scan.ptr),
+                                  s),
             "scan");
     uint32_t total = 0;
-    TG_CUDA(cudaMemcpyAsync(&total, flags + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+    TG_CUDA(cudaMemcpyAsync(&total, offsets + words, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
             "copy to host");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    TG_CUDA(level.index.reserve(n * sizeof(uint32_t)), "allocation");
     TG_CUDA(level.position.reserve(std::max<size_t>(total, 1) * sizeof(uint32_t)), "allocation");
-    compact_kernel<<<blocks_for(n), 256, 0, s>>>(flags, static_cast<const uint8_t*>(wk.marks.ptr),
-                                                n, static_cast<uint32_t*>(level.index.ptr),
-                                                static_cast<uint32_t*>(level.position.ptr));
+    positions_kernel<<<blocks_for(words), 256, 0, s>>>(
+        mask, offsets, words, pitch, w, static_cast<uint32_t*>(level.position.ptr));
     TG_CUDA(cudaGetLastError(), "compact launch");
     level.view.w = w;
     level.view.h = h;
     level.view.n = total;
-    level.view.index = static_cast<const uint32_t*>(level.index.ptr);
+    level.view.pitch = pitch;
+    level.view.mask = mask;
+    level.view.offsets = offsets;
     level.view.position = static_cast<const uint32_t*>(level.position.ptr);
     return TG_OK;
 }
@@ -1484,150 +1483,137 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
         }
         return st;
     };
-    TG_CUDA(cudaMemsetAsync(dField, 0, n * 4, s), "memset");
     Events ev;
     if (ev.create() != cudaSuccess) {
         return finish(fail(TG_ERROR_CUDA, "event"));
     }
     TG_CUDA(cudaEventRecord(ev.e[0], s), "event");
-    if (o.mode == 0u) {
+    // The field is 0 without a seam, and when the earlier source has data at every post or at
+    // none.
+    auto empty = [&]() {
+        TG_CUDA(cudaMemsetAsync(dField, 0, n * 4, s), "memset");
         return finish(TG_OK);
+    };
+    if (o.mode == 0u) {
+        return empty();
     }
-    // The field is 0 when the earlier source has data at every post or at none.
+    int sms = 0;
+    TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->ordinal),
+            "attribute");
+    const uint32_t pitch = (width + 31) / 32;
+    const size_t words = size_t(pitch) * height;
+    TG_CUDA(wk.bits.reserve(words * 4), "allocation");
     TG_CUDA(wk.count.reserve(8), "allocation");
     TG_CUDA(cudaMemsetAsync(wk.count.ptr, 0, 8, s), "memset");
-    count_data_kernel<<<1184, 256, 0, s>>>(dData, n,
-                                           static_cast<unsigned long long*>(wk.count.ptr));
+    uint32_t* bits = static_cast<uint32_t*>(wk.bits.ptr);
+    pack_data_kernel<<<uint32_t(std::min<size_t>(blocks_for(words * 32), size_t(sms) * 16)), 256,
+                       0, s>>>(dData, width, height, pitch, bits,
+                               static_cast<unsigned long long*>(wk.count.ptr));
     unsigned long long withData = 0;
     TG_CUDA(cudaMemcpyAsync(&withData, wk.count.ptr, 8, cudaMemcpyDeviceToHost, s), "copy");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
     if (withData == 0 || withData == n) {
-        return finish(TG_OK);
+        return empty();
     }
-    // The band's differences.
-    TG_CUDA(wk.marks.reserve(n), "allocation");
-    gaps_across_kernel<<<blocks_for(n), 256, 0, s>>>(dData, width, height, kBandPosts,
-                                                    static_cast<uint8_t*>(wk.marks.ptr));
-    band_kernel<<<blocks_for(n), 256, 0, s>>>(dData, dDiff, static_cast<uint8_t*>(wk.marks.ptr),
-                                             width, height, kBandPosts, dField);
-    TG_CUDA(cudaGetLastError(), "band launch");
-    // Distances to the nearest post with data, up to the reach (Height, Slope) or the width
-    // (Feather).
+    // Distances to the nearest post with data matter up to the reach (Height, Slope) or the
+    // width (Feather).
     const bool feather = o.mode == 1u;
     const double reach = feather ? o.width : 3.0 * o.decay_length;  // kSeamReachDecays
-    TG_CUDA(wk.distance.reserve(n * 4), "allocation");
-    if (feather) {
-        TG_CUDA(wk.carried.reserve(n * 4), "allocation");
-    }
     const float cap =
         float(reach) < reach ? std::nextafter(float(reach), INFINITY) : float(reach);
-    const float* distance = nullptr;
-    const float* carried = nullptr;
     // Halo of the tiled passes: a distance at most `cap` reaches cap / dx columns, cap / dy rows.
     const int mx = int(std::min(std::ceil(double(cap) / dx) + 2.0, double(width)));
     const int my = int(std::min(std::ceil(double(cap) / dy) + 2.0, double(height)));
-    int ts = 0;
-    for (int side : {128, 96, 64, 32}) {
-        if (tile_window_bytes(tile_window_posts(side, mx, my, width, height), feather) <=
-            kTileSharedBytes) {
-            ts = side;
-            break;
-        }
+    const int halo = std::max(mx, my);
+    const int ts = halo <= 128 ? 64 : std::min(1024, (halo / 2 + 31) / 32 * 32);
+    const uint32_t tilesX = (width + ts - 1) / ts, tilesY = (height + ts - 1) / ts;
+    const size_t tiles = size_t(tilesX) * tilesY;
+    TG_CUDA(wk.tileCounts.reserve(tiles * 4), "allocation");
+    TG_CUDA(wk.tileList.reserve(tiles * 4 + 4), "allocation");
+    uint32_t* counts = static_cast<uint32_t*>(wk.tileCounts.ptr);
+    uint32_t* list = static_cast<uint32_t*>(wk.tileList.ptr);
+    TG_CUDA(cudaMemsetAsync(counts, 0, tiles * 4, s), "memset");
+    TG_CUDA(cudaMemsetAsync(list, 0, 4, s), "memset");
+    // The band's differences (every post of the field written), and the posts with data per
+    // tile.
+    BandBits bb{bits, dDiff, dField, counts, width, height, pitch, ts, tilesX};
+    const size_t bandWarps = size_t((pitch + 31) / 32) * ((height + kBandRows - 1) / kBandRows);
+    band_bits_kernel<<<blocks_for(bandWarps * 32), 256, 0, s>>>(bb);
+    TG_CUDA(cudaGetLastError(), "band launch");
+    active_tiles_kernel<<<blocks_for(tiles), 256, 0, s>>>(
+        counts, width, height, ts, tilesX, tilesY, (mx + ts - 1) / ts, (my + ts - 1) / ts,
+        list + 1, list);
+    uint32_t active = 0;
+    TG_CUDA(cudaMemcpyAsync(&active, list, 4, cudaMemcpyDeviceToHost, s), "copy");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    Level& L0 = wk.levels[0];
+    if (!feather) {
+        TG_CUDA(L0.mask.reserve(words * 4), "allocation");
+        TG_CUDA(cudaMemsetAsync(L0.mask.ptr, 0, words * 4, s), "memset");
     }
-    if (ts > 0) {
-        DistanceTiles t{};
-        t.data = dData;
-        t.field = feather ? dField : nullptr;
-        t.distance = static_cast<float*>(wk.distance.ptr);
-        t.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
-        t.w = width;
-        t.h = height;
-        t.dx = float(dx);
-        t.dy = float(dy);
-        t.diagonal = float(std::hypot(dx, dy));
-        t.cap = cap;
-        t.ts = ts;
-        t.mx = mx;
-        t.my = my;
-        t.maxPosts = int(tile_window_posts(ts, mx, my, width, height));
-        t.tilesX = (width + ts - 1) / ts;
-        t.tilesY = (height + ts - 1) / ts;
-        const size_t tiles = size_t(t.tilesX) * t.tilesY;
-        TG_CUDA(wk.tileCounts.reserve(tiles * 4), "allocation");
-        TG_CUDA(wk.tileList.reserve(tiles * 4 + 4), "allocation");
-        uint32_t* counts = static_cast<uint32_t*>(wk.tileCounts.ptr);
-        uint32_t* list = static_cast<uint32_t*>(wk.tileList.ptr);
-        t.list = list + 1;
-        t.count = list;
-        distance_init_kernel<<<2368, 256, 0, s>>>(dData, dField, n, t.distance, t.carried);
-        tile_counts_kernel<<<uint32_t(tiles), 256, 0, s>>>(dData, width, height, ts, t.tilesX,
-                                                          counts);
-        TG_CUDA(cudaMemsetAsync(list, 0, 4, s), "memset");
-        active_tiles_kernel<<<blocks_for(tiles), 256, 0, s>>>(
-            counts, width, height, ts, t.tilesX, t.tilesY, (mx + ts - 1) / ts,
-            (my + ts - 1) / ts, list + 1, list);
-        const size_t bytes = tile_window_bytes(size_t(t.maxPosts), feather);
-        TG_CUDA(cudaFuncSetAttribute(distance_tile_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)),
+    if (active > 0) {
+        DistanceWarps p{};
+        p.bits = bits;
+        p.field = feather ? dField : nullptr;
+        p.w = width;
+        p.h = height;
+        p.pitch = pitch;
+        p.dx = float(dx);
+        p.dy = float(dy);
+        p.diagonal = float(std::hypot(dx, dy));
+        p.ts = ts;
+        p.mx = mx;
+        p.my = my;
+        p.tilesX = tilesX;
+        p.list = list + 1;
+        p.count = list;
+        p.unknown = feather ? nullptr : static_cast<uint32_t*>(L0.mask.ptr);
+        p.reach = reach;
+        p.feather = feather ? dField : nullptr;
+        p.width = o.width;
+        // A window is at most ts + 2 mx columns and ts + 2 my rows; the backward pass covers
+        // its rows from the tile's first.
+        const int carriedCopies = feather ? 2 : 1;
+        p.rowFloats = int(std::min<size_t>(size_t(ts) + 2 * size_t(mx), width));
+        const size_t bandsBelow = (std::min<size_t>(size_t(ts) + my, height) + 31) / 32;
+        p.scratchFloats = size_t(carriedCopies) * bandsBelow * (size_t(p.rowFloats) + 62) * 32;
+        const size_t rowBytes = size_t(p.rowFloats) * 4 * carriedCopies;
+        const bool sharedRows = rowBytes * kDistanceWarps <= kRowSharedBytes;
+        const size_t shared = sharedRows ? rowBytes * kDistanceWarps : 0;
+        auto kernel = feather ? (sharedRows ? distance_warp_kernel<true, true>
+                                            : distance_warp_kernel<true, false>)
+                              : (sharedRows ? distance_warp_kernel<false, true>
+                                            : distance_warp_kernel<false, false>);
+        TG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(shared)),
                 "shared memory attribute");
-        int perSm = 0, sms = 0;
-        TG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, distance_tile_kernel, 128,
-                                                              bytes),
+        int perSm = 0;
+        TG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel,
+                                                              32 * kDistanceWarps, shared),
                 "occupancy");
-        TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->ordinal),
-                "attribute");
-        const uint32_t blocks = uint32_t(std::max(1, perSm) * sms);
-        distance_tile_kernel<<<std::min<uint32_t>(blocks, uint32_t(tiles)), 128, bytes, s>>>(t);
+        size_t slots = size_t(std::max(1, perSm)) * size_t(sms) * kDistanceWarps;
+        slots = std::min<size_t>(slots, active);
+        slots = std::min<size_t>(
+            slots, std::max<size_t>(1, kScratchBytes / (p.scratchFloats * 4 + rowBytes)));
+        p.slots = uint32_t(slots);
+        TG_CUDA(wk.steps.reserve(slots * p.scratchFloats * 4), "allocation");
+        p.scratch = static_cast<float*>(wk.steps.ptr);
+        if (!sharedRows) {
+            TG_CUDA(wk.rows.reserve(slots * rowBytes), "allocation");
+            p.rows = static_cast<float*>(wk.rows.ptr);
+        }
+        kernel<<<uint32_t((slots + kDistanceWarps - 1) / kDistanceWarps), 32 * kDistanceWarps,
+                 shared, s>>>(p);
         TG_CUDA(cudaGetLastError(), "distance launch");
-        distance = t.distance;
-        carried = t.carried;
-    } else {
-        // Halos too wide for a window in shared memory: the passes row by row.
-        TG_CUDA(wk.distance2.reserve(n * 4), "allocation");
-        if (feather) {
-            TG_CUDA(wk.carried2.reserve(n * 4), "allocation");
-        }
-        DistanceRow row{};
-        row.data = dData;
-        row.field = dField;
-        row.distance = static_cast<float*>(wk.distance.ptr);
-        row.carried = feather ? static_cast<float*>(wk.carried.ptr) : nullptr;
-        row.distanceOut = static_cast<float*>(wk.distance2.ptr);
-        row.carriedOut = feather ? static_cast<float*>(wk.carried2.ptr) : nullptr;
-        row.w = width;
-        row.h = height;
-        row.dx = float(dx);
-        row.dy = float(dy);
-        row.diagonal = float(std::hypot(dx, dy));
-        row.cap = cap;
-        // A recurrence along a row stays within the cap for at most cap / dx steps.
-        row.window = mx;
-        const uint32_t segments = (width + kSegment - 1) / kSegment;
-        for (uint32_t r = 0; r < height; ++r) {
-            distance_forward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
-        }
-        for (uint32_t r = height; r-- > 0;) {
-            distance_backward_kernel<<<blocks_for(segments, 128), 128, 0, s>>>(row, r);
-        }
-        TG_CUDA(cudaGetLastError(), "distance launch");
-        distance = row.distanceOut;
-        carried = row.carriedOut;
     }
     if (feather) {
-        feather_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, carried, n, o.width,
-                                                    dField);
-        TG_CUDA(cudaGetLastError(), "feather launch");
         return finish(TG_OK);
     }
     // The unknowns of each level.
-    TG_CUDA(wk.flags.reserve((n + 1) * sizeof(uint32_t)), "allocation");
-    unknown_kernel<<<blocks_for(n), 256, 0, s>>>(dData, distance, width, height, reach,
-                                                static_cast<uint32_t*>(wk.flags.ptr));
-    TG_CUDA(cudaGetLastError(), "unknown launch");
     const int order = o.mode == 3u ? 2 : 1;
     const double screening = 1.0 / (o.decay_length * o.decay_length);
     int levels = 0;
-    uint32_t lw = width, lh = height;
+    uint32_t lw = width, lh = height, lp = pitch;
     double ldx = dx, ldy = dy;
     for (; levels < int(o.levels); ++levels) {
         Level& L = wk.levels[levels];
@@ -1635,15 +1621,16 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
             const Level& F = wk.levels[levels - 1];
             lw = (lw + 1) / 2;
             lh = (lh + 1) / 2;
+            lp = (lw + 31) / 32;
             ldx *= 2.0;
             ldy *= 2.0;
-            TG_CUDA(cudaMemsetAsync(wk.flags.ptr, 0, (size_t(lw) * lh + 1) * sizeof(uint32_t), s),
-                    "memset");
+            TG_CUDA(L.mask.reserve(size_t(lp) * lh * 4), "allocation");
+            TG_CUDA(cudaMemsetAsync(L.mask.ptr, 0, size_t(lp) * lh * 4, s), "memset");
             coarsen_kernel<<<blocks_for(F.view.n), 256, 0, s>>>(
-                F.view.position, F.view.n, F.view.w, lw, static_cast<uint32_t*>(wk.flags.ptr));
+                F.view.position, F.view.n, F.view.w, lp, static_cast<uint32_t*>(L.mask.ptr));
             TG_CUDA(cudaGetLastError(), "coarsen launch");
         }
-        if (int st = compact(wk, L, lw, lh, s)) {
+        if (int st = compact(wk, L, lw, lh, lp, s)) {
             return finish(st);
         }
         L.view.cx = 1.0 / (ldx * ldx);

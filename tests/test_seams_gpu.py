@@ -184,7 +184,7 @@ def test_samples_are_the_reference_lattice(device, z, scene, mode):
 
 @pytest.mark.parametrize("mode", ["feather", "height"])
 def test_wide_reach(device, mode):
-    # A reach wider than a distance window in shared memory holds: the row-by-row passes.
+    # A reach wider than the lattice: every tile's window is the whole lattice.
     rng = np.random.default_rng(12)
     h, w = 240, 260
     data = np.ones((h, w), np.uint8)
@@ -198,6 +198,27 @@ def test_wide_reach(device, mode):
         assert np.array_equal(field.view(np.uint32), want.view(np.uint32))
     else:
         want = S.solve(data, diff, 0.5, 0.5, mode, 40.0)
+        assert np.abs(field.astype(np.float64) - want).max() <= 1e-4
+
+
+@pytest.mark.parametrize("mode", ["feather", "height"])
+def test_windows_wider_than_shared_memory(device, mode):
+    # A window of 13,000 columns: the rows the distance warps hand down are kept in device memory
+    # instead of shared memory.
+    rng = np.random.default_rng(21)
+    h, w = 40, 13000
+    data = np.ones((h, w), np.uint8)
+    data[10:30, 6400:6600] = 0
+    xx = np.arange(w)[None, :]
+    diff = np.where(data != 0, 1.0 + 1e-4 * xx + 0.1 * rng.standard_normal((h, w)),
+                    np.nan).astype(np.float32)
+    field, st = device.seam_solve(data, diff, 1.0, 1.0, mode, width=7000.0, decay_length=2200.0)
+    if mode == "feather":
+        want = S.feather(data, diff, 1.0, 1.0, 7000.0)
+        assert np.array_equal(field.view(np.uint32), want.view(np.uint32))
+    else:
+        assert st["unknowns"] == 20 * 200
+        want = S.solve(data, diff, 1.0, 1.0, mode, 2200.0)
         assert np.abs(field.astype(np.float64) - want).max() <= 1e-4
 
 
