@@ -743,16 +743,6 @@ __global__ void residual_kernel(const LevelView L, const T* __restrict__ b,
     }
 }
 
-// The operator applied to a direction (FP64, for the conjugate gradients).
-template <int kOrder>
-__global__ void apply_kernel(const LevelView L, const double* __restrict__ u,
-                             double* __restrict__ out, const CgState* cg) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < L.n && !stopped(cg)) {
-        out[k] = apply_at<kOrder, double, double>(L, u, k);
-    }
-}
-
 // Restriction, gathered: coarse unknown (C, R) takes 1/4 of each fine residual whose parent or
 // parent's neighbor it is, weighted 3/4 or 1/4 per axis (the transfer weights 9/16, 3/16, 3/16,
 // 1/16, seam_field.cpp:56).
@@ -799,22 +789,10 @@ __global__ void prolong_kernel(const LevelView F, const LevelView Cl, const Tc* 
 
 constexpr int kDotBlocks = 512;
 
-// Partial sums of a . b (and of c . d when given) per block; summed by dot_finish_kernel in a
-// fixed order, so every run gives the same bits.
-__global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
-                           const double* __restrict__ c, const double* __restrict__ d, uint32_t n,
-                           double* __restrict__ partial, const CgState* cg) {
-    if (stopped(cg)) {
-        return;
-    }
+// The block's sums of x and y into partial[block] and partial[kDotBlocks + block], as a fixed
+// tree over 256 threads.
+__device__ __forceinline__ void block_partials(double x, double y, double* __restrict__ partial) {
     __shared__ double s0[256], s1[256];
-    double x = 0.0, y = 0.0;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        x += a[k] * b[k];
-        if (c != nullptr) {
-            y += c[k] * d[k];
-        }
-    }
     s0[threadIdx.x] = x;
     s1[threadIdx.x] = y;
     __syncthreads();
@@ -831,10 +809,68 @@ __global__ void dot_kernel(const double* __restrict__ a, const double* __restric
     }
 }
 
+// Partial sums of a . b (and of c . d when given) per block (kDotBlocks blocks of 256 threads);
+// summed by finish_kernel in a fixed order, so every run gives the same bits.
+__global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                           const double* __restrict__ c, const double* __restrict__ d, uint32_t n,
+                           double* __restrict__ partial, const CgState* cg) {
+    if (stopped(cg)) {
+        return;
+    }
+    double x = 0.0, y = 0.0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        x += a[k] * b[k];
+        if (c != nullptr) {
+            y += c[k] * d[k];
+        }
+    }
+    block_partials(x, y, partial);
+}
+
+// Ap = A p, with the partial sums of p . Ap.
+template <int kOrder>
+__global__ void apply_dot_kernel(const LevelView L, const double* __restrict__ p,
+                                 double* __restrict__ ap, double* __restrict__ partial,
+                                 const CgState* cg) {
+    if (stopped(cg)) {
+        return;
+    }
+    double x = 0.0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < L.n;
+         k += gridDim.x * blockDim.x) {
+        const double a = apply_at<kOrder, double, double>(L, p, k);
+        ap[k] = a;
+        x += p[k] * a;
+    }
+    block_partials(x, 0.0, partial);
+}
+
+// The partial sums of r . r and r . z, z the V-cycle's result on the finest level (float).
+__global__ void precondition_dots_kernel(const double* __restrict__ r,
+                                         const float* __restrict__ z, uint32_t n,
+                                         double* __restrict__ partial, const CgState* cg) {
+    if (stopped(cg)) {
+        return;
+    }
+    double x = 0.0, y = 0.0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double rk = r[k];
+        x += rk * rk;
+        y += rk * double(z[k]);
+    }
+    block_partials(x, y, partial);
+}
+
+enum Then { kThenNothing = 0, kThenStep = 1, kThenNext = 2 };
+
 // The block partials summed by one block of kDotBlocks threads as a fixed tree, so every run
-// adds them in the same order.
-__global__ void dot_finish_kernel(const double* __restrict__ partial, double* __restrict__ out,
-                                  const CgState* cg) {
+// adds them in the same order; then, on the device state:
+//   kThenStep, after p . Ap: the step, or the stop when the curvature is not positive or the
+//     iterations are spent (PreconditionedCg, seam_field.cpp:519-527);
+//   kThenNext, after r . r and r . z: the stop at the target residual, else the direction's
+//     ratio (seam_field.cpp:532-542).
+__global__ void finish_kernel(const double* __restrict__ partial, double* __restrict__ out,
+                              CgState* cg, int then) {
     if (stopped(cg)) {
         return;
     }
@@ -849,60 +885,94 @@ __global__ void dot_finish_kernel(const double* __restrict__ partial, double* __
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[0] = s0[0];
-        out[1] = s1[0];
+    if (threadIdx.x != 0) {
+        return;
+    }
+    out[0] = s0[0];
+    out[1] = s1[0];
+    if (then == kThenStep) {
+        const double curvature = s0[0];
+        if (cg->iterations >= cg->maxIterations || !(cg->fit > 0.0) || !(curvature > 0.0)) {
+            cg->done = 1u;
+            return;
+        }
+        cg->step = cg->fit / curvature;
+        cg->iterations += 1u;
+    } else if (then == kThenNext) {
+        if (sqrt(s0[0]) <= cg->target) {
+            cg->done = 1u;
+            return;
+        }
+        const double next = s1[0];
+        cg->ratio = next / cg->fit;
+        cg->fit = next;
     }
 }
 
-// After p . Ap: the step, or the stop when the curvature is not positive or the iterations are
-// spent (PreconditionedCg, seam_field.cpp:519-527).
-__global__ void cg_step_kernel(CgState* cg) {
-    if (cg->done != 0u) {
-        return;
-    }
-    const double curvature = cg->dots[0];
-    if (cg->iterations >= cg->maxIterations || !(cg->fit > 0.0) || !(curvature > 0.0)) {
-        cg->done = 1u;
-        return;
-    }
-    cg->step = cg->fit / curvature;
-    cg->iterations += 1u;
-}
-
-// After r . r and r . z: the stop at the target residual, else the direction's ratio
-// (seam_field.cpp:532-542).
-__global__ void cg_next_kernel(CgState* cg) {
-    if (cg->done != 0u) {
-        return;
-    }
-    if (sqrt(cg->dots[0]) <= cg->target) {
-        cg->done = 1u;
-        return;
-    }
-    const double next = cg->dots[1];
-    cg->ratio = next / cg->fit;
-    cg->fit = next;
-}
-
-// x += step p, r -= step ap.
+// x += step p, r -= step Ap; with `b0`, the finest level's right-hand side float(r) for the
+// V-cycle, and with `x0` its first smoothing sweep from 0 (scale b).
 __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
                                  const double* __restrict__ p, const double* __restrict__ ap,
-                                 uint32_t n, const CgState* cg) {
+                                 uint32_t n, float* __restrict__ b0, float* __restrict__ x0,
+                                 float scale, const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
         const double step = cg->step;
         x[k] += step * p[k];
-        r[k] -= step * ap[k];
+        const double rk = r[k] - step * ap[k];
+        r[k] = rk;
+        if (b0 != nullptr) {
+            const float bk = float(rk);
+            b0[k] = bk;
+            if (x0 != nullptr) {
+                x0[k] = scale * bk;
+            }
+        }
     }
 }
 
 // p = z + ratio p.
-__global__ void cg_direction_kernel(double* __restrict__ p, const double* __restrict__ z,
-                                    uint32_t n, const CgState* cg) {
+template <typename T>
+__global__ void cg_direction_kernel(double* __restrict__ p, const T* __restrict__ z, uint32_t n,
+                                    const CgState* cg) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
-        p[k] = z[k] + cg->ratio * p[k];
+        p[k] = double(z[k]) + cg->ratio * p[k];
+    }
+}
+
+// The coarsest level's sweeps in one block, its iterates in shared memory: the same damped
+// Jacobi steps as jacobi_kernel, a block barrier between sweeps.
+constexpr uint32_t kCoarsestBlockPosts = 4096;
+
+template <int kOrder>
+__global__ void __launch_bounds__(1024) coarsest_kernel(const LevelView L,
+                                                        const double* __restrict__ b,
+                                                        double* __restrict__ x, double omega,
+                                                        int sweeps, const CgState* cg) {
+    if (stopped(cg)) {
+        return;
+    }
+    extern __shared__ double iterates[];
+    double* cur = iterates;
+    double* next = iterates + L.n;
+    const double scale = omega / L.diagonal;
+    for (int i = 0; i < sweeps; ++i) {
+        for (uint32_t k = threadIdx.x; k < L.n; k += blockDim.x) {
+            if (i == 0) {
+                next[k] = scale * b[k];
+            } else {
+                const double r = b[k] - apply_at<kOrder, double, double>(L, cur, k);
+                next[k] = cur[k] + scale * r;
+            }
+        }
+        __syncthreads();
+        double* t = cur;
+        cur = next;
+        next = t;
+    }
+    for (uint32_t k = threadIdx.x; k < L.n; k += blockDim.x) {
+        x[k] = cur[k];
     }
 }
 
@@ -1214,25 +1284,37 @@ cudaError_t copy_level(const Solver& sv, const void* from, void* to, uint32_t n,
     return cudaGetLastError();
 }
 
+// Where a level's first smoothing sweep of `sweeps` writes: the sweeps alternate between x and t
+// and the last lands in x.
+void* first_sweep_target(Level& L, int sweeps) {
+    return sweeps % 2 == 1 ? L.x.ptr : L.t.ptr;
+}
+
 // The V-cycle from level `d` (VCycle, seam_field.cpp:423): an approximate solution of the level's
-// operator for its b, from 0, into its x.
+// operator for its b, from 0, into its x. `smoothed` sweeps of the first smoothing are done
+// already (0 or 1, the first one landing where this one would put it). Sweeps alternate between
+// x and t so that the last lands in x.
 template <int kOrder>
-int vcycle(Solver& sv, int d) {
+int vcycle(Solver& sv, int d, int smoothed = 0) {
     Level& L = sv.wk->levels[d];
     const bool last = d + 1 == sv.levels;
     if (L.view.n == 0) {
         return TG_OK;
     }
     const int sweeps = last ? sv.coarsest : sv.sweeps;
-    // Sweeps alternate between x and t; the first starts from 0.
-    void* cur = nullptr;
-    for (int i = 0; i < sweeps; ++i) {
-        void* next = (i % 2 == 0) ? L.x.ptr : L.t.ptr;
+    if (last && smoothed == 0 && L.view.n <= kCoarsestBlockPosts) {
+        const uint32_t threads = std::min<uint32_t>(1024, (L.view.n + 31) / 32 * 32);
+        coarsest_kernel<kOrder><<<1, threads, size_t(L.view.n) * 16, sv.s>>>(
+            L.view, static_cast<const double*>(L.b.ptr), static_cast<double*>(L.x.ptr),
+            sv.omega, sweeps, sv.cg);
+        TG_CUDA(cudaGetLastError(), "coarsest launch");
+        return TG_OK;
+    }
+    void* cur = smoothed > 0 ? first_sweep_target(L, sweeps) : nullptr;
+    for (int i = smoothed; i < sweeps; ++i) {
+        void* next = (sweeps - i) % 2 == 1 ? L.x.ptr : L.t.ptr;
         TG_CUDA(jacobi<kOrder>(sv, L.view, L.b.ptr, cur, next, last), "jacobi");
         cur = next;
-    }
-    if (cur != L.x.ptr) {
-        TG_CUDA(copy_level(sv, cur, L.x.ptr, L.view.n, last), "copy");
     }
     if (last) {
         return TG_OK;
@@ -1301,40 +1383,58 @@ int precondition(Solver& sv, const double* r, double* z) {
     return TG_OK;
 }
 
-// a . b and c . d (c may be null) into `out` on the device.
+// a . b and c . d (c may be null) into `out` on the device, then `then` on the state.
 cudaError_t dots(const Solver& sv, const double* a, const double* b, const double* c,
-                 const double* d, uint32_t n, double* out) {
+                 const double* d, uint32_t n, double* out, CgState* cg = nullptr,
+                 int then = kThenNothing) {
     dot_kernel<<<kDotBlocks, 256, 0, sv.s>>>(a, b, c, d, n,
                                              static_cast<double*>(sv.wk->partial.ptr), sv.cg);
-    dot_finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
-                                                  out, sv.cg);
+    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
+                                              out, cg, then);
     return cudaGetLastError();
 }
 
 // Iterations launched between looks at whether the conjugate gradients stopped.
 constexpr int kIterationsPerGraph = 4;
 
-// One iteration of PreconditionedCg (seam_field.cpp:517-542), every scalar on the device.
+// One iteration of PreconditionedCg (seam_field.cpp:517-542), every scalar on the device. With
+// more than one level, the update writes the finest level's right-hand side and first sweep, and
+// z stays the finest level's float iterate: the dots and the direction read it there.
 template <int kOrder>
 int iteration(Solver& sv, CgState* cg) {
     Work& wk = *sv.wk;
-    const LevelView& L0 = wk.levels[0].view;
-    const uint32_t n = L0.n;
+    Level& L0 = wk.levels[0];
+    const uint32_t n = L0.view.n;
     double* x = static_cast<double*>(wk.cgX.ptr);
     double* r = static_cast<double*>(wk.cgR.ptr);
     double* p = static_cast<double*>(wk.cgP.ptr);
     double* ap = static_cast<double*>(wk.cgAp.ptr);
     double* z = static_cast<double*>(wk.cgZ.ptr);
-    apply_kernel<kOrder><<<blocks_for(n), 256, 0, sv.s>>>(L0, p, ap, cg);
-    TG_CUDA(dots(sv, p, ap, nullptr, nullptr, n, cg_dots(cg)), "dot launch");
-    cg_step_kernel<<<1, 1, 0, sv.s>>>(cg);
-    cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, cg);
-    if (int st = precondition<kOrder>(sv, r, z)) {
+    double* partial = static_cast<double*>(wk.partial.ptr);
+    apply_dot_kernel<kOrder><<<kDotBlocks, 256, 0, sv.s>>>(L0.view, p, ap, partial, cg);
+    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(partial, cg_dots(cg), cg, kThenStep);
+    if (sv.levels == 1) {
+        cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, nullptr, nullptr, 0.0f,
+                                                          cg);
+        if (int st = precondition<kOrder>(sv, r, z)) {
+            return st;
+        }
+        TG_CUDA(dots(sv, r, r, r, z, n, cg_dots(cg), cg, kThenNext), "dot launch");
+        cg_direction_kernel<double><<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, cg);
+        TG_CUDA(cudaGetLastError(), "iteration launch");
+        return TG_OK;
+    }
+    const float scale = float(sv.omega / L0.view.diagonal);
+    cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(
+        x, r, p, ap, n, static_cast<float*>(L0.b.ptr),
+        static_cast<float*>(first_sweep_target(L0, sv.sweeps)), scale, cg);
+    if (int st = vcycle<kOrder>(sv, 0, 1)) {
         return st;
     }
-    TG_CUDA(dots(sv, r, r, r, z, n, cg_dots(cg)), "dot launch");
-    cg_next_kernel<<<1, 1, 0, sv.s>>>(cg);
-    cg_direction_kernel<<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, cg);
+    const float* z0 = static_cast<const float*>(L0.x.ptr);
+    precondition_dots_kernel<<<kDotBlocks, 256, 0, sv.s>>>(r, z0, n, partial, cg);
+    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(partial, cg_dots(cg), cg, kThenNext);
+    cg_direction_kernel<float><<<blocks_for(n), 256, 0, sv.s>>>(p, z0, n, cg);
     TG_CUDA(cudaGetLastError(), "iteration launch");
     return TG_OK;
 }
@@ -1707,6 +1807,11 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
                                                     static_cast<double*>(wk.cgR.ptr));
     }
     TG_CUDA(cudaGetLastError(), "rhs launch");
+    for (auto kernel : {coarsest_kernel<1>, coarsest_kernel<2>}) {
+        TG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(kCoarsestBlockPosts * 16)),
+                "shared memory attribute");
+    }
     Solver sv{&wk, levels, order, s, order == 1 ? 0.8 : 0.5, int(o.sweeps),
               int(o.coarsest_sweeps), nullptr, d->stream};
     int iterations = 0;
