@@ -414,6 +414,42 @@ int tg_crater_batch(const tg_crater_population* population, const tg_crater_shap
                     float* data, size_t data_capacity, double* footprints, size_t* n_records,
                     size_t* n_data);
 
+/* --- output -------------------------------------------------------------------------------- */
+
+/* GeoTiffWriteOptions (include/terraingen/raster/geotiff/geotiff.h:185): compression in
+ * TiffCompression's order (0 None, 1 LZW, 3 Deflate; 2, PackBits, is refused as the reference
+ * refuses it), tile_size a positive multiple of 16 (256 in the reference), big_tiff 1 to always
+ * write BigTIFF (otherwise only when the tiles could pass 4 GiB). */
+typedef struct tg_geotiff_options {
+    uint32_t compression;
+    uint32_t tile_size;
+    uint32_t big_tiff;
+    uint32_t reserved;
+} tg_geotiff_options;
+
+/* GeoKeys (geotiff.h:31): the GeoKeyDirectory, GeoDoubleParams and GeoAsciiParams tags' values;
+ * no keys when directory_count is 0. */
+typedef struct tg_geokeys {
+    const uint16_t* directory;
+    uint32_t directory_count;
+    uint32_t double_count;
+    const double* double_params;
+    const char* ascii_params; /* NUL-terminated, or null */
+} tg_geokeys;
+
+/* WriteGeoTiff (src/raster/geotiff/geotiff_write.cpp:256-297): `band_count` float rasters of
+ * grid->width x grid->height cells (row 0 first) on `grid`'s transform, as a tiled little-endian
+ * float32 GeoTIFF at `path`; `nodata` (mode 1 NaN, 2 value) is the GDAL_NODATA tag and pads the
+ * edge tiles (0 without). The tiles are laid out, run through the floating-point predictor and,
+ * for LZW, compressed on the device; Deflate tiles are compressed on host threads with zlib
+ * (level 6, the reference's miniz level: the same decoded data, other bytes). With None or LZW
+ * the file is the reference's byte for byte. `bands` are device pointers with
+ * TG_MEMORY_DEVICE (read on `stream`), host pointers with TG_MEMORY_HOST. */
+int tg_geotiff_write(tg_device* device, const char* path, const float* const* bands,
+                     uint32_t band_count, const tg_grid* grid, tg_nodata nodata,
+                     const tg_geokeys* keys, const tg_geotiff_options* options, int memory,
+                     void* stream);
+
 /* --- batched tiles ---------------------------------------------------------------------------
  * Many tiles of one layer stack (a Perlin fBm source, a crater layer and a boulder layer)
  * evaluated together: one count / scan / scatter of every tile's craters and boulders into bins,

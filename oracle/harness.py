@@ -156,6 +156,29 @@ def seam(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: i
             "field": field[:n].reshape(shape), "ms": ms.value}
 
 
+COMPRESSION = {"none": 0, "lzw": 1, "packbits": 2, "deflate": 3}  # TiffCompression's order
+
+
+def write_geotiff(lib: C.CDLL, path, bands: list, transform, nodata=None, directory=(),
+                  doubles=(), ascii: str = "", compression: str = "lzw", tile_size: int = 256,
+                  big_tiff: bool = False) -> None:
+    """The reference's WriteGeoTiff (tgref_write_geotiff) of float bands sharing one grid;
+    `nodata` None, NaN or a value."""
+    arrays = [np.ascontiguousarray(b, np.float32) for b in bands]
+    h, w = arrays[0].shape
+    ptrs = (C.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+    t = np.ascontiguousarray(transform, np.float64)
+    mode = 0 if nodata is None else (1 if np.isnan(nodata) else 2)
+    d = np.ascontiguousarray(directory, np.uint16)
+    dp = np.ascontiguousarray(doubles, np.float64)
+    st = lib.tgref_write_geotiff(str(path).encode(), C.cast(ptrs, C.c_void_p), len(arrays), w, h,
+                                 t.ctypes.data, mode, 0.0 if mode != 2 else float(nodata),
+                                 d.ctypes.data, len(d), dp.ctypes.data, len(dp), ascii.encode(),
+                                 COMPRESSION[compression], tile_size, int(big_tiff))
+    if st != 0:
+        raise RuntimeError(f"tgref_write_geotiff failed: {lib.tgref_error().decode()}")
+
+
 def chain(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: int,
           width: float, decay: float, out_grid) -> np.ndarray:
     """A SourceChain of the two rasters joined by `mode`, evaluated on `out_grid`."""
@@ -279,6 +302,11 @@ def _harness(name: str) -> C.CDLL:
         lib.tgref_chain.restype = C.c_int
         lib.tgref_patch_chain.argtypes = [_U32, P, P, P, P, C.c_int, _D, _D, _U32, _U32, P, P]
         lib.tgref_patch_chain.restype = C.c_int
+    if hasattr(lib, "tgref_write_geotiff"):
+        P = C.c_void_p
+        lib.tgref_write_geotiff.argtypes = [C.c_char_p, P, _U32, _U32, _U32, P, C.c_int, C.c_float,
+                                            P, _U32, P, _U32, C.c_char_p, C.c_int, _U32, C.c_int]
+        lib.tgref_write_geotiff.restype = C.c_int
     return lib
 
 

@@ -599,6 +599,59 @@ int tgref_datum_relief(const void* kernel, const void* records, const float* dat
 
 }  // extern "C"
 
+#include "terraingen/raster/geotiff/geotiff.h"
+
+extern "C" {
+
+/// WriteGeoTiff (src/raster/geotiff/geotiff_write.cpp) of `bandCount` width x height float
+/// rasters (row 0 first) on the GDAL-order `transform`, no-data `nodataMode` 0 none, 1 NaN, 2
+/// `nodata`; the GeoKeys given as their three tags; `compression` in TiffCompression's order.
+int tgref_write_geotiff(const char* path, const float* const* bands, uint32_t bandCount,
+                        uint32_t width, uint32_t height, const double* transform,
+                        int nodataMode, float nodata, const uint16_t* directory,
+                        uint32_t directoryCount, const double* doubles, uint32_t doubleCount,
+                        const char* ascii, int compression, uint32_t tileSize, int bigTiff) {
+    try {
+        RasterGrid grid{width, height,
+                        GeoTransform{transform[0], transform[1], transform[2], transform[3],
+                                     transform[4], transform[5]}};
+        std::vector<Raster<float>> rasters;
+        for (uint32_t b = 0; b < bandCount; ++b) {
+            Raster<float> r(grid);
+            for (uint32_t row = 0; row < height; ++row) {
+                for (uint32_t col = 0; col < width; ++col) {
+                    r(col, row) = bands[b][size_t(row) * width + col];
+                }
+            }
+            if (nodataMode == 1) {
+                r.SetNoData(std::numeric_limits<float>::quiet_NaN());
+            } else if (nodataMode == 2) {
+                r.SetNoData(nodata);
+            }
+            rasters.push_back(std::move(r));
+        }
+        GeoKeys keys;
+        keys.directory.assign(directory, directory + directoryCount);
+        keys.doubleParams.assign(doubles, doubles + doubleCount);
+        keys.asciiParams = ascii != nullptr ? ascii : "";
+        GeoTiffWriteOptions options;
+        options.compression = static_cast<TiffCompression>(compression);
+        options.tileSize = tileSize;
+        options.bigTiff = bigTiff != 0;
+        if (bandCount == 1) {
+            WriteGeoTiff(path, rasters.front(), keys, options);
+        } else {
+            WriteGeoTiff(path, rasters, keys, options);
+        }
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+}  // extern "C"
+
 #ifdef TGREF_CAPTURE
 // --- capture stubs for the tg_* C ABI the adapter calls ------------------------------------
 #include "tgb200.h"

@@ -6,7 +6,7 @@ and the reference-side drop-in device under adapter/. This package builds it in-
 to a CPU path.
 """
 
-from .device import Device, GridSpec, centered  # noqa: F401
+from .device import Device, GridSpec, centered, geographic_sphere_keys  # noqa: F401
 from ._native import TgError, library  # noqa: F401
 from . import layouts  # noqa: F401
 

@@ -205,6 +205,25 @@ SIGNATURES.update({
     "tg_server_stats_get": [_P, C.POINTER(ServerStats)],
 })
 
+class GeotiffOptions(C.Structure):
+    """tg_geotiff_options (GeoTiffWriteOptions)."""
+
+    _fields_ = [("compression", C.c_uint32), ("tile_size", C.c_uint32), ("big_tiff", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class GeoKeys(C.Structure):
+    """tg_geokeys (GeoKeys: the three GeoTIFF key tags' values)."""
+
+    _fields_ = [("directory", _P), ("directory_count", C.c_uint32), ("double_count", C.c_uint32),
+                ("double_params", _P), ("ascii_params", C.c_char_p)]
+
+
+SIGNATURES.update({
+    "tg_geotiff_write": [_P, C.c_char_p, _P, C.c_uint32, C.POINTER(Grid), NoData,
+                         C.POINTER(GeoKeys), C.POINTER(GeotiffOptions), _I, _P],
+})
+
 RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p, "tg_batch_destroy": None,
             "tg_server_destroy": None}
 

@@ -40,6 +40,7 @@ UNITS = {
     "probe.cu": [],
     "static_scratch.cu": [],
     "api.cu": [],
+    "geotiff.cu": [],
     "population.cpp": [],
 }
 
@@ -95,7 +96,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objects.append(str(obj))
     tmp = LIBRARY.with_suffix(".so.tmp")
     cmd = [compiler, *ARCH, "-shared", "-o", str(tmp), *objects, "-lcudart_static", "-lrt",
-           "-ldl", "-lpthread"]
+           "-ldl", "-lpthread", "-lz"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIBRARY)
     return LIBRARY

@@ -44,6 +44,20 @@ def centered(width: int, height: int, pixel: float, cx: float = 0.0, cy: float =
     return GridSpec(width, height, cx - 0.5 * pixel * width, cy + 0.5 * pixel * height, pixel)
 
 
+def geographic_sphere_keys(radius: float):
+    """GeographicSphereKeys (src/raster/geotiff/geotiff.cpp:103): the GeoKeys of longitude and
+    latitude in degrees on a sphere of `radius` meters, as (directory, doubles, ascii)."""
+    if not (radius > 0.0 and np.isfinite(radius)):
+        raise ValueError("A sphere's radius must be positive and finite")
+    user, params = 32767, 34736
+    entries = [(1024, 0, 2), (1025, 0, 1), (2048, 0, user), (2050, 0, user), (2054, 0, 9102),
+               (2056, 0, user), (2057, params, 0), (2058, params, 1)]
+    directory = [1, 1, 0, len(entries)]
+    for key, location, value in entries:
+        directory += [key, location, 1, value]
+    return directory, [float(radius), float(radius)], ""
+
+
 def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
 
@@ -294,6 +308,51 @@ class Device:
                                        None if win is None else C.c_void_p(win.ctypes.data),
                                        b.memory, _stream(b.memory)))
         return heights
+
+    GEOTIFF_COMPRESSION = {"none": 0, "lzw": 1, "deflate": 3}
+
+    def geotiff_write(self, path, bands, grid, nodata=None, geokeys=None,
+                      compression: str = "lzw", tile_size: int = 256, big_tiff: bool = False):
+        """WriteGeoTiff (src/raster/geotiff/geotiff_write.cpp): `bands` (one raster or a list,
+        float32 host arrays or CUDA tensors of grid.height x grid.width) as a tiled float32
+        GeoTIFF at `path`. `grid` is a GridSpec or (width, height, GDAL-order transform);
+        `nodata` None, NaN or a value; `geokeys` None or (directory, doubles, ascii) as
+        geographic_sphere_keys gives them; compression "none", "lzw" (the reference's default)
+        or "deflate". The tiles are encoded on the device."""
+        if not isinstance(bands, (list, tuple)):
+            bands = [bands]
+        b = _Buffers()
+        ptrs = [b.ptr(x, np.float32) for x in bands]
+        if isinstance(grid, GridSpec):
+            g = grid.native()
+        else:
+            width, height, t = grid
+            g = N.Grid(int(width), int(height), *[float(v) for v in t])
+        for x in bands:
+            if tuple(x.shape) != (g.height, g.width):
+                raise ValueError(f"band shape {tuple(x.shape)} is not the grid's "
+                                 f"{(g.height, g.width)}")
+        table = (C.c_void_p * len(ptrs))(*ptrs)
+        if nodata is None:
+            nd = N.NoData(0, 0.0)
+        elif np.isnan(nodata):
+            nd = N.NoData(1, 0.0)
+        else:
+            nd = N.NoData(2, float(nodata))
+        keys = None
+        if geokeys is not None:
+            directory, doubles, ascii_ = geokeys
+            d = np.ascontiguousarray(directory, np.uint16)
+            dp = np.ascontiguousarray(doubles, np.float64)
+            b.keep.extend([d, dp])
+            keys = N.GeoKeys(C.c_void_p(d.ctypes.data), len(d), len(dp),
+                             C.c_void_p(dp.ctypes.data), (ascii_ or "").encode())
+        opts = N.GeotiffOptions(self.GEOTIFF_COMPRESSION[compression], tile_size,
+                                int(big_tiff), 0)
+        N.check(self._lib.tg_geotiff_write(self._handle, str(path).encode(),
+                                           C.cast(table, C.c_void_p), len(ptrs), C.byref(g), nd,
+                                           None if keys is None else C.byref(keys),
+                                           C.byref(opts), b.memory, _stream(b.memory)))
 
     def seam_samples(self, earlier, later, grid: GridSpec, col0: int, row0: int, lw: int,
                      lh: int, data=None, difference=None, nodata=(1, 0.0)):
