@@ -204,6 +204,16 @@ __global__ void __launch_bounds__(kShapeThreads)
     }
     const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
     const bool anyLive = live[0] || live[1] || live[2] || live[3];
+    // The warp's 4 x 32 cell centers as a box (axis-aligned grids): a crater whose cull circle
+    // misses it, with a quarter cell to spare for rounding, needs none of the warp's cells, and
+    // the warp passes it over at once (the same decision in every lane).
+    const bool boxTest = grid.rowRotation == 0.0 && grid.colRotation == 0.0;
+    const double boxX = grid.originX + (double(binX * kBinCells) + 16.0) * grid.pixelWidth;
+    const double boxY = grid.originY + (double(binY * kBinCells + warp * 4u) + 2.0) * grid.pixelHeight;
+    const float boxXh = float(boxX), boxXl = float(boxX - double(boxXh));
+    const float boxYh = float(boxY), boxYl = float(boxY - double(boxYh));
+    const float halfW = 15.75f * float(fabs(grid.pixelWidth));
+    const float halfH = 1.75f * float(fabs(grid.pixelHeight));
 
     // Evaluates the 32 (or, at a flush, `n`) queued pairs from `from`, one per lane.
     auto drain = [&](const BinEntry* chunk, uint32_t from, uint32_t n) {
@@ -277,6 +287,15 @@ __global__ void __launch_bounds__(kShapeThreads)
         for (uint32_t e = 0; e < n; ++e) {
             const BinEntry& entry = stage[s][e];
             const CraterRecord& r = entry.record;
+            if (boxTest) {
+                const float gx = fmaxf(
+                    fabsf(crater::split_difference(boxXh, boxXl, r.x, r.xLow)) - halfW, 0.0f);
+                const float gy = fmaxf(
+                    fabsf(crater::split_difference(boxYh, boxYl, r.y, r.yLow)) - halfH, 0.0f);
+                if (gx * gx + gy * gy >= entry.cull * entry.cull) {
+                    continue;  // warp-uniform
+                }
+            }
             const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
                                 tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
                                 tileY <= int(entry.tileY1);
