@@ -98,7 +98,9 @@ def test_served_source_within_1mm_of_fp64(device):
 
 def test_served_budget_defers_admission(device):
     # 40 tiles of 1025^2 (42M cells) under a 0.6 GB budget: batches are cut by the budget, not by
-    # max_batch_cells, and every request still completes.
+    # max_batch_cells, and every request still completes. The stream runs twice: on the second
+    # pass every region is resident when the requests arrive, so the first batch sees all 40
+    # waiting whatever the timing of the region builds.
     from terraingen_b200.device import GridSpec
     from terraingen_b200.serve import Req, Server, dem_stack_options, run_stream
 
@@ -107,9 +109,11 @@ def test_served_budget_defers_admission(device):
             for i in range(40)]
     opts = dem_stack_options(slots=2, budget_gb=0.6, max_batch_cells=1 << 40)
     with Server(device, opts) as s:
+        run_stream(s, [Req(r.rid + len(reqs), 0.0, r.kind, grid=r.grid) for r in reqs],
+                   realtime=False)
         res = run_stream(s, reqs, realtime=False)
         st = s.stats()
-    assert st["completed"] == len(reqs)
+    assert st["completed"] == 2 * len(reqs)
     assert st["deferred"] > 0 and st["batches"] >= 2
     assert sum(len(v) for v in res.latency_ms.values()) == len(reqs)
 
