@@ -225,6 +225,7 @@ struct DistanceWarps {
 };
 
 constexpr int kDistanceWarps = 4;  // warps of a distance block
+constexpr int kGroup = 16;         // steps of a pass run between reads of their operands
 
 template <bool kCarried, bool kSharedRows>
 __global__ void __launch_bounds__(32 * kDistanceWarps)
@@ -268,12 +269,27 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                 next = (cw0 >> 5) + 1 < int(p.pitch) ? p.bits[rowBits + uint32_t(cw0 >> 5) + 1]
                                                      : 0u;
             }
-            // Lane 0's row above: columns c - 1, c, c + 1 and the next one.
-            float aL = inf, aU = inf, aR = lane == 0 && ww > 0 ? rowF[0] : inf;
-            float bL = 0.0f, bU = 0.0f, bR = kCarried && lane == 0 && ww > 0 ? rowC[0] : 0.0f;
             float* out = store + size_t(max(band, 0)) * steps * 32;
             float* outC = storeC + size_t(max(band, 0)) * steps * 32;
-            for (int t = 0; t < steps; ++t) {
+            for (int t0 = 0; t0 < steps; t0 += kGroup) {
+            // Lane 0's row above over the group's columns t0 - 1 .. t0 + kGroup, read at once
+            // (lane 31 of this band writes only columns left of them meanwhile).
+            float above[kGroup + 2], aboveC[kGroup + 2];
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i < kGroup + 2; ++i) {
+                    const int col = t0 - 1 + i;
+                    const bool in = col >= 0 && col < ww;
+                    above[i] = in ? rowF[col] : inf;
+                    if (kCarried) aboveC[i] = in ? rowC[col] : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                const int t = t0 + u;
+                if (t >= steps) {
+                    break;
+                }
                 const int c = t - 2 * lane;
                 float uR = __shfl_up_sync(0xffffffffu, h1, 1);
                 float uU = __shfl_up_sync(0xffffffffu, h2, 1);
@@ -285,19 +301,13 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                     vL = __shfl_up_sync(0xffffffffu, g3, 1);
                 }
                 if (lane == 0) {
-                    aL = aU;
-                    aU = aR;
-                    aR = c + 1 < ww ? rowF[c + 1] : inf;
-                    uL = aL;
-                    uU = aU;
-                    uR = aR;
+                    uL = above[u];
+                    uU = above[u + 1];
+                    uR = above[u + 2];
                     if (kCarried) {
-                        bL = bU;
-                        bU = bR;
-                        bR = c + 1 < ww ? rowC[c + 1] : 0.0f;
-                        vL = bL;
-                        vU = bU;
-                        vR = bR;
+                        vL = aboveC[u];
+                        vU = aboveC[u + 1];
+                        vR = aboveC[u + 2];
                     }
                 }
                 float d = inf, car = 0.0f;
@@ -351,6 +361,7 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                     if (kCarried) outC[size_t(t) * 32 + lane] = car;
                 }
             }
+            }
             __syncwarp();
         }
         // Backward, bands bottom up over the tile's rows and the halo below; lane 0 is a band's
@@ -372,12 +383,44 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                 word = p.bits[rowBits + uint32_t(last >> 5)];
                 next = (last >> 5) > 0 ? p.bits[rowBits + uint32_t(last >> 5) - 1] : 0u;
             }
-            float aL = lane == 0 && ww > 0 ? rowF[ww - 1] : inf, aU = inf, aR = inf;
-            float bL = kCarried && lane == 0 && ww > 0 ? rowC[ww - 1] : 0.0f, bU = 0.0f, bR = 0.0f;
             const float* in = store + size_t(band) * steps * 32;
             const float* inC = storeC + size_t(band) * steps * 32;
             const bool tileRow = active && row < tr1;
-            for (int t = 0; t < steps; ++t) {
+            // The forward values of a group's steps are loaded a group ahead (they come from L2).
+            float cur[kGroup], curC[kGroup];
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                const size_t at = size_t(ww + 61 - u) * 32 + uint32_t(31 - lane);
+                cur[u] = u < steps ? in[at] : inf;
+                if (kCarried) curC[u] = u < steps ? inC[at] : 0.0f;
+            }
+            for (int t0 = 0; t0 < steps; t0 += kGroup) {
+            float nxt[kGroup], nxtC[kGroup];
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                const int t = t0 + kGroup + u;
+                const size_t at = size_t(ww + 61 - t) * 32 + uint32_t(31 - lane);
+                nxt[u] = t < steps ? in[at] : inf;
+                if (kCarried) nxtC[u] = t < steps ? inC[at] : 0.0f;
+            }
+            // Lane 0's row below over the group's columns ww - t0 down to ww - t0 - kGroup - 1
+            // (lane 31 writes only columns right of them meanwhile).
+            float below[kGroup + 2], belowC[kGroup + 2];
+            if (lane == 0) {
+#pragma unroll
+                for (int i = 0; i < kGroup + 2; ++i) {
+                    const int col = ww - t0 - i;
+                    const bool ok = col >= 0 && col < ww;
+                    below[i] = ok ? rowF[col] : inf;
+                    if (kCarried) belowC[i] = ok ? rowC[col] : 0.0f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                const int t = t0 + u;
+                if (t >= steps) {
+                    break;
+                }
                 const int c = ww - 1 - t + 2 * lane;
                 float dL = __shfl_up_sync(0xffffffffu, h1, 1);
                 float dD = __shfl_up_sync(0xffffffffu, h2, 1);
@@ -389,22 +432,15 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                     eR = __shfl_up_sync(0xffffffffu, g3, 1);
                 }
                 if (lane == 0) {
-                    aR = aU;
-                    aU = aL;
-                    aL = c - 1 >= 0 ? rowF[c - 1] : inf;
-                    dL = aL;
-                    dD = aU;
-                    dR = aR;
+                    dR = below[u];
+                    dD = below[u + 1];
+                    dL = below[u + 2];
                     if (kCarried) {
-                        bR = bU;
-                        bU = bL;
-                        bL = c - 1 >= 0 ? rowC[c - 1] : 0.0f;
-                        eL = bL;
-                        eD = bU;
-                        eR = bR;
+                        eR = belowC[u];
+                        eD = belowC[u + 1];
+                        eL = belowC[u + 2];
                     }
                 }
-                const size_t stored = size_t(ww + 61 - t) * 32 + uint32_t(31 - lane);
                 float d = inf, car = 0.0f;
                 if (active && c >= 0 && c < ww) {
                     const int x = cw0 + c;
@@ -412,8 +448,8 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                         word = next;
                         next = (x >> 5) > 0 ? p.bits[rowBits + uint32_t(x >> 5) - 1] : 0u;
                     }
-                    d = in[stored];
-                    if (kCarried) car = inC[stored];
+                    d = cur[u];
+                    if (kCarried) car = curC[u];
                     const bool has = (word >> (x & 31)) & 1u;
                     if (!has) {
                         float s = h1 + p.dx;
@@ -469,6 +505,12 @@ __global__ void __launch_bounds__(32 * kDistanceWarps)
                     g2 = g1;
                     g1 = car;
                 }
+            }
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                cur[u] = nxt[u];
+                if (kCarried) curC[u] = nxtC[u];
+            }
             }
             __syncwarp();
         }
