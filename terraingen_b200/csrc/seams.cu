@@ -52,26 +52,38 @@ constexpr size_t kScratchBytes = size_t(1) << 30;  // the distance warps' stored
 // 32 j .. 32 j + 31 (bit = column % 32), `pitch` = ceil(w / 32) words a row, the bits past the
 // last column 0.
 
-constexpr int kBandRows = 64;  // rows of a band warp's span
+constexpr int kBandRows = 16;  // rows of a band warp's span
 
 __device__ __forceinline__ uint32_t row_tail_mask(uint32_t j, uint32_t pitch, uint32_t w) {
     return j + 1 == pitch && (w & 31u) != 0 ? (1u << (w & 31u)) - 1u : 0xffffffffu;
 }
 
-// Which posts have data, one bit each, and how many have.
+// Which posts have data, one bit each, and how many have. A warp packs 8 words per pass, their
+// 8 loads in flight together.
+constexpr uint32_t kPackWords = 8;
+
 __global__ void pack_data_kernel(const uint8_t* __restrict__ data, uint32_t w, uint32_t h,
                                  uint32_t pitch, uint32_t* __restrict__ bits,
                                  unsigned long long* __restrict__ count) {
     const uint32_t lane = threadIdx.x & 31u;
-    const size_t words = size_t(pitch) * h;
-    const size_t warps = size_t(gridDim.x) * (blockDim.x >> 5);
+    const uint32_t words = pitch * h;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     uint32_t mine = 0;
-    for (size_t q = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; q < words; q += warps) {
-        const uint32_t row = uint32_t(q / pitch), col = uint32_t(q % pitch) * 32u + lane;
-        const bool has = col < w && data[size_t(row) * w + col] != 0;
-        const uint32_t word = __ballot_sync(0xffffffffu, has);
-        if (lane == 0) {
-            bits[q] = word;
+    for (uint32_t q0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kPackWords; q0 < words;
+         q0 += warps * kPackWords) {
+        uint8_t v[kPackWords];
+#pragma unroll
+        for (uint32_t k = 0; k < kPackWords; ++k) {
+            const uint32_t q = q0 + k;
+            const uint32_t row = q / pitch, col = (q % pitch) * 32u + lane;
+            v[k] = q < words && col < w ? data[size_t(row) * w + col] : uint8_t(0);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kPackWords; ++k) {
+            const uint32_t word = __ballot_sync(0xffffffffu, v[k] != 0);
+            if (lane == k && q0 + k < words) {
+                bits[q0 + k] = word;
+            }
             mine += __popc(word);
         }
     }
@@ -1648,9 +1660,10 @@ int tg_seam_solve(tg_device* d, const uint8_t* data, const float* difference, ui
     TG_CUDA(wk.count.reserve(8), "allocation");
     TG_CUDA(cudaMemsetAsync(wk.count.ptr, 0, 8, s), "memset");
     uint32_t* bits = static_cast<uint32_t*>(wk.bits.ptr);
-    pack_data_kernel<<<uint32_t(std::min<size_t>(blocks_for(words * 32), size_t(sms) * 16)), 256,
-                       0, s>>>(dData, width, height, pitch, bits,
-                               static_cast<unsigned long long*>(wk.count.ptr));
+    pack_data_kernel<<<uint32_t(std::min<size_t>(
+                           blocks_for((words + kPackWords - 1) / kPackWords * 32), size_t(sms) * 8)),
+                       256, 0, s>>>(dData, width, height, pitch, bits,
+                                    static_cast<unsigned long long*>(wk.count.ptr));
     unsigned long long withData = 0;
     TG_CUDA(cudaMemcpyAsync(&withData, wk.count.ptr, 8, cudaMemcpyDeviceToHost, s), "copy");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
