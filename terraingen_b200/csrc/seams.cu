@@ -28,6 +28,7 @@
 #include <cstddef>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "../../include/tgb200.h"
@@ -771,10 +772,18 @@ __device__ __forceinline__ bool stopped(const CgState* cg) {
     return cg != nullptr && cg->done != 0u;
 }
 
+// The start of a kernel launched by pdl_launch: wait for the kernels before it, then let the
+// next one launch (a no-op for a plain launch).
+__device__ __forceinline__ void pdl_begin() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Damped Jacobi: xn = x + omega (b - A x) / diagonal; from x = 0 when `x` is null.
 template <int kOrder, typename T>
 __global__ void jacobi_kernel(const LevelView L, const T* __restrict__ b, const T* __restrict__ x,
                               T* __restrict__ xn, double omega, const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= L.n || stopped(cg)) {
         return;
@@ -791,6 +800,7 @@ __global__ void jacobi_kernel(const LevelView L, const T* __restrict__ b, const 
 template <int kOrder, typename T>
 __global__ void residual_kernel(const LevelView L, const T* __restrict__ b,
                                 const T* __restrict__ x, T* __restrict__ r, const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < L.n && !stopped(cg)) {
         r[k] = b[k] - apply_at<kOrder, T, T>(L, x, k);
@@ -803,6 +813,7 @@ __global__ void residual_kernel(const LevelView L, const T* __restrict__ b,
 template <typename Tf, typename Tc>
 __global__ void restrict_kernel(const LevelView F, const LevelView Cl, const Tf* __restrict__ r,
                                 Tc* __restrict__ b, const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= Cl.n || stopped(cg)) {
         return;
@@ -827,6 +838,7 @@ __global__ void restrict_kernel(const LevelView F, const LevelView Cl, const Tf*
 template <typename Tc, typename Tf>
 __global__ void prolong_kernel(const LevelView F, const LevelView Cl, const Tc* __restrict__ xc,
                                Tf* __restrict__ x, const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= F.n || stopped(cg)) {
         return;
@@ -868,6 +880,7 @@ __device__ __forceinline__ void block_partials(double x, double y, double* __res
 __global__ void dot_kernel(const double* __restrict__ a, const double* __restrict__ b,
                            const double* __restrict__ c, const double* __restrict__ d, uint32_t n,
                            double* __restrict__ partial, const CgState* cg) {
+    pdl_begin();
     if (stopped(cg)) {
         return;
     }
@@ -886,6 +899,7 @@ template <int kOrder>
 __global__ void apply_dot_kernel(const LevelView L, const double* __restrict__ p,
                                  double* __restrict__ ap, double* __restrict__ partial,
                                  const CgState* cg) {
+    pdl_begin();
     if (stopped(cg)) {
         return;
     }
@@ -903,6 +917,7 @@ __global__ void apply_dot_kernel(const LevelView L, const double* __restrict__ p
 __global__ void precondition_dots_kernel(const double* __restrict__ r,
                                          const float* __restrict__ z, uint32_t n,
                                          double* __restrict__ partial, const CgState* cg) {
+    pdl_begin();
     if (stopped(cg)) {
         return;
     }
@@ -925,6 +940,7 @@ enum Then { kThenNothing = 0, kThenStep = 1, kThenNext = 2 };
 //     ratio (seam_field.cpp:532-542).
 __global__ void finish_kernel(const double* __restrict__ partial, double* __restrict__ out,
                               CgState* cg, int then) {
+    pdl_begin();
     if (stopped(cg)) {
         return;
     }
@@ -969,6 +985,7 @@ __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
                                  const double* __restrict__ p, const double* __restrict__ ap,
                                  uint32_t n, float* __restrict__ b0, float* __restrict__ x0,
                                  float scale, const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
         const double step = cg->step;
@@ -989,6 +1006,7 @@ __global__ void cg_update_kernel(double* __restrict__ x, double* __restrict__ r,
 template <typename T>
 __global__ void cg_direction_kernel(double* __restrict__ p, const T* __restrict__ z, uint32_t n,
                                     const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
         p[k] = double(z[k]) + cg->ratio * p[k];
@@ -1004,6 +1022,7 @@ __global__ void __launch_bounds__(1024) coarsest_kernel(const LevelView L,
                                                         const double* __restrict__ b,
                                                         double* __restrict__ x, double omega,
                                                         int sweeps, const CgState* cg) {
+    pdl_begin();
     if (stopped(cg)) {
         return;
     }
@@ -1033,6 +1052,7 @@ __global__ void __launch_bounds__(1024) coarsest_kernel(const LevelView L,
 template <typename A, typename B>
 __global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, uint32_t n,
                                const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
         out[k] = B(in[k]);
@@ -1042,6 +1062,7 @@ __global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, ui
 template <typename T>
 __global__ void copy_kernel(const T* __restrict__ in, T* __restrict__ out, uint32_t n,
                             const CgState* cg) {
+    pdl_begin();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n && !stopped(cg)) {
         out[k] = in[k];
@@ -1297,6 +1318,41 @@ int compact(Work& wk, Level& level, uint32_t w, uint32_t h, uint32_t pitch, cuda
     return TG_OK;
 }
 
+// Launches with programmatic dependent launch: the next kernel of the stream may start before
+// this one ends; every kernel launched this way begins with pdl_begin(), which waits for the
+// kernels before it (their writes visible) and lets the next one launch.
+template <typename... K, typename... A>
+cudaError_t pdl_launch(void (*kernel)(K...), dim3 grid, dim3 block, size_t shared,
+                       cudaStream_t stream, A&&... args) {
+    cudaLaunchConfig_t config{};
+    config.gridDim = grid;
+    config.blockDim = block;
+    config.dynamicSmemBytes = shared;
+    config.stream = stream;
+    cudaLaunchAttribute attribute[1];
+    attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attribute[0].val.programmaticStreamSerializationAllowed = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+    return cudaLaunchKernelEx(&config, kernel, std::forward<A>(args)...);
+}
+
+#define TG_PDL(...)                                          \
+    do {                                                     \
+        const cudaError_t e_ = pdl_launch(__VA_ARGS__);      \
+        if (e_ != cudaSuccess) {                             \
+            return ::tgb::api::cuda_fail(e_, "launch");      \
+        }                                                    \
+    } while (0)
+
+#define TG_PDL_E(...)                                        \
+    do {                                                     \
+        const cudaError_t e_ = pdl_launch(__VA_ARGS__);      \
+        if (e_ != cudaSuccess) {                             \
+            return e_;                                       \
+        }                                                    \
+    } while (0)
+
 struct Solver {
     Work* wk;
     int levels;
@@ -1316,11 +1372,11 @@ template <int kOrder>
 cudaError_t jacobi(const Solver& sv, const LevelView& L, const void* b, const void* x, void* xn,
                    bool coarsest) {
     if (coarsest) {
-        jacobi_kernel<kOrder, double><<<blocks_for(L.n), 256, 0, sv.s>>>(
+        TG_PDL_E(jacobi_kernel<kOrder, double>, blocks_for(L.n), 256, 0, sv.s,
             L, static_cast<const double*>(b), static_cast<const double*>(x),
             static_cast<double*>(xn), sv.omega, sv.cg);
     } else {
-        jacobi_kernel<kOrder, float><<<blocks_for(L.n), 256, 0, sv.s>>>(
+        TG_PDL_E(jacobi_kernel<kOrder, float>, blocks_for(L.n), 256, 0, sv.s,
             L, static_cast<const float*>(b), static_cast<const float*>(x),
             static_cast<float*>(xn), sv.omega, sv.cg);
     }
@@ -1329,10 +1385,12 @@ cudaError_t jacobi(const Solver& sv, const LevelView& L, const void* b, const vo
 
 cudaError_t copy_level(const Solver& sv, const void* from, void* to, uint32_t n, bool wide) {
     if (wide) {
-        copy_kernel<double><<<blocks_for(n), 256, 0, sv.s>>>(static_cast<const double*>(from),
+        TG_PDL_E(copy_kernel<double>, blocks_for(n), 256, 0, sv.s,
+            static_cast<const double*>(from),
                                                             static_cast<double*>(to), n, sv.cg);
     } else {
-        copy_kernel<float><<<blocks_for(n), 256, 0, sv.s>>>(static_cast<const float*>(from),
+        TG_PDL_E(copy_kernel<float>, blocks_for(n), 256, 0, sv.s,
+            static_cast<const float*>(from),
                                                            static_cast<float*>(to), n, sv.cg);
     }
     return cudaGetLastError();
@@ -1358,7 +1416,7 @@ int vcycle(Solver& sv, int d, int smoothed = 0) {
     const int sweeps = last ? sv.coarsest : sv.sweeps;
     if (last && smoothed == 0 && L.view.n <= kCoarsestBlockPosts) {
         const uint32_t threads = std::min<uint32_t>(1024, (L.view.n + 31) / 32 * 32);
-        coarsest_kernel<kOrder><<<1, threads, size_t(L.view.n) * 16, sv.s>>>(
+        TG_PDL(coarsest_kernel<kOrder>, 1, threads, size_t(L.view.n) * 16, sv.s,
             L.view, static_cast<const double*>(L.b.ptr), static_cast<double*>(L.x.ptr),
             sv.omega, sweeps, sv.cg);
         TG_CUDA(cudaGetLastError(), "coarsest launch");
@@ -1376,15 +1434,15 @@ int vcycle(Solver& sv, int d, int smoothed = 0) {
     Level& C = sv.wk->levels[d + 1];
     const bool coarseLast = d + 2 == sv.levels;
     // residual into t, restricted into the coarse b
-    residual_kernel<kOrder, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+    TG_PDL(residual_kernel<kOrder, float>, blocks_for(L.view.n), 256, 0, sv.s,
         L.view, static_cast<const float*>(L.b.ptr), static_cast<const float*>(L.x.ptr),
         static_cast<float*>(L.t.ptr), sv.cg);
     if (coarseLast) {
-        restrict_kernel<float, double><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
+        TG_PDL(restrict_kernel<float, double>, blocks_for(C.view.n), 256, 0, sv.s,
             L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<double*>(C.b.ptr),
             sv.cg);
     } else {
-        restrict_kernel<float, float><<<blocks_for(C.view.n), 256, 0, sv.s>>>(
+        TG_PDL(restrict_kernel<float, float>, blocks_for(C.view.n), 256, 0, sv.s,
             L.view, C.view, static_cast<const float*>(L.t.ptr), static_cast<float*>(C.b.ptr),
             sv.cg);
     }
@@ -1393,11 +1451,11 @@ int vcycle(Solver& sv, int d, int smoothed = 0) {
         return st;
     }
     if (coarseLast) {
-        prolong_kernel<double, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+        TG_PDL(prolong_kernel<double, float>, blocks_for(L.view.n), 256, 0, sv.s,
             L.view, C.view, static_cast<const double*>(C.x.ptr), static_cast<float*>(L.x.ptr),
             sv.cg);
     } else {
-        prolong_kernel<float, float><<<blocks_for(L.view.n), 256, 0, sv.s>>>(
+        TG_PDL(prolong_kernel<float, float>, blocks_for(L.view.n), 256, 0, sv.s,
             L.view, C.view, static_cast<const float*>(C.x.ptr), static_cast<float*>(L.x.ptr),
             sv.cg);
     }
@@ -1426,12 +1484,12 @@ int precondition(Solver& sv, const double* r, double* z) {
         TG_CUDA(copy_level(sv, L0.x.ptr, z, n, true), "copy");
         return TG_OK;
     }
-    convert_kernel<double, float><<<blocks_for(n), 256, 0, sv.s>>>(
+    TG_PDL(convert_kernel<double, float>, blocks_for(n), 256, 0, sv.s,
         r, static_cast<float*>(L0.b.ptr), n, sv.cg);
     if (int st = vcycle<kOrder>(sv, 0)) {
         return st;
     }
-    convert_kernel<float, double><<<blocks_for(n), 256, 0, sv.s>>>(
+    TG_PDL(convert_kernel<float, double>, blocks_for(n), 256, 0, sv.s,
         static_cast<const float*>(L0.x.ptr), z, n, sv.cg);
     TG_CUDA(cudaGetLastError(), "convert launch");
     return TG_OK;
@@ -1441,9 +1499,11 @@ int precondition(Solver& sv, const double* r, double* z) {
 cudaError_t dots(const Solver& sv, const double* a, const double* b, const double* c,
                  const double* d, uint32_t n, double* out, CgState* cg = nullptr,
                  int then = kThenNothing) {
-    dot_kernel<<<kDotBlocks, 256, 0, sv.s>>>(a, b, c, d, n,
+    TG_PDL_E(dot_kernel, kDotBlocks, 256, 0, sv.s,
+        a, b, c, d, n,
                                              static_cast<double*>(sv.wk->partial.ptr), sv.cg);
-    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(static_cast<const double*>(sv.wk->partial.ptr),
+    TG_PDL_E(finish_kernel, 1, kDotBlocks, 0, sv.s,
+        static_cast<const double*>(sv.wk->partial.ptr),
                                               out, cg, then);
     return cudaGetLastError();
 }
@@ -1465,30 +1525,37 @@ int iteration(Solver& sv, CgState* cg) {
     double* ap = static_cast<double*>(wk.cgAp.ptr);
     double* z = static_cast<double*>(wk.cgZ.ptr);
     double* partial = static_cast<double*>(wk.partial.ptr);
-    apply_dot_kernel<kOrder><<<kDotBlocks, 256, 0, sv.s>>>(L0.view, p, ap, partial, cg);
-    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(partial, cg_dots(cg), cg, kThenStep);
+    TG_PDL(apply_dot_kernel<kOrder>, kDotBlocks, 256, 0, sv.s,
+        L0.view, p, ap, partial, cg);
+    TG_PDL(finish_kernel, 1, kDotBlocks, 0, sv.s,
+        partial, cg_dots(cg), cg, kThenStep);
     if (sv.levels == 1) {
-        cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(x, r, p, ap, n, nullptr, nullptr, 0.0f,
+        TG_PDL(cg_update_kernel, blocks_for(n), 256, 0, sv.s,
+            x, r, p, ap, n, nullptr, nullptr, 0.0f,
                                                           cg);
         if (int st = precondition<kOrder>(sv, r, z)) {
             return st;
         }
         TG_CUDA(dots(sv, r, r, r, z, n, cg_dots(cg), cg, kThenNext), "dot launch");
-        cg_direction_kernel<double><<<blocks_for(n), 256, 0, sv.s>>>(p, z, n, cg);
+        TG_PDL(cg_direction_kernel<double>, blocks_for(n), 256, 0, sv.s,
+            p, z, n, cg);
         TG_CUDA(cudaGetLastError(), "iteration launch");
         return TG_OK;
     }
     const float scale = float(sv.omega / L0.view.diagonal);
-    cg_update_kernel<<<blocks_for(n), 256, 0, sv.s>>>(
+    TG_PDL(cg_update_kernel, blocks_for(n), 256, 0, sv.s,
         x, r, p, ap, n, static_cast<float*>(L0.b.ptr),
         static_cast<float*>(first_sweep_target(L0, sv.sweeps)), scale, cg);
     if (int st = vcycle<kOrder>(sv, 0, 1)) {
         return st;
     }
     const float* z0 = static_cast<const float*>(L0.x.ptr);
-    precondition_dots_kernel<<<kDotBlocks, 256, 0, sv.s>>>(r, z0, n, partial, cg);
-    finish_kernel<<<1, kDotBlocks, 0, sv.s>>>(partial, cg_dots(cg), cg, kThenNext);
-    cg_direction_kernel<float><<<blocks_for(n), 256, 0, sv.s>>>(p, z0, n, cg);
+    TG_PDL(precondition_dots_kernel, kDotBlocks, 256, 0, sv.s,
+        r, z0, n, partial, cg);
+    TG_PDL(finish_kernel, 1, kDotBlocks, 0, sv.s,
+        partial, cg_dots(cg), cg, kThenNext);
+    TG_PDL(cg_direction_kernel<float>, blocks_for(n), 256, 0, sv.s,
+        p, z0, n, cg);
     TG_CUDA(cudaGetLastError(), "iteration launch");
     return TG_OK;
 }
