@@ -156,6 +156,20 @@ def seam(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: i
             "field": field[:n].reshape(shape), "ms": ms.value}
 
 
+def write_crater_list(lib: C.CDLL, path, x, y, diameter, age, ids, manual, replace,
+                      json: bool) -> None:
+    """The reference's WriteCraterList (tgref_write_crater_list) without attributes."""
+    cols = [np.ascontiguousarray(v, np.float64) for v in (x, y, diameter, age)]
+    i = np.ascontiguousarray(ids, np.uint64)
+    m = np.ascontiguousarray(manual, np.uint8)
+    r = np.ascontiguousarray(replace, np.uint8)
+    st = lib.tgref_write_crater_list(str(path).encode(), *[c.ctypes.data for c in cols],
+                                     i.ctypes.data, m.ctypes.data, r.ctypes.data, len(i),
+                                     int(json))
+    if st != 0:
+        raise RuntimeError(f"tgref_write_crater_list failed: {lib.tgref_error().decode()}")
+
+
 COMPRESSION = {"none": 0, "lzw": 1, "packbits": 2, "deflate": 3}  # TiffCompression's order
 
 
@@ -307,6 +321,11 @@ def _harness(name: str) -> C.CDLL:
         lib.tgref_write_geotiff.argtypes = [C.c_char_p, P, _U32, _U32, _U32, P, C.c_int, C.c_float,
                                             P, _U32, P, _U32, C.c_char_p, C.c_int, _U32, C.c_int]
         lib.tgref_write_geotiff.restype = C.c_int
+    if hasattr(lib, "tgref_write_crater_list"):
+        P = C.c_void_p
+        lib.tgref_write_crater_list.argtypes = [C.c_char_p, P, P, P, P, P, P, P, C.c_size_t,
+                                                C.c_int]
+        lib.tgref_write_crater_list.restype = C.c_int
     return lib
 
 

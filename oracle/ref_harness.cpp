@@ -600,6 +600,7 @@ int tgref_datum_relief(const void* kernel, const void* records, const float* dat
 }  // extern "C"
 
 #include "terraingen/raster/geotiff/geotiff.h"
+#include "terraingen/io/feature_lists.h"
 
 extern "C" {
 
@@ -643,6 +644,32 @@ int tgref_write_geotiff(const char* path, const float* const* bands, uint32_t ba
         } else {
             WriteGeoTiff(path, rasters, keys, options);
         }
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// WriteCraterList (src/io/feature_lists.cpp:395) of n craters given column by column, without
+/// attributes; `json` picks ListFormat::Json over Csv.
+int tgref_write_crater_list(const char* path, const double* x, const double* y,
+                            const double* diameter, const double* age, const uint64_t* id,
+                            const uint8_t* manual, const uint8_t* replace, size_t n, int json) {
+    try {
+        CraterList list;
+        for (size_t i = 0; i < n; ++i) {
+            Crater c;
+            c.x = x[i];
+            c.y = y[i];
+            c.diameter = diameter[i];
+            c.ageGyr = age[i];
+            c.id = id[i];
+            c.manual = manual[i] != 0;
+            c.replace = replace[i] != 0;
+            list.Append(c);
+        }
+        WriteCraterList(list, path, json ? ListFormat::Json : ListFormat::Csv, {});
         return 0;
     } catch (const std::exception& error) {
         g_error = error.what();

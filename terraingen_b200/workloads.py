@@ -53,6 +53,24 @@ def crater_population(seed: int, coefficient: float, dmin: float, dmax: float,
                         margin_radii=0.0, min_resolved_diameter=0.0)
 
 
+def generate_craters(population: N.Population, region) -> dict:
+    """The craters `population` draws over `region` (x0, y0, x1, y1 in meters) in the
+    reference's order (tg_crater_generate): x, y, diameter, age (Gyr) and id arrays."""
+    lib = N.library()
+    reg = np.ascontiguousarray(region, np.float64)
+    count = C.c_size_t()
+    N.check(lib.tg_crater_generate(C.byref(population), reg.ctypes.data, None, None, None, None,
+                                   None, 0, C.byref(count)))
+    n = count.value
+    out = {k: np.empty(n, np.float64) for k in ("x", "y", "diameter", "age")}
+    out["id"] = np.empty(n, np.uint64)
+    N.check(lib.tg_crater_generate(C.byref(population), reg.ctypes.data,
+                                   *[out[k].ctypes.data for k in ("x", "y", "diameter", "age",
+                                                                  "id")],
+                                   n, C.byref(count)))
+    return out
+
+
 def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
                  irregular: int = 1):
     """(kernel, records, data, footprints) a crater layer hands the kernel for `grid`."""
