@@ -148,6 +148,19 @@ int tg_craters_apply_lists(tg_device* device, const void* kernel, size_t kernel_
                            uint32_t first_row, float* heights, tg_nodata nodata, int memory,
                            void* stream);
 
+/* The body form of the same kernel (craters.slang's branch for tiles[2] == 1: ShapeCratersOnBody,
+ * include/terraingen/layers/kernels/craters.h:1360): `frames` holds the 52-byte CraterFrame of
+ * each record, `points` the strip's cells as 24-byte SplitPoints (width x rows, positions on the
+ * body, Surface::Position split), and each crater reads a cell in its frame (BodySplitOffset,
+ * craters.h:208: the offset on the crater's tangent plane, azimuthal equidistant on a sphere).
+ * Craters apply in list order, datums included. */
+int tg_craters_apply_body(tg_device* device, const void* kernel, size_t kernel_bytes,
+                          const void* records, uint32_t n, const float* data, uint32_t n_data,
+                          const void* frames, const uint32_t* heads, uint32_t n_heads,
+                          const uint32_t* entries, uint32_t n_entries, const void* points,
+                          uint32_t width, uint32_t rows, uint32_t first_row, float* heights,
+                          tg_nodata nodata, int memory, void* stream);
+
 
 /* --- boulders ----------------------------------------------------------------------------- */
 

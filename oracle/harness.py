@@ -40,7 +40,7 @@ class Scene(C.Structure):
         ("rimSigma", _D), ("terraceOnset", _D), ("terraceFull", _D),
         ("boulders", _I32), ("boulderSeed", _U32), ("boulderCoefficient", _D),
         ("boulderExponent", _D), ("boulderMin", _D), ("boulderMax", _D), ("heightRatio", _D),
-        ("datum", _I32), ("interiorReplacement", _D),
+        ("datum", _I32), ("interiorReplacement", _D), ("bodyRadius", _D),
     ]
 
 

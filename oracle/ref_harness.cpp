@@ -84,6 +84,9 @@ struct tgref_scene {
     // share of the interior they replace
     int32_t datum;
     double interiorReplacement;
+    // a sphere of this radius (m) when positive, the grid's transform then in degrees of
+    // longitude and latitude; a plane when 0
+    double bodyRadius;
 };
 
 const char* tgref_error() {
@@ -98,7 +101,7 @@ std::vector<Fractal> Stack(const Fractal* fractals, uint32_t count) {
     return std::vector<Fractal>(fractals, fractals + count);
 }
 
-std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s) {
+std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s, TerrainBase base = {}) {
     auto density = std::make_shared<PowerLawSfd>(s.sfdCoefficient, s.sfdExponent, SfdKind::Density,
                                                   DiameterRange{s.minDiameter, s.maxDiameter});
     CraterModels models;
@@ -149,7 +152,7 @@ std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s) {
         options.apply.terraces.onsetDiameter = s.terraceOnset;
         options.apply.terraces.fullDiameter = s.terraceFull;
     }
-    return std::make_shared<CraterLayer>(std::move(models), std::move(options));
+    return std::make_shared<CraterLayer>(std::move(models), std::move(options), std::move(base));
 }
 
 std::shared_ptr<BoulderLayer> MakeBoulderLayer(const tgref_scene& s) {
@@ -169,6 +172,20 @@ std::shared_ptr<BoulderLayer> MakeBoulderLayer(const tgref_scene& s) {
 
 Terrain MakeTerrain(const tgref_scene& s, bool withBoulders = true) {
     std::shared_ptr<const Source> source;
+    if (s.bodyRadius > 0.0) {
+        // A flat site on a sphere: the grid in degrees, the craters on the body.
+        const Surface surface = Surface::Sphere(s.bodyRadius);
+        const Vec2d center{s.transform[0] + 0.5 * s.width * s.transform[1],
+                           s.transform[3] + 0.5 * s.height * s.transform[5]};
+        source = std::make_shared<FlatSource>(s.width, s.height,
+                                              std::fabs(s.transform[1]) * surface.UnitLength(),
+                                              s.elevation, center, surface);
+        std::vector<LayerPtr> layers;
+        if (s.craters != 0) {
+            layers.push_back(MakeCraterLayer(s, TerrainBase{surface, source}));
+        }
+        return Terrain(surface, source, layers);
+    }
     if (s.source == 1) {
         source = std::make_shared<SyntheticSource>(Stack(s.sourceStack, s.sourceFractals),
                                                    s.elevation);
@@ -752,6 +769,29 @@ int tg_craters_apply_lists(tg_device*, const void* kernel, size_t kernelBytes, c
                 Bytes(xLows, width),
                 Bytes(ys, rows),
                 Bytes(yLows, size_t(firstRow) + rows),
+                Bytes(heights, size_t(width) * rows)};
+    c.width = width;
+    c.rows = rows;
+    c.firstRow = firstRow;
+    c.nodata = nodata;
+    g_captures.push_back(std::move(c));
+    return TG_OK;
+}
+
+int tg_craters_apply_body(tg_device*, const void* kernel, size_t kernelBytes, const void* records,
+                          uint32_t n, const float* data, uint32_t nData, const void* frames,
+                          const uint32_t* heads, uint32_t nHeads, const uint32_t* entries,
+                          uint32_t nEntries, const void* points, uint32_t width, uint32_t rows,
+                          uint32_t firstRow, float* heights, tg_nodata nodata, int, void*) {
+    Capture c;
+    c.kind = 4;
+    c.fields = {Bytes(static_cast<const unsigned char*>(kernel), kernelBytes),
+                Bytes(static_cast<const unsigned char*>(records), size_t(n) * 144),
+                Bytes(data, nData),
+                Bytes(heads, nHeads),
+                Bytes(entries, nEntries),
+                Bytes(static_cast<const unsigned char*>(frames), size_t(n) * 52),
+                Bytes(static_cast<const unsigned char*>(points), size_t(width) * rows * 24),
                 Bytes(heights, size_t(width) * rows)};
     c.width = width;
     c.rows = rows;

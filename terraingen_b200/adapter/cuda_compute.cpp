@@ -125,6 +125,22 @@ void CudaCompute::Run(const KernelProgram& program, Span<const DeviceBuffer> buf
         // heights, xs, ys, CraterShapeKernel, records, data, tiles, entries, frames, points,
         // lows (src/layers/kernels/craters.slang, bound by ShapeTilesOnGpu, apply.cpp:174-196)
         float* heights = reinterpret_cast<float*>(buffers[0].output);
+        const std::uint32_t* tiles = As<std::uint32_t>(buffers[6]);
+        if (Count<std::uint32_t>(buffers[6]) >= 3 && tiles[2] != 0u) {
+            // On a body: the craters' frames and the strip's cells as split points
+            // (ShapeCratersOnBody, craters.slang's body branch).
+            if (tg_craters_apply_body(
+                    m_state->device, buffers[3].bytes.data(), buffers[3].bytes.size(),
+                    buffers[4].bytes.data(), Count<CraterRecord>(buffers[4]),
+                    As<float>(buffers[5]), Count<float>(buffers[5]), buffers[8].bytes.data(),
+                    tiles, Count<std::uint32_t>(buffers[6]), As<std::uint32_t>(buffers[7]),
+                    Count<std::uint32_t>(buffers[7]), buffers[9].bytes.data(), params.width,
+                    params.rows, params.firstRow, heights, nodata, TG_MEMORY_HOST,
+                    nullptr) != TG_OK) {
+                Throw("craters on a body");
+            }
+            return;
+        }
         const float* lows = As<float>(buffers[10]);
         if (tg_craters_apply_lists(
                 m_state->device, buffers[3].bytes.data(), buffers[3].bytes.size(),

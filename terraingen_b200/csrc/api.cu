@@ -706,6 +706,91 @@ int tg_craters_apply_lists(tg_device* d, const void* kernel, size_t kernel_bytes
     return copy_heights_back(d, memory, heights, dh, cells);
 }
 
+int tg_craters_apply_body(tg_device* d, const void* kernel, size_t kernel_bytes,
+                          const void* records, uint32_t n, const float* data, uint32_t n_data,
+                          const void* frames, const uint32_t* heads, uint32_t n_heads,
+                          const uint32_t* entries, uint32_t n_entries, const void* points,
+                          uint32_t width, uint32_t rows, uint32_t first_row, float* heights,
+                          tg_nodata nodata, int memory, void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (kernel == nullptr || kernel_bytes != sizeof(CraterShapeKernel)) {
+        return fail(TG_ERROR_ARGUMENT, "CraterShapeKernel is %zu bytes", sizeof(CraterShapeKernel));
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    if (int s = check_nodata(nodata)) {
+        return s;
+    }
+    const size_t cells = size_t(width) * rows;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (heads == nullptr || n_heads < 3 || entries == nullptr || n_entries == 0 ||
+        heights == nullptr || points == nullptr || (n > 0 && frames == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "tile lists, frames, points and heights are required");
+    }
+    if (memory == TG_MEMORY_HOST) {
+        const uint32_t tilesX = heads[0], side = heads[1];
+        if (side == 0 || tilesX == 0 || tilesX < (width + side - 1) / side ||
+            n_heads < 3 + 2 * tilesX * ((first_row + rows + side - 1) / side)) {
+            return fail(TG_ERROR_ARGUMENT, "tile heads do not cover the strip");
+        }
+        for (uint32_t t = 3; t + 1 < n_heads; t += 2) {
+            if (uint64_t(heads[t]) + heads[t + 1] > n_entries) {
+                return fail(TG_ERROR_ARGUMENT, "tile list past the entries");
+            }
+        }
+        for (uint32_t e = 0; e < n_entries; ++e) {
+            if (entries[e] >= n && !(n == 0 && e == 0)) {
+                return fail(TG_ERROR_ARGUMENT, "entry %u names crater %u of %u", e, entries[e], n);
+            }
+        }
+    }
+    CraterShapeKernel k;
+    std::memcpy(&k, kernel, sizeof(k));
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void *drec, *dframes, *ddata, *dheads, *dentries, *dpoints;
+    if (int st = stage_in(d, memory, kRecords, records, size_t(n) * sizeof(CraterRecord), &drec, 16)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kFrames, frames, size_t(n) * sizeof(CraterFrame), &dframes)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kData, data, size_t(n_data) * sizeof(float), &ddata)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kHeads, heads, size_t(n_heads) * sizeof(uint32_t), &dheads)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kEntries, entries, size_t(n_entries) * sizeof(uint32_t),
+                          &dentries)) {
+        return st;
+    }
+    if (int st = stage_in(d, memory, kPoints, points, cells * sizeof(SplitPoint), &dpoints)) {
+        return st;
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+        TG_CUDA(cudaMemcpyAsync(dh, heights, cells * sizeof(float), cudaMemcpyHostToDevice, s),
+                "copy to device");
+    }
+    TG_CUDA(launch_crater_shape_body(k, static_cast<const CraterRecord*>(drec),
+                                     static_cast<const CraterFrame*>(dframes),
+                                     static_cast<const float*>(ddata),
+                                     static_cast<const uint32_t*>(dheads),
+                                     static_cast<const uint32_t*>(dentries), width, rows,
+                                     first_row, static_cast<const SplitPoint*>(dpoints),
+                                     to_nodata(nodata), dh, s),
+            "crater body launch");
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
 int tg_boulders_bake(tg_device* d, const void* boulders, uint32_t n, double width,
                      const tg_grid* grid, float* heights, tg_nodata nodata, int memory,
                      void* stream) {

@@ -85,6 +85,8 @@ enum Slot {
     kProbeIn,
     kProbeHashes,
     kProbeValues,
+    kFrames,
+    kPoints,
     kSlotCount
 };
 

@@ -429,6 +429,51 @@ __global__ void crater_shape_lists_kernel(const CraterShapeKernel k,
     heights[i] = height;
 }
 
+// The same on a body (ShapeCratersOnBody, craters.h:1360; craters.slang's body branch): each
+// cell's position is a split point in 3D and each crater is read in its frame, the offset
+// projected on the crater's tangent plane (azimuthal equidistant on a sphere, KernelFrameOffset).
+__global__ void crater_shape_body_kernel(const CraterShapeKernel k,
+                                         const CraterRecord* __restrict__ records,
+                                         const CraterFrame* __restrict__ frames,
+                                         const float* __restrict__ data,
+                                         const uint32_t* __restrict__ heads,
+                                         const uint32_t* __restrict__ entries, uint32_t width,
+                                         uint32_t rows, uint32_t firstRow,
+                                         const SplitPoint* __restrict__ points,
+                                         const NoData nodata, float* __restrict__ heights) {
+    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= width || r >= rows) {
+        return;
+    }
+    const size_t i = size_t(r) * width + col;
+    float height = heights[i];
+    if (is_nodata(nodata, height)) {
+        return;
+    }
+    const uint32_t row = firstRow + r;
+    const uint32_t side = heads[1];
+    const uint32_t head = 3u + 2u * ((row / side) * heads[0] + col / side);
+    const uint32_t first = heads[head], n = heads[head + 1];
+    const SplitPoint p = points[i];
+    for (uint32_t e = first; e < first + n; ++e) {
+        const uint32_t m = entries[e];
+        const CraterRecord& c = records[m];
+        const CraterFrame& f = frames[m];
+        const crater::Offset at =
+            crater::frame_offset(f, crater::split_difference(p.x, p.xLow, f.x, f.xLow),
+                                 crater::split_difference(p.y, p.yLow, f.y, f.yLow),
+                                 crater::split_difference(p.z, p.zLow, f.z, f.zLow));
+        const crater::Contribution q = crater::crater_contribution(k, data, c, at.dx, at.dy);
+        if (!q.reached) {
+            continue;
+        }
+        height = c.hasDatum == 1u ? crater::apply_with_datum(c, q, height, at.dx, at.dy)
+                                  : height + q.shaped;
+    }
+    heights[i] = height;
+}
+
 // --- exclusive scan ------------------------------------------------------------------------
 
 constexpr uint32_t kScanBlock = 1024;
@@ -586,6 +631,20 @@ cudaError_t launch_crater_shape_lists(const CraterShapeKernel& k, const CraterRe
     crater_shape_lists_kernel<<<blocks, block, 0, stream>>>(k, records, data, heads, entries,
                                                             width, rows, firstRow, xs, xLows, ys,
                                                             yLows, nodata, heights);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_shape_body(const CraterShapeKernel& k, const CraterRecord* records,
+                                     const CraterFrame* frames, const float* data,
+                                     const uint32_t* heads, const uint32_t* entries,
+                                     uint32_t width, uint32_t rows, uint32_t firstRow,
+                                     const SplitPoint* points, const NoData& nodata,
+                                     float* heights, cudaStream_t stream) {
+    const dim3 block(16, 16);
+    const dim3 grid((width + 15) / 16, (rows + 15) / 16);
+    crater_shape_body_kernel<<<grid, block, 0, stream>>>(k, records, frames, data, heads, entries,
+                                                         width, rows, firstRow, points, nodata,
+                                                         heights);
     return cudaGetLastError();
 }
 

@@ -105,6 +105,14 @@ cudaError_t launch_crater_shape_lists(const CraterShapeKernel& k, const CraterRe
                                       const float* ys, const float* yLows, NoData nodata,
                                       float* heights, cudaStream_t stream);
 
+// The body form: each cell's position a split point in 3D, each crater read in its frame.
+cudaError_t launch_crater_shape_body(const CraterShapeKernel& k, const CraterRecord* records,
+                                     const CraterFrame* frames, const float* data,
+                                     const uint32_t* heads, const uint32_t* entries,
+                                     uint32_t width, uint32_t rows, uint32_t firstRow,
+                                     const SplitPoint* points, const NoData& nodata,
+                                     float* heights, cudaStream_t stream);
+
 // --- boulders ------------------------------------------------------------------------------
 // One boulder drawn as a dome (tg_boulder in include/tgb200.h).
 struct BoulderRecord {

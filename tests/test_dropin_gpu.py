@@ -41,3 +41,23 @@ def test_noise_layer_through_reference_pipeline(dropin, noise_fixture):
     scene = H.make_scene(g, source_fractals=src, layer_fractals=lay)
     gpu, _ = H.evaluate(dropin, scene, 1, 1)
     assert np.array_equal(gpu.view(np.uint32), noise_fixture["layer_expected"].view(np.uint32))
+
+
+def test_craters_on_a_body_through_reference_pipeline(dropin):
+    # A site on a sphere of the Moon's radius: the reference dispatches its crater kernel with
+    # frames and split points (ShapeCratersOnBody); the adapter runs tg_craters_apply_body.
+    import importlib.util
+
+    from conftest import GOLDEN
+
+    spec = importlib.util.spec_from_file_location("body_cases", GOLDEN / "body_cases.py")
+    cases = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cases)
+    want = np.load(GOLDEN / "body.npz")["expected"]
+    scene = cases.scene()
+    cpu, _ = H.evaluate(dropin, scene, 0, 1)
+    gpu, _ = H.evaluate(dropin, scene, 1, 1)
+    assert np.array_equal(cpu.view(np.uint32), want.view(np.uint32))
+    assert np.count_nonzero(want) > 5000
+    err = np.abs(gpu.astype(np.float64) - cpu)
+    assert err.max() <= 1e-3, err.max()
