@@ -59,6 +59,8 @@ SIGNATURES = {
                          _P],
     "tg_craters_apply_lists": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _P, _P,
                                _P, _U32, _U32, _U32, _P, NoData, _I, _P],
+    "tg_craters_apply_body": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _P, _U32, _P, _U32, _P, _U32,
+                              _U32, _U32, _P, NoData, _I, _P],
 }
 
 class Population(C.Structure):
