@@ -109,6 +109,17 @@ int tg_noise_layer_rows(tg_device* device, const void* kernel, size_t kernel_byt
 int tg_noise_source(tg_device* device, const void* fractals, uint32_t count, float elevation,
                     const tg_grid* grid, float* heights, int memory, void* stream);
 
+/* SyntheticSource without posts on a sphere of `radius` meters: the grid is in degrees of
+ * longitude (x) and latitude (y), and heights = elevation + the stacked `fractals` evaluated in 3D
+ * at each cell center's position on the sphere (SyntheticSource::NoiseAt with FractalStackAt on a
+ * body, src/noise/surface_noise.cpp:14-17: EvaluateFractals3 and Fractal3,
+ * include/terraingen/noise/fractal.h:284, with lattice points split in double). The reference
+ * runs this only on the CPU. Bit-exact with it: the cosines and sines of each column's longitude
+ * and each row's latitude are taken on the host as the reference's UnitVector takes them. */
+int tg_noise_source_body(tg_device* device, const void* fractals, uint32_t count,
+                         float elevation, const tg_grid* grid, double radius, float* heights,
+                         int memory, void* stream);
+
 /* Conformance probe, the analogue of the reference's GPU test kernel
  * (tests/unit/gpu/kernels/noise_conformance.slang): for each of `n` points (x, y) in `xy`,
  * hashes[4i..4i+3] = PcgHash(i), Pcg3dHash(bits(x), bits(y), seed), and values[12i..12i+11] =

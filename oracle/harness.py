@@ -156,6 +156,18 @@ def seam(lib: C.CDLL, earlier: np.ndarray, later: np.ndarray, transform, mode: i
             "field": field[:n].reshape(shape), "ms": ms.value}
 
 
+def body_noise(lib: C.CDLL, fractals, elevation: float, radius: float, grid) -> np.ndarray:
+    """The reference's SyntheticSource heights on a sphere (tgref_body_noise) for `grid`
+    (terraingen_b200.GridSpec in degrees)."""
+    fr = np.ascontiguousarray(np.atleast_1d(fractals))
+    t = np.ascontiguousarray(grid.transform(), np.float64)
+    out = np.zeros((grid.height, grid.width), np.float32)
+    if lib.tgref_body_noise(fr.ctypes.data, len(fr), elevation, radius, grid.width, grid.height,
+                            t.ctypes.data, out.ctypes.data) != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return out
+
+
 def write_crater_list(lib: C.CDLL, path, x, y, diameter, age, ids, manual, replace,
                       json: bool) -> None:
     """The reference's WriteCraterList (tgref_write_crater_list) without attributes."""
@@ -321,6 +333,10 @@ def _harness(name: str) -> C.CDLL:
         lib.tgref_write_geotiff.argtypes = [C.c_char_p, P, _U32, _U32, _U32, P, C.c_int, C.c_float,
                                             P, _U32, P, _U32, C.c_char_p, C.c_int, _U32, C.c_int]
         lib.tgref_write_geotiff.restype = C.c_int
+    if hasattr(lib, "tgref_body_noise"):
+        lib.tgref_body_noise.argtypes = [C.c_void_p, _U32, C.c_float, _D, _U32, _U32, C.c_void_p,
+                                         C.c_void_p]
+        lib.tgref_body_noise.restype = C.c_int
     if hasattr(lib, "tgref_write_crater_list"):
         P = C.c_void_p
         lib.tgref_write_crater_list.argtypes = [C.c_char_p, P, P, P, P, P, P, P, C.c_size_t,

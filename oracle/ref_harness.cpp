@@ -618,6 +618,7 @@ int tgref_datum_relief(const void* kernel, const void* records, const float* dat
 
 #include "terraingen/raster/geotiff/geotiff.h"
 #include "terraingen/io/feature_lists.h"
+#include "terraingen/noise/surface_noise.h"
 
 extern "C" {
 
@@ -660,6 +661,30 @@ int tgref_write_geotiff(const char* path, const float* const* bands, uint32_t ba
             WriteGeoTiff(path, rasters.front(), keys, options);
         } else {
             WriteGeoTiff(path, rasters, keys, options);
+        }
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
+/// SyntheticSource::NoiseAt on a sphere: elevation + FractalStackAt (src/noise/surface_noise.cpp)
+/// at each cell center of a width x height grid in degrees (GDAL-order `transform`).
+int tgref_body_noise(const void* fractals, uint32_t count, float elevation, double radius,
+                     uint32_t width, uint32_t height, const double* transform, float* out) {
+    try {
+        const Surface surface = Surface::Sphere(radius);
+        std::vector<Fractal> stack(static_cast<const Fractal*>(fractals),
+                                   static_cast<const Fractal*>(fractals) + count);
+        const GeoTransform t = GeoTransform::FromGdal(
+            {transform[0], transform[1], transform[2], transform[3], transform[4], transform[5]});
+        for (uint32_t row = 0; row < height; ++row) {
+            for (uint32_t col = 0; col < width; ++col) {
+                const Vec2d p = t.PixelToWorld(double(col) + 0.5, double(row) + 0.5);
+                out[size_t(row) * width + col] =
+                    elevation + FractalStackAt(stack, {}, surface, p.x, p.y);
+            }
         }
         return 0;
     } catch (const std::exception& error) {

@@ -55,6 +55,7 @@ SIGNATURES = {
     "tg_noise_layer_rows": [_P, _P, _SZ, _P, _P, _U32, _U32, _P, NoData, _I, _P],
     "tg_noise_source": [_P, _P, _U32, _F, C.POINTER(Grid), _P, _I, _P],
     "tg_noise_probe": [_P, _P, _U32, _U32, _P, _P, _I],
+    "tg_noise_source_body": [_P, _P, _U32, _F, C.POINTER(Grid), _D, _P, _I, _P],
     "tg_craters_apply": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, C.POINTER(Grid), _P, NoData, _I,
                          _P],
     "tg_craters_apply_lists": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _P, _P,

@@ -367,6 +367,78 @@ int tg_noise_source(tg_device* d, const void* fractals, uint32_t count, float el
                      stream);
 }
 
+int tg_noise_source_body(tg_device* d, const void* fractals, uint32_t count, float elevation,
+                         const tg_grid* grid, double radius, float* heights, int memory,
+                         void* stream) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (count > kMaxFractals || (count > 0 && fractals == nullptr)) {
+        return fail(TG_ERROR_ARGUMENT, "at most %u fractals, and a pointer to them",
+                    kMaxFractals);
+    }
+    if (!(radius > 0.0) || !std::isfinite(radius)) {
+        return fail(TG_ERROR_ARGUMENT, "a sphere's radius must be positive and finite");
+    }
+    Grid g;
+    if (int s = to_grid(grid, g)) {
+        return s;
+    }
+    if (int s = check_memory(memory)) {
+        return s;
+    }
+    FractalStack stack;
+    std::memset(&stack, 0, sizeof(stack));
+    std::memcpy(stack.fractals, fractals, count * sizeof(Fractal));
+    stack.count = count;
+    if (int s = check_stack(stack)) {
+        return s;
+    }
+    const size_t cells = size_t(g.width) * g.height;
+    if (cells == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr) {
+        return fail(TG_ERROR_ARGUMENT, "heights is null");
+    }
+    // Cell centers in degrees as Raster::CellCenter gives them (GeoTransform::PixelToWorld, the
+    // rotation terms 0), their cosines and sines with the host's libm as the reference's
+    // UnitVector takes them (surface.cpp:45-50).
+    constexpr double kPi = 3.141592653589793238462643383279502884;
+    constexpr double kDegree = kPi / 180.0;
+    std::vector<double> trig(2 * size_t(g.width) + 2 * size_t(g.height));
+    for (uint32_t col = 0; col < g.width; ++col) {
+        const double lon = (g.originX + (double(col) + 0.5) * g.pixelWidth + 0.5 * g.rowRotation) *
+                           kDegree;
+        trig[2 * col] = std::cos(lon);
+        trig[2 * col + 1] = std::sin(lon);
+    }
+    double* latTrig = trig.data() + 2 * size_t(g.width);
+    for (uint32_t row = 0; row < g.height; ++row) {
+        const double lat =
+            (g.originY + 0.5 * g.colRotation + (double(row) + 0.5) * g.pixelHeight) * kDegree;
+        latTrig[2 * row] = std::cos(lat);
+        latTrig[2 * row + 1] = std::sin(lat);
+    }
+    const cudaStream_t s = stream_of(d, memory, stream);
+    const void* dtrig = nullptr;
+    if (int st = stage_in(d, TG_MEMORY_HOST, kProbeIn, trig.data(), trig.size() * sizeof(double),
+                          &dtrig)) {
+        return st;
+    }
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
+        dh = slot_ptr<float>(d, kHeights);
+    }
+    const double* dl = static_cast<const double*>(dtrig);
+    TG_CUDA(launch_noise_body(stack, elevation, g.width, g.height, dl, dl + 2 * size_t(g.width),
+                              radius, dh, s),
+            "body noise launch");
+    return copy_heights_back(d, memory, heights, dh, cells);
+}
+
 int tg_noise_probe(tg_device* d, const float* xy, uint32_t n, uint32_t seed, uint32_t* hashes,
                    float* values, int memory) {
     if (int s = check_device(d)) {

@@ -42,6 +42,12 @@ cudaError_t launch_noise(const FractalStack& stack, const Grid& grid, const Posi
 
 // Conformance probe (the reference's tests/unit/gpu/kernels/noise_conformance.slang analogue):
 // for each input point, the PCG hashes and basis/fractal values, for testing against the oracle.
+// A SyntheticSource on a sphere: `lons` / `lats` hold (cos, sin) of each column's longitude and
+// each row's latitude.
+cudaError_t launch_noise_body(const FractalStack& stack, float elevation, uint32_t width,
+                              uint32_t height, const double* lons, const double* lats,
+                              double radius, float* heights, cudaStream_t stream);
+
 cudaError_t launch_noise_probe(const float* xy, uint32_t n, uint32_t seed, uint32_t* hashes,
                                float* values, cudaStream_t stream);
 

@@ -209,6 +209,41 @@ __global__ void noise_probe_kernel(const float* __restrict__ xy, uint32_t n, uin
 
 }  // namespace
 
+// A SyntheticSource on a sphere (SyntheticSource::NoiseAt with FractalStackAt on a body,
+// surface_noise.cpp:14-17): each cell center's position R (cos lat cos lon, cos lat sin lon,
+// sin lat) (UnitVector, surface.cpp:45), from the host's cosines and sines of each column's
+// longitude and each row's latitude, then the stack in 3D.
+__global__ void noise_body_kernel(const FractalStack stack, float elevation, uint32_t width,
+                                  uint32_t height, const double* __restrict__ lons,
+                                  const double* __restrict__ lats, double radius,
+                                  float* __restrict__ heights) {
+    const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+    if (col >= width || row >= height) {
+        return;
+    }
+    const double cosLon = lons[2 * col], sinLon = lons[2 * col + 1];
+    const double cosLat = lats[2 * row], sinLat = lats[2 * row + 1];
+    const double x = cosLat * cosLon * radius;
+    const double y = cosLat * sinLon * radius;
+    const double z = sinLat * radius;
+    heights[size_t(row) * width + col] =
+        elevation + noise::evaluate_stack3(x, y, z, stack.fractals, stack.count);
+}
+
+cudaError_t launch_noise_body(const FractalStack& stack, float elevation, uint32_t width,
+                              uint32_t height, const double* lons, const double* lats,
+                              double radius, float* heights, cudaStream_t stream) {
+    if (width == 0 || height == 0) {
+        return cudaSuccess;
+    }
+    const dim3 block(32, 4);
+    const dim3 grid((width + 31) / 32, (height + 3) / 4);
+    noise_body_kernel<<<grid, block, 0, stream>>>(stack, elevation, width, height, lons, lats,
+                                                  radius, heights);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_noise(const FractalStack& stack, const Grid& grid, const Positions& at,
                          bool fill, float elevation, NoData nodata, float* heights,
                          cudaStream_t stream) {

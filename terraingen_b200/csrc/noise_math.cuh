@@ -476,5 +476,275 @@ __device__ __forceinline__ float evaluate_stack(float x, float y, const Fractal*
     return height;
 }
 
+// --- 3D noise on a body (the reference runs it only on the CPU) ---------------------------------
+
+// A lattice cell and fraction split in double precision (SplitLatticePrecise3, lattice.h:59).
+struct Cell3 {
+    int32_t ix, iy, iz;
+    float fx, fy, fz;
+};
+
+__device__ __forceinline__ Cell3 split3_precise(double x, double y, double z) {
+    const double cx = floor(x), cy = floor(y), cz = floor(z);
+    return Cell3{int32_t(int64_t(cx)), int32_t(int64_t(cy)), int32_t(int64_t(cz)),
+                 float(x - cx), float(y - cy), float(z - cz)};
+}
+
+// PerlinNoise3 at a cell (perlin.h:113-128): corner keys (x, y, z + pcg(seed)).
+__device__ __forceinline__ float perlin3_cell(const Cell3& c, uint32_t seed) {
+    const uint32_t key = pcg(seed);
+    const uint32_t ix = uint32_t(c.ix), iy = uint32_t(c.iy), iz = uint32_t(c.iz);
+    float k[8];
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        const uint32_t dx = corner & 1u, dy = (corner >> 1u) & 1u, dz = corner >> 2u;
+        const uint32_t h = pcg3d(U3{ix + dx, iy + dy, iz + dz + key}).x;
+        k[corner] = gradient3(h, c.fx - float(dx), c.fy - float(dy), c.fz - float(dz));
+    }
+    const float u = fade(c.fx), v = fade(c.fy), w = fade(c.fz);
+    const float near = lerp(v, lerp(u, k[0], k[1]), lerp(u, k[2], k[3]));
+    const float far = lerp(v, lerp(u, k[4], k[5]), lerp(u, k[6], k[7]));
+    return sclamp(lerp(w, near, far), -1.0f, 1.0f);
+}
+
+// One corner of a 3D simplex (SimplexCorner3, simplex.h:27).
+__device__ __forceinline__ float simplex_corner3(uint32_t ci, uint32_t cj, uint32_t ck, float dx,
+                                                 float dy, float dz, uint32_t key) {
+    const float t = 0.5f - dx * dx - dy * dy - dz * dz;
+    if (t <= 0.0f) {
+        return 0.0f;
+    }
+    const float t2 = t * t;
+    return t2 * t2 * gradient3(pcg3d(U3{ci, cj, ck + key}).x, dx, dy, dz);
+}
+
+// SimplexNoise3 at a cell (simplex.h:72-115).
+__device__ __forceinline__ float simplex3_cell(const Cell3& c, uint32_t seed) {
+    const uint32_t key = pcg(seed);
+    const int32_t cellSum = int32_t(uint32_t(c.ix) + uint32_t(c.iy) + uint32_t(c.iz));
+    int32_t third = cellSum / 3;
+    if (cellSum - 3 * third < 0) {
+        third -= 1;
+    }
+    const float remainder = float(cellSum - 3 * third);
+    const float skew = (remainder + c.fx + c.fy + c.fz) / 3.0f;
+    const float stepX = floorf(c.fx + skew);
+    const float stepY = floorf(c.fy + skew);
+    const float stepZ = floorf(c.fz + skew);
+    const float unskew = (remainder + stepX + stepY + stepZ) / 6.0f;
+    const float x0 = c.fx - stepX + unskew;
+    const float y0 = c.fy - stepY + unskew;
+    const float z0 = c.fz - stepZ + unskew;
+    const uint32_t i1 = x0 >= y0 && x0 >= z0 ? 1u : 0u;
+    const uint32_t j1 = y0 > x0 && y0 >= z0 ? 1u : 0u;
+    const uint32_t k1 = z0 > x0 && z0 > y0 ? 1u : 0u;
+    const uint32_t i2 = x0 >= y0 || x0 >= z0 ? 1u : 0u;
+    const uint32_t j2 = y0 > x0 || y0 >= z0 ? 1u : 0u;
+    const uint32_t k2 = z0 > x0 || z0 > y0 ? 1u : 0u;
+    const float kUnskew = 1.0f / 6.0f;
+    const float x1 = x0 - float(i1) + kUnskew;
+    const float y1 = y0 - float(j1) + kUnskew;
+    const float z1 = z0 - float(k1) + kUnskew;
+    const float x2 = x0 - float(i2) + 2.0f * kUnskew;
+    const float y2 = y0 - float(j2) + 2.0f * kUnskew;
+    const float z2 = z0 - float(k2) + 2.0f * kUnskew;
+    const float x3 = x0 - 1.0f + 3.0f * kUnskew;
+    const float y3 = y0 - 1.0f + 3.0f * kUnskew;
+    const float z3 = z0 - 1.0f + 3.0f * kUnskew;
+    const uint32_t i = uint32_t(c.ix) + uint32_t(third) + uint32_t(int32_t(stepX));
+    const uint32_t j = uint32_t(c.iy) + uint32_t(third) + uint32_t(int32_t(stepY));
+    const uint32_t k = uint32_t(c.iz) + uint32_t(third) + uint32_t(int32_t(stepZ));
+    const float sum = simplex_corner3(i, j, k, x0, y0, z0, key) +
+                      simplex_corner3(i + i1, j + j1, k + k1, x1, y1, z1, key) +
+                      simplex_corner3(i + i2, j + j2, k + k2, x2, y2, z2, key) +
+                      simplex_corner3(i + 1u, j + 1u, k + 1u, x3, y3, z3, key);
+    return sclamp(76.0f * sum, -1.0f, 1.0f);
+}
+
+// ValueNoise3 at a cell (value.h:57-74): corner keys (x, y, z ^ pcg(seed)).
+__device__ __forceinline__ float value3_cell(const Cell3& c, uint32_t seed) {
+    const uint32_t key = pcg(seed);
+    float v[8];
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        const U3 at{uint32_t(c.ix) + (corner & 1u), uint32_t(c.iy) + ((corner >> 1u) & 1u),
+                    (uint32_t(c.iz) + (corner >> 2u)) ^ key};
+        v[corner] = 2.0f * unit(pcg3d(at).y) - 1.0f;
+    }
+    const float u = fade(c.fx), w = fade(c.fz), vv = fade(c.fy);
+    const float near = lerp(vv, lerp(u, v[0], v[1]), lerp(u, v[2], v[3]));
+    const float far = lerp(vv, lerp(u, v[4], v[5]), lerp(u, v[6], v[7]));
+    return lerp(w, near, far);
+}
+
+// The squared gap from the fraction `f` to cell offset `d` (CellGapSquared, worley.h:24).
+__device__ __forceinline__ float cell_gap2(int32_t d, float f) {
+    float gap = 0.0f;
+    if (d > 0) {
+        gap = float(d) - f;
+    } else if (d < 0) {
+        gap = f - float(d + 1);
+    }
+    return gap * gap;
+}
+
+// Worley3 at a cell (worley.h:75-110): the 3 x 3 x 3 cells first, then the outer shell of the
+// 5 x 5 x 5 where it can still hold the second nearest point; cell keys (x ^ pcg(seed), y, z).
+__device__ __forceinline__ WorleyD worley3_cell(const Cell3& c, uint32_t seed) {
+    const uint32_t seedKey = pcg(seed);
+    float d1 = 1e30f, d2 = 1e30f;
+    uint32_t nearest = 0u;
+    for (int32_t shell = 0; shell < 2; ++shell) {
+        for (int32_t dz = -2; dz <= 2; ++dz) {
+            for (int32_t dy = -2; dy <= 2; ++dy) {
+                for (int32_t dx = -2; dx <= 2; ++dx) {
+                    const bool inner = abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1;
+                    if (inner != (shell == 0)) {
+                        continue;
+                    }
+                    if (shell == 1 &&
+                        cell_gap2(dx, c.fx) + cell_gap2(dy, c.fy) + cell_gap2(dz, c.fz) >= d2) {
+                        continue;
+                    }
+                    const U3 h = pcg3d(U3{uint32_t(c.ix + dx) ^ seedKey, uint32_t(c.iy + dy),
+                                          uint32_t(c.iz + dz)});
+                    const float px = float(dx) + unit(h.x) - c.fx;
+                    const float py = float(dy) + unit(h.y) - c.fy;
+                    const float pz = float(dz) + unit(h.z) - c.fz;
+                    const float d = px * px + py * py + pz * pz;
+                    if (d < d1) {
+                        d2 = d1;
+                        d1 = d;
+                        nearest = pcg(h.x ^ h.y ^ h.z);
+                    } else if (d < d2) {
+                        d2 = d;
+                    }
+                }
+            }
+        }
+    }
+    return WorleyD{sqrtf(d1), sqrtf(d2), 2.0f * unit(nearest) - 1.0f};
+}
+
+// One octave of any 3D basis (BasisNoise3, fractal.h:115).
+__device__ __forceinline__ float basis3(uint32_t basis, const Cell3& c, uint32_t seed) {
+    const float kInvSqrt3 = 0.577350269189625765f;
+    const float kInvSqrt6 = 0.408248290463863016f;
+    switch (basis) {
+    case kBasisSimplex:
+        return simplex3_cell(c, seed);
+    case kBasisValue:
+        return value3_cell(c, seed);
+    case kBasisWorleyF1:
+        return 2.0f * smin(worley3_cell(c, seed).f1 * kInvSqrt3, 1.0f) - 1.0f;
+    case kBasisWorleyF2:
+        return 2.0f * smin(worley3_cell(c, seed).f2 * kInvSqrt6, 1.0f) - 1.0f;
+    case kBasisWorleyF2MinusF1: {
+        const WorleyD d = worley3_cell(c, seed);
+        return 2.0f * smin((d.f2 - d.f1) * kInvSqrt6, 1.0f) - 1.0f;
+    }
+    case kBasisVoronoi:
+        return worley3_cell(c, seed).value;
+    default:
+        return perlin3_cell(c, seed);
+    }
+}
+
+// The golden-angle turn about (1, 2, 3) / sqrt(14) in double (Fractal3, fractal.h:286-289).
+__device__ __constant__ const double kTurn3d[3][3] = {
+    {-0.6132711010727254, -0.293401570821183, 0.7333580809050306},
+    {0.7897926788435601, -0.24097777005594262, 0.5640542870894418},
+    {0.011228581128535142, 0.9251190369776896, 0.37951111497202883}};
+
+// Fractal3 (fractal.h:284-316): world coordinates in double, each octave's lattice point split
+// in double before narrowing.
+__device__ __forceinline__ float fractal3(double x, double y, double z, const FractalParams& p) {
+    double frequency = 1.0 / double(p.wavelength);
+    double t[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+    Sums s = sums_start();
+    for (int o = 0; o < p.octaves; ++o) {
+        const U3 h = pcg3d(U3{p.seed, uint32_t(o), 0u});
+        const U3 g = pcg3d(U3{p.seed, uint32_t(o), 1u});
+        const double rx = t[0][0] * x + t[0][1] * y + t[0][2] * z;
+        const double ry = t[1][0] * x + t[1][1] * y + t[1][2] * z;
+        const double rz = t[2][0] * x + t[2][1] * y + t[2][2] * z;
+        const double px = rx * frequency + double(unit(h.y));
+        const double py = ry * frequency + double(unit(h.z));
+        const double pz = rz * frequency + double(unit(g.x));
+        const float n = basis3(p.basis, split3_precise(px, py, pz), h.x);
+        s = add_octave(s, p.type, p.gain, p.offset, o, n);
+        frequency *= double(p.lacunarity);
+        double next[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                next[r][c] = kTurn3d[r][0] * t[0][c] + kTurn3d[r][1] * t[1][c] +
+                             kTurn3d[r][2] * t[2][c];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                t[r][c] = next[r][c];
+            }
+        }
+    }
+    return finish(s, p.type, p.amplitude, p.offset);
+}
+
+// EvaluateFractal3 with DomainWarp3 (fractals.h:218-243).
+__device__ __forceinline__ float evaluate_fractal3(double x, double y, double z, const Fractal& f) {
+    FractalParams unitp = params_of(f);
+    unitp.amplitude = 1.0f;
+    if (f.warpAmplitude > 0.0f) {
+        FractalParams warp{pcg(f.seed ^ TGB_WARP_SALT), f.warpWavelength, f.warpAmplitude, 4, 2.0f,
+                           0.5f, kBasisPerlin, kTypeFbm, 1.0f};
+        const double dx = double(fractal3(x, y, z, warp));
+        warp.seed = pcg(warp.seed);
+        const double dy = double(fractal3(x, y, z, warp));
+        warp.seed = pcg(warp.seed);
+        const double dz = double(fractal3(x, y, z, warp));
+        return fractal3(x + dx, y + dy, z + dz, unitp);
+    }
+    return fractal3(x, y, z, unitp);
+}
+
+// EvaluateFractals3 (fractals.h:262): the stack at a point of a body, blended as in 2D.
+__device__ __forceinline__ float evaluate_stack3(double x, double y, double z,
+                                                 const Fractal* fractals, uint32_t count) {
+    float height = 0.0f;
+    bool started = false;
+    for (uint32_t i = 0; i < count; ++i) {
+        const Fractal& f = fractals[i];
+        if (!f.enabled) {
+            continue;
+        }
+        const float value = evaluate_fractal3(x, y, z, f);
+        const float scaled = f.amplitude * value;
+        if (!started) {
+            height = scaled;
+            started = true;
+            continue;
+        }
+        switch (f.blend) {
+        case kBlendMax:
+            height = smax(height, scaled);
+            break;
+        case kBlendMin:
+            height = smin(height, scaled);
+            break;
+        case kBlendMask:
+            height *= 0.5f * (value + 1.0f);
+            break;
+        default:
+            height += scaled;
+            break;
+        }
+    }
+    return height;
+}
+
 }  // namespace noise
 }  // namespace tgb

@@ -163,6 +163,20 @@ class Device:
                                           C.byref(g), h, b.memory, _stream(b.memory)))
         return heights
 
+    def noise_source_body(self, fractals: np.ndarray, grid: GridSpec, radius: float, heights,
+                          elevation: float = 0.0):
+        """SyntheticSource on a sphere of `radius` m (SyntheticSource::NoiseAt, FractalStackAt on
+        a body): `grid` in degrees of longitude and latitude; heights = elevation + the stack in
+        3D at each cell center's position."""
+        fr = _bytes(np.atleast_1d(fractals), FRACTAL)
+        b = _Buffers()
+        h = b.ptr(heights, np.float32)
+        g = grid.native()
+        N.check(self._lib.tg_noise_source_body(self._handle, fr.ctypes.data, len(fr), elevation,
+                                               C.byref(g), radius, h, b.memory,
+                                               _stream(b.memory)))
+        return heights
+
     def noise_layer(self, kernel: np.ndarray, grid: GridSpec, heights, origin=(0.0, 0.0),
                     nodata=(0, 0.0)):
         """NoiseLayer's RunKernel (noise_layer.cpp:113): heights += the NoiseLayerKernel stack."""
