@@ -397,6 +397,20 @@ int tg_crater_generate(const tg_crater_population* population, const double* reg
                        double* x, double* y, double* diameter, double* age, uint64_t* id,
                        size_t capacity, size_t* count);
 
+/* tg_crater_generate on the device: one thread per generation cell of every band, the kept
+ * craters in the reference's order into `x`, `y`, `diameter`, `age` and `id` (device pointers
+ * with TG_MEMORY_DEVICE, host pointers with TG_MEMORY_HOST; at most `capacity`; `count` receives
+ * the number). Every per-band constant comes from the host's libm; the device's `pow` (the
+ * diameter's inversion), `log` and `lgamma` (PTRS's acceptance) remain, so diameters may differ
+ * from tg_crater_generate's in their last bits while counts, positions, ages and ids match. A cell
+ * whose Poisson acceptance or keep decision lies within `tolerance` (relative; 0 for 1e-9) of its
+ * threshold is drawn on the host instead. Replaces GenerateCraters' cell loop
+ * (src/layers/craters/generation/population.cpp:381-441), which the reference runs on the CPU. */
+int tg_crater_generate_device(tg_device* device, const tg_crater_population* population,
+                              const double* region, double* x, double* y, double* diameter,
+                              double* age, uint64_t* id, size_t capacity, size_t* count,
+                              double tolerance, int memory, void* stream);
+
 /* A boulder layer's sizes and pose (BoulderLayerOptions, include/terraingen/layers/boulders/
  * boulder_options.h): power-law sizes N(>D) = c D^-exponent per m^2 on [min_diameter,
  * max_diameter] (BoulderSizes with a PowerLawSfd), height ratio and buried share uniform between

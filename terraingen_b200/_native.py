@@ -110,6 +110,8 @@ SIGNATURES.update({
     "tg_crater_generate": [C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,
                              C.POINTER(_SZ)],
     "tg_boulder_generate": [C.POINTER(BoulderPopulation), _P, _D, _P, _SZ, C.POINTER(_SZ)],
+    "tg_crater_generate_device": [_P, C.POINTER(Population), _P, _P, _P, _P, _P, _P, _SZ,
+                                  C.POINTER(_SZ), _D, _I, _P],
     "tg_crater_batch": [C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid), _P, _P, _SZ,
                         _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ)],
 })

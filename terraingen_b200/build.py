@@ -42,6 +42,7 @@ UNITS = {
     "api.cu": [],
     "geotiff.cu": [],
     "population.cpp": [],
+    "population_gpu.cu": ["-fmad=false"],
 }
 
 # Host units are compiled by the host compiler with the reference's floating-point flags, so

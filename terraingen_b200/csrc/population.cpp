@@ -22,6 +22,7 @@
 
 #include "../../include/tgb200.h"
 #include "layouts.h"
+#include "population_plan.h"
 
 namespace tgb {
 namespace host {
@@ -328,6 +329,82 @@ std::vector<Crater> generate(const tg_crater_population& spec, const Box& region
         }
     }
     return out;
+}
+
+// The plan the device generator follows: per band, its cells, SamplePoisson's and
+// PowerLawSfd::Sample's constants and the keep boxes, as `generate` uses them.
+std::vector<CraterBandPlan> crater_plan(const tg_crater_population& spec, const double* r) {
+    const Box region{r[0], r[1], r[2], r[3]};
+    const PowerLaw law{spec.sfd_coefficient, spec.sfd_exponent};
+    const double marginRadii = spec.margin_radii;
+    auto margin = [&](double d) { return 0.5 * marginRadii * d; };
+    std::vector<CraterBandPlan> plan;
+    uint64_t cells = 0;
+    for (const Band& band : crater_bands(spec.min_diameter, spec.max_diameter,
+                                         spec.cell_size_factor)) {
+        if (band.high <= spec.min_resolved_diameter) {
+            continue;
+        }
+        CraterBandPlan p{};
+        p.exponent = uint32_t(band.exponent);
+        p.low = band.low;
+        p.high = band.high;
+        p.cellSize = band.cellSize;
+        const Box cover = region.expanded(margin(band.high));
+        p.iMin = cell_coordinate(std::floor(cover.minX / band.cellSize));
+        p.jMin = cell_coordinate(std::floor(cover.minY / band.cellSize));
+        p.iMax = cell_coordinate(std::ceil(cover.maxX / band.cellSize) - 1.0);
+        p.jMax = cell_coordinate(std::ceil(cover.maxY / band.cellSize) - 1.0);
+        p.mean = law.expected(band.low, band.high) * (band.cellSize * band.cellSize);
+        p.limit = std::exp(-p.mean);
+        p.sqrtMean = std::sqrt(p.mean);
+        p.logMean = std::log(p.mean);
+        p.b = 0.931 + 2.53 * p.sqrtMean;
+        p.a = -0.059 + 0.02483 * p.b;
+        p.inverseAlpha = 1.1239 + 1.1328 / (p.b - 3.4);
+        p.vr = 0.9277 - 3.6224 / (p.b - 2.0);
+        p.logInverseAlpha = std::log(p.inverseAlpha);
+        p.count = law.expected(band.low, band.high);
+        p.top = law.cumulative(band.low);
+        p.inverseExponent = -1.0 / law.e;
+        const Box inner = region.expanded(margin(band.low));
+        const Box outer = region.expanded(margin(band.high));
+        const double in[4] = {inner.minX, inner.minY, inner.maxX, inner.maxY};
+        const double out[4] = {outer.minX, outer.minY, outer.maxX, outer.maxY};
+        std::copy(in, in + 4, p.inner);
+        std::copy(out, out + 4, p.outer);
+        p.firstCell = cells;
+        if (p.iMax >= p.iMin && p.jMax >= p.jMin) {
+            cells += uint64_t(p.iMax - p.iMin + 1) * uint64_t(p.jMax - p.jMin + 1);
+        }
+        plan.push_back(p);
+    }
+    return plan;
+}
+
+void cell_kept(const tg_crater_population& spec, const double* r, const CraterBandPlan& p,
+               int32_t i, int32_t j, std::vector<HostCrater>& out) {
+    const Box region{r[0], r[1], r[2], r[3]};
+    const PowerLaw law{spec.sfd_coefficient, spec.sfd_exponent};
+    auto margin = [&](double d) { return 0.5 * spec.margin_radii * d; };
+    const Band band{int(p.exponent), p.low, p.high, p.cellSize};
+    const Box inner{p.inner[0], p.inner[1], p.inner[2], p.inner[3]};
+    const Box outer{p.outer[0], p.outer[1], p.outer[2], p.outer[3]};
+    for (const Crater& c : cell_craters(band, i, j, law, spec.lifetime_gyr, spec.seed)) {
+        if (!(c.y >= outer.minY && c.y <= outer.maxY)) {
+            continue;
+        }
+        const bool inBand = c.diameter >= band.low && c.diameter <= band.high;
+        if (inBand && !outer.contains(c.x, c.y)) {
+            continue;
+        }
+        const bool keep = inBand ? inner.contains(c.x, c.y) ||
+                                       region.expanded(margin(c.diameter)).contains(c.x, c.y)
+                                 : region.expanded(margin(c.diameter)).contains(c.x, c.y);
+        if (keep) {
+            out.push_back(HostCrater{c.x, c.y, c.diameter, c.age, c.id});
+        }
+    }
 }
 
 // --- preparation and records ----------------------------------------------------------------

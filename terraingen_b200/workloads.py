@@ -71,6 +71,25 @@ def generate_craters(population: N.Population, region) -> dict:
     return out
 
 
+def generate_craters_device(device, population: N.Population, region,
+                           tolerance: float = 0.0) -> dict:
+    """generate_craters drawn on the device (tg_crater_generate_device), into host arrays."""
+    lib = N.library()
+    reg = np.ascontiguousarray(region, np.float64)
+    count = C.c_size_t()
+    N.check(lib.tg_crater_generate_device(device._handle, C.byref(population), reg.ctypes.data,
+                                          None, None, None, None, None, 0, C.byref(count),
+                                          tolerance, N.TG_MEMORY_HOST, None))
+    n = count.value
+    out = {k: np.empty(n, np.float64) for k in ("x", "y", "diameter", "age")}
+    out["id"] = np.empty(n, np.uint64)
+    N.check(lib.tg_crater_generate_device(
+        device._handle, C.byref(population), reg.ctypes.data,
+        *[out[k].ctypes.data for k in ("x", "y", "diameter", "age", "id")], n, C.byref(count),
+        tolerance, N.TG_MEMORY_HOST, None))
+    return out
+
+
 def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
                  irregular: int = 1):
     """(kernel, records, data, footprints) a crater layer hands the kernel for `grid`."""
