@@ -98,7 +98,7 @@ int check_nodata(tg_nodata n) {
 // A device buffer must be aligned to `align` bytes (16 for CraterRecords, read as 16-byte words;
 // 8 for doubles); a host buffer is copied into an aligned slot.
 int stage_in(tg_device* d, int memory, Slot slot, const void* src, size_t bytes,
-             const void** out, size_t align = sizeof(float)) {
+             const void** out, size_t align = sizeof(float), cudaStream_t on = nullptr) {
     if (bytes == 0) {
         *out = nullptr;
         return TG_OK;
@@ -114,7 +114,8 @@ int stage_in(tg_device* d, int memory, Slot slot, const void* src, size_t bytes,
         return TG_OK;
     }
     TG_CUDA(d->slots[slot].reserve(bytes), "device allocation");
-    TG_CUDA(cudaMemcpyAsync(d->slots[slot].ptr, src, bytes, cudaMemcpyHostToDevice, d->stream),
+    TG_CUDA(cudaMemcpyAsync(d->slots[slot].ptr, src, bytes, cudaMemcpyHostToDevice,
+                            on != nullptr ? on : d->stream),
             "copy to device");
     *out = d->slots[slot].ptr;
     return TG_OK;
@@ -217,6 +218,12 @@ int tg_open(int ordinal, tg_device** device) {
     if (err == cudaSuccess) {
         err = cudaMallocHost(&d->pinnedStatus, 4 * sizeof(uint32_t));
     }
+    if (err == cudaSuccess) {
+        err = cudaStreamCreateWithFlags(&d->copyStream, cudaStreamNonBlocking);
+    }
+    if (err == cudaSuccess) {
+        err = cudaEventCreateWithFlags(&d->copied, cudaEventDisableTiming);
+    }
     if (err != cudaSuccess) {
         delete d;
         return cuda_fail(err, "device set-up");
@@ -239,6 +246,13 @@ void tg_close(tg_device* d) {
     }
     if (d->pinnedStatus != nullptr) {
         cudaFreeHost(d->pinnedStatus);
+    }
+    if (d->copyStream != nullptr) {
+        cudaStreamSynchronize(d->copyStream);
+        cudaStreamDestroy(d->copyStream);
+    }
+    if (d->copied != nullptr) {
+        cudaEventDestroy(d->copied);
     }
     cudaStreamDestroy(d->stream);
     delete d;
@@ -975,29 +989,6 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         }
     }
     const cudaStream_t s = stream_of(d, memory, stream);
-    const void *drec = nullptr, *ddata = nullptr, *dfoot = nullptr, *db = nullptr;
-    if (t->n_craters > 0) {
-        if (int st = stage_in(d, memory, kRecords, t->crater_records,
-                              size_t(t->n_craters) * sizeof(CraterRecord), &drec, 16)) {
-            return st;
-        }
-        if (int st = stage_in(d, memory, kData, t->crater_data,
-                              size_t(t->n_crater_data) * sizeof(float), &ddata)) {
-            return st;
-        }
-        if (t->crater_footprints != nullptr) {
-            if (int st = stage_in(d, memory, kFootprints, t->crater_footprints,
-                                  size_t(t->n_craters) * 3 * sizeof(double), &dfoot, 8)) {
-                return st;
-            }
-        }
-    }
-    if (t->n_boulders > 0) {
-        if (int st = stage_in(d, memory, kBoulders, t->boulders,
-                              size_t(t->n_boulders) * sizeof(BoulderRecord), &db, 8)) {
-            return st;
-        }
-    }
     float* dh = heights;
     if (memory == TG_MEMORY_HOST) {
         TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
@@ -1010,6 +1001,37 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     if (t->noise_layer != nullptr) {
         TG_CUDA(launch_noise(layer, g, origin, false, 0.0f, NoData{0u, 0.0f}, dh, s),
                 "noise layer launch");
+    }
+    // Host-memory layer inputs are copied on the device's copy stream while the source's
+    // kernels run; the layers wait for them.
+    const cudaStream_t on = memory == TG_MEMORY_HOST ? d->copyStream : nullptr;
+    const void *drec = nullptr, *ddata = nullptr, *dfoot = nullptr, *db = nullptr;
+    if (t->n_craters > 0) {
+        if (int st = stage_in(d, memory, kRecords, t->crater_records,
+                              size_t(t->n_craters) * sizeof(CraterRecord), &drec, 16, on)) {
+            return st;
+        }
+        if (int st = stage_in(d, memory, kData, t->crater_data,
+                              size_t(t->n_crater_data) * sizeof(float), &ddata,
+                              sizeof(float), on)) {
+            return st;
+        }
+        if (t->crater_footprints != nullptr) {
+            if (int st = stage_in(d, memory, kFootprints, t->crater_footprints,
+                                  size_t(t->n_craters) * 3 * sizeof(double), &dfoot, 8, on)) {
+                return st;
+            }
+        }
+    }
+    if (t->n_boulders > 0) {
+        if (int st = stage_in(d, memory, kBoulders, t->boulders,
+                              size_t(t->n_boulders) * sizeof(BoulderRecord), &db, 8, on)) {
+            return st;
+        }
+    }
+    if (memory == TG_MEMORY_HOST) {
+        TG_CUDA(cudaEventRecord(d->copied, d->copyStream), "event");
+        TG_CUDA(cudaStreamWaitEvent(s, d->copied, 0), "event wait");
     }
     if (t->n_craters > 0) {
         if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,

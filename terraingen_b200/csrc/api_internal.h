@@ -100,6 +100,9 @@ int to_grid(const tg_grid* g, Grid& out);
 struct tg_device {
     int ordinal = 0;
     cudaStream_t stream = nullptr;
+    // Host-memory inputs copied on their own stream, to overlap the first kernels of a call.
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t copied = nullptr;
     std::mutex mutex;
     std::string name;
     tgb::api::Buffer slots[tgb::api::kSlotCount];
