@@ -224,6 +224,11 @@ int tg_open(int ordinal, tg_device** device) {
     if (err == cudaSuccess) {
         err = cudaEventCreateWithFlags(&d->copied, cudaEventDisableTiming);
     }
+    for (cudaEvent_t& e : d->strips) {
+        if (err == cudaSuccess) {
+            err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        }
+    }
     if (err != cudaSuccess) {
         delete d;
         return cuda_fail(err, "device set-up");
@@ -253,6 +258,11 @@ void tg_close(tg_device* d) {
     }
     if (d->copied != nullptr) {
         cudaEventDestroy(d->copied);
+    }
+    for (cudaEvent_t e : d->strips) {
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+        }
     }
     cudaStreamDestroy(d->stream);
     delete d;
@@ -500,13 +510,23 @@ namespace {
 
 // The crater pipeline on device buffers (count, scan, scatter, shape), on stream `s`. It reads
 // the number of binned entries back once to size the bins, and the status word at the end.
-int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
+// The crater pipeline's binning on stream `s` (count, scan, scatter, harmonics): what the shaping
+// launches need. `any` is false when no cell needs a crater.
+struct CraterPrep {
+    CraterBins bins{};
+    float* harmonics = nullptr;
+    bool fast = false;
+    bool any = false;
+};
+
+int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
                    const float* data, uint32_t nData, const double* foot, const Grid& g,
-                   float* dh, tg_nodata nodata, cudaStream_t s) {
+                   cudaStream_t s, CraterPrep& p) {
+    p = CraterPrep{};
     if (size_t(g.width) * g.height == 0 || n == 0) {
         return TG_OK;
     }
-    CraterBins bins{};
+    CraterBins& bins = p.bins;
     bins.binsX = (g.width + kBinCells - 1) / kBinCells;
     bins.binsY = (g.height + kBinCells - 1) / kBinCells;
     const uint32_t nbins = bins.binsX * bins.binsY;
@@ -546,17 +566,23 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
     bins.capacity = total;
-    const bool fast = crater_fast_path(k, d->pinnedStatus[1]);
-    float* harmonics = nullptr;
-    if (fast && nData > 0) {
+    p.fast = crater_fast_path(k, d->pinnedStatus[1]);
+    if (p.fast && nData > 0) {
         TG_CUDA(d->slots[kHarmonics].reserve(size_t(nData) * sizeof(float)), "allocation");
-        harmonics = slot_ptr<float>(d, kHarmonics);
-        TG_CUDA(launch_crater_harmonics(rec, n, data, harmonics, s), "harmonics launch");
+        p.harmonics = slot_ptr<float>(d, kHarmonics);
+        TG_CUDA(launch_crater_harmonics(rec, n, data, p.harmonics, s), "harmonics launch");
     }
     TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
-    TG_CUDA(launch_crater_shape(k, data, harmonics, fast, g, to_nodata(nodata), bins, dh, s),
-            "crater shape launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, 3 * sizeof(uint32_t),
+    p.any = true;
+    return TG_OK;
+}
+
+// After the shaping: its pair count and flags (waits for stream `s`).
+int crater_finish(tg_device* d, const CraterPrep& p, cudaStream_t s) {
+    if (!p.any) {
+        return TG_OK;
+    }
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, p.bins.total + 1, 3 * sizeof(uint32_t),
                             cudaMemcpyDeviceToHost, s),
             "copy to host");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -568,28 +594,52 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     return TG_OK;
 }
 
-// The boulder pipeline on device buffers (count, scan, scatter, bake), on stream `s`.
-int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double width,
-                    const Grid& g, float* dh, tg_nodata nodata, cudaStream_t s) {
+int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
+                   const float* data, uint32_t nData, const double* foot, const Grid& g,
+                   float* dh, tg_nodata nodata, cudaStream_t s) {
+    CraterPrep p;
+    if (int st = crater_prepare(d, k, rec, n, data, nData, foot, g, s, p)) {
+        return st;
+    }
+    if (!p.any) {
+        return TG_OK;
+    }
+    TG_CUDA(launch_crater_shape(k, data, p.harmonics, p.fast, g, to_nodata(nodata), p.bins, dh, s),
+            "crater shape launch");
+    return crater_finish(d, p, s);
+}
+
+// The boulder pipeline's binning on stream `s` (count, scan, scatter), its counts, cursor and
+// status in the given slots. `any` is false when no cell needs a boulder.
+struct BoulderPrep {
+    BoulderBins bins{};
+    uint32_t* status = nullptr;
+    bool any = false;
+};
+
+int boulder_prepare(tg_device* d, const BoulderRecord* rec, uint32_t n, double width,
+                    const Grid& g, cudaStream_t s, Slot countSlot, Slot cursorSlot,
+                    Slot statusSlot, BoulderPrep& p) {
+    p = BoulderPrep{};
     if (size_t(g.width) * g.height == 0 || n == 0) {
         return TG_OK;
     }
-    BoulderBins bins{};
+    BoulderBins& bins = p.bins;
     bins.binsX = (g.width + kBinCells - 1) / kBinCells;
     bins.binsY = (g.height + kBinCells - 1) / kBinCells;
     const uint32_t nbins = bins.binsX * bins.binsY;
-    TG_CUDA(d->slots[kCounts].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[countSlot].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[cursorSlot].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
     TG_CUDA(d->slots[kBoulderWindows].reserve(size_t(n) * sizeof(int4)), "allocation");
     TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
-    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
-    bins.counts = slot_ptr<uint32_t>(d, kCounts);
-    bins.cursor = slot_ptr<uint32_t>(d, kCursor);
+    TG_CUDA(d->slots[statusSlot].reserve(4 * sizeof(uint32_t)), "allocation");
+    bins.counts = slot_ptr<uint32_t>(d, countSlot);
+    bins.cursor = slot_ptr<uint32_t>(d, cursorSlot);
     bins.windows = slot_ptr<int4>(d, kBoulderWindows);
-    uint32_t* status = slot_ptr<uint32_t>(d, kStatus);
+    p.status = slot_ptr<uint32_t>(d, statusSlot);
     TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
     TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
-    TG_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(p.status, 0, 4 * sizeof(uint32_t), s), "memset");
     TG_CUDA(launch_boulder_count(rec, n, g, width, bins, s), "boulder count launch");
     TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
             "scan launch");
@@ -605,9 +655,16 @@ int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
     bins.entries = slot_ptr<BoulderEntry>(d, kBoulderEntries);
     bins.capacity = total;
     TG_CUDA(launch_boulder_scatter(rec, n, bins, s), "boulder scatter launch");
-    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), bins, dh, status, s),
-            "boulder bake launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, status, 4 * sizeof(uint32_t),
+    p.any = true;
+    return TG_OK;
+}
+
+// After the bake: its pair count and flags (waits for stream `s`).
+int boulder_finish(tg_device* d, const BoulderPrep& p, cudaStream_t s) {
+    if (!p.any) {
+        return TG_OK;
+    }
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, p.status, 4 * sizeof(uint32_t),
                             cudaMemcpyDeviceToHost, s),
             "copy to host");
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
@@ -617,6 +674,21 @@ int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
         return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
     }
     return TG_OK;
+}
+
+// The boulder pipeline on device buffers (count, scan, scatter, bake), on stream `s`.
+int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double width,
+                    const Grid& g, float* dh, tg_nodata nodata, cudaStream_t s) {
+    BoulderPrep p;
+    if (int st = boulder_prepare(d, rec, n, width, g, s, kCounts, kCursor, kStatus, p)) {
+        return st;
+    }
+    if (!p.any) {
+        return TG_OK;
+    }
+    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), p.bins, dh, p.status, s),
+            "boulder bake launch");
+    return boulder_finish(d, p, s);
 }
 
 int check_boulders(const void* boulders, uint32_t n) {
@@ -1032,6 +1104,72 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     if (memory == TG_MEMORY_HOST) {
         TG_CUDA(cudaEventRecord(d->copied, d->copyStream), "event");
         TG_CUDA(cudaStreamWaitEvent(s, d->copied, 0), "event wait");
+    }
+    if (memory == TG_MEMORY_HOST && (t->n_craters > 0 || t->n_boulders > 0)) {
+        // The layers by strips of bin rows, each strip copied out on the copy stream while the
+        // next is shaped and baked.
+        CraterPrep cp;
+        BoulderPrep bp;
+        auto drain = [&](int st) {
+            cudaStreamSynchronize(d->copyStream);
+            return st;
+        };
+        if (t->n_craters > 0) {
+            if (int st = crater_prepare(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,
+                                        static_cast<const float*>(ddata), t->n_crater_data,
+                                        static_cast<const double*>(dfoot), g, s, cp)) {
+                return st;
+            }
+        }
+        if (t->n_boulders > 0) {
+            if (int st = boulder_prepare(d, static_cast<const BoulderRecord*>(db), t->n_boulders,
+                                         t->boulder_width, g, s, kBoulderCounts, kBoulderCursor,
+                                         kBoulderStatus, bp)) {
+                return st;
+            }
+        }
+        const NoData none{0u, 0.0f};
+        const uint32_t binRows = (g.height + kBinCells - 1) / kBinCells;
+        const uint32_t strips = std::min<uint32_t>(8u, binRows);
+        const uint32_t per = (binRows + strips - 1) / strips;
+        for (uint32_t k0 = 0, q = 0; k0 < binRows; k0 += per, ++q) {
+            const uint32_t rows = std::min(per, binRows - k0);
+            if (cp.any) {
+                if (cudaError_t e = launch_crater_shape(k, static_cast<const float*>(ddata),
+                                                        cp.harmonics, cp.fast, g, none, cp.bins,
+                                                        dh, s, k0, rows)) {
+                    return drain(cuda_fail(e, "crater shape launch"));
+                }
+            }
+            if (bp.any) {
+                if (cudaError_t e = launch_boulder_bake(g, t->boulder_width, none, bp.bins, dh,
+                                                        bp.status, s, k0, rows)) {
+                    return drain(cuda_fail(e, "boulder bake launch"));
+                }
+            }
+            const size_t y0 = size_t(k0) * kBinCells;
+            const size_t y1 = std::min<size_t>(size_t(k0 + rows) * kBinCells, g.height);
+            cudaError_t e = cudaEventRecord(d->strips[q], s);
+            if (e == cudaSuccess) {
+                e = cudaStreamWaitEvent(d->copyStream, d->strips[q], 0);
+            }
+            if (e == cudaSuccess) {
+                e = cudaMemcpyAsync(heights + y0 * g.width, dh + y0 * g.width,
+                                    (y1 - y0) * g.width * sizeof(float), cudaMemcpyDeviceToHost,
+                                    d->copyStream);
+            }
+            if (e != cudaSuccess) {
+                return drain(cuda_fail(e, "strip copy to host"));
+            }
+        }
+        if (int st = drain(crater_finish(d, cp, s))) {
+            return st;
+        }
+        if (int st = boulder_finish(d, bp, s)) {
+            return st;
+        }
+        TG_CUDA(cudaStreamSynchronize(d->copyStream), "synchronize");
+        return TG_OK;
     }
     if (t->n_craters > 0) {
         if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,

@@ -87,6 +87,9 @@ enum Slot {
     kProbeValues,
     kFrames,
     kPoints,
+    kBoulderCounts,
+    kBoulderCursor,
+    kBoulderStatus,
     kSlotCount
 };
 
@@ -103,6 +106,7 @@ struct tg_device {
     // Host-memory inputs copied on their own stream, to overlap the first kernels of a call.
     cudaStream_t copyStream = nullptr;
     cudaEvent_t copied = nullptr;
+    cudaEvent_t strips[8] = {};  // a call's strips of output rows, ready to copy out
     std::mutex mutex;
     std::string name;
     tgb::api::Buffer slots[tgb::api::kSlotCount];

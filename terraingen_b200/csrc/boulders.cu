@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kThreads)
                         uint32_t* __restrict__ flags) {
     __shared__ __align__(128) BoulderEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
-    const uint32_t bin = blockIdx.x;
+    const uint32_t bin = bins.firstBin + blockIdx.x;
     uint32_t first = bins.counts[bin];
     uint32_t end = bins.counts[bin + 1];
     if (end > bins.capacity) {
@@ -244,12 +244,19 @@ cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
 
 cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 const BoulderBins& bins, float* heights, uint32_t* flags,
-                                cudaStream_t stream) {
-    const uint32_t nbins = bins.binsX * bins.binsY;
+                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows) {
+    if (firstBinRow >= bins.binsY) {
+        return cudaSuccess;
+    }
+    const uint32_t rowsRun = std::min(binRows, bins.binsY - firstBinRow);
+    const uint32_t nbins = bins.binsX * rowsRun;
     if (nbins == 0) {
         return cudaSuccess;
     }
-    boulder_bake_kernel<<<nbins, kThreads, 0, stream>>>(grid, width, nodata, bins, heights, flags);
+    BoulderBins strip = bins;
+    strip.firstBin = firstBinRow * bins.binsX;
+    boulder_bake_kernel<<<nbins, kThreads, 0, stream>>>(grid, width, nodata, strip, heights,
+                                                        flags);
     return cudaGetLastError();
 }
 

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kShapeThreads)
     __shared__ float2 columns[kShapeThreads / 32][32];  // split x of the warp's 32 columns
     __shared__ float2 rows[kShapeThreads / 32][4];      // split y of its 4 rows
 
-    const uint32_t bin = blockIdx.x;
+    const uint32_t bin = bins.firstBin + blockIdx.x;
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
     const uint32_t first = bins.counts[bin];
     const uint32_t count = bins.counts[bin + 1] - first;
@@ -602,17 +602,23 @@ bool crater_fast_path(const CraterShapeKernel& k, uint32_t batchFlags) {
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
                                 const float* harmonics, bool fast, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
-                                cudaStream_t stream) {
-    const uint32_t nbins = bins.binsX * bins.binsY;
+                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows) {
+    if (firstBinRow >= bins.binsY) {
+        return cudaSuccess;
+    }
+    const uint32_t rowsRun = std::min(binRows, bins.binsY - firstBinRow);
+    const uint32_t nbins = bins.binsX * rowsRun;
     if (nbins == 0) {
         return cudaSuccess;
     }
+    CraterBins strip = bins;
+    strip.firstBin = firstBinRow * bins.binsX;
     if (fast) {
         crater_shape_kernel<true><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, bins, heights, bins.total + 1);
+            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1);
     } else {
         crater_shape_kernel<false><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, bins, heights, bins.total + 1);
+            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1);
     }
     return cudaGetLastError();
 }

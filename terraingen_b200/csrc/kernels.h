@@ -79,6 +79,7 @@ struct CraterBins {
     uint32_t* total;     // [1] entries needed
     int4* boxes;         // [craters] reference-tile box per crater (x0, x1, y0, y1); empty: x0 > x1
     float* culls;        // [craters] cull distance per crater
+    uint32_t firstBin;   // the bin of a launch's first block (a strip of bin rows)
 };
 
 // Per crater: its footprint's reference-tile box on `grid` and the number of bins it covers,
@@ -100,7 +101,8 @@ cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, con
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
                                 const float* harmonics, bool fast, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
-                                cudaStream_t stream);
+                                cudaStream_t stream, uint32_t firstBinRow = 0,
+                                uint32_t binRows = 0xffffffffu);
 
 // The drop-in form: the reference's own tile lists (`CraterTiles`, apply.cpp:111-143), craters
 // applied in list order exactly as ShapeTilesOnCpu does (apply.cpp:199-222).
@@ -142,6 +144,7 @@ struct BoulderBins {
     BoulderEntry* entries;
     uint32_t capacity;
     int4* windows;     // [boulders]
+    uint32_t firstBin; // the bin of a launch's first block (a strip of bin rows)
 };
 
 cudaError_t launch_boulder_count(const BoulderRecord* boulders, uint32_t n, const Grid& grid,
@@ -150,7 +153,8 @@ cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
                                    const BoulderBins& bins, cudaStream_t stream);
 cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 const BoulderBins& bins, float* heights, uint32_t* flags,
-                                cudaStream_t stream);
+                                cudaStream_t stream, uint32_t firstBinRow = 0,
+                                uint32_t binRows = 0xffffffffu);
 
 // --- diamond-square ----------------------------------------------------------------------
 // Nodes of one level over columns [c0, c0 + w) and rows [r0, r0 + h), row-major doubles.
