@@ -394,19 +394,28 @@ def dem_form(dev, args, rank, world):
     finite = bool(torch.isfinite(heights).all())
 
     # End to end: the DEM posts copied in from pinned memory and the heights copied out to pinned
-    # memory every step, around the same device work.
+    # memory every step, around the same device work. Each step's heights are snapshotted on the
+    # device and read back on a copy stream while the next step refines, the way a producer of
+    # tiles streams them out; the timed region ends when the last step's heights are on the host.
     host_posts = torch.empty((pg.height, pg.width), dtype=torch.float32).pin_memory()
     host_posts.copy_(posts)
     host_out = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32).pin_memory()
+    snapshot = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32, device="cuda")
+    copier = torch.cuda.Stream()
     barrier(world)
     t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.dem_steps, 3))
+    e2e_steps = max(1, args.dem_steps)
     for _ in range(e2e_steps):
         posts.copy_(host_posts, non_blocking=True)
         out = step()
-        host_out.copy_(out, non_blocking=True)
-        torch.cuda.synchronize()
+        stream.wait_stream(copier)  # the previous step's read-back is done with the snapshot
+        snapshot.copy_(out)
+        copier.wait_stream(stream)
+        with torch.cuda.stream(copier):
+            host_out.copy_(snapshot, non_blocking=True)
+    torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    same_out = bool(torch.equal(host_out, chain.heights.cpu()))
     e2e_value = world * w.cells * e2e_steps / e2e_s / 1e6
     solves = chain.solves
     per_link = link_ms.reshape(-1, len(w.windows) - 1, 3).mean(axis=0)
@@ -435,7 +444,8 @@ def dem_form(dev, args, rank, world):
                     "fill bit-exact (tests/test_seams_gpu.py); craters as the plain path",
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(pg.cells * 4),
-                "d2h_bytes_per_step": int(w.cells * 4)},
+                "d2h_bytes_per_step": int(w.cells * 4), "matches_device_path": same_out,
+                "overlap": "each step's heights read back on a copy stream during the next step"},
         "clocks": clocks.summary(),
         "l2": "output (1.68 GB) far above L2, written every step",
     }
