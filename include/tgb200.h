@@ -360,6 +360,20 @@ int tg_crater_datums(tg_device* device, const void* kernel, size_t kernel_bytes,
                      uint32_t n_targets, uint32_t width, uint32_t rows, uint32_t first_row,
                      float* heights, int memory, void* stream);
 
+/* The body form (src/layers/kernels/crater_body_datums.slang, bound by FitBodyDatumsOnGpu,
+ * src/layers/craters/shaping/datum_fit.cpp): each lattice point of a strip (`positions`, 24-byte
+ * SplitPoints, width x rows) gets the relief of the craters its row lists (`lists`: per row its
+ * first entry and count into `entries`), each crater read in its 52-byte CraterFrame within its
+ * `bounds` (KernelBodyDatumRelief, include/terraingen/layers/kernels/craters.h:1326); `kernel` is
+ * the 188-byte CraterBodyDatumKernel; points holding `nodata` are left as they are. */
+int tg_crater_body_datums(tg_device* device, const void* kernel, size_t kernel_bytes,
+                          const void* records, uint32_t n_records, const float* data,
+                          uint32_t n_data, const void* frames, const float* bounds,
+                          const uint32_t* lists, uint32_t n_lists, const uint32_t* entries,
+                          uint32_t n_entries, const void* positions, uint32_t width,
+                          uint32_t rows, uint32_t first_row, float* heights, tg_nodata nodata,
+                          int memory, void* stream);
+
 /* --- crater populations and kernel batches (host) ------------------------------------------ */
 
 /* A crater layer's population on a plane: a power-law density N(>D) = c D^-exponent per m^2 on

@@ -826,6 +826,31 @@ int tg_craters_apply_body(tg_device*, const void* kernel, size_t kernelBytes, co
     return TG_OK;
 }
 
+int tg_crater_body_datums(tg_device*, const void* kernel, size_t kernelBytes,
+                          const void* records, uint32_t nRecords, const float* data,
+                          uint32_t nData, const void* frames, const float* bounds,
+                          const uint32_t* lists, uint32_t nLists, const uint32_t* entries,
+                          uint32_t nEntries, const void* positions, uint32_t width, uint32_t rows,
+                          uint32_t firstRow, float* heights, tg_nodata nodata, int, void*) {
+    Capture c;
+    c.kind = 5;
+    c.fields = {Bytes(static_cast<const unsigned char*>(kernel), kernelBytes),
+                Bytes(static_cast<const unsigned char*>(records), size_t(nRecords) * 144),
+                Bytes(data, nData),
+                Bytes(static_cast<const unsigned char*>(frames), size_t(nRecords) * 52),
+                Bytes(bounds, nRecords),
+                Bytes(lists, nLists),
+                Bytes(entries, nEntries),
+                Bytes(static_cast<const unsigned char*>(positions), size_t(width) * rows * 24),
+                Bytes(heights, size_t(width) * rows)};
+    c.width = width;
+    c.rows = rows;
+    c.firstRow = firstRow;
+    c.nodata = nodata;
+    g_captures.push_back(std::move(c));
+    return TG_OK;
+}
+
 int tg_crater_datums(tg_device*, const void* kernel, size_t kernelBytes, const void* records,
                      uint32_t nRecords, const float* data, uint32_t nData,
                      const float* bandFloats, uint32_t nBandFloats, const uint32_t* bandCells,

@@ -174,6 +174,8 @@ SIGNATURES.update({
     "tg_seam_stats_get": [C.POINTER(SeamStats)],
     "tg_crater_datums": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32, _P, _U32,
                          _P, _U32, _U32, _U32, _U32, _P, _I, _P],
+    "tg_crater_body_datums": [_P, _P, _SZ, _P, _U32, _P, _U32, _P, _P, _P, _U32, _P, _U32, _P,
+                              _U32, _U32, _U32, _P, NoData, _I, _P],
     "tg_seam_fill": [_P, _P, C.POINTER(Grid), _P, C.POINTER(Grid), _P, NoData, _P, _I, _P],
     "tg_seam_samples": [_P, _P, _P, C.POINTER(Grid), C.c_int64, C.c_int64, _U32, _U32, NoData,
                         _P, _P, _I, _P],

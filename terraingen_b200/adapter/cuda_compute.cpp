@@ -33,7 +33,7 @@ struct Params {
     std::uint32_t firstRow;
 };
 
-enum class Program { None, NoiseLayer, Craters, Datums };
+enum class Program { None, NoiseLayer, Craters, Datums, BodyDatums };
 
 /// Whether `program` is the compiled form of kernel `Kernel`.
 template <typename Kernel> bool Is(const KernelProgram& program) {
@@ -51,6 +51,9 @@ Program Identify(const KernelProgram& program) {
     }
     if (Is<CraterDatumKernel>(program)) {
         return Program::Datums;
+    }
+    if (Is<CraterBodyDatumKernel>(program)) {
+        return Program::BodyDatums;
     }
     return Program::None;
 }
@@ -170,6 +173,23 @@ void CudaCompute::Run(const KernelProgram& program, Span<const DeviceBuffer> buf
                              params.width, params.rows, params.firstRow, heights, TG_MEMORY_HOST,
                              nullptr) != TG_OK) {
             Throw("crater datums");
+        }
+        return;
+    }
+    if (kind == Program::BodyDatums && buffers.size() >= 11) {
+        // heights, xs, ys, CraterBodyDatumKernel, records, data, frames, bounds, lists, entries,
+        // positions (src/layers/kernels/crater_body_datums.slang, bound by FitBodyDatumsOnGpu)
+        float* heights = reinterpret_cast<float*>(buffers[0].output);
+        if (tg_crater_body_datums(m_state->device, buffers[3].bytes.data(),
+                                  buffers[3].bytes.size(), buffers[4].bytes.data(),
+                                  Count<CraterRecord>(buffers[4]), As<float>(buffers[5]),
+                                  Count<float>(buffers[5]), buffers[6].bytes.data(),
+                                  As<float>(buffers[7]), As<std::uint32_t>(buffers[8]),
+                                  Count<std::uint32_t>(buffers[8]), As<std::uint32_t>(buffers[9]),
+                                  Count<std::uint32_t>(buffers[9]), buffers[10].bytes.data(),
+                                  params.width, params.rows, params.firstRow, heights, nodata,
+                                  TG_MEMORY_HOST, nullptr) != TG_OK) {
+            Throw("crater datums on a body");
         }
         return;
     }

@@ -236,3 +236,166 @@ extern "C" int tg_crater_datums(tg_device* d, const void* kernel, size_t kernel_
     }
     return TG_OK;
 }
+
+// --- on a body (crater_body_datums.slang, KernelBodyDatumRelief craters.h:1326) -------------
+
+namespace {
+
+struct BodyDatumIndex {
+    const CraterRecord* records;
+    uint32_t nRecords;
+    const CraterFrame* frames;
+    const float* data;
+    const float* bounds;    // per record: the reach CraterRelief reads it within (m)
+    const uint32_t* lists;  // per row: first entry and entry count
+    uint32_t nLists;
+    const uint32_t* entries;
+    uint32_t nEntries;
+    const SplitPoint* positions;  // the strip's lattice points
+};
+
+// Each lattice point of a strip gets the relief of its row's craters, each read in its frame
+// (BodySplitOffset); points holding no data are left as they are.
+__global__ void body_datum_relief_kernel(const CraterShapeKernel k, const BodyDatumIndex ix,
+                                         uint32_t width, uint32_t rows, uint32_t firstRow,
+                                         const NoData nodata, float* __restrict__ heights,
+                                         uint32_t* __restrict__ flags) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = blockIdx.y * blockDim.y + threadIdx.y;
+    if (c >= width || r >= rows) {
+        return;
+    }
+    const size_t at = size_t(r) * width + c;
+    const float h = heights[at];
+    if ((nodata.mode == 1u && isnan(h)) || (nodata.mode == 2u && h == nodata.value)) {
+        return;
+    }
+    const uint32_t row = firstRow + r;
+    if (2u * row + 1u >= ix.nLists) {
+        atomicOr(flags, 1u);
+        return;
+    }
+    const uint32_t first = ix.lists[2u * row], count = ix.lists[2u * row + 1u];
+    const SplitPoint p = ix.positions[at];
+    float relief = 0.0f;
+    for (uint32_t e = first; e < first + count; ++e) {
+        if (e >= ix.nEntries || ix.entries[e] >= ix.nRecords) {
+            atomicOr(flags, 1u);
+            return;
+        }
+        const uint32_t n = ix.entries[e];
+        const CraterFrame& f = ix.frames[n];
+        const crater::Offset o =
+            crater::frame_offset(f, crater::split_difference(p.x, p.xLow, f.x, f.xLow),
+                                 crater::split_difference(p.y, p.yLow, f.y, f.yLow),
+                                 crater::split_difference(p.z, p.zLow, f.z, f.zLow));
+        relief += crater_relief(k, ix.data, ix.records[n], ix.bounds[n], o.dx, o.dy);
+    }
+    heights[at] = h + relief;
+}
+
+}  // namespace
+
+extern "C" int tg_crater_body_datums(tg_device* d, const void* kernel, size_t kernel_bytes,
+                                     const void* records, uint32_t n_records, const float* data,
+                                     uint32_t n_data, const void* frames, const float* bounds,
+                                     const uint32_t* lists, uint32_t n_lists,
+                                     const uint32_t* entries, uint32_t n_entries,
+                                     const void* positions, uint32_t width, uint32_t rows,
+                                     uint32_t first_row, float* heights, tg_nodata nodata,
+                                     int memory, void* stream) {
+    if (int st = check_device(d)) {
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    if (int st = check_memory(memory)) {
+        return st;
+    }
+    if (kernel == nullptr || kernel_bytes != sizeof(CraterShapeKernel)) {
+        return fail(TG_ERROR_ARGUMENT, "the body datum kernel is %zu bytes",
+                    sizeof(CraterShapeKernel));
+    }
+    if (nodata.mode > 2u) {
+        return fail(TG_ERROR_ARGUMENT, "nodata mode must be 0, 1 or 2");
+    }
+    const size_t points = size_t(width) * rows;
+    if (points == 0) {
+        return TG_OK;
+    }
+    if (heights == nullptr || positions == nullptr || lists == nullptr ||
+        (n_records > 0 && (records == nullptr || frames == nullptr || bounds == nullptr))) {
+        return fail(TG_ERROR_ARGUMENT, "heights, positions, lists and the records are required");
+    }
+    CraterShapeKernel k;
+    std::memcpy(&k, kernel, sizeof(k));
+    const cudaStream_t s = memory == TG_MEMORY_DEVICE && stream != nullptr
+                               ? static_cast<cudaStream_t>(stream)
+                               : d->stream;
+    Buffer bufs[9];
+    auto release = [&] {
+        for (Buffer& b : bufs) {
+            b.release();
+        }
+    };
+    auto stage = [&](int slot, const void* p, size_t bytes) -> const void* {
+        if (memory == TG_MEMORY_DEVICE || bytes == 0) {
+            return p;
+        }
+        if (bufs[slot].reserve(bytes) != cudaSuccess ||
+            cudaMemcpyAsync(bufs[slot].ptr, p, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            return nullptr;
+        }
+        return bufs[slot].ptr;
+    };
+    BodyDatumIndex ix{};
+    ix.records = static_cast<const CraterRecord*>(stage(0, records, size_t(n_records) * 144));
+    ix.nRecords = n_records;
+    ix.frames = static_cast<const CraterFrame*>(stage(1, frames, size_t(n_records) * 52));
+    ix.data = static_cast<const float*>(stage(2, data, size_t(n_data) * 4));
+    ix.bounds = static_cast<const float*>(stage(3, bounds, size_t(n_records) * 4));
+    ix.lists = static_cast<const uint32_t*>(stage(4, lists, size_t(n_lists) * 4));
+    ix.nLists = n_lists;
+    ix.entries = static_cast<const uint32_t*>(stage(5, entries, size_t(n_entries) * 4));
+    ix.nEntries = n_entries;
+    ix.positions = static_cast<const SplitPoint*>(stage(6, positions, points * 24));
+    float* dh = heights;
+    if (memory == TG_MEMORY_HOST) {
+        dh = static_cast<float*>(const_cast<void*>(stage(7, heights, points * 4)));
+    }
+    if ((n_records > 0 && (ix.records == nullptr || ix.frames == nullptr)) || dh == nullptr ||
+        ix.lists == nullptr || ix.positions == nullptr) {
+        release();
+        return fail(TG_ERROR_CUDA, "staging the body datum index");
+    }
+    cudaError_t e = bufs[8].reserve(sizeof(uint32_t));
+    uint32_t* flags = static_cast<uint32_t*>(bufs[8].ptr);
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(flags, 0, sizeof(uint32_t), s);
+    }
+    if (e == cudaSuccess) {
+        const dim3 block(16, 16);
+        const dim3 grid((width + 15) / 16, (rows + 15) / 16);
+        body_datum_relief_kernel<<<grid, block, 0, s>>>(k, ix, width, rows, first_row,
+                                                         NoData{nodata.mode, nodata.value}, dh,
+                                                         flags);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && memory == TG_MEMORY_HOST) {
+        e = cudaMemcpyAsync(heights, dh, points * 4, cudaMemcpyDeviceToHost, s);
+    }
+    uint32_t bad = 0;
+    if (e == cudaSuccess) {
+        e = cudaMemcpyAsync(&bad, flags, sizeof(bad), cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(s);
+    }
+    release();
+    if (e != cudaSuccess) {
+        return cuda_fail(e, "body datum relief");
+    }
+    if (bad != 0u) {
+        return fail(TG_ERROR_ARGUMENT, "the body datum lists name a row, entry or record out of range");
+    }
+    return TG_OK;
+}

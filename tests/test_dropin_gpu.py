@@ -61,3 +61,22 @@ def test_craters_on_a_body_through_reference_pipeline(dropin):
     assert np.count_nonzero(want) > 5000
     err = np.abs(gpu.astype(np.float64) - cpu)
     assert err.max() <= 1e-3, err.max()
+
+
+def test_crater_datums_on_a_body_through_reference_pipeline(dropin):
+    # Plane datums on a sphere: the reference fits them with its body datum kernel
+    # (crater_body_datums.slang), which the adapter runs as tg_crater_body_datums.
+    import importlib.util
+
+    from conftest import GOLDEN
+
+    spec = importlib.util.spec_from_file_location("body_cases", GOLDEN / "body_cases.py")
+    cases = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cases)
+    want = np.load(GOLDEN / "body.npz")["datum_expected"]
+    scene = cases.scene(datum=1)
+    cpu, _ = H.evaluate(dropin, scene, 0, 1)
+    gpu, _ = H.evaluate(dropin, scene, 1, 1)
+    assert np.array_equal(cpu.view(np.uint32), want.view(np.uint32))
+    err = np.abs(gpu.astype(np.float64) - cpu)
+    assert err.max() <= 1e-3, err.max()
