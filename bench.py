@@ -451,6 +451,64 @@ def dem_form(dev, args, rank, world):
     }
 
 
+def next_rows_form(dev):
+    """The stages beyond the per-cell path, timed once each: the dem20481 crater population drawn
+    on the device against the host restatement, a synthetic source on a sphere, and a GeoTIFF of
+    a 4097^2 grid written from device memory."""
+    import math
+    import os
+    import tempfile
+
+    import torch
+
+    from terraingen_b200 import GridSpec
+    from terraingen_b200.layouts import fractal
+    from terraingen_b200.workloads import (crater_population, generate_craters,
+                                           generate_craters_device)
+
+    side = 20481 * 0.5
+    pop = crater_population(11, 2.0e6 / (side * side * (1.0 - 100.0 ** -2)), 1.0, 100.0)
+    region = (0.0, 0.0, side, side)
+    t0 = time.perf_counter()
+    host = generate_craters(pop, region)
+    host_s = time.perf_counter() - t0
+    generate_craters_device(dev, pop, region)
+    t0 = time.perf_counter()
+    drawn = generate_craters_device(dev, pop, region)
+    device_s = time.perf_counter() - t0
+    radius = 1737400.0
+    g = GridSpec(4097, 4097, 10.0, 1.0, 0.5 / (radius * math.pi / 180.0))
+    fr = np.array([fractal(seed=1, wavelength=512.0, amplitude=5.0, octaves=8)])
+    body = torch.empty((4097, 4097), dtype=torch.float32, device="cuda")
+    dev.noise_source_body(fr, g, radius, body)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        dev.noise_source_body(fr, g, radius, body)
+    e1.record()
+    torch.cuda.synchronize()
+    body_ms = e0.elapsed_time(e1) / 5
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "dem.tif")
+        grid = (4097, 4097, (0.0, 0.5, 0.0, 0.0, 0.0, -0.5))
+        dev.geotiff_write(path, [body], grid, nodata=float("nan"))
+        t0 = time.perf_counter()
+        dev.geotiff_write(path, [body], grid, nodata=float("nan"))
+        tiff_s = time.perf_counter() - t0
+        tiff_bytes = os.path.getsize(path)
+    return {
+        "crater_population": {"craters": int(len(drawn["x"])), "device_ms": round(device_s * 1e3, 2),
+                              "host_ms": round(host_s * 1e3, 1),
+                              "ids_match_host": bool(np.array_equal(drawn["id"], host["id"]))},
+        "body_source": {"cells": 4097 * 4097, "ms": round(body_ms, 3),
+                        "mcells_per_s": round(4097 * 4097 / body_ms / 1e3, 1),
+                        "stack": "one 8-octave Perlin fBm on a sphere of 1737.4 km"},
+        "geotiff_lzw": {"cells": 4097 * 4097, "seconds": round(tiff_s, 3), "bytes": int(tiff_bytes),
+                        "from": "device memory, 256-pixel LZW tiles, file write included"},
+    }
+
+
 def served_form(dev, args, rank, world):
     """The served form on the camera request stream (terraingen_b200/serve.py): the DEM stack's
     source and craters served by continuous batching, results in device buffers. Latency per
@@ -637,6 +695,8 @@ def main():
         forms["served"] = served_form(dev, args, rank, world)
     if args.dem_steps > 0:
         forms["dem_refinement"] = dem_form(dev, args, rank, world)
+    if args.dem_steps > 0:
+        forms["next_rows"] = next_rows_form(dev)
 
     if rank != 0:
         return
