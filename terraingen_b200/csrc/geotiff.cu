@@ -445,6 +445,9 @@ void add_tags(Ifd& ifd, const tg_grid& g, uint32_t bands, uint32_t compression, 
 // A device allocation freed with its scope.
 struct DeviceBytes {
     void* ptr = nullptr;
+    DeviceBytes() = default;
+    DeviceBytes(const DeviceBytes&) = delete;
+    DeviceBytes& operator=(const DeviceBytes&) = delete;
     ~DeviceBytes() {
         if (ptr != nullptr) {
             cudaFree(ptr);

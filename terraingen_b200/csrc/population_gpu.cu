@@ -231,6 +231,23 @@ __global__ void crater_write_cells_kernel(const DevicePlan d, const uint64_t* __
     cell_pass(d, p, i, j, ambiguous, x, y, diameter, age, id, offsets[g], capacity);
 }
 
+// The craters of host-drawn cells to their places in the outputs.
+__global__ void scatter_hosted_kernel(const HostCrater* __restrict__ craters,
+                                      const uint64_t* __restrict__ places, size_t n, double* x,
+                                      double* y, double* diameter, double* age, uint64_t* id) {
+    const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n) {
+        return;
+    }
+    const HostCrater c = craters[k];
+    const uint64_t at = places[k];
+    x[at] = c.x;
+    y[at] = c.y;
+    diameter[at] = c.diameter;
+    age[at] = c.age;
+    id[at] = c.id;
+}
+
 // A device allocation freed with its scope.
 struct Scratch {
     void* ptr = nullptr;
@@ -367,16 +384,29 @@ int tg_crater_generate_device(tg_device* d, const tg_crater_population* spec,
         dp, static_cast<const uint64_t*>(offsets.ptr), static_cast<const uint8_t*>(flags.ptr),
         dx, dy, dd, da, di, writable);
     TG_CUDA(cudaGetLastError(), "write launch");
+    // The host-drawn cells' craters, gathered into one upload and scattered to their places.
+    std::vector<HostCrater> flat;
+    std::vector<uint64_t> places;
     for (const auto& [g, list] : hosted) {
         for (size_t k = 0; k < list.size() && off[g] + k < writable; ++k) {
-            const HostCrater& c = list[k];
-            const uint64_t n = off[g] + k;
-            TG_CUDA(cudaMemcpyAsync(dx + n, &c.x, 8, cudaMemcpyHostToDevice, s), "copy");
-            TG_CUDA(cudaMemcpyAsync(dy + n, &c.y, 8, cudaMemcpyHostToDevice, s), "copy");
-            TG_CUDA(cudaMemcpyAsync(dd + n, &c.diameter, 8, cudaMemcpyHostToDevice, s), "copy");
-            TG_CUDA(cudaMemcpyAsync(da + n, &c.age, 8, cudaMemcpyHostToDevice, s), "copy");
-            TG_CUDA(cudaMemcpyAsync(di + n, &c.id, 8, cudaMemcpyHostToDevice, s), "copy");
+            flat.push_back(list[k]);
+            places.push_back(off[g] + k);
         }
+    }
+    Scratch hostedCraters, hostedPlaces;
+    if (!flat.empty()) {
+        TG_CUDA(hostedCraters.allocate(flat.size() * sizeof(HostCrater)), "allocation");
+        TG_CUDA(hostedPlaces.allocate(places.size() * 8), "allocation");
+        TG_CUDA(cudaMemcpyAsync(hostedCraters.ptr, flat.data(), flat.size() * sizeof(HostCrater),
+                                cudaMemcpyHostToDevice, s),
+                "copy");
+        TG_CUDA(cudaMemcpyAsync(hostedPlaces.ptr, places.data(), places.size() * 8,
+                                cudaMemcpyHostToDevice, s),
+                "copy");
+        scatter_hosted_kernel<<<uint32_t((flat.size() + 255) / 256), 256, 0, s>>>(
+            static_cast<const HostCrater*>(hostedCraters.ptr),
+            static_cast<const uint64_t*>(hostedPlaces.ptr), flat.size(), dx, dy, dd, da, di);
+        TG_CUDA(cudaGetLastError(), "scatter launch");
     }
     if (memory == TG_MEMORY_HOST) {
         TG_CUDA(cudaMemcpyAsync(x, dx, writable * 8, cudaMemcpyDeviceToHost, s), "copy");
@@ -385,7 +415,6 @@ int tg_crater_generate_device(tg_device* d, const tg_crater_population* spec,
         TG_CUDA(cudaMemcpyAsync(age, da, writable * 8, cudaMemcpyDeviceToHost, s), "copy");
         TG_CUDA(cudaMemcpyAsync(id, di, writable * 8, cudaMemcpyDeviceToHost, s), "copy");
     }
-    // The host's crater values are read by the copies above, and the scratch is freed below.
     TG_CUDA(cudaStreamSynchronize(s), "synchronize");
     return TG_OK;
 }
