@@ -33,22 +33,26 @@ constexpr uint32_t kChunk = 96;        // entries per staged chunk (15 KB)
 
 using namespace binning;
 
+// Each warp takes 32 craters: every lane finds its crater's footprint (its 16-cell tile window
+// and cull radius, as CraterReach and TileLists give it), then the warp counts the bins of each
+// crater in turn, its lanes spread over the crater's bins.
 __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
                                     uint32_t n, const float* __restrict__ data,
                                     const double* __restrict__ footprints, const Grid grid,
                                     CraterBins bins, uint32_t* __restrict__ flags) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
-    if (warp >= n) {
+    const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (base >= n) {
         return;
     }
+    const uint32_t mine = base + lane;
     int4 tiles = make_int4(1, 0, 1, 0);
-    if (lane == 0) {
-        const CraterRecord r = records[warp];
-        const Footprint f = crater_footprint(k, r, data, footprints, warp, grid);
+    if (mine < n) {
+        const CraterRecord r = records[mine];
+        const Footprint f = crater_footprint(k, r, data, footprints, mine, grid);
         tiles = f.tiles;
-        bins.boxes[warp] = tiles;
-        bins.culls[warp] = f.cull;
+        bins.boxes[mine] = tiles;
+        bins.culls[mine] = f.cull;
         if (tiles.x <= tiles.y) {
             if (r.hasDatum == 1u) {
                 atomicOr(flags, 1u);
@@ -59,21 +63,24 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
             }
         }
     }
-    tiles.x = __shfl_sync(0xffffffffu, tiles.x, 0);
-    tiles.y = __shfl_sync(0xffffffffu, tiles.y, 0);
-    tiles.z = __shfl_sync(0xffffffffu, tiles.z, 0);
-    tiles.w = __shfl_sync(0xffffffffu, tiles.w, 0);
-    if (tiles.x > tiles.y) {
-        return;
-    }
     constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
-    const uint32_t bx0 = uint32_t(tiles.x) / kTilesPerBin, bx1 = uint32_t(tiles.y) / kTilesPerBin;
-    const uint32_t by0 = uint32_t(tiles.z) / kTilesPerBin, by1 = uint32_t(tiles.w) / kTilesPerBin;
-    const uint32_t wide = bx1 - bx0 + 1u;
-    const uint32_t total = wide * (by1 - by0 + 1u);
-    for (uint32_t t = lane; t < total; t += 32u) {
-        const uint32_t b = (by0 + t / wide) * bins.binsX + bx0 + t % wide;
-        atomicAdd(bins.counts + b, 1u);
+    const uint32_t count = min(32u, n - base);
+    for (uint32_t j = 0; j < count; ++j) {
+        const int4 t = make_int4(__shfl_sync(0xffffffffu, tiles.x, int(j)),
+                                 __shfl_sync(0xffffffffu, tiles.y, int(j)),
+                                 __shfl_sync(0xffffffffu, tiles.z, int(j)),
+                                 __shfl_sync(0xffffffffu, tiles.w, int(j)));
+        if (t.x > t.y) {
+            continue;
+        }
+        const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
+        const uint32_t by0 = uint32_t(t.z) / kTilesPerBin, by1 = uint32_t(t.w) / kTilesPerBin;
+        const uint32_t wide = bx1 - bx0 + 1u;
+        const uint32_t total = wide * (by1 - by0 + 1u);
+        for (uint32_t q = lane; q < total; q += 32u) {
+            const uint32_t b = (by0 + q / wide) * bins.binsX + bx0 + q % wide;
+            atomicAdd(bins.counts + b, 1u);
+        }
     }
 }
 
@@ -562,8 +569,8 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
     if (n == 0) {
         return cudaSuccess;
     }
-    const uint32_t threads = 256;
-    const uint32_t blocks = uint32_t((uint64_t(n) * 32u + threads - 1) / threads);
+    const uint32_t threads = 256;  // 8 warps of 32 craters
+    const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
     crater_count_kernel<<<blocks, threads, 0, stream>>>(k, records, n, data, footprints, grid,
                                                         bins, bins.total + 1);
     return cudaGetLastError();
