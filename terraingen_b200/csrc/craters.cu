@@ -84,41 +84,79 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
     }
 }
 
+// Each warp takes 32 craters and spreads all of their (crater, bin) pairs over its lanes: a
+// lane finds its pair's crater by a search of the warp's running bin counts, then copies the
+// crater's record and tail into its bin's next slot.
 __global__ void crater_scatter_kernel(const CraterRecord* __restrict__ records, uint32_t n,
                                       CraterBins bins) {
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
-    if (warp >= n) {
-        return;
-    }
-    const int4 tiles = bins.boxes[warp];
-    if (tiles.x > tiles.y) {
+    const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
+    if (base >= n) {
         return;
     }
     constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
-    const uint32_t bx0 = uint32_t(tiles.x) / kTilesPerBin, bx1 = uint32_t(tiles.y) / kTilesPerBin;
-    const uint32_t by0 = uint32_t(tiles.z) / kTilesPerBin, by1 = uint32_t(tiles.w) / kTilesPerBin;
-    const uint32_t wide = bx1 - bx0 + 1u;
-    const uint32_t total = wide * (by1 - by0 + 1u);
-    const int4* src = reinterpret_cast<const int4*>(records + warp);
-    const float cull = bins.culls[warp];
-    int4 tail;
-    tail.x = int(uint32_t(tiles.x) | (uint32_t(tiles.y) << 16));
-    tail.y = int(uint32_t(tiles.z) | (uint32_t(tiles.w) << 16));
-    tail.z = __float_as_int(cull);
-    tail.w = int(warp);
-    for (uint32_t t = lane; t < total; t += 32u) {
-        const uint32_t b = (by0 + t / wide) * bins.binsX + bx0 + t % wide;
+    const uint32_t mine = base + lane;
+    int4 tiles = make_int4(1, 0, 1, 0);
+    float cull = 0.0f;
+    uint32_t count = 0;
+    if (mine < n) {
+        tiles = bins.boxes[mine];
+        cull = bins.culls[mine];
+        if (tiles.x <= tiles.y) {
+            count = (uint32_t(tiles.y) / kTilesPerBin - uint32_t(tiles.x) / kTilesPerBin + 1u) *
+                    (uint32_t(tiles.w) / kTilesPerBin - uint32_t(tiles.z) / kTilesPerBin + 1u);
+        }
+    }
+    // Inclusive running count of the warp's pairs.
+    uint32_t upto = count;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, upto, d);
+        if (lane >= uint32_t(d)) {
+            upto += v;
+        }
+    }
+    const uint32_t pairs = __shfl_sync(0xffffffffu, upto, 31);
+    for (uint32_t q0 = 0; q0 < pairs; q0 += 32u) {
+        const uint32_t q = q0 + lane;
+        // The crater of pair q: the first lane whose running count exceeds q.
+        uint32_t owner = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint32_t probe = owner + step - 1u;
+            const uint32_t at = __shfl_sync(0xffffffffu, upto, int(probe));
+            if (at <= q) {
+                owner += step;
+            }
+        }
+        const int4 t = make_int4(__shfl_sync(0xffffffffu, tiles.x, int(owner)),
+                                 __shfl_sync(0xffffffffu, tiles.y, int(owner)),
+                                 __shfl_sync(0xffffffffu, tiles.z, int(owner)),
+                                 __shfl_sync(0xffffffffu, tiles.w, int(owner)));
+        const float c = __shfl_sync(0xffffffffu, cull, int(owner));
+        const uint32_t before = __shfl_sync(0xffffffffu, upto - count, int(owner));
+        if (q >= pairs) {
+            continue;
+        }
+        const uint32_t local = q - before;
+        const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
+        const uint32_t by0 = uint32_t(t.z) / kTilesPerBin;
+        const uint32_t wide = bx1 - bx0 + 1u;
+        const uint32_t b = (by0 + local / wide) * bins.binsX + bx0 + local % wide;
         const uint32_t slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
         if (slot >= bins.capacity) {
             continue;  // the host sized the entries from the counts; never taken
         }
+        const uint32_t crater = base + owner;
+        const int4* src = reinterpret_cast<const int4*>(records + crater);
         int4* dst = reinterpret_cast<int4*>(bins.entries + slot);
 #pragma unroll
         for (int w = 0; w < 9; ++w) {
             dst[w] = __ldg(src + w);
         }
-        dst[9] = tail;
+        dst[9] = make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
+                           int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
+                           int(crater));
     }
 }
 
@@ -582,8 +620,8 @@ cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const
     if (n == 0) {
         return cudaSuccess;
     }
-    const uint32_t threads = 256;
-    const uint32_t blocks = uint32_t((uint64_t(n) * 32u + threads - 1) / threads);
+    const uint32_t threads = 256;  // 8 warps of 32 craters
+    const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
     crater_scatter_kernel<<<blocks, threads, 0, stream>>>(records, n, bins);
     return cudaGetLastError();
 }
