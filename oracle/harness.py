@@ -182,6 +182,30 @@ def write_crater_list(lib: C.CDLL, path, x, y, diameter, age, ids, manual, repla
         raise RuntimeError(f"tgref_write_crater_list failed: {lib.tgref_error().decode()}")
 
 
+BOULDER_DOUBLES = ("x", "y", "diameter", "height", "burial", "yaw", "lean", "tilt",
+                   "tilt_azimuth", "wear", "ground")
+
+
+def write_boulder_list(lib: C.CDLL, path, columns: dict, json: bool) -> None:
+    """The reference's WriteBoulderList (tgref_write_boulder_list). `columns` holds the doubles
+    named in BOULDER_DOUBLES (angles in radians; NaN grounds are unset) and id, parent, piece,
+    rest and model."""
+    values = np.ascontiguousarray(np.stack([np.asarray(columns[k], np.float64)
+                                            for k in BOULDER_DOUBLES]))
+    n = values.shape[1]
+    known = np.ascontiguousarray(np.isfinite(values[10]), np.uint8)
+    ids = np.ascontiguousarray(columns["id"], np.uint64)
+    parent = np.ascontiguousarray(columns["parent"], np.uint64)
+    piece = np.ascontiguousarray(columns["piece"], np.uint32)
+    rest = np.ascontiguousarray(columns["rest"], np.uint8)
+    model = np.ascontiguousarray(columns["model"], np.uint8)
+    st = lib.tgref_write_boulder_list(str(path).encode(), values.ctypes.data, known.ctypes.data,
+                                      ids.ctypes.data, parent.ctypes.data, piece.ctypes.data,
+                                      rest.ctypes.data, model.ctypes.data, n, int(json))
+    if st != 0:
+        raise RuntimeError(f"tgref_write_boulder_list failed: {lib.tgref_error().decode()}")
+
+
 COMPRESSION = {"none": 0, "lzw": 1, "packbits": 2, "deflate": 3}  # TiffCompression's order
 
 
@@ -342,6 +366,11 @@ def _harness(name: str) -> C.CDLL:
         lib.tgref_write_crater_list.argtypes = [C.c_char_p, P, P, P, P, P, P, P, C.c_size_t,
                                                 C.c_int]
         lib.tgref_write_crater_list.restype = C.c_int
+    if hasattr(lib, "tgref_write_boulder_list"):
+        P = C.c_void_p
+        lib.tgref_write_boulder_list.argtypes = [C.c_char_p, P, P, P, P, P, P, P, C.c_size_t,
+                                                 C.c_int]
+        lib.tgref_write_boulder_list.restype = C.c_int
     return lib
 
 

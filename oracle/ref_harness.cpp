@@ -719,6 +719,45 @@ int tgref_write_crater_list(const char* path, const double* x, const double* y,
     }
 }
 
+/// WriteBoulderList (src/io/feature_lists.cpp:412) of n boulders given column by column.
+/// `values` holds 11 columns of n doubles each: x, y, diameter, height, burial, yaw, lean, tilt,
+/// tiltAzimuth, wear and ground (radians for the angles); `known` marks the grounds that are set.
+int tgref_write_boulder_list(const char* path, const double* values, const uint8_t* known,
+                             const uint64_t* id, const uint64_t* parent, const uint32_t* piece,
+                             const uint8_t* rest, const uint8_t* model, size_t n, int json) {
+    try {
+        BoulderList list;
+        for (size_t i = 0; i < n; ++i) {
+            const auto col = [&](int k) { return values[size_t(k) * n + i]; };
+            Boulder b;
+            b.x = col(0);
+            b.y = col(1);
+            b.diameter = col(2);
+            b.height = col(3);
+            b.burial = col(4);
+            b.yaw = col(5);
+            b.lean = col(6);
+            b.tilt = col(7);
+            b.tiltAzimuth = col(8);
+            b.wear = col(9);
+            if (known[i] != 0) {
+                b.ground = col(10);
+            }
+            b.id = id[i];
+            b.parent = parent[i];
+            b.piece = piece[i];
+            b.rest = static_cast<BoulderRest>(rest[i]);
+            b.model = model[i] != 0;
+            list.Append(b);
+        }
+        WriteBoulderList(list, path, json ? ListFormat::Json : ListFormat::Csv);
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
 }  // extern "C"
 
 #ifdef TGREF_CAPTURE
