@@ -107,6 +107,32 @@ __global__ void __launch_bounds__(kThreads)
     const int row = int(binY * kBinCells + warp * 4u + lane / 8u);
     const int col0 = int(binX * kBinCells + (lane % 8u) * kCellsPerThread);
     const bool rowIn = row < int(grid.height);
+    // Thread 0 starts the entry fetch before the cells' base heights are loaded, so the two
+    // memory latencies overlap; the barrier after the loads publishes the mbarrier init.
+    const uint32_t chunks = (count + kChunk - 1) / kChunk;
+    auto issue = [&](uint32_t c) {
+        const uint32_t s = c & 1u;
+        const uint32_t bytes = min(kChunk, count - c * kChunk) * uint32_t(sizeof(BoulderEntry));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_addr(&bars[s])),
+                     "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(smem_addr(&stage[s][0])),
+            "l"(bins.entries + first + c * kChunk), "r"(bytes), "r"(smem_addr(&bars[s]))
+            : "memory");
+    };
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
+        if (chunks > 1) {
+            issue(1);
+        }
+    }
     // Cell centers in double (Raster::CellCenter), the base heights and the running maxima.
     const double cy = grid.originY + (double(col0) + 0.5) * grid.colRotation +
                       (double(row) + 0.5) * grid.pixelHeight;
@@ -126,33 +152,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         best[j] = double(base[j]);
     }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[1])));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
     __syncthreads();
-    const uint32_t chunks = (count + kChunk - 1) / kChunk;
-    auto issue = [&](uint32_t c) {
-        const uint32_t s = c & 1u;
-        const uint32_t bytes = min(kChunk, count - c * kChunk) * uint32_t(sizeof(BoulderEntry));
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                         smem_addr(&bars[s])),
-                     "r"(bytes)
-                     : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-            "[%3];" ::"r"(smem_addr(&stage[s][0])),
-            "l"(bins.entries + first + c * kChunk), "r"(bytes), "r"(smem_addr(&bars[s]))
-            : "memory");
-    };
-    if (tid == 0) {
-        issue(0);
-        if (chunks > 1) {
-            issue(1);
-        }
-    }
     uint32_t phase[2] = {0u, 0u};
     uint32_t evaluated = 0;
     for (uint32_t c = 0; c < chunks; ++c) {
