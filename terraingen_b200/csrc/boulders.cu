@@ -81,7 +81,8 @@ __global__ void boulder_scatter_kernel(const BoulderRecord* __restrict__ boulder
     }
 }
 
-__global__ void __launch_bounds__(kThreads)
+// Four CTAs per SM (64 registers a thread) to hide the bake's memory latencies.
+__global__ void __launch_bounds__(kThreads, 4)
     boulder_bake_kernel(const Grid grid, const double width, const NoData nodata,
                         const BoulderBins bins, float* __restrict__ heights,
                         uint32_t* __restrict__ flags) {
