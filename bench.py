@@ -727,8 +727,10 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded): fBm source, the reference's crater batch and boulders "
                 "(restated on the host, bit-exact)",
-        "config": {"workload": "terrain4097: 4097x4097 at 0.5 m, 8-octave fBm + 200k craters + "
-                               "1M boulders (resolved ones drawn)",
+        "config": {"workload": "terrain4097: 4097x4097 at 0.5 m, 8-octave fBm + 200k craters "
+                               "(5% central peaks: complex profile from 4.47 m, massif peaks; "
+                               "terraces from 200 m on the freshest 10%) + 1M boulders "
+                               "(resolved ones drawn)",
                    "cells_per_gpu": w.cells, "craters_on_tile": int(len(w.crater_records)),
                    "boulders_drawn": int(len(w.boulders)), "l2": "flushed between steps",
                    "parallelism": f"replicas x{world} (one tile per GPU)"},

@@ -84,6 +84,12 @@ const char* tg_last_error(void);
 int tg_device_name(tg_device* device, char* name, size_t capacity);
 /* Waits for the device's stream. */
 int tg_synchronize(tg_device* device);
+/* How many times the binned crater and boulder kernels of this device poll a staged copy (a TMA
+ * bulk copy into shared memory) before they give up on it and the call returns TG_ERROR_TIMEOUT
+ * with the device still usable; by default 2^26 (seconds). 0 gives up without polling, which
+ * exercises that error path without any fault. The reference has no counterpart: its CUDA
+ * backend does not wait on device-side copies. */
+int tg_set_wait_limit(tg_device* device, uint32_t polls);
 
 /* --- noise (fBm sources and layers) --------------------------------------------------------- */
 
@@ -205,7 +211,8 @@ int tg_boulders_bake(tg_device* device, const void* boulders, uint32_t n, double
  * cudaStream_t; NULL for the legacy default stream) and the call returns when it is done. Its
  * scratch is one static 16 MiB device array inside the library, which every GPU that loads the
  * library holds until exit; at most 65536 boulders, 32768 bins of 32x32 cells (a 5792 x 5792 grid)
- * and 196608 binned boulders (TG_ERROR_MEMORY past that). The first call on a device finds the
+ * and 196608 binned boulders (TG_ERROR_MEMORY past that, found before anything is written, so the
+ * heights are left as they were). The first call on a device finds the
  * array's device address (cudaGetSymbolAddress) and should come before any stream capture. Calls
  * share the array: calls whose work overlaps on the GPU race and must not overlap. Errors go to
  * `error` (capacity bytes, may be null), not to tg_last_error. */
@@ -281,8 +288,9 @@ int tg_evaluate(tg_device* device, const tg_terrain* terrain, const tg_grid* gri
 int tg_device_counters(tg_device* device, uint64_t* counters, size_t n);
 
 /* The device's measured lane-operation rate for a mix of 32-bit integer multiply-adds and FP32
- * fused multiply-adds (the noise and shaping kernels' roofline denominator), in operations per
- * second. */
+ * fused multiply-adds (the noise and shaping kernels' roofline denominator), in thread
+ * instructions per second: dependent chains no compiler can shorten (quadratic IMAD, FFMA), so
+ * the rate stays below the issue ceiling of 128 lanes per SM per clock. */
 int tg_measure_alu(tg_device* device, double* lane_ops_per_second);
 
 /* --- seams between chained sources ---------------------------------------------------------
@@ -396,11 +404,24 @@ typedef struct tg_crater_population {
     double min_resolved_diameter; /* bands wholly below are skipped (tg_crater_population only) */
 } tg_crater_population;
 
-/* How the layer shapes its craters: `profile` 0 Fassett-Thomson, 1 Martin-Parkes-Dunstan;
- * `irregular` 1 for the default irregular outlines (DefaultCraterApply, apply_options.cpp:49). */
+/* How the layer shapes its craters.
+ * `profile`: 0 Fassett-Thomson, 1 Martin-Parkes-Dunstan, 2 and 3 a ComplexCraterProfile over
+ *   those (include/terraingen/layers/craters/profiles/complex.h:78) with the lunar shape
+ *   (LunarComplexCraterShape, src/layers/craters/shaping/morphometry.cpp:40) from
+ *   `transition_diameter` meters: flat floors, central peaks, a power-law exterior to 3 radii.
+ * `irregular`: 1 for DefaultCraterApply (apply_options.cpp:49): irregular outlines, wall
+ *   terraces (CraterTerraces) and massif central peaks (CraterPeaks) at their defaults; 0 for
+ *   plain CraterApplyOptions (none of them).
+ * Terraces: with `terrace_onset` > 0 the three terrace fields replace CraterTerraces'
+ *   onsetDiameter, fullDiameter and minFreshness (apply_options.h:183-226); otherwise the
+ *   defaults (20 km, 65 km, 0.3). */
 typedef struct tg_crater_shaping {
     uint32_t profile;
     uint32_t irregular;
+    double transition_diameter;
+    double terrace_onset;
+    double terrace_full;
+    double terrace_min_freshness;
 } tg_crater_shaping;
 
 /* The craters the layer draws over `region` (x0, y0, x1, y1 in meters), in the reference's order

@@ -41,6 +41,7 @@ class Scene(C.Structure):
         ("boulders", _I32), ("boulderSeed", _U32), ("boulderCoefficient", _D),
         ("boulderExponent", _D), ("boulderMin", _D), ("boulderMax", _D), ("heightRatio", _D),
         ("datum", _I32), ("interiorReplacement", _D), ("bodyRadius", _D),
+        ("terraceMinFreshness", _D),
     ]
 
 
@@ -70,7 +71,7 @@ def make_scene(grid, source_fractals=None, elevation=0.0, layer_fractals=None, c
                         profile=0, transitionDiameter=15000.0, applyPreset=0,
                         noiseAmplitude=0.0, rimNoiseAmplitude=0.0, wallStreaks=0.0, ejecta=0.0,
                         rimSigma=0.0, terraceOnset=0.0, terraceFull=0.0, datum=0,
-                        interiorReplacement=0.0)
+                        interiorReplacement=0.0, terraceMinFreshness=0.0)
         defaults.update(craters)
         for k, v in defaults.items():
             setattr(s, k, v)

@@ -87,6 +87,8 @@ struct tgref_scene {
     // a sphere of this radius (m) when positive, the grid's transform then in degrees of
     // longitude and latitude; a plane when 0
     double bodyRadius;
+    // CraterTerraces::minFreshness when positive (with terraceOnset); the default 0.3 otherwise
+    double terraceMinFreshness;
 };
 
 const char* tgref_error() {
@@ -151,6 +153,9 @@ std::shared_ptr<CraterLayer> MakeCraterLayer(const tgref_scene& s, TerrainBase b
     if (s.terraceOnset > 0.0) {
         options.apply.terraces.onsetDiameter = s.terraceOnset;
         options.apply.terraces.fullDiameter = s.terraceFull;
+        if (s.terraceMinFreshness > 0.0) {
+            options.apply.terraces.minFreshness = s.terraceMinFreshness;
+        }
     }
     return std::make_shared<CraterLayer>(std::move(models), std::move(options), std::move(base));
 }

@@ -51,6 +51,7 @@ SIGNATURES = {
     "tg_last_error": [],
     "tg_device_name": [_P, C.c_char_p, _SZ],
     "tg_synchronize": [_P],
+    "tg_set_wait_limit": [_P, _U32],
     "tg_noise_layer": [_P, _P, _SZ, C.POINTER(Grid), _D, _D, _P, NoData, _I, _P],
     "tg_noise_layer_rows": [_P, _P, _SZ, _P, _P, _U32, _U32, _P, NoData, _I, _P],
     "tg_noise_source": [_P, _P, _U32, _F, C.POINTER(Grid), _P, _I, _P],
@@ -74,7 +75,9 @@ class Population(C.Structure):
 
 
 class Shaping(C.Structure):
-    _fields_ = [("profile", C.c_uint32), ("irregular", C.c_uint32)]
+    _fields_ = [("profile", C.c_uint32), ("irregular", C.c_uint32),
+                ("transition_diameter", C.c_double), ("terrace_onset", C.c_double),
+                ("terrace_full", C.c_double), ("terrace_min_freshness", C.c_double)]
 
 
 class BoulderPopulation(C.Structure):

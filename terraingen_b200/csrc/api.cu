@@ -276,6 +276,15 @@ int tg_device_name(tg_device* d, char* name, size_t capacity) {
     return TG_OK;
 }
 
+int tg_set_wait_limit(tg_device* d, uint32_t polls) {
+    if (int s = check_device(d)) {
+        return s;
+    }
+    std::lock_guard<std::mutex> lock(d->mutex);
+    d->waitPolls = polls;
+    return TG_OK;
+}
+
 int tg_synchronize(tg_device* d) {
     if (int s = check_device(d)) {
         return s;
@@ -566,13 +575,13 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
     bins.capacity = total;
-    p.fast = crater_fast_path(k, d->pinnedStatus[1]);
+    p.fast = crater_lean_entries(k);
     if (p.fast && nData > 0) {
         TG_CUDA(d->slots[kHarmonics].reserve(size_t(nData) * sizeof(float)), "allocation");
         p.harmonics = slot_ptr<float>(d, kHarmonics);
         TG_CUDA(launch_crater_harmonics(rec, n, data, p.harmonics, s), "harmonics launch");
     }
-    TG_CUDA(launch_crater_scatter(rec, n, g, bins, s), "crater scatter launch");
+    TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, s), "crater scatter launch");
     p.any = true;
     return TG_OK;
 }
@@ -604,7 +613,8 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(launch_crater_shape(k, data, p.harmonics, p.fast, g, to_nodata(nodata), p.bins, dh, s),
+    TG_CUDA(launch_crater_shape(k, data, p.harmonics, p.fast, g, to_nodata(nodata), p.bins, dh, s,
+                                0, 0xffffffffu, d->waitPolls),
             "crater shape launch");
     return crater_finish(d, p, s);
 }
@@ -686,7 +696,8 @@ int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), p.bins, dh, p.status, s),
+    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), p.bins, dh, p.status, s, 0,
+                                0xffffffffu, d->waitPolls),
             "boulder bake launch");
     return boulder_finish(d, p, s);
 }
@@ -1137,13 +1148,13 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
             if (cp.any) {
                 if (cudaError_t e = launch_crater_shape(k, static_cast<const float*>(ddata),
                                                         cp.harmonics, cp.fast, g, none, cp.bins,
-                                                        dh, s, k0, rows)) {
+                                                        dh, s, k0, rows, d->waitPolls)) {
                     return drain(cuda_fail(e, "crater shape launch"));
                 }
             }
             if (bp.any) {
                 if (cudaError_t e = launch_boulder_bake(g, t->boulder_width, none, bp.bins, dh,
-                                                        bp.status, s, k0, rows)) {
+                                                        bp.status, s, k0, rows, d->waitPolls)) {
                     return drain(cuda_fail(e, "boulder bake launch"));
                 }
             }

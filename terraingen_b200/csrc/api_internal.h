@@ -113,6 +113,8 @@ struct tg_device {
     uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
     // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
     unsigned long long craterPairs = 0, boulderPairs = 0;
+    // Polls of a staged copy before the binned kernels give up on it (tg_set_wait_limit).
+    uint32_t waitPolls = tgb::kWaitPolls;
     // The seam solve's scratch, kept across calls and released by tg_close.
     void* seams = nullptr;
     void (*releaseSeams)(void*) = nullptr;

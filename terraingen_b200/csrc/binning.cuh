@@ -10,7 +10,7 @@
 namespace tgb {
 namespace binning {
 
-constexpr uint32_t kSpinLimit = 1u << 26;  // polls before a staged copy is given up on
+constexpr uint32_t kSpinLimit = kWaitPolls;  // polls before a staged copy is given up on
 
 __device__ __forceinline__ bool is_nodata(NoData nd, float h) {
     if (nd.mode == 1u) {
@@ -98,6 +98,38 @@ __device__ __forceinline__ bool disk_meets_box(double x, double y, double radius
     return dx * dx + dy * dy <= radius * radius;
 }
 
+// Whether the kernel's options add nothing beyond the profile and the outline: a closed-form
+// simple profile (complex craters allowed), no diffusion tables, rim smoothing, noise, texture,
+// ejecta or burial.
+__host__ __device__ inline bool crater_options_plain(const CraterShapeKernel& k) {
+    const CraterProfileKernel& p = k.profile;
+    return (p.simple == kProfileFassettThomson || p.simple == kProfileMartinParkesDunstan) &&
+           p.diffused == 0u && k.rimSigma == 0.0f && k.noiseAmplitude == 0.0f &&
+           k.noiseRimAmplitude == 0.0f && k.wallStreaks == 0.0f && k.ejecta == 0.0f &&
+           k.mantling == 0.0f;
+}
+
+// Whether crater `r` shapes as a complex crater (FreshProfileHeight, craters.h:500).
+__host__ __device__ inline bool crater_is_complex(const CraterShapeKernel& k,
+                                                  const CraterRecord& r) {
+    return k.profile.complex == 1u && r.diameter >= k.profile.transitionDiameter;
+}
+
+// Radii (of the outline-scaled profile distance) beyond which crater `r` adds nothing. The
+// kernel's reach, except for a simple crater under a complex profile with plain options: the
+// complex profile stretches every crater's reach to 3 radii (ComplexCraterProfile::ReachRadii),
+// but a simple crater's relief is its simple profile's, exactly 0 beyond 1.5 radii
+// (FassettThomsonShape) or 2 (MartinParkesDunstanHeight), and nothing else adds to it.
+__host__ __device__ inline float crater_cull_radii(const CraterShapeKernel& k,
+                                                   const CraterRecord& r) {
+    if (k.profile.complex == 1u && !crater_is_complex(k, r) && crater_options_plain(k) &&
+        r.peakCount == 0u && r.upslopeX == 0.0f && r.upslopeY == 0.0f && r.hasDatum == 0u) {
+        const float simple = k.profile.simple == kProfileMartinParkesDunstan ? 2.0f : 1.5f;
+        return simple < k.reachRadii ? simple : k.reachRadii;
+    }
+    return k.reachRadii;
+}
+
 __device__ inline Footprint crater_footprint(const CraterShapeKernel& k, const CraterRecord& r,
                                              const float* data, const double* footprints,
                                              uint32_t i, const Grid& g) {
@@ -141,8 +173,8 @@ __device__ inline Footprint crater_footprint(const CraterShapeKernel& k, const C
                            r.shiftY != 0.0f;
     // A little slack over the bound: the profile distance is rounded in float.
     f.cull = stretched ? INFINITY
-                       : float(scale * double(k.reachRadii) * (0.5 * double(r.diameter)) *
-                               (1.0 + 1e-5)) + 1e-6f;
+                       : float(scale * double(crater_cull_radii(k, r)) *
+                               (0.5 * double(r.diameter)) * (1.0 + 1e-5)) + 1e-6f;
     return f;
 }
 
@@ -152,6 +184,16 @@ __device__ __forceinline__ bool crater_heavy(const CraterRecord& r) {
     return r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u || r.peakCount > 0u ||
            r.shiftX != 0.0f || r.shiftY != 0.0f || r.upslopeX != 0.0f || r.upslopeY != 0.0f ||
            r.hasDatum == 1u;
+}
+
+// Whether the plain binned kernel's lean path (crater_math.cuh `lean_contribution`) cannot shape
+// crater `r`: tables, marks, terraces, a floor shift, an upslope or a datum. Complex craters and
+// their massif peaks are lean.
+__device__ __forceinline__ bool crater_entry_heavy(const CraterShapeKernel& k,
+                                                   const CraterRecord& r) {
+    (void)k;
+    return r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
+           r.shiftY != 0.0f || r.upslopeX != 0.0f || r.upslopeY != 0.0f || r.hasDatum == 1u;
 }
 
 // The pixel window of a box on the grid (PixelWindowIn, src/raster/cell_loops.cpp:21-28).
@@ -235,9 +277,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return done != 0u;
 }
 
-// Waits for the barrier's phase, giving up after kSpinLimit polls (returns false then).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    for (uint32_t spin = 0; spin < kSpinLimit; ++spin) {
+// Waits for the barrier's phase, giving up after `limit` polls (returns false then).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase,
+                                          uint32_t limit = kSpinLimit) {
+    for (uint32_t spin = 0; spin < limit; ++spin) {
         if (mbar_try_wait(bar, phase)) {
             return true;
         }

@@ -85,7 +85,7 @@ __global__ void boulder_scatter_kernel(const BoulderRecord* __restrict__ boulder
 __global__ void __launch_bounds__(kThreads, 4)
     boulder_bake_kernel(const Grid grid, const double width, const NoData nodata,
                         const BoulderBins bins, float* __restrict__ heights,
-                        uint32_t* __restrict__ flags) {
+                        uint32_t* __restrict__ flags, const uint32_t polls) {
     __shared__ __align__(128) BoulderEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
     const uint32_t bin = bins.firstBin + blockIdx.x;
@@ -158,24 +158,21 @@ __global__ void __launch_bounds__(kThreads, 4)
     uint32_t evaluated = 0;
     for (uint32_t c = 0; c < chunks; ++c) {
         const uint32_t s = c & 1u;
-        bool arrived = false;
-        for (uint32_t spin = 0; spin < kSpinLimit && !arrived; ++spin) {
-            uint32_t done;
-            asm volatile(
-                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n "
-                "selp.u32 %0, 1, 0, p;\n}"
-                : "=r"(done)
-                : "r"(smem_addr(&bars[s])), "r"(phase[s])
-                : "memory");
-            arrived = done != 0u;
-        }
-        phase[s] ^= 1u;
+        const bool arrived = mbar_wait(&bars[s], phase[s], polls);
         if (__syncthreads_or(!arrived)) {
+            // A copy did not land within `polls`: record it, then wait (bounded by the default
+            // limit) for the copies still in flight into this buffer and the other one (chunk
+            // c + 1 is issued by now), so no bulk copy is left writing into a finished CTA.
             if (tid == 0) {
                 atomicOr(flags, 2u);
+                mbar_wait(&bars[s], phase[s]);
+                if (c + 1 < chunks) {
+                    mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                }
             }
             return;
         }
+        phase[s] ^= 1u;
         const uint32_t n = min(kChunk, count - c * kChunk);
         for (uint32_t e = 0; e < n; ++e) {
             const BoulderEntry& b = stage[s][e];
@@ -245,7 +242,8 @@ cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
 
 cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 const BoulderBins& bins, float* heights, uint32_t* flags,
-                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows) {
+                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows,
+                                uint32_t polls) {
     if (firstBinRow >= bins.binsY) {
         return cudaSuccess;
     }
@@ -257,7 +255,7 @@ cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
     BoulderBins strip = bins;
     strip.firstBin = firstBinRow * bins.binsX;
     boulder_bake_kernel<<<nbins, kThreads, 0, stream>>>(grid, width, nodata, strip, heights,
-                                                        flags);
+                                                        flags, polls);
     return cudaGetLastError();
 }
 

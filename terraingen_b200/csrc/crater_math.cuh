@@ -1011,5 +1011,50 @@ __device__ __forceinline__ float fast_contribution(const FastKernel& k,
     return c.resolution * height;
 }
 
+// The lean path of the plain binned kernel: fast_contribution's outline by rotation, and also
+// complex craters (a closed-form `ComplexProfileHeight` with its round dome) and their massif
+// peaks (`KernelPeakRelief`, whose noise runs in a separate function only near the center). The
+// record must carry nothing the general path alone handles (tables, marks, terraces, a floor
+// shift, an upslope or a datum), and the kernel's options must be plain (crater_options_plain).
+__device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
+                                                   const float* __restrict__ harmonics,
+                                                   const float* __restrict__ data,
+                                                   const CraterRecord& c, float dx, float dy,
+                                                   bool& reached) {
+    const float radius = 0.5f * c.diameter;
+    float distance = sqrtf(dx * dx + dy * dy);
+    if (c.ellipticity != 1.0f || c.harmonicCount > 0u) {
+        const float share = outline_share(distance / radius) * worn_outline_share(c);
+        distance /= fast_outline_scale(harmonics, c, dx, dy, distance, share);
+    }
+    reached = distance < k.reachRadii * radius;
+    if (!reached) {
+        return 0.0f;
+    }
+    float height;
+    if (k.profile.complex == 1u && c.diameter >= k.profile.transitionDiameter) {
+        const State s{c.freshDepth, c.freshRim, c.currentDepth, c.currentRim};
+        height = complex_height(k.profile, distance, c.diameter, s);
+        if (c.peakCount > 0u) {
+            height += peak_relief(k, data, c, s, distance, dx, dy);
+        }
+    } else if (k.profile.simple == kProfileMartinParkesDunstan) {
+        height = mpd_height(distance, c.diameter, c.freshRim, c.currentDepth, c.currentRim);
+    } else {
+        height = ft_shape(distance / radius, k.profile.rim, c.freshRim, c.currentDepth) *
+                 c.diameter;
+    }
+    return c.resolution * height;
+}
+
+// The general contribution as a function of its own, so the kernels that call it for a few
+// heavy records keep the lean path's register budget.
+static __device__ __noinline__ Contribution general_contribution(const CraterShapeKernel& k,
+                                                                 const float* data,
+                                                                 const CraterRecord& c, float dx,
+                                                                 float dy) {
+    return crater_contribution(k, data, c, dx, dy);
+}
+
 }  // namespace crater
 }  // namespace tgb

@@ -57,8 +57,9 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
             if (r.hasDatum == 1u) {
                 atomicOr(flags, 1u);
             }
-            // Anything beyond an ellipse and power-law harmonics needs the general path.
-            if (crater_heavy(r)) {
+            // Anything beyond an ellipse and power-law harmonics, or a complex crater, needs
+            // the general path.
+            if (crater_entry_heavy(k, r)) {
                 atomicOr(flags, 4u);
             }
         }
@@ -87,7 +88,8 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
 // Each warp takes 32 craters and spreads all of their (crater, bin) pairs over its lanes: a
 // lane finds its pair's crater by a search of the warp's running bin counts, then copies the
 // crater's record and tail into its bin's next slot.
-__global__ void crater_scatter_kernel(const CraterRecord* __restrict__ records, uint32_t n,
+__global__ void crater_scatter_kernel(const CraterShapeKernel k,
+                                      const CraterRecord* __restrict__ records, uint32_t n,
                                       CraterBins bins) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
@@ -154,9 +156,10 @@ __global__ void crater_scatter_kernel(const CraterRecord* __restrict__ records, 
         for (int w = 0; w < 9; ++w) {
             dst[w] = __ldg(src + w);
         }
+        const uint32_t heavy = crater_entry_heavy(k, records[crater]) ? kHeavyEntry : 0u;
         dst[9] = make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
                            int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
-                           int(crater));
+                           int(crater | heavy));
     }
 }
 
@@ -187,19 +190,23 @@ __global__ void crater_harmonics_kernel(const CraterRecord* __restrict__ records
 // small crater that needs a handful of cells no longer leaves most lanes of the warp idle. The
 // contributions are FP32 values added into FP64 accumulators in shared memory: that sum is exact
 // for these magnitudes, so the atomic adds give the same bits in any order.
+//
+// With kFast, entries marked kHeavyEntry (complex craters, peaks, terraces, tables) queue apart
+// and are drained through the general contribution, so a batch with a few such craters keeps the
+// lean path for all the others.
 constexpr int kQueue = 160;  // 31 pairs left over plus one crater's 128
 
 template <bool kFast>
-__global__ void __launch_bounds__(kShapeThreads)
+__global__ void __launch_bounds__(kShapeThreads, kFast ? 2 : 1)
     crater_shape_kernel(const CraterShapeKernel k, const float* __restrict__ data,
                         const float* __restrict__ harmonics, const Grid grid, const NoData nodata,
                         const CraterBins bins, float* __restrict__ heights,
-                        uint32_t* __restrict__ flags) {
-    const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
+                        uint32_t* __restrict__ flags, const uint32_t polls) {
     __shared__ __align__(128) BinEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ double accs[kShapeThreads / 32][128];
     __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
+    __shared__ uint16_t heavyQueues[kShapeThreads / 32][kFast ? kQueue : 1];
     __shared__ float2 columns[kShapeThreads / 32][32];  // split x of the warp's 32 columns
     __shared__ float2 rows[kShapeThreads / 32][4];      // split y of its 4 rows
 
@@ -215,6 +222,7 @@ __global__ void __launch_bounds__(kShapeThreads)
     const uint32_t col0 = binX * kBinCells + (lane % 8u) * kCellsPerThread;
     double* acc = accs[warp];
     uint16_t* queue = queues[warp];
+    uint16_t* heavyQueue = heavyQueues[warp];
     const uint32_t cell0 = (lane / 8u) * 32u + (lane % 8u) * kCellsPerThread;
 
     // This thread's cells: split positions (MakeSplitPoint, crater_kernel.cpp:303) of the
@@ -260,10 +268,12 @@ __global__ void __launch_bounds__(kShapeThreads)
     const float halfW = 15.75f * float(fabs(grid.pixelWidth));
     const float halfH = 1.75f * float(fabs(grid.pixelHeight));
 
-    // Evaluates the 32 (or, at a flush, `n`) queued pairs from `from`, one per lane.
-    auto drain = [&](const BinEntry* chunk, uint32_t from, uint32_t n) {
+    // Evaluates the 32 (or, at a flush, `n`) pairs queued in `q` from `from`, one per lane; the
+    // general contribution when `general` (always without kFast).
+    auto drain = [&](const BinEntry* chunk, const uint16_t* q, uint32_t from, uint32_t n,
+                     bool general) {
         if (lane < n) {
-            const uint32_t code = queue[from + lane];
+            const uint32_t code = q[from + lane];
             const BinEntry& entry = chunk[code >> 7];
             const CraterRecord& r = entry.record;
             const uint32_t cell = code & 127u;
@@ -271,11 +281,17 @@ __global__ void __launch_bounds__(kShapeThreads)
             const float2 cy = rows[warp][cell >> 5];
             const float dy = crater::split_difference(cy.x, cy.y, r.y, r.yLow);
             const float dx = crater::split_difference(cx.x, cx.y, r.x, r.xLow);
-            if (kFast) {
+            if (kFast && !general) {
                 bool reached;
-                const float shaped = crater::fast_contribution(fk, harmonics, r, dx, dy, reached);
+                const float shaped =
+                    crater::lean_contribution(k, harmonics, data, r, dx, dy, reached);
                 if (reached) {
                     atomicAdd(acc + cell, double(shaped));
+                }
+            } else if (kFast) {
+                const crater::Contribution q = crater::general_contribution(k, data, r, dx, dy);
+                if (q.reached) {
+                    atomicAdd(acc + cell, double(q.shaped));
                 }
             } else {
                 const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
@@ -312,23 +328,26 @@ __global__ void __launch_bounds__(kShapeThreads)
     uint32_t evaluated = 0;  // (cell, crater) pairs this warp queued, for the pair counter
     for (uint32_t c = 0; c < chunks; ++c) {
         const uint32_t s = c & 1u;
-        if (!mbar_wait(&bars[s], phase[s])) {
+        if (!mbar_wait(&bars[s], phase[s], polls)) {
             failed = true;
         }
-        phase[s] ^= 1u;
         if (__syncthreads_or(failed)) {
-            // A copy did not land: record it and wait (bounded) for the other buffer's copy
-            // before leaving, so no bulk copy is left writing into a finished CTA.
+            // A copy did not land within `polls`: record it, then wait (bounded by the default
+            // limit) for the copies still in flight into this buffer and the other one (chunk
+            // c + 1 is issued by now), so no bulk copy is left writing into a finished CTA.
             if (tid == 0) {
                 atomicOr(flags, 2u);
+                mbar_wait(&bars[s], phase[s]);
                 if (c + 1 < chunks) {
                     mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
                 }
             }
             return;
         }
+        phase[s] ^= 1u;
         const uint32_t n = min(kChunk, count - c * kChunk);
-        uint32_t queued = 0;  // warp-uniform
+        uint32_t queued = 0;       // warp-uniform
+        uint32_t heavyQueued = 0;  // warp-uniform
         for (uint32_t e = 0; e < n; ++e) {
             const BinEntry& entry = stage[s][e];
             const CraterRecord& r = entry.record;
@@ -375,23 +394,30 @@ __global__ void __launch_bounds__(kShapeThreads)
                 continue;
             }
             before -= mine;
-            uint32_t slot = queued + before;
+            const bool heavy = kFast && (entry.index & kHeavyEntry) != 0u;  // warp-uniform
+            uint16_t* q = heavy ? heavyQueue : queue;
+            uint32_t& length = heavy ? heavyQueued : queued;
+            uint32_t slot = length + before;
             for (int j = 0; j < kCellsPerThread; ++j) {
                 if (need & (1u << j)) {
-                    queue[slot++] = uint16_t((e << 7) | (cell0 + j));
+                    q[slot++] = uint16_t((e << 7) | (cell0 + j));
                 }
             }
             evaluated += mine;
-            queued += total;
+            length += total;
             __syncwarp();
-            while (queued >= 32u) {
-                queued -= 32u;
-                drain(stage[s], queued, 32u);
+            while (length >= 32u) {
+                length -= 32u;
+                drain(stage[s], q, length, 32u, heavy);
                 __syncwarp();
             }
         }
         if (queued > 0u) {
-            drain(stage[s], 0u, queued);
+            drain(stage[s], queue, 0u, queued, false);
+            __syncwarp();
+        }
+        if (kFast && heavyQueued > 0u) {
+            drain(stage[s], heavyQueue, 0u, heavyQueued, true);
             __syncwarp();
         }
         if (c + 2 < chunks) {
@@ -614,15 +640,16 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const Grid& grid,
-                                  const CraterBins& bins, cudaStream_t stream) {
+cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
+                                  uint32_t n, const Grid& grid, const CraterBins& bins,
+                                  cudaStream_t stream) {
     (void)grid;
     if (n == 0) {
         return cudaSuccess;
     }
     const uint32_t threads = 256;  // 8 warps of 32 craters
     const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
-    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(records, n, bins);
+    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(k, records, n, bins);
     return cudaGetLastError();
 }
 
@@ -644,10 +671,15 @@ bool crater_fast_path(const CraterShapeKernel& k, uint32_t batchFlags) {
            k.ejecta == 0.0f;
 }
 
+bool crater_lean_entries(const CraterShapeKernel& k) {
+    return crater_options_plain(k);
+}
+
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
                                 const float* harmonics, bool fast, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
-                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows) {
+                                cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows,
+                                uint32_t polls) {
     if (firstBinRow >= bins.binsY) {
         return cudaSuccess;
     }
@@ -660,10 +692,10 @@ cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
     strip.firstBin = firstBinRow * bins.binsX;
     if (fast) {
         crater_shape_kernel<true><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1);
+            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1, polls);
     } else {
         crater_shape_kernel<false><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1);
+            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1, polls);
     }
     return cudaGetLastError();
 }

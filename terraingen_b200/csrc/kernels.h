@@ -89,20 +89,32 @@ struct CraterBins {
 cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
                                 uint32_t n, const float* data, const double* footprints,
                                 const Grid& grid, const CraterBins& bins, cudaStream_t stream);
-cudaError_t launch_crater_scatter(const CraterRecord* records, uint32_t n, const Grid& grid,
-                                  const CraterBins& bins, cudaStream_t stream);
+// Scatters each crater's BinEntry into its bins; an entry whose crater needs the general shaping
+// path (crater_entry_heavy) carries kHeavyEntry in its `index`.
+cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
+                                  uint32_t n, const Grid& grid, const CraterBins& bins,
+                                  cudaStream_t stream);
+constexpr uint32_t kHeavyEntry = 0x80000000u;
 // Whether a batch takes the lean shaping path (crater_math.cuh `fast_contribution`): the
 // kernel's options allow it and the count pass saw no record feature beyond outlines
-// (`batchFlags` bit 2).
+// (`batchFlags` bit 2). The batched and served forms use this whole-batch rule.
 bool crater_fast_path(const CraterShapeKernel& k, uint32_t batchFlags);
+// Whether the plain path's binned kernel shapes the batch lean entry by entry: the kernel's
+// options allow the lean path (a closed-form simple profile, complex craters allowed, no rim
+// smoothing, noise or texture); entries marked kHeavyEntry (complex craters, terraces, peaks,
+// tables, marks, shifts) take the general path inside the same launch.
+bool crater_lean_entries(const CraterShapeKernel& k);
 // The lean path's harmonics: (amplitude cos phase, amplitude sin phase) at the data's offsets.
 cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, const float* data,
                                     float* harmonics, cudaStream_t stream);
+// Polls of a staged copy before a binned kernel gives up on it (flag 2, TG_ERROR_TIMEOUT).
+constexpr uint32_t kWaitPolls = 1u << 26;
+
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
                                 const float* harmonics, bool fast, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
                                 cudaStream_t stream, uint32_t firstBinRow = 0,
-                                uint32_t binRows = 0xffffffffu);
+                                uint32_t binRows = 0xffffffffu, uint32_t polls = kWaitPolls);
 
 // The drop-in form: the reference's own tile lists (`CraterTiles`, apply.cpp:111-143), craters
 // applied in list order exactly as ShapeTilesOnCpu does (apply.cpp:199-222).
@@ -154,7 +166,7 @@ cudaError_t launch_boulder_scatter(const BoulderRecord* boulders, uint32_t n,
 cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 const BoulderBins& bins, float* heights, uint32_t* flags,
                                 cudaStream_t stream, uint32_t firstBinRow = 0,
-                                uint32_t binRows = 0xffffffffu);
+                                uint32_t binRows = 0xffffffffu, uint32_t polls = kWaitPolls);
 
 // --- diamond-square ----------------------------------------------------------------------
 // Nodes of one level over columns [c0, c0 + w) and rows [r0, r0 + h), row-major doubles.

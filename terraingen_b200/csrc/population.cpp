@@ -477,6 +477,465 @@ double max_outline_scale(bool irregular) {  // MaxOutlineScale (irregularity.cpp
     return rough * std::sqrt(1.5);
 }
 
+// --- profile heights ------------------------------------------------------------------------
+//
+// The reference's CraterProfile::Height implementations evaluate the kernel header's float math
+// (fassett_thomson.cpp:14, martin_parkes_dunstan.cpp, complex.cpp:70-78, on
+// include/terraingen/layers/kernels/craters.h:330-505). Terrace records sample them, so they are
+// restated here in float, in the header's operation order (this unit is compiled with
+// -ffp-contract=off and calls the host libm's powf and sqrtf, as the reference's build does).
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kDegree = kPi / 180.0;
+constexpr float kKernelPiF = 3.14159265358979f;
+
+// The shape fields of a record (KernelStateRecord, profiles/profile.h:34).
+struct ShapeState {
+    float diameter, freshDepth, freshRim, currentDepth, currentRim;
+};
+
+ShapeState shape_state(double diameter, double freshDepth, double freshRim, double currentDepth,
+                       double currentRim) {
+    return ShapeState{float(diameter), float(freshDepth), float(freshRim), float(currentDepth),
+                      float(currentRim)};
+}
+
+float ft_exterior(float x, float start) {  // craters.h:330
+    const float polynomial =
+        0.188253307f + x * (-0.187050452f + x * (0.01844746f + x * 0.01505647f));
+    const float u = (x - start) / (1.5f - start);
+    return polynomial * (1.0f - u * u);
+}
+
+float ft_shape(float x, uint32_t rim, float freshRim, float currentDepth) {  // craters.h:337
+    if (x > 1.5f) {
+        return 0.0f;
+    }
+    const float interior =
+        -0.228809953f + x * (0.227533882f + x * (0.083116795f - x * 0.039499407f));
+    float h = 0.0f;
+    if (rim == 2u) {
+        h = x <= 0.98f ? interior : (x <= 1.02f ? freshRim : ft_exterior(x, 1.02f));
+    } else {
+        const float edge = rim == 0u ? 0.98f : 1.0f;
+        h = x <= 0.2f ? -0.181f : (x <= edge ? interior : ft_exterior(x, edge));
+    }
+    return std::max(h, freshRim - currentDepth);
+}
+
+struct ProfilePoint {
+    float height, slope;
+};
+
+ProfilePoint mpd_exterior(float x, float rim, float ejectaScale) {  // craters.h:377
+    const float offset = rim - ejectaScale;
+    const float gradient = -ejectaScale / 8.0f - offset;
+    const float r = 1.0f / (x + 1.0f);
+    const float law = ejectaScale * r * r * r + offset + gradient * x;
+    const float lawSlope = -3.0f * ejectaScale * r * r * r * r + gradient;
+    const float taper = 1.0f - x * x;
+    return ProfilePoint{law * taper, lawSlope * taper - 2.0f * x * law};
+}
+
+float mpd_height(float distance, float diameter, const ShapeState& c) {  // craters.h:391
+    const float depth = c.currentDepth * diameter;
+    const float rim = c.currentRim * diameter;
+    const float freshRim = c.freshRim * diameter;
+    const float radius = 0.5f * diameter;
+    const float x = distance / radius - 1.0f;
+    if (x >= 1.0f) {
+        return 0.0f;
+    }
+    const float k = freshRim - rim + depth;
+    const float alpha = (rim - freshRim) / k;
+    if (x <= alpha) {
+        return (k * x + 2.0f * k) * x + freshRim;
+    }
+    if (x <= 0.0f) {
+        return k * (alpha + 1.0f) / alpha * x * x + rim;
+    }
+    const float scale = 0.14f * std::pow(radius, 0.74f);  // KernelEjectaScale
+    const float ejectaScale = freshRim > 0.0f ? scale * rim / freshRim : scale;
+    const float beta = std::min(1.0f, 1.5f * (freshRim - rim) / k);
+    if (x <= beta) {
+        const ProfilePoint join = mpd_exterior(beta, rim, ejectaScale);
+        const float drop = rim - join.height;
+        const float slope = drop > 0.0f ? std::max(join.slope, -3.0f * drop / beta) : join.slope;
+        const float t = x / beta;
+        return rim + (join.height - rim) * t * t * (3.0f - 2.0f * t) +
+               beta * slope * t * t * (t - 1.0f);
+    }
+    return mpd_exterior(x, rim, ejectaScale).height;
+}
+
+float kilometer_law(float coefficient, float exponent, float diameter, bool volume) {
+    const float kilometers = coefficient * std::pow(diameter / 1000.0f, exponent);
+    return volume ? kilometers * 1e9f : kilometers * 1000.0f;
+}
+
+// The lunar complex shape (LunarComplexCraterShape) from a transition diameter, in the kernel's
+// form (SetKernelComplexShape, complex.cpp:37-52).
+void set_complex_shape(CraterProfileKernel& p, double transition) {
+    p.complex = 1u;
+    p.transitionDiameter = float(transition);
+    p.floorCoefficient = float(0.187);
+    p.floorExponent = float(1.249);
+    p.peakHeightCoefficient = float(0.589e-3);
+    p.peakHeightExponent = float(1.969);
+    p.peakWidthCoefficient = float(0.987e-7);  // the peak volume law: no peak diameter law
+    p.peakWidthExponent = float(5.078);
+    p.peakFromVolume = 1u;
+    p.peakFitMaxDiameter = float(51000.0);
+    p.ejectaExponent = 3.0f;
+    p.complexReachRadii = 3.0f;
+}
+
+float complex_height(const CraterProfileKernel& p, float distance, float diameter,
+                     const ShapeState& c) {  // ComplexProfileHeight, craters.h:477
+    const float radius = 0.5f * diameter;
+    const float x = distance / radius;
+    const float depth = c.currentDepth * diameter;
+    const float rim = c.currentRim * diameter;
+    if (x >= 1.0f) {
+        if (x >= p.complexReachRadii) {
+            return 0.0f;
+        }
+        const float edge = std::pow(p.complexReachRadii, -p.ejectaExponent);
+        return rim * (std::pow(x, -p.ejectaExponent) - edge) / (1.0f - edge);
+    }
+    const float floorShare = std::min(
+        0.9f, kilometer_law(p.floorCoefficient, p.floorExponent, diameter, false) / diameter);
+    float height = rim - depth;
+    if (x > floorShare) {
+        const float t = (x - floorShare) / (1.0f - floorShare);
+        height += depth * t * t;
+    }
+    // KernelComplexPeak and KernelPeakDome (craters.h:446-471), lowered by the kept depth.
+    const float fitted =
+        p.peakFitMaxDiameter > 0.0f ? std::min(diameter, p.peakFitMaxDiameter) : diameter;
+    float peakHeight = kilometer_law(p.peakHeightCoefficient, p.peakHeightExponent, fitted, false);
+    float base;
+    if (p.peakFromVolume == 1u) {
+        const float volume = kilometer_law(p.peakWidthCoefficient, p.peakWidthExponent, fitted, true);
+        base = std::sqrt(3.0f * volume / (kKernelPiF * peakHeight));
+    } else {
+        base = 0.5f * kilometer_law(p.peakWidthCoefficient, p.peakWidthExponent, fitted, false);
+    }
+    base *= diameter / fitted;
+    float dome = 0.0f;
+    if (distance < base) {
+        const float u = 1.0f - (distance / base) * (distance / base);
+        dome = peakHeight * u * u;
+    }
+    const float kept = c.freshDepth > 0.0f ? c.currentDepth / c.freshDepth : 1.0f;
+    return height + kept * dome;
+}
+
+// The layer's profile as CraterProfile::Height evaluates it (in double, from float math).
+struct LayerProfile {
+    uint32_t simple = 0;  // 0 Fassett-Thomson (Original rim), 1 Martin-Parkes-Dunstan
+    bool complex = false;
+    double transition = 0.0;
+    CraterProfileKernel kernel{};  // the complex profile's own kernel form
+
+    double simple_reach() const { return simple == 1u ? 2.0 : 1.5; }
+    // ComplexCraterProfile::ReachRadii (complex.cpp:66): the larger of the two reaches.
+    double reach() const { return complex ? std::fmax(simple_reach(), 3.0) : simple_reach(); }
+    bool is_complex(double diameter) const { return complex && diameter >= transition; }
+
+    double height(double distance, double diameter, const ShapeState& s) const {
+        if (is_complex(diameter)) {
+            return double(complex_height(kernel, float(distance), float(diameter), s));
+        }
+        const float d = float(diameter);
+        if (simple == 1u) {
+            return double(mpd_height(float(distance), d, s));
+        }
+        return double(ft_shape(float(distance) / (0.5f * d), 0u, s.freshRim, s.currentDepth) * d);
+    }
+};
+
+// --- wall terraces (AppendKernelTerraces, crater_kernel.cpp:312-509) --------------------------
+
+struct TerraceOptions {  // CraterTerraces' defaults (apply_options.h:183-226)
+    double onset = 20000.0, full = 65000.0;
+    int minBenches = 1, maxBenches = 4;
+    double benchSlopeDegrees = 3.0, scarpShare = 0.25, scarpSlopeDegrees = 35.0;
+    double arcShare = 0.6, rimVariation = 0.08, blockOffset = 0.6, blockGaps = 0.25;
+    double minFreshness = 0.3;
+};
+
+float terrace_ease(float v, float rounding) {  // KernelTerraceEase, craters.h:968
+    const float steepest = 1.0f / (1.0f - 0.5f * rounding);
+    if (v < rounding) {
+        return steepest * v * v / (2.0f * rounding);
+    }
+    return steepest * (v - 0.5f * rounding);
+}
+
+// The record's terraces, appended to `data`: the constants of the reference's terrace
+// construction (bench arcs, step bases by wall height, scarp scallops and block offsets, bench
+// levels that keep each step's mean height) and its draws, in its order.
+void append_terraces(const TerraceOptions& t, uint32_t seed, const LayerProfile& profile,
+                     double diameter, uint64_t id, double freshDepth, double freshRim,
+                     double currentDepth, double currentRim, CraterRecord& record,
+                     std::vector<float>& data) {
+    constexpr double kFullCover = 0.9, kArcWidth = 0.3, kNarrowest = 0.25, kRounding = 0.4;
+    constexpr double kMostScarp = 0.9, kSteepStep = 0.7, kSqueeze = 0.75, kScarpRoom = 0.4;
+    constexpr double kScarpReach = 1.2, kMinScallops = 6.0, kMaxScallops = 12.0;
+    constexpr double kRimScallop = 0.5, kLevelMargin = 0.1;
+    constexpr int kWallSamples = 256, kMeanSamples = 64, kLevelIterations = 30;
+    if (diameter < t.onset) {
+        return;
+    }
+    const ShapeState s = shape_state(diameter, freshDepth, freshRim, currentDepth, currentRim);
+    const double freshness = freshDepth > 0.0 ? currentDepth / freshDepth : 1.0;
+    const double strength = smoothstep((freshness - t.minFreshness) / (1.0 - t.minFreshness));
+    if (!(strength > 0.0)) {
+        return;
+    }
+    // The floor edge: the lunar shape's floor law, which is also the default (Pike's).
+    const double floorAt = double(kilometer_law(float(0.187), float(1.249), float(diameter), false));
+    const double inner = std::clamp(floorAt / diameter, 0.2, 0.9);
+    const double radius = 0.5 * diameter;
+    const double drop =
+        profile.height(radius, diameter, s) - profile.height(inner * radius, diameter, s);
+    const double meanSlope = drop / ((1.0 - inner) * radius);
+    const double benchSlope = std::tan(t.benchSlopeDegrees * kDegree);
+    const double scarpSlope =
+        std::tan(t.scarpSlopeDegrees * kDegree) * (1.0 - 0.5 * kRounding) * kSqueeze;
+    const double slopeShare =
+        meanSlope > 0.0 ? std::clamp(benchSlope / meanSlope, 0.02, 0.5) : 0.5;
+    const double size = std::clamp((diameter - t.onset) / (t.full - t.onset), 0.0, 1.0);
+    Stream random(seed, kCraterTerraceStream, uint32_t(id), uint32_t(id >> 32));
+    const double spread = t.maxBenches - t.minBenches;
+    const int benches = std::clamp(
+        int(std::lround(t.minBenches + spread * size + random.next_double() - 0.5)),
+        t.minBenches, t.maxBenches);
+    // Bench arcs: harmonics 2..6 with weights 1/k normalised, random phases.
+    double arcs[10];
+    {
+        double total = 0.0;
+        for (int k = 2; k < 7; ++k) {
+            total += 1.0 / k;
+        }
+        for (int k = 2; k < 7; ++k) {
+            arcs[2 * (k - 2)] = 1.0 / k / total;
+            arcs[2 * (k - 2) + 1] = 2.0 * kPi * random.next_double();
+        }
+    }
+    const double cover =
+        t.arcShare >= 1.0 ? 1.0 : t.arcShare + std::max(0.0, kFullCover - t.arcShare) * size;
+    double cut = -2.0;
+    if (cover < 1.0) {
+        constexpr size_t kSamples = 360;
+        std::vector<double> values(kSamples);
+        for (size_t n = 0; n < kSamples; ++n) {
+            const double theta = 2.0 * kPi * double(n) / double{kSamples};
+            double sum = 0.0;
+            for (size_t k = 0; k < 5; ++k) {
+                sum += arcs[2 * k] * std::cos((double(k) + 2.0) * theta + arcs[2 * k + 1]);
+            }
+            values[n] = sum;
+        }
+        const auto at = values.begin() + std::ptrdiff_t((1.0 - cover) * double{kSamples - 1});
+        std::nth_element(values.begin(), at, values.end());
+        cut = *at;
+    }
+    record.terraceCount = uint32_t(benches);
+    record.terraceOffset = uint32_t(data.size());
+    for (const double v : {inner, slopeShare, strength, kRounding, cut, kArcWidth}) {
+        data.push_back(float(v));
+    }
+    for (const double v : arcs) {
+        data.push_back(float(v));
+    }
+    auto scallopCount = [&random] {
+        return kMinScallops + std::floor((kMaxScallops - kMinScallops + 1.0) * random.next_double());
+    };
+    const double rimScallop =
+        kRimScallop * t.rimVariation * strength * (0.6 + 0.8 * random.next_double());
+    {
+        // Drawn left to right, as the reference's braced list is.
+        const double count = scallopCount();
+        const double phase = random.next_double();
+        for (const double v : {rimScallop, count, phase, t.blockGaps}) {
+            data.push_back(float(v));
+        }
+    }
+    // The wall's running-maximum height from the floor edge to the rim, 257 samples.
+    std::vector<double> wall(kWallSamples + 1);
+    for (size_t n = 0; n < wall.size(); ++n) {
+        const double u = double(n) / kWallSamples;
+        const double h = profile.height((inner + u * (1.0 - inner)) * radius, diameter, s);
+        wall[n] = n == 0 ? h : std::max(h, wall[n - 1]);
+    }
+    const double rise = wall.back() - wall.front();
+    auto across = [&](double share) {
+        if (!(rise > 0.0)) {
+            return share;
+        }
+        const double target = wall.front() + share * rise;
+        const auto above = std::lower_bound(wall.begin(), wall.end(), target);
+        if (above == wall.begin()) {
+            return 0.0;
+        }
+        if (above == wall.end()) {
+            return 1.0;
+        }
+        const double n = double(above - wall.begin());
+        const double gap = *above - *(above - 1);
+        const double part = gap > 0.0 ? (*above - target) / gap : 0.0;
+        return (n - part) / kWallSamples;
+    };
+    std::vector<double> heights{0.0};
+    double total = 0.0;
+    for (int i = 0; i < benches; ++i) {
+        total += 0.5 + random.next_double();
+        heights.push_back(total);
+    }
+    std::vector<double> bases;
+    for (double& h : heights) {
+        h /= total;
+        bases.push_back(across(h));
+    }
+    bases.back() = 1.0;
+    const double narrowest = kNarrowest / benches;
+    for (size_t k = 1; k + 1 < bases.size(); ++k) {
+        bases[k] = std::max(bases[k], bases[k - 1] + narrowest);
+    }
+    for (size_t k = bases.size() - 2; k > 0; --k) {
+        bases[k] = std::min(bases[k], bases[k + 1] - narrowest);
+    }
+    const double variation = t.rimVariation / (1.0 - inner);
+    for (size_t k = 1; k < bases.size() - 1; ++k) {
+        const double room = kScarpRoom * std::min(bases[k] - bases[k - 1], bases[k + 1] - bases[k]);
+        double scallop = std::min(variation * (0.6 + 0.8 * random.next_double()), 0.9 * room);
+        const double scallops = scallopCount();
+        const double phase = random.next_double();
+        double wobble = std::min(0.5 * variation * random.next_double(), 0.4 * room);
+        const double wobblePhase = 2.0 * kPi * random.next_double();
+        double block = t.blockOffset * room;
+        const double reach = 2.0 / 3.0 * scallop + wobble + block;
+        if (reach > kScarpReach * room) {
+            const double fit = kScarpReach * room / reach;
+            scallop *= fit;
+            wobble *= fit;
+            block *= fit;
+        }
+        const double key = double(random.next_u32() >> 8u);
+        for (const double v : {bases[k], scallop, scallops, phase, wobble, wobblePhase, block, key}) {
+            data.push_back(float(v));
+        }
+    }
+    auto wallAt = [&](double u) {
+        const double at = std::clamp(u, 0.0, 1.0) * kWallSamples;
+        const size_t n = std::min(size_t(at), wall.size() - 2);
+        return wall[n] + (at - double(n)) * (wall[n + 1] - wall[n]);
+    };
+    auto stairAt = [&](double within, double level, double scarp) {
+        const float rounding = float(kRounding);
+        const double lower = scarp * level;
+        const double upper = scarp * (1.0 - level);
+        double stair = level;
+        if (within < lower) {
+            stair = level * (1.0 - double{terrace_ease(float(1.0 - within / lower), rounding)});
+        } else if (within > 1.0 - upper) {
+            stair = level + (1.0 - level) *
+                                double{terrace_ease(float((within - (1.0 - upper)) / upper),
+                                                    rounding)};
+        }
+        return slopeShare * within + (1.0 - slopeShare) * stair;
+    };
+    auto meanHeight = [&](double from, double to, double level, double scarp) {
+        double weighted = 0.0, weights = 0.0;
+        for (int n = 0; n < kMeanSamples; ++n) {
+            const double within = (n + 0.5) / kMeanSamples;
+            const double r = inner + (from + within * (to - from)) * (1.0 - inner);
+            const double shaped = level < 0.0 ? within : stairAt(within, level, scarp);
+            weighted += r * wallAt(from + shaped * (to - from));
+            weights += r;
+        }
+        return weighted / weights;
+    };
+    for (size_t k = 0; k + 1 < bases.size(); ++k) {
+        const double from = bases[k], to = bases[k + 1];
+        const double stepSlope = (wallAt(to) - wallAt(from)) / ((to - from) * (1.0 - inner) * radius);
+        const double needed =
+            scarpSlope > benchSlope ? (stepSlope - benchSlope) / (scarpSlope - benchSlope) : 1.0;
+        const double scarp = std::clamp(needed, t.scarpShare, kMostScarp);
+        const double kept = 1.0 - smoothstep((needed - kSteepStep) / (1.0 - kSteepStep));
+        const double target = meanHeight(from, to, -1.0, scarp);
+        // Bisect (util/numerics.h:23) for the level whose stair keeps the mean height.
+        double low = kLevelMargin, high = 1.0 - kLevelMargin;
+        for (int i = 0; i < kLevelIterations && high - low > 0.0; ++i) {
+            const double middle = 0.5 * (low + high);
+            (!(meanHeight(from, to, middle, scarp) < target) ? high : low) = middle;
+        }
+        for (const double v : {0.5 * (low + high), scarp, kept}) {
+            data.push_back(float(v));
+        }
+    }
+}
+
+// --- central peaks (AppendKernelPeaks, crater_kernel.cpp:524-579) ----------------------------
+
+struct PeakOptions {  // CraterPeaks' defaults (apply_options.h:241-268)
+    int minMassifs = 1, maxMassifs = 4;
+    double spreadRadii = 0.8, elongation = 2.0, chainSpreadDegrees = 70.0, sharpness = 0.6;
+    double lopsidedness = 0.5, heightVariation = 0.5, roughness = 0.35;
+    double roughnessWavelength = 0.35, warp = 0.12, heightScale = 1.0, widthScale = 1.0;
+};
+
+void append_peaks(const PeakOptions& o, uint32_t seed, uint64_t id, double freshDepth,
+                  double currentDepth, CraterRecord& record, std::vector<float>& data) {
+    constexpr double kPeakRoom = 2.3, kMainRadius = 1.0, kLesserRadius = 0.6, kMaxPull = 0.45;
+    const double freshness =
+        freshDepth > 0.0 ? std::clamp(currentDepth / freshDepth, 0.0, 1.0) : 1.0;
+    Stream random(seed, kCraterPeakStream, uint32_t(id), uint32_t(id >> 32));
+    const int massifs =
+        o.minMassifs + std::min(o.maxMassifs - o.minMassifs,
+                                int((o.maxMassifs - o.minMassifs + 1) * random.next_double()));
+    record.peakCount = uint32_t(massifs);
+    record.peakOffset = uint32_t(data.size());
+    const double key = double(random.next_u32() >> 8u);
+    for (const double v : {o.roughness * freshness, o.roughnessWavelength, o.warp, key,
+                           o.heightScale, o.widthScale}) {
+        data.push_back(float(v));
+    }
+    const double chain = 2.0 * kPi * random.next_double();
+    const double room = kPeakRoom - o.warp;
+    for (int n = 0; n < massifs; ++n) {
+        // One draw per line below except where a main massif takes a constant, in this order.
+        const bool main = n == 0;
+        const double side = n % 2 == 0 ? kPi : 0.0;
+        const double bearing =
+            main ? 2.0 * kPi * random.next_double()
+                 : chain + side + o.chainSpreadDegrees * kDegree * (random.next_double() - 0.5);
+        const double reach =
+            o.spreadRadii * (main ? 0.25 * random.next_double() : 0.35 + 0.65 * random.next_double());
+        const double aspect = 1.0 + (o.elongation - 1.0) * random.next_double();
+        const double stretch = std::sqrt(aspect);
+        const double crowding = massifs == 1 ? 1.0 : std::sqrt(2.0 / massifs);
+        double radius =
+            crowding * (main ? kMainRadius : kLesserRadius * (0.5 + random.next_double()));
+        radius = std::max(0.1, std::min(radius, (room - reach) / stretch));
+        const double heading =
+            main ? 2.0 * kPi * random.next_double() : bearing + 0.5 * (random.next_double() - 0.5);
+        const double height = main ? 1.0 : 1.0 - o.heightVariation * random.next_double();
+        const double exponent = std::clamp(
+            (2.0 - 1.5 * o.sharpness) * (0.8 + 0.4 * random.next_double()), 0.4, 2.5);
+        const double pull = kMaxPull * o.lopsidedness * std::sqrt(random.next_double());
+        const double pullBearing = 2.0 * kPi * random.next_double();
+        for (const double v : {reach * std::cos(bearing), reach * std::sin(bearing), radius, stretch,
+                               std::cos(heading), std::sin(heading), height, exponent,
+                               pull * std::cos(pullBearing), pull * std::sin(pullBearing),
+                               2.0 - o.sharpness}) {
+            data.push_back(float(v));
+        }
+    }
+}
+
 }  // namespace host
 }  // namespace tgb
 
@@ -595,13 +1054,40 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         !(grid->pixel_height < 0.0)) {
         return TG_ERROR_UNSUPPORTED;
     }
+    if (shaping->profile > 3u) {
+        return TG_ERROR_ARGUMENT;
+    }
+    LayerProfile profile;
+    profile.simple = shaping->profile & 1u;
+    profile.complex = shaping->profile >= 2u;
+    if (profile.complex) {
+        // ValidateComplexCraterShape (complex.cpp:19): a positive transition diameter.
+        if (!(shaping->transition_diameter > 0.0) || !std::isfinite(shaping->transition_diameter)) {
+            return TG_ERROR_ARGUMENT;
+        }
+        profile.transition = shaping->transition_diameter;
+        set_complex_shape(profile.kernel, profile.transition);
+    }
+    TerraceOptions terraces;
+    if (shaping->terrace_onset > 0.0) {
+        // ValidateCraterTerraces (apply_options.cpp:20): full above onset, min freshness in [0, 1).
+        if (!(shaping->terrace_full > shaping->terrace_onset) ||
+            !(shaping->terrace_min_freshness >= 0.0 && shaping->terrace_min_freshness < 1.0)) {
+            return TG_ERROR_ARGUMENT;
+        }
+        terraces.onset = shaping->terrace_onset;
+        terraces.full = shaping->terrace_full;
+        terraces.minFreshness = shaping->terrace_min_freshness;
+    }
+    const PeakOptions peaks;
     const double spacing = std::max(grid->pixel_width, -grid->pixel_height);
     // The grid's bounds (its cell edges), the region CraterLayer::ApplySamples draws over.
     const Box bounds{grid->origin_x, grid->origin_y + grid->height * grid->pixel_height,
                      grid->origin_x + grid->width * grid->pixel_width, grid->origin_y};
     tg_crater_population p = *spec;
+    // DefaultCraterApply: irregular outlines, terraces and peaks; plain options: none.
     const bool irregular = shaping->irregular != 0;
-    const double reachRadii = shaping->profile == 1 ? 2.0 : 1.5;  // MPD reaches 2 R, FT 1.5 R
+    const double reachRadii = profile.reach();  // FT 1.5 R, MPD 2 R, complex 3 R
     p.margin_radii = reachRadii * max_outline_scale(irregular);
     p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
     std::vector<Crater> craters = generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent});
@@ -626,6 +1112,8 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
     const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
     const uint32_t noiseSeed = substream_seed(spec->seed, kCraterNoiseStream);
+    const uint32_t terraceSeed = substream_seed(spec->seed, kCraterTerraceStream);
+    const uint32_t peakSeed = substream_seed(spec->seed, kCraterPeakStream);
     const uint32_t textureSeed = substream_seed(spec->seed, kCraterTextureStream);
     const uint32_t textureKeySeed = substream_seed(textureSeed, kCraterTextureStream);
 
@@ -703,6 +1191,15 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         r.tableOffset = uint32_t(values.size());
         r.markCount = 0;
         r.markOffset = uint32_t(values.size());
+        if (irregular) {
+            // AppendKernelTerraces, then AppendKernelPeaks (MakeCraterKernelBatch,
+            // crater_kernel.cpp:592-593); peaks only on complex craters.
+            append_terraces(terraces, terraceSeed, profile, c.diameter, c.id, freshDepth,
+                            freshRim, erosion * freshDepth, erosion * freshRim, r, values);
+            if (profile.is_complex(c.diameter)) {
+                append_peaks(peaks, peakSeed, c.id, freshDepth, erosion * freshDepth, r, values);
+            }
+        }
         out.push_back(r);
         foot.push_back(c.x);
         foot.push_back(c.y);
@@ -717,10 +1214,13 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         // MakeCraterShapeKernel (crater_kernel.cpp:277) for a simple FT or MPD profile and the
         // default shaping options.
         CraterShapeKernel k{};
-        k.profile.simple = shaping->profile == 1 ? kProfileMartinParkesDunstan
-                                                 : kProfileFassettThomson;
         k.profile.ejectaExponent = 3.0f;
         k.profile.complexReachRadii = 3.0f;
+        if (profile.complex) {
+            set_complex_shape(k.profile, profile.transition);
+        }
+        k.profile.simple = profile.simple == 1u ? kProfileMartinParkesDunstan
+                                                : kProfileFassettThomson;
         k.profile.tableExtent = 1.5f;
         k.reachRadii = float(reachRadii);
         k.profileReachRadii = float(reachRadii);

@@ -69,14 +69,6 @@ const char* scratch_address(int device, unsigned char** out) {
     return nullptr;
 }
 
-// Turns any entry past the capacity into a status flag the host reads.
-__global__ void capacity_check_kernel(const uint32_t* counts, uint32_t nbins, uint32_t capacity,
-                                      uint32_t* status) {
-    if (threadIdx.x == 0 && blockIdx.x == 0 && counts[nbins] > capacity) {
-        status[0] |= 4u;
-    }
-}
-
 }  // namespace
 }  // namespace tgb
 
@@ -158,10 +150,22 @@ extern "C" int tg_boulders_bake_static(const void* boulders, uint32_t n, double 
         cudaGetLastError();
         return fail(TG_ERROR_CUDA, "a launch of the static bake failed");
     }
-    capacity_check_kernel<<<1, 32, 0, s>>>(bins.counts, nbins, kStaticMaxEntries, status);
+    // The binned entries the boulders need, read back before anything is written: beyond the
+    // scratch's capacity the call stops here and leaves the heights as they were.
+    uint32_t total = 0;
+    if (cudaMemcpyAsync(&total, bins.counts + nbins, sizeof(total), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(TG_ERROR_CUDA, "reading the static bake's entry count failed");
+    }
+    if (total > kStaticMaxEntries) {
+        return fail(TG_ERROR_MEMORY,
+                    "the boulders cover more bin entries than the static scratch holds (196608); "
+                    "the heights are unchanged");
+    }
     const NoData nd{nodata.mode, nodata.value};
-    if (cudaGetLastError() != cudaSuccess ||
-        launch_boulder_scatter(rec, n, bins, s) != cudaSuccess ||
+    if (launch_boulder_scatter(rec, n, bins, s) != cudaSuccess ||
         launch_boulder_bake(g, width, nd, bins, heights, status, s) != cudaSuccess) {
         cudaGetLastError();
         return fail(TG_ERROR_CUDA, "a launch of the static bake failed");
@@ -171,10 +175,6 @@ extern "C" int tg_boulders_bake_static(const void* boulders, uint32_t n, double 
         cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         return fail(TG_ERROR_CUDA, "reading the static bake's status failed");
-    }
-    if (flags & 4u) {
-        return fail(TG_ERROR_MEMORY,
-                    "the boulders cover more bin entries than the static scratch holds (196608)");
     }
     if (flags & 2u) {
         return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");

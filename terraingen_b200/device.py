@@ -148,6 +148,11 @@ class Device:
         N.check(self._lib.tg_device_name(self._handle, buf, 256))
         return buf.value.decode()
 
+    def set_wait_limit(self, polls: int) -> None:
+        """tg_set_wait_limit: polls of a staged copy before the binned crater and boulder
+        kernels give up with TG_ERROR_TIMEOUT (2^26 by default; 0 gives up at once)."""
+        N.check(self._lib.tg_set_wait_limit(self._handle, polls))
+
     def synchronize(self) -> None:
         N.check(self._lib.tg_synchronize(self._handle))
 

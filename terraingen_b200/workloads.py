@@ -5,10 +5,20 @@ tg_boulder_generate (the reference's populations, records and boulders, bit for 
 Synthetic terrain, 4097 x 4097 at 0.5 m ("terrain4097"): an 8-octave Perlin fBm source
 (wavelength 512 m, lacunarity 2, gain 0.5, amplitude 5 m, seed 7); 200,000 craters expected over
 the tile, N(>D) ~ D^-2 on [1, 500] m, uniform ages over 1 Gyr, fresh depth 0.2 D and rim 0.04 D
-worn by freshness, Fassett-Thomson profiles with the default irregular outlines; 1,000,000
-boulders expected, N(>D) ~ D^-2.5 on [0.2, 3] m, heights 0.5 D, of which those 2 samples or more
-across (D > 1 m at 0.5 m, about 1.7 %) are drawn.
+worn by freshness, with the default crater apply (irregular outlines, wall terraces, massif
+central peaks); 1,000,000 boulders expected, N(>D) ~ D^-2.5 on [0.2, 3] m, heights 0.5 D, of
+which those 2 samples or more across (D > 1 m at 0.5 m, about 1.7 %) are drawn.
+
+The configuration's "5 % with central peaks, 10 % with terraced rims for D > 200 m" is mapped
+onto the reference's own options, which key both features by diameter and freshness:
+  - central peaks: a ComplexCraterProfile over Fassett-Thomson (lunar shape) whose transition
+    diameter leaves 5 % of the D^-2 population on [1, 500] m complex (CONFIG2_TRANSITION, about
+    4.47 m); every complex crater gets a central peak (massifs, CraterPeaks' defaults);
+  - terraced rims: terraces from 200 m (onset) with the minimum freshness set so that 10 % of
+    the craters above 200 m are fresh enough to keep them (freshness is uniform on [0.2, 1]
+    under these ages and the 0.04 visibility depth, so 0.92).
 """
+
 
 from __future__ import annotations
 
@@ -90,11 +100,25 @@ def generate_craters_device(device, population: N.Population, region,
     return out
 
 
+# The configuration's peaks and terraces as reference options (module docstring).
+CONFIG2_TRANSITION = (0.05 * (1.0 - 500.0 ** -2.0) + 500.0 ** -2.0) ** -0.5
+CONFIG2_TERRACES = (200.0, 65000.0, 0.92)  # onset, full diameter, minimum freshness
+
+
+def config2_shaping() -> N.Shaping:
+    """The synthetic terrain's crater shaping: complex craters over Fassett-Thomson from
+    CONFIG2_TRANSITION, the default apply (outlines, terraces, peaks), terraces from 200 m."""
+    onset, full, freshness = CONFIG2_TERRACES
+    return N.Shaping(profile=2, irregular=1, transition_diameter=CONFIG2_TRANSITION,
+                     terrace_onset=onset, terrace_full=full, terrace_min_freshness=freshness)
+
+
 def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
-                 irregular: int = 1):
+                 irregular: int = 1, shaping: N.Shaping | None = None):
     """(kernel, records, data, footprints) a crater layer hands the kernel for `grid`."""
     lib = N.library()
-    shaping = N.Shaping(profile=profile, irregular=irregular)
+    if shaping is None:
+        shaping = N.Shaping(profile=profile, irregular=irregular)
     g = grid.native()
     nr, nd = C.c_size_t(), C.c_size_t()
     N.check(lib.tg_crater_batch(C.byref(population), C.byref(shaping), C.byref(g), None, None, 0,
@@ -151,7 +175,7 @@ def terrain4097(side: int = 4097, pixel: float = 0.5, cx: float = 0.0, cy: float
     grid = centered(side, side, pixel, cx, cy)
     crater_c = 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
     kernel, records, data, footprints = crater_batch(
-        crater_population(seed, crater_c, 1.0, 500.0), grid)
+        crater_population(seed, crater_c, 1.0, 500.0), grid, shaping=config2_shaping())
     boulder_c = 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5))
     boulders = generate_boulders(boulder_population(seed, boulder_c), grid)
     return Workload("terrain4097", grid,
@@ -164,9 +188,11 @@ def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
     full_area = (4097 * pixel) ** 2
     crater_c = 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
     boulder_c = 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5))
+    onset, full, freshness = CONFIG2_TERRACES
     craters = dict(seed=seed, sfdCoefficient=crater_c, sfdExponent=2.0, minDiameter=1.0,
-                   maxDiameter=500.0, lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04, profile=0,
-                   applyPreset=0)
+                   maxDiameter=500.0, lifetimeGyr=1.0, depthRatio=0.2, rimRatio=0.04, profile=2,
+                   transitionDiameter=CONFIG2_TRANSITION, applyPreset=0, terraceOnset=onset,
+                   terraceFull=full, terraceMinFreshness=freshness)
     boulders = dict(boulderSeed=seed, boulderCoefficient=boulder_c, boulderExponent=2.5,
                     boulderMin=0.2, boulderMax=3.0, heightRatio=0.5)
     grid = centered(side, side, pixel)

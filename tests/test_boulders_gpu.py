@@ -59,3 +59,25 @@ def test_boulders_point_dome_and_edges(device):
     assert not far.any()
     with pytest.raises(TgError):
         device.boulders_bake(np.array([[0.0, 0.0, -1.0, 1.0, 1.0]]), grid, far, width=1.0)
+
+
+def test_staged_copy_timeout_is_reported_and_recovers(device, fx):
+    # A wait limit of 0 polls makes every bin's first staged-copy wait give up at once (no fault:
+    # the copies still land, and each CTA waits, bounded, for its copies in flight before it
+    # leaves). The call reports TG_ERROR_TIMEOUT and the device keeps working: with the default
+    # limit restored the same bake gives the reference's heights.
+    from terraingen_b200 import TgError
+
+    grid = grid_of(fx["dense_grid"])
+    boulders = np.ascontiguousarray(fx["dense_boulders"])
+    heights = fx["dense_base"].copy()
+    device.set_wait_limit(0)
+    try:
+        with pytest.raises(TgError) as error:
+            device.boulders_bake(boulders, grid, heights, width=grid.pixel)
+        assert error.value.status == 5  # TG_ERROR_TIMEOUT
+    finally:
+        device.set_wait_limit(1 << 26)
+    heights = fx["dense_base"].copy()
+    device.boulders_bake(boulders, grid, heights, width=grid.pixel)
+    assert np.abs(heights.astype(np.float64) - fx["dense_expected"]).max() <= 1e-3

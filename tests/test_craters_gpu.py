@@ -170,3 +170,27 @@ def test_binned_odd_data_offsets_and_alignment(device, crater_fixture):
     with pytest.raises(TgError):
         device.craters_apply(kernel, raw[8:8 + records.nbytes], torch.from_numpy(data).cuda(), grid,
                              h)
+
+
+@pytest.mark.parametrize("name", ["config1", "complex"])
+def test_staged_copy_timeout_is_reported_and_recovers(device, crater_fixture, name):
+    # A wait limit of 0 polls makes the binned kernel (lean and general variants) give up on its
+    # first staged copy at once, without a fault: TG_ERROR_TIMEOUT, then the same call with the
+    # default limit gives the reference's heights.
+    from terraingen_b200 import TgError
+
+    fx = crater_fixture
+    kernel, records, data = inputs(fx, name)
+    grid = grid_of(fx[f"{name}_grid"])
+    heights = np.zeros((grid.height, grid.width), np.float32)
+    device.set_wait_limit(0)
+    try:
+        with pytest.raises(TgError) as error:
+            device.craters_apply(kernel, records, data, grid, heights)
+        assert error.value.status == 5  # TG_ERROR_TIMEOUT
+    finally:
+        device.set_wait_limit(1 << 26)
+    heights = np.zeros((grid.height, grid.width), np.float32)
+    device.craters_apply(kernel, records, data, grid, heights)
+    err = np.abs(heights.astype(np.float64) - fx[f"{name}_expected"])
+    assert err.max() <= TOLERANCE_M

@@ -42,9 +42,9 @@ def generate(pop: N.Population, region) -> dict:
     return out
 
 
-def batch(pop: N.Population, profile: int, irregular: int, grid):
+def batch(pop: N.Population, profile: int, irregular: int, grid, **shaping):
     lib = N.library()
-    shp = N.Shaping(profile=profile, irregular=irregular)
+    shp = N.Shaping(profile=profile, irregular=irregular, **shaping)
     g = grid.native()
     nr, nd = C.c_size_t(), C.c_size_t()
     N.check(lib.tg_crater_batch(C.byref(pop), C.byref(shp), C.byref(g), None, None, 0, None, 0,
@@ -85,6 +85,61 @@ def test_batch_matches_captured_mpd(crater_fixture):
     assert k.tobytes() == crater_fixture["mpd_kernel"].tobytes()
     assert rec.tobytes() == crater_fixture["mpd_records"].tobytes()
     assert data.tobytes() == crater_fixture["mpd_data"].tobytes()
+
+
+def test_batch_matches_captured_complex(crater_fixture):
+    # Complex craters over Fassett-Thomson (lowered transition) with the default apply: massif
+    # peaks on every complex crater and wall terraces from 80 m, records and data bit-exact with
+    # what the reference hands its GPU backend (AppendKernelTerraces, AppendKernelPeaks). The
+    # scene's rim smoothing is a kernel option only; every other kernel field matches.
+    grid = centered(192, 192, 2.0)
+    fields = dict(seed=9, sfdCoefficient=0.6, minDiameter=8.0, maxDiameter=300.0)
+    k, rec, data, _ = batch(population(fields), 2, 1, grid, transition_diameter=60.0,
+                            terrace_onset=80.0, terrace_full=200.0, terrace_min_freshness=0.3)
+    want = crater_fixture["complex_records"].view(CRATER_RECORD)
+    assert np.any(rec["peakCount"] > 0) and np.any(rec["terraceCount"] > 0)
+    assert rec.tobytes() == want.tobytes()
+    assert data.tobytes() == crater_fixture["complex_data"].tobytes()
+    wk = crater_fixture["complex_kernel"].view(CRATER_SHAPE_KERNEL).reshape(())
+    for name in CRATER_SHAPE_KERNEL.names:
+        if name != "rimSigma":
+            assert np.asarray(k[name]).tobytes() == np.asarray(wk[name]).tobytes(), name
+
+
+def test_batch_rejects_bad_shaping():
+    lib = N.library()
+    pop = population(dict(seed=1, sfdCoefficient=0.1, minDiameter=2.0, maxDiameter=20.0))
+    g = centered(32, 32, 1.0).native()
+    nr, nd = C.c_size_t(), C.c_size_t()
+    for shaping in (N.Shaping(profile=4), N.Shaping(profile=2, transition_diameter=0.0),
+                    N.Shaping(profile=0, irregular=1, terrace_onset=100.0, terrace_full=50.0),
+                    N.Shaping(profile=0, irregular=1, terrace_onset=100.0, terrace_full=200.0,
+                              terrace_min_freshness=1.0)):
+        assert lib.tg_crater_batch(C.byref(pop), C.byref(shaping), C.byref(g), None, None, 0,
+                                   None, 0, None, C.byref(nr), C.byref(nd)) == 1
+
+
+@pytest.mark.skipif(not H.available("libtgref_capture.so"), reason="reference build not present")
+@pytest.mark.parametrize("cx,cy", [(300.0, -450.0), (-700.0, 820.0)])
+def test_config2_window_matches_reference_live(cx, cy):
+    # A window of the synthetic 4097^2 terrain's crater layer with its peaks and terraces mapped
+    # onto the reference's options (terraingen_b200.workloads): the kernel, records and data the
+    # reference's CraterLayer hands its GPU backend, captured live, against tg_crater_batch.
+    from terraingen_b200 import workloads as W
+
+    grid = centered(257, 257, 0.5, cx, cy)
+    _, _, craters, _ = W.terrain4097_reference_scene(257)
+    cap = H.capture()
+    H.evaluate(cap, H.make_scene(grid, craters=craters), 1, 1)
+    call = [c for c in H.captured(cap) if c["kind"] == 2][-1]
+    area = (4097 * 0.5) ** 2
+    coefficient = 200000.0 / (area * (1.0 ** -2.0 - 500.0 ** -2.0))
+    k, rec, data, _ = W.crater_batch(W.crater_population(7, coefficient, 1.0, 500.0), grid,
+                                     shaping=W.config2_shaping())
+    assert np.any(rec["peakCount"] > 0)
+    assert k.tobytes() == call["kernel"].tobytes()
+    assert rec.tobytes() == call["records"].tobytes()
+    assert data.tobytes() == call["data"].tobytes()
 
 
 def test_population_deterministic_and_tiled():
