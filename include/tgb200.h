@@ -424,6 +424,12 @@ typedef struct tg_crater_shaping {
     double terrace_min_freshness;
 } tg_crater_shaping;
 
+/* Host threads tg_crater_batch and tg_boulder_generate use (0, the default, for every core), as
+ * EvaluationOptions::threads sets the reference's (include/terraingen/pipeline/terrain.h). The
+ * results do not depend on it: work is split by generation rows and crater blocks and joined in
+ * order. */
+void tg_set_host_threads(unsigned threads);
+
 /* The craters the layer draws over `region` (x0, y0, x1, y1 in meters), in the reference's order
  * (GenerateCraters, src/layers/craters/generation/population.cpp:414): centers, diameters, ages
  * and 64-bit ids, bit-exact. `count` receives the number; arrays (any may be null) hold at most

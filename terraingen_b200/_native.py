@@ -52,6 +52,7 @@ SIGNATURES = {
     "tg_device_name": [_P, C.c_char_p, _SZ],
     "tg_synchronize": [_P],
     "tg_set_wait_limit": [_P, _U32],
+    "tg_set_host_threads": [C.c_uint],
     "tg_noise_layer": [_P, _P, _SZ, C.POINTER(Grid), _D, _D, _P, NoData, _I, _P],
     "tg_noise_layer_rows": [_P, _P, _SZ, _P, _P, _U32, _U32, _P, NoData, _I, _P],
     "tg_noise_source": [_P, _P, _U32, _F, C.POINTER(Grid), _P, _I, _P],
@@ -235,6 +236,7 @@ SIGNATURES.update({
 })
 
 RESTYPES = {"tg_close": None, "tg_last_error": C.c_char_p, "tg_batch_destroy": None,
+            "tg_set_host_threads": None,
             "tg_server_destroy": None}
 
 _lib = None

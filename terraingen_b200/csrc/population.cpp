@@ -14,10 +14,12 @@
 //   BaseRecord / AppendKernelOutline      (shaping/crater_kernel.cpp:187, irregularity.cpp:295)
 // This file is compiled with -ffp-contract=off and uses the host libm, as the reference does.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/tgb200.h"
@@ -282,13 +284,57 @@ std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const P
     return out;
 }
 
+// Host threads the batch builders use (tg_set_host_threads); 0 for every core.
+std::atomic<unsigned> g_host_threads{0};
+
+unsigned host_threads() {
+    const unsigned asked = g_host_threads.load();
+    const unsigned cores = std::max(1u, std::thread::hardware_concurrency());
+    return std::min(asked == 0 ? cores : asked, 256u);
+}
+
+// Runs body(i) for every i in [0, n) on up to `threads` host threads, the caller's included;
+// items are taken in order from a shared counter, so each runs exactly once.
+template <typename Body>
+void parallel_for(size_t n, unsigned threads, const Body& body) {
+    const size_t workers = std::min<size_t>(threads, n);
+    if (workers <= 1) {
+        for (size_t i = 0; i < n; ++i) {
+            body(i);
+        }
+        return;
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
+            body(i);
+        }
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(workers - 1);
+    for (size_t t = 1; t < workers; ++t) {
+        pool.emplace_back(work);
+    }
+    work();
+    for (std::thread& t : pool) {
+        t.join();
+    }
+}
+
 // Craters over `region` with their candidate margin (GenerateCraters, planar, no spacing,
-// density map or manual craters).
+// density map or manual craters). Each band's row of generation cells is drawn on its own (by
+// `threads` host threads when asked), and the rows are joined in the reference's order: bands
+// ascending, rows j, cells i, craters in draw order.
 std::vector<Crater> generate(const tg_crater_population& spec, const Box& region,
-                             const PowerLaw& law) {
+                             const PowerLaw& law, unsigned threads = 1) {
     const double marginRadii = spec.margin_radii;
     auto margin = [&](double d) { return 0.5 * marginRadii * d; };
-    std::vector<Crater> out;
+    struct Row {
+        Band band;
+        int32_t j, iMin, iMax;
+        Box inner, outer;
+    };
+    std::vector<Row> rows;
     for (const Band& band : crater_bands(spec.min_diameter, spec.max_diameter,
                                          spec.cell_size_factor)) {
         if (band.high <= spec.min_resolved_diameter) {
@@ -299,10 +345,21 @@ std::vector<Crater> generate(const tg_crater_population& spec, const Box& region
         const int32_t jMin = cell_coordinate(std::floor(cover.minY / band.cellSize));
         const int32_t iMax = cell_coordinate(std::ceil(cover.maxX / band.cellSize) - 1.0);
         const int32_t jMax = cell_coordinate(std::ceil(cover.maxY / band.cellSize) - 1.0);
-        const Box inner = region.expanded(margin(band.low));
-        const Box outer = region.expanded(margin(band.high));
         for (int32_t j = jMin; j <= jMax; ++j) {
-            for (int32_t i = iMin; i <= iMax; ++i) {
+            rows.push_back(Row{band, j, iMin, iMax, region.expanded(margin(band.low)),
+                               region.expanded(margin(band.high))});
+        }
+    }
+    std::vector<std::vector<Crater>> drawn(rows.size());
+    parallel_for(rows.size(), threads, [&](size_t q) {
+        const Row& row = rows[q];
+        const Band& band = row.band;
+        const int32_t j = row.j;
+        const Box& inner = row.inner;
+        const Box& outer = row.outer;
+        std::vector<Crater>& out = drawn[q];
+        {
+            for (int32_t i = row.iMin; i <= row.iMax; ++i) {
                 std::vector<Crater> list = cell_craters(band, i, j, law, spec.lifetime_gyr,
                                                         spec.seed);
                 // CellCraters::Rows(outer y range): the draw order, filtered by y.
@@ -327,6 +384,15 @@ std::vector<Crater> generate(const tg_crater_population& spec, const Box& region
                 }
             }
         }
+    });
+    size_t total = 0;
+    for (const std::vector<Crater>& d : drawn) {
+        total += d.size();
+    }
+    std::vector<Crater> out;
+    out.reserve(total);
+    for (const std::vector<Crater>& d : drawn) {
+        out.insert(out.end(), d.begin(), d.end());
     }
     return out;
 }
@@ -437,7 +503,26 @@ struct Outline {
 
 // IrregularOutline with the default irregularity (power-law harmonics 2-12, roughness uniform
 // in [0.01, 0.03], slope 1.5, 5.4% elliptical with ellipticity uniform in [1.1, 1.5]).
+// The default outline's per-harmonic power law, k^-slope for k = 2..12, and sqrt(2 / sum of
+// k^-2 slope): the same host pow calls for every crater, made once.
+struct OutlineLaw {
+    double power[11];
+    double scale;
+    OutlineLaw() {
+        const double slope = 1.5;
+        double sum = 0.0;
+        for (int k = 2; k <= 12; ++k) {
+            sum += std::pow(double(k), -2.0 * slope);
+        }
+        scale = std::sqrt(2.0 / sum);
+        for (int k = 2; k <= 12; ++k) {
+            power[k - 2] = std::pow(double(k), -slope);
+        }
+    }
+};
+
 Outline irregular_outline(const Crater& c, uint32_t seed) {
+    static const OutlineLaw law;
     Outline o;
     Stream random(seed, kCraterIrregularityStream, uint32_t(c.id), uint32_t(c.id >> 32));
     double d[9];
@@ -452,16 +537,13 @@ Outline irregular_outline(const Crater& c, uint32_t seed) {
     }
     if (rough < 1.0) {
         const double roughness = 0.01 + (0.03 - 0.01) * r1;  // clamped to (-inf, inf)
-        const double slope = 1.5;
-        double sum = 0.0;
-        for (int k = 2; k <= 12; ++k) {
-            sum += std::pow(double(k), -2.0 * slope);
-        }
-        const double norm = roughness * std::sqrt(2.0 / sum);
+        const double norm = roughness * law.scale;
         o.firstHarmonic = 2;
         if (roughness > 0.0) {
+            o.amplitudes.reserve(11);
+            o.phases.reserve(11);
             for (int k = 2; k <= 12; ++k) {
-                o.amplitudes.push_back(norm * std::pow(double(k), -slope));
+                o.amplitudes.push_back(norm * law.power[k - 2]);
                 o.phases.push_back(2.0 * 3.14159265358979323846 * random.next_double());
             }
         }
@@ -936,6 +1018,14 @@ void append_peaks(const PeakOptions& o, uint32_t seed, uint64_t id, double fresh
     }
 }
 
+// The records of a block of consecutive craters in apply order, with data offsets relative to
+// the block's own data until the blocks are placed in the outputs.
+struct RecordBlock {
+    std::vector<CraterRecord> records;
+    std::vector<float> values;
+    std::vector<double> foot;
+};
+
 }  // namespace host
 }  // namespace tgb
 
@@ -944,9 +1034,66 @@ using namespace tgb::host;
 
 namespace {
 thread_local std::string g_population_error;
+
+bool same_population(const tg_crater_population& a, const tg_crater_population& b) {
+    return a.seed == b.seed && a.sfd_coefficient == b.sfd_coefficient &&
+           a.sfd_exponent == b.sfd_exponent && a.min_diameter == b.min_diameter &&
+           a.max_diameter == b.max_diameter && a.lifetime_gyr == b.lifetime_gyr &&
+           a.depth_ratio == b.depth_ratio && a.rim_ratio == b.rim_ratio &&
+           a.cutoff_depth_ratio == b.cutoff_depth_ratio &&
+           a.cell_size_factor == b.cell_size_factor && a.margin_radii == b.margin_radii &&
+           a.min_resolved_diameter == b.min_resolved_diameter;
+}
+
+bool same_shaping(const tg_crater_shaping& a, const tg_crater_shaping& b) {
+    return a.profile == b.profile && a.irregular == b.irregular &&
+           a.transition_diameter == b.transition_diameter && a.terrace_onset == b.terrace_onset &&
+           a.terrace_full == b.terrace_full && a.terrace_min_freshness == b.terrace_min_freshness;
+}
+
+bool same_grid(const tg_grid& a, const tg_grid& b) {
+    return a.width == b.width && a.height == b.height && a.origin_x == b.origin_x &&
+           a.pixel_width == b.pixel_width && a.row_rotation == b.row_rotation &&
+           a.origin_y == b.origin_y && a.col_rotation == b.col_rotation &&
+           a.pixel_height == b.pixel_height;
+}
+
+// The batch a size query built, for the fill call that follows it.
+struct BatchCache {
+    bool valid = false;
+    tg_crater_population spec{};
+    tg_crater_shaping shaping{};
+    tg_grid grid{};
+    std::vector<RecordBlock> blocks;
+
+    bool take(const tg_crater_population& p, const tg_crater_shaping& s, const tg_grid& g,
+              std::vector<RecordBlock>& out) {
+        const bool hit =
+            valid && same_population(spec, p) && same_shaping(shaping, s) && same_grid(grid, g);
+        if (hit) {
+            out.swap(blocks);
+        }
+        valid = false;
+        blocks = {};
+        return hit;
+    }
+
+    void keep(const tg_crater_population& p, const tg_crater_shaping& s, const tg_grid& g,
+              std::vector<RecordBlock>& in) {
+        valid = true;
+        spec = p;
+        shaping = s;
+        grid = g;
+        blocks.swap(in);
+    }
+};
 }
 
 extern "C" {
+
+void tg_set_host_threads(unsigned threads) {
+    g_host_threads.store(threads);
+}
 
 int tg_crater_generate(const tg_crater_population* spec, const double* region, double* x,
                          double* y, double* diameter, double* age, uint64_t* id, size_t capacity,
@@ -1004,7 +1151,7 @@ int tg_boulder_generate(const tg_boulder_population* spec, const double* region,
     const PowerLaw sizes{b.sfd_coefficient, b.sfd_exponent};
     const PowerLaw candidates{b.sfd_coefficient, b.sfd_exponent, 1.0};
     const std::vector<Crater> drawn =
-        generate(p, Box{region[0], region[1], region[2], region[3]}, candidates);
+        generate(p, Box{region[0], region[1], region[2], region[3]}, candidates, host_threads());
     size_t n = 0;
     for (const Crater& c : drawn) {
         const uint32_t low = uint32_t(c.id), high = uint32_t(c.id >> 32);
@@ -1090,126 +1237,179 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     const double reachRadii = profile.reach();  // FT 1.5 R, MPD 2 R, complex 3 R
     p.margin_radii = reachRadii * max_outline_scale(irregular);
     p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
-    std::vector<Crater> craters = generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent});
+    // A call that asks only for the sizes keeps what it built, and the next call from the same
+    // thread with the same inputs copies that out instead of building it again.
+    std::vector<RecordBlock> blocks;
+    const unsigned threads = host_threads();
+    static thread_local BatchCache cache;
+    if (!cache.take(*spec, *shaping, *grid, blocks)) {
+        std::vector<Crater> craters =
+            generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads);
 
-    // CraterApplyOrder, oldest first (apply_options.cpp:96).
-    std::vector<size_t> order(craters.size());
-    for (size_t n = 0; n < order.size(); ++n) {
-        order[n] = n;
-    }
-    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-        const Crater& ca = craters[a];
-        const Crater& cb = craters[b];
-        if (ca.age != cb.age) {
-            return ca.age > cb.age;
+        // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
+        // descending, id, draw index. The keys are sorted by value in chunks on the host threads,
+        // then merged; the order is total, so the result is the one order whatever the split.
+        struct OrderKey {
+            double age, diameter;
+            uint64_t id;
+            size_t index;
+            bool operator<(const OrderKey& o) const {
+                if (age != o.age) {
+                    return age > o.age;
+                }
+                if (diameter != o.diameter) {
+                    return diameter > o.diameter;
+                }
+                return id != o.id ? id < o.id : index < o.index;
+            }
+        };
+        std::vector<OrderKey> keys(craters.size());
+        for (size_t n = 0; n < keys.size(); ++n) {
+            keys[n] = OrderKey{craters[n].age, craters[n].diameter, craters[n].id, n};
         }
-        if (ca.diameter != cb.diameter) {
-            return ca.diameter > cb.diameter;
-        }
-        return ca.id != cb.id ? ca.id < cb.id : a < b;
-    });
-
-    // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
-    const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
-    const uint32_t noiseSeed = substream_seed(spec->seed, kCraterNoiseStream);
-    const uint32_t terraceSeed = substream_seed(spec->seed, kCraterTerraceStream);
-    const uint32_t peakSeed = substream_seed(spec->seed, kCraterPeakStream);
-    const uint32_t textureSeed = substream_seed(spec->seed, kCraterTextureStream);
-    const uint32_t textureKeySeed = substream_seed(textureSeed, kCraterTextureStream);
-
-    std::vector<CraterRecord> out;
-    std::vector<float> values;
-    std::vector<double> foot;
-    for (const size_t n : order) {
-        const Crater& c = craters[n];
-        const double resolution = resolution_weight(c.diameter, spacing);
-        if (resolution == 0.0) {
-            continue;
-        }
-        const Outline outline = irregular ? irregular_outline(c, irregularitySeed) : Outline{};
-        // CratersOnRaster: the footprint window must hold a cell of the grid.
-        double scale = 1.0;
-        for (const double a : outline.amplitudes) {
-            scale += std::fabs(a);
-        }
-        scale *= std::sqrt(outline.ellipticity);
-        const double reach = scale * reachRadii * (0.5 * c.diameter);
-        // Surface::Expand, then MappedBounds of GeoTransform::WorldToPixel over the box's corners
-        // (src/raster/cell_loops.cpp:21-28, geo_transform.h:70), then ClampIndex.
-        const double det =
-            grid->pixel_width * grid->pixel_height - grid->row_rotation * grid->col_rotation;
-        double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
-        for (const double wx : {c.x - reach, c.x + reach}) {
-            for (const double wy : {c.y - reach, c.y + reach}) {
-                const double dx = wx - grid->origin_x;
-                const double dy = wy - grid->origin_y;
-                const double px = (dx * grid->pixel_height - dy * grid->row_rotation) / det;
-                const double py = (dy * grid->pixel_width - dx * grid->col_rotation) / det;
-                minX = std::fmin(minX, px);
-                minY = std::fmin(minY, py);
-                maxX = std::fmax(maxX, px);
-                maxY = std::fmax(maxY, py);
+        {
+            const size_t parts = std::max<size_t>(1, std::min<size_t>(threads, keys.size() / 4096));
+            std::vector<size_t> bounds(parts + 1);
+            for (size_t q = 0; q <= parts; ++q) {
+                bounds[q] = keys.size() * q / parts;
+            }
+            parallel_for(parts, threads, [&](size_t q) {
+                std::sort(keys.begin() + bounds[q], keys.begin() + bounds[q + 1]);
+            });
+            for (size_t width = 1; width < parts; width *= 2) {
+                std::vector<size_t> merges;
+                for (size_t q = 0; q + width < parts; q += 2 * width) {
+                    merges.push_back(q);
+                }
+                parallel_for(merges.size(), threads, [&](size_t m) {
+                    const size_t q = merges[m];
+                    std::inplace_merge(keys.begin() + bounds[q], keys.begin() + bounds[q + width],
+                                       keys.begin() + bounds[std::min(parts, q + 2 * width)]);
+                });
             }
         }
-        const double w = grid->width, h = grid->height;
-        const double c0 = std::clamp(std::floor(minX), 0.0, w);
-        const double c1 = std::clamp(std::ceil(maxX), 0.0, w);
-        const double r0 = std::clamp(std::floor(minY), 0.0, h);
-        const double r1 = std::clamp(std::ceil(maxY), 0.0, h);
-        if (!(size_t(c0) < size_t(c1) && size_t(r0) < size_t(r1))) {
-            continue;
+        std::vector<size_t> order(keys.size());
+        for (size_t n = 0; n < order.size(); ++n) {
+            order[n] = keys[n].index;
         }
-        // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
-        const double freshDepth = spec->depth_ratio, freshRim = spec->rim_ratio;
-        const double floorShare = std::fmin(spec->cutoff_depth_ratio / freshDepth, 1.0);
-        const double remaining = std::clamp(1.0 - c.age / spec->lifetime_gyr, 0.0, 1.0);
-        const double erosion = floorShare + (1.0 - floorShare) * remaining;
-        CraterRecord r{};
-        r.diameter = float(c.diameter);
-        r.freshDepth = float(freshDepth);
-        r.freshRim = float(freshRim);
-        r.currentDepth = float(erosion * freshDepth);
-        r.currentRim = float(erosion * freshRim);
-        r.diffusion = 0.0f;
-        r.resolution = float(resolution);
-        r.noiseKey = crater_key(c.id, noiseSeed);
-        r.textureKey = crater_key(c.id, textureKeySeed);
-        r.x = float(c.x);
-        r.xLow = float(c.x - double(r.x));
-        r.y = float(c.y);
-        r.yLow = float(c.y - double(r.y));
-        r.ellipticity = float(outline.ellipticity);
-        r.heading = float(outline.heading);
-        r.harmonicOffset = uint32_t(values.size());
-        r.firstHarmonic = uint32_t(outline.firstHarmonic);
-        r.harmonicCount = uint32_t(outline.amplitudes.size());
-        for (size_t k = 0; k < outline.amplitudes.size(); ++k) {
-            values.push_back(float(outline.amplitudes[k]));
-            values.push_back(float(outline.phases[k]));
-        }
-        r.tableCount = 0;
-        r.tableOffset = uint32_t(values.size());
-        r.markCount = 0;
-        r.markOffset = uint32_t(values.size());
-        if (irregular) {
-            // AppendKernelTerraces, then AppendKernelPeaks (MakeCraterKernelBatch,
-            // crater_kernel.cpp:592-593); peaks only on complex craters.
-            append_terraces(terraces, terraceSeed, profile, c.diameter, c.id, freshDepth,
-                            freshRim, erosion * freshDepth, erosion * freshRim, r, values);
-            if (profile.is_complex(c.diameter)) {
-                append_peaks(peaks, peakSeed, c.id, freshDepth, erosion * freshDepth, r, values);
+
+        // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
+        const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
+        const uint32_t noiseSeed = substream_seed(spec->seed, kCraterNoiseStream);
+        const uint32_t terraceSeed = substream_seed(spec->seed, kCraterTerraceStream);
+        const uint32_t peakSeed = substream_seed(spec->seed, kCraterPeakStream);
+        const uint32_t textureSeed = substream_seed(spec->seed, kCraterTextureStream);
+        const uint32_t textureKeySeed = substream_seed(textureSeed, kCraterTextureStream);
+
+        auto build = [&](const Crater& c, RecordBlock& block) {
+            std::vector<CraterRecord>& out = block.records;
+            std::vector<float>& values = block.values;
+            std::vector<double>& foot = block.foot;
+            const double resolution = resolution_weight(c.diameter, spacing);
+            if (resolution == 0.0) {
+                return;
             }
-        }
-        out.push_back(r);
-        foot.push_back(c.x);
-        foot.push_back(c.y);
-        foot.push_back(reach);
+            const Outline outline = irregular ? irregular_outline(c, irregularitySeed) : Outline{};
+            // CratersOnRaster: the footprint window must hold a cell of the grid.
+            double scale = 1.0;
+            for (const double a : outline.amplitudes) {
+                scale += std::fabs(a);
+            }
+            scale *= std::sqrt(outline.ellipticity);
+            const double reach = scale * reachRadii * (0.5 * c.diameter);
+            // Surface::Expand, then MappedBounds of GeoTransform::WorldToPixel over the box's corners
+            // (src/raster/cell_loops.cpp:21-28, geo_transform.h:70), then ClampIndex.
+            const double det =
+                grid->pixel_width * grid->pixel_height - grid->row_rotation * grid->col_rotation;
+            double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
+            for (const double wx : {c.x - reach, c.x + reach}) {
+                for (const double wy : {c.y - reach, c.y + reach}) {
+                    const double dx = wx - grid->origin_x;
+                    const double dy = wy - grid->origin_y;
+                    const double px = (dx * grid->pixel_height - dy * grid->row_rotation) / det;
+                    const double py = (dy * grid->pixel_width - dx * grid->col_rotation) / det;
+                    minX = std::fmin(minX, px);
+                    minY = std::fmin(minY, py);
+                    maxX = std::fmax(maxX, px);
+                    maxY = std::fmax(maxY, py);
+                }
+            }
+            const double w = grid->width, h = grid->height;
+            const double c0 = std::clamp(std::floor(minX), 0.0, w);
+            const double c1 = std::clamp(std::ceil(maxX), 0.0, w);
+            const double r0 = std::clamp(std::floor(minY), 0.0, h);
+            const double r1 = std::clamp(std::ceil(maxY), 0.0, h);
+            if (!(size_t(c0) < size_t(c1) && size_t(r0) < size_t(r1))) {
+                return;
+            }
+            // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
+            const double freshDepth = spec->depth_ratio, freshRim = spec->rim_ratio;
+            const double floorShare = std::fmin(spec->cutoff_depth_ratio / freshDepth, 1.0);
+            const double remaining = std::clamp(1.0 - c.age / spec->lifetime_gyr, 0.0, 1.0);
+            const double erosion = floorShare + (1.0 - floorShare) * remaining;
+            CraterRecord r{};
+            r.diameter = float(c.diameter);
+            r.freshDepth = float(freshDepth);
+            r.freshRim = float(freshRim);
+            r.currentDepth = float(erosion * freshDepth);
+            r.currentRim = float(erosion * freshRim);
+            r.diffusion = 0.0f;
+            r.resolution = float(resolution);
+            r.noiseKey = crater_key(c.id, noiseSeed);
+            r.textureKey = crater_key(c.id, textureKeySeed);
+            r.x = float(c.x);
+            r.xLow = float(c.x - double(r.x));
+            r.y = float(c.y);
+            r.yLow = float(c.y - double(r.y));
+            r.ellipticity = float(outline.ellipticity);
+            r.heading = float(outline.heading);
+            r.harmonicOffset = uint32_t(values.size());
+            r.firstHarmonic = uint32_t(outline.firstHarmonic);
+            r.harmonicCount = uint32_t(outline.amplitudes.size());
+            for (size_t k = 0; k < outline.amplitudes.size(); ++k) {
+                values.push_back(float(outline.amplitudes[k]));
+                values.push_back(float(outline.phases[k]));
+            }
+            r.tableCount = 0;
+            r.tableOffset = uint32_t(values.size());
+            r.markCount = 0;
+            r.markOffset = uint32_t(values.size());
+            if (irregular) {
+                // AppendKernelTerraces, then AppendKernelPeaks (MakeCraterKernelBatch,
+                // crater_kernel.cpp:592-593); peaks only on complex craters.
+                append_terraces(terraces, terraceSeed, profile, c.diameter, c.id, freshDepth,
+                                freshRim, erosion * freshDepth, erosion * freshRim, r, values);
+                if (profile.is_complex(c.diameter)) {
+                    append_peaks(peaks, peakSeed, c.id, freshDepth, erosion * freshDepth, r, values);
+                }
+            }
+            out.push_back(r);
+            foot.push_back(c.x);
+            foot.push_back(c.y);
+            foot.push_back(reach);
+        };
+        constexpr size_t kBlock = 512;
+        const size_t nblocks = (order.size() + kBlock - 1) / kBlock;
+        blocks.resize(nblocks);
+        parallel_for(nblocks, threads, [&](size_t b) {
+            const size_t end = std::min(order.size(), (b + 1) * kBlock);
+            for (size_t q = b * kBlock; q < end; ++q) {
+                build(craters[order[q]], blocks[b]);
+            }
+        });
     }
-    if (values.empty()) {
-        values.push_back(0.0f);
+    // Where each block lands in the outputs: records and footprints in order, data offsets moved
+    // by the data before (an empty batch still hands the kernel one data float, 0).
+    std::vector<size_t> recordBase(blocks.size() + 1, 0), dataBase(blocks.size() + 1, 0);
+    for (size_t b = 0; b < blocks.size(); ++b) {
+        recordBase[b + 1] = recordBase[b] + blocks[b].records.size();
+        dataBase[b + 1] = dataBase[b] + blocks[b].values.size();
     }
-    *n_records = out.size();
-    *n_data = values.size();
+    const size_t nRecords = recordBase.back();
+    const size_t nValues = std::max<size_t>(dataBase.back(), 1);
+    const bool query = records == nullptr && data == nullptr && footprints == nullptr;
+    *n_records = nRecords;
+    *n_data = nValues;
     if (kernel != nullptr) {
         // MakeCraterShapeKernel (crater_kernel.cpp:277) for a simple FT or MPD profile and the
         // default shaping options.
@@ -1245,20 +1445,48 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         k.minFreshness = 0.5f;
         std::memcpy(kernel, &k, sizeof(k));
     }
-    if (records != nullptr) {
-        if (record_capacity < out.size()) {
-            return TG_ERROR_ARGUMENT;
-        }
-        std::memcpy(records, out.data(), out.size() * sizeof(CraterRecord));
+    if (records != nullptr && record_capacity < nRecords) {
+        return TG_ERROR_ARGUMENT;
     }
-    if (data != nullptr) {
-        if (data_capacity < values.size()) {
-            return TG_ERROR_ARGUMENT;
-        }
-        std::memcpy(data, values.data(), values.size() * sizeof(float));
+    if (data != nullptr && data_capacity < nValues) {
+        return TG_ERROR_ARGUMENT;
     }
-    if (footprints != nullptr && record_capacity >= out.size()) {
-        std::memcpy(footprints, foot.data(), foot.size() * sizeof(double));
+    const bool withFoot = footprints != nullptr && record_capacity >= nRecords;
+    if (!query) {
+        // Each block's records, data and footprints copied to their place on the host threads.
+        parallel_for(blocks.size(), threads, [&](size_t b) {
+            const RecordBlock& block = blocks[b];
+            const uint32_t base = uint32_t(dataBase[b]);
+            if (records != nullptr) {
+                CraterRecord* dst = static_cast<CraterRecord*>(records) + recordBase[b];
+                for (size_t i = 0; i < block.records.size(); ++i) {
+                    CraterRecord r = block.records[i];
+                    r.harmonicOffset += base;
+                    r.tableOffset += base;
+                    r.markOffset += base;
+                    if (r.terraceCount > 0u) {
+                        r.terraceOffset += base;
+                    }
+                    if (r.peakCount > 0u) {
+                        r.peakOffset += base;
+                    }
+                    dst[i] = r;
+                }
+            }
+            if (data != nullptr && !block.values.empty()) {
+                std::memcpy(data + base, block.values.data(), block.values.size() * sizeof(float));
+            }
+            if (withFoot && !block.foot.empty()) {
+                std::memcpy(footprints + 3 * recordBase[b], block.foot.data(),
+                            block.foot.size() * sizeof(double));
+            }
+        });
+        if (data != nullptr && dataBase.back() == 0) {
+            data[0] = 0.0f;
+        }
+    }
+    if (query) {
+        cache.keep(*spec, *shaping, *grid, blocks);
     }
     return TG_OK;
 }

@@ -124,9 +124,9 @@ def crater_batch(population: N.Population, grid: GridSpec, profile: int = 0,
     N.check(lib.tg_crater_batch(C.byref(population), C.byref(shaping), C.byref(g), None, None, 0,
                                 None, 0, None, C.byref(nr), C.byref(nd)))
     kernel = np.zeros((), CRATER_SHAPE_KERNEL)
-    records = np.zeros(nr.value, CRATER_RECORD)
-    data = np.zeros(nd.value, np.float32)
-    footprints = np.zeros(3 * nr.value, np.float64)
+    records = np.empty(nr.value, CRATER_RECORD)
+    data = np.empty(nd.value, np.float32)
+    footprints = np.empty(3 * nr.value, np.float64)
     N.check(lib.tg_crater_batch(C.byref(population), C.byref(shaping), C.byref(g),
                                 kernel.ctypes.data, records.ctypes.data, nr.value,
                                 data.ctypes.data, nd.value, footprints.ctypes.data,
