@@ -1,16 +1,20 @@
 """Benchmark: Mcells/s of the plain GPU path on the synthetic 4097 x 4097 terrain at 0.5 m
-(8-octave fBm source, 200,000 craters, 1,000,000 boulders of which those resolved are drawn), and
-under "forms" the batched form on 4096 uneven tiles and the served form on a camera request stream,
-each against the plain per-tile path.
+(8-octave fBm source; 200,000 craters with 5 % central peaks and terraced rims above 200 m, as
+terraingen_b200.workloads maps them onto the reference's options; 1,000,000 boulders of which
+those resolved are drawn), and under "forms" the batched form on 4096 uneven tiles, the served
+form on a camera request stream and the DEM refinement, each against the plain per-tile path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tgb200|reference]
 
 A step evaluates one whole tile: the source fill, the crater layer and the boulder layer.
-`value` is device-resident throughput (inputs already in HBM); `e2e` runs the same step through
-the public C ABI with host buffers (tg_evaluate: layer inputs copied in from pinned memory, heights
-copied out, every step). With N ranks (torchrun) each rank evaluates its own tile, with no
-exchange (weak scaling). `--impl reference` times the reference CPU path on a bounded window of
-the same terrain with every host core. Rank 0 prints one JSON line.
+`value` is device-resident throughput (layer inputs already in HBM). `e2e` starts each step from
+the layers' definitions: the crater batch (population, apply order, records) and the boulders are
+built on the host threads and the tile is evaluated through the public C ABI with host buffers
+(tg_evaluate: inputs copied in from pinned memory, heights copied out). `dropin` times the
+reference's own Terrain::Evaluate with Backend::Cuda on this library against Backend::Cpu. With N
+ranks each rank evaluates its own tile, with no exchange (weak scaling); `--gpus N` without
+torchrun starts the N ranks itself. `--impl reference` times the reference CPU path on a bounded
+window of the same terrain with every host core. Rank 0 prints one JSON line.
 """
 
 from __future__ import annotations
@@ -197,10 +201,13 @@ def run_reference(args, rank, world):
               f"crater and boulder densities), reference CPU path, {n} evaluations")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
-        "n_gpus": args.gpus, "steps": n, "warmup": args.warmup, "ms_per_step": round(per * 1e3, 3),
+        "n_gpus": world, "steps": n, "warmup": args.warmup, "ms_per_step": round(per * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": "terrain4097 window", "cells": grid.cells, "pixel_m": PIXEL},
+        "config": {"workload": f"terrain4097 window ({grid.width}x{grid.height} at the tile's "
+                               "center): the same stack as the GPU arm's terrain4097 (fBm, 200k "
+                               "craters per tile with the peak and terrace mapping, 1M boulders "
+                               "per tile)", "cells": grid.cells, "pixel_m": PIXEL},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -584,9 +591,128 @@ def served_form(dev, args, rank, world):
     }
 
 
+def e2e_leg(dev, w, args, world, device_heights):
+    """The e2e leg (see main). Returns the line's `e2e` object plus "_same": whether the last
+    step's heights are the device-resident path's bits (`device_heights`)."""
+    import threading
+
+    import torch
+
+    from terraingen_b200.workloads import TerrainPrep
+
+    def pinned(n, dtype):
+        return torch.empty(n * np.dtype(dtype).itemsize, dtype=torch.uint8).pin_memory() \
+            .numpy().view(dtype)
+
+    preps = [TerrainPrep(w.grid, alloc=pinned), TerrainPrep(w.grid, alloc=pinned)]
+    h_heights = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32).pin_memory()
+    h_out = h_heights.numpy()
+    prep_ms, eval_ms = [], []
+
+    def build(q):
+        t = time.perf_counter()
+        out = preps[q].run()
+        prep_ms.append((time.perf_counter() - t) * 1e3)
+        return out
+
+    def run(steps):
+        ready = [None]
+        worker = None
+
+        def ahead(q):
+            ready[0] = build(q)
+
+        ready[0] = build(0)
+        for i in range(steps):
+            inputs = ready[0]
+            if i + 1 < steps:
+                worker = threading.Thread(target=ahead, args=((i + 1) % 2,))
+                worker.start()
+            kernel, rec, data, foot, stones = inputs
+            t = time.perf_counter()
+            dev.evaluate(w.grid, h_out, fractals=w.fractals, elevation=w.elevation,
+                         craters=(kernel, rec, data, foot), boulders=stones,
+                         boulder_width=w.boulder_width)
+            eval_ms.append((time.perf_counter() - t) * 1e3)
+            if worker is not None:
+                worker.join()
+                worker = None
+
+    run(args.warmup)
+    prep_ms.clear()
+    eval_ms.clear()
+    barrier(world)
+    t0 = time.perf_counter()
+    run(args.steps)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    nr, nd, nb = preps[0].counts
+    h2d = nr * (144 + 24) + nd * 4 + nb * 40
+    return {"value": round(world * w.cells * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(w.cells * 4),
+            "includes": "every step: crater population, apply order and records "
+                        "(tg_crater_batch) and boulder placement (tg_boulder_generate) on "
+                        f"{os.cpu_count()} host threads into pinned buffers, then tg_evaluate "
+                        "with host buffers (inputs in, heights out); the next step's host work "
+                        "overlaps this step's evaluation",
+            "host_prep_ms": round(float(np.median(prep_ms)), 3),
+            "evaluate_ms": round(float(np.median(eval_ms)), 3),
+            "_same": bool(np.array_equal(h_out.view(np.uint32),
+                                         device_heights.cpu().numpy().view(np.uint32)))}
+
+
+def dropin_leg(window):
+    """The reference's own Terrain::Evaluate on the reference arm's window, with Backend::Cuda
+    served by this library's drop-in device (oracle/_ref/libtgref_cuda.so: the reference's
+    pipeline, crater shaping through tg_craters_apply_lists; its source, population, records
+    and boulders stay on its CPU path) against Backend::Cpu of the same build."""
+    from oracle import harness as H
+    from terraingen_b200.workloads import terrain4097_reference_scene
+
+    if not H.available("libtgref_cuda.so"):
+        return {"unavailable": "oracle/_ref/libtgref_cuda.so is not built"}
+    grid, fr, craters, boulders = terrain4097_reference_scene(window, PIXEL)
+    scene = H.make_scene(grid, source_fractals=fr, craters=craters, boulders=boulders)
+    lib = H.dropin()
+    cpu = H.reference()
+    out = {}
+    for name, l, backend in (("cuda", lib, 1), ("cpu", cpu, 0)):
+        H.evaluate(l, scene, backend, 0)
+        times = [H.evaluate(l, scene, backend, 0)[1] for _ in range(3)]
+        out[name] = float(np.median(times))
+    a, _ = H.evaluate(lib, scene, 1, 0)
+    b, _ = H.evaluate(cpu, scene, 0, 0)
+    return {"workload": f"{grid.width}x{grid.height} window of terrain4097 through the "
+                        "reference's Terrain::Evaluate",
+            "cuda_mcells_per_s": round(grid.cells / (out["cuda"] * 1e-3) / 1e6, 3),
+            "cpu_mcells_per_s": round(grid.cells / (out["cpu"] * 1e-3) / 1e6, 3),
+            "speedup": round(out["cpu"] / out["cuda"], 3),
+            "max_abs_diff_m": float(np.abs(a.astype(np.float64) - b).max()),
+            "on_gpu": "crater shaping (RunKernel -> tg_craters_apply_lists)",
+            "cores": os.cpu_count()}
+
+
+def spawn_ranks(n):
+    """`--gpus N` (N > 1) started without torchrun: the same command as N ranks on this node under
+    torch.distributed.run (rendezvous on 127.0.0.1, a free port); returns their exit status."""
+    import socket
+    import subprocess
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()),
+           *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     rank, world, local = dist_setup(args.gpus)
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but {world} ranks were started")
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -662,32 +788,14 @@ def main():
     total_s = max_over_ranks(float(phases.sum()) * 1e-3, world)
     value = world * w.cells * args.steps / total_s / 1e6
 
-    # End to end through the public C ABI with host buffers from pinned memory.
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-    h_rec, h_data, h_foot, h_b = (pin(w.crater_records.view(np.uint8)), pin(w.crater_data),
-                                  pin(w.crater_footprints), pin(w.boulders))
-    h_heights = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32).pin_memory()
-    h_out = h_heights.numpy()
-
-    def e2e_step():
-        dev.evaluate(w.grid, h_out, fractals=w.fractals, elevation=w.elevation,
-                     craters=(w.crater_kernel, h_rec.view(w.crater_records.dtype), h_data,
-                              h_foot),
-                     boulders=h_b, boulder_width=w.boulder_width)
-
-    for _ in range(args.warmup):
-        e2e_step()
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    e2e_value = world * w.cells * args.steps / e2e_s / 1e6
-    h2d = w.input_bytes()
-    d2h = w.cells * 4
-
-    # Parity of the device-resident and end-to-end results (same inputs, same bits).
-    same = bool(torch.equal(heights.cpu(), h_heights))
+    # End to end through the public C ABI from the layers' definitions: every step builds the
+    # crater batch (population, apply order, records) and places the boulders on the host threads
+    # (TerrainPrep: tg_crater_batch, tg_boulder_generate, into pinned buffers), then evaluates
+    # with host buffers (tg_evaluate: inputs copied in, heights copied out). The next step's host
+    # work runs on a second thread while this step evaluates, two sets of buffers in turn.
+    e2e = e2e_leg(dev, w, args, world, heights)
+    same = e2e.pop("_same")
+    e2e_value = e2e["value"]
     forms = {}
     if args.tiles > 0:
         forms["batched"] = batched_form(dev, args, rank, world, alu_peak)
@@ -721,6 +829,7 @@ def main():
     nbins = ((w.grid.width + 31) // 32) * ((w.grid.height + 31) // 32)
     launches = 1 + (3 + scan_launches(nbins)) * 2  # noise; count, scan, scatter, shape/bake x 2
     cpu_value, cpu_per, cpu_n, cpu_grid = cpu_sample(1, 1, args.cpu_window)
+    dropin = dropin_leg(args.cpu_window)
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
@@ -750,8 +859,8 @@ def main():
                          "kind": "reference",
                          "sample": f"{cpu_grid.width}x{cpu_grid.height} window of the same terrain "
                                    f"on the reference CPU path, {cpu_per * 1e3:.0f} ms"},
-        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "matches_device_path": same},
+        "e2e": {**e2e, "matches_device_path": same},
+        "dropin": dropin,
         "gpu_launches": int(launches * args.steps),
         "clocks": clocks.summary(),
         "forms": forms,

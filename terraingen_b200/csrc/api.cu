@@ -523,8 +523,8 @@ namespace {
 // launches need. `any` is false when no cell needs a crater.
 struct CraterPrep {
     CraterBins bins{};
-    float* harmonics = nullptr;
-    bool fast = false;
+    bool lean = false;    // lean kernel on LeanEntry bins (plain kernel options)
+    bool extras = false;  // some crater has work for the extras pass
     bool any = false;
 };
 
@@ -572,16 +572,20 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     if (total == 0) {
         return TG_OK;
     }
-    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) * sizeof(BinEntry)), "allocation");
+    p.lean = crater_lean_entries(k);
+    p.extras = (d->pinnedStatus[1] & 4u) != 0u;
+    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) *
+                                          (p.lean ? kLeanEntryBytes : sizeof(BinEntry))),
+            "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
     bins.capacity = total;
-    p.fast = crater_lean_entries(k);
-    if (p.fast && nData > 0) {
-        TG_CUDA(d->slots[kHarmonics].reserve(size_t(nData) * sizeof(float)), "allocation");
-        p.harmonics = slot_ptr<float>(d, kHarmonics);
-        TG_CUDA(launch_crater_harmonics(rec, n, data, p.harmonics, s), "harmonics launch");
+    void* leans = nullptr;
+    if (p.lean) {
+        TG_CUDA(d->slots[kHarmonics].reserve(size_t(n) * kLeanCraterBytes), "allocation");
+        leans = d->slots[kHarmonics].ptr;
+        TG_CUDA(launch_crater_lean(k, rec, n, data, leans, s), "lean crater launch");
     }
-    TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, s), "crater scatter launch");
+    TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, leans, s), "crater scatter launch");
     p.any = true;
     return TG_OK;
 }
@@ -613,8 +617,8 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(launch_crater_shape(k, data, p.harmonics, p.fast, g, to_nodata(nodata), p.bins, dh, s,
-                                0, 0xffffffffu, d->waitPolls),
+    TG_CUDA(launch_crater_shape(k, rec, data, p.lean, p.extras, g, to_nodata(nodata), p.bins, dh,
+                                s, 0, 0xffffffffu, d->waitPolls),
             "crater shape launch");
     return crater_finish(d, p, s);
 }
@@ -1146,9 +1150,10 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         for (uint32_t k0 = 0, q = 0; k0 < binRows; k0 += per, ++q) {
             const uint32_t rows = std::min(per, binRows - k0);
             if (cp.any) {
-                if (cudaError_t e = launch_crater_shape(k, static_cast<const float*>(ddata),
-                                                        cp.harmonics, cp.fast, g, none, cp.bins,
-                                                        dh, s, k0, rows, d->waitPolls)) {
+                if (cudaError_t e = launch_crater_shape(
+                        k, static_cast<const CraterRecord*>(drec),
+                        static_cast<const float*>(ddata), cp.lean, cp.extras, g, none, cp.bins,
+                        dh, s, k0, rows, d->waitPolls)) {
                     return drain(cuda_fail(e, "crater shape launch"));
                 }
             }

@@ -1011,49 +1011,227 @@ __device__ __forceinline__ float fast_contribution(const FastKernel& k,
     return c.resolution * height;
 }
 
-// The lean path of the plain binned kernel: fast_contribution's outline by rotation, and also
-// complex craters (a closed-form `ComplexProfileHeight` with its round dome) and their massif
-// peaks (`KernelPeakRelief`, whose noise runs in a separate function only near the center). The
-// record must carry nothing the general path alone handles (tables, marks, terraces, a floor
-// shift, an upslope or a datum), and the kernel's options must be plain (crater_options_plain).
-__device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
-                                                   const float* __restrict__ harmonics,
-                                                   const float* __restrict__ data,
-                                                   const CraterRecord& c, float dx, float dy,
-                                                   bool& reached) {
-    const float radius = 0.5f * c.diameter;
-    float distance = sqrtf(dx * dx + dy * dy);
-    if (c.ellipticity != 1.0f || c.harmonicCount > 0u) {
-        const float share = outline_share(distance / radius) * worn_outline_share(c);
-        distance /= fast_outline_scale(harmonics, c, dx, dy, distance, share);
+// --- the plain path's lean craters -------------------------------------------------------------
+//
+// The plain binned kernel shapes most craters from a LeanCrater: what one crater's contribution
+// reads, prepared once per crater (lean_crater) so that a (cell, crater) pair reads it in a few
+// 16-byte shared-memory loads and spends no instruction on per-crater constants. It covers the
+// closed-form simple profiles (Fassett-Thomson, Martin-Parkes-Dunstan), complex craters with their
+// round central dome, ellipses and up to kLeanHarmonics power-law outline harmonics, under plain
+// kernel options (no rim smoothing, noise, texture or diffusion). Each per-crater constant is the
+// same float expression the per-pair path evaluates (complex_peak, the floor share, sincosf of
+// the heading, ...), so it has the same bits. Per pair the outline's harmonics are summed by
+// Horner's rule in the complex plane, sum_k (A_k + i B_k) (q e^{i theta})^k with q the square root
+// of the kept share, which is the reference's sum of A_k cos(k theta + phase) share^(k/2) within
+// a few float roundings. A crater with massif peaks is shaped here with its round dome; the
+// massifs' difference from the dome is added by the extras pass, as is every crater the lean path
+// cannot shape (flag kLeanHeavy: tables, marks, terraces, floor shifts, upslopes, datums, more
+// harmonics).
+constexpr uint32_t kLeanHarmonics = 11;
+constexpr uint32_t kLeanComplex = 2u;       // profile kind: 0 FT, 1 MPD, 2 complex
+constexpr uint32_t kLeanOutline = 1u << 2;  // ellipse or harmonics
+constexpr uint32_t kLeanEllipse = 1u << 3;
+constexpr uint32_t kLeanHeavy = 1u << 4;    // the extras pass shapes it whole
+constexpr uint32_t kLeanMassifs = 1u << 5;  // the extras pass adds its massif peak
+
+struct LeanCrater {
+    float x, xLow, y, yLow;
+    float diameter, radius, resolution, reach;        // reach = reachRadii * radius
+    float freshRim, currentDepth, currentRim, worn;   // worn = worn_outline_share
+    float floorShare, peakBase, peakHeight, kept;     // complex craters
+    float headingCos, headingSin, along, across;      // ellipse
+    uint32_t flags;        // profile kind, kLean* bits, first harmonic << 8, count << 16
+    uint32_t record;       // the crater's index in the batch
+    float peakReach2;      // squared reach of its massif peak (kLeanMassifs)
+    float ellipticity;
+    float2 harmonics[kLeanHarmonics];  // (A cos phase, A sin phase)
+    float pad[2];
+};
+static_assert(sizeof(LeanCrater) == 192, "LeanCrater must be a multiple of 16 bytes");
+
+// The lean form of record `c` under kernel `k` (harmonics from `data`).
+__device__ inline LeanCrater lean_crater(const CraterShapeKernel& k, const CraterRecord& c,
+                                         const float* __restrict__ data, uint32_t index) {
+    LeanCrater l{};
+    l.x = c.x;
+    l.xLow = c.xLow;
+    l.y = c.y;
+    l.yLow = c.yLow;
+    l.diameter = c.diameter;
+    l.radius = 0.5f * c.diameter;
+    l.resolution = c.resolution;
+    l.reach = k.reachRadii * l.radius;
+    l.freshRim = c.freshRim;
+    l.currentDepth = c.currentDepth;
+    l.currentRim = c.currentRim;
+    l.worn = worn_outline_share(c);
+    l.record = index;
+    l.ellipticity = c.ellipticity;
+    uint32_t flags = k.profile.simple == kProfileMartinParkesDunstan ? 1u : 0u;
+    const bool complex = k.profile.complex == 1u && c.diameter >= k.profile.transitionDiameter;
+    if (complex) {
+        flags = kLeanComplex;
+        const CraterProfileKernel& p = k.profile;
+        l.floorShare = smin(
+            0.9f, kilometer_law(p.floorCoefficient, p.floorExponent, c.diameter, false) /
+                      c.diameter);
+        const PeakSize size = complex_peak(p, c.diameter);
+        l.peakBase = size.base;
+        l.peakHeight = size.height;
+        const State s{c.freshDepth, c.freshRim, c.currentDepth, c.currentRim};
+        l.kept = kept_depth(s);
+        if (c.peakCount > 0u) {
+            flags |= kLeanMassifs;
+            PeakSize scaled = size;
+            scaled.base *= value(data, c.peakOffset + 5u);
+            const float reach = TGB_PEAK_REACH * smax(size.base, scaled.base);
+            l.peakReach2 = reach * reach;
+        }
     }
-    reached = distance < k.reachRadii * radius;
+    if (c.ellipticity != 1.0f) {
+        flags |= kLeanEllipse;
+        sincosf(c.heading, &l.headingSin, &l.headingCos);
+        l.along = sqrtf(c.ellipticity);
+        l.across = 1.0f / l.along;
+    }
+    if (c.ellipticity != 1.0f || c.harmonicCount > 0u) {
+        flags |= kLeanOutline;
+    }
+    const bool heavy = c.tableCount > 0u || c.markCount > 0u || c.terraceCount > 0u ||
+                       c.shiftX != 0.0f || c.shiftY != 0.0f || c.upslopeX != 0.0f ||
+                       c.upslopeY != 0.0f || c.hasDatum == 1u ||
+                       c.harmonicCount > kLeanHarmonics || c.firstHarmonic > 255u;
+    if (heavy) {
+        flags |= kLeanHeavy;
+    } else {
+        for (uint32_t h = 0; h < c.harmonicCount; ++h) {
+            const float amplitude = value(data, c.harmonicOffset + 2u * h);
+            const float phase = value(data, c.harmonicOffset + 2u * h + 1u);
+            float sp, cp;
+            sincosf(phase, &sp, &cp);
+            l.harmonics[h] = make_float2(amplitude * cp, amplitude * sp);
+        }
+        flags |= (c.firstHarmonic << 8) | (c.harmonicCount << 16);
+    }
+    l.flags = flags;
+    return l;
+}
+
+// The kernel's constants the lean path reads per pair, made once per launch: the complex
+// exterior's value at its reach, edge = complexReachRadii^-ejectaExponent, and 1 / (1 - edge).
+struct LeanKernel {
+    float edge, fallScale;
+};
+
+__device__ __forceinline__ LeanKernel lean_kernel(const CraterShapeKernel& k) {
+    const float edge = powf(k.profile.complexReachRadii, -k.profile.ejectaExponent);
+    return LeanKernel{edge, 1.0f / (1.0f - edge)};
+}
+
+// What lean crater `l` adds at (dx, dy) from its center (resolution times the shaped relief, the
+// round dome in place of massifs); `reached` is false beyond its reach.
+__device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
+                                                   const LeanKernel& lk, const LeanCrater& l,
+                                                   float dx, float dy, bool& reached) {
+    const uint32_t flags = l.flags;
+    const float d2 = dx * dx + dy * dy;
+    float distance = sqrtf(d2);
+    if (flags & kLeanOutline) {
+        // KernelProfileDistance (craters.h:1028) with the outline's scale. The share is
+        // smoothstep(distance / radius), exactly 1 from the rim out.
+        const float share =
+            (distance >= l.radius ? 1.0f : outline_share(distance / l.radius)) * l.worn;
+        float c1 = 1.0f, s1 = 0.0f;  // the direction; angle 0 at the center, as KernelAngle
+        if (distance > 0.0f) {
+            const float inv = rsqrtf(d2);
+            c1 = dx * inv;
+            s1 = dy * inv;
+        }
+        float scale = 1.0f;
+        if (flags & kLeanEllipse) {
+            const float cd = c1 * l.headingCos + s1 * l.headingSin;
+            const float sd = s1 * l.headingCos - c1 * l.headingSin;
+            const float u = cd * l.across;  // cd / along
+            const float v = sd * l.along;   // sd / across
+            scale = rsqrtf(u * u + v * v);
+        }
+        const uint32_t count = (flags >> 16) & 0xffu;
+        if (share > 0.0f && count > 0u) {
+            // w = q e^{i theta}, q = share^(1/2) (1 at full share).
+            const float q = share < 1.0f ? sqrtf(share) : 1.0f;
+            const float wr = q * c1, wi = q * s1;
+            float pr = l.harmonics[count - 1u].x, pi = l.harmonics[count - 1u].y;
+            for (int h = int(count) - 2; h >= 0; --h) {
+                const float t = pr * wr - pi * wi + l.harmonics[h].x;
+                pi = pr * wi + pi * wr + l.harmonics[h].y;
+                pr = t;
+            }
+            // times w^first
+            for (uint32_t m = (flags >> 8) & 0xffu; m > 0u; --m) {
+                const float t = pr * wr - pi * wi;
+                pi = pr * wi + pi * wr;
+                pr = t;
+            }
+            scale *= 1.0f + pr;
+        }
+        distance /= scale;
+    }
+    reached = distance < l.reach;
     if (!reached) {
         return 0.0f;
     }
     float height;
-    if (k.profile.complex == 1u && c.diameter >= k.profile.transitionDiameter) {
-        const State s{c.freshDepth, c.freshRim, c.currentDepth, c.currentRim};
-        height = complex_height(k.profile, distance, c.diameter, s);
-        if (c.peakCount > 0u) {
-            height += peak_relief(k, data, c, s, distance, dx, dy);
+    const uint32_t kind = flags & 3u;
+    if (kind == kLeanComplex) {
+        // ComplexProfileHeight (craters.h:479) with its per-crater constants made once.
+        const float x = distance / l.radius;
+        const float depth = l.currentDepth * l.diameter;
+        const float rim = l.currentRim * l.diameter;
+        const CraterProfileKernel& p = k.profile;
+        if (x >= 1.0f) {
+            if (x >= p.complexReachRadii) {
+                height = 0.0f;
+            } else {
+                const float fall = p.ejectaExponent == 3.0f ? __frcp_rn(x * x * x)
+                                                            : powf(x, -p.ejectaExponent);
+                height = rim * (fall - lk.edge) * lk.fallScale;
+            }
+        } else {
+            height = rim - depth;
+            if (x > l.floorShare) {
+                const float t = (x - l.floorShare) / (1.0f - l.floorShare);
+                height += depth * t * t;
+            }
+            height += l.kept * peak_dome(PeakSize{l.peakHeight, l.peakBase}, distance);
         }
-    } else if (k.profile.simple == kProfileMartinParkesDunstan) {
-        height = mpd_height(distance, c.diameter, c.freshRim, c.currentDepth, c.currentRim);
+    } else if (kind == 1u) {
+        height = mpd_height(distance, l.diameter, l.freshRim, l.currentDepth, l.currentRim);
     } else {
-        height = ft_shape(distance / radius, k.profile.rim, c.freshRim, c.currentDepth) *
-                 c.diameter;
+        height = ft_shape(distance / l.radius, k.profile.rim, l.freshRim, l.currentDepth) *
+                 l.diameter;
     }
-    return c.resolution * height;
+    return l.resolution * height;
 }
 
-// The general contribution as a function of its own, so the kernels that call it for a few
-// heavy records keep the lean path's register budget.
-static __device__ __noinline__ Contribution general_contribution(const CraterShapeKernel& k,
-                                                                 const float* data,
-                                                                 const CraterRecord& c, float dx,
-                                                                 float dy) {
-    return crater_contribution(k, data, c, dx, dy);
+// The extras of crater `c` at (dx, dy): with kLeanHeavy its whole contribution (the general
+// path); otherwise the massif peak's difference from the round dome the lean path gave it
+// (KernelPeakRelief, craters.h:1161), 0 beyond the peak's reach.
+static __device__ __noinline__ float extra_contribution(const CraterShapeKernel& k,
+                                                        const float* data, const CraterRecord& c,
+                                                        uint32_t flags, float dx, float dy,
+                                                        bool& reached) {
+    if (flags & kLeanHeavy) {
+        const Contribution q = crater_contribution(k, data, c, dx, dy);
+        reached = q.reached;
+        return q.shaped;
+    }
+    const float distance = shifted_distance(data, c, dx, dy);
+    reached = distance < k.reachRadii * (0.5f * c.diameter);
+    if (!reached) {
+        return 0.0f;
+    }
+    const State s{c.freshDepth, c.freshRim, c.currentDepth, c.currentRim};
+    return c.resolution * peak_relief(k, data, c, s, distance, dx, dy);
 }
 
 }  // namespace crater

@@ -57,9 +57,8 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
             if (r.hasDatum == 1u) {
                 atomicOr(flags, 1u);
             }
-            // Anything beyond an ellipse and power-law harmonics, or a complex crater, needs
-            // the general path.
-            if (crater_entry_heavy(k, r)) {
+            // Work for the extras pass after the lean kernel (heavy records, massif peaks).
+            if (crater_needs_extras(k, r)) {
                 atomicOr(flags, 4u);
             }
         }
@@ -88,9 +87,11 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
 // Each warp takes 32 craters and spreads all of their (crater, bin) pairs over its lanes: a
 // lane finds its pair's crater by a search of the warp's running bin counts, then copies the
 // crater's record and tail into its bin's next slot.
+// With `leans` the entries are LeanEntry (the crater's LeanCrater and the tail), else BinEntry
+// (its record and the tail).
 __global__ void crater_scatter_kernel(const CraterShapeKernel k,
                                       const CraterRecord* __restrict__ records, uint32_t n,
-                                      CraterBins bins) {
+                                      const int4* __restrict__ leans, CraterBins bins) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
     if (base >= n) {
@@ -137,29 +138,38 @@ __global__ void crater_scatter_kernel(const CraterShapeKernel k,
                                  __shfl_sync(0xffffffffu, tiles.w, int(owner)));
         const float c = __shfl_sync(0xffffffffu, cull, int(owner));
         const uint32_t before = __shfl_sync(0xffffffffu, upto - count, int(owner));
-        if (q >= pairs) {
-            continue;
-        }
-        const uint32_t local = q - before;
-        const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
-        const uint32_t by0 = uint32_t(t.z) / kTilesPerBin;
-        const uint32_t wide = bx1 - bx0 + 1u;
-        const uint32_t b = (by0 + local / wide) * bins.binsX + bx0 + local % wide;
-        const uint32_t slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
-        if (slot >= bins.capacity) {
-            continue;  // the host sized the entries from the counts; never taken
-        }
         const uint32_t crater = base + owner;
-        const int4* src = reinterpret_cast<const int4*>(records + crater);
-        int4* dst = reinterpret_cast<int4*>(bins.entries + slot);
-#pragma unroll
-        for (int w = 0; w < 9; ++w) {
-            dst[w] = __ldg(src + w);
+        uint32_t slot = 0xffffffffu;  // none
+        if (q < pairs) {
+            const uint32_t local = q - before;
+            const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
+            const uint32_t by0 = uint32_t(t.z) / kTilesPerBin;
+            const uint32_t wide = bx1 - bx0 + 1u;
+            const uint32_t b = (by0 + local / wide) * bins.binsX + bx0 + local % wide;
+            slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
+            if (slot >= bins.capacity) {
+                slot = 0xffffffffu;  // the host sized the entries from the counts; never taken
+            }
         }
-        const uint32_t heavy = crater_entry_heavy(k, records[crater]) ? kHeavyEntry : 0u;
-        dst[9] = make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
-                           int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
-                           int(crater | heavy));
+        // Each lane writes its entry's 16-byte tail; the bodies (the crater's LeanCrater or
+        // record) are copied one entry at a time by the whole warp, 16 contiguous bytes a lane.
+        const uint32_t words = leans != nullptr ? 13u : 10u;
+        int4* entries = reinterpret_cast<int4*>(bins.entries);
+        if (slot != 0xffffffffu) {
+            const uint32_t extras = crater_needs_extras(k, records[crater]) ? kHeavyEntry : 0u;
+            entries[size_t(slot) * words + words - 1u] =
+                make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
+                          int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
+                          int(crater | extras));
+        }
+        const int4* bodies = leans != nullptr ? leans : reinterpret_cast<const int4*>(records);
+        for (uint32_t from = 0; from < 32u; ++from) {
+            const uint32_t s = __shfl_sync(0xffffffffu, slot, int(from));
+            const uint32_t src = __shfl_sync(0xffffffffu, crater, int(from));
+            if (s != 0xffffffffu && lane < words - 1u) {
+                entries[size_t(s) * words + lane] = __ldg(bodies + size_t(src) * (words - 1u) + lane);
+            }
+        }
     }
 }
 
@@ -184,31 +194,243 @@ __global__ void crater_harmonics_kernel(const CraterRecord* __restrict__ records
 }
 
 // Shaping a bin. Each warp owns 4 rows x 32 columns of the bin (each thread 4 adjacent cells of
-// one row). For every staged crater the warp first finds which of its 128 cells need it (inside
-// a reference tile the crater's window touches, and within its cull radius), then queues those
-// (crater, cell) pairs in shared memory and evaluates them 32 at a time, one pair per lane, so a
-// small crater that needs a handful of cells no longer leaves most lanes of the warp idle. The
-// contributions are FP32 values added into FP64 accumulators in shared memory: that sum is exact
-// for these magnitudes, so the atomic adds give the same bits in any order.
+// one row). For every staged crater the warp first finds which of its 128 cells need it (within
+// its cull radius, and for stretched craters inside a reference tile its window touches), then
+// queues those (crater, cell) pairs in shared memory and evaluates them 32 at a time, one pair
+// per lane, so a small crater that needs a handful of cells does not leave most lanes of the
+// warp idle.
 //
-// With kFast, entries marked kHeavyEntry (complex craters, peaks, terraces, tables) queue apart
-// and are drained through the general contribution, so a batch with a few such craters keeps the
-// lean path for all the others.
+// Accumulation is in 64-bit fixed point (2^-32 m): each contribution is rounded once to a
+// multiple of 2^-32 m and the integers are summed, which is exact and associative, so the bins'
+// atomically scattered entry order cannot change a bit; the cell's height is the float of its
+// height before the layer plus that sum. The warp owns its 128 accumulators, so lanes of one
+// drain that land on different cells never collide; lanes on the same cell add atomically.
 constexpr int kQueue = 160;  // 31 pairs left over plus one crater's 128
+constexpr float kFixedScale = 4294967296.0f;  // 2^32 per meter
+constexpr double kFixedUnit = 1.0 / 4294967296.0;
 
-template <bool kFast>
-__global__ void __launch_bounds__(kShapeThreads, kFast ? 2 : 1)
+__device__ __forceinline__ long long to_fixed(float v) {
+    return __float2ll_rn(v * kFixedScale);
+}
+
+__device__ __forceinline__ void add_fixed(long long* acc, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(acc), static_cast<unsigned long long>(v));
+}
+
+// The cells a warp owns and their split positions (MakeSplitPoint, crater_kernel.cpp:303: the
+// column centers at row 0 and the row center at column 0, as the reference's strips carry them).
+struct WarpCells {
+    uint32_t row, col0, cell0;
+    bool rowIn;
+    bool live[kCellsPerThread];
+    float base[kCellsPerThread];
+    float pxh[kCellsPerThread], pxl[kCellsPerThread];
+    float pyh, pyl;
+    int tileX, tileY;
+    bool anyLive;
+};
+
+__device__ __forceinline__ WarpCells warp_cells(const Grid& grid, const NoData& nodata,
+                                                const float* __restrict__ heights, uint32_t binX,
+                                                uint32_t binY, uint32_t warp, uint32_t lane) {
+    WarpCells w;
+    w.row = binY * kBinCells + warp * 4u + lane / 8u;
+    w.col0 = binX * kBinCells + (lane % 8u) * kCellsPerThread;
+    w.cell0 = (lane / 8u) * 32u + (lane % 8u) * kCellsPerThread;
+    const double yd =
+        grid.originY + 0.5 * grid.colRotation + (double(w.row) + 0.5) * grid.pixelHeight;
+    w.pyh = float(yd);
+    w.pyl = float(yd - double(w.pyh));
+    w.rowIn = w.row < grid.height;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        const uint32_t col = w.col0 + j;
+        const double xd =
+            grid.originX + (double(col) + 0.5) * grid.pixelWidth + 0.5 * grid.rowRotation;
+        w.pxh[j] = float(xd);
+        w.pxl[j] = float(xd - double(w.pxh[j]));
+        w.live[j] = w.rowIn && col < grid.width;
+        w.base[j] = 0.0f;
+        if (w.live[j]) {
+            w.base[j] = heights[size_t(w.row) * grid.width + col];
+            w.live[j] = !is_nodata(nodata, w.base[j]);
+        }
+    }
+    w.tileX = int(w.col0 / kRefTileCells);
+    w.tileY = int(w.row / kRefTileCells);
+    w.anyLive = w.live[0] || w.live[1] || w.live[2] || w.live[3];
+    return w;
+}
+
+// The cell-center box of a warp's 4 x 32 cells on an axis-aligned grid, with a quarter cell to
+// spare for rounding: a crater whose cull circle misses it needs none of the warp's cells.
+struct WarpBox {
+    float xh, xl, yh, yl, halfW, halfH;
+    bool on;
+};
+
+__device__ __forceinline__ WarpBox warp_box(const Grid& grid, uint32_t binX, uint32_t binY,
+                                            uint32_t warp) {
+    WarpBox b;
+    b.on = grid.rowRotation == 0.0 && grid.colRotation == 0.0;
+    const double x = grid.originX + (double(binX * kBinCells) + 16.0) * grid.pixelWidth;
+    const double y = grid.originY + (double(binY * kBinCells + warp * 4u) + 2.0) * grid.pixelHeight;
+    b.xh = float(x);
+    b.xl = float(x - double(b.xh));
+    b.yh = float(y);
+    b.yl = float(y - double(b.yh));
+    b.halfW = 15.75f * float(fabs(grid.pixelWidth));
+    b.halfH = 1.75f * float(fabs(grid.pixelHeight));
+    return b;
+}
+
+__device__ __forceinline__ bool box_misses(const WarpBox& b, float x, float xLow, float y,
+                                           float yLow, float cull) {
+    if (!b.on) {
+        return false;
+    }
+    const float gx = fmaxf(fabsf(crater::split_difference(b.xh, b.xl, x, xLow)) - b.halfW, 0.0f);
+    const float gy = fmaxf(fabsf(crater::split_difference(b.yh, b.yl, y, yLow)) - b.halfH, 0.0f);
+    return gx * gx + gy * gy >= cull * cull;
+}
+
+// The lane's cells that need a crater at (x, y) within `cull`, as bits.
+__device__ __forceinline__ uint32_t need_mask(const WarpCells& w, bool inTile, float x,
+                                              float xLow, float y, float yLow, float cull) {
+    const float dy = crater::split_difference(w.pyh, w.pyl, y, yLow);
+    const float cull2 = cull * cull;
+    uint32_t need = 0;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        const float dx = crater::split_difference(w.pxh[j], w.pxl[j], x, xLow);
+        if (inTile && w.live[j] && dx * dx + dy * dy < cull2) {
+            need |= 1u << j;
+        }
+    }
+    return need;
+}
+
+// Appends the lanes' needed pairs (entry e, cell) to the warp's queue; returns how many.
+__device__ __forceinline__ uint32_t enqueue(uint16_t* queue, uint32_t length, uint32_t need,
+                                            uint32_t e, uint32_t cell0, uint32_t lane) {
+    const uint32_t mine = __popc(need);
+    uint32_t before = mine;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, before, d);
+        if (lane >= uint32_t(d)) {
+            before += v;
+        }
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, before, 31);
+    uint32_t slot = length + before - mine;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        if (need & (1u << j)) {
+            queue[slot++] = uint16_t((e << 7) | (cell0 + j));
+        }
+    }
+    return total;
+}
+
+// Writes a thread's cells: base height plus the fixed-point sum, one 16-byte store when it can.
+__device__ __forceinline__ void write_cells(const Grid& grid, const WarpCells& w,
+                                            const long long* acc, float* __restrict__ heights) {
+    if (!w.rowIn) {
+        return;
+    }
+    float out[kCellsPerThread];
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        out[j] = float(double(w.base[j]) + double(acc[w.cell0 + j]) * kFixedUnit);
+    }
+    float* dst = heights + size_t(w.row) * grid.width + w.col0;
+    const bool vec = (grid.width % 4u == 0u) && w.col0 + 3 < grid.width &&
+                     ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0u) && w.live[0] &&
+                     w.live[1] && w.live[2] && w.live[3];
+    if (vec) {
+        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kCellsPerThread; ++j) {
+            if (w.live[j]) {
+                dst[j] = out[j];
+            }
+        }
+    }
+}
+
+// The staged-copy pipeline of a bin's entries: two shared buffers, each filled by one TMA bulk
+// copy completing on its mbarrier. On a wait that gives up (`polls`) it records flag 2 and waits,
+// bounded by the default limit, for the copies still in flight, so none lands in a finished CTA.
+template <typename Entry, uint32_t kStage>
+struct Stager {
+    Entry (*stage)[kStage];
+    uint64_t* bars;
+    const Entry* src;
+    uint32_t count, chunks, phase[2];
+
+    __device__ void issue(uint32_t c) {
+        const uint32_t s = c & 1u;
+        const uint32_t n = min(kStage, count - c * kStage);
+        const uint32_t bytes = n * uint32_t(sizeof(Entry));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bars[s], bytes);
+        bulk_copy_g2s(&stage[s][0], src + c * kStage, bytes, &bars[s]);
+    }
+
+    // Thread 0 only: inits the barriers and starts the first two chunks.
+    __device__ void start() {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
+        if (chunks > 1) {
+            issue(1);
+        }
+    }
+
+    // Every thread: waits for chunk c; false (after the drain) when it did not arrive.
+    __device__ bool wait(uint32_t c, uint32_t polls, uint32_t* flags) {
+        const uint32_t s = c & 1u;
+        const bool failed = !mbar_wait(&bars[s], phase[s], polls);
+        if (__syncthreads_or(failed)) {
+            if (threadIdx.x == 0) {
+                atomicOr(flags, 2u);
+                mbar_wait(&bars[s], phase[s]);
+                if (c + 1 < chunks) {
+                    mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                }
+            }
+            return false;
+        }
+        phase[s] ^= 1u;
+        return true;
+    }
+
+    // After every warp has read chunk c: its buffer takes chunk c + 2.
+    __device__ void refill(uint32_t c) {
+        if (c + 2 < chunks) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                issue(c + 2);
+            }
+        }
+    }
+};
+
+// The general binned kernel: any kernel options and any record, from the 160-byte BinEntry.
+__global__ void __launch_bounds__(kShapeThreads)
     crater_shape_kernel(const CraterShapeKernel k, const float* __restrict__ data,
-                        const float* __restrict__ harmonics, const Grid grid, const NoData nodata,
-                        const CraterBins bins, float* __restrict__ heights,
-                        uint32_t* __restrict__ flags, const uint32_t polls) {
+                        const Grid grid, const NoData nodata, const CraterBins bins,
+                        float* __restrict__ heights, uint32_t* __restrict__ flags,
+                        const uint32_t polls) {
     __shared__ __align__(128) BinEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
-    __shared__ double accs[kShapeThreads / 32][128];
+    __shared__ long long accs[kShapeThreads / 32][128];
     __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
-    __shared__ uint16_t heavyQueues[kShapeThreads / 32][kFast ? kQueue : 1];
-    __shared__ float2 columns[kShapeThreads / 32][32];  // split x of the warp's 32 columns
-    __shared__ float2 rows[kShapeThreads / 32][4];      // split y of its 4 rows
+    __shared__ float2 columns[kShapeThreads / 32][32];
+    __shared__ float2 rows[kShapeThreads / 32][4];
 
     const uint32_t bin = bins.firstBin + blockIdx.x;
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
@@ -218,242 +440,299 @@ __global__ void __launch_bounds__(kShapeThreads, kFast ? 2 : 1)
         return;
     }
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    const uint32_t row = binY * kBinCells + warp * 4u + lane / 8u;
-    const uint32_t col0 = binX * kBinCells + (lane % 8u) * kCellsPerThread;
-    double* acc = accs[warp];
+    Stager<BinEntry, kChunk> st{stage, bars, bins.entries + first, count,
+                                (count + kChunk - 1) / kChunk, {0u, 0u}};
+    if (tid == 0) {
+        st.start();
+    }
+    const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
+    const WarpBox box = warp_box(grid, binX, binY, warp);
+    long long* acc = accs[warp];
     uint16_t* queue = queues[warp];
-    uint16_t* heavyQueue = heavyQueues[warp];
-    const uint32_t cell0 = (lane / 8u) * 32u + (lane % 8u) * kCellsPerThread;
-
-    // This thread's cells: split positions (MakeSplitPoint, crater_kernel.cpp:303) of the
-    // column centers at row 0 and the row center at column 0, as the reference's strips carry.
-    float pxh[kCellsPerThread], pxl[kCellsPerThread];
-    bool live[kCellsPerThread];
-    const double yd = grid.originY + 0.5 * grid.colRotation + (double(row) + 0.5) * grid.pixelHeight;
-    const float pyh = float(yd);
-    const float pyl = float(yd - double(pyh));
-    const bool rowIn = row < grid.height;
 #pragma unroll
     for (int j = 0; j < kCellsPerThread; ++j) {
-        const uint32_t col = col0 + j;
-        const double xd =
-            grid.originX + (double(col) + 0.5) * grid.pixelWidth + 0.5 * grid.rowRotation;
-        pxh[j] = float(xd);
-        pxl[j] = float(xd - double(pxh[j]));
-        live[j] = rowIn && col < grid.width;
-        double h = 0.0;
-        if (live[j]) {
-            const float v = heights[size_t(row) * grid.width + col];
-            live[j] = !is_nodata(nodata, v);
-            h = double(v);
-        }
-        acc[cell0 + j] = h;
+        acc[w.cell0 + j] = 0;
         if (lane < 8u) {
-            columns[warp][(lane % 8u) * kCellsPerThread + j] = make_float2(pxh[j], pxl[j]);
+            columns[warp][(lane % 8u) * kCellsPerThread + j] = make_float2(w.pxh[j], w.pxl[j]);
         }
     }
     if (lane % 8u == 0u) {
-        rows[warp][lane / 8u] = make_float2(pyh, pyl);
+        rows[warp][lane / 8u] = make_float2(w.pyh, w.pyl);
     }
-    const int tileX = int(col0 / kRefTileCells), tileY = int(row / kRefTileCells);
-    const bool anyLive = live[0] || live[1] || live[2] || live[3];
-    // The warp's 4 x 32 cell centers as a box (axis-aligned grids): a crater whose cull circle
-    // misses it, with a quarter cell to spare for rounding, needs none of the warp's cells, and
-    // the warp passes it over at once (the same decision in every lane).
-    const bool boxTest = grid.rowRotation == 0.0 && grid.colRotation == 0.0;
-    const double boxX = grid.originX + (double(binX * kBinCells) + 16.0) * grid.pixelWidth;
-    const double boxY = grid.originY + (double(binY * kBinCells + warp * 4u) + 2.0) * grid.pixelHeight;
-    const float boxXh = float(boxX), boxXl = float(boxX - double(boxXh));
-    const float boxYh = float(boxY), boxYl = float(boxY - double(boxYh));
-    const float halfW = 15.75f * float(fabs(grid.pixelWidth));
-    const float halfH = 1.75f * float(fabs(grid.pixelHeight));
+    __syncthreads();
 
-    // Evaluates the 32 (or, at a flush, `n`) pairs queued in `q` from `from`, one per lane; the
-    // general contribution when `general` (always without kFast).
-    auto drain = [&](const BinEntry* chunk, const uint16_t* q, uint32_t from, uint32_t n,
-                     bool general) {
+    auto drain = [&](const BinEntry* chunk, uint32_t from, uint32_t n) {
         if (lane < n) {
-            const uint32_t code = q[from + lane];
-            const BinEntry& entry = chunk[code >> 7];
-            const CraterRecord& r = entry.record;
+            const uint32_t code = queue[from + lane];
+            const CraterRecord& r = chunk[code >> 7].record;
             const uint32_t cell = code & 127u;
             const float2 cx = columns[warp][cell & 31u];
             const float2 cy = rows[warp][cell >> 5];
             const float dy = crater::split_difference(cy.x, cy.y, r.y, r.yLow);
             const float dx = crater::split_difference(cx.x, cx.y, r.x, r.xLow);
-            if (kFast && !general) {
-                bool reached;
-                const float shaped =
-                    crater::lean_contribution(k, harmonics, data, r, dx, dy, reached);
-                if (reached) {
-                    atomicAdd(acc + cell, double(shaped));
-                }
-            } else if (kFast) {
-                const crater::Contribution q = crater::general_contribution(k, data, r, dx, dy);
-                if (q.reached) {
-                    atomicAdd(acc + cell, double(q.shaped));
-                }
-            } else {
-                const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
-                if (q.reached) {
-                    atomicAdd(acc + cell, double(q.shaped));
-                }
+            const crater::Contribution q = crater::crater_contribution(k, data, r, dx, dy);
+            if (q.reached) {
+                add_fixed(acc + cell, to_fixed(q.shaped));
             }
         }
     };
 
-    const uint32_t chunks = (count + kChunk - 1) / kChunk;
-    if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    auto issue = [&](uint32_t c) {
-        const uint32_t s = c & 1u;
-        const uint32_t n = min(kChunk, count - c * kChunk);
-        const uint32_t bytes = n * uint32_t(sizeof(BinEntry));
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bars[s], bytes);
-        bulk_copy_g2s(&stage[s][0], bins.entries + first + c * kChunk, bytes, &bars[s]);
-    };
-    if (tid == 0) {
-        issue(0);
-        if (chunks > 1) {
-            issue(1);
-        }
-    }
-    uint32_t phase[2] = {0u, 0u};
-    bool failed = false;
-    uint32_t evaluated = 0;  // (cell, crater) pairs this warp queued, for the pair counter
-    for (uint32_t c = 0; c < chunks; ++c) {
-        const uint32_t s = c & 1u;
-        if (!mbar_wait(&bars[s], phase[s], polls)) {
-            failed = true;
-        }
-        if (__syncthreads_or(failed)) {
-            // A copy did not land within `polls`: record it, then wait (bounded by the default
-            // limit) for the copies still in flight into this buffer and the other one (chunk
-            // c + 1 is issued by now), so no bulk copy is left writing into a finished CTA.
-            if (tid == 0) {
-                atomicOr(flags, 2u);
-                mbar_wait(&bars[s], phase[s]);
-                if (c + 1 < chunks) {
-                    mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
-                }
-            }
+    uint32_t evaluated = 0;
+    for (uint32_t c = 0; c < st.chunks; ++c) {
+        if (!st.wait(c, polls, flags)) {
             return;
         }
-        phase[s] ^= 1u;
+        const uint32_t s = c & 1u;
         const uint32_t n = min(kChunk, count - c * kChunk);
-        uint32_t queued = 0;       // warp-uniform
-        uint32_t heavyQueued = 0;  // warp-uniform
+        uint32_t queued = 0;  // warp-uniform
         for (uint32_t e = 0; e < n; ++e) {
             const BinEntry& entry = stage[s][e];
             const CraterRecord& r = entry.record;
-            if (boxTest) {
-                const float gx = fmaxf(
-                    fabsf(crater::split_difference(boxXh, boxXl, r.x, r.xLow)) - halfW, 0.0f);
-                const float gy = fmaxf(
-                    fabsf(crater::split_difference(boxYh, boxYl, r.y, r.yLow)) - halfH, 0.0f);
-                if (gx * gx + gy * gy >= entry.cull * entry.cull) {
-                    continue;  // warp-uniform
-                }
+            if (box_misses(box, r.x, r.xLow, r.y, r.yLow, entry.cull)) {
+                continue;  // warp-uniform
             }
-            const bool inTile = anyLive && tileX >= int(entry.tileX0) &&
-                                tileX <= int(entry.tileX1) && tileY >= int(entry.tileY0) &&
-                                tileY <= int(entry.tileY1);
-            if (!__any_sync(0xffffffffu, inTile)) {
-                continue;  // none of the warp's reference tiles is in the crater's window
-            }
-            const float dy = crater::split_difference(pyh, pyl, r.y, r.yLow);
-            const float cull2 = entry.cull * entry.cull;
-            uint32_t need = 0;
-#pragma unroll
-            for (int j = 0; j < kCellsPerThread; ++j) {
-                const float dx = crater::split_difference(pxh[j], pxl[j], r.x, r.xLow);
-                if (inTile && live[j] && dx * dx + dy * dy < cull2) {
-                    need |= 1u << j;
-                }
-            }
+            const bool inTile = w.anyLive && w.tileX >= int(entry.tileX0) &&
+                                w.tileX <= int(entry.tileX1) && w.tileY >= int(entry.tileY0) &&
+                                w.tileY <= int(entry.tileY1);
+            const uint32_t need = need_mask(w, inTile, r.x, r.xLow, r.y, r.yLow, entry.cull);
             if (!__any_sync(0xffffffffu, need != 0u)) {
                 continue;
             }
-            const uint32_t mine = __popc(need);
-            // Exclusive prefix of the lanes' counts.
-            uint32_t before = mine;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, before, d);
-                if (lane >= uint32_t(d)) {
-                    before += v;
-                }
-            }
-            const uint32_t total = __shfl_sync(0xffffffffu, before, 31);
-            if (total == 0u) {
-                continue;
-            }
-            before -= mine;
-            const bool heavy = kFast && (entry.index & kHeavyEntry) != 0u;  // warp-uniform
-            uint16_t* q = heavy ? heavyQueue : queue;
-            uint32_t& length = heavy ? heavyQueued : queued;
-            uint32_t slot = length + before;
-            for (int j = 0; j < kCellsPerThread; ++j) {
-                if (need & (1u << j)) {
-                    q[slot++] = uint16_t((e << 7) | (cell0 + j));
-                }
-            }
-            evaluated += mine;
-            length += total;
+            evaluated += __popc(need);
+            queued += enqueue(queue, queued, need, e, w.cell0, lane);
             __syncwarp();
-            while (length >= 32u) {
-                length -= 32u;
-                drain(stage[s], q, length, 32u, heavy);
+            while (queued >= 32u) {
+                queued -= 32u;
+                drain(stage[s], queued, 32u);
                 __syncwarp();
             }
         }
         if (queued > 0u) {
-            drain(stage[s], queue, 0u, queued, false);
+            drain(stage[s], 0u, queued);
             __syncwarp();
         }
-        if (kFast && heavyQueued > 0u) {
-            drain(stage[s], heavyQueue, 0u, heavyQueued, true);
-            __syncwarp();
-        }
-        if (c + 2 < chunks) {
-            // The buffer is read by every warp before it is refilled.
-            __syncthreads();
-            if (tid == 0) {
-                issue(c + 2);
-            }
-        }
+        st.refill(c);
     }
-    // One atomic per warp: the pairs this CTA evaluated, into the 64-bit counter after the flags.
     const uint32_t warpPairs = __reduce_add_sync(0xffffffffu, evaluated);
     if (lane == 0 && warpPairs > 0) {
         atomicAdd(reinterpret_cast<unsigned long long*>(flags + 1), (unsigned long long)warpPairs);
     }
     __syncwarp();
-    if (!rowIn) {
+    write_cells(grid, w, acc, heights);
+}
+
+// One lean crater in a bin: its LeanCrater, the reference-tile range its window touches, its
+// cull radius, and its index (kHeavyEntry when the extras pass has work on it). 208 bytes.
+struct LeanEntry {
+    crater::LeanCrater lean;
+    uint16_t tileX0, tileX1, tileY0, tileY1;
+    float cull;
+    uint32_t index;
+};
+static_assert(sizeof(LeanEntry) == 208, "LeanEntry must be a multiple of 16 bytes");
+constexpr uint32_t kLeanChunk = 64;  // 13 KB a buffer
+
+// Each crater's LeanCrater (crater_math.cuh), made once before the scatter copies it to its bins.
+__global__ void crater_lean_kernel(const CraterShapeKernel k,
+                                   const CraterRecord* __restrict__ records, uint32_t n,
+                                   const float* __restrict__ data,
+                                   crater::LeanCrater* __restrict__ leans) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        leans[i] = crater::lean_crater(k, records[i], data, i);
+    }
+}
+
+// The lean binned kernel (plain kernel options): each pair through `lean_contribution`, heavy
+// entries left to the extras pass. Three CTAs of 256 threads per SM.
+__global__ void __launch_bounds__(kShapeThreads, 3)
+    crater_lean_shape_kernel(const CraterShapeKernel k, const Grid grid, const NoData nodata,
+                             const CraterBins bins, float* __restrict__ heights,
+                             uint32_t* __restrict__ flags, const uint32_t polls) {
+    __shared__ __align__(128) LeanEntry stage[2][kLeanChunk];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ long long accs[kShapeThreads / 32][128];
+    __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
+    __shared__ float2 columns[kShapeThreads / 32][32];
+    __shared__ float2 rows[kShapeThreads / 32][4];
+
+    const uint32_t bin = bins.firstBin + blockIdx.x;
+    const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
+    const uint32_t first = bins.counts[bin];
+    const uint32_t count = bins.counts[bin + 1] - first;
+    if (count == 0u) {
         return;
     }
-    float out[kCellsPerThread];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    Stager<LeanEntry, kLeanChunk> st{stage, bars,
+                                     reinterpret_cast<const LeanEntry*>(bins.entries) + first,
+                                     count, (count + kLeanChunk - 1) / kLeanChunk, {0u, 0u}};
+    if (tid == 0) {
+        st.start();
+    }
+    const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
+    const WarpBox box = warp_box(grid, binX, binY, warp);
+    long long* acc = accs[warp];
+    uint16_t* queue = queues[warp];
 #pragma unroll
     for (int j = 0; j < kCellsPerThread; ++j) {
-        out[j] = float(acc[cell0 + j]);
+        acc[w.cell0 + j] = 0;
+        if (lane < 8u) {
+            columns[warp][(lane % 8u) * kCellsPerThread + j] = make_float2(w.pxh[j], w.pxl[j]);
+        }
     }
-    float* dst = heights + size_t(row) * grid.width + col0;
-    const bool vec = (grid.width % 4u == 0u) && col0 + 3 < grid.width &&
-                     ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0u) && live[0] && live[1] &&
-                     live[2] && live[3];
-    if (vec) {
-        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
-    } else {
+    if (lane % 8u == 0u) {
+        rows[warp][lane / 8u] = make_float2(w.pyh, w.pyl);
+    }
+    const crater::LeanKernel lk = crater::lean_kernel(k);
+    __syncthreads();
+
+    auto drain = [&](const LeanEntry* chunk, uint32_t from, uint32_t n) {
+        if (lane < n) {
+            const uint32_t code = queue[from + lane];
+            const crater::LeanCrater& l = chunk[code >> 7].lean;
+            const uint32_t cell = code & 127u;
+            const float2 cx = columns[warp][cell & 31u];
+            const float2 cy = rows[warp][cell >> 5];
+            const float dy = crater::split_difference(cy.x, cy.y, l.y, l.yLow);
+            const float dx = crater::split_difference(cx.x, cx.y, l.x, l.xLow);
+            bool reached;
+            const float v = crater::lean_contribution(k, lk, l, dx, dy, reached);
+            if (reached) {
+                add_fixed(acc + cell, to_fixed(v));
+            }
+        }
+    };
+
+    uint32_t evaluated = 0;
+    for (uint32_t c = 0; c < st.chunks; ++c) {
+        if (!st.wait(c, polls, flags)) {
+            return;
+        }
+        const uint32_t s = c & 1u;
+        const uint32_t n = min(kLeanChunk, count - c * kLeanChunk);
+        uint32_t queued = 0;  // warp-uniform
+        for (uint32_t e = 0; e < n; ++e) {
+            const LeanEntry& entry = stage[s][e];
+            const crater::LeanCrater& l = entry.lean;
+            // Heavy craters are the extras pass's. A lean crater is never stretched, so every
+            // cell within its cull radius lies inside its footprint window: no tile test.
+            if ((l.flags & crater::kLeanHeavy) ||
+                box_misses(box, l.x, l.xLow, l.y, l.yLow, entry.cull)) {
+                continue;  // warp-uniform
+            }
+            const uint32_t need = need_mask(w, true, l.x, l.xLow, l.y, l.yLow, entry.cull);
+            if (!__any_sync(0xffffffffu, need != 0u)) {
+                continue;
+            }
+            evaluated += __popc(need);
+            queued += enqueue(queue, queued, need, e, w.cell0, lane);
+            __syncwarp();
+            while (queued >= 32u) {
+                queued -= 32u;
+                drain(stage[s], queued, 32u);
+                __syncwarp();
+            }
+        }
+        if (queued > 0u) {
+            drain(stage[s], 0u, queued);
+            __syncwarp();
+        }
+        st.refill(c);
+    }
+    const uint32_t warpPairs = __reduce_add_sync(0xffffffffu, evaluated);
+    if (lane == 0 && warpPairs > 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(flags + 1), (unsigned long long)warpPairs);
+    }
+    __syncwarp();
+    write_cells(grid, w, acc, heights);
+}
+
+// The extras pass after the lean kernel, over the same bins: heavy craters (tables, marks,
+// terraces, shifts, upslopes, long outlines) through the general contribution, and the massif
+// peaks' difference from the round dome the lean pass gave their craters. Rare work: each thread
+// evaluates its own 4 cells against each such entry of its bin, read from global memory, and adds
+// the fixed-point sum to the heights the lean pass wrote.
+__global__ void __launch_bounds__(kShapeThreads)
+    crater_extras_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
+                         const float* __restrict__ data, const Grid grid, const NoData nodata,
+                         const CraterBins bins, float* __restrict__ heights) {
+    const uint32_t bin = bins.firstBin + blockIdx.x;
+    const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
+    const uint32_t first = bins.counts[bin];
+    const uint32_t count = bins.counts[bin + 1] - first;
+    const LeanEntry* entries = reinterpret_cast<const LeanEntry*>(bins.entries) + first;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    // The bin's entries with extras work, found by all threads at once (most bins have none).
+    constexpr uint32_t kList = 256;
+    __shared__ uint32_t list[kList];
+    __shared__ uint32_t listed;
+    if (threadIdx.x == 0) {
+        listed = 0;
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < count; e += blockDim.x) {
+        if (__ldg(&entries[e].index) & kHeavyEntry) {
+            const uint32_t slot = atomicAdd(&listed, 1u);
+            if (slot < kList) {
+                list[slot] = e;
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t found = listed;
+    if (found == 0u) {
+        return;
+    }
+    // Past the list's room every entry is looked at in turn (the fixed-point sum does not depend
+    // on the order).
+    const bool all = found > kList;
+    const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
+    long long sum[kCellsPerThread] = {0, 0, 0, 0};
+    for (uint32_t q = 0; q < (all ? count : found); ++q) {
+        const uint32_t e = all ? q : list[q];
+        const uint32_t index = __ldg(&entries[e].index);
+        if ((index & kHeavyEntry) == 0u) {
+            continue;  // block-uniform
+        }
+        const crater::LeanCrater& l = entries[e].lean;
+        const uint32_t flags = __ldg(&l.flags);
+        const CraterRecord& r = records[index & ~kHeavyEntry];
+        float cull = __ldg(&entries[e].cull);
+        bool inTile = true;
+        if (flags & crater::kLeanHeavy) {
+            inTile = w.anyLive && w.tileX >= int(__ldg(&entries[e].tileX0)) &&
+                     w.tileX <= int(__ldg(&entries[e].tileX1)) &&
+                     w.tileY >= int(__ldg(&entries[e].tileY0)) &&
+                     w.tileY <= int(__ldg(&entries[e].tileY1));
+        } else {
+            cull = sqrtf(__ldg(&l.peakReach2)) * (1.0f + 1e-5f) + 1e-6f;
+        }
+        const uint32_t need = need_mask(w, inTile, r.x, r.xLow, r.y, r.yLow, cull);
+        if (need == 0u) {
+            continue;
+        }
+        const float dy = crater::split_difference(w.pyh, w.pyl, r.y, r.yLow);
 #pragma unroll
         for (int j = 0; j < kCellsPerThread; ++j) {
-            if (live[j]) {
-                dst[j] = out[j];
+            if (need & (1u << j)) {
+                const float dx = crater::split_difference(w.pxh[j], w.pxl[j], r.x, r.xLow);
+                bool reached;
+                const float v = crater::extra_contribution(k, data, r, flags, dx, dy, reached);
+                if (reached) {
+                    sum[j] += to_fixed(v);
+                }
             }
+        }
+    }
+    if (!w.rowIn) {
+        return;
+    }
+    float* dst = heights + size_t(w.row) * grid.width + w.col0;
+#pragma unroll
+    for (int j = 0; j < kCellsPerThread; ++j) {
+        if (w.live[j] && sum[j] != 0) {
+            dst[j] = float(double(w.base[j]) + double(sum[j]) * kFixedUnit);
         }
     }
 }
@@ -642,14 +921,27 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
 
 cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
                                   uint32_t n, const Grid& grid, const CraterBins& bins,
-                                  cudaStream_t stream) {
+                                  const void* leans, cudaStream_t stream) {
     (void)grid;
     if (n == 0) {
         return cudaSuccess;
     }
     const uint32_t threads = 256;  // 8 warps of 32 craters
     const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
-    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(k, records, n, bins);
+    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(k, records, n,
+                                                          static_cast<const int4*>(leans), bins);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crater_lean(const CraterShapeKernel& k, const CraterRecord* records, uint32_t n,
+                               const float* data, void* leans, cudaStream_t stream) {
+    static_assert(sizeof(crater::LeanCrater) == kLeanCraterBytes, "lean crater size");
+    static_assert(sizeof(LeanEntry) == kLeanEntryBytes, "lean entry size");
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    crater_lean_kernel<<<(n + 127) / 128, 128, 0, stream>>>(
+        k, records, n, data, static_cast<crater::LeanCrater*>(leans));
     return cudaGetLastError();
 }
 
@@ -675,8 +967,8 @@ bool crater_lean_entries(const CraterShapeKernel& k) {
     return crater_options_plain(k);
 }
 
-cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
-                                const float* harmonics, bool fast, const Grid& grid,
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* records,
+                                const float* data, bool lean, bool extras, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
                                 cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows,
                                 uint32_t polls) {
@@ -690,12 +982,20 @@ cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
     }
     CraterBins strip = bins;
     strip.firstBin = firstBinRow * bins.binsX;
-    if (fast) {
-        crater_shape_kernel<true><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1, polls);
+    if (lean) {
+        crater_lean_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(
+            k, grid, nodata, strip, heights, bins.total + 1, polls);
+        if (extras) {
+            const cudaError_t err = cudaGetLastError();
+            if (err != cudaSuccess) {
+                return err;
+            }
+            crater_extras_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, records, data, grid,
+                                                                    nodata, strip, heights);
+        }
     } else {
-        crater_shape_kernel<false><<<nbins, kShapeThreads, 0, stream>>>(
-            k, data, harmonics, grid, nodata, strip, heights, bins.total + 1, polls);
+        crater_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, data, grid, nodata, strip,
+                                                                 heights, bins.total + 1, polls);
     }
     return cudaGetLastError();
 }

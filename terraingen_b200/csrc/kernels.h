@@ -89,11 +89,18 @@ struct CraterBins {
 cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
                                 uint32_t n, const float* data, const double* footprints,
                                 const Grid& grid, const CraterBins& bins, cudaStream_t stream);
-// Scatters each crater's BinEntry into its bins; an entry whose crater needs the general shaping
-// path (crater_entry_heavy) carries kHeavyEntry in its `index`.
+// The plain path's lean craters (crater_math.cuh LeanCrater): kLeanCraterBytes per crater, made
+// by launch_crater_lean; with them the bins hold kLeanEntryBytes entries, else 160-byte BinEntry.
+constexpr size_t kLeanCraterBytes = 192;
+constexpr size_t kLeanEntryBytes = 208;
+cudaError_t launch_crater_lean(const CraterShapeKernel& k, const CraterRecord* records, uint32_t n,
+                               const float* data, void* leans, cudaStream_t stream);
+// Scatters each crater's entry into its bins (a LeanEntry from `leans` when given, else a
+// BinEntry); an entry whose crater has work for the extras pass (crater_needs_extras) carries
+// kHeavyEntry in its `index`.
 cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
                                   uint32_t n, const Grid& grid, const CraterBins& bins,
-                                  cudaStream_t stream);
+                                  const void* leans, cudaStream_t stream);
 constexpr uint32_t kHeavyEntry = 0x80000000u;
 // Whether a batch takes the lean shaping path (crater_math.cuh `fast_contribution`): the
 // kernel's options allow it and the count pass saw no record feature beyond outlines
@@ -110,8 +117,11 @@ cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, con
 // Polls of a staged copy before a binned kernel gives up on it (flag 2, TG_ERROR_TIMEOUT).
 constexpr uint32_t kWaitPolls = 1u << 26;
 
-cudaError_t launch_crater_shape(const CraterShapeKernel& k, const float* data,
-                                const float* harmonics, bool fast, const Grid& grid,
+// Shapes the bins of rows [firstBinRow, firstBinRow + binRows): with `lean` (LeanEntry bins) the
+// lean kernel, then, when `extras`, the extras pass over the same bins; otherwise the general
+// kernel on BinEntry bins.
+cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* records,
+                                const float* data, bool lean, bool extras, const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
                                 cudaStream_t stream, uint32_t firstBinRow = 0,
                                 uint32_t binRows = 0xffffffffu, uint32_t polls = kWaitPolls);

@@ -183,6 +183,67 @@ def terrain4097(side: int = 4097, pixel: float = 0.5, cx: float = 0.0, cy: float
                     0.0, kernel, records, data, footprints, boulders, pixel)
 
 
+class TerrainPrep:
+    """The host work the synthetic terrain's layers do before any shaping, for one grid: the
+    crater layer's population, apply order and kernel records (tg_crater_batch) and the boulder
+    layer's placement (tg_boulder_generate), written into buffers made once (`alloc`, e.g. a
+    pinned allocator) and reused by every `run`. The reference's CraterLayer and BoulderLayer
+    redo this work on every Terrain::Evaluate."""
+
+    def __init__(self, grid: GridSpec, seed: int = 7, alloc=np.empty, margin: float = 1.25):
+        full_area = (4097 * 0.5) ** 2
+        self.grid = grid
+        self.population = crater_population(
+            seed, 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0)), 1.0, 500.0)
+        self.shaping = config2_shaping()
+        self.stones = boulder_population(seed, 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5)))
+        half = 0.5 * grid.pixel
+        self.region = np.array([grid.x0 - half, grid.y0 - grid.height * grid.pixel - half,
+                                grid.x0 + grid.width * grid.pixel + half, grid.y0 + half],
+                               np.float64)
+        self._grid = grid.native()
+        lib = N.library()
+        nr, nd, nb = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        N.check(lib.tg_crater_batch(C.byref(self.population), C.byref(self.shaping),
+                                    C.byref(self._grid), None, None, 0, None, 0, None,
+                                    C.byref(nr), C.byref(nd)))
+        N.check(lib.tg_boulder_generate(C.byref(self.stones), self.region.ctypes.data,
+                                        grid.pixel, None, 0, C.byref(nb)))
+        self.record_capacity = int(nr.value * margin) + 64
+        self.data_capacity = int(nd.value * margin) + 64
+        self.boulder_capacity = int(nb.value * margin) + 64
+        self.kernel = np.zeros((), CRATER_SHAPE_KERNEL)
+        self.records = alloc(self.record_capacity * CRATER_RECORD.itemsize, np.uint8)
+        self.data = alloc(self.data_capacity, np.float32)
+        self.footprints = alloc(3 * self.record_capacity, np.float64)
+        self.boulders = alloc(5 * self.boulder_capacity, np.float64)
+        self.counts = (0, 0, 0)
+
+    def input_bytes(self) -> int:
+        nr, nd, nb = self.counts
+        return nr * (CRATER_RECORD.itemsize + 24) + nd * 4 + nb * 40
+
+    def run(self):
+        """Builds this grid's crater batch and boulders; returns (kernel, records, data,
+        footprints, boulders) as views of the buffers."""
+        lib = N.library()
+        nr, nd, nb = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        N.check(lib.tg_crater_batch(C.byref(self.population), C.byref(self.shaping),
+                                    C.byref(self._grid), self.kernel.ctypes.data,
+                                    self.records.ctypes.data, self.record_capacity,
+                                    self.data.ctypes.data, self.data_capacity,
+                                    self.footprints.ctypes.data, C.byref(nr), C.byref(nd)))
+        N.check(lib.tg_boulder_generate(C.byref(self.stones), self.region.ctypes.data,
+                                        self.grid.pixel, self.boulders.ctypes.data,
+                                        self.boulder_capacity, C.byref(nb)))
+        if nb.value > self.boulder_capacity:
+            raise RuntimeError("boulder buffer too small")
+        self.counts = (nr.value, nd.value, nb.value)
+        records = self.records[:nr.value * CRATER_RECORD.itemsize].view(CRATER_RECORD)
+        return (self.kernel, records, self.data[:nd.value], self.footprints[:3 * nr.value],
+                self.boulders[:5 * nb.value].reshape(-1, 5))
+
+
 def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
     """The same terrain as the reference CPU path builds it (oracle harness scene fields)."""
     full_area = (4097 * pixel) ** 2
