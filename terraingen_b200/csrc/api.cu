@@ -523,8 +523,8 @@ namespace {
 // launches need. `any` is false when no cell needs a crater.
 struct CraterPrep {
     CraterBins bins{};
-    bool lean = false;    // lean kernel on LeanEntry bins (plain kernel options)
-    bool extras = false;  // some crater has work for the extras pass
+    const void* leans = nullptr;  // the lean craters (plain kernel options), else null
+    bool extras = false;          // some crater needs the extras pass
     bool any = false;
 };
 
@@ -572,20 +572,20 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     if (total == 0) {
         return TG_OK;
     }
-    p.lean = crater_lean_entries(k);
+    const bool lean = crater_lean_entries(k);
     p.extras = (d->pinnedStatus[1] & 4u) != 0u;
     TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) *
-                                          (p.lean ? kLeanEntryBytes : sizeof(BinEntry))),
+                                          (lean ? kLeanEntryBytes : sizeof(BinEntry))),
             "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
     bins.capacity = total;
-    void* leans = nullptr;
-    if (p.lean) {
+    if (lean) {
         TG_CUDA(d->slots[kHarmonics].reserve(size_t(n) * kLeanCraterBytes), "allocation");
-        leans = d->slots[kHarmonics].ptr;
-        TG_CUDA(launch_crater_lean(k, rec, n, data, leans, s), "lean crater launch");
+        p.leans = d->slots[kHarmonics].ptr;
+        TG_CUDA(launch_crater_lean(k, rec, n, data, bins, d->slots[kHarmonics].ptr, s),
+                "lean crater launch");
     }
-    TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, leans, s), "crater scatter launch");
+    TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, p.leans, s), "crater scatter launch");
     p.any = true;
     return TG_OK;
 }
@@ -617,7 +617,7 @@ int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(launch_crater_shape(k, rec, data, p.lean, p.extras, g, to_nodata(nodata), p.bins, dh,
+    TG_CUDA(launch_crater_shape(k, rec, data, p.leans, p.extras, g, to_nodata(nodata), p.bins, dh,
                                 s, 0, 0xffffffffu, d->waitPolls),
             "crater shape launch");
     return crater_finish(d, p, s);
@@ -1152,7 +1152,7 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
             if (cp.any) {
                 if (cudaError_t e = launch_crater_shape(
                         k, static_cast<const CraterRecord*>(drec),
-                        static_cast<const float*>(ddata), cp.lean, cp.extras, g, none, cp.bins,
+                        static_cast<const float*>(ddata), cp.leans, cp.extras, g, none, cp.bins,
                         dh, s, k0, rows, d->waitPolls)) {
                     return drain(cuda_fail(e, "crater shape launch"));
                 }

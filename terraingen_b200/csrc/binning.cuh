@@ -186,15 +186,15 @@ __device__ __forceinline__ bool crater_heavy(const CraterRecord& r) {
            r.hasDatum == 1u;
 }
 
-// Whether the plain binned kernel's extras pass has work on crater `r` (crater_math.cuh
+// Whether the plain binned kernel's extras pass shapes crater `r` (crater_math.cuh
 // `lean_crater`): a record the lean path cannot shape (tables, marks, terraces, a floor shift, an
-// upslope, a datum, more than 11 outline harmonics), or a complex crater's massif peak.
+// upslope, a datum, more than 11 outline harmonics).
 __device__ __forceinline__ bool crater_needs_extras(const CraterShapeKernel& k,
                                                     const CraterRecord& r) {
+    (void)k;
     return r.tableCount > 0u || r.markCount > 0u || r.terraceCount > 0u || r.shiftX != 0.0f ||
            r.shiftY != 0.0f || r.upslopeX != 0.0f || r.upslopeY != 0.0f || r.hasDatum == 1u ||
-           r.harmonicCount > 11u || r.firstHarmonic > 255u ||
-           (crater_is_complex(k, r) && r.peakCount > 0u);
+           r.harmonicCount > 11u || r.firstHarmonic > 255u;
 }
 
 // The pixel window of a box on the grid (PixelWindowIn, src/raster/cell_loops.cpp:21-28).

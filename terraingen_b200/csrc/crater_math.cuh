@@ -1023,10 +1023,10 @@ __device__ __forceinline__ float fast_contribution(const FastKernel& k,
 // the heading, ...), so it has the same bits. Per pair the outline's harmonics are summed by
 // Horner's rule in the complex plane, sum_k (A_k + i B_k) (q e^{i theta})^k with q the square root
 // of the kept share, which is the reference's sum of A_k cos(k theta + phase) share^(k/2) within
-// a few float roundings. A crater with massif peaks is shaped here with its round dome; the
-// massifs' difference from the dome is added by the extras pass, as is every crater the lean path
-// cannot shape (flag kLeanHeavy: tables, marks, terraces, floor shifts, upslopes, datums, more
-// harmonics).
+// a few float roundings. A crater with massif peaks is shaped here with its round dome, and the
+// extras pass adds the massifs' difference from the dome in the bins the peak reaches; it also
+// shapes the craters the lean path cannot (flag kLeanHeavy: tables, marks, terraces, floor
+// shifts, upslopes, datums, more harmonics).
 constexpr uint32_t kLeanHarmonics = 11;
 constexpr uint32_t kLeanComplex = 2u;       // profile kind: 0 FT, 1 MPD, 2 complex
 constexpr uint32_t kLeanOutline = 1u << 2;  // ellipse or harmonics
@@ -1045,14 +1045,23 @@ struct LeanCrater {
     float peakReach2;      // squared reach of its massif peak (kLeanMassifs)
     float ellipticity;
     float2 harmonics[kLeanHarmonics];  // (A cos phase, A sin phase)
-    float pad[2];
+    uint16_t tileX0, tileX1, tileY0, tileY1;  // the reference tiles its footprint window touches
+    float cull;            // no cell beyond this distance (m) can be within its reach
+    uint32_t pad[3];
 };
-static_assert(sizeof(LeanCrater) == 192, "LeanCrater must be a multiple of 16 bytes");
+static_assert(sizeof(LeanCrater) == 208, "LeanCrater must be a multiple of 16 bytes");
 
-// The lean form of record `c` under kernel `k` (harmonics from `data`).
+// The lean form of record `c` under kernel `k` (harmonics from `data`), with its footprint's
+// reference-tile box (x0, x1, y0, y1) and cull distance from the binning's count pass.
 __device__ inline LeanCrater lean_crater(const CraterShapeKernel& k, const CraterRecord& c,
-                                         const float* __restrict__ data, uint32_t index) {
+                                         const float* __restrict__ data, uint32_t index,
+                                         int4 tiles, float cull) {
     LeanCrater l{};
+    l.tileX0 = uint16_t(tiles.x);
+    l.tileX1 = uint16_t(tiles.y);
+    l.tileY0 = uint16_t(tiles.z);
+    l.tileY1 = uint16_t(tiles.w);
+    l.cull = cull;
     l.x = c.x;
     l.xLow = c.xLow;
     l.y = c.y;
@@ -1129,10 +1138,12 @@ __device__ __forceinline__ LeanKernel lean_kernel(const CraterShapeKernel& k) {
 }
 
 // What lean crater `l` adds at (dx, dy) from its center (resolution times the shaped relief, the
-// round dome in place of massifs); `reached` is false beyond its reach.
+// round dome in place of massifs); `reached` is false beyond its reach. `shaped` receives the
+// profile distance (after the outline), which the massif peak reads.
 __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
                                                    const LeanKernel& lk, const LeanCrater& l,
-                                                   float dx, float dy, bool& reached) {
+                                                   float dx, float dy, bool& reached,
+                                                   float& shaped) {
     const uint32_t flags = l.flags;
     const float d2 = dx * dx + dy * dy;
     float distance = sqrtf(d2);
@@ -1176,6 +1187,7 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
         }
         distance /= scale;
     }
+    shaped = distance;
     reached = distance < l.reach;
     if (!reached) {
         return 0.0f;
@@ -1213,9 +1225,10 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
     return l.resolution * height;
 }
 
-// The extras of crater `c` at (dx, dy): with kLeanHeavy its whole contribution (the general
-// path); otherwise the massif peak's difference from the round dome the lean path gave it
-// (KernelPeakRelief, craters.h:1161), 0 beyond the peak's reach.
+// The extras pass's contribution of crater `c` at (dx, dy): with kLeanHeavy its whole
+// contribution (the general path); otherwise its massif peak's difference from the round dome
+// the lean path gave it (KernelPeakRelief, craters.h:1161), times its resolution weight, 0 beyond
+// the peak's reach.
 static __device__ __noinline__ float extra_contribution(const CraterShapeKernel& k,
                                                         const float* data, const CraterRecord& c,
                                                         uint32_t flags, float dx, float dy,

@@ -58,7 +58,7 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
                 atomicOr(flags, 1u);
             }
             // Work for the extras pass after the lean kernel (heavy records, massif peaks).
-            if (crater_needs_extras(k, r)) {
+            if (crater_needs_extras(k, r) || (crater_is_complex(k, r) && r.peakCount > 0u)) {
                 atomicOr(flags, 4u);
             }
         }
@@ -87,11 +87,28 @@ __global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecor
 // Each warp takes 32 craters and spreads all of their (crater, bin) pairs over its lanes: a
 // lane finds its pair's crater by a search of the warp's running bin counts, then copies the
 // crater's record and tail into its bin's next slot.
-// With `leans` the entries are LeanEntry (the crater's LeanCrater and the tail), else BinEntry
-// (its record and the tail).
+// Whether a disk of `radius` m around (x, y) meets the cell centers of bin (bx, by) of an
+// axis-aligned grid, with a cell to spare (rotated grids: always).
+__device__ inline bool peak_meets_bin(const Grid& g, double x, double y, double radius,
+                                      uint32_t bx, uint32_t by) {
+    if (g.rowRotation != 0.0 || g.colRotation != 0.0) {
+        return true;
+    }
+    const double xa = g.originX + double(bx * kBinCells) * g.pixelWidth;
+    const double xb = xa + double(kBinCells) * g.pixelWidth;
+    const double ya = g.originY + double(by * kBinCells) * g.pixelHeight;
+    const double yb = ya + double(kBinCells) * g.pixelHeight;
+    const double box[4] = {fmin(xa, xb), fmin(ya, yb), fmax(xa, xb), fmax(ya, yb)};
+    const double spare = fabs(g.pixelWidth) + fabs(g.pixelHeight);
+    return disk_meets_box(x, y, radius + spare, box);
+}
+
+// With `leans` the entries are crater indices (kHeavyEntry set where the extras pass has work),
+// else BinEntry copies (the record and the tail).
 __global__ void crater_scatter_kernel(const CraterShapeKernel k,
                                       const CraterRecord* __restrict__ records, uint32_t n,
-                                      const int4* __restrict__ leans, CraterBins bins) {
+                                      const int4* __restrict__ leans, const Grid grid,
+                                      CraterBins bins) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
     if (base >= n) {
@@ -151,9 +168,32 @@ __global__ void crater_scatter_kernel(const CraterShapeKernel k,
                 slot = 0xffffffffu;  // the host sized the entries from the counts; never taken
             }
         }
-        // Each lane writes its entry's 16-byte tail; the bodies (the crater's LeanCrater or
-        // record) are copied one entry at a time by the whole warp, 16 contiguous bytes a lane.
-        const uint32_t words = leans != nullptr ? 13u : 10u;
+        if (leans != nullptr) {
+            // Index bins: the shaping kernel gathers the crater's LeanCrater itself. The extras
+            // pass looks at a heavy crater in all its bins and at a massif peak in the bins the
+            // peak's reach meets.
+            if (slot != 0xffffffffu) {
+                const CraterRecord& r = records[crater];
+                bool extras = crater_needs_extras(k, r);
+                if (!extras && crater_is_complex(k, r) && r.peakCount > 0u) {
+                    const crater::LeanCrater* l =
+                        reinterpret_cast<const crater::LeanCrater*>(leans) + crater;
+                    const uint32_t local = q - before;
+                    const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin;
+                    const uint32_t wide = uint32_t(t.y) / kTilesPerBin - bx0 + 1u;
+                    const uint32_t bx = bx0 + local % wide;
+                    const uint32_t by = uint32_t(t.z) / kTilesPerBin + local / wide;
+                    extras = peak_meets_bin(grid, double(r.x) + double(r.xLow),
+                                            double(r.y) + double(r.yLow),
+                                            sqrt(double(__ldg(&l->peakReach2))), bx, by);
+                }
+                reinterpret_cast<uint32_t*>(bins.entries)[slot] = crater | (extras ? kHeavyEntry : 0u);
+            }
+            continue;
+        }
+        // Each lane writes its entry's 16-byte tail; the records are copied one entry at a time
+        // by the whole warp, 16 contiguous bytes a lane.
+        const uint32_t words = 10u;
         int4* entries = reinterpret_cast<int4*>(bins.entries);
         if (slot != 0xffffffffu) {
             const uint32_t extras = crater_needs_extras(k, records[crater]) ? kHeavyEntry : 0u;
@@ -162,7 +202,7 @@ __global__ void crater_scatter_kernel(const CraterShapeKernel k,
                           int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
                           int(crater | extras));
         }
-        const int4* bodies = leans != nullptr ? leans : reinterpret_cast<const int4*>(records);
+        const int4* bodies = reinterpret_cast<const int4*>(records);
         for (uint32_t from = 0; from < 32u; ++from) {
             const uint32_t s = __shfl_sync(0xffffffffu, slot, int(from));
             const uint32_t src = __shfl_sync(0xffffffffu, crater, int(from));
@@ -521,35 +561,97 @@ __global__ void __launch_bounds__(kShapeThreads)
     write_cells(grid, w, acc, heights);
 }
 
-// One lean crater in a bin: its LeanCrater, the reference-tile range its window touches, its
-// cull radius, and its index (kHeavyEntry when the extras pass has work on it). 208 bytes.
-struct LeanEntry {
-    crater::LeanCrater lean;
-    uint16_t tileX0, tileX1, tileY0, tileY1;
-    float cull;
-    uint32_t index;
-};
-static_assert(sizeof(LeanEntry) == 208, "LeanEntry must be a multiple of 16 bytes");
-constexpr uint32_t kLeanChunk = 64;  // 13 KB a buffer
-
-// Each crater's LeanCrater (crater_math.cuh), made once before the scatter copies it to its bins.
+// Each crater's LeanCrater (crater_math.cuh), made once after the count pass.
 __global__ void crater_lean_kernel(const CraterShapeKernel k,
                                    const CraterRecord* __restrict__ records, uint32_t n,
-                                   const float* __restrict__ data,
+                                   const float* __restrict__ data, const CraterBins bins,
                                    crater::LeanCrater* __restrict__ leans) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        leans[i] = crater::lean_crater(k, records[i], data, i);
+        leans[i] = crater::lean_crater(k, records[i], data, i, bins.boxes[i], bins.culls[i]);
     }
 }
 
-// The lean binned kernel (plain kernel options): each pair through `lean_contribution`, heavy
-// entries left to the extras pass. Three CTAs of 256 threads per SM.
+constexpr uint32_t kLeanChunk = 64;  // 13 KB a buffer
+
+// The lean kernel's staging: a bin holds crater indices, and warp 0 gathers each chunk's
+// LeanCraters into a shared buffer with one 208-byte TMA bulk copy per entry, all completing on
+// the buffer's mbarrier (lane 0 arrives with the chunk's byte count before any copy is issued).
+// Waits give up after `polls`, record flag 2 and drain the copies in flight, as Stager's do.
+struct LeanStager {
+    crater::LeanCrater (*stage)[kLeanChunk];
+    uint64_t* bars;
+    const uint32_t* indices;
+    const crater::LeanCrater* leans;
+    uint32_t count, chunks, phase[2];
+
+    // Warp 0 only.
+    __device__ void issue(uint32_t c, uint32_t lane) {
+        const uint32_t s = c & 1u;
+        const uint32_t n = min(kLeanChunk, count - c * kLeanChunk);
+        if (lane == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bars[s], n * uint32_t(sizeof(crater::LeanCrater)));
+        }
+        __syncwarp();
+        for (uint32_t e = lane; e < n; e += 32u) {
+            const uint32_t index = __ldg(indices + c * kLeanChunk + e) & ~kHeavyEntry;
+            bulk_copy_g2s(&stage[s][e], leans + index, uint32_t(sizeof(crater::LeanCrater)),
+                          &bars[s]);
+        }
+    }
+
+    // Warp 0 only: inits the barriers and starts the first two chunks.
+    __device__ void start(uint32_t lane) {
+        if (lane == 0) {
+            mbar_init(&bars[0], 1);
+            mbar_init(&bars[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+        issue(0, lane);
+        if (chunks > 1) {
+            issue(1, lane);
+        }
+    }
+
+    __device__ bool wait(uint32_t c, uint32_t polls, uint32_t* flags) {
+        const uint32_t s = c & 1u;
+        const bool failed = !mbar_wait(&bars[s], phase[s], polls);
+        if (__syncthreads_or(failed)) {
+            if (threadIdx.x == 0) {
+                atomicOr(flags, 2u);
+                mbar_wait(&bars[s], phase[s]);
+                if (c + 1 < chunks) {
+                    mbar_wait(&bars[s ^ 1u], phase[s ^ 1u]);
+                }
+            }
+            return false;
+        }
+        phase[s] ^= 1u;
+        return true;
+    }
+
+    __device__ void refill(uint32_t c, uint32_t warp, uint32_t lane) {
+        if (c + 2 < chunks) {
+            __syncthreads();
+            if (warp == 0) {
+                issue(c + 2, lane);
+            }
+        }
+    }
+};
+
+// The lean binned kernel (plain kernel options): each pair through `lean_contribution`; heavy
+// craters and massif peaks are left to the extras pass. Three CTAs of 256 threads per SM.
 __global__ void __launch_bounds__(kShapeThreads, 3)
-    crater_lean_shape_kernel(const CraterShapeKernel k, const Grid grid, const NoData nodata,
-                             const CraterBins bins, float* __restrict__ heights,
-                             uint32_t* __restrict__ flags, const uint32_t polls) {
-    __shared__ __align__(128) LeanEntry stage[2][kLeanChunk];
+    crater_lean_shape_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
+                             const float* __restrict__ data,
+                             const crater::LeanCrater* __restrict__ leans, const Grid grid,
+                             const NoData nodata, const CraterBins bins,
+                             float* __restrict__ heights, uint32_t* __restrict__ flags,
+                             const uint32_t polls) {
+    __shared__ __align__(128) crater::LeanCrater stage[2][kLeanChunk];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ long long accs[kShapeThreads / 32][128];
     __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
@@ -564,11 +666,10 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
         return;
     }
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-    Stager<LeanEntry, kLeanChunk> st{stage, bars,
-                                     reinterpret_cast<const LeanEntry*>(bins.entries) + first,
-                                     count, (count + kLeanChunk - 1) / kLeanChunk, {0u, 0u}};
-    if (tid == 0) {
-        st.start();
+    LeanStager st{stage, bars, reinterpret_cast<const uint32_t*>(bins.entries) + first, leans,
+                  count, (count + kLeanChunk - 1) / kLeanChunk, {0u, 0u}};
+    if (warp == 0) {
+        st.start(lane);
     }
     const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
     const WarpBox box = warp_box(grid, binX, binY, warp);
@@ -587,17 +688,18 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
     const crater::LeanKernel lk = crater::lean_kernel(k);
     __syncthreads();
 
-    auto drain = [&](const LeanEntry* chunk, uint32_t from, uint32_t n) {
+    auto drain = [&](const crater::LeanCrater* chunk, uint32_t from, uint32_t n) {
         if (lane < n) {
             const uint32_t code = queue[from + lane];
-            const crater::LeanCrater& l = chunk[code >> 7].lean;
+            const crater::LeanCrater& l = chunk[code >> 7];
             const uint32_t cell = code & 127u;
             const float2 cx = columns[warp][cell & 31u];
             const float2 cy = rows[warp][cell >> 5];
             const float dy = crater::split_difference(cy.x, cy.y, l.y, l.yLow);
             const float dx = crater::split_difference(cx.x, cx.y, l.x, l.xLow);
             bool reached;
-            const float v = crater::lean_contribution(k, lk, l, dx, dy, reached);
+            float shaped;
+            const float v = crater::lean_contribution(k, lk, l, dx, dy, reached, shaped);
             if (reached) {
                 add_fixed(acc + cell, to_fixed(v));
             }
@@ -613,15 +715,13 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
         const uint32_t n = min(kLeanChunk, count - c * kLeanChunk);
         uint32_t queued = 0;  // warp-uniform
         for (uint32_t e = 0; e < n; ++e) {
-            const LeanEntry& entry = stage[s][e];
-            const crater::LeanCrater& l = entry.lean;
+            const crater::LeanCrater& l = stage[s][e];
             // Heavy craters are the extras pass's. A lean crater is never stretched, so every
             // cell within its cull radius lies inside its footprint window: no tile test.
-            if ((l.flags & crater::kLeanHeavy) ||
-                box_misses(box, l.x, l.xLow, l.y, l.yLow, entry.cull)) {
+            if ((l.flags & crater::kLeanHeavy) || box_misses(box, l.x, l.xLow, l.y, l.yLow, l.cull)) {
                 continue;  // warp-uniform
             }
-            const uint32_t need = need_mask(w, true, l.x, l.xLow, l.y, l.yLow, entry.cull);
+            const uint32_t need = need_mask(w, true, l.x, l.xLow, l.y, l.yLow, l.cull);
             if (!__any_sync(0xffffffffu, need != 0u)) {
                 continue;
             }
@@ -638,7 +738,7 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
             drain(stage[s], 0u, queued);
             __syncwarp();
         }
-        st.refill(c);
+        st.refill(c, warp, lane);
     }
     const uint32_t warpPairs = __reduce_add_sync(0xffffffffu, evaluated);
     if (lane == 0 && warpPairs > 0) {
@@ -650,20 +750,22 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
 
 // The extras pass after the lean kernel, over the same bins: heavy craters (tables, marks,
 // terraces, shifts, upslopes, long outlines) through the general contribution, and the massif
-// peaks' difference from the round dome the lean pass gave their craters. Rare work: each thread
-// evaluates its own 4 cells against each such entry of its bin, read from global memory, and adds
-// the fixed-point sum to the heights the lean pass wrote.
+// peaks' difference from the round dome the lean pass gave their craters, in the bins a peak
+// reaches. Rare work: each thread evaluates its own 4 cells against each such entry of its bin,
+// read from global memory, and adds the fixed-point sum to the heights the lean pass wrote.
 __global__ void __launch_bounds__(kShapeThreads)
     crater_extras_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
-                         const float* __restrict__ data, const Grid grid, const NoData nodata,
-                         const CraterBins bins, float* __restrict__ heights) {
+                         const float* __restrict__ data,
+                         const crater::LeanCrater* __restrict__ leans, const Grid grid,
+                         const NoData nodata, const CraterBins bins,
+                         float* __restrict__ heights) {
     const uint32_t bin = bins.firstBin + blockIdx.x;
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
     const uint32_t first = bins.counts[bin];
     const uint32_t count = bins.counts[bin + 1] - first;
-    const LeanEntry* entries = reinterpret_cast<const LeanEntry*>(bins.entries) + first;
+    const uint32_t* indices = reinterpret_cast<const uint32_t*>(bins.entries) + first;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // The bin's entries with extras work, found by all threads at once (most bins have none).
+    // The bin's heavy craters, found by all threads at once (most bins have none).
     constexpr uint32_t kList = 256;
     __shared__ uint32_t list[kList];
     __shared__ uint32_t listed;
@@ -672,10 +774,11 @@ __global__ void __launch_bounds__(kShapeThreads)
     }
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < count; e += blockDim.x) {
-        if (__ldg(&entries[e].index) & kHeavyEntry) {
+        const uint32_t index = __ldg(indices + e);
+        if (index & kHeavyEntry) {
             const uint32_t slot = atomicAdd(&listed, 1u);
             if (slot < kList) {
-                list[slot] = e;
+                list[slot] = index & ~kHeavyEntry;
             }
         }
     }
@@ -690,23 +793,27 @@ __global__ void __launch_bounds__(kShapeThreads)
     const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
     long long sum[kCellsPerThread] = {0, 0, 0, 0};
     for (uint32_t q = 0; q < (all ? count : found); ++q) {
-        const uint32_t e = all ? q : list[q];
-        const uint32_t index = __ldg(&entries[e].index);
-        if ((index & kHeavyEntry) == 0u) {
-            continue;  // block-uniform
-        }
-        const crater::LeanCrater& l = entries[e].lean;
-        const uint32_t flags = __ldg(&l.flags);
-        const CraterRecord& r = records[index & ~kHeavyEntry];
-        float cull = __ldg(&entries[e].cull);
-        bool inTile = true;
-        if (flags & crater::kLeanHeavy) {
-            inTile = w.anyLive && w.tileX >= int(__ldg(&entries[e].tileX0)) &&
-                     w.tileX <= int(__ldg(&entries[e].tileX1)) &&
-                     w.tileY >= int(__ldg(&entries[e].tileY0)) &&
-                     w.tileY <= int(__ldg(&entries[e].tileY1));
+        uint32_t crater_index;
+        if (all) {
+            const uint32_t index = __ldg(indices + q);
+            if ((index & kHeavyEntry) == 0u) {
+                continue;  // block-uniform
+            }
+            crater_index = index & ~kHeavyEntry;
         } else {
-            cull = sqrtf(__ldg(&l.peakReach2)) * (1.0f + 1e-5f) + 1e-6f;
+            crater_index = list[q];
+        }
+        const crater::LeanCrater& l = leans[crater_index];
+        const CraterRecord& r = records[crater_index];
+        const uint32_t lflags = __ldg(&l.flags);
+        float cull = __ldg(&l.cull);
+        bool inTile = true;
+        if (lflags & crater::kLeanHeavy) {
+            inTile = w.anyLive && w.tileX >= int(__ldg(&l.tileX0)) &&
+                     w.tileX <= int(__ldg(&l.tileX1)) && w.tileY >= int(__ldg(&l.tileY0)) &&
+                     w.tileY <= int(__ldg(&l.tileY1));
+        } else {
+            cull = sqrtf(__ldg(&l.peakReach2)) * (1.0f + 1e-5f) + 1e-6f;  // the massif peak's
         }
         const uint32_t need = need_mask(w, inTile, r.x, r.xLow, r.y, r.yLow, cull);
         if (need == 0u) {
@@ -718,7 +825,7 @@ __global__ void __launch_bounds__(kShapeThreads)
             if (need & (1u << j)) {
                 const float dx = crater::split_difference(w.pxh[j], w.pxl[j], r.x, r.xLow);
                 bool reached;
-                const float v = crater::extra_contribution(k, data, r, flags, dx, dy, reached);
+                const float v = crater::extra_contribution(k, data, r, lflags, dx, dy, reached);
                 if (reached) {
                     sum[j] += to_fixed(v);
                 }
@@ -922,26 +1029,25 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
 cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
                                   uint32_t n, const Grid& grid, const CraterBins& bins,
                                   const void* leans, cudaStream_t stream) {
-    (void)grid;
     if (n == 0) {
         return cudaSuccess;
     }
     const uint32_t threads = 256;  // 8 warps of 32 craters
     const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
-    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(k, records, n,
-                                                          static_cast<const int4*>(leans), bins);
+    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(
+        k, records, n, static_cast<const int4*>(leans), grid, bins);
     return cudaGetLastError();
 }
 
 cudaError_t launch_crater_lean(const CraterShapeKernel& k, const CraterRecord* records, uint32_t n,
-                               const float* data, void* leans, cudaStream_t stream) {
+                               const float* data, const CraterBins& bins, void* leans,
+                               cudaStream_t stream) {
     static_assert(sizeof(crater::LeanCrater) == kLeanCraterBytes, "lean crater size");
-    static_assert(sizeof(LeanEntry) == kLeanEntryBytes, "lean entry size");
     if (n == 0) {
         return cudaSuccess;
     }
     crater_lean_kernel<<<(n + 127) / 128, 128, 0, stream>>>(
-        k, records, n, data, static_cast<crater::LeanCrater*>(leans));
+        k, records, n, data, bins, static_cast<crater::LeanCrater*>(leans));
     return cudaGetLastError();
 }
 
@@ -968,7 +1074,8 @@ bool crater_lean_entries(const CraterShapeKernel& k) {
 }
 
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* records,
-                                const float* data, bool lean, bool extras, const Grid& grid,
+                                const float* data, const void* leans, bool extras,
+                                const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
                                 cudaStream_t stream, uint32_t firstBinRow, uint32_t binRows,
                                 uint32_t polls) {
@@ -982,16 +1089,17 @@ cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* 
     }
     CraterBins strip = bins;
     strip.firstBin = firstBinRow * bins.binsX;
-    if (lean) {
+    if (leans != nullptr) {
+        const auto* lean = static_cast<const crater::LeanCrater*>(leans);
         crater_lean_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(
-            k, grid, nodata, strip, heights, bins.total + 1, polls);
+            k, records, data, lean, grid, nodata, strip, heights, bins.total + 1, polls);
         if (extras) {
             const cudaError_t err = cudaGetLastError();
             if (err != cudaSuccess) {
                 return err;
             }
-            crater_extras_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, records, data, grid,
-                                                                    nodata, strip, heights);
+            crater_extras_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, records, data, lean,
+                                                                    grid, nodata, strip, heights);
         }
     } else {
         crater_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, data, grid, nodata, strip,

@@ -91,13 +91,17 @@ cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* 
                                 const Grid& grid, const CraterBins& bins, cudaStream_t stream);
 // The plain path's lean craters (crater_math.cuh LeanCrater): kLeanCraterBytes per crater, made
 // by launch_crater_lean; with them the bins hold kLeanEntryBytes entries, else 160-byte BinEntry.
-constexpr size_t kLeanCraterBytes = 192;
-constexpr size_t kLeanEntryBytes = 208;
+// The plain path's lean craters (crater_math.cuh LeanCrater): kLeanCraterBytes per crater, made
+// by launch_crater_lean after the count pass (it reads the footprint boxes and culls). With them
+// the bins hold 4-byte crater indices (the shaping kernel gathers each entry's LeanCrater into
+// shared memory), else 160-byte BinEntry copies of the records.
+constexpr size_t kLeanCraterBytes = 208;
+constexpr size_t kLeanEntryBytes = 4;
 cudaError_t launch_crater_lean(const CraterShapeKernel& k, const CraterRecord* records, uint32_t n,
-                               const float* data, void* leans, cudaStream_t stream);
-// Scatters each crater's entry into its bins (a LeanEntry from `leans` when given, else a
-// BinEntry); an entry whose crater has work for the extras pass (crater_needs_extras) carries
-// kHeavyEntry in its `index`.
+                               const float* data, const CraterBins& bins, void* leans,
+                               cudaStream_t stream);
+// Scatters each crater into its bins (its index when `leans` is given, else a BinEntry); an entry
+// whose crater needs the extras pass (crater_needs_extras) carries kHeavyEntry in its index.
 cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord* records,
                                   uint32_t n, const Grid& grid, const CraterBins& bins,
                                   const void* leans, cudaStream_t stream);
@@ -117,11 +121,12 @@ cudaError_t launch_crater_harmonics(const CraterRecord* records, uint32_t n, con
 // Polls of a staged copy before a binned kernel gives up on it (flag 2, TG_ERROR_TIMEOUT).
 constexpr uint32_t kWaitPolls = 1u << 26;
 
-// Shapes the bins of rows [firstBinRow, firstBinRow + binRows): with `lean` (LeanEntry bins) the
-// lean kernel, then, when `extras`, the extras pass over the same bins; otherwise the general
-// kernel on BinEntry bins.
+// Shapes the bins of rows [firstBinRow, firstBinRow + binRows): with `leans` (index bins) the lean
+// kernel, then, when `extras`, the extras pass over the same bins; otherwise the general kernel on
+// BinEntry bins.
 cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* records,
-                                const float* data, bool lean, bool extras, const Grid& grid,
+                                const float* data, const void* leans, bool extras,
+                                const Grid& grid,
                                 NoData nodata, const CraterBins& bins, float* heights,
                                 cudaStream_t stream, uint32_t firstBinRow = 0,
                                 uint32_t binRows = 0xffffffffu, uint32_t polls = kWaitPolls);
