@@ -543,17 +543,27 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
     TG_CUDA(d->slots[kCursor].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
     TG_CUDA(d->slots[kBoxes].reserve(size_t(n) * sizeof(int4)), "allocation");
     TG_CUDA(d->slots[kCulls].reserve(size_t(n) * sizeof(float)), "allocation");
-    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(std::max(nbins, n)) * sizeof(uint32_t)),
+            "allocation");
     TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kPairStart].reserve((size_t(n) + 1) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kExtrasMark].reserve(size_t(nbins) * sizeof(uint32_t)), "allocation");
+    TG_CUDA(d->slots[kExtrasList].reserve((size_t(nbins) + 1) * sizeof(uint32_t)), "allocation");
     bins.counts = slot_ptr<uint32_t>(d, kCounts);
     bins.cursor = slot_ptr<uint32_t>(d, kCursor);
     bins.boxes = slot_ptr<int4>(d, kBoxes);
     bins.culls = slot_ptr<float>(d, kCulls);
     bins.total = slot_ptr<uint32_t>(d, kStatus);
+    bins.pairStart = slot_ptr<uint32_t>(d, kPairStart);
+    bins.extrasMark = slot_ptr<uint32_t>(d, kExtrasMark);
+    bins.extrasList = slot_ptr<uint32_t>(d, kExtrasList);
     TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
     TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
     TG_CUDA(cudaMemsetAsync(bins.total, 0, 4 * sizeof(uint32_t), s), "memset");
-    TG_CUDA(launch_crater_count(k, rec, n, data, foot, g, bins, s), "crater count launch");
+    TG_CUDA(cudaMemsetAsync(bins.extrasMark, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
+    TG_CUDA(cudaMemsetAsync(bins.extrasList, 0, sizeof(uint32_t), s), "memset");
+    TG_CUDA(launch_crater_count(k, rec, n, data, foot, g, bins, slot_ptr<uint32_t>(d, kScan), s),
+            "crater count launch");
     TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
             "scan launch");
     // The entries needed and the datum flag, to size the bins.

@@ -90,6 +90,9 @@ enum Slot {
     kBoulderCounts,
     kBoulderCursor,
     kBoulderStatus,
+    kPairStart,
+    kExtrasMark,
+    kExtrasList,
     kSlotCount
 };
 

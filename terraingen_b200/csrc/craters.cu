@@ -33,183 +33,144 @@ constexpr uint32_t kChunk = 96;        // entries per staged chunk (15 KB)
 
 using namespace binning;
 
-// Each warp takes 32 craters: every lane finds its crater's footprint (its 16-cell tile window
-// and cull radius, as CraterReach and TileLists give it), then the warp counts the bins of each
-// crater in turn, its lanes spread over the crater's bins.
-__global__ void crater_count_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
-                                    uint32_t n, const float* __restrict__ data,
-                                    const double* __restrict__ footprints, const Grid grid,
-                                    CraterBins bins, uint32_t* __restrict__ flags) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
-    if (base >= n) {
+// Binning runs over (crater, bin) pairs, so a crater covering thousands of bins costs no more
+// than as many small ones: the footprint pass finds each crater's tile box, cull radius and bin
+// count; an exclusive scan of those counts numbers the pairs; the count and scatter passes take
+// one pair per thread (grid-stride), each finding its crater by binary search in the scan.
+
+// Per crater: its footprint (the 16-cell tile window and cull radius, as CraterReach and
+// TileLists give it) and how many bins it covers, into pairStart[i] (scanned afterwards).
+__global__ void crater_footprint_kernel(const CraterShapeKernel k,
+                                        const CraterRecord* __restrict__ records, uint32_t n,
+                                        const float* __restrict__ data,
+                                        const double* __restrict__ footprints, const Grid grid,
+                                        CraterBins bins, uint32_t* __restrict__ flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
         return;
     }
-    const uint32_t mine = base + lane;
-    int4 tiles = make_int4(1, 0, 1, 0);
-    if (mine < n) {
-        const CraterRecord r = records[mine];
-        const Footprint f = crater_footprint(k, r, data, footprints, mine, grid);
-        tiles = f.tiles;
-        bins.boxes[mine] = tiles;
-        bins.culls[mine] = f.cull;
-        if (tiles.x <= tiles.y) {
-            if (r.hasDatum == 1u) {
-                atomicOr(flags, 1u);
-            }
-            // Work for the extras pass after the lean kernel (heavy records, massif peaks).
-            if (crater_needs_extras(k, r) || (crater_is_complex(k, r) && r.peakCount > 0u)) {
-                atomicOr(flags, 4u);
-            }
+    constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
+    const CraterRecord& r = records[i];
+    const Footprint f = crater_footprint(k, r, data, footprints, i, grid);
+    bins.boxes[i] = f.tiles;
+    bins.culls[i] = f.cull;
+    uint32_t pairs = 0;
+    if (f.tiles.x <= f.tiles.y) {
+        pairs = (uint32_t(f.tiles.y) / kTilesPerBin - uint32_t(f.tiles.x) / kTilesPerBin + 1u) *
+                (uint32_t(f.tiles.w) / kTilesPerBin - uint32_t(f.tiles.z) / kTilesPerBin + 1u);
+        if (r.hasDatum == 1u) {
+            atomicOr(flags, 1u);
+        }
+        // Work for the extras pass after the lean kernel (heavy records, massif peaks).
+        if (crater_needs_extras(k, r) || (crater_is_complex(k, r) && r.peakCount > 0u)) {
+            atomicOr(flags, 4u);
         }
     }
+    bins.pairStart[i] = pairs;
+}
+
+// The crater of pair p: the last crater whose first pair is at most p (pairStart scanned, with
+// pairStart[n] the number of pairs).
+__device__ __forceinline__ uint32_t pair_crater(const uint32_t* __restrict__ start, uint32_t n,
+                                                uint32_t p) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(start + mid) <= p) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// Pair p's crater and bin.
+__device__ __forceinline__ void pair_bin(const CraterBins& bins, uint32_t n, uint32_t p,
+                                         uint32_t& crater, int4& tiles, uint32_t& bx,
+                                         uint32_t& by) {
     constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
-    const uint32_t count = min(32u, n - base);
-    for (uint32_t j = 0; j < count; ++j) {
-        const int4 t = make_int4(__shfl_sync(0xffffffffu, tiles.x, int(j)),
-                                 __shfl_sync(0xffffffffu, tiles.y, int(j)),
-                                 __shfl_sync(0xffffffffu, tiles.z, int(j)),
-                                 __shfl_sync(0xffffffffu, tiles.w, int(j)));
-        if (t.x > t.y) {
-            continue;
-        }
-        const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
-        const uint32_t by0 = uint32_t(t.z) / kTilesPerBin, by1 = uint32_t(t.w) / kTilesPerBin;
-        const uint32_t wide = bx1 - bx0 + 1u;
-        const uint32_t total = wide * (by1 - by0 + 1u);
-        for (uint32_t q = lane; q < total; q += 32u) {
-            const uint32_t b = (by0 + q / wide) * bins.binsX + bx0 + q % wide;
-            atomicAdd(bins.counts + b, 1u);
-        }
+    crater = pair_crater(bins.pairStart, n, p);
+    tiles = bins.boxes[crater];
+    const uint32_t local = p - __ldg(bins.pairStart + crater);
+    const uint32_t bx0 = uint32_t(tiles.x) / kTilesPerBin;
+    const uint32_t wide = uint32_t(tiles.y) / kTilesPerBin - bx0 + 1u;
+    bx = bx0 + local % wide;
+    by = uint32_t(tiles.z) / kTilesPerBin + local / wide;
+}
+
+__global__ void crater_bin_count_kernel(uint32_t n, CraterBins bins) {
+    const uint32_t pairs = bins.pairStart[n];
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
+         p += gridDim.x * blockDim.x) {
+        uint32_t crater, bx, by;
+        int4 tiles;
+        pair_bin(bins, n, p, crater, tiles, bx, by);
+        atomicAdd(bins.counts + by * bins.binsX + bx, 1u);
     }
 }
 
-// Each warp takes 32 craters and spreads all of their (crater, bin) pairs over its lanes: a
-// lane finds its pair's crater by a search of the warp's running bin counts, then copies the
-// crater's record and tail into its bin's next slot.
-// Whether a disk of `radius` m around (x, y) meets the cell centers of bin (bx, by) of an
-// axis-aligned grid, with a cell to spare (rotated grids: always).
+// Whether a massif peak of `radius` m around (x, y) can reach a cell center of bin (bx, by): the
+// columns and rows of cell centers within the radius (a box, with a little slack) meet the bin's
+// (rotated grids: always).
 __device__ inline bool peak_meets_bin(const Grid& g, double x, double y, double radius,
                                       uint32_t bx, uint32_t by) {
     if (g.rowRotation != 0.0 || g.colRotation != 0.0) {
         return true;
     }
-    const double xa = g.originX + double(bx * kBinCells) * g.pixelWidth;
-    const double xb = xa + double(kBinCells) * g.pixelWidth;
-    const double ya = g.originY + double(by * kBinCells) * g.pixelHeight;
-    const double yb = ya + double(kBinCells) * g.pixelHeight;
-    const double box[4] = {fmin(xa, xb), fmin(ya, yb), fmax(xa, xb), fmax(ya, yb)};
-    const double spare = fabs(g.pixelWidth) + fabs(g.pixelHeight);
-    return disk_meets_box(x, y, radius + spare, box);
+    const double px = (x - g.originX) / g.pixelWidth - 0.5;  // cell column whose center is at x
+    const double py = (y - g.originY) / g.pixelHeight - 0.5;
+    const double rx = radius / fabs(g.pixelWidth) * (1.0 + 1e-6) + 1e-6;
+    const double ry = radius / fabs(g.pixelHeight) * (1.0 + 1e-6) + 1e-6;
+    const double c0 = fmax(ceil(px - rx), double(bx * kBinCells));
+    const double c1 = fmin(floor(px + rx), double(bx * kBinCells + kBinCells - 1u));
+    const double r0 = fmax(ceil(py - ry), double(by * kBinCells));
+    const double r1 = fmin(floor(py + ry), double(by * kBinCells + kBinCells - 1u));
+    return c0 <= c1 && r0 <= r1;
 }
 
-// With `leans` the entries are crater indices (kHeavyEntry set where the extras pass has work),
-// else BinEntry copies (the record and the tail).
-__global__ void crater_scatter_kernel(const CraterShapeKernel k,
-                                      const CraterRecord* __restrict__ records, uint32_t n,
-                                      const int4* __restrict__ leans, const Grid grid,
-                                      CraterBins bins) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
-    if (base >= n) {
-        return;
-    }
-    constexpr uint32_t kTilesPerBin = kBinCells / kRefTileCells;
-    const uint32_t mine = base + lane;
-    int4 tiles = make_int4(1, 0, 1, 0);
-    float cull = 0.0f;
-    uint32_t count = 0;
-    if (mine < n) {
-        tiles = bins.boxes[mine];
-        cull = bins.culls[mine];
-        if (tiles.x <= tiles.y) {
-            count = (uint32_t(tiles.y) / kTilesPerBin - uint32_t(tiles.x) / kTilesPerBin + 1u) *
-                    (uint32_t(tiles.w) / kTilesPerBin - uint32_t(tiles.z) / kTilesPerBin + 1u);
+// Each pair's entry in its bin's next slot. With `leans` the entries are crater indices, with
+// kHeavyEntry where the extras pass has work (a heavy crater in all its bins, a massif peak in the
+// bins its reach meets), and each such bin is listed once in bins.extrasList; otherwise they are
+// BinEntry copies (the record and the tail).
+__global__ void crater_bin_scatter_kernel(const CraterShapeKernel k,
+                                          const CraterRecord* __restrict__ records, uint32_t n,
+                                          const crater::LeanCrater* __restrict__ leans,
+                                          const Grid grid, CraterBins bins) {
+    const uint32_t pairs = bins.pairStart[n];
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
+         p += gridDim.x * blockDim.x) {
+        uint32_t crater, bx, by;
+        int4 t;
+        pair_bin(bins, n, p, crater, t, bx, by);
+        const uint32_t b = by * bins.binsX + bx;
+        const uint32_t slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
+        if (slot >= bins.capacity) {
+            continue;  // the host sized the entries from the counts; never taken
         }
-    }
-    // Inclusive running count of the warp's pairs.
-    uint32_t upto = count;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, upto, d);
-        if (lane >= uint32_t(d)) {
-            upto += v;
-        }
-    }
-    const uint32_t pairs = __shfl_sync(0xffffffffu, upto, 31);
-    for (uint32_t q0 = 0; q0 < pairs; q0 += 32u) {
-        const uint32_t q = q0 + lane;
-        // The crater of pair q: the first lane whose running count exceeds q.
-        uint32_t owner = 0;
-#pragma unroll
-        for (uint32_t step = 16; step > 0; step >>= 1) {
-            const uint32_t probe = owner + step - 1u;
-            const uint32_t at = __shfl_sync(0xffffffffu, upto, int(probe));
-            if (at <= q) {
-                owner += step;
-            }
-        }
-        const int4 t = make_int4(__shfl_sync(0xffffffffu, tiles.x, int(owner)),
-                                 __shfl_sync(0xffffffffu, tiles.y, int(owner)),
-                                 __shfl_sync(0xffffffffu, tiles.z, int(owner)),
-                                 __shfl_sync(0xffffffffu, tiles.w, int(owner)));
-        const float c = __shfl_sync(0xffffffffu, cull, int(owner));
-        const uint32_t before = __shfl_sync(0xffffffffu, upto - count, int(owner));
-        const uint32_t crater = base + owner;
-        uint32_t slot = 0xffffffffu;  // none
-        if (q < pairs) {
-            const uint32_t local = q - before;
-            const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin, bx1 = uint32_t(t.y) / kTilesPerBin;
-            const uint32_t by0 = uint32_t(t.z) / kTilesPerBin;
-            const uint32_t wide = bx1 - bx0 + 1u;
-            const uint32_t b = (by0 + local / wide) * bins.binsX + bx0 + local % wide;
-            slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
-            if (slot >= bins.capacity) {
-                slot = 0xffffffffu;  // the host sized the entries from the counts; never taken
-            }
-        }
+        const CraterRecord& r = records[crater];
         if (leans != nullptr) {
-            // Index bins: the shaping kernel gathers the crater's LeanCrater itself. The extras
-            // pass looks at a heavy crater in all its bins and at a massif peak in the bins the
-            // peak's reach meets.
-            if (slot != 0xffffffffu) {
-                const CraterRecord& r = records[crater];
-                bool extras = crater_needs_extras(k, r);
-                if (!extras && crater_is_complex(k, r) && r.peakCount > 0u) {
-                    const crater::LeanCrater* l =
-                        reinterpret_cast<const crater::LeanCrater*>(leans) + crater;
-                    const uint32_t local = q - before;
-                    const uint32_t bx0 = uint32_t(t.x) / kTilesPerBin;
-                    const uint32_t wide = uint32_t(t.y) / kTilesPerBin - bx0 + 1u;
-                    const uint32_t bx = bx0 + local % wide;
-                    const uint32_t by = uint32_t(t.z) / kTilesPerBin + local / wide;
-                    extras = peak_meets_bin(grid, double(r.x) + double(r.xLow),
-                                            double(r.y) + double(r.yLow),
-                                            sqrt(double(__ldg(&l->peakReach2))), bx, by);
-                }
-                reinterpret_cast<uint32_t*>(bins.entries)[slot] = crater | (extras ? kHeavyEntry : 0u);
+            bool extras = crater_needs_extras(k, r);
+            if (!extras && crater_is_complex(k, r) && r.peakCount > 0u) {
+                extras = peak_meets_bin(grid, double(r.x) + double(r.xLow),
+                                        double(r.y) + double(r.yLow),
+                                        sqrt(double(__ldg(&leans[crater].peakReach2))), bx, by);
+            }
+            reinterpret_cast<uint32_t*>(bins.entries)[slot] = crater | (extras ? kHeavyEntry : 0u);
+            if (extras && atomicOr(bins.extrasMark + b, 1u) == 0u) {
+                bins.extrasList[1u + atomicAdd(bins.extrasList, 1u)] = b;
             }
             continue;
         }
-        // Each lane writes its entry's 16-byte tail; the records are copied one entry at a time
-        // by the whole warp, 16 contiguous bytes a lane.
-        const uint32_t words = 10u;
-        int4* entries = reinterpret_cast<int4*>(bins.entries);
-        if (slot != 0xffffffffu) {
-            const uint32_t extras = crater_needs_extras(k, records[crater]) ? kHeavyEntry : 0u;
-            entries[size_t(slot) * words + words - 1u] =
-                make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
-                          int(uint32_t(t.z) | (uint32_t(t.w) << 16)), __float_as_int(c),
-                          int(crater | extras));
+        const int4* src = reinterpret_cast<const int4*>(records + crater);
+        int4* dst = reinterpret_cast<int4*>(bins.entries + slot);
+#pragma unroll
+        for (int w = 0; w < 9; ++w) {
+            dst[w] = __ldg(src + w);
         }
-        const int4* bodies = reinterpret_cast<const int4*>(records);
-        for (uint32_t from = 0; from < 32u; ++from) {
-            const uint32_t s = __shfl_sync(0xffffffffu, slot, int(from));
-            const uint32_t src = __shfl_sync(0xffffffffu, crater, int(from));
-            if (s != 0xffffffffu && lane < words - 1u) {
-                entries[size_t(s) * words + lane] = __ldg(bodies + size_t(src) * (words - 1u) + lane);
-            }
-        }
+        dst[9] = make_int4(int(uint32_t(t.x) | (uint32_t(t.y) << 16)),
+                           int(uint32_t(t.z) | (uint32_t(t.w) << 16)),
+                           __float_as_int(bins.culls[crater]), int(crater));
     }
 }
 
@@ -748,99 +709,77 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
     write_cells(grid, w, acc, heights);
 }
 
-// The extras pass after the lean kernel, over the same bins: heavy craters (tables, marks,
-// terraces, shifts, upslopes, long outlines) through the general contribution, and the massif
-// peaks' difference from the round dome the lean pass gave their craters, in the bins a peak
-// reaches. Rare work: each thread evaluates its own 4 cells against each such entry of its bin,
-// read from global memory, and adds the fixed-point sum to the heights the lean pass wrote.
+// The extras pass after the lean kernel: heavy craters (tables, marks, terraces, shifts,
+// upslopes, long outlines) through the general contribution, and the massif peaks' difference
+// from the round dome the lean pass gave their craters, in the bins the scatter listed
+// (bins.extrasList) and only those of this launch's strip of bin rows. Rare work: each CTA takes
+// listed bins in turn, each thread evaluates its own 4 cells against each flagged entry of the
+// bin, read from global memory, and adds the fixed-point sum to the heights the lean pass wrote.
 __global__ void __launch_bounds__(kShapeThreads)
     crater_extras_kernel(const CraterShapeKernel k, const CraterRecord* __restrict__ records,
                          const float* __restrict__ data,
                          const crater::LeanCrater* __restrict__ leans, const Grid grid,
-                         const NoData nodata, const CraterBins bins,
+                         const NoData nodata, const CraterBins bins, uint32_t binsInStrip,
                          float* __restrict__ heights) {
-    const uint32_t bin = bins.firstBin + blockIdx.x;
-    const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
-    const uint32_t first = bins.counts[bin];
-    const uint32_t count = bins.counts[bin + 1] - first;
-    const uint32_t* indices = reinterpret_cast<const uint32_t*>(bins.entries) + first;
+    const uint32_t listed = bins.extrasList[0];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    // The bin's heavy craters, found by all threads at once (most bins have none).
-    constexpr uint32_t kList = 256;
-    __shared__ uint32_t list[kList];
-    __shared__ uint32_t listed;
-    if (threadIdx.x == 0) {
-        listed = 0;
-    }
-    __syncthreads();
-    for (uint32_t e = threadIdx.x; e < count; e += blockDim.x) {
-        const uint32_t index = __ldg(indices + e);
-        if (index & kHeavyEntry) {
-            const uint32_t slot = atomicAdd(&listed, 1u);
-            if (slot < kList) {
-                list[slot] = index & ~kHeavyEntry;
-            }
+    for (uint32_t item = blockIdx.x; item < listed; item += gridDim.x) {
+        const uint32_t bin = bins.extrasList[1u + item];
+        if (bin < bins.firstBin || bin >= bins.firstBin + binsInStrip) {
+            continue;  // block-uniform: another strip's bin
         }
-    }
-    __syncthreads();
-    const uint32_t found = listed;
-    if (found == 0u) {
-        return;
-    }
-    // Past the list's room every entry is looked at in turn (the fixed-point sum does not depend
-    // on the order).
-    const bool all = found > kList;
-    const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
-    long long sum[kCellsPerThread] = {0, 0, 0, 0};
-    for (uint32_t q = 0; q < (all ? count : found); ++q) {
-        uint32_t crater_index;
-        if (all) {
-            const uint32_t index = __ldg(indices + q);
+        const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
+        const uint32_t first = bins.counts[bin];
+        const uint32_t count = bins.counts[bin + 1] - first;
+        const uint32_t* indices = reinterpret_cast<const uint32_t*>(bins.entries) + first;
+        const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
+        long long sum[kCellsPerThread] = {0, 0, 0, 0};
+        for (uint32_t e = 0; e < count; ++e) {
+            const uint32_t index = __ldg(indices + e);
             if ((index & kHeavyEntry) == 0u) {
                 continue;  // block-uniform
             }
-            crater_index = index & ~kHeavyEntry;
-        } else {
-            crater_index = list[q];
-        }
-        const crater::LeanCrater& l = leans[crater_index];
-        const CraterRecord& r = records[crater_index];
-        const uint32_t lflags = __ldg(&l.flags);
-        float cull = __ldg(&l.cull);
-        bool inTile = true;
-        if (lflags & crater::kLeanHeavy) {
-            inTile = w.anyLive && w.tileX >= int(__ldg(&l.tileX0)) &&
-                     w.tileX <= int(__ldg(&l.tileX1)) && w.tileY >= int(__ldg(&l.tileY0)) &&
-                     w.tileY <= int(__ldg(&l.tileY1));
-        } else {
-            cull = sqrtf(__ldg(&l.peakReach2)) * (1.0f + 1e-5f) + 1e-6f;  // the massif peak's
-        }
-        const uint32_t need = need_mask(w, inTile, r.x, r.xLow, r.y, r.yLow, cull);
-        if (need == 0u) {
-            continue;
-        }
-        const float dy = crater::split_difference(w.pyh, w.pyl, r.y, r.yLow);
+            const uint32_t c = index & ~kHeavyEntry;
+            const crater::LeanCrater& l = leans[c];
+            const CraterRecord& r = records[c];
+            const uint32_t lflags = __ldg(&l.flags);
+            float cull = __ldg(&l.cull);
+            bool inTile = true;
+            if (lflags & crater::kLeanHeavy) {
+                inTile = w.anyLive && w.tileX >= int(__ldg(&l.tileX0)) &&
+                         w.tileX <= int(__ldg(&l.tileX1)) && w.tileY >= int(__ldg(&l.tileY0)) &&
+                         w.tileY <= int(__ldg(&l.tileY1));
+            } else {
+                cull = sqrtf(__ldg(&l.peakReach2)) * (1.0f + 1e-5f) + 1e-6f;  // the massif peak's
+            }
+            const uint32_t need = need_mask(w, inTile, r.x, r.xLow, r.y, r.yLow, cull);
+            if (need == 0u) {
+                continue;
+            }
+            const float dy = crater::split_difference(w.pyh, w.pyl, r.y, r.yLow);
 #pragma unroll
-        for (int j = 0; j < kCellsPerThread; ++j) {
-            if (need & (1u << j)) {
-                const float dx = crater::split_difference(w.pxh[j], w.pxl[j], r.x, r.xLow);
-                bool reached;
-                const float v = crater::extra_contribution(k, data, r, lflags, dx, dy, reached);
-                if (reached) {
-                    sum[j] += to_fixed(v);
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                if (need & (1u << j)) {
+                    const float dx = crater::split_difference(w.pxh[j], w.pxl[j], r.x, r.xLow);
+                    bool reached;
+                    const float v =
+                        crater::extra_contribution(k, data, r, lflags, dx, dy, reached);
+                    if (reached) {
+                        sum[j] += to_fixed(v);
+                    }
                 }
             }
         }
-    }
-    if (!w.rowIn) {
-        return;
-    }
-    float* dst = heights + size_t(w.row) * grid.width + w.col0;
+        if (w.rowIn) {
+            float* dst = heights + size_t(w.row) * grid.width + w.col0;
 #pragma unroll
-    for (int j = 0; j < kCellsPerThread; ++j) {
-        if (w.live[j] && sum[j] != 0) {
-            dst[j] = float(double(w.base[j]) + double(sum[j]) * kFixedUnit);
+            for (int j = 0; j < kCellsPerThread; ++j) {
+                if (w.live[j] && sum[j] != 0) {
+                    dst[j] = float(double(w.base[j]) + double(sum[j]) * kFixedUnit);
+                }
+            }
         }
+        __syncthreads();  // the next bin's cells are read only after this one's are written
     }
 }
 
@@ -1013,16 +952,26 @@ cudaError_t launch_exclusive_scan(uint32_t* counts, uint32_t n, uint32_t* scratc
     return cudaGetLastError();
 }
 
+// Grid of the pair-parallel passes (grid-stride over the pairs, whose number stays on the device).
+constexpr uint32_t kPairBlocks = 148u * 8u;
+
 cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
                                 uint32_t n, const float* data, const double* footprints,
-                                const Grid& grid, const CraterBins& bins, cudaStream_t stream) {
+                                const Grid& grid, const CraterBins& bins, uint32_t* scratch,
+                                cudaStream_t stream) {
     if (n == 0) {
         return cudaSuccess;
     }
-    const uint32_t threads = 256;  // 8 warps of 32 craters
-    const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
-    crater_count_kernel<<<blocks, threads, 0, stream>>>(k, records, n, data, footprints, grid,
-                                                        bins, bins.total + 1);
+    crater_footprint_kernel<<<(n + 255) / 256, 256, 0, stream>>>(k, records, n, data, footprints,
+                                                                 grid, bins, bins.total + 1);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        err = launch_exclusive_scan(bins.pairStart, n, scratch, stream);
+    }
+    if (err != cudaSuccess) {
+        return err;
+    }
+    crater_bin_count_kernel<<<kPairBlocks, 256, 0, stream>>>(n, bins);
     return cudaGetLastError();
 }
 
@@ -1032,10 +981,8 @@ cudaError_t launch_crater_scatter(const CraterShapeKernel& k, const CraterRecord
     if (n == 0) {
         return cudaSuccess;
     }
-    const uint32_t threads = 256;  // 8 warps of 32 craters
-    const uint32_t blocks = uint32_t((uint64_t(n) + threads - 1) / threads);
-    crater_scatter_kernel<<<blocks, threads, 0, stream>>>(
-        k, records, n, static_cast<const int4*>(leans), grid, bins);
+    crater_bin_scatter_kernel<<<kPairBlocks, 256, 0, stream>>>(
+        k, records, n, static_cast<const crater::LeanCrater*>(leans), grid, bins);
     return cudaGetLastError();
 }
 
@@ -1098,8 +1045,9 @@ cudaError_t launch_crater_shape(const CraterShapeKernel& k, const CraterRecord* 
             if (err != cudaSuccess) {
                 return err;
             }
-            crater_extras_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, records, data, lean,
-                                                                    grid, nodata, strip, heights);
+            const uint32_t grid2 = std::min(nbins, 148u * 4u);
+            crater_extras_kernel<<<grid2, kShapeThreads, 0, stream>>>(
+                k, records, data, lean, grid, nodata, strip, nbins, heights);
         }
     } else {
         crater_shape_kernel<<<nbins, kShapeThreads, 0, stream>>>(k, data, grid, nodata, strip,

@@ -80,15 +80,20 @@ struct CraterBins {
     int4* boxes;         // [craters] reference-tile box per crater (x0, x1, y0, y1); empty: x0 > x1
     float* culls;        // [craters] cull distance per crater
     uint32_t firstBin;   // the bin of a launch's first block (a strip of bin rows)
+    uint32_t* pairStart; // [craters + 1]: bins per crater, then their exclusive scan
+    uint32_t* extrasMark;  // [bins], zeroed: a bin listed for the extras pass
+    uint32_t* extrasList;  // [bins + 1], [0] zeroed: how many bins are listed, then the bins
 };
 
 // Per crater: its footprint's reference-tile box on `grid` and the number of bins it covers,
 // added to bins.counts. `footprints` (x, y, reach in meters, as doubles) is optional; without it
 // the footprint follows from the record (center hi + lo, reach = outline stretch x reachRadii x
 // radius).
+// `scratch` holds scan_scratch_words(n) words for the scan of the pairs.
 cudaError_t launch_crater_count(const CraterShapeKernel& k, const CraterRecord* records,
                                 uint32_t n, const float* data, const double* footprints,
-                                const Grid& grid, const CraterBins& bins, cudaStream_t stream);
+                                const Grid& grid, const CraterBins& bins, uint32_t* scratch,
+                                cudaStream_t stream);
 // The plain path's lean craters (crater_math.cuh LeanCrater): kLeanCraterBytes per crater, made
 // by launch_crater_lean; with them the bins hold kLeanEntryBytes entries, else 160-byte BinEntry.
 // The plain path's lean craters (crater_math.cuh LeanCrater): kLeanCraterBytes per crater, made
