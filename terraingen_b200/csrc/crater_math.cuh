@@ -1168,20 +1168,31 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
         }
         const uint32_t count = (flags >> 16) & 0xffu;
         if (share > 0.0f && count > 0u) {
-            // w = q e^{i theta}, q = share^(1/2) (1 at full share).
+            // w = q e^{i theta}, q = share^(1/2) (1 at full share). The harmonics past `count`
+            // are zero, so Horner's rule runs over all kLeanHarmonics slots, unrolled: leading
+            // zero terms leave the sum exactly as it is.
             const float q = share < 1.0f ? sqrtf(share) : 1.0f;
             const float wr = q * c1, wi = q * s1;
-            float pr = l.harmonics[count - 1u].x, pi = l.harmonics[count - 1u].y;
-            for (int h = int(count) - 2; h >= 0; --h) {
+            float pr = l.harmonics[kLeanHarmonics - 1u].x, pi = l.harmonics[kLeanHarmonics - 1u].y;
+#pragma unroll
+            for (int h = int(kLeanHarmonics) - 2; h >= 0; --h) {
                 const float t = pr * wr - pi * wi + l.harmonics[h].x;
                 pi = pr * wi + pi * wr + l.harmonics[h].y;
                 pr = t;
             }
             // times w^first
-            for (uint32_t m = (flags >> 8) & 0xffu; m > 0u; --m) {
-                const float t = pr * wr - pi * wi;
-                pi = pr * wi + pi * wr;
+            uint32_t first = (flags >> 8) & 0xffu;
+            if (first == 2u) {
+                const float sr = wr * wr - wi * wi, si = 2.0f * wr * wi;  // w^2
+                const float t = pr * sr - pi * si;
+                pi = pr * si + pi * sr;
                 pr = t;
+            } else {
+                for (; first > 0u; --first) {
+                    const float t = pr * wr - pi * wi;
+                    pi = pr * wi + pi * wr;
+                    pr = t;
+                }
             }
             scale *= 1.0f + pr;
         }

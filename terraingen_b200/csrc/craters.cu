@@ -618,6 +618,8 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
     __shared__ uint16_t queues[kShapeThreads / 32][kQueue];
     __shared__ float2 columns[kShapeThreads / 32][32];
     __shared__ float2 rows[kShapeThreads / 32][4];
+    __shared__ WarpBox boxes[kShapeThreads / 32];
+    __shared__ uint8_t warpMasks[2][kLeanChunk];  // per staged crater: the warps it can touch
 
     const uint32_t bin = bins.firstBin + blockIdx.x;
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
@@ -633,7 +635,6 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
         st.start(lane);
     }
     const WarpCells w = warp_cells(grid, nodata, heights, binX, binY, warp, lane);
-    const WarpBox box = warp_box(grid, binX, binY, warp);
     long long* acc = accs[warp];
     uint16_t* queue = queues[warp];
 #pragma unroll
@@ -645,6 +646,9 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
     }
     if (lane % 8u == 0u) {
         rows[warp][lane / 8u] = make_float2(w.pyh, w.pyl);
+    }
+    if (lane == 0) {
+        boxes[warp] = warp_box(grid, binX, binY, warp);
     }
     const crater::LeanKernel lk = crater::lean_kernel(k);
     __syncthreads();
@@ -674,14 +678,31 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
         }
         const uint32_t s = c & 1u;
         const uint32_t n = min(kLeanChunk, count - c * kLeanChunk);
+        // Which warps' cell boxes each staged crater's cull circle meets, one thread a crater
+        // (heavy craters are the extras pass's: none). The masks are double-buffered like the
+        // stage: the wait before chunk c + 2 is a block barrier, so chunk c's are read by then.
+        if (tid < n) {
+            const crater::LeanCrater& l = stage[s][tid];
+            uint32_t mask = 0;
+            if (!(l.flags & crater::kLeanHeavy)) {
+#pragma unroll
+                for (uint32_t v = 0; v < kShapeThreads / 32; ++v) {
+                    if (!box_misses(boxes[v], l.x, l.xLow, l.y, l.yLow, l.cull)) {
+                        mask |= 1u << v;
+                    }
+                }
+            }
+            warpMasks[s][tid] = uint8_t(mask);
+        }
+        __syncthreads();
         uint32_t queued = 0;  // warp-uniform
         for (uint32_t e = 0; e < n; ++e) {
-            const crater::LeanCrater& l = stage[s][e];
-            // Heavy craters are the extras pass's. A lean crater is never stretched, so every
-            // cell within its cull radius lies inside its footprint window: no tile test.
-            if ((l.flags & crater::kLeanHeavy) || box_misses(box, l.x, l.xLow, l.y, l.yLow, l.cull)) {
+            // A lean crater is never stretched, so every cell within its cull radius lies inside
+            // its footprint window: no tile test.
+            if (((warpMasks[s][e] >> warp) & 1u) == 0u) {
                 continue;  // warp-uniform
             }
+            const crater::LeanCrater& l = stage[s][e];
             const uint32_t need = need_mask(w, true, l.x, l.xLow, l.y, l.yLow, l.cull);
             if (!__any_sync(0xffffffffu, need != 0u)) {
                 continue;
