@@ -2,7 +2,8 @@
 // src/gpu/cuda.cpp, implementing the same `CudaCompute` (src/gpu/cuda.h) over the C ABI in
 // include/tgb200.h.
 //
-// Built inside a TerrainGen tree in place of src/gpu/cuda.cpp, it makes
+// Built inside a TerrainGen tree in place of src/gpu/cuda.cpp, with src/gpu/backend.cpp
+// compiled with TERRAINGEN_HAS_CUDA_KERNELS=1 and linked to libtgb200.so, it makes
 // Backend::Cuda run the noise-layer and crater kernels on the B200 kernels of libtgb200 instead of
 // JIT-compiled Slang PTX: RunKernel (src/gpu/kernel.cpp) binds the same buffers and push
 // constants, and this device maps them onto tg_noise_layer_rows, tg_craters_apply_lists and
