@@ -41,16 +41,23 @@ PIXEL = 0.5
 # key hash and offsets 21, turn 6, lattice 4, split 6, 4 corner hashes 45, 4 gradients 56 plus 2
 # offsets, 2 fades 14, lerps and scale 10, sums 5, turn update 6, loop 3.
 NOISE_OPS_PER_CELL_OCTAVE = 180
-# Counted from terraingen_b200/csrc/crater_math.cuh (fast_contribution) per (cell, crater) pair of
-# a Fassett-Thomson crater with 11 outline harmonics: distance and radii 12, outline share 14,
-# direction 18, first-harmonic rotation and kept share 14, 11 harmonics x 10, scale and division
-# 10, profile 18, resolution and FP64 sum 4.
-CRATER_OPS_PER_PAIR = 200
+# Counted from the reference's crater kernel (include/terraingen/layers/kernels/craters.h:
+# KernelProfileDistance, ComplexProfileHeight / FassettThomsonShape, ApplyCraterKernel) per
+# (cell, crater) pair of the synthetic terrain's craters (11 outline harmonics; a transcendental
+# counts one): offset and distance 6, outline share 7, angle 1, 11 harmonics x 7 (k theta, phase,
+# cos, amplitude, kept share's pow, product, sum) 77, scale and division 2, reach test 1, profile
+# 8, resolution and the add 2: 104, plus the ellipse of 5 % of craters (10): 105.
+CRATER_OPS_PER_PAIR = 105
+# Thread instructions the lean crater kernel executes per pair, measured (ncu smsp__inst_executed
+# x active lanes / pairs, profiles/terrain4097_crater_lean.md): the issue-rate view of the same
+# work (IEEE divisions and square roots, loads, the queue).
+CRATER_THREAD_INST_PER_PAIR = 339
 # Counted from terraingen_b200/csrc/boulders.cu per (cell, boulder) pair: window test 6, offset
 # and hypot 12, dome band average (2 sqrt, 2 asin, clamps) 60, max-composite 4; FP64.
 BOULDER_OPS_PER_PAIR = 82
-# DRAM bytes per launch from the ncu capture of this workload (profiles/terrain4097_kernels.md).
-TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 136.2e6 + 26.4e6, "boulders": 61.9e6 + 7.9e6}
+# DRAM bytes per launch from the ncu captures of this workload (profiles/terrain4097_kernels.md;
+# the crater figure is the lean shaping kernel, profiles/terrain4097_crater_lean.md).
+TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 112.7e6 + 24.1e6, "boulders": 61.9e6 + 7.9e6}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -170,6 +177,22 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "NVML, 2 ms"}
 
 
+FP64_FIXTURE = ROOT / "tests" / "golden" / "fp64.npz"
+
+
+def fp64_error(got, case, rows=None, cols=None):
+    """Max and RMS height error (m) of `got` (the cells of fixture case `case`'s grid, or a
+    larger array and the rows / cols slices of the case's window in it) against the FP64 oracle
+    heights in tests/golden/fp64.npz (tests/golden/fp64_cases.py)."""
+    want = np.load(FP64_FIXTURE)[f"{case}_fp64"]
+    got = np.asarray(got)
+    if rows is not None:
+        got = got[rows, cols]
+    err = np.abs(got.reshape(want.shape).astype(np.float64) - want)
+    return {"max_err_m": float(err.max()), "rms_err_m": float(np.sqrt(np.mean(err ** 2))),
+            "cells": int(want.size)}
+
+
 def cpu_sample(steps, warmup, window, quiet=False):
     """The reference CPU path on a `window`^2 window of the terrain, every host core: (Mcells/s,
     seconds per evaluation, evaluations timed)."""
@@ -252,6 +275,21 @@ def batched_form(dev, args, rank, world, alu_peak):
             graphs.append(st["graph_ms"])
     total_s = max_over_ranks(float(np.sum(graphs)) * 1e-3, world)
     value = world * ts.cells * args.steps / total_s / 1e6
+    # The fixture's far-out tiles of the set (rank 0's set, 4096 tiles) against the FP64 oracle.
+    fp64 = None
+    if args.tiles == 4096 and ranks.tiles_seed(rank) == 11:
+        host = out.cpu().numpy()
+        picks = np.load(FP64_FIXTURE)["tiles_index"]
+        worst = []
+        for k, i in enumerate(picks):
+            g, o, p = ts.grids[i], int(ts.tiles["height_offset"][i]), int(ts.tiles["pitch"][i])
+            cells = np.stack([host[o + r * p:o + r * p + g.width] for r in range(g.height)])
+            worst.append(fp64_error(cells, f"tile{k}"))
+        fp64 = {"tiles": [int(i) for i in picks],
+                "max_err_m": max(e["max_err_m"] for e in worst),
+                "rms_err_m": float(np.sqrt(np.mean([e["rms_err_m"] ** 2 for e in worst]))),
+                "farthest_m": float(max(np.hypot(ts.grids[i].x0, ts.grids[i].y0)
+                                        for i in picks))}
 
     # The plain per-tile path over the same tiles, inputs resident on the device.
     stream = torch.cuda.current_stream()
@@ -322,6 +360,7 @@ def batched_form(dev, args, rank, world, alu_peak):
                            "ms": round(plain_s * 1e3, 3),
                            "path": "tg_noise_source + tg_craters_apply + tg_boulders_bake per tile"},
         "speedup_vs_plain": round(value / plain_value, 2),
+        "fp64": fp64,
         "kernel_shape": {"bin": [st["bin_width"], st["bin_height"]],
                          "cells_per_thread": st["cells_per_thread"], "ctas": st["ctas"]},
         "autotuner_ms": [None if not np.isfinite(m) else round(m, 3) for m in tune_ms],
@@ -423,6 +462,7 @@ def dem_form(dev, args, rank, world):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     same_out = bool(torch.equal(host_out, chain.heights.cpu()))
+    accuracy = dem_accuracy(dev)
     e2e_value = world * w.cells * e2e_steps / e2e_s / 1e6
     solves = chain.solves
     per_link = link_ms.reshape(-1, len(w.windows) - 1, 3).mean(axis=0)
@@ -445,6 +485,7 @@ def dem_form(dev, args, rank, world):
                            (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}}
                        for (a, b, c), st in zip(per_link, solves)],
         "crater_pairs": int(counters["crater_pairs"]),
+        "fp64": accuracy,
         "all_cells_filled": finite,
         "accuracy": "diamond-square within 1e-3 m of the reference (tests/test_ds_gpu.py); seam "
                     "fields within 1e-4 m of the reference's converged PCG, Feather and the gap "
@@ -524,6 +565,7 @@ def served_form(dev, args, rank, world):
     resident) on tile requests of the same stream."""
     import torch
 
+    from terraingen_b200.device import GridSpec
     from terraingen_b200.serve import Server, camera_stream, dem_stack_options, run_stream
     from terraingen_b200.workloads import crater_batch
 
@@ -541,6 +583,13 @@ def served_form(dev, args, rank, world):
         tiles_only = run_stream(server, tiles, realtime=False, device=True)
         host = run_stream(server, sat_reqs, realtime=False)
         stats = server.stats()
+        # A tile of the stack 1e6 m out, served by the same server, against the FP64 oracle.
+        probe_grid = GridSpec(*[int(v) if i < 2 else float(v) for i, v in
+                                enumerate(np.load(FP64_FIXTURE)["served_grid"])])
+        probe = np.empty(probe_grid.cells, np.float32)
+        server.submit_tile(1 << 30, probe_grid, probe)
+        server.drain()
+        fp64 = {"tile": "257^2 at 0.5 m, 1e6 m out", **fp64_error(probe, "served")}
     # The plain per-request path on the stream's tile requests (crater records per tile built
     # and resident before timing).
     sample = tiles[:300]
@@ -586,9 +635,47 @@ def served_form(dev, args, rank, world):
                              "tiles": round(tonly["mcells_per_s"] / plain_value, 2)},
         "server": {k: stats[k] for k in ("batches", "regions_built", "regions_resident",
                                          "feature_bytes", "peak_bytes", "deferred")},
-        "accuracy": "source within 1e-3 m of the FP64 oracle at 1.2e6 m, results identical alone "
-                    "and in the mix (tests/test_serve_gpu.py)",
+        "fp64": fp64,
+        "accuracy": "results identical alone and in the mix (tests/test_serve_gpu.py)",
     }
+
+
+def dem_accuracy(dev):
+    """The DEM form's steps against the reference's FP64 computations on their fixtures
+    (tests/golden/ds.npz, chain.npz): diamond-square refinement (the reference's nodes are FP64,
+    read to float) and the Height seam chain of four patches (the reference's FP64 MG-PCG field)."""
+    import torch
+
+    from terraingen_b200.chain import PatchChain, Seams, Window
+    from terraingen_b200.device import GridSpec
+
+    def grid_of(row):
+        return GridSpec(int(row[0]), int(row[1]), float(row[2]), float(row[3]), float(row[4]))
+
+    def error(got, want):
+        err = np.abs(np.asarray(got, np.float64) - want)
+        ok = np.isfinite(err)
+        return {"max_err_m": float(err[ok].max()), "rms_err_m": float(np.sqrt(np.mean(err[ok] ** 2))),
+                "cells": int(ok.sum())}
+
+    out = {}
+    ds = np.load(ROOT / "tests" / "golden" / "ds.npz")
+    for name in ("dem5m", "tenfold"):
+        pg, g = grid_of(ds[f"{name}_post_grid"]), grid_of(ds[f"{name}_grid"])
+        fd, scale, seed = ds[f"{name}_options"]
+        h = np.zeros((g.height, g.width), np.float32)
+        dev.ds_refine(ds[f"{name}_posts"], pg, g, h, fd, scale, int(seed))
+        out[f"diamond_square_{name}"] = error(h, ds[f"{name}_expected"])
+    z = np.load(ROOT / "tests" / "golden" / "chain.npz")
+    g = grid_of(z["grid"])
+    wins = [Window(*(int(x) for x in w)) for w in z["windows"]]
+    _, width, decay = z["height_options"]
+    chain = PatchChain(dev, g, wins, Seams("height", width=float(width), decay_length=float(decay)))
+    got = chain.compose([torch.from_numpy(z[f"patch{k}"]).cuda() for k in range(4)])
+    out["height_seam_chain"] = error(got.cpu().numpy(), z["height_heights"])
+    out["against"] = ("the reference CPU path: FP64 diamond-square nodes and FP64 MG-PCG seam "
+                      "fields, read to float (fixtures of its own runs)")
+    return out
 
 
 def e2e_leg(dev, w, args, world, device_heights):
@@ -796,6 +883,12 @@ def main():
     e2e = e2e_leg(dev, w, args, world, heights)
     same = e2e.pop("_same")
     e2e_value = e2e["value"]
+    # The timed tile's center 257^2 window against the FP64 oracle (rank 0's tile is centered
+    # on the origin, as the fixture's window is).
+    lo = (SIDE - 257) // 2
+    fp64 = {"window": "257^2 at the tile's center",
+            **fp64_error(heights.cpu().numpy(), "terrain", slice(lo, lo + 257),
+                         slice(lo, lo + 257))}
     forms = {}
     if args.tiles > 0:
         forms["batched"] = batched_form(dev, args, rank, world, alu_peak)
@@ -848,7 +941,18 @@ def main():
         "roofline": {"kernel": kernel_name, "bound": "alu",
                      "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "Tops/s",
                      "frac": round(achieved / peak, 3) if peak else None,
-                     "peak_source": "measured IMAD+FFMA lane-op rate (tg_measure_alu) on this GPU",
+                     "peak_source": "tg_measure_alu on this GPU: 4 quadratic IMAD and 4 FFMA "
+                                    "dependent chains per thread that no compiler can shorten, "
+                                    "thread instructions per second (below the 128 lanes per SM "
+                                    "per clock issue ceiling)",
+                     "issue": {"thread_inst_per_pair": CRATER_THREAD_INST_PER_PAIR,
+                               "achieved": round(counters["crater_pairs"] *
+                                                 CRATER_THREAD_INST_PER_PAIR /
+                                                 (crater_ms * 1e-3) / 1e12, 3),
+                               "frac": round(counters["crater_pairs"] * CRATER_THREAD_INST_PER_PAIR
+                                             / (crater_ms * 1e-3) / alu_peak, 3),
+                               "note": "crater phase (all its kernels) at the measured per-pair "
+                                       "instruction count of the lean kernel"},
                      "algorithmic_ops": unit_note, "traffic": TRAFFIC[dominant],
                      "traffic_source": "ncu dram__bytes_read+write of the shaping/bake/fill "
                                        "kernel, profiles/terrain4097_kernels.md",
@@ -859,6 +963,7 @@ def main():
                          "kind": "reference",
                          "sample": f"{cpu_grid.width}x{cpu_grid.height} window of the same terrain "
                                    f"on the reference CPU path, {cpu_per * 1e3:.0f} ms"},
+        "fp64": fp64,
         "e2e": {**e2e, "matches_device_path": same},
         "dropin": dropin,
         "gpu_launches": int(launches * args.steps),

@@ -261,6 +261,30 @@ def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
     return grid, fr, craters, boulders
 
 
+def uneven_tile_grids(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0),
+                      radius: float = 1.7e6, seed: int = 11) -> list:
+    """The grids of `uneven_tiles` (sides, spacings and centers drawn from `seed`)."""
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(side[0]), np.log(side[1] + 1), n)).astype(np.int64)
+    sides = np.clip(sides, side[0], side[1])
+    pixels = np.exp(rng.uniform(np.log(spacing[0]), np.log(spacing[1]), n))
+    r = radius * np.sqrt(rng.random(n))
+    theta = rng.uniform(0.0, 2.0 * np.pi, n)
+    cxs, cys = r * np.cos(theta), r * np.sin(theta)
+    return [centered(int(s), int(s), float(p), float(x), float(y))
+            for s, p, x, y in zip(sides, pixels, cxs, cys)]
+
+
+def uneven_tile_layers(density: float = 0.1):
+    """The crater population and boulder sizes of `uneven_tiles` at `density` times the
+    synthetic terrain's."""
+    full_area = (4097 * 0.5) ** 2
+    crater_c = density * 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
+    population = crater_population(7, crater_c, 1.0, 500.0)
+    stones_of = boulder_population(7, density * 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5)))
+    return population, stones_of
+
+
 def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: float = 1.7e6,
                  density: float = 0.1, seed: int = 11, boulders: bool = True):
     """Uneven tiles of the synthetic terrain's stack ("tiles4096"): `n` square tiles with sides
@@ -271,19 +295,8 @@ def uneven_tiles(n: int = 4096, side=(65, 1025), spacing=(0.25, 2.0), radius: fl
     it."""
     from .batch import TILE, TileSet, layout
 
-    rng = np.random.default_rng(seed)
-    sides = np.exp(rng.uniform(np.log(side[0]), np.log(side[1] + 1), n)).astype(np.int64)
-    sides = np.clip(sides, side[0], side[1])
-    pixels = np.exp(rng.uniform(np.log(spacing[0]), np.log(spacing[1]), n))
-    r = radius * np.sqrt(rng.random(n))
-    theta = rng.uniform(0.0, 2.0 * np.pi, n)
-    cxs, cys = r * np.cos(theta), r * np.sin(theta)
-    full_area = (4097 * 0.5) ** 2
-    crater_c = density * 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0))
-    population = crater_population(7, crater_c, 1.0, 500.0)
-    stones_of = boulder_population(7, density * 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5)))
-    grids = [centered(int(s), int(s), float(p), float(x), float(y))
-             for s, p, x, y in zip(sides, pixels, cxs, cys)]
+    grids = uneven_tile_grids(n, side, spacing, radius, seed)
+    population, stones_of = uneven_tile_layers(density)
     offsets, pitch = layout(grids)
     tiles = np.zeros(n, TILE)
     kernel = None
