@@ -749,9 +749,10 @@ def e2e_leg(dev, w, args, world, device_heights):
 
 def dropin_leg(window):
     """The reference's own Terrain::Evaluate on the reference arm's window, with Backend::Cuda
-    served by this library's drop-in device (oracle/_ref/libtgref_cuda.so: the reference's
-    pipeline, crater shaping through tg_craters_apply_lists; its source, population, records
-    and boulders stay on its CPU path) against Backend::Cpu of the same build."""
+    served by this library (oracle/_ref/libtgref_cuda.so: the reference's pipeline with crater
+    shaping through the drop-in device's tg_craters_apply_lists, and its synthetic source and
+    boulder domes through tg_noise_source and tg_boulders_bake; the crater population, records and
+    boulder list stay on its CPU path) against Backend::Cpu of the reference's own build."""
     from oracle import harness as H
     from terraingen_b200.workloads import terrain4097_reference_scene
 
@@ -774,7 +775,8 @@ def dropin_leg(window):
             "cpu_mcells_per_s": round(grid.cells / (out["cpu"] * 1e-3) / 1e6, 3),
             "speedup": round(out["cpu"] / out["cuda"], 3),
             "max_abs_diff_m": float(np.abs(a.astype(np.float64) - b).max()),
-            "on_gpu": "crater shaping (RunKernel -> tg_craters_apply_lists)",
+            "on_gpu": "fBm source (tg_noise_source), crater shaping (RunKernel -> "
+                      "tg_craters_apply_lists), boulder domes (tg_boulders_bake)",
             "cores": os.cpu_count()}
 
 

@@ -115,17 +115,19 @@ def below_boulders(lib: C.CDLL, scene: Scene, threads: int = 0) -> np.ndarray:
 
 
 def diamond_square(lib: C.CDLL, posts: np.ndarray, post_grid, grid, fractal_dimension: float,
-                   scale: float, seed: int = 1, interp: int = 0, threads: int = 0):
-    """(heights [h, w] float32, ms): the reference's DiamondSquareUpsampler through a RasterSource."""
+                   scale: float, seed: int = 1, interp: int = 0, threads: int = 0,
+                   backend: int = 0):
+    """(heights [h, w] float32, ms): the reference's DiamondSquareUpsampler through a RasterSource,
+    evaluated on Backend::Cpu (0) or Backend::Cuda (1)."""
     posts = np.ascontiguousarray(posts, np.float32)
     ph, pw = posts.shape
     pt = np.array(post_grid.transform(), np.float64)
     ot = np.array(grid.transform(), np.float64)
     out = np.zeros((grid.height, grid.width), np.float32)
     ms = _D()
-    if lib.tgref_ds(posts.ctypes.data, pw, ph, pt.ctypes.data, fractal_dimension, scale, interp,
-                    seed, grid.width, grid.height, ot.ctypes.data, threads, out.ctypes.data,
-                    C.byref(ms)) != 0:
+    if lib.tgref_ds_on(backend, posts.ctypes.data, pw, ph, pt.ctypes.data, fractal_dimension,
+                       scale, interp, seed, grid.width, grid.height, ot.ctypes.data, threads,
+                       out.ctypes.data, C.byref(ms)) != 0:
         raise RuntimeError(lib.tgref_error().decode())
     return out, ms.value
 
@@ -344,6 +346,9 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_ds.argtypes = [C.c_void_p, _U32, _U32, C.c_void_p, _D, _D, C.c_int, _U32, _U32, _U32,
                              C.c_void_p, C.c_uint, C.c_void_p, C.POINTER(_D)]
     lib.tgref_ds.restype = C.c_int
+    lib.tgref_ds_on.argtypes = [C.c_int] + lib.tgref_ds.argtypes
+    lib.tgref_ds_on.restype = C.c_int
+    lib.tgref_hook_calls.restype = C.c_long
     if hasattr(lib, "tgref_seam"):
         P = C.c_void_p
         lib.tgref_seam.argtypes = [P, P, _U32, _U32, P, C.c_int, _D, _D, P, P, P, P, P, P,
@@ -381,6 +386,11 @@ def reference() -> C.CDLL:
 
 def dropin() -> C.CDLL:
     return _harness("libtgref_cuda.so")
+
+
+def hook_calls(lib: C.CDLL) -> int:
+    """How many CPU-only pipeline stages the drop-in build has run on the device so far."""
+    return int(lib.tgref_hook_calls())
 
 
 def capture() -> C.CDLL:

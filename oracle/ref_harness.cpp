@@ -40,6 +40,10 @@
 #include <string>
 #include <vector>
 
+#ifdef TGREF_HOOKS
+#include "tgb200_hooks.h"
+#endif
+
 using namespace terraingen;
 
 namespace {
@@ -93,6 +97,16 @@ struct tgref_scene {
 
 const char* tgref_error() {
     return g_error.c_str();
+}
+
+/// How many times the drop-in build's hooks at the CPU-only stages ran on the device (0 in the
+/// other builds).
+long tgref_hook_calls() {
+#ifdef TGREF_HOOKS
+    return tgb200_hook_calls();
+#else
+    return 0;
+#endif
 }
 
 }  // extern "C"
@@ -232,6 +246,10 @@ int tgref_evaluate(const tgref_scene* s, int backend, unsigned threads, float* o
         EvaluationOptions options;
         options.threads = threads;
         options.backend = backend == 1 ? Backend::Cuda : Backend::Cpu;
+#ifdef TGREF_HOOKS
+        // The drop-in build's hooks at the CPU-only stages follow the evaluation's backend.
+        tgb200_set_hooks_active(backend == 1);
+#endif
         const auto t0 = std::chrono::steady_clock::now();
         const Raster<float> heights = terrain.Evaluate(grid, options);
         const auto t1 = std::chrono::steady_clock::now();
@@ -359,9 +377,24 @@ long tgref_boulders_posed(const tgref_scene* s, const double* pose, double* out,
 /// The reference's DiamondSquareUpsampler over `posts` (pw x ph floats on `postTransform`), read at
 /// the cells of an `ow` x `oh` grid on `outTransform`, through a RasterSource in a Terrain: the
 /// heights into `out`, the evaluation's wall time into `ms`.
+int tgref_ds_on(int backend, const float* posts, uint32_t pw, uint32_t ph,
+                const double* postTransform, double fractalDimension, double scale, int interp,
+                uint32_t seed, uint32_t ow, uint32_t oh, const double* outTransform,
+                unsigned threads, float* out, double* ms);
+
 int tgref_ds(const float* posts, uint32_t pw, uint32_t ph, const double* postTransform,
              double fractalDimension, double scale, int interp, uint32_t seed, uint32_t ow,
              uint32_t oh, const double* outTransform, unsigned threads, float* out, double* ms) {
+    return tgref_ds_on(0, posts, pw, ph, postTransform, fractalDimension, scale, interp, seed,
+                       ow, oh, outTransform, threads, out, ms);
+}
+
+/// tgref_ds on Backend::Cpu (backend 0) or Backend::Cuda (1; in the drop-in build the
+/// refinement then runs through libtgb200's hook).
+int tgref_ds_on(int backend, const float* posts, uint32_t pw, uint32_t ph,
+                const double* postTransform, double fractalDimension, double scale, int interp,
+                uint32_t seed, uint32_t ow, uint32_t oh, const double* outTransform,
+                unsigned threads, float* out, double* ms) {
     try {
         SetLogLevel(LogLevel::Warning);
         const RasterGrid postGrid{pw, ph,
@@ -381,7 +414,10 @@ int tgref_ds(const float* posts, uint32_t pw, uint32_t ph, const double* postTra
         const Terrain terrain(Surface{}, source, {});
         EvaluationOptions evaluation;
         evaluation.threads = threads;
-        evaluation.backend = Backend::Cpu;
+        evaluation.backend = backend == 1 ? Backend::Cuda : Backend::Cpu;
+#ifdef TGREF_HOOKS
+        tgb200_set_hooks_active(backend == 1);
+#endif
         const RasterGrid grid{ow, oh,
                               GeoTransform::FromGdal({outTransform[0], outTransform[1],
                                                       outTransform[2], outTransform[3],

@@ -80,3 +80,41 @@ def test_crater_datums_on_a_body_through_reference_pipeline(dropin):
     assert np.array_equal(cpu.view(np.uint32), want.view(np.uint32))
     err = np.abs(gpu.astype(np.float64) - cpu)
     assert err.max() <= 1e-3, err.max()
+
+
+def test_terrain_through_hooked_reference_pipeline(dropin):
+    # The synthetic terrain's stack (fBm source, Config-2 craters with peaks and terraces,
+    # boulder domes) through the reference's Terrain::Evaluate on Backend::Cuda: the drop-in build
+    # runs its source fill (tg_noise_source), crater shaping (the adapter) and boulder bake
+    # (tg_boulders_bake) on the device, and the population and records stay on the reference's
+    # CPU path. The result is the CPU backend's within 1e-3 m.
+    from terraingen_b200.workloads import terrain4097_reference_scene
+
+    grid, fr, craters, boulders = terrain4097_reference_scene(257)
+    scene = H.make_scene(grid, source_fractals=fr, craters=craters, boulders=boulders)
+    before = H.hook_calls(dropin)
+    gpu, _ = H.evaluate(dropin, scene, 1, 1)
+    assert H.hook_calls(dropin) - before >= 2  # the source and the boulders ran on the device
+    cpu, _ = H.evaluate(dropin, scene, 0, 1)
+    err = np.abs(gpu.astype(np.float64) - cpu)
+    assert err.max() <= 1e-3, err.max()
+    assert np.count_nonzero(gpu != gpu[0, 0]) > 0.9 * gpu.size
+
+
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+def test_ds_through_hooked_reference_pipeline(dropin, name):
+    # The reference's DiamondSquareUpsampler behind a RasterSource on Backend::Cuda: the drop-in
+    # build's hook hands the refinement to tg_ds_refine, which gives the committed fixture (the
+    # reference's CPU refinement) within 1e-3 m.
+    from conftest import GOLDEN, grid_of
+
+    fx = dict(np.load(GOLDEN / "ds.npz"))
+    pg = grid_of(fx[f"{name}_post_grid"])
+    grid = grid_of(fx[f"{name}_grid"])
+    fd, scale, seed = fx[f"{name}_options"]
+    before = H.hook_calls(dropin)
+    gpu, _ = H.diamond_square(dropin, fx[f"{name}_posts"], pg, grid, fd, scale, int(seed), 0, 1,
+                              backend=1)
+    assert H.hook_calls(dropin) - before >= 1
+    err = np.abs(gpu.astype(np.float64) - fx[f"{name}_expected"])
+    assert err.max() <= 1e-3, (name, err.max())
