@@ -243,6 +243,18 @@ int tg_ds_refine(tg_device* device, const float* posts, uint32_t pw, uint32_t ph
                  const tg_grid* post_grid, const tg_ds_options* options, const tg_grid* grid,
                  float* heights, int memory, void* stream);
 
+/* tg_ds_refine on a window of a larger lattice of posts (a PostLattice read over a box:
+ * src/sources/diamond_square.cpp:488-516 with Refinement::Frame at :302-309): `post_grid` is the
+ * whole lattice's (its post (0, 0) anchors the node frame, so the displacement draws are the
+ * lattice's own), and `posts` holds its columns [col0, col0 + pw) and rows [row0, row0 + ph),
+ * reads past them repeating their edge. A window that ends at the lattice's bounds repeats its
+ * edge as the reference's bounded lattices do; elsewhere the caller gives the window a margin of
+ * posts beyond those the refinement reads (eight posts past the grid's bounds always suffice). */
+int tg_ds_refine_window(tg_device* device, const float* posts, int64_t col0, int64_t row0,
+                        uint32_t pw, uint32_t ph, const tg_grid* post_grid,
+                        const tg_ds_options* options, const tg_grid* grid, float* heights,
+                        int memory, void* stream);
+
 /* Philox4x32-10 conformance (the analogue of the reference's Philox tests,
  * tests/unit/random/philox_test.cpp): for each of `n` sextets (counter x, y, z, w, key x, y) in
  * `in`, the four output words into `out`, and into `normals` the diamond-square displacement normal

@@ -81,14 +81,15 @@ DS_BLOCK = """
         m_options.scale && m_options.interp == DiamondSquareInterp::Bilinear &&
         tgb200_at_grid_spacing(*grid, spacing)) {
         std::vector<float> window;
-        tg_grid postGrid{};
+        int64_t col0 = 0, row0 = 0;
+        tg_grid lattice{};
         const tg_grid out = tgb200_grid(*grid);
-        if (tgb200_post_window(posts, *grid, 16, window, postGrid)) {
+        if (tgb200_post_window(posts, *grid, 16, window, col0, row0, lattice)) {
             const tg_ds_options o{*m_options.fractalDimension, *m_options.scale, 0,
                                   m_options.seed, m_options.minPixelSize};
-            if (tg_ds_refine(tgb200_device(), window.data(), postGrid.width, postGrid.height,
-                             &postGrid, &o, &out, grid->Values().data(), TG_MEMORY_HOST,
-                             nullptr) == TG_OK) {
+            if (tg_ds_refine_window(tgb200_device(), window.data(), col0, row0, lattice.width,
+                                    lattice.height, &lattice, &o, &out, grid->Values().data(),
+                                    TG_MEMORY_HOST, nullptr) == TG_OK) {
                 return;
             }
         }

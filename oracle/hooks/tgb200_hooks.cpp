@@ -2,6 +2,7 @@
 // into the drop-in build of the reference (oracle/_ref/libtgref_cuda.so).
 #include "tgb200_hooks.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <mutex>
@@ -62,7 +63,8 @@ bool tgb200_at_grid_spacing(const terraingen::Raster<float>& raster, double spac
 
 bool tgb200_post_window(const terraingen::PostLattice& lattice,
                         const terraingen::Raster<float>& raster, int margin,
-                        std::vector<float>& posts, tg_grid& grid) {
+                        std::vector<float>& posts, int64_t& first_col, int64_t& first_row,
+                        tg_grid& grid) {
     const terraingen::GeoTransform p = lattice.Transform();
     const terraingen::GeoTransform& r = raster.Transform();
     if (p.rowRotation != 0.0 || p.colRotation != 0.0 || r.rowRotation != 0.0 ||
@@ -76,15 +78,31 @@ bool tgb200_post_window(const terraingen::PostLattice& lattice,
     const double c1 = (std::fmax(xa, xb) - p.originX) / p.pixelWidth;
     const double r0 = (std::fmin(ya, yb) - p.originY) / p.pixelHeight;
     const double r1 = (std::fmax(ya, yb) - p.originY) / p.pixelHeight;
-    const int64_t col0 = int64_t(std::floor(std::fmin(c0, c1))) - margin;
-    const int64_t col1 = int64_t(std::ceil(std::fmax(c0, c1))) + margin;
-    const int64_t row0 = int64_t(std::floor(std::fmin(r0, r1))) - margin;
-    const int64_t row1 = int64_t(std::ceil(std::fmax(r0, r1))) + margin;
+    int64_t col0 = int64_t(std::floor(std::fmin(c0, c1))) - margin;
+    int64_t col1 = int64_t(std::ceil(std::fmax(c0, c1))) + margin;
+    int64_t row0 = int64_t(std::floor(std::fmin(r0, r1))) - margin;
+    int64_t row1 = int64_t(std::ceil(std::fmax(r0, r1))) + margin;
+    // A bounded lattice repeats its edge posts beyond its extent, as the device repeats the
+    // window's: the window stops at the extent.
+    if (const auto extent = lattice.Extent()) {
+        col0 = std::max(col0, int64_t(extent->colBegin));
+        col1 = std::min(col1, int64_t(extent->colEnd));
+        row0 = std::max(row0, int64_t(extent->rowBegin));
+        row1 = std::min(row1, int64_t(extent->rowEnd));
+        if (col0 >= col1 || row0 >= row1) {
+            col0 = std::min(col0, int64_t(extent->colEnd) - 1);
+            row0 = std::min(row0, int64_t(extent->rowEnd) - 1);
+            col1 = col0 + 1;
+            row1 = row0 + 1;
+        }
+    }
     const size_t width = size_t(col1 - col0), height = size_t(row1 - row0);
     posts.assign(width * height, 0.0f);
     lattice.Read(col0, row0, width, height, terraingen::Span<float>(posts.data(), posts.size()));
-    grid = tg_grid{uint32_t(width), uint32_t(height), p.originX + double(col0) * p.pixelWidth,
-                   p.pixelWidth, 0.0, p.originY + double(row0) * p.pixelHeight, 0.0,
-                   p.pixelHeight};
+    first_col = col0;
+    first_row = row0;
+    // The whole lattice's transform: its post (0, 0) anchors the refinement's node frame.
+    grid = tg_grid{uint32_t(width), uint32_t(height), p.originX, p.pixelWidth, 0.0, p.originY,
+                   0.0, p.pixelHeight};
     return true;
 }

@@ -29,8 +29,10 @@ tg_nodata tgb200_nodata(const terraingen::Raster<float>& raster);
 // Whether `spacing` is the raster's own cell size (the refinement's levels follow the spacing).
 bool tgb200_at_grid_spacing(const terraingen::Raster<float>& raster, double spacing);
 
-// The lattice's posts over the raster's bounds and `margin` posts around, into `posts` (row 0
-// north) on `grid`; false for a rotated lattice or raster.
+// The lattice's posts over the raster's bounds and `margin` posts around (within its extent,
+// for a bounded lattice), into `posts` (row 0 north): columns first_col.. and rows first_row.. of
+// the lattice, whose transform goes to `grid`; false for a rotated lattice or raster.
 bool tgb200_post_window(const terraingen::PostLattice& lattice,
                         const terraingen::Raster<float>& raster, int margin,
-                        std::vector<float>& posts, tg_grid& grid);
+                        std::vector<float>& posts, int64_t& first_col, int64_t& first_row,
+                        tg_grid& grid);

@@ -108,6 +108,8 @@ SIGNATURES.update({
     "tg_device_counters": [_P, _P, _SZ],
     "tg_ds_refine": [_P, _P, _U32, _U32, C.POINTER(Grid), C.POINTER(DsOptions), C.POINTER(Grid),
                      _P, _I, _P],
+    "tg_ds_refine_window": [_P, _P, C.c_int64, C.c_int64, _U32, _U32, C.POINTER(Grid),
+                            C.POINTER(DsOptions), C.POINTER(Grid), _P, _I, _P],
     "tg_philox_probe": [_P, _P, _U32, _P, _P],
     "tg_boulders_bake": [_P, _P, _U32, _D, C.POINTER(Grid), _P, NoData, _I, _P],
     "tg_boulders_bake_static": [_P, _U32, _D, C.POINTER(Grid), _P, NoData, _P, C.c_char_p, _SZ],

@@ -1232,6 +1232,14 @@ struct Box {
 int tg_ds_refine(tg_device* d, const float* posts, uint32_t pw, uint32_t ph,
                  const tg_grid* post_grid, const tg_ds_options* o, const tg_grid* grid,
                  float* heights, int memory, void* stream) {
+    return tg_ds_refine_window(d, posts, 0, 0, pw, ph, post_grid, o, grid, heights, memory,
+                               stream);
+}
+
+int tg_ds_refine_window(tg_device* d, const float* posts, int64_t col0, int64_t row0,
+                        uint32_t pw, uint32_t ph, const tg_grid* post_grid,
+                        const tg_ds_options* o, const tg_grid* grid, float* heights, int memory,
+                        void* stream) {
     if (int s = check_device(d)) {
         return s;
     }
@@ -1329,7 +1337,8 @@ int tg_ds_refine(tg_device* d, const float* posts, uint32_t pw, uint32_t ph,
     double* buffers[2] = {slot_ptr<double>(d, kDsLevelA), slot_ptr<double>(d, kDsLevelB)};
     const Box b0 = array_box(0);
     DsLevel current{b0.c0, b0.r0, b0.w(), b0.h(), buffers[0]};
-    TG_CUDA(launch_ds_base(static_cast<const float*>(dposts), pw, ph, current, s), "ds base");
+    TG_CUDA(launch_ds_base(static_cast<const float*>(dposts), col0, row0, pw, ph, current, s),
+            "ds base");
     // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
     const double stepFactor = std::pow(2.0, -(3.0 - o->fractal_dimension) / 2.0);
     for (int l = 1; l <= levels; ++l) {

@@ -75,18 +75,19 @@ __device__ __forceinline__ double at(const DsLevel& l, int64_t col, int64_t row)
 // Catmull-Rom weights of four nodes around a midpoint (diamond_square.cpp:37).
 __device__ __constant__ const double kMid[4] = {-1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0};
 
-// Level 0: node (col, row) is post (col, -row), reads past the lattice repeating its edge
-// (BaseNodes, diamond_square.cpp:308; PostIndex, src/sources/lattice.h:99).
-__global__ void ds_base_kernel(const float* __restrict__ posts, uint32_t pw, uint32_t ph,
-                               DsLevel out) {
+// Level 0: node (col, row) is post (col, -row), reads past the held posts repeating their edge
+// (BaseNodes, diamond_square.cpp:308; PostIndex, src/sources/lattice.h:99). The `pw` x `ph`
+// posts held are those of columns [col0, col0 + pw) and rows [row0, row0 + ph) of the lattice.
+__global__ void ds_base_kernel(const float* __restrict__ posts, int64_t col0, int64_t row0,
+                               uint32_t pw, uint32_t ph, DsLevel out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= out.w || j >= out.h) {
         return;
     }
-    const int64_t col = out.c0 + i, row = out.r0 + j;
+    const int64_t col = out.c0 + i - col0, row = -(out.r0 + j) - row0;
     const int64_t pc = col < 0 ? 0 : (col >= int64_t(pw) ? int64_t(pw) - 1 : col);
-    const int64_t pr = -row < 0 ? 0 : (-row >= int64_t(ph) ? int64_t(ph) - 1 : -row);
+    const int64_t pr = row < 0 ? 0 : (row >= int64_t(ph) ? int64_t(ph) - 1 : row);
     out.nodes[size_t(j) * out.w + i] = double(posts[size_t(pr) * pw + size_t(pc)]);
 }
 
@@ -248,10 +249,11 @@ dim3 blocks_for(uint32_t w, uint32_t h, dim3 block) {
 
 }  // namespace
 
-cudaError_t launch_ds_base(const float* posts, uint32_t pw, uint32_t ph, const DsLevel& out,
-                           cudaStream_t stream) {
+cudaError_t launch_ds_base(const float* posts, int64_t col0, int64_t row0, uint32_t pw,
+                           uint32_t ph, const DsLevel& out, cudaStream_t stream) {
     const dim3 block(32, 8);
-    ds_base_kernel<<<blocks_for(out.w, out.h, block), block, 0, stream>>>(posts, pw, ph, out);
+    ds_base_kernel<<<blocks_for(out.w, out.h, block), block, 0, stream>>>(posts, col0, row0, pw,
+                                                                          ph, out);
     return cudaGetLastError();
 }
 

@@ -200,8 +200,8 @@ struct DsFrame {
     double originX, originY, stepX, stepY;
 };
 
-cudaError_t launch_ds_base(const float* posts, uint32_t pw, uint32_t ph, const DsLevel& out,
-                           cudaStream_t stream);
+cudaError_t launch_ds_base(const float* posts, int64_t col0, int64_t row0, uint32_t pw,
+                           uint32_t ph, const DsLevel& out, cudaStream_t stream);
 // The square step over `out`'s whole box, then the diamond step over the inner box
 // [c0, c0 + w) x [r0, r0 + h), displacements scaled by `squareStep` and `diamondStep`.
 cudaError_t launch_ds_level(const DsLevel& parents, const DsLevel& out, int64_t c0, int64_t r0,

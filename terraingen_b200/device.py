@@ -257,9 +257,11 @@ class Device:
     # --- diamond-square -------------------------------------------------------------------
     def ds_refine(self, posts, post_grid: GridSpec, grid: GridSpec, heights,
                   fractal_dimension: float, scale: float, seed: int = 1, interp: int = 0,
-                  min_pixel_size: float = 0.0):
+                  min_pixel_size: float = 0.0, window=(0, 0)):
         """DiamondSquareUpsampler::FillSamples (diamond_square.cpp:488): `posts` [ph, pw] float32
-        on `post_grid`, refined and read at every cell of `grid` into `heights`."""
+        on `post_grid`, refined and read at every cell of `grid` into `heights`. With `window`
+        (col0, row0), `posts` are the lattice's columns col0.. and rows row0.. and `post_grid` the
+        whole lattice's (tg_ds_refine_window)."""
         b = _Buffers()
         if _is_torch(posts):
             ph, pw = posts.shape
@@ -270,8 +272,9 @@ class Device:
         h = b.ptr(heights, np.float32)
         o = N.DsOptions(fractal_dimension, scale, interp, seed, min_pixel_size)
         pg, g = post_grid.native(), grid.native()
-        N.check(self._lib.tg_ds_refine(self._handle, pp, pw, ph, C.byref(pg), C.byref(o),
-                                       C.byref(g), h, b.memory, _stream(b.memory)))
+        N.check(self._lib.tg_ds_refine_window(self._handle, pp, int(window[0]), int(window[1]),
+                                              pw, ph, C.byref(pg), C.byref(o), C.byref(g), h,
+                                              b.memory, _stream(b.memory)))
         return heights
 
     # --- seams ---------------------------------------------------------------------------

@@ -93,3 +93,35 @@ def test_ds_zero_scale_is_interpolation(device, fx):
     heights = np.zeros((grid.height, grid.width), np.float32)
     device.ds_refine(posts, pg, grid, heights, 2.2, 0.0, 1)
     assert heights.min() >= posts.min() - 1e-3 and heights.max() <= posts.max() + 1e-3
+
+
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+def test_ds_window_of_posts_matches_whole(device, fx, name):
+    # A 64^2 block inside the fixture's grid, refined from only the posts over its bounds and
+    # eight posts around (tg_ds_refine_window: the node frame still the whole lattice's), is the
+    # whole lattice's refinement of that block bit for bit.
+    import math
+
+    from terraingen_b200 import GridSpec
+
+    pg = grid_of(fx[f"{name}_post_grid"])
+    grid = grid_of(fx[f"{name}_grid"])
+    fd, scale, seed = fx[f"{name}_options"]
+    posts = fx[f"{name}_posts"]
+    block = GridSpec(64, 64, grid.x0 + 100 * grid.pixel, grid.y0 - 90 * grid.pixel, grid.pixel)
+    whole = np.zeros((64, 64), np.float32)
+    device.ds_refine(posts, pg, block, whole, fd, scale, int(seed))
+    c0 = max(0, math.floor((block.x0 - pg.x0) / pg.pixel) - 8)
+    c1 = min(pg.width, math.ceil((block.x0 + 64 * block.pixel - pg.x0) / pg.pixel) + 8)
+    r0 = max(0, math.floor((pg.y0 - block.y0) / pg.pixel) - 8)
+    r1 = min(pg.height, math.ceil((pg.y0 - block.y0 + 64 * block.pixel) / pg.pixel) + 8)
+    assert c0 > 0 and r0 > 0 and c1 < pg.width and r1 < pg.height
+    window = np.ascontiguousarray(posts[r0:r1, c0:c1])
+    part = np.zeros_like(whole)
+    device.ds_refine(window, pg, block, part, fd, scale, int(seed), window=(c0, r0))
+    assert np.array_equal(part.view(np.uint32), whole.view(np.uint32)), name
+    # The same posts passed as a lattice of their own draw other displacements.
+    alone = np.zeros_like(whole)
+    shifted = GridSpec(c1 - c0, r1 - r0, pg.x0 + c0 * pg.pixel, pg.y0 - r0 * pg.pixel, pg.pixel)
+    device.ds_refine(window, shifted, block, alone, fd, scale, int(seed))
+    assert not np.array_equal(alone, whole)
