@@ -922,7 +922,10 @@ def main():
     achieved = ops / (ms * 1e-3) / 1e12
     peak = alu_peak / 1e12
     nbins = ((w.grid.width + 31) // 32) * ((w.grid.height + 31) // 32)
-    launches = 1 + (3 + scan_launches(nbins)) * 2  # noise; count, scan, scatter, shape/bake x 2
+    # noise; craters: footprints, pair scan, count, bin scan, lean records, scatter, lean shape,
+    # extras pass; boulders: count, bin scan, scatter, bake.
+    launches = (1 + (6 + scan_launches(len(w.crater_records)) + scan_launches(nbins)) +
+                (3 + scan_launches(nbins)))
     cpu_value, cpu_per, cpu_n, cpu_grid = cpu_sample(1, 1, args.cpu_window)
     dropin = dropin_leg(args.cpu_window)
     line = {

@@ -145,7 +145,9 @@ int tg_noise_probe(tg_device* device, const float* xy, uint32_t n, uint32_t seed
  * `footprints` (optional; 3 doubles per crater: center x, y and reach in meters, as
  * CraterReach gives it) makes the footprint windows exactly the reference's; without it they
  * follow from the records. Craters with a datum are TG_ERROR_UNSUPPORTED here (their blend reads
- * the running height in apply order; tg_craters_apply_lists takes them). */
+ * the running height in apply order; tg_craters_apply_lists takes them), and the heights are left
+ * as they were. Binning, scatter and shaping are ordered on the stream with no round trip to the
+ * host; the call synchronizes once at the end to read its status. */
 int tg_craters_apply(tg_device* device, const void* kernel, size_t kernel_bytes,
                      const void* records, uint32_t n, const float* data, uint32_t n_data,
                      const double* footprints, const tg_grid* grid, float* heights,
@@ -290,7 +292,8 @@ typedef struct tg_terrain {
 /* Evaluates `terrain` on `grid` into `heights` (row-major, width x height floats): the source
  * fills, each layer applies in turn, all on the device; with host memory the layer inputs are
  * copied in once and the heights copied out once. Replaces Terrain::Evaluate / Fill for this
- * stack (src/pipeline/terrain.cpp:289-331). */
+ * stack (src/pipeline/terrain.cpp:289-331). The call synchronizes once, at the end (the layers'
+ * binning sizes itself on the device). On an error return the heights are unspecified. */
 int tg_evaluate(tg_device* device, const tg_terrain* terrain, const tg_grid* grid,
                 float* heights, int memory, void* stream);
 

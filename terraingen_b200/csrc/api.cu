@@ -216,7 +216,7 @@ int tg_open(int ordinal, tg_device** device) {
     d->name = prop.name;
     cudaError_t err = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
     if (err == cudaSuccess) {
-        err = cudaMallocHost(&d->pinnedStatus, 4 * sizeof(uint32_t));
+        err = cudaMallocHost(&d->pinnedStatus, 16 * sizeof(uint32_t));
     }
     if (err == cudaSuccess) {
         err = cudaStreamCreateWithFlags(&d->copyStream, cudaStreamNonBlocking);
@@ -517,15 +517,17 @@ int tg_noise_probe(tg_device* d, const float* xy, uint32_t n, uint32_t seed, uin
 
 namespace {
 
-// The crater pipeline on device buffers (count, scan, scatter, shape), on stream `s`. It reads
-// the number of binned entries back once to size the bins, and the status word at the end.
-// The crater pipeline's binning on stream `s` (count, scan, scatter, harmonics): what the shaping
-// launches need. `any` is false when no cell needs a crater.
+// The crater pipeline's binning on stream `s` (footprints, count, scan, lean craters, scatter):
+// what the shaping launches need, with no round trip to the host. The entries get the capacity
+// the device's slot already has (at least a guess from the craters and bins); when the scan's
+// total is larger the scatter and the shaping do nothing (crater_bins_usable) and layers_settle
+// grows the slot and asks for the layer again. `any` is false when no cell can need a crater.
 struct CraterPrep {
     CraterBins bins{};
     const void* leans = nullptr;  // the lean craters (plain kernel options), else null
-    bool extras = false;          // some crater needs the extras pass
+    bool extras = false;          // launch the extras pass (it returns at once without work)
     bool any = false;
+    size_t entryBytes = 0;
 };
 
 int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
@@ -566,29 +568,16 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
             "crater count launch");
     TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
             "scan launch");
-    // The entries needed and the datum flag, to size the bins.
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, bins.total + 1, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    const uint32_t total = d->pinnedStatus[0];
-    if (d->pinnedStatus[1] & 1u) {
-        return fail(TG_ERROR_UNSUPPORTED,
-                    "craters with a datum need the ordered form (tg_craters_apply_lists)");
-    }
-    if (total == 0) {
-        return TG_OK;
-    }
+    // The entries get the slot's capacity, at least a guess; a larger total is found on the
+    // device and settled after the layer.
     const bool lean = crater_lean_entries(k);
-    p.extras = (d->pinnedStatus[1] & 4u) != 0u;
-    TG_CUDA(d->slots[kBinEntries].reserve(size_t(total) *
-                                          (lean ? kLeanEntryBytes : sizeof(BinEntry))),
-            "allocation");
+    p.entryBytes = lean ? kLeanEntryBytes : sizeof(BinEntry);
+    const size_t guess = (lean ? 4 : 2) * size_t(n) + nbins;
+    const size_t have = d->slots[kBinEntries].bytes / p.entryBytes;
+    TG_CUDA(d->slots[kBinEntries].reserve(std::max(have, guess) * p.entryBytes), "allocation");
     bins.entries = slot_ptr<BinEntry>(d, kBinEntries);
-    bins.capacity = total;
+    bins.capacity = uint32_t(std::min<size_t>(d->slots[kBinEntries].bytes / p.entryBytes,
+                                              0xffffffffu));
     if (lean) {
         TG_CUDA(d->slots[kHarmonics].reserve(size_t(n) * kLeanCraterBytes), "allocation");
         p.leans = d->slots[kHarmonics].ptr;
@@ -596,45 +585,32 @@ int crater_prepare(tg_device* d, const CraterShapeKernel& k, const CraterRecord*
                 "lean crater launch");
     }
     TG_CUDA(launch_crater_scatter(k, rec, n, g, bins, p.leans, s), "crater scatter launch");
+    p.extras = lean;
     p.any = true;
     return TG_OK;
 }
 
-// After the shaping: its pair count and flags (waits for stream `s`).
+// The words a layer's settling reads, copied after its last kernel on stream `s`: for craters
+// the entries needed and the status (flags, pairs), for boulders the same at kBoulderWords.
+constexpr uint32_t kCraterWords = 0, kBoulderWords = 8;  // of tg_device::pinnedStatus's 16
+
 int crater_finish(tg_device* d, const CraterPrep& p, cudaStream_t s) {
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + 1, p.bins.total + 1, 3 * sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
+    const uint32_t nbins = p.bins.binsX * p.bins.binsY;
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + kCraterWords, p.bins.counts + nbins,
+                            sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
             "copy to host");
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    d->craterPairs = (static_cast<unsigned long long>(d->pinnedStatus[3]) << 32) |
-                     d->pinnedStatus[2];
-    if (d->pinnedStatus[1] & 2u) {
-        return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
-    }
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + kCraterWords + 1, p.bins.total + 1,
+                            3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+            "copy to host");
     return TG_OK;
 }
 
-int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
-                   const float* data, uint32_t nData, const double* foot, const Grid& g,
-                   float* dh, tg_nodata nodata, cudaStream_t s) {
-    CraterPrep p;
-    if (int st = crater_prepare(d, k, rec, n, data, nData, foot, g, s, p)) {
-        return st;
-    }
-    if (!p.any) {
-        return TG_OK;
-    }
-    TG_CUDA(launch_crater_shape(k, rec, data, p.leans, p.extras, g, to_nodata(nodata), p.bins, dh,
-                                s, 0, 0xffffffffu, d->waitPolls),
-            "crater shape launch");
-    return crater_finish(d, p, s);
-}
-
 // The boulder pipeline's binning on stream `s` (count, scan, scatter), its counts, cursor and
-// status in the given slots. `any` is false when no cell needs a boulder.
+// status in the given slots, sized as the craters' are (no round trip to the host; see
+// CraterPrep). `any` is false when no cell can need a boulder.
 struct BoulderPrep {
     BoulderBins bins{};
     uint32_t* status = nullptr;
@@ -657,9 +633,16 @@ int boulder_prepare(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
     TG_CUDA(d->slots[kBoulderWindows].reserve(size_t(n) * sizeof(int4)), "allocation");
     TG_CUDA(d->slots[kScan].reserve(scan_scratch_words(nbins) * sizeof(uint32_t)), "allocation");
     TG_CUDA(d->slots[statusSlot].reserve(4 * sizeof(uint32_t)), "allocation");
+    const size_t guess = 2 * size_t(n) + nbins;
+    const size_t have = d->slots[kBoulderEntries].bytes / sizeof(BoulderEntry);
+    TG_CUDA(d->slots[kBoulderEntries].reserve(std::max(have, guess) * sizeof(BoulderEntry)),
+            "allocation");
     bins.counts = slot_ptr<uint32_t>(d, countSlot);
     bins.cursor = slot_ptr<uint32_t>(d, cursorSlot);
     bins.windows = slot_ptr<int4>(d, kBoulderWindows);
+    bins.entries = slot_ptr<BoulderEntry>(d, kBoulderEntries);
+    bins.capacity = uint32_t(std::min<size_t>(
+        d->slots[kBoulderEntries].bytes / sizeof(BoulderEntry), 0xffffffffu));
     p.status = slot_ptr<uint32_t>(d, statusSlot);
     TG_CUDA(cudaMemsetAsync(bins.counts, 0, (size_t(nbins) + 1) * sizeof(uint32_t), s), "memset");
     TG_CUDA(cudaMemsetAsync(bins.cursor, 0, size_t(nbins) * sizeof(uint32_t), s), "memset");
@@ -667,53 +650,123 @@ int boulder_prepare(tg_device* d, const BoulderRecord* rec, uint32_t n, double w
     TG_CUDA(launch_boulder_count(rec, n, g, width, bins, s), "boulder count launch");
     TG_CUDA(launch_exclusive_scan(bins.counts, nbins, slot_ptr<uint32_t>(d, kScan), s),
             "scan launch");
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, bins.counts + nbins, sizeof(uint32_t),
-                            cudaMemcpyDeviceToHost, s),
-            "copy to host");
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    const uint32_t total = d->pinnedStatus[0];
-    if (total == 0) {
-        return TG_OK;
-    }
-    TG_CUDA(d->slots[kBoulderEntries].reserve(size_t(total) * sizeof(BoulderEntry)), "allocation");
-    bins.entries = slot_ptr<BoulderEntry>(d, kBoulderEntries);
-    bins.capacity = total;
     TG_CUDA(launch_boulder_scatter(rec, n, bins, s), "boulder scatter launch");
     p.any = true;
     return TG_OK;
 }
 
-// After the bake: its pair count and flags (waits for stream `s`).
 int boulder_finish(tg_device* d, const BoulderPrep& p, cudaStream_t s) {
     if (!p.any) {
         return TG_OK;
     }
-    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, p.status, 4 * sizeof(uint32_t),
+    const uint32_t nbins = p.bins.binsX * p.bins.binsY;
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + kBoulderWords, p.bins.counts + nbins,
+                            sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus + kBoulderWords + 1, p.status, 4 * sizeof(uint32_t),
                             cudaMemcpyDeviceToHost, s),
             "copy to host");
-    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
-    d->boulderPairs = (static_cast<unsigned long long>(d->pinnedStatus[3]) << 32) |
-                      d->pinnedStatus[2];
-    if (d->pinnedStatus[0] & 2u) {
-        return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
+    return TG_OK;
+}
+
+// After the layers' streams are synchronized: their pair counts and errors, and whether a layer's
+// entries outgrew their capacity (`again`: its slot is grown to the total and the caller runs the
+// layers again from the heights they started from).
+int layers_settle(tg_device* d, const CraterPrep* cp, const BoulderPrep* bp, bool& again) {
+    again = false;
+    const uint32_t* w = d->pinnedStatus;
+    if (cp != nullptr && cp->any) {
+        const uint32_t needed = w[kCraterWords], flags = w[kCraterWords + 1];
+        if (flags & 1u) {
+            return fail(TG_ERROR_UNSUPPORTED,
+                        "craters with a datum need the ordered form (tg_craters_apply_lists)");
+        }
+        if (needed > cp->bins.capacity) {
+            TG_CUDA(d->slots[kBinEntries].reserve(size_t(needed) * cp->entryBytes), "allocation");
+            again = true;
+        } else {
+            if (flags & 2u) {
+                return fail(TG_ERROR_TIMEOUT, "a crater bin's staged copy did not arrive");
+            }
+            d->craterPairs = (static_cast<unsigned long long>(w[kCraterWords + 3]) << 32) |
+                             w[kCraterWords + 2];
+        }
+    }
+    if (bp != nullptr && bp->any) {
+        const uint32_t needed = w[kBoulderWords];
+        const uint32_t* status = w + kBoulderWords + 1;
+        if (needed > bp->bins.capacity) {
+            TG_CUDA(d->slots[kBoulderEntries].reserve(size_t(needed) * sizeof(BoulderEntry)),
+                    "allocation");
+            again = true;
+        } else {
+            if (status[0] & 2u) {
+                return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
+            }
+            d->boulderPairs = (static_cast<unsigned long long>(status[3]) << 32) | status[2];
+        }
     }
     return TG_OK;
 }
 
-// The boulder pipeline on device buffers (count, scan, scatter, bake), on stream `s`.
+// The crater layer on device heights `dh` (stream `s`): binning, shaping and one synchronize at
+// the end; again once with grown entries when they did not fit (the heights are untouched then).
+int craters_device(tg_device* d, const CraterShapeKernel& k, const CraterRecord* rec, uint32_t n,
+                   const float* data, uint32_t nData, const double* foot, const Grid& g,
+                   float* dh, tg_nodata nodata, cudaStream_t s) {
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        CraterPrep p;
+        if (int st = crater_prepare(d, k, rec, n, data, nData, foot, g, s, p)) {
+            return st;
+        }
+        if (!p.any) {
+            return TG_OK;
+        }
+        TG_CUDA(launch_crater_shape(k, rec, data, p.leans, p.extras, g, to_nodata(nodata),
+                                    p.bins, dh, s, 0, 0xffffffffu, d->waitPolls),
+                "crater shape launch");
+        if (int st = crater_finish(d, p, s)) {
+            return st;
+        }
+        TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+        bool again = false;
+        if (int st = layers_settle(d, &p, nullptr, again)) {
+            return st;
+        }
+        if (!again) {
+            return TG_OK;
+        }
+    }
+    return fail(TG_ERROR_MEMORY, "the crater entries did not fit after growing");
+}
+
+// The boulder pipeline on device heights (count, scan, scatter, bake), as craters_device.
 int boulders_device(tg_device* d, const BoulderRecord* rec, uint32_t n, double width,
                     const Grid& g, float* dh, tg_nodata nodata, cudaStream_t s) {
-    BoulderPrep p;
-    if (int st = boulder_prepare(d, rec, n, width, g, s, kCounts, kCursor, kStatus, p)) {
-        return st;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        BoulderPrep p;
+        if (int st = boulder_prepare(d, rec, n, width, g, s, kCounts, kCursor, kStatus, p)) {
+            return st;
+        }
+        if (!p.any) {
+            return TG_OK;
+        }
+        TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), p.bins, dh, p.status, s, 0,
+                                    0xffffffffu, d->waitPolls),
+                "boulder bake launch");
+        if (int st = boulder_finish(d, p, s)) {
+            return st;
+        }
+        TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+        bool again = false;
+        if (int st = layers_settle(d, nullptr, &p, again)) {
+            return st;
+        }
+        if (!again) {
+            return TG_OK;
+        }
     }
-    if (!p.any) {
-        return TG_OK;
-    }
-    TG_CUDA(launch_boulder_bake(g, width, to_nodata(nodata), p.bins, dh, p.status, s, 0,
-                                0xffffffffu, d->waitPolls),
-            "boulder bake launch");
-    return boulder_finish(d, p, s);
+    return fail(TG_ERROR_MEMORY, "the boulder entries did not fit after growing");
 }
 
 int check_boulders(const void* boulders, uint32_t n) {
@@ -1093,11 +1146,17 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     }
     // Terrain::Fill: the source, then each layer in order (src/pipeline/terrain.cpp:299-331).
     const Positions origin{0.0, 0.0, nullptr, nullptr};
-    TG_CUDA(launch_noise(source, g, origin, true, t->elevation, NoData{0u, 0.0f}, dh, s),
-            "noise source launch");
-    if (t->noise_layer != nullptr) {
-        TG_CUDA(launch_noise(layer, g, origin, false, 0.0f, NoData{0u, 0.0f}, dh, s),
-                "noise layer launch");
+    auto sources = [&]() -> int {
+        TG_CUDA(launch_noise(source, g, origin, true, t->elevation, NoData{0u, 0.0f}, dh, s),
+                "noise source launch");
+        if (t->noise_layer != nullptr) {
+            TG_CUDA(launch_noise(layer, g, origin, false, 0.0f, NoData{0u, 0.0f}, dh, s),
+                    "noise layer launch");
+        }
+        return TG_OK;
+    };
+    if (int st = sources()) {
+        return st;
     }
     // Host-memory layer inputs are copied on the device's copy stream while the source's
     // kernels run; the layers wait for them.
@@ -1130,32 +1189,44 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
         TG_CUDA(cudaEventRecord(d->copied, d->copyStream), "event");
         TG_CUDA(cudaStreamWaitEvent(s, d->copied, 0), "event wait");
     }
-    if (memory == TG_MEMORY_HOST && (t->n_craters > 0 || t->n_boulders > 0)) {
-        // The layers by strips of bin rows, each strip copied out on the copy stream while the
-        // next is shaped and baked.
+    const bool layers = t->n_craters > 0 || t->n_boulders > 0;
+    if (!layers) {
+        return copy_heights_back(d, memory, heights, dh, cells);
+    }
+    // The layers, then one synchronize; when a layer's binned entries outgrew their capacity the
+    // kernels after its scan did nothing, and the whole evaluation runs again with grown entries.
+    const NoData none{0u, 0.0f};
+    auto drain = [&](int st) {
+        cudaStreamSynchronize(d->copyStream);
+        return st;
+    };
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if (attempt > 0) {
+            if (int st = sources()) {
+                return st;
+            }
+        }
         CraterPrep cp;
         BoulderPrep bp;
-        auto drain = [&](int st) {
-            cudaStreamSynchronize(d->copyStream);
-            return st;
-        };
         if (t->n_craters > 0) {
-            if (int st = crater_prepare(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,
-                                        static_cast<const float*>(ddata), t->n_crater_data,
-                                        static_cast<const double*>(dfoot), g, s, cp)) {
+            if (int st = crater_prepare(d, k, static_cast<const CraterRecord*>(drec),
+                                        t->n_craters, static_cast<const float*>(ddata),
+                                        t->n_crater_data, static_cast<const double*>(dfoot), g,
+                                        s, cp)) {
                 return st;
             }
         }
         if (t->n_boulders > 0) {
-            if (int st = boulder_prepare(d, static_cast<const BoulderRecord*>(db), t->n_boulders,
-                                         t->boulder_width, g, s, kBoulderCounts, kBoulderCursor,
-                                         kBoulderStatus, bp)) {
+            if (int st = boulder_prepare(d, static_cast<const BoulderRecord*>(db),
+                                         t->n_boulders, t->boulder_width, g, s, kBoulderCounts,
+                                         kBoulderCursor, kBoulderStatus, bp)) {
                 return st;
             }
         }
-        const NoData none{0u, 0.0f};
+        // Host memory: the layers by strips of bin rows, each strip copied out on the copy
+        // stream while the next is shaped and baked. Device memory: one launch per layer.
         const uint32_t binRows = (g.height + kBinCells - 1) / kBinCells;
-        const uint32_t strips = std::min<uint32_t>(8u, binRows);
+        const uint32_t strips = memory == TG_MEMORY_HOST ? std::min<uint32_t>(8u, binRows) : 1u;
         const uint32_t per = (binRows + strips - 1) / strips;
         for (uint32_t k0 = 0, q = 0; k0 < binRows; k0 += per, ++q) {
             const uint32_t rows = std::min(per, binRows - k0);
@@ -1173,6 +1244,9 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
                     return drain(cuda_fail(e, "boulder bake launch"));
                 }
             }
+            if (memory != TG_MEMORY_HOST) {
+                continue;
+            }
             const size_t y0 = size_t(k0) * kBinCells;
             const size_t y1 = std::min<size_t>(size_t(k0 + rows) * kBinCells, g.height);
             cudaError_t e = cudaEventRecord(d->strips[q], s);
@@ -1188,30 +1262,23 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
                 return drain(cuda_fail(e, "strip copy to host"));
             }
         }
-        if (int st = drain(crater_finish(d, cp, s))) {
-            return st;
+        if (int st = crater_finish(d, cp, s)) {
+            return drain(st);
         }
         if (int st = boulder_finish(d, bp, s)) {
-            return st;
+            return drain(st);
         }
+        TG_CUDA(cudaStreamSynchronize(s), "synchronize");
         TG_CUDA(cudaStreamSynchronize(d->copyStream), "synchronize");
-        return TG_OK;
-    }
-    if (t->n_craters > 0) {
-        if (int st = craters_device(d, k, static_cast<const CraterRecord*>(drec), t->n_craters,
-                                    static_cast<const float*>(ddata), t->n_crater_data,
-                                    static_cast<const double*>(dfoot), g, dh, tg_nodata{0u, 0.0f},
-                                    s)) {
+        bool again = false;
+        if (int st = layers_settle(d, &cp, &bp, again)) {
             return st;
         }
-    }
-    if (t->n_boulders > 0) {
-        if (int st = boulders_device(d, static_cast<const BoulderRecord*>(db), t->n_boulders,
-                                     t->boulder_width, g, dh, tg_nodata{0u, 0.0f}, s)) {
-            return st;
+        if (!again) {
+            return TG_OK;
         }
     }
-    return copy_heights_back(d, memory, heights, dh, cells);
+    return fail(TG_ERROR_MEMORY, "the layers' entries did not fit after growing");
 }
 
 namespace {

@@ -113,7 +113,7 @@ struct tg_device {
     std::mutex mutex;
     std::string name;
     tgb::api::Buffer slots[tgb::api::kSlotCount];
-    uint32_t* pinnedStatus = nullptr;  // host-pinned words read back after shaping
+    uint32_t* pinnedStatus = nullptr;  // 16 host-pinned words read back after the layers
     // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
     unsigned long long craterPairs = 0, boulderPairs = 0;
     // Polls of a staged copy before the binned kernels give up on it (tg_set_wait_limit).

@@ -109,6 +109,18 @@ __host__ __device__ inline bool crater_options_plain(const CraterShapeKernel& k)
            k.mantling == 0.0f;
 }
 
+// Whether a layer's binned entries fit the capacity the host gave them (the scan's total is in
+// counts[bins]) and, for craters, none needs the ordered form (flag 1: a datum). The kernels after
+// the scan do nothing otherwise; after the layer the host reads the total and the flags, grows the
+// entries and runs the layer again (or reports the datum), so that binning needs no round trip to
+// the host between the scan and the scatter.
+__device__ __forceinline__ bool crater_bins_usable(const CraterBins& b) {
+    return __ldg(b.counts + b.binsX * b.binsY) <= b.capacity && (b.total[1] & 1u) == 0u;
+}
+__device__ __forceinline__ bool boulder_bins_usable(const BoulderBins& b) {
+    return __ldg(b.counts + b.binsX * b.binsY) <= b.capacity;
+}
+
 // Whether crater `r` shapes as a complex crater (FreshProfileHeight, craters.h:500).
 __host__ __device__ inline bool crater_is_complex(const CraterShapeKernel& k,
                                                   const CraterRecord& r) {

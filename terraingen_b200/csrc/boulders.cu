@@ -50,7 +50,7 @@ __global__ void boulder_count_kernel(const BoulderRecord* __restrict__ boulders,
 __global__ void boulder_scatter_kernel(const BoulderRecord* __restrict__ boulders, uint32_t n,
                                        BoulderBins bins) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) {
+    if (i >= n || !boulder_bins_usable(bins)) {
         return;
     }
     const int4 w = bins.windows[i];
@@ -89,17 +89,15 @@ __global__ void __launch_bounds__(kThreads, 4)
     __shared__ __align__(128) BoulderEntry stage[2][kChunk];
     __shared__ __align__(8) uint64_t bars[2];
     const uint32_t bin = bins.firstBin + blockIdx.x;
-    uint32_t first = bins.counts[bin];
-    uint32_t end = bins.counts[bin + 1];
-    if (end > bins.capacity) {
-        // Entries past the capacity were never scattered: bake what is there and flag it.
-        if (threadIdx.x == 0) {
+    if (!boulder_bins_usable(bins)) {
+        // The entries were not scattered: nothing is baked, the host grows them and runs again.
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
             atomicOr(flags, 4u);
         }
-        end = bins.capacity;
-        first = min(first, end);
+        return;
     }
-    const uint32_t count = end - first;
+    const uint32_t first = bins.counts[bin];
+    const uint32_t count = bins.counts[bin + 1] - first;
     if (count == 0u) {
         return;
     }

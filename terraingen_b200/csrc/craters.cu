@@ -137,6 +137,9 @@ __global__ void crater_bin_scatter_kernel(const CraterShapeKernel k,
                                           const CraterRecord* __restrict__ records, uint32_t n,
                                           const crater::LeanCrater* __restrict__ leans,
                                           const Grid grid, CraterBins bins) {
+    if (!crater_bins_usable(bins)) {
+        return;
+    }
     const uint32_t pairs = bins.pairStart[n];
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
          p += gridDim.x * blockDim.x) {
@@ -146,7 +149,7 @@ __global__ void crater_bin_scatter_kernel(const CraterShapeKernel k,
         const uint32_t b = by * bins.binsX + bx;
         const uint32_t slot = bins.counts[b] + atomicAdd(bins.cursor + b, 1u);
         if (slot >= bins.capacity) {
-            continue;  // the host sized the entries from the counts; never taken
+            continue;  // the total fits the capacity (checked above); never taken
         }
         const CraterRecord& r = records[crater];
         if (leans != nullptr) {
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kShapeThreads)
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
     const uint32_t first = bins.counts[bin];
     const uint32_t count = bins.counts[bin + 1] - first;
-    if (count == 0u) {
+    if (count == 0u || !crater_bins_usable(bins)) {
         return;
     }
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -625,7 +628,7 @@ __global__ void __launch_bounds__(kShapeThreads, 3)
     const uint32_t binX = bin % bins.binsX, binY = bin / bins.binsX;
     const uint32_t first = bins.counts[bin];
     const uint32_t count = bins.counts[bin + 1] - first;
-    if (count == 0u) {
+    if (count == 0u || !crater_bins_usable(bins)) {
         return;
     }
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -742,6 +745,9 @@ __global__ void __launch_bounds__(kShapeThreads)
                          const crater::LeanCrater* __restrict__ leans, const Grid grid,
                          const NoData nodata, const CraterBins bins, uint32_t binsInStrip,
                          float* __restrict__ heights) {
+    if ((bins.total[1] & 4u) == 0u || !crater_bins_usable(bins)) {
+        return;  // no heavy record nor massif peak in the layer
+    }
     const uint32_t listed = bins.extrasList[0];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     for (uint32_t item = blockIdx.x; item < listed; item += gridDim.x) {

@@ -150,20 +150,8 @@ extern "C" int tg_boulders_bake_static(const void* boulders, uint32_t n, double 
         cudaGetLastError();
         return fail(TG_ERROR_CUDA, "a launch of the static bake failed");
     }
-    // The binned entries the boulders need, read back before anything is written: beyond the
-    // scratch's capacity the call stops here and leaves the heights as they were.
-    uint32_t total = 0;
-    if (cudaMemcpyAsync(&total, bins.counts + nbins, sizeof(total), cudaMemcpyDeviceToHost, s) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(TG_ERROR_CUDA, "reading the static bake's entry count failed");
-    }
-    if (total > kStaticMaxEntries) {
-        return fail(TG_ERROR_MEMORY,
-                    "the boulders cover more bin entries than the static scratch holds (196608); "
-                    "the heights are unchanged");
-    }
+    // Beyond the scratch's capacity (the scan's total, checked on the device) the scatter and the
+    // bake write nothing and the bake sets flag 4, so the heights are left as they were.
     const NoData nd{nodata.mode, nodata.value};
     if (launch_boulder_scatter(rec, n, bins, s) != cudaSuccess ||
         launch_boulder_bake(g, width, nd, bins, heights, status, s) != cudaSuccess) {
@@ -175,6 +163,11 @@ extern "C" int tg_boulders_bake_static(const void* boulders, uint32_t n, double 
         cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         return fail(TG_ERROR_CUDA, "reading the static bake's status failed");
+    }
+    if (flags & 4u) {
+        return fail(TG_ERROR_MEMORY,
+                    "the boulders cover more bin entries than the static scratch holds (196608); "
+                    "the heights are unchanged");
     }
     if (flags & 2u) {
         return fail(TG_ERROR_TIMEOUT, "a boulder bin's staged copy did not arrive");
