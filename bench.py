@@ -660,11 +660,11 @@ def dem_accuracy(dev):
 
     out = {}
     ds = np.load(ROOT / "tests" / "golden" / "ds.npz")
-    for name in ("dem5m", "tenfold"):
+    for name in ("dem5m", "tenfold", "tenfold_cr"):
         pg, g = grid_of(ds[f"{name}_post_grid"]), grid_of(ds[f"{name}_grid"])
-        fd, scale, seed = ds[f"{name}_options"]
+        fd, scale, seed, interp = ds[f"{name}_options"]
         h = np.zeros((g.height, g.width), np.float32)
-        dev.ds_refine(ds[f"{name}_posts"], pg, g, h, fd, scale, int(seed))
+        dev.ds_refine(ds[f"{name}_posts"], pg, g, h, fd, scale, int(seed), int(interp))
         out[f"diamond_square_{name}"] = error(h, ds[f"{name}_expected"])
     z = np.load(ROOT / "tests" / "golden" / "chain.npz")
     g = grid_of(z["grid"])

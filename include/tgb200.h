@@ -226,8 +226,9 @@ int tg_boulders_bake_static(const void* boulders, uint32_t n, double width, cons
 
 /* DiamondSquareOptions (include/terraingen/sources/diamond_square.h:26-33) with a given scale:
  * fractal dimension D in [2, 3] (the displacement shrinks by 2^-((3 - D) / 2) per step), scale Se
- * (m), interp 0 bilinear (1 Catmull-Rom is TG_ERROR_UNSUPPORTED for now), seed, and
- * min_pixel_size (m; 0 for none) capping the levels. */
+ * (m), interp 0 bilinear or 1 Catmull-Rom (DiamondSquareInterp: Catmull-Rom midpoint means in
+ * both steps and a Keys cubic read), seed, and min_pixel_size (m; 0 for none) capping the
+ * levels. */
 typedef struct tg_ds_options {
     double fractal_dimension;
     double scale;
@@ -239,8 +240,8 @@ typedef struct tg_ds_options {
 /* DiamondSquareUpsampler::FillSamples on a grid (src/sources/diamond_square.cpp:488-516), which
  * the reference runs only on the CPU: the `pw` x `ph` float posts on `post_grid` (row 0 north,
  * reads past the edge repeating it) refined Levels(post spacing, grid spacing) times and read
- * bilinearly at every cell of `grid` into `heights`. Nodes are doubles in device memory; the finest
- * two levels are resident at once (8 bytes per node). */
+ * at every cell of `grid` into `heights`. Nodes are doubles; each block of output cells refines
+ * the nodes it reads in on-chip memory, so only the heights are written to device memory. */
 int tg_ds_refine(tg_device* device, const float* posts, uint32_t pw, uint32_t ph,
                  const tg_grid* post_grid, const tg_ds_options* options, const tg_grid* grid,
                  float* heights, int memory, void* stream);

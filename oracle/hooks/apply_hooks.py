@@ -74,18 +74,19 @@ HOOKS = [
 
 DS_OPEN_TAIL = "                                         double spacing, unsigned threads) const {"
 DS_BLOCK = """
-    // libtgb200: bilinear refinement of a grid at the grid's own spacing, with F and the scale
-    // given, on the device; the posts it reads come from the lattice with a margin.
+    // libtgb200: refinement of a grid at the grid's own spacing, with F and the scale given, on
+    // the device; the posts it reads come from the lattice with a margin.
     if (Raster<float>* grid = samples.Grid();
         grid != nullptr && tgb200_hooks_active() && m_options.fractalDimension &&
-        m_options.scale && m_options.interp == DiamondSquareInterp::Bilinear &&
-        tgb200_at_grid_spacing(*grid, spacing)) {
+        m_options.scale && tgb200_at_grid_spacing(*grid, spacing)) {
         std::vector<float> window;
         int64_t col0 = 0, row0 = 0;
         tg_grid lattice{};
         const tg_grid out = tgb200_grid(*grid);
         if (tgb200_post_window(posts, *grid, 16, window, col0, row0, lattice)) {
-            const tg_ds_options o{*m_options.fractalDimension, *m_options.scale, 0,
+            const uint32_t interp =
+                m_options.interp == DiamondSquareInterp::CatmullRom ? 1u : 0u;
+            const tg_ds_options o{*m_options.fractalDimension, *m_options.scale, interp,
                                   m_options.seed, m_options.minPixelSize};
             if (tg_ds_refine_window(tgb200_device(), window.data(), col0, row0, lattice.width,
                                     lattice.height, &lattice, &o, &out, grid->Values().data(),

@@ -1283,16 +1283,44 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
 
 namespace {
 
-int64_t host_floor_half(int64_t v) {
-    return v >= 0 ? v / 2 : -((1 - v) / 2);
-}
+// The output block of a diamond-square CTA and the shared buffers its node pyramid needs: the
+// largest side in 64, 32, ..., 1 whose two buffers fit kDsSharedBudget bytes. Each level's box is
+// bounded from the block's extent in finest nodes (what the device works out, plus two nodes for
+// the rounding of either side's arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
+// its parents' box is half of it plus the square mean's margins.
+constexpr size_t kDsSharedBudget = 100 * 1024;
 
-struct Box {
-    int64_t c0, c1, r0, r1;  // inclusive
-    uint32_t w() const { return uint32_t(c1 - c0 + 1); }
-    uint32_t h() const { return uint32_t(r1 - r0 + 1); }
-    size_t size() const { return size_t(w()) * h(); }
-};
+bool ds_tile_shape(DsTile& t, bool spline) {
+    const int64_t reach = spline ? 3 : 1, before = spline ? 1 : 0, after = spline ? 2 : 1;
+    const Grid& g = t.grid;
+    for (uint32_t side = 64; side >= 1; side /= 2) {
+        const double spanX = double(side - 1) * (std::fabs(g.pixelWidth) + std::fabs(g.rowRotation)) /
+                             std::fabs(t.frame.stepX);
+        const double spanY = double(side - 1) * (std::fabs(g.colRotation) + std::fabs(g.pixelHeight)) /
+                             std::fabs(t.frame.stepY);
+        if (!(spanX < 4096.0 && spanY < 4096.0)) {
+            continue;
+        }
+        int64_t w = int64_t(std::floor(spanX)) + 6 + after;
+        int64_t h = int64_t(std::floor(spanY)) + 6 + after;
+        uint64_t cap[2] = {0, 0};
+        for (int l = t.levels; l >= 1; --l) {
+            const int64_t ow = w + 2 * reach, oh = h + 2 * reach;
+            cap[l & 1] = std::max<uint64_t>(cap[l & 1], uint64_t(ow * oh));
+            w = ow / 2 + before + after + 1;
+            h = oh / 2 + before + after + 1;
+        }
+        cap[0] = std::max<uint64_t>(cap[0], uint64_t(w * h));
+        if ((cap[0] + cap[1]) * sizeof(double) <= kDsSharedBudget) {
+            t.block = side;
+            t.blocksX = (g.width + side - 1) / side;
+            t.capEven = uint32_t(cap[0]);
+            t.capOdd = uint32_t(cap[1]);
+            return true;
+        }
+    }
+    return false;
+}
 
 }  // namespace
 
@@ -1328,8 +1356,8 @@ int tg_ds_refine_window(tg_device* d, const float* posts, int64_t col0, int64_t 
         !std::isfinite(o->scale) || !(o->min_pixel_size >= 0.0)) {
         return fail(TG_ERROR_ARGUMENT, "fractal dimension in [2, 3], scale and min pixel size >= 0");
     }
-    if (o->interp != 0u) {
-        return fail(TG_ERROR_UNSUPPORTED, "Catmull-Rom diamond-square is not supported yet");
+    if (o->interp > 1u) {
+        return fail(TG_ERROR_ARGUMENT, "interp is 0 (bilinear) or 1 (Catmull-Rom)");
     }
     const size_t cells = size_t(g.width) * g.height;
     if (cells == 0) {
@@ -1352,79 +1380,55 @@ int tg_ds_refine_window(tg_device* d, const float* posts, int64_t col0, int64_t 
         }
         levels = int(std::min(std::ceil(std::log2(ratio) - 1e-9), most));
     }
-    // Frame (diamond_square.cpp:299-306): post (0, 0)'s center and the node steps.
-    DsFrame frame;
-    frame.originX = pg.originX + 0.5 * pg.pixelWidth + 0.5 * pg.rowRotation;
-    frame.originY = pg.originY + 0.5 * pg.colRotation + 0.5 * pg.pixelHeight;
-    frame.stepX = std::ldexp(pg.pixelWidth, -levels);
-    frame.stepY = std::ldexp(-pg.pixelHeight, -levels);
-    // The finest nodes the read-out touches, with a node to spare on every side.
-    auto node_range = [](double a, double b, int64_t& lo, int64_t& hi) {
-        lo = int64_t(std::floor(std::min(a, b))) - 1;
-        hi = int64_t(std::ceil(std::max(a, b))) + 1;
-    };
-    const double x0 = g.originX + 0.5 * g.pixelWidth, x1 = g.originX + (g.width - 0.5) * g.pixelWidth;
-    const double y0 = g.originY + 0.5 * g.pixelHeight,
-                 y1 = g.originY + (g.height - 0.5) * g.pixelHeight;
-    std::vector<Box> inner(levels + 1);
-    node_range((x0 - frame.originX) / frame.stepX, (x1 - frame.originX) / frame.stepX,
-               inner[levels].c0, inner[levels].c1);
-    node_range((y0 - frame.originY) / frame.stepY, (y1 - frame.originY) / frame.stepY,
-               inner[levels].r0, inner[levels].r1);
-    const int64_t reach = 1;
-    for (int l = levels; l >= 1; --l) {
-        const Box outer{inner[l].c0 - reach, inner[l].c1 + reach, inner[l].r0 - reach,
-                        inner[l].r1 + reach};
-        inner[l - 1] = Box{host_floor_half(outer.c0) - 2, host_floor_half(outer.c1) + 3,
-                           host_floor_half(outer.r0) - 2, host_floor_half(outer.r1) + 3};
+    // Frame (diamond_square.cpp:299-306): post (0, 0)'s center and the finest node steps.
+    const bool spline = o->interp == 1u;
+    DsTile t{};
+    t.grid = g;
+    t.frame.originX = pg.originX + 0.5 * pg.pixelWidth + 0.5 * pg.rowRotation;
+    t.frame.originY = pg.originY + 0.5 * pg.colRotation + 0.5 * pg.pixelHeight;
+    t.frame.stepX = std::ldexp(pg.pixelWidth, -levels);
+    t.frame.stepY = std::ldexp(-pg.pixelHeight, -levels);
+    t.levels = levels;
+    t.seed = o->seed;
+    // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
+    const double stepFactor = std::pow(2.0, -(3.0 - o->fractal_dimension) / 2.0);
+    for (int l = 1; l <= levels; ++l) {
+        t.squareStep[l] = o->scale * std::pow(stepFactor, 2 * l - 1);
+        t.diamondStep[l] = o->scale * std::pow(stepFactor, 2 * l);
     }
-    auto array_box = [&](int l) {
-        return l == 0 ? inner[0]
-                      : Box{inner[l].c0 - reach, inner[l].c1 + reach, inner[l].r0 - reach,
-                            inner[l].r1 + reach};
-    };
-    size_t most = 0;
-    for (int l = 0; l <= levels; ++l) {
-        const Box b = array_box(l);
-        if (b.w() > (1u << 30) || b.h() > (1u << 30)) {
-            return fail(TG_ERROR_ARGUMENT, "the refined node grid is too large");
-        }
-        most = std::max(most, b.size());
+    if (!ds_tile_shape(t, spline)) {
+        return fail(TG_ERROR_ARGUMENT, "the output cells are too coarse for the posts' nodes");
     }
     const cudaStream_t s = stream_of(d, memory, stream);
     const void* dposts = nullptr;
     if (int st = stage_in(d, memory, kDsPosts, posts, size_t(pw) * ph * sizeof(float), &dposts)) {
         return st;
     }
-    if (d->slots[kDsLevelA].reserve(most * sizeof(double)) != cudaSuccess ||
-        d->slots[kDsLevelB].reserve(most * sizeof(double)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(TG_ERROR_MEMORY, "no room for two levels of %zu nodes", most);
-    }
-    double* buffers[2] = {slot_ptr<double>(d, kDsLevelA), slot_ptr<double>(d, kDsLevelB)};
-    const Box b0 = array_box(0);
-    DsLevel current{b0.c0, b0.r0, b0.w(), b0.h(), buffers[0]};
-    TG_CUDA(launch_ds_base(static_cast<const float*>(dposts), col0, row0, pw, ph, current, s),
-            "ds base");
-    // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
-    const double stepFactor = std::pow(2.0, -(3.0 - o->fractal_dimension) / 2.0);
-    for (int l = 1; l <= levels; ++l) {
-        const Box b = array_box(l);
-        DsLevel next{b.c0, b.r0, b.w(), b.h(), buffers[l & 1]};
-        const double squareStep = o->scale * std::pow(stepFactor, 2 * l - 1);
-        const double diamondStep = o->scale * std::pow(stepFactor, 2 * l);
-        TG_CUDA(launch_ds_level(current, next, inner[l].c0, inner[l].r0, inner[l].w(), inner[l].h(),
-                                l, squareStep, diamondStep, o->seed, false, s),
-                "ds level");
-        current = next;
-    }
+    t.posts = static_cast<const float*>(dposts);
+    t.col0 = col0;
+    t.row0 = row0;
+    t.pw = pw;
+    t.ph = ph;
     float* dh = heights;
     if (memory == TG_MEMORY_HOST) {
         TG_CUDA(d->slots[kHeights].reserve(cells * sizeof(float)), "device allocation");
         dh = slot_ptr<float>(d, kHeights);
     }
-    TG_CUDA(launch_ds_read(current, frame, g, dh, s), "ds read");
-    return copy_heights_back(d, memory, heights, dh, cells);
+    t.heights = dh;
+    TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
+    t.status = slot_ptr<uint32_t>(d, kStatus);
+    TG_CUDA(cudaMemsetAsync(t.status, 0, sizeof(uint32_t), s), "memset");
+    TG_CUDA(launch_ds_tiles(t, spline, s), "diamond-square launch");
+    TG_CUDA(cudaMemcpyAsync(d->pinnedStatus, t.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s),
+            "copy to host");
+    if (int st = copy_heights_back(d, memory, heights, dh, cells)) {
+        return st;
+    }
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    if (d->pinnedStatus[0] & 1u) {
+        return fail(TG_ERROR_MEMORY, "a diamond-square block outgrew its shared memory");
+    }
+    return TG_OK;
 }
 
 int tg_philox_probe(tg_device* d, const uint32_t* in, uint32_t n, uint32_t* out,

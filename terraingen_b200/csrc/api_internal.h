@@ -80,8 +80,6 @@ enum Slot {
     kBoulderWindows,
     kBoulderEntries,
     kDsPosts,
-    kDsLevelA,
-    kDsLevelB,
     kProbeIn,
     kProbeHashes,
     kProbeValues,

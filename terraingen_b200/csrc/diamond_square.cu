@@ -4,11 +4,12 @@
 // a diamond step (mixed nodes: mean of the four neighbors plus a displacement), then read
 // bilinearly at every output cell.
 //
-// Nodes are doubles, as in the reference, materialised level by level in HBM over boxes that
-// contain what the next level reads (worked out top-down from the output grid, as Refine's
-// recursion does with its margins). Node values do not depend on the box they are computed in:
-// displacements are keyed by (seed, node, level) through Philox4x32-10 and means are local, which
-// is what lets the GPU compute every node once instead of recomputing parents per tile.
+// Nodes are doubles, as in the reference. One CTA per output block builds the block's node
+// pyramid in shared memory, every level over the box the next one reads (worked out top-down
+// from the block's cells, as Refine's recursion does with its margins), and writes only the
+// block's heights: no level touches HBM. Node values do not depend on the box they are computed
+// in (displacements keyed by (seed, node, level) through Philox4x32-10, local means), so blocks
+// agree on the nodes they share, and on the reference's.
 //
 // Compiled with -fmad=false, so the means and the read-out round as the reference's; the normal
 // draws are float Box-Muller on exact double uniforms (node_normal).
@@ -68,118 +69,32 @@ __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int leve
     return double(radius) * double(c);
 }
 
-__device__ __forceinline__ double at(const DsLevel& l, int64_t col, int64_t row) {
-    return l.nodes[size_t(row - l.r0) * l.w + size_t(col - l.c0)];
-}
-
 // Catmull-Rom weights of four nodes around a midpoint (diamond_square.cpp:37).
 __device__ __constant__ const double kMid[4] = {-1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0};
 
-// Level 0: node (col, row) is post (col, -row), reads past the held posts repeating their edge
-// (BaseNodes, diamond_square.cpp:308; PostIndex, src/sources/lattice.h:99). The `pw` x `ph`
-// posts held are those of columns [col0, col0 + pw) and rows [row0, row0 + ph) of the lattice.
-__global__ void ds_base_kernel(const float* __restrict__ posts, int64_t col0, int64_t row0,
-                               uint32_t pw, uint32_t ph, DsLevel out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= out.w || j >= out.h) {
-        return;
-    }
-    const int64_t col = out.c0 + i - col0, row = -(out.r0 + j) - row0;
-    const int64_t pc = col < 0 ? 0 : (col >= int64_t(pw) ? int64_t(pw) - 1 : col);
-    const int64_t pr = row < 0 ? 0 : (row >= int64_t(ph) ? int64_t(ph) - 1 : row);
-    out.nodes[size_t(j) * out.w + i] = double(posts[size_t(pr) * pw + size_t(pc)]);
+__device__ __forceinline__ int64_t floor_half(int64_t v) {  // FloorHalf, diamond_square.cpp:39
+    return v >= 0 ? v / 2 : -((1 - v) / 2);
 }
 
-// Nodes are handled in 2 x 2 blocks anchored at even (col, row): every thread of a step draws
-// the same number of normals (one in the square step, two in the diamond step), so no lane of
-// a warp idles while the others run Philox and Box-Muller.
+// A box of nodes [c0, c0 + w) x [r0, r0 + h) of one level, row-major in shared memory.
+struct NodeBox {
+    int64_t c0, r0;
+    int32_t w, h;
+};
 
-// The square step of `level` over `out`'s box: kept parents (even/even) and displaced odd/odd
-// nodes (SquareStep, diamond_square.cpp:392-407), block (bc0 + i, br0 + j) per thread. Mixed
-// nodes are left for the diamond step.
-template <bool kSpline>
-__global__ void ds_square_kernel(const DsLevel parents, DsLevel out, int64_t bc0, int64_t br0,
-                                 uint32_t bw, uint32_t bh, int level, double step,
-                                 uint32_t seed) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= bw || j >= bh) {
-        return;
+struct Nodes {
+    NodeBox b;
+    double* v;
+    __device__ __forceinline__ double at(int64_t col, int64_t row) const {
+        return v[int32_t(row - b.r0) * b.w + int32_t(col - b.c0)];
     }
-    const int64_t bc = bc0 + i, br = br0 + j;
-    const int64_t c1 = out.c0 + int64_t(out.w), r1 = out.r0 + int64_t(out.h);
-    // The kept parent at (2 bc, 2 br).
-    const int64_t ec = 2 * bc, er = 2 * br;
-    if (ec >= out.c0 && ec < c1 && er >= out.r0 && er < r1) {
-        out.nodes[size_t(er - out.r0) * out.w + size_t(ec - out.c0)] = at(parents, bc, br);
+    __device__ __forceinline__ double& ref(int64_t col, int64_t row) const {
+        return v[int32_t(row - b.r0) * b.w + int32_t(col - b.c0)];
     }
-    // The displaced node at (2 bc + 1, 2 br + 1): the mean of the four parents around it.
-    const int64_t col = ec + 1, row = er + 1;
-    if (col < out.c0 || col >= c1 || row < out.r0 || row >= r1) {
-        return;
+    __device__ __forceinline__ bool holds(int64_t col, int64_t row) const {
+        return col >= b.c0 && col < b.c0 + b.w && row >= b.r0 && row < b.r0 + b.h;
     }
-    const int64_t left = bc, bottom = br;
-    double mean;
-    if (!kSpline) {
-        mean = 0.25 * (at(parents, left, bottom) + at(parents, left + 1, bottom) +
-                       at(parents, left, bottom + 1) + at(parents, left + 1, bottom + 1));
-    } else {
-        mean = 0.0;
-        for (int64_t b = 0; b < 4; ++b) {
-            double line = 0.0;
-            for (int64_t a = 0; a < 4; ++a) {
-                line += kMid[a] * at(parents, left - 1 + a, bottom - 1 + b);
-            }
-            mean += kMid[b] * line;
-        }
-    }
-    out.nodes[size_t(row - out.r0) * out.w + size_t(col - out.c0)] =
-        mean + step * node_normal(col, row, level, seed);
-}
-
-// A mixed node (col, row) of the diamond step: the mean of the four square-step nodes around it
-// plus its displacement.
-template <bool kSpline>
-__device__ __forceinline__ void diamond_node(DsLevel& nodes, int64_t col, int64_t row, int level,
-                                             double step, uint32_t seed) {
-    double mean;
-    if (!kSpline) {
-        mean = 0.25 * (at(nodes, col - 1, row) + at(nodes, col + 1, row) + at(nodes, col, row - 1) +
-                       at(nodes, col, row + 1));
-    } else {
-        double alongX = 0.0, alongY = 0.0;
-        for (int64_t k = 0; k < 4; ++k) {
-            alongX += kMid[k] * at(nodes, col - 3 + 2 * k, row);
-            alongY += kMid[k] * at(nodes, col, row - 3 + 2 * k);
-        }
-        mean = 0.5 * (alongX + alongY);
-    }
-    nodes.nodes[size_t(row - nodes.r0) * nodes.w + size_t(col - nodes.c0)] =
-        mean + step * node_normal(col, row, level, seed);
-}
-
-// The diamond step of `level`: the mixed nodes (2 bc + 1, 2 br) and (2 bc, 2 br + 1) of block
-// (bc0 + i, br0 + j) that lie in `box` (inner box of `nodes`), from the square step's nodes
-// around them (DiamondStep, diamond_square.cpp:410-424).
-template <bool kSpline>
-__global__ void ds_diamond_kernel(DsLevel nodes, int64_t c0, int64_t r0, uint32_t w, uint32_t h,
-                                  int64_t bc0, int64_t br0, uint32_t bw, uint32_t bh, int level,
-                                  double step, uint32_t seed) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= bw || j >= bh) {
-        return;
-    }
-    const int64_t bc = bc0 + i, br = br0 + j;
-    const int64_t c1 = c0 + int64_t(w), r1 = r0 + int64_t(h);
-    const int64_t cols[2] = {2 * bc + 1, 2 * bc}, rows[2] = {2 * br, 2 * br + 1};
-    for (int n = 0; n < 2; ++n) {
-        if (cols[n] >= c0 && cols[n] < c1 && rows[n] >= r0 && rows[n] < r1) {
-            diamond_node<kSpline>(nodes, cols[n], rows[n], level, step, seed);
-        }
-    }
-}
+};
 
 // `value` as an integer when within 1e-6 of one (NearestWhole, src/sources/lattice.h:33), else
 // the node below and the share of the way to the next (NodeAndShare, diamond_square.cpp:53).
@@ -195,35 +110,213 @@ __device__ __forceinline__ void node_and_share(double u, int64_t& node, double& 
     share = u - below;
 }
 
-// Bilinear read of the finest nodes at every cell of the output grid (Interpolate,
-// diamond_square.cpp:461-485).
-__global__ void ds_read_kernel(const DsLevel nodes, DsFrame frame, const Grid grid,
-                               float* __restrict__ heights) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t r = blockIdx.y * blockDim.y + threadIdx.y;
-    if (c >= grid.width || r >= grid.height) {
-        return;
+// The Keys cubic (a = -0.5) at an offset of `x` nodes (CubicWeight, src/raster/resample.cpp:20).
+__device__ __forceinline__ double cubic_weight(double x) {
+    x = fabs(x);
+    if (x <= 1.0) {
+        return (1.5 * x - 2.5) * x * x + 1.0;
     }
-    const double x = grid.originX + (double(c) + 0.5) * grid.pixelWidth +
-                     (double(r) + 0.5) * grid.rowRotation;
-    const double y = grid.originY + (double(c) + 0.5) * grid.colRotation +
-                     (double(r) + 0.5) * grid.pixelHeight;
+    if (x < 2.0) {
+        return ((-0.5 * x + 2.5) * x - 4.0) * x + 2.0;
+    }
+    return 0.0;
+}
+
+// The finest nodes read at (x, y) (Refinement::Interpolate, diamond_square.cpp:461-485):
+// bilinear, or Catmull-Rom over the 4 x 4 nodes around (InterpolateLatticeWeights with the
+// cubic's KernelWeights, src/raster/kernels.h:32-51; taps of zero weight skipped).
+template <bool kSpline>
+__device__ __forceinline__ double read_nodes(const Nodes& n, const DsFrame& frame, double x,
+                                             double y) {
     int64_t col, row;
     double u, v;
     node_and_share((x - frame.originX) / frame.stepX, col, u);
     node_and_share((y - frame.originY) / frame.stepY, row, v);
-    double value = at(nodes, col, row);
+    if (kSpline) {
+        double wx[4], wy[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            wx[i] = cubic_weight(u - double(i - 1));
+            wy[i] = cubic_weight(v - double(i - 1));
+        }
+        double sum = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            for (int i = 0; i < 4; ++i) {
+                if (wx[i] * wy[j] == 0.0) {
+                    continue;
+                }
+                sum += wx[i] * wy[j] * n.at(col - 1 + i, row - 1 + j);
+            }
+        }
+        return sum;
+    }
+    double value = n.at(col, row);
     if (u > 0.0) {
-        value = value * (1.0 - u) + at(nodes, col + 1, row) * u;
+        value = value * (1.0 - u) + n.at(col + 1, row) * u;
     }
     if (v > 0.0) {
-        double above = at(nodes, col, row + 1);
+        double above = n.at(col, row + 1);
         if (u > 0.0) {
-            above = above * (1.0 - u) + at(nodes, col + 1, row + 1) * u;
+            above = above * (1.0 - u) + n.at(col + 1, row + 1) * u;
         }
         value = value * (1.0 - v) + above * v;
     }
-    heights[size_t(r) * grid.width + c] = float(value);
+    return value;
+}
+
+__device__ __forceinline__ void cell_center(const Grid& g, uint32_t c, uint32_t r, double& x,
+                                            double& y) {
+    x = g.originX + (double(c) + 0.5) * g.pixelWidth + (double(r) + 0.5) * g.rowRotation;
+    y = g.originY + (double(c) + 0.5) * g.colRotation + (double(r) + 0.5) * g.pixelHeight;
+}
+
+// One CTA refines the nodes an output block of `block` x `block` cells reads, every level in
+// shared memory, and writes only the block's heights (Refinement::Refine, diamond_square.cpp:
+// 426-448, with the boxes worked out top-down as its recursion does). Node values do not depend
+// on the box they are computed in: displacements are keyed by (seed, node, level) through
+// Philox4x32-10 and means are local, so neighbouring blocks agree on every node they share.
+//   level 0   nodes from the posts: node (col, row) is post (col, -row) of the lattice, the
+//             window held being its columns col0.. and rows row0.., reads past it repeating its
+//             edge (BaseNodes, diamond_square.cpp:311; PostIndex, src/sources/lattice.h:99);
+//   level l   the square step over the box the diamond step reads (SquareStep, :392-407: kept
+//             parents and displaced odd/odd nodes), then the diamond step over the box the next
+//             level reads (DiamondStep, :410-424), in place;
+//   read      each cell from the finest level.
+// Levels of even and odd number alternate between two shared buffers of t.capEven and t.capOdd
+// doubles. Thread 0 works out the boxes; one that would outgrow its buffer (the host sizes them
+// from the block's extent, so never) sets flag 1 and the CTA writes nothing.
+template <bool kSpline>
+__global__ void __launch_bounds__(kDsTileThreads) ds_tile_kernel(const DsTile t) {
+    extern __shared__ double pool[];
+    __shared__ NodeBox inner[kMaxDsLevels + 1];
+    __shared__ int fits;
+    constexpr int64_t kReach = kSpline ? 3 : 1;   // the diamond mean's reach (Refine's `reach`)
+    constexpr int64_t kBefore = kSpline ? 1 : 0;  // parents a square mean reads before its block
+    constexpr int64_t kAfter = kSpline ? 2 : 1;   // and after it; the read's nodes after a cell
+    const uint32_t bx = blockIdx.x % t.blocksX, by = blockIdx.x / t.blocksX;
+    const uint32_t c0 = bx * t.block, r0 = by * t.block;
+    const uint32_t cw = min(t.block, t.grid.width - c0), rh = min(t.block, t.grid.height - r0);
+    const int levels = t.levels;
+    if (threadIdx.x == 0) {
+        double umin = INFINITY, umax = -INFINITY, vmin = INFINITY, vmax = -INFINITY;
+        for (int k = 0; k < 4; ++k) {
+            double x, y;
+            cell_center(t.grid, c0 + ((k & 1) ? cw - 1 : 0), r0 + ((k & 2) ? rh - 1 : 0), x, y);
+            const double u = (x - t.frame.originX) / t.frame.stepX;
+            const double v = (y - t.frame.originY) / t.frame.stepY;
+            umin = fmin(umin, u);
+            umax = fmax(umax, u);
+            vmin = fmin(vmin, v);
+            vmax = fmax(vmax, v);
+        }
+        const int64_t fc0 = int64_t(floor(umin)) - 1, fc1 = int64_t(ceil(umax)) + kAfter;
+        const int64_t fr0 = int64_t(floor(vmin)) - 1, fr1 = int64_t(ceil(vmax)) + kAfter;
+        bool ok = fc1 - fc0 < 65536 && fr1 - fr0 < 65536;
+        inner[levels] = NodeBox{fc0, fr0, int32_t(fc1 - fc0 + 1), int32_t(fr1 - fr0 + 1)};
+        for (int l = levels; l >= 1 && ok; --l) {
+            const NodeBox& b = inner[l];
+            const int64_t oc0 = b.c0 - kReach, oc1 = b.c0 + b.w - 1 + kReach;
+            const int64_t or0 = b.r0 - kReach, or1 = b.r0 + b.h - 1 + kReach;
+            ok = (oc1 - oc0 + 1) * (or1 - or0 + 1) <= int64_t((l & 1) ? t.capOdd : t.capEven);
+            const int64_t pc0 = floor_half(oc0) - kBefore, pc1 = floor_half(oc1) + kAfter;
+            const int64_t pr0 = floor_half(or0) - kBefore, pr1 = floor_half(or1) + kAfter;
+            inner[l - 1] = NodeBox{pc0, pr0, int32_t(pc1 - pc0 + 1), int32_t(pr1 - pr0 + 1)};
+        }
+        ok = ok && int64_t(inner[0].w) * inner[0].h <= int64_t(t.capEven);
+        fits = ok ? 1 : 0;
+        if (!ok) {
+            atomicOr(t.status, 1u);
+        }
+    }
+    __syncthreads();
+    if (!fits) {
+        return;
+    }
+    Nodes parents{inner[0], pool};
+    for (int32_t i = threadIdx.x; i < parents.b.w * parents.b.h; i += blockDim.x) {
+        const int64_t col = parents.b.c0 + i % parents.b.w - t.col0;
+        const int64_t row = -(parents.b.r0 + i / parents.b.w) - t.row0;
+        const int64_t pc = col < 0 ? 0 : (col >= int64_t(t.pw) ? int64_t(t.pw) - 1 : col);
+        const int64_t pr = row < 0 ? 0 : (row >= int64_t(t.ph) ? int64_t(t.ph) - 1 : row);
+        parents.v[i] = double(t.posts[size_t(pr) * t.pw + size_t(pc)]);
+    }
+    __syncthreads();
+    for (int l = 1; l <= levels; ++l) {
+        const NodeBox& d = inner[l];
+        const Nodes out{NodeBox{d.c0 - kReach, d.r0 - kReach, int32_t(d.w + 2 * kReach),
+                                int32_t(d.h + 2 * kReach)},
+                        (l & 1) ? pool + t.capEven : pool};
+        // Square step: the 2 x 2 blocks anchored at even (col, row) that meet the box.
+        const int64_t sc0 = floor_half(out.b.c0), sr0 = floor_half(out.b.r0);
+        const int32_t sw = int32_t(floor_half(out.b.c0 + out.b.w - 1) - sc0 + 1);
+        const int32_t sh = int32_t(floor_half(out.b.r0 + out.b.h - 1) - sr0 + 1);
+        const double squareStep = t.squareStep[l], diamondStep = t.diamondStep[l];
+        for (int32_t i = threadIdx.x; i < sw * sh; i += blockDim.x) {
+            const int64_t bc = sc0 + i % sw, br = sr0 + i / sw;
+            if (out.holds(2 * bc, 2 * br)) {
+                out.ref(2 * bc, 2 * br) = parents.at(bc, br);
+            }
+            const int64_t col = 2 * bc + 1, row = 2 * br + 1;
+            if (!out.holds(col, row)) {
+                continue;
+            }
+            double mean;
+            if (!kSpline) {
+                mean = 0.25 * (parents.at(bc, br) + parents.at(bc + 1, br) +
+                               parents.at(bc, br + 1) + parents.at(bc + 1, br + 1));
+            } else {
+                mean = 0.0;
+                for (int64_t b = 0; b < 4; ++b) {
+                    double line = 0.0;
+                    for (int64_t a = 0; a < 4; ++a) {
+                        line += kMid[a] * parents.at(bc - 1 + a, br - 1 + b);
+                    }
+                    mean += kMid[b] * line;
+                }
+            }
+            out.ref(col, row) = mean + squareStep * node_normal(col, row, l, t.seed);
+        }
+        __syncthreads();
+        // Diamond step: the mixed nodes (2 bc + 1, 2 br) and (2 bc, 2 br + 1) inside the box the
+        // next level reads, from the square step's nodes around them.
+        const int64_t dc0 = floor_half(d.c0), dr0 = floor_half(d.r0);
+        const int32_t dw = int32_t(floor_half(d.c0 + d.w - 1) - dc0 + 1);
+        const int32_t dh = int32_t(floor_half(d.r0 + d.h - 1) - dr0 + 1);
+        const Nodes inside{d, nullptr};
+        for (int32_t i = threadIdx.x; i < dw * dh; i += blockDim.x) {
+            const int64_t bc = dc0 + i % dw, br = dr0 + i / dw;
+            const int64_t cols[2] = {2 * bc + 1, 2 * bc}, rows[2] = {2 * br, 2 * br + 1};
+#pragma unroll
+            for (int n = 0; n < 2; ++n) {
+                const int64_t col = cols[n], row = rows[n];
+                if (!inside.holds(col, row)) {
+                    continue;
+                }
+                double mean;
+                if (!kSpline) {
+                    mean = 0.25 * (out.at(col - 1, row) + out.at(col + 1, row) +
+                                   out.at(col, row - 1) + out.at(col, row + 1));
+                } else {
+                    double alongX = 0.0, alongY = 0.0;
+                    for (int64_t k = 0; k < 4; ++k) {
+                        alongX += kMid[k] * out.at(col - 3 + 2 * k, row);
+                        alongY += kMid[k] * out.at(col, row - 3 + 2 * k);
+                    }
+                    mean = 0.5 * (alongX + alongY);
+                }
+                out.ref(col, row) = mean + diamondStep * node_normal(col, row, l, t.seed);
+            }
+        }
+        __syncthreads();
+        parents = out;
+    }
+    // The read: consecutive threads take consecutive cells of a row.
+    for (uint32_t i = threadIdx.x; i < cw * rh; i += blockDim.x) {
+        const uint32_t c = c0 + i % cw, r = r0 + i / cw;
+        double x, y;
+        cell_center(t.grid, c, r, x, y);
+        t.heights[size_t(r) * t.grid.width + c] = float(read_nodes<kSpline>(parents, t.frame, x, y));
+    }
 }
 
 __global__ void philox_probe_kernel(const uint32_t* __restrict__ in, uint32_t n,
@@ -243,58 +336,30 @@ __global__ void philox_probe_kernel(const uint32_t* __restrict__ in, uint32_t n,
     normals[i] = node_normal(int64_t(int32_t(c[0])), int64_t(int32_t(c[1])), int(c[2] & 31u), c[4]);
 }
 
-dim3 blocks_for(uint32_t w, uint32_t h, dim3 block) {
-    return dim3((w + block.x - 1) / block.x, (h + block.y - 1) / block.y);
-}
 
 }  // namespace
 
-cudaError_t launch_ds_base(const float* posts, int64_t col0, int64_t row0, uint32_t pw,
-                           uint32_t ph, const DsLevel& out, cudaStream_t stream) {
-    const dim3 block(32, 8);
-    ds_base_kernel<<<blocks_for(out.w, out.h, block), block, 0, stream>>>(posts, col0, row0, pw,
-                                                                          ph, out);
-    return cudaGetLastError();
-}
-
-// The 2 x 2 blocks anchored at even coordinates that hold the nodes [lo, lo + n).
-void block_range(int64_t lo, uint32_t n, int64_t& b0, uint32_t& count) {
-    const auto half = [](int64_t v) { return v >= 0 ? v / 2 : -((1 - v) / 2); };
-    b0 = half(lo);
-    count = n == 0 ? 0u : uint32_t(half(lo + int64_t(n) - 1) - b0 + 1);
-}
-
-cudaError_t launch_ds_level(const DsLevel& parents, const DsLevel& out, int64_t c0, int64_t r0,
-                            uint32_t w, uint32_t h, int level, double squareStep,
-                            double diamondStep, uint32_t seed, bool spline,
-                            cudaStream_t stream) {
-    const dim3 block(32, 8);
-    int64_t sc0, sr0, dc0, dr0;
-    uint32_t sw, sh, dw, dh;
-    block_range(out.c0, out.w, sc0, sw);
-    block_range(out.r0, out.h, sr0, sh);
-    block_range(c0, w, dc0, dw);
-    block_range(r0, h, dr0, dh);
-    if (spline) {
-        ds_square_kernel<true><<<blocks_for(sw, sh, block), block, 0, stream>>>(
-            parents, out, sc0, sr0, sw, sh, level, squareStep, seed);
-        ds_diamond_kernel<true><<<blocks_for(dw, dh, block), block, 0, stream>>>(
-            out, c0, r0, w, h, dc0, dr0, dw, dh, level, diamondStep, seed);
-    } else {
-        ds_square_kernel<false><<<blocks_for(sw, sh, block), block, 0, stream>>>(
-            parents, out, sc0, sr0, sw, sh, level, squareStep, seed);
-        ds_diamond_kernel<false><<<blocks_for(dw, dh, block), block, 0, stream>>>(
-            out, c0, r0, w, h, dc0, dr0, dw, dh, level, diamondStep, seed);
+cudaError_t launch_ds_tiles(const DsTile& t, bool spline, cudaStream_t stream) {
+    const uint32_t blocks = t.blocksX * ((t.grid.height + t.block - 1) / t.block);
+    if (blocks == 0) {
+        return cudaSuccess;
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_ds_read(const DsLevel& nodes, const DsFrame& frame, const Grid& grid,
-                           float* heights, cudaStream_t stream) {
-    const dim3 block(32, 8);
-    ds_read_kernel<<<blocks_for(grid.width, grid.height, block), block, 0, stream>>>(
-        nodes, frame, grid, heights);
-    return cudaGetLastError();
+    const size_t bytes = size_t(t.capEven + t.capOdd) * sizeof(double);
+    cudaError_t err;
+    if (spline) {
+        err = cudaFuncSetAttribute(ds_tile_kernel<true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (err == cudaSuccess) {
+            ds_tile_kernel<true><<<blocks, kDsTileThreads, bytes, stream>>>(t);
+        }
+    } else {
+        err = cudaFuncSetAttribute(ds_tile_kernel<false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (err == cudaSuccess) {
+            ds_tile_kernel<false><<<blocks, kDsTileThreads, bytes, stream>>>(t);
+        }
+    }
+    return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t launch_philox_probe(const uint32_t* in, uint32_t n, uint32_t* out, double* normals,

@@ -189,26 +189,30 @@ cudaError_t launch_boulder_bake(const Grid& grid, double width, NoData nodata,
                                 uint32_t binRows = 0xffffffffu, uint32_t polls = kWaitPolls);
 
 // --- diamond-square ----------------------------------------------------------------------
-// Nodes of one level over columns [c0, c0 + w) and rows [r0, r0 + h), row-major doubles.
-struct DsLevel {
-    int64_t c0, r0;
-    uint32_t w, h;
-    double* nodes;
-};
 // Where the finest nodes lie: node (0, 0) and the node steps along x and y (north up).
 struct DsFrame {
     double originX, originY, stepX, stepY;
 };
-
-cudaError_t launch_ds_base(const float* posts, int64_t col0, int64_t row0, uint32_t pw,
-                           uint32_t ph, const DsLevel& out, cudaStream_t stream);
-// The square step over `out`'s whole box, then the diamond step over the inner box
-// [c0, c0 + w) x [r0, r0 + h), displacements scaled by `squareStep` and `diamondStep`.
-cudaError_t launch_ds_level(const DsLevel& parents, const DsLevel& out, int64_t c0, int64_t r0,
-                            uint32_t w, uint32_t h, int level, double squareStep,
-                            double diamondStep, uint32_t seed, bool spline, cudaStream_t stream);
-cudaError_t launch_ds_read(const DsLevel& nodes, const DsFrame& frame, const Grid& grid,
-                           float* heights, cudaStream_t stream);
+constexpr int kMaxDsLevels = 30;
+constexpr uint32_t kDsTileThreads = 256;
+// One refinement's launch (launch_ds_tiles): `levels` refinements of the posts read at every cell
+// of `grid` into `heights` (row-major, grid.width a row), a CTA per `block` x `block` cells.
+struct DsTile {
+    Grid grid;
+    DsFrame frame;                           // the finest level's
+    int levels;
+    uint32_t seed;
+    uint32_t block, blocksX;
+    uint32_t capEven, capOdd;                // doubles of the even / odd levels' shared buffers
+    double squareStep[kMaxDsLevels + 1];     // displacement scale per level (index 1..levels)
+    double diamondStep[kMaxDsLevels + 1];
+    const float* posts;                      // the lattice's columns col0.. and rows row0..
+    int64_t col0, row0;
+    uint32_t pw, ph;
+    float* heights;
+    uint32_t* status;                        // flag 1: a block's boxes outgrew their buffers
+};
+cudaError_t launch_ds_tiles(const DsTile& t, bool spline, cudaStream_t stream);
 // Philox4x32-10 of n (counter, key) sextets, and the displacement normal the first two counter
 // words, the third's low 5 bits and the key's first word key as (col, row, level, seed).
 cudaError_t launch_philox_probe(const uint32_t* in, uint32_t n, uint32_t* out, double* normals,

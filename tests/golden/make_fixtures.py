@@ -167,17 +167,21 @@ def ds_fixtures() -> None:
                   0.8, 3),
         # Ten-fold, as the 20481^2 refinement (4 levels), on a small window.
         "tenfold": (centered(41, 41, 5.0), centered(351, 351, 0.5, -10.0, 5.0), 2.2, 2.0, 11),
+        # Catmull-Rom (DiamondSquareInterp::CatmullRom): spline midpoints and the cubic read.
+        "dem5m_cr": (centered(65, 65, 5.0), centered(301, 301, 1.0, 3.25, -1.75), 2.2, 1.5, 7),
+        "tenfold_cr": (centered(41, 41, 5.0), centered(351, 351, 0.5, -10.0, 5.0), 2.2, 2.0, 11),
     }
     for name, (pg, grid, fd, scale, seed) in cases.items():
+        interp = 1 if name.endswith("_cr") else 0
         posts = np.zeros((pg.height, pg.width), np.float32)
         rs.rs_fbm_grid_f32(pg.width, pg.height, pg.x0, pg.y0, pg.pixel, 3, 20000.0, 2000.0, 12,
                            2.0, 0.5, 0.0, posts.ctypes.data)
-        heights, _ = H.diamond_square(ref, posts, pg, grid, fd, scale, seed, 0, 1)
+        heights, _ = H.diamond_square(ref, posts, pg, grid, fd, scale, seed, interp, 1)
         assert not np.isnan(heights).any(), name
         arrays[f"{name}_posts"] = posts
         arrays[f"{name}_post_grid"] = np.array([pg.width, pg.height, pg.x0, pg.y0, pg.pixel])
         arrays[f"{name}_grid"] = np.array([grid.width, grid.height, grid.x0, grid.y0, grid.pixel])
-        arrays[f"{name}_options"] = np.array([fd, scale, seed], np.float64)
+        arrays[f"{name}_options"] = np.array([fd, scale, seed, interp], np.float64)
         arrays[f"{name}_expected"] = heights
         print(name, heights.shape, float(heights.std()))
     np.savez_compressed(OUT / "ds.npz", **arrays)

@@ -101,7 +101,7 @@ def test_terrain_through_hooked_reference_pipeline(dropin):
     assert np.count_nonzero(gpu != gpu[0, 0]) > 0.9 * gpu.size
 
 
-@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold", "tenfold_cr"])
 def test_ds_through_hooked_reference_pipeline(dropin, name):
     # The reference's DiamondSquareUpsampler behind a RasterSource on Backend::Cuda: the drop-in
     # build's hook hands the refinement to tg_ds_refine, which gives the committed fixture (the
@@ -111,10 +111,10 @@ def test_ds_through_hooked_reference_pipeline(dropin, name):
     fx = dict(np.load(GOLDEN / "ds.npz"))
     pg = grid_of(fx[f"{name}_post_grid"])
     grid = grid_of(fx[f"{name}_grid"])
-    fd, scale, seed = fx[f"{name}_options"]
+    fd, scale, seed, interp = fx[f"{name}_options"]
     before = H.hook_calls(dropin)
-    gpu, _ = H.diamond_square(dropin, fx[f"{name}_posts"], pg, grid, fd, scale, int(seed), 0, 1,
-                              backend=1)
+    gpu, _ = H.diamond_square(dropin, fx[f"{name}_posts"], pg, grid, fd, scale, int(seed),
+                              int(interp), 1, backend=1)
     assert H.hook_calls(dropin) - before >= 1
     err = np.abs(gpu.astype(np.float64) - fx[f"{name}_expected"])
     assert err.max() <= 1e-3, (name, err.max())

@@ -21,13 +21,14 @@ def fx():
     return dict(np.load(GOLDEN / "ds.npz"))
 
 
-@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold", "dem5m_cr", "tenfold_cr"])
 def test_ds_matches_reference(device, fx, name):
+    # Bilinear and Catmull-Rom (the _cr cases) refinements against the reference's.
     pg = grid_of(fx[f"{name}_post_grid"])
     grid = grid_of(fx[f"{name}_grid"])
-    fd, scale, seed = fx[f"{name}_options"]
+    fd, scale, seed, interp = fx[f"{name}_options"]
     heights = np.zeros((grid.height, grid.width), np.float32)
-    device.ds_refine(fx[f"{name}_posts"], pg, grid, heights, fd, scale, int(seed))
+    device.ds_refine(fx[f"{name}_posts"], pg, grid, heights, fd, scale, int(seed), int(interp))
     err = np.abs(heights.astype(np.float64) - fx[f"{name}_expected"])
     assert err.max() <= TOLERANCE_M, (name, err.max())
 
@@ -72,7 +73,7 @@ def test_ds_deterministic_and_windowed(device, fx):
 
     pg = grid_of(fx["exact_post_grid"])
     grid = grid_of(fx["exact_grid"])
-    fd, scale, seed = fx["exact_options"]
+    fd, scale, seed, _ = fx["exact_options"]
     whole = np.zeros((grid.height, grid.width), np.float32)
     device.ds_refine(fx["exact_posts"], pg, grid, whole, fd, scale, int(seed))
     again = np.zeros_like(whole)
@@ -95,7 +96,7 @@ def test_ds_zero_scale_is_interpolation(device, fx):
     assert heights.min() >= posts.min() - 1e-3 and heights.max() <= posts.max() + 1e-3
 
 
-@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold"])
+@pytest.mark.parametrize("name", ["dem5m", "exact", "tenfold", "tenfold_cr"])
 def test_ds_window_of_posts_matches_whole(device, fx, name):
     # A 64^2 block inside the fixture's grid, refined from only the posts over its bounds and
     # eight posts around (tg_ds_refine_window: the node frame still the whole lattice's), is the
@@ -106,11 +107,12 @@ def test_ds_window_of_posts_matches_whole(device, fx, name):
 
     pg = grid_of(fx[f"{name}_post_grid"])
     grid = grid_of(fx[f"{name}_grid"])
-    fd, scale, seed = fx[f"{name}_options"]
+    fd, scale, seed, interp = fx[f"{name}_options"]
+    interp = int(interp)
     posts = fx[f"{name}_posts"]
     block = GridSpec(64, 64, grid.x0 + 100 * grid.pixel, grid.y0 - 90 * grid.pixel, grid.pixel)
     whole = np.zeros((64, 64), np.float32)
-    device.ds_refine(posts, pg, block, whole, fd, scale, int(seed))
+    device.ds_refine(posts, pg, block, whole, fd, scale, int(seed), interp)
     c0 = max(0, math.floor((block.x0 - pg.x0) / pg.pixel) - 8)
     c1 = min(pg.width, math.ceil((block.x0 + 64 * block.pixel - pg.x0) / pg.pixel) + 8)
     r0 = max(0, math.floor((pg.y0 - block.y0) / pg.pixel) - 8)
@@ -118,10 +120,10 @@ def test_ds_window_of_posts_matches_whole(device, fx, name):
     assert c0 > 0 and r0 > 0 and c1 < pg.width and r1 < pg.height
     window = np.ascontiguousarray(posts[r0:r1, c0:c1])
     part = np.zeros_like(whole)
-    device.ds_refine(window, pg, block, part, fd, scale, int(seed), window=(c0, r0))
+    device.ds_refine(window, pg, block, part, fd, scale, int(seed), interp, window=(c0, r0))
     assert np.array_equal(part.view(np.uint32), whole.view(np.uint32)), name
     # The same posts passed as a lattice of their own draw other displacements.
     alone = np.zeros_like(whole)
     shifted = GridSpec(c1 - c0, r1 - r0, pg.x0 + c0 * pg.pixel, pg.y0 - r0 * pg.pixel, pg.pixel)
-    device.ds_refine(window, shifted, block, alone, fd, scale, int(seed))
+    device.ds_refine(window, shifted, block, alone, fd, scale, int(seed), interp)
     assert not np.array_equal(alone, whole)
