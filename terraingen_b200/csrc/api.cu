@@ -1284,19 +1284,29 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
 namespace {
 
 // The output block of a diamond-square CTA and the shared buffers its node pyramid needs: the
-// largest side in 64, 32, ..., 1 whose two buffers fit kDsSharedBudget bytes. Each level's box is
-// bounded from the block's extent in finest nodes (what the device works out, plus two nodes for
-// the rounding of either side's arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
+// largest block (64 x 64, 64 x 32, 32 x 32, ... cells) whose two buffers fit kDsSharedBudget
+// bytes, so that three CTAs share an SM. A bigger block recomputes fewer nodes of its neighbours'
+// (the margins the means need) per cell. Each level's box is bounded from the block's extent in
+// finest nodes (what the device works out, plus two nodes for the rounding of either side's
+// arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
 // its parents' box is half of it plus the square mean's margins.
-constexpr size_t kDsSharedBudget = 100 * 1024;
+#ifndef TGB_DS_SHARED_BUDGET
+#define TGB_DS_SHARED_BUDGET (72 * 1024)
+#endif
+constexpr size_t kDsSharedBudget = TGB_DS_SHARED_BUDGET;
 
 bool ds_tile_shape(DsTile& t, bool spline) {
     const int64_t reach = spline ? 3 : 1, before = spline ? 1 : 0, after = spline ? 2 : 1;
     const Grid& g = t.grid;
-    for (uint32_t side = 64; side >= 1; side /= 2) {
-        const double spanX = double(side - 1) * (std::fabs(g.pixelWidth) + std::fabs(g.rowRotation)) /
+    constexpr uint32_t kShapes[][2] = {{64, 64}, {64, 32}, {32, 32}, {32, 16}, {16, 16}, {16, 8},
+                                       {8, 8},   {8, 4},   {4, 4},   {4, 2},   {2, 2},   {1, 1}};
+    for (const auto& shape : kShapes) {
+        const uint32_t bw = shape[0], bh = shape[1];
+        const double spanX = (double(bw - 1) * std::fabs(g.pixelWidth) +
+                              double(bh - 1) * std::fabs(g.rowRotation)) /
                              std::fabs(t.frame.stepX);
-        const double spanY = double(side - 1) * (std::fabs(g.colRotation) + std::fabs(g.pixelHeight)) /
+        const double spanY = (double(bw - 1) * std::fabs(g.colRotation) +
+                              double(bh - 1) * std::fabs(g.pixelHeight)) /
                              std::fabs(t.frame.stepY);
         if (!(spanX < 4096.0 && spanY < 4096.0)) {
             continue;
@@ -1312,8 +1322,9 @@ bool ds_tile_shape(DsTile& t, bool spline) {
         }
         cap[0] = std::max<uint64_t>(cap[0], uint64_t(w * h));
         if ((cap[0] + cap[1]) * sizeof(double) <= kDsSharedBudget) {
-            t.block = side;
-            t.blocksX = (g.width + side - 1) / side;
+            t.blockW = bw;
+            t.blockH = bh;
+            t.blocksX = (g.width + bw - 1) / bw;
             t.capEven = uint32_t(cap[0]);
             t.capOdd = uint32_t(cap[1]);
             return true;
@@ -1415,6 +1426,7 @@ int tg_ds_refine_window(tg_device* d, const float* posts, int64_t col0, int64_t 
         dh = slot_ptr<float>(d, kHeights);
     }
     t.heights = dh;
+    t.pitch = g.width;
     TG_CUDA(d->slots[kStatus].reserve(4 * sizeof(uint32_t)), "allocation");
     t.status = slot_ptr<uint32_t>(d, kStatus);
     TG_CUDA(cudaMemsetAsync(t.status, 0, sizeof(uint32_t), s), "memset");

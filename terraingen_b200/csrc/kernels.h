@@ -194,15 +194,19 @@ struct DsFrame {
     double originX, originY, stepX, stepY;
 };
 constexpr int kMaxDsLevels = 30;
-constexpr uint32_t kDsTileThreads = 256;
+#ifndef TGB_DS_THREADS
+#define TGB_DS_THREADS 256
+#endif
+constexpr uint32_t kDsTileThreads = TGB_DS_THREADS;  // threads of a diamond-square CTA
 // One refinement's launch (launch_ds_tiles): `levels` refinements of the posts read at every cell
-// of `grid` into `heights` (row-major, grid.width a row), a CTA per `block` x `block` cells.
+// of `grid` into `heights` (row-major, `pitch` floats a row), a CTA per blockW x blockH cells
+// (sides at most 64).
 struct DsTile {
     Grid grid;
     DsFrame frame;                           // the finest level's
     int levels;
     uint32_t seed;
-    uint32_t block, blocksX;
+    uint32_t blockW, blockH, blocksX, pitch;
     uint32_t capEven, capOdd;                // doubles of the even / odd levels' shared buffers
     double squareStep[kMaxDsLevels + 1];     // displacement scale per level (index 1..levels)
     double diamondStep[kMaxDsLevels + 1];
