@@ -558,15 +558,18 @@ def next_rows_form(dev):
 
 
 def served_form(dev, args, rank, world):
-    """The served form on the camera request stream (terraingen_b200/serve.py): the DEM stack's
-    source and craters served by continuous batching, results in device buffers. Latency per
-    class at 2000 requests/s in real time; sustained throughput with the stream submitted at
-    once; the plain per-request path (tg_noise_source + tg_craters_apply per tile, inputs
-    resident) on tile requests of the same stream."""
+    """The served form on the camera request stream (terraingen_b200/serve.py): the DEM
+    refinement's stack (the 12-octave fBm at 5 m posts, refined by diamond-square to each
+    request's spacing, craters on top) served by continuous batching, results in device buffers.
+    Latency per class at 2000 requests/s in real time; sustained throughput with the stream
+    submitted at once; the plain per-request path (per tile: tg_noise_source on its post window,
+    tg_ds_refine_window, tg_craters_apply; inputs resident) on tile requests of the same
+    stream."""
     import torch
 
     from terraingen_b200.device import GridSpec
-    from terraingen_b200.serve import Server, camera_stream, dem_stack_options, run_stream
+    from terraingen_b200.serve import (POST_SPACING, Server, camera_stream, dem_stack_options,
+                                       post_lattice, refine_options, run_stream)
     from terraingen_b200.workloads import crater_batch
 
     opts = dem_stack_options(slots=3, max_batch_cells=8 << 20)
@@ -581,30 +584,55 @@ def served_form(dev, args, rank, world):
         saturated = run_stream(server, sat_reqs, realtime=False, device=True)
         tiles = [r for r in sat_reqs if r.grid is not None]
         tiles_only = run_stream(server, tiles, realtime=False, device=True)
-        host = run_stream(server, sat_reqs, realtime=False)
+        host = run_stream(server, sat_reqs, realtime=False, pinned=True)
+        pageable = run_stream(server, sat_reqs, realtime=False)
         stats = server.stats()
-        # A tile of the stack 1e6 m out, served by the same server, against the FP64 oracle.
+        # A tile of the stack, served by the same server, against the FP64 oracle (the
+        # reference's diamond-square over FP64 posts, craters in double).
         probe_grid = GridSpec(*[int(v) if i < 2 else float(v) for i, v in
-                                enumerate(np.load(FP64_FIXTURE)["served_grid"])])
+                                enumerate(np.load(FP64_FIXTURE)["served_refined_grid"])])
         probe = np.empty(probe_grid.cells, np.float32)
         server.submit_tile(1 << 30, probe_grid, probe)
         server.drain()
-        fp64 = {"tile": "257^2 at 0.5 m, 1e6 m out", **fp64_error(probe, "served")}
+        fp64 = {"tile": "257^2 at 0.5 m near the origin (the reference's diamond-square keys "
+                        "draws by its raster's posts, which start at the origin)",
+                **fp64_error(probe, "served_refined")}
+    # The fBm-at-every-cell stack 1e6 m out against the FP64 oracle (the source's far-coordinate
+    # precision, which the refined stack's posts share).
+    with Server(dev, dem_stack_options(slots=1, refine=False)) as fbm:
+        far_grid = GridSpec(*[int(v) if i < 2 else float(v) for i, v in
+                              enumerate(np.load(FP64_FIXTURE)["served_grid"])])
+        far = np.empty(far_grid.cells, np.float32)
+        fbm.submit_tile(1 << 30, far_grid, far)
+        fbm.drain()
+        fp64_far = {"tile": "257^2 at 0.5 m, 1e6 m out, fBm at every cell",
+                    **fp64_error(far, "served")}
     # The plain per-request path on the stream's tile requests (crater records per tile built
-    # and resident before timing).
+    # and resident before timing): the posts of the tile's window, the refinement, the craters.
     sample = tiles[:300]
     prep = []
+    ro = refine_options()
+    lattice = post_lattice()
     for r in sample:
-        k, rec, dat, foot = crater_batch(opts.craters, r.grid)
-        prep.append((r.grid, k, torch.from_numpy(rec.view(np.uint8).copy()).cuda(),
+        g = r.grid
+        col0 = int(np.floor(g.x0 / POST_SPACING)) - 8
+        row0 = int(np.floor(-g.y0 / POST_SPACING)) - 8
+        pw = int(np.ceil((g.x0 + g.width * g.pixel) / POST_SPACING)) + 9 - col0
+        ph = int(np.ceil(-(g.y0 - g.height * g.pixel) / POST_SPACING)) + 9 - row0
+        window = GridSpec(pw, ph, lattice.x0 + col0 * POST_SPACING,
+                          lattice.y0 - row0 * POST_SPACING, POST_SPACING)
+        k, rec, dat, foot = crater_batch(opts.craters, g)
+        prep.append((g, window, (col0, row0), k, torch.from_numpy(rec.view(np.uint8).copy()).cuda(),
                      torch.from_numpy(np.ascontiguousarray(dat)).cuda(),
                      torch.from_numpy(np.ascontiguousarray(foot)).cuda(), len(rec),
-                     torch.empty((r.grid.height, r.grid.width), dtype=torch.float32,
-                                 device="cuda")))
+                     torch.empty((ph, pw), dtype=torch.float32, device="cuda"),
+                     torch.empty((g.height, g.width), dtype=torch.float32, device="cuda")))
 
     def plain():
-        for g, k, rec, dat, foot, n, h in prep:
-            dev.noise_source(opts._fractals, g, h, 0.0)
+        for g, window, at, k, rec, dat, foot, n, posts, h in prep:
+            dev.noise_source(opts._fractals, window, posts, 0.0)
+            dev.ds_refine(posts, lattice, g, h, ro.fractal_dimension, ro.scale, seed=ro.seed,
+                          window=at)
             if n:
                 dev.craters_apply(k, rec, dat, g, h, footprints=foot)
 
@@ -621,22 +649,30 @@ def served_form(dev, args, rank, world):
     return {
         "workload": "camera stream at 10 km over a 1737.4 km sphere (planar polar frame, nadir "
                     "1e6 m out): Poisson 2000 req/s, 70% 257^2 / 25% 1025^2 tiles at 0.25-4 m, "
-                    "5% x 10,000 points; DEM stack: 12-octave fBm (20 km, +-2000 m) + craters "
-                    "(2M per 20481^2 at 0.5 m, D 1-100 m)",
+                    "5% x 10,000 points; DEM-refinement stack: 12-octave fBm (20 km, +-2000 m) "
+                    "at 5 m posts refined by diamond-square (F 2.2, scale 1.5 m, bilinear) to "
+                    "each request's spacing, + craters (2M per 20481^2 at 0.5 m, D 1-100 m)",
         "nominal": nominal.summary(),
         "saturated_device": sat,
         "tiles_only_device": tonly,
         "saturated_host": {"mcells_per_s": host.summary()["mcells_per_s"],
-                           "note": "heights copied to pageable host arrays"},
+                           "note": "heights copied by the slots' streams straight into "
+                                   "page-locked host arrays"},
+        "saturated_host_pageable": {"mcells_per_s": pageable.summary()["mcells_per_s"],
+                                    "note": "pageable host arrays: through the slots' pinned "
+                                            "mirrors and a host copy each"},
         "plain_per_request": {"value": round(plain_value, 3), "unit": UNIT,
                               "requests": len(sample), "ms": round(plain_ms, 3),
-                              "path": "tg_noise_source + tg_craters_apply per tile request"},
+                              "path": "tg_noise_source on the tile's post window + "
+                                      "tg_ds_refine_window + tg_craters_apply per tile request"},
         "speedup_vs_plain": {"mixed": round(sat["mcells_per_s"] / plain_value, 2),
                              "tiles": round(tonly["mcells_per_s"] / plain_value, 2)},
         "server": {k: stats[k] for k in ("batches", "regions_built", "regions_resident",
                                          "feature_bytes", "peak_bytes", "deferred")},
         "fp64": fp64,
-        "accuracy": "results identical alone and in the mix (tests/test_serve_gpu.py)",
+        "fp64_far_source": fp64_far,
+        "accuracy": "results identical alone and in the mix; a refined tile is tg_ds_refine_window "
+                    "over the same posts bit for bit (tests/test_serve_gpu.py)",
     }
 
 

@@ -688,6 +688,13 @@ typedef struct tg_server_options {
     uint32_t region_cells;          /* side of a feature region in cells of its level */
     int32_t variant;                /* batch kernel shape; -1 lets the autotuner pick */
     uint32_t reserved;
+    /* The DEM-refinement stack (DiamondSquareUpsampler over a DEM, src/sources/diamond_square.cpp:
+     * 488-516): with post_spacing > 0 the source is the fBm above sampled at a post lattice of
+     * that spacing (post (i, j) at (i * post_spacing, -j * post_spacing), rounded to float as a
+     * DEM's posts) and refined by diamond-square under `refine` to each tile's spacing (point
+     * queries: point_spacing), the craters added on top; 0 evaluates the fBm at every cell. */
+    double post_spacing;
+    tg_ds_options refine;
 } tg_server_options;
 
 typedef struct tg_request {

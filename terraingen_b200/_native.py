@@ -193,7 +193,8 @@ class ServerOptions(C.Structure):
                 ("craters", Population), ("shaping", Shaping), ("base_spacing", _D),
                 ("point_spacing", _D), ("hbm_budget", C.c_uint64),
                 ("max_batch_cells", C.c_uint64), ("slots", _U32), ("region_cells", _U32),
-                ("variant", C.c_int32), ("reserved", _U32)]
+                ("variant", C.c_int32), ("reserved", _U32), ("post_spacing", _D),
+                ("refine", DsOptions)]
 
 
 class Request(C.Structure):

@@ -1281,60 +1281,6 @@ int tg_evaluate(tg_device* d, const tg_terrain* t, const tg_grid* grid, float* h
     return fail(TG_ERROR_MEMORY, "the layers' entries did not fit after growing");
 }
 
-namespace {
-
-// The output block of a diamond-square CTA and the shared buffers its node pyramid needs: the
-// largest block (64 x 64, 64 x 32, 32 x 32, ... cells) whose two buffers fit kDsSharedBudget
-// bytes, so that three CTAs share an SM. A bigger block recomputes fewer nodes of its neighbours'
-// (the margins the means need) per cell. Each level's box is bounded from the block's extent in
-// finest nodes (what the device works out, plus two nodes for the rounding of either side's
-// arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
-// its parents' box is half of it plus the square mean's margins.
-#ifndef TGB_DS_SHARED_BUDGET
-#define TGB_DS_SHARED_BUDGET (72 * 1024)
-#endif
-constexpr size_t kDsSharedBudget = TGB_DS_SHARED_BUDGET;
-
-bool ds_tile_shape(DsTile& t, bool spline) {
-    const int64_t reach = spline ? 3 : 1, before = spline ? 1 : 0, after = spline ? 2 : 1;
-    const Grid& g = t.grid;
-    constexpr uint32_t kShapes[][2] = {{64, 64}, {64, 32}, {32, 32}, {32, 16}, {16, 16}, {16, 8},
-                                       {8, 8},   {8, 4},   {4, 4},   {4, 2},   {2, 2},   {1, 1}};
-    for (const auto& shape : kShapes) {
-        const uint32_t bw = shape[0], bh = shape[1];
-        const double spanX = (double(bw - 1) * std::fabs(g.pixelWidth) +
-                              double(bh - 1) * std::fabs(g.rowRotation)) /
-                             std::fabs(t.frame.stepX);
-        const double spanY = (double(bw - 1) * std::fabs(g.colRotation) +
-                              double(bh - 1) * std::fabs(g.pixelHeight)) /
-                             std::fabs(t.frame.stepY);
-        if (!(spanX < 4096.0 && spanY < 4096.0)) {
-            continue;
-        }
-        int64_t w = int64_t(std::floor(spanX)) + 6 + after;
-        int64_t h = int64_t(std::floor(spanY)) + 6 + after;
-        uint64_t cap[2] = {0, 0};
-        for (int l = t.levels; l >= 1; --l) {
-            const int64_t ow = w + 2 * reach, oh = h + 2 * reach;
-            cap[l & 1] = std::max<uint64_t>(cap[l & 1], uint64_t(ow * oh));
-            w = ow / 2 + before + after + 1;
-            h = oh / 2 + before + after + 1;
-        }
-        cap[0] = std::max<uint64_t>(cap[0], uint64_t(w * h));
-        if ((cap[0] + cap[1]) * sizeof(double) <= kDsSharedBudget) {
-            t.blockW = bw;
-            t.blockH = bh;
-            t.blocksX = (g.width + bw - 1) / bw;
-            t.capEven = uint32_t(cap[0]);
-            t.capOdd = uint32_t(cap[1]);
-            return true;
-        }
-    }
-    return false;
-}
-
-}  // namespace
-
 int tg_ds_refine(tg_device* d, const float* posts, uint32_t pw, uint32_t ph,
                  const tg_grid* post_grid, const tg_ds_options* o, const tg_grid* grid,
                  float* heights, int memory, void* stream) {
@@ -1377,37 +1323,9 @@ int tg_ds_refine_window(tg_device* d, const float* posts, int64_t col0, int64_t 
     if (pw == 0 || ph == 0 || posts == nullptr || heights == nullptr) {
         return fail(TG_ERROR_ARGUMENT, "posts and heights are required");
     }
-    // Levels(post spacing, spacing) (diamond_square.cpp:289-300).
-    const double postSpacing = std::max(std::fabs(pg.pixelWidth), std::fabs(pg.pixelHeight));
-    const double spacing = std::max(std::fabs(g.pixelWidth), std::fabs(g.pixelHeight));
-    const double ratio = postSpacing / spacing;
-    int levels = 0;
-    if (ratio > 1.0) {
-        double most = 30.0;
-        if (o->min_pixel_size > 0.0) {
-            most = std::min(std::max(std::floor(std::log2(postSpacing / o->min_pixel_size) + 1e-9),
-                                     0.0),
-                            30.0);
-        }
-        levels = int(std::min(std::ceil(std::log2(ratio) - 1e-9), most));
-    }
-    // Frame (diamond_square.cpp:299-306): post (0, 0)'s center and the finest node steps.
     const bool spline = o->interp == 1u;
     DsTile t{};
-    t.grid = g;
-    t.frame.originX = pg.originX + 0.5 * pg.pixelWidth + 0.5 * pg.rowRotation;
-    t.frame.originY = pg.originY + 0.5 * pg.colRotation + 0.5 * pg.pixelHeight;
-    t.frame.stepX = std::ldexp(pg.pixelWidth, -levels);
-    t.frame.stepY = std::ldexp(-pg.pixelHeight, -levels);
-    t.levels = levels;
-    t.seed = o->seed;
-    // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
-    const double stepFactor = std::pow(2.0, -(3.0 - o->fractal_dimension) / 2.0);
-    for (int l = 1; l <= levels; ++l) {
-        t.squareStep[l] = o->scale * std::pow(stepFactor, 2 * l - 1);
-        t.diamondStep[l] = o->scale * std::pow(stepFactor, 2 * l);
-    }
-    if (!ds_tile_shape(t, spline)) {
+    if (!ds_setup(t, pg, o->fractal_dimension, o->scale, o->seed, o->min_pixel_size, spline, g)) {
         return fail(TG_ERROR_ARGUMENT, "the output cells are too coarse for the posts' nodes");
     }
     const cudaStream_t s = stream_of(d, memory, stream);

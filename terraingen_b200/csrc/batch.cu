@@ -22,6 +22,7 @@
 // whichever kernel shape (bin size, cells per thread) the autotuner picks.
 #include "binning.cuh"
 #include "crater_math.cuh"
+#include "ds_tile.cuh"
 #include "kernels.h"
 #include "noise_math.cuh"
 
@@ -444,6 +445,50 @@ __device__ __forceinline__ float point_source(const BatchNoise& noise, double x,
     return float(fma(noise.scale, double(sum) + double(err), double(noise.elevation)));
 }
 
+// Level-0 diamond-square nodes from the batch's source: node (col, row) is the post at
+// (col, row) * spacing, the fBm there as point_source evaluates it (rounded to float, as a DEM's
+// posts are).
+struct PostsFromSource {
+    const BatchNoise& noise;
+    double spacing;
+    __device__ __forceinline__ double operator()(int64_t col, int64_t row) const {
+        return double(point_source(noise, double(col) * spacing, double(row) * spacing));
+    }
+};
+
+// The diamond-square pass of a batch: persistent CTAs take the jobs' blocks in turn (a block's
+// job by binary search over the jobs' first blocks) and write each block's base heights into the
+// batch's output.
+template <bool kSpline>
+__global__ void __launch_bounds__(kDsTileThreads) batch_ds_kernel(const BatchNoise noise,
+                                                                 const BatchView v) {
+    extern __shared__ double pool[];
+    __shared__ DsShared sh;
+    __shared__ uint32_t sJob;
+    const BatchHeader* header = v.header;
+    const uint32_t jobs = header->dsJobs, blocks = header->dsBlocks;
+    float* const heights = header->heights;
+    for (uint32_t g = blockIdx.x; g < blocks; g += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t lo = 0, hi = jobs;
+            while (hi - lo > 1u) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (v.dsFirst[mid] <= g) {
+                    lo = mid;
+                } else {
+                    hi = mid;
+                }
+            }
+            sJob = lo;
+        }
+        __syncthreads();
+        const DsTile& t = v.dsJobs[sJob];
+        const PostsFromSource posts{noise, t.postSpacing};
+        ds_block<kSpline>(t, g - v.dsFirst[sJob], posts, heights + t.heightOffset, pool, sh);
+        __syncthreads();  // the next block's boxes overwrite this one's shared state
+    }
+}
+
 // One point of an indexed point set per thread: the source, then the craters of its resident
 // region's cell list (each within its cull distance), one write. Threads run independently.
 template <bool kFast>
@@ -457,7 +502,8 @@ __device__ __forceinline__ void indexed_points(const CraterShapeKernel& k,
     }
     const size_t at = size_t(t.pointBase) + i;
     const double x = v.points[2 * at], y = v.points[2 * at + 1];
-    const float base = point_source(noise, x, y);
+    const float base =
+        noise.baseInOutput ? heights[t.heightOffset + i] : point_source(noise, x, y);
     double acc = double(base);
     // The point's region from the set's region table.
     const double side = t.grid.pixelWidth;
@@ -604,68 +650,82 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells, 768 / (kBinW * kBinH / 
             }
         }
 
-        // 1. The source: Fractal2's octaves (fractal.h:219-240). Grid cells take their lattice
-        //    position from the tile's per-octave anchor (split in double) plus float steps;
-        //    points split their own position in double. Corner hashes are reused while the
-        //    lattice cell does not change.
-        // Compensated octave sums: sum + err carries the weighted octaves to about twice float
-        // precision (each product's rounding from an FMA residual, each sum's by TwoSum), so a
-        // source of kilometers keeps its millimeters.
-        float sum[kCells], err[kCells];
+        // 1. The source: the base a diamond-square pass already wrote into the output, or
+        //    Fractal2's octaves.
+        float h[kCells];
+        if (noise.baseInOutput) {
 #pragma unroll
-        for (int j = 0; j < kCells; ++j) {
-            sum[j] = 0.0f;
-            err[j] = 0.0f;
-        }
-        for (int o = 0; o < noise.octaves; ++o) {
-            const uint32_t sz = noise.seedTerm[o];
-            const float w = noise.weight[o];
-            int32_t cx = INT32_MIN, cy = INT32_MIN;
-            uint32_t h00 = 0, h10 = 0, h01 = 0, h11 = 0;
-            if (points) {
-                const double tc = noise.tc[o], ts = noise.ts[o], f = noise.frequency[o];
-#pragma unroll
-                for (int j = 0; j < kCells; ++j) {
-                    const double px = fma(fma(xd[j], tc, -yd[j] * ts), f, noise.ox[o]);
-                    const double py = fma(fma(xd[j], ts, yd[j] * tc), f, noise.oy[o]);
-                    const double lx = floor(px), ly = floor(py);
-                    const int32_t ix = int32_t(uint32_t(uint64_t(int64_t(lx))));
-                    const int32_t iy = int32_t(uint32_t(uint64_t(int64_t(ly))));
-                    if (ix != cx || iy != cy) {
-                        cx = ix;
-                        cy = iy;
-                        corners(ix, iy, sz, h00, h10, h01, h11);
-                    }
-                    accumulate(sum[j], err[j], w,
-                               perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)));
-                }
-            } else {
-                const OctaveAnchor a = v.anchors[t.anchorBase + o];
-                // Each cell from its own column, so heights do not depend on the kernel shape.
-                const float fr = float(row);
-                const float px = fmaf(fr, a.ay, a.fx);
-                const float py = fmaf(fr, a.by, a.fy);
-#pragma unroll
-                for (int j = 0; j < kCells; ++j) {
-                    const float qx = fmaf(float(col0 + j), a.ax, px);
-                    const float qy = fmaf(float(col0 + j), a.bx, py);
-                    const float lx = floorf(qx), ly = floorf(qy);
-                    const int32_t ix = int32_t(uint32_t(a.ix) + uint32_t(int32_t(lx)));
-                    const int32_t iy = int32_t(uint32_t(a.iy) + uint32_t(int32_t(ly)));
-                    if (ix != cx || iy != cy) {
-                        cx = ix;
-                        cy = iy;
-                        corners(ix, iy, sz, h00, h10, h01, h11);
-                    }
-                    accumulate(sum[j], err[j], w, perlin_at(h00, h10, h01, h11, qx - lx, qy - ly));
+            for (int j = 0; j < kCells; ++j) {
+                h[j] = 0.0f;
+                if (live[j]) {
+                    h[j] = points ? heights[t.heightOffset + v.pointIndex[t.pointBase + first + j]]
+                                  : heights[t.heightOffset + size_t(row) * t.pitch + col0 + j];
                 }
             }
-        }
-        float h[kCells];
+        } else {
+            // Fractal2's octaves (fractal.h:219-240). Grid cells take their lattice
+            //    position from the tile's per-octave anchor (split in double) plus float steps;
+            //    points split their own position in double. Corner hashes are reused while the
+            //    lattice cell does not change.
+            // Compensated octave sums: sum + err carries the weighted octaves to about twice float
+            // precision (each product's rounding from an FMA residual, each sum's by TwoSum), so a
+            // source of kilometers keeps its millimeters.
+            float sum[kCells], err[kCells];
 #pragma unroll
-        for (int j = 0; j < kCells; ++j) {
-            // elevation + amplitude * sum / total, formed once per cell in double.
-            h[j] = float(fma(noise.scale, double(sum[j]) + double(err[j]), double(noise.elevation)));
+            for (int j = 0; j < kCells; ++j) {
+                sum[j] = 0.0f;
+                err[j] = 0.0f;
+            }
+            for (int o = 0; o < noise.octaves; ++o) {
+                const uint32_t sz = noise.seedTerm[o];
+                const float w = noise.weight[o];
+                int32_t cx = INT32_MIN, cy = INT32_MIN;
+                uint32_t h00 = 0, h10 = 0, h01 = 0, h11 = 0;
+                if (points) {
+                    const double tc = noise.tc[o], ts = noise.ts[o], f = noise.frequency[o];
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        const double px = fma(fma(xd[j], tc, -yd[j] * ts), f, noise.ox[o]);
+                        const double py = fma(fma(xd[j], ts, yd[j] * tc), f, noise.oy[o]);
+                        const double lx = floor(px), ly = floor(py);
+                        const int32_t ix = int32_t(uint32_t(uint64_t(int64_t(lx))));
+                        const int32_t iy = int32_t(uint32_t(uint64_t(int64_t(ly))));
+                        if (ix != cx || iy != cy) {
+                            cx = ix;
+                            cy = iy;
+                            corners(ix, iy, sz, h00, h10, h01, h11);
+                        }
+                        accumulate(sum[j], err[j], w,
+                                   perlin_at(h00, h10, h01, h11, float(px - lx), float(py - ly)));
+                    }
+                } else {
+                    const OctaveAnchor a = v.anchors[t.anchorBase + o];
+                    // Each cell from its own column, so heights do not depend on the kernel shape.
+                    const float fr = float(row);
+                    const float px = fmaf(fr, a.ay, a.fx);
+                    const float py = fmaf(fr, a.by, a.fy);
+#pragma unroll
+                    for (int j = 0; j < kCells; ++j) {
+                        const float qx = fmaf(float(col0 + j), a.ax, px);
+                        const float qy = fmaf(float(col0 + j), a.bx, py);
+                        const float lx = floorf(qx), ly = floorf(qy);
+                        const int32_t ix = int32_t(uint32_t(a.ix) + uint32_t(int32_t(lx)));
+                        const int32_t iy = int32_t(uint32_t(a.iy) + uint32_t(int32_t(ly)));
+                        if (ix != cx || iy != cy) {
+                            cx = ix;
+                            cy = iy;
+                            corners(ix, iy, sz, h00, h10, h01, h11);
+                        }
+                        accumulate(sum[j], err[j], w, perlin_at(h00, h10, h01, h11, qx - lx, qy - ly));
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kCells; ++j) {
+                // elevation + amplitude * sum / total, formed once per cell in double.
+                h[j] = float(fma(noise.scale, double(sum[j]) + double(err[j]),
+                                 double(noise.elevation)));
+            }
         }
 
         // 2. Craters: each entry's data at its ref's base (the BinEntry's index field).
@@ -1107,6 +1167,39 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
         }
     }
     batch_totals_kernel<<<1, 1, 0, stream>>>(v);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_ds_setup(uint32_t& ctas) {
+    static const cudaError_t allowed = [] {
+        const cudaError_t e = cudaFuncSetAttribute(
+            batch_ds_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            int(kDsSharedBudget));
+        return e != cudaSuccess ? e
+                                : cudaFuncSetAttribute(batch_ds_kernel<false>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       int(kDsSharedBudget));
+    }();
+    if (allowed != cudaSuccess) {
+        return allowed;
+    }
+    int device = 0, sms = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err == cudaSuccess) {
+        err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    }
+    ctas = uint32_t(sms) * 3u;  // three CTAs of kDsSharedBudget node buffers share an SM
+    return err;
+}
+
+cudaError_t launch_batch_ds(const BatchNoise& noise, const BatchView& v, bool spline,
+                            uint32_t ctas, cudaStream_t stream) {
+    const size_t bytes = kDsSharedBudget;
+    if (spline) {
+        batch_ds_kernel<true><<<ctas, kDsTileThreads, bytes, stream>>>(noise, v);
+    } else {
+        batch_ds_kernel<false><<<ctas, kDsTileThreads, bytes, stream>>>(noise, v);
+    }
     return cudaGetLastError();
 }
 

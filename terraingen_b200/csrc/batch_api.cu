@@ -68,6 +68,8 @@ enum BatchSlot {
     kSlotScanScratch,
     kSlotHeader,
     kSlotOutput,
+    kSlotDsJobs,
+    kSlotDsFirst,
     kBatchSlotCount
 };
 
@@ -79,6 +81,7 @@ struct Signature {
     uint32_t ctas, maxRecordPairs, maxBoulderPairs;
     CraterShapeKernel kernel;
     BatchNoise noise;
+    uint32_t dsCtas, dsSpline;  // the diamond-square pass's CTAs (0: none), Catmull-Rom (1)
 };
 
 }  // namespace
@@ -95,6 +98,7 @@ struct tg_batch {
     bool loaded = false;
     Spec spec;
     std::vector<BatchTile> tiles;   // spec.items numbered for the current variant
+    uint32_t dsJobs = 0, dsBlocks = 0, dsCtas = 0;  // the diamond-square pass
     uint32_t bins = 0;
     uint32_t recordPairs = 0, boulderPairs = 0;
     size_t outputFloats = 0;
@@ -259,6 +263,8 @@ BatchView make_view(tg_batch* b) {
     v.pointRegions = ptr<PointRegion>(b, kSlotPointRegions);
     v.pointLists = f.pointLists;
     v.culls = f.culls;
+    v.dsJobs = ptr<DsTile>(b, kSlotDsJobs);
+    v.dsFirst = ptr<uint32_t>(b, kSlotDsFirst);
     return v;
 }
 
@@ -277,6 +283,8 @@ Signature signature(tg_batch* b) {
     s.maxBoulderPairs = capacity<int4>(b, kSlotBoulderWindows);
     std::memcpy(&s.kernel, &b->spec.kernel, sizeof(s.kernel));
     std::memcpy(&s.noise, &b->spec.noise, sizeof(s.noise));
+    s.dsCtas = b->spec.ds.on ? b->dsCtas : 0u;
+    s.dsSpline = b->spec.ds.on && b->spec.ds.spline ? 1u : 0u;
     return s;
 }
 
@@ -326,7 +334,12 @@ int capture(tg_batch* b, const Signature& s) {
         return st;
     }
     TG_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-    err = launch_batch_evaluate(s.kernel, s.noise, s.view, s.variant, s.fast, s.ctas, b->stream);
+    err = s.dsCtas != 0u ? launch_batch_ds(s.noise, s.view, s.dsSpline != 0u, s.dsCtas, b->stream)
+                         : cudaSuccess;
+    if (err == cudaSuccess) {
+        err = launch_batch_evaluate(s.kernel, s.noise, s.view, s.variant, s.fast, s.ctas,
+                                    b->stream);
+    }
     if (err == cudaSuccess) {
         err = cudaMemcpyAsync(&b->pinned[1], s.view.header, sizeof(BatchHeader),
                               cudaMemcpyDeviceToHost, b->stream);
@@ -458,6 +471,78 @@ void append_points(Spec& spec, const double* xy, uint32_t count) {
     }
 }
 
+// The diamond-square pass's jobs, one per item (after the points are on the device): a grid
+// item's blocks, or a point set's points, each written at its item's output offset.
+int load_ds(tg_batch* b) {
+    Spec& s = b->spec;
+    s.noise.baseInOutput = s.ds.on ? 1u : 0u;
+    b->dsJobs = 0;
+    b->dsBlocks = 0;
+    if (!s.ds.on) {
+        return TG_OK;
+    }
+    const double P = s.ds.postSpacing;
+    if (!(P > 0.0) || !std::isfinite(P) || !(s.ds.fractalDimension >= 2.0) ||
+        !(s.ds.fractalDimension <= 3.0) || !(s.ds.scale >= 0.0) || !(s.ds.minPixelSize >= 0.0)) {
+        return fail(TG_ERROR_ARGUMENT, "diamond-square source: post spacing > 0, fractal "
+                                       "dimension in [2, 3], scale and min pixel size >= 0");
+    }
+    TG_CUDA(batch_ds_setup(b->dsCtas), "diamond-square set-up");
+    // The post lattice as a grid whose cell (0, 0) is centered on the origin.
+    const Grid lattice{1u, 1u, -0.5 * P, P, 0.0, 0.5 * P, 0.0, -P};
+    uint32_t* flags = &ptr<BatchHeader>(b, kSlotHeader)->flags;
+    std::vector<DsTile> jobs;
+    std::vector<uint32_t> first;
+    jobs.reserve(s.items.size());
+    uint64_t blocks = 0;
+    for (const Item& it : s.items) {
+        DsTile t{};
+        if (it.points) {
+            const double d = it.dsSpacing;
+            if (!(d > 0.0) || !std::isfinite(d)) {
+                return fail(TG_ERROR_ARGUMENT, "point sets under a diamond-square source need "
+                                               "the spacing they are read at");
+            }
+            const Grid one{1u, 1u, -0.5 * d, d, 0.0, 0.5 * d, 0.0, -d};
+            if (!ds_setup(t, lattice, s.ds.fractalDimension, s.ds.scale, s.ds.seed,
+                          s.ds.minPixelSize, s.ds.spline, one)) {
+                return fail(TG_ERROR_ARGUMENT, "the points are too coarse for the posts' nodes");
+            }
+            t.points = ptr<double>(b, kSlotPoints) + 2 * size_t(it.pointBegin);
+            t.pointIndex = it.kind == kTileIndexedPoints
+                               ? nullptr
+                               : ptr<uint32_t>(b, kSlotPointIndex) + it.pointBegin;
+            t.blocks = it.grid.width;
+        } else {
+            if (!ds_setup(t, lattice, s.ds.fractalDimension, s.ds.scale, s.ds.seed,
+                          s.ds.minPixelSize, s.ds.spline, it.grid)) {
+                return fail(TG_ERROR_ARGUMENT, "a tile is too coarse for the posts' nodes");
+            }
+            t.pitch = it.pitch;
+        }
+        t.postSpacing = P;
+        t.heightOffset = it.heightOffset;
+        t.status = flags;
+        first.push_back(uint32_t(blocks));
+        blocks += t.blocks;
+        jobs.push_back(t);
+    }
+    if (blocks >= 0xffffffffull) {
+        return fail(TG_ERROR_UNSUPPORTED, "a batch's diamond-square pass holds fewer than 2^32 "
+                                          "blocks");
+    }
+    first.push_back(uint32_t(blocks));
+    if (int st = upload(b, kSlotDsJobs, jobs.data(), jobs.size())) {
+        return st;
+    }
+    if (int st = upload(b, kSlotDsFirst, first.data(), first.size())) {
+        return st;
+    }
+    b->dsJobs = uint32_t(jobs.size());
+    b->dsBlocks = uint32_t(blocks);
+    return TG_OK;
+}
+
 int load(tg_batch* b, Spec&& spec) {
     if (b->pending) {
         return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
@@ -540,6 +625,9 @@ int load(tg_batch* b, Spec&& spec) {
     TG_CUDA(b->slots[kSlotBoulderWindows].reserve(std::max<size_t>(bp, 1) * sizeof(int4)),
             "allocation");
     TG_CUDA(b->slots[kSlotHeader].reserve(sizeof(BatchHeader)), "allocation");
+    if (int st = load_ds(b)) {  // after the points and the header are on the device
+        return st;
+    }
     if (int st = plan_bins(b)) {
         return st;
     }
@@ -568,6 +656,8 @@ int launch(tg_batch* b, float* out, cudaStream_t stream) {
     h.refRecords = b->recordPairs;
     h.refBoulders = b->boulderPairs;
     h.heights = out;
+    h.dsJobs = b->dsJobs;
+    h.dsBlocks = b->dsBlocks;
     b->pinned[0] = h;
     const Signature s = signature(b);
     if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
@@ -608,6 +698,9 @@ int finish(tg_batch* b) {
         }
         if ((r.flags & 8u) && b->spec.fast) {
             return fail(TG_ERROR_STATE, "a record needs the general shaping path");
+        }
+        if (r.flags & 16u) {
+            return fail(TG_ERROR_MEMORY, "a diamond-square block outgrew its shared memory");
         }
         b->last.crater_pairs = r.craterPairs;
         b->last.boulder_pairs = r.boulderPairs;

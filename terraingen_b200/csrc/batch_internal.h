@@ -35,6 +35,21 @@ struct Item {
     double boulderWidth;
     uint32_t kind = kTileGrid;  // kTileGrid, kTilePoints or kTileIndexedPoints
     uint32_t tableBase = 0;     // indexed points: their region table in Spec::pointTable
+    double dsSpacing = 0.0;     // point sets under a diamond-square source: the spacing read at
+};
+
+// A diamond-square source in place of the fBm at every cell (DiamondSquareUpsampler over a DEM,
+// src/sources/diamond_square.cpp:488-516): the batch's fBm sampled at a post lattice of
+// `postSpacing` (post (i, j) at (i, -j) * postSpacing, node (i, j) of level 0 at (i, j) *
+// postSpacing), rounded to float as a DEM's posts, refined to each item's spacing (point sets:
+// Item::dsSpacing) with DiamondSquareOptions' fractal dimension, scale, seed, minimum pixel size
+// and interpolation.
+struct DsSource {
+    bool on = false;
+    double postSpacing = 0.0;
+    double fractalDimension = 2.2, scale = 0.0, minPixelSize = 0.0;
+    uint32_t seed = 0;
+    bool spline = false;
 };
 
 // Device arrays the refs index; the batch reads them and owns none.
@@ -60,6 +75,7 @@ struct Spec {
     std::vector<uint32_t> pointTable;       // indexed points: region tables (kernels.h)
     BatchNoise noise{};
     std::vector<Octave> octaves;
+    DsSource ds;
     CraterShapeKernel kernel{};
     bool fast = true;
     Features features;

@@ -13,443 +13,20 @@
 //
 // Compiled with -fmad=false, so the means and the read-out round as the reference's; the normal
 // draws are float Box-Muller on exact double uniforms (node_normal).
-#include "kernels.h"
+#include <algorithm>
+#include <cmath>
+
+#include "ds_tile.cuh"
 
 namespace tgb {
 namespace {
-
-constexpr uint32_t kMidpointDisplacementStream = 0x524D4450u;  // streams.h:73
-
-struct Words {
-    uint32_t x, y, z, w;
-};
-
-// Philox4x32-10 (include/terraingen/random/philox.h:43-91).
-__device__ __forceinline__ Words philox(Words c, uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int round = 0; round < 10; ++round) {
-        if (round > 0) {
-            k0 += 0x9E3779B9u;
-            k1 += 0xBB67AE85u;
-        }
-        // Each 32 x 32 -> 64-bit product in one wide multiply: its high and low words.
-        const uint64_t p0 = uint64_t(0xD2511F53u) * c.x, p1 = uint64_t(0xCD9E8D57u) * c.z;
-        c = Words{uint32_t(p1 >> 32) ^ c.y ^ k0, uint32_t(p1), uint32_t(p0 >> 32) ^ c.w ^ k1,
-                  uint32_t(p0)};
-    }
-    return c;
-}
-
-// ln 2 split for k ln 2 + log1p(f) (Cody and Waite): the high part has 12 significant bits, so
-// its product with any |k| <= 64 is exact in float.
-constexpr float kLn2High = 0.693145751953125f;
-constexpr float kLn2Low = float(0.69314718055994530942 - 0.693145751953125);
-
-// log(n 2^-53) in float for an integer 1 <= n <= 2^53, with the relative accuracy of log1pf near
-// n = 2^53 (where the logarithm goes to 0). n 2^-53 = 2^k (1 + f) with 1 + f in [0.75, 1.5): f is
-// an integer difference, exact before its one rounding to float, and the logarithm is
-// k ln 2 + log1pf(f), one path for every lane.
-__device__ __forceinline__ float log_of_ratio(uint64_t n) {
-    const int bits = 64 - __clzll(n);  // n in [2^(bits - 1), 2^bits)
-    const bool upper = n >= (3ull << (bits - 2 < 0 ? 0 : bits - 2)) && bits >= 2;
-    const int e = upper ? bits : bits - 1;  // 1 + f = n / 2^e
-    const float f = float(int64_t(n) - int64_t(1ull << e)) * __int_as_float((127 - e) << 23);
-    const float k = float(e - 53);
-    return fmaf(k, kLn2High, fmaf(k, kLn2Low, log1pf(f)));
-}
-
-// The standard normal of node (col, row) of `level` (Refinement::Displacement,
-// diamond_square.cpp:382-389): one Philox block is RandomStream's first two NextDouble draws
-// (u1, u2, 53 bits each, exact), turned into a normal by Box-Muller (StandardNormal,
-// src/random/samplers.cpp:65-69), sqrt(-2 log(1 - u1)) cos(2 pi u2). The reference evaluates it
-// in double; here the logarithm, the square root and the cosine run in float on arguments formed
-// exactly in integers or double, within 2e-6 of the double normal (a few 1e-7 of the radius;
-// under 1e-5 m in the refined heights) for a fraction of the instructions: the steps are bound by
-// issuing them.
-__device__ __forceinline__ double node_normal(int64_t col, int64_t row, int level,
-                                              uint32_t seed) {
-    const uint32_t high = uint32_t((col >> 32) ^ (row >> 32));
-    const Words b = philox(Words{uint32_t(col), uint32_t(row), uint32_t(level) | (high << 5), 0u},
-                           seed, kMidpointDisplacementStream);
-    // u1 = m1 2^-53 and u2 = m2 2^-53; 1 - u1 = (2^53 - m1) 2^-53 exactly.
-    const uint64_t m1 = (uint64_t(b.x >> 5u) << 26u) | uint64_t(b.y >> 6u);
-    const uint64_t m2 = (uint64_t(b.z >> 5u) << 26u) | uint64_t(b.w >> 6u);
-    const float radius = sqrtf(-2.0f * log_of_ratio((1ull << 53) - m1));
-    // cos(pi a) for a = 2 u2 split into float parts a = high + low: cos(pi high) - pi low
-    // sin(pi high), so the float rounding of a costs no accuracy.
-    const double a = double(m2) * 0x1p-52;
-    const float aHigh = float(a), aLow = float(a - double(aHigh));
-    float sine, cosine;
-    sincospif(aHigh, &sine, &cosine);
-    const float c = fmaf(-3.14159265f * aLow, sine, cosine);
-    return double(radius) * double(c);
-}
-
-// Catmull-Rom weights of four nodes around a midpoint (diamond_square.cpp:37).
-__device__ __constant__ const double kMid[4] = {-1.0 / 16.0, 9.0 / 16.0, 9.0 / 16.0, -1.0 / 16.0};
-
-__device__ __forceinline__ int64_t floor_half(int64_t v) {  // FloorHalf, diamond_square.cpp:39
-    return v >= 0 ? v / 2 : -((1 - v) / 2);
-}
-
-// A box of nodes [c0, c0 + w) x [r0, r0 + h) of one level, row-major in shared memory.
-struct NodeBox {
-    int64_t c0, r0;
-    int32_t w, h;
-};
-
-struct Nodes {
-    NodeBox b;
-    double* v;
-    __device__ __forceinline__ double at(int64_t col, int64_t row) const {
-        return v[int32_t(row - b.r0) * b.w + int32_t(col - b.c0)];
-    }
-};
-
-// `value` as an integer when within 1e-6 of one (NearestWhole, src/sources/lattice.h:33), else
-// the node below and the share of the way to the next (NodeAndShare, diamond_square.cpp:53).
-__device__ __forceinline__ void node_and_share(double u, int64_t& node, double& share) {
-    const double rounded = round(u);
-    if (fabs(u - rounded) <= 1e-6) {
-        node = int64_t(rounded);
-        share = 0.0;
-        return;
-    }
-    const double below = floor(u);
-    node = int64_t(below);
-    share = u - below;
-}
-
-// The Keys cubic (a = -0.5) at an offset of `x` nodes (CubicWeight, src/raster/resample.cpp:20).
-__device__ __forceinline__ double cubic_weight(double x) {
-    x = fabs(x);
-    if (x <= 1.0) {
-        return (1.5 * x - 2.5) * x * x + 1.0;
-    }
-    if (x < 2.0) {
-        return ((-0.5 * x + 2.5) * x - 4.0) * x + 2.0;
-    }
-    return 0.0;
-}
-
-// The finest nodes read at (x, y) (Refinement::Interpolate, diamond_square.cpp:461-485):
-// bilinear, or Catmull-Rom over the 4 x 4 nodes around (InterpolateLatticeWeights with the
-// cubic's KernelWeights, src/raster/kernels.h:32-51; taps of zero weight skipped).
-template <bool kSpline>
-__device__ __forceinline__ double read_nodes(const Nodes& n, const DsFrame& frame, double x,
-                                             double y) {
-    int64_t col, row;
-    double u, v;
-    node_and_share((x - frame.originX) / frame.stepX, col, u);
-    node_and_share((y - frame.originY) / frame.stepY, row, v);
-    if (kSpline) {
-        double wx[4], wy[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            wx[i] = cubic_weight(u - double(i - 1));
-            wy[i] = cubic_weight(v - double(i - 1));
-        }
-        double sum = 0.0;
-        for (int j = 0; j < 4; ++j) {
-            for (int i = 0; i < 4; ++i) {
-                if (wx[i] * wy[j] == 0.0) {
-                    continue;
-                }
-                sum += wx[i] * wy[j] * n.at(col - 1 + i, row - 1 + j);
-            }
-        }
-        return sum;
-    }
-    double value = n.at(col, row);
-    if (u > 0.0) {
-        value = value * (1.0 - u) + n.at(col + 1, row) * u;
-    }
-    if (v > 0.0) {
-        double above = n.at(col, row + 1);
-        if (u > 0.0) {
-            above = above * (1.0 - u) + n.at(col + 1, row + 1) * u;
-        }
-        value = value * (1.0 - v) + above * v;
-    }
-    return value;
-}
-
-__device__ __forceinline__ void cell_center(const Grid& g, uint32_t c, uint32_t r, double& x,
-                                            double& y) {
-    x = g.originX + (double(c) + 0.5) * g.pixelWidth + (double(r) + 0.5) * g.rowRotation;
-    y = g.originY + (double(c) + 0.5) * g.colRotation + (double(r) + 0.5) * g.pixelHeight;
-}
-
-// Walks a w x h box (w > 0) in row-major order with the CTA's threads, thread k taking items k,
-// k + n, k + 2n, ... (n threads): consecutive threads take neighbouring nodes, the work splits
-// evenly, and a thread steps its (x, y) without dividing.
-struct BoxWalk {
-    int32_t x, y, dx, dy, w;
-    __device__ __forceinline__ explicit BoxWalk(int32_t width) : w(width) {
-        const int32_t k = int32_t(threadIdx.x), n = int32_t(blockDim.x);
-        x = k % w;
-        y = k / w;
-        dx = n % w;
-        dy = n / w;
-    }
-    __device__ __forceinline__ void next() {
-        x += dx;
-        y += dy;
-        if (x >= w) {
-            x -= w;
-            ++y;
-        }
-    }
-};
-
-constexpr uint32_t kDsMaxBlock = 64;  // the largest block side the host picks
-
-// Per-block shared state besides the node buffers.
-struct DsShared {
-    NodeBox inner[kMaxDsLevels + 1];
-    int32_t colNode[kDsMaxBlock], rowNode[kDsMaxBlock];  // north-up grids: a column's and a row's
-    double colShare[kDsMaxBlock], rowShare[kDsMaxBlock];  // finest node and share (read step)
-    int fits;
-};
-
-// One CTA refines the nodes an output block of t.blockW x t.blockH cells reads, every level in
-// shared memory, and writes only the block's heights (Refinement::Refine, diamond_square.cpp:
-// 426-448, with the boxes worked out top-down as its recursion does). Node values do not depend
-// on the box they are computed in: displacements are keyed by (seed, node, level) through
-// Philox4x32-10 and means are local, so neighbouring blocks agree on every node they share.
-//   level 0   nodes from the posts: node (col, row) is post (col, -row) of the lattice, the
-//             window held being its columns col0.. and rows row0.., reads past it repeating its
-//             edge (BaseNodes, diamond_square.cpp:311; PostIndex, src/sources/lattice.h:99);
-//   level l   the square step over the box the diamond step reads (SquareStep, :392-407: kept
-//             parents and displaced odd/odd nodes), then the diamond step over the box the next
-//             level reads (DiamondStep, :410-424), in place;
-//   read      each cell from the finest level.
-// Levels of even and odd number alternate between two shared buffers of t.capEven and t.capOdd
-// doubles. Thread 0 works out the boxes; one that would outgrow its buffer (the host sizes them
-// from the block's extent, so never) sets flag 1 and the CTA writes nothing. Loops run over local
-// 32-bit box coordinates; only the displacement's key takes the node's 64-bit index.
-template <bool kSpline>
-__device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, double* pool,
-                                         DsShared& sh) {
-    constexpr int64_t kReach = kSpline ? 3 : 1;   // the diamond mean's reach (Refine's `reach`)
-    constexpr int64_t kBefore = kSpline ? 1 : 0;  // parents a square mean reads before its block
-    constexpr int64_t kAfter = kSpline ? 2 : 1;   // and after it; the read's nodes after a cell
-    const uint32_t bx = block % t.blocksX, by = block / t.blocksX;
-    const uint32_t c0 = bx * t.blockW, r0 = by * t.blockH;
-    const uint32_t cw = min(t.blockW, t.grid.width - c0), rh = min(t.blockH, t.grid.height - r0);
-    const int levels = t.levels;
-    const bool northUp = t.grid.rowRotation == 0.0 && t.grid.colRotation == 0.0;
-    if (threadIdx.x == 0) {
-        double umin = INFINITY, umax = -INFINITY, vmin = INFINITY, vmax = -INFINITY;
-        for (int k = 0; k < 4; ++k) {
-            double x, y;
-            cell_center(t.grid, c0 + ((k & 1) ? cw - 1 : 0), r0 + ((k & 2) ? rh - 1 : 0), x, y);
-            const double u = (x - t.frame.originX) / t.frame.stepX;
-            const double v = (y - t.frame.originY) / t.frame.stepY;
-            umin = fmin(umin, u);
-            umax = fmax(umax, u);
-            vmin = fmin(vmin, v);
-            vmax = fmax(vmax, v);
-        }
-        const int64_t fc0 = int64_t(floor(umin)) - 1, fc1 = int64_t(ceil(umax)) + kAfter;
-        const int64_t fr0 = int64_t(floor(vmin)) - 1, fr1 = int64_t(ceil(vmax)) + kAfter;
-        bool ok = fc1 - fc0 < 65536 && fr1 - fr0 < 65536;
-        sh.inner[levels] = NodeBox{fc0, fr0, int32_t(fc1 - fc0 + 1), int32_t(fr1 - fr0 + 1)};
-        for (int l = levels; l >= 1 && ok; --l) {
-            const NodeBox& b = sh.inner[l];
-            const int64_t oc0 = b.c0 - kReach, oc1 = b.c0 + b.w - 1 + kReach;
-            const int64_t or0 = b.r0 - kReach, or1 = b.r0 + b.h - 1 + kReach;
-            ok = (oc1 - oc0 + 1) * (or1 - or0 + 1) <= int64_t((l & 1) ? t.capOdd : t.capEven);
-            const int64_t pc0 = floor_half(oc0) - kBefore, pc1 = floor_half(oc1) + kAfter;
-            const int64_t pr0 = floor_half(or0) - kBefore, pr1 = floor_half(or1) + kAfter;
-            sh.inner[l - 1] = NodeBox{pc0, pr0, int32_t(pc1 - pc0 + 1), int32_t(pr1 - pr0 + 1)};
-        }
-        ok = ok && int64_t(sh.inner[0].w) * sh.inner[0].h <= int64_t(t.capEven);
-        sh.fits = ok ? 1 : 0;
-        if (!ok) {
-            atomicOr(t.status, 1u);
-        }
-    }
-    __syncthreads();
-    if (!sh.fits) {
-        return;
-    }
-    if (northUp) {
-        // A north-up cell's x depends on its column alone and its y on its row alone (the other
-        // term of cell_center is an exact zero), so their finest node (relative to the finest
-        // box) and share are found once per column and row.
-        const int64_t fc0 = sh.inner[levels].c0 - (levels > 0 ? kReach : 0);
-        const int64_t fr0 = sh.inner[levels].r0 - (levels > 0 ? kReach : 0);
-        for (uint32_t i = threadIdx.x; i < cw + rh; i += blockDim.x) {
-            double x, y;
-            int64_t node;
-            double share;
-            if (i < cw) {
-                cell_center(t.grid, c0 + i, r0, x, y);
-                node_and_share((x - t.frame.originX) / t.frame.stepX, node, share);
-                sh.colShare[i] = share;
-                sh.colNode[i] = int32_t(node - fc0);
-            } else {
-                cell_center(t.grid, c0, r0 + (i - cw), x, y);
-                node_and_share((y - t.frame.originY) / t.frame.stepY, node, share);
-                sh.rowShare[i - cw] = share;
-                sh.rowNode[i - cw] = int32_t(node - fr0);
-            }
-        }
-    }
-    {
-        const NodeBox p = sh.inner[0];
-        for (BoxWalk it(p.w); it.y < p.h; it.next()) {
-            const int64_t row = -(p.r0 + it.y) - t.row0;
-            const int64_t col = p.c0 + it.x - t.col0;
-            const int64_t pr = row < 0 ? 0 : (row >= int64_t(t.ph) ? int64_t(t.ph) - 1 : row);
-            const int64_t pc = col < 0 ? 0 : (col >= int64_t(t.pw) ? int64_t(t.pw) - 1 : col);
-            pool[it.y * p.w + it.x] = double(t.posts[size_t(pr) * t.pw + size_t(pc)]);
-        }
-    }
-    __syncthreads();
-    NodeBox pb = sh.inner[0];
-    const double* parents = pool;
-    for (int l = 1; l <= levels; ++l) {
-        const NodeBox d = sh.inner[l];
-        const NodeBox ob{d.c0 - kReach, d.r0 - kReach, int32_t(d.w + 2 * kReach),
-                         int32_t(d.h + 2 * kReach)};
-        double* out = (l & 1) ? pool + t.capEven : pool;
-        const double squareStep = t.squareStep[l], diamondStep = t.diamondStep[l];
-        // Square step: the 2 x 2 blocks anchored at even (col, row) that meet the box. Block
-        // (i, j) is parent (sc0 + i, sr0 + j); its even node sits at local (oc, orow) of the
-        // output box and its odd/odd node one further along both axes. A thread takes two
-        // neighbouring blocks of a row at a time and draws both displacements before it reads
-        // any node, so their two Philox chains run interleaved.
-        {
-            const int64_t sc0 = floor_half(ob.c0), sr0 = floor_half(ob.r0);
-            const int32_t sw = int32_t(floor_half(ob.c0 + ob.w - 1) - sc0 + 1);
-            const int32_t shh = int32_t(floor_half(ob.r0 + ob.h - 1) - sr0 + 1);
-            const int32_t pcBase = int32_t(sc0 - pb.c0), prBase = int32_t(sr0 - pb.r0);
-            const int32_t ocBase = int32_t(2 * sc0 - ob.c0), orBase = int32_t(2 * sr0 - ob.r0);
-            for (BoxWalk it((sw + 1) / 2); it.y < shh; it.next()) {
-                const int32_t j = it.y;
-                const int64_t row = 2 * (sr0 + j) + 1;
-                double normal[2];
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    normal[k] = node_normal(2 * (sc0 + 2 * it.x + k) + 1, row, l, t.seed);
-                }
-                const int32_t orow = orBase + 2 * j;
-                const double* p0 = parents + (prBase + j) * pb.w + pcBase;
-                const double* p1 = p0 + pb.w;
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int32_t i = 2 * it.x + k;
-                    const int32_t oc = ocBase + 2 * i;
-                    if (i >= sw) {
-                        break;
-                    }
-                    if (oc >= 0 && orow >= 0) {
-                        out[orow * ob.w + oc] = p0[i];
-                    }
-                    if (oc + 1 >= ob.w || orow + 1 >= ob.h) {
-                        continue;
-                    }
-                    double mean;
-                    if (!kSpline) {
-                        mean = 0.25 * (p0[i] + p0[i + 1] + p1[i] + p1[i + 1]);
-                    } else {
-                        mean = 0.0;
-                        for (int32_t b = 0; b < 4; ++b) {
-                            const double* line = p0 + (b - 1) * pb.w + i - 1;
-                            double acc = 0.0;
-                            for (int32_t a = 0; a < 4; ++a) {
-                                acc += kMid[a] * line[a];
-                            }
-                            mean += kMid[b] * acc;
-                        }
-                    }
-                    out[(orow + 1) * ob.w + oc + 1] = mean + squareStep * normal[k];
-                }
-            }
-        }
-        __syncthreads();
-        // Diamond step: the mixed nodes (2 bc + 1, 2 br) and (2 bc, 2 br + 1) inside the box the
-        // next level reads, from the square step's nodes around them (kReach local columns and
-        // rows of the output box lie before the inner box). Both displacements of a block are
-        // drawn before its nodes are read.
-        {
-            const int64_t dc0 = floor_half(d.c0), dr0 = floor_half(d.r0);
-            const int32_t dw = int32_t(floor_half(d.c0 + d.w - 1) - dc0 + 1);
-            const int32_t dh = int32_t(floor_half(d.r0 + d.h - 1) - dr0 + 1);
-            const int32_t lcBase = int32_t(2 * dc0 - d.c0), lrBase = int32_t(2 * dr0 - d.r0);
-            for (BoxWalk it(dw); it.y < dh; it.next()) {
-                const int32_t i = it.x, j = it.y;
-                double normal[2];
-#pragma unroll
-                for (int n = 0; n < 2; ++n) {
-                    // Inner-box local position of the node: (2 i + 1, 2 j) or (2 i, 2 j + 1).
-                    const int32_t lc = lcBase + 2 * i + (n == 0 ? 1 : 0);
-                    const int32_t lr = lrBase + 2 * j + (n == 0 ? 0 : 1);
-                    normal[n] = node_normal(d.c0 + lc, d.r0 + lr, l, t.seed);
-                }
-#pragma unroll
-                for (int n = 0; n < 2; ++n) {
-                    const int32_t lc = lcBase + 2 * i + (n == 0 ? 1 : 0);
-                    const int32_t lr = lrBase + 2 * j + (n == 0 ? 0 : 1);
-                    if (lc < 0 || lc >= d.w || lr < 0 || lr >= d.h) {
-                        continue;
-                    }
-                    double* at = out + (lr + int32_t(kReach)) * ob.w + lc + int32_t(kReach);
-                    double mean;
-                    if (!kSpline) {
-                        mean = 0.25 * (at[-1] + at[1] + at[-ob.w] + at[ob.w]);
-                    } else {
-                        double alongX = 0.0, alongY = 0.0;
-                        for (int32_t k = 0; k < 4; ++k) {
-                            alongX += kMid[k] * at[-3 + 2 * k];
-                            alongY += kMid[k] * at[(-3 + 2 * k) * ob.w];
-                        }
-                        mean = 0.5 * (alongX + alongY);
-                    }
-                    *at = mean + diamondStep * normal[n];
-                }
-            }
-        }
-        __syncthreads();
-        parents = out;
-        pb = ob;
-    }
-    // The read: consecutive threads take consecutive cells of a row.
-    const Nodes finest{pb, const_cast<double*>(parents)};
-    for (BoxWalk it{int32_t(cw)}; it.y < int32_t(rh); it.next()) {
-        const uint32_t c = uint32_t(it.x), r = uint32_t(it.y);
-        double value;
-        if (northUp && !kSpline) {
-            const int32_t lc = sh.colNode[c], lr = sh.rowNode[r];
-            const double u = sh.colShare[c], v = sh.rowShare[r];
-            const double* at = parents + lr * pb.w + lc;
-            value = at[0];
-            if (u > 0.0) {
-                value = value * (1.0 - u) + at[1] * u;
-            }
-            if (v > 0.0) {
-                double above = at[pb.w];
-                if (u > 0.0) {
-                    above = above * (1.0 - u) + at[pb.w + 1] * u;
-                }
-                value = value * (1.0 - v) + above * v;
-            }
-        } else {
-            double x, y;
-            cell_center(t.grid, c0 + c, r0 + r, x, y);
-            value = read_nodes<kSpline>(finest, t.frame, x, y);
-        }
-        t.heights[size_t(r0 + r) * t.pitch + c0 + c] = float(value);
-    }
-}
 
 template <bool kSpline>
 __global__ void __launch_bounds__(kDsTileThreads) ds_tile_kernel(const DsTile t) {
     extern __shared__ double pool[];
     __shared__ DsShared sh;
-    ds_block<kSpline>(t, blockIdx.x, pool, sh);
+    const PostsFromArray posts{t.posts, t.col0, t.row0, t.pw, t.ph};
+    ds_block<kSpline>(t, blockIdx.x, posts, t.heights, pool, sh);
 }
 
 __global__ void philox_probe_kernel(const uint32_t* __restrict__ in, uint32_t n,
@@ -470,7 +47,91 @@ __global__ void philox_probe_kernel(const uint32_t* __restrict__ in, uint32_t n,
 }
 
 
+// The output block of a diamond-square CTA and the shared buffers its node pyramid needs: the
+// largest block (64 x 64, 64 x 32, 32 x 32, ... cells) whose two buffers fit kDsSharedBudget
+// bytes, so that three CTAs share an SM. A bigger block recomputes fewer nodes of its neighbours'
+// (the margins the means need) per cell. Each level's box is bounded from the block's extent in
+// finest nodes (what the device works out, plus two nodes for the rounding of either side's
+// arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
+// its parents' box is half of it plus the square mean's margins.
+
+bool ds_tile_shape(DsTile& t, bool spline) {
+    const int64_t reach = spline ? 3 : 1, before = spline ? 1 : 0, after = spline ? 2 : 1;
+    const Grid& g = t.grid;
+    constexpr uint32_t kShapes[][2] = {{64, 64}, {64, 32}, {32, 32}, {32, 16}, {16, 16}, {16, 8},
+                                       {8, 8},   {8, 4},   {4, 4},   {4, 2},   {2, 2},   {1, 1}};
+    for (const auto& shape : kShapes) {
+        const uint32_t bw = shape[0], bh = shape[1];
+        const double spanX = (double(bw - 1) * std::fabs(g.pixelWidth) +
+                              double(bh - 1) * std::fabs(g.rowRotation)) /
+                             std::fabs(t.frame.stepX);
+        const double spanY = (double(bw - 1) * std::fabs(g.colRotation) +
+                              double(bh - 1) * std::fabs(g.pixelHeight)) /
+                             std::fabs(t.frame.stepY);
+        if (!(spanX < 4096.0 && spanY < 4096.0)) {
+            continue;
+        }
+        int64_t w = int64_t(std::floor(spanX)) + 6 + after;
+        int64_t h = int64_t(std::floor(spanY)) + 6 + after;
+        uint64_t cap[2] = {0, 0};
+        for (int l = t.levels; l >= 1; --l) {
+            const int64_t ow = w + 2 * reach, oh = h + 2 * reach;
+            cap[l & 1] = std::max<uint64_t>(cap[l & 1], uint64_t(ow * oh));
+            w = ow / 2 + before + after + 1;
+            h = oh / 2 + before + after + 1;
+        }
+        cap[0] = std::max<uint64_t>(cap[0], uint64_t(w * h));
+        if ((cap[0] + cap[1]) * sizeof(double) <= kDsSharedBudget) {
+            t.blockW = bw;
+            t.blockH = bh;
+            t.blocksX = (g.width + bw - 1) / bw;
+            t.capEven = uint32_t(cap[0]);
+            t.capOdd = uint32_t(cap[1]);
+            return true;
+        }
+    }
+    return false;
+}
+
+
 }  // namespace
+
+bool ds_setup(DsTile& t, const Grid& pg, double fractalDimension, double scale, uint32_t seed,
+              double minPixelSize, bool spline, const Grid& g) {
+    // Levels(post spacing, spacing) (diamond_square.cpp:289-300).
+    const double postSpacing = std::max(std::fabs(pg.pixelWidth), std::fabs(pg.pixelHeight));
+    const double spacing = std::max(std::fabs(g.pixelWidth), std::fabs(g.pixelHeight));
+    const double ratio = postSpacing / spacing;
+    int levels = 0;
+    if (ratio > 1.0) {
+        double most = 30.0;
+        if (minPixelSize > 0.0) {
+            most = std::min(std::max(std::floor(std::log2(postSpacing / minPixelSize) + 1e-9), 0.0),
+                            30.0);
+        }
+        levels = int(std::min(std::ceil(std::log2(ratio) - 1e-9), most));
+    }
+    // Frame (diamond_square.cpp:299-306): post (0, 0)'s center and the finest node steps.
+    t.grid = g;
+    t.frame.originX = pg.originX + 0.5 * pg.pixelWidth + 0.5 * pg.rowRotation;
+    t.frame.originY = pg.originY + 0.5 * pg.colRotation + 0.5 * pg.pixelHeight;
+    t.frame.stepX = std::ldexp(pg.pixelWidth, -levels);
+    t.frame.stepY = std::ldexp(-pg.pixelHeight, -levels);
+    t.levels = levels;
+    t.seed = seed;
+    // Displacement scales per level (Refinement::Displacement, diamond_square.cpp:382-389).
+    const double stepFactor = std::pow(2.0, -(3.0 - fractalDimension) / 2.0);
+    for (int l = 1; l <= levels; ++l) {
+        t.squareStep[l] = scale * std::pow(stepFactor, 2 * l - 1);
+        t.diamondStep[l] = scale * std::pow(stepFactor, 2 * l);
+    }
+    t.pitch = g.width;
+    if (!ds_tile_shape(t, spline)) {
+        return false;
+    }
+    t.blocks = t.blocksX * ((g.height + t.blockH - 1) / t.blockH);
+    return true;
+}
 
 cudaError_t launch_ds_tiles(const DsTile& t, bool spline, cudaStream_t stream) {
     const uint32_t blocks = t.blocksX * ((t.grid.height + t.blockH - 1) / t.blockH);

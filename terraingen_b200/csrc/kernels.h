@@ -198,24 +198,42 @@ constexpr int kMaxDsLevels = 30;
 #define TGB_DS_THREADS 256
 #endif
 constexpr uint32_t kDsTileThreads = TGB_DS_THREADS;  // threads of a diamond-square CTA
-// One refinement's launch (launch_ds_tiles): `levels` refinements of the posts read at every cell
-// of `grid` into `heights` (row-major, `pitch` floats a row), a CTA per blockW x blockH cells
-// (sides at most 64).
+// One refinement job: `levels` refinements of the posts read at every cell of `grid` into
+// `heights` (row-major, `pitch` floats a row), a CTA per blockW x blockH cells (sides at most 64);
+// or, with `points` set, at each of `blocks` points (x, y pairs), a CTA per point, point k's
+// height at heights[pointIndex[k]] (heights[k] without an index). launch_ds_tiles runs one job
+// with posts from an array; the batch engine runs many with posts from its source.
 struct DsTile {
     Grid grid;
     DsFrame frame;                           // the finest level's
     int levels;
     uint32_t seed;
     uint32_t blockW, blockH, blocksX, pitch;
+    uint32_t blocks;                         // blocks of the job
     uint32_t capEven, capOdd;                // doubles of the even / odd levels' shared buffers
     double squareStep[kMaxDsLevels + 1];     // displacement scale per level (index 1..levels)
     double diamondStep[kMaxDsLevels + 1];
     const float* posts;                      // the lattice's columns col0.. and rows row0..
     int64_t col0, row0;
     uint32_t pw, ph;
+    double postSpacing;                      // posts from a source: node (c, r) at (c, r) * this
+    const double* points;                    // point jobs: the points
+    const uint32_t* pointIndex;              // point jobs: where each one's height goes
+    uint64_t heightOffset;                   // batch jobs: heights of the batch's output
     float* heights;
     uint32_t* status;                        // flag 1: a block's boxes outgrew their buffers
 };
+// Shared bytes of a diamond-square CTA's node buffers: three CTAs share an SM.
+#ifndef TGB_DS_SHARED_BUDGET
+#define TGB_DS_SHARED_BUDGET (72 * 1024)
+#endif
+constexpr size_t kDsSharedBudget = TGB_DS_SHARED_BUDGET;
+// The refinement of posts on `postGrid` (a lattice: post (0, 0) at its cell (0, 0)) read at
+// `grid`'s cells (Levels, the frame and Displacement, diamond_square.cpp:289-389): fills t's
+// grid, frame, levels, seed, displacement scales, pitch (grid.width), block shape and blocks.
+// False when no block's node buffers fit kDsSharedBudget.
+bool ds_setup(DsTile& t, const Grid& postGrid, double fractalDimension, double scale,
+              uint32_t seed, double minPixelSize, bool spline, const Grid& grid);
 cudaError_t launch_ds_tiles(const DsTile& t, bool spline, cudaStream_t stream);
 // Philox4x32-10 of n (counter, key) sextets, and the displacement normal the first two counter
 // words, the third's low 5 bits and the key's first word key as (col, row, level, seed).
@@ -292,6 +310,7 @@ static_assert(sizeof(OctaveAnchor) == 32, "OctaveAnchor layout");
 struct BatchNoise {
     int32_t octaves;
     float amplitude, total, elevation;
+    uint32_t baseInOutput;  // 1: the source is already in the output (a diamond-square pass)
     double scale;  // amplitude / total
     uint32_t seedTerm[kBatchMaxOctaves];  // octave seed through pcg3d's first LCG step
     float weight[kBatchMaxOctaves];
@@ -309,6 +328,7 @@ struct BatchHeader {
     uint32_t flags;    // 1 datum seen, 2 staged copy timed out, 8 a record needs the general path
     unsigned long long craterPairs, boulderPairs;  // (cell, feature) pairs evaluated
     uint32_t craterEntries, boulderEntries;         // entries the bins needed
+    uint32_t dsJobs, dsBlocks;                      // the diamond-square pass's jobs and blocks
 };
 
 struct BatchView {
@@ -341,6 +361,8 @@ struct BatchView {
     const PointRegion* pointRegions;
     const uint32_t* pointLists;    // the regions' cell lists
     const float* culls;            // indexed points: each record's cull distance
+    const DsTile* dsJobs;          // diamond-square source: one job per item
+    const uint32_t* dsFirst;       // [jobs + 1]: each job's first block of the pass
 };
 
 // A kernel shape of the persistent evaluation: bins of binW x binH cells (point sets: blocks of
@@ -360,6 +382,16 @@ int batch_blocks_per_sm(int index, bool fast);
 cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
                              const BatchVariant& variant, uint32_t maxRecordPairs,
                              uint32_t maxBoulderPairs, uint32_t* scanScratch, cudaStream_t stream);
+// The diamond-square source of a batch (header->dsJobs jobs over header->dsBlocks blocks, the
+// jobs in v.dsJobs): persistent CTAs take the blocks in turn, each job's level-0 nodes from the
+// batch's fBm at its post lattice, and write every item's base heights into the output before the
+// evaluation adds the layers (noise.baseInOutput). A block whose node boxes outgrow the shared
+// buffers sets header flag 16 and writes nothing.
+// batch_ds_setup lets the pass take its shared memory and gives the CTAs of a launch (call it
+// before any capture).
+cudaError_t batch_ds_setup(uint32_t& ctas);
+cudaError_t launch_batch_ds(const BatchNoise& noise, const BatchView& v, bool spline,
+                            uint32_t ctas, cudaStream_t stream);
 // The persistent evaluation over every bin of the batch, `ctas` CTAs.
 cudaError_t launch_batch_evaluate(const CraterShapeKernel& k, const BatchNoise& noise,
                                   const BatchView& v, int variant, bool fast, uint32_t ctas,

@@ -107,6 +107,7 @@ private:
 
 struct Pending {
     tg_request req;
+    bool pinned = false;  // host heights in page-locked memory: copied into directly
     std::vector<double> xy;
     int lod = 0;
     uint64_t cells = 0;
@@ -567,11 +568,12 @@ bool ready(tg_server* s, const Pending& p) {
 int deliver(ServeSlot& slot, bool wait) {
     for (size_t i = 0; i < slot.reqs.size(); ++i) {
         const tg_request& r = slot.reqs[i].req;
+        const bool direct = r.memory == TG_MEMORY_DEVICE || slot.reqs[i].pinned;
         const float* src = static_cast<const float*>(slot.out.ptr) + slot.offsets[i];
-        float* dst = r.memory == TG_MEMORY_DEVICE ? r.heights : slot.host + slot.offsets[i];
+        float* dst = direct ? r.heights : slot.host + slot.offsets[i];
         const cudaMemcpyKind kind =
             r.memory == TG_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-        if (r.kind == 0 && r.memory == TG_MEMORY_DEVICE) {
+        if (r.kind == 0 && direct) {
             TG_CUDA(cudaMemcpy2DAsync(dst, r.grid.width * sizeof(float), src,
                                       slot.pitches[i] * sizeof(float),
                                       r.grid.width * sizeof(float), r.grid.height, kind,
@@ -657,6 +659,7 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
             it.pointBegin = uint32_t(spec.points.size() / 2);
             it.tableBase = uint32_t(spec.pointTable.size());
             it.boulderWidth = 0.0;
+            it.dsSpacing = s->opt.point_spacing;
             it.heightOffset = outFloats;
             outFloats += p.req.n_points;
             spec.points.insert(spec.points.end(), p.xy.begin(), p.xy.end());
@@ -697,6 +700,16 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
         return TG_OK;
     }
     spec.fast = s->fast;
+    if (s->opt.post_spacing > 0.0) {
+        const tg_ds_options& r = s->opt.refine;
+        spec.ds.on = true;
+        spec.ds.postSpacing = s->opt.post_spacing;
+        spec.ds.fractalDimension = r.fractal_dimension;
+        spec.ds.scale = r.scale;
+        spec.ds.minPixelSize = r.min_pixel_size;
+        spec.ds.seed = r.seed;
+        spec.ds.spline = r.interp == 1u;
+    }
     if (int st = batch::load(slot.batch, std::move(spec))) {
         return st;
     }
@@ -722,9 +735,9 @@ int launch_slot(tg_server* s, ServeSlot& slot) {
     }
     slot.outFloats = outFloats;
     TG_CUDA(slot.out.reserve(outFloats * sizeof(float)), "allocation");
-    bool toHost = false;
+    bool toHost = false;  // a pageable host request needs the pinned mirror
     for (const Pending& p : slot.reqs) {
-        toHost |= p.req.memory == TG_MEMORY_HOST;
+        toHost |= p.req.memory == TG_MEMORY_HOST && !p.pinned;
     }
     if (toHost && slot.hostFloats < outFloats) {
         if (slot.host != nullptr) {
@@ -769,8 +782,8 @@ int complete_slot(tg_server* s, ServeSlot& slot, uint64_t* ids, size_t capacity,
     for (size_t i = 0; i < slot.reqs.size(); ++i) {
         const Pending& p = slot.reqs[i];
         const float* src = slot.host + slot.offsets[i];
-        if (p.req.memory == TG_MEMORY_DEVICE) {
-            // Already copied on the device.
+        if (p.req.memory == TG_MEMORY_DEVICE || p.pinned) {
+            // Already copied by the slot's stream.
         } else if (p.req.kind == 0) {
             for (uint32_t r = 0; r < p.req.grid.height; ++r) {
                 std::memcpy(p.req.heights + size_t(r) * p.req.grid.width,
@@ -825,6 +838,14 @@ int tg_server_create(tg_device* device, const tg_server_options* options, tg_ser
     };
     if (level_of(s, o.point_spacing) < 0) {
         return undo(fail(TG_ERROR_ARGUMENT, "point_spacing must be base_spacing * 2^k"));
+    }
+    if (o.post_spacing != 0.0 &&
+        (!(o.post_spacing > 0.0) || !std::isfinite(o.post_spacing) ||
+         !(o.refine.fractal_dimension >= 2.0 && o.refine.fractal_dimension <= 3.0) ||
+         !(o.refine.scale >= 0.0) || !std::isfinite(o.refine.scale) ||
+         !(o.refine.min_pixel_size >= 0.0) || o.refine.interp > 1u)) {
+        return undo(fail(TG_ERROR_ARGUMENT, "refinement: post spacing > 0, fractal dimension in "
+                                            "[2, 3], scale and min pixel size >= 0, interp 0 or 1"));
     }
     if (int st = batch::make_noise(o.fractals, o.n_fractals, o.elevation, s->noise,
                                    s->octaves)) {
@@ -955,6 +976,14 @@ int tg_server_submit(tg_server* s, const tg_request* request) {
     if (r.memory == TG_MEMORY_DEVICE && reinterpret_cast<uintptr_t>(r.heights) % 4u != 0u) {
         return fail(TG_ERROR_ARGUMENT, "request %llu: heights not 4-byte aligned",
                     (unsigned long long)r.id);
+    }
+    if (r.memory == TG_MEMORY_HOST) {
+        // Page-locked host heights take the device-to-host copy directly; pageable ones go
+        // through the slot's pinned mirror and a host copy at completion.
+        cudaPointerAttributes a{};
+        p.pinned = cudaPointerGetAttributes(&a, r.heights) == cudaSuccess &&
+                   a.type == cudaMemoryTypeHost;
+        (void)cudaGetLastError();
     }
     if (r.kind == 0) {
         Grid g;

@@ -29,13 +29,18 @@ MOON_GM = 4.9048695e12
 
 def dem_stack_options(seed: int = 3, budget_gb: float = 40.0, slots: int = 3,
                       max_batch_cells: int = 24 << 20, variant: int = -1,
-                      base_spacing: float = 0.25, point_spacing: float = 0.5) -> N.ServerOptions:
-    """The DEM-refinement stack's layers as a server serves them: its 12-octave fBm relief
-    (wavelength 20 km, amplitude 2000 m) as the source, and its crater layer: 2,000,000 craters
-    expected over 20481^2 cells of 0.5 m, N(>D) ~ D^-2 on [1, 100] m, uniform ages over 1 Gyr."""
+                      base_spacing: float = 0.25, point_spacing: float = 0.5,
+                      refine: bool = True, refine_seed: int = 7,
+                      crater_density: float = 1.0) -> N.ServerOptions:
+    """The DEM-refinement stack's layers as a server serves them. The source is its 12-octave fBm
+    relief (wavelength 20 km, amplitude 2000 m) sampled at 5 m posts, refined by diamond-square
+    (fractal dimension 2.2, i.e. Hurst 0.8; scale 1.5 m; bilinear) to each request's spacing;
+    `refine=False` evaluates the fBm at every cell instead. The crater layer: 2,000,000 craters
+    expected over 20481^2 cells of 0.5 m (times `crater_density`), N(>D) ~ D^-2 on [1, 100] m,
+    uniform ages over 1 Gyr."""
     fr = np.array([fractal(seed=seed, wavelength=20000.0, amplitude=2000.0, octaves=12)])
     area = (20481 * 0.5) ** 2
-    c = 2e6 / (area * (1.0 ** -2.0 - 100.0 ** -2.0))
+    c = crater_density * 2e6 / (area * (1.0 ** -2.0 - 100.0 ** -2.0))
     pop = N.Population(seed=seed, sfd_coefficient=c, sfd_exponent=2.0, min_diameter=1.0,
                        max_diameter=100.0, lifetime_gyr=1.0, depth_ratio=0.2, rim_ratio=0.04,
                        cutoff_depth_ratio=0.04, cell_size_factor=16.0, margin_radii=0.0,
@@ -44,9 +49,25 @@ def dem_stack_options(seed: int = 3, budget_gb: float = 40.0, slots: int = 3,
                            shaping=N.Shaping(profile=0, irregular=1), base_spacing=base_spacing,
                            point_spacing=point_spacing, hbm_budget=int(budget_gb * (1 << 30)),
                            max_batch_cells=max_batch_cells, slots=slots, region_cells=1024,
-                           variant=variant)
+                           variant=variant, post_spacing=POST_SPACING if refine else 0.0,
+                           refine=refine_options(refine_seed))
     opts._fractals = fr  # keep the array alive with the options
     return opts
+
+
+# The DEM-refinement stack's input DEM: posts every 5 m.
+POST_SPACING = 5.0
+
+
+def refine_options(seed: int = 7) -> N.DsOptions:
+    """The DEM refinement's diamond-square options: fractal dimension 2.2 (Hurst 0.8), scale
+    1.5 m, bilinear reads."""
+    return N.DsOptions(fractal_dimension=2.2, scale=1.5, interp=0, seed=seed, min_pixel_size=0.0)
+
+
+def post_lattice() -> GridSpec:
+    """The served DEM's post lattice as a grid: post (i, j) centered at (i, -j) * 5 m."""
+    return GridSpec(1, 1, -0.5 * POST_SPACING, 0.5 * POST_SPACING, POST_SPACING)
 
 
 class Server:
@@ -196,14 +217,20 @@ class StreamResult:
 
 
 def run_stream(server: Server, reqs: list[Req], realtime: bool = True,
-               keep: bool = False, device: bool = False) -> StreamResult:
+               keep: bool = False, device: bool = False, pinned: bool = False) -> StreamResult:
     """Submits each request at its arrival time (all at once when not `realtime`), polling in
-    between; latency is completion minus arrival. Results go to host arrays, or with `device` to
-    CUDA tensors allocated before the stream starts."""
+    between; latency is completion minus arrival. Results go to host arrays (page-locked with
+    `pinned`, which the server copies into directly), or with `device` to CUDA tensors, all
+    allocated before the stream starts."""
     if device:
         import torch
 
         outs = {r.rid: torch.empty(r.cells, dtype=torch.float32, device="cuda") for r in reqs}
+    elif pinned:
+        import torch
+
+        outs = {r.rid: torch.empty(r.cells, dtype=torch.float32, pin_memory=True).numpy()
+                for r in reqs}
     else:
         outs = {r.rid: np.empty(r.cells, np.float32) for r in reqs}
     arrival = {r.rid: r.arrival for r in reqs}

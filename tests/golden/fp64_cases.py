@@ -17,7 +17,14 @@ Cases:
             mapping, boulders), a 257^2 window at its center;
   tile_k    three tiles of the batched form's 4096 uneven tiles (1/10 density), the farthest from
             the origin among those at most 160 cells wide (up to 1.7e6 m out);
-  served    a 257^2 tile of the served form's DEM stack (12-octave fBm, craters) 1e6 m out.
+  served    a 257^2 tile of the served form's fBm-at-every-cell stack (12-octave fBm, craters)
+            1e6 m out;
+  served_refined
+            a 257^2 tile of the served form's DEM-refinement stack near the origin: the FP64 fBm
+            at the 5 m posts (rounded to float, as a DEM's posts), refined by the reference's own
+            diamond-square (FP64 nodes; it keys draws by the node's place in its input raster, so
+            the raster starts at post (0, 0) as the served lattice does), then the craters in
+            double.
 """
 
 from __future__ import annotations
@@ -97,10 +104,34 @@ def main() -> None:
     # A served tile of the DEM stack.
     from terraingen_b200.serve import dem_stack_options
 
-    opts = dem_stack_options(slots=1)
+    opts = dem_stack_options(slots=1, refine=False)
     g = GridSpec(257, 257, 1.0e6 + 1000.0, 2000.0 + 257 * 0.5, 0.5)
     arrays["served_grid"] = grid_row(g)
     arrays["served_fp64"] = fp64_heights(g, opts._fractals, W.crater_batch(opts.craters, g))
+    # The served DEM-refinement stack.
+    from terraingen_b200.serve import POST_SPACING, post_lattice, refine_options
+
+    opts = dem_stack_options(slots=1)
+    g = GridSpec(257, 257, 100.0, -100.0, 0.5)
+    n = 64  # posts 0..63 along both axes: 0 to 315 m east and south, the tile well inside
+    f = opts._fractals[0]
+    posts = np.zeros((n, n), np.float64)
+    H.restate().rs_fbm_grid_f64(n, n, -0.5 * POST_SPACING, 0.5 * POST_SPACING, POST_SPACING,
+                                int(f["seed"]), float(f["wavelength"]), float(f["amplitude"]),
+                                int(f["octaves"]), float(f["lacunarity"]), float(f["gain"]), 0.0,
+                                posts.ctypes.data)
+    lattice = post_lattice()
+    r = refine_options()
+    refined, _ = H.diamond_square(H.reference(), posts.astype(np.float32),
+                                  GridSpec(n, n, lattice.x0, lattice.y0, POST_SPACING), g,
+                                  r.fractal_dimension, r.scale, seed=r.seed)
+    out = refined.astype(np.float64)
+    kernel, records, data, foot = W.crater_batch(opts.craters, g)
+    fp64_library().f64_craters(kernel.ctypes.data, records.ctypes.data, len(records),
+                               data.ctypes.data, len(data), foot.ctypes.data, g.width, g.height,
+                               g.x0, g.y0, g.pixel, out.ctypes.data)
+    arrays["served_refined_grid"] = grid_row(g)
+    arrays["served_refined_fp64"] = out
     np.savez_compressed(OUT, **arrays)
     for k, v in arrays.items():
         if k.endswith("_fp64"):

@@ -86,12 +86,15 @@ def test_batched_far_tiles_within_1mm_of_fp64(device, fx):
         _check(got, fx[f"tile{k}_fp64"])
 
 
-def test_served_tile_within_1mm_of_fp64(device, fx):
+@pytest.mark.parametrize("case,refine", [("served", False), ("served_refined", True)])
+def test_served_tile_within_1mm_of_fp64(device, fx, case, refine):
+    # The fBm-at-every-cell stack 1e6 m out, and the DEM-refinement stack (diamond-square over
+    # the fBm's posts, the reference's own refinement over FP64 posts as the oracle).
     from terraingen_b200.serve import Server, dem_stack_options
 
-    grid = grid_of(fx["served_grid"])
+    grid = grid_of(fx[f"{case}_grid"])
     out = np.empty(grid.cells, np.float32)
-    with Server(device, dem_stack_options(slots=1)) as s:
+    with Server(device, dem_stack_options(slots=1, refine=refine)) as s:
         s.submit_tile(3, grid, out)
         assert s.drain() == [3]
-    _check(out, fx["served_fp64"])
+    _check(out, fx[f"{case}_fp64"])
