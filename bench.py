@@ -548,7 +548,10 @@ def next_rows_form(dev):
     return {
         "crater_population": {"craters": int(len(drawn["x"])), "device_ms": round(device_s * 1e3, 2),
                               "host_ms": round(host_s * 1e3, 1),
-                              "ids_match_host": bool(np.array_equal(drawn["id"], host["id"]))},
+                              "ids_match_host": bool(np.array_equal(drawn["id"], host["id"])),
+                              "identical_to_host": bool(all(
+                                  np.array_equal(drawn[k], host[k])
+                                  for k in ("x", "y", "diameter", "age", "id")))},
         "body_source": {"cells": 4097 * 4097, "ms": round(body_ms, 3),
                         "mcells_per_s": round(4097 * 4097 / body_ms / 1e3, 1),
                         "stack": "one 8-octave Perlin fBm on a sphere of 1737.4 km"},

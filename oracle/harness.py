@@ -333,6 +333,9 @@ def _harness(name: str) -> C.CDLL:
     lib.tgref_craters.argtypes = [C.POINTER(Scene), C.c_void_p, _D, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
     lib.tgref_craters.restype = C.c_long
+    if hasattr(lib, "tgref_points"):
+        lib.tgref_points.argtypes = [C.POINTER(Scene), C.c_void_p, _U32, _D, C.c_void_p]
+        lib.tgref_points.restype = C.c_int
     lib.tgref_boulders.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_long]
     lib.tgref_boulders.restype = C.c_long
     if hasattr(lib, "tgref_datum_relief"):
@@ -409,6 +412,16 @@ def evaluate(lib: C.CDLL, scene: Scene, backend: int = 0, threads: int = 0):
     if lib.tgref_evaluate(C.byref(scene), backend, threads, out.ctypes.data, C.byref(ms)) != 0:
         raise RuntimeError(lib.tgref_error().decode())
     return out, ms.value
+
+
+def points(lib: C.CDLL, scene: Scene, xy: np.ndarray, spacing: float) -> np.ndarray:
+    """The scene's heights (float32) at the (x, y) rows of `xy` through the reference's point path
+    (Terrain::HeightsAt -> EvaluatePoints) at sample `spacing`."""
+    xy = np.ascontiguousarray(xy, np.float64).reshape(-1, 2)
+    out = np.zeros(len(xy), np.float32)
+    if lib.tgref_points(C.byref(scene), xy.ctypes.data, len(xy), spacing, out.ctypes.data) != 0:
+        raise RuntimeError(lib.tgref_error().decode())
+    return out
 
 
 def craters(lib: C.CDLL, scene: Scene, region, spacing: float = 0.0) -> dict:

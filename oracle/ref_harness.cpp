@@ -264,6 +264,26 @@ int tgref_evaluate(const tgref_scene* s, int backend, unsigned threads, float* o
     }
 }
 
+/// The scene's heights at `n` points (x, y pairs) through the reference's point path:
+/// Terrain::HeightsAt (Source::HeightsAt, src/pipeline/terrain.cpp:133-154: EvaluatePoints, the
+/// points in Morton-ordered batches of nearby points, each batch's layers prepared over its own
+/// area) at sample `spacing`. Returns 0, or -1 with tgref_error() set.
+int tgref_points(const tgref_scene* s, const double* xy, uint32_t n, double spacing, float* out) {
+    try {
+        SetLogLevel(LogLevel::Warning);
+        const Terrain terrain = MakeTerrain(*s);
+        std::vector<Vec2d> points(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            points[i] = Vec2d{xy[2 * size_t(i)], xy[2 * size_t(i) + 1]};
+        }
+        terrain.HeightsAt(Span<const Vec2d>(points), Span<float>(out, n), spacing);
+        return 0;
+    } catch (const std::exception& error) {
+        g_error = error.what();
+        return -1;
+    }
+}
+
 /// The number of craters the scene's crater layer generates over `region`
 /// (x0, y0, x1, y1 in meters), and their centers, diameters and ids into the arrays when given
 /// (capacity `n`).

@@ -84,7 +84,70 @@ struct DevicePlan {
     double c, lifetime, marginRadii;
     double region[4];
     double tolerance;  // relative width of a threshold within which a cell is flagged
+    int32_t rootP, rootQ;  // the inversion's power as -rootQ / rootP (rootP a power of two), or 0
 };
+
+// Double-double numbers (a value hi + lo, |lo| <= ulp(hi) / 2): Dekker's exact product by FMA
+// and a renormalising sum, about 2^-104 relative per product.
+struct Dd {
+    double hi, lo;
+};
+
+__device__ __forceinline__ Dd dd_mul(Dd a, Dd b) {
+    const double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e += a.hi * b.lo + a.lo * b.hi;
+    const double s = p + e;
+    return Dd{s, e - (s - p)};
+}
+
+__device__ __forceinline__ Dd dd_pow(Dd a, int n) {
+    Dd r{1.0, 0.0};
+    for (int k = 0; k < n; ++k) {
+        r = dd_mul(r, a);
+    }
+    return r;
+}
+
+// The diameter of an inverse-CDF draw, x^(-q/p) for x = target / c (PowerLawSfd's inversion,
+// std::pow(target / c, -1 / e) where the double -1 / e is exactly -q / p), correctly rounded: the
+// device's pow gives a start within a few ulps, and each step compares the midpoints around the
+// candidate with the root through m^p x^q = 1, in double-double (exact far beyond the decision
+// below). The host's
+// libm pow is within 0.54 ulp, so it returns the correctly rounded root whenever the root lies
+// more than 0.04 ulp from a midpoint: a root within 0.1 ulp of one flags the cell (`ambiguous`)
+// and the host draws it. With no p / q (rootP 0) the device's pow stands and the diameter may
+// differ from the host's in its last bits.
+__device__ double sfd_root(double x, double inverseExponent, int p, int q, bool& ambiguous) {
+    double y = pow(x, inverseExponent);
+    if (p == 0) {
+        return y;
+    }
+    const Dd xq = dd_pow(Dd{x, 0.0}, q);
+    // m^p x^q - 1 for the double-double m.
+    auto excess = [&](Dd m) {
+        const Dd v = dd_mul(dd_pow(m, p), xq);
+        return (v.hi - 1.0) + v.lo;
+    };
+    for (int step = 0; step < 8; ++step) {
+        const double up = nextafter(y, INFINITY), down = nextafter(y, -INFINITY);
+        const double halfUp = 0.5 * (up - y), halfDown = 0.5 * (down - y);
+        const double above = excess(Dd{y, halfUp}), below = excess(Dd{y, halfDown});
+        if (above > 0.0 && below < 0.0) {
+            // The root is between the midpoints; its distance from each in ulps is about
+            // |excess| y / p over the half-gap doubled.
+            const double toUp = fabs(above) * y / (double(p) * 2.0 * halfUp);
+            const double toDown = fabs(below) * y / (double(p) * -2.0 * halfDown);
+            if (toUp < 0.1 || toDown < 0.1) {
+                ambiguous = true;
+            }
+            return y;
+        }
+        y = above <= 0.0 ? up : down;
+    }
+    ambiguous = true;  // not bracketed in eight steps (never for pow's few-ulp start)
+    return y;
+}
 
 __device__ __forceinline__ bool inside(const double* box, double x, double y) {
     return x >= box[0] && x < box[2] && y >= box[1] && y < box[3];
@@ -144,7 +207,7 @@ __device__ uint32_t cell_pass(const DevicePlan& d, const CraterBandPlan& p, int3
     uint32_t kept = 0;
     for (uint64_t index = 0; index < count; ++index) {
         const double target = p.top - geometry.next_double() * p.count;
-        double dia = pow(target / d.c, p.inverseExponent);
+        double dia = sfd_root(target / d.c, p.inverseExponent, d.rootP, d.rootQ, ambiguous);
         dia = dia < p.low ? p.low : (p.high < dia ? p.high : dia);
         const double u = geometry.next_double();
         const double v = geometry.next_double();
@@ -331,6 +394,18 @@ int tg_crater_generate_device(tg_device* d, const tg_crater_population* spec,
     dp.marginRadii = spec->margin_radii;
     std::memcpy(dp.region, region, 4 * sizeof(double));
     dp.tolerance = tolerance;
+    // The inversion's power -1 / e as the double the host's pow takes: when that is -q / p with
+    // p a power of two up to 16 and q up to 16 (e = 2, the craters' slope, gives -1 / 2), the
+    // root is found correctly rounded.
+    const double power = plan.empty() ? 0.0 : plan.front().inverseExponent;
+    for (int p = 1; p <= 16; p *= 2) {
+        const double q = -power * p;  // exact: a product by a power of two
+        if (q >= 1.0 && q <= 16.0 && q == std::floor(q)) {
+            dp.rootP = p;
+            dp.rootQ = int32_t(q);
+            break;
+        }
+    }
     const uint32_t blocks = uint32_t((cells + 127) / 128);
     crater_count_cells_kernel<<<blocks, 128, 0, s>>>(dp, static_cast<uint32_t*>(counts.ptr),
                                                      static_cast<uint8_t*>(flags.ptr));
