@@ -87,6 +87,12 @@ struct DevicePlan {
     int32_t rootP, rootQ;  // the inversion's power as -rootQ / rootP (rootP a power of two), or 0
 };
 
+// A written diameter whose root lies near a rounding midpoint: its place and pow's argument.
+struct RootFix {
+    uint64_t at;
+    double ratio;
+};
+
 // Double-double numbers (a value hi + lo, |lo| <= ulp(hi) / 2): Dekker's exact product by FMA
 // and a renormalising sum, about 2^-104 relative per product.
 struct Dd {
@@ -113,11 +119,11 @@ __device__ __forceinline__ Dd dd_pow(Dd a, int n) {
 // std::pow(target / c, -1 / e) where the double -1 / e is exactly -q / p), correctly rounded: the
 // device's pow gives a start within a few ulps, and each step compares the midpoints around the
 // candidate with the root through m^p x^q = 1, in double-double (exact far beyond the decision
-// below). The host's
-// libm pow is within 0.54 ulp, so it returns the correctly rounded root whenever the root lies
-// more than 0.04 ulp from a midpoint: a root within 0.1 ulp of one flags the cell (`ambiguous`)
-// and the host draws it. With no p / q (rootP 0) the device's pow stands and the diameter may
-// differ from the host's in its last bits.
+// below). The host's libm pow (glibc's: its exp step within 0.509 ulp, the log's error a few 1e-4
+// ulp here) returns the correctly rounded root whenever the root lies more than about 0.01 ulp
+// from a midpoint; a root within 0.05 ulp of one sets `ambiguous`, and the host's pow gives that
+// diameter. With no -q / p (rootP 0) the device's pow stands and the diameter may differ from the
+// host's in its last bits.
 __device__ double sfd_root(double x, double inverseExponent, int p, int q, bool& ambiguous) {
     double y = pow(x, inverseExponent);
     if (p == 0) {
@@ -138,7 +144,7 @@ __device__ double sfd_root(double x, double inverseExponent, int p, int q, bool&
             // |excess| y / p over the half-gap doubled.
             const double toUp = fabs(above) * y / (double(p) * 2.0 * halfUp);
             const double toDown = fabs(below) * y / (double(p) * -2.0 * halfDown);
-            if (toUp < 0.1 || toDown < 0.1) {
+            if (toUp < 0.05 || toDown < 0.05) {
                 ambiguous = true;
             }
             return y;
@@ -200,14 +206,20 @@ __device__ uint64_t poisson(Stream& random, const CraterBandPlan& p, double tole
 // written from `at`. Returns the kept count.
 __device__ uint32_t cell_pass(const DevicePlan& d, const CraterBandPlan& p, int32_t i, int32_t j,
                               bool& ambiguous, double* x, double* y, double* diameter,
-                              double* age, uint64_t* id, uint64_t at, uint64_t capacity) {
+                              double* age, uint64_t* id, uint64_t at, uint64_t capacity,
+                              RootFix* fixes = nullptr, uint32_t* fixCount = nullptr) {
     Stream geometry(d.seed, kCraterStream, uint32_t(i), uint32_t(j), p.exponent);
     Stream ages(d.seed, kCraterAgeStream, uint32_t(i), uint32_t(j), p.exponent);
     const uint64_t count = poisson(geometry, p, d.tolerance, ambiguous);
     uint32_t kept = 0;
     for (uint64_t index = 0; index < count; ++index) {
         const double target = p.top - geometry.next_double() * p.count;
-        double dia = sfd_root(target / d.c, p.inverseExponent, d.rootP, d.rootQ, ambiguous);
+        // A root near a rounding midpoint leaves the cell's membership alone (the keep margin's
+        // own slack covers a last-bit change); its diameter is the host's pow, patched in after
+        // the write pass.
+        bool nearMidpoint = false;
+        const double ratio = target / d.c;
+        double dia = sfd_root(ratio, p.inverseExponent, d.rootP, d.rootQ, nearMidpoint);
         dia = dia < p.low ? p.low : (p.high < dia ? p.high : dia);
         const double u = geometry.next_double();
         const double v = geometry.next_double();
@@ -244,6 +256,12 @@ __device__ uint32_t cell_pass(const DevicePlan& d, const CraterBandPlan& p, int3
             x[n] = cx;
             y[n] = cy;
             diameter[n] = dia;
+            if (nearMidpoint && fixes != nullptr) {
+                const uint32_t k = atomicAdd(fixCount, 1u);
+                if (k < capacity) {
+                    fixes[k] = RootFix{n, ratio};
+                }
+            }
             age[n] = a;
             id[n] = (uint64_t(w.x) << 32) | w.y;
         }
@@ -283,7 +301,7 @@ __global__ void crater_count_cells_kernel(const DevicePlan d, uint32_t* __restri
 __global__ void crater_write_cells_kernel(const DevicePlan d, const uint64_t* __restrict__ offsets,
                                           const uint8_t* __restrict__ flags, double* x, double* y,
                                           double* diameter, double* age, uint64_t* id,
-                                          uint64_t capacity) {
+                                          uint64_t capacity, RootFix* fixes, uint32_t* fixCount) {
     const uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (g >= d.cells || flags[g] != 0u) {
         return;
@@ -291,7 +309,18 @@ __global__ void crater_write_cells_kernel(const DevicePlan d, const uint64_t* __
     int32_t i, j;
     const CraterBandPlan& p = band_of(d, g, i, j);
     bool ambiguous = false;
-    cell_pass(d, p, i, j, ambiguous, x, y, diameter, age, id, offsets[g], capacity);
+    cell_pass(d, p, i, j, ambiguous, x, y, diameter, age, id, offsets[g], capacity, fixes,
+              fixCount);
+}
+
+// The host's pow of the diameters whose roots lie near a rounding midpoint, to their places.
+__global__ void patch_roots_kernel(const uint64_t* __restrict__ places,
+                                   const double* __restrict__ values, uint32_t n,
+                                   double* diameter) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        diameter[places[k]] = values[k];
+    }
 }
 
 // The craters of host-drawn cells to their places in the outputs.
@@ -455,10 +484,47 @@ int tg_crater_generate_device(tg_device* d, const tg_crater_population* spec,
     }
     TG_CUDA(cudaMemcpyAsync(offsets.ptr, off.data(), cells * 8, cudaMemcpyHostToDevice, s),
             "copy");
+    // Room for every written crater's root fix (at most one each) and their count.
+    Scratch fixes;
+    TG_CUDA(fixes.allocate(writable * sizeof(RootFix) + 16), "allocation");
+    uint32_t* fixCount = reinterpret_cast<uint32_t*>(static_cast<char*>(fixes.ptr) +
+                                                     writable * sizeof(RootFix));
+    TG_CUDA(cudaMemsetAsync(fixCount, 0, sizeof(uint32_t), s), "memset");
     crater_write_cells_kernel<<<blocks, 128, 0, s>>>(
         dp, static_cast<const uint64_t*>(offsets.ptr), static_cast<const uint8_t*>(flags.ptr),
-        dx, dy, dd, da, di, writable);
+        dx, dy, dd, da, di, writable, static_cast<RootFix*>(fixes.ptr), fixCount);
     TG_CUDA(cudaGetLastError(), "write launch");
+    // The roots near a midpoint: the host's pow (the reference's libm) for each, patched in.
+    uint32_t nFix = 0;
+    TG_CUDA(cudaMemcpyAsync(&nFix, fixCount, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "copy");
+    TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+    Scratch patch;
+    if (nFix > 0) {
+        std::vector<RootFix> hostFixes(nFix);
+        TG_CUDA(cudaMemcpyAsync(hostFixes.data(), fixes.ptr, nFix * sizeof(RootFix),
+                                cudaMemcpyDeviceToHost, s),
+                "copy");
+        TG_CUDA(cudaStreamSynchronize(s), "synchronize");
+        const double power = plan.front().inverseExponent;
+        std::vector<uint64_t> places(nFix);
+        std::vector<double> values(nFix);
+        for (uint32_t k = 0; k < nFix; ++k) {
+            places[k] = hostFixes[k].at;
+            values[k] = std::pow(hostFixes[k].ratio, power);
+        }
+        TG_CUDA(patch.allocate(size_t(nFix) * 16), "allocation");
+        uint64_t* dPlaces = static_cast<uint64_t*>(patch.ptr);
+        double* dValues = reinterpret_cast<double*>(dPlaces + nFix);
+        TG_CUDA(cudaMemcpyAsync(dPlaces, places.data(), size_t(nFix) * 8, cudaMemcpyHostToDevice,
+                                s),
+                "copy");
+        TG_CUDA(cudaMemcpyAsync(dValues, values.data(), size_t(nFix) * 8, cudaMemcpyHostToDevice,
+                                s),
+                "copy");
+        patch_roots_kernel<<<(nFix + 255) / 256, 256, 0, s>>>(dPlaces, dValues, nFix, dd);
+        TG_CUDA(cudaGetLastError(), "patch launch");
+        TG_CUDA(cudaStreamSynchronize(s), "synchronize");  // before the host vectors go
+    }
     // The host-drawn cells' craters, gathered into one upload and scattered to their places.
     std::vector<HostCrater> flat;
     std::vector<uint64_t> places;
