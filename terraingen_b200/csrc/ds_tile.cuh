@@ -36,28 +36,39 @@ __device__ __forceinline__ Words philox(Words c, uint32_t k0, uint32_t k1) {
 // its product with any |k| <= 64 is exact in float.
 constexpr float kLn2High = 0.693145751953125f;
 constexpr float kLn2Low = float(0.69314718055994530942 - 0.693145751953125);
+// pi 2^-52: a 53-bit integer times this is pi times the integer's share of 2^52.
+constexpr float kPiOver2p52 = float(3.14159265358979323846 / 4503599627370496.0);
 
-// log(n 2^-53) in float for an integer 1 <= n <= 2^53, with the relative accuracy of log1pf near
-// n = 2^53 (where the logarithm goes to 0). n 2^-53 = 2^k (1 + f) with 1 + f in [0.75, 1.5): f is
-// an integer difference, exact before its one rounding to float, and the logarithm is
-// k ln 2 + log1pf(f), one path for every lane.
+// log(n 2^-53) in float for an integer 1 <= n <= 2^53, with relative accuracy near n = 2^53
+// (where the logarithm goes to 0), one path for every lane. n 2^-53 = 2^k (1 + f) with 1 + f in
+// [0.75, 1.5) (f an integer difference, exact before its one rounding to float), and
+// log(1 + f) = 2 atanh(s) = 2 (s + s^3/3 + s^5/5 + s^7/7 + s^9/9 + ...) for s = f / (2 + f),
+// |s| <= 1/5, the series cut after s^9 (its tail is below 1e-8 of the sum): within 3e-7 of the
+// logarithm relative.
 __device__ __forceinline__ float log_of_ratio(uint64_t n) {
     const int bits = 64 - __clzll(n);  // n in [2^(bits - 1), 2^bits)
     const bool upper = n >= (3ull << (bits - 2 < 0 ? 0 : bits - 2)) && bits >= 2;
     const int e = upper ? bits : bits - 1;  // 1 + f = n / 2^e
     const float f = float(int64_t(n) - int64_t(1ull << e)) * __int_as_float((127 - e) << 23);
+    const float s = __fdividef(f, 2.0f + f);
+    const float s2 = s * s;
+    float series = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
+    series = fmaf(s2, series, 1.0f / 5.0f);
+    series = fmaf(s2, series, 1.0f / 3.0f);
+    const float log1p = fmaf(2.0f * s * s2, series, 2.0f * s);
     const float k = float(e - 53);
-    return fmaf(k, kLn2High, fmaf(k, kLn2Low, log1pf(f)));
+    return fmaf(k, kLn2High, fmaf(k, kLn2Low, log1p));
 }
 
 // The standard normal of node (col, row) of `level` (Refinement::Displacement,
 // diamond_square.cpp:382-389): one Philox block is RandomStream's first two NextDouble draws
 // (u1, u2, 53 bits each, exact), turned into a normal by Box-Muller (StandardNormal,
 // src/random/samplers.cpp:65-69), sqrt(-2 log(1 - u1)) cos(2 pi u2). The reference evaluates it
-// in double; here the logarithm, the square root and the cosine run in float on arguments formed
-// exactly in integers or double, within 2e-6 of the double normal (a few 1e-7 of the radius;
-// under 1e-5 m in the refined heights) for a fraction of the instructions: the steps are bound by
-// issuing them.
+// in double; here in float on arguments formed exactly from the draws' integers: the logarithm
+// as above, the square root as x rsqrt(x), and the cosine of pi a with a = 2 u2 moved into
+// [-1, 1) by an exact integer subtraction (the hardware cosine is within 4e-7 there). Within 1e-5
+// of the double normal (a few 1e-7 of the radius; under 2e-5 m in the refined heights), for the
+// fewest instructions: the refinement is bound by issuing them.
 __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int level,
                                               uint32_t seed) {
     const uint32_t high = uint32_t((col >> 32) ^ (row >> 32));
@@ -66,15 +77,12 @@ __device__ __forceinline__ double node_normal(int64_t col, int64_t row, int leve
     // u1 = m1 2^-53 and u2 = m2 2^-53; 1 - u1 = (2^53 - m1) 2^-53 exactly.
     const uint64_t m1 = (uint64_t(b.x >> 5u) << 26u) | uint64_t(b.y >> 6u);
     const uint64_t m2 = (uint64_t(b.z >> 5u) << 26u) | uint64_t(b.w >> 6u);
-    const float radius = sqrtf(-2.0f * log_of_ratio((1ull << 53) - m1));
-    // cos(pi a) for a = 2 u2 split into float parts a = high + low: cos(pi high) - pi low
-    // sin(pi high), so the float rounding of a costs no accuracy.
-    const double a = double(m2) * 0x1p-52;
-    const float aHigh = float(a), aLow = float(a - double(aHigh));
-    float sine, cosine;
-    sincospif(aHigh, &sine, &cosine);
-    const float c = fmaf(-3.14159265f * aLow, sine, cosine);
-    return double(radius) * double(c);
+    const float twice = -2.0f * log_of_ratio((1ull << 53) - m1);
+    const float radius = twice > 0.0f ? twice * rsqrtf(twice) : 0.0f;
+    // 2 u2 = m2 2^-52 in [0, 2), as m2 - 2^53 2^-52 in [-1, 0) from 1 on.
+    const int64_t turn = int64_t(m2) - (m2 >= (1ull << 52) ? int64_t(1ull << 53) : int64_t(0));
+    const float c = __cosf(float(turn) * kPiOver2p52);
+    return double(radius * c);
 }
 
 // Catmull-Rom weights of four nodes around a midpoint (diamond_square.cpp:37).

@@ -11,8 +11,9 @@ from conftest import GOLDEN, grid_of
 
 pytestmark = pytest.mark.gpu
 
-# Heights are FP64 nodes read to float; only CUDA's double log1p / cos may differ from the host's
-# by an ulp, so the bar is far below the 1e-3 m of the configurations.
+# Heights are FP64 nodes read to float; the displacements' normals are a float Box-Muller on the
+# exact uniforms (within 1e-5 of the double normal), so the heights stay far below the 1e-3 m of
+# the configurations.
 TOLERANCE_M = 1e-3
 
 
@@ -50,20 +51,23 @@ def test_displacement_draws_match_oracle(device):
 
     rs = H.restate()
     rng = np.random.default_rng(4)
-    cols = rng.integers(-50000, 50000, 500)
-    rows = rng.integers(-50000, 50000, 500)
-    levels = rng.integers(1, 6, 500)
-    sext = np.zeros((500, 6), np.uint32)
+    cols = rng.integers(-50000, 50000, 20000)
+    rows = rng.integers(-50000, 50000, 20000)
+    levels = rng.integers(1, 6, 20000)
+    sext = np.zeros((20000, 6), np.uint32)
     sext[:, 0] = cols.astype(np.int64).astype(np.uint32)
     sext[:, 1] = rows.astype(np.int64).astype(np.uint32)
     sext[:, 2] = levels
     sext[:, 4] = 7
     sext[:, 5] = 0x524D4450
     words, normals = device.philox_probe(sext)
-    for i in range(500):
-        want = rs.rs_ds_normal(int(cols[i]), int(rows[i]), int(levels[i]), 7)
-        # Box-Muller in float on the exact uniforms: a few 1e-7 of the radius (at most 8.6).
-        assert abs(normals[i] - want) <= 2e-6, (i, normals[i], want)
+    want = np.array([rs.rs_ds_normal(int(cols[i]), int(rows[i]), int(levels[i]), 7)
+                     for i in range(len(cols))])
+    # Box-Muller in float on the exact uniforms: a few 1e-7 of the radius (at most 8.6), the
+    # hardware cosine within 4e-7.
+    err = np.abs(normals - want)
+    assert err.max() <= 1e-5, (int(err.argmax()), float(err.max()))
+    assert float(np.abs(want).max()) > 3.0
 
 
 def test_ds_deterministic_and_windowed(device, fx):
