@@ -15,12 +15,16 @@
 // This file is compiled with -ffp-contract=off and uses the host libm, as the reference does.
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #include "../../include/tgb200.h"
 #include "layouts.h"
@@ -295,6 +299,82 @@ unsigned host_threads() {
 
 // Runs body(i) for every i in [0, n) on up to `threads` host threads, the caller's included;
 // items are taken in order from a shared counter, so each runs exactly once.
+// Host worker threads kept for the life of the process: a call hands them its loop instead of
+// starting threads of its own (tens of microseconds each, several loops a batch). One call at a
+// time holds them; a call made while another holds them (the served form's region builders run
+// batches side by side), or in a process forked after they started, runs on threads of its own.
+class HostPool {
+  public:
+    static HostPool& instance() {
+        static HostPool* pool = new HostPool();  // never destroyed: its threads wait until exit
+        return *pool;
+    }
+
+    // body(i) for every i < n on `workers` threads, the caller one of them; false, with nothing
+    // run, when the pool is held or belongs to the process this one was forked from.
+    template <typename Body>
+    bool run(size_t n, size_t workers, const Body& body) {
+        std::unique_lock<std::mutex> held(m_held, std::try_to_lock);
+        if (!held.owns_lock() || getpid() != m_pid) {
+            return false;
+        }
+        std::unique_lock<std::mutex> lock(m_mutex);
+        while (m_started < workers - 1) {
+            std::thread(&HostPool::serve, this, m_started++).detach();
+        }
+        m_call = [](const void* context, size_t i) { (*static_cast<const Body*>(context))(i); };
+        m_context = &body;
+        m_n = n;
+        m_next.store(0);
+        m_want = workers - 1;
+        m_finished = 0;
+        ++m_generation;
+        lock.unlock();
+        m_wake.notify_all();
+        drain();
+        lock.lock();
+        m_done.wait(lock, [&] { return m_finished == m_want; });
+        return true;
+    }
+
+  private:
+    HostPool() : m_pid(getpid()) {}
+
+    void drain() {
+        for (size_t i = m_next.fetch_add(1); i < m_n; i = m_next.fetch_add(1)) {
+            m_call(m_context, i);
+        }
+    }
+
+    // A worker: each generation it is one of the m_want first, it drains the loop and reports.
+    void serve(size_t id) {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lock(m_mutex);
+        for (;;) {
+            m_wake.wait(lock, [&] { return m_generation != seen; });
+            seen = m_generation;
+            if (id >= m_want) {
+                continue;
+            }
+            lock.unlock();
+            drain();
+            lock.lock();
+            if (++m_finished == m_want) {
+                m_done.notify_one();
+            }
+        }
+    }
+
+    const pid_t m_pid;
+    std::mutex m_held, m_mutex;
+    std::condition_variable m_wake, m_done;
+    size_t m_started = 0, m_want = 0, m_finished = 0, m_n = 0;
+    uint64_t m_generation = 0;
+    std::atomic<size_t> m_next{0};
+    void (*m_call)(const void*, size_t) = nullptr;
+    const void* m_context = nullptr;
+};
+
 template <typename Body>
 void parallel_for(size_t n, unsigned threads, const Body& body) {
     const size_t workers = std::min<size_t>(threads, n);
@@ -302,6 +382,9 @@ void parallel_for(size_t n, unsigned threads, const Body& body) {
         for (size_t i = 0; i < n; ++i) {
             body(i);
         }
+        return;
+    }
+    if (HostPool::instance().run(n, workers, body)) {
         return;
     }
     std::atomic<size_t> next{0};
@@ -497,7 +580,8 @@ double resolution_weight(double diameter, double spacing, double start = 2.0,
 
 struct Outline {
     double ellipticity = 1.0, heading = 0.0;
-    std::vector<double> amplitudes, phases;
+    double amplitudes[11], phases[11];  // the first `harmonics` of them
+    int harmonics = 0;
     int firstHarmonic = 2;
 };
 
@@ -540,15 +624,40 @@ Outline irregular_outline(const Crater& c, uint32_t seed) {
         const double norm = roughness * law.scale;
         o.firstHarmonic = 2;
         if (roughness > 0.0) {
-            o.amplitudes.reserve(11);
-            o.phases.reserve(11);
             for (int k = 2; k <= 12; ++k) {
-                o.amplitudes.push_back(norm * law.power[k - 2]);
-                o.phases.push_back(2.0 * 3.14159265358979323846 * random.next_double());
+                o.amplitudes[o.harmonics] = norm * law.power[k - 2];
+                o.phases[o.harmonics] = 2.0 * 3.14159265358979323846 * random.next_double();
+                ++o.harmonics;
             }
         }
     }
     return o;
+}
+
+// Whether the footprint box of half-width `reach` around (x, y) holds a cell of the grid:
+// Surface::Expand, then MappedBounds of GeoTransform::WorldToPixel over the box's corners
+// (src/raster/cell_loops.cpp:21-28, geo_transform.h:70), then ClampIndex.
+bool footprint_cells(const tg_grid& grid, double x, double y, double reach) {
+    const double det = grid.pixel_width * grid.pixel_height - grid.row_rotation * grid.col_rotation;
+    double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
+    for (const double wx : {x - reach, x + reach}) {
+        for (const double wy : {y - reach, y + reach}) {
+            const double dx = wx - grid.origin_x;
+            const double dy = wy - grid.origin_y;
+            const double px = (dx * grid.pixel_height - dy * grid.row_rotation) / det;
+            const double py = (dy * grid.pixel_width - dx * grid.col_rotation) / det;
+            minX = std::fmin(minX, px);
+            minY = std::fmin(minY, py);
+            maxX = std::fmax(maxX, px);
+            maxY = std::fmax(maxY, py);
+        }
+    }
+    const double w = grid.width, h = grid.height;
+    const double c0 = std::clamp(std::floor(minX), 0.0, w);
+    const double c1 = std::clamp(std::ceil(maxX), 0.0, w);
+    const double r0 = std::clamp(std::floor(minY), 0.0, h);
+    const double r1 = std::clamp(std::ceil(maxY), 0.0, h);
+    return size_t(c0) < size_t(c1) && size_t(r0) < size_t(r1);
 }
 
 double max_outline_scale(bool irregular) {  // MaxOutlineScale (irregularity.cpp:279)
@@ -1246,52 +1355,82 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         std::vector<Crater> craters =
             generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads);
 
+        // The craters that can give a record: a resolution weight above 0 and a footprint, grown
+        // to the largest outline scale any crater can draw (MaxOutlineScale, irregularity.cpp:
+        // 279, the bound the reference's own binning takes), that holds a cell of the grid. The
+        // rest (most of the candidates the margins bring in) are neither ordered nor built; the
+        // records are unchanged, as every crater left out would be dropped by its exact
+        // footprint below.
+        const double growth = max_outline_scale(irregular) * (1.0 + 1e-9);
+        std::vector<uint8_t> candidate(craters.size());
+        parallel_for((craters.size() + 4095) / 4096, threads, [&](size_t part) {
+            const size_t end = std::min(craters.size(), (part + 1) * 4096);
+            for (size_t i = part * 4096; i < end; ++i) {
+                const Crater& c = craters[i];
+                candidate[i] = resolution_weight(c.diameter, spacing) != 0.0 &&
+                               footprint_cells(*grid, c.x, c.y,
+                                               growth * reachRadii * (0.5 * c.diameter));
+            }
+        });
         // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
-        // descending, id, draw index. The keys are sorted by value in chunks on the host threads,
-        // then merged; the order is total, so the result is the one order whatever the split.
-        struct OrderKey {
-            double age, diameter;
-            uint64_t id;
-            size_t index;
-            bool operator<(const OrderKey& o) const {
-                if (age != o.age) {
-                    return age > o.age;
-                }
-                if (diameter != o.diameter) {
-                    return diameter > o.diameter;
-                }
-                return id != o.id ? id < o.id : index < o.index;
+        // descending, id, draw index. The candidates are spread over one bucket each on average by
+        // age (floor((oldest - age) * scale): monotone in the age, so every bucket precedes the
+        // next in the order and equal ages share one), then each bucket is sorted by the whole
+        // comparison on the host threads. The order is total, so it is the one the comparison
+        // defines, whatever the ages' spread.
+        if (craters.size() >= (size_t(1) << 32)) {
+            return TG_ERROR_UNSUPPORTED;
+        }
+        std::vector<uint32_t> kept;
+        kept.reserve(craters.size());
+        double oldest = -INFINITY, youngest = INFINITY;
+        for (size_t n = 0; n < craters.size(); ++n) {
+            if (candidate[n]) {
+                kept.push_back(uint32_t(n));
+                oldest = std::fmax(oldest, craters[n].age);
+                youngest = std::fmin(youngest, craters[n].age);
             }
+        }
+        const size_t buckets = std::max<size_t>(kept.size(), 1);
+        const double spread = oldest - youngest;
+        const double scale = spread > 0.0 ? double(buckets) / spread : 0.0;
+        auto bucket_of = [&](uint32_t n) {
+            const double at = std::floor((oldest - craters[n].age) * scale);
+            return size_t(std::clamp(at, 0.0, double(buckets - 1)));
         };
-        std::vector<OrderKey> keys(craters.size());
-        for (size_t n = 0; n < keys.size(); ++n) {
-            keys[n] = OrderKey{craters[n].age, craters[n].diameter, craters[n].id, n};
+        std::vector<uint32_t> start(buckets + 1, 0);
+        for (const uint32_t n : kept) {
+            ++start[bucket_of(n) + 1];
         }
+        for (size_t q = 0; q < buckets; ++q) {
+            start[q + 1] += start[q];
+        }
+        std::vector<uint32_t> sorted(kept.size());
         {
-            const size_t parts = std::max<size_t>(1, std::min<size_t>(threads, keys.size() / 4096));
-            std::vector<size_t> bounds(parts + 1);
-            for (size_t q = 0; q <= parts; ++q) {
-                bounds[q] = keys.size() * q / parts;
+            std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+            for (const uint32_t n : kept) {
+                sorted[fill[bucket_of(n)]++] = n;
             }
-            parallel_for(parts, threads, [&](size_t q) {
-                std::sort(keys.begin() + bounds[q], keys.begin() + bounds[q + 1]);
-            });
-            for (size_t width = 1; width < parts; width *= 2) {
-                std::vector<size_t> merges;
-                for (size_t q = 0; q + width < parts; q += 2 * width) {
-                    merges.push_back(q);
+        }
+        const auto earlier = [&](uint32_t a, uint32_t b) {
+            const Crater &ca = craters[a], &cb = craters[b];
+            if (ca.age != cb.age) {
+                return ca.age > cb.age;
+            }
+            if (ca.diameter != cb.diameter) {
+                return ca.diameter > cb.diameter;
+            }
+            return ca.id != cb.id ? ca.id < cb.id : a < b;
+        };
+        parallel_for((buckets + 4095) / 4096, threads, [&](size_t part) {
+            const size_t end = std::min(buckets, (part + 1) * 4096);
+            for (size_t q = part * 4096; q < end; ++q) {
+                if (start[q + 1] - start[q] > 1) {
+                    std::sort(sorted.begin() + start[q], sorted.begin() + start[q + 1], earlier);
                 }
-                parallel_for(merges.size(), threads, [&](size_t m) {
-                    const size_t q = merges[m];
-                    std::inplace_merge(keys.begin() + bounds[q], keys.begin() + bounds[q + width],
-                                       keys.begin() + bounds[std::min(parts, q + 2 * width)]);
-                });
             }
-        }
-        std::vector<size_t> order(keys.size());
-        for (size_t n = 0; n < order.size(); ++n) {
-            order[n] = keys[n].index;
-        }
+        });
+        std::vector<size_t> order(sorted.begin(), sorted.end());
 
         // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
         const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
@@ -1312,34 +1451,12 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
             const Outline outline = irregular ? irregular_outline(c, irregularitySeed) : Outline{};
             // CratersOnRaster: the footprint window must hold a cell of the grid.
             double scale = 1.0;
-            for (const double a : outline.amplitudes) {
-                scale += std::fabs(a);
+            for (int k = 0; k < outline.harmonics; ++k) {
+                scale += std::fabs(outline.amplitudes[k]);
             }
             scale *= std::sqrt(outline.ellipticity);
             const double reach = scale * reachRadii * (0.5 * c.diameter);
-            // Surface::Expand, then MappedBounds of GeoTransform::WorldToPixel over the box's corners
-            // (src/raster/cell_loops.cpp:21-28, geo_transform.h:70), then ClampIndex.
-            const double det =
-                grid->pixel_width * grid->pixel_height - grid->row_rotation * grid->col_rotation;
-            double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
-            for (const double wx : {c.x - reach, c.x + reach}) {
-                for (const double wy : {c.y - reach, c.y + reach}) {
-                    const double dx = wx - grid->origin_x;
-                    const double dy = wy - grid->origin_y;
-                    const double px = (dx * grid->pixel_height - dy * grid->row_rotation) / det;
-                    const double py = (dy * grid->pixel_width - dx * grid->col_rotation) / det;
-                    minX = std::fmin(minX, px);
-                    minY = std::fmin(minY, py);
-                    maxX = std::fmax(maxX, px);
-                    maxY = std::fmax(maxY, py);
-                }
-            }
-            const double w = grid->width, h = grid->height;
-            const double c0 = std::clamp(std::floor(minX), 0.0, w);
-            const double c1 = std::clamp(std::ceil(maxX), 0.0, w);
-            const double r0 = std::clamp(std::floor(minY), 0.0, h);
-            const double r1 = std::clamp(std::ceil(maxY), 0.0, h);
-            if (!(size_t(c0) < size_t(c1) && size_t(r0) < size_t(r1))) {
+            if (!footprint_cells(*grid, c.x, c.y, reach)) {
                 return;
             }
             // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
@@ -1365,8 +1482,8 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
             r.heading = float(outline.heading);
             r.harmonicOffset = uint32_t(values.size());
             r.firstHarmonic = uint32_t(outline.firstHarmonic);
-            r.harmonicCount = uint32_t(outline.amplitudes.size());
-            for (size_t k = 0; k < outline.amplitudes.size(); ++k) {
+            r.harmonicCount = uint32_t(outline.harmonics);
+            for (int k = 0; k < outline.harmonics; ++k) {
                 values.push_back(float(outline.amplitudes[k]));
                 values.push_back(float(outline.phases[k]));
             }
