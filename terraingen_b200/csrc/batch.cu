@@ -20,6 +20,8 @@
 //
 // Built with -fmad=false: every fused multiply-add is written out, so heights are the same bits
 // whichever kernel shape (bin size, cells per thread) the autotuner picks.
+#include <utility>
+
 #include "binning.cuh"
 #include "crater_math.cuh"
 #include "ds_tile.cuh"
@@ -460,7 +462,7 @@ struct PostsFromSource {
 // job by binary search over the jobs' first blocks) and write each block's base heights into the
 // batch's output.
 template <bool kSpline>
-__global__ void __launch_bounds__(kDsTileThreads) batch_ds_kernel(const BatchNoise noise,
+__global__ void __launch_bounds__(kDsTileThreads, 3) batch_ds_kernel(const BatchNoise noise,
                                                                  const BatchView v) {
     extern __shared__ double pool[];
     __shared__ DsShared sh;
@@ -486,6 +488,35 @@ __global__ void __launch_bounds__(kDsTileThreads) batch_ds_kernel(const BatchNoi
         const PostsFromSource posts{noise, t.postSpacing};
         ds_block<kSpline>(t, g - v.dsFirst[sJob], posts, heights + t.heightOffset, pool, sh);
         __syncthreads();  // the next block's boxes overwrite this one's shared state
+    }
+}
+
+// The points' diamond-square pass: each warp takes one point at a time (its node boxes are a
+// few nodes wide), eight warps a CTA, each with its own node buffers.
+template <bool kSpline>
+__global__ void __launch_bounds__(256, 3) batch_ds_points_kernel(const BatchNoise noise,
+                                                              const BatchView v) {
+    extern __shared__ double pointPool[];
+    __shared__ DsShared sh[8];
+    const uint32_t warp = threadIdx.x >> 5u;
+    const BatchHeader* header = v.header;
+    const uint32_t jobs = header->dsPointJobs, points = header->dsPoints;
+    float* const heights = header->heights;
+    for (uint32_t g = blockIdx.x * 8u + warp; g < points; g += gridDim.x * 8u) {
+        uint32_t lo = 0, hi = jobs;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (v.dsPointFirst[mid] <= g) {
+                lo = mid;
+            } else {
+                hi = mid;
+            }
+        }
+        const DsTile& t = v.dsPointJobs[lo];
+        const PostsFromSource posts{noise, t.postSpacing};
+        ds_block<kSpline>(t, g - v.dsPointFirst[lo], posts, heights + t.heightOffset,
+                          pointPool + size_t(warp) * kDsPointPool, sh[warp], WarpGroup());
+        __syncwarp();  // the next point's boxes overwrite this one's shared state
     }
 }
 
@@ -1172,13 +1203,22 @@ cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
 
 cudaError_t batch_ds_setup(uint32_t& ctas) {
     static const cudaError_t allowed = [] {
-        const cudaError_t e = cudaFuncSetAttribute(
-            batch_ds_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            int(kDsSharedBudget));
-        return e != cudaSuccess ? e
-                                : cudaFuncSetAttribute(batch_ds_kernel<false>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       int(kDsSharedBudget));
+        const int points = int(8 * kDsPointPool * sizeof(double));
+        for (const auto& [kernel, bytes] :
+             {std::make_pair(reinterpret_cast<const void*>(batch_ds_kernel<true>),
+                             int(kDsSharedBudget)),
+              std::make_pair(reinterpret_cast<const void*>(batch_ds_kernel<false>),
+                             int(kDsSharedBudget)),
+              std::make_pair(reinterpret_cast<const void*>(batch_ds_points_kernel<true>), points),
+              std::make_pair(reinterpret_cast<const void*>(batch_ds_points_kernel<false>),
+                             points)}) {
+            const cudaError_t e =
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) {
+                return e;
+            }
+        }
+        return cudaSuccess;
     }();
     if (allowed != cudaSuccess) {
         return allowed;
@@ -1194,11 +1234,13 @@ cudaError_t batch_ds_setup(uint32_t& ctas) {
 
 cudaError_t launch_batch_ds(const BatchNoise& noise, const BatchView& v, bool spline,
                             uint32_t ctas, cudaStream_t stream) {
-    const size_t bytes = kDsSharedBudget;
+    const size_t bytes = kDsSharedBudget, points = 8 * kDsPointPool * sizeof(double);
     if (spline) {
         batch_ds_kernel<true><<<ctas, kDsTileThreads, bytes, stream>>>(noise, v);
+        batch_ds_points_kernel<true><<<ctas, 256, points, stream>>>(noise, v);
     } else {
         batch_ds_kernel<false><<<ctas, kDsTileThreads, bytes, stream>>>(noise, v);
+        batch_ds_points_kernel<false><<<ctas, 256, points, stream>>>(noise, v);
     }
     return cudaGetLastError();
 }

@@ -70,6 +70,8 @@ enum BatchSlot {
     kSlotOutput,
     kSlotDsJobs,
     kSlotDsFirst,
+    kSlotDsPointJobs,
+    kSlotDsPointFirst,
     kBatchSlotCount
 };
 
@@ -98,7 +100,8 @@ struct tg_batch {
     bool loaded = false;
     Spec spec;
     std::vector<BatchTile> tiles;   // spec.items numbered for the current variant
-    uint32_t dsJobs = 0, dsBlocks = 0, dsCtas = 0;  // the diamond-square pass
+    uint32_t dsJobs = 0, dsBlocks = 0, dsCtas = 0;  // the diamond-square pass: grid jobs
+    uint32_t dsPointJobs = 0, dsPoints = 0;          // and point-set jobs
     uint32_t bins = 0;
     uint32_t recordPairs = 0, boulderPairs = 0;
     size_t outputFloats = 0;
@@ -265,6 +268,8 @@ BatchView make_view(tg_batch* b) {
     v.culls = f.culls;
     v.dsJobs = ptr<DsTile>(b, kSlotDsJobs);
     v.dsFirst = ptr<uint32_t>(b, kSlotDsFirst);
+    v.dsPointJobs = ptr<DsTile>(b, kSlotDsPointJobs);
+    v.dsPointFirst = ptr<uint32_t>(b, kSlotDsPointFirst);
     return v;
 }
 
@@ -478,6 +483,8 @@ int load_ds(tg_batch* b) {
     s.noise.baseInOutput = s.ds.on ? 1u : 0u;
     b->dsJobs = 0;
     b->dsBlocks = 0;
+    b->dsPointJobs = 0;
+    b->dsPoints = 0;
     if (!s.ds.on) {
         return TG_OK;
     }
@@ -491,10 +498,10 @@ int load_ds(tg_batch* b) {
     // The post lattice as a grid whose cell (0, 0) is centered on the origin.
     const Grid lattice{1u, 1u, -0.5 * P, P, 0.0, 0.5 * P, 0.0, -P};
     uint32_t* flags = &ptr<BatchHeader>(b, kSlotHeader)->flags;
-    std::vector<DsTile> jobs;
-    std::vector<uint32_t> first;
+    std::vector<DsTile> jobs, pointJobs;
+    std::vector<uint32_t> first, pointFirst;
     jobs.reserve(s.items.size());
-    uint64_t blocks = 0;
+    uint64_t blocks = 0, points = 0;
     for (const Item& it : s.items) {
         DsTile t{};
         if (it.points) {
@@ -505,7 +512,8 @@ int load_ds(tg_batch* b) {
             }
             const Grid one{1u, 1u, -0.5 * d, d, 0.0, 0.5 * d, 0.0, -d};
             if (!ds_setup(t, lattice, s.ds.fractalDimension, s.ds.scale, s.ds.seed,
-                          s.ds.minPixelSize, s.ds.spline, one)) {
+                          s.ds.minPixelSize, s.ds.spline, one, true) ||
+                t.capEven + t.capOdd > kDsPointPool) {
                 return fail(TG_ERROR_ARGUMENT, "the points are too coarse for the posts' nodes");
             }
             t.points = ptr<double>(b, kSlotPoints) + 2 * size_t(it.pointBegin);
@@ -523,23 +531,38 @@ int load_ds(tg_batch* b) {
         t.postSpacing = P;
         t.heightOffset = it.heightOffset;
         t.status = flags;
-        first.push_back(uint32_t(blocks));
-        blocks += t.blocks;
-        jobs.push_back(t);
+        if (it.points) {
+            pointFirst.push_back(uint32_t(points));
+            points += t.blocks;
+            pointJobs.push_back(t);
+        } else {
+            first.push_back(uint32_t(blocks));
+            blocks += t.blocks;
+            jobs.push_back(t);
+        }
     }
-    if (blocks >= 0xffffffffull) {
+    if (blocks >= 0xffffffffull || points >= 0xffffffffull) {
         return fail(TG_ERROR_UNSUPPORTED, "a batch's diamond-square pass holds fewer than 2^32 "
-                                          "blocks");
+                                          "blocks and points");
     }
     first.push_back(uint32_t(blocks));
-    if (int st = upload(b, kSlotDsJobs, jobs.data(), jobs.size())) {
-        return st;
+    pointFirst.push_back(uint32_t(points));
+    for (const auto& [slot, v] : {std::make_pair(kSlotDsJobs, &jobs),
+                                  std::make_pair(kSlotDsPointJobs, &pointJobs)}) {
+        if (int st = upload(b, slot, v->data(), v->size())) {
+            return st;
+        }
     }
-    if (int st = upload(b, kSlotDsFirst, first.data(), first.size())) {
-        return st;
+    for (const auto& [slot, v] : {std::make_pair(kSlotDsFirst, &first),
+                                  std::make_pair(kSlotDsPointFirst, &pointFirst)}) {
+        if (int st = upload(b, slot, v->data(), v->size())) {
+            return st;
+        }
     }
     b->dsJobs = uint32_t(jobs.size());
     b->dsBlocks = uint32_t(blocks);
+    b->dsPointJobs = uint32_t(pointJobs.size());
+    b->dsPoints = uint32_t(points);
     return TG_OK;
 }
 
@@ -658,6 +681,8 @@ int launch(tg_batch* b, float* out, cudaStream_t stream) {
     h.heights = out;
     h.dsJobs = b->dsJobs;
     h.dsBlocks = b->dsBlocks;
+    h.dsPointJobs = b->dsPointJobs;
+    h.dsPoints = b->dsPoints;
     b->pinned[0] = h;
     const Signature s = signature(b);
     if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {

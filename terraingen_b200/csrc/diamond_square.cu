@@ -48,20 +48,20 @@ __global__ void philox_probe_kernel(const uint32_t* __restrict__ in, uint32_t n,
 
 
 // The output block of a diamond-square CTA and the shared buffers its node pyramid needs: the
-// largest block (64 x 64, 64 x 32, 32 x 32, ... cells) whose two buffers fit kDsSharedBudget
-// bytes, so that three CTAs share an SM. A bigger block recomputes fewer nodes of its neighbours'
+// largest block (64 x 64, 64 x 32, 32 x 32, ... cells; one cell for a point) whose two buffers
+// fit kDsSharedBudget bytes, so that three CTAs share an SM. A bigger block recomputes fewer nodes of its neighbours'
 // (the margins the means need) per cell. Each level's box is bounded from the block's extent in
 // finest nodes (what the device works out, plus two nodes for the rounding of either side's
 // arithmetic), then level by level: the box the diamond step reads grows by the mean's reach, and
 // its parents' box is half of it plus the square mean's margins.
 
-bool ds_tile_shape(DsTile& t, bool spline) {
+bool ds_tile_shape(DsTile& t, bool spline, bool single) {
     const int64_t reach = spline ? 3 : 1, before = spline ? 1 : 0, after = spline ? 2 : 1;
     const Grid& g = t.grid;
     constexpr uint32_t kShapes[][2] = {{64, 64}, {64, 32}, {32, 32}, {32, 16}, {16, 16}, {16, 8},
                                        {8, 8},   {8, 4},   {4, 4},   {4, 2},   {2, 2},   {1, 1}};
     for (const auto& shape : kShapes) {
-        const uint32_t bw = shape[0], bh = shape[1];
+        const uint32_t bw = single ? 1u : shape[0], bh = single ? 1u : shape[1];
         const double spanX = (double(bw - 1) * std::fabs(g.pixelWidth) +
                               double(bh - 1) * std::fabs(g.rowRotation)) /
                              std::fabs(t.frame.stepX);
@@ -97,7 +97,7 @@ bool ds_tile_shape(DsTile& t, bool spline) {
 }  // namespace
 
 bool ds_setup(DsTile& t, const Grid& pg, double fractalDimension, double scale, uint32_t seed,
-              double minPixelSize, bool spline, const Grid& g) {
+              double minPixelSize, bool spline, const Grid& g, bool single) {
     // Levels(post spacing, spacing) (diamond_square.cpp:289-300).
     const double postSpacing = std::max(std::fabs(pg.pixelWidth), std::fabs(pg.pixelHeight));
     const double spacing = std::max(std::fabs(g.pixelWidth), std::fabs(g.pixelHeight));
@@ -126,7 +126,7 @@ bool ds_setup(DsTile& t, const Grid& pg, double fractalDimension, double scale, 
         t.diamondStep[l] = scale * std::pow(stepFactor, 2 * l);
     }
     t.pitch = g.width;
-    if (!ds_tile_shape(t, spline)) {
+    if (!ds_tile_shape(t, spline, single)) {
         return false;
     }
     t.blocks = t.blocksX * ((g.height + t.blockH - 1) / t.blockH);

@@ -180,13 +180,27 @@ __device__ __forceinline__ void cell_center(const Grid& g, uint32_t c, uint32_t 
     y = g.originY + (double(c) + 0.5) * g.colRotation + (double(r) + 0.5) * g.pixelHeight;
 }
 
-// Walks a w x h box (w > 0) in row-major order with the CTA's threads, thread k taking items k,
+// The threads that refine one block together: the whole CTA (a grid block), or one warp (a
+// point, whose node boxes are a few nodes wide).
+struct CtaGroup {
+    __device__ __forceinline__ int32_t rank() const { return int32_t(threadIdx.x); }
+    __device__ __forceinline__ int32_t size() const { return int32_t(blockDim.x); }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct WarpGroup {
+    __device__ __forceinline__ int32_t rank() const { return int32_t(threadIdx.x & 31u); }
+    __device__ __forceinline__ int32_t size() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+
+// Walks a w x h box (w > 0) in row-major order with a group's threads, thread k taking items k,
 // k + n, k + 2n, ... (n threads): consecutive threads take neighbouring nodes, the work splits
 // evenly, and a thread steps its (x, y) without dividing.
 struct BoxWalk {
     int32_t x, y, dx, dy, w;
-    __device__ __forceinline__ explicit BoxWalk(int32_t width) : w(width) {
-        const int32_t k = int32_t(threadIdx.x), n = int32_t(blockDim.x);
+    template <class Group>
+    __device__ __forceinline__ BoxWalk(int32_t width, const Group& g) : w(width) {
+        const int32_t k = g.rank(), n = g.size();
         x = k % w;
         y = k / w;
         dx = n % w;
@@ -240,12 +254,13 @@ struct PostsFromArray {
 //             level reads (DiamondStep, :410-424), in place;
 //   read      each cell from the finest level.
 // Levels of even and odd number alternate between two shared buffers of t.capEven and t.capOdd
-// doubles. Thread 0 works out the boxes; one that would outgrow its buffer (the host sizes them
+// doubles. The group's first thread works out the boxes; one that would outgrow its buffer (the host sizes them
 // from the block's extent, so never) sets flag 1 and the CTA writes nothing. Loops run over local
 // 32-bit box coordinates; only the displacement's key takes the node's 64-bit index.
-template <bool kSpline, class Posts>
+template <bool kSpline, class Posts, class Group = CtaGroup>
 __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const Posts& posts,
-                                         float* heights, double* pool, DsShared& sh) {
+                                         float* heights, double* pool, DsShared& sh,
+                                         const Group group = Group()) {
     constexpr int64_t kReach = kSpline ? 3 : 1;   // the diamond mean's reach (Refine's `reach`)
     constexpr int64_t kBefore = kSpline ? 1 : 0;  // parents a square mean reads before its block
     constexpr int64_t kAfter = kSpline ? 2 : 1;   // and after it; the read's nodes after a cell
@@ -273,7 +288,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
     };
     const int levels = t.levels;
     const bool northUp = !single && t.grid.rowRotation == 0.0 && t.grid.colRotation == 0.0;
-    if (threadIdx.x == 0) {
+    if (group.rank() == 0) {
         double umin = INFINITY, umax = -INFINITY, vmin = INFINITY, vmax = -INFINITY;
         for (int k = 0; k < 4; ++k) {
             double x, y;
@@ -304,7 +319,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
             atomicOr(t.status, 1u);
         }
     }
-    __syncthreads();
+    group.sync();
     if (!sh.fits) {
         return;
     }
@@ -314,7 +329,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
         // box) and share are found once per column and row.
         const int64_t fc0 = sh.inner[levels].c0 - (levels > 0 ? kReach : 0);
         const int64_t fr0 = sh.inner[levels].r0 - (levels > 0 ? kReach : 0);
-        for (uint32_t i = threadIdx.x; i < cw + rh; i += blockDim.x) {
+        for (uint32_t i = uint32_t(group.rank()); i < cw + rh; i += uint32_t(group.size())) {
             double x, y;
             int64_t node;
             double share;
@@ -333,11 +348,11 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
     }
     {
         const NodeBox p = sh.inner[0];
-        for (BoxWalk it(p.w); it.y < p.h; it.next()) {
+        for (BoxWalk it(p.w, group); it.y < p.h; it.next()) {
             pool[it.y * p.w + it.x] = posts(p.c0 + it.x, p.r0 + it.y);
         }
     }
-    __syncthreads();
+    group.sync();
     NodeBox pb = sh.inner[0];
     const double* parents = pool;
     for (int l = 1; l <= levels; ++l) {
@@ -357,7 +372,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
             const int32_t shh = int32_t(floor_half(ob.r0 + ob.h - 1) - sr0 + 1);
             const int32_t pcBase = int32_t(sc0 - pb.c0), prBase = int32_t(sr0 - pb.r0);
             const int32_t ocBase = int32_t(2 * sc0 - ob.c0), orBase = int32_t(2 * sr0 - ob.r0);
-            for (BoxWalk it((sw + 1) / 2); it.y < shh; it.next()) {
+            for (BoxWalk it((sw + 1) / 2, group); it.y < shh; it.next()) {
                 const int32_t j = it.y;
                 const int64_t row = 2 * (sr0 + j) + 1;
                 double normal[2];
@@ -399,7 +414,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
                 }
             }
         }
-        __syncthreads();
+        group.sync();
         // Diamond step: the mixed nodes (2 bc + 1, 2 br) and (2 bc, 2 br + 1) inside the box the
         // next level reads, from the square step's nodes around them (kReach local columns and
         // rows of the output box lie before the inner box). Both displacements of a block are
@@ -409,7 +424,7 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
             const int32_t dw = int32_t(floor_half(d.c0 + d.w - 1) - dc0 + 1);
             const int32_t dh = int32_t(floor_half(d.r0 + d.h - 1) - dr0 + 1);
             const int32_t lcBase = int32_t(2 * dc0 - d.c0), lrBase = int32_t(2 * dr0 - d.r0);
-            for (BoxWalk it(dw); it.y < dh; it.next()) {
+            for (BoxWalk it(dw, group); it.y < dh; it.next()) {
                 const int32_t i = it.x, j = it.y;
                 double normal[2];
 #pragma unroll
@@ -442,13 +457,13 @@ __device__ __forceinline__ void ds_block(const DsTile& t, uint32_t block, const 
                 }
             }
         }
-        __syncthreads();
+        group.sync();
         parents = out;
         pb = ob;
     }
     // The read: consecutive threads take consecutive cells of a row.
     const Nodes finest{pb, const_cast<double*>(parents)};
-    for (BoxWalk it{int32_t(cw)}; it.y < int32_t(rh); it.next()) {
+    for (BoxWalk it(int32_t(cw), group); it.y < int32_t(rh); it.next()) {
         const uint32_t c = uint32_t(it.x), r = uint32_t(it.y);
         double value;
         if (northUp && !kSpline) {

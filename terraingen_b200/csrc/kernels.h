@@ -230,10 +230,12 @@ struct DsTile {
 constexpr size_t kDsSharedBudget = TGB_DS_SHARED_BUDGET;
 // The refinement of posts on `postGrid` (a lattice: post (0, 0) at its cell (0, 0)) read at
 // `grid`'s cells (Levels, the frame and Displacement, diamond_square.cpp:289-389): fills t's
-// grid, frame, levels, seed, displacement scales, pitch (grid.width), block shape and blocks.
-// False when no block's node buffers fit kDsSharedBudget.
+// grid, frame, levels, seed, displacement scales, pitch (grid.width), block shape and blocks;
+// with `single`, the buffers of a one-cell block (a point). False when no block's node buffers
+// fit kDsSharedBudget.
 bool ds_setup(DsTile& t, const Grid& postGrid, double fractalDimension, double scale,
-              uint32_t seed, double minPixelSize, bool spline, const Grid& grid);
+              uint32_t seed, double minPixelSize, bool spline, const Grid& grid,
+              bool single = false);
 cudaError_t launch_ds_tiles(const DsTile& t, bool spline, cudaStream_t stream);
 // Philox4x32-10 of n (counter, key) sextets, and the displacement normal the first two counter
 // words, the third's low 5 bits and the key's first word key as (col, row, level, seed).
@@ -328,7 +330,8 @@ struct BatchHeader {
     uint32_t flags;    // 1 datum seen, 2 staged copy timed out, 8 a record needs the general path
     unsigned long long craterPairs, boulderPairs;  // (cell, feature) pairs evaluated
     uint32_t craterEntries, boulderEntries;         // entries the bins needed
-    uint32_t dsJobs, dsBlocks;                      // the diamond-square pass's jobs and blocks
+    uint32_t dsJobs, dsBlocks;                      // the diamond-square pass: grid jobs, blocks
+    uint32_t dsPointJobs, dsPoints;                 // and point-set jobs, points
 };
 
 struct BatchView {
@@ -361,8 +364,10 @@ struct BatchView {
     const PointRegion* pointRegions;
     const uint32_t* pointLists;    // the regions' cell lists
     const float* culls;            // indexed points: each record's cull distance
-    const DsTile* dsJobs;          // diamond-square source: one job per item
+    const DsTile* dsJobs;          // diamond-square source: one job per grid item
     const uint32_t* dsFirst;       // [jobs + 1]: each job's first block of the pass
+    const DsTile* dsPointJobs;     // one job per point set
+    const uint32_t* dsPointFirst;  // [point jobs + 1]: each job's first point of the pass
 };
 
 // A kernel shape of the persistent evaluation: bins of binW x binH cells (point sets: blocks of
@@ -382,11 +387,14 @@ int batch_blocks_per_sm(int index, bool fast);
 cudaError_t launch_batch_bin(const CraterShapeKernel& k, const BatchView& v,
                              const BatchVariant& variant, uint32_t maxRecordPairs,
                              uint32_t maxBoulderPairs, uint32_t* scanScratch, cudaStream_t stream);
-// The diamond-square source of a batch (header->dsJobs jobs over header->dsBlocks blocks, the
-// jobs in v.dsJobs): persistent CTAs take the blocks in turn, each job's level-0 nodes from the
-// batch's fBm at its post lattice, and write every item's base heights into the output before the
-// evaluation adds the layers (noise.baseInOutput). A block whose node boxes outgrow the shared
-// buffers sets header flag 16 and writes nothing.
+// The diamond-square source of a batch (header->dsJobs grid jobs over header->dsBlocks blocks,
+// header->dsPointJobs point-set jobs over header->dsPoints points): persistent CTAs take the
+// grid blocks in turn and, in a second launch, their warps take the points one each, each job's
+// level-0 nodes from the batch's fBm at its post lattice, and write every item's base heights
+// into the output before the evaluation adds the layers (noise.baseInOutput). A block whose node
+// boxes outgrow the shared buffers sets header flag 16 and writes nothing.
+// A point's node pyramid in doubles, both buffers (one warp's share of the points' launch).
+constexpr uint32_t kDsPointPool = 768;
 // batch_ds_setup lets the pass take its shared memory and gives the CTAs of a launch (call it
 // before any capture).
 cudaError_t batch_ds_setup(uint32_t& ctas);
