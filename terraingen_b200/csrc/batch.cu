@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(kBinW* kBinH / kCells, 768 / (kBinW * kBinH / 
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const crater::FastKernel fk{k.profile.simple, k.profile.rim, k.reachRadii};
     BatchHeader* header = v.header;
-    const uint32_t nbins = header->bins, ntiles = header->tiles;
+    const uint32_t nbins = min(header->bins, header->evalEnd), ntiles = header->tiles;
     float* const heights = header->heights;
     if (tid == 0) {
         mbar_init(&bars[0], 1);

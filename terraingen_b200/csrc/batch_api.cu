@@ -75,6 +75,10 @@ enum BatchSlot {
     kBatchSlotCount
 };
 
+// Chunks of a batch whose heights go to host memory: each one's copy overlaps the next one's
+// evaluation.
+constexpr int kOutputChunks = 8;
+
 // What a captured graph depends on; a change means a new capture.
 struct Signature {
     BatchView view;
@@ -114,6 +118,12 @@ struct tg_batch {
     Signature launched{};
 
     cudaGraph_t graph[2] = {nullptr, nullptr};  // binning, evaluation
+
+    // Host outputs: the evaluation by chunks of items, each chunk's heights copied out on
+    // `copyStream` while the next chunk is evaluated (made on the first such call).
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t chunkDone[kOutputChunks] = {};
+    uint32_t* chunkWords = nullptr;  // pinned: each chunk's first bin and end bin
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     Signature captured{};
     uint32_t captures = 0, replays = 0;
@@ -668,10 +678,9 @@ int load(tg_batch* b, Spec&& spec) {
     return TG_OK;
 }
 
-int launch(tg_batch* b, float* out, cudaStream_t stream) {
-    if (b->pending) {
-        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
-    }
+// The header of a launch into `out` in pinned[0], and the graphs captured for it; `s` its
+// signature.
+int prepare(tg_batch* b, float* out, Signature& s) {
     BatchHeader h{};
     h.tiles = uint32_t(b->tiles.size());
     h.refs = uint32_t(b->spec.refs.size());
@@ -683,12 +692,24 @@ int launch(tg_batch* b, float* out, cudaStream_t stream) {
     h.dsBlocks = b->dsBlocks;
     h.dsPointJobs = b->dsPointJobs;
     h.dsPoints = b->dsPoints;
+    h.evalEnd = 0xffffffffu;
     b->pinned[0] = h;
-    const Signature s = signature(b);
+    s = signature(b);
     if (b->exec[1] == nullptr || std::memcmp(&s, &b->captured, sizeof(Signature)) != 0) {
         if (int st = capture(b, s)) {
             return st;
         }
+    }
+    return TG_OK;
+}
+
+int launch(tg_batch* b, float* out, cudaStream_t stream) {
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
+    Signature s;
+    if (int st = prepare(b, out, s)) {
+        return st;
     }
     TG_CUDA(cudaEventRecord(b->events[0], stream), "event record");
     TG_CUDA(cudaGraphLaunch(b->exec[0], stream), "graph launch");
@@ -700,6 +721,101 @@ int launch(tg_batch* b, float* out, cudaStream_t stream) {
     b->out = out;
     b->launchStream = stream;
     b->launched = s;
+    return TG_OK;
+}
+
+// launch() for host heights: the binning graph, then the evaluation by chunks of consecutive
+// items in the work queue's order (about equal output each: the queue's cursor and end set per
+// chunk), each chunk's items' output ranges (merged where they meet) copied into `heights` on the
+// copy stream while the next chunk is evaluated. Pending like launch(); finish() completes it (a
+// relaunch for more entries copies nothing).
+int launch_chunked(tg_batch* b, float* out, float* heights, cudaStream_t stream) {
+    if (b->pending) {
+        return fail(TG_ERROR_STATE, "the batch's last launch has not finished");
+    }
+    if (b->copyStream == nullptr) {
+        TG_CUDA(cudaStreamCreateWithFlags(&b->copyStream, cudaStreamNonBlocking), "stream");
+        for (cudaEvent_t& e : b->chunkDone) {
+            TG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        }
+        TG_CUDA(cudaMallocHost(&b->chunkWords, 2 * kOutputChunks * sizeof(uint32_t)),
+                "pinned allocation");
+    }
+    Signature sig;
+    if (int st = prepare(b, out, sig)) {
+        return st;
+    }
+    // Each item's output range; chunks cut at about equal shares of the output.
+    const size_t items = b->tiles.size();
+    std::vector<uint64_t> lo(items), hi(items);
+    uint64_t total = 0;
+    for (size_t i = 0; i < items; ++i) {
+        const Item& it = b->spec.items[i];
+        lo[i] = it.heightOffset;
+        hi[i] = it.points ? lo[i] + it.grid.width
+                          : lo[i] + uint64_t(it.grid.height - 1) * it.pitch + it.grid.width;
+        total += hi[i] - lo[i];
+    }
+    BatchHeader* header = ptr<BatchHeader>(b, kSlotHeader);
+    TG_CUDA(cudaEventRecord(b->events[0], stream), "event record");
+    TG_CUDA(cudaGraphLaunch(b->exec[0], stream), "graph launch");
+    TG_CUDA(cudaEventRecord(b->events[1], stream), "event record");
+    size_t first = 0;
+    uint64_t covered = 0;
+    for (int c = 0; c < kOutputChunks && first < items; ++c) {
+        size_t end = first;
+        const uint64_t target = total * uint64_t(c + 1) / kOutputChunks;
+        while (end < items && (end == first || covered < target || c + 1 == kOutputChunks)) {
+            covered += hi[end] - lo[end];
+            ++end;
+        }
+        // The chunk's output ranges in address order, merged across gaps under 16 KB.
+        std::vector<std::pair<uint64_t, uint64_t>> ranges;
+        for (size_t i = first; i < end; ++i) {
+            ranges.emplace_back(lo[i], hi[i]);
+        }
+        std::sort(ranges.begin(), ranges.end());
+        std::vector<std::pair<uint64_t, uint64_t>> merged;
+        for (const auto& r : ranges) {
+            if (!merged.empty() && r.first <= merged.back().second + 4096) {
+                merged.back().second = std::max(merged.back().second, r.second);
+            } else {
+                merged.push_back(r);
+            }
+        }
+        uint32_t* words = b->chunkWords + 2 * c;
+        words[0] = b->tiles[first].binBase;
+        words[1] = end < items ? b->tiles[end].binBase : b->bins;
+        TG_CUDA(cudaMemcpyAsync(&header->next, &words[0], sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, stream),
+                "copy to device");
+        TG_CUDA(cudaMemcpyAsync(&header->evalEnd, &words[1], sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, stream),
+                "copy to device");
+        TG_CUDA(launch_batch_evaluate(sig.kernel, sig.noise, sig.view, sig.variant, sig.fast,
+                                      sig.ctas, stream),
+                "evaluation launch");
+        TG_CUDA(cudaEventRecord(b->chunkDone[c], stream), "event record");
+        TG_CUDA(cudaStreamWaitEvent(b->copyStream, b->chunkDone[c], 0), "stream wait");
+        for (const auto& [from, to] : merged) {
+            TG_CUDA(cudaMemcpyAsync(heights + from, out + from, (to - from) * sizeof(float),
+                                    cudaMemcpyDeviceToHost, b->copyStream),
+                    "copy to host");
+        }
+        first = end;
+    }
+    TG_CUDA(cudaMemcpyAsync(&b->pinned[1], header, sizeof(BatchHeader), cudaMemcpyDeviceToHost,
+                            stream),
+            "copy to host");
+    // The launch ends when its copies have.
+    TG_CUDA(cudaEventRecord(b->chunkDone[0], b->copyStream), "event record");
+    TG_CUDA(cudaStreamWaitEvent(stream, b->chunkDone[0], 0), "stream wait");
+    TG_CUDA(cudaEventRecord(b->events[2], stream), "event record");
+    ++b->replays;
+    b->pending = true;
+    b->out = out;
+    b->launchStream = stream;
+    b->launched = sig;
     return TG_OK;
 }
 
@@ -900,6 +1016,18 @@ void tg_batch_destroy(tg_batch* b) {
     if (b->pinned != nullptr) {
         cudaFreeHost(b->pinned);
     }
+    if (b->chunkWords != nullptr) {
+        cudaFreeHost(b->chunkWords);
+    }
+    for (cudaEvent_t e : b->chunkDone) {
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+        }
+    }
+    if (b->copyStream != nullptr) {
+        cudaStreamSynchronize(b->copyStream);
+        cudaStreamDestroy(b->copyStream);
+    }
     if (b->stream != nullptr) {
         cudaStreamDestroy(b->stream);
     }
@@ -1061,7 +1189,26 @@ int tg_batch_evaluate(tg_batch* b, float* heights, size_t n_heights, int memory,
         TG_CUDA(b->slots[kSlotOutput].reserve(b->outputFloats * sizeof(float)), "allocation");
         out = ptr<float>(b, kSlotOutput);
     }
-    if (int st = replay(b, out, s)) {
+    cudaPointerAttributes where{};
+    const bool pinned = memory == TG_MEMORY_HOST &&
+                        cudaPointerGetAttributes(&where, heights) == cudaSuccess &&
+                        where.type == cudaMemoryTypeHost;
+    (void)cudaGetLastError();
+    if (pinned && !b->spec.ds.on && b->tiles.size() >= 2) {
+        // Page-locked heights cross to the host chunk by chunk while later chunks are evaluated;
+        // if the bins needed more entries, the batch ran again whole and its heights are copied
+        // again.
+        const uint32_t before = b->replays;
+        if (int st = launch_chunked(b, out, heights, s)) {
+            return st;
+        }
+        if (int st = finish(b)) {
+            return st;
+        }
+        if (b->replays == before + 1) {
+            return TG_OK;
+        }
+    } else if (int st = replay(b, out, s)) {
         return st;
     }
     if (memory == TG_MEMORY_HOST) {

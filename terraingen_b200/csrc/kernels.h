@@ -332,6 +332,7 @@ struct BatchHeader {
     uint32_t craterEntries, boulderEntries;         // entries the bins needed
     uint32_t dsJobs, dsBlocks;                      // the diamond-square pass: grid jobs, blocks
     uint32_t dsPointJobs, dsPoints;                 // and point-set jobs, points
+    uint32_t evalEnd, pad2_;                        // the evaluation takes bins below this
 };
 
 struct BatchView {

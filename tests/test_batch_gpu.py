@@ -271,3 +271,27 @@ def test_batch_shared_records(batch, tiles):
     a = ts.tile_view(out, 0)
     b = ts.tile_view(out, len(t) - 1)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_batch_pinned_host_output_equals_device(device, tiles):
+    # Page-locked host heights cross chunk by chunk while later chunks are evaluated: the same
+    # bits as a device evaluation, on a fresh batch (whose first run grows its bins' entries and
+    # runs again whole) and on the replays after it.
+    import torch
+
+    from terraingen_b200.batch import Batch
+
+    dev = torch.zeros(tiles.output_floats, dtype=torch.float32, device="cuda")
+    with Batch(device) as fresh:
+        fresh.load(tiles)
+        pinned = torch.zeros(tiles.output_floats, dtype=torch.float32).pin_memory().numpy()
+        fresh.evaluate(pinned)
+        fresh.evaluate(dev)
+        want = dev.cpu().numpy()
+        for i in range(len(tiles.grids)):
+            assert np.array_equal(tiles.tile_view(pinned, i), tiles.tile_view(want, i)), i
+        pinned[:] = np.nan
+        fresh.evaluate(pinned)
+        fresh.evaluate(pinned)
+        for i in range(len(tiles.grids)):
+            assert np.array_equal(tiles.tile_view(pinned, i), tiles.tile_view(want, i)), i
