@@ -53,6 +53,37 @@ inline Words4 philox(Words4 c, uint32_t k0, uint32_t k1) {
     return c;
 }
 
+// Philox4x32-10 of n counters held as four word arrays, in place: the blocks of many streams at
+// once, in a loop the host compiler vectorizes across counters (one build per vector width, the
+// widest the host supports taken at load time). Integer work only, so every build gives the
+// bits `philox` gives.
+__attribute__((target_clones("avx512f", "avx2", "default"))) void philox_soa(
+    uint32_t* __restrict x, uint32_t* __restrict y, uint32_t* __restrict z,
+    uint32_t* __restrict w, size_t n, uint32_t k0, uint32_t k1) {
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t cx = x[i], cy = y[i], cz = z[i], cw = w[i];
+        uint32_t a = k0, b = k1;
+        for (int round = 0; round < 10; ++round) {
+            if (round > 0) {
+                a += 0x9E3779B9u;
+                b += 0xBB67AE85u;
+            }
+            const uint64_t p0 = uint64_t(0xD2511F53u) * cx;
+            const uint64_t p1 = uint64_t(0xCD9E8D57u) * cz;
+            const uint32_t nx = uint32_t(p1 >> 32) ^ cy ^ a;
+            const uint32_t nz = uint32_t(p0 >> 32) ^ cw ^ b;
+            cy = uint32_t(p1);
+            cw = uint32_t(p0);
+            cx = nx;
+            cz = nz;
+        }
+        x[i] = cx;
+        y[i] = cy;
+        z[i] = cz;
+        w[i] = cw;
+    }
+}
+
 // Stream tags (include/terraingen/random/streams.h:15-26).
 constexpr uint32_t kCraterStream = 0x43524154u;
 constexpr uint32_t kCraterAgeStream = 0x43524147u;
@@ -263,17 +294,16 @@ int32_t cell_coordinate(double v) {
     return int32_t(v);
 }
 
-// GenerateCellCraters on a plane (population.cpp:381).
-std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const PowerLaw& law,
-                                 double lifetime, uint32_t seed) {
+// GenerateCellCraters on a plane (population.cpp:381): sink(crater) for each in draw order.
+template <typename Sink>
+void each_cell_crater(const Band& band, int32_t i, int32_t j, const PowerLaw& law,
+                      double lifetime, uint32_t seed, const Sink& sink) {
     const uint32_t k = uint32_t(band.exponent);
     Stream geometry(seed, kCraterStream, uint32_t(i), uint32_t(j), k);
     Stream ages(seed, kCraterAgeStream, uint32_t(i), uint32_t(j), k);
     const double perArea = law.expected(band.low, band.high);
     const double area = band.cellSize * band.cellSize;
     const uint64_t count = poisson(geometry, perArea * area);
-    std::vector<Crater> out;
-    out.reserve(size_t(count));
     for (uint64_t index = 0; index < count; ++index) {
         const double diameter = law.sample(geometry, band.low, band.high);
         const double u = geometry.next_double();
@@ -283,8 +313,14 @@ std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const P
         const double age = std::clamp(ages.next_double() * lifetime, 0.0, lifetime);
         const Words4 id = philox(Words4{uint32_t(i), uint32_t(j), k, uint32_t(index)}, seed,
                                  kCraterIdStream);
-        out.push_back({x, y, diameter, age, (uint64_t(id.x) << 32) | id.y});
+        sink(Crater{x, y, diameter, age, (uint64_t(id.x) << 32) | id.y});
     }
+}
+
+std::vector<Crater> cell_craters(const Band& band, int32_t i, int32_t j, const PowerLaw& law,
+                                 double lifetime, uint32_t seed) {
+    std::vector<Crater> out;
+    each_cell_crater(band, i, j, law, lifetime, seed, [&](const Crater& c) { out.push_back(c); });
     return out;
 }
 
@@ -405,11 +441,14 @@ void parallel_for(size_t n, unsigned threads, const Body& body) {
 }
 
 // Craters over `region` with their candidate margin (GenerateCraters, planar, no spacing,
-// density map or manual craters). Each band's row of generation cells is drawn on its own (by
-// `threads` host threads when asked), and the rows are joined in the reference's order: bands
-// ascending, rows j, cells i, craters in draw order.
-std::vector<Crater> generate(const tg_crater_population& spec, const Box& region,
-                             const PowerLaw& law, unsigned threads = 1) {
+// density map or manual craters), into `out`, those for which `wanted` holds. Each band's row of
+// generation cells is drawn on its own (by `threads` host threads when asked), and the rows are
+// joined in the reference's order: bands ascending, rows j, cells i, craters in draw order. The
+// rows' lists are kept per calling thread from call to call, so repeated calls allocate nothing
+// once they have grown.
+template <typename Wanted>
+void generate_into(const tg_crater_population& spec, const Box& region, const PowerLaw& law,
+                   unsigned threads, const Wanted& wanted, std::vector<Crater>& result) {
     const double marginRadii = spec.margin_radii;
     auto margin = [&](double d) { return 0.5 * marginRadii * d; };
     struct Row {
@@ -433,7 +472,13 @@ std::vector<Crater> generate(const tg_crater_population& spec, const Box& region
                                region.expanded(margin(band.high))});
         }
     }
-    std::vector<std::vector<Crater>> drawn(rows.size());
+    // The calling thread's lists, named by reference: inside the loop body, run on other
+    // threads, the thread_local's own name would be theirs.
+    static thread_local std::vector<std::vector<Crater>> keptRows;
+    std::vector<std::vector<Crater>>& drawn = keptRows;
+    if (drawn.size() < rows.size()) {
+        drawn.resize(rows.size());
+    }
     parallel_for(rows.size(), threads, [&](size_t q) {
         const Row& row = rows[q];
         const Band& band = row.band;
@@ -441,42 +486,45 @@ std::vector<Crater> generate(const tg_crater_population& spec, const Box& region
         const Box& inner = row.inner;
         const Box& outer = row.outer;
         std::vector<Crater>& out = drawn[q];
-        {
-            for (int32_t i = row.iMin; i <= row.iMax; ++i) {
-                std::vector<Crater> list = cell_craters(band, i, j, law, spec.lifetime_gyr,
-                                                        spec.seed);
-                // CellCraters::Rows(outer y range): the draw order, filtered by y.
-                for (const Crater& c : list) {
-                    if (!(c.y >= outer.minY && c.y <= outer.maxY)) {
-                        continue;
-                    }
-                    const bool inBand = c.diameter >= band.low && c.diameter <= band.high;
-                    if (inBand && !outer.contains(c.x, c.y)) {
-                        continue;
-                    }
-                    bool keep;
-                    if (!inBand) {
-                        keep = region.expanded(margin(c.diameter)).contains(c.x, c.y);
-                    } else {
-                        keep = inner.contains(c.x, c.y) ||
-                               region.expanded(margin(c.diameter)).contains(c.x, c.y);
-                    }
-                    if (keep) {
-                        out.push_back(c);
-                    }
+        out.clear();
+        for (int32_t i = row.iMin; i <= row.iMax; ++i) {
+            // CellCraters::Rows(outer y range): the draw order, filtered by y.
+            each_cell_crater(band, i, j, law, spec.lifetime_gyr, spec.seed, [&](const Crater& c) {
+                if (!(c.y >= outer.minY && c.y <= outer.maxY)) {
+                    return;
                 }
-            }
+                const bool inBand = c.diameter >= band.low && c.diameter <= band.high;
+                if (inBand && !outer.contains(c.x, c.y)) {
+                    return;
+                }
+                bool keep;
+                if (!inBand) {
+                    keep = region.expanded(margin(c.diameter)).contains(c.x, c.y);
+                } else {
+                    keep = inner.contains(c.x, c.y) ||
+                           region.expanded(margin(c.diameter)).contains(c.x, c.y);
+                }
+                if (keep && wanted(c)) {
+                    out.push_back(c);
+                }
+            });
         }
     });
-    size_t total = 0;
-    for (const std::vector<Crater>& d : drawn) {
-        total += d.size();
+    // Rows joined in order: each row's craters copied to its offset on the host threads.
+    std::vector<size_t> base(rows.size() + 1, 0);
+    for (size_t q = 0; q < rows.size(); ++q) {
+        base[q + 1] = base[q] + drawn[q].size();
     }
+    result.resize(base.back());
+    parallel_for(rows.size(), threads, [&](size_t q) {
+        std::copy(drawn[q].begin(), drawn[q].end(), result.begin() + base[q]);
+    });
+}
+
+std::vector<Crater> generate(const tg_crater_population& spec, const Box& region,
+                             const PowerLaw& law, unsigned threads = 1) {
     std::vector<Crater> out;
-    out.reserve(total);
-    for (const std::vector<Crater>& d : drawn) {
-        out.insert(out.end(), d.begin(), d.end());
-    }
+    generate_into(spec, region, law, threads, [](const Crater&) { return true; }, out);
     return out;
 }
 
@@ -605,10 +653,55 @@ struct OutlineLaw {
     }
 };
 
-Outline irregular_outline(const Crater& c, uint32_t seed) {
+// The words IrregularOutline draws, at most kOutlineDraws doubles: blocks 0 to 9 of the crater's
+// irregularity stream (counter id low, id high, 0, block), as Stream would hand them out.
+constexpr int kOutlineDraws = 20;
+constexpr int kOutlineBlocks = kOutlineDraws / 2;
+
+// The outline words of `n` craters (ids[i]) at once, words[i * 4 kOutlineBlocks + 4 b + lane].
+void outline_words(const uint64_t* ids, size_t n, uint32_t seed, std::vector<uint32_t>& words) {
+    const size_t lanes = n * kOutlineBlocks;
+    static thread_local std::vector<uint32_t> soa;
+    soa.resize(4 * lanes);
+    uint32_t *x = soa.data(), *y = x + lanes, *z = y + lanes, *w = z + lanes;
+    for (size_t i = 0; i < n; ++i) {
+        for (int b = 0; b < kOutlineBlocks; ++b) {
+            const size_t q = i * kOutlineBlocks + b;
+            x[q] = uint32_t(ids[i]);
+            y[q] = uint32_t(ids[i] >> 32);
+            z[q] = 0u;
+            w[q] = uint32_t(b);
+        }
+    }
+    philox_soa(x, y, z, w, lanes, seed, kCraterIrregularityStream);
+    words.resize(4 * lanes);
+    for (size_t q = 0; q < lanes; ++q) {
+        words[4 * q] = x[q];
+        words[4 * q + 1] = y[q];
+        words[4 * q + 2] = z[q];
+        words[4 * q + 3] = w[q];
+    }
+}
+
+// Stream::next_double from two consecutive words.
+inline double unit_double(const uint32_t* words) {
+    const uint64_t high = words[0] >> 5u;
+    const uint64_t low = words[1] >> 6u;
+    return double((high << 26u) | low) * 0x1p-53;
+}
+
+// IrregularOutline from the crater's outline words (outline_words).
+Outline irregular_outline(const uint32_t* words) {
     static const OutlineLaw law;
     Outline o;
-    Stream random(seed, kCraterIrregularityStream, uint32_t(c.id), uint32_t(c.id >> 32));
+    struct {
+        const uint32_t* at;
+        double next_double() {
+            const double v = unit_double(at);
+            at += 2;
+            return v;
+        }
+    } random{words};
     double d[9];
     for (double& v : d) {
         v = random.next_double();
@@ -640,16 +733,35 @@ Outline irregular_outline(const Crater& c, uint32_t seed) {
 bool footprint_cells(const tg_grid& grid, double x, double y, double reach) {
     const double det = grid.pixel_width * grid.pixel_height - grid.row_rotation * grid.col_rotation;
     double minX = INFINITY, minY = INFINITY, maxX = -INFINITY, maxY = -INFINITY;
-    for (const double wx : {x - reach, x + reach}) {
-        for (const double wy : {y - reach, y + reach}) {
-            const double dx = wx - grid.origin_x;
-            const double dy = wy - grid.origin_y;
-            const double px = (dx * grid.pixel_height - dy * grid.row_rotation) / det;
-            const double py = (dy * grid.pixel_width - dx * grid.col_rotation) / det;
-            minX = std::fmin(minX, px);
-            minY = std::fmin(minY, py);
-            maxX = std::fmax(maxX, px);
-            maxY = std::fmax(maxY, py);
+    if (grid.row_rotation == 0.0 && grid.col_rotation == 0.0 && grid.pixel_width > 0.0 &&
+        grid.pixel_height < 0.0 && reach >= 0.0) {
+        // Unrotated and north-up: det < 0, the column coordinate rises with x and the row
+        // coordinate falls with y (rounding keeps both monotone), so two corners give the box's
+        // extremes, by the same expressions.
+        const auto px = [&](double wx, double wy) {
+            return ((wx - grid.origin_x) * grid.pixel_height -
+                    (wy - grid.origin_y) * grid.row_rotation) / det;
+        };
+        const auto py = [&](double wx, double wy) {
+            return ((wy - grid.origin_y) * grid.pixel_width -
+                    (wx - grid.origin_x) * grid.col_rotation) / det;
+        };
+        minX = px(x - reach, y - reach);
+        maxX = px(x + reach, y - reach);
+        minY = py(x - reach, y + reach);
+        maxY = py(x - reach, y - reach);
+    } else {
+        for (const double wx : {x - reach, x + reach}) {
+            for (const double wy : {y - reach, y + reach}) {
+                const double dx = wx - grid.origin_x;
+                const double dy = wy - grid.origin_y;
+                const double px = (dx * grid.pixel_height - dy * grid.row_rotation) / det;
+                const double py = (dy * grid.pixel_width - dx * grid.col_rotation) / det;
+                minX = std::fmin(minX, px);
+                minY = std::fmin(minY, py);
+                maxX = std::fmax(maxX, px);
+                maxY = std::fmax(maxY, py);
+            }
         }
     }
     const double w = grid.width, h = grid.height;
@@ -1135,6 +1247,14 @@ struct RecordBlock {
     std::vector<double> foot;
 };
 
+// A batch builder's working arrays, kept per calling thread so that repeated batches reuse
+// their memory: the drawn craters, the apply order's buckets and the record blocks.
+struct BatchWork {
+    std::vector<Crater> craters;
+    std::vector<uint32_t> bucket, sorted, moved, slots;
+    std::vector<RecordBlock> blocks;
+};
+
 }  // namespace host
 }  // namespace tgb
 
@@ -1261,38 +1381,51 @@ int tg_boulder_generate(const tg_boulder_population* spec, const double* region,
     const PowerLaw candidates{b.sfd_coefficient, b.sfd_exponent, 1.0};
     const std::vector<Crater> drawn =
         generate(p, Box{region[0], region[1], region[2], region[3]}, candidates, host_threads());
+    // Each part of 4096 candidates thinned on the host threads; the kept joined in order.
+    constexpr size_t kPart = 4096;
+    const size_t parts = (drawn.size() + kPart - 1) / kPart;
+    std::vector<std::vector<tg_boulder>> kept(parts);
+    parallel_for(parts, host_threads(), [&](size_t part) {
+        const size_t end = std::min(drawn.size(), (part + 1) * kPart);
+        for (size_t q = part * kPart; q < end; ++q) {
+            const Crater& c = drawn[q];
+            const uint32_t low = uint32_t(c.id), high = uint32_t(c.id >> 32);
+            // Thin (boulder_layer.cpp:345-358): kept when a draw falls below the background density
+            // over the candidates' (1 here: the background abundance is 1 everywhere).
+            Stream keep(b.seed, kBoulderAttributeStream, low, high, 0u /* Keep */);
+            const double density = 1.0 * sizes.incremental(c.diameter);
+            if (keep.next_double() >= density / candidates.incremental(c.diameter)) {
+                continue;
+            }
+            // DrawPose and Wear (boulder_pose.cpp:28-77): height ratio, then wear (its own stream),
+            // then the buried share, each uniform between its bounds.
+            Stream pose(b.seed, kBoulderAttributeStream, low, high, 1u /* Pose */);
+            const double ratio =
+                b.min_height_ratio + (b.max_height_ratio - b.min_height_ratio) * pose.next_double();
+            Stream wear(b.seed, kBoulderAttributeStream, low, high, 2u /* Wear */);
+            wear.next_double();
+            wear.next_double();
+            const double share = pose.next_double();
+            const double burial = b.min_burial + (b.max_burial - b.min_burial) * share;
+            const double height = ratio * c.diameter;
+            // Drawn into the heights when its resolution weight is positive (boulder_relief.cpp:
+            // 298-302, the default relief range holding every boulder that is not a model).
+            const double weight = resolution_weight(c.diameter, spacing, b.fade_start_samples,
+                                                    b.fade_end_samples);
+            if (!(weight > 0.0)) {
+                continue;
+            }
+            kept[part].push_back(tg_boulder{c.x, c.y, c.diameter, height * (1.0 - burial), weight});
+        }
+    });
     size_t n = 0;
-    for (const Crater& c : drawn) {
-        const uint32_t low = uint32_t(c.id), high = uint32_t(c.id >> 32);
-        // Thin (boulder_layer.cpp:345-358): kept when a draw falls below the background density
-        // over the candidates' (1 here: the background abundance is 1 everywhere).
-        Stream keep(b.seed, kBoulderAttributeStream, low, high, 0u /* Keep */);
-        const double density = 1.0 * sizes.incremental(c.diameter);
-        if (keep.next_double() >= density / candidates.incremental(c.diameter)) {
-            continue;
+    for (const std::vector<tg_boulder>& list : kept) {
+        for (const tg_boulder& stone : list) {
+            if (out != nullptr && n < capacity) {
+                out[n] = stone;
+            }
+            ++n;
         }
-        // DrawPose and Wear (boulder_pose.cpp:28-77): height ratio, then wear (its own stream),
-        // then the buried share, each uniform between its bounds.
-        Stream pose(b.seed, kBoulderAttributeStream, low, high, 1u /* Pose */);
-        const double ratio =
-            b.min_height_ratio + (b.max_height_ratio - b.min_height_ratio) * pose.next_double();
-        Stream wear(b.seed, kBoulderAttributeStream, low, high, 2u /* Wear */);
-        wear.next_double();
-        wear.next_double();
-        const double share = pose.next_double();
-        const double burial = b.min_burial + (b.max_burial - b.min_burial) * share;
-        const double height = ratio * c.diameter;
-        // Drawn into the heights when its resolution weight is positive (boulder_relief.cpp:
-        // 298-302, the default relief range holding every boulder that is not a model).
-        const double weight = resolution_weight(c.diameter, spacing, b.fade_start_samples,
-                                                b.fade_end_samples);
-        if (!(weight > 0.0)) {
-            continue;
-        }
-        if (out != nullptr && n < capacity) {
-            out[n] = tg_boulder{c.x, c.y, c.diameter, height * (1.0 - burial), weight};
-        }
-        ++n;
     }
     *count = n;
     return TG_OK;
@@ -1351,66 +1484,109 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     std::vector<RecordBlock> blocks;
     const unsigned threads = host_threads();
     static thread_local BatchCache cache;
+    // The calling thread's working arrays, kept from call to call (named by reference: the loop
+    // bodies run on other threads).
+    static thread_local BatchWork workspace;
+    BatchWork& work = workspace;
     if (!cache.take(*spec, *shaping, *grid, blocks)) {
-        std::vector<Crater> craters =
-            generate(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads);
-
         // The craters that can give a record: a resolution weight above 0 and a footprint, grown
         // to the largest outline scale any crater can draw (MaxOutlineScale, irregularity.cpp:
         // 279, the bound the reference's own binning takes), that holds a cell of the grid. The
-        // rest (most of the candidates the margins bring in) are neither ordered nor built; the
-        // records are unchanged, as every crater left out would be dropped by its exact
-        // footprint below.
+        // rest (most of the candidates the margins bring in) are dropped as they are drawn,
+        // neither ordered nor built; the records are unchanged, as every crater left out would
+        // be dropped by its exact footprint below, and the draw order of those kept stays theirs.
         const double growth = max_outline_scale(irregular) * (1.0 + 1e-9);
-        std::vector<uint8_t> candidate(craters.size());
-        parallel_for((craters.size() + 4095) / 4096, threads, [&](size_t part) {
-            const size_t end = std::min(craters.size(), (part + 1) * 4096);
-            for (size_t i = part * 4096; i < end; ++i) {
-                const Crater& c = craters[i];
-                candidate[i] = resolution_weight(c.diameter, spacing) != 0.0 &&
-                               footprint_cells(*grid, c.x, c.y,
-                                               growth * reachRadii * (0.5 * c.diameter));
-            }
-        });
-        // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
-        // descending, id, draw index. The candidates are spread over one bucket each on average by
-        // age (floor((oldest - age) * scale): monotone in the age, so every bucket precedes the
-        // next in the order and equal ages share one), then each bucket is sorted by the whole
-        // comparison on the host threads. The order is total, so it is the one the comparison
-        // defines, whatever the ages' spread.
+        std::vector<Crater>& craters = work.craters;
+        generate_into(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads,
+                      [&](const Crater& c) {
+                          return resolution_weight(c.diameter, spacing) != 0.0 &&
+                                 footprint_cells(*grid, c.x, c.y,
+                                                 growth * reachRadii * (0.5 * c.diameter));
+                      },
+                      craters);
         if (craters.size() >= (size_t(1) << 32)) {
             return TG_ERROR_UNSUPPORTED;
         }
-        std::vector<uint32_t> kept;
-        kept.reserve(craters.size());
-        double oldest = -INFINITY, youngest = INFINITY;
-        for (size_t n = 0; n < craters.size(); ++n) {
-            if (candidate[n]) {
-                kept.push_back(uint32_t(n));
-                oldest = std::fmax(oldest, craters[n].age);
-                youngest = std::fmin(youngest, craters[n].age);
+        const size_t nKept = craters.size();
+        // The ages' range, by parts of 4096 craters on the host threads.
+        constexpr size_t kPart = 4096;
+        const size_t parts = (nKept + kPart - 1) / kPart;
+        std::vector<double> partOldest(parts, -INFINITY), partYoungest(parts, INFINITY);
+        parallel_for(parts, threads, [&](size_t part) {
+            const size_t end = std::min(nKept, (part + 1) * kPart);
+            double oldest = -INFINITY, youngest = INFINITY;
+            for (size_t i = part * kPart; i < end; ++i) {
+                oldest = std::fmax(oldest, craters[i].age);
+                youngest = std::fmin(youngest, craters[i].age);
             }
+            partOldest[part] = oldest;
+            partYoungest[part] = youngest;
+        });
+        double oldest = -INFINITY, youngest = INFINITY;
+        for (size_t part = 0; part < parts; ++part) {
+            oldest = std::fmax(oldest, partOldest[part]);
+            youngest = std::fmin(youngest, partYoungest[part]);
         }
-        const size_t buckets = std::max<size_t>(kept.size(), 1);
+        // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
+        // descending, id, draw index. The craters are spread over one bucket each on average by
+        // age (floor((oldest - age) * scale): monotone in the age, so every bucket precedes the
+        // next in the order and equal ages share one), put in bucket order by a stable radix
+        // sort (two digits; per part counts, so each part writes its own slots and no thread
+        // waits on another), then each run of one bucket is sorted by the whole comparison on
+        // the host threads. The order is total, so it is the one the comparison defines,
+        // whatever the ages' spread.
+        const size_t buckets = std::max<size_t>(nKept, 1);
         const double spread = oldest - youngest;
         const double scale = spread > 0.0 ? double(buckets) / spread : 0.0;
-        auto bucket_of = [&](uint32_t n) {
-            const double at = std::floor((oldest - craters[n].age) * scale);
-            return size_t(std::clamp(at, 0.0, double(buckets - 1)));
-        };
-        std::vector<uint32_t> start(buckets + 1, 0);
-        for (const uint32_t n : kept) {
-            ++start[bucket_of(n) + 1];
-        }
-        for (size_t q = 0; q < buckets; ++q) {
-            start[q + 1] += start[q];
-        }
-        std::vector<uint32_t> sorted(kept.size());
-        {
-            std::vector<uint32_t> fill(start.begin(), start.end() - 1);
-            for (const uint32_t n : kept) {
-                sorted[fill[bucket_of(n)]++] = n;
+        std::vector<uint32_t>& bucket = work.bucket;
+        std::vector<uint32_t>& sorted = work.sorted;
+        std::vector<uint32_t>& moved = work.moved;
+        bucket.resize(nKept);
+        sorted.resize(nKept);
+        moved.resize(nKept);
+        parallel_for(parts, threads, [&](size_t part) {
+            const size_t end = std::min(nKept, (part + 1) * kPart);
+            for (size_t i = part * kPart; i < end; ++i) {
+                const double at = std::floor((oldest - craters[i].age) * scale);
+                bucket[i] = uint32_t(std::clamp(at, 0.0, double(buckets - 1)));
+                sorted[i] = uint32_t(i);
             }
+        });
+        int bits = 1;
+        while (bits < 32 && (size_t(1) << bits) < buckets) {
+            ++bits;
+        }
+        const int digitBits = (bits + 1) / 2;
+        const size_t radix = size_t(1) << digitBits;
+        std::vector<uint32_t>& slots = work.slots;
+        slots.resize(parts * radix);
+        for (int pass = 0; pass < 2; ++pass) {
+            const int shift = pass * digitBits;
+            const std::vector<uint32_t>& from = pass == 0 ? sorted : moved;
+            std::vector<uint32_t>& to = pass == 0 ? moved : sorted;
+            parallel_for(parts, threads, [&](size_t part) {
+                uint32_t* count = slots.data() + part * radix;
+                std::fill(count, count + radix, 0u);
+                const size_t end = std::min(nKept, (part + 1) * kPart);
+                for (size_t q = part * kPart; q < end; ++q) {
+                    ++count[(bucket[from[q]] >> shift) & (radix - 1)];
+                }
+            });
+            uint32_t running = 0;
+            for (size_t d = 0; d < radix; ++d) {
+                for (size_t part = 0; part < parts; ++part) {
+                    const uint32_t n = slots[part * radix + d];
+                    slots[part * radix + d] = running;
+                    running += n;
+                }
+            }
+            parallel_for(parts, threads, [&](size_t part) {
+                uint32_t* slot = slots.data() + part * radix;
+                const size_t end = std::min(nKept, (part + 1) * kPart);
+                for (size_t q = part * kPart; q < end; ++q) {
+                    to[slot[(bucket[from[q]] >> shift) & (radix - 1)]++] = from[q];
+                }
+            });
         }
         const auto earlier = [&](uint32_t a, uint32_t b) {
             const Crater &ca = craters[a], &cb = craters[b];
@@ -1422,15 +1598,26 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
             }
             return ca.id != cb.id ? ca.id < cb.id : a < b;
         };
-        parallel_for((buckets + 4095) / 4096, threads, [&](size_t part) {
-            const size_t end = std::min(buckets, (part + 1) * 4096);
-            for (size_t q = part * 4096; q < end; ++q) {
-                if (start[q + 1] - start[q] > 1) {
-                    std::sort(sorted.begin() + start[q], sorted.begin() + start[q + 1], earlier);
+        // Runs of one bucket, sorted by the segment of kPart positions each run starts in.
+        const auto same = [&](size_t q) { return bucket[sorted[q]] == bucket[sorted[q - 1]]; };
+        parallel_for(parts, threads, [&](size_t part) {
+            size_t q = part * kPart;
+            const size_t limit = std::min(nKept, (part + 1) * kPart);
+            while (q > 0 && q < limit && same(q)) {
+                ++q;  // this run started in an earlier segment
+            }
+            while (q < limit) {
+                size_t end = q + 1;
+                while (end < nKept && same(end)) {
+                    ++end;
                 }
+                if (end - q > 1) {
+                    std::sort(sorted.begin() + q, sorted.begin() + end, earlier);
+                }
+                q = end;
             }
         });
-        std::vector<size_t> order(sorted.begin(), sorted.end());
+        const std::vector<uint32_t>& order = sorted;
 
         // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
         const uint32_t irregularitySeed = substream_seed(spec->seed, kCraterIrregularityStream);
@@ -1440,7 +1627,7 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         const uint32_t textureSeed = substream_seed(spec->seed, kCraterTextureStream);
         const uint32_t textureKeySeed = substream_seed(textureSeed, kCraterTextureStream);
 
-        auto build = [&](const Crater& c, RecordBlock& block) {
+        auto build = [&](const Crater& c, RecordBlock& block, const uint32_t* words) {
             std::vector<CraterRecord>& out = block.records;
             std::vector<float>& values = block.values;
             std::vector<double>& foot = block.foot;
@@ -1448,7 +1635,7 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
             if (resolution == 0.0) {
                 return;
             }
-            const Outline outline = irregular ? irregular_outline(c, irregularitySeed) : Outline{};
+            const Outline outline = irregular ? irregular_outline(words) : Outline{};
             // CratersOnRaster: the footprint window must hold a cell of the grid.
             double scale = 1.0;
             for (int k = 0; k < outline.harmonics; ++k) {
@@ -1507,11 +1694,26 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         };
         constexpr size_t kBlock = 512;
         const size_t nblocks = (order.size() + kBlock - 1) / kBlock;
+        blocks.swap(work.blocks);  // the blocks' vectors keep their memory from the last batch
         blocks.resize(nblocks);
         parallel_for(nblocks, threads, [&](size_t b) {
-            const size_t end = std::min(order.size(), (b + 1) * kBlock);
-            for (size_t q = b * kBlock; q < end; ++q) {
-                build(craters[order[q]], blocks[b]);
+            const size_t begin = b * kBlock, end = std::min(order.size(), (b + 1) * kBlock);
+            blocks[b].records.clear();
+            blocks[b].values.clear();
+            blocks[b].foot.clear();
+            // The block's outline draws first, all its craters' streams at once (the words in
+            // the running thread's own scratch).
+            static thread_local std::vector<uint32_t> words;
+            if (irregular) {
+                uint64_t ids[kBlock];
+                for (size_t q = begin; q < end; ++q) {
+                    ids[q - begin] = craters[order[q]].id;
+                }
+                outline_words(ids, end - begin, irregularitySeed, words);
+            }
+            for (size_t q = begin; q < end; ++q) {
+                build(craters[order[q]], blocks[b],
+                      irregular ? words.data() + (q - begin) * 4 * kOutlineBlocks : nullptr);
             }
         });
     }
@@ -1604,6 +1806,8 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     }
     if (query) {
         cache.keep(*spec, *shaping, *grid, blocks);
+    } else {
+        work.blocks.swap(blocks);
     }
     return TG_OK;
 }
