@@ -225,8 +225,10 @@ struct PowerLaw {
     }
     double expected(double lo, double hi) const { return 1.0 * (cumulative(lo) - cumulative(hi)); }
     double sample(Stream& random, double lo, double hi) const {
-        const double count = expected(lo, hi);
-        const double top = cumulative(lo);
+        return sample(random, lo, hi, expected(lo, hi), cumulative(lo));
+    }
+    // The same draw with the band's expected count and cumulative(lo) made once by the caller.
+    double sample(Stream& random, double lo, double hi, double count, double top) const {
         const double target = top - random.next_double() * count;
         const double d = weight > 0.0 ? invert(target, lo, hi) : std::pow(target / c, -1.0 / e);
         return std::clamp(d, lo, hi);
@@ -302,10 +304,11 @@ void each_cell_crater(const Band& band, int32_t i, int32_t j, const PowerLaw& la
     Stream geometry(seed, kCraterStream, uint32_t(i), uint32_t(j), k);
     Stream ages(seed, kCraterAgeStream, uint32_t(i), uint32_t(j), k);
     const double perArea = law.expected(band.low, band.high);
+    const double top = law.cumulative(band.low);
     const double area = band.cellSize * band.cellSize;
     const uint64_t count = poisson(geometry, perArea * area);
     for (uint64_t index = 0; index < count; ++index) {
-        const double diameter = law.sample(geometry, band.low, band.high);
+        const double diameter = law.sample(geometry, band.low, band.high, perArea, top);
         const double u = geometry.next_double();
         const double v = geometry.next_double();
         const double x = (i + u) * band.cellSize;
