@@ -1047,7 +1047,8 @@ struct LeanCrater {
     float2 harmonics[kLeanHarmonics];  // (A cos phase, A sin phase)
     uint16_t tileX0, tileX1, tileY0, tileY1;  // the reference tiles its footprint window touches
     float cull;            // no cell beyond this distance (m) can be within its reach
-    uint32_t pad[3];
+    float invRadius;       // 1 / radius
+    uint32_t pad[2];
 };
 static_assert(sizeof(LeanCrater) == 208, "LeanCrater must be a multiple of 16 bytes");
 
@@ -1068,6 +1069,7 @@ __device__ inline LeanCrater lean_crater(const CraterShapeKernel& k, const Crate
     l.yLow = c.yLow;
     l.diameter = c.diameter;
     l.radius = 0.5f * c.diameter;
+    l.invRadius = 1.0f / l.radius;
     l.resolution = c.resolution;
     l.reach = k.reachRadii * l.radius;
     l.freshRim = c.freshRim;
@@ -1146,15 +1148,19 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
                                                    float& shaped) {
     const uint32_t flags = l.flags;
     const float d2 = dx * dx + dy * dy;
-    float distance = sqrtf(d2);
+    // The distance and the direction from one reciprocal square root; the quotients below by
+    // reciprocals made once per crater or by the fast divide. Each is within a few ulp of the
+    // correctly rounded operation, far inside the heights' 1e-3 m tolerance and the cull
+    // radius's 1e-5 relative margin.
+    const float inv = d2 > 0.0f ? rsqrtf(d2) : 0.0f;
+    float distance = d2 * inv;
     if (flags & kLeanOutline) {
         // KernelProfileDistance (craters.h:1028) with the outline's scale. The share is
         // smoothstep(distance / radius), exactly 1 from the rim out.
         const float share =
-            (distance >= l.radius ? 1.0f : outline_share(distance / l.radius)) * l.worn;
+            (distance >= l.radius ? 1.0f : outline_share(distance * l.invRadius)) * l.worn;
         float c1 = 1.0f, s1 = 0.0f;  // the direction; angle 0 at the center, as KernelAngle
         if (distance > 0.0f) {
-            const float inv = rsqrtf(d2);
             c1 = dx * inv;
             s1 = dy * inv;
         }
@@ -1171,7 +1177,7 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
             // w = q e^{i theta}, q = share^(1/2) (1 at full share). The harmonics past `count`
             // are zero, so Horner's rule runs over all kLeanHarmonics slots, unrolled: leading
             // zero terms leave the sum exactly as it is.
-            const float q = share < 1.0f ? sqrtf(share) : 1.0f;
+            const float q = share < 1.0f ? share * rsqrtf(share) : 1.0f;
             const float wr = q * c1, wi = q * s1;
             float pr = l.harmonics[kLeanHarmonics - 1u].x, pi = l.harmonics[kLeanHarmonics - 1u].y;
 #pragma unroll
@@ -1196,7 +1202,7 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
             }
             scale *= 1.0f + pr;
         }
-        distance /= scale;
+        distance = __fdividef(distance, scale);
     }
     shaped = distance;
     reached = distance < l.reach;
@@ -1207,7 +1213,7 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
     const uint32_t kind = flags & 3u;
     if (kind == kLeanComplex) {
         // ComplexProfileHeight (craters.h:479) with its per-crater constants made once.
-        const float x = distance / l.radius;
+        const float x = distance * l.invRadius;
         const float depth = l.currentDepth * l.diameter;
         const float rim = l.currentRim * l.diameter;
         const CraterProfileKernel& p = k.profile;
@@ -1230,7 +1236,7 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
     } else if (kind == 1u) {
         height = mpd_height(distance, l.diameter, l.freshRim, l.currentDepth, l.currentRim);
     } else {
-        height = ft_shape(distance / l.radius, k.profile.rim, l.freshRim, l.currentDepth) *
+        height = ft_shape(distance * l.invRadius, k.profile.rim, l.freshRim, l.currentDepth) *
                  l.diameter;
     }
     return l.resolution * height;
