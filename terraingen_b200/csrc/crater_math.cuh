@@ -9,6 +9,7 @@
 // host libm to a few ulp.
 #pragma once
 
+#include <stddef.h>
 #include <stdint.h>
 
 #include "layouts.h"
@@ -1034,7 +1035,7 @@ constexpr uint32_t kLeanEllipse = 1u << 3;
 constexpr uint32_t kLeanHeavy = 1u << 4;    // the extras pass shapes it whole
 constexpr uint32_t kLeanMassifs = 1u << 5;  // the extras pass adds its massif peak
 
-struct LeanCrater {
+struct __align__(16) LeanCrater {
     float x, xLow, y, yLow;
     float diameter, radius, resolution, reach;        // reach = reachRadii * radius
     float freshRim, currentDepth, currentRim, worn;   // worn = worn_outline_share
@@ -1051,6 +1052,8 @@ struct LeanCrater {
     uint32_t pad[2];
 };
 static_assert(sizeof(LeanCrater) == 208, "LeanCrater must be a multiple of 16 bytes");
+static_assert(offsetof(LeanCrater, harmonics) % 16 == 0 && kLeanHarmonics == 11,
+              "the harmonics are read as five float4 and one float2");
 
 // The lean form of record `c` under kernel `k` (harmonics from `data`), with its footprint's
 // reference-tile box (x0, x1, y0, y1) and cull distance from the binning's count pass.
@@ -1180,10 +1183,16 @@ __device__ __forceinline__ float lean_contribution(const CraterShapeKernel& k,
             const float q = share < 1.0f ? share * rsqrtf(share) : 1.0f;
             const float wr = q * c1, wi = q * s1;
             float pr = l.harmonics[kLeanHarmonics - 1u].x, pi = l.harmonics[kLeanHarmonics - 1u].y;
+            // Harmonics 9 down to 0, two to a 16-byte load.
+            const float4* pairs = reinterpret_cast<const float4*>(l.harmonics);
 #pragma unroll
-            for (int h = int(kLeanHarmonics) - 2; h >= 0; --h) {
-                const float t = pr * wr - pi * wi + l.harmonics[h].x;
-                pi = pr * wi + pi * wr + l.harmonics[h].y;
+            for (int h = 4; h >= 0; --h) {
+                const float4 v = pairs[h];  // harmonics 2h (x, y) and 2h + 1 (z, w)
+                float t = pr * wr - pi * wi + v.z;
+                pi = pr * wi + pi * wr + v.w;
+                pr = t;
+                t = pr * wr - pi * wi + v.x;
+                pi = pr * wi + pi * wr + v.y;
                 pr = t;
             }
             // times w^first

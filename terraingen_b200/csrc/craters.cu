@@ -664,8 +664,9 @@ __global__ void __launch_bounds__(kShapeThreads, 4)
             const uint32_t cell = code & 127u;
             const float2 cx = columns[warp][cell & 31u];
             const float2 cy = rows[warp][cell >> 5];
-            const float dy = crater::split_difference(cy.x, cy.y, l.y, l.yLow);
-            const float dx = crater::split_difference(cx.x, cx.y, l.x, l.xLow);
+            const float4 center = *reinterpret_cast<const float4*>(&l.x);  // x, xLow, y, yLow
+            const float dy = crater::split_difference(cy.x, cy.y, center.z, center.w);
+            const float dx = crater::split_difference(cx.x, cx.y, center.x, center.y);
             bool reached;
             float shaped;
             const float v = crater::lean_contribution(k, lk, l, dx, dy, reached, shaped);
