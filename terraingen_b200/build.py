@@ -43,6 +43,7 @@ UNITS = {
     "geotiff.cu": [],
     "population.cpp": [],
     "population_gpu.cu": ["-fmad=false"],
+    "crater_records.cu": ["-fmad=false"],
 }
 
 # Host units are compiled by the host compiler with the reference's floating-point flags, so

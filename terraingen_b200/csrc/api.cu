@@ -252,6 +252,9 @@ void tg_close(tg_device* d) {
     if (d->pinnedStatus != nullptr) {
         cudaFreeHost(d->pinnedStatus);
     }
+    if (d->recordStage != nullptr) {
+        cudaFreeHost(d->recordStage);
+    }
     if (d->copyStream != nullptr) {
         cudaStreamSynchronize(d->copyStream);
         cudaStreamDestroy(d->copyStream);

@@ -91,6 +91,8 @@ enum Slot {
     kPairStart,
     kExtrasMark,
     kExtrasList,
+    kRecordCraters,  // the device record builder's plan: craters, then extras
+    kRecordCounts,   // its records and floats per crater, then their scans
     kSlotCount
 };
 
@@ -112,6 +114,9 @@ struct tg_device {
     std::string name;
     tgb::api::Buffer slots[tgb::api::kSlotCount];
     uint32_t* pinnedStatus = nullptr;  // 16 host-pinned words read back after the layers
+    // The device record builder's page-locked staging (tg_crater_batch_device).
+    void* recordStage = nullptr;
+    size_t recordStageBytes = 0;
     // (cell, crater) and (cell, boulder) pairs evaluated by the last shaping and bake.
     unsigned long long craterPairs = 0, boulderPairs = 0;
     // Polls of a staged copy before the binned kernels give up on it (tg_set_wait_limit).

@@ -28,6 +28,7 @@
 
 #include "../../include/tgb200.h"
 #include "layouts.h"
+#include "crater_records.h"
 #include "population_plan.h"
 
 namespace tgb {
@@ -1258,6 +1259,343 @@ struct BatchWork {
     std::vector<RecordBlock> blocks;
 };
 
+// A batch's settings from the caller's population, shaping and grid: the layer profile, the
+// terrace and peak options, the spacing, the grid's bounds and the population with the layer's
+// candidate margins.
+struct BatchSetup {
+    LayerProfile profile;
+    TerraceOptions terraces;
+    PeakOptions peaks;
+    double spacing = 0.0;
+    Box bounds{};
+    tg_crater_population p{};
+    bool irregular = false;
+    double reachRadii = 0.0;
+};
+
+int batch_setup(const tg_crater_population& spec, const tg_crater_shaping& shaping,
+                const tg_grid& grid, BatchSetup& out) {
+    if (grid.row_rotation != 0.0 || grid.col_rotation != 0.0 || !(grid.pixel_width > 0.0) ||
+        !(grid.pixel_height < 0.0)) {
+        return TG_ERROR_UNSUPPORTED;
+    }
+    if (shaping.profile > 3u) {
+        return TG_ERROR_ARGUMENT;
+    }
+    LayerProfile& profile = out.profile;
+    profile.simple = shaping.profile & 1u;
+    profile.complex = shaping.profile >= 2u;
+    if (profile.complex) {
+        // ValidateComplexCraterShape (complex.cpp:19): a positive transition diameter.
+        if (!(shaping.transition_diameter > 0.0) || !std::isfinite(shaping.transition_diameter)) {
+            return TG_ERROR_ARGUMENT;
+        }
+        profile.transition = shaping.transition_diameter;
+        set_complex_shape(profile.kernel, profile.transition);
+    }
+    TerraceOptions& terraces = out.terraces;
+    if (shaping.terrace_onset > 0.0) {
+        // ValidateCraterTerraces (apply_options.cpp:20): full above onset, min freshness in [0, 1).
+        if (!(shaping.terrace_full > shaping.terrace_onset) ||
+            !(shaping.terrace_min_freshness >= 0.0 && shaping.terrace_min_freshness < 1.0)) {
+            return TG_ERROR_ARGUMENT;
+        }
+        terraces.onset = shaping.terrace_onset;
+        terraces.full = shaping.terrace_full;
+        terraces.minFreshness = shaping.terrace_min_freshness;
+    }
+    const double spacing = out.spacing = std::max(grid.pixel_width, -grid.pixel_height);
+    // The grid's bounds (its cell edges), the region CraterLayer::ApplySamples draws over.
+    out.bounds = Box{grid.origin_x, grid.origin_y + grid.height * grid.pixel_height,
+                     grid.origin_x + grid.width * grid.pixel_width, grid.origin_y};
+    tg_crater_population& p = out.p;
+    p = spec;
+    // DefaultCraterApply: irregular outlines, terraces and peaks; plain options: none.
+    const bool irregular = out.irregular = shaping.irregular != 0;
+    const double reachRadii = out.reachRadii = profile.reach();  // FT 1.5 R, MPD 2 R, complex 3 R
+    p.margin_radii = reachRadii * max_outline_scale(irregular);
+    p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
+    return TG_OK;
+}
+
+// The batch's craters in apply order: the population drawn over the grid's bounds, the
+// candidates kept as they are drawn, the order by the ages' buckets (work.craters and, in apply
+// order, their indices work.sorted).
+int batch_order(const BatchSetup& setup, const tg_grid& grid, unsigned threads, BatchWork& work) {
+    // The craters that can give a record: a resolution weight above 0 and a footprint, grown
+    // to the largest outline scale any crater can draw (MaxOutlineScale, irregularity.cpp:
+    // 279, the bound the reference's own binning takes), that holds a cell of the grid. The
+    // rest (most of the candidates the margins bring in) are dropped as they are drawn,
+    // neither ordered nor built; the records are unchanged, as every crater left out would
+    // be dropped by its exact footprint below, and the draw order of those kept stays theirs.
+    const double growth = max_outline_scale(setup.irregular) * (1.0 + 1e-9);
+    const tg_crater_population& p = setup.p;
+    const double spacing = setup.spacing, reachRadii = setup.reachRadii;
+    std::vector<Crater>& craters = work.craters;
+    generate_into(p, setup.bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads,
+                  [&](const Crater& c) {
+                      return resolution_weight(c.diameter, spacing) != 0.0 &&
+                             footprint_cells(grid, c.x, c.y,
+                                             growth * reachRadii * (0.5 * c.diameter));
+                  },
+                  craters);
+    if (craters.size() >= (size_t(1) << 32)) {
+        return TG_ERROR_UNSUPPORTED;
+    }
+    const size_t nKept = craters.size();
+    // The ages' range, by parts of 4096 craters on the host threads.
+    constexpr size_t kPart = 4096;
+    const size_t parts = (nKept + kPart - 1) / kPart;
+    std::vector<double> partOldest(parts, -INFINITY), partYoungest(parts, INFINITY);
+    parallel_for(parts, threads, [&](size_t part) {
+        const size_t end = std::min(nKept, (part + 1) * kPart);
+        double oldest = -INFINITY, youngest = INFINITY;
+        for (size_t i = part * kPart; i < end; ++i) {
+            oldest = std::fmax(oldest, craters[i].age);
+            youngest = std::fmin(youngest, craters[i].age);
+        }
+        partOldest[part] = oldest;
+        partYoungest[part] = youngest;
+    });
+    double oldest = -INFINITY, youngest = INFINITY;
+    for (size_t part = 0; part < parts; ++part) {
+        oldest = std::fmax(oldest, partOldest[part]);
+        youngest = std::fmin(youngest, partYoungest[part]);
+    }
+    // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
+    // descending, id, draw index. The craters are spread over one bucket each on average by
+    // age (floor((oldest - age) * scale): monotone in the age, so every bucket precedes the
+    // next in the order and equal ages share one), put in bucket order by a stable radix
+    // sort (two digits; per part counts, so each part writes its own slots and no thread
+    // waits on another), then each run of one bucket is sorted by the whole comparison on
+    // the host threads. The order is total, so it is the one the comparison defines,
+    // whatever the ages' spread.
+    const size_t buckets = std::max<size_t>(nKept, 1);
+    const double spread = oldest - youngest;
+    const double scale = spread > 0.0 ? double(buckets) / spread : 0.0;
+    std::vector<uint32_t>& bucket = work.bucket;
+    std::vector<uint32_t>& sorted = work.sorted;
+    std::vector<uint32_t>& moved = work.moved;
+    bucket.resize(nKept);
+    sorted.resize(nKept);
+    moved.resize(nKept);
+    parallel_for(parts, threads, [&](size_t part) {
+        const size_t end = std::min(nKept, (part + 1) * kPart);
+        for (size_t i = part * kPart; i < end; ++i) {
+            const double at = std::floor((oldest - craters[i].age) * scale);
+            bucket[i] = uint32_t(std::clamp(at, 0.0, double(buckets - 1)));
+            sorted[i] = uint32_t(i);
+        }
+    });
+    int bits = 1;
+    while (bits < 32 && (size_t(1) << bits) < buckets) {
+        ++bits;
+    }
+    const int digitBits = (bits + 1) / 2;
+    const size_t radix = size_t(1) << digitBits;
+    std::vector<uint32_t>& slots = work.slots;
+    slots.resize(parts * radix);
+    for (int pass = 0; pass < 2; ++pass) {
+        const int shift = pass * digitBits;
+        const std::vector<uint32_t>& from = pass == 0 ? sorted : moved;
+        std::vector<uint32_t>& to = pass == 0 ? moved : sorted;
+        parallel_for(parts, threads, [&](size_t part) {
+            uint32_t* count = slots.data() + part * radix;
+            std::fill(count, count + radix, 0u);
+            const size_t end = std::min(nKept, (part + 1) * kPart);
+            for (size_t q = part * kPart; q < end; ++q) {
+                ++count[(bucket[from[q]] >> shift) & (radix - 1)];
+            }
+        });
+        uint32_t running = 0;
+        for (size_t d = 0; d < radix; ++d) {
+            for (size_t part = 0; part < parts; ++part) {
+                const uint32_t n = slots[part * radix + d];
+                slots[part * radix + d] = running;
+                running += n;
+            }
+        }
+        parallel_for(parts, threads, [&](size_t part) {
+            uint32_t* slot = slots.data() + part * radix;
+            const size_t end = std::min(nKept, (part + 1) * kPart);
+            for (size_t q = part * kPart; q < end; ++q) {
+                to[slot[(bucket[from[q]] >> shift) & (radix - 1)]++] = from[q];
+            }
+        });
+    }
+    const auto earlier = [&](uint32_t a, uint32_t b) {
+        const Crater &ca = craters[a], &cb = craters[b];
+        if (ca.age != cb.age) {
+            return ca.age > cb.age;
+        }
+        if (ca.diameter != cb.diameter) {
+            return ca.diameter > cb.diameter;
+        }
+        return ca.id != cb.id ? ca.id < cb.id : a < b;
+    };
+    // Runs of one bucket, sorted by the segment of kPart positions each run starts in.
+    const auto same = [&](size_t q) { return bucket[sorted[q]] == bucket[sorted[q - 1]]; };
+    parallel_for(parts, threads, [&](size_t part) {
+        size_t q = part * kPart;
+        const size_t limit = std::min(nKept, (part + 1) * kPart);
+        while (q > 0 && q < limit && same(q)) {
+            ++q;  // this run started in an earlier segment
+        }
+        while (q < limit) {
+            size_t end = q + 1;
+            while (end < nKept && same(end)) {
+                ++end;
+            }
+            if (end - q > 1) {
+                std::sort(sorted.begin() + q, sorted.begin() + end, earlier);
+            }
+            q = end;
+        }
+    });
+    return TG_OK;
+}
+
+// The batch's CraterShapeKernel bytes into `kernel`.
+void batch_shape_kernel(const BatchSetup& setup, void* kernel) {
+    // MakeCraterShapeKernel (crater_kernel.cpp:277) for a simple FT or MPD profile and the
+    // default shaping options.
+    CraterShapeKernel k{};
+    k.profile.ejectaExponent = 3.0f;
+    k.profile.complexReachRadii = 3.0f;
+    if (setup.profile.complex) {
+        set_complex_shape(k.profile, setup.profile.transition);
+    }
+    k.profile.simple = setup.profile.simple == 1u ? kProfileMartinParkesDunstan
+                                                  : kProfileFassettThomson;
+    k.profile.tableExtent = 1.5f;
+    k.reachRadii = float(setup.reachRadii);
+    k.profileReachRadii = float(setup.reachRadii);
+    k.blendStart = 0.8f;
+    k.blendEnd = 1.2f;
+    k.blendShape = 2u;
+    k.replaceStart = 1.0f;
+    k.replaceEnd = float(setup.reachRadii);
+    k.ejectaReachRadii = 3.0f;
+    k.rimInner = 0.8f;
+    k.rimOuter = 1.2f;
+    k.rimStrength = 1.0f;
+    k.rimShape = 2u;
+    k.noiseWavelength = 0.5f;
+    k.noiseOctaves = 4;
+    k.noiseGain = 0.5f;
+    k.noiseRimWavelength = 0.1f;
+    k.noiseRimInner = 0.8f;
+    k.noiseRimOuter = 1.2f;
+    k.wallStreakWidth = 0.15f;
+    k.ejectaLineation = 0.15f;
+    k.minFreshness = 0.5f;
+    std::memcpy(kernel, &k, sizeof(k));
+}
+
+int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shaping,
+                const tg_grid& grid, void* kernel, RecordConstants& k,
+                std::vector<RecordCrater>& out, std::vector<float>& extras) {
+    BatchSetup setup;
+    if (int st = batch_setup(spec, shaping, grid, setup)) {
+        return st;
+    }
+    const unsigned threads = host_threads();
+    static thread_local BatchWork workspace;
+    BatchWork& work = workspace;
+    if (int st = batch_order(setup, grid, threads, work)) {
+        return st;
+    }
+    if (kernel != nullptr) {
+        batch_shape_kernel(setup, kernel);
+    }
+    static const OutlineLaw law;
+    k = RecordConstants{};
+    k.originX = grid.origin_x;
+    k.originY = grid.origin_y;
+    k.pixelWidth = grid.pixel_width;
+    k.pixelHeight = grid.pixel_height;
+    k.rowRotation = grid.row_rotation;
+    k.colRotation = grid.col_rotation;
+    k.width = grid.width;
+    k.height = grid.height;
+    k.spacing = setup.spacing;
+    k.reachRadii = setup.reachRadii;
+    k.freshDepth = spec.depth_ratio;
+    k.freshRim = spec.rim_ratio;
+    for (int i = 0; i < 11; ++i) {
+        k.outlinePower[i] = law.power[i];
+    }
+    k.outlineScale = law.scale;
+    k.irregular = setup.irregular ? 1u : 0u;
+    // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
+    k.irregularitySeed = substream_seed(spec.seed, kCraterIrregularityStream);
+    k.noiseSeed = substream_seed(spec.seed, kCraterNoiseStream);
+    k.textureKeySeed = substream_seed(substream_seed(spec.seed, kCraterTextureStream),
+                                      kCraterTextureStream);
+    const uint32_t terraceSeed = substream_seed(spec.seed, kCraterTerraceStream);
+    const uint32_t peakSeed = substream_seed(spec.seed, kCraterPeakStream);
+    const double freshDepth = spec.depth_ratio, freshRim = spec.rim_ratio;
+    const double floorShare = std::fmin(spec.cutoff_depth_ratio / freshDepth, 1.0);
+    const size_t n = work.sorted.size();
+    out.resize(n);
+    // Blocks of 512 craters on the host threads, each with its own extras, joined in order.
+    constexpr size_t kBlock = 512;
+    const size_t nblocks = (n + kBlock - 1) / kBlock;
+    static thread_local std::vector<std::vector<float>> blockExtras;
+    std::vector<std::vector<float>>& blocks = blockExtras;  // the caller's (see generate_into)
+    if (blocks.size() < nblocks) {
+        blocks.resize(nblocks);
+    }
+    parallel_for(nblocks, threads, [&](size_t b) {
+        std::vector<float>& values = blocks[b];
+        values.clear();
+        const size_t end = std::min(n, (b + 1) * kBlock);
+        for (size_t q = b * kBlock; q < end; ++q) {
+            const Crater& c = work.craters[work.sorted[q]];
+            // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
+            const double remaining = std::clamp(1.0 - c.age / spec.lifetime_gyr, 0.0, 1.0);
+            const double erosion = floorShare + (1.0 - floorShare) * remaining;
+            RecordCrater& r = out[q];
+            r = RecordCrater{c.x, c.y, c.diameter, erosion, c.id, uint32_t(values.size()), 0u, 0u,
+                             0u, 0u};
+            if (!setup.irregular) {
+                continue;
+            }
+            // AppendKernelTerraces, then AppendKernelPeaks (crater_kernel.cpp:592-593) into a
+            // scratch record: only their counts matter, the offsets are the device's.
+            CraterRecord scratch{};
+            const size_t start = values.size();
+            append_terraces(setup.terraces, terraceSeed, setup.profile, c.diameter, c.id,
+                            freshDepth, freshRim, erosion * freshDepth, erosion * freshRim,
+                            scratch, values);
+            r.terraceCount = uint16_t(scratch.terraceCount);
+            r.terraceFloats = uint32_t(values.size() - start);
+            if (setup.profile.is_complex(c.diameter)) {
+                append_peaks(setup.peaks, peakSeed, c.id, freshDepth, erosion * freshDepth, scratch,
+                             values);
+                r.peakCount = uint16_t(scratch.peakCount);
+            }
+            r.extraFloats = uint32_t(values.size() - start);
+        }
+    });
+    std::vector<size_t> base(nblocks + 1, 0);
+    for (size_t b = 0; b < nblocks; ++b) {
+        base[b + 1] = base[b] + blocks[b].size();
+    }
+    if (base.back() >= (size_t(1) << 32)) {
+        return TG_ERROR_UNSUPPORTED;
+    }
+    extras.resize(base.back());
+    parallel_for(nblocks, threads, [&](size_t b) {
+        std::copy(blocks[b].begin(), blocks[b].end(), extras.begin() + base[b]);
+        const size_t end = std::min(n, (b + 1) * kBlock);
+        for (size_t q = b * kBlock; q < end; ++q) {
+            out[q].extraOffset += uint32_t(base[b]);
+        }
+    });
+    return TG_OK;
+}
+
 }  // namespace host
 }  // namespace tgb
 
@@ -1442,46 +1780,16 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
         n_data == nullptr) {
         return TG_ERROR_ARGUMENT;
     }
-    if (grid->row_rotation != 0.0 || grid->col_rotation != 0.0 || !(grid->pixel_width > 0.0) ||
-        !(grid->pixel_height < 0.0)) {
-        return TG_ERROR_UNSUPPORTED;
+    BatchSetup setup;
+    if (int st = batch_setup(*spec, *shaping, *grid, setup)) {
+        return st;
     }
-    if (shaping->profile > 3u) {
-        return TG_ERROR_ARGUMENT;
-    }
-    LayerProfile profile;
-    profile.simple = shaping->profile & 1u;
-    profile.complex = shaping->profile >= 2u;
-    if (profile.complex) {
-        // ValidateComplexCraterShape (complex.cpp:19): a positive transition diameter.
-        if (!(shaping->transition_diameter > 0.0) || !std::isfinite(shaping->transition_diameter)) {
-            return TG_ERROR_ARGUMENT;
-        }
-        profile.transition = shaping->transition_diameter;
-        set_complex_shape(profile.kernel, profile.transition);
-    }
-    TerraceOptions terraces;
-    if (shaping->terrace_onset > 0.0) {
-        // ValidateCraterTerraces (apply_options.cpp:20): full above onset, min freshness in [0, 1).
-        if (!(shaping->terrace_full > shaping->terrace_onset) ||
-            !(shaping->terrace_min_freshness >= 0.0 && shaping->terrace_min_freshness < 1.0)) {
-            return TG_ERROR_ARGUMENT;
-        }
-        terraces.onset = shaping->terrace_onset;
-        terraces.full = shaping->terrace_full;
-        terraces.minFreshness = shaping->terrace_min_freshness;
-    }
-    const PeakOptions peaks;
-    const double spacing = std::max(grid->pixel_width, -grid->pixel_height);
-    // The grid's bounds (its cell edges), the region CraterLayer::ApplySamples draws over.
-    const Box bounds{grid->origin_x, grid->origin_y + grid->height * grid->pixel_height,
-                     grid->origin_x + grid->width * grid->pixel_width, grid->origin_y};
-    tg_crater_population p = *spec;
-    // DefaultCraterApply: irregular outlines, terraces and peaks; plain options: none.
-    const bool irregular = shaping->irregular != 0;
-    const double reachRadii = profile.reach();  // FT 1.5 R, MPD 2 R, complex 3 R
-    p.margin_radii = reachRadii * max_outline_scale(irregular);
-    p.min_resolved_diameter = std::fmax(2.0 * spacing, 0.0);
+    const LayerProfile& profile = setup.profile;
+    const TerraceOptions& terraces = setup.terraces;
+    const PeakOptions& peaks = setup.peaks;
+    const double spacing = setup.spacing;
+    const bool irregular = setup.irregular;
+    const double reachRadii = setup.reachRadii;
     // A call that asks only for the sizes keeps what it built, and the next call from the same
     // thread with the same inputs copies that out instead of building it again.
     std::vector<RecordBlock> blocks;
@@ -1492,134 +1800,11 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     static thread_local BatchWork workspace;
     BatchWork& work = workspace;
     if (!cache.take(*spec, *shaping, *grid, blocks)) {
-        // The craters that can give a record: a resolution weight above 0 and a footprint, grown
-        // to the largest outline scale any crater can draw (MaxOutlineScale, irregularity.cpp:
-        // 279, the bound the reference's own binning takes), that holds a cell of the grid. The
-        // rest (most of the candidates the margins bring in) are dropped as they are drawn,
-        // neither ordered nor built; the records are unchanged, as every crater left out would
-        // be dropped by its exact footprint below, and the draw order of those kept stays theirs.
-        const double growth = max_outline_scale(irregular) * (1.0 + 1e-9);
-        std::vector<Crater>& craters = work.craters;
-        generate_into(p, bounds, PowerLaw{p.sfd_coefficient, p.sfd_exponent}, threads,
-                      [&](const Crater& c) {
-                          return resolution_weight(c.diameter, spacing) != 0.0 &&
-                                 footprint_cells(*grid, c.x, c.y,
-                                                 growth * reachRadii * (0.5 * c.diameter));
-                      },
-                      craters);
-        if (craters.size() >= (size_t(1) << 32)) {
-            return TG_ERROR_UNSUPPORTED;
+        if (int st = batch_order(setup, *grid, threads, work)) {
+            return st;
         }
-        const size_t nKept = craters.size();
-        // The ages' range, by parts of 4096 craters on the host threads.
-        constexpr size_t kPart = 4096;
-        const size_t parts = (nKept + kPart - 1) / kPart;
-        std::vector<double> partOldest(parts, -INFINITY), partYoungest(parts, INFINITY);
-        parallel_for(parts, threads, [&](size_t part) {
-            const size_t end = std::min(nKept, (part + 1) * kPart);
-            double oldest = -INFINITY, youngest = INFINITY;
-            for (size_t i = part * kPart; i < end; ++i) {
-                oldest = std::fmax(oldest, craters[i].age);
-                youngest = std::fmin(youngest, craters[i].age);
-            }
-            partOldest[part] = oldest;
-            partYoungest[part] = youngest;
-        });
-        double oldest = -INFINITY, youngest = INFINITY;
-        for (size_t part = 0; part < parts; ++part) {
-            oldest = std::fmax(oldest, partOldest[part]);
-            youngest = std::fmin(youngest, partYoungest[part]);
-        }
-        // CraterApplyOrder, oldest first (apply_options.cpp:96): age descending, then diameter
-        // descending, id, draw index. The craters are spread over one bucket each on average by
-        // age (floor((oldest - age) * scale): monotone in the age, so every bucket precedes the
-        // next in the order and equal ages share one), put in bucket order by a stable radix
-        // sort (two digits; per part counts, so each part writes its own slots and no thread
-        // waits on another), then each run of one bucket is sorted by the whole comparison on
-        // the host threads. The order is total, so it is the one the comparison defines,
-        // whatever the ages' spread.
-        const size_t buckets = std::max<size_t>(nKept, 1);
-        const double spread = oldest - youngest;
-        const double scale = spread > 0.0 ? double(buckets) / spread : 0.0;
-        std::vector<uint32_t>& bucket = work.bucket;
-        std::vector<uint32_t>& sorted = work.sorted;
-        std::vector<uint32_t>& moved = work.moved;
-        bucket.resize(nKept);
-        sorted.resize(nKept);
-        moved.resize(nKept);
-        parallel_for(parts, threads, [&](size_t part) {
-            const size_t end = std::min(nKept, (part + 1) * kPart);
-            for (size_t i = part * kPart; i < end; ++i) {
-                const double at = std::floor((oldest - craters[i].age) * scale);
-                bucket[i] = uint32_t(std::clamp(at, 0.0, double(buckets - 1)));
-                sorted[i] = uint32_t(i);
-            }
-        });
-        int bits = 1;
-        while (bits < 32 && (size_t(1) << bits) < buckets) {
-            ++bits;
-        }
-        const int digitBits = (bits + 1) / 2;
-        const size_t radix = size_t(1) << digitBits;
-        std::vector<uint32_t>& slots = work.slots;
-        slots.resize(parts * radix);
-        for (int pass = 0; pass < 2; ++pass) {
-            const int shift = pass * digitBits;
-            const std::vector<uint32_t>& from = pass == 0 ? sorted : moved;
-            std::vector<uint32_t>& to = pass == 0 ? moved : sorted;
-            parallel_for(parts, threads, [&](size_t part) {
-                uint32_t* count = slots.data() + part * radix;
-                std::fill(count, count + radix, 0u);
-                const size_t end = std::min(nKept, (part + 1) * kPart);
-                for (size_t q = part * kPart; q < end; ++q) {
-                    ++count[(bucket[from[q]] >> shift) & (radix - 1)];
-                }
-            });
-            uint32_t running = 0;
-            for (size_t d = 0; d < radix; ++d) {
-                for (size_t part = 0; part < parts; ++part) {
-                    const uint32_t n = slots[part * radix + d];
-                    slots[part * radix + d] = running;
-                    running += n;
-                }
-            }
-            parallel_for(parts, threads, [&](size_t part) {
-                uint32_t* slot = slots.data() + part * radix;
-                const size_t end = std::min(nKept, (part + 1) * kPart);
-                for (size_t q = part * kPart; q < end; ++q) {
-                    to[slot[(bucket[from[q]] >> shift) & (radix - 1)]++] = from[q];
-                }
-            });
-        }
-        const auto earlier = [&](uint32_t a, uint32_t b) {
-            const Crater &ca = craters[a], &cb = craters[b];
-            if (ca.age != cb.age) {
-                return ca.age > cb.age;
-            }
-            if (ca.diameter != cb.diameter) {
-                return ca.diameter > cb.diameter;
-            }
-            return ca.id != cb.id ? ca.id < cb.id : a < b;
-        };
-        // Runs of one bucket, sorted by the segment of kPart positions each run starts in.
-        const auto same = [&](size_t q) { return bucket[sorted[q]] == bucket[sorted[q - 1]]; };
-        parallel_for(parts, threads, [&](size_t part) {
-            size_t q = part * kPart;
-            const size_t limit = std::min(nKept, (part + 1) * kPart);
-            while (q > 0 && q < limit && same(q)) {
-                ++q;  // this run started in an earlier segment
-            }
-            while (q < limit) {
-                size_t end = q + 1;
-                while (end < nKept && same(end)) {
-                    ++end;
-                }
-                if (end - q > 1) {
-                    std::sort(sorted.begin() + q, sorted.begin() + end, earlier);
-                }
-                q = end;
-            }
-        });
+        const std::vector<Crater>& craters = work.craters;
+        const std::vector<uint32_t>& sorted = work.sorted;
         const std::vector<uint32_t>& order = sorted;
 
         // SeededCraterApply (apply_options.cpp:57): every per-crater stream follows the layer seed.
@@ -1733,39 +1918,7 @@ int tg_crater_batch(const tg_crater_population* spec, const tg_crater_shaping* s
     *n_records = nRecords;
     *n_data = nValues;
     if (kernel != nullptr) {
-        // MakeCraterShapeKernel (crater_kernel.cpp:277) for a simple FT or MPD profile and the
-        // default shaping options.
-        CraterShapeKernel k{};
-        k.profile.ejectaExponent = 3.0f;
-        k.profile.complexReachRadii = 3.0f;
-        if (profile.complex) {
-            set_complex_shape(k.profile, profile.transition);
-        }
-        k.profile.simple = profile.simple == 1u ? kProfileMartinParkesDunstan
-                                                : kProfileFassettThomson;
-        k.profile.tableExtent = 1.5f;
-        k.reachRadii = float(reachRadii);
-        k.profileReachRadii = float(reachRadii);
-        k.blendStart = 0.8f;
-        k.blendEnd = 1.2f;
-        k.blendShape = 2u;
-        k.replaceStart = 1.0f;
-        k.replaceEnd = float(reachRadii);
-        k.ejectaReachRadii = 3.0f;
-        k.rimInner = 0.8f;
-        k.rimOuter = 1.2f;
-        k.rimStrength = 1.0f;
-        k.rimShape = 2u;
-        k.noiseWavelength = 0.5f;
-        k.noiseOctaves = 4;
-        k.noiseGain = 0.5f;
-        k.noiseRimWavelength = 0.1f;
-        k.noiseRimInner = 0.8f;
-        k.noiseRimOuter = 1.2f;
-        k.wallStreakWidth = 0.15f;
-        k.ejectaLineation = 0.15f;
-        k.minFreshness = 0.5f;
-        std::memcpy(kernel, &k, sizeof(k));
+        batch_shape_kernel(setup, kernel);
     }
     if (records != nullptr && record_capacity < nRecords) {
         return TG_ERROR_ARGUMENT;

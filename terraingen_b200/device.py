@@ -490,6 +490,32 @@ class Device:
                                            _stream(b.memory)))
         return heights
 
+    def crater_batch(self, population, shaping, grid: GridSpec, records=None, data=None,
+                     footprints=None):
+        """The crater layer's batch for `grid` with its records made on the device
+        (tg_crater_batch_device): `records` a uint8 device tensor of 144-byte records, `data`
+        float32 and `footprints` float64 device tensors, or all None for the sizes only. Returns
+        (kernel, records, floats): the CraterShapeKernel bytes and the batch's sizes."""
+        import torch
+
+        kernel = np.zeros((), CRATER_SHAPE_KERNEL)
+        ptrs, caps = [], []
+        for t, unit in ((records, CRATER_RECORD.itemsize), (data, 1), (footprints, 3)):
+            if t is not None and not (_is_torch(t) and t.is_cuda and t.is_contiguous()):
+                raise ValueError("outputs must be contiguous device tensors")
+            ptrs.append(C.c_void_p(t.data_ptr()) if t is not None else None)
+            caps.append(t.numel() // unit if t is not None else 0)
+        capacity = min([c for c, t in zip((caps[0], caps[2]), (records, footprints))
+                        if t is not None], default=0)
+        g = grid.native()
+        nr, nd = C.c_size_t(), C.c_size_t()
+        handle = torch.cuda.current_stream().cuda_stream
+        N.check(self._lib.tg_crater_batch_device(
+            self._handle, C.byref(population), C.byref(shaping), C.byref(g), kernel.ctypes.data,
+            ptrs[0], capacity, ptrs[1], caps[1], ptrs[2], C.byref(nr), C.byref(nd),
+            C.c_void_p(handle if handle != 0 else _CUDA_STREAM_LEGACY)))
+        return kernel, nr.value, nd.value
+
     def craters_apply_lists(self, kernel, records, data, heads, entries, xs, x_lows, ys, y_lows,
                             heights, first_row=0, nodata=(0, 0.0)):
         """The drop-in strip form (craters.slang via ShapeTilesOnGpu, apply.cpp:174-196)."""
