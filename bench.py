@@ -720,11 +720,85 @@ def dem_accuracy(dev):
 def e2e_leg(dev, w, args, world, device_heights):
     """The e2e leg (see main). Returns the line's `e2e` object plus "_same": whether the last
     step's heights are the device-resident path's bits (`device_heights`)."""
-    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from terraingen_b200 import Device
+    from terraingen_b200.workloads import DeviceTerrainPrep
+
+    prep_thread = ThreadPoolExecutor(max_workers=1)
+
+    # Record building on a second handle of the same GPU (its own stream and scratch), so the
+    # next step's batch is made while this step evaluates.
+    builder = Device(0)
+    side, main = torch.cuda.Stream(), torch.cuda.Stream()
+    preps = [DeviceTerrainPrep(w.grid, builder, side), DeviceTerrainPrep(w.grid, builder, side)]
+    heights = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32, device="cuda")
+    h_heights = torch.empty((w.grid.height, w.grid.width), dtype=torch.float32).pin_memory()
+    prep_ms, eval_ms = [], []
+
+    def build(q):
+        t = time.perf_counter()
+        out = preps[q].run()
+        prep_ms.append((time.perf_counter() - t) * 1e3)
+        return out
+
+    def run(steps):
+        # One long-lived preparing thread (the library keeps its working arrays per thread).
+        ahead = prep_thread.submit(build, 0)
+        for i in range(steps):
+            inputs = ahead.result()
+            if i + 1 < steps:
+                ahead = prep_thread.submit(build, (i + 1) % 2)
+            kernel, rec, data, foot, stones = inputs
+            t = time.perf_counter()
+            with torch.cuda.stream(main):
+                dev.evaluate(w.grid, heights, fractals=w.fractals, elevation=w.elevation,
+                             craters=(kernel, rec, data, foot), boulders=stones,
+                             boulder_width=w.boulder_width)
+                h_heights.copy_(heights, non_blocking=True)
+            main.synchronize()
+            eval_ms.append((time.perf_counter() - t) * 1e3)
+        ahead.result()
+
+    try:
+        run(args.warmup)
+        prep_ms.clear()
+        eval_ms.clear()
+        barrier(world)
+        t0 = time.perf_counter()
+        run(args.steps)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    finally:
+        prep_thread.shutdown()
+        builder.close()
+    h2d = preps[0].staged_bytes + w.fractals.nbytes + 188  # + the CraterShapeKernel
+    return {"value": round(world * w.cells * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(w.cells * 4),
+            "includes": "every step: crater population, apply order, wall terraces and massif "
+                        f"peaks on {os.cpu_count()} host threads, then the records, their data and "
+                        "footprints made on the device (tg_crater_batch_device, its plan copied "
+                        "in from page-locked memory), boulder placement (tg_boulder_generate) "
+                        "on the host and copied in, tg_evaluate on the device and the heights "
+                        "copied out to page-locked memory; the next step's batch is made while "
+                        "this step evaluates",
+            "host_prep_ms": round(float(np.median(prep_ms)), 3),
+            "evaluate_ms": round(float(np.median(eval_ms)), 3),
+            "_same": bool(np.array_equal(h_heights.numpy().view(np.uint32),
+                                         device_heights.cpu().numpy().view(np.uint32)))}
+
+
+def e2e_host_records_leg(dev, w, args, world, device_heights):
+    """The e2e leg with the crater records made on the host (tg_crater_batch) and every layer
+    input passed to tg_evaluate as host buffers; reported beside the e2e line for comparison."""
+    from concurrent.futures import ThreadPoolExecutor
 
     import torch
 
     from terraingen_b200.workloads import TerrainPrep
+
+    prep_thread = ThreadPoolExecutor(max_workers=1)
 
     def pinned(n, dtype):
         return torch.empty(n * np.dtype(dtype).itemsize, dtype=torch.uint8).pin_memory() \
@@ -742,27 +816,19 @@ def e2e_leg(dev, w, args, world, device_heights):
         return out
 
     def run(steps):
-        ready = [None]
-        worker = None
-
-        def ahead(q):
-            ready[0] = build(q)
-
-        ready[0] = build(0)
+        # One long-lived preparing thread (the library keeps its working arrays per thread).
+        ahead = prep_thread.submit(build, 0)
         for i in range(steps):
-            inputs = ready[0]
+            inputs = ahead.result()
             if i + 1 < steps:
-                worker = threading.Thread(target=ahead, args=((i + 1) % 2,))
-                worker.start()
+                ahead = prep_thread.submit(build, (i + 1) % 2)
             kernel, rec, data, foot, stones = inputs
             t = time.perf_counter()
             dev.evaluate(w.grid, h_out, fractals=w.fractals, elevation=w.elevation,
                          craters=(kernel, rec, data, foot), boulders=stones,
                          boulder_width=w.boulder_width)
             eval_ms.append((time.perf_counter() - t) * 1e3)
-            if worker is not None:
-                worker.join()
-                worker = None
+        ahead.result()
 
     run(args.warmup)
     prep_ms.clear()
@@ -771,6 +837,7 @@ def e2e_leg(dev, w, args, world, device_heights):
     t0 = time.perf_counter()
     run(args.steps)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    prep_thread.shutdown()
     nr, nd, nb = preps[0].counts
     h2d = nr * (144 + 24) + nd * 4 + nb * 40
     return {"value": round(world * w.cells * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
@@ -917,12 +984,17 @@ def main():
     value = world * w.cells * args.steps / total_s / 1e6
 
     # End to end through the public C ABI from the layers' definitions: every step builds the
-    # crater batch (population, apply order, records) and places the boulders on the host threads
-    # (TerrainPrep: tg_crater_batch, tg_boulder_generate, into pinned buffers), then evaluates
-    # with host buffers (tg_evaluate: inputs copied in, heights copied out). The next step's host
-    # work runs on a second thread while this step evaluates, two sets of buffers in turn.
+    # crater batch (population, apply order, terraces and peaks on the host threads, the records
+    # on the device: tg_crater_batch_device) and places the boulders (tg_boulder_generate), then
+    # evaluates (tg_evaluate) and copies the heights out. The next step's batch is made on a
+    # second thread while this step evaluates, two sets of buffers in turn. The same with the
+    # records made on the host and every input passed as host buffers follows for comparison.
     e2e = e2e_leg(dev, w, args, world, heights)
     same = e2e.pop("_same")
+    host_records = e2e_host_records_leg(dev, w, args, world, heights)
+    same = same and host_records.pop("_same")
+    e2e["host_records"] = {k: host_records[k] for k in ("value", "host_prep_ms", "evaluate_ms",
+                                                         "h2d_bytes_per_step")}
     e2e_value = e2e["value"]
     # The timed tile's center 257^2 window against the FP64 oracle (rank 0's tile is centered
     # on the origin, as the fixture's window is).

@@ -515,7 +515,9 @@ int tg_crater_batch(const tg_crater_population* population, const tg_crater_shap
  * footprint and writes its record, data floats and footprint; `records`, `data` and `footprints`
  * are device memory (any may be null; all null asks for the sizes), `kernel` host memory. The
  * outputs are tg_crater_batch's byte for byte. Ordered on `stream` (the device's own when null);
- * the call synchronizes it once, to read the sizes. Replaces the same host work as tg_crater_batch
+ * the call synchronizes it once, to read the sizes; `staged_bytes` (may be null) receives the bytes
+ * it copied to the device (56 per crater of the apply order, 4 per terrace or peak float). Replaces
+ * the same host work as tg_crater_batch
  * (MakeCraterKernelBatch, src/layers/craters/shaping/crater_kernel.cpp:187-622, after
  * PrepareCraters, src/layers/craters/shaping/prepared.cpp:60). TG_ERROR_ARGUMENT, the sizes set,
  * when a capacity is below them (no output written past it). */
@@ -523,7 +525,7 @@ int tg_crater_batch_device(tg_device* device, const tg_crater_population* popula
                            const tg_crater_shaping* shaping, const tg_grid* grid, void* kernel,
                            void* records, size_t record_capacity, float* data,
                            size_t data_capacity, double* footprints, size_t* n_records,
-                           size_t* n_data, void* stream);
+                           size_t* n_data, size_t* staged_bytes, void* stream);
 
 /* --- output -------------------------------------------------------------------------------- */
 

@@ -121,7 +121,8 @@ SIGNATURES.update({
     "tg_crater_batch": [C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid), _P, _P, _SZ,
                         _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ)],
     "tg_crater_batch_device": [_P, C.POINTER(Population), C.POINTER(Shaping), C.POINTER(Grid),
-                               _P, _P, _SZ, _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ), _P],
+                               _P, _P, _SZ, _P, _SZ, _P, C.POINTER(_SZ), C.POINTER(_SZ),
+                               C.POINTER(_SZ), _P],
 })
 
 class Tile(C.Structure):

@@ -284,7 +284,7 @@ int tg_crater_batch_device(tg_device* d, const tg_crater_population* spec,
                            const tg_crater_shaping* shaping, const tg_grid* grid, void* kernel,
                            void* records, size_t record_capacity, float* data,
                            size_t data_capacity, double* footprints, size_t* n_records,
-                           size_t* n_data, void* stream) {
+                           size_t* n_data, size_t* staged_bytes, void* stream) {
     if (int st = check_device(d)) {
         return st;
     }
@@ -292,25 +292,37 @@ int tg_crater_batch_device(tg_device* d, const tg_crater_population* spec,
         n_data == nullptr) {
         return fail(TG_ERROR_ARGUMENT, "population, shaping, grid and counts are required");
     }
-    // The host's part first, outside the device's lock: the population, the apply order, the
-    // terraces and peaks, into this thread's plan.
-    static thread_local std::vector<RecordCrater> craters;
+    // The device is held for the whole call, its host part included: the plan is written
+    // straight into the device's page-locked staging.
+    std::lock_guard<std::mutex> lock(d->mutex);
+    TG_CUDA(cudaSetDevice(d->ordinal), "set device");
+    // The population, the apply order, the terraces and peaks on the host threads; the craters
+    // in apply order into the staging, the extras after them below.
     static thread_local std::vector<float> extras;
     RecordConstants k{};
-    if (int st = host::record_plan(*spec, *shaping, *grid, kernel, k, craters, extras)) {
+    size_t n = 0;
+    int staged = TG_OK;
+    const auto place = [&](size_t count) -> RecordCrater* {
+        staged = stage(d, count * sizeof(RecordCrater) + (size_t(1) << 20));
+        return staged == TG_OK ? static_cast<RecordCrater*>(d->recordStage) : nullptr;
+    };
+    if (int st = host::record_plan(*spec, *shaping, *grid, kernel, k, place, n, extras)) {
+        if (staged != TG_OK) {
+            return staged;
+        }
         return fail(st, st == TG_ERROR_UNSUPPORTED
                             ? "rotated or south-up grids, or more than 2^32 craters or floats"
                             : "population or shaping out of range");
     }
-    const size_t n = craters.size();
     if (n >= 0xffffffffu) {
         return fail(TG_ERROR_UNSUPPORTED, "more than 2^32 - 1 craters");
     }
-    std::lock_guard<std::mutex> lock(d->mutex);
-    TG_CUDA(cudaSetDevice(d->ordinal), "set device");
     const cudaStream_t s = stream != nullptr ? static_cast<cudaStream_t>(stream) : d->stream;
     *n_records = 0;
     *n_data = 1;
+    if (staged_bytes != nullptr) {
+        *staged_bytes = 0;
+    }
     const bool query = records == nullptr && data == nullptr && footprints == nullptr;
     if (n == 0) {
         if (data != nullptr && data_capacity >= 1) {
@@ -321,13 +333,18 @@ int tg_crater_batch_device(tg_device* d, const tg_crater_population* spec,
                    ? fail(TG_ERROR_ARGUMENT, "data capacity below the batch's 1 float")
                    : TG_OK;
     }
-    // The plan crosses once, through the device's page-locked staging.
+    // The plan crosses once, through the device's page-locked staging: the craters are there,
+    // the extras follow them (the staging grown, the craters kept, when they do not fit).
     const size_t craterBytes = n * sizeof(RecordCrater);
     const size_t extraBytes = std::max<size_t>(extras.size(), 1) * sizeof(float);
-    if (int st = stage(d, craterBytes + extraBytes)) {
-        return st;
+    if (craterBytes + extraBytes > d->recordStageBytes) {
+        std::vector<char> keep(static_cast<char*>(d->recordStage),
+                               static_cast<char*>(d->recordStage) + craterBytes);
+        if (int st = stage(d, craterBytes + extraBytes)) {
+            return st;
+        }
+        std::memcpy(d->recordStage, keep.data(), craterBytes);
     }
-    std::memcpy(d->recordStage, craters.data(), craterBytes);
     if (!extras.empty()) {
         std::memcpy(static_cast<char*>(d->recordStage) + craterBytes, extras.data(),
                     extras.size() * sizeof(float));
@@ -344,6 +361,9 @@ int tg_crater_batch_device(tg_device* d, const tg_crater_population* spec,
     TG_CUDA(cudaMemcpyAsync(dCraters, d->recordStage, craterBytes + extraBytes,
                             cudaMemcpyHostToDevice, s),
             "copy");
+    if (staged_bytes != nullptr) {
+        *staged_bytes = craterBytes + extraBytes;
+    }
     const uint32_t blocks = uint32_t((n + 255) / 256);
     record_count_kernel<<<blocks, 256, 0, s>>>(dCraters, uint32_t(n), k, recordAt, dataAt);
     TG_CUDA(cudaGetLastError(), "record count launch");

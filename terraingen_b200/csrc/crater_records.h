@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <vector>
 
 #include "../../include/tgb200.h"
@@ -41,10 +42,13 @@ namespace host {
 // tg_crater_batch up to its records: the population drawn over the grid's bounds, the
 // candidates, the apply order, and for every candidate that carries them its wall terraces and
 // massif peaks (built as tg_crater_batch builds them); `kernel` (when not null) receives the
-// batch's CraterShapeKernel. Returns a TG_* status.
+// batch's CraterShapeKernel. The craters in apply order go where `place(n)` says (room for n,
+// or null to refuse: TG_ERROR_MEMORY), their extras into `extras`. `n` receives their number.
+// Returns a TG_* status.
 int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shaping,
                 const tg_grid& grid, void* kernel, RecordConstants& constants,
-                std::vector<RecordCrater>& craters, std::vector<float>& extras);
+                const std::function<RecordCrater*(size_t)>& place, size_t& n,
+                std::vector<float>& extras);
 
 }  // namespace host
 }  // namespace tgb

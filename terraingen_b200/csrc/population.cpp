@@ -1494,7 +1494,8 @@ void batch_shape_kernel(const BatchSetup& setup, void* kernel) {
 
 int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shaping,
                 const tg_grid& grid, void* kernel, RecordConstants& k,
-                std::vector<RecordCrater>& out, std::vector<float>& extras) {
+                const std::function<RecordCrater*(size_t)>& place, size_t& count,
+                std::vector<float>& extras) {
     BatchSetup setup;
     if (int st = batch_setup(spec, shaping, grid, setup)) {
         return st;
@@ -1537,7 +1538,11 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
     const double freshDepth = spec.depth_ratio, freshRim = spec.rim_ratio;
     const double floorShare = std::fmin(spec.cutoff_depth_ratio / freshDepth, 1.0);
     const size_t n = work.sorted.size();
-    out.resize(n);
+    count = n;
+    RecordCrater* out = place(n);
+    if (out == nullptr && n > 0) {
+        return TG_ERROR_MEMORY;
+    }
     // Blocks of 512 craters on the host threads, each with its own extras, joined in order.
     constexpr size_t kBlock = 512;
     const size_t nblocks = (n + kBlock - 1) / kBlock;
@@ -1551,6 +1556,9 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
         values.clear();
         const size_t end = std::min(n, (b + 1) * kBlock);
         for (size_t q = b * kBlock; q < end; ++q) {
+            if (q + 16 < end) {
+                __builtin_prefetch(&work.craters[work.sorted[q + 16]]);  // apply order gathers
+            }
             const Crater& c = work.craters[work.sorted[q]];
             // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
             const double remaining = std::clamp(1.0 - c.age / spec.lifetime_gyr, 0.0, 1.0);
@@ -1558,7 +1566,9 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
             RecordCrater& r = out[q];
             r = RecordCrater{c.x, c.y, c.diameter, erosion, c.id, uint32_t(values.size()), 0u, 0u,
                              0u, 0u};
-            if (!setup.irregular) {
+            const bool terraced = c.diameter >= setup.terraces.onset;  // else none drawn
+            const bool complex = setup.profile.is_complex(c.diameter);
+            if (!setup.irregular || (!terraced && !complex)) {
                 continue;
             }
             // AppendKernelTerraces, then AppendKernelPeaks (crater_kernel.cpp:592-593) into a
@@ -1570,7 +1580,7 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
                             scratch, values);
             r.terraceCount = uint16_t(scratch.terraceCount);
             r.terraceFloats = uint32_t(values.size() - start);
-            if (setup.profile.is_complex(c.diameter)) {
+            if (complex) {
                 append_peaks(setup.peaks, peakSeed, c.id, freshDepth, erosion * freshDepth, scratch,
                              values);
                 r.peakCount = uint16_t(scratch.peakCount);

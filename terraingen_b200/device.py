@@ -495,7 +495,8 @@ class Device:
         """The crater layer's batch for `grid` with its records made on the device
         (tg_crater_batch_device): `records` a uint8 device tensor of 144-byte records, `data`
         float32 and `footprints` float64 device tensors, or all None for the sizes only. Returns
-        (kernel, records, floats): the CraterShapeKernel bytes and the batch's sizes."""
+        (kernel, records, floats): the CraterShapeKernel bytes and the batch's sizes; the bytes
+        the call copied to the device are then `last_staged_bytes`."""
         import torch
 
         kernel = np.zeros((), CRATER_SHAPE_KERNEL)
@@ -508,12 +509,13 @@ class Device:
         capacity = min([c for c, t in zip((caps[0], caps[2]), (records, footprints))
                         if t is not None], default=0)
         g = grid.native()
-        nr, nd = C.c_size_t(), C.c_size_t()
+        nr, nd, staged = C.c_size_t(), C.c_size_t(), C.c_size_t()
         handle = torch.cuda.current_stream().cuda_stream
         N.check(self._lib.tg_crater_batch_device(
             self._handle, C.byref(population), C.byref(shaping), C.byref(g), kernel.ctypes.data,
             ptrs[0], capacity, ptrs[1], caps[1], ptrs[2], C.byref(nr), C.byref(nd),
-            C.c_void_p(handle if handle != 0 else _CUDA_STREAM_LEGACY)))
+            C.byref(staged), C.c_void_p(handle if handle != 0 else _CUDA_STREAM_LEGACY)))
+        self.last_staged_bytes = staged.value
         return kernel, nr.value, nd.value
 
     def craters_apply_lists(self, kernel, records, data, heads, entries, xs, x_lows, ys, y_lows,

@@ -244,6 +244,71 @@ class TerrainPrep:
                 self.boulders[:5 * nb.value].reshape(-1, 5))
 
 
+class DeviceTerrainPrep:
+    """TerrainPrep with the crater records made on the device (tg_crater_batch_device on
+    `builder`, ordered on `stream`): the crater layer's population, apply order, terraces and
+    peaks on the host threads, its records, data and footprints into device tensors made once;
+    the boulder layer's placement (tg_boulder_generate) into a pinned buffer, then copied to a
+    device tensor on the same stream. Each `run` ends with the stream synchronized, so its
+    outputs are ready for any stream."""
+
+    def __init__(self, grid: GridSpec, builder, stream, seed: int = 7, margin: float = 1.25):
+        import torch
+
+        full_area = (4097 * 0.5) ** 2
+        self.grid = grid
+        self.builder = builder
+        self.stream = stream
+        self.population = crater_population(
+            seed, 200000.0 / (full_area * (1.0 ** -2.0 - 500.0 ** -2.0)), 1.0, 500.0)
+        self.shaping = config2_shaping()
+        self.stones = boulder_population(seed, 1e6 / (full_area * (0.2 ** -2.5 - 3.0 ** -2.5)))
+        half = 0.5 * grid.pixel
+        self.region = np.array([grid.x0 - half, grid.y0 - grid.height * grid.pixel - half,
+                                grid.x0 + grid.width * grid.pixel + half, grid.y0 + half],
+                               np.float64)
+        with torch.cuda.stream(stream):
+            _, nr, nd = builder.crater_batch(self.population, self.shaping, grid)
+        nb = C.c_size_t()
+        N.check(N.library().tg_boulder_generate(C.byref(self.stones), self.region.ctypes.data,
+                                                grid.pixel, None, 0, C.byref(nb)))
+        self.record_capacity = int(nr * margin) + 64
+        self.data_capacity = int(nd * margin) + 64
+        self.boulder_capacity = int(nb.value * margin) + 64
+        cuda = dict(device="cuda")
+        self.records = torch.empty(self.record_capacity * CRATER_RECORD.itemsize,
+                                   dtype=torch.uint8, **cuda)
+        self.data = torch.empty(self.data_capacity, dtype=torch.float32, **cuda)
+        self.footprints = torch.empty(3 * self.record_capacity, dtype=torch.float64, **cuda)
+        self.boulders = torch.empty(5 * self.boulder_capacity, dtype=torch.float64, **cuda)
+        self.host_boulders = torch.empty(5 * self.boulder_capacity,
+                                         dtype=torch.float64).pin_memory()
+        self.counts = (0, 0, 0)
+        self.staged_bytes = 0
+
+    def run(self):
+        """Builds this grid's crater batch and boulders; returns (kernel, records, data,
+        footprints, boulders), the last four device tensors (views of the buffers)."""
+        import torch
+
+        with torch.cuda.stream(self.stream):
+            kernel, nr, nd = self.builder.crater_batch(self.population, self.shaping, self.grid,
+                                                       self.records, self.data, self.footprints)
+            nb = C.c_size_t()
+            N.check(N.library().tg_boulder_generate(
+                C.byref(self.stones), self.region.ctypes.data, self.grid.pixel,
+                self.host_boulders.data_ptr(), self.boulder_capacity, C.byref(nb)))
+            if nb.value > self.boulder_capacity:
+                raise RuntimeError("boulder buffer too small")
+            stones = self.boulders[:5 * nb.value]
+            stones.copy_(self.host_boulders[:5 * nb.value], non_blocking=True)
+        self.stream.synchronize()
+        self.counts = (nr, nd, nb.value)
+        self.staged_bytes = self.builder.last_staged_bytes + 40 * nb.value
+        return (kernel, self.records[:nr * CRATER_RECORD.itemsize], self.data[:nd],
+                self.footprints[:3 * nr], stones)
+
+
 def terrain4097_reference_scene(side: int, pixel: float = 0.5, seed: int = 7):
     """The same terrain as the reference CPU path builds it (oracle harness scene fields)."""
     full_area = (4097 * pixel) ** 2
