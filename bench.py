@@ -49,9 +49,9 @@ NOISE_OPS_PER_CELL_OCTAVE = 180
 # 8, resolution and the add 2: 104, plus the ellipse of 5 % of craters (10): 105.
 CRATER_OPS_PER_PAIR = 105
 # Thread instructions the lean crater kernel executes per pair, measured (ncu smsp__inst_executed
-# x active lanes / pairs, profiles/terrain4097_crater_lean.md): the issue-rate view of the same
-# work (IEEE divisions and square roots, loads, the queue).
-CRATER_THREAD_INST_PER_PAIR = 339
+# x active lanes / pairs: 771.3 M x 29.79 / 64,216,893, profiles/terrain4097_crater_lean.md): the
+# issue-rate view of the same work (loads, the queue, compares and selects).
+CRATER_THREAD_INST_PER_PAIR = 358
 # Counted from terraingen_b200/csrc/boulders.cu per (cell, boulder) pair: window test 6, offset
 # and hypot 12, dome band average (2 sqrt, 2 asin, clamps) 60, max-composite 4; FP64.
 BOULDER_OPS_PER_PAIR = 82
