@@ -728,6 +728,7 @@ def e2e_leg(dev, w, args, world, device_heights):
     from terraingen_b200.workloads import DeviceTerrainPrep
 
     prep_thread = ThreadPoolExecutor(max_workers=1)
+    boulder_thread = ThreadPoolExecutor(max_workers=1)
 
     # Record building on a second handle of the same GPU (its own stream and scratch), so the
     # next step's batch is made while this step evaluates.
@@ -740,7 +741,7 @@ def e2e_leg(dev, w, args, world, device_heights):
 
     def build(q):
         t = time.perf_counter()
-        out = preps[q].run()
+        out = preps[q].run(boulder_thread)
         prep_ms.append((time.perf_counter() - t) * 1e3)
         return out
 
@@ -772,6 +773,7 @@ def e2e_leg(dev, w, args, world, device_heights):
         e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     finally:
         prep_thread.shutdown()
+        boulder_thread.shutdown()
         builder.close()
     h2d = preps[0].staged_bytes + w.fractals.nbytes + 188  # + the CraterShapeKernel
     return {"value": round(world * w.cells * args.steps / e2e_s / 1e6, 3), "unit": UNIT,

@@ -286,25 +286,32 @@ class DeviceTerrainPrep:
         self.counts = (0, 0, 0)
         self.staged_bytes = 0
 
-    def run(self):
+    def _place_boulders(self) -> int:
+        nb = C.c_size_t()
+        N.check(N.library().tg_boulder_generate(
+            C.byref(self.stones), self.region.ctypes.data, self.grid.pixel,
+            self.host_boulders.data_ptr(), self.boulder_capacity, C.byref(nb)))
+        return nb.value
+
+    def run(self, boulder_thread=None):
         """Builds this grid's crater batch and boulders; returns (kernel, records, data,
-        footprints, boulders), the last four device tensors (views of the buffers)."""
+        footprints, boulders), the last four device tensors (views of the buffers). With
+        `boulder_thread` (an executor) the boulders are placed there while the crater batch is
+        made."""
         import torch
 
+        placing = boulder_thread.submit(self._place_boulders) if boulder_thread else None
         with torch.cuda.stream(self.stream):
             kernel, nr, nd = self.builder.crater_batch(self.population, self.shaping, self.grid,
                                                        self.records, self.data, self.footprints)
-            nb = C.c_size_t()
-            N.check(N.library().tg_boulder_generate(
-                C.byref(self.stones), self.region.ctypes.data, self.grid.pixel,
-                self.host_boulders.data_ptr(), self.boulder_capacity, C.byref(nb)))
-            if nb.value > self.boulder_capacity:
+            nb = placing.result() if placing else self._place_boulders()
+            if nb > self.boulder_capacity:
                 raise RuntimeError("boulder buffer too small")
-            stones = self.boulders[:5 * nb.value]
-            stones.copy_(self.host_boulders[:5 * nb.value], non_blocking=True)
+            stones = self.boulders[:5 * nb]
+            stones.copy_(self.host_boulders[:5 * nb], non_blocking=True)
         self.stream.synchronize()
-        self.counts = (nr, nd, nb.value)
-        self.staged_bytes = self.builder.last_staged_bytes + 40 * nb.value
+        self.counts = (nr, nd, nb)
+        self.staged_bytes = self.builder.last_staged_bytes + 40 * nb
         return (kernel, self.records[:nr * CRATER_RECORD.itemsize], self.data[:nd],
                 self.footprints[:3 * nr], stones)
 
