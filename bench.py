@@ -778,10 +778,10 @@ def e2e_leg(dev, w, args, world, device_heights):
     h2d = preps[0].staged_bytes + w.fractals.nbytes + 188  # + the CraterShapeKernel
     return {"value": round(world * w.cells * args.steps / e2e_s / 1e6, 3), "unit": UNIT,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(w.cells * 4),
-            "includes": "every step: crater population, apply order, wall terraces and massif "
-                        f"peaks on {os.cpu_count()} host threads, then the records, their data and "
-                        "footprints made on the device (tg_crater_batch_device, its plan copied "
-                        "in from page-locked memory), boulder placement (tg_boulder_generate) "
+            "includes": "every step: crater population, wall terraces and massif peaks on "
+                        f"{os.cpu_count()} host threads, then the apply order, the records, their "
+                        "data and footprints made on the device (tg_crater_batch_device, its plan "
+                        "copied in from page-locked memory), boulder placement (tg_boulder_generate) "
                         "on the host and copied in, tg_evaluate on the device and the heights "
                         "copied out to page-locked memory; the next step's batch is made while "
                         "this step evaluates",

@@ -509,14 +509,15 @@ int tg_crater_batch(const tg_crater_population* population, const tg_crater_shap
                     float* data, size_t data_capacity, double* footprints, size_t* n_records,
                     size_t* n_data);
 
-/* tg_crater_batch with the records made on the device: the population, the apply order and the
- * wall terraces and massif peaks of the craters that carry them are made on the host threads as
- * tg_crater_batch makes them, then one device thread per crater draws its outline, takes its
- * footprint and writes its record, data floats and footprint; `records`, `data` and `footprints`
+/* tg_crater_batch with the apply order and the records made on the device: the population and
+ * the wall terraces and massif peaks of the craters that carry them are made on the host threads
+ * as tg_crater_batch makes them, the apply order by stable radix sorts on the device, then one
+ * device thread per crater draws its outline, takes its footprint and writes its record, data
+ * floats and footprint; `records`, `data` and `footprints`
  * are device memory (any may be null; all null asks for the sizes), `kernel` host memory. The
  * outputs are tg_crater_batch's byte for byte. Ordered on `stream` (the device's own when null);
  * the call synchronizes it once, to read the sizes; `staged_bytes` (may be null) receives the bytes
- * it copied to the device (56 per crater of the apply order, 4 per terrace or peak float). Replaces
+ * it copied to the device (64 per candidate crater, 4 per terrace or peak float). Replaces
  * the same host work as tg_crater_batch
  * (MakeCraterKernelBatch, src/layers/craters/shaping/crater_kernel.cpp:187-622, after
  * PrepareCraters, src/layers/craters/shaping/prepared.cpp:60). TG_ERROR_ARGUMENT, the sizes set,

@@ -93,6 +93,7 @@ enum Slot {
     kExtrasList,
     kRecordCraters,  // the device record builder's plan: craters, then extras
     kRecordCounts,   // its records and floats per crater, then their scans
+    kRecordSort,     // the apply order's keys, orders and sort scratch
     kSlotCount
 };
 

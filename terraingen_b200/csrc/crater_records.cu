@@ -1,14 +1,18 @@
-// Crater kernel records built on the device: MakeCraterKernelBatch's per-crater work
-// (src/layers/craters/shaping/crater_kernel.cpp:187-622, irregularity.cpp:165-300) for a batch
-// whose population, candidates, apply order, wall terraces and massif peaks the host has made
-// (population.cpp record_plan). One thread per crater draws its outline (Philox4x32-10 on its
-// irregularity stream), takes its exact footprint and writes its record, its harmonics, its
-// extras and its footprint at offsets an exclusive scan gives, so the batch is tg_crater_batch's
-// byte for byte: every operation here is IEEE double arithmetic the host does in the same order
-// (this unit is compiled with -fmad=false), and the only libm work of a record, the terraces'
-// and peaks' trigonometry, stays on the host.
+// Crater kernel records built on the device: CraterApplyOrder and MakeCraterKernelBatch's
+// per-crater work (src/layers/craters/shaping/crater_kernel.cpp:187-622, irregularity.cpp:
+// 165-300, apply_options.cpp:96) for a batch whose population, candidates, wall terraces and
+// massif peaks the host has made (population.cpp record_plan). The apply order (age descending,
+// then diameter descending, id, draw index) is three stable radix sorts of 64-bit keys, least
+// significant first, from the draw order. Then one thread per crater, in apply order, draws its
+// outline (Philox4x32-10 on its irregularity stream), takes its exact footprint and writes its
+// record, its harmonics, its extras and its footprint at offsets an exclusive scan gives, so the
+// batch is tg_crater_batch's byte for byte: every operation here is IEEE double arithmetic the
+// host does in the same order (this unit is compiled with -fmad=false), and the only libm work of
+// a record, the terraces' and peaks' trigonometry, stays on the host.
 
 #include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cstring>
@@ -177,15 +181,37 @@ __device__ __forceinline__ uint32_t crater_key(uint64_t id, uint32_t seed) {  //
     return noise::pcg(uint32_t(id) ^ noise::pcg(uint32_t(id >> 32u) ^ seed));
 }
 
-// Pass 1: each crater's record (1 or 0) and data floats.
-__global__ void record_count_kernel(const RecordCrater* __restrict__ craters, uint32_t n,
+// The apply order's sort keys, as unsigned integers in ascending order: `field` 0 the id, 1 the
+// diameter descending, 2 the age descending (both positive doubles, whose bits order as their
+// values, complemented), read through the order so far (`order`; null: the draw order, which
+// `orderOut` then receives).
+__global__ void order_keys_kernel(const RecordCrater* __restrict__ craters, uint32_t n,
+                                  const uint32_t* __restrict__ order, int field,
+                                  uint64_t* __restrict__ keys, uint32_t* __restrict__ orderOut) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const uint32_t at = order != nullptr ? order[i] : i;
+    if (order == nullptr) {
+        orderOut[i] = i;
+    }
+    const RecordCrater& c = craters[at];
+    keys[i] = field == 0   ? c.id
+              : field == 1 ? ~uint64_t(__double_as_longlong(c.diameter))
+                           : ~uint64_t(__double_as_longlong(c.age));
+}
+
+// Pass 1: each crater's record (1 or 0) and data floats, in apply order.
+__global__ void record_count_kernel(const RecordCrater* __restrict__ craters,
+                                    const uint32_t* __restrict__ order, uint32_t n,
                                     const RecordConstants k, uint32_t* __restrict__ records,
                                     uint32_t* __restrict__ floats) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
         return;
     }
-    const RecordCrater c = craters[i];
+    const RecordCrater c = craters[order[i]];
     DeviceOutline o;
     double resolution, reach;
     const bool kept = crater_reach(k, c, o, resolution, reach);
@@ -194,7 +220,8 @@ __global__ void record_count_kernel(const RecordCrater* __restrict__ craters, ui
 }
 
 // Pass 2: the records, data and footprints at the scanned offsets (nothing past a capacity).
-__global__ void record_write_kernel(const RecordCrater* __restrict__ craters, uint32_t n,
+__global__ void record_write_kernel(const RecordCrater* __restrict__ craters,
+                                    const uint32_t* __restrict__ order, uint32_t n,
                                     const RecordConstants k, const float* __restrict__ extras,
                                     const uint32_t* __restrict__ recordAt,
                                     const uint32_t* __restrict__ dataAt, size_t recordCapacity,
@@ -204,7 +231,7 @@ __global__ void record_write_kernel(const RecordCrater* __restrict__ craters, ui
     if (i >= n || recordAt[i + 1] == recordAt[i]) {
         return;
     }
-    const RecordCrater c = craters[i];
+    const RecordCrater c = craters[order[i]];
     DeviceOutline o;
     double resolution, reach;
     crater_reach(k, c, o, resolution, reach);
@@ -365,15 +392,48 @@ int tg_crater_batch_device(tg_device* d, const tg_crater_population* spec,
         *staged_bytes = craterBytes + extraBytes;
     }
     const uint32_t blocks = uint32_t((n + 255) / 256);
-    record_count_kernel<<<blocks, 256, 0, s>>>(dCraters, uint32_t(n), k, recordAt, dataAt);
+    // CraterApplyOrder: stable sorts by the id, then the diameter descending, then the age
+    // descending, from the draw order (the last key of the comparison).
+    size_t sortBytes = 0;
+    TG_CUDA(cub::DeviceRadixSort::SortPairs(
+                nullptr, sortBytes, static_cast<const uint64_t*>(nullptr),
+                static_cast<uint64_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                static_cast<uint32_t*>(nullptr), uint32_t(n), 0, 64, s),
+            "sort size");
+    const size_t keyBytes = (n * sizeof(uint64_t) + 255) / 256 * 256;
+    const size_t orderBytes = (n * sizeof(uint32_t) + 255) / 256 * 256;
+    TG_CUDA(d->slots[kRecordSort].reserve(2 * keyBytes + 2 * orderBytes + sortBytes),
+            "allocation");
+    char* sortBase = static_cast<char*>(d->slots[kRecordSort].ptr);
+    uint64_t* keys[2] = {reinterpret_cast<uint64_t*>(sortBase),
+                         reinterpret_cast<uint64_t*>(sortBase + keyBytes)};
+    uint32_t* order[2] = {reinterpret_cast<uint32_t*>(sortBase + 2 * keyBytes),
+                          reinterpret_cast<uint32_t*>(sortBase + 2 * keyBytes + orderBytes)};
+    void* sortTemp = sortBase + 2 * keyBytes + 2 * orderBytes;
+    int cur = 0;  // order[cur] holds the order so far
+    for (int field = 0; field < 3; ++field) {
+        order_keys_kernel<<<blocks, 256, 0, s>>>(dCraters, uint32_t(n),
+                                                 field == 0 ? nullptr : order[cur], field, keys[0],
+                                                 order[cur]);
+        TG_CUDA(cudaGetLastError(), "order keys launch");
+        size_t bytes = sortBytes;
+        TG_CUDA(cub::DeviceRadixSort::SortPairs(sortTemp, bytes, keys[0], keys[1], order[cur],
+                                                order[cur ^ 1], uint32_t(n), 0, 64, s),
+                "sort");
+        cur ^= 1;
+    }
+    const uint32_t* applyOrder = order[cur];
+    record_count_kernel<<<blocks, 256, 0, s>>>(dCraters, applyOrder, uint32_t(n), k, recordAt,
+                                               dataAt);
     TG_CUDA(cudaGetLastError(), "record count launch");
     uint32_t* scratch = static_cast<uint32_t*>(d->slots[kScan].ptr);
     TG_CUDA(launch_exclusive_scan(recordAt, uint32_t(n), scratch, s), "scan launch");
     TG_CUDA(launch_exclusive_scan(dataAt, uint32_t(n), scratch, s), "scan launch");
     if (!query) {
         record_write_kernel<<<blocks, 256, 0, s>>>(
-            dCraters, uint32_t(n), k, dExtras, recordAt, dataAt, records ? record_capacity : 0,
-            data ? data_capacity : 0, static_cast<CraterRecord*>(records), data, footprints);
+            dCraters, applyOrder, uint32_t(n), k, dExtras, recordAt, dataAt,
+            records ? record_capacity : 0, data ? data_capacity : 0,
+            static_cast<CraterRecord*>(records), data, footprints);
         TG_CUDA(cudaGetLastError(), "record write launch");
     }
     // The totals (the scans' last words) back to the host: the one synchronization.

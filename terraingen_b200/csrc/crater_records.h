@@ -11,9 +11,11 @@
 
 namespace tgb {
 
-// One crater of a batch, in apply order (CraterApplyOrder, apply_options.cpp:96).
+// One candidate crater of a batch, in the population's draw order (the device puts them in
+// CraterApplyOrder, apply_options.cpp:96).
 struct RecordCrater {
     double x, y, diameter;
+    double age;             // Gyr (the apply order's first key)
     double erosion;         // the share of the fresh depth and rim left (FreshnessDegradation)
     uint64_t id;
     uint32_t extraOffset;   // its terrace floats, then its peak floats, in the plan's extras
@@ -22,7 +24,7 @@ struct RecordCrater {
     uint16_t terraceCount;  // AppendKernelTerraces' benches (0: none)
     uint16_t peakCount;     // AppendKernelPeaks' massifs (0: none)
 };
-static_assert(sizeof(RecordCrater) == 56, "RecordCrater is 56 bytes");
+static_assert(sizeof(RecordCrater) == 64, "RecordCrater is 64 bytes");
 
 // The constants of a batch's records (MakeCraterKernelBatch under the batch's shaping).
 struct RecordConstants {
@@ -39,11 +41,11 @@ struct RecordConstants {
 
 namespace host {
 
-// tg_crater_batch up to its records: the population drawn over the grid's bounds, the
-// candidates, the apply order, and for every candidate that carries them its wall terraces and
-// massif peaks (built as tg_crater_batch builds them); `kernel` (when not null) receives the
-// batch's CraterShapeKernel. The craters in apply order go where `place(n)` says (room for n,
-// or null to refuse: TG_ERROR_MEMORY), their extras into `extras`. `n` receives their number.
+// tg_crater_batch up to its records, less the apply order: the population drawn over the grid's
+// bounds, the candidates, and for every candidate that carries them its wall terraces and massif
+// peaks (built as tg_crater_batch builds them); `kernel` (when not null) receives the batch's
+// CraterShapeKernel. The candidates, in draw order, go where `place(n)` says (room for n, or
+// null to refuse: TG_ERROR_MEMORY), their extras into `extras`. `n` receives their number.
 // Returns a TG_* status.
 int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shaping,
                 const tg_grid& grid, void* kernel, RecordConstants& constants,

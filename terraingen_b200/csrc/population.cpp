@@ -1321,7 +1321,8 @@ int batch_setup(const tg_crater_population& spec, const tg_crater_shaping& shapi
 // The batch's craters in apply order: the population drawn over the grid's bounds, the
 // candidates kept as they are drawn, the order by the ages' buckets (work.craters and, in apply
 // order, their indices work.sorted).
-int batch_order(const BatchSetup& setup, const tg_grid& grid, unsigned threads, BatchWork& work) {
+int batch_order(const BatchSetup& setup, const tg_grid& grid, unsigned threads, BatchWork& work,
+                bool order = true) {
     // The craters that can give a record: a resolution weight above 0 and a footprint, grown
     // to the largest outline scale any crater can draw (MaxOutlineScale, irregularity.cpp:
     // 279, the bound the reference's own binning takes), that holds a cell of the grid. The
@@ -1341,6 +1342,9 @@ int batch_order(const BatchSetup& setup, const tg_grid& grid, unsigned threads, 
                   craters);
     if (craters.size() >= (size_t(1) << 32)) {
         return TG_ERROR_UNSUPPORTED;
+    }
+    if (!order) {
+        return TG_OK;
     }
     const size_t nKept = craters.size();
     // The ages' range, by parts of 4096 craters on the host threads.
@@ -1503,7 +1507,7 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
     const unsigned threads = host_threads();
     static thread_local BatchWork workspace;
     BatchWork& work = workspace;
-    if (int st = batch_order(setup, grid, threads, work)) {
+    if (int st = batch_order(setup, grid, threads, work, false)) {
         return st;
     }
     if (kernel != nullptr) {
@@ -1537,7 +1541,7 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
     const uint32_t peakSeed = substream_seed(spec.seed, kCraterPeakStream);
     const double freshDepth = spec.depth_ratio, freshRim = spec.rim_ratio;
     const double floorShare = std::fmin(spec.cutoff_depth_ratio / freshDepth, 1.0);
-    const size_t n = work.sorted.size();
+    const size_t n = work.craters.size();
     count = n;
     RecordCrater* out = place(n);
     if (out == nullptr && n > 0) {
@@ -1556,16 +1560,13 @@ int record_plan(const tg_crater_population& spec, const tg_crater_shaping& shapi
         values.clear();
         const size_t end = std::min(n, (b + 1) * kBlock);
         for (size_t q = b * kBlock; q < end; ++q) {
-            if (q + 16 < end) {
-                __builtin_prefetch(&work.craters[work.sorted[q + 16]]);  // apply order gathers
-            }
-            const Crater& c = work.craters[work.sorted[q]];
+            const Crater& c = work.craters[q];
             // FreshnessDegradation::State with constant fresh morphometry and uniform ages.
             const double remaining = std::clamp(1.0 - c.age / spec.lifetime_gyr, 0.0, 1.0);
             const double erosion = floorShare + (1.0 - floorShare) * remaining;
             RecordCrater& r = out[q];
-            r = RecordCrater{c.x, c.y, c.diameter, erosion, c.id, uint32_t(values.size()), 0u, 0u,
-                             0u, 0u};
+            r = RecordCrater{c.x, c.y, c.diameter, c.age, erosion, c.id,
+                             uint32_t(values.size()), 0u, 0u, 0u, 0u};
             const bool terraced = c.diameter >= setup.terraces.onset;  // else none drawn
             const bool complex = setup.profile.is_complex(c.diameter);
             if (!setup.irregular || (!terraced && !complex)) {

@@ -108,3 +108,34 @@ def test_device_records_empty_batch(device):
     torch.cuda.synchronize()
     assert (nr, nd) == (0, 1) and float(out[0]) == 0.0
     assert got.tobytes() == kernel.tobytes()
+
+
+def test_evaluate_with_device_records_equals_host_records(device):
+    # The e2e path: the batch made on the device and evaluated in device memory gives the heights
+    # of the host-built batch evaluated with host buffers, bit for bit.
+    import torch
+
+    from terraingen_b200.layouts import fractal
+    from terraingen_b200.workloads import boulder_population, generate_boulders
+
+    grid = centered(1025, 769, 0.5, 120.0, -40.0)
+    pop, shaping = _terrain_population(), config2_shaping()
+    fractals = np.array([fractal(seed=7, wavelength=512.0, amplitude=5.0, octaves=8)])
+    full_area = (4097 * 0.5) ** 2
+    stones = generate_boulders(boulder_population(7, 1e6 / (full_area * (0.2 ** -2.5 -
+                                                                          3.0 ** -2.5))), grid)
+    kernel, records, data, foot = crater_batch(pop, grid, shaping=shaping)
+    want = np.zeros((grid.height, grid.width), np.float32)
+    device.evaluate(grid, want, fractals=fractals, craters=(kernel, records, data, foot),
+                    boulders=stones, boulder_width=0.5)
+    got_kernel, rec_d, data_d, foot_d = _device_batch(device, pop, shaping, grid)
+    cuda = dict(device="cuda")
+    heights = torch.empty((grid.height, grid.width), dtype=torch.float32, **cuda)
+    device.evaluate(grid, heights, fractals=fractals,
+                    craters=(got_kernel, torch.from_numpy(rec_d).to(**cuda),
+                             torch.from_numpy(data_d).to(**cuda),
+                             torch.from_numpy(foot_d).to(**cuda)),
+                    boulders=torch.from_numpy(np.ascontiguousarray(stones).ravel()).to(**cuda),
+                    boulder_width=0.5)
+    torch.cuda.synchronize()
+    assert np.array_equal(heights.cpu().numpy().view(np.uint32), want.view(np.uint32))
