@@ -8,9 +8,12 @@ form on a camera request stream and the DEM refinement, each against the plain p
 
 A step evaluates one whole tile: the source fill, the crater layer and the boulder layer.
 `value` is device-resident throughput (layer inputs already in HBM). `e2e` starts each step from
-the layers' definitions: the crater batch (population, apply order, records) and the boulders are
-built on the host threads and the tile is evaluated through the public C ABI with host buffers
-(tg_evaluate: inputs copied in from pinned memory, heights copied out). `dropin` times the
+the layers' definitions through the public C ABI: the crater batch (population, terraces and
+peaks on the host threads, apply order and records on the device: tg_crater_batch_device, its
+plan copied in from pinned memory), the boulders placed on the host and copied in, the tile
+evaluated (tg_evaluate) and its heights copied out to pinned memory; `e2e.host_records` is the
+same with the batch made on the host (tg_crater_batch) and every input passed as host buffers
+(inputs copied in, heights copied out inside tg_evaluate). `dropin` times the
 reference's own Terrain::Evaluate with Backend::Cuda on this library against Backend::Cpu. With N
 ranks each rank evaluates its own tile, with no exchange (weak scaling); `--gpus N` without
 torchrun starts the N ranks itself. `--impl reference` times the reference CPU path on a bounded
