@@ -51,8 +51,8 @@ NOISE_OPS_PER_CELL_OCTAVE = 180
 # cos, amplitude, kept share's pow, product, sum) 77, scale and division 2, reach test 1, profile
 # 8, resolution and the add 2: 104, plus the ellipse of 5 % of craters (10): 105.
 CRATER_OPS_PER_PAIR = 105
-# Thread instructions the lean crater kernel executes per pair, measured (ncu smsp__inst_executed
-# x active lanes / pairs: 771.3 M x 29.79 / 64,216,893, profiles/terrain4097_crater_lean.md): the
+# Thread instructions the lean crater kernel executes per pair, measured with ncu on this
+# workload (smsp__inst_executed x active lanes / pairs: 771.3 M x 29.79 / 64,216,893): the
 # issue-rate view of the same work (loads, the queue, compares and selects).
 CRATER_THREAD_INST_PER_PAIR = 358
 # Counted from terraingen_b200/csrc/boulders.cu per (cell, boulder) pair: window test 6, offset
