@@ -58,9 +58,9 @@ CRATER_THREAD_INST_PER_PAIR = 358
 # Counted from terraingen_b200/csrc/boulders.cu per (cell, boulder) pair: window test 6, offset
 # and hypot 12, dome band average (2 sqrt, 2 asin, clamps) 60, max-composite 4; FP64.
 BOULDER_OPS_PER_PAIR = 82
-# DRAM bytes per launch from the ncu captures of this workload (profiles/terrain4097_kernels.md;
-# the crater figure is the lean shaping kernel, profiles/terrain4097_crater_lean.md).
-TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 112.7e6 + 24.1e6, "boulders": 61.9e6 + 7.9e6}
+# DRAM bytes (read + write) per launch from the ncu captures of this workload: the fBm kernel,
+# the lean crater shaping kernel (as built now: 113.3 + 25.9 MB) and the boulder bake.
+TRAFFIC = {"noise": 0.062e6 + 10.28e6, "craters": 113.33e6 + 25.86e6, "boulders": 61.9e6 + 7.9e6}
 L2_FLUSH_BYTES = 256 << 20
 
 
